@@ -1,0 +1,103 @@
+/*
+ * pwdft_b200 -- C ABI of the B200-native PWDFT Hamiltonian / eigensolver path.
+ *
+ * Every entry point returns an int status (PW_OK = 0, negative on error) and
+ * never lets a C++ exception cross the boundary; pw_last_error() returns the
+ * message of the last failure on the calling thread.  Sizes are 32-bit ints
+ * like the reference's `Int` (include/environment.hpp:136).  Wavefunction
+ * blocks are column-major N_grid x nband with leading dimension ld, each band
+ * contiguous, exactly the layout of the reference's NumTns<Real>(ntot, ncom=1,
+ * nband) (include/spinor.hpp:80, src/SCF/spinor.cpp:127-133).  Grid index is
+ * i + n0*j + n0*n1*k (x fastest).  A context has one arithmetic precision:
+ * PW_F64 (double buffers) or PW_F32 (float buffers); "device" pointers are
+ * CUDA device memory, "host" pointers are ordinary host memory.
+ */
+#ifndef PWDFT_B200_H
+#define PWDFT_B200_H
+
+#if defined(__GNUC__)
+#define PW_API __attribute__((visibility("default")))
+#else
+#define PW_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  PW_OK = 0,
+  PW_EINVAL = -1,        /* bad argument / size mismatch (reference: ErrorHandling) */
+  PW_ECUDA = -2,         /* CUDA runtime error */
+  PW_ENOMEM = -3,        /* device allocation failed */
+  PW_EUNSUPPORTED = -4,  /* grid size or configuration not built into this library */
+  PW_ETIMEOUT = -5,      /* a bounded device-side wait gave up */
+  PW_ENOTREADY = -6,     /* required tables (potential, projectors) not set */
+  PW_ENUMERIC = -7       /* numerical breakdown (e.g. Cholesky of a singular Gram) */
+};
+
+enum { PW_F64 = 0, PW_F32 = 1 };
+
+typedef struct pw_ctx pw_ctx;
+
+/* Message of the last failed call on this thread ("" if none). */
+PW_API const char* pw_last_error(void);
+/* Library version string. */
+PW_API const char* pw_version(void);
+
+/* Create a context for an orthorhombic cell with coarse (wavefunction) grid
+ * numGrid and fine (density) grid numGridFine = 2*numGrid.  Replaces
+ * Fourier::Initialize / Fourier::InitializeFine (src/SCF/fourier.cpp:97-244,
+ * 246-418) and KohnSham::CalculateEkin (src/SCF/hamiltonian.cpp:2630-2667):
+ * builds |G|^2/2 and the Teter table on the device. */
+PW_API int pw_ctx_create(const double length[3], const int numGrid[3], const int numGridFine[3],
+                  int precision, int device, pw_ctx** out);
+PW_API int pw_ctx_destroy(pw_ctx* ctx);
+/* Query grid totals: ntot (coarse), ntotFine. */
+PW_API int pw_ctx_sizes(const pw_ctx* ctx, long* ntot, long* ntotFine);
+
+/* Total local potential on the fine grid (host, double, N_fine values).
+ * Replaces the vtot argument of Spinor::AddMultSpinorFineR2C
+ * (src/SCF/spinor.cpp:377-378, copied per call at hamiltonian.cpp:3121-3122). */
+PW_API int pw_set_vtot(pw_ctx* ctx, const double* vtot_fine_host);
+
+/* Real-space nonlocal projectors, the flat form of std::vector<PseudoPot>
+ * with vnlList = vector<pair<SparseVec,Real>> (include/periodtable.hpp:62-63,
+ * include/utility.hpp:127-151), as built by PeriodTable::CalculateNonlocalPP
+ * (src/SCF/periodtable.cpp:994-1240).  For atom a: atom_npts[a] fine-grid
+ * indices (one index set shared by all projectors of the atom), atom_nproj[a]
+ * projectors.  idx: concatenation over atoms of the index sets.  beta:
+ * concatenation over atoms of nproj x npts VAL columns (projector-major).
+ * weight: concatenation over atoms of the nproj vnlList weights (gamma).
+ * All host pointers. */
+PW_API int pw_set_nonlocal(pw_ctx* ctx, int natom, const int* atom_npts, const int* atom_nproj,
+                    const int* idx, const double* beta, const double* weight);
+
+/* H*psi for nband bands: hpsi (+)= (-1/2 Laplacian + V_loc + V_nl) psi.
+ * Replaces Spinor::AddMultSpinorFineR2C(fft, ekin, vtot, pseudo, a3)
+ * (src/SCF/spinor.cpp:377-525; accumulate=1 gives its a3 += semantics) and
+ * KohnSham::MultSpinor without hybrid exchange (src/SCF/hamiltonian.cpp:
+ * 3059-3268; accumulate=0 overwrites a3).  psi, hpsi: device pointers of the
+ * context's precision.  stream: cudaStream_t (NULL = legacy default). */
+PW_API int pw_hpsi(pw_ctx* ctx, const void* psi, int ld, void* hpsi, int ldh, int nband,
+            int accumulate, void* stream);
+
+/* Same as pw_hpsi with host buffers: copies psi in and hpsi out around the
+ * device computation (the path a host-side reference caller binds). */
+PW_API int pw_hpsi_host(pw_ctx* ctx, const void* psi, int ld, void* hpsi, int ldh, int nband,
+                 int accumulate);
+
+/* Teter preconditioner: w (+)= C2R(teter * R2C(r)).  Replaces
+ * Spinor::AddTeterPrecond(Fourier*, DblNumVec& teter, NumTns<Real>& a3)
+ * (src/SCF/spinor.cpp:310-346). Device pointers. */
+PW_API int pw_teter_precond(pw_ctx* ctx, const void* r, int ld, void* w, int ldw, int nband,
+                     int accumulate, void* stream);
+
+/* Maximum number of bands processed per internal batch (sets scratch size).
+ * Default 64. Scratch grows to hold ceil(nband_batch/2) band pairs. */
+PW_API int pw_set_band_batch(pw_ctx* ctx, int nband_batch);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PWDFT_B200_H */

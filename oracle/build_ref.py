@@ -1,0 +1,110 @@
+"""Compile standalone reference functions into ``oracle/_ref/libpwref.so``.
+
+Test infrastructure.  The reference's full build needs MPI, FFTW, MKL,
+libxc and yaml-cpp, which are absent, so it cannot be built.  Four of its
+functions are self-contained and are compiled here directly from the
+reference source tree (never copied into this repository): ``spline`` and
+``seval`` (src/utility.cpp:54-225) and ``IP_c2f`` / ``IP_f2c``
+(src/utility.cpp:3148-3275).  The recipe extracts each function body from
+``<reference>/src/utility.cpp`` by brace matching into ``oracle/_ref/`` (git
+ignored), prepends the two typedefs it needs, adds extern "C" wrappers and
+builds a shared object with g++.  Tests use it to pin the NumPy restatement.
+"""
+from __future__ import annotations
+
+import os
+import re
+import subprocess
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+OUT = HERE / "_ref"
+LIB = OUT / "libpwref.so"
+DEFAULT_REF = Path(os.environ.get("PWDFT_REFERENCE", "/root/reference"))
+
+FUNCS = [("void spline(", "spline"), ("void seval(", "seval"),
+         ("void IP_c2f(", "IP_c2f"), ("void IP_f2c(", "IP_f2c")]
+
+PRELUDE = """// generated: functions compiled from the reference source tree
+#include <complex>
+#include <stdexcept>
+typedef std::complex<double> Complex;
+static void ErrorHandling(const char* m) { throw std::runtime_error(m); }
+namespace pwref {
+"""
+
+WRAPPERS = """
+}  // namespace pwref
+extern "C" {
+void ref_spline(int n, double* x, double* y, double* b, double* c, double* d) { pwref::spline(n, x, y, b, c, d); }
+void ref_seval(double* v, int m, double* u, int n, double* x, double* y, double* b, double* c, double* d) {
+  pwref::seval(v, m, u, n, x, y, b, c, d);
+}
+void ref_ip_c2f(int* Nc, int* Nf, double* tilde, double* tildef) {
+  pwref::IP_c2f(Nc, Nf, reinterpret_cast<Complex*>(tilde), reinterpret_cast<Complex*>(tildef));
+}
+void ref_ip_f2c(int* Nc, int* Nf, double* tilde, double* tildef) {
+  pwref::IP_f2c(Nc, Nf, reinterpret_cast<Complex*>(tilde), reinterpret_cast<Complex*>(tildef));
+}
+}
+"""
+
+
+def _strip_comments(text: str) -> str:
+    """Blank out /* */ and // comments (keeping newlines) so that commented-out
+    definitions (e.g. the disabled "method I" IP_c2f at src/utility.cpp:2980-3144)
+    are not picked up."""
+    out, i, n = [], 0, len(text)
+    while i < n:
+        if text.startswith("/*", i):
+            j = text.find("*/", i + 2)
+            j = n if j < 0 else j + 2
+            out.append("".join(ch if ch == "\n" else " " for ch in text[i:j]))
+            i = j
+        elif text.startswith("//", i):
+            j = text.find("\n", i)
+            j = n if j < 0 else j
+            out.append(" " * (j - i))
+            i = j
+        else:
+            out.append(text[i])
+            i += 1
+    return "".join(out)
+
+
+def _extract(text: str, head: str) -> str:
+    i = text.find(head)
+    if i < 0:
+        raise RuntimeError(f"function {head!r} not found")
+    j = text.find("{", i)
+    depth = 0
+    k = j
+    while True:
+        ch = text[k]
+        if ch == "{":
+            depth += 1
+        elif ch == "}":
+            depth -= 1
+            if depth == 0:
+                break
+        k += 1
+    return text[i:k + 1]
+
+
+def build(ref_root: Path = DEFAULT_REF) -> Path | None:
+    src = ref_root / "src" / "utility.cpp"
+    if not src.exists():
+        return LIB if LIB.exists() else None
+    text = _strip_comments(src.read_text(errors="replace"))
+    body = [_extract(text, h) for h, _ in FUNCS]
+    OUT.mkdir(exist_ok=True)
+    cpp = OUT / "ref_funcs.cpp"
+    cpp.write_text(PRELUDE + "\n\n".join(body) + WRAPPERS)
+    r = subprocess.run(["g++", "-O2", "-fPIC", "-shared", "-o", str(LIB), str(cpp)], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(r.stderr)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build())

@@ -1,0 +1,59 @@
+"""ctypes binding of ``libpwdft_b200.so`` (the C ABI in include/pwdft_b200.h).
+
+The library is required: importing this module raises if the shared object
+is missing, and every call that returns a non-zero status raises
+``PwError`` with the library's message.  There is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libpwdft_b200.so"
+
+PW_OK, PW_EINVAL, PW_ECUDA, PW_ENOMEM, PW_EUNSUPPORTED, PW_ETIMEOUT, PW_ENOTREADY, PW_ENUMERIC = \
+    0, -1, -2, -3, -4, -5, -6, -7
+PW_F64, PW_F32 = 0, 1
+
+
+class PwError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"pwdft_b200 error {code}: {msg}")
+        self.code = code
+
+
+def _load() -> C.CDLL:
+    if not LIB_PATH.exists():
+        raise ImportError(f"{LIB_PATH} is missing: run pwdft_develop_b200.build.build() (nvcc, sm_100a)")
+    return C.CDLL(str(LIB_PATH))
+
+
+lib = _load()
+
+_vp, _i, _l, _d = C.c_void_p, C.c_int, C.c_long, C.c_double
+_ip, _dp = C.POINTER(C.c_int), C.POINTER(C.c_double)
+
+# name -> (restype, argtypes); every name here is declared in include/pwdft_b200.h
+SIGNATURES: dict[str, tuple] = {
+    "pw_last_error": (C.c_char_p, []),
+    "pw_version": (C.c_char_p, []),
+    "pw_ctx_create": (_i, [_dp, _ip, _ip, _i, _i, C.POINTER(_vp)]),
+    "pw_ctx_destroy": (_i, [_vp]),
+    "pw_ctx_sizes": (_i, [_vp, C.POINTER(_l), C.POINTER(_l)]),
+    "pw_set_vtot": (_i, [_vp, _dp]),
+    "pw_set_nonlocal": (_i, [_vp, _i, _ip, _ip, _ip, _dp, _dp]),
+    "pw_hpsi": (_i, [_vp, _vp, _i, _vp, _i, _i, _i, _vp]),
+    "pw_hpsi_host": (_i, [_vp, _vp, _i, _vp, _i, _i, _i]),
+    "pw_teter_precond": (_i, [_vp, _vp, _i, _vp, _i, _i, _i, _vp]),
+    "pw_set_band_batch": (_i, [_vp, _i]),
+}
+
+for _name, (_res, _args) in SIGNATURES.items():
+    _f = getattr(lib, _name)
+    _f.restype = _res
+    _f.argtypes = _args
+
+
+def check(rc: int) -> None:
+    if rc != PW_OK:
+        raise PwError(rc, lib.pw_last_error().decode(errors="replace"))

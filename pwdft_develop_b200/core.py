@@ -1,0 +1,134 @@
+"""Python host mirror of the reference's Fourier / Spinor / Hamiltonian entry
+points for the real (Gamma-point) H*psi path, over the C ABI.
+
+Device buffers are torch CUDA tensors of shape (nband, ntot) -- band-major
+rows, i.e. the column-major ntot x nband layout of the reference's
+NumTns<Real>(ntot, 1, nband) -- and are passed to the library as raw
+pointers.  torch is used only for device memory and streams.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import PW_F32, PW_F64, check, lib
+
+
+def _ptr(t) -> C.c_void_p:
+    return C.c_void_p(t.data_ptr())
+
+
+def _stream(stream) -> C.c_void_p:
+    if stream is None:
+        import torch
+        stream = torch.cuda.current_stream()
+    return C.c_void_p(stream.cuda_stream)
+
+
+class Context:
+    """One cell + grid + precision.  Mirrors ``Fourier::Initialize /
+    InitializeFine`` (src/SCF/fourier.cpp:97-418) and the tables
+    ``KohnSham`` owns (ekin_, teter_, vtot_, pseudo_)."""
+
+    def __init__(self, length, numGrid, numGridFine, precision: str = "f64", device: int = 0):
+        self.precision = precision
+        prec = PW_F64 if precision == "f64" else PW_F32
+        L = (C.c_double * 3)(*[float(x) for x in length])
+        n = (C.c_int * 3)(*[int(x) for x in numGrid])
+        nf = (C.c_int * 3)(*[int(x) for x in numGridFine])
+        h = C.c_void_p()
+        check(lib.pw_ctx_create(L, n, nf, prec, device, C.byref(h)))
+        self._h = h
+        nt, ntf = C.c_long(), C.c_long()
+        check(lib.pw_ctx_sizes(h, C.byref(nt), C.byref(ntf)))
+        self.ntot, self.ntotFine = nt.value, ntf.value
+        self.numGrid = tuple(int(x) for x in numGrid)
+        self.numGridFine = tuple(int(x) for x in numGridFine)
+        self.length = tuple(float(x) for x in length)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib.pw_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def np_dtype(self):
+        return np.float64 if self.precision == "f64" else np.float32
+
+    @property
+    def torch_dtype(self):
+        import torch
+        return torch.float64 if self.precision == "f64" else torch.float32
+
+    # -- tables ---------------------------------------------------------
+    def set_vtot(self, vtot: np.ndarray):
+        v = np.ascontiguousarray(vtot, dtype=np.float64).ravel()
+        if v.size != self.ntotFine:
+            raise ValueError("vtot must have ntotFine entries")
+        check(lib.pw_set_vtot(self._h, v.ctypes.data_as(_lib._dp)))
+
+    def set_nonlocal(self, atoms):
+        """atoms: list of (idx[npts], beta[nproj, npts], weight[nproj]) --
+        one entry per atom, the flat form of PseudoPot::vnlList."""
+        natom = len(atoms)
+        npts = np.array([len(a[0]) for a in atoms], dtype=np.int32)
+        nproj = np.array([len(a[2]) for a in atoms], dtype=np.int32)
+        idx = np.ascontiguousarray(np.concatenate([np.asarray(a[0], np.int32) for a in atoms])
+                                   if natom else np.zeros(0, np.int32))
+        beta = np.ascontiguousarray(np.concatenate([np.asarray(a[1], np.float64).ravel() for a in atoms])
+                                    if natom else np.zeros(0))
+        wgt = np.ascontiguousarray(np.concatenate([np.asarray(a[2], np.float64) for a in atoms])
+                                   if natom else np.zeros(0))
+        check(lib.pw_set_nonlocal(self._h, natom, npts.ctypes.data_as(_lib._ip), nproj.ctypes.data_as(_lib._ip),
+                                  idx.ctypes.data_as(_lib._ip), beta.ctypes.data_as(_lib._dp),
+                                  wgt.ctypes.data_as(_lib._dp)))
+
+    def set_band_batch(self, nb: int):
+        check(lib.pw_set_band_batch(self._h, int(nb)))
+
+    # -- operators ------------------------------------------------------
+    def hpsi(self, psi, out=None, accumulate: bool = False, stream=None):
+        """Spinor::AddMultSpinorFineR2C / KohnSham::MultSpinor on device
+        tensors of shape (nband, ntot)."""
+        import torch
+        assert psi.is_cuda and psi.dtype == self.torch_dtype and psi.is_contiguous()
+        nb = psi.shape[0]
+        if out is None:
+            out = torch.empty_like(psi)
+            accumulate = False
+        check(lib.pw_hpsi(self._h, _ptr(psi), self.ntot, _ptr(out), self.ntot, nb, int(accumulate), _stream(stream)))
+        return out
+
+    def hpsi_host(self, psi: np.ndarray, out: np.ndarray | None = None, accumulate: bool = False):
+        psi = np.ascontiguousarray(psi, dtype=self.np_dtype)
+        nb = psi.shape[0]
+        if out is None:
+            out = np.zeros_like(psi)
+            accumulate = False
+        check(lib.pw_hpsi_host(self._h, psi.ctypes.data_as(C.c_void_p), self.ntot,
+                               out.ctypes.data_as(C.c_void_p), self.ntot, nb, int(accumulate)))
+        return out
+
+    def teter(self, r, out=None, accumulate: bool = False, stream=None):
+        """Spinor::AddTeterPrecond on device tensors (nband, ntot)."""
+        import torch
+        assert r.is_cuda and r.dtype == self.torch_dtype and r.is_contiguous()
+        nb = r.shape[0]
+        if out is None:
+            out = torch.empty_like(r)
+            accumulate = False
+        check(lib.pw_teter_precond(self._h, _ptr(r), self.ntot, _ptr(out), self.ntot, nb, int(accumulate),
+                                   _stream(stream)))
+        return out

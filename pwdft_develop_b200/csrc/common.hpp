@@ -1,0 +1,86 @@
+// Shared declarations for the pwdft_b200 native library.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/pwdft_b200.h"
+
+namespace pwb {
+
+// Last error message of the calling thread (returned by pw_last_error()).
+void set_error(const std::string& msg);
+
+#define PWB_CUDA(call)                                                              \
+  do {                                                                              \
+    cudaError_t e_ = (call);                                                        \
+    if (e_ != cudaSuccess) {                                                        \
+      ::pwb::set_error(std::string(#call) + ": " + cudaGetErrorString(e_));         \
+      return PW_ECUDA;                                                              \
+    }                                                                               \
+  } while (0)
+
+#define PWB_CHECK(cond, code, msg)                                                  \
+  do {                                                                              \
+    if (!(cond)) {                                                                  \
+      ::pwb::set_error(msg);                                                        \
+      return (code);                                                                \
+    }                                                                               \
+  } while (0)
+
+// Device buffer owned by a context.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  int alloc(size_t nbytes);
+  void release();
+  ~DevBuf() { release(); }
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+};
+
+// Nonlocal projector tables in the fine-plane ("tile") sorted layout used by
+// the gather / apply kernels.  A tile is one fine z-plane and one chunk of
+// CR rows; within a tile entries are grouped by atom ("slots").
+struct NonlocalDev {
+  int natom = 0, npmax = 0, nent = 0, nslot = 0, ntile = 0, cr = 0, nchunk = 0;
+  DevBuf ent_xy;          // int32 [nent]   y*NX + x (fine plane coordinates)
+  DevBuf ent_beta;        // T     [npmax][nent] projector values (VAL column)
+  DevBuf tile_slot;       // int32 [ntile+1]
+  DevBuf slot_atom;       // int32 [nslot]
+  DevBuf slot_ent;        // int32 [nslot+1]
+  DevBuf atom_slot;       // int32 [natom+1]
+  DevBuf atom_slot_list;  // int32 [nslot]
+  DevBuf wgt;             // T     [natom*npmax]  gamma * vol / N_fine
+};
+
+}  // namespace pwb
+
+// Opaque context behind the C ABI.
+struct pw_ctx {
+  int prec = PW_F64;            // PW_F64 or PW_F32 storage / arithmetic
+  double L[3] = {0, 0, 0};      // orthorhombic cell lengths (bohr)
+  double vol = 0;
+  int n[3] = {0, 0, 0};         // coarse (wavefunction) grid
+  int nf[3] = {0, 0, 0};        // fine (density) grid
+  long ntot = 0, ntotf = 0;
+  int device = 0;
+  size_t esz = 8;               // bytes per real
+  // Fourier tables
+  pwb::DevBuf ekin;             // T [n2][n1][n0]  |G|^2/2 on the full coarse spectrum
+  pwb::DevBuf teter;            // T [n2][n1][n0]
+  pwb::DevBuf vtot;             // T [N_fine]
+  pwb::DevBuf tw[6];            // complex T twiddles for n0,n1,n2,nf0,nf1,nf2
+  bool have_vtot = false;
+  bool have_nl = false;
+  pwb::NonlocalDev nl;
+  // host copies kept for setup-time work
+  std::vector<double> h_vtot;
+  // scratch for the band-pair pipeline
+  int pair_cap = 0;
+  pwb::DevBuf s_ad, s_k, s_bc, s_wp, s_w;
+  pwb::DevBuf s_host_in, s_host_out;   // device staging for the host-pointer entry points
+};

@@ -1,0 +1,342 @@
+// Context set-up: Fourier tables, potential, projector tables, scratch, and
+// the C ABI for the H*psi / Teter entry points.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+
+#include "common.hpp"
+#include "fft.cuh"
+
+namespace pwb {
+
+static thread_local std::string g_err;
+void set_error(const std::string& msg) { g_err = msg; }
+
+int DevBuf::alloc(size_t nbytes) {
+  if (nbytes <= bytes && p) return PW_OK;
+  release();
+  if (nbytes == 0) return PW_OK;
+  cudaError_t e = cudaMalloc(&p, nbytes);
+  if (e != cudaSuccess) {
+    p = nullptr;
+    set_error(std::string("cudaMalloc failed: ") + cudaGetErrorString(e));
+    return PW_ENOMEM;
+  }
+  bytes = nbytes;
+  return PW_OK;
+}
+void DevBuf::release() {
+  if (p) cudaFree(p);
+  p = nullptr;
+  bytes = 0;
+}
+
+// defined in hpsi.cu
+struct GridEntry;
+const GridEntry* find_grid(const int n[3]);
+int grid_chunk_rows(const int n[3], int prec);
+int run_hpsi(pw_ctx* c, const void* psi, int ld, void* out, int ldo, int nband, int band0, int npair, int acc,
+             cudaStream_t st);
+int run_teter(pw_ctx* c, const void* r, int ld, void* out, int ldo, int nband, int band0, int npair, int acc,
+              cudaStream_t st);
+
+// upload a double host vector as the context's precision
+int upload_real(pw_ctx* c, DevBuf& dst, const double* src, size_t n) {
+  int rc = dst.alloc(n * c->esz);
+  if (rc) return rc;
+  if (c->prec == PW_F64) {
+    PWB_CUDA(cudaMemcpy(dst.p, src, n * 8, cudaMemcpyHostToDevice));
+  } else {
+    std::vector<float> tmp(n);
+    for (size_t i = 0; i < n; ++i) tmp[i] = (float)src[i];
+    PWB_CUDA(cudaMemcpy(dst.p, tmp.data(), n * 4, cudaMemcpyHostToDevice));
+  }
+  return PW_OK;
+}
+
+static int upload_twiddles(pw_ctx* c, int slot, int n) {
+  std::vector<double> t(2 * n);
+  for (int m = 0; m < n; ++m) {
+    // exact values at the quarter points, cos/sin of 2*pi*m/n elsewhere
+    const double a = 2.0 * M_PI * (double)m / (double)n;
+    double cs = std::cos(a), sn = std::sin(a);
+    if (4 * m == n) { cs = 0; sn = 1; }
+    if (2 * m == n) { cs = -1; sn = 0; }
+    if (4 * m == 3 * n) { cs = 0; sn = -1; }
+    t[2 * m] = cs;
+    t[2 * m + 1] = -sn;
+  }
+  return upload_real(c, c->tw[slot], t.data(), 2 * (size_t)n);
+}
+
+int ensure_scratch(pw_ctx* c, int npair) {
+  if (npair <= c->pair_cap && c->s_ad.p) return PW_OK;
+  const size_t cs = 2 * c->esz;   // complex element
+  const size_t nb = (size_t)c->nf[2] * (c->n[1] + 1) * (c->n[0] + 1);
+  int rc;
+  if ((rc = c->s_ad.alloc((size_t)npair * c->ntot * cs))) return rc;
+  if ((rc = c->s_k.alloc((size_t)npair * c->ntot * cs))) return rc;
+  if ((rc = c->s_bc.alloc((size_t)npair * nb * cs))) return rc;
+  const size_t nslot = std::max(1, c->nl.nslot), nat = std::max(1, c->nl.natom), np = std::max(1, c->nl.npmax);
+  if ((rc = c->s_wp.alloc((size_t)npair * nslot * np * cs))) return rc;
+  if ((rc = c->s_w.alloc((size_t)npair * nat * np * cs))) return rc;
+  c->pair_cap = npair;
+  return PW_OK;
+}
+
+}  // namespace pwb
+
+using namespace pwb;
+
+extern "C" {
+
+const char* pw_last_error(void) { return g_err.c_str(); }
+const char* pw_version(void) { return "pwdft_b200 0.1 (sm_100a)"; }
+
+int pw_ctx_create(const double length[3], const int numGrid[3], const int numGridFine[3], int precision, int device,
+                  pw_ctx** out) {
+  PWB_CHECK(out && length && numGrid && numGridFine, PW_EINVAL, "null argument");
+  *out = nullptr;
+  PWB_CHECK(precision == PW_F64 || precision == PW_F32, PW_EINVAL, "precision must be PW_F64 or PW_F32");
+  for (int d = 0; d < 3; ++d) {
+    PWB_CHECK(length[d] > 0, PW_EINVAL, "cell length must be positive");
+    PWB_CHECK(numGrid[d] > 0 && numGrid[d] % 2 == 0, PW_EINVAL, "coarse grid sizes must be even");
+    PWB_CHECK(numGridFine[d] == 2 * numGrid[d], PW_EUNSUPPORTED,
+              "this path needs numGridFine = 2*numGrid (Density_Grid_Factor 2)");
+    PWB_CHECK(fft_len_supported(numGrid[d]) && fft_len_supported(numGridFine[d]), PW_EUNSUPPORTED,
+              "FFT length not supported");
+  }
+  PWB_CHECK(find_grid(numGrid) != nullptr, PW_EUNSUPPORTED, "grid not instantiated in this build");
+  PWB_CUDA(cudaSetDevice(device));
+  pw_ctx* c = new pw_ctx();
+  c->prec = precision;
+  c->esz = precision == PW_F64 ? 8 : 4;
+  c->device = device;
+  for (int d = 0; d < 3; ++d) {
+    c->L[d] = length[d];
+    c->n[d] = numGrid[d];
+    c->nf[d] = numGridFine[d];
+  }
+  c->vol = length[0] * length[1] * length[2];
+  c->ntot = (long)numGrid[0] * numGrid[1] * numGrid[2];
+  c->ntotf = (long)numGridFine[0] * numGridFine[1] * numGridFine[2];
+  // |G|^2/2 and Teter on the full coarse spectrum, KGrid with Nyquist at +n/2
+  // (src/SCF/fourier.cpp:124-133, src/SCF/hamiltonian.cpp:2651-2663)
+  std::vector<double> ek(c->ntot), te(c->ntot);
+  const int n0 = c->n[0], n1 = c->n[1], n2 = c->n[2];
+  for (int k = 0; k < n2; ++k)
+    for (int j = 0; j < n1; ++j)
+      for (int i = 0; i < n0; ++i) {
+        const double m0 = i <= n0 / 2 ? i : i - n0, m1 = j <= n1 / 2 ? j : j - n1, m2 = k <= n2 / 2 ? k : k - n2;
+        const double g0 = 2 * M_PI / c->L[0] * m0, g1 = 2 * M_PI / c->L[1] * m1, g2 = 2 * M_PI / c->L[2] * m2;
+        const double e = (g0 * g0 + g1 * g1 + g2 * g2) / 2;
+        const long idx = i + (long)n0 * (j + (long)n1 * k);
+        ek[idx] = e;
+        const double a = e * 2.0;
+        const double b = 27.0 + a * (18.0 + a * (12.0 + a * 8.0));
+        te[idx] = b / (b + 16.0 * std::pow(a, 4.0));
+      }
+  int rc;
+  if ((rc = upload_real(c, c->ekin, ek.data(), ek.size())) ||
+      (rc = upload_real(c, c->teter, te.data(), te.size()))) {
+    delete c;
+    return rc;
+  }
+  const int lens[6] = {n0, n1, n2, c->nf[0], c->nf[1], c->nf[2]};
+  for (int s = 0; s < 6; ++s)
+    if ((rc = upload_twiddles(c, s, lens[s]))) { delete c; return rc; }
+  c->nl.cr = grid_chunk_rows(c->n, c->prec);
+  if ((rc = ensure_scratch(c, 32))) { delete c; return rc; }
+  *out = c;
+  return PW_OK;
+}
+
+int pw_ctx_destroy(pw_ctx* ctx) {
+  if (!ctx) return PW_OK;
+  cudaSetDevice(ctx->device);
+  delete ctx;
+  return PW_OK;
+}
+
+int pw_ctx_sizes(const pw_ctx* ctx, long* ntot, long* ntotFine) {
+  PWB_CHECK(ctx, PW_EINVAL, "null context");
+  if (ntot) *ntot = ctx->ntot;
+  if (ntotFine) *ntotFine = ctx->ntotf;
+  return PW_OK;
+}
+
+int pw_set_vtot(pw_ctx* ctx, const double* vtot) {
+  PWB_CHECK(ctx && vtot, PW_EINVAL, "null argument");
+  PWB_CUDA(cudaSetDevice(ctx->device));
+  int rc = upload_real(ctx, ctx->vtot, vtot, ctx->ntotf);
+  if (rc) return rc;
+  ctx->h_vtot.assign(vtot, vtot + ctx->ntotf);
+  ctx->have_vtot = true;
+  return PW_OK;
+}
+
+int pw_set_band_batch(pw_ctx* ctx, int nband_batch) {
+  PWB_CHECK(ctx && nband_batch > 0, PW_EINVAL, "bad band batch");
+  PWB_CUDA(cudaSetDevice(ctx->device));
+  ctx->pair_cap = 0;
+  return ensure_scratch(ctx, (nband_batch + 1) / 2);
+}
+
+int pw_set_nonlocal(pw_ctx* ctx, int natom, const int* atom_npts, const int* atom_nproj, const int* idx,
+                    const double* beta, const double* weight) {
+  PWB_CHECK(ctx && natom >= 0, PW_EINVAL, "bad arguments");
+  PWB_CUDA(cudaSetDevice(ctx->device));
+  NonlocalDev& nl = ctx->nl;
+  const int NXF = ctx->nf[0], NYF = ctx->nf[1], NZF = ctx->nf[2];
+  const int cr = nl.cr;
+  PWB_CHECK(cr > 0 && NYF % cr == 0, PW_EINVAL, "bad chunk rows");
+  const int nchunk = NYF / cr;
+  const int ntile = NZF * nchunk;
+  int npmax = 0;
+  long nent = 0;
+  for (int a = 0; a < natom; ++a) {
+    PWB_CHECK(atom_npts[a] >= 0 && atom_nproj[a] >= 0, PW_EINVAL, "negative sizes");
+    npmax = std::max(npmax, atom_nproj[a]);
+    nent += atom_npts[a];
+  }
+  PWB_CHECK(npmax <= 8, PW_EUNSUPPORTED, "at most 8 projectors per atom are supported");
+  PWB_CHECK(nent < (1L << 31), PW_EUNSUPPORTED, "too many projector points");
+  // bucket entries by tile, stable in (atom, point order)
+  std::vector<int> tile_count(ntile + 1, 0);
+  {
+    long off = 0;
+    for (int a = 0; a < natom; ++a) {
+      for (int i = 0; i < atom_npts[a]; ++i) {
+        const int g = idx[off + i];
+        PWB_CHECK(g >= 0 && g < ctx->ntotf, PW_EINVAL, "projector index outside the fine grid");
+        const int z = g / (NXF * NYF), y = (g / NXF) % NYF;
+        tile_count[z * nchunk + y / cr + 1]++;
+      }
+      off += atom_npts[a];
+    }
+  }
+  for (int t = 0; t < ntile; ++t) tile_count[t + 1] += tile_count[t];
+  std::vector<int> e_xy(nent), e_atom(nent);
+  std::vector<double> e_beta((size_t)std::max(npmax, 1) * nent, 0.0);
+  {
+    std::vector<int> fill(tile_count.begin(), tile_count.end() - 1);
+    long off = 0, boff = 0;
+    for (int a = 0; a < natom; ++a) {
+      const int np = atom_npts[a];
+      for (int i = 0; i < np; ++i) {
+        const int g = idx[off + i];
+        const int z = g / (NXF * NYF), y = (g / NXF) % NYF, x = g % NXF;
+        const int e = fill[z * nchunk + y / cr]++;
+        e_xy[e] = y * NXF + x;
+        e_atom[e] = a;
+        for (int q = 0; q < atom_nproj[a]; ++q) e_beta[(size_t)q * nent + e] = beta[boff + (long)q * np + i];
+      }
+      off += np;
+      boff += (long)atom_nproj[a] * np;
+    }
+  }
+  // slots: runs of equal atom inside a tile
+  std::vector<int> tile_slot(ntile + 1, 0), slot_atom, slot_ent;
+  for (int t = 0; t < ntile; ++t) {
+    tile_slot[t] = (int)slot_atom.size();
+    for (int e = tile_count[t]; e < tile_count[t + 1]; ++e) {
+      if (e == tile_count[t] || e_atom[e] != e_atom[e - 1]) {
+        slot_atom.push_back(e_atom[e]);
+        slot_ent.push_back(e);
+      }
+    }
+  }
+  tile_slot[ntile] = (int)slot_atom.size();
+  slot_ent.push_back((int)nent);
+  const int nslot = (int)slot_atom.size();
+  std::vector<int> atom_slot(natom + 1, 0), atom_slot_list(nslot);
+  for (int s = 0; s < nslot; ++s) atom_slot[slot_atom[s] + 1]++;
+  for (int a = 0; a < natom; ++a) atom_slot[a + 1] += atom_slot[a];
+  {
+    std::vector<int> fill(atom_slot.begin(), atom_slot.end() - 1);
+    for (int s = 0; s < nslot; ++s) atom_slot_list[fill[slot_atom[s]]++] = s;
+  }
+  std::vector<double> wg((size_t)std::max(natom, 1) * std::max(npmax, 1), 0.0);
+  {
+    long woff = 0;
+    const double fac = ctx->vol / (double)ctx->ntotf;
+    for (int a = 0; a < natom; ++a) {
+      for (int q = 0; q < atom_nproj[a]; ++q) wg[(size_t)a * npmax + q] = weight[woff + q] * fac;
+      woff += atom_nproj[a];
+    }
+  }
+  int rc;
+  auto up_int = [&](DevBuf& b, const std::vector<int>& v) -> int {
+    int r = b.alloc(std::max<size_t>(v.size(), 1) * 4);
+    if (r) return r;
+    if (!v.empty()) PWB_CUDA(cudaMemcpy(b.p, v.data(), v.size() * 4, cudaMemcpyHostToDevice));
+    return PW_OK;
+  };
+  if ((rc = up_int(nl.ent_xy, e_xy)) || (rc = up_int(nl.tile_slot, tile_slot)) ||
+      (rc = up_int(nl.slot_atom, slot_atom)) || (rc = up_int(nl.slot_ent, slot_ent)) ||
+      (rc = up_int(nl.atom_slot, atom_slot)) || (rc = up_int(nl.atom_slot_list, atom_slot_list)))
+    return rc;
+  if ((rc = upload_real(ctx, nl.ent_beta, e_beta.data(), e_beta.size()))) return rc;
+  if ((rc = upload_real(ctx, nl.wgt, wg.data(), wg.size()))) return rc;
+  nl.natom = natom;
+  nl.npmax = npmax;
+  nl.nent = (int)nent;
+  nl.nslot = nslot;
+  nl.ntile = ntile;
+  nl.nchunk = nchunk;
+  ctx->have_nl = true;
+  const int cap = std::max(ctx->pair_cap, 1);
+  ctx->pair_cap = 0;
+  return ensure_scratch(ctx, cap);
+}
+
+int pw_hpsi(pw_ctx* ctx, const void* psi, int ld, void* hpsi, int ldh, int nband, int accumulate, void* stream) {
+  PWB_CHECK(ctx && psi && hpsi, PW_EINVAL, "null argument");
+  PWB_CHECK(nband >= 0 && ld >= ctx->ntot && ldh >= ctx->ntot, PW_EINVAL, "Domain size does not match.");
+  PWB_CHECK(ctx->have_vtot, PW_ENOTREADY, "local potential not set (pw_set_vtot)");
+  PWB_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t st = (cudaStream_t)stream;
+  const int cap = ctx->pair_cap;
+  for (int b0 = 0; b0 < nband; b0 += 2 * cap) {
+    const int npair = std::min(cap, (nband - b0 + 1) / 2);
+    int rc = run_hpsi(ctx, psi, ld, hpsi, ldh, nband, b0, npair, accumulate, st);
+    if (rc) return rc;
+  }
+  return PW_OK;
+}
+
+int pw_teter_precond(pw_ctx* ctx, const void* r, int ld, void* w, int ldw, int nband, int accumulate, void* stream) {
+  PWB_CHECK(ctx && r && w, PW_EINVAL, "null argument");
+  PWB_CHECK(nband >= 0 && ld >= ctx->ntot && ldw >= ctx->ntot, PW_EINVAL, "Domain size does not match.");
+  PWB_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t st = (cudaStream_t)stream;
+  const int cap = ctx->pair_cap;
+  for (int b0 = 0; b0 < nband; b0 += 2 * cap) {
+    const int npair = std::min(cap, (nband - b0 + 1) / 2);
+    int rc = run_teter(ctx, r, ld, w, ldw, nband, b0, npair, accumulate, st);
+    if (rc) return rc;
+  }
+  return PW_OK;
+}
+
+int pw_hpsi_host(pw_ctx* ctx, const void* psi, int ld, void* hpsi, int ldh, int nband, int accumulate) {
+  PWB_CHECK(ctx && psi && hpsi, PW_EINVAL, "null argument");
+  PWB_CHECK(nband >= 0 && ld >= ctx->ntot && ldh >= ctx->ntot, PW_EINVAL, "Domain size does not match.");
+  PWB_CUDA(cudaSetDevice(ctx->device));
+  const size_t bytes = (size_t)ctx->ntot * nband * ctx->esz;
+  int rc;
+  if ((rc = ctx->s_host_in.alloc(bytes)) || (rc = ctx->s_host_out.alloc(bytes))) return rc;
+  PWB_CUDA(cudaMemcpy2D(ctx->s_host_in.p, ctx->ntot * ctx->esz, psi, (size_t)ld * ctx->esz, ctx->ntot * ctx->esz,
+                        nband, cudaMemcpyHostToDevice));
+  if (accumulate)
+    PWB_CUDA(cudaMemcpy2D(ctx->s_host_out.p, ctx->ntot * ctx->esz, hpsi, (size_t)ldh * ctx->esz,
+                          ctx->ntot * ctx->esz, nband, cudaMemcpyHostToDevice));
+  rc = pw_hpsi(ctx, ctx->s_host_in.p, (int)ctx->ntot, ctx->s_host_out.p, (int)ctx->ntot, nband, accumulate, nullptr);
+  if (rc) return rc;
+  PWB_CUDA(cudaMemcpy2D(hpsi, (size_t)ldh * ctx->esz, ctx->s_host_out.p, ctx->ntot * ctx->esz, ctx->ntot * ctx->esz,
+                        nband, cudaMemcpyDeviceToHost));
+  return PW_OK;
+}
+
+}  // extern "C"

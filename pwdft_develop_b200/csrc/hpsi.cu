@@ -1,0 +1,671 @@
+// Band-pair H*psi pipeline on sm_100a.
+//
+// Two real bands a, b of the Gamma-point wavefunction are packed into one
+// complex field Z = psi_a + i psi_b.  The reference's real-to-complex path
+// (Spinor::AddMultSpinorFineR2C, src/SCF/spinor.cpp:377-525) is a real-linear
+// map, so running its complex-linear extension on Z gives H psi_a + i H psi_b.
+// The coarse->fine spectrum placement of IP_c2f / IP_f2c
+// (src/utility.cpp:3150-3275: a coefficient whose index is Nyquist in the set
+// S of axes goes, halved, to the all-plus and the all-minus fine positions)
+// is separable once every Nyquist coefficient is given a "+" and a "-" slot;
+// the z-pencil kernels do that unfolding so the fine-plane kernels only see
+// plain zero padding.
+//
+// Kernels (one launch each per band batch, all pairs in the grid):
+//   k_cxy_fwd    coarse plane: FFT x, FFT y                     psi -> A
+//   k_zpad       coarse z FFT, kinetic, unfold + pad, fine z IFFT  A -> K, B
+//   k_fplane<G>  fine plane: IFFT y, IFFT x, projector partial dots  B -> Wp
+//   k_nl_reduce  sum partial dots, scale by gamma*vol/N_fine     Wp -> W
+//   k_fplane<A>  fine plane: IFFT y, IFFT x, *V + projector scatter,
+//                FFT x, FFT y, truncate                           B -> C (in place)
+//   k_zfold      fine z FFT, fold (IP_f2c rule) + kinetic, coarse z IFFT  C,K -> D
+//   k_cxy_inv    coarse plane: IFFT y, IFFT x, (accumulate) into hpsi   D -> hpsi
+#include "common.hpp"
+#include "fft.cuh"
+
+namespace pwb {
+
+constexpr int TX = 16;          // kx columns per z-pencil CTA
+constexpr int PLANE_THREADS = 256;
+constexpr int PENCIL_THREADS = 256;
+
+template <typename T> using VT = typename C2<T>::t;
+
+__device__ __forceinline__ int sgn_idx(int k, int n) { return k <= n / 2 ? k : k - n; }
+// slot s in [0, n]: s < n is the FFT index (Nyquist = "+" slot), s == n is the "-" Nyquist slot
+__device__ __forceinline__ int slot_fine(int s, int n, int nf) {
+  int m = (s < n) ? sgn_idx(s, n) : -(n / 2);
+  return (m + nf) % nf;
+}
+
+template <typename V>
+__device__ __forceinline__ void load_tw(V* dst, const V* src, int n) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+}
+
+// ---------------------------------------------------------------------------
+// coarse plane forward: psi (two real bands) -> A[pair][z][ky][kx]
+// ---------------------------------------------------------------------------
+template <typename T, int N0, int N1>
+__global__ void __launch_bounds__(PLANE_THREADS)
+k_cxy_fwd(const T* __restrict__ psi, int ld, int nband, int band0, VT<T>* __restrict__ A,
+          const VT<T>* twx_g, const VT<T>* twy_g) {
+  using V = VT<T>;
+  constexpr int P0 = N0 + 1;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  V* pl = reinterpret_cast<V*>(smraw);
+  V* twx = pl + N1 * P0;
+  V* twy = twx + N0;
+  load_tw(twx, twx_g, N0);
+  load_tw(twy, twy_g, N1);
+  const int z = blockIdx.x, p = blockIdx.y;
+  const long ntot_plane = (long)N0 * N1;
+  const int ba = band0 + 2 * p, bb = ba + 1;
+  const T* pa = psi + (long)ba * ld + z * ntot_plane;
+  const T* pb = (bb < nband) ? psi + (long)bb * ld + z * ntot_plane : nullptr;
+  for (int i = threadIdx.x; i < N0 * N1; i += blockDim.x) {
+    const int y = i / N0, x = i - y * N0;
+    pl[y * P0 + x] = mkc<V>(pa[i], pb ? pb[i] : (T)0);
+  }
+  __syncthreads();
+  smem_fft<N0, -1>(pl, N1, 1, P0, twx);
+  __syncthreads();
+  smem_fft<N1, -1>(pl, N0, P0, 1, twy);
+  __syncthreads();
+  const int N2 = gridDim.x;
+  V* Ap = A + ((long)p * N2 + z) * ntot_plane;
+  for (int i = threadIdx.x; i < N0 * N1; i += blockDim.x) {
+    const int y = i / N0, x = i - y * N0;
+    Ap[i] = pl[y * P0 + x];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// column bookkeeping shared by k_zpad and k_zfold.
+// Tile: fixed ky, kx in [kx0, kx0+TX).  Output/input columns:
+//   ky not Nyquist: col i <-> (ky, kx0+i); if kx0+i == n0/2 its "-" partner is col TX
+//   ky Nyquist:     col i <-> (ky+, kx0+i (+ slot)); col TX+i <-> (ky-, kx0+i or n0 if kx Nyquist)
+// ---------------------------------------------------------------------------
+struct ColMap {
+  int ncols;
+  bool nyy;
+  int nyx_i;  // tile-local index of the kx Nyquist column, -1 if none
+};
+__device__ __forceinline__ ColMap colmap(int ky, int kx0, int tw, int n0, int n1) {
+  ColMap m;
+  m.nyy = (ky == n1 / 2);
+  m.nyx_i = (n0 / 2 >= kx0 && n0 / 2 < kx0 + tw) ? (n0 / 2 - kx0) : -1;
+  m.ncols = m.nyy ? 2 * TX : (m.nyx_i >= 0 ? TX + 1 : TX);
+  return m;
+}
+// slot coordinates of column c
+__device__ __forceinline__ void col_slot(const ColMap& m, int c, int ky, int kx0, int n0, int n1,
+                                         int& ky_s, int& kx_s) {
+  if (m.nyy) {
+    if (c < TX) { ky_s = ky; kx_s = kx0 + c; }
+    else { ky_s = n1; kx_s = (kx0 + c - TX == n0 / 2) ? n0 : kx0 + c - TX; }
+  } else {
+    if (c < TX) { ky_s = ky; kx_s = kx0 + c; }
+    else { ky_s = ky; kx_s = n0; }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// z pencils: coarse FFT z, kinetic, Nyquist unfold, fine pad, fine IFFT z
+// ---------------------------------------------------------------------------
+template <typename T, int NZ, int NZF>
+__global__ void __launch_bounds__(PENCIL_THREADS)
+k_zpad(const VT<T>* __restrict__ A, VT<T>* __restrict__ K, VT<T>* __restrict__ B,
+       const T* __restrict__ ekin, int n0, int n1, T inv_nc,
+       const VT<T>* twz_g, const VT<T>* twzf_g) {
+  using V = VT<T>;
+  constexpr int PI = TX + 1;
+  constexpr int PO = 2 * TX + 1;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  V* in = reinterpret_cast<V*>(smraw);     // [NZ][PI]
+  V* out = in + NZ * PI;                   // [NZF][PO]
+  V* twz = out + NZF * PO;
+  V* twzf = twz + NZ;
+  load_tw(twz, twz_g, NZ);
+  load_tw(twzf, twzf_g, NZF);
+  const int ky = blockIdx.x, kx0 = blockIdx.y * TX, p = blockIdx.z;
+  const int tw = min(TX, n0 - kx0);
+  const long nplane = (long)n0 * n1;
+  const V* Ap = A + (long)p * NZ * nplane;
+  for (int i = threadIdx.x; i < NZ * TX; i += blockDim.x) {
+    const int z = i / TX, c = i - z * TX;
+    in[z * PI + c] = (c < tw) ? Ap[z * nplane + (long)ky * n0 + kx0 + c] : mkc<V>(0, 0);
+  }
+  const ColMap m = colmap(ky, kx0, tw, n0, n1);
+  for (int i = threadIdx.x; i < NZF * PO; i += blockDim.x) out[i] = mkc<V>(0, 0);
+  __syncthreads();
+  smem_fft<NZ, -1>(in, tw, PI, 1, twz);
+  __syncthreads();
+  V* Kp = K + (long)p * NZ * nplane;
+  for (int i = threadIdx.x; i < NZ * TX; i += blockDim.x) {
+    const int kz = i / TX, c = i - kz * TX;
+    if (c >= tw) continue;
+    const long g = kz * nplane + (long)ky * n0 + kx0 + c;
+    const V v = cscale(in[kz * PI + c], inv_nc);
+    Kp[g] = cscale(v, ekin[g]);
+    const bool nyz = (kz == NZ / 2);
+    const int fz = (sgn_idx(kz, NZ) + NZF) % NZF;
+    const bool split = m.nyy || (c == m.nyx_i);
+    if (!split) {
+      if (nyz) {
+        out[(NZ / 2) * PO + c] = cscale(v, (T)0.5);
+        out[(NZF - NZ / 2) * PO + c] = cscale(v, (T)0.5);
+      } else {
+        out[fz * PO + c] = v;
+      }
+    } else {
+      const int cp = c, cm = m.nyy ? TX + c : TX;
+      const V h = cscale(v, (T)0.5);
+      if (nyz) {
+        out[(NZ / 2) * PO + cp] = h;
+        out[(NZF - NZ / 2) * PO + cm] = h;
+      } else {
+        out[fz * PO + cp] = h;
+        out[fz * PO + cm] = h;
+      }
+    }
+  }
+  __syncthreads();
+  smem_fft<NZF, +1>(out, m.ncols, PO, 1, twzf);
+  __syncthreads();
+  const int nsx = n0 + 1, nsy = n1 + 1;
+  V* Bp = B + (long)p * NZF * nsy * nsx;
+  for (int i = threadIdx.x; i < NZF * m.ncols; i += blockDim.x) {
+    const int zf = i / m.ncols, c = i - zf * m.ncols;
+    if (c < TX && c >= tw) continue;
+    if (m.nyy && c >= TX && c - TX >= tw) continue;
+    int ky_s, kx_s;
+    col_slot(m, c, ky, kx0, n0, n1, ky_s, kx_s);
+    Bp[((long)zf * nsy + ky_s) * nsx + kx_s] = out[zf * PO + c];
+  }
+  // the two Nyquist corner slots that no coarse coefficient reaches
+  if (m.nyy && m.nyx_i >= 0) {
+    for (int zf = threadIdx.x; zf < NZF; zf += blockDim.x) {
+      Bp[((long)zf * nsy + n1 / 2) * nsx + n0] = mkc<V>(0, 0);
+      Bp[((long)zf * nsy + n1) * nsx + n0 / 2] = mkc<V>(0, 0);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// fine plane kernel (gather or apply mode)
+// ---------------------------------------------------------------------------
+struct NLArgs {
+  const int* ent_xy;
+  const void* ent_beta;
+  const int* tile_slot;
+  const int* slot_atom;
+  const int* slot_ent;
+  int nent, npmax, nchunk, cr;
+  bool present;
+};
+
+template <typename T, int NXF, int NYF, bool APPLY>
+__global__ void __launch_bounds__(PLANE_THREADS)
+k_fplane(VT<T>* __restrict__ BC, const T* __restrict__ vtot, NLArgs nl, VT<T>* __restrict__ Wp,
+         const VT<T>* __restrict__ W, int natom, int nslot, T inv_nf,
+         const VT<T>* twx_g, const VT<T>* twy_g) {
+  using V = VT<T>;
+  constexpr int n0 = NXF / 2, n1 = NYF / 2;
+  constexpr int nsx = n0 + 1, nsy = n1 + 1;
+  constexpr int PS = nsx;          // odd pitch
+  constexpr int PR = NXF + 1;      // odd pitch
+  const int CR = nl.cr;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  V* S = reinterpret_cast<V*>(smraw);     // [NYF][PS]
+  V* R = S + NYF * PS;                     // [CR][PR]
+  V* twx = R + CR * PR;
+  V* twy = twx + NXF;
+  load_tw(twx, twx_g, NXF);
+  load_tw(twy, twy_g, NYF);
+  const int zf = blockIdx.x, p = blockIdx.y;
+  const int NZF = gridDim.x;
+  V* Bp = BC + ((long)p * NZF + zf) * nsy * nsx;
+  for (int i = threadIdx.x; i < NYF * PS; i += blockDim.x) S[i] = mkc<V>(0, 0);
+  __syncthreads();
+  for (int i = threadIdx.x; i < nsy * nsx; i += blockDim.x) {
+    const int ys = i / nsx, xs = i - ys * nsx;
+    S[slot_fine(ys, n1, NYF) * PS + xs] = Bp[i];
+  }
+  __syncthreads();
+  smem_fft<NYF, +1>(S, nsx, PS, 1, twy);
+  __syncthreads();
+  const T* beta = reinterpret_cast<const T*>(nl.ent_beta);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int c = 0; c < nl.nchunk; ++c) {
+    const int y0 = c * CR;
+    for (int i = threadIdx.x; i < CR * PR; i += blockDim.x) R[i] = mkc<V>(0, 0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < CR * nsx; i += blockDim.x) {
+      const int yl = i / nsx, xs = i - yl * nsx;
+      R[yl * PR + slot_fine(xs, n0, NXF)] = S[(y0 + yl) * PS + xs];
+    }
+    __syncthreads();
+    smem_fft<NXF, +1>(R, CR, 1, PR, twx);
+    __syncthreads();
+    const int tile = zf * nl.nchunk + c;
+    if (!APPLY) {
+      if (nl.present) {
+        const int s0 = nl.tile_slot[tile], s1 = nl.tile_slot[tile + 1];
+        for (int s = s0 + warp; s < s1; s += nw) {
+          V acc[8];
+#pragma unroll
+          for (int q = 0; q < 8; ++q) acc[q] = mkc<V>(0, 0);
+          const int e0 = nl.slot_ent[s], e1 = nl.slot_ent[s + 1];
+          for (int e = e0 + lane; e < e1; e += 32) {
+            const int xy = nl.ent_xy[e];
+            const int yl = xy / NXF - y0, x = xy - (xy / NXF) * NXF;
+            const V v = R[yl * PR + x];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+              if (q < nl.npmax) {
+                const T b = beta[(long)q * nl.nent + e];
+                acc[q].x += b * v.x;
+                acc[q].y += b * v.y;
+              }
+            }
+          }
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            if (q < nl.npmax) {
+              T ax = acc[q].x, ay = acc[q].y;
+#pragma unroll
+              for (int o = 16; o > 0; o >>= 1) {
+                ax += __shfl_xor_sync(0xffffffffu, ax, o);
+                ay += __shfl_xor_sync(0xffffffffu, ay, o);
+              }
+              if (lane == 0) Wp[((long)p * nslot + s) * nl.npmax + q] = mkc<V>(ax, ay);
+            }
+          }
+        }
+      }
+      __syncthreads();
+    } else {
+      const T* vp = vtot + ((long)zf * NYF + y0) * NXF;
+      for (int i = threadIdx.x; i < CR * NXF; i += blockDim.x) {
+        const int yl = i / NXF, x = i - yl * NXF;
+        R[yl * PR + x] = cscale(R[yl * PR + x], vp[i]);
+      }
+      __syncthreads();
+      if (nl.present) {
+        const int s0 = nl.tile_slot[tile], s1 = nl.tile_slot[tile + 1];
+        for (int s = s0 + warp; s < s1; s += nw) {
+          const int a = nl.slot_atom[s];
+          V w[8];
+#pragma unroll
+          for (int q = 0; q < 8; ++q)
+            w[q] = (q < nl.npmax) ? W[((long)p * natom + a) * nl.npmax + q] : mkc<V>(0, 0);
+          const int e0 = nl.slot_ent[s], e1 = nl.slot_ent[s + 1];
+          for (int e = e0 + lane; e < e1; e += 32) {
+            const int xy = nl.ent_xy[e];
+            const int yl = xy / NXF - y0, x = xy - (xy / NXF) * NXF;
+            T ax = 0, ay = 0;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+              if (q < nl.npmax) {
+                const T b = beta[(long)q * nl.nent + e];
+                ax += b * w[q].x;
+                ay += b * w[q].y;
+              }
+            }
+            atomicAdd(&R[yl * PR + x].x, ax);
+            atomicAdd(&R[yl * PR + x].y, ay);
+          }
+        }
+      }
+      __syncthreads();
+      smem_fft<NXF, -1>(R, CR, 1, PR, twx);
+      __syncthreads();
+      for (int i = threadIdx.x; i < CR * nsx; i += blockDim.x) {
+        const int yl = i / nsx, xs = i - yl * nsx;
+        S[(y0 + yl) * PS + xs] = R[yl * PR + slot_fine(xs, n0, NXF)];
+      }
+      __syncthreads();
+    }
+  }
+  if (APPLY) {
+    smem_fft<NYF, -1>(S, nsx, PS, 1, twy);
+    __syncthreads();
+    for (int i = threadIdx.x; i < nsy * nsx; i += blockDim.x) {
+      const int ys = i / nsx, xs = i - ys * nsx;
+      Bp[i] = cscale(S[slot_fine(ys, n1, NYF) * PS + xs], inv_nf);
+    }
+  }
+}
+
+// W[p][a][q] = wgt[a][q] * sum over the atom's slots of Wp[p][slot][q]
+template <typename T>
+__global__ void k_nl_reduce(const VT<T>* __restrict__ Wp, VT<T>* __restrict__ W, const int* atom_slot,
+                            const int* atom_slot_list, const T* wgt, int natom, int nslot, int npmax) {
+  using V = VT<T>;
+  const int p = blockIdx.y;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= natom * npmax) return;
+  const int a = i / npmax, q = i - a * npmax;
+  T sx = 0, sy = 0;
+  for (int j = atom_slot[a]; j < atom_slot[a + 1]; ++j) {
+    const V v = Wp[((long)p * nslot + atom_slot_list[j]) * npmax + q];
+    sx += v.x;
+    sy += v.y;
+  }
+  const T g = wgt[i];
+  W[(long)p * natom * npmax + i] = mkc<V>(sx * g, sy * g);
+}
+
+// ---------------------------------------------------------------------------
+// z pencils: fine FFT z, fold to coarse (IP_f2c), add kinetic, coarse IFFT z
+// ---------------------------------------------------------------------------
+template <typename T, int NZ, int NZF>
+__global__ void __launch_bounds__(PENCIL_THREADS)
+k_zfold(const VT<T>* __restrict__ C, const VT<T>* __restrict__ K, VT<T>* __restrict__ D, int n0, int n1,
+        const VT<T>* twz_g, const VT<T>* twzf_g) {
+  using V = VT<T>;
+  constexpr int PI = 2 * TX + 1;
+  constexpr int PA = TX + 1;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  V* in = reinterpret_cast<V*>(smraw);    // [NZF][PI]
+  V* acc = in + NZF * PI;                 // [NZ][PA]
+  V* twz = acc + NZ * PA;
+  V* twzf = twz + NZ;
+  load_tw(twz, twz_g, NZ);
+  load_tw(twzf, twzf_g, NZF);
+  const int ky = blockIdx.x, kx0 = blockIdx.y * TX, p = blockIdx.z;
+  const int tw = min(TX, n0 - kx0);
+  const ColMap m = colmap(ky, kx0, tw, n0, n1);
+  const int nsx = n0 + 1, nsy = n1 + 1;
+  const V* Cp = C + (long)p * NZF * nsy * nsx;
+  for (int i = threadIdx.x; i < NZF * m.ncols; i += blockDim.x) {
+    const int zf = i / m.ncols, c = i - zf * m.ncols;
+    bool valid = !(c < TX && c >= tw) && !(m.nyy && c >= TX && c - TX >= tw);
+    int ky_s, kx_s;
+    col_slot(m, c, ky, kx0, n0, n1, ky_s, kx_s);
+    in[zf * PI + c] = valid ? Cp[((long)zf * nsy + ky_s) * nsx + kx_s] : mkc<V>(0, 0);
+  }
+  __syncthreads();
+  smem_fft<NZF, -1>(in, m.ncols, PI, 1, twzf);
+  __syncthreads();
+  const long nplane = (long)n0 * n1;
+  const V* Kp = K + (long)p * NZ * nplane;
+  for (int i = threadIdx.x; i < NZ * TX; i += blockDim.x) {
+    const int kz = i / TX, c = i - kz * TX;
+    if (c >= tw) { acc[kz * PA + c] = mkc<V>(0, 0); continue; }
+    V v = Kp[kz * nplane + (long)ky * n0 + kx0 + c];
+    const bool nyz = (kz == NZ / 2);
+    const int fz = (sgn_idx(kz, NZ) + NZF) % NZF;
+    const bool split = m.nyy || (c == m.nyx_i);
+    if (!split) {
+      if (nyz) v = cadd(v, cscale(cadd(in[(NZ / 2) * PI + c], in[(NZF - NZ / 2) * PI + c]), (T)0.5));
+      else v = cadd(v, in[fz * PI + c]);
+    } else {
+      const int cp = c, cm = m.nyy ? TX + c : TX;
+      if (nyz) v = cadd(v, cscale(cadd(in[(NZ / 2) * PI + cp], in[(NZF - NZ / 2) * PI + cm]), (T)0.5));
+      else v = cadd(v, cscale(cadd(in[fz * PI + cp], in[fz * PI + cm]), (T)0.5));
+    }
+    acc[kz * PA + c] = v;
+  }
+  __syncthreads();
+  smem_fft<NZ, +1>(acc, tw, PA, 1, twz);
+  __syncthreads();
+  V* Dp = D + (long)p * NZ * nplane;
+  for (int i = threadIdx.x; i < NZ * TX; i += blockDim.x) {
+    const int z = i / TX, c = i - z * TX;
+    if (c < tw) Dp[z * nplane + (long)ky * n0 + kx0 + c] = acc[z * PA + c];
+  }
+}
+
+// z pencils for the Teter preconditioner: FFT z, * teter / N_c, IFFT z
+template <typename T, int NZ>
+__global__ void __launch_bounds__(PENCIL_THREADS)
+k_zteter(VT<T>* __restrict__ A, const T* __restrict__ teter, int n0, int n1, T inv_nc, const VT<T>* twz_g) {
+  using V = VT<T>;
+  constexpr int PI = TX + 1;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  V* in = reinterpret_cast<V*>(smraw);
+  V* twz = in + NZ * PI;
+  load_tw(twz, twz_g, NZ);
+  const int ky = blockIdx.x, kx0 = blockIdx.y * TX, p = blockIdx.z;
+  const int tw = min(TX, n0 - kx0);
+  const long nplane = (long)n0 * n1;
+  V* Ap = A + (long)p * NZ * nplane;
+  for (int i = threadIdx.x; i < NZ * TX; i += blockDim.x) {
+    const int z = i / TX, c = i - z * TX;
+    in[z * PI + c] = (c < tw) ? Ap[z * nplane + (long)ky * n0 + kx0 + c] : mkc<V>(0, 0);
+  }
+  __syncthreads();
+  smem_fft<NZ, -1>(in, tw, PI, 1, twz);
+  __syncthreads();
+  for (int i = threadIdx.x; i < NZ * TX; i += blockDim.x) {
+    const int kz = i / TX, c = i - kz * TX;
+    if (c < tw) in[kz * PI + c] = cscale(in[kz * PI + c], teter[kz * nplane + (long)ky * n0 + kx0 + c] * inv_nc);
+  }
+  __syncthreads();
+  smem_fft<NZ, +1>(in, tw, PI, 1, twz);
+  __syncthreads();
+  for (int i = threadIdx.x; i < NZ * TX; i += blockDim.x) {
+    const int z = i / TX, c = i - z * TX;
+    if (c < tw) Ap[z * nplane + (long)ky * n0 + kx0 + c] = in[z * PI + c];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// coarse plane inverse: D -> hpsi (two real bands)
+// ---------------------------------------------------------------------------
+template <typename T, int N0, int N1>
+__global__ void __launch_bounds__(PLANE_THREADS)
+k_cxy_inv(const VT<T>* __restrict__ D, T* __restrict__ out, int ldo, int nband, int band0, int accumulate,
+          const VT<T>* twx_g, const VT<T>* twy_g) {
+  using V = VT<T>;
+  constexpr int P0 = N0 + 1;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  V* pl = reinterpret_cast<V*>(smraw);
+  V* twx = pl + N1 * P0;
+  V* twy = twx + N0;
+  load_tw(twx, twx_g, N0);
+  load_tw(twy, twy_g, N1);
+  const int z = blockIdx.x, p = blockIdx.y;
+  const int N2 = gridDim.x;
+  const long ntot_plane = (long)N0 * N1;
+  const V* Dp = D + ((long)p * N2 + z) * ntot_plane;
+  for (int i = threadIdx.x; i < N0 * N1; i += blockDim.x) {
+    const int y = i / N0, x = i - y * N0;
+    pl[y * P0 + x] = Dp[i];
+  }
+  __syncthreads();
+  smem_fft<N1, +1>(pl, N0, P0, 1, twy);
+  __syncthreads();
+  smem_fft<N0, +1>(pl, N1, 1, P0, twx);
+  __syncthreads();
+  const int ba = band0 + 2 * p, bb = ba + 1;
+  T* oa = out + (long)ba * ldo + z * ntot_plane;
+  T* ob = (bb < nband) ? out + (long)bb * ldo + z * ntot_plane : nullptr;
+  for (int i = threadIdx.x; i < N0 * N1; i += blockDim.x) {
+    const int y = i / N0, x = i - y * N0;
+    const V v = pl[y * P0 + x];
+    if (accumulate) {
+      oa[i] += v.x;
+      if (ob) ob[i] += v.y;
+    } else {
+      oa[i] = v.x;
+      if (ob) ob[i] = v.y;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host-side launch plan for one (precision, grid) instantiation
+// ---------------------------------------------------------------------------
+template <typename T> static int fplane_cr(int NXF, int NYF) {
+  // rows per chunk so that S + R (+ twiddles) fit in ~200 KB of shared memory
+  const size_t vs = sizeof(T) * 2;
+  const size_t S = (size_t)NYF * (NXF / 2 + 1) * vs;
+  const size_t budget = 200 * 1024;
+  int best = 1;
+  for (int cr = 1; cr <= NYF; ++cr) {
+    if (NYF % cr) continue;
+    if (S + (size_t)cr * (NXF + 1) * vs + (NXF + NYF) * vs <= budget) best = cr;
+  }
+  return best;
+}
+
+template <typename T, int N0, int N1, int N2>
+struct Plan {
+  using V = VT<T>;
+  static constexpr int NF0 = 2 * N0, NF1 = 2 * N1, NF2 = 2 * N2;
+
+  static int chunk_rows() { return fplane_cr<T>(NF0, NF1); }
+
+  static size_t sm_cxy() { return sizeof(V) * (N1 * (N0 + 1) + N0 + N1); }
+  static size_t sm_zpad() { return sizeof(V) * (N2 * (TX + 1) + NF2 * (2 * TX + 1) + N2 + NF2); }
+  static size_t sm_zfold() { return sizeof(V) * (NF2 * (2 * TX + 1) + N2 * (TX + 1) + N2 + NF2); }
+  static size_t sm_zteter() { return sizeof(V) * (N2 * (TX + 1) + N2); }
+  static size_t sm_fplane(int cr) {
+    return sizeof(V) * ((size_t)NF1 * (N0 + 1) + (size_t)cr * (NF0 + 1) + NF0 + NF1);
+  }
+
+  static int set_attrs() {
+    static bool done = false;
+    if (done) return PW_OK;
+    const int cr = chunk_rows();
+    PWB_CUDA(cudaFuncSetAttribute(k_fplane<T, NF0, NF1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_fplane(cr)));
+    PWB_CUDA(cudaFuncSetAttribute(k_fplane<T, NF0, NF1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_fplane(cr)));
+    PWB_CUDA(cudaFuncSetAttribute(k_zpad<T, N2, NF2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_zpad()));
+    PWB_CUDA(cudaFuncSetAttribute(k_zfold<T, N2, NF2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_zfold()));
+    PWB_CUDA(cudaFuncSetAttribute(k_cxy_fwd<T, N0, N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_cxy()));
+    PWB_CUDA(cudaFuncSetAttribute(k_cxy_inv<T, N0, N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_cxy()));
+    PWB_CUDA(cudaFuncSetAttribute(k_zteter<T, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_zteter()));
+    done = true;
+    return PW_OK;
+  }
+
+  static const V* tw(pw_ctx* c, int i) { return reinterpret_cast<const V*>(c->tw[i].p); }
+
+  // one batch of npair band pairs starting at band0
+  static int hpsi_batch(pw_ctx* c, const T* psi, int ld, T* out, int ldo, int nband, int band0, int npair,
+                        int accumulate, cudaStream_t st) {
+    int rc = set_attrs();
+    if (rc) return rc;
+    V* AD = reinterpret_cast<V*>(c->s_ad.p);
+    V* K = reinterpret_cast<V*>(c->s_k.p);
+    V* BC = reinterpret_cast<V*>(c->s_bc.p);
+    V* Wp = reinterpret_cast<V*>(c->s_wp.p);
+    V* W = reinterpret_cast<V*>(c->s_w.p);
+    const T inv_nc = (T)(1.0 / (double)c->ntot);
+    const T inv_nf = (T)(1.0 / (double)c->ntotf);
+    const int ntx = (N0 + TX - 1) / TX;
+    k_cxy_fwd<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(psi, ld, nband, band0, AD, tw(c, 0), tw(c, 1));
+    k_zpad<T, N2, NF2><<<dim3(N1, ntx, npair), PENCIL_THREADS, sm_zpad(), st>>>(
+        AD, K, BC, reinterpret_cast<const T*>(c->ekin.p), N0, N1, inv_nc, tw(c, 2), tw(c, 5));
+    NLArgs nl{};
+    const int cr = chunk_rows();
+    nl.cr = cr;
+    nl.nchunk = NF1 / cr;
+    nl.present = c->have_nl && c->nl.nent > 0;
+    int natom = 0, nslot = 0;
+    if (nl.present) {
+      nl.ent_xy = reinterpret_cast<const int*>(c->nl.ent_xy.p);
+      nl.ent_beta = c->nl.ent_beta.p;
+      nl.tile_slot = reinterpret_cast<const int*>(c->nl.tile_slot.p);
+      nl.slot_atom = reinterpret_cast<const int*>(c->nl.slot_atom.p);
+      nl.slot_ent = reinterpret_cast<const int*>(c->nl.slot_ent.p);
+      nl.nent = c->nl.nent;
+      nl.npmax = c->nl.npmax;
+      natom = c->nl.natom;
+      nslot = c->nl.nslot;
+      if (c->nl.cr != cr) { set_error("projector tables built for another chunk size"); return PW_EINVAL; }
+      k_fplane<T, NF0, NF1, false><<<dim3(NF2, npair), PLANE_THREADS, sm_fplane(cr), st>>>(
+          BC, reinterpret_cast<const T*>(c->vtot.p), nl, Wp, W, natom, nslot, inv_nf, tw(c, 3), tw(c, 4));
+      const int nthr = 128;
+      k_nl_reduce<T><<<dim3((natom * nl.npmax + nthr - 1) / nthr, npair), nthr, 0, st>>>(
+          Wp, W, reinterpret_cast<const int*>(c->nl.atom_slot.p), reinterpret_cast<const int*>(c->nl.atom_slot_list.p),
+          reinterpret_cast<const T*>(c->nl.wgt.p), natom, nslot, nl.npmax);
+    }
+    k_fplane<T, NF0, NF1, true><<<dim3(NF2, npair), PLANE_THREADS, sm_fplane(cr), st>>>(
+        BC, reinterpret_cast<const T*>(c->vtot.p), nl, Wp, W, natom, nslot, inv_nf, tw(c, 3), tw(c, 4));
+    k_zfold<T, N2, NF2><<<dim3(N1, ntx, npair), PENCIL_THREADS, sm_zfold(), st>>>(BC, K, AD, N0, N1, tw(c, 2), tw(c, 5));
+    k_cxy_inv<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(AD, out, ldo, nband, band0, accumulate, tw(c, 0), tw(c, 1));
+    PWB_CUDA(cudaGetLastError());
+    return PW_OK;
+  }
+
+  static int teter_batch(pw_ctx* c, const T* r, int ld, T* out, int ldo, int nband, int band0, int npair,
+                         int accumulate, cudaStream_t st) {
+    int rc = set_attrs();
+    if (rc) return rc;
+    V* AD = reinterpret_cast<V*>(c->s_ad.p);
+    const T inv_nc = (T)(1.0 / (double)c->ntot);
+    const int ntx = (N0 + TX - 1) / TX;
+    k_cxy_fwd<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(r, ld, nband, band0, AD, tw(c, 0), tw(c, 1));
+    k_zteter<T, N2><<<dim3(N1, ntx, npair), PENCIL_THREADS, sm_zteter(), st>>>(
+        AD, reinterpret_cast<const T*>(c->teter.p), N0, N1, inv_nc, tw(c, 2));
+    k_cxy_inv<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(AD, out, ldo, nband, band0, accumulate, tw(c, 0), tw(c, 1));
+    PWB_CUDA(cudaGetLastError());
+    return PW_OK;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// dispatch over the instantiated grids
+// ---------------------------------------------------------------------------
+using HpsiFn = int (*)(pw_ctx*, const void*, int, void*, int, int, int, int, int, cudaStream_t);
+using ChunkFn = int (*)();
+
+template <typename T, int N0, int N1, int N2>
+static int hpsi_thunk(pw_ctx* c, const void* psi, int ld, void* out, int ldo, int nband, int band0, int npair,
+                      int acc, cudaStream_t st) {
+  return Plan<T, N0, N1, N2>::hpsi_batch(c, (const T*)psi, ld, (T*)out, ldo, nband, band0, npair, acc, st);
+}
+template <typename T, int N0, int N1, int N2>
+static int teter_thunk(pw_ctx* c, const void* psi, int ld, void* out, int ldo, int nband, int band0, int npair,
+                       int acc, cudaStream_t st) {
+  return Plan<T, N0, N1, N2>::teter_batch(c, (const T*)psi, ld, (T*)out, ldo, nband, band0, npair, acc, st);
+}
+template <typename T, int N0, int N1, int N2> static int cr_thunk() { return Plan<T, N0, N1, N2>::chunk_rows(); }
+
+struct GridEntry {
+  int n0, n1, n2;
+  HpsiFn hpsi[2];
+  HpsiFn teter[2];
+  ChunkFn cr[2];
+};
+
+#define PWB_GRID(a, b, c)                                                                          \
+  {a, b, c, {hpsi_thunk<double, a, b, c>, hpsi_thunk<float, a, b, c>},                             \
+   {teter_thunk<double, a, b, c>, teter_thunk<float, a, b, c>},                                    \
+   {cr_thunk<double, a, b, c>, cr_thunk<float, a, b, c>}},
+
+static const GridEntry kGrids[] = {
+#include "grids.inc"
+};
+#undef PWB_GRID
+
+const GridEntry* find_grid(const int n[3]) {
+  for (const auto& g : kGrids)
+    if (g.n0 == n[0] && g.n1 == n[1] && g.n2 == n[2]) return &g;
+  return nullptr;
+}
+
+int grid_chunk_rows(const int n[3], int prec) {
+  const GridEntry* g = find_grid(n);
+  return g ? g->cr[prec == PW_F32 ? 1 : 0]() : -1;
+}
+
+int run_hpsi(pw_ctx* c, const void* psi, int ld, void* out, int ldo, int nband, int band0, int npair, int acc,
+             cudaStream_t st) {
+  const GridEntry* g = find_grid(c->n);
+  if (!g) { set_error("grid not built into this library"); return PW_EUNSUPPORTED; }
+  return g->hpsi[c->prec == PW_F32 ? 1 : 0](c, psi, ld, out, ldo, nband, band0, npair, acc, st);
+}
+
+int run_teter(pw_ctx* c, const void* r, int ld, void* out, int ldo, int nband, int band0, int npair, int acc,
+              cudaStream_t st) {
+  const GridEntry* g = find_grid(c->n);
+  if (!g) { set_error("grid not built into this library"); return PW_EUNSUPPORTED; }
+  return g->teter[c->prec == PW_F32 ? 1 : 0](c, r, ld, out, ldo, nband, band0, npair, acc, st);
+}
+
+}  // namespace pwb

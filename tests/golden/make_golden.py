@@ -1,0 +1,60 @@
+"""Regenerate the golden fixtures in this folder from reference functions.
+
+The vectors come from the reference's own ``IP_c2f``, ``IP_f2c``, ``spline``
+and ``seval`` (src/utility.cpp), compiled from the reference source tree by
+``oracle/build_ref.py``.  Inputs are seeded.  Run from the repository root:
+``python tests/golden/make_golden.py``.
+"""
+import ctypes as C
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+from oracle import build_ref  # noqa: E402
+
+OUT = Path(__file__).resolve().parent / "ref_utility.npz"
+
+
+def main():
+    lib = C.CDLL(str(build_ref.build()))
+    dp = C.POINTER(C.c_double)
+    ip = C.POINTER(C.c_int)
+    rng = np.random.Generator(np.random.Philox(20261203))
+    data = {}
+    for tag, Nc, Nf in (("a", (4, 4, 4), (8, 8, 8)), ("b", (6, 4, 8), (12, 8, 16)), ("c", (8, 6, 4), (16, 12, 8))):
+        nhc = (Nc[0] // 2 + 1) * Nc[1] * Nc[2]
+        nhf = (Nf[0] // 2 + 1) * Nf[1] * Nf[2]
+        X = rng.standard_normal(nhc) + 1j * rng.standard_normal(nhc)
+        Y = np.zeros(nhf, complex)
+        nc = (C.c_int * 3)(*Nc)
+        nf = (C.c_int * 3)(*Nf)
+        lib.ref_ip_c2f(nc, nf, X.ctypes.data_as(dp), Y.ctypes.data_as(dp))
+        Yin = rng.standard_normal(nhf) + 1j * rng.standard_normal(nhf)
+        Z = np.zeros(nhc, complex)
+        lib.ref_ip_f2c(nc, nf, Z.ctypes.data_as(dp), Yin.ctypes.data_as(dp))
+        data[f"c2f_{tag}_Nc"] = np.array(Nc)
+        data[f"c2f_{tag}_Nf"] = np.array(Nf)
+        data[f"c2f_{tag}_in"] = X
+        data[f"c2f_{tag}_out"] = Y
+        data[f"f2c_{tag}_in"] = Yin
+        data[f"f2c_{tag}_out"] = Z
+    n = 200
+    x = np.sort(rng.uniform(-3, 3, n))
+    y = np.exp(-x * x) * np.cos(3 * x)
+    b, c, d = np.zeros(n), np.zeros(n), np.zeros(n)
+    lib.ref_spline(n, x.ctypes.data_as(dp), y.ctypes.data_as(dp), b.ctypes.data_as(dp), c.ctypes.data_as(dp),
+                   d.ctypes.data_as(dp))
+    u = rng.uniform(-3.5, 3.5, 100)
+    v = np.zeros(100)
+    lib.ref_seval(v.ctypes.data_as(dp), 100, u.ctypes.data_as(dp), n, x.ctypes.data_as(dp), y.ctypes.data_as(dp),
+                  b.ctypes.data_as(dp), c.ctypes.data_as(dp), d.ctypes.data_as(dp))
+    data.update(spl_x=x, spl_y=y, spl_b=b, spl_c=c, spl_d=d, sev_u=u, sev_v=v)
+    np.savez_compressed(OUT, **data)
+    print(OUT, OUT.stat().st_size)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,166 @@
+"""GPU parity of the H*psi and Teter kernels against the FP64 oracle, called
+through the C ABI.  Tolerances (relative, max-norm over the block):
+H*psi <= 1e-12 in FP64 and <= 1e-5 in FP32; Teter the same."""
+import numpy as np
+import pytest
+
+from oracle import pw
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"f64": 1e-12, "f32": 1e-5}
+
+
+def _rel(a, b):
+    return float(np.abs(a - b).max() / np.abs(b).max())
+
+
+def make_system(nc, reps=(1, 1, 1), a=10.26, seed=20261203 + 1, lengths=None):
+    L, z, pos = pw.make_crystal("Si", reps, a, 0.02, seed)
+    if lengths is not None:
+        L = np.asarray(lengths, dtype=np.float64)
+    nf = tuple(2 * n for n in nc)
+    T, sp = pw.build_tables(L, z, pos, nc, nf, seed_v=seed + 100)
+    return T
+
+
+def make_ctx(T, prec, band_batch=None):
+    from pwdft_develop_b200 import Context
+    c = Context(T.dm.length, T.dm.numGrid, T.dm.numGridFine, precision=prec)
+    c.set_vtot(T.vtot)
+    c.set_nonlocal([(a[0].idx, np.stack([pp.val[:, 0] for pp in a]), np.array([pp.wgt for pp in a]))
+                    for a in T.pseudo])
+    if band_batch:
+        c.set_band_batch(band_batch)
+    return c
+
+
+@pytest.fixture(scope="module")
+def si8():
+    return make_system((24, 24, 24))
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_hpsi_parity_si8(si8, prec):
+    import torch
+    T = si8
+    psi = pw.random_orthonormal_psi(T.dm.ntot, 24, 5)
+    ref = pw.mult_spinor(T, psi)
+    c = make_ctx(T, prec)
+    x = torch.tensor(psi, dtype=c.torch_dtype, device="cuda")
+    y = c.hpsi(x)
+    torch.cuda.synchronize()
+    got = y.double().cpu().numpy()
+    assert _rel(got, ref) <= TOL[prec]
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_teter_parity_si8(si8, prec):
+    import torch
+    T = si8
+    rng = np.random.default_rng(9)
+    r = rng.standard_normal((7, T.dm.ntot))
+    ref = pw.add_teter_precond(T, r)
+    c = make_ctx(T, prec)
+    got = c.teter(torch.tensor(r, dtype=c.torch_dtype, device="cuda")).double().cpu().numpy()
+    assert _rel(got, ref) <= TOL[prec]
+
+
+def test_hpsi_noncubic_grid_f64():
+    """(24,16,20) coarse grid in a 10.26 x 7.0 x 8.5 cell."""
+    import torch
+    T = make_system((24, 16, 20), lengths=(10.26, 7.0, 8.5))
+    psi = pw.random_orthonormal_psi(T.dm.ntot, 6, 8)
+    ref = pw.mult_spinor(T, psi)
+    c = make_ctx(T, "f64")
+    got = c.hpsi(torch.tensor(psi, device="cuda")).cpu().numpy()
+    assert _rel(got, ref) <= TOL["f64"]
+
+
+@pytest.mark.parametrize("nband,batch", [(1, None), (5, None), (7, 2), (9, 4)])
+def test_hpsi_odd_bands_and_batches(si8, nband, batch):
+    import torch
+    T = si8
+    psi = pw.random_orthonormal_psi(T.dm.ntot, nband, 11 + nband)
+    ref = pw.mult_spinor(T, psi)
+    c = make_ctx(T, "f64", band_batch=batch)
+    got = c.hpsi(torch.tensor(psi, device="cuda")).cpu().numpy()
+    assert _rel(got, ref) <= TOL["f64"]
+
+
+def test_hpsi_accumulate_and_zero_bands(si8):
+    import torch
+    T = si8
+    psi = pw.random_orthonormal_psi(T.dm.ntot, 4, 21)
+    base = np.random.default_rng(2).standard_normal(psi.shape)
+    ref = base + pw.mult_spinor(T, psi)
+    c = make_ctx(T, "f64")
+    out = torch.tensor(base, device="cuda")
+    c.hpsi(torch.tensor(psi, device="cuda"), out=out, accumulate=True)
+    assert _rel(out.cpu().numpy(), ref) <= TOL["f64"]
+    empty = torch.zeros((0, T.dm.ntot), dtype=torch.float64, device="cuda")
+    assert c.hpsi(empty).shape == (0, T.dm.ntot)
+
+
+def test_hpsi_host_entry_matches_device(si8):
+    import torch
+    T = si8
+    psi = pw.random_orthonormal_psi(T.dm.ntot, 6, 31)
+    c = make_ctx(T, "f64")
+    dev = c.hpsi(torch.tensor(psi, device="cuda")).cpu().numpy()
+    host = c.hpsi_host(psi)
+    assert np.array_equal(dev, host)
+
+
+def test_hpsi_local_only_and_no_projectors(si8):
+    import torch
+    from pwdft_develop_b200 import Context
+    T0 = pw.HamTables(si8.dm, si8.ekin, si8.teter, si8.vtot, [])
+    psi = pw.random_orthonormal_psi(T0.dm.ntot, 4, 41)
+    ref = pw.mult_spinor(T0, psi)
+    c = Context(T0.dm.length, T0.dm.numGrid, T0.dm.numGridFine, "f64")
+    c.set_vtot(T0.vtot)
+    got = c.hpsi(torch.tensor(psi, device="cuda")).cpu().numpy()
+    assert _rel(got, ref) <= TOL["f64"]
+
+
+def test_hpsi_requires_potential(si8):
+    import torch
+    from pwdft_develop_b200 import Context, PwError
+    c = Context(si8.dm.length, si8.dm.numGrid, si8.dm.numGridFine, "f64")
+    with pytest.raises(PwError) as e:
+        c.hpsi(torch.zeros((2, si8.dm.ntot), dtype=torch.float64, device="cuda"))
+    assert e.value.code == -6
+
+
+@pytest.fixture(scope="module")
+def si64():
+    return make_system((48, 48, 48), reps=(2, 2, 2))
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_hpsi_parity_si64_subset(si64, prec):
+    """Si64 (48^3 / 96^3, 320 projectors): a block of 6 bands vs the oracle."""
+    import torch
+    T = si64
+    psi = pw.random_orthonormal_psi(T.dm.ntot, 6, 51)
+    ref = pw.mult_spinor(T, psi)
+    c = make_ctx(T, prec)
+    got = c.hpsi(torch.tensor(psi, dtype=c.torch_dtype, device="cuda")).double().cpu().numpy()
+    assert _rel(got, ref) <= TOL[prec]
+
+
+def test_hpsi_si64_full_block_properties(si64):
+    """160 bands: Hermiticity of psi^T H psi and linearity H(a x + y)."""
+    import torch
+    T = si64
+    c = make_ctx(T, "f64", band_batch=160)
+    g = torch.Generator(device="cuda").manual_seed(5)
+    X = torch.randn((160, T.dm.ntot), dtype=torch.float64, device="cuda", generator=g)
+    HX = c.hpsi(X)
+    M = X @ HX.T
+    assert float((M - M.T).abs().max() / M.abs().max()) < 1e-12
+    Y = torch.randn((160, T.dm.ntot), dtype=torch.float64, device="cuda", generator=g)
+    lhs = c.hpsi(2.5 * X + Y)
+    rhs = 2.5 * HX + c.hpsi(Y)
+    assert float((lhs - rhs).abs().max() / rhs.abs().max()) < 1e-12
