@@ -1,0 +1,373 @@
+"""Benchmark: H*psi bands/s on Si64 (2x2x2 diamond Si, a = 20.52 bohr, 48^3
+coarse / 96^3 fine grids, 160 bands, HGH LDA with real-space projectors).
+
+One step = one H*psi sweep over the 160-band block (KohnSham::MultSpinor on
+every band).  `value` is the device-timed throughput with inputs resident in
+HBM (L2 flushed between steps); `e2e` is the same sweep through the host
+C-ABI entry pw_hpsi_host (host->device copy of psi and device->host copy of
+H*psi inside the timed region).  Under torchrun each rank runs its own
+160-band block (bands shard with no exchange: weak scaling) and rank 0 prints
+the JSON line with the max-over-ranks time.
+
+--impl reference times the reference algorithm's CPU form (the FP64 NumPy
+restatement in oracle/, one band per worker process over all host cores).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+SEED = 20261203 + 2          # configuration 2 (Si64)
+NC = (48, 48, 48)
+NF = (96, 96, 96)
+NBAND = 160
+A_CELL = 10.26
+WORKLOAD = ("Si64 diamond 2x2x2 (a=20.52 bohr, +-0.02 bohr seeded displacements), HGH LDA, "
+            "48^3 coarse / 96^3 fine grids, 160 bands (128 occ + 32 extra), real-space projectors")
+
+
+def si64_atoms():
+    rng = np.random.Generator(np.random.Philox(SEED))
+    base = np.array([[0, 0, 0], [0, .5, .5], [.5, 0, .5], [.5, .5, 0],
+                     [.25, .25, .25], [.25, .75, .75], [.75, .25, .75], [.75, .75, .25]])
+    pos = []
+    for cz in range(2):
+        for cy in range(2):
+            for cx in range(2):
+                for f in base:
+                    pos.append((np.array([cx, cy, cz]) + f) * A_CELL)
+    pos = np.array(pos) + rng.uniform(-0.02, 0.02, size=(64, 3))
+    return np.array([2 * A_CELL] * 3), np.full(64, 14, np.int32), pos
+
+
+def synthetic_vtot(n):
+    rng = np.random.Generator(np.random.Philox(SEED + 100))
+    return rng.uniform(-1.0, 0.5, size=n)
+
+
+def load_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# algorithmic bytes per launch of each kernel kind for one batch of npair pairs
+def algorithmic_bytes(kind: int, npair: int, s: int, nent: int, npmax: int, nslot: int, natom: int) -> float:
+    nc = NC[0] * NC[1] * NC[2]
+    nf = NF[0] * NF[1] * NF[2]
+    nb = NF[2] * (NC[1] + 1) * (NC[0] + 1)
+    c = 2 * s
+    tables = nent * (4 + npmax * s) + nslot * 12
+    if kind == 0:   # coarse xy forward: 2 real bands in, complex field out
+        return npair * (2 * nc * s + nc * c)
+    if kind == 1:   # z pad: A in, K out, B out (+ ekin table once)
+        return npair * (nc * c + nc * c + nb * c) + nc * s
+    if kind == 2:   # fine-plane gather: B in, partial dots out (+ tables once)
+        return npair * (nb * c + nslot * npmax * c) + tables
+    if kind == 3:   # projector reduce
+        return npair * (nslot * npmax * c + natom * npmax * c)
+    if kind == 4:   # fine-plane apply: B in, C out (+ V_loc and tables once)
+        return npair * (2 * nb * c + natom * npmax * c) + nf * s + tables
+    if kind == 5:   # z fold: C in, K in, D out
+        return npair * (nb * c + 2 * nc * c)
+    if kind == 6:   # coarse xy inverse: D in, 2 real bands out
+        return npair * (nc * c + 2 * nc * s)
+    return 0.0
+
+
+def hpsi_model_bytes_per_band(s: int, bw: int, nproj: int, natom: int, npts_total: int) -> float:
+    """Pinned whole-H*psi model: B_band(s) = 2sN_c + 4s(2H_c+2H_f) + 2sN_f + 4sH_c
+    + [sN_f + (s n_proj + 4 n_atom) n_pts]/bw."""
+    nc = NC[0] * NC[1] * NC[2]
+    nf = NF[0] * NF[1] * NF[2]
+    hc = (NC[0] // 2 + 1) * NC[1] * NC[2]
+    hf = (NF[0] // 2 + 1) * NF[1] * NF[2]
+    npts = npts_total / max(natom, 1)
+    return 2 * s * nc + 4 * s * (2 * hc + 2 * hf) + 2 * s * nf + 4 * s * hc + \
+        (s * nf + (s * nproj + 4 * natom) * npts) / bw
+
+
+class Clocks:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.file = None
+
+    def start(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.file.flush()
+        lines = Path(self.file.name).read_text().strip().splitlines()
+        os.unlink(self.file.name)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def oracle_sample_worker(args):
+    """One H*psi band through the FP64 NumPy restatement (CPU baseline)."""
+    os.environ["OMP_NUM_THREADS"] = "1"
+    band = args
+    from oracle import pw
+    L, z, pos = si64_atoms()
+    T, _ = pw.build_tables(L, 14, pos, NC, NF, vtot=synthetic_vtot(int(np.prod(NF))))
+    rng = np.random.Generator(np.random.Philox(SEED + 7 + band))
+    psi = rng.standard_normal((1, T.dm.ntot))
+    t0 = time.perf_counter()
+    pw.mult_spinor(T, psi)
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(bands: int = 4):
+    """Serial oracle on a bounded sample: `bands` single-band H*psi calls."""
+    from oracle import pw
+    L, z, pos = si64_atoms()
+    T, _ = pw.build_tables(L, 14, pos, NC, NF, vtot=synthetic_vtot(int(np.prod(NF))))
+    rng = np.random.Generator(np.random.Philox(SEED + 7))
+    psi = rng.standard_normal((bands, T.dm.ntot))
+    pw.mult_spinor(T, psi[:1])      # warm
+    t0 = time.perf_counter()
+    for b in range(bands):
+        pw.mult_spinor(T, psi[b:b + 1])
+    dt = time.perf_counter() - t0
+    return {"value": bands / dt, "unit": "bands/s", "cores": 1, "kind": "port",
+            "sample": f"{bands} single-band H*psi applications of the Si64 workload through the FP64 NumPy "
+                      f"restatement (oracle/pw.py), one thread, {dt:.1f} s"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import multiprocessing as mp
+    ncores = os.cpu_count() or 1
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(ncores) as pool:
+        for w in range(args.warmup):
+            pool.map(oracle_sample_worker, list(range(ncores)))
+        t0 = time.perf_counter()
+        for s in range(args.steps):
+            pool.map(oracle_sample_worker, [s * ncores + i for i in range(ncores)])
+        dt = time.perf_counter() - t0
+    v = args.steps * ncores / dt
+    line = {"impl": "reference", "metric": "H*psi bands/s", "value": v, "unit": "bands/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": WORKLOAD, "sample_bands_per_step": ncores},
+            "cpu_baseline": {"value": v, "unit": "bands/s", "cores": ncores, "kind": "port",
+                             "sample": f"each step: {ncores} single-band H*psi (one per process) through the FP64 "
+                                       f"NumPy restatement of the reference path (oracle/pw.py)"},
+            "e2e": {"value": v, "unit": "bands/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    from pwdft_develop_b200 import Context
+    from pwdft_develop_b200.core import KERNEL_KINDS
+
+    prec = args.precision
+    L, z, pos = si64_atoms()
+    ctx = Context(L, NC, NF, precision=prec, device=local)
+    ctx.set_vtot(synthetic_vtot(ctx.ntotFine))
+    ctx.set_atoms(z, pos)
+    ctx.set_band_batch(NBAND)
+    dt_t = ctx.torch_dtype
+    g = torch.Generator(device="cuda").manual_seed(SEED + rank)
+    X = torch.randn((NBAND, ctx.ntot), dtype=torch.float64, device="cuda", generator=g)
+    R = torch.linalg.cholesky(X @ X.T).T                     # Cholesky-QR (set-up, untimed)
+    X = torch.linalg.solve_triangular(R, X, upper=True, left=True).contiguous()
+    X = X.to(dt_t).contiguous()
+    Y = torch.empty_like(X)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    for _ in range(args.warmup):
+        ctx.hpsi(X, out=Y)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = Clocks(local)
+    clocks.start()
+    l0 = ctx.launches()
+    total_ms = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        ctx.hpsi(X, out=Y)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        total_ms += e0.elapsed_time(e1)
+    launches = ctx.launches() - l0
+    ck = clocks.stop()
+    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.barrier()
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    value = world * NBAND * args.steps / (total_ms / 1e3)
+
+    # per-kernel device time (event-bracketed launches, same stream)
+    ctx.profile(True)
+    for _ in range(args.steps):
+        flush.zero_()
+        ctx.hpsi(X, out=Y)
+    torch.cuda.synchronize()
+    kern = {}
+    for k in range(8):
+        ms, n = ctx.profile_read(k)
+        if n:
+            kern[KERNEL_KINDS[k]] = {"launches": n, "avg_us": ms / n * 1e3, "total_ms": ms}
+    ctx.profile(False)
+    dom_name = max(kern, key=lambda k: kern[k]["total_ms"])
+    dom_kind = [k for k, v in KERNEL_KINDS.items() if v == dom_name][0]
+    s = 4 if prec == "f32" else 8
+    npts_total = 0
+    natom = len(pos)
+    from pwdft_develop_b200.core import hgh_atom_projectors
+    idx0, val0, _ = hgh_atom_projectors(L, NF, 14, pos[0])
+    npts_total = sum(len(hgh_atom_projectors(L, NF, 14, p)[0]) for p in pos)
+    # tile slots ~ atoms x fine planes they touch (exact count from the library is not exported)
+    nslot_est = int(natom * (2 * 3.5 / (2 * A_CELL) * NF[2] + 1))
+    alg = algorithmic_bytes(dom_kind, NBAND // 2, s, npts_total, 5, nslot_est, natom)
+    achieved = alg / (kern[dom_name]["avg_us"] * 1e-6) / 1e9
+    peak, peak_kind = load_peaks()
+    traffic = None
+    tf = ROOT / "profiles" / f"traffic_{prec}.json"
+    if tf.exists():
+        traffic = json.loads(tf.read_text()).get(dom_name)
+    model = hpsi_model_bytes_per_band(s, NBAND, 5 * natom, natom, npts_total)
+
+    # end to end through the host C-ABI entry (pinned host buffers)
+    Xh = X.cpu().pin_memory()
+    Yh = torch.empty_like(Xh).pin_memory()
+    import ctypes as C
+    from pwdft_develop_b200._lib import check, lib
+    for _ in range(max(1, args.warmup)):
+        check(lib.pw_hpsi_host(ctx.handle, C.c_void_p(Xh.data_ptr()), ctx.ntot, C.c_void_p(Yh.data_ptr()),
+                               ctx.ntot, NBAND, 0))
+    torch.cuda.synchronize()
+    e2e_ms = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        check(lib.pw_hpsi_host(ctx.handle, C.c_void_p(Xh.data_ptr()), ctx.ntot, C.c_void_p(Yh.data_ptr()),
+                               ctx.ntot, NBAND, 0))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms += e0.elapsed_time(e1)
+    t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_ms = float(t.item())
+    bytes_io = NBAND * ctx.ntot * s
+
+    if rank == 0:
+        line = {
+            "metric": "H*psi bands/s", "value": value, "unit": "bands/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": prec, "data": "synthetic",
+            "config": {"workload": WORKLOAD, "grid": list(NC), "fine_grid": list(NF), "bands": NBAND,
+                       "band_batch": NBAND, "l2": "flushed between steps (256 MB device write)",
+                       "parallelism": f"band blocks, {world} replica(s)"},
+            "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
+                         "algorithmic_bytes_per_launch": alg, "avg_launch_us": kern[dom_name]["avg_us"]},
+            "hpsi_model": {"bytes_per_band": model, "achieved_GBs": model * value / world / 1e9,
+                           "frac": model * value / world / 1e9 / peak},
+            "kernels": kern,
+            "gpu_launches": launches,
+            "e2e": {"value": world * NBAND * args.steps / (e2e_ms / 1e3), "unit": "bands/s",
+                    "h2d_bytes_per_step": bytes_io, "d2h_bytes_per_step": bytes_io},
+            "clocks": ck,
+        }
+        if args.cpu_baseline and world == 1:
+            line["cpu_baseline"] = cpu_baseline(args.cpu_bands)
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
+    ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--cpu-bands", type=int, default=64)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

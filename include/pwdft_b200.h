@@ -93,6 +93,44 @@ PW_API int pw_hpsi_host(pw_ctx* ctx, const void* psi, int ld, void* hpsi, int ld
 PW_API int pw_teter_precond(pw_ctx* ctx, const void* r, int ld, void* w, int ldw, int nband,
                      int accumulate, void* stream);
 
+/* HGH species built into the library (Si: 14, Al: 13; utilities/HGH.m:234-276):
+ * valence charge, self energy E_self (HGH.m:995), cut-off radii, number of
+ * nonlocal projectors. */
+PW_API int pw_hgh_species(int znuc, double* zion, double* eself, double* rcut_nonlocal, double* rcut_rho,
+                          int* nproj);
+
+/* Atoms (Cartesian bohr, natom x 3) with the library's HGH tables: builds every
+ * atom's projector set as PeriodTable::CalculateNonlocalPP does
+ * (src/SCF/periodtable.cpp:994-1240) and the pseudocharge of
+ * PeriodTable::CalculatePseudoCharge (periodtable.cpp:282-377, with Cartesian
+ * minimum-image distances), the work of KohnSham::CalculatePseudoPotential
+ * (src/SCF/hamiltonian.cpp:327-918).  Calls pw_set_nonlocal internally. */
+PW_API int pw_set_atoms(pw_ctx* ctx, int natom, const int* znuc, const double* pos);
+/* Pseudocharge rho_ps on the fine grid (host, N_fine doubles). */
+PW_API int pw_get_pseudocharge(const pw_ctx* ctx, double* rho_fine_host);
+/* One atom's projector set: npts, nproj, idx[npts], val4[nproj][npts][4]
+ * (VAL, DX, DY, DZ), wgt[nproj].  Output pointers may be NULL. */
+PW_API int pw_get_atom_projectors(const pw_ctx* ctx, int atom, int* npts, int* nproj, int* idx, double* val4,
+                                  double* wgt);
+/* Host-only variants (no context, no GPU): one atom's projector set for a cell
+ * and fine grid (call with NULL outputs first to get npts, nproj), and the
+ * summed pseudocharge of natom atoms on the fine grid. */
+PW_API int pw_hgh_atom_projectors(const double length[3], const int numGridFine[3], int znuc, const double pos[3],
+                                  int* npts, int* nproj, int* idx, double* val4, double* wgt);
+PW_API int pw_hgh_pseudocharge(const double length[3], const int numGridFine[3], int natom, const int* znuc,
+                               const double* pos, double* rho_fine_host);
+/* Number of CUDA kernels this context has launched. */
+PW_API int pw_stats(const pw_ctx* ctx, long* kernel_launches);
+
+/* Per-kernel CUDA-event timing.  pw_profile(ctx, 1) clears the records and
+ * brackets every later kernel launch of this context with events on its
+ * stream; pw_profile_read returns the summed device time and the number of
+ * launches of one kernel kind: 0 coarse-plane FFT, 1 z-pad, 2 fine-plane
+ * projector gather, 3 projector reduce, 4 fine-plane apply, 5 z-fold,
+ * 6 coarse-plane inverse, 7 Teter z-pencil, 8 Gram, 9 density, 10 other. */
+PW_API int pw_profile(pw_ctx* ctx, int enable);
+PW_API int pw_profile_read(pw_ctx* ctx, int kind, double* total_ms, long* count);
+
 /* Maximum number of bands processed per internal batch (sets scratch size).
  * Default 64. Scratch grows to hold ceil(nband_batch/2) band pairs. */
 PW_API int pw_set_band_batch(pw_ctx* ctx, int nband_batch);

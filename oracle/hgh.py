@@ -195,6 +195,10 @@ def hgh_table(znuc: int, with_splines: bool = True) -> HGHSpecies:
         D, V = np.linalg.eigh(H)
         order = np.argsort(-D, kind="stable")
         D, V = D[order], V[:, order]
+        # eigenvector sign is arbitrary (MATLAB eig); fix it: largest |component| > 0
+        for a in range(3):
+            if V[np.argmax(np.abs(V[:, a])), a] < 0:
+                V[:, a] = -V[:, a]
         fns = [_proj_radial(l, i, rl) for i in (1, 2, 3)]
         for a in range(3):
             if abs(D[a]) <= 1e-10:

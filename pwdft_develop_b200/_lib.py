@@ -46,6 +46,15 @@ SIGNATURES: dict[str, tuple] = {
     "pw_hpsi_host": (_i, [_vp, _vp, _i, _vp, _i, _i, _i]),
     "pw_teter_precond": (_i, [_vp, _vp, _i, _vp, _i, _i, _i, _vp]),
     "pw_set_band_batch": (_i, [_vp, _i]),
+    "pw_hgh_species": (_i, [_i, _dp, _dp, _dp, _dp, _ip]),
+    "pw_set_atoms": (_i, [_vp, _i, _ip, _dp]),
+    "pw_get_pseudocharge": (_i, [_vp, _dp]),
+    "pw_get_atom_projectors": (_i, [_vp, _i, _ip, _ip, _ip, _dp, _dp]),
+    "pw_stats": (_i, [_vp, C.POINTER(_l)]),
+    "pw_hgh_atom_projectors": (_i, [_dp, _ip, _i, _dp, _ip, _ip, _ip, _dp, _dp]),
+    "pw_hgh_pseudocharge": (_i, [_dp, _ip, _i, _ip, _dp, _dp]),
+    "pw_profile": (_i, [_vp, _i]),
+    "pw_profile_read": (_i, [_vp, _i, _dp, C.POINTER(_l)]),
 }
 
 for _name, (_res, _args) in SIGNATURES.items():

@@ -132,3 +132,77 @@ class Context:
         check(lib.pw_teter_precond(self._h, _ptr(r), self.ntot, _ptr(out), self.ntot, nb, int(accumulate),
                                    _stream(stream)))
         return out
+
+
+# ---------------------------------------------------------------------------
+# set-up helpers over the library's own HGH tables
+# ---------------------------------------------------------------------------
+def hgh_species(znuc: int) -> dict:
+    zion, eself, rnl, rrho = C.c_double(), C.c_double(), C.c_double(), C.c_double()
+    npj = C.c_int()
+    check(lib.pw_hgh_species(int(znuc), C.byref(zion), C.byref(eself), C.byref(rnl), C.byref(rrho), C.byref(npj)))
+    return dict(zion=zion.value, eself=eself.value, rcut_nonlocal=rnl.value, rcut_rho=rrho.value, nproj=npj.value)
+
+
+def hgh_atom_projectors(length, numGridFine, znuc: int, pos):
+    """Host-only projector set of one atom: (idx, val4[nproj, npts, 4], wgt)."""
+    L = (C.c_double * 3)(*[float(x) for x in length])
+    nf = (C.c_int * 3)(*[int(x) for x in numGridFine])
+    p = (C.c_double * 3)(*[float(x) for x in pos])
+    npts, nproj = C.c_int(), C.c_int()
+    check(lib.pw_hgh_atom_projectors(L, nf, int(znuc), p, C.byref(npts), C.byref(nproj), None, None, None))
+    idx = np.zeros(npts.value, np.int32)
+    val = np.zeros((nproj.value, npts.value, 4))
+    wgt = np.zeros(nproj.value)
+    check(lib.pw_hgh_atom_projectors(L, nf, int(znuc), p, None, None, idx.ctypes.data_as(_lib._ip),
+                                     val.ctypes.data_as(_lib._dp), wgt.ctypes.data_as(_lib._dp)))
+    return idx, val, wgt
+
+
+def hgh_pseudocharge(length, numGridFine, znuc, pos) -> np.ndarray:
+    L = (C.c_double * 3)(*[float(x) for x in length])
+    nf = (C.c_int * 3)(*[int(x) for x in numGridFine])
+    z = np.ascontiguousarray(znuc, np.int32)
+    ps = np.ascontiguousarray(pos, np.float64)
+    out = np.zeros(int(np.prod(numGridFine)))
+    check(lib.pw_hgh_pseudocharge(L, nf, len(z), z.ctypes.data_as(_lib._ip), ps.ctypes.data_as(_lib._dp),
+                                  out.ctypes.data_as(_lib._dp)))
+    return out
+
+
+def _ctx_set_atoms(self, znuc, pos):
+    z = np.ascontiguousarray(znuc, np.int32)
+    ps = np.ascontiguousarray(pos, np.float64)
+    check(lib.pw_set_atoms(self._h, len(z), z.ctypes.data_as(_lib._ip), ps.ctypes.data_as(_lib._dp)))
+
+
+def _ctx_pseudocharge(self) -> np.ndarray:
+    out = np.zeros(self.ntotFine)
+    check(lib.pw_get_pseudocharge(self._h, out.ctypes.data_as(_lib._dp)))
+    return out
+
+
+def _ctx_launches(self) -> int:
+    n = C.c_long()
+    check(lib.pw_stats(self._h, C.byref(n)))
+    return n.value
+
+
+def _ctx_profile(self, enable: bool):
+    check(lib.pw_profile(self._h, int(enable)))
+
+
+def _ctx_profile_read(self, kind: int):
+    t, n = C.c_double(), C.c_long()
+    check(lib.pw_profile_read(self._h, int(kind), C.byref(t), C.byref(n)))
+    return t.value, n.value
+
+
+Context.set_atoms = _ctx_set_atoms
+Context.pseudocharge = _ctx_pseudocharge
+Context.launches = _ctx_launches
+Context.profile = _ctx_profile
+Context.profile_read = _ctx_profile_read
+
+KERNEL_KINDS = {0: "coarse_xy_fwd", 1: "z_pad", 2: "fine_plane_gather", 3: "nl_reduce", 4: "fine_plane_apply",
+                5: "z_fold", 6: "coarse_xy_inv", 7: "z_teter", 8: "gram", 9: "density", 10: "other"}

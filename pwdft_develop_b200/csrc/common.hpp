@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "../../include/pwdft_b200.h"
+#include "pseudo.hpp"
 
 namespace pwb {
 
@@ -57,6 +58,12 @@ struct NonlocalDev {
   DevBuf wgt;             // T     [natom*npmax]  gamma * vol / N_fine
 };
 
+// Kernel kinds for pw_profile_read.
+enum KernelKind {
+  KK_CXY_FWD = 0, KK_ZPAD, KK_FPLANE_GATHER, KK_NL_REDUCE, KK_FPLANE_APPLY, KK_ZFOLD, KK_CXY_INV, KK_ZTETER,
+  KK_GRAM, KK_DENSITY, KK_MISC, KK_COUNT
+};
+
 }  // namespace pwb
 
 // Opaque context behind the C ABI.
@@ -79,6 +86,17 @@ struct pw_ctx {
   pwb::NonlocalDev nl;
   // host copies kept for setup-time work
   std::vector<double> h_vtot;
+  // atoms set through pw_set_atoms (HGH species built in this library)
+  std::vector<int> atom_z;
+  std::vector<double> atom_pos;            // natom x 3, Cartesian bohr
+  std::vector<pwb::AtomNL> h_nl;           // per-atom vnlList incl. DX/DY/DZ columns
+  std::vector<double> h_rhops;             // pseudocharge on the fine grid
+  // kernel launch accounting (pw_stats) and optional per-kernel event timing
+  long launches = 0;
+  bool prof_on = false;
+  struct ProfRec { int kind; cudaEvent_t a, b; };
+  std::vector<ProfRec> prof;
+  std::vector<cudaEvent_t> ev_pool;
   // scratch for the band-pair pipeline
   int pair_cap = 0;
   pwb::DevBuf s_ad, s_k, s_bc, s_wp, s_w;

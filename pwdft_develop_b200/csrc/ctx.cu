@@ -155,7 +155,37 @@ int pw_ctx_create(const double length[3], const int numGrid[3], const int numGri
 int pw_ctx_destroy(pw_ctx* ctx) {
   if (!ctx) return PW_OK;
   cudaSetDevice(ctx->device);
+  for (auto& r : ctx->prof) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
+  for (auto e : ctx->ev_pool) cudaEventDestroy(e);
   delete ctx;
+  return PW_OK;
+}
+
+int pw_profile(pw_ctx* ctx, int enable) {
+  PWB_CHECK(ctx, PW_EINVAL, "null context");
+  PWB_CUDA(cudaSetDevice(ctx->device));
+  PWB_CUDA(cudaDeviceSynchronize());
+  for (auto& r : ctx->prof) { ctx->ev_pool.push_back(r.a); ctx->ev_pool.push_back(r.b); }
+  ctx->prof.clear();
+  ctx->prof_on = enable != 0;
+  return PW_OK;
+}
+
+int pw_profile_read(pw_ctx* ctx, int kind, double* total_ms, long* count) {
+  PWB_CHECK(ctx, PW_EINVAL, "null context");
+  PWB_CUDA(cudaSetDevice(ctx->device));
+  double t = 0;
+  long n = 0;
+  for (auto& r : ctx->prof) {
+    if (r.kind != kind) continue;
+    PWB_CUDA(cudaEventSynchronize(r.b));
+    float ms = 0;
+    PWB_CUDA(cudaEventElapsedTime(&ms, r.a, r.b));
+    t += ms;
+    ++n;
+  }
+  if (total_ms) *total_ms = t;
+  if (count) *count = n;
   return PW_OK;
 }
 
@@ -292,7 +322,7 @@ int pw_set_nonlocal(pw_ctx* ctx, int natom, const int* atom_npts, const int* ato
 }
 
 int pw_hpsi(pw_ctx* ctx, const void* psi, int ld, void* hpsi, int ldh, int nband, int accumulate, void* stream) {
-  PWB_CHECK(ctx && psi && hpsi, PW_EINVAL, "null argument");
+  PWB_CHECK(ctx && (nband == 0 || (psi && hpsi)), PW_EINVAL, "null argument");
   PWB_CHECK(nband >= 0 && ld >= ctx->ntot && ldh >= ctx->ntot, PW_EINVAL, "Domain size does not match.");
   PWB_CHECK(ctx->have_vtot, PW_ENOTREADY, "local potential not set (pw_set_vtot)");
   PWB_CUDA(cudaSetDevice(ctx->device));
@@ -307,7 +337,7 @@ int pw_hpsi(pw_ctx* ctx, const void* psi, int ld, void* hpsi, int ldh, int nband
 }
 
 int pw_teter_precond(pw_ctx* ctx, const void* r, int ld, void* w, int ldw, int nband, int accumulate, void* stream) {
-  PWB_CHECK(ctx && r && w, PW_EINVAL, "null argument");
+  PWB_CHECK(ctx && (nband == 0 || (r && w)), PW_EINVAL, "null argument");
   PWB_CHECK(nband >= 0 && ld >= ctx->ntot && ldw >= ctx->ntot, PW_EINVAL, "Domain size does not match.");
   PWB_CUDA(cudaSetDevice(ctx->device));
   cudaStream_t st = (cudaStream_t)stream;
@@ -321,7 +351,8 @@ int pw_teter_precond(pw_ctx* ctx, const void* r, int ld, void* w, int ldw, int n
 }
 
 int pw_hpsi_host(pw_ctx* ctx, const void* psi, int ld, void* hpsi, int ldh, int nband, int accumulate) {
-  PWB_CHECK(ctx && psi && hpsi, PW_EINVAL, "null argument");
+  PWB_CHECK(ctx && (nband == 0 || (psi && hpsi)), PW_EINVAL, "null argument");
+  if (nband == 0) return PW_OK;
   PWB_CHECK(nband >= 0 && ld >= ctx->ntot && ldh >= ctx->ntot, PW_EINVAL, "Domain size does not match.");
   PWB_CUDA(cudaSetDevice(ctx->device));
   const size_t bytes = (size_t)ctx->ntot * nband * ctx->esz;

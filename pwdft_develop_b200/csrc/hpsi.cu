@@ -499,6 +499,38 @@ k_cxy_inv(const VT<T>* __restrict__ D, T* __restrict__ out, int ldo, int nband, 
 // ---------------------------------------------------------------------------
 // host-side launch plan for one (precision, grid) instantiation
 // ---------------------------------------------------------------------------
+// Records a launch; when profiling is on, brackets it with events on the stream.
+struct Launch {
+  pw_ctx* c;
+  cudaStream_t st;
+  int kind;
+  cudaEvent_t a = nullptr, b = nullptr;
+  static cudaEvent_t take(pw_ctx* c) {
+    if (!c->ev_pool.empty()) {
+      cudaEvent_t e = c->ev_pool.back();
+      c->ev_pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+  }
+  Launch(pw_ctx* c_, cudaStream_t st_, int kind_) : c(c_), st(st_), kind(kind_) {
+    c->launches++;
+    if (c->prof_on) {
+      a = take(c);
+      b = take(c);
+      cudaEventRecord(a, st);
+    }
+  }
+  ~Launch() {
+    if (a) {
+      cudaEventRecord(b, st);
+      c->prof.push_back({kind, a, b});
+    }
+  }
+};
+
 template <typename T> static int fplane_cr(int NXF, int NYF) {
   // rows per chunk so that S + R (+ twiddles) fit in ~200 KB of shared memory
   const size_t vs = sizeof(T) * 2;
@@ -557,9 +589,11 @@ struct Plan {
     const T inv_nc = (T)(1.0 / (double)c->ntot);
     const T inv_nf = (T)(1.0 / (double)c->ntotf);
     const int ntx = (N0 + TX - 1) / TX;
-    k_cxy_fwd<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(psi, ld, nband, band0, AD, tw(c, 0), tw(c, 1));
+    { Launch L_(c, st, KK_CXY_FWD);
+    k_cxy_fwd<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(psi, ld, nband, band0, AD, tw(c, 0), tw(c, 1)); }
+    { Launch L_(c, st, KK_ZPAD);
     k_zpad<T, N2, NF2><<<dim3(N1, ntx, npair), PENCIL_THREADS, sm_zpad(), st>>>(
-        AD, K, BC, reinterpret_cast<const T*>(c->ekin.p), N0, N1, inv_nc, tw(c, 2), tw(c, 5));
+        AD, K, BC, reinterpret_cast<const T*>(c->ekin.p), N0, N1, inv_nc, tw(c, 2), tw(c, 5)); }
     NLArgs nl{};
     const int cr = chunk_rows();
     nl.cr = cr;
@@ -577,17 +611,22 @@ struct Plan {
       natom = c->nl.natom;
       nslot = c->nl.nslot;
       if (c->nl.cr != cr) { set_error("projector tables built for another chunk size"); return PW_EINVAL; }
-      k_fplane<T, NF0, NF1, false><<<dim3(NF2, npair), PLANE_THREADS, sm_fplane(cr), st>>>(
-          BC, reinterpret_cast<const T*>(c->vtot.p), nl, Wp, W, natom, nslot, inv_nf, tw(c, 3), tw(c, 4));
+      { Launch L_(c, st, KK_FPLANE_GATHER);
+    k_fplane<T, NF0, NF1, false><<<dim3(NF2, npair), PLANE_THREADS, sm_fplane(cr), st>>>(
+          BC, reinterpret_cast<const T*>(c->vtot.p), nl, Wp, W, natom, nslot, inv_nf, tw(c, 3), tw(c, 4)); }
       const int nthr = 128;
-      k_nl_reduce<T><<<dim3((natom * nl.npmax + nthr - 1) / nthr, npair), nthr, 0, st>>>(
+      { Launch L_(c, st, KK_NL_REDUCE);
+    k_nl_reduce<T><<<dim3((natom * nl.npmax + nthr - 1) / nthr, npair), nthr, 0, st>>>(
           Wp, W, reinterpret_cast<const int*>(c->nl.atom_slot.p), reinterpret_cast<const int*>(c->nl.atom_slot_list.p),
-          reinterpret_cast<const T*>(c->nl.wgt.p), natom, nslot, nl.npmax);
+          reinterpret_cast<const T*>(c->nl.wgt.p), natom, nslot, nl.npmax); }
     }
+    { Launch L_(c, st, KK_FPLANE_APPLY);
     k_fplane<T, NF0, NF1, true><<<dim3(NF2, npair), PLANE_THREADS, sm_fplane(cr), st>>>(
-        BC, reinterpret_cast<const T*>(c->vtot.p), nl, Wp, W, natom, nslot, inv_nf, tw(c, 3), tw(c, 4));
-    k_zfold<T, N2, NF2><<<dim3(N1, ntx, npair), PENCIL_THREADS, sm_zfold(), st>>>(BC, K, AD, N0, N1, tw(c, 2), tw(c, 5));
-    k_cxy_inv<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(AD, out, ldo, nband, band0, accumulate, tw(c, 0), tw(c, 1));
+        BC, reinterpret_cast<const T*>(c->vtot.p), nl, Wp, W, natom, nslot, inv_nf, tw(c, 3), tw(c, 4)); }
+    { Launch L_(c, st, KK_ZFOLD);
+    k_zfold<T, N2, NF2><<<dim3(N1, ntx, npair), PENCIL_THREADS, sm_zfold(), st>>>(BC, K, AD, N0, N1, tw(c, 2), tw(c, 5)); }
+    { Launch L_(c, st, KK_CXY_INV);
+    k_cxy_inv<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(AD, out, ldo, nband, band0, accumulate, tw(c, 0), tw(c, 1)); }
     PWB_CUDA(cudaGetLastError());
     return PW_OK;
   }
@@ -599,10 +638,13 @@ struct Plan {
     V* AD = reinterpret_cast<V*>(c->s_ad.p);
     const T inv_nc = (T)(1.0 / (double)c->ntot);
     const int ntx = (N0 + TX - 1) / TX;
-    k_cxy_fwd<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(r, ld, nband, band0, AD, tw(c, 0), tw(c, 1));
+    { Launch L_(c, st, KK_CXY_FWD);
+    k_cxy_fwd<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(r, ld, nband, band0, AD, tw(c, 0), tw(c, 1)); }
+    { Launch L_(c, st, KK_ZTETER);
     k_zteter<T, N2><<<dim3(N1, ntx, npair), PENCIL_THREADS, sm_zteter(), st>>>(
-        AD, reinterpret_cast<const T*>(c->teter.p), N0, N1, inv_nc, tw(c, 2));
-    k_cxy_inv<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(AD, out, ldo, nband, band0, accumulate, tw(c, 0), tw(c, 1));
+        AD, reinterpret_cast<const T*>(c->teter.p), N0, N1, inv_nc, tw(c, 2)); }
+    { Launch L_(c, st, KK_CXY_INV);
+    k_cxy_inv<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(AD, out, ldo, nband, band0, accumulate, tw(c, 0), tw(c, 1)); }
     PWB_CUDA(cudaGetLastError());
     return PW_OK;
   }
