@@ -214,6 +214,8 @@ def run_reference(args):
 
 
 def run_ours(args):
+    global NBAND
+    NBAND = args.bands
     import torch
     import torch.distributed as dist
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -363,6 +365,7 @@ def main():
     ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--cpu-bands", type=int, default=64)
+    ap.add_argument("--bands", type=int, default=NBAND, help="band block size (profiling runs use a small block)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

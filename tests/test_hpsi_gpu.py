@@ -109,7 +109,9 @@ def test_hpsi_host_entry_matches_device(si8):
     c = make_ctx(T, "f64")
     dev = c.hpsi(torch.tensor(psi, device="cuda")).cpu().numpy()
     host = c.hpsi_host(psi)
-    assert np.array_equal(dev, host)
+    # the projector scatter sums overlapping spheres with shared-memory atomics,
+    # so two runs agree to rounding, not bit for bit
+    assert _rel(host, dev) <= 1e-14
 
 
 def test_hpsi_local_only_and_no_projectors(si8):
