@@ -38,6 +38,14 @@ enum {
 
 enum { PW_F64 = 0, PW_F32 = 1 };
 
+/* Nonlocal apply modes.  PW_NL_DENSE: the fine-grid projector sums of the
+ * reference are folded into dense coarse-grid columns q_l = T(beta_l) (T is
+ * the fine->coarse map R2C fine, IP_f2c, C2R coarse) and applied as
+ * H psi += Q diag(gamma vol/N) Q^T psi on tensor-core GEMMs; exact in exact
+ * arithmetic because IP_f2c is the transpose of IP_c2f.  PW_NL_REALSPACE: the
+ * reference's gather / scaled-dot / scatter over the index sets on the fine grid. */
+enum { PW_NL_DENSE = 0, PW_NL_REALSPACE = 1 };
+
 typedef struct pw_ctx pw_ctx;
 
 /* Message of the last failed call on this thread ("" if none). */
@@ -72,6 +80,9 @@ PW_API int pw_set_vtot(pw_ctx* ctx, const double* vtot_fine_host);
  * All host pointers. */
 PW_API int pw_set_nonlocal(pw_ctx* ctx, int natom, const int* atom_npts, const int* atom_nproj,
                     const int* idx, const double* beta, const double* weight);
+
+/* Select the nonlocal apply mode (call before pw_set_nonlocal / pw_set_atoms). */
+PW_API int pw_set_nonlocal_mode(pw_ctx* ctx, int mode);
 
 /* H*psi for nband bands: hpsi (+)= (-1/2 Laplacian + V_loc + V_nl) psi.
  * Replaces Spinor::AddMultSpinorFineR2C(fft, ekin, vtot, pseudo, a3)
@@ -119,15 +130,17 @@ PW_API int pw_hgh_atom_projectors(const double length[3], const int numGridFine[
                                   int* npts, int* nproj, int* idx, double* val4, double* wgt);
 PW_API int pw_hgh_pseudocharge(const double length[3], const int numGridFine[3], int natom, const int* znuc,
                                const double* pos, double* rho_fine_host);
-/* Number of CUDA kernels this context has launched. */
-PW_API int pw_stats(const pw_ctx* ctx, long* kernel_launches);
+/* Number of this library's CUDA kernels the context has launched, and of
+ * vendor-library (cuBLAS / cuSOLVER) calls it made. */
+PW_API int pw_stats(const pw_ctx* ctx, long* kernel_launches, long* library_calls);
 
 /* Per-kernel CUDA-event timing.  pw_profile(ctx, 1) clears the records and
  * brackets every later kernel launch of this context with events on its
  * stream; pw_profile_read returns the summed device time and the number of
  * launches of one kernel kind: 0 coarse-plane FFT, 1 z-pad, 2 fine-plane
  * projector gather, 3 projector reduce, 4 fine-plane apply, 5 z-fold,
- * 6 coarse-plane inverse, 7 Teter z-pencil, 8 Gram, 9 density, 10 other. */
+ * 6 coarse-plane inverse, 7 Teter z-pencil, 8 Gram, 9 density, 10 other,
+ * 11 vendor-library GEMM. */
 PW_API int pw_profile(pw_ctx* ctx, int enable);
 PW_API int pw_profile_read(pw_ctx* ctx, int kind, double* total_ms, long* count);
 

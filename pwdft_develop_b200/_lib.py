@@ -14,6 +14,7 @@ LIB_PATH = Path(__file__).resolve().parent / "libpwdft_b200.so"
 PW_OK, PW_EINVAL, PW_ECUDA, PW_ENOMEM, PW_EUNSUPPORTED, PW_ETIMEOUT, PW_ENOTREADY, PW_ENUMERIC = \
     0, -1, -2, -3, -4, -5, -6, -7
 PW_F64, PW_F32 = 0, 1
+PW_NL_DENSE, PW_NL_REALSPACE = 0, 1
 
 
 class PwError(RuntimeError):
@@ -46,11 +47,12 @@ SIGNATURES: dict[str, tuple] = {
     "pw_hpsi_host": (_i, [_vp, _vp, _i, _vp, _i, _i, _i]),
     "pw_teter_precond": (_i, [_vp, _vp, _i, _vp, _i, _i, _i, _vp]),
     "pw_set_band_batch": (_i, [_vp, _i]),
+    "pw_set_nonlocal_mode": (_i, [_vp, _i]),
     "pw_hgh_species": (_i, [_i, _dp, _dp, _dp, _dp, _ip]),
     "pw_set_atoms": (_i, [_vp, _i, _ip, _dp]),
     "pw_get_pseudocharge": (_i, [_vp, _dp]),
     "pw_get_atom_projectors": (_i, [_vp, _i, _ip, _ip, _ip, _dp, _dp]),
-    "pw_stats": (_i, [_vp, C.POINTER(_l)]),
+    "pw_stats": (_i, [_vp, C.POINTER(_l), C.POINTER(_l)]),
     "pw_hgh_atom_projectors": (_i, [_dp, _ip, _i, _dp, _ip, _ip, _ip, _dp, _dp]),
     "pw_hgh_pseudocharge": (_i, [_dp, _ip, _i, _ip, _dp, _dp]),
     "pw_profile": (_i, [_vp, _i]),

@@ -183,9 +183,19 @@ def _ctx_pseudocharge(self) -> np.ndarray:
 
 
 def _ctx_launches(self) -> int:
-    n = C.c_long()
-    check(lib.pw_stats(self._h, C.byref(n)))
+    n, m = C.c_long(), C.c_long()
+    check(lib.pw_stats(self._h, C.byref(n), C.byref(m)))
     return n.value
+
+
+def _ctx_library_calls(self) -> int:
+    n, m = C.c_long(), C.c_long()
+    check(lib.pw_stats(self._h, C.byref(n), C.byref(m)))
+    return m.value
+
+
+def _ctx_set_nonlocal_mode(self, mode: str):
+    check(lib.pw_set_nonlocal_mode(self._h, _lib.PW_NL_DENSE if mode == "dense" else _lib.PW_NL_REALSPACE))
 
 
 def _ctx_profile(self, enable: bool):
@@ -201,8 +211,11 @@ def _ctx_profile_read(self, kind: int):
 Context.set_atoms = _ctx_set_atoms
 Context.pseudocharge = _ctx_pseudocharge
 Context.launches = _ctx_launches
+Context.library_calls = _ctx_library_calls
+Context.set_nonlocal_mode = _ctx_set_nonlocal_mode
 Context.profile = _ctx_profile
 Context.profile_read = _ctx_profile_read
 
 KERNEL_KINDS = {0: "coarse_xy_fwd", 1: "z_pad", 2: "fine_plane_gather", 3: "nl_reduce", 4: "fine_plane_apply",
-                5: "z_fold", 6: "coarse_xy_inv", 7: "z_teter", 8: "gram", 9: "density", 10: "other"}
+                5: "z_fold", 6: "coarse_xy_inv", 7: "z_teter", 8: "gram", 9: "density", 10: "other",
+                11: "library_gemm"}

@@ -110,9 +110,10 @@ int pw_hgh_pseudocharge(const double length[3], const int numGridFine[3], int na
   return PW_OK;
 }
 
-int pw_stats(const pw_ctx* ctx, long* kernel_launches) {
+int pw_stats(const pw_ctx* ctx, long* kernel_launches, long* library_calls) {
   PWB_CHECK(ctx, PW_EINVAL, "null context");
   if (kernel_launches) *kernel_launches = ctx->launches;
+  if (library_calls) *library_calls = ctx->lib_launches;
   return PW_OK;
 }
 

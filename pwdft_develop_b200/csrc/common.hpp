@@ -61,7 +61,7 @@ struct NonlocalDev {
 // Kernel kinds for pw_profile_read.
 enum KernelKind {
   KK_CXY_FWD = 0, KK_ZPAD, KK_FPLANE_GATHER, KK_NL_REDUCE, KK_FPLANE_APPLY, KK_ZFOLD, KK_CXY_INV, KK_ZTETER,
-  KK_GRAM, KK_DENSITY, KK_MISC, KK_COUNT
+  KK_GRAM, KK_DENSITY, KK_MISC, KK_LIBGEMM, KK_COUNT
 };
 
 }  // namespace pwb
@@ -84,6 +84,14 @@ struct pw_ctx {
   bool have_vtot = false;
   bool have_nl = false;
   pwb::NonlocalDev nl;
+  // nonlocal apply mode: PW_NL_DENSE (coarse-grid projector matrix, GEMMs) or
+  // PW_NL_REALSPACE (fine-grid gather / scatter over the projector index sets)
+  int nl_mode = PW_NL_DENSE;
+  int nproj = 0;                 // total projectors over all atoms
+  pwb::DevBuf q;                 // T [nproj][ntot]  coarse projector columns q_l
+  pwb::DevBuf qd;                // T [nproj]        gamma_l * vol / ntot
+  pwb::DevBuf s_wq;              // T [nproj][band batch] projections
+  void* blas = nullptr;          // cublasHandle_t
   // host copies kept for setup-time work
   std::vector<double> h_vtot;
   // atoms set through pw_set_atoms (HGH species built in this library)
@@ -93,6 +101,7 @@ struct pw_ctx {
   std::vector<double> h_rhops;             // pseudocharge on the fine grid
   // kernel launch accounting (pw_stats) and optional per-kernel event timing
   long launches = 0;
+  long lib_launches = 0;          // cuBLAS / cuSOLVER calls (not this library's kernels)
   bool prof_on = false;
   struct ProfRec { int kind; cudaEvent_t a, b; };
   std::vector<ProfRec> prof;

@@ -5,6 +5,8 @@
 #include <cstring>
 #include <mutex>
 
+#include <cublas_v2.h>
+
 #include "common.hpp"
 #include "fft.cuh"
 
@@ -40,6 +42,8 @@ int run_hpsi(pw_ctx* c, const void* psi, int ld, void* out, int ldo, int nband, 
              cudaStream_t st);
 int run_teter(pw_ctx* c, const void* r, int ld, void* out, int ldo, int nband, int band0, int npair, int acc,
               cudaStream_t st);
+int run_build_q(pw_ctx* c, const int* d_idx, const double* d_beta, const long* d_pio, const long* d_pbo,
+                const int* d_pnp, int nproj, cudaStream_t st);
 
 // upload a double host vector as the context's precision
 int upload_real(pw_ctx* c, DevBuf& dst, const double* src, size_t n) {
@@ -81,6 +85,7 @@ int ensure_scratch(pw_ctx* c, int npair) {
   const size_t nslot = std::max(1, c->nl.nslot), nat = std::max(1, c->nl.natom), np = std::max(1, c->nl.npmax);
   if ((rc = c->s_wp.alloc((size_t)npair * nslot * np * cs))) return rc;
   if ((rc = c->s_w.alloc((size_t)npair * nat * np * cs))) return rc;
+  if ((rc = c->s_wq.alloc((size_t)std::max(1, c->nproj) * 2 * npair * c->esz))) return rc;
   c->pair_cap = npair;
   return PW_OK;
 }
@@ -148,6 +153,12 @@ int pw_ctx_create(const double length[3], const int numGrid[3], const int numGri
     if ((rc = upload_twiddles(c, s, lens[s]))) { delete c; return rc; }
   c->nl.cr = grid_chunk_rows(c->n, c->prec);
   if ((rc = ensure_scratch(c, 32))) { delete c; return rc; }
+  {
+    cublasHandle_t h;
+    if (cublasCreate(&h) != CUBLAS_STATUS_SUCCESS) { delete c; set_error("cublasCreate failed"); return PW_ECUDA; }
+    cublasSetMathMode(h, CUBLAS_DEFAULT_MATH);
+    c->blas = h;
+  }
   *out = c;
   return PW_OK;
 }
@@ -157,6 +168,7 @@ int pw_ctx_destroy(pw_ctx* ctx) {
   cudaSetDevice(ctx->device);
   for (auto& r : ctx->prof) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
   for (auto e : ctx->ev_pool) cudaEventDestroy(e);
+  if (ctx->blas) cublasDestroy((cublasHandle_t)ctx->blas);
   delete ctx;
   return PW_OK;
 }
@@ -206,6 +218,13 @@ int pw_set_vtot(pw_ctx* ctx, const double* vtot) {
   return PW_OK;
 }
 
+int pw_set_nonlocal_mode(pw_ctx* ctx, int mode) {
+  PWB_CHECK(ctx && (mode == PW_NL_DENSE || mode == PW_NL_REALSPACE), PW_EINVAL, "bad nonlocal mode");
+  PWB_CHECK(!ctx->have_nl || mode == ctx->nl_mode, PW_EINVAL, "set the nonlocal mode before the projectors");
+  ctx->nl_mode = mode;
+  return PW_OK;
+}
+
 int pw_set_band_batch(pw_ctx* ctx, int nband_batch) {
   PWB_CHECK(ctx && nband_batch > 0, PW_EINVAL, "bad band batch");
   PWB_CUDA(cudaSetDevice(ctx->device));
@@ -232,6 +251,55 @@ int pw_set_nonlocal(pw_ctx* ctx, int natom, const int* atom_npts, const int* ato
   }
   PWB_CHECK(npmax <= 8, PW_EUNSUPPORTED, "at most 8 projectors per atom are supported");
   PWB_CHECK(nent < (1L << 31), PW_EUNSUPPORTED, "too many projector points");
+  if (ctx->nl_mode == PW_NL_DENSE) {
+    // per-projector offsets into idx / beta, weights gamma_l * vol / ntot
+    std::vector<long> pio, pbo;
+    std::vector<int> pnp;
+    std::vector<double> qd;
+    long off = 0, boff = 0, woff = 0;
+    for (int a = 0; a < natom; ++a) {
+      for (int q = 0; q < atom_nproj[a]; ++q) {
+        pio.push_back(off);
+        pbo.push_back(boff + (long)q * atom_npts[a]);
+        pnp.push_back(atom_npts[a]);
+        qd.push_back(weight[woff + q] * ctx->vol / (double)ctx->ntot);
+      }
+      for (int i = 0; i < atom_npts[a]; ++i) {
+        const int g = idx[off + i];
+        PWB_CHECK(g >= 0 && g < ctx->ntotf, PW_EINVAL, "projector index outside the fine grid");
+      }
+      off += atom_npts[a];
+      boff += (long)atom_nproj[a] * atom_npts[a];
+      woff += atom_nproj[a];
+    }
+    const int nproj = (int)pnp.size();
+    ctx->nproj = nproj;
+    ctx->have_nl = false;
+    int rc;
+    if (nproj > 0) {
+      DevBuf d_idx, d_beta, d_pio, d_pbo, d_pnp;
+      if ((rc = d_idx.alloc(std::max<long>(off, 1) * 4)) || (rc = d_beta.alloc(std::max<long>(boff, 1) * 8)) ||
+          (rc = d_pio.alloc(nproj * 8)) || (rc = d_pbo.alloc(nproj * 8)) || (rc = d_pnp.alloc(nproj * 4)))
+        return rc;
+      if (off) PWB_CUDA(cudaMemcpy(d_idx.p, idx, off * 4, cudaMemcpyHostToDevice));
+      if (boff) PWB_CUDA(cudaMemcpy(d_beta.p, beta, boff * 8, cudaMemcpyHostToDevice));
+      PWB_CUDA(cudaMemcpy(d_pio.p, pio.data(), nproj * 8, cudaMemcpyHostToDevice));
+      PWB_CUDA(cudaMemcpy(d_pbo.p, pbo.data(), nproj * 8, cudaMemcpyHostToDevice));
+      PWB_CUDA(cudaMemcpy(d_pnp.p, pnp.data(), nproj * 4, cudaMemcpyHostToDevice));
+      if ((rc = ctx->q.alloc((size_t)nproj * ctx->ntot * ctx->esz))) return rc;
+      if ((rc = upload_real(ctx, ctx->qd, qd.data(), nproj))) return rc;
+      const int cap = std::max(ctx->pair_cap, 1);
+      ctx->pair_cap = 0;
+      if ((rc = ensure_scratch(ctx, cap))) return rc;
+      rc = run_build_q(ctx, (const int*)d_idx.p, (const double*)d_beta.p, (const long*)d_pio.p,
+                       (const long*)d_pbo.p, (const int*)d_pnp.p, nproj, nullptr);
+      if (rc) return rc;
+    }
+    nl.natom = natom;
+    nl.npmax = npmax;
+    ctx->have_nl = nproj > 0;
+    return PW_OK;
+  }
   // bucket entries by tile, stable in (atom, point order)
   std::vector<int> tile_count(ntile + 1, 0);
   {

@@ -172,15 +172,15 @@ PWB_SPLIT(72, 8) PWB_SPLIT(80, 8) PWB_SPLIT(96, 8) PWB_SPLIT(120, 10) PWB_SPLIT(
 // `count` in-place transforms of length N on shared memory.  Element e of
 // transform b sits at base[b*bs + e*es].  tw[m] = exp(-2 pi i m / N) for
 // m < N, in shared memory.  All threads of the block must call this.
+// Explicit work split: warp `warp` of `nw` cooperating warps (a single warp
+// with warp = 0, nw = 1 runs a warp-private batch without block barriers).
 template <int N, int DIR, typename V>
-__device__ __forceinline__ void smem_fft(V* base, int count, int es, int bs, const V* tw) {
+__device__ __forceinline__ void smem_fft_w(V* base, int count, int es, int bs, const V* tw, int warp, int nw) {
   constexpr int N1 = Split<N>::n1;
   constexpr int N2 = N / N1;
   static_assert(N1 * N2 == N && N1 <= 32, "bad split");
   constexpr int F = 32 / N1;
   const int lane = threadIdx.x & 31;
-  const int warp = threadIdx.x >> 5;
-  const int nw = blockDim.x >> 5;
   for (int g = warp * F; g < count; g += nw * F) {
     // pass 1: DFT_N1 over j1 for each (f, j2), twiddle, store in place
     for (int it = lane; it < F * N2; it += 32) {
@@ -221,6 +221,16 @@ __device__ __forceinline__ void smem_fft(V* base, int count, int es, int bs, con
     __syncwarp();
   }
 }
+
+template <int N, int DIR, typename V>
+__device__ __forceinline__ void smem_fft(V* base, int count, int es, int bs, const V* tw) {
+  smem_fft_w<N, DIR>(base, count, es, bs, tw, (int)(threadIdx.x >> 5), (int)(blockDim.x >> 5));
+}
+
+// Number of transforms one warp processes together for length N.
+template <int N> struct FftGroup {
+  static constexpr int f = 32 / Split<N>::n1;
+};
 
 // Runtime-length dispatch over the supported sizes.  Returns false when N is
 // not supported (the host validates sizes before launching).

@@ -20,6 +20,8 @@
 //                FFT x, FFT y, truncate                           B -> C (in place)
 //   k_zfold      fine z FFT, fold (IP_f2c rule) + kinetic, coarse z IFFT  C,K -> D
 //   k_cxy_inv    coarse plane: IFFT y, IFFT x, (accumulate) into hpsi   D -> hpsi
+#include <cublas_v2.h>
+
 #include "common.hpp"
 #include "fft.cuh"
 
@@ -338,6 +340,110 @@ k_fplane(VT<T>* __restrict__ BC, const T* __restrict__ vtot, NLArgs nl, VT<T>* _
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// fine plane, local potential only (the projectors are applied on the coarse
+// grid as dense GEMMs): IFFT y on the slot columns, then per warp a group of
+// rows: IFFT x, * V_loc, FFT x, truncate; FFT y; truncate.  MODE 1 starts
+// from two real fine-grid fields instead (used to build the coarse projector
+// matrix) and skips the inverse transforms and the potential.
+// ---------------------------------------------------------------------------
+constexpr int FLOC_THREADS = 256;
+
+template <typename T, int NXF, int NYF, int MODE>
+__global__ void __launch_bounds__(FLOC_THREADS)
+k_floc(VT<T>* __restrict__ BC, const T* __restrict__ vtot, const T* __restrict__ fin, long fin_pair_stride,
+       T inv_nf, const VT<T>* twx_g, const VT<T>* twy_g) {
+  using V = VT<T>;
+  constexpr int n0 = NXF / 2, n1 = NYF / 2;
+  constexpr int nsx = n0 + 1, nsy = n1 + 1;
+  constexpr int PS = nsx;
+  constexpr int PR = NXF + 1;
+  constexpr int F = FftGroup<NXF>::f;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  V* S = reinterpret_cast<V*>(smraw);          // [NYF][PS]
+  V* twx = S + NYF * PS;
+  V* twy = twx + NXF;
+  V* Rall = twy + NYF;                          // [nwarps][F][PR]
+  load_tw(twx, twx_g, NXF);
+  load_tw(twy, twy_g, NYF);
+  const int zf = blockIdx.x, p = blockIdx.y;
+  const int NZF = gridDim.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  V* Rw = Rall + warp * F * PR;
+  V* Bp = BC + ((long)p * NZF + zf) * nsy * nsx;
+  if (MODE == 0) {
+    for (int i = threadIdx.x; i < NYF * PS; i += blockDim.x) S[i] = mkc<V>(0, 0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < nsy * nsx; i += blockDim.x) {
+      const int ys = i / nsx, xs = i - ys * nsx;
+      S[slot_fine(ys, n1, NYF) * PS + xs] = Bp[i];
+    }
+    __syncthreads();
+    smem_fft<NYF, +1>(S, nsx, PS, 1, twy);
+  }
+  __syncthreads();
+  for (int r0 = warp * F; r0 < NYF; r0 += nw * F) {
+    const int nr = min(F, NYF - r0);
+    if (MODE == 0) {
+      for (int i = lane; i < F * PR; i += 32) Rw[i] = mkc<V>(0, 0);
+      __syncwarp();
+      for (int i = lane; i < nr * nsx; i += 32) {
+        const int f = i / nsx, xs = i - f * nsx;
+        Rw[f * PR + slot_fine(xs, n0, NXF)] = S[(r0 + f) * PS + xs];
+      }
+      __syncwarp();
+      smem_fft_w<NXF, +1>(Rw, nr, 1, PR, twx, 0, 1);
+      const T* vp = vtot + ((long)zf * NYF + r0) * NXF;
+      for (int i = lane; i < nr * NXF; i += 32) {
+        const int f = i / NXF, x = i - f * NXF;
+        Rw[f * PR + x] = cscale(Rw[f * PR + x], vp[i]);
+      }
+    } else {
+      const T* fa = fin + (long)(2 * p) * fin_pair_stride + ((long)zf * NYF + r0) * NXF;
+      const T* fb = fin + (long)(2 * p + 1) * fin_pair_stride + ((long)zf * NYF + r0) * NXF;
+      for (int i = lane; i < nr * NXF; i += 32) {
+        const int f = i / NXF, x = i - f * NXF;
+        Rw[f * PR + x] = mkc<V>(fa[i], fb[i]);
+      }
+    }
+    __syncwarp();
+    smem_fft_w<NXF, -1>(Rw, nr, 1, PR, twx, 0, 1);
+    for (int i = lane; i < nr * nsx; i += 32) {
+      const int f = i / nsx, xs = i - f * nsx;
+      S[(r0 + f) * PS + xs] = Rw[f * PR + slot_fine(xs, n0, NXF)];
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+  smem_fft<NYF, -1>(S, nsx, PS, 1, twy);
+  __syncthreads();
+  for (int i = threadIdx.x; i < nsy * nsx; i += blockDim.x) {
+    const int ys = i / nsx, xs = i - ys * nsx;
+    Bp[i] = cscale(S[slot_fine(ys, n1, NYF) * PS + xs], inv_nf);
+  }
+}
+
+// projector fields: field[l][idx] = beta for the projectors of one batch
+template <typename T>
+__global__ void k_scatter_beta(T* __restrict__ fields, long nf, const int* __restrict__ idx,
+                               const double* __restrict__ beta, const long* __restrict__ pidx_off,
+                               const long* __restrict__ pbeta_off, const int* __restrict__ pnpts, int l0, int nl) {
+  const int l = blockIdx.y;
+  if (l0 + l >= nl) return;
+  const long io = pidx_off[l0 + l], bo = pbeta_off[l0 + l];
+  const int np = pnpts[l0 + l];
+  T* f = fields + (long)l * nf;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np; i += gridDim.x * blockDim.x) f[idx[io + i]] = (T)beta[bo + i];
+}
+
+// W[l][b] *= d[l]  (W column-major nproj x nb)
+template <typename T>
+__global__ void k_scale_rows(T* __restrict__ W, const T* __restrict__ d, int nproj, int nb) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i < (long)nproj * nb) W[i] *= d[i % nproj];
+}
+
 // W[p][a][q] = wgt[a][q] * sum over the atom's slots of Wp[p][slot][q]
 template <typename T>
 __global__ void k_nl_reduce(const VT<T>* __restrict__ Wp, VT<T>* __restrict__ W, const int* atom_slot,
@@ -394,7 +500,7 @@ k_zfold(const VT<T>* __restrict__ C, const VT<T>* __restrict__ K, VT<T>* __restr
   for (int i = threadIdx.x; i < NZ * TX; i += blockDim.x) {
     const int kz = i / TX, c = i - kz * TX;
     if (c >= tw) { acc[kz * PA + c] = mkc<V>(0, 0); continue; }
-    V v = Kp[kz * nplane + (long)ky * n0 + kx0 + c];
+    V v = K ? Kp[kz * nplane + (long)ky * n0 + kx0 + c] : mkc<V>(0, 0);
     const bool nyz = (kz == NZ / 2);
     const int fz = (sgn_idx(kz, NZ) + NZF) % NZF;
     const bool split = m.nyy || (c == m.nyx_i);
@@ -516,7 +622,7 @@ struct Launch {
     return e;
   }
   Launch(pw_ctx* c_, cudaStream_t st_, int kind_) : c(c_), st(st_), kind(kind_) {
-    c->launches++;
+    if (kind == KK_LIBGEMM) c->lib_launches++; else c->launches++;
     if (c->prof_on) {
       a = take(c);
       b = take(c);
@@ -555,6 +661,9 @@ struct Plan {
   static size_t sm_zpad() { return sizeof(V) * (N2 * (TX + 1) + NF2 * (2 * TX + 1) + N2 + NF2); }
   static size_t sm_zfold() { return sizeof(V) * (NF2 * (2 * TX + 1) + N2 * (TX + 1) + N2 + NF2); }
   static size_t sm_zteter() { return sizeof(V) * (N2 * (TX + 1) + N2); }
+  static size_t sm_floc() {
+    return sizeof(V) * ((size_t)NF1 * (N0 + 1) + NF0 + NF1 + (size_t)(FLOC_THREADS / 32) * FftGroup<NF0>::f * (NF0 + 1));
+  }
   static size_t sm_fplane(int cr) {
     return sizeof(V) * ((size_t)NF1 * (N0 + 1) + (size_t)cr * (NF0 + 1) + NF0 + NF1);
   }
@@ -570,6 +679,8 @@ struct Plan {
     PWB_CUDA(cudaFuncSetAttribute(k_cxy_fwd<T, N0, N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_cxy()));
     PWB_CUDA(cudaFuncSetAttribute(k_cxy_inv<T, N0, N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_cxy()));
     PWB_CUDA(cudaFuncSetAttribute(k_zteter<T, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_zteter()));
+    PWB_CUDA(cudaFuncSetAttribute(k_floc<T, NF0, NF1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_floc()));
+    PWB_CUDA(cudaFuncSetAttribute(k_floc<T, NF0, NF1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_floc()));
     done = true;
     return PW_OK;
   }
@@ -594,6 +705,19 @@ struct Plan {
     { Launch L_(c, st, KK_ZPAD);
     k_zpad<T, N2, NF2><<<dim3(N1, ntx, npair), PENCIL_THREADS, sm_zpad(), st>>>(
         AD, K, BC, reinterpret_cast<const T*>(c->ekin.p), N0, N1, inv_nc, tw(c, 2), tw(c, 5)); }
+    if (c->nl_mode == PW_NL_DENSE) {
+      { Launch L_(c, st, KK_FPLANE_APPLY);
+      k_floc<T, NF0, NF1, 0><<<dim3(NF2, npair), FLOC_THREADS, sm_floc(), st>>>(
+          BC, reinterpret_cast<const T*>(c->vtot.p), nullptr, 0, inv_nf, tw(c, 3), tw(c, 4)); }
+      { Launch L_(c, st, KK_ZFOLD);
+      k_zfold<T, N2, NF2><<<dim3(N1, ntx, npair), PENCIL_THREADS, sm_zfold(), st>>>(BC, K, AD, N0, N1, tw(c, 2), tw(c, 5)); }
+      { Launch L_(c, st, KK_CXY_INV);
+      k_cxy_inv<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(AD, out, ldo, nband, band0, accumulate, tw(c, 0), tw(c, 1)); }
+      PWB_CUDA(cudaGetLastError());
+      const int nb = std::min(2 * npair, nband - band0);
+      if (c->have_nl && c->nproj > 0 && nb > 0) return dense_nl(c, psi + (long)band0 * ld, ld, out + (long)band0 * ldo, ldo, nb, st);
+      return PW_OK;
+    }
     NLArgs nl{};
     const int cr = chunk_rows();
     nl.cr = cr;
@@ -628,6 +752,63 @@ struct Plan {
     { Launch L_(c, st, KK_CXY_INV);
     k_cxy_inv<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(AD, out, ldo, nband, band0, accumulate, tw(c, 0), tw(c, 1)); }
     PWB_CUDA(cudaGetLastError());
+    return PW_OK;
+  }
+
+  // H psi += Q diag(qd) Q^T psi  for nb bands (column-major, ld)
+  static int dense_nl(pw_ctx* c, const T* psi, int ld, T* out, int ldo, int nb, cudaStream_t st) {
+    cublasHandle_t h = (cublasHandle_t)c->blas;
+    if (cublasSetStream(h, st) != CUBLAS_STATUS_SUCCESS) { set_error("cublasSetStream failed"); return PW_ECUDA; }
+    T* W = reinterpret_cast<T*>(c->s_wq.p);
+    const T* Q = reinterpret_cast<const T*>(c->q.p);
+    const T one = 1, zero = 0;
+    const int np = c->nproj, nt = (int)c->ntot;
+    cublasStatus_t r;
+    { Launch L_(c, st, KK_LIBGEMM);
+    if constexpr (std::is_same<T, double>::value)
+      r = cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, np, nb, nt, &one, Q, nt, psi, ld, &zero, W, np);
+    else
+      r = cublasSgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, np, nb, nt, &one, Q, nt, psi, ld, &zero, W, np); }
+    if (r != CUBLAS_STATUS_SUCCESS) { set_error("projector GEMM (Q^T psi) failed"); return PW_ECUDA; }
+    { Launch L_(c, st, KK_MISC);
+    k_scale_rows<T><<<(unsigned)(((long)np * nb + 255) / 256), 256, 0, st>>>(W, reinterpret_cast<const T*>(c->qd.p), np, nb); }
+    { Launch L_(c, st, KK_LIBGEMM);
+    if constexpr (std::is_same<T, double>::value)
+      r = cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, nt, nb, np, &one, Q, nt, W, np, &one, out, ldo);
+    else
+      r = cublasSgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, nt, nb, np, &one, Q, nt, W, np, &one, out, ldo); }
+    if (r != CUBLAS_STATUS_SUCCESS) { set_error("projector GEMM (Q W) failed"); return PW_ECUDA; }
+    PWB_CUDA(cudaGetLastError());
+    return PW_OK;
+  }
+
+  // Build q_l = T(beta_l) for all projectors with the fine->coarse half of
+  // the pipeline, two projectors per complex field.
+  static int build_q(pw_ctx* c, const int* d_idx, const double* d_beta, const long* d_pio, const long* d_pbo,
+                     const int* d_pnp, int nproj, cudaStream_t st) {
+    int rc = set_attrs();
+    if (rc) return rc;
+    const int cap = c->pair_cap;                 // pairs per pass
+    const long nf = c->ntotf;
+    DevBuf fields;
+    if ((rc = fields.alloc((size_t)2 * cap * nf * sizeof(T)))) return rc;
+    V* AD = reinterpret_cast<V*>(c->s_ad.p);
+    V* BC = reinterpret_cast<V*>(c->s_bc.p);
+    T* Q = reinterpret_cast<T*>(c->q.p);
+    const T inv_nf = (T)(1.0 / (double)c->ntotf);
+    const int ntx = (N0 + TX - 1) / TX;
+    for (int l0 = 0; l0 < nproj; l0 += 2 * cap) {
+      const int nl = std::min(2 * cap, nproj - l0);
+      const int npair = (nl + 1) / 2;
+      PWB_CUDA(cudaMemsetAsync(fields.p, 0, (size_t)2 * npair * nf * sizeof(T), st));
+      k_scatter_beta<T><<<dim3(64, nl), 256, 0, st>>>(reinterpret_cast<T*>(fields.p), nf, d_idx, d_beta, d_pio, d_pbo, d_pnp, l0, nproj);
+      k_floc<T, NF0, NF1, 1><<<dim3(NF2, npair), FLOC_THREADS, sm_floc(), st>>>(
+          BC, nullptr, reinterpret_cast<const T*>(fields.p), nf, inv_nf, tw(c, 3), tw(c, 4));
+      k_zfold<T, N2, NF2><<<dim3(N1, ntx, npair), PENCIL_THREADS, sm_zfold(), st>>>(BC, nullptr, AD, N0, N1, tw(c, 2), tw(c, 5));
+      k_cxy_inv<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(AD, Q, (int)c->ntot, nproj, l0, 0, tw(c, 0), tw(c, 1));
+      PWB_CUDA(cudaGetLastError());
+    }
+    PWB_CUDA(cudaStreamSynchronize(st));
     return PW_OK;
   }
 
@@ -667,18 +848,26 @@ static int teter_thunk(pw_ctx* c, const void* psi, int ld, void* out, int ldo, i
   return Plan<T, N0, N1, N2>::teter_batch(c, (const T*)psi, ld, (T*)out, ldo, nband, band0, npair, acc, st);
 }
 template <typename T, int N0, int N1, int N2> static int cr_thunk() { return Plan<T, N0, N1, N2>::chunk_rows(); }
+using BuildQFn = int (*)(pw_ctx*, const int*, const double*, const long*, const long*, const int*, int, cudaStream_t);
+template <typename T, int N0, int N1, int N2>
+static int buildq_thunk(pw_ctx* c, const int* a, const double* b, const long* d, const long* e, const int* f, int n,
+                        cudaStream_t st) {
+  return Plan<T, N0, N1, N2>::build_q(c, a, b, d, e, f, n, st);
+}
 
 struct GridEntry {
   int n0, n1, n2;
   HpsiFn hpsi[2];
   HpsiFn teter[2];
   ChunkFn cr[2];
+  BuildQFn bq[2];
 };
 
 #define PWB_GRID(a, b, c)                                                                          \
   {a, b, c, {hpsi_thunk<double, a, b, c>, hpsi_thunk<float, a, b, c>},                             \
    {teter_thunk<double, a, b, c>, teter_thunk<float, a, b, c>},                                    \
-   {cr_thunk<double, a, b, c>, cr_thunk<float, a, b, c>}},
+   {cr_thunk<double, a, b, c>, cr_thunk<float, a, b, c>},                                          \
+   {buildq_thunk<double, a, b, c>, buildq_thunk<float, a, b, c>}},
 
 static const GridEntry kGrids[] = {
 #include "grids.inc"
@@ -701,6 +890,13 @@ int run_hpsi(pw_ctx* c, const void* psi, int ld, void* out, int ldo, int nband, 
   const GridEntry* g = find_grid(c->n);
   if (!g) { set_error("grid not built into this library"); return PW_EUNSUPPORTED; }
   return g->hpsi[c->prec == PW_F32 ? 1 : 0](c, psi, ld, out, ldo, nband, band0, npair, acc, st);
+}
+
+int run_build_q(pw_ctx* c, const int* d_idx, const double* d_beta, const long* d_pio, const long* d_pbo,
+                const int* d_pnp, int nproj, cudaStream_t st) {
+  const GridEntry* g = find_grid(c->n);
+  if (!g) { set_error("grid not built into this library"); return PW_EUNSUPPORTED; }
+  return g->bq[c->prec == PW_F32 ? 1 : 0](c, d_idx, d_beta, d_pio, d_pbo, d_pnp, nproj, st);
 }
 
 int run_teter(pw_ctx* c, const void* r, int ld, void* out, int ldo, int nband, int band0, int npair, int acc,

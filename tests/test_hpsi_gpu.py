@@ -24,9 +24,10 @@ def make_system(nc, reps=(1, 1, 1), a=10.26, seed=20261203 + 1, lengths=None):
     return T
 
 
-def make_ctx(T, prec, band_batch=None):
+def make_ctx(T, prec, band_batch=None, mode="dense"):
     from pwdft_develop_b200 import Context
     c = Context(T.dm.length, T.dm.numGrid, T.dm.numGridFine, precision=prec)
+    c.set_nonlocal_mode(mode)
     c.set_vtot(T.vtot)
     c.set_nonlocal([(a[0].idx, np.stack([pp.val[:, 0] for pp in a]), np.array([pp.wgt for pp in a]))
                     for a in T.pseudo])
@@ -40,13 +41,14 @@ def si8():
     return make_system((24, 24, 24))
 
 
+@pytest.mark.parametrize("mode", ["dense", "realspace"])
 @pytest.mark.parametrize("prec", ["f64", "f32"])
-def test_hpsi_parity_si8(si8, prec):
+def test_hpsi_parity_si8(si8, prec, mode):
     import torch
     T = si8
     psi = pw.random_orthonormal_psi(T.dm.ntot, 24, 5)
     ref = pw.mult_spinor(T, psi)
-    c = make_ctx(T, prec)
+    c = make_ctx(T, prec, mode=mode)
     x = torch.tensor(psi, dtype=c.torch_dtype, device="cuda")
     y = c.hpsi(x)
     torch.cuda.synchronize()
@@ -66,24 +68,26 @@ def test_teter_parity_si8(si8, prec):
     assert _rel(got, ref) <= TOL[prec]
 
 
-def test_hpsi_noncubic_grid_f64():
+@pytest.mark.parametrize("mode", ["dense", "realspace"])
+def test_hpsi_noncubic_grid_f64(mode):
     """(24,16,20) coarse grid in a 10.26 x 7.0 x 8.5 cell."""
     import torch
     T = make_system((24, 16, 20), lengths=(10.26, 7.0, 8.5))
     psi = pw.random_orthonormal_psi(T.dm.ntot, 6, 8)
     ref = pw.mult_spinor(T, psi)
-    c = make_ctx(T, "f64")
+    c = make_ctx(T, "f64", mode=mode)
     got = c.hpsi(torch.tensor(psi, device="cuda")).cpu().numpy()
     assert _rel(got, ref) <= TOL["f64"]
 
 
+@pytest.mark.parametrize("mode", ["dense", "realspace"])
 @pytest.mark.parametrize("nband,batch", [(1, None), (5, None), (7, 2), (9, 4)])
-def test_hpsi_odd_bands_and_batches(si8, nband, batch):
+def test_hpsi_odd_bands_and_batches(si8, nband, batch, mode):
     import torch
     T = si8
     psi = pw.random_orthonormal_psi(T.dm.ntot, nband, 11 + nband)
     ref = pw.mult_spinor(T, psi)
-    c = make_ctx(T, "f64", band_batch=batch)
+    c = make_ctx(T, "f64", band_batch=batch, mode=mode)
     got = c.hpsi(torch.tensor(psi, device="cuda")).cpu().numpy()
     assert _rel(got, ref) <= TOL["f64"]
 
@@ -140,14 +144,15 @@ def si64():
     return make_system((48, 48, 48), reps=(2, 2, 2))
 
 
+@pytest.mark.parametrize("mode", ["dense", "realspace"])
 @pytest.mark.parametrize("prec", ["f64", "f32"])
-def test_hpsi_parity_si64_subset(si64, prec):
+def test_hpsi_parity_si64_subset(si64, prec, mode):
     """Si64 (48^3 / 96^3, 320 projectors): a block of 6 bands vs the oracle."""
     import torch
     T = si64
     psi = pw.random_orthonormal_psi(T.dm.ntot, 6, 51)
     ref = pw.mult_spinor(T, psi)
-    c = make_ctx(T, prec)
+    c = make_ctx(T, prec, mode=mode)
     got = c.hpsi(torch.tensor(psi, dtype=c.torch_dtype, device="cuda")).double().cpu().numpy()
     assert _rel(got, ref) <= TOL[prec]
 
