@@ -84,6 +84,14 @@ PW_API int pw_set_nonlocal(pw_ctx* ctx, int natom, const int* atom_npts, const i
 /* Select the nonlocal apply mode (call before pw_set_nonlocal / pw_set_atoms). */
 PW_API int pw_set_nonlocal_mode(pw_ctx* ctx, int mode);
 
+/* GEMM engine for FP32 contexts: mode 0 = split-BF16 tcgen05 kernels with
+ * `terms` products per k-step (3: hi*hi + hi*lo + lo*hi, 4: + lo*lo),
+ * mode 1 = vendor SGEMM.  FP64 contexts always use FP64 GEMMs. */
+PW_API int pw_set_gemm_mode(pw_ctx* ctx, int mode, int terms);
+/* When enabled, every H*psi call synchronises and returns PW_ETIMEOUT if a
+ * bounded device-side pipeline wait gave up (default off). */
+PW_API int pw_set_check_errors(pw_ctx* ctx, int enable);
+
 /* H*psi for nband bands: hpsi (+)= (-1/2 Laplacian + V_loc + V_nl) psi.
  * Replaces Spinor::AddMultSpinorFineR2C(fft, ekin, vtot, pseudo, a3)
  * (src/SCF/spinor.cpp:377-525; accumulate=1 gives its a3 += semantics) and
@@ -143,6 +151,16 @@ PW_API int pw_stats(const pw_ctx* ctx, long* kernel_launches, long* library_call
  * 11 vendor-library GEMM. */
 PW_API int pw_profile(pw_ctx* ctx, int enable);
 PW_API int pw_profile_read(pw_ctx* ctx, int kind, double* total_ms, long* count);
+
+/* Gram block over the coarse grid: G (nx x ny, column-major, leading
+ * dimension ldg, FP64, device) = X^T Y for X (ntot x nx, ldx) and Y
+ * (ntot x ny, ldy) in the context's precision.  Replaces the
+ * blas::Gemm('T','N', ...) + MPI_Allreduce Gram blocks of
+ * EigenSolver::Orthogonalize (src/EigenSolver/eigensolver.cpp:301-384) and
+ * LOBPCGSolveReal (src/EigenSolver/lobpcg.cpp:683-874).  FP32 contexts run
+ * split-BF16 tensor-core GEMMs with FP32 accumulation. */
+PW_API int pw_gram(pw_ctx* ctx, const void* X, int ldx, int nx, const void* Y, int ldy, int ny, double* G, int ldg,
+                   void* stream);
 
 /* Maximum number of bands processed per internal batch (sets scratch size).
  * Default 64. Scratch grows to hold ceil(nband_batch/2) band pairs. */

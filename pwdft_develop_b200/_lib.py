@@ -48,6 +48,9 @@ SIGNATURES: dict[str, tuple] = {
     "pw_teter_precond": (_i, [_vp, _vp, _i, _vp, _i, _i, _i, _vp]),
     "pw_set_band_batch": (_i, [_vp, _i]),
     "pw_set_nonlocal_mode": (_i, [_vp, _i]),
+    "pw_set_gemm_mode": (_i, [_vp, _i, _i]),
+    "pw_set_check_errors": (_i, [_vp, _i]),
+    "pw_gram": (_i, [_vp, _vp, _i, _i, _vp, _i, _i, _vp, _i, _vp]),
     "pw_hgh_species": (_i, [_i, _dp, _dp, _dp, _dp, _ip]),
     "pw_set_atoms": (_i, [_vp, _i, _ip, _dp]),
     "pw_get_pseudocharge": (_i, [_vp, _dp]),

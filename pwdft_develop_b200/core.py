@@ -208,6 +208,27 @@ def _ctx_profile_read(self, kind: int):
     return t.value, n.value
 
 
+def _ctx_gram(self, X, Y=None, stream=None):
+    """G = X^T Y (X, Y: (n, ntot) device tensors) as an (nx, ny) FP64 tensor."""
+    import torch
+    Y = X if Y is None else Y
+    G = torch.empty((Y.shape[0], X.shape[0]), dtype=torch.float64, device=X.device)   # column-major nx x ny
+    check(lib.pw_gram(self._h, _ptr(X), self.ntot, X.shape[0], _ptr(Y), self.ntot, Y.shape[0], _ptr(G),
+                      X.shape[0], _stream(stream)))
+    return G.T
+
+
+def _ctx_set_gemm_mode(self, mode: str = "tc", terms: int = 3):
+    check(lib.pw_set_gemm_mode(self._h, 0 if mode == "tc" else 1, int(terms)))
+
+
+def _ctx_set_check_errors(self, on: bool = True):
+    check(lib.pw_set_check_errors(self._h, int(on)))
+
+
+Context.gram = _ctx_gram
+Context.set_gemm_mode = _ctx_set_gemm_mode
+Context.set_check_errors = _ctx_set_check_errors
 Context.set_atoms = _ctx_set_atoms
 Context.pseudocharge = _ctx_pseudocharge
 Context.launches = _ctx_launches

@@ -92,6 +92,13 @@ struct pw_ctx {
   pwb::DevBuf qd;                // T [nproj]        gamma_l * vol / ntot
   pwb::DevBuf s_wq;              // T [nproj][band batch] projections
   void* blas = nullptr;          // cublasHandle_t
+  // FP32 contexts: bf16 hi/lo copies of Q ([l][g]) and Q^T ([g][l], rows padded
+  // to nproj_pad) for the split-BF16 tensor-core GEMMs
+  int gemm_mode = 0;             // 0 tensor-core split-BF16, 1 vendor SGEMM
+  int gemm_terms = 3;            // split products per k-step (3 or 4)
+  bool check_errors = false;     // read the device error flag after each call (synchronises)
+  int nproj_pad = 0;
+  pwb::DevBuf q_bf, qt_bf, s_psi_bf, s_w_bf, s_ws, s_gx_bf, s_gy_bf;
   // host copies kept for setup-time work
   std::vector<double> h_vtot;
   // atoms set through pw_set_atoms (HGH species built in this library)

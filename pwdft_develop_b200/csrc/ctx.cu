@@ -9,6 +9,7 @@
 
 #include "common.hpp"
 #include "fft.cuh"
+#include "gemm.hpp"
 
 namespace pwb {
 
@@ -225,6 +226,19 @@ int pw_set_nonlocal_mode(pw_ctx* ctx, int mode) {
   return PW_OK;
 }
 
+int pw_set_gemm_mode(pw_ctx* ctx, int mode, int terms) {
+  PWB_CHECK(ctx && (mode == 0 || mode == 1) && (terms == 3 || terms == 4), PW_EINVAL, "bad GEMM mode");
+  ctx->gemm_mode = mode;
+  ctx->gemm_terms = terms;
+  return PW_OK;
+}
+
+int pw_set_check_errors(pw_ctx* ctx, int enable) {
+  PWB_CHECK(ctx, PW_EINVAL, "null context");
+  ctx->check_errors = enable != 0;
+  return PW_OK;
+}
+
 int pw_set_band_batch(pw_ctx* ctx, int nband_batch) {
   PWB_CHECK(ctx && nband_batch > 0, PW_EINVAL, "bad band batch");
   PWB_CUDA(cudaSetDevice(ctx->device));
@@ -294,6 +308,22 @@ int pw_set_nonlocal(pw_ctx* ctx, int natom, const int* atom_npts, const int* ato
       rc = run_build_q(ctx, (const int*)d_idx.p, (const double*)d_beta.p, (const long*)d_pio.p,
                        (const long*)d_pbo.p, (const int*)d_pnp.p, nproj, nullptr);
       if (rc) return rc;
+      if (ctx->prec == PW_F32) {
+        const int npp = (nproj + 7) / 8 * 8;
+        ctx->nproj_pad = npp;
+        const size_t nt = ctx->ntot;
+        if ((rc = ctx->q_bf.alloc((size_t)2 * nproj * nt * 2)) || (rc = ctx->qt_bf.alloc((size_t)2 * nt * npp * 2)))
+          return rc;
+        PWB_CUDA(cudaMemset(ctx->qt_bf.p, 0, (size_t)2 * nt * npp * 2));
+        char* qb = (char*)ctx->q_bf.p;
+        char* qtb = (char*)ctx->qt_bf.p;
+        if ((rc = split_bf16((const float*)ctx->q.p, nt, (int)nt, nproj, qb, qb + (size_t)nproj * nt * 2, nt, 1.0f,
+                             nullptr)))
+          return rc;
+        if ((rc = split_bf16_t((const float*)ctx->q.p, nt, (int)nt, nproj, qtb, qtb + nt * npp * 2, npp, nullptr)))
+          return rc;
+        PWB_CUDA(cudaDeviceSynchronize());
+      }
     }
     nl.natom = natom;
     nl.npmax = npmax;
@@ -401,6 +431,7 @@ int pw_hpsi(pw_ctx* ctx, const void* psi, int ld, void* hpsi, int ldh, int nband
     int rc = run_hpsi(ctx, psi, ld, hpsi, ldh, nband, b0, npair, accumulate, st);
     if (rc) return rc;
   }
+  if (ctx->check_errors) return gemm_error_check();
   return PW_OK;
 }
 

@@ -1,0 +1,71 @@
+// Grid-reduction Gram products and subspace operations for the block
+// eigensolvers (EigenSolver::Orthogonalize, SolveGenEig, LOBPCG / PPCG
+// Gram blocks: src/EigenSolver/eigensolver.cpp:133-384, lobpcg.cpp:683-874).
+// FP32 contexts use the split-BF16 tcgen05 GEMMs, FP64 contexts FP64 GEMMs.
+#include <cublas_v2.h>
+
+#include <algorithm>
+
+#include "common.hpp"
+#include "gemm.hpp"
+
+using namespace pwb;
+
+namespace pwb {
+
+// G (nx x ny, column-major, ldg, double, device) = alpha * X^T Y over the grid
+int gram(pw_ctx* c, const void* X, int ldx, int nx, const void* Y, int ldy, int ny, double* G, int ldg,
+         cudaStream_t st) {
+  const int nt = (int)c->ntot;
+  if (nx == 0 || ny == 0) return PW_OK;
+  if (c->prec == PW_F64) {
+    cublasHandle_t h = (cublasHandle_t)c->blas;
+    cublasSetStream(h, st);
+    const double one = 1.0, zero = 0.0;
+    c->lib_launches++;
+    if (cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, nx, ny, nt, &one, (const double*)X, ldx, (const double*)Y, ldy, &zero,
+                    G, ldg) != CUBLAS_STATUS_SUCCESS) {
+      set_error("FP64 Gram GEMM failed");
+      return PW_ECUDA;
+    }
+    return PW_OK;
+  }
+  int rc;
+  const bool same = (X == Y && ldx == ldy && nx == ny);
+  const size_t bx = (size_t)nx * nt * 2, by = (size_t)ny * nt * 2;
+  if ((rc = c->s_gx_bf.alloc(2 * bx)) || (!same && (rc = c->s_gy_bf.alloc(2 * by)))) return rc;
+  char* xb = (char*)c->s_gx_bf.p;
+  char* yb = same ? xb : (char*)c->s_gy_bf.p;
+  c->launches++;
+  if ((rc = split_bf16((const float*)X, ldx, nt, nx, xb, xb + bx, nt, 1.0f, st))) return rc;
+  if (!same) {
+    c->launches++;
+    if ((rc = split_bf16((const float*)Y, ldy, nt, ny, yb, yb + by, nt, 1.0f, st))) return rc;
+  }
+  SplitOperand A{xb, xb + bx, nx, nt};
+  SplitOperand B{yb, yb + (same ? bx : by), ny, nt};
+  ReduceOut ro;
+  ro.out = G;
+  ro.ldo = ldg;
+  ro.f64 = 1;
+  ro.transpose = 1;    // G[j*ldg + i] = sum_g X[i][g] Y[j][g]
+  c->launches += 2;
+  return gemm_tn_reduce(A, B, nt, c->gemm_terms, c->s_ws, ro, st);
+}
+
+}  // namespace pwb
+
+extern "C" {
+
+int pw_gram(pw_ctx* ctx, const void* X, int ldx, int nx, const void* Y, int ldy, int ny, double* G, int ldg,
+            void* stream) {
+  PWB_CHECK(ctx && (nx == 0 || X) && (ny == 0 || Y) && (nx * ny == 0 || G), PW_EINVAL, "null argument");
+  PWB_CHECK(ldx >= ctx->ntot && ldy >= ctx->ntot && ldg >= nx, PW_EINVAL, "bad leading dimension");
+  PWB_CUDA(cudaSetDevice(ctx->device));
+  int rc = gram(ctx, X, ldx, nx, Y, ldy, ny, G, ldg, (cudaStream_t)stream);
+  if (rc) return rc;
+  if (ctx->check_errors) return gemm_error_check();
+  return PW_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,475 @@
+// Split-BF16 tensor-core GEMM for sm_100a (tcgen05 + TMA + TMEM).
+//
+//   C[m][n] = sum_k A[m][k] * B[n][k]        (both operands K-major)
+//
+// Each FP32 operand x is split into x_hi = bf16(x), x_lo = bf16(x - x_hi);
+// the kernel accumulates A_hi B_hi + A_hi B_lo + A_lo B_hi (optionally
+// + A_lo B_lo) in FP32 in tensor memory.  With the operands' bf16 pair
+// carrying ~16 mantissa bits this reproduces an FP32 product to ~1e-5
+// relative per term.
+//
+// One CTA computes a 128 x BN tile over a K range: warp 0 issues TMA loads
+// into a ring of shared-memory stages, warp 1 issues the UMMAs (one elected
+// thread) and commits each stage back to the producer, warps 2-5 read the
+// accumulator from TMEM and write the tile.  Two epilogues: a split-K
+// partial (deterministically reduced by a second kernel) and a direct
+// row-major (optionally accumulating) store.  No cluster multicast is used.
+// Every mbarrier wait is bounded: on timeout the kernel records an error code,
+// drains its own copies and frees its tensor memory.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cstring>
+
+#include "common.hpp"
+#include "gemm.hpp"
+
+namespace pwb {
+
+constexpr int GM = 128;             // tile rows (UMMA M)
+constexpr int GK = 64;              // K per stage (one 128-byte swizzle row of bf16)
+constexpr int GEMM_THREADS = 192;   // 6 warps
+constexpr unsigned long long WAIT_NS = 2000000000ull;   // 2 s per wait
+
+__device__ int g_gemm_error = 0;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* b, int count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count));
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t* b, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ unsigned long long gtimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+// bounded wait; returns false (and records code) on timeout
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, int code) {
+  if (mbar_try(b, parity)) return true;
+  const unsigned long long t0 = gtimer();
+  for (unsigned it = 1;; ++it) {
+    if (mbar_try(b, parity)) return true;
+    if ((it & 255) == 0 && gtimer() - t0 > WAIT_NS) break;
+  }
+  atomicCAS(&g_gemm_error, 0, code);
+  return false;
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
+      ::"r"(smem_u32(dst)), "l"(map), "r"(smem_u32(bar)), "r"(x), "r"(y)
+      : "memory");
+}
+
+// UMMA shared-memory descriptor: K-major, 128-byte swizzle, 8-row groups 1024 B apart
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+  d |= (uint64_t)1 << 16;                 // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)(1024 >> 4) << 32;       // stride byte offset
+  d |= (uint64_t)1 << 46;                 // descriptor version (sm100)
+  d |= (uint64_t)2 << 61;                 // SWIZZLE_128B
+  return d;
+}
+
+template <int BN> __host__ __device__ constexpr uint32_t umma_idesc() {
+  // F32 accumulate, BF16 A and B, both K-major, N = BN, M = 128
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(GM >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accum) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+      ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accum));
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+template <int BN> struct GemmSmem {
+  static constexpr int A_BYTES = GM * GK * 2;          // one bf16 tile of A
+  static constexpr int B_BYTES = BN * GK * 2;
+  static constexpr int STAGE = 2 * A_BYTES + 2 * B_BYTES;
+  static constexpr int NSTAGE = (3 * STAGE + 2048 <= 226 * 1024) ? 3 : 2;
+  static constexpr int BYTES = NSTAGE * STAGE + 1024 /*align*/ + 256 /*barriers*/;
+  static constexpr int TMEM_COLS = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
+};
+
+struct GemmArgs {
+  int M, N, K;           // full problem
+  int kchunk;            // K per split (multiple of GK)
+  int nterms;            // 3 or 4 split products
+  int epi;               // 0: split-K partial, 1: row-major store
+  float* ws;             // epi 0: [split][M][N]
+  float* C;              // epi 1: C[m*ldc + n]
+  long ldc;
+  int accumulate;        // epi 1: C += tile
+};
+
+template <int BN>
+__global__ void __launch_bounds__(GEMM_THREADS, 1)
+k_gemm_tn(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant__ CUtensorMap tmA_lo,
+          const __grid_constant__ CUtensorMap tmB_hi, const __grid_constant__ CUtensorMap tmB_lo, GemmArgs g) {
+  using SM = GemmSmem<BN>;
+  extern __shared__ __align__(1024) unsigned char smraw[];
+  unsigned char* base = (unsigned char*)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
+  uint64_t* full = reinterpret_cast<uint64_t*>(base + SM::NSTAGE * SM::STAGE);
+  uint64_t* empty = full + SM::NSTAGE;
+  uint64_t* accum_bar = empty + SM::NSTAGE;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accum_bar + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m0 = blockIdx.x * GM, n0 = blockIdx.y * BN;
+  const int kbeg = blockIdx.z * g.kchunk;
+  const int kend = min(g.K, kbeg + g.kchunk);
+  const int nkb = (kend > kbeg) ? (kend - kbeg + GK - 1) / GK : 0;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < SM::NSTAGE; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(accum_bar, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(SM::TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      int issued = 0;
+      for (int kb = 0; kb < nkb; ++kb) {
+        const int s = kb % SM::NSTAGE;
+        if (kb >= SM::NSTAGE && !mbar_wait(&empty[s], ((kb / SM::NSTAGE) - 1) & 1, 1)) { *abort_flag = 1; break; }
+        if (*abort_flag) break;
+        unsigned char* st = base + s * SM::STAGE;
+        mbar_expect_tx(&full[s], SM::STAGE);
+        const int kx = kbeg + kb * GK;
+        tma_load_2d(st, &tmA_hi, &full[s], kx, m0);
+        tma_load_2d(st + SM::A_BYTES, &tmA_lo, &full[s], kx, m0);
+        tma_load_2d(st + 2 * SM::A_BYTES, &tmB_hi, &full[s], kx, n0);
+        tma_load_2d(st + 2 * SM::A_BYTES + SM::B_BYTES, &tmB_lo, &full[s], kx, n0);
+        issued = kb + 1;
+      }
+      // drain: every issued stage must have landed before the CTA exits
+      for (int kb = std::max(0, issued - SM::NSTAGE); kb < issued; ++kb)
+        mbar_wait(&full[kb % SM::NSTAGE], (kb / SM::NSTAGE) & 1, 2);
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      constexpr uint32_t idesc = umma_idesc<BN>();
+      bool ok = true;
+      for (int kb = 0; kb < nkb; ++kb) {
+        const int s = kb % SM::NSTAGE;
+        if (!mbar_wait(&full[s], (kb / SM::NSTAGE) & 1, 3)) { *abort_flag = 1; ok = false; break; }
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        const uint32_t sa = smem_u32(base + s * SM::STAGE);
+        const uint32_t ahi = sa, alo = sa + SM::A_BYTES;
+        const uint32_t bhi = sa + 2 * SM::A_BYTES, blo = bhi + SM::B_BYTES;
+#pragma unroll
+        for (int kk = 0; kk < GK / 16; ++kk) {
+          const uint32_t off = kk * 32;   // 16 bf16 along K inside the swizzled 128-byte row
+          const uint32_t acc0 = (kb > 0 || kk > 0) ? 1u : 0u;
+          umma_bf16(tmem, umma_desc(ahi + off), umma_desc(bhi + off), idesc, acc0);
+          umma_bf16(tmem, umma_desc(ahi + off), umma_desc(blo + off), idesc, 1u);
+          umma_bf16(tmem, umma_desc(alo + off), umma_desc(bhi + off), idesc, 1u);
+          if (g.nterms > 3) umma_bf16(tmem, umma_desc(alo + off), umma_desc(blo + off), idesc, 1u);
+        }
+        umma_commit(&empty[s]);
+      }
+      if (ok) umma_commit(accum_bar);
+      else {
+        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(accum_bar)) : "memory");
+      }
+    }
+  } else {
+    // epilogue warps 2..5: TMEM lanes 32*(warp%4) .. +31
+    const int q = warp & 3;
+    const int row = m0 + q * 32 + lane;
+    int ok = 1;
+    if (nkb > 0 && lane == 0) ok = mbar_wait(accum_bar, 0, 4) ? 1 : 0;
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    const int ab = __shfl_sync(0xffffffffu, *abort_flag, 0);
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    if (ok && !ab) {
+      for (int c0 = 0; c0 < BN; c0 += 16) {
+        uint32_t r[16];
+        const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c0;
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+            : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (row < g.M) {
+          if (nkb == 0) {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) r[j] = 0u;
+          }
+          if (g.epi == 0) {
+            float* dst = g.ws + ((long)blockIdx.z * g.M + row) * g.N + n0 + c0;
+#pragma unroll
+            for (int j = 0; j < 16; ++j)
+              if (n0 + c0 + j < g.N) dst[j] = __uint_as_float(r[j]);
+          } else {
+            float* dst = g.C + (long)row * g.ldc + n0 + c0;
+            if (g.accumulate) {
+#pragma unroll
+              for (int j = 0; j < 16; ++j)
+                if (n0 + c0 + j < g.N) dst[j] += __uint_as_float(r[j]);
+            } else {
+#pragma unroll
+              for (int j = 0; j < 16; ++j)
+                if (n0 + c0 + j < g.N) dst[j] = __uint_as_float(r[j]);
+            }
+          }
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  if (warp == 1) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(SM::TMEM_COLS));
+  }
+}
+
+// fp32 -> (bf16 hi, bf16 lo) with rows of length ncol at stride ld_in -> packed ld_out
+__global__ void k_split_bf16(const float* __restrict__ x, long ld_in, int ncol, int nrow, __nv_bfloat16* __restrict__ hi,
+                             __nv_bfloat16* __restrict__ lo, long ld_out, float scale) {
+  const long total = (long)nrow * ncol;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+    const long r = i / ncol, c = i - r * ncol;
+    const float v = x[r * ld_in + c] * scale;
+    const __nv_bfloat16 h = __float2bfloat16_rn(v);
+    const __nv_bfloat16 l = __float2bfloat16_rn(v - __bfloat162float(h));
+    hi[r * ld_out + c] = h;
+    lo[r * ld_out + c] = l;
+  }
+}
+
+// transpose + split: x is nrow x ncol (row stride ld_in); writes the ncol x nrow
+// transpose as bf16 hi/lo with row stride ld_out
+__global__ void k_split_bf16_t(const float* __restrict__ x, long ld_in, int ncol, int nrow, __nv_bfloat16* __restrict__ hi,
+                               __nv_bfloat16* __restrict__ lo, long ld_out) {
+  __shared__ float tile[32][33];
+  const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    const int r = r0 + j, c = c0 + threadIdx.x;
+    tile[j][threadIdx.x] = (r < nrow && c < ncol) ? x[(long)r * ld_in + c] : 0.f;
+  }
+  __syncthreads();
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    const int c = c0 + j, r = r0 + threadIdx.x;
+    if (c < ncol && r < nrow) {
+      const float v = tile[threadIdx.x][j];
+      const __nv_bfloat16 h = __float2bfloat16_rn(v);
+      hi[(long)c * ld_out + r] = h;
+      lo[(long)c * ld_out + r] = __float2bfloat16_rn(v - __bfloat162float(h));
+    }
+  }
+}
+
+// out = sum over splits of ws[split][M][N], with optional per-row / per-column
+// scale, written as double or float, directly or transposed.
+__global__ void k_splitk_reduce(const float* __restrict__ ws, int nsplit, int M, int N, const float* __restrict__ rs,
+                                const float* __restrict__ cs, int transpose, int out_f64, void* out, long ldo,
+                                __nv_bfloat16* bhi, __nv_bfloat16* blo, long ldb) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= (long)M * N) return;
+  const int m = (int)(i / N), n = (int)(i - (long)m * N);
+  double s = 0;
+  for (int k = 0; k < nsplit; ++k) s += (double)ws[((long)k * M + m) * N + n];
+  if (rs) s *= rs[m];
+  if (cs) s *= cs[n];
+  const long o = transpose ? (long)n * ldo + m : (long)m * ldo + n;
+  if (out) {
+    if (out_f64) reinterpret_cast<double*>(out)[o] = s;
+    else reinterpret_cast<float*>(out)[o] = (float)s;
+  }
+  if (bhi) {
+    const long ob = transpose ? (long)n * ldb + m : (long)m * ldb + n;
+    const float v = (float)s;
+    const __nv_bfloat16 h = __float2bfloat16_rn(v);
+    bhi[ob] = h;
+    blo[ob] = __float2bfloat16_rn(v - __bfloat162float(h));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+static PFN_cuTensorMapEncodeTiled_v12000 get_encode() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+// 2-D bf16 tensor map over rows x K (K contiguous, row stride ld elements), box GK x box_rows
+static int make_tmap(CUtensorMap* m, const void* ptr, long rows, long K, long ld, int box_rows) {
+  auto enc = get_encode();
+  PWB_CHECK(enc, PW_ECUDA, "cuTensorMapEncodeTiled unavailable");
+  PWB_CHECK(((uintptr_t)ptr & 15) == 0 && (ld * 2) % 16 == 0, PW_EINVAL, "TMA operand not 16-byte aligned");
+  cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)(ld * 2)};
+  cuuint32_t box[2] = {(cuuint32_t)GK, (cuuint32_t)box_rows};
+  cuuint32_t es[2] = {1, 1};
+  CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(ptr), dims, strides, box, es,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  PWB_CHECK(r == CUDA_SUCCESS, PW_ECUDA, "cuTensorMapEncodeTiled failed");
+  return PW_OK;
+}
+
+template <int BN> static int launch_bn(const SplitOperand& A, const SplitOperand& B, const GemmArgs& g, int nsplit,
+                                       cudaStream_t st) {
+  using SM = GemmSmem<BN>;
+  static bool attr = false;
+  if (!attr) {
+    PWB_CUDA(cudaFuncSetAttribute(k_gemm_tn<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM::BYTES));
+    attr = true;
+  }
+  CUtensorMap ah, al, bh, bl;
+  int rc;
+  if ((rc = make_tmap(&ah, A.hi, A.rows, g.K, A.ld, GM)) || (rc = make_tmap(&al, A.lo, A.rows, g.K, A.ld, GM)) ||
+      (rc = make_tmap(&bh, B.hi, B.rows, g.K, B.ld, BN)) || (rc = make_tmap(&bl, B.lo, B.rows, g.K, B.ld, BN)))
+    return rc;
+  dim3 grid((g.M + GM - 1) / GM, (g.N + BN - 1) / BN, nsplit);
+  k_gemm_tn<BN><<<grid, GEMM_THREADS, SM::BYTES, st>>>(ah, al, bh, bl, g);
+  PWB_CUDA(cudaGetLastError());
+  return PW_OK;
+}
+
+static int launch(const SplitOperand& A, const SplitOperand& B, const GemmArgs& g, int BN, int nsplit,
+                  cudaStream_t st) {
+  switch (BN) {
+    case 32: return launch_bn<32>(A, B, g, nsplit, st);
+    case 64: return launch_bn<64>(A, B, g, nsplit, st);
+    case 96: return launch_bn<96>(A, B, g, nsplit, st);
+    case 128: return launch_bn<128>(A, B, g, nsplit, st);
+    case 160: return launch_bn<160>(A, B, g, nsplit, st);
+    case 192: return launch_bn<192>(A, B, g, nsplit, st);
+    case 256: return launch_bn<256>(A, B, g, nsplit, st);
+    default: set_error("unsupported GEMM tile width"); return PW_EUNSUPPORTED;
+  }
+}
+
+static int pick_bn(int N) {
+  static const int cands[] = {32, 64, 96, 128, 160, 192, 256};
+  // smallest padding waste, then widest tile
+  int best = 256;
+  long bestw = -1;
+  for (int bn : cands) {
+    const long pad = ((N + bn - 1) / bn) * (long)bn;
+    if (bestw < 0 || pad < bestw || (pad == bestw && bn > best)) { bestw = pad; best = bn; }
+  }
+  return best;
+}
+
+int gemm_error_check() {
+  int h = 0;
+  PWB_CUDA(cudaMemcpyFromSymbol(&h, g_gemm_error, sizeof(int)));
+  if (h) {
+    int z = 0;
+    cudaMemcpyToSymbol(g_gemm_error, &z, sizeof(int));
+    set_error("tensor-core GEMM pipeline wait timed out (code " + std::to_string(h) + ")");
+    return PW_ETIMEOUT;
+  }
+  return PW_OK;
+}
+
+int split_bf16(const float* x, long ld_in, int ncol, int nrow, void* hi, void* lo, long ld_out, float scale,
+               cudaStream_t st) {
+  const long total = (long)nrow * ncol;
+  if (total == 0) return PW_OK;
+  const int nb = (int)std::min<long>((total + 255) / 256, 148L * 16);
+  k_split_bf16<<<nb, 256, 0, st>>>(x, ld_in, ncol, nrow, (__nv_bfloat16*)hi, (__nv_bfloat16*)lo, ld_out, scale);
+  PWB_CUDA(cudaGetLastError());
+  return PW_OK;
+}
+
+int split_bf16_t(const float* x, long ld_in, int ncol, int nrow, void* hi, void* lo, long ld_out, cudaStream_t st) {
+  if ((long)nrow * ncol == 0) return PW_OK;
+  dim3 grid((ncol + 31) / 32, (nrow + 31) / 32);
+  k_split_bf16_t<<<grid, dim3(32, 8), 0, st>>>(x, ld_in, ncol, nrow, (__nv_bfloat16*)hi, (__nv_bfloat16*)lo, ld_out);
+  PWB_CUDA(cudaGetLastError());
+  return PW_OK;
+}
+
+int gemm_tn_reduce(const SplitOperand& A, const SplitOperand& B, int K, int nterms, DevBuf& ws,
+                   const ReduceOut& out, cudaStream_t st) {
+  const int M = A.rows, N = B.rows;
+  if (M == 0 || N == 0) return PW_OK;
+  const int BN = pick_bn(N);
+  const int tiles = ((M + GM - 1) / GM) * ((N + BN - 1) / BN);
+  // enough CTAs to fill the GPU twice over, each with >= 4 K-blocks
+  int nsplit = std::max(1, (2 * 148 + tiles - 1) / tiles);
+  const int maxsplit = std::max(1, (K + 4 * GK - 1) / (4 * GK));
+  nsplit = std::min(nsplit, maxsplit);
+  int kchunk = ((K + nsplit - 1) / nsplit + GK - 1) / GK * GK;
+  nsplit = (K + kchunk - 1) / kchunk;
+  int rc = ws.alloc((size_t)nsplit * M * N * sizeof(float));
+  if (rc) return rc;
+  GemmArgs g{};
+  g.M = M; g.N = N; g.K = K; g.kchunk = kchunk; g.nterms = nterms; g.epi = 0;
+  g.ws = reinterpret_cast<float*>(ws.p);
+  if ((rc = launch(A, B, g, BN, nsplit, st))) return rc;
+  const long tot = (long)M * N;
+  k_splitk_reduce<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(
+      g.ws, nsplit, M, N, out.row_scale, out.col_scale, out.transpose, out.f64, out.out, out.ldo,
+      (__nv_bfloat16*)out.bf_hi, (__nv_bfloat16*)out.bf_lo, out.ldb);
+  PWB_CUDA(cudaGetLastError());
+  return PW_OK;
+}
+
+int gemm_tn_store(const SplitOperand& A, const SplitOperand& B, int K, int nterms, float* C, long ldc, int accumulate,
+                  cudaStream_t st) {
+  const int M = A.rows, N = B.rows;
+  if (M == 0 || N == 0) return PW_OK;
+  const int BN = N >= 256 ? 256 : pick_bn(N);
+  GemmArgs g{};
+  g.M = M; g.N = N; g.K = K; g.kchunk = ((K + GK - 1) / GK) * GK; g.nterms = nterms; g.epi = 1;
+  g.C = C; g.ldc = ldc; g.accumulate = accumulate;
+  return launch(A, B, g, BN, 1, st);
+}
+
+}  // namespace pwb

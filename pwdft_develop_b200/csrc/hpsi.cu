@@ -24,6 +24,7 @@
 
 #include "common.hpp"
 #include "fft.cuh"
+#include "gemm.hpp"
 
 namespace pwb {
 
@@ -757,6 +758,9 @@ struct Plan {
 
   // H psi += Q diag(qd) Q^T psi  for nb bands (column-major, ld)
   static int dense_nl(pw_ctx* c, const T* psi, int ld, T* out, int ldo, int nb, cudaStream_t st) {
+    if constexpr (std::is_same<T, float>::value) {
+      if (c->gemm_mode == 0) return dense_nl_tc(c, psi, ld, out, ldo, nb, st);
+    }
     cublasHandle_t h = (cublasHandle_t)c->blas;
     if (cublasSetStream(h, st) != CUBLAS_STATUS_SUCCESS) { set_error("cublasSetStream failed"); return PW_ECUDA; }
     T* W = reinterpret_cast<T*>(c->s_wq.p);
@@ -779,6 +783,35 @@ struct Plan {
       r = cublasSgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, nt, nb, np, &one, Q, nt, W, np, &one, out, ldo); }
     if (r != CUBLAS_STATUS_SUCCESS) { set_error("projector GEMM (Q W) failed"); return PW_ECUDA; }
     PWB_CUDA(cudaGetLastError());
+    return PW_OK;
+  }
+
+  // FP32 context: split-BF16 tcgen05 GEMMs
+  static int dense_nl_tc(pw_ctx* c, const float* psi, int ld, float* out, int ldo, int nb, cudaStream_t st) {
+    const int np = c->nproj, nt = (int)c->ntot, npp = c->nproj_pad;
+    int rc;
+    if ((rc = c->s_psi_bf.alloc((size_t)2 * nb * nt * 2))) return rc;
+    if ((rc = c->s_w_bf.alloc((size_t)2 * nb * npp * 2))) return rc;
+    char* pb = (char*)c->s_psi_bf.p;
+    char* wb = (char*)c->s_w_bf.p;
+    { Launch L_(c, st, KK_MISC);
+    if ((rc = split_bf16(psi, ld, nt, nb, pb, pb + (size_t)nb * nt * 2, nt, 1.0f, st))) return rc; }
+    // W^T[b][l] = d_l * sum_g Q[l][g] psi[b][g]   (split-K, deterministic reduce)
+    SplitOperand A{c->q_bf.p, (char*)c->q_bf.p + (size_t)np * nt * 2, np, nt};
+    SplitOperand B{pb, pb + (size_t)nb * nt * 2, nb, nt};
+    ReduceOut ro;
+    ro.transpose = 1;
+    ro.row_scale = reinterpret_cast<const float*>(c->qd.p);
+    ro.bf_hi = wb;
+    ro.bf_lo = wb + (size_t)nb * npp * 2;
+    ro.ldb = npp;
+    { Launch L_(c, st, KK_GRAM);
+    if ((rc = gemm_tn_reduce(A, B, nt, c->gemm_terms, c->s_ws, ro, st))) return rc; }
+    // out[b][g] += sum_l W^T[b][l] QT[g][l]
+    SplitOperand W{wb, wb + (size_t)nb * npp * 2, nb, npp};
+    SplitOperand QT{c->qt_bf.p, (char*)c->qt_bf.p + (size_t)nt * npp * 2, nt, npp};
+    { Launch L_(c, st, KK_GRAM);
+    if ((rc = gemm_tn_store(W, QT, np, c->gemm_terms, out, ldo, 1, st))) return rc; }
     return PW_OK;
   }
 
