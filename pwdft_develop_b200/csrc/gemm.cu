@@ -122,9 +122,9 @@ struct GemmArgs {
   int M, N, K;           // full problem
   int kchunk;            // K per split (multiple of GK)
   int nterms;            // 3 or 4 split products
-  int epi;               // 0: split-K partial, 1: row-major store
-  float* ws;             // epi 0: [split][M][N]
-  float* C;              // epi 1: C[m*ldc + n]
+  int epi;               // 0: split-K partial, 1: row-major store, 2: transposed store
+  float* ws;             // epi 0: [split][N][M]
+  float* C;              // epi 1: C[m*ldc + n], epi 2: C[n*ldc + m]
   long ldc;
   int accumulate;        // epi 1: C += tile
 };
@@ -239,10 +239,23 @@ k_gemm_tn(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant__ CU
             for (int j = 0; j < 16; ++j) r[j] = 0u;
           }
           if (g.epi == 0) {
-            float* dst = g.ws + ((long)blockIdx.z * g.M + row) * g.N + n0 + c0;
+            // split-K partial, stored [split][n][m]: lanes (consecutive m) coalesce
+            float* dst = g.ws + ((long)blockIdx.z * g.N + n0 + c0) * g.M + row;
 #pragma unroll
             for (int j = 0; j < 16; ++j)
-              if (n0 + c0 + j < g.N) dst[j] = __uint_as_float(r[j]);
+              if (n0 + c0 + j < g.N) dst[(long)j * g.M] = __uint_as_float(r[j]);
+          } else if (g.epi == 2) {
+            // transposed store C[n*ldc + m]: lanes (consecutive m) coalesce
+            float* dst = g.C + (long)(n0 + c0) * g.ldc + row;
+            if (g.accumulate) {
+#pragma unroll
+              for (int j = 0; j < 16; ++j)
+                if (n0 + c0 + j < g.N) dst[(long)j * g.ldc] += __uint_as_float(r[j]);
+            } else {
+#pragma unroll
+              for (int j = 0; j < 16; ++j)
+                if (n0 + c0 + j < g.N) dst[(long)j * g.ldc] = __uint_as_float(r[j]);
+            }
           } else {
             float* dst = g.C + (long)row * g.ldc + n0 + c0;
             if (g.accumulate) {
@@ -267,17 +280,36 @@ k_gemm_tn(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant__ CU
   }
 }
 
-// fp32 -> (bf16 hi, bf16 lo) with rows of length ncol at stride ld_in -> packed ld_out
+// fp32 -> (bf16 hi, bf16 lo): nrow rows of ncol values (row stride ld_in) into
+// packed rows of stride ld_out; 4 values per thread when the rows allow it
 __global__ void k_split_bf16(const float* __restrict__ x, long ld_in, int ncol, int nrow, __nv_bfloat16* __restrict__ hi,
                              __nv_bfloat16* __restrict__ lo, long ld_out, float scale) {
-  const long total = (long)nrow * ncol;
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
-    const long r = i / ncol, c = i - r * ncol;
-    const float v = x[r * ld_in + c] * scale;
-    const __nv_bfloat16 h = __float2bfloat16_rn(v);
-    const __nv_bfloat16 l = __float2bfloat16_rn(v - __bfloat162float(h));
-    hi[r * ld_out + c] = h;
-    lo[r * ld_out + c] = l;
+  const int r = blockIdx.y;
+  const float* xr = x + (long)r * ld_in;
+  __nv_bfloat16* hr = hi + (long)r * ld_out;
+  __nv_bfloat16* lr = lo + (long)r * ld_out;
+  const bool vec = ((ncol & 3) == 0) && ((ld_in & 3) == 0) && ((ld_out & 3) == 0) &&
+                   (((uintptr_t)x & 15) == 0) && (((uintptr_t)hi & 7) == 0) && (((uintptr_t)lo & 7) == 0);
+  if (vec) {
+    for (int c = (blockIdx.x * blockDim.x + threadIdx.x) * 4; c < ncol; c += gridDim.x * blockDim.x * 4) {
+      const float4 v = *reinterpret_cast<const float4*>(xr + c);
+      const float a[4] = {v.x * scale, v.y * scale, v.z * scale, v.w * scale};
+      __nv_bfloat16 h[4], l[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        h[j] = __float2bfloat16_rn(a[j]);
+        l[j] = __float2bfloat16_rn(a[j] - __bfloat162float(h[j]));
+      }
+      *reinterpret_cast<uint2*>(hr + c) = *reinterpret_cast<const uint2*>(h);
+      *reinterpret_cast<uint2*>(lr + c) = *reinterpret_cast<const uint2*>(l);
+    }
+  } else {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncol; c += gridDim.x * blockDim.x) {
+      const float v = xr[c] * scale;
+      const __nv_bfloat16 h = __float2bfloat16_rn(v);
+      hr[c] = h;
+      lr[c] = __float2bfloat16_rn(v - __bfloat162float(h));
+    }
   }
 }
 
@@ -310,9 +342,9 @@ __global__ void k_splitk_reduce(const float* __restrict__ ws, int nsplit, int M,
                                 __nv_bfloat16* bhi, __nv_bfloat16* blo, long ldb) {
   const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (i >= (long)M * N) return;
-  const int m = (int)(i / N), n = (int)(i - (long)m * N);
+  const int n = (int)(i / M), m = (int)(i - (long)n * M);
   double s = 0;
-  for (int k = 0; k < nsplit; ++k) s += (double)ws[((long)k * M + m) * N + n];
+  for (int k = 0; k < nsplit; ++k) s += (double)ws[((long)k * N + n) * M + m];
   if (rs) s *= rs[m];
   if (cs) s *= cs[n];
   const long o = transpose ? (long)n * ldo + m : (long)m * ldo + n;
@@ -419,10 +451,10 @@ int gemm_error_check() {
 
 int split_bf16(const float* x, long ld_in, int ncol, int nrow, void* hi, void* lo, long ld_out, float scale,
                cudaStream_t st) {
-  const long total = (long)nrow * ncol;
-  if (total == 0) return PW_OK;
-  const int nb = (int)std::min<long>((total + 255) / 256, 148L * 16);
-  k_split_bf16<<<nb, 256, 0, st>>>(x, ld_in, ncol, nrow, (__nv_bfloat16*)hi, (__nv_bfloat16*)lo, ld_out, scale);
+  if ((long)nrow * ncol == 0) return PW_OK;
+  const int bx = std::max(1, std::min((ncol + 1023) / 1024, 64));
+  k_split_bf16<<<dim3(bx, nrow), 256, 0, st>>>(x, ld_in, ncol, nrow, (__nv_bfloat16*)hi, (__nv_bfloat16*)lo, ld_out,
+                                                scale);
   PWB_CUDA(cudaGetLastError());
   return PW_OK;
 }
@@ -462,12 +494,12 @@ int gemm_tn_reduce(const SplitOperand& A, const SplitOperand& B, int K, int nter
 }
 
 int gemm_tn_store(const SplitOperand& A, const SplitOperand& B, int K, int nterms, float* C, long ldc, int accumulate,
-                  cudaStream_t st) {
+                  cudaStream_t st, int transposed) {
   const int M = A.rows, N = B.rows;
   if (M == 0 || N == 0) return PW_OK;
   const int BN = N >= 256 ? 256 : pick_bn(N);
   GemmArgs g{};
-  g.M = M; g.N = N; g.K = K; g.kchunk = ((K + GK - 1) / GK) * GK; g.nterms = nterms; g.epi = 1;
+  g.M = M; g.N = N; g.K = K; g.kchunk = ((K + GK - 1) / GK) * GK; g.nterms = nterms; g.epi = transposed ? 2 : 1;
   g.C = C; g.ldc = ldc; g.accumulate = accumulate;
   return launch(A, B, g, BN, 1, st);
 }

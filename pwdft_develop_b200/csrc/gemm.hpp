@@ -34,9 +34,10 @@ int split_bf16_t(const float* x, long ld_in, int ncol, int nrow, void* hi, void*
 // C[m][n] = sum_k A[m][k] B[n][k] with split-K and a deterministic reduction
 int gemm_tn_reduce(const SplitOperand& A, const SplitOperand& B, int K, int nterms, DevBuf& ws, const ReduceOut& out,
                    cudaStream_t st);
-// C[m*ldc + n] (+)= sum_k A[m][k] B[n][k]  (K small, N large)
+// C[m*ldc + n] (+)= sum_k A[m][k] B[n][k]  (K small); with transposed = 1
+// the tile is written as C[n*ldc + m] (coalesced when M is the long dimension)
 int gemm_tn_store(const SplitOperand& A, const SplitOperand& B, int K, int nterms, float* C, long ldc, int accumulate,
-                  cudaStream_t st);
+                  cudaStream_t st, int transposed = 0);
 // PW_ETIMEOUT (and clears the flag) if a GEMM pipeline wait gave up
 int gemm_error_check();
 

@@ -807,11 +807,11 @@ struct Plan {
     ro.ldb = npp;
     { Launch L_(c, st, KK_GRAM);
     if ((rc = gemm_tn_reduce(A, B, nt, c->gemm_terms, c->s_ws, ro, st))) return rc; }
-    // out[b][g] += sum_l W^T[b][l] QT[g][l]
+    // out[b][g] += sum_l QT[g][l] W^T[b][l]  (tile rows = grid points: coalesced stores)
     SplitOperand W{wb, wb + (size_t)nb * npp * 2, nb, npp};
     SplitOperand QT{c->qt_bf.p, (char*)c->qt_bf.p + (size_t)nt * npp * 2, nt, npp};
     { Launch L_(c, st, KK_GRAM);
-    if ((rc = gemm_tn_store(W, QT, np, c->gemm_terms, out, ldo, 1, st))) return rc; }
+    if ((rc = gemm_tn_store(QT, W, np, c->gemm_terms, out, ldo, 1, st, 1))) return rc; }
     return PW_OK;
   }
 
