@@ -227,6 +227,70 @@ __device__ __forceinline__ void smem_fft(V* base, int count, int es, int bs, con
   smem_fft_w<N, DIR>(base, count, es, bs, tw, (int)(threadIdx.x >> 5), (int)(blockDim.x >> 5));
 }
 
+// Same transform with compile-time element stride ES and batch stride BS:
+// addresses fold to 32-bit immediates and each lane keeps its pass-1
+// twiddles in registers across the batch loop.
+template <int N, int DIR, int ES, int BS, typename V>
+__device__ __forceinline__ void smem_fft_c(V* base, int count, const V* tw, int warp, int nw) {
+  constexpr int N1 = Split<N>::n1;
+  constexpr int N2 = N / N1;
+  constexpr int F = 32 / N1;
+  constexpr int R1 = (F * N2 + 31) / 32;   // pass-1 rounds per group
+  const int lane = threadIdx.x & 31;
+  V twr[R1][N1 > 1 ? N1 - 1 : 1];
+#pragma unroll
+  for (int r = 0; r < R1; ++r) {
+    const int it = lane + 32 * r;
+    const int j2 = it % N2;
+#pragma unroll
+    for (int k1 = 1; k1 < N1; ++k1) {
+      V w = tw[j2 * k1];
+      if (DIR > 0) w.y = -w.y;
+      twr[r][k1 - 1] = w;
+    }
+  }
+  const int f2 = lane / N1, k1_2 = lane - f2 * N1;
+  for (int g = warp * F; g < count; g += nw * F) {
+#pragma unroll
+    for (int r = 0; r < R1; ++r) {
+      const int it = lane + 32 * r;
+      const int f = it / N2, j2 = it - f * N2;
+      const int b = g + f;
+      if (it < F * N2 && b < count) {
+        V* p = base + b * BS + j2 * ES;
+        V t[N1];
+#pragma unroll
+        for (int j1 = 0; j1 < N1; ++j1) t[j1] = p[N2 * j1 * ES];
+        DFT<N1, DIR, V>::run(t);
+#pragma unroll
+        for (int k1 = 1; k1 < N1; ++k1) t[k1] = cmul(t[k1], twr[r][k1 - 1]);
+#pragma unroll
+        for (int k1 = 0; k1 < N1; ++k1) p[N2 * k1 * ES] = t[k1];
+      }
+    }
+    __syncwarp();
+    const bool act = (lane < F * N1) && (g + f2 < count);
+    V u[N2];
+    V* p = base + (g + f2) * BS;
+    if (act) {
+#pragma unroll
+      for (int j2 = 0; j2 < N2; ++j2) u[j2] = p[(N2 * k1_2 + j2) * ES];
+      DFT<N2, DIR, V>::run(u);
+    }
+    __syncwarp();
+    if (act) {
+#pragma unroll
+      for (int k2 = 0; k2 < N2; ++k2) p[(k1_2 + N1 * k2) * ES] = u[k2];
+    }
+    __syncwarp();
+  }
+}
+
+template <int N, int DIR, int ES, int BS, typename V>
+__device__ __forceinline__ void smem_fft_cb(V* base, int count, const V* tw) {
+  smem_fft_c<N, DIR, ES, BS>(base, count, tw, (int)(threadIdx.x >> 5), (int)(blockDim.x >> 5));
+}
+
 // Number of transforms one warp processes together for length N.
 template <int N> struct FftGroup {
   static constexpr int f = 32 / Split<N>::n1;

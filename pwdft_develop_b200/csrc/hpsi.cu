@@ -71,9 +71,9 @@ k_cxy_fwd(const T* __restrict__ psi, int ld, int nband, int band0, VT<T>* __rest
     pl[y * P0 + x] = mkc<V>(pa[i], pb ? pb[i] : (T)0);
   }
   __syncthreads();
-  smem_fft<N0, -1>(pl, N1, 1, P0, twx);
+  smem_fft_cb<N0, -1, 1, P0>(pl, N1, twx);
   __syncthreads();
-  smem_fft<N1, -1>(pl, N0, P0, 1, twy);
+  smem_fft_cb<N1, -1, P0, 1>(pl, N0, twy);
   __syncthreads();
   const int N2 = gridDim.x;
   V* Ap = A + ((long)p * N2 + z) * ntot_plane;
@@ -142,7 +142,7 @@ k_zpad(const VT<T>* __restrict__ A, VT<T>* __restrict__ K, VT<T>* __restrict__ B
   const ColMap m = colmap(ky, kx0, tw, n0, n1);
   for (int i = threadIdx.x; i < NZF * PO; i += blockDim.x) out[i] = mkc<V>(0, 0);
   __syncthreads();
-  smem_fft<NZ, -1>(in, tw, PI, 1, twz);
+  smem_fft_cb<NZ, -1, PI, 1>(in, tw, twz);
   __syncthreads();
   V* Kp = K + (long)p * NZ * nplane;
   for (int i = threadIdx.x; i < NZ * TX; i += blockDim.x) {
@@ -174,7 +174,7 @@ k_zpad(const VT<T>* __restrict__ A, VT<T>* __restrict__ K, VT<T>* __restrict__ B
     }
   }
   __syncthreads();
-  smem_fft<NZF, +1>(out, m.ncols, PO, 1, twzf);
+  smem_fft_cb<NZF, +1, PO, 1>(out, m.ncols, twzf);
   __syncthreads();
   const int nsx = n0 + 1, nsy = n1 + 1;
   V* Bp = B + (long)p * NZF * nsy * nsx;
@@ -381,7 +381,7 @@ k_floc(VT<T>* __restrict__ BC, const T* __restrict__ vtot, const T* __restrict__
       S[slot_fine(ys, n1, NYF) * PS + xs] = Bp[i];
     }
     __syncthreads();
-    smem_fft<NYF, +1>(S, nsx, PS, 1, twy);
+    smem_fft_cb<NYF, +1, PS, 1>(S, nsx, twy);
   }
   __syncthreads();
   for (int r0 = warp * F; r0 < NYF; r0 += nw * F) {
@@ -394,7 +394,7 @@ k_floc(VT<T>* __restrict__ BC, const T* __restrict__ vtot, const T* __restrict__
         Rw[f * PR + slot_fine(xs, n0, NXF)] = S[(r0 + f) * PS + xs];
       }
       __syncwarp();
-      smem_fft_w<NXF, +1>(Rw, nr, 1, PR, twx, 0, 1);
+      smem_fft_c<NXF, +1, 1, PR>(Rw, nr, twx, 0, 1);
       const T* vp = vtot + ((long)zf * NYF + r0) * NXF;
       for (int i = lane; i < nr * NXF; i += 32) {
         const int f = i / NXF, x = i - f * NXF;
@@ -409,7 +409,7 @@ k_floc(VT<T>* __restrict__ BC, const T* __restrict__ vtot, const T* __restrict__
       }
     }
     __syncwarp();
-    smem_fft_w<NXF, -1>(Rw, nr, 1, PR, twx, 0, 1);
+    smem_fft_c<NXF, -1, 1, PR>(Rw, nr, twx, 0, 1);
     for (int i = lane; i < nr * nsx; i += 32) {
       const int f = i / nsx, xs = i - f * nsx;
       S[(r0 + f) * PS + xs] = Rw[f * PR + slot_fine(xs, n0, NXF)];
@@ -417,7 +417,7 @@ k_floc(VT<T>* __restrict__ BC, const T* __restrict__ vtot, const T* __restrict__
     __syncwarp();
   }
   __syncthreads();
-  smem_fft<NYF, -1>(S, nsx, PS, 1, twy);
+  smem_fft_cb<NYF, -1, PS, 1>(S, nsx, twy);
   __syncthreads();
   for (int i = threadIdx.x; i < nsy * nsx; i += blockDim.x) {
     const int ys = i / nsx, xs = i - ys * nsx;
@@ -494,7 +494,7 @@ k_zfold(const VT<T>* __restrict__ C, const VT<T>* __restrict__ K, VT<T>* __restr
     in[zf * PI + c] = valid ? Cp[((long)zf * nsy + ky_s) * nsx + kx_s] : mkc<V>(0, 0);
   }
   __syncthreads();
-  smem_fft<NZF, -1>(in, m.ncols, PI, 1, twzf);
+  smem_fft_cb<NZF, -1, PI, 1>(in, m.ncols, twzf);
   __syncthreads();
   const long nplane = (long)n0 * n1;
   const V* Kp = K + (long)p * NZ * nplane;
@@ -516,7 +516,7 @@ k_zfold(const VT<T>* __restrict__ C, const VT<T>* __restrict__ K, VT<T>* __restr
     acc[kz * PA + c] = v;
   }
   __syncthreads();
-  smem_fft<NZ, +1>(acc, tw, PA, 1, twz);
+  smem_fft_cb<NZ, +1, PA, 1>(acc, tw, twz);
   __syncthreads();
   V* Dp = D + (long)p * NZ * nplane;
   for (int i = threadIdx.x; i < NZ * TX; i += blockDim.x) {
@@ -544,14 +544,14 @@ k_zteter(VT<T>* __restrict__ A, const T* __restrict__ teter, int n0, int n1, T i
     in[z * PI + c] = (c < tw) ? Ap[z * nplane + (long)ky * n0 + kx0 + c] : mkc<V>(0, 0);
   }
   __syncthreads();
-  smem_fft<NZ, -1>(in, tw, PI, 1, twz);
+  smem_fft_cb<NZ, -1, PI, 1>(in, tw, twz);
   __syncthreads();
   for (int i = threadIdx.x; i < NZ * TX; i += blockDim.x) {
     const int kz = i / TX, c = i - kz * TX;
     if (c < tw) in[kz * PI + c] = cscale(in[kz * PI + c], teter[kz * nplane + (long)ky * n0 + kx0 + c] * inv_nc);
   }
   __syncthreads();
-  smem_fft<NZ, +1>(in, tw, PI, 1, twz);
+  smem_fft_cb<NZ, +1, PI, 1>(in, tw, twz);
   __syncthreads();
   for (int i = threadIdx.x; i < NZ * TX; i += blockDim.x) {
     const int z = i / TX, c = i - z * TX;
@@ -583,9 +583,9 @@ k_cxy_inv(const VT<T>* __restrict__ D, T* __restrict__ out, int ldo, int nband, 
     pl[y * P0 + x] = Dp[i];
   }
   __syncthreads();
-  smem_fft<N1, +1>(pl, N0, P0, 1, twy);
+  smem_fft_cb<N1, +1, P0, 1>(pl, N0, twy);
   __syncthreads();
-  smem_fft<N0, +1>(pl, N1, 1, P0, twx);
+  smem_fft_cb<N0, +1, 1, P0>(pl, N1, twx);
   __syncthreads();
   const int ba = band0 + 2 * p, bb = ba + 1;
   T* oa = out + (long)ba * ldo + z * ntot_plane;
