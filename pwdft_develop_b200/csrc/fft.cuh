@@ -228,8 +228,7 @@ __device__ __forceinline__ void smem_fft(V* base, int count, int es, int bs, con
 }
 
 // Same transform with compile-time element stride ES and batch stride BS:
-// addresses fold to 32-bit immediates and each lane keeps its pass-1
-// twiddles in registers across the batch loop.
+// addresses fold to 32-bit immediates.
 template <int N, int DIR, int ES, int BS, typename V>
 __device__ __forceinline__ void smem_fft_c(V* base, int count, const V* tw, int warp, int nw) {
   constexpr int N1 = Split<N>::n1;
@@ -237,18 +236,6 @@ __device__ __forceinline__ void smem_fft_c(V* base, int count, const V* tw, int 
   constexpr int F = 32 / N1;
   constexpr int R1 = (F * N2 + 31) / 32;   // pass-1 rounds per group
   const int lane = threadIdx.x & 31;
-  V twr[R1][N1 > 1 ? N1 - 1 : 1];
-#pragma unroll
-  for (int r = 0; r < R1; ++r) {
-    const int it = lane + 32 * r;
-    const int j2 = it % N2;
-#pragma unroll
-    for (int k1 = 1; k1 < N1; ++k1) {
-      V w = tw[j2 * k1];
-      if (DIR > 0) w.y = -w.y;
-      twr[r][k1 - 1] = w;
-    }
-  }
   const int f2 = lane / N1, k1_2 = lane - f2 * N1;
   for (int g = warp * F; g < count; g += nw * F) {
 #pragma unroll
@@ -263,7 +250,11 @@ __device__ __forceinline__ void smem_fft_c(V* base, int count, const V* tw, int 
         for (int j1 = 0; j1 < N1; ++j1) t[j1] = p[N2 * j1 * ES];
         DFT<N1, DIR, V>::run(t);
 #pragma unroll
-        for (int k1 = 1; k1 < N1; ++k1) t[k1] = cmul(t[k1], twr[r][k1 - 1]);
+        for (int k1 = 1; k1 < N1; ++k1) {
+          V w = tw[j2 * k1];
+          if (DIR > 0) w.y = -w.y;
+          t[k1] = cmul(t[k1], w);
+        }
 #pragma unroll
         for (int k1 = 0; k1 < N1; ++k1) p[N2 * k1 * ES] = t[k1];
       }
