@@ -162,6 +162,67 @@ PW_API int pw_profile_read(pw_ctx* ctx, int kind, double* total_ms, long* count)
 PW_API int pw_gram(pw_ctx* ctx, const void* X, int ldx, int nx, const void* Y, int ldy, int ny, double* G, int ldg,
                    void* stream);
 
+/* ---------------------------------------------------------------------------
+ * Block eigensolvers and SCF
+ * ------------------------------------------------------------------------- */
+enum { PW_SOLVER_LOBPCG = 0, PW_SOLVER_CHEBFSI = 1 };
+
+/* In-place Cholesky-QR of nb device columns X (ntot x nb): X <- X U^{-1},
+ * X^T X = U^T U.  Replaces EigenSolver::Orthogonalize
+ * (src/EigenSolver/eigensolver.cpp:301-384). */
+PW_API int pw_cholqr(pw_ctx* ctx, void* X, int nb);
+
+/* Lowest nb eigenpairs of H (current potential and projectors) starting from
+ * the device block X (overwritten by the Ritz vectors).  solver:
+ * PW_SOLVER_LOBPCG restates EigenSolver::LOBPCGSolveReal
+ * (src/EigenSolver/lobpcg.cpp:577-1031: maxit = Eig_MaxIter, tol = residual
+ * tolerance); PW_SOLVER_CHEBFSI runs Chebyshev-filtered subspace iteration of
+ * the given degree (the reference's CheFSI parameters, src/esdf.cpp:2715-2719)
+ * for up to maxit cycles.  eig, resnorm: host arrays of nb (may be NULL). */
+PW_API int pw_eigsolve(pw_ctx* ctx, int solver, void* X, int nb, int maxit, double tol, int degree, double* eig,
+                       double* resnorm, int* iters);
+
+/* Electron density on the fine grid from nband device wavefunctions and host
+ * occupation rates (numSpin = 2), renormalised to 2*nocc_total electrons:
+ * KohnSham::CalculateDensity (src/SCF/hamiltonian.cpp:2455-2627).  rho_dev:
+ * device, N_fine doubles. */
+PW_API int pw_density(pw_ctx* ctx, const void* psi, int ld, int nband, const double* occ_host, int nocc_total,
+                      double* rho_dev);
+
+typedef struct pw_scf_params {
+  int nocc;                 /* occupied states (numOccupiedState) */
+  int nextra;               /* Extra_States */
+  int solver;               /* PW_SOLVER_LOBPCG or PW_SOLVER_CHEBFSI */
+  int cheby_degree;         /* ChebFSI filter degree */
+  int cheby_first_cycles;   /* filter cycles in the first SCF iteration */
+  int eig_max_iter;         /* Eig_MaxIter (LOBPCG) */
+  int max_iter;             /* SCF_Outer_MaxIter */
+  int mix_dim;              /* Mixing_MaxDim */
+  int mixed;                /* 1: FP32 H*psi / split-BF16 Gram eigensolver, FP64 refinement */
+  int verbose;
+  double ecut;              /* Ecut_Wavefunction (Hartree cut-off 4*Ecut) */
+  double temperature;       /* Kelvin, Fermi-Dirac */
+  double eig_tol;           /* Eig_Tolerance */
+  double mix_step;          /* Mixing_StepLength */
+  double tol_efree;         /* converged when |E_free - E_Harris| / N_atom < tol_efree */
+  double refine_threshold;  /* mixed mode: switch the eigensolver to FP64 below this */
+  unsigned long long seed;  /* random start */
+} pw_scf_params;
+
+typedef struct pw_scf_result {
+  double etot, efree, eharris, exc, ehart, eself, fermi, time_s;
+  int iterations, converged, refine_iter;
+  long hpsi_bands;          /* single-band H*psi applications performed */
+} pw_scf_result;
+
+/* Self-consistent field iteration for the atoms of an FP64 context
+ * (pw_set_atoms): SCF::Iterate / InnerSolve with potential Anderson mixing
+ * (src/SCF/scf.cpp:372-591, 1261-1589, 2299-2365), density, Hartree and LDA
+ * Teter93 XC (src/SCF/hamiltonian.cpp:1242-1308, 1990-2069, 2455-2627) and the
+ * energies of scf.cpp:1834-2140, all on the device.  eig_out: host, nocc+nextra
+ * doubles; rho_out: host, N_fine doubles (either may be NULL). */
+PW_API int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* eig_out, double* rho_out);
+
 /* Maximum number of bands processed per internal batch (sets scratch size).
  * Default 64. Scratch grows to hold ceil(nband_batch/2) band pairs. */
 PW_API int pw_set_band_batch(pw_ctx* ctx, int nband_batch);

@@ -34,6 +34,25 @@ lib = _load()
 _vp, _i, _l, _d = C.c_void_p, C.c_int, C.c_long, C.c_double
 _ip, _dp = C.POINTER(C.c_int), C.POINTER(C.c_double)
 
+PW_SOLVER_LOBPCG, PW_SOLVER_CHEBFSI = 0, 1
+
+
+class ScfParams(C.Structure):
+    _fields_ = [("nocc", C.c_int), ("nextra", C.c_int), ("solver", C.c_int), ("cheby_degree", C.c_int),
+                ("cheby_first_cycles", C.c_int), ("eig_max_iter", C.c_int), ("max_iter", C.c_int),
+                ("mix_dim", C.c_int), ("mixed", C.c_int), ("verbose", C.c_int),
+                ("ecut", C.c_double), ("temperature", C.c_double), ("eig_tol", C.c_double),
+                ("mix_step", C.c_double), ("tol_efree", C.c_double), ("refine_threshold", C.c_double),
+                ("seed", C.c_ulonglong)]
+
+
+class ScfResult(C.Structure):
+    _fields_ = [("etot", C.c_double), ("efree", C.c_double), ("eharris", C.c_double), ("exc", C.c_double),
+                ("ehart", C.c_double), ("eself", C.c_double), ("fermi", C.c_double), ("time_s", C.c_double),
+                ("iterations", C.c_int), ("converged", C.c_int), ("refine_iter", C.c_int),
+                ("hpsi_bands", C.c_long)]
+
+
 # name -> (restype, argtypes); every name here is declared in include/pwdft_b200.h
 SIGNATURES: dict[str, tuple] = {
     "pw_last_error": (C.c_char_p, []),
@@ -51,6 +70,10 @@ SIGNATURES: dict[str, tuple] = {
     "pw_set_gemm_mode": (_i, [_vp, _i, _i]),
     "pw_set_check_errors": (_i, [_vp, _i]),
     "pw_gram": (_i, [_vp, _vp, _i, _i, _vp, _i, _i, _vp, _i, _vp]),
+    "pw_cholqr": (_i, [_vp, _vp, _i]),
+    "pw_eigsolve": (_i, [_vp, _i, _vp, _i, _i, _d, _i, _dp, _dp, _ip]),
+    "pw_density": (_i, [_vp, _vp, _i, _i, _dp, _i, _vp]),
+    "pw_scf_run": (_i, [_vp, C.POINTER(ScfParams), C.POINTER(ScfResult), _dp, _dp]),
     "pw_hgh_species": (_i, [_i, _dp, _dp, _dp, _dp, _ip]),
     "pw_set_atoms": (_i, [_vp, _i, _ip, _dp]),
     "pw_get_pseudocharge": (_i, [_vp, _dp]),

@@ -240,3 +240,60 @@ Context.profile_read = _ctx_profile_read
 KERNEL_KINDS = {0: "coarse_xy_fwd", 1: "z_pad", 2: "fine_plane_gather", 3: "nl_reduce", 4: "fine_plane_apply",
                 5: "z_fold", 6: "coarse_xy_inv", 7: "z_teter", 8: "gram", 9: "density", 10: "other",
                 11: "library_gemm"}
+
+
+# ---------------------------------------------------------------------------
+# eigensolvers and SCF
+# ---------------------------------------------------------------------------
+def _ctx_cholqr(self, X):
+    check(lib.pw_cholqr(self._h, _ptr(X), X.shape[0]))
+    return X
+
+
+def _ctx_eigsolve(self, X, solver: str = "lobpcg", maxit: int = 10, tol: float = 1e-8, degree: int = 10):
+    """EigenSolver::LOBPCGSolveReal / ChebFSI on the device block X (nb, ntot),
+    overwritten by the Ritz vectors.  Returns (eig, resnorm, iterations)."""
+    nb = X.shape[0]
+    eig = np.zeros(nb)
+    res = np.zeros(nb)
+    it = C.c_int()
+    sid = _lib.PW_SOLVER_LOBPCG if solver == "lobpcg" else _lib.PW_SOLVER_CHEBFSI
+    check(lib.pw_eigsolve(self._h, sid, _ptr(X), nb, int(maxit), float(tol), int(degree),
+                          eig.ctypes.data_as(_lib._dp), res.ctypes.data_as(_lib._dp), C.byref(it)))
+    return eig, res, it.value
+
+
+def _ctx_density(self, psi, occ, nocc_total: int):
+    import torch
+    rho = torch.empty(self.ntotFine, dtype=torch.float64, device=psi.device)
+    occ = np.ascontiguousarray(occ, np.float64)
+    check(lib.pw_density(self._h, _ptr(psi), self.ntot, psi.shape[0], occ.ctypes.data_as(_lib._dp),
+                         int(nocc_total), _ptr(rho)))
+    return rho
+
+
+def _ctx_scf(self, nocc: int, nextra: int, ecut: float, solver: str = "chebfsi", mixed: bool = False,
+             temperature: float = 300.0, cheby_degree: int = 10, cheby_first_cycles: int = 5,
+             eig_max_iter: int = 3, eig_tol: float = 1e-10, max_iter: int = 100, mix_dim: int = 8,
+             mix_step: float = 0.7, tol_efree: float = 1e-6, refine_threshold: float = 1e-4, seed: int = 1,
+             verbose: bool = False):
+    """SCF::Iterate on the device (FP64 context; mixed=True runs the eigensolver in
+    an FP32 twin and refines in FP64).  Returns (result dict, eigenvalues, rho)."""
+    p = _lib.ScfParams(nocc=nocc, nextra=nextra,
+                       solver=_lib.PW_SOLVER_LOBPCG if solver == "lobpcg" else _lib.PW_SOLVER_CHEBFSI,
+                       cheby_degree=cheby_degree, cheby_first_cycles=cheby_first_cycles, eig_max_iter=eig_max_iter,
+                       max_iter=max_iter, mix_dim=mix_dim, mixed=int(mixed), verbose=int(verbose), ecut=ecut,
+                       temperature=temperature, eig_tol=eig_tol, mix_step=mix_step, tol_efree=tol_efree,
+                       refine_threshold=refine_threshold, seed=seed)
+    r = _lib.ScfResult()
+    eig = np.zeros(nocc + nextra)
+    rho = np.zeros(self.ntotFine)
+    check(lib.pw_scf_run(self._h, C.byref(p), C.byref(r), eig.ctypes.data_as(_lib._dp), rho.ctypes.data_as(_lib._dp)))
+    res = {k: getattr(r, k) for k, _ in r._fields_}
+    return res, eig, rho
+
+
+Context.cholqr = _ctx_cholqr
+Context.eigsolve = _ctx_eigsolve
+Context.density = _ctx_density
+Context.scf = _ctx_scf

@@ -1,0 +1,57 @@
+// Device block operations used by the eigensolvers and the SCF driver.
+#pragma once
+#include <cublas_v2.h>
+#include <cusolverDn.h>
+
+#include "common.hpp"
+
+namespace pwb {
+
+// Y = a*X + b*Y for nb columns of length n (column stride ldx / ldy)
+template <typename T> int axpby(int n, int nb, double a, const T* X, long ldx, double b, T* Y, long ldy, cudaStream_t st);
+// Z = a*X + b*Y + c*W (three blocks, element-wise), used by the Chebyshev recurrence
+template <typename T>
+int axpbypcz(int n, int nb, double a, const T* X, double b, const T* Y, double c, const T* W, T* Z, long ld,
+             cudaStream_t st);
+// out[j] = sum_i X[j*ld + i]^2 (double)
+template <typename T> int colnorm2(int n, int nb, const T* X, long ld, double* out, cudaStream_t st);
+// X[:, j] *= s[j]
+template <typename T> int colscale(int n, int nb, T* X, long ld, const double* s, cudaStream_t st);
+// copy with precision change
+int copy_d2f(long n, const double* x, float* y, cudaStream_t st);
+int copy_f2d(long n, const float* x, double* y, cudaStream_t st);
+int copy_d2f_2d(int n, int nb, const double* x, long ldx, float* y, long ldy, cudaStream_t st);
+int copy_f2d_2d(int n, int nb, const float* x, long ldx, double* y, long ldy, cudaStream_t st);
+
+// Out (n x m, ldo) = sum over blocks of X_b (n x k_b, ld) * C_b (k_b x m, FP64 column-major, ldc),
+// beta = 0 or 1 for Out.  The context precision decides FP64 or FP32 storage of X / Out.
+struct RotBlock {
+  const void* X;
+  long ldx;
+  int k;
+  const double* C;   // device, FP64
+  int ldc;
+};
+int rotate(pw_ctx* c, int n, int m, const RotBlock* blocks, int nblk, void* out, long ldo, double beta, cudaStream_t st);
+
+// Small dense FP64 algebra on the device (cuSOLVER / cuBLAS), n <= a few thousand.
+struct Dense {
+  cusolverDnHandle_t sol = nullptr;
+  cublasHandle_t blas = nullptr;
+  DevBuf work, info, tmp1, tmp2, tmp3, wvec;
+  int init(cublasHandle_t b);
+  void release();
+  // eigen-decomposition in place: A (n x n, lda) -> eigenvectors, w (device) ascending
+  int syevd(int n, double* A, int lda, double* w, cudaStream_t st);
+  // upper Cholesky A = U^T U in place; returns PW_ENUMERIC if not positive definite
+  int potrf_upper(int n, double* A, int lda, cudaStream_t st);
+};
+
+// Symmetric generalized eigenproblem of EigenSolver::SolveGenEig (serial path,
+// src/EigenSolver/eigensolver.cpp:224-297): symmetrise from the upper triangle,
+// eig(B), keep sigma/sigma_max > 1e-8, eig of the reduced A, C = U sigma^-1/2 Z.
+// On exit A holds C (numCol x numKeep), eig (host) the first `width` values.
+int solve_gen_eig(Dense& d, int lda, int numCol, int width, double* A, double* B, double* eig_host, int* numKeep,
+                  cudaStream_t st);
+
+}  // namespace pwb

@@ -98,7 +98,7 @@ struct pw_ctx {
   int gemm_terms = 3;            // split products per k-step (3 or 4)
   bool check_errors = false;     // read the device error flag after each call (synchronises)
   int nproj_pad = 0;
-  pwb::DevBuf q_bf, qt_bf, s_psi_bf, s_w_bf, s_ws, s_gx_bf, s_gy_bf;
+  pwb::DevBuf q_bf, qt_bf, s_psi_bf, s_w_bf, s_ws, s_gx_bf, s_gy_bf, s_rot;
   // host copies kept for setup-time work
   std::vector<double> h_vtot;
   // atoms set through pw_set_atoms (HGH species built in this library)

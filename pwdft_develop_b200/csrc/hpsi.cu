@@ -150,7 +150,7 @@ k_zpad(const VT<T>* __restrict__ A, VT<T>* __restrict__ K, VT<T>* __restrict__ B
     if (c >= tw) continue;
     const long g = kz * nplane + (long)ky * n0 + kx0 + c;
     const V v = cscale(in[kz * PI + c], inv_nc);
-    Kp[g] = cscale(v, ekin[g]);
+    if (K) Kp[g] = cscale(v, ekin[g]);
     const bool nyz = (kz == NZ / 2);
     const int fz = (sgn_idx(kz, NZ) + NZF) % NZF;
     const bool split = m.nyy || (c == m.nyx_i);
@@ -422,6 +422,95 @@ k_floc(VT<T>* __restrict__ BC, const T* __restrict__ vtot, const T* __restrict__
   for (int i = threadIdx.x; i < nsy * nsx; i += blockDim.x) {
     const int ys = i / nsx, xs = i - ys * nsx;
     Bp[i] = cscale(S[slot_fine(ys, n1, NYF) * PS + xs], inv_nf);
+  }
+}
+
+
+// ---------------------------------------------------------------------------
+// density: rho(r) += w_a |Re psi_f|^2 + w_b |Im psi_f|^2 over the pairs of a
+// chunk (CalculateDensity, src/SCF/hamiltonian.cpp:2511-2547).  One CTA owns
+// one fine plane for `ppc` pairs and keeps its partial sums in registers.
+// ---------------------------------------------------------------------------
+template <typename T, int NXF, int NYF>
+__global__ void __launch_bounds__(FLOC_THREADS)
+k_fdens(const VT<T>* __restrict__ BC, int npair, int ppc, const double* __restrict__ w, double* __restrict__ rho,
+        const VT<T>* twx_g, const VT<T>* twy_g) {
+  using V = VT<T>;
+  constexpr int n0 = NXF / 2, n1 = NYF / 2;
+  constexpr int nsx = n0 + 1, nsy = n1 + 1;
+  constexpr int PS = nsx;
+  constexpr int PR = NXF + 1;
+  constexpr int F = FftGroup<NXF>::f;
+  constexpr int NW = FLOC_THREADS / 32;
+  constexpr int RG = (NYF + NW * F - 1) / (NW * F);
+  constexpr int EPL = (F * NXF + 31) / 32;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  V* S = reinterpret_cast<V*>(smraw);
+  V* twx = S + NYF * PS;
+  V* twy = twx + NXF;
+  V* Rall = twy + NYF;
+  load_tw(twx, twx_g, NXF);
+  load_tw(twy, twy_g, NYF);
+  const int zf = blockIdx.x;
+  const int NZF = gridDim.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  V* Rw = Rall + warp * F * PR;
+  double acc[RG][EPL];
+#pragma unroll
+  for (int a = 0; a < RG; ++a)
+#pragma unroll
+    for (int k = 0; k < EPL; ++k) acc[a][k] = 0.0;
+  const int p0 = blockIdx.y * ppc, p1 = min(npair, p0 + ppc);
+  for (int p = p0; p < p1; ++p) {
+    const V* Bp = BC + ((long)p * NZF + zf) * nsy * nsx;
+    const double wa = w[2 * p], wb = w[2 * p + 1];
+    __syncthreads();
+    for (int i = threadIdx.x; i < NYF * PS; i += blockDim.x) S[i] = mkc<V>(0, 0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < nsy * nsx; i += blockDim.x) {
+      const int ys = i / nsx, xs = i - ys * nsx;
+      S[slot_fine(ys, n1, NYF) * PS + xs] = Bp[i];
+    }
+    __syncthreads();
+    smem_fft_cb<NYF, +1, PS, 1>(S, nsx, twy);
+    __syncthreads();
+#pragma unroll
+    for (int rg = 0; rg < RG; ++rg) {
+      const int r0 = (warp + rg * NW) * F;
+      if (r0 < NYF) {
+        const int nr = min(F, NYF - r0);
+        for (int i = lane; i < F * PR; i += 32) Rw[i] = mkc<V>(0, 0);
+        __syncwarp();
+        for (int i = lane; i < nr * nsx; i += 32) {
+          const int f = i / nsx, xs = i - f * nsx;
+          Rw[f * PR + slot_fine(xs, n0, NXF)] = S[(r0 + f) * PS + xs];
+        }
+        __syncwarp();
+        smem_fft_c<NXF, +1, 1, PR>(Rw, nr, twx, 0, 1);
+#pragma unroll
+        for (int k = 0; k < EPL; ++k) {
+          const int i = lane + 32 * k;
+          if (i < nr * NXF) {
+            const int f = i / NXF, x = i - f * NXF;
+            const V v = Rw[f * PR + x];
+            acc[rg][k] += wa * (double)v.x * (double)v.x + wb * (double)v.y * (double)v.y;
+          }
+        }
+        __syncwarp();
+      }
+    }
+  }
+#pragma unroll
+  for (int rg = 0; rg < RG; ++rg) {
+    const int r0 = (warp + rg * NW) * F;
+    if (r0 < NYF) {
+      const int nr = min(F, NYF - r0);
+#pragma unroll
+      for (int k = 0; k < EPL; ++k) {
+        const int i = lane + 32 * k;
+        if (i < nr * NXF) atomicAdd(&rho[((long)zf * NYF + r0) * NXF + i], acc[rg][k]);
+      }
+    }
   }
 }
 
@@ -786,6 +875,33 @@ struct Plan {
     return PW_OK;
   }
 
+  // rho += sum over the batch's bands of w_b |psi_b,fine|^2 (unnormalised)
+  static int density_batch(pw_ctx* c, const T* psi, int ld, int nband, int band0, int npair, const double* w,
+                           double* rho, cudaStream_t st) {
+    int rc = set_attrs();
+    if (rc) return rc;
+    static bool attr = false;
+    if (!attr) {
+      PWB_CUDA(cudaFuncSetAttribute(k_fdens<T, NF0, NF1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_floc()));
+      attr = true;
+    }
+    V* AD = reinterpret_cast<V*>(c->s_ad.p);
+    V* BC = reinterpret_cast<V*>(c->s_bc.p);
+    const T inv_nc = (T)(1.0 / (double)c->ntot);
+    const int ntx = (N0 + TX - 1) / TX;
+    { Launch L_(c, st, KK_DENSITY);
+    k_cxy_fwd<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(psi, ld, nband, band0, AD, tw(c, 0), tw(c, 1)); }
+    { Launch L_(c, st, KK_DENSITY);
+    k_zpad<T, N2, NF2><<<dim3(N1, ntx, npair), PENCIL_THREADS, sm_zpad(), st>>>(
+        AD, nullptr, BC, reinterpret_cast<const T*>(c->ekin.p), N0, N1, inv_nc, tw(c, 2), tw(c, 5)); }
+    const int ppc = std::max(1, std::min(8, npair));
+    { Launch L_(c, st, KK_DENSITY);
+    k_fdens<T, NF0, NF1><<<dim3(NF2, (npair + ppc - 1) / ppc), FLOC_THREADS, sm_floc(), st>>>(
+        BC, npair, ppc, w + 2 * (band0 / 2), rho, tw(c, 3), tw(c, 4)); }
+    PWB_CUDA(cudaGetLastError());
+    return PW_OK;
+  }
+
   // FP32 context: split-BF16 tcgen05 GEMMs
   static int dense_nl_tc(pw_ctx* c, const float* psi, int ld, float* out, int ldo, int nb, cudaStream_t st) {
     const int np = c->nproj, nt = (int)c->ntot, npp = c->nproj_pad;
@@ -882,6 +998,12 @@ static int teter_thunk(pw_ctx* c, const void* psi, int ld, void* out, int ldo, i
 }
 template <typename T, int N0, int N1, int N2> static int cr_thunk() { return Plan<T, N0, N1, N2>::chunk_rows(); }
 using BuildQFn = int (*)(pw_ctx*, const int*, const double*, const long*, const long*, const int*, int, cudaStream_t);
+using DensFn = int (*)(pw_ctx*, const void*, int, int, int, int, const double*, double*, cudaStream_t);
+template <typename T, int N0, int N1, int N2>
+static int dens_thunk(pw_ctx* c, const void* psi, int ld, int nband, int band0, int npair, const double* w, double* rho,
+                      cudaStream_t st) {
+  return Plan<T, N0, N1, N2>::density_batch(c, (const T*)psi, ld, nband, band0, npair, w, rho, st);
+}
 template <typename T, int N0, int N1, int N2>
 static int buildq_thunk(pw_ctx* c, const int* a, const double* b, const long* d, const long* e, const int* f, int n,
                         cudaStream_t st) {
@@ -894,13 +1016,15 @@ struct GridEntry {
   HpsiFn teter[2];
   ChunkFn cr[2];
   BuildQFn bq[2];
+  DensFn dens[2];
 };
 
 #define PWB_GRID(a, b, c)                                                                          \
   {a, b, c, {hpsi_thunk<double, a, b, c>, hpsi_thunk<float, a, b, c>},                             \
    {teter_thunk<double, a, b, c>, teter_thunk<float, a, b, c>},                                    \
    {cr_thunk<double, a, b, c>, cr_thunk<float, a, b, c>},                                          \
-   {buildq_thunk<double, a, b, c>, buildq_thunk<float, a, b, c>}},
+   {buildq_thunk<double, a, b, c>, buildq_thunk<float, a, b, c>},                                  \
+   {dens_thunk<double, a, b, c>, dens_thunk<float, a, b, c>}},
 
 static const GridEntry kGrids[] = {
 #include "grids.inc"
@@ -930,6 +1054,13 @@ int run_build_q(pw_ctx* c, const int* d_idx, const double* d_beta, const long* d
   const GridEntry* g = find_grid(c->n);
   if (!g) { set_error("grid not built into this library"); return PW_EUNSUPPORTED; }
   return g->bq[c->prec == PW_F32 ? 1 : 0](c, d_idx, d_beta, d_pio, d_pbo, d_pnp, nproj, st);
+}
+
+int run_density(pw_ctx* c, const void* psi, int ld, int nband, int band0, int npair, const double* w, double* rho,
+                cudaStream_t st) {
+  const GridEntry* g = find_grid(c->n);
+  if (!g) { set_error("grid not built into this library"); return PW_EUNSUPPORTED; }
+  return g->dens[c->prec == PW_F32 ? 1 : 0](c, psi, ld, nband, band0, npair, w, rho, st);
 }
 
 int run_teter(pw_ctx* c, const void* r, int ld, void* out, int ldo, int nband, int band0, int npair, int acc,

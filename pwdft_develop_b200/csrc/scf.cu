@@ -1,0 +1,1012 @@
+// Block eigensolvers and the Gamma-point SCF driver on the device.
+//
+//  * Cholesky-QR        EigenSolver::Orthogonalize   src/EigenSolver/eigensolver.cpp:301-384
+//  * LOBPCG             EigenSolver::LOBPCGSolveReal src/EigenSolver/lobpcg.cpp:577-1031
+//    (no locking, first iteration on (X, W), later (X, W, P), residual
+//    ||r|| / max(1, |lambda|), SolveGenEig on the 2n or 3n block, final RR)
+//  * ChebFSI            Chebyshev-filtered subspace iteration (Zhou, Saad,
+//    Tiago, Chelikowsky, J. Comput. Phys. 219, 172 (2006)); the reference only
+//    keeps its parameters (src/esdf.cpp:2715-2719) and calls (scf.cpp:1299-1334)
+//  * SCF                SCF::Iterate / InnerSolve (scf.cpp:372-591, 1261-1589):
+//    density (hamiltonian.cpp:2455-2627), Hartree (:1990-2026), LDA Teter93 XC
+//    (:1242-1308), Vtot (:2029-2069), occupations (scf.cpp:1748-1830), energies
+//    (:1834-2140), Anderson potential mixing (:2299-2365).
+//
+// FP64 everywhere except, in mixed mode, the eigensolver's H*psi, block
+// updates and Gram products, which run in an FP32 twin context (FP32 FFTs,
+// split-BF16 tensor-core Grams with FP32 accumulation).  Small dense problems
+// (Cholesky, Rayleigh-Ritz eigenproblems) are FP64 on the device.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <random>
+#include <vector>
+
+#include "blockops.hpp"
+#include "common.hpp"
+#include "fft.cuh"
+#include "gemm.hpp"
+
+namespace pwb {
+
+int run_density(pw_ctx* c, const void* psi, int ld, int nband, int band0, int npair, const double* w, double* rho,
+                cudaStream_t st);
+int gram(pw_ctx* c, const void* X, int ldx, int nx, const void* Y, int ldy, int ny, double* G, int ldg,
+         cudaStream_t st);
+int upload_real(pw_ctx* c, DevBuf& dst, const double* src, size_t n);
+
+// ---------------------------------------------------------------------------
+// FP64 3-D FFT of the fine grid along one axis, 16 pencils per CTA
+// ---------------------------------------------------------------------------
+constexpr int AX_TILE = 16;
+constexpr int AX_THREADS = 256;
+
+// axis 0 (x, contiguous): CTA = 16 consecutive rows; axis 1 (y): CTA = (z, x tile);
+// axis 2 (z): CTA = (y, x tile).  MODE 0: plain, 1: real input (load re(x) -
+// y_sub), 2: multiply by kern after the forward transform and inverse in place,
+// 3: store the real part scaled into out.
+template <int N, int DIR, int AXIS, int MODE>
+__global__ void __launch_bounds__(AX_THREADS)
+k_fft_axis(double2* __restrict__ data, int nx, int ny, int nz, const double* __restrict__ rin,
+           const double* __restrict__ rsub, const double* __restrict__ kern, double* __restrict__ rout, double scale,
+           const double2* tw_g) {
+  constexpr int P = AX_TILE + 1;
+  __shared__ double2 buf[N * P];
+  __shared__ double2 tw[N];
+  for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = tw_g[i];
+  long base;
+  long estride;
+  int cnt;
+  if (AXIS == 0) {
+    const long row0 = (long)blockIdx.x * AX_TILE;
+    const long nrow = (long)ny * nz;
+    cnt = (int)min((long)AX_TILE, nrow - row0);
+    base = row0 * nx;
+    estride = 1;
+    // rows: element e of row r at base + r*nx + e -> buf[e*P + r]
+    for (int i = threadIdx.x; i < N * AX_TILE; i += blockDim.x) {
+      const int r = i / N, e = i - r * N;
+      double2 v = make_double2(0, 0);
+      if (r < cnt) {
+        const long g = base + (long)r * nx + e;
+        if (MODE == 1) v = make_double2(rin[g] - (rsub ? rsub[g] : 0.0), 0.0);
+        else v = data[g];
+      }
+      buf[e * P + r] = v;
+    }
+  } else {
+    const int x0 = blockIdx.x * AX_TILE;
+    cnt = min(AX_TILE, nx - x0);
+    if (AXIS == 1) { base = (long)blockIdx.y * nx * ny + x0; estride = nx; }
+    else { base = (long)blockIdx.y * nx + x0; estride = (long)nx * ny; }
+    for (int i = threadIdx.x; i < N * AX_TILE; i += blockDim.x) {
+      const int e = i / AX_TILE, c = i - e * AX_TILE;
+      buf[e * P + c] = (c < cnt) ? data[base + e * estride + c] : make_double2(0, 0);
+    }
+  }
+  __syncthreads();
+  smem_fft_cb<N, DIR, P, 1>(buf, cnt, tw);
+  __syncthreads();
+  if (MODE == 2) {
+    for (int i = threadIdx.x; i < N * AX_TILE; i += blockDim.x) {
+      const int e = i / AX_TILE, c = i - e * AX_TILE;
+      if (c < cnt) buf[e * P + c] = cscale(buf[e * P + c], kern[base + e * estride + c]);
+    }
+    __syncthreads();
+    smem_fft_cb<N, -DIR, P, 1>(buf, cnt, tw);
+    __syncthreads();
+  }
+  if (AXIS == 0) {
+    for (int i = threadIdx.x; i < N * AX_TILE; i += blockDim.x) {
+      const int r = i / N, e = i - r * N;
+      if (r < cnt) {
+        const long g = base + (long)r * nx + e;
+        if (MODE == 3) rout[g] = buf[e * P + r].x * scale;
+        else data[g] = buf[e * P + r];
+      }
+    }
+  } else {
+    for (int i = threadIdx.x; i < N * AX_TILE; i += blockDim.x) {
+      const int e = i / AX_TILE, c = i - e * AX_TILE;
+      if (c < cnt) data[base + e * estride + c] = buf[e * P + c];
+    }
+  }
+}
+
+// Hartree on the fine grid: vh = (1/N) IFFT( kern * FFT(rho - rho_ps) ),
+// kern = 2 pi / gkk (0 for gkk <= 1e-16 or gkk > 4 Ecut).  Cubic grids only.
+template <int N> static int hartree_n(double2* work, const double* rho, const double* rps, const double* kern,
+                                      double* vh, const double2* tw, cudaStream_t st) {
+  const int nrowtiles = (N * N + AX_TILE - 1) / AX_TILE;
+  const int nxt = (N + AX_TILE - 1) / AX_TILE;
+  k_fft_axis<N, -1, 0, 1><<<nrowtiles, AX_THREADS, 0, st>>>(work, N, N, N, rho, rps, nullptr, nullptr, 1.0, tw);
+  k_fft_axis<N, -1, 1, 0><<<dim3(nxt, N), AX_THREADS, 0, st>>>(work, N, N, N, nullptr, nullptr, nullptr, nullptr, 1.0, tw);
+  k_fft_axis<N, -1, 2, 2><<<dim3(nxt, N), AX_THREADS, 0, st>>>(work, N, N, N, nullptr, nullptr, kern, nullptr, 1.0, tw);
+  k_fft_axis<N, +1, 1, 0><<<dim3(nxt, N), AX_THREADS, 0, st>>>(work, N, N, N, nullptr, nullptr, nullptr, nullptr, 1.0, tw);
+  k_fft_axis<N, +1, 0, 3><<<nrowtiles, AX_THREADS, 0, st>>>(work, N, N, N, nullptr, nullptr, nullptr, vh,
+                                                             1.0 / ((double)N * N * N), tw);
+  PWB_CUDA(cudaGetLastError());
+  return PW_OK;
+}
+
+static int hartree(pw_ctx* c, double2* work, const double* rho, const double* rps, const double* kern, double* vh,
+                   const double2* tw, cudaStream_t st) {
+  PWB_CHECK(c->nf[0] == c->nf[1] && c->nf[1] == c->nf[2], PW_EUNSUPPORTED, "SCF Hartree needs a cubic fine grid");
+  switch (c->nf[0]) {
+    case 24: return hartree_n<24>(work, rho, rps, kern, vh, tw, st);
+    case 32: return hartree_n<32>(work, rho, rps, kern, vh, tw, st);
+    case 48: return hartree_n<48>(work, rho, rps, kern, vh, tw, st);
+    case 96: return hartree_n<96>(work, rho, rps, kern, vh, tw, st);
+    case 144: return hartree_n<144>(work, rho, rps, kern, vh, tw, st);
+    default: set_error("SCF fine grid size not built"); return PW_EUNSUPPORTED;
+  }
+}
+
+// LDA Teter93 (Goedecker, Teter, Hutter, PRB 54, 1703 (1996)); bad points zeroed
+__global__ void k_xc_teter93(long n, const double* __restrict__ rho, double* __restrict__ eps, double* __restrict__ vxc) {
+  const double a0 = 0.4581652932831429, a1 = 2.217058676663745, a2 = 0.7405551735357053, a3 = 0.01968227878617998;
+  const double b1 = 1.0, b2 = 4.504130959426697, b3 = 1.110667363742916, b4 = 0.02359291751427506;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const double r = rho[i];
+    if (r < 1e-10) { eps[i] = 0.0; vxc[i] = 0.0; continue; }
+    const double rs = cbrt(3.0 / (4.0 * M_PI * r));
+    const double N_ = a0 + rs * (a1 + rs * (a2 + rs * a3));
+    const double D = rs * (b1 + rs * (b2 + rs * (b3 + rs * b4)));
+    const double dN = a1 + rs * (2 * a2 + rs * 3 * a3);
+    const double dD = b1 + rs * (2 * b2 + rs * (3 * b3 + rs * 4 * b4));
+    const double e = -N_ / D;
+    const double de = -(dN * D - N_ * dD) / (D * D);
+    eps[i] = e;
+    vxc[i] = e - rs / 3.0 * de;
+  }
+}
+
+// out[k] += sum_i a_k[i] * b_k[i] for K pairs
+struct DotSet {
+  const double* a[6];
+  const double* b[6];
+  int k;
+};
+__global__ void k_dots(long n, DotSet d, double* out) {
+  double s[6] = {0, 0, 0, 0, 0, 0};
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    for (int k = 0; k < d.k; ++k) s[k] += d.a[k][i] * (d.b[k] ? d.b[k][i] : 1.0);
+  __shared__ double red[6][32];
+  for (int k = 0; k < d.k; ++k) {
+    double v = s[k];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) red[k][threadIdx.x >> 5] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    for (int k = 0; k < d.k; ++k) {
+      double v = (threadIdx.x < (blockDim.x >> 5)) ? red[k][threadIdx.x] : 0.0;
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (threadIdx.x == 0) atomicAdd(&out[k], v);
+    }
+  }
+}
+
+__global__ void k_lincomb(long n, double a, const double* __restrict__ x, double b, const double* __restrict__ y,
+                          double* __restrict__ z) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    z[i] = a * x[i] + (y ? b * y[i] : 0.0);
+}
+__global__ void k_init_rho(long n, const double* __restrict__ rps, double* __restrict__ rho) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    rho[i] = rps[i] > 1e-6 ? rps[i] : 1e-6;
+}
+
+static inline int nblk(long n) { return (int)std::min<long>((n + 255) / 256, 148L * 8); }
+
+// ---------------------------------------------------------------------------
+// SCF / eigensolver state
+// ---------------------------------------------------------------------------
+struct Solver {
+  pw_ctx* c = nullptr;   // context doing the eigensolve (FP64 or FP32 twin)
+  int nb = 0;            // block width
+  long nt = 0;
+  size_t esz = 8;
+  DevBuf X, HX, W, HW, P, HP, Y, HY, Z;   // [nb][nt] blocks
+  DevBuf S, HS;                            // LOBPCG [3nb][nt] (X,W,P contiguous)
+  DevBuf G1, G2, wbuf;                     // dense FP64 work (3nb x 3nb)
+  std::vector<double> eig, res;
+  void* ptr(DevBuf& b, long col = 0) { return (char*)b.p + (size_t)col * nt * esz; }
+};
+
+static int hpsi(pw_ctx* c, const void* x, void* y, int nb, cudaStream_t st) {
+  return pw_hpsi(c, x, (int)c->ntot, y, (int)c->ntot, nb, 0, st);
+}
+
+template <typename T> static int t_axpby(Solver& s, int n, int nb, double a, const void* X, double b, void* Y) {
+  return axpby<T>(n, nb, a, (const T*)X, s.nt, b, (T*)Y, s.nt, nullptr);
+}
+static int v_axpby(Solver& s, int nb, double a, const void* X, double b, void* Y) {
+  return s.c->prec == PW_F64 ? t_axpby<double>(s, (int)s.nt, nb, a, X, b, Y) : t_axpby<float>(s, (int)s.nt, nb, a, X, b, Y);
+}
+static int v_colnorm2(Solver& s, int nb, const void* X, double* out_dev) {
+  return s.c->prec == PW_F64 ? colnorm2<double>((int)s.nt, nb, (const double*)X, s.nt, out_dev, nullptr)
+                             : colnorm2<float>((int)s.nt, nb, (const float*)X, s.nt, out_dev, nullptr);
+}
+static int v_colscale(Solver& s, int nb, void* X, const double* sc) {
+  return s.c->prec == PW_F64 ? colscale<double>((int)s.nt, nb, (double*)X, s.nt, sc, nullptr)
+                             : colscale<float>((int)s.nt, nb, (float*)X, s.nt, sc, nullptr);
+}
+
+static int alloc_block(Solver& s, DevBuf& b, int ncol) { return b.alloc((size_t)ncol * s.nt * s.esz); }
+
+// Cholesky-QR: X <- X U^{-1}, S = X^T X = U^T U (Orthogonalize, eigensolver.cpp:301-384)
+static int cholqr(Solver& s, Dense& d, void* X, int nb, void* tmp) {
+  const cudaStream_t st = nullptr;
+  int rc;
+  if ((rc = s.G1.alloc((size_t)nb * nb * 8))) return rc;
+  double* G = (double*)s.G1.p;
+  if ((rc = gram(s.c, X, (int)s.nt, nb, X, (int)s.nt, nb, G, nb, st))) return rc;
+  if ((rc = d.potrf_upper(nb, G, nb, st))) return rc;
+  // Uinv = U^{-1} (upper): solve U * Uinv = I
+  if ((rc = s.G2.alloc((size_t)nb * nb * 8))) return rc;
+  double* Ui = (double*)s.G2.p;
+  std::vector<double> I((size_t)nb * nb, 0.0);
+  for (int i = 0; i < nb; ++i) I[(size_t)i * nb + i] = 1.0;
+  PWB_CUDA(cudaMemcpy(Ui, I.data(), (size_t)nb * nb * 8, cudaMemcpyHostToDevice));
+  const double one = 1.0;
+  cublasSetStream(d.blas, st);
+  // zero the strict lower part of G first (potrf leaves it untouched)
+  std::vector<double> hg((size_t)nb * nb);
+  PWB_CUDA(cudaMemcpy(hg.data(), G, hg.size() * 8, cudaMemcpyDeviceToHost));
+  for (int j = 0; j < nb; ++j)
+    for (int i = j + 1; i < nb; ++i) hg[(size_t)j * nb + i] = 0.0;
+  PWB_CUDA(cudaMemcpy(G, hg.data(), hg.size() * 8, cudaMemcpyHostToDevice));
+  if (cublasDtrsm(d.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, nb, nb, &one, G,
+                  nb, Ui, nb) != CUBLAS_STATUS_SUCCESS) {
+    set_error("trsm failed");
+    return PW_ECUDA;
+  }
+  RotBlock rb{X, s.nt, nb, Ui, nb};
+  if ((rc = rotate(s.c, (int)s.nt, nb, &rb, 1, tmp, s.nt, 0.0, st))) return rc;
+  PWB_CUDA(cudaMemcpy(X, tmp, (size_t)nb * s.nt * s.esz, cudaMemcpyDeviceToDevice));
+  return PW_OK;
+}
+
+// Rayleigh-Ritz on an orthonormal block Y with HY: eig(Y^T HY) = V diag(l),
+// X = Y V, HX = HY V
+static int rayleigh_ritz(Solver& s, Dense& d, void* Y, void* HY, void* X, void* HX, int nb) {
+  int rc;
+  if ((rc = s.G1.alloc((size_t)nb * nb * 8)) || (rc = s.wbuf.alloc((size_t)nb * 8 * 2))) return rc;
+  double* A = (double*)s.G1.p;
+  if ((rc = gram(s.c, Y, (int)s.nt, nb, HY, (int)s.nt, nb, A, nb, nullptr))) return rc;
+  // symmetrise from the upper triangle
+  std::vector<double> ha((size_t)nb * nb);
+  PWB_CUDA(cudaMemcpy(ha.data(), A, ha.size() * 8, cudaMemcpyDeviceToHost));
+  for (int j = 0; j < nb; ++j)
+    for (int i = j + 1; i < nb; ++i) ha[(size_t)j * nb + i] = ha[(size_t)i * nb + j];
+  PWB_CUDA(cudaMemcpy(A, ha.data(), ha.size() * 8, cudaMemcpyHostToDevice));
+  double* w = (double*)s.wbuf.p;
+  if ((rc = d.syevd(nb, A, nb, w, nullptr))) return rc;
+  s.eig.resize(nb);
+  PWB_CUDA(cudaMemcpy(s.eig.data(), w, nb * 8, cudaMemcpyDeviceToHost));
+  RotBlock r1{Y, s.nt, nb, A, nb};
+  if ((rc = rotate(s.c, (int)s.nt, nb, &r1, 1, X, s.nt, 0.0, nullptr))) return rc;
+  RotBlock r2{HY, s.nt, nb, A, nb};
+  return rotate(s.c, (int)s.nt, nb, &r2, 1, HX, s.nt, 0.0, nullptr);
+}
+
+// Chebyshev filter of degree m on [a, b] scaled at a0 (Zhou et al. 2006,
+// Algorithm 3.2): on exit Y = p_m(H) X.  X is overwritten.
+static int cheby_filter(Solver& s, int nb, int m, double a, double b, double a0, void* X, void* Y, void* Z, void* HY,
+                        void** result) {
+  const double e = (b - a) / 2.0, cc = (b + a) / 2.0;
+  double sigma = e / (a0 - cc);
+  const double sigma1 = sigma, gamma = 2.0 / sigma1;
+  int rc;
+  if ((rc = hpsi(s.c, X, HY, nb, nullptr))) return rc;
+  // Y = (HX - c X) sigma1 / e
+  PWB_CUDA(cudaMemcpy(Y, HY, (size_t)nb * s.nt * s.esz, cudaMemcpyDeviceToDevice));
+  if ((rc = v_axpby(s, nb, -cc * sigma1 / e, X, sigma1 / e, Y))) return rc;
+  void* xp = X;
+  void* yp = Y;
+  void* zp = Z;
+  for (int i = 2; i <= m; ++i) {
+    const double sigma2 = 1.0 / (gamma - sigma);
+    if ((rc = hpsi(s.c, yp, HY, nb, nullptr))) return rc;
+    // Z = (2 sigma2 / e)(HY - c Y) - sigma sigma2 X
+    if (s.c->prec == PW_F64)
+      rc = axpbypcz<double>((int)s.nt, nb, 2 * sigma2 / e, (const double*)HY, -2 * sigma2 * cc / e, (const double*)yp,
+                            -sigma * sigma2, (const double*)xp, (double*)zp, s.nt, nullptr);
+    else
+      rc = axpbypcz<float>((int)s.nt, nb, 2 * sigma2 / e, (const float*)HY, -2 * sigma2 * cc / e, (const float*)yp,
+                           -sigma * sigma2, (const float*)xp, (float*)zp, s.nt, nullptr);
+    if (rc) return rc;
+    void* t = xp;
+    xp = yp;
+    yp = zp;
+    zp = t;
+    sigma = sigma2;
+  }
+  *result = yp;
+  return PW_OK;
+}
+
+// k-step Lanczos on a random vector: upper bound of the spectrum
+static int lanczos_upper(Solver& s, int k, double* upper, double* lower) {
+  DevBuf v, w, v0;
+  int rc;
+  if ((rc = v.alloc(s.nt * s.esz)) || (rc = w.alloc(s.nt * s.esz)) || (rc = v0.alloc(s.nt * s.esz))) return rc;
+  std::mt19937_64 gen(12345);
+  std::normal_distribution<double> nd;
+  std::vector<double> hv(s.nt);
+  double nrm = 0;
+  for (auto& x : hv) { x = nd(gen); nrm += x * x; }
+  nrm = std::sqrt(nrm);
+  for (auto& x : hv) x /= nrm;
+  if (s.c->prec == PW_F64) PWB_CUDA(cudaMemcpy(v.p, hv.data(), s.nt * 8, cudaMemcpyHostToDevice));
+  else {
+    std::vector<float> hf(hv.begin(), hv.end());
+    PWB_CUDA(cudaMemcpy(v.p, hf.data(), s.nt * 4, cudaMemcpyHostToDevice));
+  }
+  PWB_CUDA(cudaMemset(v0.p, 0, s.nt * s.esz));
+  std::vector<double> al, be;
+  DevBuf dot;
+  if ((rc = dot.alloc(16))) return rc;
+  double beta = 0;
+  for (int j = 0; j < k; ++j) {
+    if ((rc = hpsi(s.c, v.p, w.p, 1, nullptr))) return rc;
+    // alpha = v . w
+    double* G = (double*)dot.p;
+    if ((rc = gram(s.c, v.p, (int)s.nt, 1, w.p, (int)s.nt, 1, G, 1, nullptr))) return rc;
+    double alpha;
+    PWB_CUDA(cudaMemcpy(&alpha, G, 8, cudaMemcpyDeviceToHost));
+    al.push_back(alpha);
+    // w = w - alpha v - beta v0
+    if ((rc = v_axpby(s, 1, -alpha, v.p, 1.0, w.p))) return rc;
+    if (j > 0 && (rc = v_axpby(s, 1, -beta, v0.p, 1.0, w.p))) return rc;
+    if ((rc = v_colnorm2(s, 1, w.p, G))) return rc;
+    double b2;
+    PWB_CUDA(cudaMemcpy(&b2, G, 8, cudaMemcpyDeviceToHost));
+    beta = std::sqrt(b2);
+    be.push_back(beta);
+    PWB_CUDA(cudaMemcpy(v0.p, v.p, s.nt * s.esz, cudaMemcpyDeviceToDevice));
+    PWB_CUDA(cudaMemcpy(v.p, w.p, s.nt * s.esz, cudaMemcpyDeviceToDevice));
+    const double inv = 1.0 / beta;
+    if ((rc = v_axpby(s, 1, 0.0, w.p, inv, v.p))) return rc;
+  }
+  // eigenvalues of the tridiagonal T (host, Jacobi on a k x k matrix)
+  const int n = (int)al.size();
+  std::vector<double> T((size_t)n * n, 0.0);
+  for (int i = 0; i < n; ++i) {
+    T[(size_t)i * n + i] = al[i];
+    if (i + 1 < n) T[(size_t)i * n + i + 1] = T[(size_t)(i + 1) * n + i] = be[i];
+  }
+  for (int sweep = 0; sweep < 100; ++sweep) {
+    double off = 0;
+    for (int p = 0; p < n; ++p)
+      for (int q = p + 1; q < n; ++q) off += T[(size_t)p * n + q] * T[(size_t)p * n + q];
+    if (off < 1e-24) break;
+    for (int p = 0; p < n; ++p)
+      for (int q = p + 1; q < n; ++q) {
+        const double apq = T[(size_t)p * n + q];
+        if (std::fabs(apq) < 1e-300) continue;
+        const double theta = (T[(size_t)q * n + q] - T[(size_t)p * n + p]) / (2 * apq);
+        const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1));
+        const double cs = 1 / std::sqrt(t * t + 1), sn = t * cs;
+        for (int r = 0; r < n; ++r) {
+          const double a1 = T[(size_t)r * n + p], a2 = T[(size_t)r * n + q];
+          T[(size_t)r * n + p] = cs * a1 - sn * a2;
+          T[(size_t)r * n + q] = sn * a1 + cs * a2;
+        }
+        for (int r = 0; r < n; ++r) {
+          const double a1 = T[(size_t)p * n + r], a2 = T[(size_t)q * n + r];
+          T[(size_t)p * n + r] = cs * a1 - sn * a2;
+          T[(size_t)q * n + r] = sn * a1 + cs * a2;
+        }
+      }
+  }
+  double mx = -1e300, mn = 1e300;
+  for (int i = 0; i < n; ++i) {
+    mx = std::max(mx, T[(size_t)i * n + i]);
+    mn = std::min(mn, T[(size_t)i * n + i]);
+  }
+  *upper = mx + beta;
+  *lower = mn;
+  return PW_OK;
+}
+
+// one ChebFSI step on the block X (orthonormal on entry and exit); eigenvalues in s.eig
+static int chebfsi_step(Solver& s, Dense& d, int nb, int degree, double a, double b, double a0) {
+  int rc;
+  void* res = nullptr;
+  if ((rc = cheby_filter(s, nb, degree, a, b, a0, s.X.p, s.Y.p, s.Z.p, s.HY.p, &res))) return rc;
+  // res is one of X, Y, Z; orthonormalise it, then Rayleigh-Ritz into X / HX
+  void* tmp = (res == s.Z.p) ? s.Y.p : s.Z.p;
+  if ((rc = cholqr(s, d, res, nb, tmp))) return rc;
+  if ((rc = hpsi(s.c, res, s.HY.p, nb, nullptr))) return rc;
+  void* outX = (res == s.X.p) ? tmp : s.X.p;
+  if ((rc = rayleigh_ritz(s, d, res, s.HY.p, outX, s.HX.p, nb))) return rc;
+  if (outX != s.X.p) PWB_CUDA(cudaMemcpy(s.X.p, outX, (size_t)nb * s.nt * s.esz, cudaMemcpyDeviceToDevice));
+  return PW_OK;
+}
+
+// residual norms ||HX - X diag(l)|| / max(1, |l|) (lobpcg.cpp:697-709)
+static int residuals(Solver& s, int nb) {
+  int rc;
+  if ((rc = alloc_block(s, s.Z, nb))) return rc;
+  PWB_CUDA(cudaMemcpy(s.Z.p, s.HX.p, (size_t)nb * s.nt * s.esz, cudaMemcpyDeviceToDevice));
+  std::vector<double> ml(nb);
+  for (int i = 0; i < nb; ++i) ml[i] = -s.eig[i];
+  DevBuf dl;
+  if ((rc = dl.alloc(nb * 8 * 2))) return rc;
+  PWB_CUDA(cudaMemcpy(dl.p, ml.data(), nb * 8, cudaMemcpyHostToDevice));
+  // Z = HX - X diag(l): scale a copy of X then add
+  if ((rc = alloc_block(s, s.Y, nb))) return rc;
+  PWB_CUDA(cudaMemcpy(s.Y.p, s.X.p, (size_t)nb * s.nt * s.esz, cudaMemcpyDeviceToDevice));
+  if ((rc = v_colscale(s, nb, s.Y.p, (double*)dl.p))) return rc;
+  if ((rc = v_axpby(s, nb, 1.0, s.Y.p, 1.0, s.Z.p))) return rc;
+  double* nr = (double*)dl.p + nb;
+  if ((rc = v_colnorm2(s, nb, s.Z.p, nr))) return rc;
+  std::vector<double> h(nb);
+  PWB_CUDA(cudaMemcpy(h.data(), nr, nb * 8, cudaMemcpyDeviceToHost));
+  s.res.resize(nb);
+  for (int i = 0; i < nb; ++i) s.res[i] = std::sqrt(h[i]) / std::max(1.0, std::fabs(s.eig[i]));
+  return PW_OK;
+}
+
+// LOBPCG restated from EigenSolver::LOBPCGSolveReal (real-space branch).
+static int lobpcg(Solver& s, Dense& d, int width, int maxit, double tol, bool first_scf, int* iters) {
+  int rc;
+  const long nt = s.nt;
+  const size_t esz = s.esz;
+  const int lda = 3 * width;
+  if ((rc = alloc_block(s, s.S, 3 * width)) || (rc = alloc_block(s, s.HS, 3 * width)) || (rc = alloc_block(s, s.Y, width)))
+    return rc;
+  void* X = s.ptr(s.S, 0);
+  void* W = s.ptr(s.S, width);
+  void* P = s.ptr(s.S, 2 * width);
+  void* AX = s.ptr(s.HS, 0);
+  void* AW = s.ptr(s.HS, width);
+  void* AP = s.ptr(s.HS, 2 * width);
+  PWB_CUDA(cudaMemcpy(X, s.X.p, (size_t)width * nt * esz, cudaMemcpyDeviceToDevice));
+  if (first_scf && (rc = cholqr(s, d, X, width, s.Y.p))) return rc;
+  if ((rc = hpsi(s.c, X, AX, width, nullptr))) return rc;
+  if ((rc = s.G1.alloc((size_t)lda * lda * 8)) || (rc = s.G2.alloc((size_t)lda * lda * 8))) return rc;
+  DevBuf xtx, dvec;
+  if ((rc = xtx.alloc((size_t)width * width * 8)) || (rc = dvec.alloc((size_t)3 * width * 8))) return rc;
+  std::vector<double> eigS(lda), hXTX((size_t)width * width);
+  double resMax = 0;
+  int iter = 0;
+  std::vector<double> resNorm(width);
+  do {
+    ++iter;
+    const int numSet = (iter == 1) ? 2 : 3;
+    // XTX = X^T AX;  R = AX - X XTX
+    double* XTX = (double*)xtx.p;
+    if ((rc = gram(s.c, X, (int)nt, width, AX, (int)nt, width, XTX, width, nullptr))) return rc;
+    PWB_CUDA(cudaMemcpy(hXTX.data(), XTX, hXTX.size() * 8, cudaMemcpyDeviceToHost));
+    PWB_CUDA(cudaMemcpy(s.Y.p, AX, (size_t)width * nt * esz, cudaMemcpyDeviceToDevice));
+    std::vector<double> mX((size_t)width * width);
+    for (size_t i = 0; i < mX.size(); ++i) mX[i] = -hXTX[i];
+    PWB_CUDA(cudaMemcpy(s.G2.p, mX.data(), mX.size() * 8, cudaMemcpyHostToDevice));
+    RotBlock rb{X, nt, width, (double*)s.G2.p, width};
+    if ((rc = rotate(s.c, (int)nt, width, &rb, 1, s.Y.p, nt, 1.0, nullptr))) return rc;
+    double* nrm = (double*)dvec.p;
+    if ((rc = v_colnorm2(s, width, s.Y.p, nrm))) return rc;
+    std::vector<double> hn(width);
+    PWB_CUDA(cudaMemcpy(hn.data(), nrm, width * 8, cudaMemcpyDeviceToHost));
+    for (int k = 0; k < width; ++k)
+      resNorm[k] = std::sqrt(hn[k]) / std::max(1.0, std::fabs(hXTX[(size_t)k * width + k]));
+    resMax = *std::max_element(resNorm.begin(), resNorm.end());
+    // W = Teter * R, normalised
+    if ((rc = pw_teter_precond(s.c, s.Y.p, (int)nt, W, (int)nt, width, 0, nullptr))) return rc;
+    if ((rc = v_colnorm2(s, width, W, nrm))) return rc;
+    PWB_CUDA(cudaMemcpy(hn.data(), nrm, width * 8, cudaMemcpyDeviceToHost));
+    for (int k = 0; k < width; ++k) hn[k] = 1.0 / std::sqrt(hn[k]);
+    PWB_CUDA(cudaMemcpy(nrm, hn.data(), width * 8, cudaMemcpyHostToDevice));
+    if ((rc = v_colscale(s, width, W, nrm))) return rc;
+    if (numSet == 3) {
+      if ((rc = v_colnorm2(s, width, P, nrm))) return rc;
+      PWB_CUDA(cudaMemcpy(hn.data(), nrm, width * 8, cudaMemcpyDeviceToHost));
+      for (int k = 0; k < width; ++k) hn[k] = 1.0 / std::sqrt(hn[k]);
+      PWB_CUDA(cudaMemcpy(nrm, hn.data(), width * 8, cudaMemcpyHostToDevice));
+      if ((rc = v_colscale(s, width, P, nrm)) || (rc = v_colscale(s, width, AP, nrm))) return rc;
+    }
+    if ((rc = hpsi(s.c, W, AW, width, nullptr))) return rc;
+    // AMat = S^T AS, BMat = S^T S over the active sets (upper blocks used)
+    const int numCol = numSet * width;
+    double* A = (double*)s.G1.p;
+    double* B = (double*)s.G2.p;
+    if ((rc = gram(s.c, s.S.p, (int)nt, numCol, s.HS.p, (int)nt, numCol, A, lda, nullptr))) return rc;
+    if ((rc = gram(s.c, s.S.p, (int)nt, numCol, s.S.p, (int)nt, numCol, B, lda, nullptr))) return rc;
+    int numKeep = 0;
+    if ((rc = solve_gen_eig(d, lda, numCol, width, A, B, eigS.data(), &numKeep, nullptr))) return rc;
+    // X_new = X Cx + W Cw (+ P Cp);  P_new = W Cw (+ P Cp); same for AX, AP
+    const double* Cx = A;
+    const double* Cw = A + width;
+    const double* Cp = A + 2 * width;
+    RotBlock pb[2] = {{W, nt, width, Cw, lda}, {P, nt, width, Cp, lda}};
+    if ((rc = rotate(s.c, (int)nt, width, pb, numSet - 1, s.Y.p, nt, 0.0, nullptr))) return rc;
+    RotBlock xb{X, nt, width, Cx, lda};
+    if ((rc = rotate(s.c, (int)nt, width, &xb, 1, s.Z.p, nt, 0.0, nullptr))) return rc;
+    // Z = X Cx ; X = Z + Y ; P = Y
+    if ((rc = v_axpby(s, width, 1.0, s.Z.p, 0.0, X))) return rc;
+    if ((rc = v_axpby(s, width, 1.0, s.Y.p, 1.0, X))) return rc;
+    PWB_CUDA(cudaMemcpy(P, s.Y.p, (size_t)width * nt * esz, cudaMemcpyDeviceToDevice));
+    RotBlock apb[2] = {{AW, nt, width, Cw, lda}, {AP, nt, width, Cp, lda}};
+    if ((rc = rotate(s.c, (int)nt, width, apb, numSet - 1, s.Y.p, nt, 0.0, nullptr))) return rc;
+    RotBlock axb{AX, nt, width, Cx, lda};
+    if ((rc = rotate(s.c, (int)nt, width, &axb, 1, s.Z.p, nt, 0.0, nullptr))) return rc;
+    if ((rc = v_axpby(s, width, 1.0, s.Z.p, 0.0, AX))) return rc;
+    if ((rc = v_axpby(s, width, 1.0, s.Y.p, 1.0, AX))) return rc;
+    PWB_CUDA(cudaMemcpy(AP, s.Y.p, (size_t)width * nt * esz, cudaMemcpyDeviceToDevice));
+  } while (iter < maxit && resMax > tol);
+  // final Rayleigh-Ritz with X^T AX (lobpcg.cpp:991-1003)
+  if ((rc = rayleigh_ritz(s, d, X, AX, s.X.p, s.HX.p, width))) return rc;
+  s.res = resNorm;
+  if (iters) *iters = iter;
+  return PW_OK;
+}
+
+}  // namespace pwb
+
+using namespace pwb;
+
+namespace {
+
+struct ScfState {
+  pw_ctx* c64 = nullptr;
+  pw_ctx* c32 = nullptr;
+  bool own32 = false;
+  DevBuf rho, rho_out, rps, vtot, vtot_new, vxc, eps, vh, kern, work, tw, dots, wocc;
+  DevBuf dvh, dfh, dif_v, dif_f;   // Anderson history [mixdim][nf] and differences
+  int nhist = 0, hpos = 0;
+  ~ScfState() {
+    if (own32 && c32) pw_ctx_destroy(c32);
+  }
+};
+
+int dots(ScfState& S, long n, std::initializer_list<std::pair<const double*, const double*>> pr, double* out) {
+  DotSet ds{};
+  ds.k = 0;
+  for (auto& p : pr) {
+    ds.a[ds.k] = p.first;
+    ds.b[ds.k] = p.second;
+    ds.k++;
+  }
+  PWB_CUDA(cudaMemset(S.dots.p, 0, 64));
+  k_dots<<<nblk(n), 256>>>(n, ds, (double*)S.dots.p);
+  PWB_CUDA(cudaMemcpy(out, S.dots.p, ds.k * 8, cudaMemcpyDeviceToHost));
+  return PW_OK;
+}
+
+int set_vtot_dev(pw_ctx* c, const double* vtot_dev) {
+  int rc = c->vtot.alloc(c->ntotf * c->esz);
+  if (rc) return rc;
+  if (c->prec == PW_F64) PWB_CUDA(cudaMemcpy(c->vtot.p, vtot_dev, c->ntotf * 8, cudaMemcpyDeviceToDevice));
+  else if ((rc = copy_d2f(c->ntotf, vtot_dev, (float*)c->vtot.p, nullptr))) return rc;
+  c->have_vtot = true;
+  return PW_OK;
+}
+
+double wgauss(double ev, double ef, double tbeta) { return 1.0 / (1.0 + std::exp(-tbeta * (ef - ev))); }
+double fd_entropy(double ev, double ef, double tbeta) {
+  const double x = tbeta * (ef - ev);
+  if (std::fabs(x) > 36.0) return 0.0;
+  const double occ = 1.0 / (1.0 + std::exp(-x));
+  return (occ * std::log(occ) + (1.0 - occ) * std::log(1.0 - occ)) / tbeta;
+}
+
+void occupations(const std::vector<double>& eig, int nocc, double tbeta, std::vector<double>& occ, double& ef) {
+  std::vector<double> ev(eig);
+  std::sort(ev.begin(), ev.end());
+  const int npsi = (int)ev.size();
+  occ.assign(npsi, 1.0);
+  if (npsi == nocc) { ef = ev[npsi - 1]; return; }
+  double lb = ev[0], ub = ev[npsi - 1];
+  ef = 0.5 * (lb + ub);
+  auto sum = [&](double f) { double s = 0; for (double e : ev) s += wgauss(e, f, tbeta); return s; };
+  double os = sum(ef);
+  int it = 1;
+  while (std::fabs(os - nocc) > 1e-16 && it < 200) {
+    if (os < nocc) lb = ef; else ub = ef;
+    ef = 0.5 * (lb + ub);
+    os = sum(ef);
+    ++it;
+  }
+  for (int j = 0; j < npsi; ++j) occ[j] = wgauss(eig[j], ef, tbeta);
+}
+
+}  // namespace
+
+extern "C" {
+
+int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* eig_out, double* rho_out) {
+  PWB_CHECK(ctx && p && r, PW_EINVAL, "null argument");
+  PWB_CHECK(ctx->prec == PW_F64, PW_EINVAL, "pw_scf_run takes the FP64 context (mixed mode builds an FP32 twin)");
+  PWB_CHECK(!ctx->atom_z.empty(), PW_ENOTREADY, "atoms not set (pw_set_atoms)");
+  PWB_CHECK(p->nocc > 0 && p->nextra >= 0 && p->ecut > 0, PW_EINVAL, "bad SCF parameters");
+  PWB_CUDA(cudaSetDevice(ctx->device));
+  const auto t_start = std::chrono::steady_clock::now();
+  ScfState S;
+  S.c64 = ctx;
+  const long nf = ctx->ntotf, nt = ctx->ntot;
+  const int nb = p->nocc + p->nextra;
+  const int natom = (int)ctx->atom_z.size();
+  int rc;
+  if (p->mixed) {
+    pw_ctx* c32 = nullptr;
+    if ((rc = pw_ctx_create(ctx->L, ctx->n, ctx->nf, PW_F32, ctx->device, &c32))) return rc;
+    S.c32 = c32;
+    S.own32 = true;
+    if ((rc = pw_set_band_batch(c32, nb))) return rc;
+    if ((rc = pw_set_atoms(c32, natom, ctx->atom_z.data(), ctx->atom_pos.data()))) return rc;
+  }
+  if ((rc = pw_set_band_batch(ctx, nb))) return rc;
+  // device arrays
+  for (DevBuf* b : {&S.rho, &S.rho_out, &S.rps, &S.vtot, &S.vtot_new, &S.vxc, &S.eps, &S.vh, &S.kern})
+    if ((rc = b->alloc(nf * 8))) return rc;
+  if ((rc = S.work.alloc(nf * 16)) || (rc = S.dots.alloc(64)) || (rc = S.wocc.alloc((nb + 2) * 8))) return rc;
+  const int mixdim = std::max(1, p->mix_dim);
+  if ((rc = S.dvh.alloc((size_t)mixdim * nf * 8)) || (rc = S.dfh.alloc((size_t)mixdim * nf * 8)) ||
+      (rc = S.dif_v.alloc((size_t)mixdim * nf * 8)) || (rc = S.dif_f.alloc((size_t)mixdim * nf * 8)))
+    return rc;
+  PWB_CUDA(cudaMemcpy(S.rps.p, ctx->h_rhops.data(), nf * 8, cudaMemcpyHostToDevice));
+  {
+    // Hartree kernel 2 pi / gkk / N on the fine grid (fourier.cpp:323-344 gkkFine)
+    std::vector<double> k(nf);
+    const int N0 = ctx->nf[0], N1 = ctx->nf[1], N2 = ctx->nf[2];
+    for (int z = 0; z < N2; ++z)
+      for (int y = 0; y < N1; ++y)
+        for (int x = 0; x < N0; ++x) {
+          const double m0 = x <= N0 / 2 ? x : x - N0, m1 = y <= N1 / 2 ? y : y - N1, m2 = z <= N2 / 2 ? z : z - N2;
+          const double g0 = 2 * M_PI / ctx->L[0] * m0, g1 = 2 * M_PI / ctx->L[1] * m1, g2 = 2 * M_PI / ctx->L[2] * m2;
+          const double gkk = (g0 * g0 + g1 * g1 + g2 * g2) / 2;
+          k[x + (size_t)N0 * (y + (size_t)N1 * z)] =
+              (gkk <= 1e-16 || gkk > 4.0 * p->ecut) ? 0.0 : 2.0 * M_PI / gkk / (double)nf;
+        }
+    PWB_CUDA(cudaMemcpy(S.kern.p, k.data(), nf * 8, cudaMemcpyHostToDevice));
+    std::vector<double> t(2 * N0);
+    for (int m = 0; m < N0; ++m) {
+      t[2 * m] = std::cos(2 * M_PI * m / N0);
+      t[2 * m + 1] = -std::sin(2 * M_PI * m / N0);
+    }
+    if ((rc = S.tw.alloc(N0 * 16))) return rc;
+    PWB_CUDA(cudaMemcpy(S.tw.p, t.data(), N0 * 16, cudaMemcpyHostToDevice));
+  }
+  const double w = ctx->vol / (double)nf;
+  double eself = 0;
+  for (int z : ctx->atom_z) {
+    double es;
+    pw_hgh_species(z, nullptr, &es, nullptr, nullptr, nullptr);
+    eself += es;
+  }
+  // initial density from the pseudocharge (scf.cpp:232-255)
+  double* rho = (double*)S.rho.p;
+  double* rps = (double*)S.rps.p;
+  k_init_rho<<<nblk(nf), 256>>>(nf, rps, rho);
+  {
+    double sums[2];
+    if ((rc = dots(S, nf, {{rho, nullptr}, {rps, nullptr}}, sums))) return rc;
+    k_lincomb<<<nblk(nf), 256>>>(nf, sums[1] / sums[0], rho, 0.0, nullptr, rho);
+  }
+  auto potentials = [&](const double* rh, double* exc_out) -> int {
+    k_xc_teter93<<<nblk(nf), 256>>>(nf, rh, (double*)S.eps.p, (double*)S.vxc.p);
+    int q = hartree(ctx, (double2*)S.work.p, rh, rps, (const double*)S.kern.p, (double*)S.vh.p, (const double2*)S.tw.p,
+                    nullptr);
+    if (q) return q;
+    double e;
+    if ((q = dots(S, nf, {{(const double*)S.eps.p, rh}}, &e))) return q;
+    *exc_out = e * w;
+    return PW_OK;
+  };
+  double exc = 0;
+  if ((rc = potentials(rho, &exc))) return rc;
+  k_lincomb<<<nblk(nf), 256>>>(nf, 1.0, (double*)S.vh.p, 1.0, (double*)S.vxc.p, (double*)S.vtot.p);
+  // eigensolver state: start in the FP32 twin when mixed
+  Dense dn;
+  if ((rc = dn.init((cublasHandle_t)ctx->blas))) return rc;
+  Solver sv;
+  auto bind = [&](pw_ctx* c) -> int {
+    sv.c = c;
+    sv.nt = nt;
+    sv.esz = c->esz;
+    sv.nb = nb;
+    int q;
+    for (DevBuf* b : {&sv.X, &sv.HX, &sv.Y, &sv.HY, &sv.Z})
+      if ((q = alloc_block(sv, *b, nb))) return q;
+    return PW_OK;
+  };
+  pw_ctx* cur = p->mixed ? S.c32 : ctx;
+  if ((rc = bind(cur))) return rc;
+  {
+    // random start, Gaussian (seeded), orthonormalised by Cholesky-QR
+    std::mt19937_64 gen(p->seed);
+    std::normal_distribution<double> nd;
+    std::vector<double> h((size_t)nb * nt);
+    for (auto& x : h) x = nd(gen);
+    if (cur->prec == PW_F64) PWB_CUDA(cudaMemcpy(sv.X.p, h.data(), h.size() * 8, cudaMemcpyHostToDevice));
+    else {
+      std::vector<float> hf(h.begin(), h.end());
+      PWB_CUDA(cudaMemcpy(sv.X.p, hf.data(), hf.size() * 4, cudaMemcpyHostToDevice));
+    }
+    if ((rc = cholqr(sv, dn, sv.X.p, nb, sv.Y.p))) return rc;
+  }
+  const double tbeta = 315774.67 / p->temperature;
+  double b_up = 0, lmin = 0;
+  bool have_bounds = false, refined = !p->mixed;
+  std::vector<double> occ, eig;
+  double ef = 0, etot = 0, efree = 0, eharris = 0, ehart = 0;
+  int it = 0;
+  bool conv = false;
+  r->hpsi_bands = 0;
+  for (it = 1; it <= p->max_iter; ++it) {
+    if ((rc = set_vtot_dev(sv.c, (const double*)S.vtot.p))) return rc;
+    if (p->solver == PW_SOLVER_CHEBFSI) {
+      if (!have_bounds) {
+        double lo;
+        if ((rc = lanczos_upper(sv, 16, &b_up, &lo))) return rc;
+        r->hpsi_bands += 16;
+        lmin = lo;
+        have_bounds = true;
+        // first cycle: cutoff from the free-electron counting estimate
+        const double frac = std::pow((double)nb / (double)nt, 2.0 / 3.0);
+        double a = lo + 2.0 * frac * (b_up - lo);
+        const int ncyc = std::max(1, p->cheby_first_cycles);
+        for (int cyc = 0; cyc < ncyc; ++cyc) {
+          if ((rc = chebfsi_step(sv, dn, nb, p->cheby_degree, a, b_up, lmin))) return rc;
+          r->hpsi_bands += (long)nb * (p->cheby_degree + 1);
+          a = sv.eig[nb - 1];
+          lmin = sv.eig[0];
+        }
+      } else {
+        if ((rc = chebfsi_step(sv, dn, nb, p->cheby_degree, sv.eig[nb - 1], b_up, sv.eig[0]))) return rc;
+        r->hpsi_bands += (long)nb * (p->cheby_degree + 1);
+      }
+    } else {
+      int li = 0;
+      const double tolnow = p->eig_tol;
+      if ((rc = lobpcg(sv, dn, nb, p->eig_max_iter, tolnow, it == 1, &li))) return rc;
+      r->hpsi_bands += (long)nb * (2 * li + 1);
+    }
+    eig = sv.eig;
+    occupations(eig, p->nocc, tbeta, occ, ef);
+    double ekin = 0, ent = 0;
+    for (int i = 0; i < nb; ++i) {
+      ekin += 2.0 * eig[i] * occ[i];
+      ent += 2.0 * fd_entropy(eig[i], ef, tbeta);
+    }
+    // Harris energy with the input density (scf.cpp:2025-2060)
+    double hd[3];
+    if ((rc = dots(S, nf, {{(const double*)S.vh.p, rho}, {(const double*)S.vh.p, rps}, {(const double*)S.vxc.p, rho}}, hd)))
+      return rc;
+    const double ehart_h = 0.5 * (hd[0] + hd[1]) * w, evxc = hd[2] * w;
+    eharris = ekin + (exc - evxc) - ehart_h - eself + ent;
+    // new density
+    {
+      std::vector<double> wv(nb + 2, 0.0);
+      for (int i = 0; i < nb; ++i) wv[i] = 2.0 * occ[i];
+      PWB_CUDA(cudaMemcpy(S.wocc.p, wv.data(), wv.size() * 8, cudaMemcpyHostToDevice));
+      double* ro = (double*)S.rho_out.p;
+      PWB_CUDA(cudaMemset(ro, 0, nf * 8));
+      const int cap = sv.c->pair_cap;
+      for (int b0 = 0; b0 < nb; b0 += 2 * cap) {
+        const int npair = std::min(cap, (nb - b0 + 1) / 2);
+        if ((rc = run_density(sv.c, sv.X.p, (int)nt, nb, b0, npair, (const double*)S.wocc.p, ro, nullptr))) return rc;
+      }
+      double tot;
+      if ((rc = dots(S, nf, {{ro, nullptr}}, &tot))) return rc;
+      k_lincomb<<<nblk(nf), 256>>>(nf, (2.0 * p->nocc * (double)nf) / (ctx->vol * tot), ro, 0.0, nullptr, ro);
+    }
+    double* ro = (double*)S.rho_out.p;
+    if ((rc = potentials(ro, &exc))) return rc;
+    k_lincomb<<<nblk(nf), 256>>>(nf, 1.0, (double*)S.vh.p, 1.0, (double*)S.vxc.p, (double*)S.vtot_new.p);
+    double ed[2];
+    if ((rc = dots(S, nf, {{(const double*)S.vtot.p, ro}, {(const double*)S.vh.p, ro}}, ed))) return rc;
+    double ehps;
+    if ((rc = dots(S, nf, {{(const double*)S.vh.p, rps}}, &ehps))) return rc;
+    ehart = 0.5 * (ed[1] - ehps) * w;
+    etot = ekin + (-ed[0] * w) + exc + ehart - eself;
+    efree = etot + ent;
+    const double dif = std::fabs(efree - eharris) / natom;
+    if (p->verbose)
+      fprintf(stderr, "SCF %3d %s Etot %.10f Efree %.10f Eharris %.10f dif %.3e\n", it,
+              sv.c->prec == PW_F32 ? "f32" : "f64", etot, efree, eharris, dif);
+    PWB_CUDA(cudaMemcpy(rho, ro, nf * 8, cudaMemcpyDeviceToDevice));
+    if (refined && dif < p->tol_efree) { conv = true; break; }
+    // switch the eigensolver to FP64 for the final iterations (iterative refinement)
+    if (!refined && dif < p->refine_threshold) {
+      pw_ctx* c32 = sv.c;
+      DevBuf x32;
+      if ((rc = x32.alloc((size_t)nb * nt * 4))) return rc;
+      PWB_CUDA(cudaMemcpy(x32.p, sv.X.p, (size_t)nb * nt * 4, cudaMemcpyDeviceToDevice));
+      std::vector<double> keep_eig = sv.eig;
+      if ((rc = bind(ctx))) return rc;
+      if ((rc = copy_f2d_2d((int)nt, nb, (const float*)x32.p, nt, (double*)sv.X.p, nt, nullptr))) return rc;
+      if ((rc = cholqr(sv, dn, sv.X.p, nb, sv.Y.p))) return rc;
+      sv.eig = keep_eig;
+      refined = true;
+      r->refine_iter = it;
+      (void)c32;
+    }
+    // Anderson mixing of the potential (scf.cpp:2299-2365)
+    {
+      double* vin = (double*)S.vtot.p;
+      double* vout = (double*)S.vtot_new.p;
+      double* F = vout;   // F = vout - vin (in place)
+      k_lincomb<<<nblk(nf), 256>>>(nf, 1.0, vout, -1.0, vin, F);
+      const int dim = std::min(S.nhist, mixdim);
+      std::vector<double> theta(dim, 0.0);
+      double* dv = (double*)S.dvh.p;
+      double* df = (double*)S.dfh.p;
+      double* difv = (double*)S.dif_v.p;
+      double* diff = (double*)S.dif_f.p;
+      if (dim > 0) {
+        for (int i = 0; i < dim; ++i) {
+          k_lincomb<<<nblk(nf), 256>>>(nf, 1.0, dv + (size_t)i * nf, -1.0, vin, difv + (size_t)i * nf);
+          k_lincomb<<<nblk(nf), 256>>>(nf, 1.0, df + (size_t)i * nf, -1.0, F, diff + (size_t)i * nf);
+        }
+        cublasHandle_t h = (cublasHandle_t)ctx->blas;
+        cublasSetStream(h, nullptr);
+        DevBuf ov;
+        if ((rc = ov.alloc((size_t)(dim + 1) * dim * 8))) return rc;
+        const double one = 1.0, zero = 0.0;
+        double* O = (double*)ov.p;
+        cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, dim, dim, (int)nf, &one, diff, (int)nf, diff, (int)nf, &zero, O, dim);
+        cublasDgemv(h, CUBLAS_OP_T, (int)nf, dim, &one, diff, (int)nf, F, 1, &zero, O + (size_t)dim * dim, 1);
+        std::vector<double> hO((size_t)(dim + 1) * dim);
+        PWB_CUDA(cudaMemcpy(hO.data(), O, hO.size() * 8, cudaMemcpyDeviceToHost));
+        // Cholesky solve of the dim x dim system (lapack Potrf/Potrs, scf.cpp:2340-2341)
+        std::vector<double> L((size_t)dim * dim, 0.0), b(hO.begin() + (size_t)dim * dim, hO.end());
+        for (int j = 0; j < dim; ++j) {
+          double s0 = hO[(size_t)j * dim + j];
+          for (int k = 0; k < j; ++k) s0 -= L[(size_t)k * dim + j] * L[(size_t)k * dim + j];
+          PWB_CHECK(s0 > 0, PW_ENUMERIC, "Anderson overlap not positive definite");
+          L[(size_t)j * dim + j] = std::sqrt(s0);
+          for (int i2 = j + 1; i2 < dim; ++i2) {
+            double s1 = hO[(size_t)j * dim + i2];
+            for (int k = 0; k < j; ++k) s1 -= L[(size_t)k * dim + i2] * L[(size_t)k * dim + j];
+            L[(size_t)j * dim + i2] = s1 / L[(size_t)j * dim + j];
+          }
+        }
+        for (int i2 = 0; i2 < dim; ++i2) {
+          double s1 = b[i2];
+          for (int k = 0; k < i2; ++k) s1 -= L[(size_t)k * dim + i2] * b[k];
+          b[i2] = s1 / L[(size_t)i2 * dim + i2];
+        }
+        for (int i2 = dim - 1; i2 >= 0; --i2) {
+          double s1 = b[i2];
+          for (int k = i2 + 1; k < dim; ++k) s1 -= L[(size_t)i2 * dim + k] * b[k];
+          b[i2] = s1 / L[(size_t)i2 * dim + i2];
+        }
+        theta = b;
+      }
+      // save history (Xin, F) before forming the mix
+      const int slot = S.hpos % mixdim;
+      PWB_CUDA(cudaMemcpy(dv + (size_t)slot * nf, vin, nf * 8, cudaMemcpyDeviceToDevice));
+      PWB_CUDA(cudaMemcpy(df + (size_t)slot * nf, F, nf * 8, cudaMemcpyDeviceToDevice));
+      for (int i = 0; i < dim; ++i) {
+        k_lincomb<<<nblk(nf), 256>>>(nf, 1.0, vin, -theta[i], difv + (size_t)i * nf, vin);
+        k_lincomb<<<nblk(nf), 256>>>(nf, 1.0, F, -theta[i], diff + (size_t)i * nf, F);
+      }
+      k_lincomb<<<nblk(nf), 256>>>(nf, 1.0, vin, p->mix_step, F, vin);
+      S.hpos++;
+      S.nhist = std::min(S.nhist + 1, mixdim);
+      PWB_CUDA(cudaGetLastError());
+    }
+  }
+  PWB_CUDA(cudaDeviceSynchronize());
+  const auto t_end = std::chrono::steady_clock::now();
+  r->etot = etot;
+  r->efree = efree;
+  r->eharris = eharris;
+  r->exc = exc;
+  r->ehart = ehart;
+  r->eself = eself;
+  r->fermi = ef;
+  r->iterations = std::min(it, p->max_iter);
+  r->converged = conv ? 1 : 0;
+  r->time_s = std::chrono::duration<double>(t_end - t_start).count();
+  if (eig_out) std::copy(eig.begin(), eig.end(), eig_out);
+  if (rho_out) PWB_CUDA(cudaMemcpy(rho_out, rho, nf * 8, cudaMemcpyDeviceToHost));
+  dn.release();
+  return PW_OK;
+}
+
+int pw_cholqr(pw_ctx* ctx, void* X, int nb) {
+  PWB_CHECK(ctx && X && nb > 0, PW_EINVAL, "bad arguments");
+  PWB_CUDA(cudaSetDevice(ctx->device));
+  Dense dn;
+  int rc = dn.init((cublasHandle_t)ctx->blas);
+  if (rc) return rc;
+  Solver sv;
+  sv.c = ctx;
+  sv.nt = ctx->ntot;
+  sv.esz = ctx->esz;
+  if ((rc = alloc_block(sv, sv.Y, nb))) return rc;
+  rc = cholqr(sv, dn, X, nb, sv.Y.p);
+  PWB_CUDA(cudaDeviceSynchronize());
+  dn.release();
+  return rc;
+}
+
+int pw_eigsolve(pw_ctx* ctx, int solver, void* X, int nb, int maxit, double tol, int degree, double* eig,
+                double* resnorm, int* iters) {
+  PWB_CHECK(ctx && X && nb > 0, PW_EINVAL, "bad arguments");
+  PWB_CHECK(ctx->have_vtot, PW_ENOTREADY, "local potential not set (pw_set_vtot)");
+  PWB_CUDA(cudaSetDevice(ctx->device));
+  Dense dn;
+  int rc = dn.init((cublasHandle_t)ctx->blas);
+  if (rc) return rc;
+  if ((rc = pw_set_band_batch(ctx, nb))) return rc;
+  Solver sv;
+  sv.c = ctx;
+  sv.nt = ctx->ntot;
+  sv.esz = ctx->esz;
+  sv.nb = nb;
+  for (DevBuf* b : {&sv.X, &sv.HX, &sv.Y, &sv.HY, &sv.Z})
+    if ((rc = alloc_block(sv, *b, nb))) return rc;
+  PWB_CUDA(cudaMemcpy(sv.X.p, X, (size_t)nb * sv.nt * sv.esz, cudaMemcpyDeviceToDevice));
+  int it = 0;
+  if (solver == PW_SOLVER_LOBPCG) {
+    rc = lobpcg(sv, dn, nb, maxit, tol, true, &it);
+  } else {
+    double up, lo;
+    if ((rc = lanczos_upper(sv, 16, &up, &lo))) return rc;
+    if ((rc = cholqr(sv, dn, sv.X.p, nb, sv.Y.p))) return rc;
+    if ((rc = hpsi(ctx, sv.X.p, sv.HX.p, nb, nullptr))) return rc;
+    if ((rc = rayleigh_ritz(sv, dn, sv.X.p, sv.HX.p, sv.Z.p, sv.HY.p, nb))) return rc;
+    PWB_CUDA(cudaMemcpy(sv.X.p, sv.Z.p, (size_t)nb * sv.nt * sv.esz, cudaMemcpyDeviceToDevice));
+    PWB_CUDA(cudaMemcpy(sv.HX.p, sv.HY.p, (size_t)nb * sv.nt * sv.esz, cudaMemcpyDeviceToDevice));
+    const double frac = std::pow((double)nb / (double)sv.nt, 2.0 / 3.0);
+    double a = lo + 2.0 * frac * (up - lo), a0 = lo;
+    for (it = 1; it <= maxit; ++it) {
+      if ((rc = chebfsi_step(sv, dn, nb, degree, a, up, a0))) break;
+      a = sv.eig[nb - 1];
+      a0 = sv.eig[0];
+      if ((rc = residuals(sv, nb))) break;
+      if (*std::max_element(sv.res.begin(), sv.res.end()) < tol) break;
+    }
+    it = std::min(it, maxit);
+  }
+  if (rc) return rc;
+  if (sv.res.empty() && (rc = residuals(sv, nb))) return rc;
+  PWB_CUDA(cudaMemcpy(X, sv.X.p, (size_t)nb * sv.nt * sv.esz, cudaMemcpyDeviceToDevice));
+  if (eig) std::copy(sv.eig.begin(), sv.eig.end(), eig);
+  if (resnorm) std::copy(sv.res.begin(), sv.res.end(), resnorm);
+  if (iters) *iters = it;
+  PWB_CUDA(cudaDeviceSynchronize());
+  dn.release();
+  return PW_OK;
+}
+
+int pw_density(pw_ctx* ctx, const void* psi, int ld, int nband, const double* occ_host, int nocc_total,
+               double* rho_dev) {
+  PWB_CHECK(ctx && psi && occ_host && rho_dev && nband > 0, PW_EINVAL, "bad arguments");
+  PWB_CUDA(cudaSetDevice(ctx->device));
+  DevBuf wv;
+  int rc = wv.alloc((nband + 2) * 8);
+  if (rc) return rc;
+  std::vector<double> h(nband + 2, 0.0);
+  for (int i = 0; i < nband; ++i) h[i] = 2.0 * occ_host[i];
+  PWB_CUDA(cudaMemcpy(wv.p, h.data(), h.size() * 8, cudaMemcpyHostToDevice));
+  PWB_CUDA(cudaMemset(rho_dev, 0, ctx->ntotf * 8));
+  const int cap = ctx->pair_cap;
+  for (int b0 = 0; b0 < nband; b0 += 2 * cap) {
+    const int npair = std::min(cap, (nband - b0 + 1) / 2);
+    if ((rc = run_density(ctx, psi, ld, nband, b0, npair, (const double*)wv.p, rho_dev, nullptr))) return rc;
+  }
+  // renormalise to 2 * nocc electrons (hamiltonian.cpp:2596-2600)
+  DevBuf d;
+  if ((rc = d.alloc(64))) return rc;
+  PWB_CUDA(cudaMemset(d.p, 0, 64));
+  DotSet ds{};
+  ds.k = 1;
+  ds.a[0] = rho_dev;
+  ds.b[0] = nullptr;
+  k_dots<<<nblk(ctx->ntotf), 256>>>(ctx->ntotf, ds, (double*)d.p);
+  double tot;
+  PWB_CUDA(cudaMemcpy(&tot, d.p, 8, cudaMemcpyDeviceToHost));
+  k_lincomb<<<nblk(ctx->ntotf), 256>>>(ctx->ntotf, (2.0 * nocc_total * (double)ctx->ntotf) / (ctx->vol * tot), rho_dev,
+                                       0.0, nullptr, rho_dev);
+  PWB_CUDA(cudaDeviceSynchronize());
+  return PW_OK;
+}
+
+}  // extern "C"
