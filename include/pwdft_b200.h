@@ -189,6 +189,17 @@ PW_API int pw_eigsolve(pw_ctx* ctx, int solver, void* X, int nb, int maxit, doub
 PW_API int pw_density(pw_ctx* ctx, const void* psi, int ld, int nband, const double* occ_host, int nocc_total,
                       double* rho_dev);
 
+/* Hartree potential of a charge on the fine grid (device, N_fine doubles):
+ * V_H = IFFT(2 pi / gkk * FFT(drho)) with gkk = |G|^2 / 2, zero for
+ * gkk <= 1e-16 or gkk > 4*ecut -- KohnSham::CalculateHartree
+ * (src/SCF/hamiltonian.cpp:1990-2026) with drho = rho - pseudocharge.
+ * Cubic fine grids. */
+PW_API int pw_hartree(pw_ctx* ctx, const double* drho_dev, double ecut, double* vh_dev);
+/* LDA Teter93 exchange-correlation energy density and potential on the fine
+ * grid (device), points with rho < 1e-10 zeroed -- KohnSham::CalculateXC
+ * (src/SCF/hamiltonian.cpp:1278-1308). */
+PW_API int pw_xc_teter93(pw_ctx* ctx, const double* rho_dev, double* eps_dev, double* vxc_dev);
+
 typedef struct pw_scf_params {
   int nocc;                 /* occupied states (numOccupiedState) */
   int nextra;               /* Extra_States */

@@ -71,6 +71,8 @@ SIGNATURES: dict[str, tuple] = {
     "pw_set_check_errors": (_i, [_vp, _i]),
     "pw_gram": (_i, [_vp, _vp, _i, _i, _vp, _i, _i, _vp, _i, _vp]),
     "pw_cholqr": (_i, [_vp, _vp, _i]),
+    "pw_hartree": (_i, [_vp, _vp, _d, _vp]),
+    "pw_xc_teter93": (_i, [_vp, _vp, _vp, _vp]),
     "pw_eigsolve": (_i, [_vp, _i, _vp, _i, _i, _d, _i, _dp, _dp, _ip]),
     "pw_density": (_i, [_vp, _vp, _i, _i, _dp, _i, _vp]),
     "pw_scf_run": (_i, [_vp, C.POINTER(ScfParams), C.POINTER(ScfResult), _dp, _dp]),

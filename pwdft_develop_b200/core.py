@@ -293,6 +293,22 @@ def _ctx_scf(self, nocc: int, nextra: int, ecut: float, solver: str = "chebfsi",
     return res, eig, rho
 
 
+def _ctx_hartree(self, drho, ecut: float):
+    import torch
+    vh = torch.empty_like(drho)
+    check(lib.pw_hartree(self._h, _ptr(drho), float(ecut), _ptr(vh)))
+    return vh
+
+
+def _ctx_xc(self, rho):
+    import torch
+    eps, v = torch.empty_like(rho), torch.empty_like(rho)
+    check(lib.pw_xc_teter93(self._h, _ptr(rho), _ptr(eps), _ptr(v)))
+    return eps, v
+
+
+Context.hartree = _ctx_hartree
+Context.xc = _ctx_xc
 Context.cholqr = _ctx_cholqr
 Context.eigsolve = _ctx_eigsolve
 Context.density = _ctx_density

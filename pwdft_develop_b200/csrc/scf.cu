@@ -123,8 +123,8 @@ template <int N> static int hartree_n(double2* work, const double* rho, const do
   k_fft_axis<N, -1, 1, 0><<<dim3(nxt, N), AX_THREADS, 0, st>>>(work, N, N, N, nullptr, nullptr, nullptr, nullptr, 1.0, tw);
   k_fft_axis<N, -1, 2, 2><<<dim3(nxt, N), AX_THREADS, 0, st>>>(work, N, N, N, nullptr, nullptr, kern, nullptr, 1.0, tw);
   k_fft_axis<N, +1, 1, 0><<<dim3(nxt, N), AX_THREADS, 0, st>>>(work, N, N, N, nullptr, nullptr, nullptr, nullptr, 1.0, tw);
-  k_fft_axis<N, +1, 0, 3><<<nrowtiles, AX_THREADS, 0, st>>>(work, N, N, N, nullptr, nullptr, nullptr, vh,
-                                                             1.0 / ((double)N * N * N), tw);
+  // kern already carries the 1/N normalisation of the unnormalised transforms
+  k_fft_axis<N, +1, 0, 3><<<nrowtiles, AX_THREADS, 0, st>>>(work, N, N, N, nullptr, nullptr, nullptr, vh, 1.0, tw);
   PWB_CUDA(cudaGetLastError());
   return PW_OK;
 }
@@ -906,6 +906,45 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
   if (eig_out) std::copy(eig.begin(), eig.end(), eig_out);
   if (rho_out) PWB_CUDA(cudaMemcpy(rho_out, rho, nf * 8, cudaMemcpyDeviceToHost));
   dn.release();
+  return PW_OK;
+}
+
+int pw_hartree(pw_ctx* ctx, const double* drho_dev, double ecut, double* vh_dev) {
+  PWB_CHECK(ctx && drho_dev && vh_dev && ecut > 0, PW_EINVAL, "bad arguments");
+  PWB_CUDA(cudaSetDevice(ctx->device));
+  const long nf = ctx->ntotf;
+  DevBuf kern, work, tw;
+  int rc;
+  if ((rc = kern.alloc(nf * 8)) || (rc = work.alloc(nf * 16)) || (rc = tw.alloc(ctx->nf[0] * 16))) return rc;
+  std::vector<double> k(nf);
+  const int N0 = ctx->nf[0], N1 = ctx->nf[1], N2 = ctx->nf[2];
+  for (int z = 0; z < N2; ++z)
+    for (int y = 0; y < N1; ++y)
+      for (int x = 0; x < N0; ++x) {
+        const double m0 = x <= N0 / 2 ? x : x - N0, m1 = y <= N1 / 2 ? y : y - N1, m2 = z <= N2 / 2 ? z : z - N2;
+        const double g0 = 2 * M_PI / ctx->L[0] * m0, g1 = 2 * M_PI / ctx->L[1] * m1, g2 = 2 * M_PI / ctx->L[2] * m2;
+        const double gkk = (g0 * g0 + g1 * g1 + g2 * g2) / 2;
+        k[x + (size_t)N0 * (y + (size_t)N1 * z)] = (gkk <= 1e-16 || gkk > 4.0 * ecut) ? 0.0 : 2.0 * M_PI / gkk / (double)nf;
+      }
+  PWB_CUDA(cudaMemcpy(kern.p, k.data(), nf * 8, cudaMemcpyHostToDevice));
+  std::vector<double> t(2 * N0);
+  for (int m = 0; m < N0; ++m) {
+    t[2 * m] = std::cos(2 * M_PI * m / N0);
+    t[2 * m + 1] = -std::sin(2 * M_PI * m / N0);
+  }
+  PWB_CUDA(cudaMemcpy(tw.p, t.data(), N0 * 16, cudaMemcpyHostToDevice));
+  rc = hartree(ctx, (double2*)work.p, drho_dev, nullptr, (const double*)kern.p, vh_dev, (const double2*)tw.p, nullptr);
+  if (rc) return rc;
+  PWB_CUDA(cudaDeviceSynchronize());
+  return PW_OK;
+}
+
+int pw_xc_teter93(pw_ctx* ctx, const double* rho_dev, double* eps_dev, double* vxc_dev) {
+  PWB_CHECK(ctx && rho_dev && eps_dev && vxc_dev, PW_EINVAL, "bad arguments");
+  PWB_CUDA(cudaSetDevice(ctx->device));
+  k_xc_teter93<<<nblk(ctx->ntotf), 256>>>(ctx->ntotf, rho_dev, eps_dev, vxc_dev);
+  PWB_CUDA(cudaGetLastError());
+  PWB_CUDA(cudaDeviceSynchronize());
   return PW_OK;
 }
 

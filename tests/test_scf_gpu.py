@@ -39,6 +39,27 @@ def test_density_matches_oracle(prec, tol):
     assert abs(rho.sum() * T.dm.vol / T.dm.ntotFine - 32.0) < 1e-9
 
 
+@pytest.mark.parametrize("nc", [(16, 16, 16), (48, 48, 48)])
+def test_hartree_and_xc_match_oracle(nc):
+    import torch
+    L, z, pos, _, _ = _si8()
+    if nc[0] == 48:
+        L, z, pos = pw.make_crystal("Si", (2, 2, 2), 10.26, 0.02, 7)
+    nf = tuple(2 * n for n in nc)
+    dm = pw.Domain(tuple(L), nc, nf)
+    rng = np.random.default_rng(3)
+    rho = rng.uniform(0.0, 0.1, dm.ntotFine)
+    rps = rng.uniform(0.0, 0.1, dm.ntotFine)
+    ref = scf.hartree(dm, rho, rps, 10.0)
+    c = _ctx(L, z, pos, nc, nf)
+    vh = c.hartree(torch.tensor(rho - rps, device="cuda"), 10.0).cpu().numpy()
+    assert np.abs(vh - ref).max() / np.abs(ref).max() < 1e-12
+    rho[::97] = 1e-12     # bad points
+    e_ref, v_ref = scf.xc_teter93(rho)
+    e, v = c.xc(torch.tensor(rho, device="cuda"))
+    assert np.abs(e.cpu().numpy() - e_ref).max() < 1e-14 and np.abs(v.cpu().numpy() - v_ref).max() < 1e-14
+
+
 def test_cholqr_orthonormalises():
     import torch
     L, z, pos, nc, nf = _si8()
