@@ -186,6 +186,38 @@ def cpu_baseline(bands: int = 4):
                       f"restatement (oracle/pw.py), one thread, {dt:.1f} s"}
 
 
+def scf_bench(device: int, max_iter: int = 60):
+    """SCF time to |E_free - E_Harris| / N_atom < 1e-6 Ha/atom on Si64 with
+    ChebFSI (degree 10): plain FP64 against the mixed form (FP32 H*psi and
+    Chebyshev filter, split-BF16 tensor-core Gram products, FP64 Cholesky /
+    Rayleigh-Ritz / mixing, FP64 refinement in the last iterations).  Each run
+    is bracketed by CUDA events on the device."""
+    import torch
+    from pwdft_develop_b200 import Context
+    L, z, pos = si64_atoms()
+    out = {}
+    for mode in ("f64", "mixed"):
+        c = Context(L, NC, NF, precision="f64", device=device)
+        c.set_atoms(z, pos)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        res, eig, _ = c.scf(nocc=128, nextra=32, ecut=20.0, solver="chebfsi", mixed=(mode == "mixed"),
+                            cheby_degree=10, cheby_first_cycles=5, tol_efree=1e-6, refine_threshold=1e-5,
+                            max_iter=max_iter, seed=SEED)
+        e1.record()
+        torch.cuda.synchronize()
+        out[mode] = dict(seconds=e0.elapsed_time(e1) / 1e3, iterations=res["iterations"],
+                         converged=bool(res["converged"]), efree=res["efree"], etot=res["etot"],
+                         refine_iter=res["refine_iter"], hpsi_bands=res["hpsi_bands"], homo=float(eig[127]),
+                         lumo=float(eig[128]))
+        c.close()
+    out["speedup_mixed_vs_f64"] = out["f64"]["seconds"] / out["mixed"]["seconds"]
+    out["efree_agreement_per_atom"] = abs(out["f64"]["efree"] - out["mixed"]["efree"]) / 64
+    out["workload"] = "Si64, ChebFSI degree 10 (5 cycles in the first SCF step), Anderson(8, 0.7), 300 K, tol 1e-6 Ha/atom"
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -351,6 +383,8 @@ def run_ours(args):
                     "h2d_bytes_per_step": bytes_io, "d2h_bytes_per_step": bytes_io},
             "clocks": ck,
         }
+        if args.scf and world == 1:
+            line["scf"] = scf_bench(local)
         if args.cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(args.cpu_bands)
         print(json.dumps(line), flush=True)
@@ -368,6 +402,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--no-scf", dest="scf", action="store_false", help="skip the SCF time-to-solution leg")
     ap.add_argument("--cpu-bands", type=int, default=64)
     ap.add_argument("--bands", type=int, default=NBAND, help="band block size (profiling runs use a small block)")
     args = ap.parse_args()
