@@ -234,6 +234,23 @@ typedef struct pw_scf_result {
  * doubles; rho_out: host, N_fine doubles (either may be NULL). */
 PW_API int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* eig_out, double* rho_out);
 
+/* Teter preconditioner that allocates nothing (no counterpart in the
+ * reference).  Same result as pw_teter_precond; for callers that cannot call
+ * cudaMalloc where they need it -- code inside CUDA stream capture, hosts that
+ * forbid device allocation after start-up, frameworks whose own memory pool
+ * must not see the device heap change.  Its working memory is one fixed
+ * 16 MiB device array in the library (held by every GPU that loads it until
+ * the process exits), so a grid whose single band pair needs more than
+ * 16 MiB (ntot * 2 * sizeof(real) bytes) is rejected with PW_EINVAL; larger
+ * band counts run in batches that fit.  The first call on a device looks up
+ * the array's device address: make that first call before any stream
+ * capture.  All calls share the array (each call writes every element it
+ * reads, so nothing needs clearing between calls); calls that overlap on the
+ * GPU -- concurrent streams, devices sharing the process' array on the same
+ * device -- race on it and must be serialised by the caller. */
+PW_API int pw_teter_precond_noalloc(pw_ctx* ctx, const void* r, int ld, void* w, int ldw, int nband, int accumulate,
+                                    void* stream);
+
 /* Maximum number of bands processed per internal batch (sets scratch size).
  * Default 64. Scratch grows to hold ceil(nband_batch/2) band pairs. */
 PW_API int pw_set_band_batch(pw_ctx* ctx, int nband_batch);

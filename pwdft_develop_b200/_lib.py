@@ -65,6 +65,7 @@ SIGNATURES: dict[str, tuple] = {
     "pw_hpsi": (_i, [_vp, _vp, _i, _vp, _i, _i, _i, _vp]),
     "pw_hpsi_host": (_i, [_vp, _vp, _i, _vp, _i, _i, _i]),
     "pw_teter_precond": (_i, [_vp, _vp, _i, _vp, _i, _i, _i, _vp]),
+    "pw_teter_precond_noalloc": (_i, [_vp, _vp, _i, _vp, _i, _i, _i, _vp]),
     "pw_set_band_batch": (_i, [_vp, _i]),
     "pw_set_nonlocal_mode": (_i, [_vp, _i]),
     "pw_set_gemm_mode": (_i, [_vp, _i, _i]),

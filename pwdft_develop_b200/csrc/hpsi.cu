@@ -22,6 +22,9 @@
 //   k_cxy_inv    coarse plane: IFFT y, IFFT x, (accumulate) into hpsi   D -> hpsi
 #include <cublas_v2.h>
 
+#include <mutex>
+#include <string>
+
 #include "common.hpp"
 #include "fft.cuh"
 #include "gemm.hpp"
@@ -978,6 +981,25 @@ struct Plan {
     PWB_CUDA(cudaGetLastError());
     return PW_OK;
   }
+
+  // Teter preconditioner with caller-provided device scratch (npair complex
+  // coarse fields); launches kernels only, allocates nothing.
+  static int teter_batch_scratch(pw_ctx* c, const T* r, int ld, T* out, int ldo, int nband, int band0, int npair,
+                                 int accumulate, cudaStream_t st, void* scratch) {
+    int rc = set_attrs();
+    if (rc) return rc;
+    V* AD = reinterpret_cast<V*>(scratch);
+    const T inv_nc = (T)(1.0 / (double)c->ntot);
+    const int ntx = (N0 + TX - 1) / TX;
+    c->launches += 3;
+    k_cxy_fwd<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(r, ld, nband, band0, AD, tw(c, 0), tw(c, 1));
+    k_zteter<T, N2><<<dim3(N1, ntx, npair), PENCIL_THREADS, sm_zteter(), st>>>(
+        AD, reinterpret_cast<const T*>(c->teter.p), N0, N1, inv_nc, tw(c, 2));
+    k_cxy_inv<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(AD, out, ldo, nband, band0, accumulate,
+                                                                            tw(c, 0), tw(c, 1));
+    PWB_CUDA(cudaGetLastError());
+    return PW_OK;
+  }
 };
 
 // ---------------------------------------------------------------------------
@@ -999,6 +1021,13 @@ static int teter_thunk(pw_ctx* c, const void* psi, int ld, void* out, int ldo, i
 template <typename T, int N0, int N1, int N2> static int cr_thunk() { return Plan<T, N0, N1, N2>::chunk_rows(); }
 using BuildQFn = int (*)(pw_ctx*, const int*, const double*, const long*, const long*, const int*, int, cudaStream_t);
 using DensFn = int (*)(pw_ctx*, const void*, int, int, int, int, const double*, double*, cudaStream_t);
+using TeterScratchFn = int (*)(pw_ctx*, const void*, int, void*, int, int, int, int, int, cudaStream_t, void*);
+template <typename T, int N0, int N1, int N2>
+static int teter_scratch_thunk(pw_ctx* c, const void* r, int ld, void* out, int ldo, int nband, int band0, int npair,
+                               int acc, cudaStream_t st, void* scratch) {
+  return Plan<T, N0, N1, N2>::teter_batch_scratch(c, (const T*)r, ld, (T*)out, ldo, nband, band0, npair, acc, st,
+                                                  scratch);
+}
 template <typename T, int N0, int N1, int N2>
 static int dens_thunk(pw_ctx* c, const void* psi, int ld, int nband, int band0, int npair, const double* w, double* rho,
                       cudaStream_t st) {
@@ -1017,6 +1046,7 @@ struct GridEntry {
   ChunkFn cr[2];
   BuildQFn bq[2];
   DensFn dens[2];
+  TeterScratchFn teter_scratch[2];
 };
 
 #define PWB_GRID(a, b, c)                                                                          \
@@ -1024,7 +1054,8 @@ struct GridEntry {
    {teter_thunk<double, a, b, c>, teter_thunk<float, a, b, c>},                                    \
    {cr_thunk<double, a, b, c>, cr_thunk<float, a, b, c>},                                          \
    {buildq_thunk<double, a, b, c>, buildq_thunk<float, a, b, c>},                                  \
-   {dens_thunk<double, a, b, c>, dens_thunk<float, a, b, c>}},
+   {dens_thunk<double, a, b, c>, dens_thunk<float, a, b, c>},                                      \
+   {teter_scratch_thunk<double, a, b, c>, teter_scratch_thunk<float, a, b, c>}},
 
 static const GridEntry kGrids[] = {
 #include "grids.inc"
@@ -1071,3 +1102,65 @@ int run_teter(pw_ctx* c, const void* r, int ld, void* out, int ldo, int nband, i
 }
 
 }  // namespace pwb
+
+// ---------------------------------------------------------------------------
+// Allocation-free Teter preconditioner.
+//
+// Some callers cannot call cudaMalloc at the point where they need the
+// preconditioner: code running while a CUDA stream is being captured into a
+// graph, real-time or embedded hosts that forbid device allocation after
+// start-up, and allocator-owning frameworks (a host code with its own memory
+// pool) that must not see device memory change underneath them.  For them the
+// entry point pw_teter_precond_noalloc below takes its working memory from one
+// fixed array in this file instead of the context's scratch.
+// ---------------------------------------------------------------------------
+#define PWB_NOALLOC_SCRATCH_BYTES (16u << 20)    // 16 MiB per GPU that loads the library
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[PWB_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[64] = {nullptr};   // device address of g_noalloc_scratch, per device ordinal
+}  // namespace
+
+extern "C" int pw_teter_precond_noalloc(pw_ctx* ctx, const void* r, int ld, void* w, int ldw, int nband,
+                                        int accumulate, void* stream) {
+  using namespace pwb;
+  PWB_CHECK(ctx && (nband == 0 || (r && w)), PW_EINVAL, "null argument");
+  PWB_CHECK(nband >= 0 && ld >= ctx->ntot && ldw >= ctx->ntot, PW_EINVAL, "Domain size does not match.");
+  PWB_CHECK(ctx->device >= 0 && ctx->device < 64, PW_EINVAL, "device ordinal out of range");
+  if (nband == 0) return PW_OK;
+  // one band pair needs ntot complex values of the context's precision
+  const size_t pair_bytes = (size_t)ctx->ntot * 2 * ctx->esz;
+  PWB_CHECK(pair_bytes <= PWB_NOALLOC_SCRATCH_BYTES, PW_EINVAL,
+            "pw_teter_precond_noalloc: one band pair needs " + std::to_string(pair_bytes) +
+                " bytes of scratch, more than the fixed 16 MiB array; use pw_teter_precond");
+  PWB_CUDA(cudaSetDevice(ctx->device));
+  void* scratch;
+  {
+    // host code may not use g_noalloc_scratch as a pointer (it names a host-side
+    // stand-in); fetch the device address once per device
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_addr[ctx->device]) {
+      void* ptr = nullptr;
+      cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+      if (e != cudaSuccess || !ptr) {
+        set_error(std::string("cudaGetSymbolAddress(g_noalloc_scratch) failed: ") + cudaGetErrorString(e));
+        return PW_ECUDA;
+      }
+      g_noalloc_addr[ctx->device] = ptr;
+    }
+    scratch = g_noalloc_addr[ctx->device];
+  }
+  const GridEntry* g = find_grid(ctx->n);
+  PWB_CHECK(g, PW_EUNSUPPORTED, "grid not built into this library");
+  const int max_pairs = (int)(PWB_NOALLOC_SCRATCH_BYTES / pair_bytes);
+  cudaStream_t st = (cudaStream_t)stream;
+  for (int b0 = 0; b0 < nband; b0 += 2 * max_pairs) {
+    const int npair = std::min(max_pairs, (nband - b0 + 1) / 2);
+    int rc = g->teter_scratch[ctx->prec == PW_F32 ? 1 : 0](ctx, r, ld, w, ldw, nband, b0, npair, accumulate, st,
+                                                           scratch);
+    if (rc) return rc;
+  }
+  return PW_OK;
+}
