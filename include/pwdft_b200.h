@@ -224,7 +224,14 @@ typedef struct pw_scf_result {
   double etot, efree, eharris, exc, ehart, eself, fermi, time_s;
   int iterations, converged, refine_iter;
   long hpsi_bands;          /* single-band H*psi applications performed */
+  double phase_s[6];        /* verbose >= 2: eigensolver, density, potentials, energies, mixing, other (s) */
+  double sub_s[4];          /* verbose >= 2, inside the eigensolver: H*psi, Gram, dense FP64, rotations (s) */
 } pw_scf_result;
+
+/* Build (once) the FP32 twin of an FP64 context with the same cell, grids and
+ * atoms; the mixed-precision SCF runs its eigensolver there.  Set-up work:
+ * call it after pw_set_atoms, before timing an SCF. */
+PW_API int pw_ctx_build_twin(pw_ctx* ctx);
 
 /* Self-consistent field iteration for the atoms of an FP64 context
  * (pw_set_atoms): SCF::Iterate / InnerSolve with potential Anderson mixing

@@ -50,7 +50,8 @@ class ScfResult(C.Structure):
     _fields_ = [("etot", C.c_double), ("efree", C.c_double), ("eharris", C.c_double), ("exc", C.c_double),
                 ("ehart", C.c_double), ("eself", C.c_double), ("fermi", C.c_double), ("time_s", C.c_double),
                 ("iterations", C.c_int), ("converged", C.c_int), ("refine_iter", C.c_int),
-                ("hpsi_bands", C.c_long)]
+                ("hpsi_bands", C.c_long), ("phase_s", C.c_double * 6),
+                ("sub_s", C.c_double * 4)]
 
 
 # name -> (restype, argtypes); every name here is declared in include/pwdft_b200.h
@@ -72,6 +73,7 @@ SIGNATURES: dict[str, tuple] = {
     "pw_set_check_errors": (_i, [_vp, _i]),
     "pw_gram": (_i, [_vp, _vp, _i, _i, _vp, _i, _i, _vp, _i, _vp]),
     "pw_cholqr": (_i, [_vp, _vp, _i]),
+    "pw_ctx_build_twin": (_i, [_vp]),
     "pw_hartree": (_i, [_vp, _vp, _d, _vp]),
     "pw_xc_teter93": (_i, [_vp, _vp, _vp, _vp]),
     "pw_eigsolve": (_i, [_vp, _i, _vp, _i, _i, _d, _i, _dp, _dp, _ip]),

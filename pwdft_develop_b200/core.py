@@ -290,7 +290,13 @@ def _ctx_scf(self, nocc: int, nextra: int, ecut: float, solver: str = "chebfsi",
     rho = np.zeros(self.ntotFine)
     check(lib.pw_scf_run(self._h, C.byref(p), C.byref(r), eig.ctypes.data_as(_lib._dp), rho.ctypes.data_as(_lib._dp)))
     res = {k: getattr(r, k) for k, _ in r._fields_}
+    res["phase_s"] = list(r.phase_s)
+    res["sub_s"] = list(r.sub_s)
     return res, eig, rho
+
+
+def _ctx_build_twin(self):
+    check(lib.pw_ctx_build_twin(self._h))
 
 
 def _ctx_hartree(self, drho, ecut: float):
@@ -313,3 +319,4 @@ Context.cholqr = _ctx_cholqr
 Context.eigsolve = _ctx_eigsolve
 Context.density = _ctx_density
 Context.scf = _ctx_scf
+Context.build_twin = _ctx_build_twin

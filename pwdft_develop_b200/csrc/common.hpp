@@ -97,6 +97,7 @@ struct pw_ctx {
   int gemm_mode = 0;             // 0 tensor-core split-BF16, 1 vendor SGEMM
   int gemm_terms = 3;            // split products per k-step (3 or 4)
   bool check_errors = false;     // read the device error flag after each call (synchronises)
+  pw_ctx* twin = nullptr;        // FP32 twin of an FP64 context (mixed-precision SCF), owned
   int nproj_pad = 0;
   pwb::DevBuf q_bf, qt_bf, s_psi_bf, s_w_bf, s_ws, s_gx_bf, s_gy_bf, s_rot;
   // host copies kept for setup-time work

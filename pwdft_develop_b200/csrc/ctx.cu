@@ -170,6 +170,7 @@ int pw_ctx_destroy(pw_ctx* ctx) {
   for (auto& r : ctx->prof) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
   for (auto e : ctx->ev_pool) cudaEventDestroy(e);
   if (ctx->blas) cublasDestroy((cublasHandle_t)ctx->blas);
+  if (ctx->twin) pw_ctx_destroy(ctx->twin);
   delete ctx;
   return PW_OK;
 }

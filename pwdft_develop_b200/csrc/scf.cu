@@ -214,7 +214,25 @@ struct Solver {
   void* ptr(DevBuf& b, long col = 0) { return (char*)b.p + (size_t)col * nt * esz; }
 };
 
+// eigensolver sub-phase timers (H*psi, Gram, dense FP64, rotations), seconds
+static bool g_sub_on = false;
+static double g_sub[4] = {0, 0, 0, 0};
+struct SubTimer {
+  int k;
+  std::chrono::steady_clock::time_point t0;
+  explicit SubTimer(int k_) : k(k_) {
+    if (g_sub_on) { cudaDeviceSynchronize(); t0 = std::chrono::steady_clock::now(); }
+  }
+  ~SubTimer() {
+    if (g_sub_on) {
+      cudaDeviceSynchronize();
+      g_sub[k] += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+  }
+};
+
 static int hpsi(pw_ctx* c, const void* x, void* y, int nb, cudaStream_t st) {
+  SubTimer t_(0);
   return pw_hpsi(c, x, (int)c->ntot, y, (int)c->ntot, nb, 0, st);
 }
 
@@ -241,7 +259,8 @@ static int cholqr(Solver& s, Dense& d, void* X, int nb, void* tmp) {
   int rc;
   if ((rc = s.G1.alloc((size_t)nb * nb * 8))) return rc;
   double* G = (double*)s.G1.p;
-  if ((rc = gram(s.c, X, (int)s.nt, nb, X, (int)s.nt, nb, G, nb, st))) return rc;
+  { SubTimer t_(1); if ((rc = gram(s.c, X, (int)s.nt, nb, X, (int)s.nt, nb, G, nb, st))) return rc; }
+  SubTimer td_(2);
   if ((rc = d.potrf_upper(nb, G, nb, st))) return rc;
   // Uinv = U^{-1} (upper): solve U * Uinv = I
   if ((rc = s.G2.alloc((size_t)nb * nb * 8))) return rc;
@@ -263,7 +282,7 @@ static int cholqr(Solver& s, Dense& d, void* X, int nb, void* tmp) {
     return PW_ECUDA;
   }
   RotBlock rb{X, s.nt, nb, Ui, nb};
-  if ((rc = rotate(s.c, (int)s.nt, nb, &rb, 1, tmp, s.nt, 0.0, st))) return rc;
+  { SubTimer t_(3); if ((rc = rotate(s.c, (int)s.nt, nb, &rb, 1, tmp, s.nt, 0.0, st))) return rc; }
   PWB_CUDA(cudaMemcpy(X, tmp, (size_t)nb * s.nt * s.esz, cudaMemcpyDeviceToDevice));
   return PW_OK;
 }
@@ -274,7 +293,7 @@ static int rayleigh_ritz(Solver& s, Dense& d, void* Y, void* HY, void* X, void* 
   int rc;
   if ((rc = s.G1.alloc((size_t)nb * nb * 8)) || (rc = s.wbuf.alloc((size_t)nb * 8 * 2))) return rc;
   double* A = (double*)s.G1.p;
-  if ((rc = gram(s.c, Y, (int)s.nt, nb, HY, (int)s.nt, nb, A, nb, nullptr))) return rc;
+  { SubTimer t_(1); if ((rc = gram(s.c, Y, (int)s.nt, nb, HY, (int)s.nt, nb, A, nb, nullptr))) return rc; }
   // symmetrise from the upper triangle
   std::vector<double> ha((size_t)nb * nb);
   PWB_CUDA(cudaMemcpy(ha.data(), A, ha.size() * 8, cudaMemcpyDeviceToHost));
@@ -282,9 +301,10 @@ static int rayleigh_ritz(Solver& s, Dense& d, void* Y, void* HY, void* X, void* 
     for (int i = j + 1; i < nb; ++i) ha[(size_t)j * nb + i] = ha[(size_t)i * nb + j];
   PWB_CUDA(cudaMemcpy(A, ha.data(), ha.size() * 8, cudaMemcpyHostToDevice));
   double* w = (double*)s.wbuf.p;
-  if ((rc = d.syevd(nb, A, nb, w, nullptr))) return rc;
+  { SubTimer t_(2); if ((rc = d.syevd(nb, A, nb, w, nullptr))) return rc; }
   s.eig.resize(nb);
   PWB_CUDA(cudaMemcpy(s.eig.data(), w, nb * 8, cudaMemcpyDeviceToHost));
+  SubTimer t_(3);
   RotBlock r1{Y, s.nt, nb, A, nb};
   if ((rc = rotate(s.c, (int)s.nt, nb, &r1, 1, X, s.nt, 0.0, nullptr))) return rc;
   RotBlock r2{HY, s.nt, nb, A, nb};
@@ -553,12 +573,23 @@ namespace {
 struct ScfState {
   pw_ctx* c64 = nullptr;
   pw_ctx* c32 = nullptr;
-  bool own32 = false;
   DevBuf rho, rho_out, rps, vtot, vtot_new, vxc, eps, vh, kern, work, tw, dots, wocc;
   DevBuf dvh, dfh, dif_v, dif_f;   // Anderson history [mixdim][nf] and differences
   int nhist = 0, hpos = 0;
-  ~ScfState() {
-    if (own32 && c32) pw_ctx_destroy(c32);
+};
+
+struct PhaseTimer {
+  bool on;
+  std::chrono::steady_clock::time_point t0;
+  double* acc;
+  PhaseTimer(bool on_, double* acc_) : on(on_), acc(acc_) {
+    if (on) { cudaDeviceSynchronize(); t0 = std::chrono::steady_clock::now(); }
+  }
+  ~PhaseTimer() {
+    if (on) {
+      cudaDeviceSynchronize();
+      *acc += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
   }
 };
 
@@ -631,13 +662,14 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
   const int natom = (int)ctx->atom_z.size();
   int rc;
   if (p->mixed) {
-    pw_ctx* c32 = nullptr;
-    if ((rc = pw_ctx_create(ctx->L, ctx->n, ctx->nf, PW_F32, ctx->device, &c32))) return rc;
-    S.c32 = c32;
-    S.own32 = true;
-    if ((rc = pw_set_band_batch(c32, nb))) return rc;
-    if ((rc = pw_set_atoms(c32, natom, ctx->atom_z.data(), ctx->atom_pos.data()))) return rc;
+    if (!ctx->twin && (rc = pw_ctx_build_twin(ctx))) return rc;
+    S.c32 = ctx->twin;
+    if ((rc = pw_set_band_batch(S.c32, nb))) return rc;
   }
+  const bool prof = p->verbose >= 2;
+  g_sub_on = prof;
+  for (double& x : g_sub) x = 0;
+  double tph[6] = {0, 0, 0, 0, 0, 0};   // eigensolver, density, potentials, energies, mixing, refine switch
   if ((rc = pw_set_band_batch(ctx, nb))) return rc;
   // device arrays
   for (DevBuf* b : {&S.rho, &S.rho_out, &S.rps, &S.vtot, &S.vtot_new, &S.vxc, &S.eps, &S.vh, &S.kern})
@@ -738,6 +770,8 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
   r->hpsi_bands = 0;
   for (it = 1; it <= p->max_iter; ++it) {
     if ((rc = set_vtot_dev(sv.c, (const double*)S.vtot.p))) return rc;
+    {
+    PhaseTimer pt_(prof, &tph[0]);
     if (p->solver == PW_SOLVER_CHEBFSI) {
       if (!have_bounds) {
         double lo;
@@ -765,6 +799,7 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
       if ((rc = lobpcg(sv, dn, nb, p->eig_max_iter, tolnow, it == 1, &li))) return rc;
       r->hpsi_bands += (long)nb * (2 * li + 1);
     }
+    }
     eig = sv.eig;
     occupations(eig, p->nocc, tbeta, occ, ef);
     double ekin = 0, ent = 0;
@@ -780,6 +815,7 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
     eharris = ekin + (exc - evxc) - ehart_h - eself + ent;
     // new density
     {
+      PhaseTimer pt_(prof, &tph[1]);
       std::vector<double> wv(nb + 2, 0.0);
       for (int i = 0; i < nb; ++i) wv[i] = 2.0 * occ[i];
       PWB_CUDA(cudaMemcpy(S.wocc.p, wv.data(), wv.size() * 8, cudaMemcpyHostToDevice));
@@ -795,7 +831,10 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
       k_lincomb<<<nblk(nf), 256>>>(nf, (2.0 * p->nocc * (double)nf) / (ctx->vol * tot), ro, 0.0, nullptr, ro);
     }
     double* ro = (double*)S.rho_out.p;
-    if ((rc = potentials(ro, &exc))) return rc;
+    {
+      PhaseTimer pt_(prof, &tph[2]);
+      if ((rc = potentials(ro, &exc))) return rc;
+    }
     k_lincomb<<<nblk(nf), 256>>>(nf, 1.0, (double*)S.vh.p, 1.0, (double*)S.vxc.p, (double*)S.vtot_new.p);
     double ed[2];
     if ((rc = dots(S, nf, {{(const double*)S.vtot.p, ro}, {(const double*)S.vh.p, ro}}, ed))) return rc;
@@ -827,6 +866,7 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
     }
     // Anderson mixing of the potential (scf.cpp:2299-2365)
     {
+      PhaseTimer pt_(prof, &tph[4]);
       double* vin = (double*)S.vtot.p;
       double* vout = (double*)S.vtot_new.p;
       double* F = vout;   // F = vout - vin (in place)
@@ -903,6 +943,9 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
   r->iterations = std::min(it, p->max_iter);
   r->converged = conv ? 1 : 0;
   r->time_s = std::chrono::duration<double>(t_end - t_start).count();
+  for (int i = 0; i < 6; ++i) r->phase_s[i] = tph[i];
+  for (int i = 0; i < 4; ++i) r->sub_s[i] = g_sub[i];
+  g_sub_on = false;
   if (eig_out) std::copy(eig.begin(), eig.end(), eig_out);
   if (rho_out) PWB_CUDA(cudaMemcpy(rho_out, rho, nf * 8, cudaMemcpyDeviceToHost));
   dn.release();
@@ -945,6 +988,22 @@ int pw_xc_teter93(pw_ctx* ctx, const double* rho_dev, double* eps_dev, double* v
   k_xc_teter93<<<nblk(ctx->ntotf), 256>>>(ctx->ntotf, rho_dev, eps_dev, vxc_dev);
   PWB_CUDA(cudaGetLastError());
   PWB_CUDA(cudaDeviceSynchronize());
+  return PW_OK;
+}
+
+int pw_ctx_build_twin(pw_ctx* ctx) {
+  PWB_CHECK(ctx && ctx->prec == PW_F64, PW_EINVAL, "the twin is built for an FP64 context");
+  PWB_CHECK(!ctx->atom_z.empty(), PW_ENOTREADY, "atoms not set (pw_set_atoms)");
+  if (ctx->twin) return PW_OK;
+  pw_ctx* c32 = nullptr;
+  int rc = pw_ctx_create(ctx->L, ctx->n, ctx->nf, PW_F32, ctx->device, &c32);
+  if (rc) return rc;
+  if ((rc = pw_set_band_batch(c32, std::max(2, 2 * ctx->pair_cap))) ||
+      (rc = pw_set_atoms(c32, (int)ctx->atom_z.size(), ctx->atom_z.data(), ctx->atom_pos.data()))) {
+    pw_ctx_destroy(c32);
+    return rc;
+  }
+  ctx->twin = c32;
   return PW_OK;
 }
 
