@@ -199,6 +199,37 @@ __global__ void k_init_rho(long n, const double* __restrict__ rps, double* __res
 
 static inline int nblk(long n) { return (int)std::min<long>((n + 255) / 256, 148L * 8); }
 
+// Philox4x32-10 counter-based generator (Salmon, Moraes, Dror, Shaw, SC'11)
+// and Box-Muller: out[i] ~ N(0,1) for the key `seed`, counter = i / 4.
+__device__ __forceinline__ void philox4x32(uint32_t c[4], uint32_t k0, uint32_t k1) {
+  const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u, W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const uint32_t hi0 = __umulhi(M0, c[0]), lo0 = M0 * c[0];
+    const uint32_t hi1 = __umulhi(M1, c[2]), lo1 = M1 * c[2];
+    const uint32_t n0 = hi1 ^ c[1] ^ k0, n2 = hi0 ^ c[3] ^ k1;
+    c[0] = n0; c[1] = lo1; c[2] = n2; c[3] = lo0;
+    k0 += W0; k1 += W1;
+  }
+}
+template <typename T>
+__global__ void k_gaussian(long n, unsigned long long seed, T* __restrict__ out) {
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; 4 * q < n; q += (long)gridDim.x * blockDim.x) {
+    uint32_t c[4] = {(uint32_t)q, (uint32_t)(q >> 32), 0u, 0u};
+    philox4x32(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+    const double two32 = 4294967296.0;
+    for (int h = 0; h < 2; ++h) {
+      const double u1 = ((double)c[2 * h] + 0.5) / two32, u2 = ((double)c[2 * h + 1] + 0.5) / two32;
+      const double rr = sqrt(-2.0 * log(u1));
+      double sn, cs;
+      sincospi(2.0 * u2, &sn, &cs);
+      const long i = 4 * q + 2 * h;
+      if (i < n) out[i] = (T)(rr * cs);
+      if (i + 1 < n) out[i + 1] = (T)(rr * sn);
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // SCF / eigensolver state
 // ---------------------------------------------------------------------------
@@ -748,16 +779,11 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
   pw_ctx* cur = p->mixed ? S.c32 : ctx;
   if ((rc = bind(cur))) return rc;
   {
-    // random start, Gaussian (seeded), orthonormalised by Cholesky-QR
-    std::mt19937_64 gen(p->seed);
-    std::normal_distribution<double> nd;
-    std::vector<double> h((size_t)nb * nt);
-    for (auto& x : h) x = nd(gen);
-    if (cur->prec == PW_F64) PWB_CUDA(cudaMemcpy(sv.X.p, h.data(), h.size() * 8, cudaMemcpyHostToDevice));
-    else {
-      std::vector<float> hf(h.begin(), h.end());
-      PWB_CUDA(cudaMemcpy(sv.X.p, hf.data(), hf.size() * 4, cudaMemcpyHostToDevice));
-    }
+    // random start, Gaussian (seeded Philox on the device), orthonormalised by Cholesky-QR
+    const long ntot_b = (long)nb * nt;
+    if (cur->prec == PW_F64) k_gaussian<double><<<nblk(ntot_b / 4 + 1), 256>>>(ntot_b, p->seed, (double*)sv.X.p);
+    else k_gaussian<float><<<nblk(ntot_b / 4 + 1), 256>>>(ntot_b, p->seed, (float*)sv.X.p);
+    PWB_CUDA(cudaGetLastError());
     if ((rc = cholqr(sv, dn, sv.X.p, nb, sv.Y.p))) return rc;
   }
   const double tbeta = 315774.67 / p->temperature;
