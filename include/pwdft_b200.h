@@ -224,7 +224,7 @@ typedef struct pw_scf_result {
   double etot, efree, eharris, exc, ehart, eself, fermi, time_s;
   int iterations, converged, refine_iter;
   long hpsi_bands;          /* single-band H*psi applications performed */
-  double phase_s[6];        /* verbose >= 2: eigensolver, density, potentials, energies, mixing, other (s) */
+  double phase_s[6];        /* verbose >= 2: eigensolver, density, potentials, set-up, mixing, refine switch (s) */
   double sub_s[4];          /* verbose >= 2, inside the eigensolver: H*psi, Gram, dense FP64, rotations (s) */
 } pw_scf_result;
 

@@ -700,7 +700,8 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
   const bool prof = p->verbose >= 2;
   g_sub_on = prof;
   for (double& x : g_sub) x = 0;
-  double tph[6] = {0, 0, 0, 0, 0, 0};   // eigensolver, density, potentials, energies, mixing, refine switch
+  double tph[6] = {0, 0, 0, 0, 0, 0};   // eigensolver, density, potentials, set-up, mixing, refine switch
+  auto t_setup0 = std::chrono::steady_clock::now();
   if ((rc = pw_set_band_batch(ctx, nb))) return rc;
   // device arrays
   for (DevBuf* b : {&S.rho, &S.rho_out, &S.rps, &S.vtot, &S.vtot_new, &S.vxc, &S.eps, &S.vh, &S.kern})
@@ -785,6 +786,10 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
     else k_gaussian<float><<<nblk(ntot_b / 4 + 1), 256>>>(ntot_b, p->seed, (float*)sv.X.p);
     PWB_CUDA(cudaGetLastError());
     if ((rc = cholqr(sv, dn, sv.X.p, nb, sv.Y.p))) return rc;
+  }
+  if (prof) {
+    cudaDeviceSynchronize();
+    tph[3] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_setup0).count();
   }
   const double tbeta = 315774.67 / p->temperature;
   double b_up = 0, lmin = 0;
@@ -877,7 +882,7 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
     if (refined && dif < p->tol_efree) { conv = true; break; }
     // switch the eigensolver to FP64 for the final iterations (iterative refinement)
     if (!refined && dif < p->refine_threshold) {
-      pw_ctx* c32 = sv.c;
+      PhaseTimer pt_(prof, &tph[5]);
       DevBuf x32;
       if ((rc = x32.alloc((size_t)nb * nt * 4))) return rc;
       PWB_CUDA(cudaMemcpy(x32.p, sv.X.p, (size_t)nb * nt * 4, cudaMemcpyDeviceToDevice));
@@ -888,7 +893,6 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
       sv.eig = keep_eig;
       refined = true;
       r->refine_iter = it;
-      (void)c32;
     }
     // Anderson mixing of the potential (scf.cpp:2299-2365)
     {
