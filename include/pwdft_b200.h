@@ -241,6 +241,22 @@ PW_API int pw_ctx_build_twin(pw_ctx* ctx);
  * doubles; rho_out: host, N_fine doubles (either may be NULL). */
 PW_API int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* eig_out, double* rho_out);
 
+/* Atomic forces of an FP64 context with atoms (pw_set_atoms),
+ * KohnSham::CalculateForce (src/SCF/hamiltonian.cpp:2670-3056), pseudocharge
+ * form: local part pseudocharge . grad V_H[rho - rho_ps] (:2716-2800) plus the
+ * nonlocal part of :2907-3006.  rho_dev: device, N_fine doubles; psi_dev:
+ * device, nband columns of N_coarse doubles (leading dimension ldpsi); occ:
+ * host, nband occupation rates in [0, 1]; num_spin: 1 or 2 (numSpin).  force:
+ * host, natom x 3 (Hartree / bohr); force_local / force_nonlocal (host, may be
+ * NULL) receive the two parts.  The reference's VdW, short-range ion and
+ * external terms are not part of this path. */
+PW_API int pw_forces(pw_ctx* ctx, const double* rho_dev, const void* psi_dev, int ldpsi, int nband,
+                     const double* occ, int num_spin, double* force, double* force_local, double* force_nonlocal);
+
+/* Forces from the state the last pw_scf_run left in the context (its final
+ * FP64 bands, occupations and output density), numSpin = 2. */
+PW_API int pw_scf_forces(pw_ctx* ctx, double* force, double* force_local, double* force_nonlocal);
+
 /* Teter preconditioner that allocates nothing (no counterpart in the
  * reference).  Same result as pw_teter_precond; for callers that cannot call
  * cudaMalloc where they need it -- code inside CUDA stream capture, hosts that

@@ -88,6 +88,8 @@ SIGNATURES: dict[str, tuple] = {
     "pw_hgh_pseudocharge": (_i, [_dp, _ip, _i, _ip, _dp, _dp]),
     "pw_profile": (_i, [_vp, _i]),
     "pw_profile_read": (_i, [_vp, _i, _dp, C.POINTER(_l)]),
+    "pw_forces": (_i, [_vp, _vp, _vp, _i, _i, _dp, _i, _dp, _dp, _dp]),
+    "pw_scf_forces": (_i, [_vp, _dp, _dp, _dp]),
 }
 
 for _name, (_res, _args) in SIGNATURES.items():

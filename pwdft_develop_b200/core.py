@@ -174,6 +174,7 @@ def _ctx_set_atoms(self, znuc, pos):
     z = np.ascontiguousarray(znuc, np.int32)
     ps = np.ascontiguousarray(pos, np.float64)
     check(lib.pw_set_atoms(self._h, len(z), z.ctypes.data_as(_lib._ip), ps.ctypes.data_as(_lib._dp)))
+    self._atoms_z = z.copy()
 
 
 def _ctx_pseudocharge(self) -> np.ndarray:
@@ -313,6 +314,31 @@ def _ctx_xc(self, rho):
     return eps, v
 
 
+def _ctx_forces(self, rho, psi, occ, num_spin: int = 2):
+    """KohnSham::CalculateForce (hamiltonian.cpp:2670-3056) for an FP64 context with
+    atoms: rho (N_fine) and psi (nband, N_coarse) float64 device tensors, occ the
+    occupation rates.  Returns (total, local, nonlocal), each natom x 3."""
+    if not hasattr(self, "_atoms_z"):
+        raise RuntimeError("atoms not set (set_atoms)")
+    natom = len(self._atoms_z)
+    occ = np.ascontiguousarray(occ, np.float64)
+    nb = 0 if psi is None else psi.shape[0]
+    out = [np.zeros((natom, 3)) for _ in range(3)]
+    check(lib.pw_forces(self._h, _ptr(rho), _ptr(psi) if nb else None, self.ntot, nb,
+                        occ.ctypes.data_as(_lib._dp), int(num_spin), *[o.ctypes.data_as(_lib._dp) for o in out]))
+    return tuple(out)
+
+
+def _ctx_scf_forces(self):
+    """Forces from the final state of the last scf() call: (total, local, nonlocal)."""
+    natom = len(self._atoms_z)
+    out = [np.zeros((natom, 3)) for _ in range(3)]
+    check(lib.pw_scf_forces(self._h, *[o.ctypes.data_as(_lib._dp) for o in out]))
+    return tuple(out)
+
+
+Context.forces = _ctx_forces
+Context.scf_forces = _ctx_scf_forces
 Context.hartree = _ctx_hartree
 Context.xc = _ctx_xc
 Context.cholqr = _ctx_cholqr

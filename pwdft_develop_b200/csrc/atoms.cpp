@@ -28,6 +28,9 @@ int pw_set_atoms(pw_ctx* ctx, int natom, const int* znuc, const double* pos) {
   PWB_CHECK(ctx && natom >= 0 && (natom == 0 || (znuc && pos)), PW_EINVAL, "bad arguments");
   std::vector<AtomNL> nl(natom);
   std::vector<double> rhops(ctx->ntotf, 0.0);
+  std::vector<long> ps_off(1, 0);
+  std::vector<int> ps_idx;
+  std::vector<double> ps_val;
   for (int a = 0; a < natom; ++a) {
     const Species* sp = species(znuc[a]);
     PWB_CHECK(sp, PW_EUNSUPPORTED, "HGH table only built for Si (14) and Al (13)");
@@ -36,7 +39,12 @@ int pw_set_atoms(pw_ctx* ctx, int natom, const int* znuc, const double* pos) {
     AtomRho rho;
     rc = pseudo_charge(*sp, pos + 3 * a, ctx->L, ctx->nf, rho);
     if (rc) return rc;
-    for (size_t i = 0; i < rho.idx.size(); ++i) rhops[rho.idx[i]] += rho.val[4 * i];
+    for (size_t i = 0; i < rho.idx.size(); ++i) {
+      rhops[rho.idx[i]] += rho.val[4 * i];
+      ps_idx.push_back(rho.idx[i]);
+      ps_val.push_back(rho.val[4 * i]);
+    }
+    ps_off.push_back((long)ps_idx.size());
   }
   std::vector<int> npts(natom), nproj(natom), idx;
   std::vector<double> beta, wgt;
@@ -54,6 +62,9 @@ int pw_set_atoms(pw_ctx* ctx, int natom, const int* znuc, const double* pos) {
   ctx->atom_pos.assign(pos, pos + 3 * natom);
   ctx->h_nl = std::move(nl);
   ctx->h_rhops = std::move(rhops);
+  ctx->h_ps_off = std::move(ps_off);
+  ctx->h_ps_idx = std::move(ps_idx);
+  ctx->h_ps_val = std::move(ps_val);
   return PW_OK;
 }
 

@@ -107,6 +107,17 @@ struct pw_ctx {
   std::vector<double> atom_pos;            // natom x 3, Cartesian bohr
   std::vector<pwb::AtomNL> h_nl;           // per-atom vnlList incl. DX/DY/DZ columns
   std::vector<double> h_rhops;             // pseudocharge on the fine grid
+  std::vector<long> h_ps_off;              // natom + 1 offsets into h_ps_idx / h_ps_val
+  std::vector<int> h_ps_idx;               // per-atom pseudocharge support (fine-grid index)
+  std::vector<double> h_ps_val;            // per-atom pseudocharge values
+  // converged SCF state kept for pw_scf_forces: FP64 bands, occupations, density
+  pwb::DevBuf scf_psi, scf_rho;
+  std::vector<double> scf_occ;
+  int scf_nband = 0;
+  // flattened projector sets as last passed to pw_set_nonlocal (for forces)
+  std::vector<int> h_nl_idx, h_pnp, h_patom;
+  std::vector<double> h_nl_beta, h_pgamma;
+  std::vector<long> h_pio, h_pbo;
   // kernel launch accounting (pw_stats) and optional per-kernel event timing
   long launches = 0;
   long lib_launches = 0;          // cuBLAS / cuSOLVER calls (not this library's kernels)

@@ -44,7 +44,7 @@ int run_hpsi(pw_ctx* c, const void* psi, int ld, void* out, int ldo, int nband, 
 int run_teter(pw_ctx* c, const void* r, int ld, void* out, int ldo, int nband, int band0, int npair, int acc,
               cudaStream_t st);
 int run_build_q(pw_ctx* c, const int* d_idx, const double* d_beta, const long* d_pio, const long* d_pbo,
-                const int* d_pnp, int nproj, cudaStream_t st);
+                const int* d_pnp, int nproj, cudaStream_t st, int deriv = 0, void* out = nullptr);
 
 // upload a double host vector as the context's precision
 int upload_real(pw_ctx* c, DevBuf& dst, const double* src, size_t n) {
@@ -266,6 +266,26 @@ int pw_set_nonlocal(pw_ctx* ctx, int natom, const int* atom_npts, const int* ato
   }
   PWB_CHECK(npmax <= 8, PW_EUNSUPPORTED, "at most 8 projectors per atom are supported");
   PWB_CHECK(nent < (1L << 31), PW_EUNSUPPORTED, "too many projector points");
+  {
+    // host copy of the flattened sets: projector l of atom a has its points at
+    // idx[pio[l] ..] and values at beta[pbo[l] ..], pnp[l] of them, weight gamma_l
+    long off = 0, boff = 0, woff = 0;
+    ctx->h_pio.clear(); ctx->h_pbo.clear(); ctx->h_pnp.clear(); ctx->h_patom.clear(); ctx->h_pgamma.clear();
+    for (int a = 0; a < natom; ++a) {
+      for (int q = 0; q < atom_nproj[a]; ++q) {
+        ctx->h_pio.push_back(off);
+        ctx->h_pbo.push_back(boff + (long)q * atom_npts[a]);
+        ctx->h_pnp.push_back(atom_npts[a]);
+        ctx->h_patom.push_back(a);
+        ctx->h_pgamma.push_back(weight[woff + q]);
+      }
+      off += atom_npts[a];
+      boff += (long)atom_nproj[a] * atom_npts[a];
+      woff += atom_nproj[a];
+    }
+    ctx->h_nl_idx.assign(idx, idx + off);
+    ctx->h_nl_beta.assign(beta, beta + boff);
+  }
   if (ctx->nl_mode == PW_NL_DENSE) {
     // per-projector offsets into idx / beta, weights gamma_l * vol / ntot
     std::vector<long> pio, pbo;

@@ -357,7 +357,7 @@ constexpr int FLOC_THREADS = 256;
 template <typename T, int NXF, int NYF, int MODE>
 __global__ void __launch_bounds__(FLOC_THREADS)
 k_floc(VT<T>* __restrict__ BC, const T* __restrict__ vtot, const T* __restrict__ fin, long fin_pair_stride,
-       T inv_nf, const VT<T>* twx_g, const VT<T>* twy_g) {
+       T inv_nf, const VT<T>* twx_g, const VT<T>* twy_g, int deriv = 0, T gfac = 0) {
   using V = VT<T>;
   constexpr int n0 = NXF / 2, n1 = NYF / 2;
   constexpr int nsx = n0 + 1, nsy = n1 + 1;
@@ -413,6 +413,16 @@ k_floc(VT<T>* __restrict__ BC, const T* __restrict__ vtot, const T* __restrict__
     }
     __syncwarp();
     smem_fft_c<NXF, -1, 1, PR>(Rw, nr, twx, 0, 1);
+    if (MODE == 1 && deriv == 1) {
+      // spectral d/dx: multiply by i G_x of the fine frequency
+      for (int i = lane; i < nr * NXF; i += 32) {
+        const int f = i / NXF, x = i - f * NXF;
+        const T g = gfac * (T)sgn_idx(x, NXF);
+        const V v = Rw[f * PR + x];
+        Rw[f * PR + x] = mkc<V>(-g * v.y, g * v.x);
+      }
+      __syncwarp();
+    }
     for (int i = lane; i < nr * nsx; i += 32) {
       const int f = i / nsx, xs = i - f * nsx;
       S[(r0 + f) * PS + xs] = Rw[f * PR + slot_fine(xs, n0, NXF)];
@@ -422,6 +432,15 @@ k_floc(VT<T>* __restrict__ BC, const T* __restrict__ vtot, const T* __restrict__
   __syncthreads();
   smem_fft_cb<NYF, -1, PS, 1>(S, nsx, twy);
   __syncthreads();
+  if (MODE == 1 && deriv == 2) {
+    for (int i = threadIdx.x; i < NYF * nsx; i += blockDim.x) {
+      const int y = i / nsx, xs = i - y * nsx;
+      const T g = gfac * (T)sgn_idx(y, NYF);
+      const V v = S[y * PS + xs];
+      S[y * PS + xs] = mkc<V>(-g * v.y, g * v.x);
+    }
+    __syncthreads();
+  }
   for (int i = threadIdx.x; i < nsy * nsx; i += blockDim.x) {
     const int ys = i / nsx, xs = i - ys * nsx;
     Bp[i] = cscale(S[slot_fine(ys, n1, NYF) * PS + xs], inv_nf);
@@ -562,7 +581,7 @@ __global__ void k_nl_reduce(const VT<T>* __restrict__ Wp, VT<T>* __restrict__ W,
 template <typename T, int NZ, int NZF>
 __global__ void __launch_bounds__(PENCIL_THREADS)
 k_zfold(const VT<T>* __restrict__ C, const VT<T>* __restrict__ K, VT<T>* __restrict__ D, int n0, int n1,
-        const VT<T>* twz_g, const VT<T>* twzf_g) {
+        const VT<T>* twz_g, const VT<T>* twzf_g, int deriv = 0, T gfac = 0) {
   using V = VT<T>;
   constexpr int PI = 2 * TX + 1;
   constexpr int PA = TX + 1;
@@ -588,6 +607,16 @@ k_zfold(const VT<T>* __restrict__ C, const VT<T>* __restrict__ K, VT<T>* __restr
   __syncthreads();
   smem_fft_cb<NZF, -1, PI, 1>(in, m.ncols, twzf);
   __syncthreads();
+  if (deriv == 3) {
+    // spectral d/dz before the fold: multiply by i G_z of the fine frequency
+    for (int i = threadIdx.x; i < NZF * m.ncols; i += blockDim.x) {
+      const int zf = i / m.ncols, c = i - zf * m.ncols;
+      const T g = gfac * (T)sgn_idx(zf, NZF);
+      const V v = in[zf * PI + c];
+      in[zf * PI + c] = mkc<V>(-g * v.y, g * v.x);
+    }
+    __syncthreads();
+  }
   const long nplane = (long)n0 * n1;
   const V* Kp = K + (long)p * NZ * nplane;
   for (int i = threadIdx.x; i < NZ * TX; i += blockDim.x) {
@@ -937,7 +966,7 @@ struct Plan {
   // Build q_l = T(beta_l) for all projectors with the fine->coarse half of
   // the pipeline, two projectors per complex field.
   static int build_q(pw_ctx* c, const int* d_idx, const double* d_beta, const long* d_pio, const long* d_pbo,
-                     const int* d_pnp, int nproj, cudaStream_t st) {
+                     const int* d_pnp, int nproj, cudaStream_t st, int deriv = 0, T* Qout = nullptr) {
     int rc = set_attrs();
     if (rc) return rc;
     const int cap = c->pair_cap;                 // pairs per pass
@@ -946,17 +975,20 @@ struct Plan {
     if ((rc = fields.alloc((size_t)2 * cap * nf * sizeof(T)))) return rc;
     V* AD = reinterpret_cast<V*>(c->s_ad.p);
     V* BC = reinterpret_cast<V*>(c->s_bc.p);
-    T* Q = reinterpret_cast<T*>(c->q.p);
+    T* Q = Qout ? Qout : reinterpret_cast<T*>(c->q.p);
     const T inv_nf = (T)(1.0 / (double)c->ntotf);
     const int ntx = (N0 + TX - 1) / TX;
+    const T gx = (T)(2 * M_PI / c->L[0]), gy = (T)(2 * M_PI / c->L[1]), gz = (T)(2 * M_PI / c->L[2]);
     for (int l0 = 0; l0 < nproj; l0 += 2 * cap) {
       const int nl = std::min(2 * cap, nproj - l0);
       const int npair = (nl + 1) / 2;
       PWB_CUDA(cudaMemsetAsync(fields.p, 0, (size_t)2 * npair * nf * sizeof(T), st));
       k_scatter_beta<T><<<dim3(64, nl), 256, 0, st>>>(reinterpret_cast<T*>(fields.p), nf, d_idx, d_beta, d_pio, d_pbo, d_pnp, l0, nproj);
       k_floc<T, NF0, NF1, 1><<<dim3(NF2, npair), FLOC_THREADS, sm_floc(), st>>>(
-          BC, nullptr, reinterpret_cast<const T*>(fields.p), nf, inv_nf, tw(c, 3), tw(c, 4));
-      k_zfold<T, N2, NF2><<<dim3(N1, ntx, npair), PENCIL_THREADS, sm_zfold(), st>>>(BC, nullptr, AD, N0, N1, tw(c, 2), tw(c, 5));
+          BC, nullptr, reinterpret_cast<const T*>(fields.p), nf, inv_nf, tw(c, 3), tw(c, 4), deriv,
+          deriv == 1 ? gx : gy);
+      k_zfold<T, N2, NF2><<<dim3(N1, ntx, npair), PENCIL_THREADS, sm_zfold(), st>>>(BC, nullptr, AD, N0, N1, tw(c, 2),
+                                                                                     tw(c, 5), deriv, gz);
       k_cxy_inv<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(AD, Q, (int)c->ntot, nproj, l0, 0, tw(c, 0), tw(c, 1));
       PWB_CUDA(cudaGetLastError());
     }
@@ -1019,7 +1051,8 @@ static int teter_thunk(pw_ctx* c, const void* psi, int ld, void* out, int ldo, i
   return Plan<T, N0, N1, N2>::teter_batch(c, (const T*)psi, ld, (T*)out, ldo, nband, band0, npair, acc, st);
 }
 template <typename T, int N0, int N1, int N2> static int cr_thunk() { return Plan<T, N0, N1, N2>::chunk_rows(); }
-using BuildQFn = int (*)(pw_ctx*, const int*, const double*, const long*, const long*, const int*, int, cudaStream_t);
+using BuildQFn = int (*)(pw_ctx*, const int*, const double*, const long*, const long*, const int*, int, cudaStream_t,
+                         int, void*);
 using DensFn = int (*)(pw_ctx*, const void*, int, int, int, int, const double*, double*, cudaStream_t);
 using TeterScratchFn = int (*)(pw_ctx*, const void*, int, void*, int, int, int, int, int, cudaStream_t, void*);
 template <typename T, int N0, int N1, int N2>
@@ -1035,8 +1068,8 @@ static int dens_thunk(pw_ctx* c, const void* psi, int ld, int nband, int band0, 
 }
 template <typename T, int N0, int N1, int N2>
 static int buildq_thunk(pw_ctx* c, const int* a, const double* b, const long* d, const long* e, const int* f, int n,
-                        cudaStream_t st) {
-  return Plan<T, N0, N1, N2>::build_q(c, a, b, d, e, f, n, st);
+                        cudaStream_t st, int deriv, void* out) {
+  return Plan<T, N0, N1, N2>::build_q(c, a, b, d, e, f, n, st, deriv, (T*)out);
 }
 
 struct GridEntry {
@@ -1081,10 +1114,10 @@ int run_hpsi(pw_ctx* c, const void* psi, int ld, void* out, int ldo, int nband, 
 }
 
 int run_build_q(pw_ctx* c, const int* d_idx, const double* d_beta, const long* d_pio, const long* d_pbo,
-                const int* d_pnp, int nproj, cudaStream_t st) {
+                const int* d_pnp, int nproj, cudaStream_t st, int deriv, void* out) {
   const GridEntry* g = find_grid(c->n);
   if (!g) { set_error("grid not built into this library"); return PW_EUNSUPPORTED; }
-  return g->bq[c->prec == PW_F32 ? 1 : 0](c, d_idx, d_beta, d_pio, d_pbo, d_pnp, nproj, st);
+  return g->bq[c->prec == PW_F32 ? 1 : 0](c, d_idx, d_beta, d_pio, d_pbo, d_pnp, nproj, st, deriv, out);
 }
 
 int run_density(pw_ctx* c, const void* psi, int ld, int nband, int band0, int npair, const double* w, double* rho,

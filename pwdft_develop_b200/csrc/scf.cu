@@ -25,6 +25,7 @@
 #include "blockops.hpp"
 #include "common.hpp"
 #include "fft.cuh"
+#include "fft3d.cuh"
 #include "gemm.hpp"
 
 namespace pwb {
@@ -34,84 +35,6 @@ int run_density(pw_ctx* c, const void* psi, int ld, int nband, int band0, int np
 int gram(pw_ctx* c, const void* X, int ldx, int nx, const void* Y, int ldy, int ny, double* G, int ldg,
          cudaStream_t st);
 int upload_real(pw_ctx* c, DevBuf& dst, const double* src, size_t n);
-
-// ---------------------------------------------------------------------------
-// FP64 3-D FFT of the fine grid along one axis, 16 pencils per CTA
-// ---------------------------------------------------------------------------
-constexpr int AX_TILE = 16;
-constexpr int AX_THREADS = 256;
-
-// axis 0 (x, contiguous): CTA = 16 consecutive rows; axis 1 (y): CTA = (z, x tile);
-// axis 2 (z): CTA = (y, x tile).  MODE 0: plain, 1: real input (load re(x) -
-// y_sub), 2: multiply by kern after the forward transform and inverse in place,
-// 3: store the real part scaled into out.
-template <int N, int DIR, int AXIS, int MODE>
-__global__ void __launch_bounds__(AX_THREADS)
-k_fft_axis(double2* __restrict__ data, int nx, int ny, int nz, const double* __restrict__ rin,
-           const double* __restrict__ rsub, const double* __restrict__ kern, double* __restrict__ rout, double scale,
-           const double2* tw_g) {
-  constexpr int P = AX_TILE + 1;
-  __shared__ double2 buf[N * P];
-  __shared__ double2 tw[N];
-  for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = tw_g[i];
-  long base;
-  long estride;
-  int cnt;
-  if (AXIS == 0) {
-    const long row0 = (long)blockIdx.x * AX_TILE;
-    const long nrow = (long)ny * nz;
-    cnt = (int)min((long)AX_TILE, nrow - row0);
-    base = row0 * nx;
-    estride = 1;
-    // rows: element e of row r at base + r*nx + e -> buf[e*P + r]
-    for (int i = threadIdx.x; i < N * AX_TILE; i += blockDim.x) {
-      const int r = i / N, e = i - r * N;
-      double2 v = make_double2(0, 0);
-      if (r < cnt) {
-        const long g = base + (long)r * nx + e;
-        if (MODE == 1) v = make_double2(rin[g] - (rsub ? rsub[g] : 0.0), 0.0);
-        else v = data[g];
-      }
-      buf[e * P + r] = v;
-    }
-  } else {
-    const int x0 = blockIdx.x * AX_TILE;
-    cnt = min(AX_TILE, nx - x0);
-    if (AXIS == 1) { base = (long)blockIdx.y * nx * ny + x0; estride = nx; }
-    else { base = (long)blockIdx.y * nx + x0; estride = (long)nx * ny; }
-    for (int i = threadIdx.x; i < N * AX_TILE; i += blockDim.x) {
-      const int e = i / AX_TILE, c = i - e * AX_TILE;
-      buf[e * P + c] = (c < cnt) ? data[base + e * estride + c] : make_double2(0, 0);
-    }
-  }
-  __syncthreads();
-  smem_fft_cb<N, DIR, P, 1>(buf, cnt, tw);
-  __syncthreads();
-  if (MODE == 2) {
-    for (int i = threadIdx.x; i < N * AX_TILE; i += blockDim.x) {
-      const int e = i / AX_TILE, c = i - e * AX_TILE;
-      if (c < cnt) buf[e * P + c] = cscale(buf[e * P + c], kern[base + e * estride + c]);
-    }
-    __syncthreads();
-    smem_fft_cb<N, -DIR, P, 1>(buf, cnt, tw);
-    __syncthreads();
-  }
-  if (AXIS == 0) {
-    for (int i = threadIdx.x; i < N * AX_TILE; i += blockDim.x) {
-      const int r = i / N, e = i - r * N;
-      if (r < cnt) {
-        const long g = base + (long)r * nx + e;
-        if (MODE == 3) rout[g] = buf[e * P + r].x * scale;
-        else data[g] = buf[e * P + r];
-      }
-    }
-  } else {
-    for (int i = threadIdx.x; i < N * AX_TILE; i += blockDim.x) {
-      const int e = i / AX_TILE, c = i - e * AX_TILE;
-      if (c < cnt) data[base + e * estride + c] = buf[e * P + c];
-    }
-  }
-}
 
 // Hartree on the fine grid: vh = (1/N) IFFT( kern * FFT(rho - rho_ps) ),
 // kern = 2 pi / gkk (0 for gkk <= 1e-16 or gkk > 4 Ecut).  Cubic grids only.
@@ -978,6 +901,15 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
   g_sub_on = false;
   if (eig_out) std::copy(eig.begin(), eig.end(), eig_out);
   if (rho_out) PWB_CUDA(cudaMemcpy(rho_out, rho, nf * 8, cudaMemcpyDeviceToHost));
+  // keep the final FP64 bands, occupations and output density for pw_scf_forces
+  ctx->scf_nband = 0;
+  if (sv.c == ctx) {
+    if ((rc = ctx->scf_psi.alloc((size_t)nb * nt * 8)) || (rc = ctx->scf_rho.alloc(nf * 8))) return rc;
+    PWB_CUDA(cudaMemcpy(ctx->scf_psi.p, sv.X.p, (size_t)nb * nt * 8, cudaMemcpyDeviceToDevice));
+    PWB_CUDA(cudaMemcpy(ctx->scf_rho.p, rho, nf * 8, cudaMemcpyDeviceToDevice));
+    ctx->scf_occ = occ;
+    ctx->scf_nband = nb;
+  }
   dn.release();
   return PW_OK;
 }

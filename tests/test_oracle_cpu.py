@@ -192,3 +192,38 @@ def test_pipeline_model_equals_oracle():
         ref = pw.mult_spinor(T, psi)
         got = model_hpsi(T, psi)
         assert np.abs(got - ref).max() / np.abs(ref).max() < 1e-14
+
+
+def test_nonlocal_force_coarse_identity():
+    """The device's nonlocal force form -- coarse projectors q_l = T beta_l and
+    derivative projectors T(d beta_l), T the fine->coarse transpose of the
+    interpolation, F = 2 numSpin f gamma (vol/N_c)(q.psi)(Tdbeta.psi) -- equals
+    the reference's per-band fine-grid "Method 4" (hamiltonian.cpp:2907-3006)."""
+    from oracle import forces
+    L, z, pos = pw.make_crystal("Si", (1, 1, 1), 10.26, 0.05, 7)
+    nc, nf = (8, 8, 8), (16, 16, 16)
+    T, _ = pw.build_tables(L, z, pos, nc, nf)
+    dm = T.dm
+    N0, N1, N2 = nf
+    n0, n1, n2 = nc
+    gf = pw.gvec_full(dm, fine=True)
+
+    def t_of(B, d=None):
+        Y = np.fft.fftn(B.reshape(N2, N1, N0))
+        if d is not None:
+            Y = Y * (1j * gf[..., d])
+        X = T.ip.f2c(Y[..., :N0 // 2 + 1].reshape(-1)) / dm.ntotFine
+        return np.fft.irfftn(X.reshape(n2, n1, n0 // 2 + 1), s=(n2, n1, n0)).ravel() * dm.ntot
+
+    psi = pw.random_orthonormal_psi(dm.ntot, 5, 3)
+    occ = np.array([1, 1, .9, .5, .1])
+    ref = forces.nonlocal_force(T, psi, occ)
+    F = np.zeros_like(ref)
+    for a, app in enumerate(T.pseudo):
+        for pp in app:
+            B = np.zeros(dm.ntotFine)
+            B[pp.idx] = pp.val[:, 0]
+            q = psi @ t_of(B)
+            for d in range(3):
+                F[a, d] += np.sum(2 * 2 * occ * pp.wgt * (dm.vol / dm.ntot) * q * (psi @ t_of(B, d)))
+    assert np.abs(F - ref).max() <= 1e-12 * np.abs(ref).max()
