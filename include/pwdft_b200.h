@@ -253,6 +253,27 @@ PW_API int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, dou
 PW_API int pw_forces(pw_ctx* ctx, const double* rho_dev, const void* psi_dev, int ldpsi, int nband,
                      const double* occ, int num_spin, double* force, double* force_local, double* force_nonlocal);
 
+/* Band energy E = sum_b w_b <psi_b, H psi_b> (the forward half of the
+ * adjoint pair; no reference counterpart as an entry point -- the reference
+ * forms the same sum inside its energy and force routines).  psi: device,
+ * context precision, nband columns (leading dimension ld); w: host, nband
+ * weights (numSpin * occupation for a band energy); e: host, one double. */
+PW_API int pw_band_energy(pw_ctx* ctx, const void* psi, int ld, int nband, const double* w, double* e);
+
+/* Backward of pw_band_energy at fixed psi.  dE_dV_dev (device, N_fine
+ * doubles, may be NULL): dE/dV_loc(r) on the density grid, recomputing the
+ * fine-grid bands per batch instead of storing them.  dE_dR (host, natom x 3,
+ * may be NULL; FP64 context with pw_set_atoms): dE/dR of every atom through
+ * the analytic projector derivatives (the DX/DY/DZ columns of vnlList,
+ * src/SCF/periodtable.cpp:994-1240). */
+PW_API int pw_band_energy_backward(pw_ctx* ctx, const void* psi, int ld, int nband, const double* w,
+                                   double* dE_dV_dev, double* dE_dR);
+
+/* The state the last pw_scf_run left in an FP64 context: band count,
+ * occupation rates (host, nband), bands (device, nband columns, leading
+ * dimension ldpsi) and output density (device, N_fine); pointers may be NULL. */
+PW_API int pw_scf_state(const pw_ctx* ctx, int* nband, double* occ, double* psi_dev, int ldpsi, double* rho_dev);
+
 /* Forces from the state the last pw_scf_run left in the context (its final
  * FP64 bands, occupations and output density), numSpin = 2. */
 PW_API int pw_scf_forces(pw_ctx* ctx, double* force, double* force_local, double* force_nonlocal);

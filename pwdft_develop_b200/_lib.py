@@ -90,6 +90,9 @@ SIGNATURES: dict[str, tuple] = {
     "pw_profile_read": (_i, [_vp, _i, _dp, C.POINTER(_l)]),
     "pw_forces": (_i, [_vp, _vp, _vp, _i, _i, _dp, _i, _dp, _dp, _dp]),
     "pw_scf_forces": (_i, [_vp, _dp, _dp, _dp]),
+    "pw_band_energy": (_i, [_vp, _vp, _i, _i, _dp, _dp]),
+    "pw_scf_state": (_i, [_vp, _ip, _dp, _vp, _i, _vp]),
+    "pw_band_energy_backward": (_i, [_vp, _vp, _i, _i, _dp, _vp, _dp]),
 }
 
 for _name, (_res, _args) in SIGNATURES.items():

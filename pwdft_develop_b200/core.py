@@ -337,6 +337,41 @@ def _ctx_scf_forces(self):
     return tuple(out)
 
 
+def _ctx_band_energy(self, psi, w):
+    """E = sum_b w_b <psi_b, H psi_b> (psi: (nband, N_coarse) device tensor)."""
+    w = np.ascontiguousarray(w, np.float64)
+    e = C.c_double(0.0)
+    check(lib.pw_band_energy(self._h, _ptr(psi), self.ntot, psi.shape[0], w.ctypes.data_as(_lib._dp), C.byref(e)))
+    return e.value
+
+
+def _ctx_band_energy_backward(self, psi, w, dv: bool = True, dr: bool = True):
+    """(dE/dV_loc on the fine grid as a float64 device tensor or None,
+    dE/dR natom x 3 numpy array or None) at fixed psi."""
+    import torch
+    w = np.ascontiguousarray(w, np.float64)
+    g = torch.empty(self.ntotFine, dtype=torch.float64, device=psi.device) if dv else None
+    r = np.zeros((len(self._atoms_z), 3)) if dr else None
+    check(lib.pw_band_energy_backward(self._h, _ptr(psi), self.ntot, psi.shape[0], w.ctypes.data_as(_lib._dp),
+                                      _ptr(g) if dv else None, r.ctypes.data_as(_lib._dp) if dr else None))
+    return g, r
+
+
+def _ctx_scf_state(self):
+    """(occupations, bands (nband, N_coarse) float64 device tensor, density) of the last scf()."""
+    import torch
+    nb = C.c_int(0)
+    check(lib.pw_scf_state(self._h, C.byref(nb), None, None, 0, None))
+    occ = np.zeros(nb.value)
+    psi = torch.empty((nb.value, self.ntot), dtype=torch.float64, device="cuda")
+    rho = torch.empty(self.ntotFine, dtype=torch.float64, device="cuda")
+    check(lib.pw_scf_state(self._h, C.byref(nb), occ.ctypes.data_as(_lib._dp), _ptr(psi), self.ntot, _ptr(rho)))
+    return occ, psi, rho
+
+
+Context.scf_state = _ctx_scf_state
+Context.band_energy = _ctx_band_energy
+Context.band_energy_backward = _ctx_band_energy_backward
 Context.forces = _ctx_forces
 Context.scf_forces = _ctx_scf_forces
 Context.hartree = _ctx_hartree

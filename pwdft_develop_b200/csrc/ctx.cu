@@ -266,6 +266,7 @@ int pw_set_nonlocal(pw_ctx* ctx, int natom, const int* atom_npts, const int* ato
   }
   PWB_CHECK(npmax <= 8, PW_EUNSUPPORTED, "at most 8 projectors per atom are supported");
   PWB_CHECK(nent < (1L << 31), PW_EUNSUPPORTED, "too many projector points");
+  ctx->h_nl.clear();   // analytic derivative columns stay only for sets built by pw_set_atoms
   {
     // host copy of the flattened sets: projector l of atom a has its points at
     // idx[pio[l] ..] and values at beta[pbo[l] ..], pnp[l] of them, weight gamma_l

@@ -29,6 +29,8 @@ namespace pwb {
 int run_build_q(pw_ctx* c, const int* d_idx, const double* d_beta, const long* d_pio, const long* d_pbo,
                 const int* d_pnp, int nproj, cudaStream_t st, int deriv, void* out);
 int ensure_scratch(pw_ctx* c, int npair);
+int run_density(pw_ctx* c, const void* psi, int ld, int nband, int band0, int npair, const double* w, double* rho,
+                cudaStream_t st);
 
 constexpr int FRC_THREADS = 256;
 
@@ -171,8 +173,12 @@ static int local_part(pw_ctx* ctx, const double* rho, double* F_dev) {
   return PW_OK;
 }
 
-static int nonlocal_part(pw_ctx* ctx, const double* psi, int ld, int nb, const double* occ, int num_spin,
-                          double* F_dev) {
+// sum_{l in a} sum_b cb_b gamma_l (vol/N_c) (q_l . psi_b)(p_l,d . psi_b) into F_dev[a][d], where
+// p_l,d = T(d_d beta_l) from the spectral derivative inside the fine->coarse
+// pipeline (columns == false) or T applied to the projector's analytic
+// derivative column DX/DY/DZ (columns == true, sets built by pw_set_atoms)
+static int nl_contract(pw_ctx* ctx, const double* psi, int ld, int nb, const std::vector<double>& cb, bool columns,
+                       double* F_dev) {
   const int np = (int)ctx->h_pnp.size();
   const int natom = (int)ctx->atom_z.size();
   const long nt = ctx->ntot;
@@ -184,10 +190,23 @@ static int nonlocal_part(pw_ctx* ctx, const double* psi, int ld, int nb, const d
   std::vector<int> aoff(natom + 1, 0);
   for (int l = 0; l < np; ++l) aoff[ctx->h_patom[l] + 1]++;
   for (int a = 0; a < natom; ++a) aoff[a + 1] += aoff[a];
-  std::vector<double> gl(np), cb(nb);
+  std::vector<double> gl(np);
   for (int l = 0; l < np; ++l) gl[l] = ctx->h_pgamma[l] * ctx->vol / (double)nt;
-  for (int b = 0; b < nb; ++b) cb[b] = 2.0 * num_spin * occ[b];
-  DevBuf d_idx, d_beta, d_pio, d_pbo, d_pnp, d_aoff, d_gl, d_cb, Qd, W, Wd, Qv;
+  std::vector<double> dcol[3];
+  if (columns) {
+    size_t tot = 0;
+    for (const auto& a : ctx->h_nl) tot += a.val.size();
+    PWB_CHECK(ctx->h_nl.size() == (size_t)natom && tot == (size_t)np, PW_ENOTREADY,
+              "analytic projector derivatives need the sets of pw_set_atoms");
+    for (int d = 0; d < 3; ++d) {
+      dcol[d].reserve(ctx->h_nl_beta.size());
+      for (const auto& a : ctx->h_nl)
+        for (const auto& v : a.val)
+          for (int g = 0; g < a.npts; ++g) dcol[d].push_back(v[4 * g + 1 + d]);
+      PWB_CHECK(dcol[d].size() == ctx->h_nl_beta.size(), PW_EINVAL, "projector sets changed since pw_set_atoms");
+    }
+  }
+  DevBuf d_idx, d_beta, d_pio, d_pbo, d_pnp, d_aoff, d_gl, d_cb, Qd, W, Wd, Qv, d_col;
   int rc;
   if ((rc = upload(d_idx, ctx->h_nl_idx)) || (rc = upload(d_beta, ctx->h_nl_beta)) || (rc = upload(d_pio, ctx->h_pio)) ||
       (rc = upload(d_pbo, ctx->h_pbo)) || (rc = upload(d_pnp, ctx->h_pnp)) || (rc = upload(d_aoff, aoff)) ||
@@ -214,9 +233,15 @@ static int nonlocal_part(pw_ctx* ctx, const double* psi, int ld, int nb, const d
   }
   ctx->lib_launches += 1;
   for (int d = 0; d < 3; ++d) {
-    if ((rc = run_build_q(ctx, (const int*)d_idx.p, (const double*)d_beta.p, (const long*)d_pio.p,
-                          (const long*)d_pbo.p, (const int*)d_pnp.p, np, nullptr, d + 1, Qd.p)))
-      return rc;
+    if (columns) {
+      if ((rc = upload(d_col, dcol[d]))) return rc;
+      rc = run_build_q(ctx, (const int*)d_idx.p, (const double*)d_col.p, (const long*)d_pio.p, (const long*)d_pbo.p,
+                       (const int*)d_pnp.p, np, nullptr, 0, Qd.p);
+    } else {
+      rc = run_build_q(ctx, (const int*)d_idx.p, (const double*)d_beta.p, (const long*)d_pio.p, (const long*)d_pbo.p,
+                       (const int*)d_pnp.p, np, nullptr, d + 1, Qd.p);
+    }
+    if (rc) return rc;
     if (cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, np, nb, (int)nt, &one, (const double*)Qd.p, (int)nt, psi, ld, &zero,
                     (double*)Wd.p + (size_t)d * np * nb, np) != CUBLAS_STATUS_SUCCESS) {
       set_error("derivative projector GEMM failed");
@@ -230,6 +255,18 @@ static int nonlocal_part(pw_ctx* ctx, const double* psi, int ld, int nb, const d
   PWB_CUDA(cudaGetLastError());
   PWB_CUDA(cudaDeviceSynchronize());
   return PW_OK;
+}
+
+// sum_i w_b psi_b(i) y_b(i) per band, FP64 accumulation; one CTA per band
+template <typename T>
+__global__ void __launch_bounds__(FRC_THREADS)
+k_band_dots(const T* __restrict__ x, int ldx, const T* __restrict__ y, int ldy, long n, double* __restrict__ out) {
+  __shared__ double sh[3 * FRC_THREADS / 32];
+  const int b = blockIdx.x;
+  double s[3] = {0, 0, 0};
+  for (long i = threadIdx.x; i < n; i += blockDim.x) s[0] += (double)x[(long)b * ldx + i] * (double)y[(long)b * ldy + i];
+  block_sum3(s, sh);
+  if (threadIdx.x == 0) out[b] = s[0];
 }
 
 }  // namespace pwb
@@ -257,12 +294,95 @@ int pw_forces(pw_ctx* ctx, const double* rho_dev, const void* psi_dev, int ldpsi
   double* Fnl = Floc + natom * 3;
   PWB_CUDA(cudaMemset(F.p, 0, (size_t)2 * natom * 3 * 8));
   if ((rc = local_part(ctx, rho_dev, Floc))) return rc;
-  if ((rc = nonlocal_part(ctx, (const double*)psi_dev, ldpsi, nband, occ, num_spin, Fnl))) return rc;
+  std::vector<double> cb(nband);
+  for (int b = 0; b < nband; ++b) cb[b] = 2.0 * num_spin * occ[b];
+  if ((rc = nl_contract(ctx, (const double*)psi_dev, ldpsi, nband, cb, false, Fnl))) return rc;
   std::vector<double> h(2 * natom * 3);
   PWB_CUDA(cudaMemcpy(h.data(), F.p, h.size() * 8, cudaMemcpyDeviceToHost));
   for (int i = 0; i < natom * 3; ++i) force[i] = h[i] + h[natom * 3 + i];
   if (force_local) std::copy(h.begin(), h.begin() + natom * 3, force_local);
   if (force_nonlocal) std::copy(h.begin() + natom * 3, h.end(), force_nonlocal);
+  return PW_OK;
+}
+
+int pw_band_energy(pw_ctx* ctx, const void* psi, int ld, int nband, const double* w, double* e) {
+  PWB_CHECK(ctx && e && (nband == 0 || (psi && w)), PW_EINVAL, "null argument");
+  PWB_CHECK(nband >= 0 && ld >= ctx->ntot, PW_EINVAL, "Domain size does not match.");
+  PWB_CUDA(cudaSetDevice(ctx->device));
+  *e = 0.0;
+  if (nband == 0) return PW_OK;
+  const long nt = ctx->ntot;
+  DevBuf hp, dd;
+  int rc;
+  if ((rc = hp.alloc((size_t)nband * nt * ctx->esz)) || (rc = dd.alloc((size_t)nband * 8))) return rc;
+  if ((rc = pw_hpsi(ctx, psi, ld, hp.p, (int)nt, nband, 0, nullptr))) return rc;
+  if (ctx->prec == PW_F64)
+    k_band_dots<double><<<nband, FRC_THREADS>>>((const double*)psi, ld, (const double*)hp.p, (int)nt, nt, (double*)dd.p);
+  else
+    k_band_dots<float><<<nband, FRC_THREADS>>>((const float*)psi, ld, (const float*)hp.p, (int)nt, nt, (double*)dd.p);
+  ctx->launches += 1;
+  PWB_CUDA(cudaGetLastError());
+  std::vector<double> h(nband);
+  PWB_CUDA(cudaMemcpy(h.data(), dd.p, nband * 8, cudaMemcpyDeviceToHost));
+  double s = 0;
+  for (int b = 0; b < nband; ++b) s += w[b] * h[b];
+  *e = s;
+  return PW_OK;
+}
+
+int pw_band_energy_backward(pw_ctx* ctx, const void* psi, int ld, int nband, const double* w, double* dE_dV_dev,
+                            double* dE_dR) {
+  PWB_CHECK(ctx && (nband == 0 || (psi && w)), PW_EINVAL, "null argument");
+  PWB_CHECK(nband >= 0 && ld >= ctx->ntot, PW_EINVAL, "Domain size does not match.");
+  PWB_CHECK(!dE_dR || ctx->prec == PW_F64, PW_EINVAL, "d/dR takes an FP64 context");
+  PWB_CHECK(!dE_dR || !ctx->atom_z.empty(), PW_ENOTREADY, "atoms not set (pw_set_atoms)");
+  PWB_CUDA(cudaSetDevice(ctx->device));
+  int rc;
+  if (dE_dV_dev) {
+    // E = sum_b w_b <psi_b, T(V M psi_b)> = sum_r V(r) sum_b w_b (N_c/N_f) (M psi_b)(r)^2,
+    // M the value-preserving coarse->fine interpolation, recomputed per batch
+    PWB_CUDA(cudaMemset(dE_dV_dev, 0, ctx->ntotf * 8));
+    if (nband > 0) {
+      DevBuf wv;
+      if ((rc = wv.alloc((size_t)(nband + 2) * 8))) return rc;
+      std::vector<double> h(nband + 2, 0.0);
+      for (int b = 0; b < nband; ++b) h[b] = w[b] * (double)ctx->ntot / (double)ctx->ntotf;
+      PWB_CUDA(cudaMemcpy(wv.p, h.data(), h.size() * 8, cudaMemcpyHostToDevice));
+      const int cap = ctx->pair_cap;
+      for (int b0 = 0; b0 < nband; b0 += 2 * cap) {
+        const int npair = std::min(cap, (nband - b0 + 1) / 2);
+        if ((rc = run_density(ctx, psi, ld, nband, b0, npair, (const double*)wv.p, dE_dV_dev, nullptr))) return rc;
+      }
+      PWB_CUDA(cudaDeviceSynchronize());
+    }
+  }
+  if (dE_dR) {
+    const int natom = (int)ctx->atom_z.size();
+    DevBuf F;
+    if ((rc = F.alloc((size_t)natom * 3 * 8))) return rc;
+    PWB_CUDA(cudaMemset(F.p, 0, (size_t)natom * 3 * 8));
+    // E_nl = sum_b w_b sum_l D_l (q_l . psi_b)^2 with q_l = T beta_l(. - R_a):
+    // dE/dR_a,d = -2 sum_b w_b sum_{l in a} D_l (q_l . psi_b)(T(d_d beta_l) . psi_b)
+    std::vector<double> cb(nband);
+    for (int b = 0; b < nband; ++b) cb[b] = -2.0 * w[b];
+    if ((rc = nl_contract(ctx, (const double*)psi, ld, nband, cb, true, (double*)F.p))) return rc;
+    PWB_CUDA(cudaMemcpy(dE_dR, F.p, (size_t)natom * 3 * 8, cudaMemcpyDeviceToHost));
+  }
+  return PW_OK;
+}
+
+int pw_scf_state(const pw_ctx* ctx, int* nband, double* occ, double* psi_dev, int ldpsi, double* rho_dev) {
+  PWB_CHECK(ctx, PW_EINVAL, "null context");
+  PWB_CHECK(ctx->scf_nband > 0, PW_ENOTREADY, "no FP64 SCF state (run pw_scf_run to the FP64 stage first)");
+  const int nb = ctx->scf_nband;
+  if (nband) *nband = nb;
+  if (occ) std::copy(ctx->scf_occ.begin(), ctx->scf_occ.end(), occ);
+  if (psi_dev) {
+    PWB_CHECK(ldpsi >= ctx->ntot, PW_EINVAL, "Domain size does not match.");
+    PWB_CUDA(cudaMemcpy2D(psi_dev, (size_t)ldpsi * 8, ctx->scf_psi.p, (size_t)ctx->ntot * 8, (size_t)ctx->ntot * 8, nb,
+                          cudaMemcpyDeviceToDevice));
+  }
+  if (rho_dev) PWB_CUDA(cudaMemcpy(rho_dev, ctx->scf_rho.p, ctx->ntotf * 8, cudaMemcpyDeviceToDevice));
   return PW_OK;
 }
 
