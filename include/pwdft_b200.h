@@ -15,6 +15,8 @@
 #ifndef PWDFT_B200_H
 #define PWDFT_B200_H
 
+#include <stddef.h>
+
 #if defined(__GNUC__)
 #define PW_API __attribute__((visibility("default")))
 #else
@@ -148,7 +150,7 @@ PW_API int pw_stats(const pw_ctx* ctx, long* kernel_launches, long* library_call
  * launches of one kernel kind: 0 coarse-plane FFT, 1 z-pad, 2 fine-plane
  * projector gather, 3 projector reduce, 4 fine-plane apply, 5 z-fold,
  * 6 coarse-plane inverse, 7 Teter z-pencil, 8 Gram, 9 density, 10 other,
- * 11 vendor-library GEMM. */
+ * 11 vendor-library GEMM, 12 exact-exchange pair FFTs. */
 PW_API int pw_profile(pw_ctx* ctx, int enable);
 PW_API int pw_profile_read(pw_ctx* ctx, int kind, double* total_ms, long* count);
 
@@ -240,6 +242,45 @@ PW_API int pw_ctx_build_twin(pw_ctx* ctx);
  * energies of scf.cpp:1834-2140, all on the device.  eig_out: host, nocc+nextra
  * doubles; rho_out: host, N_fine doubles (either may be NULL). */
 PW_API int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* eig_out, double* rho_out);
+
+/* Hybrid exact exchange (Gamma point, real bands).  Modes of the exchange
+ * term inside pw_hpsi: off, the full pair-FFT operator
+ * (Spinor::AddMultSpinorEXX, src/SCF/spinor.cpp:682-781) or the ACE operator
+ * (KohnSham::MultSpinor, src/SCF/hamiltonian.cpp:3135-3218). */
+enum { PW_EXX_OFF = 0, PW_EXX_FULL = 1, PW_EXX_ACE = 2 };
+
+/* Coulomb kernel of KohnSham::InitializeEXX (src/SCF/hamiltonian.cpp:3454-3551):
+ * v(G) = 4 pi / |G|^2 (times 1 - exp(-|G|^2 / 4 mu^2) when screen_mu > 0),
+ * G = 0 set to -exxDiv (+ pi / mu^2), exxDiv from divergence_type 0 (none) or
+ * 1 (auxiliary function with alpha = 10 / (2 Ecut)).  exx_fraction is the
+ * mixing alpha (0.25 for PBE0). */
+PW_API int pw_exx_setup(pw_ctx* ctx, double exx_fraction, double screen_mu, int divergence_type,
+                        double ecut_wavefunction);
+/* exxDiv and the kernel on the full coarse spectrum (host, N_coarse doubles;
+ * either pointer may be NULL). */
+PW_API int pw_exx_get(const pw_ctx* ctx, double* exx_div, double* kern_host);
+/* Exchange orbitals phi = sqrt(N_c / vol) psi with their occupation rates
+ * (KohnSham::SetPhiEXX, hamiltonian.cpp:3554-3641).  psi: device, context
+ * precision, nphi columns; occ: host, nphi. */
+PW_API int pw_exx_set_phi(pw_ctx* ctx, const void* psi, int ld, int nphi, const double* occ);
+PW_API int pw_exx_set_mode(pw_ctx* ctx, int mode);
+/* Device memory budget for the exchange pair fields (default 1 GiB); V_x psi
+ * runs in batches of (band, orbital pair) fields that fit it. */
+PW_API int pw_exx_set_scratch(pw_ctx* ctx, size_t bytes);
+/* out (+)= V_x psi for nband bands (AddMultSpinorEXX), device pointers. */
+PW_API int pw_exx_apply(pw_ctx* ctx, const void* psi, int ld, void* out, int ldo, int nband, int accumulate,
+                        void* stream);
+/* ACE operator from nband bands (KohnSham::CalculateVexxACE,
+ * hamiltonian.cpp:3686-3818): W = V_x psi, M = -psi^T W = L L^T, xi = W L^-T;
+ * switches the context to PW_EXX_ACE. */
+PW_API int pw_ace_build(pw_ctx* ctx, const void* psi, int ld, int nband);
+/* out += -xi (xi^T psi) (the ACE term alone). */
+PW_API int pw_ace_apply(pw_ctx* ctx, const void* psi, int ld, void* out, int ldo, int nband, void* stream);
+/* Exchange energy num_spin / 2 * sum_j occ_j psi_j^T V_x psi_j
+ * (KohnSham::CalculateEXXEnergy, hamiltonian.cpp:3936-4192), with the full
+ * operator (use_ace = 0) or the ACE operator (use_ace = 1); e: host. */
+PW_API int pw_exx_energy(pw_ctx* ctx, const void* psi, int ld, int nband, const double* occ, int num_spin,
+                         int use_ace, double* e);
 
 /* Atomic forces of an FP64 context with atoms (pw_set_atoms),
  * KohnSham::CalculateForce (src/SCF/hamiltonian.cpp:2670-3056), pseudocharge

@@ -34,6 +34,7 @@ lib = _load()
 _vp, _i, _l, _d = C.c_void_p, C.c_int, C.c_long, C.c_double
 _ip, _dp = C.POINTER(C.c_int), C.POINTER(C.c_double)
 
+PW_EXX_OFF, PW_EXX_FULL, PW_EXX_ACE = 0, 1, 2
 PW_SOLVER_LOBPCG, PW_SOLVER_CHEBFSI = 0, 1
 
 
@@ -92,6 +93,15 @@ SIGNATURES: dict[str, tuple] = {
     "pw_scf_forces": (_i, [_vp, _dp, _dp, _dp]),
     "pw_band_energy": (_i, [_vp, _vp, _i, _i, _dp, _dp]),
     "pw_scf_state": (_i, [_vp, _ip, _dp, _vp, _i, _vp]),
+    "pw_exx_setup": (_i, [_vp, _d, _d, _i, _d]),
+    "pw_exx_get": (_i, [_vp, _dp, _dp]),
+    "pw_exx_set_phi": (_i, [_vp, _vp, _i, _i, _dp]),
+    "pw_exx_set_mode": (_i, [_vp, _i]),
+    "pw_exx_set_scratch": (_i, [_vp, C.c_size_t]),
+    "pw_exx_apply": (_i, [_vp, _vp, _i, _vp, _i, _i, _i, _vp]),
+    "pw_ace_build": (_i, [_vp, _vp, _i, _i]),
+    "pw_ace_apply": (_i, [_vp, _vp, _i, _vp, _i, _i, _vp]),
+    "pw_exx_energy": (_i, [_vp, _vp, _i, _i, _dp, _i, _i, _dp]),
     "pw_band_energy_backward": (_i, [_vp, _vp, _i, _i, _dp, _vp, _dp]),
 }
 

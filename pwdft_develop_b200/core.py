@@ -240,7 +240,7 @@ Context.profile_read = _ctx_profile_read
 
 KERNEL_KINDS = {0: "coarse_xy_fwd", 1: "z_pad", 2: "fine_plane_gather", 3: "nl_reduce", 4: "fine_plane_apply",
                 5: "z_fold", 6: "coarse_xy_inv", 7: "z_teter", 8: "gram", 9: "density", 10: "other",
-                11: "library_gemm"}
+                11: "library_gemm", 12: "exchange"}
 
 
 # ---------------------------------------------------------------------------
@@ -369,6 +369,67 @@ def _ctx_scf_state(self):
     return occ, psi, rho
 
 
+def _ctx_exx_setup(self, fraction: float = 0.25, screen_mu: float = 0.0, divergence_type: int = 1,
+                   ecut: float = 10.0):
+    """InitializeEXX: Coulomb kernel (PBE0: fraction 0.25, mu 0)."""
+    check(lib.pw_exx_setup(self._h, float(fraction), float(screen_mu), int(divergence_type), float(ecut)))
+
+
+def _ctx_exx_kernel(self):
+    """(exxDiv, kernel on the full coarse spectrum as an (n2, n1, n0) array)."""
+    d = C.c_double(0.0)
+    k = np.zeros(self.ntot)
+    check(lib.pw_exx_get(self._h, C.byref(d), k.ctypes.data_as(_lib._dp)))
+    return d.value, k.reshape(self.numGrid[2], self.numGrid[1], self.numGrid[0])
+
+
+def _ctx_exx_set_phi(self, psi, occ):
+    occ = np.ascontiguousarray(occ, np.float64)
+    check(lib.pw_exx_set_phi(self._h, _ptr(psi), self.ntot, psi.shape[0], occ.ctypes.data_as(_lib._dp)))
+
+
+def _ctx_exx_set_mode(self, mode: str):
+    m = {"off": _lib.PW_EXX_OFF, "full": _lib.PW_EXX_FULL, "ace": _lib.PW_EXX_ACE}[mode]
+    check(lib.pw_exx_set_mode(self._h, m))
+
+
+def _ctx_exx_apply(self, psi, out=None, accumulate: bool = False, stream=None):
+    import torch
+    if out is None:
+        out = torch.zeros_like(psi)
+    check(lib.pw_exx_apply(self._h, _ptr(psi), self.ntot, _ptr(out), self.ntot, psi.shape[0], int(accumulate),
+                           _stream(stream)))
+    return out
+
+
+def _ctx_ace_build(self, psi):
+    check(lib.pw_ace_build(self._h, _ptr(psi), self.ntot, psi.shape[0]))
+
+
+def _ctx_ace_apply(self, psi, out=None, stream=None):
+    import torch
+    if out is None:
+        out = torch.zeros_like(psi)
+    check(lib.pw_ace_apply(self._h, _ptr(psi), self.ntot, _ptr(out), self.ntot, psi.shape[0], _stream(stream)))
+    return out
+
+
+def _ctx_exx_energy(self, psi, occ, num_spin: int = 2, use_ace: bool = False) -> float:
+    occ = np.ascontiguousarray(occ, np.float64)
+    e = C.c_double(0.0)
+    check(lib.pw_exx_energy(self._h, _ptr(psi), self.ntot, psi.shape[0], occ.ctypes.data_as(_lib._dp),
+                            int(num_spin), int(use_ace), C.byref(e)))
+    return e.value
+
+
+Context.exx_setup = _ctx_exx_setup
+Context.exx_kernel = _ctx_exx_kernel
+Context.exx_set_phi = _ctx_exx_set_phi
+Context.exx_set_mode = _ctx_exx_set_mode
+Context.exx_apply = _ctx_exx_apply
+Context.ace_build = _ctx_ace_build
+Context.ace_apply = _ctx_ace_apply
+Context.exx_energy = _ctx_exx_energy
 Context.scf_state = _ctx_scf_state
 Context.band_energy = _ctx_band_energy
 Context.band_energy_backward = _ctx_band_energy_backward

@@ -61,7 +61,18 @@ struct NonlocalDev {
 // Kernel kinds for pw_profile_read.
 enum KernelKind {
   KK_CXY_FWD = 0, KK_ZPAD, KK_FPLANE_GATHER, KK_NL_REDUCE, KK_FPLANE_APPLY, KK_ZFOLD, KK_CXY_INV, KK_ZTETER,
-  KK_GRAM, KK_DENSITY, KK_MISC, KK_LIBGEMM, KK_COUNT
+  KK_GRAM, KK_DENSITY, KK_MISC, KK_LIBGEMM, KK_EXX, KK_COUNT
+};
+
+// A dense coarse-grid operator Q diag(qd) Q^T: the projector matrix, or the
+// ACE vectors with qd = -1.  q: T [np][ntot]; q_bf / qt_bf: split-BF16 copies
+// (FP32 contexts) of Q (np x ntot) and Q^T (ntot x npp, npp = np padded to 8).
+struct DenseSet {
+  const void* q;
+  const void* qd;
+  const void* q_bf;
+  const void* qt_bf;
+  int np, npp;
 };
 
 }  // namespace pwb
@@ -110,6 +121,18 @@ struct pw_ctx {
   std::vector<long> h_ps_off;              // natom + 1 offsets into h_ps_idx / h_ps_val
   std::vector<int> h_ps_idx;               // per-atom pseudocharge support (fine-grid index)
   std::vector<double> h_ps_val;            // per-atom pseudocharge values
+  // hybrid exchange (AddMultSpinorEXX / CalculateVexxACE)
+  int exx_mode = 0;                 // PW_EXX_OFF / PW_EXX_FULL / PW_EXX_ACE
+  double exx_frac = 0.0, exx_mu = 0.0, exx_div = 0.0;
+  pwb::DevBuf exx_kern;             // T [ntot]  Coulomb kernel on the full coarse spectrum
+  pwb::DevBuf exx_phi;              // T [nphi][ntot]  phi = sqrt(N_c / vol) psi
+  pwb::DevBuf exx_w;                // T [nphi]  -exx_frac * occupation
+  std::vector<double> exx_occ;      // host copy of the occupations of phi
+  int exx_nphi = 0;
+  pwb::DevBuf s_exx;                // pair-field scratch
+  size_t exx_scratch_bytes = (size_t)1 << 30;
+  pwb::DevBuf ace_xi, ace_qd, ace_bf, ace_t_bf;   // ACE vectors xi (T [nace][ntot]) and -1 weights
+  int ace_n = 0, ace_npad = 0;
   // converged SCF state kept for pw_scf_forces: FP64 bands, occupations, density
   pwb::DevBuf scf_psi, scf_rho;
   std::vector<double> scf_occ;

@@ -346,6 +346,96 @@ k_fplane(VT<T>* __restrict__ BC, const T* __restrict__ vtot, NLArgs nl, VT<T>* _
 
 
 // ---------------------------------------------------------------------------
+// exact exchange pair fields (AddMultSpinorEXX, src/SCF/spinor.cpp:682-781).
+// Field f = (band k0 + f / njp, orbital pair jp = f % njp): the plane of
+// psi_k (phi_ja + i phi_jb), ja = j0 + 2 jp, jb = ja + 1 (zero past nphi),
+// forward 2-D FFT in shared memory, stored like k_cxy_fwd's output.
+// ---------------------------------------------------------------------------
+template <typename T, int N0, int N1>
+__global__ void __launch_bounds__(PLANE_THREADS)
+k_exx_fwd(const T* __restrict__ psi, int ld, int k0, const T* __restrict__ phi, int ldp, int j0, int nphi, int njp,
+          VT<T>* __restrict__ A, const VT<T>* twx_g, const VT<T>* twy_g) {
+  using V = VT<T>;
+  constexpr int P0 = N0 + 1;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  V* pl = reinterpret_cast<V*>(smraw);
+  V* twx = pl + N1 * P0;
+  V* twy = twx + N0;
+  load_tw(twx, twx_g, N0);
+  load_tw(twy, twy_g, N1);
+  const int z = blockIdx.x, f = blockIdx.y;
+  const int kk = f / njp, jp = f - kk * njp;
+  const long ntot_plane = (long)N0 * N1;
+  const int ja = j0 + 2 * jp, jb = ja + 1;
+  const T* pk = psi + (long)(k0 + kk) * ld + z * ntot_plane;
+  const T* pa = phi + (long)ja * ldp + z * ntot_plane;
+  const T* pb = (jb < nphi) ? phi + (long)jb * ldp + z * ntot_plane : nullptr;
+  for (int i = threadIdx.x; i < N0 * N1; i += blockDim.x) {
+    const int y = i / N0, x = i - y * N0;
+    const T v = pk[i];
+    pl[y * P0 + x] = mkc<V>(v * pa[i], pb ? v * pb[i] : (T)0);
+  }
+  __syncthreads();
+  smem_fft_cb<N0, -1, 1, P0>(pl, N1, twx);
+  __syncthreads();
+  smem_fft_cb<N1, -1, P0, 1>(pl, N0, twy);
+  __syncthreads();
+  const int N2 = gridDim.x;
+  V* Ap = A + ((long)f * N2 + z) * ntot_plane;
+  for (int i = threadIdx.x; i < N0 * N1; i += blockDim.x) {
+    const int y = i / N0, x = i - y * N0;
+    Ap[i] = pl[y * P0 + x];
+  }
+}
+
+// inverse 2-D FFT of the njp fields of band k0 + blockIdx.y on plane z and
+// out_k (+)= sum_jp w_ja phi_ja Re + w_jb phi_jb Im, accumulated in shared memory
+template <typename T, int N0, int N1>
+__global__ void __launch_bounds__(PLANE_THREADS)
+k_exx_inv(const VT<T>* __restrict__ A, int njp, const T* __restrict__ phi, int ldp, int j0, int nphi,
+          const T* __restrict__ wj, T* __restrict__ out, int ldo, int k0, int accumulate, const VT<T>* twx_g,
+          const VT<T>* twy_g) {
+  using V = VT<T>;
+  constexpr int P0 = N0 + 1;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  V* pl = reinterpret_cast<V*>(smraw);
+  V* twx = pl + N1 * P0;
+  V* twy = twx + N0;
+  T* acc = reinterpret_cast<T*>(twy + N1);
+  load_tw(twx, twx_g, N0);
+  load_tw(twy, twy_g, N1);
+  const int z = blockIdx.x, kk = blockIdx.y;
+  const int N2 = gridDim.x;
+  const long ntot_plane = (long)N0 * N1;
+  for (int i = threadIdx.x; i < N0 * N1; i += blockDim.x) acc[i] = (T)0;
+  for (int jp = 0; jp < njp; ++jp) {
+    const V* Dp = A + ((long)(kk * njp + jp) * N2 + z) * ntot_plane;
+    __syncthreads();
+    for (int i = threadIdx.x; i < N0 * N1; i += blockDim.x) {
+      const int y = i / N0, x = i - y * N0;
+      pl[y * P0 + x] = Dp[i];
+    }
+    __syncthreads();
+    smem_fft_cb<N1, +1, P0, 1>(pl, N0, twy);
+    __syncthreads();
+    smem_fft_cb<N0, +1, 1, P0>(pl, N1, twx);
+    __syncthreads();
+    const int ja = j0 + 2 * jp, jb = ja + 1;
+    const T wa = wj[ja], wb = (jb < nphi) ? wj[jb] : (T)0;
+    const T* pa = phi + (long)ja * ldp + z * ntot_plane;
+    const T* pb = (jb < nphi) ? phi + (long)jb * ldp + z * ntot_plane : pa;
+    for (int i = threadIdx.x; i < N0 * N1; i += blockDim.x) {
+      const int y = i / N0, x = i - y * N0;
+      const V v = pl[y * P0 + x];
+      acc[i] += wa * pa[i] * v.x + wb * pb[i] * v.y;
+    }
+  }
+  __syncthreads();
+  T* o = out + (long)(k0 + kk) * ldo + z * ntot_plane;
+  for (int i = threadIdx.x; i < N0 * N1; i += blockDim.x) o[i] = accumulate ? o[i] + acc[i] : acc[i];
+}
+
+// ---------------------------------------------------------------------------
 // fine plane, local potential only (the projectors are applied on the coarse
 // grid as dense GEMMs): IFFT y on the slot columns, then per warp a group of
 // rows: IFFT x, * V_loc, FFT x, truncate; FFT y; truncate.  MODE 1 starts
@@ -783,6 +873,7 @@ struct Plan {
   static size_t sm_zpad() { return sizeof(V) * (N2 * (TX + 1) + NF2 * (2 * TX + 1) + N2 + NF2); }
   static size_t sm_zfold() { return sizeof(V) * (NF2 * (2 * TX + 1) + N2 * (TX + 1) + N2 + NF2); }
   static size_t sm_zteter() { return sizeof(V) * (N2 * (TX + 1) + N2); }
+  static size_t sm_exx_inv() { return sm_cxy() + sizeof(T) * N0 * N1; }
   static size_t sm_floc() {
     return sizeof(V) * ((size_t)NF1 * (N0 + 1) + NF0 + NF1 + (size_t)(FLOC_THREADS / 32) * FftGroup<NF0>::f * (NF0 + 1));
   }
@@ -837,8 +928,10 @@ struct Plan {
       k_cxy_inv<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(AD, out, ldo, nband, band0, accumulate, tw(c, 0), tw(c, 1)); }
       PWB_CUDA(cudaGetLastError());
       const int nb = std::min(2 * npair, nband - band0);
-      if (c->have_nl && c->nproj > 0 && nb > 0) return dense_nl(c, psi + (long)band0 * ld, ld, out + (long)band0 * ldo, ldo, nb, st);
-      return PW_OK;
+      if (c->have_nl && c->nproj > 0 && nb > 0)
+        if ((rc = dense_apply(c, nl_set(c), psi + (long)band0 * ld, ld, out + (long)band0 * ldo, ldo, nb, st)))
+          return rc;
+      return exchange_batch(c, psi, ld, out, ldo, nband, band0, npair, st);
     }
     NLArgs nl{};
     const int cr = chunk_rows();
@@ -874,20 +967,90 @@ struct Plan {
     { Launch L_(c, st, KK_CXY_INV);
     k_cxy_inv<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(AD, out, ldo, nband, band0, accumulate, tw(c, 0), tw(c, 1)); }
     PWB_CUDA(cudaGetLastError());
+    return exchange_batch(c, psi, ld, out, ldo, nband, band0, npair, st);
+  }
+
+  // exact exchange of the batch's bands: the ACE operator (two GEMMs) or the
+  // full pair-FFT exchange, depending on the context's hybrid mode
+  static int exchange_batch(pw_ctx* c, const T* psi, int ld, T* out, int ldo, int nband, int band0, int npair,
+                            cudaStream_t st) {
+    const int nb = std::min(2 * npair, nband - band0);
+    if (nb <= 0 || c->exx_mode == PW_EXX_OFF) return PW_OK;
+    if (c->exx_mode == PW_EXX_ACE) {
+      if (c->ace_n == 0) return PW_OK;
+      DenseSet ds{c->ace_xi.p, c->ace_qd.p, c->ace_bf.p, c->ace_t_bf.p, c->ace_n, c->ace_npad};
+      return dense_apply(c, ds, psi + (long)band0 * ld, ld, out + (long)band0 * ldo, ldo, nb, st);
+    }
+    return exx_apply(c, psi + (long)band0 * ld, ld, nb, out + (long)band0 * ldo, ldo, 1, st);
+  }
+
+  static DenseSet nl_set(pw_ctx* c) { return DenseSet{c->q.p, c->qd.p, c->q_bf.p, c->qt_bf.p, c->nproj, c->nproj_pad}; }
+
+  // out (+)= V_x psi, AddMultSpinorEXX (src/SCF/spinor.cpp:682-781): for every
+  // band k and exchange orbital j, out_k -= alpha f_j phi_j (1/N_c) IFFT(v FFT(psi_k phi_j)).
+  // Two orbitals share one complex field (v is real and even, so the real and
+  // imaginary parts stay separate); batches of (band, orbital pair) fields.
+  static int exx_apply(pw_ctx* c, const T* psi, int ld, int nb, T* out, int ldo, int accumulate, cudaStream_t st) {
+    int rc = set_attrs();
+    if (rc) return rc;
+    static bool attr = false;
+    if (!attr) {
+      PWB_CUDA(cudaFuncSetAttribute(k_exx_fwd<T, N0, N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_cxy()));
+      PWB_CUDA(cudaFuncSetAttribute(k_exx_inv<T, N0, N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_exx_inv()));
+      attr = true;
+    }
+    const int nphi = c->exx_nphi;
+    if (nphi == 0 || nb == 0) {
+      if (!accumulate && nb > 0)
+        PWB_CUDA(cudaMemset2DAsync(out, (size_t)ldo * sizeof(T), 0, (size_t)c->ntot * sizeof(T), nb, st));
+      return PW_OK;
+    }
+    const long nt = c->ntot;
+    const int njp = (nphi + 1) / 2;
+    const long cap = std::max<long>(1, (long)(c->exx_scratch_bytes / ((size_t)nt * sizeof(V))));
+    const int jc = (int)std::min<long>(njp, std::max<long>(1, cap / nb));
+    const int kc = (int)std::max<long>(1, std::min<long>(nb, cap / jc));
+    if ((rc = c->s_exx.alloc((size_t)kc * jc * nt * sizeof(V)))) return rc;
+    V* A = reinterpret_cast<V*>(c->s_exx.p);
+    const T* phi = reinterpret_cast<const T*>(c->exx_phi.p);
+    const T* wj = reinterpret_cast<const T*>(c->exx_w.p);
+    const T* kern = reinterpret_cast<const T*>(c->exx_kern.p);
+    const T inv_nc = (T)(1.0 / (double)nt);
+    const int ntx = (N0 + TX - 1) / TX;
+    for (int k0 = 0; k0 < nb; k0 += kc) {
+      const int nk = std::min(kc, nb - k0);
+      for (int jp0 = 0; jp0 < njp; jp0 += jc) {
+        const int nj = std::min(jc, njp - jp0);
+        { Launch L_(c, st, KK_EXX);
+        k_exx_fwd<T, N0, N1><<<dim3(N2, nk * nj), PLANE_THREADS, sm_cxy(), st>>>(
+            psi, ld, k0, phi, (int)nt, 2 * jp0, nphi, nj, A, tw(c, 0), tw(c, 1)); }
+        { Launch L_(c, st, KK_EXX);
+        k_zteter<T, N2><<<dim3(N1, ntx, nk * nj), PENCIL_THREADS, sm_zteter(), st>>>(A, kern, N0, N1, inv_nc, tw(c, 2)); }
+        { Launch L_(c, st, KK_EXX);
+        k_exx_inv<T, N0, N1><<<dim3(N2, nk), PLANE_THREADS, sm_exx_inv(), st>>>(
+            A, nj, phi, (int)nt, 2 * jp0, nphi, wj, out, ldo, k0, (accumulate || jp0 > 0) ? 1 : 0, tw(c, 0),
+            tw(c, 1)); }
+        PWB_CUDA(cudaGetLastError());
+      }
+    }
     return PW_OK;
   }
 
-  // H psi += Q diag(qd) Q^T psi  for nb bands (column-major, ld)
-  static int dense_nl(pw_ctx* c, const T* psi, int ld, T* out, int ldo, int nb, cudaStream_t st) {
+  // H psi += Q diag(qd) Q^T psi  for nb bands (column-major, ld); Q is the
+  // coarse projector matrix or the ACE vectors (qd = -1)
+  static int dense_apply(pw_ctx* c, const DenseSet& ds, const T* psi, int ld, T* out, int ldo, int nb,
+                         cudaStream_t st) {
     if constexpr (std::is_same<T, float>::value) {
-      if (c->gemm_mode == 0) return dense_nl_tc(c, psi, ld, out, ldo, nb, st);
+      if (c->gemm_mode == 0) return dense_apply_tc(c, ds, psi, ld, out, ldo, nb, st);
     }
     cublasHandle_t h = (cublasHandle_t)c->blas;
     if (cublasSetStream(h, st) != CUBLAS_STATUS_SUCCESS) { set_error("cublasSetStream failed"); return PW_ECUDA; }
+    const int np = ds.np, nt = (int)c->ntot;
+    int rc;
+    if ((rc = c->s_wq.alloc((size_t)np * nb * sizeof(T)))) return rc;
     T* W = reinterpret_cast<T*>(c->s_wq.p);
-    const T* Q = reinterpret_cast<const T*>(c->q.p);
+    const T* Q = reinterpret_cast<const T*>(ds.q);
     const T one = 1, zero = 0;
-    const int np = c->nproj, nt = (int)c->ntot;
     cublasStatus_t r;
     { Launch L_(c, st, KK_LIBGEMM);
     if constexpr (std::is_same<T, double>::value)
@@ -896,7 +1059,7 @@ struct Plan {
       r = cublasSgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, np, nb, nt, &one, Q, nt, psi, ld, &zero, W, np); }
     if (r != CUBLAS_STATUS_SUCCESS) { set_error("projector GEMM (Q^T psi) failed"); return PW_ECUDA; }
     { Launch L_(c, st, KK_MISC);
-    k_scale_rows<T><<<(unsigned)(((long)np * nb + 255) / 256), 256, 0, st>>>(W, reinterpret_cast<const T*>(c->qd.p), np, nb); }
+    k_scale_rows<T><<<(unsigned)(((long)np * nb + 255) / 256), 256, 0, st>>>(W, reinterpret_cast<const T*>(ds.qd), np, nb); }
     { Launch L_(c, st, KK_LIBGEMM);
     if constexpr (std::is_same<T, double>::value)
       r = cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, nt, nb, np, &one, Q, nt, W, np, &one, out, ldo);
@@ -935,8 +1098,9 @@ struct Plan {
   }
 
   // FP32 context: split-BF16 tcgen05 GEMMs
-  static int dense_nl_tc(pw_ctx* c, const float* psi, int ld, float* out, int ldo, int nb, cudaStream_t st) {
-    const int np = c->nproj, nt = (int)c->ntot, npp = c->nproj_pad;
+  static int dense_apply_tc(pw_ctx* c, const DenseSet& ds, const float* psi, int ld, float* out, int ldo, int nb,
+                            cudaStream_t st) {
+    const int np = ds.np, nt = (int)c->ntot, npp = ds.npp;
     int rc;
     if ((rc = c->s_psi_bf.alloc((size_t)2 * nb * nt * 2))) return rc;
     if ((rc = c->s_w_bf.alloc((size_t)2 * nb * npp * 2))) return rc;
@@ -945,11 +1109,11 @@ struct Plan {
     { Launch L_(c, st, KK_MISC);
     if ((rc = split_bf16(psi, ld, nt, nb, pb, pb + (size_t)nb * nt * 2, nt, 1.0f, st))) return rc; }
     // W^T[b][l] = d_l * sum_g Q[l][g] psi[b][g]   (split-K, deterministic reduce)
-    SplitOperand A{c->q_bf.p, (char*)c->q_bf.p + (size_t)np * nt * 2, np, nt};
+    SplitOperand A{ds.q_bf, (const char*)ds.q_bf + (size_t)np * nt * 2, np, nt};
     SplitOperand B{pb, pb + (size_t)nb * nt * 2, nb, nt};
     ReduceOut ro;
     ro.transpose = 1;
-    ro.row_scale = reinterpret_cast<const float*>(c->qd.p);
+    ro.row_scale = reinterpret_cast<const float*>(ds.qd);
     ro.bf_hi = wb;
     ro.bf_lo = wb + (size_t)nb * npp * 2;
     ro.ldb = npp;
@@ -957,7 +1121,7 @@ struct Plan {
     if ((rc = gemm_tn_reduce(A, B, nt, c->gemm_terms, c->s_ws, ro, st))) return rc; }
     // out[b][g] += sum_l QT[g][l] W^T[b][l]  (tile rows = grid points: coalesced stores)
     SplitOperand W{wb, wb + (size_t)nb * npp * 2, nb, npp};
-    SplitOperand QT{c->qt_bf.p, (char*)c->qt_bf.p + (size_t)nt * npp * 2, nt, npp};
+    SplitOperand QT{ds.qt_bf, (const char*)ds.qt_bf + (size_t)nt * npp * 2, nt, npp};
     { Launch L_(c, st, KK_GRAM);
     if ((rc = gemm_tn_store(QT, W, np, c->gemm_terms, out, ldo, 1, st, 1))) return rc; }
     return PW_OK;
@@ -1072,6 +1236,19 @@ static int buildq_thunk(pw_ctx* c, const int* a, const double* b, const long* d,
   return Plan<T, N0, N1, N2>::build_q(c, a, b, d, e, f, n, st, deriv, (T*)out);
 }
 
+using ExxFn = int (*)(pw_ctx*, const void*, int, int, void*, int, int, cudaStream_t);
+template <typename T, int N0, int N1, int N2>
+static int exx_thunk(pw_ctx* c, const void* psi, int ld, int nb, void* out, int ldo, int acc, cudaStream_t st) {
+  return Plan<T, N0, N1, N2>::exx_apply(c, (const T*)psi, ld, nb, (T*)out, ldo, acc, st);
+}
+
+template <typename T, int N0, int N1, int N2>
+static int ace_thunk(pw_ctx* c, const void* psi, int ld, int nb, void* out, int ldo, int acc, cudaStream_t st) {
+  (void)acc;
+  DenseSet ds{c->ace_xi.p, c->ace_qd.p, c->ace_bf.p, c->ace_t_bf.p, c->ace_n, c->ace_npad};
+  return Plan<T, N0, N1, N2>::dense_apply(c, ds, (const T*)psi, ld, (T*)out, ldo, nb, st);
+}
+
 struct GridEntry {
   int n0, n1, n2;
   HpsiFn hpsi[2];
@@ -1080,6 +1257,8 @@ struct GridEntry {
   BuildQFn bq[2];
   DensFn dens[2];
   TeterScratchFn teter_scratch[2];
+  ExxFn exx[2];
+  ExxFn ace[2];
 };
 
 #define PWB_GRID(a, b, c)                                                                          \
@@ -1088,7 +1267,9 @@ struct GridEntry {
    {cr_thunk<double, a, b, c>, cr_thunk<float, a, b, c>},                                          \
    {buildq_thunk<double, a, b, c>, buildq_thunk<float, a, b, c>},                                  \
    {dens_thunk<double, a, b, c>, dens_thunk<float, a, b, c>},                                      \
-   {teter_scratch_thunk<double, a, b, c>, teter_scratch_thunk<float, a, b, c>}},
+   {teter_scratch_thunk<double, a, b, c>, teter_scratch_thunk<float, a, b, c>},                    \
+   {exx_thunk<double, a, b, c>, exx_thunk<float, a, b, c>},                                        \
+   {ace_thunk<double, a, b, c>, ace_thunk<float, a, b, c>}},
 
 static const GridEntry kGrids[] = {
 #include "grids.inc"
@@ -1125,6 +1306,18 @@ int run_density(pw_ctx* c, const void* psi, int ld, int nband, int band0, int np
   const GridEntry* g = find_grid(c->n);
   if (!g) { set_error("grid not built into this library"); return PW_EUNSUPPORTED; }
   return g->dens[c->prec == PW_F32 ? 1 : 0](c, psi, ld, nband, band0, npair, w, rho, st);
+}
+
+int run_exx(pw_ctx* c, const void* psi, int ld, int nb, void* out, int ldo, int acc, cudaStream_t st) {
+  const GridEntry* g = find_grid(c->n);
+  if (!g) { set_error("grid not built into this library"); return PW_EUNSUPPORTED; }
+  return g->exx[c->prec == PW_F32 ? 1 : 0](c, psi, ld, nb, out, ldo, acc, st);
+}
+
+int run_ace(pw_ctx* c, const void* psi, int ld, int nb, void* out, int ldo, cudaStream_t st) {
+  const GridEntry* g = find_grid(c->n);
+  if (!g) { set_error("grid not built into this library"); return PW_EUNSUPPORTED; }
+  return g->ace[c->prec == PW_F32 ? 1 : 0](c, psi, ld, nb, out, ldo, 1, st);
 }
 
 int run_teter(pw_ctx* c, const void* r, int ld, void* out, int ldo, int nband, int band0, int npair, int acc,

@@ -1,0 +1,121 @@
+"""Hybrid exchange on the device against the FP64 oracle (oracle/exx.py):
+Coulomb kernel, V_x psi (AddMultSpinorEXX), ACE build/apply, H*psi with the
+exchange term, exchange energy.  Tolerances: FP64 1e-12 relative (kernel,
+V_x psi, energies) and 1e-10 for the ACE factorisation; FP32 pair FFTs 1e-5
+relative on V_x psi and 1e-6 Ha/atom on the exchange energy."""
+import numpy as np
+import pytest
+
+from oracle import exx, pw
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(nc=(16, 16, 16), nb=12, nphi=11):
+    L, z, pos = pw.make_crystal("Si", (1, 1, 1), 10.26, 0.02, 20261203 + 4)
+    nf = tuple(2 * n for n in nc)
+    T, _ = pw.build_tables(L, z, pos, nc, nf, seed_v=2)
+    psi = pw.random_orthonormal_psi(T.dm.ntot, nb, 17)
+    occ = np.ones(nphi)
+    occ[-3:] = [0.6, 0.25, 0.0]
+    return L, z, pos, nc, nf, T, psi, occ
+
+
+def _ctx(L, z, pos, nc, nf, T, prec, ecut=10.0):
+    from pwdft_develop_b200 import Context
+    c = Context(L, nc, nf, precision=prec)
+    c.set_atoms([z] * len(pos), pos)
+    c.set_vtot(T.vtot)
+    c.exx_setup(0.25, 0.0, 1, ecut)
+    return c
+
+
+def _rel(a, b):
+    return np.abs(a - b).max() / np.abs(b).max()
+
+
+def test_exx_kernel_matches_oracle():
+    L, z, pos, nc, nf, T, psi, occ = _setup()
+    k_ref, div_ref = exx.exx_kernel_r2c(T.dm, 10.0)
+    c = _ctx(L, z, pos, nc, nf, T, "f64")
+    div, k = c.exx_kernel()
+    assert abs(div - div_ref) <= 1e-12 * abs(div_ref)
+    assert _rel(k[:, :, : nc[0] // 2 + 1], k_ref) <= 1e-13
+
+
+@pytest.mark.parametrize("prec,tol", [("f64", 1e-12), ("f32", 1e-5)])
+def test_exx_apply_matches_oracle(prec, tol):
+    import torch
+    L, z, pos, nc, nf, T, psi, occ = _setup()
+    nphi = len(occ)
+    k_ref, _ = exx.exx_kernel_r2c(T.dm, 10.0)
+    ref = exx.add_mult_spinor_exx(T.dm, psi, exx.set_phi(T.dm, psi[:nphi]), k_ref, 0.25, occ)
+    c = _ctx(L, z, pos, nc, nf, T, prec)
+    X = torch.tensor(psi, dtype=c.torch_dtype, device="cuda")
+    c.exx_set_phi(X[:nphi], occ)
+    out = c.exx_apply(X).double().cpu().numpy()
+    assert _rel(out, ref) <= tol
+    # accumulate adds to what is there
+    out2 = c.exx_apply(X, out=torch.ones_like(X), accumulate=True).double().cpu().numpy()
+    assert _rel(out2 - 1.0, ref) <= 10 * tol
+
+
+def test_exx_scratch_batching_is_invisible():
+    """Band / orbital-pair batches sized by the scratch budget give the same result."""
+    import torch
+    L, z, pos, nc, nf, T, psi, occ = _setup()
+    c = _ctx(L, z, pos, nc, nf, T, "f64")
+    X = torch.tensor(psi, device="cuda")
+    c.exx_set_phi(X[: len(occ)], occ)
+    full = c.exx_apply(X).cpu().numpy()
+    lib = __import__("pwdft_develop_b200._lib", fromlist=["lib"]).lib
+    assert lib.pw_exx_set_scratch(c.handle, 3 * c.ntot * 16) == 0     # 3 pair fields per batch
+    small = c.exx_apply(X).cpu().numpy()
+    assert _rel(small, full) <= 1e-14
+
+
+@pytest.mark.parametrize("prec,tol", [("f64", 1e-10), ("f32", 2e-5)])
+def test_ace_and_hpsi_with_exchange(prec, tol):
+    import torch
+    L, z, pos, nc, nf, T, psi, occ = _setup(nphi=12)
+    k_ref, _ = exx.exx_kernel_r2c(T.dm, 10.0)
+    phi = exx.set_phi(T.dm, psi)
+    vx = exx.add_mult_spinor_exx(T.dm, psi, phi, k_ref, 0.25, occ)
+    xi = exx.ace_build(T.dm, psi, phi, k_ref, 0.25, occ)
+    hloc = pw.mult_spinor(T, psi)
+    c = _ctx(L, z, pos, nc, nf, T, prec)
+    X = torch.tensor(psi, dtype=c.torch_dtype, device="cuda")
+    c.exx_set_phi(X, occ)
+    # full exchange inside H*psi
+    c.exx_set_mode("full")
+    assert _rel(c.hpsi(X).double().cpu().numpy(), hloc + vx) <= tol
+    # ACE: exact on span(psi)
+    c.ace_build(X)
+    assert _rel(c.ace_apply(X).double().cpu().numpy(), vx) <= tol
+    assert _rel(c.hpsi(X).double().cpu().numpy(), hloc + exx.ace_apply(xi, psi)) <= tol
+    # on vectors outside the span ACE and the oracle's ACE agree
+    Y = pw.random_orthonormal_psi(T.dm.ntot, 5, 99)
+    got = c.ace_apply(torch.tensor(Y, dtype=c.torch_dtype, device="cuda")).double().cpu().numpy()
+    assert _rel(got, exx.ace_apply(xi, Y)) <= 10 * tol
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_exx_energy(prec):
+    import torch
+    L, z, pos, nc, nf, T, psi, occ = _setup(nphi=12)
+    k_ref, _ = exx.exx_kernel_r2c(T.dm, 10.0)
+    phi = exx.set_phi(T.dm, psi)
+    e_ref = exx.exx_energy(exx.add_mult_spinor_exx(T.dm, psi, phi, k_ref, 0.25, occ), psi, occ)
+    c = _ctx(L, z, pos, nc, nf, T, prec)
+    X = torch.tensor(psi, dtype=c.torch_dtype, device="cuda")
+    c.exx_set_phi(X, occ)
+    e_full = c.exx_energy(X, occ)
+    c.ace_build(X)
+    e_ace = c.exx_energy(X, occ, use_ace=True)
+    nat = len(pos)
+    if prec == "f64":
+        assert abs(e_full - e_ref) <= 1e-12 * abs(e_ref)
+        assert abs(e_ace - e_ref) <= 1e-10 * abs(e_ref)
+    else:
+        assert abs(e_full - e_ref) / nat <= 1e-6, (e_full - e_ref) / nat
+        assert abs(e_ace - e_ref) / nat <= 1e-6, (e_ace - e_ref) / nat
