@@ -8,10 +8,12 @@
 // carrying ~16 mantissa bits this reproduces an FP32 product to ~1e-5
 // relative per term.
 //
-// One CTA computes a 128 x BN tile over a K range: warp 0 issues TMA loads
-// into a ring of shared-memory stages, warp 1 issues the UMMAs (one elected
-// thread) and commits each stage back to the producer, warps 2-5 read the
-// accumulator from TMEM and write the tile.  Two epilogues: a split-K
+// A persistent CTA (one per SM) walks 128 x BN tiles over K ranges: warp 0
+// issues TMA loads into a ring of shared-memory stages, warp 1 issues the
+// UMMAs (one elected thread) and commits each stage back to the producer,
+// warps 2-5 read the accumulator from TMEM and write the tile.  Two TMEM
+// accumulators alternate between tiles so the epilogue of one tile overlaps
+// the loads and MMAs of the next.  Two epilogues: a split-K
 // partial (deterministically reduced by a second kernel) and a direct
 // row-major (optionally accumulating) store.  No cluster multicast is used.
 // Every mbarrier wait is bounded: on timeout the kernel records an error code,
@@ -115,20 +117,30 @@ template <int BN> struct GemmSmem {
   static constexpr int STAGE = 2 * A_BYTES + 2 * B_BYTES;
   static constexpr int NSTAGE = (3 * STAGE + 2048 <= 226 * 1024) ? 3 : 2;
   static constexpr int BYTES = NSTAGE * STAGE + 1024 /*align*/ + 256 /*barriers*/;
-  static constexpr int TMEM_COLS = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
+  // two accumulators (double-buffered across the tiles of a persistent CTA)
+  static constexpr int TMEM_COLS = 2 * BN <= 64 ? 64 : 2 * BN <= 128 ? 128 : 2 * BN <= 256 ? 256 : 512;
 };
 
 struct GemmArgs {
   int M, N, K;           // full problem
   int kchunk;            // K per split (multiple of GK)
+  int nsplit;            // K splits
   int nterms;            // 3 or 4 split products
   int epi;               // 0: split-K partial, 1: row-major store, 2: transposed store
   float* ws;             // epi 0: [split][N][M]
   float* C;              // epi 1: C[m*ldc + n], epi 2: C[n*ldc + m]
   long ldc;
-  int accumulate;        // epi 1: C += tile
+  int accumulate;        // epi 1 / 2: C += tile
 };
 
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
+}
+
+// Persistent CTA: tile t = (m tile, n tile, K split), m fastest, strided by
+// gridDim.x.  The stage ring runs across tiles; the accumulator alternates
+// between two TMEM buffers so that the epilogue of one tile overlaps the
+// loads and MMAs of the next.
 template <int BN>
 __global__ void __launch_bounds__(GEMM_THREADS, 1)
 k_gemm_tn(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant__ CUtensorMap tmA_lo,
@@ -138,22 +150,26 @@ k_gemm_tn(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant__ CU
   unsigned char* base = (unsigned char*)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
   uint64_t* full = reinterpret_cast<uint64_t*>(base + SM::NSTAGE * SM::STAGE);
   uint64_t* empty = full + SM::NSTAGE;
-  uint64_t* accum_bar = empty + SM::NSTAGE;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(accum_bar + 1);
+  uint64_t* tfull = empty + SM::NSTAGE;      // [2] accumulator ready
+  uint64_t* tempty = tfull + 2;              // [2] accumulator drained (4 epilogue warps)
+  uint64_t* final_bar = tempty + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(final_bar + 1);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int m0 = blockIdx.x * GM, n0 = blockIdx.y * BN;
-  const int kbeg = blockIdx.z * g.kchunk;
-  const int kend = min(g.K, kbeg + g.kchunk);
-  const int nkb = (kend > kbeg) ? (kend - kbeg + GK - 1) / GK : 0;
+  const int tilesM = (g.M + GM - 1) / GM, tilesN = (g.N + BN - 1) / BN;
+  const int total = tilesM * tilesN * g.nsplit;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < SM::NSTAGE; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    mbar_init(accum_bar, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&tfull[b], 1);
+      mbar_init(&tempty[b], 4);
+    }
+    mbar_init(final_bar, 1);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -167,109 +183,154 @@ k_gemm_tn(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant__ CU
   asm volatile("tcgen05.fence::after_thread_sync;");
   const uint32_t tmem = *tmem_slot;
 
+  auto coords = [&](int t, int& m0, int& n0, int& split, int& kbeg, int& nkb) {
+    const int mt = t % tilesM;
+    const int r = t / tilesM;
+    const int ntl = r % tilesN;
+    split = r / tilesN;
+    m0 = mt * GM;
+    n0 = ntl * BN;
+    kbeg = split * g.kchunk;
+    const int kend = min(g.K, kbeg + g.kchunk);
+    nkb = (kend > kbeg) ? (kend - kbeg + GK - 1) / GK : 0;
+  };
+
   if (warp == 0) {
     if (lane == 0) {
-      int issued = 0;
-      for (int kb = 0; kb < nkb; ++kb) {
-        const int s = kb % SM::NSTAGE;
-        if (kb >= SM::NSTAGE && !mbar_wait(&empty[s], ((kb / SM::NSTAGE) - 1) & 1, 1)) { *abort_flag = 1; break; }
-        if (*abort_flag) break;
-        unsigned char* st = base + s * SM::STAGE;
-        mbar_expect_tx(&full[s], SM::STAGE);
-        const int kx = kbeg + kb * GK;
-        tma_load_2d(st, &tmA_hi, &full[s], kx, m0);
-        tma_load_2d(st + SM::A_BYTES, &tmA_lo, &full[s], kx, m0);
-        tma_load_2d(st + 2 * SM::A_BYTES, &tmB_hi, &full[s], kx, n0);
-        tma_load_2d(st + 2 * SM::A_BYTES + SM::B_BYTES, &tmB_lo, &full[s], kx, n0);
-        issued = kb + 1;
+      long it = 0;
+      bool stop = false;
+      for (int t = blockIdx.x; t < total && !stop; t += gridDim.x) {
+        int m0, n0, split, kbeg, nkb;
+        coords(t, m0, n0, split, kbeg, nkb);
+        for (int kb = 0; kb < nkb; ++kb) {
+          const int s = (int)(it % SM::NSTAGE);
+          if (it >= SM::NSTAGE && !mbar_wait(&empty[s], (uint32_t)(((it / SM::NSTAGE) - 1) & 1), 1)) {
+            *abort_flag = 1;
+            stop = true;
+            break;
+          }
+          if (*abort_flag) { stop = true; break; }
+          unsigned char* st = base + s * SM::STAGE;
+          mbar_expect_tx(&full[s], SM::STAGE);
+          const int kx = kbeg + kb * GK;
+          tma_load_2d(st, &tmA_hi, &full[s], kx, m0);
+          tma_load_2d(st + SM::A_BYTES, &tmA_lo, &full[s], kx, m0);
+          tma_load_2d(st + 2 * SM::A_BYTES, &tmB_hi, &full[s], kx, n0);
+          tma_load_2d(st + 2 * SM::A_BYTES + SM::B_BYTES, &tmB_lo, &full[s], kx, n0);
+          ++it;
+        }
       }
       // drain: every issued stage must have landed before the CTA exits
-      for (int kb = std::max(0, issued - SM::NSTAGE); kb < issued; ++kb)
-        mbar_wait(&full[kb % SM::NSTAGE], (kb / SM::NSTAGE) & 1, 2);
+      for (long k = (it > SM::NSTAGE ? it - SM::NSTAGE : 0); k < it; ++k)
+        mbar_wait(&full[k % SM::NSTAGE], (uint32_t)((k / SM::NSTAGE) & 1), 2);
     }
   } else if (warp == 1) {
     if (lane == 0) {
       constexpr uint32_t idesc = umma_idesc<BN>();
-      bool ok = true;
-      for (int kb = 0; kb < nkb; ++kb) {
-        const int s = kb % SM::NSTAGE;
-        if (!mbar_wait(&full[s], (kb / SM::NSTAGE) & 1, 3)) { *abort_flag = 1; ok = false; break; }
+      long it = 0;
+      int lt = 0;
+      bool ok = true, any = false;
+      for (int t = blockIdx.x; t < total && ok; t += gridDim.x, ++lt) {
+        int m0, n0, split, kbeg, nkb;
+        coords(t, m0, n0, split, kbeg, nkb);
+        const int buf = lt & 1;
+        if (lt >= 2 && !mbar_wait(&tempty[buf], (uint32_t)(((lt >> 1) - 1) & 1), 5)) { ok = false; break; }
         asm volatile("tcgen05.fence::after_thread_sync;");
-        const uint32_t sa = smem_u32(base + s * SM::STAGE);
-        const uint32_t ahi = sa, alo = sa + SM::A_BYTES;
-        const uint32_t bhi = sa + 2 * SM::A_BYTES, blo = bhi + SM::B_BYTES;
+        const uint32_t acc = tmem + (uint32_t)(buf * BN);
+        for (int kb = 0; kb < nkb; ++kb, ++it) {
+          const int s = (int)(it % SM::NSTAGE);
+          if (!mbar_wait(&full[s], (uint32_t)((it / SM::NSTAGE) & 1), 3)) { ok = false; break; }
+          asm volatile("tcgen05.fence::after_thread_sync;");
+          const uint32_t sa = smem_u32(base + s * SM::STAGE);
+          const uint32_t ahi = sa, alo = sa + SM::A_BYTES;
+          const uint32_t bhi = sa + 2 * SM::A_BYTES, blo = bhi + SM::B_BYTES;
 #pragma unroll
-        for (int kk = 0; kk < GK / 16; ++kk) {
-          const uint32_t off = kk * 32;   // 16 bf16 along K inside the swizzled 128-byte row
-          const uint32_t acc0 = (kb > 0 || kk > 0) ? 1u : 0u;
-          umma_bf16(tmem, umma_desc(ahi + off), umma_desc(bhi + off), idesc, acc0);
-          umma_bf16(tmem, umma_desc(ahi + off), umma_desc(blo + off), idesc, 1u);
-          umma_bf16(tmem, umma_desc(alo + off), umma_desc(bhi + off), idesc, 1u);
-          if (g.nterms > 3) umma_bf16(tmem, umma_desc(alo + off), umma_desc(blo + off), idesc, 1u);
+          for (int kk = 0; kk < GK / 16; ++kk) {
+            const uint32_t off = kk * 32;   // 16 bf16 along K inside the swizzled 128-byte row
+            const uint32_t acc0 = (kb > 0 || kk > 0) ? 1u : 0u;
+            umma_bf16(acc, umma_desc(ahi + off), umma_desc(bhi + off), idesc, acc0);
+            umma_bf16(acc, umma_desc(ahi + off), umma_desc(blo + off), idesc, 1u);
+            umma_bf16(acc, umma_desc(alo + off), umma_desc(bhi + off), idesc, 1u);
+            if (g.nterms > 3) umma_bf16(acc, umma_desc(alo + off), umma_desc(blo + off), idesc, 1u);
+          }
+          umma_commit(&empty[s]);
+          any = true;
         }
-        umma_commit(&empty[s]);
+        if (!ok) break;
+        if (nkb > 0) umma_commit(&tfull[buf]);
+        else mbar_arrive(&tfull[buf]);
       }
-      if (ok) umma_commit(accum_bar);
-      else {
-        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(accum_bar)) : "memory");
+      if (!ok) *abort_flag = 1;
+      // every issued MMA must have completed before the tensor memory is freed
+      if (any) {
+        umma_commit(final_bar);
+        mbar_wait(final_bar, 0, 6);
       }
     }
   } else {
     // epilogue warps 2..5: TMEM lanes 32*(warp%4) .. +31
     const int q = warp & 3;
-    const int row = m0 + q * 32 + lane;
-    int ok = 1;
-    if (nkb > 0 && lane == 0) ok = mbar_wait(accum_bar, 0, 4) ? 1 : 0;
-    ok = __shfl_sync(0xffffffffu, ok, 0);
-    const int ab = __shfl_sync(0xffffffffu, *abort_flag, 0);
-    asm volatile("tcgen05.fence::after_thread_sync;");
-    if (ok && !ab) {
-      for (int c0 = 0; c0 < BN; c0 += 16) {
-        uint32_t r[16];
-        const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c0;
+    int lt = 0;
+    for (int t = blockIdx.x; t < total; t += gridDim.x, ++lt) {
+      int m0, n0, split, kbeg, nkb;
+      coords(t, m0, n0, split, kbeg, nkb);
+      const int buf = lt & 1;
+      int ok = 1;
+      if (lane == 0) ok = mbar_wait(&tfull[buf], (uint32_t)((lt >> 1) & 1), 4) ? 1 : 0;
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      const int ab = __shfl_sync(0xffffffffu, *abort_flag, 0);
+      if (!ok || ab) break;
+      asm volatile("tcgen05.fence::after_thread_sync;");
+      const int row = m0 + q * 32 + lane;
+      const bool rowok = row < g.M;
+      for (int c0 = 0; c0 < BN; c0 += 32) {
+        const int nc = g.N - (n0 + c0);    // valid columns in this chunk (may be <= 0)
+        float* dst;
+        long cs;                            // column stride of the destination
+        if (g.epi == 0) {
+          dst = g.ws + ((long)split * g.N + n0 + c0) * g.M + row;
+          cs = g.M;
+        } else if (g.epi == 2) {
+          dst = g.C + (long)(n0 + c0) * g.ldc + row;
+          cs = g.ldc;
+        } else {
+          dst = g.C + (long)row * g.ldc + n0 + c0;
+          cs = 1;
+        }
+        float cv[32];
+        const bool acc = g.epi != 0 && g.accumulate;
+        if (acc && rowok) {
+          // issue the destination loads before the TMEM read so their latencies overlap
+#pragma unroll
+          for (int j = 0; j < 32; ++j) cv[j] = (j < nc) ? dst[(long)j * cs] : 0.0f;
+        }
+        uint32_t r[32];
+        const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * BN + c0);
         asm volatile(
             "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
             : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
               "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
             : "r"(taddr));
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+            : "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+              "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+            : "r"(taddr + 16u));
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        if (row < g.M) {
-          if (nkb == 0) {
+        if (rowok) {
 #pragma unroll
-            for (int j = 0; j < 16; ++j) r[j] = 0u;
-          }
-          if (g.epi == 0) {
-            // split-K partial, stored [split][n][m]: lanes (consecutive m) coalesce
-            float* dst = g.ws + ((long)blockIdx.z * g.N + n0 + c0) * g.M + row;
-#pragma unroll
-            for (int j = 0; j < 16; ++j)
-              if (n0 + c0 + j < g.N) dst[(long)j * g.M] = __uint_as_float(r[j]);
-          } else if (g.epi == 2) {
-            // transposed store C[n*ldc + m]: lanes (consecutive m) coalesce
-            float* dst = g.C + (long)(n0 + c0) * g.ldc + row;
-            if (g.accumulate) {
-#pragma unroll
-              for (int j = 0; j < 16; ++j)
-                if (n0 + c0 + j < g.N) dst[(long)j * g.ldc] += __uint_as_float(r[j]);
-            } else {
-#pragma unroll
-              for (int j = 0; j < 16; ++j)
-                if (n0 + c0 + j < g.N) dst[(long)j * g.ldc] = __uint_as_float(r[j]);
-            }
-          } else {
-            float* dst = g.C + (long)row * g.ldc + n0 + c0;
-            if (g.accumulate) {
-#pragma unroll
-              for (int j = 0; j < 16; ++j)
-                if (n0 + c0 + j < g.N) dst[j] += __uint_as_float(r[j]);
-            } else {
-#pragma unroll
-              for (int j = 0; j < 16; ++j)
-                if (n0 + c0 + j < g.N) dst[j] = __uint_as_float(r[j]);
+          for (int j = 0; j < 32; ++j) {
+            if (j < nc) {
+              const float v = nkb > 0 ? __uint_as_float(r[j]) : 0.0f;
+              dst[(long)j * cs] = acc ? cv[j] + v : v;
             }
           }
         }
       }
+      // hand the accumulator back to the MMA warp
+      asm volatile("tcgen05.fence::before_thread_sync;");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&tempty[buf]);
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;");
@@ -392,6 +453,16 @@ static int make_tmap(CUtensorMap* m, const void* ptr, long rows, long K, long ld
   return PW_OK;
 }
 
+static int num_sms() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+  }
+  return n;
+}
+
 template <int BN> static int launch_bn(const SplitOperand& A, const SplitOperand& B, const GemmArgs& g, int nsplit,
                                        cudaStream_t st) {
   using SM = GemmSmem<BN>;
@@ -405,8 +476,11 @@ template <int BN> static int launch_bn(const SplitOperand& A, const SplitOperand
   if ((rc = make_tmap(&ah, A.hi, A.rows, g.K, A.ld, GM)) || (rc = make_tmap(&al, A.lo, A.rows, g.K, A.ld, GM)) ||
       (rc = make_tmap(&bh, B.hi, B.rows, g.K, B.ld, BN)) || (rc = make_tmap(&bl, B.lo, B.rows, g.K, B.ld, BN)))
     return rc;
-  dim3 grid((g.M + GM - 1) / GM, (g.N + BN - 1) / BN, nsplit);
-  k_gemm_tn<BN><<<grid, GEMM_THREADS, SM::BYTES, st>>>(ah, al, bh, bl, g);
+  GemmArgs ga = g;
+  ga.nsplit = nsplit;
+  const long total = (long)((g.M + GM - 1) / GM) * ((g.N + BN - 1) / BN) * nsplit;
+  const int grid = (int)std::min<long>(total, num_sms());
+  k_gemm_tn<BN><<<grid, GEMM_THREADS, SM::BYTES, st>>>(ah, al, bh, bl, ga);
   PWB_CUDA(cudaGetLastError());
   return PW_OK;
 }
@@ -474,7 +548,7 @@ int gemm_tn_reduce(const SplitOperand& A, const SplitOperand& B, int K, int nter
   const int BN = pick_bn(N);
   const int tiles = ((M + GM - 1) / GM) * ((N + BN - 1) / BN);
   // enough CTAs to fill the GPU twice over, each with >= 4 K-blocks
-  int nsplit = std::max(1, (2 * 148 + tiles - 1) / tiles);
+  int nsplit = std::max(1, (2 * num_sms() + tiles - 1) / tiles);
   const int maxsplit = std::max(1, (K + 4 * GK - 1) / (4 * GK));
   nsplit = std::min(nsplit, maxsplit);
   int kchunk = ((K + nsplit - 1) / nsplit + GK - 1) / GK * GK;
