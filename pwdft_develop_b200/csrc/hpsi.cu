@@ -31,7 +31,11 @@
 
 namespace pwb {
 
-constexpr int TX = 16;          // kx columns per z-pencil CTA
+// kx columns per z-pencil CTA: 24 for FP32 grids divisible by 24 (two
+// balanced tiles at n0 = 48), otherwise 16
+template <typename T, int N0> struct PencilTile {
+  static constexpr int v = (sizeof(T) == 4 && N0 % 24 == 0) ? 24 : 16;
+};
 constexpr int PLANE_THREADS = 256;
 constexpr int PENCIL_THREADS = 256;
 
@@ -97,7 +101,7 @@ struct ColMap {
   bool nyy;
   int nyx_i;  // tile-local index of the kx Nyquist column, -1 if none
 };
-__device__ __forceinline__ ColMap colmap(int ky, int kx0, int tw, int n0, int n1) {
+template <int TX> __device__ __forceinline__ ColMap colmap(int ky, int kx0, int tw, int n0, int n1) {
   ColMap m;
   m.nyy = (ky == n1 / 2);
   m.nyx_i = (n0 / 2 >= kx0 && n0 / 2 < kx0 + tw) ? (n0 / 2 - kx0) : -1;
@@ -105,6 +109,7 @@ __device__ __forceinline__ ColMap colmap(int ky, int kx0, int tw, int n0, int n1
   return m;
 }
 // slot coordinates of column c
+template <int TX>
 __device__ __forceinline__ void col_slot(const ColMap& m, int c, int ky, int kx0, int n0, int n1,
                                          int& ky_s, int& kx_s) {
   if (m.nyy) {
@@ -116,11 +121,32 @@ __device__ __forceinline__ void col_slot(const ColMap& m, int c, int ky, int kx0
   }
 }
 
+// The tile's used columns in compact order: j < tw -> column j, then the
+// Nyquist partners (column TX for a kx Nyquist, TX + j' for a ky Nyquist row).
+__device__ __forceinline__ int ncompact(const ColMap& m, int tw) {
+  return tw + (m.nyy ? tw : (m.nyx_i >= 0 ? 1 : 0));
+}
+template <int TX> __device__ __forceinline__ int compact_col(int j, int tw) { return j < tw ? j : TX + (j - tw); }
+
+// for (i = threadIdx.x; i < rows * n; i += blockDim.x) f(i / n, i % n) without
+// a division per step
+template <typename F> __device__ __forceinline__ void for_rows_cols(int rows, int n, F&& f) {
+  const int step = blockDim.x;
+  const int q = step / n, r = step - q * n;
+  int a = threadIdx.x / n, b = threadIdx.x - a * n;
+  while (a < rows) {
+    f(a, b);
+    a += q;
+    b += r;
+    if (b >= n) { b -= n; ++a; }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // z pencils: coarse FFT z, kinetic, Nyquist unfold, fine pad, fine IFFT z
 // ---------------------------------------------------------------------------
-template <typename T, int NZ, int NZF>
-__global__ void __launch_bounds__(PENCIL_THREADS)
+template <typename T, int NZ, int NZF, int TX>
+__global__ void __launch_bounds__(PENCIL_THREADS, sizeof(T) == 4 ? 4 : 1)
 k_zpad(const VT<T>* __restrict__ A, VT<T>* __restrict__ K, VT<T>* __restrict__ B,
        const T* __restrict__ ekin, int n0, int n1, T inv_nc,
        const VT<T>* twz_g, const VT<T>* twzf_g) {
@@ -132,31 +158,42 @@ k_zpad(const VT<T>* __restrict__ A, VT<T>* __restrict__ K, VT<T>* __restrict__ B
   V* out = in + NZ * PI;                   // [NZF][PO]
   V* twz = out + NZF * PO;
   V* twzf = twz + NZ;
+  __shared__ int colofs[2 * TX];           // slot offset of output column c in a fine plane, -1 if unused
   load_tw(twz, twz_g, NZ);
   load_tw(twzf, twzf_g, NZF);
   const int ky = blockIdx.x, kx0 = blockIdx.y * TX, p = blockIdx.z;
   const int tw = min(TX, n0 - kx0);
   const long nplane = (long)n0 * n1;
-  const V* Ap = A + (long)p * NZ * nplane;
+  const int nsx = n0 + 1, nsy = n1 + 1;
+  const V* Ap = A + (long)p * NZ * nplane + (long)ky * n0 + kx0;
   for (int i = threadIdx.x; i < NZ * TX; i += blockDim.x) {
     const int z = i / TX, c = i - z * TX;
-    in[z * PI + c] = (c < tw) ? Ap[z * nplane + (long)ky * n0 + kx0 + c] : mkc<V>(0, 0);
+    in[z * PI + c] = (c < tw) ? Ap[z * nplane + c] : mkc<V>(0, 0);
   }
-  const ColMap m = colmap(ky, kx0, tw, n0, n1);
+  const ColMap m = colmap<TX>(ky, kx0, tw, n0, n1);
+  if (threadIdx.x < 2 * TX) {
+    const int c = threadIdx.x;
+    const bool valid = c < m.ncols && !(c < TX && c >= tw) && !(m.nyy && c >= TX && c - TX >= tw);
+    int ky_s = 0, kx_s = 0;
+    col_slot<TX>(m, c, ky, kx0, n0, n1, ky_s, kx_s);
+    colofs[c] = valid ? ky_s * nsx + kx_s : -1;
+  }
   for (int i = threadIdx.x; i < NZF * PO; i += blockDim.x) out[i] = mkc<V>(0, 0);
   __syncthreads();
   smem_fft_cb<NZ, -1, PI, 1>(in, tw, twz);
   __syncthreads();
-  V* Kp = K + (long)p * NZ * nplane;
+  V* Kp = K ? K + (long)p * NZ * nplane + (long)ky * n0 + kx0 : nullptr;
+  const T* ek = ekin + (long)ky * n0 + kx0;
+  const bool splitrow = m.nyy;
   for (int i = threadIdx.x; i < NZ * TX; i += blockDim.x) {
     const int kz = i / TX, c = i - kz * TX;
     if (c >= tw) continue;
-    const long g = kz * nplane + (long)ky * n0 + kx0 + c;
+    const long g = kz * nplane + c;
     const V v = cscale(in[kz * PI + c], inv_nc);
-    if (K) Kp[g] = cscale(v, ekin[g]);
+    if (Kp) Kp[g] = cscale(v, ek[g]);
     const bool nyz = (kz == NZ / 2);
-    const int fz = (sgn_idx(kz, NZ) + NZF) % NZF;
-    const bool split = m.nyy || (c == m.nyx_i);
+    const int fz = kz <= NZ / 2 ? kz : kz + (NZF - NZ);
+    const bool split = splitrow || (c == m.nyx_i);
     if (!split) {
       if (nyz) {
         out[(NZ / 2) * PO + c] = cscale(v, (T)0.5);
@@ -165,7 +202,7 @@ k_zpad(const VT<T>* __restrict__ A, VT<T>* __restrict__ K, VT<T>* __restrict__ B
         out[fz * PO + c] = v;
       }
     } else {
-      const int cp = c, cm = m.nyy ? TX + c : TX;
+      const int cp = c, cm = splitrow ? TX + c : TX;
       const V h = cscale(v, (T)0.5);
       if (nyz) {
         out[(NZ / 2) * PO + cp] = h;
@@ -179,16 +216,12 @@ k_zpad(const VT<T>* __restrict__ A, VT<T>* __restrict__ K, VT<T>* __restrict__ B
   __syncthreads();
   smem_fft_cb<NZF, +1, PO, 1>(out, m.ncols, twzf);
   __syncthreads();
-  const int nsx = n0 + 1, nsy = n1 + 1;
   V* Bp = B + (long)p * NZF * nsy * nsx;
-  for (int i = threadIdx.x; i < NZF * m.ncols; i += blockDim.x) {
-    const int zf = i / m.ncols, c = i - zf * m.ncols;
-    if (c < TX && c >= tw) continue;
-    if (m.nyy && c >= TX && c - TX >= tw) continue;
-    int ky_s, kx_s;
-    col_slot(m, c, ky, kx0, n0, n1, ky_s, kx_s);
-    Bp[((long)zf * nsy + ky_s) * nsx + kx_s] = out[zf * PO + c];
-  }
+  const long fplane = (long)nsy * nsx;
+  for_rows_cols(NZF, ncompact(m, tw), [&](int zf, int j) {
+    const int c = compact_col<TX>(j, tw);
+    Bp[zf * fplane + colofs[c]] = out[zf * PO + c];
+  });
   // the two Nyquist corner slots that no coarse coefficient reaches
   if (m.nyy && m.nyx_i >= 0) {
     for (int zf = threadIdx.x; zf < NZF; zf += blockDim.x) {
@@ -445,7 +478,7 @@ k_exx_inv(const VT<T>* __restrict__ A, int njp, const T* __restrict__ phi, int l
 constexpr int FLOC_THREADS = 256;
 
 template <typename T, int NXF, int NYF, int MODE>
-__global__ void __launch_bounds__(FLOC_THREADS)
+__global__ void __launch_bounds__(FLOC_THREADS, sizeof(T) == 4 ? 3 : 1)
 k_floc(VT<T>* __restrict__ BC, const T* __restrict__ vtot, const T* __restrict__ fin, long fin_pair_stride,
        T inv_nf, const VT<T>* twx_g, const VT<T>* twy_g, int deriv = 0, T gfac = 0) {
   using V = VT<T>;
@@ -668,8 +701,8 @@ __global__ void k_nl_reduce(const VT<T>* __restrict__ Wp, VT<T>* __restrict__ W,
 // ---------------------------------------------------------------------------
 // z pencils: fine FFT z, fold to coarse (IP_f2c), add kinetic, coarse IFFT z
 // ---------------------------------------------------------------------------
-template <typename T, int NZ, int NZF>
-__global__ void __launch_bounds__(PENCIL_THREADS)
+template <typename T, int NZ, int NZF, int TX>
+__global__ void __launch_bounds__(PENCIL_THREADS, sizeof(T) == 4 ? 4 : 1)
 k_zfold(const VT<T>* __restrict__ C, const VT<T>* __restrict__ K, VT<T>* __restrict__ D, int n0, int n1,
         const VT<T>* twz_g, const VT<T>* twzf_g, int deriv = 0, T gfac = 0) {
   using V = VT<T>;
@@ -680,27 +713,42 @@ k_zfold(const VT<T>* __restrict__ C, const VT<T>* __restrict__ K, VT<T>* __restr
   V* acc = in + NZF * PI;                 // [NZ][PA]
   V* twz = acc + NZ * PA;
   V* twzf = twz + NZ;
+  __shared__ int colofs[2 * TX];          // slot offset of input column c in a fine plane, -1 if unused
   load_tw(twz, twz_g, NZ);
   load_tw(twzf, twzf_g, NZF);
   const int ky = blockIdx.x, kx0 = blockIdx.y * TX, p = blockIdx.z;
   const int tw = min(TX, n0 - kx0);
-  const ColMap m = colmap(ky, kx0, tw, n0, n1);
+  const ColMap m = colmap<TX>(ky, kx0, tw, n0, n1);
   const int nsx = n0 + 1, nsy = n1 + 1;
-  const V* Cp = C + (long)p * NZF * nsy * nsx;
-  for (int i = threadIdx.x; i < NZF * m.ncols; i += blockDim.x) {
-    const int zf = i / m.ncols, c = i - zf * m.ncols;
-    bool valid = !(c < TX && c >= tw) && !(m.nyy && c >= TX && c - TX >= tw);
-    int ky_s, kx_s;
-    col_slot(m, c, ky, kx0, n0, n1, ky_s, kx_s);
-    in[zf * PI + c] = valid ? Cp[((long)zf * nsy + ky_s) * nsx + kx_s] : mkc<V>(0, 0);
+  if (threadIdx.x < 2 * TX) {
+    const int c = threadIdx.x;
+    const bool valid = c < m.ncols && !(c < TX && c >= tw) && !(m.nyy && c >= TX && c - TX >= tw);
+    int ky_s = 0, kx_s = 0;
+    col_slot<TX>(m, c, ky, kx0, n0, n1, ky_s, kx_s);
+    colofs[c] = valid ? ky_s * nsx + kx_s : -1;
   }
+  __syncthreads();
+  const V* Cp = C + (long)p * NZF * nsy * nsx;
+  const long fplane = (long)nsy * nsx;
+  // columns the FFT reads but no slot feeds (c < ncols, not in the compact list)
+  if (tw < TX) {
+    for (int i = threadIdx.x; i < NZF * 2 * TX; i += blockDim.x) {
+      const int zf = i / (2 * TX), c = i - zf * (2 * TX);
+      if (c < m.ncols && colofs[c] < 0) in[zf * PI + c] = mkc<V>(0, 0);
+    }
+  }
+  for_rows_cols(NZF, ncompact(m, tw), [&](int zf, int j) {
+    const int c = compact_col<TX>(j, tw);
+    in[zf * PI + c] = Cp[zf * fplane + colofs[c]];
+  });
   __syncthreads();
   smem_fft_cb<NZF, -1, PI, 1>(in, m.ncols, twzf);
   __syncthreads();
   if (deriv == 3) {
     // spectral d/dz before the fold: multiply by i G_z of the fine frequency
-    for (int i = threadIdx.x; i < NZF * m.ncols; i += blockDim.x) {
-      const int zf = i / m.ncols, c = i - zf * m.ncols;
+    for (int i = threadIdx.x; i < NZF * 2 * TX; i += blockDim.x) {
+      const int zf = i / (2 * TX), c = i - zf * (2 * TX);
+      if (c >= m.ncols) continue;
       const T g = gfac * (T)sgn_idx(zf, NZF);
       const V v = in[zf * PI + c];
       in[zf * PI + c] = mkc<V>(-g * v.y, g * v.x);
@@ -708,19 +756,20 @@ k_zfold(const VT<T>* __restrict__ C, const VT<T>* __restrict__ K, VT<T>* __restr
     __syncthreads();
   }
   const long nplane = (long)n0 * n1;
-  const V* Kp = K + (long)p * NZ * nplane;
+  const V* Kp = K ? K + (long)p * NZ * nplane + (long)ky * n0 + kx0 : nullptr;
+  const bool splitrow = m.nyy;
   for (int i = threadIdx.x; i < NZ * TX; i += blockDim.x) {
     const int kz = i / TX, c = i - kz * TX;
     if (c >= tw) { acc[kz * PA + c] = mkc<V>(0, 0); continue; }
-    V v = K ? Kp[kz * nplane + (long)ky * n0 + kx0 + c] : mkc<V>(0, 0);
+    V v = Kp ? Kp[kz * nplane + c] : mkc<V>(0, 0);
     const bool nyz = (kz == NZ / 2);
-    const int fz = (sgn_idx(kz, NZ) + NZF) % NZF;
-    const bool split = m.nyy || (c == m.nyx_i);
+    const int fz = kz <= NZ / 2 ? kz : kz + (NZF - NZ);
+    const bool split = splitrow || (c == m.nyx_i);
     if (!split) {
       if (nyz) v = cadd(v, cscale(cadd(in[(NZ / 2) * PI + c], in[(NZF - NZ / 2) * PI + c]), (T)0.5));
       else v = cadd(v, in[fz * PI + c]);
     } else {
-      const int cp = c, cm = m.nyy ? TX + c : TX;
+      const int cp = c, cm = splitrow ? TX + c : TX;
       if (nyz) v = cadd(v, cscale(cadd(in[(NZ / 2) * PI + cp], in[(NZF - NZ / 2) * PI + cm]), (T)0.5));
       else v = cadd(v, cscale(cadd(in[fz * PI + cp], in[fz * PI + cm]), (T)0.5));
     }
@@ -729,16 +778,16 @@ k_zfold(const VT<T>* __restrict__ C, const VT<T>* __restrict__ K, VT<T>* __restr
   __syncthreads();
   smem_fft_cb<NZ, +1, PA, 1>(acc, tw, twz);
   __syncthreads();
-  V* Dp = D + (long)p * NZ * nplane;
+  V* Dp = D + (long)p * NZ * nplane + (long)ky * n0 + kx0;
   for (int i = threadIdx.x; i < NZ * TX; i += blockDim.x) {
     const int z = i / TX, c = i - z * TX;
-    if (c < tw) Dp[z * nplane + (long)ky * n0 + kx0 + c] = acc[z * PA + c];
+    if (c < tw) Dp[z * nplane + c] = acc[z * PA + c];
   }
 }
 
 // z pencils for the Teter preconditioner: FFT z, * teter / N_c, IFFT z
-template <typename T, int NZ>
-__global__ void __launch_bounds__(PENCIL_THREADS)
+template <typename T, int NZ, int TX>
+__global__ void __launch_bounds__(PENCIL_THREADS, sizeof(T) == 4 ? 4 : 1)
 k_zteter(VT<T>* __restrict__ A, const T* __restrict__ teter, int n0, int n1, T inv_nc, const VT<T>* twz_g) {
   using V = VT<T>;
   constexpr int PI = TX + 1;
@@ -864,6 +913,8 @@ template <typename T> static int fplane_cr(int NXF, int NYF) {
 
 template <typename T, int N0, int N1, int N2>
 struct Plan {
+  static constexpr int TX = PencilTile<T, N0>::v;
+  static constexpr int TXF = TX;   // z-fold tile width
   using V = VT<T>;
   static constexpr int NF0 = 2 * N0, NF1 = 2 * N1, NF2 = 2 * N2;
 
@@ -871,7 +922,7 @@ struct Plan {
 
   static size_t sm_cxy() { return sizeof(V) * (N1 * (N0 + 1) + N0 + N1); }
   static size_t sm_zpad() { return sizeof(V) * (N2 * (TX + 1) + NF2 * (2 * TX + 1) + N2 + NF2); }
-  static size_t sm_zfold() { return sizeof(V) * (NF2 * (2 * TX + 1) + N2 * (TX + 1) + N2 + NF2); }
+  static size_t sm_zfold() { return sizeof(V) * (NF2 * (2 * TXF + 1) + N2 * (TXF + 1) + N2 + NF2); }
   static size_t sm_zteter() { return sizeof(V) * (N2 * (TX + 1) + N2); }
   static size_t sm_exx_inv() { return sm_cxy() + sizeof(T) * N0 * N1; }
   static size_t sm_floc() {
@@ -887,11 +938,11 @@ struct Plan {
     const int cr = chunk_rows();
     PWB_CUDA(cudaFuncSetAttribute(k_fplane<T, NF0, NF1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_fplane(cr)));
     PWB_CUDA(cudaFuncSetAttribute(k_fplane<T, NF0, NF1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_fplane(cr)));
-    PWB_CUDA(cudaFuncSetAttribute(k_zpad<T, N2, NF2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_zpad()));
-    PWB_CUDA(cudaFuncSetAttribute(k_zfold<T, N2, NF2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_zfold()));
+    PWB_CUDA(cudaFuncSetAttribute(k_zpad<T, N2, NF2, TX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_zpad()));
+    PWB_CUDA(cudaFuncSetAttribute(k_zfold<T, N2, NF2, TXF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_zfold()));
     PWB_CUDA(cudaFuncSetAttribute(k_cxy_fwd<T, N0, N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_cxy()));
     PWB_CUDA(cudaFuncSetAttribute(k_cxy_inv<T, N0, N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_cxy()));
-    PWB_CUDA(cudaFuncSetAttribute(k_zteter<T, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_zteter()));
+    PWB_CUDA(cudaFuncSetAttribute(k_zteter<T, N2, TX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_zteter()));
     PWB_CUDA(cudaFuncSetAttribute(k_floc<T, NF0, NF1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_floc()));
     PWB_CUDA(cudaFuncSetAttribute(k_floc<T, NF0, NF1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_floc()));
     done = true;
@@ -916,14 +967,14 @@ struct Plan {
     { Launch L_(c, st, KK_CXY_FWD);
     k_cxy_fwd<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(psi, ld, nband, band0, AD, tw(c, 0), tw(c, 1)); }
     { Launch L_(c, st, KK_ZPAD);
-    k_zpad<T, N2, NF2><<<dim3(N1, ntx, npair), PENCIL_THREADS, sm_zpad(), st>>>(
+    k_zpad<T, N2, NF2, TX><<<dim3(N1, ntx, npair), PENCIL_THREADS, sm_zpad(), st>>>(
         AD, K, BC, reinterpret_cast<const T*>(c->ekin.p), N0, N1, inv_nc, tw(c, 2), tw(c, 5)); }
     if (c->nl_mode == PW_NL_DENSE) {
       { Launch L_(c, st, KK_FPLANE_APPLY);
       k_floc<T, NF0, NF1, 0><<<dim3(NF2, npair), FLOC_THREADS, sm_floc(), st>>>(
           BC, reinterpret_cast<const T*>(c->vtot.p), nullptr, 0, inv_nf, tw(c, 3), tw(c, 4)); }
       { Launch L_(c, st, KK_ZFOLD);
-      k_zfold<T, N2, NF2><<<dim3(N1, ntx, npair), PENCIL_THREADS, sm_zfold(), st>>>(BC, K, AD, N0, N1, tw(c, 2), tw(c, 5)); }
+      k_zfold<T, N2, NF2, TXF><<<dim3(N1, (N0 + TXF - 1) / TXF, npair), PENCIL_THREADS, sm_zfold(), st>>>(BC, K, AD, N0, N1, tw(c, 2), tw(c, 5)); }
       { Launch L_(c, st, KK_CXY_INV);
       k_cxy_inv<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(AD, out, ldo, nband, band0, accumulate, tw(c, 0), tw(c, 1)); }
       PWB_CUDA(cudaGetLastError());
@@ -963,7 +1014,7 @@ struct Plan {
     k_fplane<T, NF0, NF1, true><<<dim3(NF2, npair), PLANE_THREADS, sm_fplane(cr), st>>>(
         BC, reinterpret_cast<const T*>(c->vtot.p), nl, Wp, W, natom, nslot, inv_nf, tw(c, 3), tw(c, 4)); }
     { Launch L_(c, st, KK_ZFOLD);
-    k_zfold<T, N2, NF2><<<dim3(N1, ntx, npair), PENCIL_THREADS, sm_zfold(), st>>>(BC, K, AD, N0, N1, tw(c, 2), tw(c, 5)); }
+    k_zfold<T, N2, NF2, TXF><<<dim3(N1, (N0 + TXF - 1) / TXF, npair), PENCIL_THREADS, sm_zfold(), st>>>(BC, K, AD, N0, N1, tw(c, 2), tw(c, 5)); }
     { Launch L_(c, st, KK_CXY_INV);
     k_cxy_inv<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(AD, out, ldo, nband, band0, accumulate, tw(c, 0), tw(c, 1)); }
     PWB_CUDA(cudaGetLastError());
@@ -1025,7 +1076,7 @@ struct Plan {
         k_exx_fwd<T, N0, N1><<<dim3(N2, nk * nj), PLANE_THREADS, sm_cxy(), st>>>(
             psi, ld, k0, phi, (int)nt, 2 * jp0, nphi, nj, A, tw(c, 0), tw(c, 1)); }
         { Launch L_(c, st, KK_EXX);
-        k_zteter<T, N2><<<dim3(N1, ntx, nk * nj), PENCIL_THREADS, sm_zteter(), st>>>(A, kern, N0, N1, inv_nc, tw(c, 2)); }
+        k_zteter<T, N2, TX><<<dim3(N1, ntx, nk * nj), PENCIL_THREADS, sm_zteter(), st>>>(A, kern, N0, N1, inv_nc, tw(c, 2)); }
         { Launch L_(c, st, KK_EXX);
         k_exx_inv<T, N0, N1><<<dim3(N2, nk), PLANE_THREADS, sm_exx_inv(), st>>>(
             A, nj, phi, (int)nt, 2 * jp0, nphi, wj, out, ldo, k0, (accumulate || jp0 > 0) ? 1 : 0, tw(c, 0),
@@ -1087,7 +1138,7 @@ struct Plan {
     { Launch L_(c, st, KK_DENSITY);
     k_cxy_fwd<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(psi, ld, nband, band0, AD, tw(c, 0), tw(c, 1)); }
     { Launch L_(c, st, KK_DENSITY);
-    k_zpad<T, N2, NF2><<<dim3(N1, ntx, npair), PENCIL_THREADS, sm_zpad(), st>>>(
+    k_zpad<T, N2, NF2, TX><<<dim3(N1, ntx, npair), PENCIL_THREADS, sm_zpad(), st>>>(
         AD, nullptr, BC, reinterpret_cast<const T*>(c->ekin.p), N0, N1, inv_nc, tw(c, 2), tw(c, 5)); }
     const int ppc = std::max(1, std::min(8, npair));
     { Launch L_(c, st, KK_DENSITY);
@@ -1151,7 +1202,7 @@ struct Plan {
       k_floc<T, NF0, NF1, 1><<<dim3(NF2, npair), FLOC_THREADS, sm_floc(), st>>>(
           BC, nullptr, reinterpret_cast<const T*>(fields.p), nf, inv_nf, tw(c, 3), tw(c, 4), deriv,
           deriv == 1 ? gx : gy);
-      k_zfold<T, N2, NF2><<<dim3(N1, ntx, npair), PENCIL_THREADS, sm_zfold(), st>>>(BC, nullptr, AD, N0, N1, tw(c, 2),
+      k_zfold<T, N2, NF2, TXF><<<dim3(N1, (N0 + TXF - 1) / TXF, npair), PENCIL_THREADS, sm_zfold(), st>>>(BC, nullptr, AD, N0, N1, tw(c, 2),
                                                                                      tw(c, 5), deriv, gz);
       k_cxy_inv<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(AD, Q, (int)c->ntot, nproj, l0, 0, tw(c, 0), tw(c, 1));
       PWB_CUDA(cudaGetLastError());
@@ -1170,7 +1221,7 @@ struct Plan {
     { Launch L_(c, st, KK_CXY_FWD);
     k_cxy_fwd<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(r, ld, nband, band0, AD, tw(c, 0), tw(c, 1)); }
     { Launch L_(c, st, KK_ZTETER);
-    k_zteter<T, N2><<<dim3(N1, ntx, npair), PENCIL_THREADS, sm_zteter(), st>>>(
+    k_zteter<T, N2, TX><<<dim3(N1, ntx, npair), PENCIL_THREADS, sm_zteter(), st>>>(
         AD, reinterpret_cast<const T*>(c->teter.p), N0, N1, inv_nc, tw(c, 2)); }
     { Launch L_(c, st, KK_CXY_INV);
     k_cxy_inv<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(AD, out, ldo, nband, band0, accumulate, tw(c, 0), tw(c, 1)); }
@@ -1189,7 +1240,7 @@ struct Plan {
     const int ntx = (N0 + TX - 1) / TX;
     c->launches += 3;
     k_cxy_fwd<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(r, ld, nband, band0, AD, tw(c, 0), tw(c, 1));
-    k_zteter<T, N2><<<dim3(N1, ntx, npair), PENCIL_THREADS, sm_zteter(), st>>>(
+    k_zteter<T, N2, TX><<<dim3(N1, ntx, npair), PENCIL_THREADS, sm_zteter(), st>>>(
         AD, reinterpret_cast<const T*>(c->teter.p), N0, N1, inv_nc, tw(c, 2));
     k_cxy_inv<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(AD, out, ldo, nband, band0, accumulate,
                                                                             tw(c, 0), tw(c, 1));
