@@ -167,7 +167,7 @@ PW_API int pw_gram(pw_ctx* ctx, const void* X, int ldx, int nx, const void* Y, i
 /* ---------------------------------------------------------------------------
  * Block eigensolvers and SCF
  * ------------------------------------------------------------------------- */
-enum { PW_SOLVER_LOBPCG = 0, PW_SOLVER_CHEBFSI = 1 };
+enum { PW_SOLVER_LOBPCG = 0, PW_SOLVER_CHEBFSI = 1, PW_SOLVER_PPCG = 2, PW_SOLVER_DAVIDSON = 3 };
 
 /* In-place Cholesky-QR of nb device columns X (ntot x nb): X <- X U^{-1},
  * X^T X = U^T U.  Replaces EigenSolver::Orthogonalize
@@ -180,7 +180,12 @@ PW_API int pw_cholqr(pw_ctx* ctx, void* X, int nb);
  * (src/EigenSolver/lobpcg.cpp:577-1031: maxit = Eig_MaxIter, tol = residual
  * tolerance); PW_SOLVER_CHEBFSI runs Chebyshev-filtered subspace iteration of
  * the given degree (the reference's CheFSI parameters, src/esdf.cpp:2715-2719)
- * for up to maxit cycles.  eig, resnorm: host arrays of nb (may be NULL). */
+ * for up to maxit cycles; PW_SOLVER_PPCG restates EigenSolver::PPCGSolveReal
+ * (src/EigenSolver/ppcg.cpp:670-1243) with sub-block size `degree` (PPCG_sbSize,
+ * 1..8); PW_SOLVER_DAVIDSON restates EigenSolver::DavidsonSolveReal
+ * (src/EigenSolver/davidson.cpp:60-806) with a subspace of `degree` blocks
+ * (maxdim, >= 2) and convergence on the change of each Ritz value.  eig,
+ * resnorm: host arrays of nb (may be NULL). */
 PW_API int pw_eigsolve(pw_ctx* ctx, int solver, void* X, int nb, int maxit, double tol, int degree, double* eig,
                        double* resnorm, int* iters);
 
@@ -220,6 +225,8 @@ typedef struct pw_scf_params {
   double tol_efree;         /* converged when |E_free - E_Harris| / N_atom < tol_efree */
   double refine_threshold;  /* mixed mode: switch the eigensolver to FP64 below this */
   unsigned long long seed;  /* random start */
+  int ppcg_sbsize;          /* PPCG_sbSize (PW_SOLVER_PPCG), 1..8 */
+  int davidson_maxdim;      /* subspace size in blocks (PW_SOLVER_DAVIDSON), >= 2 */
 } pw_scf_params;
 
 typedef struct pw_scf_result {

@@ -35,7 +35,7 @@ _vp, _i, _l, _d = C.c_void_p, C.c_int, C.c_long, C.c_double
 _ip, _dp = C.POINTER(C.c_int), C.POINTER(C.c_double)
 
 PW_EXX_OFF, PW_EXX_FULL, PW_EXX_ACE = 0, 1, 2
-PW_SOLVER_LOBPCG, PW_SOLVER_CHEBFSI = 0, 1
+PW_SOLVER_LOBPCG, PW_SOLVER_CHEBFSI, PW_SOLVER_PPCG, PW_SOLVER_DAVIDSON = 0, 1, 2, 3
 
 
 class ScfParams(C.Structure):
@@ -44,7 +44,7 @@ class ScfParams(C.Structure):
                 ("mix_dim", C.c_int), ("mixed", C.c_int), ("verbose", C.c_int),
                 ("ecut", C.c_double), ("temperature", C.c_double), ("eig_tol", C.c_double),
                 ("mix_step", C.c_double), ("tol_efree", C.c_double), ("refine_threshold", C.c_double),
-                ("seed", C.c_ulonglong)]
+                ("seed", C.c_ulonglong), ("ppcg_sbsize", C.c_int), ("davidson_maxdim", C.c_int)]
 
 
 class ScfResult(C.Structure):

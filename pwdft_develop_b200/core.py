@@ -251,14 +251,20 @@ def _ctx_cholqr(self, X):
     return X
 
 
+_SOLVERS = {"lobpcg": _lib.PW_SOLVER_LOBPCG, "chebfsi": _lib.PW_SOLVER_CHEBFSI, "ppcg": _lib.PW_SOLVER_PPCG,
+            "davidson": _lib.PW_SOLVER_DAVIDSON}
+
+
 def _ctx_eigsolve(self, X, solver: str = "lobpcg", maxit: int = 10, tol: float = 1e-8, degree: int = 10):
-    """EigenSolver::LOBPCGSolveReal / ChebFSI on the device block X (nb, ntot),
-    overwritten by the Ritz vectors.  Returns (eig, resnorm, iterations)."""
+    """EigenSolver::LOBPCGSolveReal / PPCGSolveReal / DavidsonSolveReal / ChebFSI
+    on the device block X (nb, ntot), overwritten by the Ritz vectors.  degree:
+    ChebFSI filter degree, PPCG sub-block size or Davidson subspace blocks.
+    Returns (eig, resnorm, iterations)."""
     nb = X.shape[0]
     eig = np.zeros(nb)
     res = np.zeros(nb)
     it = C.c_int()
-    sid = _lib.PW_SOLVER_LOBPCG if solver == "lobpcg" else _lib.PW_SOLVER_CHEBFSI
+    sid = _SOLVERS[solver]
     check(lib.pw_eigsolve(self._h, sid, _ptr(X), nb, int(maxit), float(tol), int(degree),
                           eig.ctypes.data_as(_lib._dp), res.ctypes.data_as(_lib._dp), C.byref(it)))
     return eig, res, it.value
@@ -277,11 +283,11 @@ def _ctx_scf(self, nocc: int, nextra: int, ecut: float, solver: str = "chebfsi",
              temperature: float = 300.0, cheby_degree: int = 10, cheby_first_cycles: int = 5,
              eig_max_iter: int = 3, eig_tol: float = 1e-10, max_iter: int = 100, mix_dim: int = 8,
              mix_step: float = 0.7, tol_efree: float = 1e-6, refine_threshold: float = 1e-4, seed: int = 1,
-             verbose: bool = False):
+             verbose: bool = False, ppcg_sbsize: int = 1, davidson_maxdim: int = 2):
     """SCF::Iterate on the device (FP64 context; mixed=True runs the eigensolver in
     an FP32 twin and refines in FP64).  Returns (result dict, eigenvalues, rho)."""
     p = _lib.ScfParams(nocc=nocc, nextra=nextra,
-                       solver=_lib.PW_SOLVER_LOBPCG if solver == "lobpcg" else _lib.PW_SOLVER_CHEBFSI,
+                       solver=_SOLVERS[solver], ppcg_sbsize=ppcg_sbsize, davidson_maxdim=davidson_maxdim,
                        cheby_degree=cheby_degree, cheby_first_cycles=cheby_first_cycles, eig_max_iter=eig_max_iter,
                        max_iter=max_iter, mix_dim=mix_dim, mixed=int(mixed), verbose=int(verbose), ecut=ecut,
                        temperature=temperature, eig_tol=eig_tol, mix_step=mix_step, tol_efree=tol_efree,

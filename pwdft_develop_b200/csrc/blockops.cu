@@ -115,6 +115,129 @@ template int colnorm2<double>(int, int, const double*, long, double*, cudaStream
 template int colscale<float>(int, int, float*, long, const double*, cudaStream_t);
 template int colscale<double>(int, int, double*, long, const double*, cudaStream_t);
 
+// Diagonal sb x sb blocks of U^T V over one grid-point split; partial sums
+// written to part[(split * nsb + k) * SB * SB + i + j * SB].
+template <typename T, int SB>
+__global__ void __launch_bounds__(256)
+k_bdiag_dots(int n, int width, int sb, const T* __restrict__ U, const T* __restrict__ V, long ld, int chunk,
+             double* __restrict__ part) {
+  const int k = blockIdx.x, split = blockIdx.y, nsb = gridDim.x;
+  const int c0 = k * sb;
+  const int sbk = min(sb, width - c0);
+  const int g0 = split * chunk, g1 = min(n, g0 + chunk);
+  double acc[SB * SB];
+#pragma unroll
+  for (int e = 0; e < SB * SB; ++e) acc[e] = 0.0;
+  for (int g = g0 + threadIdx.x; g < g1; g += blockDim.x) {
+    double u[SB], v[SB];
+#pragma unroll
+    for (int i = 0; i < SB; ++i) {
+      u[i] = i < sbk ? (double)U[(long)(c0 + i) * ld + g] : 0.0;
+      v[i] = i < sbk ? (double)V[(long)(c0 + i) * ld + g] : 0.0;
+    }
+#pragma unroll
+    for (int j = 0; j < SB; ++j)
+#pragma unroll
+      for (int i = 0; i < SB; ++i) acc[i + j * SB] += u[i] * v[j];
+  }
+  __shared__ double red[8][SB * SB];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int e = 0; e < SB * SB; ++e) {
+    double x = acc[e];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if (lane == 0) red[warp][e] = x;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < SB * SB; e += blockDim.x) {
+    double x = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) x += red[w][e];
+    part[((long)split * nsb + k) * SB * SB + e] = x;
+  }
+}
+
+// Y[:, k*sb + j] = beta Y + sum_i X[:, k*sb + i] C[k*sb*sb + i + j*sb]
+template <typename T, int SB>
+__global__ void k_bdiag_rotate(int n, int width, int sb, const T* __restrict__ X, long ldx,
+                               const double* __restrict__ C, T* __restrict__ Y, long ldy, double beta) {
+  const int k = blockIdx.y;
+  const int c0 = k * sb;
+  const int sbk = min(sb, width - c0);
+  const double* Ck = C + (long)k * sb * sb;
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < n; g += gridDim.x * blockDim.x) {
+    double x[SB];
+#pragma unroll
+    for (int i = 0; i < SB; ++i) x[i] = i < sbk ? (double)X[(long)(c0 + i) * ldx + g] : 0.0;
+#pragma unroll
+    for (int j = 0; j < SB; ++j) {
+      if (j < sbk) {
+        double y = 0;
+#pragma unroll
+        for (int i = 0; i < SB; ++i)
+          if (i < sbk) y += x[i] * Ck[i + j * sb];
+        T* yp = Y + (long)(c0 + j) * ldy + g;
+        *yp = (T)(beta == 0.0 ? y : y + beta * (double)*yp);
+      }
+    }
+  }
+}
+
+template <typename T>
+int bdiag_dots(int n, int width, int sb, const T* U, const T* V, long ld, DevBuf& part, double* out_host,
+               cudaStream_t st) {
+  PWB_CHECK(sb >= 1 && sb <= 8, PW_EUNSUPPORTED, "sub-block size 1..8");
+  const int nsb = (width + sb - 1) / sb;
+  const int nsplit = std::max(1, std::min(64, (2 * 148 + nsb - 1) / nsb));
+  const int chunk = (n + nsplit - 1) / nsplit;
+  const int SBp = sb == 1 ? 1 : sb == 2 ? 2 : sb <= 4 ? 4 : 8;
+  int rc = part.alloc((size_t)nsplit * nsb * SBp * SBp * 8);
+  if (rc) return rc;
+  double* pp = (double*)part.p;
+  dim3 grid(nsb, nsplit);
+  switch (SBp) {
+    case 1: k_bdiag_dots<T, 1><<<grid, 256, 0, st>>>(n, width, sb, U, V, ld, chunk, pp); break;
+    case 2: k_bdiag_dots<T, 2><<<grid, 256, 0, st>>>(n, width, sb, U, V, ld, chunk, pp); break;
+    case 4: k_bdiag_dots<T, 4><<<grid, 256, 0, st>>>(n, width, sb, U, V, ld, chunk, pp); break;
+    default: k_bdiag_dots<T, 8><<<grid, 256, 0, st>>>(n, width, sb, U, V, ld, chunk, pp); break;
+  }
+  PWB_CUDA(cudaGetLastError());
+  std::vector<double> h((size_t)nsplit * nsb * SBp * SBp);
+  PWB_CUDA(cudaMemcpyAsync(h.data(), pp, h.size() * 8, cudaMemcpyDeviceToHost, st));
+  PWB_CUDA(cudaStreamSynchronize(st));
+  // deterministic sum over splits; out_host[k][i + j*sb]
+  for (int k = 0; k < nsb; ++k)
+    for (int j = 0; j < sb; ++j)
+      for (int i = 0; i < sb; ++i) {
+        double x = 0;
+        for (int sp = 0; sp < nsplit; ++sp) x += h[((size_t)sp * nsb + k) * SBp * SBp + i + j * SBp];
+        out_host[(size_t)k * sb * sb + i + j * sb] = x;
+      }
+  return PW_OK;
+}
+
+template <typename T>
+int bdiag_rotate(int n, int width, int sb, const T* X, long ldx, const double* C_dev, T* Y, long ldy, double beta,
+                 cudaStream_t st) {
+  PWB_CHECK(sb >= 1 && sb <= 8, PW_EUNSUPPORTED, "sub-block size 1..8");
+  const int nsb = (width + sb - 1) / sb;
+  dim3 grid(std::max(1, std::min((n + 255) / 256, 128)), nsb);
+  const int SBp = sb == 1 ? 1 : sb == 2 ? 2 : sb <= 4 ? 4 : 8;
+  switch (SBp) {
+    case 1: k_bdiag_rotate<T, 1><<<grid, 256, 0, st>>>(n, width, sb, X, ldx, C_dev, Y, ldy, beta); break;
+    case 2: k_bdiag_rotate<T, 2><<<grid, 256, 0, st>>>(n, width, sb, X, ldx, C_dev, Y, ldy, beta); break;
+    case 4: k_bdiag_rotate<T, 4><<<grid, 256, 0, st>>>(n, width, sb, X, ldx, C_dev, Y, ldy, beta); break;
+    default: k_bdiag_rotate<T, 8><<<grid, 256, 0, st>>>(n, width, sb, X, ldx, C_dev, Y, ldy, beta); break;
+  }
+  PWB_CUDA(cudaGetLastError());
+  return PW_OK;
+}
+
+template int bdiag_dots<float>(int, int, int, const float*, const float*, long, DevBuf&, double*, cudaStream_t);
+template int bdiag_dots<double>(int, int, int, const double*, const double*, long, DevBuf&, double*, cudaStream_t);
+template int bdiag_rotate<float>(int, int, int, const float*, long, const double*, float*, long, double, cudaStream_t);
+template int bdiag_rotate<double>(int, int, int, const double*, long, const double*, double*, long, double,
+                                  cudaStream_t);
+
 int rotate(pw_ctx* c, int n, int m, const RotBlock* blocks, int nblk, void* out, long ldo, double beta, cudaStream_t st) {
   cublasHandle_t h = (cublasHandle_t)c->blas;
   cublasSetStream(h, st);

@@ -23,6 +23,17 @@ int copy_f2d(long n, const float* x, double* y, cudaStream_t st);
 int copy_d2f_2d(int n, int nb, const double* x, long ldx, float* y, long ldy, cudaStream_t st);
 int copy_f2d_2d(int n, int nb, const float* x, long ldx, double* y, long ldy, cudaStream_t st);
 
+// Diagonal sb x sb blocks of U^T V (width columns, grid length n) for the PPCG
+// sub-block sweep: out_host[k * sb * sb + i + j * sb], k < ceil(width / sb),
+// FP64, summed over grid-point splits in a fixed order.  sb in 1..8.
+template <typename T>
+int bdiag_dots(int n, int width, int sb, const T* U, const T* V, long ld, DevBuf& part, double* out_host,
+               cudaStream_t st);
+// Y (+)= X * blockdiag(C_k): Y[:, k*sb + j] = beta Y + sum_i X[:, k*sb + i] C[k*sb*sb + i + j*sb]
+template <typename T>
+int bdiag_rotate(int n, int width, int sb, const T* X, long ldx, const double* C_dev, T* Y, long ldy, double beta,
+                 cudaStream_t st);
+
 // Out (n x m, ldo) = sum over blocks of X_b (n x k_b, ld) * C_b (k_b x m, FP64 column-major, ldc),
 // beta = 0 or 1 for Out.  The context precision decides FP64 or FP32 storage of X / Out.
 struct RotBlock {

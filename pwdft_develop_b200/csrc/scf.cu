@@ -518,6 +518,452 @@ static int lobpcg(Solver& s, Dense& d, int width, int maxit, double tol, bool fi
   return PW_OK;
 }
 
+// ---------------------------------------------------------------------------
+// small dense generalized symmetric eigenproblem on the host (PPCG sub-blocks)
+// ---------------------------------------------------------------------------
+// cyclic Jacobi: M (n x n, column major, symmetric) -> V diag(M) V^T, in place
+static void jacobi_eig(int n, std::vector<double>& M, std::vector<double>& V) {
+  V.assign((size_t)n * n, 0.0);
+  for (int i = 0; i < n; ++i) V[i + (size_t)i * n] = 1.0;
+  for (int sweep = 0; sweep < 100; ++sweep) {
+    double off = 0.0, tot = 0.0;
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < n; ++i) {
+        const double x = M[i + (size_t)j * n];
+        tot += x * x;
+        if (i != j) off += x * x;
+      }
+    if (off == 0.0 || off <= 1e-30 * tot) break;
+    for (int p = 0; p < n - 1; ++p)
+      for (int q = p + 1; q < n; ++q) {
+        const double apq = M[p + (size_t)q * n];
+        if (apq == 0.0) continue;
+        const double app = M[p + (size_t)p * n], aqq = M[q + (size_t)q * n];
+        const double theta = (aqq - app) / (2.0 * apq);
+        const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+        const double c = 1.0 / std::sqrt(t * t + 1.0), sn = t * c;
+        for (int k = 0; k < n; ++k) {
+          const double mkp = M[k + (size_t)p * n], mkq = M[k + (size_t)q * n];
+          M[k + (size_t)p * n] = c * mkp - sn * mkq;
+          M[k + (size_t)q * n] = sn * mkp + c * mkq;
+        }
+        for (int k = 0; k < n; ++k) {
+          const double mpk = M[p + (size_t)k * n], mqk = M[q + (size_t)k * n];
+          M[p + (size_t)k * n] = c * mpk - sn * mqk;
+          M[q + (size_t)k * n] = sn * mpk + c * mqk;
+        }
+        for (int k = 0; k < n; ++k) {
+          const double vkp = V[k + (size_t)p * n], vkq = V[k + (size_t)q * n];
+          V[k + (size_t)p * n] = c * vkp - sn * vkq;
+          V[k + (size_t)q * n] = sn * vkp + c * vkq;
+        }
+      }
+  }
+}
+
+// A z = lambda B z for n <= 24 from the upper triangles of A and B (column
+// major, leading dimension ld).  The reference calls LAPACK dsygvd here; to
+// stay defined when the sub-block's search directions become numerically
+// dependent (a converged column's residual), B is diagonalised first and only
+// directions with sigma / sigma_max > 1e-8 are kept -- the SolveGenEig
+// treatment (eigensolver.cpp:224-297) -- which equals dsygvd for a
+// well-conditioned B.  Returns the number r of kept directions; Z (n x r) holds
+// B-orthonormal eigenvectors for the r ascending eigenvalues w.
+static int small_sygv(int n, const double* A, const double* B, int ld, double* w, double* Z) {
+  std::vector<double> a((size_t)n * n), b((size_t)n * n), U;
+  for (int j = 0; j < n; ++j)
+    for (int i = 0; i <= j; ++i) {
+      a[i + (size_t)j * n] = a[j + (size_t)i * n] = A[i + (size_t)j * ld];
+      b[i + (size_t)j * n] = b[j + (size_t)i * n] = B[i + (size_t)j * ld];
+    }
+  jacobi_eig(n, b, U);
+  double smax = 0.0;
+  for (int i = 0; i < n; ++i) smax = std::max(smax, b[i + (size_t)i * n]);
+  std::vector<int> kept;
+  for (int i = 0; i < n; ++i)
+    if (smax > 0.0 && b[i + (size_t)i * n] / smax > 1e-8) kept.push_back(i);
+  const int r = (int)kept.size();
+  if (r == 0) return 0;
+  // Q = U_k sigma_k^-1/2 (n x r); M = Q^T A Q
+  std::vector<double> Q((size_t)n * r), AQ((size_t)n * r), M((size_t)r * r), V;
+  for (int j = 0; j < r; ++j) {
+    const int c = kept[j];
+    const double f = 1.0 / std::sqrt(b[c + (size_t)c * n]);
+    for (int i = 0; i < n; ++i) Q[i + (size_t)j * n] = U[i + (size_t)c * n] * f;
+  }
+  for (int j = 0; j < r; ++j)
+    for (int i = 0; i < n; ++i) {
+      double t = 0.0;
+      for (int k = 0; k < n; ++k) t += a[i + (size_t)k * n] * Q[k + (size_t)j * n];
+      AQ[i + (size_t)j * n] = t;
+    }
+  for (int j = 0; j < r; ++j)
+    for (int i = 0; i < r; ++i) {
+      double t = 0.0;
+      for (int k = 0; k < n; ++k) t += Q[k + (size_t)i * n] * AQ[k + (size_t)j * n];
+      M[i + (size_t)j * r] = t;
+    }
+  for (int j = 0; j < r; ++j)
+    for (int i = 0; i < j; ++i) M[i + (size_t)j * r] = M[j + (size_t)i * r] = 0.5 * (M[i + (size_t)j * r] + M[j + (size_t)i * r]);
+  jacobi_eig(r, M, V);
+  std::vector<int> ord(r);
+  for (int i = 0; i < r; ++i) ord[i] = i;
+  std::sort(ord.begin(), ord.end(), [&](int x, int y) { return M[x + (size_t)x * r] < M[y + (size_t)y * r]; });
+  for (int jj = 0; jj < r; ++jj) {
+    const int j = ord[jj];
+    w[jj] = M[j + (size_t)j * r];
+    for (int i = 0; i < n; ++i) {
+      double t = 0.0;
+      for (int k = 0; k < r; ++k) t += Q[i + (size_t)k * n] * V[k + (size_t)j * r];
+      Z[i + (size_t)jj * n] = t;
+    }
+  }
+  return r;
+}
+
+static int v_bdiag_dots(Solver& s, int width, int sb, const void* U, const void* V, DevBuf& part, double* out) {
+  return s.c->prec == PW_F64
+             ? bdiag_dots<double>((int)s.nt, width, sb, (const double*)U, (const double*)V, s.nt, part, out, nullptr)
+             : bdiag_dots<float>((int)s.nt, width, sb, (const float*)U, (const float*)V, s.nt, part, out, nullptr);
+}
+static int v_bdiag_rotate(Solver& s, int width, int sb, const void* X, const double* C, void* Y, double beta) {
+  return s.c->prec == PW_F64
+             ? bdiag_rotate<double>((int)s.nt, width, sb, (const double*)X, s.nt, C, (double*)Y, s.nt, beta, nullptr)
+             : bdiag_rotate<float>((int)s.nt, width, sb, (const float*)X, s.nt, C, (float*)Y, s.nt, beta, nullptr);
+}
+
+// V -= X (X^T V), AV -= AX (X^T V)
+static int project_out(Solver& s, int width, void* X, void* AX, void* V, void* AV, DevBuf& G) {
+  int rc;
+  if ((rc = G.alloc((size_t)width * width * 8))) return rc;
+  double* g = (double*)G.p;
+  if ((rc = gram(s.c, X, (int)s.nt, width, V, (int)s.nt, width, g, width, nullptr))) return rc;
+  std::vector<double> h((size_t)width * width);
+  PWB_CUDA(cudaMemcpy(h.data(), g, h.size() * 8, cudaMemcpyDeviceToHost));
+  for (double& x : h) x = -x;
+  PWB_CUDA(cudaMemcpy(g, h.data(), h.size() * 8, cudaMemcpyHostToDevice));
+  RotBlock rb{X, s.nt, width, g, width};
+  if ((rc = rotate(s.c, (int)s.nt, width, &rb, 1, V, s.nt, 1.0, nullptr))) return rc;
+  RotBlock ra{AX, s.nt, width, g, width};
+  return rotate(s.c, (int)s.nt, width, &ra, 1, AV, s.nt, 1.0, nullptr);
+}
+
+// V, AV /= ||V|| column-wise
+static int normalize_pair(Solver& s, int width, void* V, void* AV, DevBuf& tmp) {
+  int rc;
+  if ((rc = tmp.alloc((size_t)width * 8))) return rc;
+  double* d = (double*)tmp.p;
+  if ((rc = v_colnorm2(s, width, V, d))) return rc;
+  std::vector<double> h(width);
+  PWB_CUDA(cudaMemcpy(h.data(), d, width * 8, cudaMemcpyDeviceToHost));
+  // a vanishing direction (exactly converged column) stays zero instead of 0/0
+  for (double& x : h) x = x > 1e-300 ? 1.0 / std::sqrt(x) : 0.0;
+  PWB_CUDA(cudaMemcpy(d, h.data(), width * 8, cudaMemcpyHostToDevice));
+  if ((rc = v_colscale(s, width, V, d))) return rc;
+  return AV ? v_colscale(s, width, AV, d) : PW_OK;
+}
+
+// Cholesky-QR of X with AX transformed alongside: X <- X U^-1, AX <- AX U^-1
+static int cholqr_pair(Solver& s, Dense& d, void* X, void* AX, int nb, void* tmp) {
+  const cudaStream_t st = nullptr;
+  int rc;
+  if ((rc = s.G1.alloc((size_t)nb * nb * 8)) || (rc = s.G2.alloc((size_t)nb * nb * 8))) return rc;
+  double* G = (double*)s.G1.p;
+  if ((rc = gram(s.c, X, (int)s.nt, nb, X, (int)s.nt, nb, G, nb, st))) return rc;
+  if ((rc = d.potrf_upper(nb, G, nb, st))) return rc;
+  std::vector<double> hg((size_t)nb * nb);
+  PWB_CUDA(cudaMemcpy(hg.data(), G, hg.size() * 8, cudaMemcpyDeviceToHost));
+  for (int j = 0; j < nb; ++j)
+    for (int i = j + 1; i < nb; ++i) hg[(size_t)j * nb + i] = 0.0;
+  PWB_CUDA(cudaMemcpy(G, hg.data(), hg.size() * 8, cudaMemcpyHostToDevice));
+  double* Ui = (double*)s.G2.p;
+  std::vector<double> I((size_t)nb * nb, 0.0);
+  for (int i = 0; i < nb; ++i) I[(size_t)i * nb + i] = 1.0;
+  PWB_CUDA(cudaMemcpy(Ui, I.data(), I.size() * 8, cudaMemcpyHostToDevice));
+  const double one = 1.0;
+  cublasSetStream(d.blas, st);
+  if (cublasDtrsm(d.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, nb, nb, &one, G,
+                  nb, Ui, nb) != CUBLAS_STATUS_SUCCESS) {
+    set_error("trsm failed");
+    return PW_ECUDA;
+  }
+  RotBlock rb{X, s.nt, nb, Ui, nb};
+  if ((rc = rotate(s.c, (int)s.nt, nb, &rb, 1, tmp, s.nt, 0.0, st))) return rc;
+  PWB_CUDA(cudaMemcpy(X, tmp, (size_t)nb * s.nt * s.esz, cudaMemcpyDeviceToDevice));
+  RotBlock ra{AX, s.nt, nb, Ui, nb};
+  if ((rc = rotate(s.c, (int)s.nt, nb, &ra, 1, tmp, s.nt, 0.0, st))) return rc;
+  PWB_CUDA(cudaMemcpy(AX, tmp, (size_t)nb * s.nt * s.esz, cudaMemcpyDeviceToDevice));
+  return PW_OK;
+}
+
+// PPCG restated from EigenSolver::PPCGSolveReal, real-space branch
+// (src/EigenSolver/ppcg.cpp:670-1243): residual R = AX - X (X^T AX), W = T R,
+// W and P made orthogonal to X, per sub-block of sb columns a 2sb / 3sb
+// generalized Rayleigh-Ritz (Sygvd) giving x <- x cx + p, p <- w cw + p cp,
+// Cholesky-QR of X every iteration, final Rayleigh-Ritz.  No locking.
+static int ppcg(Solver& s, Dense& d, int width, int sb, int maxit, double tol, bool first_scf, int* iters) {
+  int rc;
+  const long nt = s.nt;
+  const size_t esz = s.esz;
+  sb = std::max(1, std::min(sb, std::min(8, width)));
+  const int nsb = (width + sb - 1) / sb;
+  if ((rc = alloc_block(s, s.S, 3 * width)) || (rc = alloc_block(s, s.HS, 3 * width)) || (rc = alloc_block(s, s.Y, width)))
+    return rc;
+  void* X = s.ptr(s.S, 0);
+  void* W = s.ptr(s.S, width);
+  void* P = s.ptr(s.S, 2 * width);
+  void* AX = s.ptr(s.HS, 0);
+  void* AW = s.ptr(s.HS, width);
+  void* AP = s.ptr(s.HS, 2 * width);
+  PWB_CUDA(cudaMemcpy(X, s.X.p, (size_t)width * nt * esz, cudaMemcpyDeviceToDevice));
+  if (first_scf && (rc = cholqr(s, d, X, width, s.Y.p))) return rc;
+  if ((rc = hpsi(s.c, X, AX, width, nullptr))) return rc;
+  DevBuf G, tmpv, part, Cd;
+  if ((rc = Cd.alloc((size_t)3 * nsb * sb * sb * 8))) return rc;
+  double* Cx = (double*)Cd.p;
+  double* Cw = Cx + (size_t)nsb * sb * sb;
+  double* Cp = Cw + (size_t)nsb * sb * sb;
+  const size_t bs = (size_t)nsb * sb * sb;
+  std::vector<double> xax(bs), waw(bs), xaw(bs), xx(bs), ww(bs), xw(bs), pap(bs), xap(bs), wap(bs), pp(bs), xp(bs),
+      wp(bs), hc(3 * bs);
+  std::vector<double> resNorm(width);
+  double resMax = 0;
+  int iter = 0;
+  do {
+    ++iter;
+    const int numSet = (iter == 1) ? 2 : 3;
+    // R = AX - X (X^T AX) into Y
+    if ((rc = G.alloc((size_t)width * width * 8))) return rc;
+    double* g = (double*)G.p;
+    if ((rc = gram(s.c, X, (int)nt, width, AX, (int)nt, width, g, width, nullptr))) return rc;
+    std::vector<double> hg((size_t)width * width);
+    PWB_CUDA(cudaMemcpy(hg.data(), g, hg.size() * 8, cudaMemcpyDeviceToHost));
+    std::vector<double> mg(hg.size());
+    for (size_t i = 0; i < hg.size(); ++i) mg[i] = -hg[i];
+    PWB_CUDA(cudaMemcpy(g, mg.data(), mg.size() * 8, cudaMemcpyHostToDevice));
+    PWB_CUDA(cudaMemcpy(s.Y.p, AX, (size_t)width * nt * esz, cudaMemcpyDeviceToDevice));
+    RotBlock rb{X, nt, width, g, width};
+    if ((rc = rotate(s.c, (int)nt, width, &rb, 1, s.Y.p, nt, 1.0, nullptr))) return rc;
+    if ((rc = tmpv.alloc((size_t)width * 8))) return rc;
+    if ((rc = v_colnorm2(s, width, s.Y.p, (double*)tmpv.p))) return rc;
+    std::vector<double> hn(width);
+    PWB_CUDA(cudaMemcpy(hn.data(), tmpv.p, width * 8, cudaMemcpyDeviceToHost));
+    for (int k = 0; k < width; ++k)
+      resNorm[k] = std::sqrt(hn[k]) / std::max(1.0, std::fabs(hg[(size_t)k * width + k]));
+    resMax = *std::max_element(resNorm.begin(), resNorm.end());
+    // W = T R, AW = H W, orthogonal to X, normalised
+    if ((rc = pw_teter_precond(s.c, s.Y.p, (int)nt, W, (int)nt, width, 0, nullptr))) return rc;
+    if ((rc = hpsi(s.c, W, AW, width, nullptr))) return rc;
+    if ((rc = project_out(s, width, X, AX, W, AW, G))) return rc;
+    if ((rc = normalize_pair(s, width, W, AW, tmpv))) return rc;
+    if (numSet == 3) {
+      if ((rc = project_out(s, width, X, AX, P, AP, G))) return rc;
+      if ((rc = normalize_pair(s, width, P, AP, tmpv))) return rc;
+    }
+    // sub-block Gram blocks
+    {
+      SubTimer t_(1);
+      if ((rc = v_bdiag_dots(s, width, sb, X, AX, part, xax.data())) ||
+          (rc = v_bdiag_dots(s, width, sb, W, AW, part, waw.data())) ||
+          (rc = v_bdiag_dots(s, width, sb, X, AW, part, xaw.data())) ||
+          (rc = v_bdiag_dots(s, width, sb, X, X, part, xx.data())) ||
+          (rc = v_bdiag_dots(s, width, sb, W, W, part, ww.data())) ||
+          (rc = v_bdiag_dots(s, width, sb, X, W, part, xw.data())))
+        return rc;
+      if (numSet == 3 &&
+          ((rc = v_bdiag_dots(s, width, sb, P, AP, part, pap.data())) ||
+           (rc = v_bdiag_dots(s, width, sb, X, AP, part, xap.data())) ||
+           (rc = v_bdiag_dots(s, width, sb, W, AP, part, wap.data())) ||
+           (rc = v_bdiag_dots(s, width, sb, P, P, part, pp.data())) ||
+           (rc = v_bdiag_dots(s, width, sb, X, P, part, xp.data())) ||
+           (rc = v_bdiag_dots(s, width, sb, W, P, part, wp.data()))))
+        return rc;
+    }
+    // nsb small generalized eigenproblems (Sygvd)
+    std::fill(hc.begin(), hc.end(), 0.0);
+    for (int k = 0; k < nsb; ++k) {
+      const int m = std::min(sb, width - k * sb);
+      const int dim = numSet * m, ld = 3 * sb;
+      std::vector<double> A((size_t)ld * ld, 0.0), B((size_t)ld * ld, 0.0), Z((size_t)dim * dim), ev(dim);
+      auto put = [&](std::vector<double>& M, int r0, int c0, const std::vector<double>& src) {
+        for (int j = 0; j < m; ++j)
+          for (int i = 0; i < m; ++i) M[(r0 + i) + (size_t)(c0 + j) * ld] = src[(size_t)k * sb * sb + i + j * sb];
+      };
+      put(A, 0, 0, xax); put(A, m, m, waw); put(A, 0, m, xaw);
+      put(B, 0, 0, xx); put(B, m, m, ww); put(B, 0, m, xw);
+      if (numSet == 3) {
+        put(A, 2 * m, 2 * m, pap); put(A, 0, 2 * m, xap); put(A, m, 2 * m, wap);
+        put(B, 2 * m, 2 * m, pp); put(B, 0, 2 * m, xp); put(B, m, 2 * m, wp);
+      }
+      double* cx = &hc[(size_t)k * sb * sb];
+      double* cw = cx + bs;
+      double* cp = cw + bs;
+      if (small_sygv(dim, A.data(), B.data(), ld, ev.data(), Z.data()) >= m) {
+        for (int j = 0; j < m; ++j)
+          for (int i = 0; i < m; ++i) {
+            cx[i + j * sb] = Z[i + (size_t)j * dim];
+            cw[i + j * sb] = Z[(m + i) + (size_t)j * dim];
+            if (numSet == 3) cp[i + j * sb] = Z[(2 * m + i) + (size_t)j * dim];
+          }
+      } else {
+        // fewer independent directions than columns: keep x
+        for (int i = 0; i < m; ++i) cx[i + i * sb] = 1.0;
+      }
+    }
+    PWB_CUDA(cudaMemcpy(Cx, hc.data(), hc.size() * 8, cudaMemcpyHostToDevice));
+    {
+      SubTimer t_(3);
+      // p = w cw (+ p cp); ap = aw cw (+ ap cp)
+      if (numSet == 3) {
+        if ((rc = v_bdiag_rotate(s, width, sb, P, Cp, s.Y.p, 0.0)) ||
+            (rc = v_bdiag_rotate(s, width, sb, W, Cw, s.Y.p, 1.0)))
+          return rc;
+        PWB_CUDA(cudaMemcpy(P, s.Y.p, (size_t)width * nt * esz, cudaMemcpyDeviceToDevice));
+        if ((rc = v_bdiag_rotate(s, width, sb, AP, Cp, s.Y.p, 0.0)) ||
+            (rc = v_bdiag_rotate(s, width, sb, AW, Cw, s.Y.p, 1.0)))
+          return rc;
+        PWB_CUDA(cudaMemcpy(AP, s.Y.p, (size_t)width * nt * esz, cudaMemcpyDeviceToDevice));
+      } else {
+        if ((rc = v_bdiag_rotate(s, width, sb, W, Cw, P, 0.0)) || (rc = v_bdiag_rotate(s, width, sb, AW, Cw, AP, 0.0)))
+          return rc;
+      }
+      // x = x cx + p; ax = ax cx + ap
+      PWB_CUDA(cudaMemcpy(s.Y.p, P, (size_t)width * nt * esz, cudaMemcpyDeviceToDevice));
+      if ((rc = v_bdiag_rotate(s, width, sb, X, Cx, s.Y.p, 1.0))) return rc;
+      PWB_CUDA(cudaMemcpy(X, s.Y.p, (size_t)width * nt * esz, cudaMemcpyDeviceToDevice));
+      PWB_CUDA(cudaMemcpy(s.Y.p, AP, (size_t)width * nt * esz, cudaMemcpyDeviceToDevice));
+      if ((rc = v_bdiag_rotate(s, width, sb, AX, Cx, s.Y.p, 1.0))) return rc;
+      PWB_CUDA(cudaMemcpy(AX, s.Y.p, (size_t)width * nt * esz, cudaMemcpyDeviceToDevice));
+    }
+    // Cholesky-QR of X, AX transformed alongside
+    if ((rc = cholqr_pair(s, d, X, AX, width, s.Y.p))) return rc;
+  } while (iter < maxit && resMax > tol);
+  // final Rayleigh-Ritz (ppcg.cpp:1112-1166)
+  if ((rc = rayleigh_ritz(s, d, X, AX, s.X.p, s.HX.p, width))) return rc;
+  if (iters) *iters = iter;
+  return residuals(s, width);
+}
+
+// Block Davidson restated from EigenSolver::DavidsonSolveReal
+// (src/EigenSolver/davidson.cpp:60-806): subspace S = (X | W_1 | ...) of at
+// most maxdim * width columns; residuals of the unconverged Ritz pairs,
+// Teter-preconditioned and normalised, are appended; generalized
+// Rayleigh-Ritz on S (SolveGenEig); convergence on the change of each Ritz
+// value; restart from the Ritz vectors when the subspace is full.
+static int davidson(Solver& s, Dense& d, int width, int maxdim, int maxit, double tol, bool first_scf, int* iters) {
+  int rc;
+  const long nt = s.nt;
+  const size_t esz = s.esz;
+  maxdim = std::max(2, maxdim);
+  const int w = width, lda = maxdim * w;
+  if ((rc = alloc_block(s, s.S, lda)) || (rc = alloc_block(s, s.HS, lda)) || (rc = alloc_block(s, s.Y, w)))
+    return rc;
+  void* X = s.ptr(s.S, 0);
+  void* AX = s.ptr(s.HS, 0);
+  PWB_CUDA(cudaMemcpy(X, s.X.p, (size_t)w * nt * esz, cudaMemcpyDeviceToDevice));
+  if (first_scf && (rc = cholqr(s, d, X, w, s.Y.p))) return rc;
+  if ((rc = hpsi(s.c, X, AX, w, nullptr))) return rc;
+  if ((rc = s.G1.alloc((size_t)lda * lda * 8)) || (rc = s.G2.alloc((size_t)lda * lda * 8))) return rc;
+  double* A = (double*)s.G1.p;
+  double* B = (double*)s.G2.p;
+  std::vector<double> Asave((size_t)lda * lda, 0.0), Bsave((size_t)lda * lda, 0.0), hC((size_t)lda * lda);
+  DevBuf G, Cd, tmpv;
+  if ((rc = G.alloc((size_t)lda * w * 8)) || (rc = Cd.alloc((size_t)lda * w * 8)) || (rc = tmpv.alloc((size_t)w * 8)))
+    return rc;
+  auto fetch = [&](int nrow, int ncol, std::vector<double>& dst, int r0, int c0) -> int {
+    std::vector<double> h((size_t)nrow * ncol);
+    PWB_CUDA(cudaMemcpy(h.data(), G.p, h.size() * 8, cudaMemcpyDeviceToHost));
+    for (int j = 0; j < ncol; ++j)
+      for (int i = 0; i < nrow; ++i) dst[(r0 + i) + (size_t)(c0 + j) * lda] = h[i + (size_t)j * nrow];
+    return PW_OK;
+  };
+  if ((rc = gram(s.c, X, (int)nt, w, AX, (int)nt, w, (double*)G.p, w, nullptr)) || (rc = fetch(w, w, Asave, 0, 0)))
+    return rc;
+  if ((rc = gram(s.c, X, (int)nt, w, X, (int)nt, w, (double*)G.p, w, nullptr)) || (rc = fetch(w, w, Bsave, 0, 0)))
+    return rc;
+  PWB_CUDA(cudaMemcpy(A, Asave.data(), Asave.size() * 8, cudaMemcpyHostToDevice));
+  PWB_CUDA(cudaMemcpy(B, Bsave.data(), Bsave.size() * 8, cudaMemcpyHostToDevice));
+  std::vector<double> eigS(w), eigT(lda), res(w, 0.0);
+  int keep = 0;
+  if ((rc = solve_gen_eig(d, lda, w, w, A, B, eigT.data(), &keep, nullptr))) return rc;
+  std::copy(eigT.begin(), eigT.begin() + w, eigS.begin());
+  std::vector<int> conv(w, 0);
+  int nb = w, na = w, iter = 0;
+  for (iter = 1; iter <= maxit; ++iter) {
+    // compact the Ritz coefficients of the unconverged pairs
+    PWB_CUDA(cudaMemcpy(hC.data(), A, hC.size() * 8, cudaMemcpyDeviceToHost));
+    std::vector<double> cc((size_t)nb * na), lam(na);
+    for (int i = 0, j = 0; i < w; ++i)
+      if (!conv[i]) {
+        for (int r = 0; r < nb; ++r) cc[r + (size_t)j * nb] = hC[r + (size_t)i * lda];
+        lam[j] = -eigS[i];
+        ++j;
+      }
+    PWB_CUDA(cudaMemcpy(Cd.p, cc.data(), cc.size() * 8, cudaMemcpyHostToDevice));
+    // Wn = AS C - S C diag(lambda), appended at column nb
+    void* Wn = s.ptr(s.S, nb);
+    void* AWn = s.ptr(s.HS, nb);
+    RotBlock r1{s.S.p, nt, nb, (const double*)Cd.p, nb};
+    if ((rc = rotate(s.c, (int)nt, na, &r1, 1, s.Y.p, nt, 0.0, nullptr))) return rc;
+    PWB_CUDA(cudaMemcpy(tmpv.p, lam.data(), na * 8, cudaMemcpyHostToDevice));
+    if ((rc = v_colscale(s, na, s.Y.p, (const double*)tmpv.p))) return rc;
+    RotBlock r2{s.HS.p, nt, nb, (const double*)Cd.p, nb};
+    if ((rc = rotate(s.c, (int)nt, na, &r2, 1, Wn, nt, 0.0, nullptr))) return rc;
+    if ((rc = v_axpby(s, na, 1.0, s.Y.p, 1.0, Wn))) return rc;
+    // precondition, normalise, apply H
+    if ((rc = pw_teter_precond(s.c, Wn, (int)nt, s.Y.p, (int)nt, na, 0, nullptr))) return rc;
+    PWB_CUDA(cudaMemcpy(Wn, s.Y.p, (size_t)na * nt * esz, cudaMemcpyDeviceToDevice));
+    if ((rc = normalize_pair(s, na, Wn, nullptr, tmpv))) return rc;
+    if ((rc = hpsi(s.c, Wn, AWn, na, nullptr))) return rc;
+    // extend the projected pencil by the new columns
+    if ((rc = gram(s.c, s.S.p, (int)nt, nb + na, AWn, (int)nt, na, (double*)G.p, nb + na, nullptr)) ||
+        (rc = fetch(nb + na, na, Asave, 0, nb)))
+      return rc;
+    if ((rc = gram(s.c, s.S.p, (int)nt, nb + na, Wn, (int)nt, na, (double*)G.p, nb + na, nullptr)) ||
+        (rc = fetch(nb + na, na, Bsave, 0, nb)))
+      return rc;
+    nb += na;
+    PWB_CUDA(cudaMemcpy(A, Asave.data(), Asave.size() * 8, cudaMemcpyHostToDevice));
+    PWB_CUDA(cudaMemcpy(B, Bsave.data(), Bsave.size() * 8, cudaMemcpyHostToDevice));
+    if ((rc = solve_gen_eig(d, lda, nb, w, A, B, eigT.data(), &keep, nullptr))) return rc;
+    na = 0;
+    for (int i = 0; i < w; ++i) {
+      res[i] = std::fabs(eigS[i] - eigT[i]);
+      conv[i] = res[i] < tol ? 1 : 0;
+      if (!conv[i]) ++na;
+    }
+    std::copy(eigT.begin(), eigT.begin() + w, eigS.begin());
+    const bool done = (na == 0) || iter == maxit;
+    if (done || nb + na > lda) {
+      // X = S C, AX = AS C (Ritz vectors)
+      RotBlock rx{s.S.p, nt, nb, A, lda};
+      if ((rc = rotate(s.c, (int)nt, w, &rx, 1, s.Y.p, nt, 0.0, nullptr))) return rc;
+      PWB_CUDA(cudaMemcpy(X, s.Y.p, (size_t)w * nt * esz, cudaMemcpyDeviceToDevice));
+      RotBlock ra{s.HS.p, nt, nb, A, lda};
+      if ((rc = rotate(s.c, (int)nt, w, &ra, 1, s.Y.p, nt, 0.0, nullptr))) return rc;
+      PWB_CUDA(cudaMemcpy(AX, s.Y.p, (size_t)w * nt * esz, cudaMemcpyDeviceToDevice));
+      if (done) break;
+      // restart from the Ritz vectors
+      nb = w;
+      std::fill(Asave.begin(), Asave.end(), 0.0);
+      std::fill(Bsave.begin(), Bsave.end(), 0.0);
+      std::vector<double> I((size_t)lda * lda, 0.0);
+      for (int i = 0; i < w; ++i) {
+        Asave[i + (size_t)i * lda] = eigS[i];
+        Bsave[i + (size_t)i * lda] = 1.0;
+        I[i + (size_t)i * lda] = 1.0;
+      }
+      PWB_CUDA(cudaMemcpy(A, I.data(), I.size() * 8, cudaMemcpyHostToDevice));
+    }
+  }
+  PWB_CUDA(cudaMemcpy(s.X.p, X, (size_t)w * nt * esz, cudaMemcpyDeviceToDevice));
+  PWB_CUDA(cudaMemcpy(s.HX.p, AX, (size_t)w * nt * esz, cudaMemcpyDeviceToDevice));
+  s.eig = eigS;
+  s.res = res;
+  if (iters) *iters = std::min(iter, maxit);
+  return PW_OK;
+}
+
 }  // namespace pwb
 
 using namespace pwb;
@@ -607,6 +1053,7 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
   PWB_CHECK(ctx->prec == PW_F64, PW_EINVAL, "pw_scf_run takes the FP64 context (mixed mode builds an FP32 twin)");
   PWB_CHECK(!ctx->atom_z.empty(), PW_ENOTREADY, "atoms not set (pw_set_atoms)");
   PWB_CHECK(p->nocc > 0 && p->nextra >= 0 && p->ecut > 0, PW_EINVAL, "bad SCF parameters");
+  PWB_CHECK(p->solver >= PW_SOLVER_LOBPCG && p->solver <= PW_SOLVER_DAVIDSON, PW_EINVAL, "unknown eigensolver");
   PWB_CUDA(cudaSetDevice(ctx->device));
   const auto t_start = std::chrono::steady_clock::now();
   ScfState S;
@@ -747,6 +1194,17 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
         if ((rc = chebfsi_step(sv, dn, nb, p->cheby_degree, sv.eig[nb - 1], b_up, sv.eig[0]))) return rc;
         r->hpsi_bands += (long)nb * (p->cheby_degree + 1);
       }
+    } else if (p->solver == PW_SOLVER_PPCG) {
+      int li = 0;
+      if ((rc = ppcg(sv, dn, nb, p->ppcg_sbsize > 0 ? p->ppcg_sbsize : 1, p->eig_max_iter, p->eig_tol, it == 1, &li)))
+        return rc;
+      r->hpsi_bands += (long)nb * (li + 1);
+    } else if (p->solver == PW_SOLVER_DAVIDSON) {
+      int li = 0;
+      if ((rc = davidson(sv, dn, nb, p->davidson_maxdim >= 2 ? p->davidson_maxdim : 2, p->eig_max_iter, p->eig_tol,
+                         it == 1, &li)))
+        return rc;
+      r->hpsi_bands += (long)nb * (li + 1);
     } else {
       int li = 0;
       const double tolnow = p->eig_tol;
@@ -1006,6 +1464,10 @@ int pw_eigsolve(pw_ctx* ctx, int solver, void* X, int nb, int maxit, double tol,
   int it = 0;
   if (solver == PW_SOLVER_LOBPCG) {
     rc = lobpcg(sv, dn, nb, maxit, tol, true, &it);
+  } else if (solver == PW_SOLVER_PPCG) {
+    rc = ppcg(sv, dn, nb, degree > 0 ? degree : 1, maxit, tol, true, &it);
+  } else if (solver == PW_SOLVER_DAVIDSON) {
+    rc = davidson(sv, dn, nb, degree >= 2 ? degree : 2, maxit, tol, true, &it);
   } else {
     double up, lo;
     if ((rc = lanczos_upper(sv, 16, &up, &lo))) return rc;

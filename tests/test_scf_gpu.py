@@ -74,7 +74,7 @@ def test_cholqr_orthonormalises():
     assert float((X0 - (X0 @ X.T) @ X).abs().max() / X0.abs().max()) < 1e-10
 
 
-@pytest.mark.parametrize("solver", ["lobpcg", "chebfsi"])
+@pytest.mark.parametrize("solver", ["lobpcg", "chebfsi", "ppcg", "davidson"])
 def test_eigsolve_fixed_potential(solver):
     """Lowest 24 eigenpairs of H[V] against ARPACK on the oracle operator."""
     import torch
@@ -85,8 +85,12 @@ def test_eigsolve_fixed_potential(solver):
     c = _ctx(L, z, pos, nc, nf)
     c.set_vtot(T.vtot)
     X = torch.tensor(pw.random_orthonormal_psi(T.dm.ntot, 24, 9), device="cuda")
-    maxit = 200 if solver == "lobpcg" else 300
-    eig, res, it = c.eigsolve(X, solver=solver, maxit=maxit, tol=1e-9, degree=12)
+    # PPCG's cheap sub-block sweeps (no locking, no periodic Rayleigh-Ritz, as in
+    # the reference) need more iterations on the clustered spectrum
+    maxit = {"chebfsi": 300, "ppcg": 500}.get(solver, 200)
+    degree = {"chebfsi": 12, "ppcg": 4, "davidson": 3}.get(solver, 12)
+    tol = 1e-12 if solver == "davidson" else 1e-9     # Davidson converges on the Ritz-value change
+    eig, res, it = c.eigsolve(X, solver=solver, maxit=maxit, tol=tol, degree=degree)
     # the occupied states (the lowest 16 of the 24-wide block; the top of a
     # filtered block converges at the rate of the filter edge, which is why
     # the SCF carries extra states)
@@ -100,7 +104,8 @@ def _gold(which):
     return json.loads(p.read_text())
 
 
-@pytest.mark.parametrize("solver,mixed", [("lobpcg", False), ("chebfsi", False), ("chebfsi", True)])
+@pytest.mark.parametrize("solver,mixed", [("lobpcg", False), ("chebfsi", False), ("chebfsi", True), ("ppcg", False),
+                                          ("davidson", False), ("ppcg", True)])
 def test_scf_si8_small_matches_oracle(solver, mixed):
     g = _gold("small")
     L = np.array(g["length"])
