@@ -250,6 +250,21 @@ PW_API int pw_ctx_build_twin(pw_ctx* ctx);
  * doubles; rho_out: host, N_fine doubles (either may be NULL). */
 PW_API int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* eig_out, double* rho_out);
 
+/* k-point mode (complex bands).  pw_set_kpoint builds, for the Bloch vector
+ * k (Cartesian, bohr^-1), the kinetic 1/2 |k+G|^2 and Teter tables
+ * (KohnSham::CalculateEkin, complex version, src/SCF/hamiltonian_complex.cpp:
+ * 234-277) and the coarse projectors with the phase e^{i k.(r - R_a)}
+ * (src/SCF/periodtable.cpp:1104-1121; needs pw_set_atoms).  pw_hpsi_k applies
+ * H(k) (Spinor::AddMultSpinorFine, complex, src/SCF/spinor_complex.cpp:292-542)
+ * to nband complex bands: device arrays of interleaved (re, im) pairs of the
+ * context precision, leading dimensions ld / ldh in complex elements. */
+PW_API int pw_set_kpoint(pw_ctx* ctx, const double k[3]);
+PW_API int pw_hpsi_k(pw_ctx* ctx, const void* psi, int ld, void* hpsi, int ldh, int nband, int accumulate,
+                     void* stream);
+/* The kinetic and Teter tables of the current k on the full coarse grid (host,
+ * N_coarse doubles each; either may be NULL). */
+PW_API int pw_get_kpoint_tables(const pw_ctx* ctx, double* ekin_host, double* teter_host);
+
 /* Hybrid exact exchange (Gamma point, real bands).  Modes of the exchange
  * term inside pw_hpsi: off, the full pair-FFT operator
  * (Spinor::AddMultSpinorEXX, src/SCF/spinor.cpp:682-781) or the ACE operator

@@ -279,6 +279,7 @@ class NonlocalPP:
     idx: np.ndarray
     val: np.ndarray            # (npts, 4): VAL, DX, DY, DZ
     wgt: float
+    disp: np.ndarray = None    # (npts, 3): grid point - atom, Cartesian (vnlPos, periodtable.cpp:1096)
 
 
 def nonlocal_pp(atom: Atom, dm: Domain, sp: _hgh.HGHSpecies):
@@ -307,6 +308,7 @@ def nonlocal_pp(atom: Atom, dm: Domain, sp: _hgh.HGHSpecies):
     idx = (ii + jj * nG[0] + kk * nG[0] * nG[1]).astype(np.int64)
     rad = dist[sel]
     xx, yy, zz = car[sel, 0], car[sel, 1], car[sel, 2]
+    disp = car[sel].copy()
     out = []
     big = rad > MIN_RADIAL
     safe = np.where(big, rad, 1.0)
@@ -320,7 +322,7 @@ def nonlocal_pp(atom: Atom, dm: Domain, sp: _hgh.HGHSpecies):
             dv[:, 1] = np.where(big, coef * der * xx / safe, 0.0)
             dv[:, 2] = np.where(big, coef * der * yy / safe, 0.0)
             dv[:, 3] = np.where(big, coef * der * zz / safe, 0.0)
-            out.append(NonlocalPP(idx, dv, h))
+            out.append(NonlocalPP(idx, dv, h, disp))
         elif l == _hgh.TYPE_L1:
             coef = math.sqrt(3.0 / (4 * math.pi))
             dvr = der - val / safe
@@ -334,7 +336,7 @@ def nonlocal_pp(atom: Atom, dm: Domain, sp: _hgh.HGHSpecies):
                     if a == dirn:
                         t = t + coef * val / safe
                     dv[:, 1 + a] = np.where(big, t, coef * der if a == dirn else 0.0)
-                out.append(NonlocalPP(idx, dv, h))
+                out.append(NonlocalPP(idx, dv, h, disp))
         else:
             raise NotImplementedError("only L0/L1 channels (Si, Al HGH)")
     return out

@@ -94,6 +94,9 @@ SIGNATURES: dict[str, tuple] = {
     "pw_band_energy": (_i, [_vp, _vp, _i, _i, _dp, _dp]),
     "pw_scf_state": (_i, [_vp, _ip, _dp, _vp, _i, _vp]),
     "pw_exx_setup": (_i, [_vp, _d, _d, _i, _d]),
+    "pw_set_kpoint": (_i, [_vp, _dp]),
+    "pw_hpsi_k": (_i, [_vp, _vp, _i, _vp, _i, _i, _i, _vp]),
+    "pw_get_kpoint_tables": (_i, [_vp, _dp, _dp]),
     "pw_exx_get": (_i, [_vp, _dp, _dp]),
     "pw_exx_set_phi": (_i, [_vp, _vp, _i, _i, _dp]),
     "pw_exx_set_mode": (_i, [_vp, _i]),

@@ -428,6 +428,32 @@ def _ctx_exx_energy(self, psi, occ, num_spin: int = 2, use_ace: bool = False) ->
     return e.value
 
 
+def _ctx_set_kpoint(self, k):
+    """Bloch vector k (Cartesian, 1/bohr) for pw_hpsi_k."""
+    kk = np.ascontiguousarray(k, np.float64)
+    check(lib.pw_set_kpoint(self._h, kk.ctypes.data_as(_lib._dp)))
+
+
+def _ctx_hpsi_k(self, psi, out=None, accumulate: bool = False, stream=None):
+    """H(k) psi for complex bands psi (nband, N_coarse) complex128 / complex64 device tensor."""
+    import torch
+    if out is None:
+        out = torch.zeros_like(psi)
+    check(lib.pw_hpsi_k(self._h, _ptr(psi), self.ntot, _ptr(out), self.ntot, psi.shape[0], int(accumulate),
+                        _stream(stream)))
+    return out
+
+
+def _ctx_kpoint_tables(self):
+    ek = np.zeros(self.ntot)
+    te = np.zeros(self.ntot)
+    check(lib.pw_get_kpoint_tables(self._h, ek.ctypes.data_as(_lib._dp), te.ctypes.data_as(_lib._dp)))
+    return ek, te
+
+
+Context.set_kpoint = _ctx_set_kpoint
+Context.hpsi_k = _ctx_hpsi_k
+Context.kpoint_tables = _ctx_kpoint_tables
 Context.exx_setup = _ctx_exx_setup
 Context.exx_kernel = _ctx_exx_kernel
 Context.exx_set_phi = _ctx_exx_set_phi

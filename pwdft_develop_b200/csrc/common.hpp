@@ -121,6 +121,12 @@ struct pw_ctx {
   std::vector<long> h_ps_off;              // natom + 1 offsets into h_ps_idx / h_ps_val
   std::vector<int> h_ps_idx;               // per-atom pseudocharge support (fine-grid index)
   std::vector<double> h_ps_val;            // per-atom pseudocharge values
+  // k-point mode: complex bands at Bloch vector kvec (AddMultSpinorFine, complex)
+  bool have_k = false;
+  double kvec[3] = {0.0, 0.0, 0.0};
+  pwb::DevBuf ekin_k, teter_k;      // T [ntot]  1/2 |k+G|^2 and Teter on the full coarse spectrum
+  pwb::DevBuf qk;                   // complex T [nproj][ntot]  projectors with the Bloch phase
+  pwb::DevBuf qdk;                  // T [nproj]  gamma_l * vol / ntot
   // hybrid exchange (AddMultSpinorEXX / CalculateVexxACE)
   int exx_mode = 0;                 // PW_EXX_OFF / PW_EXX_FULL / PW_EXX_ACE
   double exx_frac = 0.0, exx_mu = 0.0, exx_div = 0.0;

@@ -56,7 +56,7 @@ __device__ __forceinline__ void load_tw(V* dst, const V* src, int n) {
 // ---------------------------------------------------------------------------
 // coarse plane forward: psi (two real bands) -> A[pair][z][ky][kx]
 // ---------------------------------------------------------------------------
-template <typename T, int N0, int N1>
+template <typename T, int N0, int N1, bool CPLX = false>
 __global__ void __launch_bounds__(PLANE_THREADS)
 k_cxy_fwd(const T* __restrict__ psi, int ld, int nband, int band0, VT<T>* __restrict__ A,
           const VT<T>* twx_g, const VT<T>* twy_g) {
@@ -70,12 +70,21 @@ k_cxy_fwd(const T* __restrict__ psi, int ld, int nband, int band0, VT<T>* __rest
   load_tw(twy, twy_g, N1);
   const int z = blockIdx.x, p = blockIdx.y;
   const long ntot_plane = (long)N0 * N1;
-  const int ba = band0 + 2 * p, bb = ba + 1;
-  const T* pa = psi + (long)ba * ld + z * ntot_plane;
-  const T* pb = (bb < nband) ? psi + (long)bb * ld + z * ntot_plane : nullptr;
-  for (int i = threadIdx.x; i < N0 * N1; i += blockDim.x) {
-    const int y = i / N0, x = i - y * N0;
-    pl[y * P0 + x] = mkc<V>(pa[i], pb ? pb[i] : (T)0);
+  if (CPLX) {
+    // one complex band per field (ld in complex elements)
+    const V* pc = reinterpret_cast<const V*>(psi) + (long)(band0 + p) * ld + z * ntot_plane;
+    for (int i = threadIdx.x; i < N0 * N1; i += blockDim.x) {
+      const int y = i / N0, x = i - y * N0;
+      pl[y * P0 + x] = pc[i];
+    }
+  } else {
+    const int ba = band0 + 2 * p, bb = ba + 1;
+    const T* pa = psi + (long)ba * ld + z * ntot_plane;
+    const T* pb = (bb < nband) ? psi + (long)bb * ld + z * ntot_plane : nullptr;
+    for (int i = threadIdx.x; i < N0 * N1; i += blockDim.x) {
+      const int y = i / N0, x = i - y * N0;
+      pl[y * P0 + x] = mkc<V>(pa[i], pb ? pb[i] : (T)0);
+    }
   }
   __syncthreads();
   smem_fft_cb<N0, -1, 1, P0>(pl, N1, twx);
@@ -149,7 +158,7 @@ template <typename T, int NZ, int NZF, int TX>
 __global__ void __launch_bounds__(PENCIL_THREADS, sizeof(T) == 4 ? 4 : 1)
 k_zpad(const VT<T>* __restrict__ A, VT<T>* __restrict__ K, VT<T>* __restrict__ B,
        const T* __restrict__ ekin, int n0, int n1, T inv_nc,
-       const VT<T>* twz_g, const VT<T>* twzf_g) {
+       const VT<T>* twz_g, const VT<T>* twzf_g, int cplx = 0) {
   using V = VT<T>;
   constexpr int PI = TX + 1;
   constexpr int PO = 2 * TX + 1;
@@ -194,7 +203,11 @@ k_zpad(const VT<T>* __restrict__ A, VT<T>* __restrict__ K, VT<T>* __restrict__ B
     const bool nyz = (kz == NZ / 2);
     const int fz = kz <= NZ / 2 ? kz : kz + (NZF - NZ);
     const bool split = splitrow || (c == m.nyx_i);
-    if (!split) {
+    if (cplx) {
+      // complex bands (idxFineGrid, fourier.cpp:291-311): a coarse Nyquist
+      // coefficient goes to the "+" fine position only; "-" slots stay zero
+      out[fz * PO + c] = v;
+    } else if (!split) {
       if (nyz) {
         out[(NZ / 2) * PO + c] = cscale(v, (T)0.5);
         out[(NZF - NZ / 2) * PO + c] = cscale(v, (T)0.5);
@@ -672,6 +685,36 @@ __global__ void k_scatter_beta(T* __restrict__ fields, long nf, const int* __res
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np; i += gridDim.x * blockDim.x) f[idx[io + i]] = (T)beta[bo + i];
 }
 
+// complex projector field conj(e^{i k.d}) beta for projector l0 + l into the
+// real / imaginary field pair (2l, 2l + 1); d = grid point - atom (Cartesian)
+template <typename T>
+__global__ void k_scatter_beta_k(T* __restrict__ fields, long nf, const int* __restrict__ idx,
+                                 const double* __restrict__ beta, const double* __restrict__ disp,
+                                 const long* __restrict__ pidx_off, const long* __restrict__ pbeta_off,
+                                 const int* __restrict__ pnpts, int l0, int nl, double kx, double ky, double kz) {
+  const int l = blockIdx.y;
+  if (l0 + l >= nl) return;
+  const long io = pidx_off[l0 + l], bo = pbeta_off[l0 + l];
+  const int np = pnpts[l0 + l];
+  T* fr = fields + (long)(2 * l) * nf;
+  T* fi = fr + nf;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np; i += gridDim.x * blockDim.x) {
+    const double* d = disp + 3 * (io + i);
+    double sn, cs;
+    sincos(kx * d[0] + ky * d[1] + kz * d[2], &sn, &cs);
+    const double b = beta[bo + i];
+    fr[idx[io + i]] = (T)(b * cs);
+    fi[idx[io + i]] = (T)(-b * sn);
+  }
+}
+
+// complex W[l][b] *= d[l] (d real)
+template <typename T>
+__global__ void k_scale_rows_c(VT<T>* __restrict__ W, const T* __restrict__ d, int nproj, int nb) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i < (long)nproj * nb) W[i] = cscale(W[i], d[i % nproj]);
+}
+
 // W[l][b] *= d[l]  (W column-major nproj x nb)
 template <typename T>
 __global__ void k_scale_rows(T* __restrict__ W, const T* __restrict__ d, int nproj, int nb) {
@@ -704,7 +747,7 @@ __global__ void k_nl_reduce(const VT<T>* __restrict__ Wp, VT<T>* __restrict__ W,
 template <typename T, int NZ, int NZF, int TX>
 __global__ void __launch_bounds__(PENCIL_THREADS, sizeof(T) == 4 ? 4 : 1)
 k_zfold(const VT<T>* __restrict__ C, const VT<T>* __restrict__ K, VT<T>* __restrict__ D, int n0, int n1,
-        const VT<T>* twz_g, const VT<T>* twzf_g, int deriv = 0, T gfac = 0) {
+        const VT<T>* twz_g, const VT<T>* twzf_g, int deriv = 0, T gfac = 0, int cplx = 0) {
   using V = VT<T>;
   constexpr int PI = 2 * TX + 1;
   constexpr int PA = TX + 1;
@@ -765,7 +808,10 @@ k_zfold(const VT<T>* __restrict__ C, const VT<T>* __restrict__ K, VT<T>* __restr
     const bool nyz = (kz == NZ / 2);
     const int fz = kz <= NZ / 2 ? kz : kz + (NZF - NZ);
     const bool split = splitrow || (c == m.nyx_i);
-    if (!split) {
+    if (cplx) {
+      // complex bands: the "+" fine position only (idxFineGrid pick)
+      v = cadd(v, in[fz * PI + c]);
+    } else if (!split) {
       if (nyz) v = cadd(v, cscale(cadd(in[(NZ / 2) * PI + c], in[(NZF - NZ / 2) * PI + c]), (T)0.5));
       else v = cadd(v, in[fz * PI + c]);
     } else {
@@ -822,7 +868,7 @@ k_zteter(VT<T>* __restrict__ A, const T* __restrict__ teter, int n0, int n1, T i
 // ---------------------------------------------------------------------------
 // coarse plane inverse: D -> hpsi (two real bands)
 // ---------------------------------------------------------------------------
-template <typename T, int N0, int N1>
+template <typename T, int N0, int N1, bool CPLX = false>
 __global__ void __launch_bounds__(PLANE_THREADS)
 k_cxy_inv(const VT<T>* __restrict__ D, T* __restrict__ out, int ldo, int nband, int band0, int accumulate,
           const VT<T>* twx_g, const VT<T>* twy_g) {
@@ -847,6 +893,15 @@ k_cxy_inv(const VT<T>* __restrict__ D, T* __restrict__ out, int ldo, int nband, 
   __syncthreads();
   smem_fft_cb<N0, +1, 1, P0>(pl, N1, twx);
   __syncthreads();
+  if (CPLX) {
+    V* oc = reinterpret_cast<V*>(out) + (long)(band0 + p) * ldo + z * ntot_plane;
+    for (int i = threadIdx.x; i < N0 * N1; i += blockDim.x) {
+      const int y = i / N0, x = i - y * N0;
+      const V v = pl[y * P0 + x];
+      oc[i] = accumulate ? cadd(oc[i], v) : v;
+    }
+    return;
+  }
   const int ba = band0 + 2 * p, bb = ba + 1;
   T* oa = out + (long)ba * ldo + z * ntot_plane;
   T* ob = (bb < nband) ? out + (long)bb * ldo + z * ntot_plane : nullptr;
@@ -1178,6 +1233,116 @@ struct Plan {
     return PW_OK;
   }
 
+  // complex bands at Bloch vector k (Spinor::AddMultSpinorFine, complex
+  // version, src/SCF/spinor_complex.cpp:292-542): one band per complex field,
+  // idxFineGrid placement, kinetic 1/2 |k+G|^2, projectors with the Bloch phase
+  static int hpsi_batch_k(pw_ctx* c, const V* psi, int ld, V* out, int ldo, int band0, int nb, int accumulate,
+                          cudaStream_t st) {
+    int rc = set_attrs();
+    if (rc) return rc;
+    static bool attr = false;
+    if (!attr) {
+      PWB_CUDA(cudaFuncSetAttribute(k_cxy_fwd<T, N0, N1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_cxy()));
+      PWB_CUDA(cudaFuncSetAttribute(k_cxy_inv<T, N0, N1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_cxy()));
+      attr = true;
+    }
+    V* AD = reinterpret_cast<V*>(c->s_ad.p);
+    V* K = reinterpret_cast<V*>(c->s_k.p);
+    V* BC = reinterpret_cast<V*>(c->s_bc.p);
+    const T inv_nc = (T)(1.0 / (double)c->ntot);
+    const T inv_nf = (T)(1.0 / (double)c->ntotf);
+    const int ntx = (N0 + TX - 1) / TX;
+    const T* pr = reinterpret_cast<const T*>(psi);
+    { Launch L_(c, st, KK_CXY_FWD);
+    k_cxy_fwd<T, N0, N1, true><<<dim3(N2, nb), PLANE_THREADS, sm_cxy(), st>>>(pr, ld, 0, band0, AD, tw(c, 0), tw(c, 1)); }
+    { Launch L_(c, st, KK_ZPAD);
+    k_zpad<T, N2, NF2, TX><<<dim3(N1, ntx, nb), PENCIL_THREADS, sm_zpad(), st>>>(
+        AD, K, BC, reinterpret_cast<const T*>(c->ekin_k.p), N0, N1, inv_nc, tw(c, 2), tw(c, 5), 1); }
+    { Launch L_(c, st, KK_FPLANE_APPLY);
+    k_floc<T, NF0, NF1, 0><<<dim3(NF2, nb), FLOC_THREADS, sm_floc(), st>>>(
+        BC, reinterpret_cast<const T*>(c->vtot.p), nullptr, 0, inv_nf, tw(c, 3), tw(c, 4)); }
+    { Launch L_(c, st, KK_ZFOLD);
+    k_zfold<T, N2, NF2, TXF><<<dim3(N1, (N0 + TXF - 1) / TXF, nb), PENCIL_THREADS, sm_zfold(), st>>>(
+        BC, K, AD, N0, N1, tw(c, 2), tw(c, 5), 0, (T)0, 1); }
+    { Launch L_(c, st, KK_CXY_INV);
+    k_cxy_inv<T, N0, N1, true><<<dim3(N2, nb), PLANE_THREADS, sm_cxy(), st>>>(AD, reinterpret_cast<T*>(out), ldo, 0,
+                                                                              band0, accumulate, tw(c, 0), tw(c, 1)); }
+    PWB_CUDA(cudaGetLastError());
+    if (c->nproj == 0 || !c->qk.p) return PW_OK;
+    // V_nl psi = Q diag(d) Q^H psi with the complex coarse projector matrix Q of this k
+    cublasHandle_t h = (cublasHandle_t)c->blas;
+    if (cublasSetStream(h, st) != CUBLAS_STATUS_SUCCESS) { set_error("cublasSetStream failed"); return PW_ECUDA; }
+    const int np = c->nproj, nt = (int)c->ntot;
+    if ((rc = c->s_wq.alloc((size_t)np * nb * sizeof(V)))) return rc;
+    V* W = reinterpret_cast<V*>(c->s_wq.p);
+    const V* Q = reinterpret_cast<const V*>(c->qk.p);
+    const V* x = psi + (long)band0 * ld;
+    V* y = out + (long)band0 * ldo;
+    cublasStatus_t r;
+    { Launch L_(c, st, KK_LIBGEMM);
+    if constexpr (std::is_same<T, double>::value) {
+      const cuDoubleComplex one = make_cuDoubleComplex(1, 0), zero = make_cuDoubleComplex(0, 0);
+      r = cublasZgemm(h, CUBLAS_OP_C, CUBLAS_OP_N, np, nb, nt, &one, (const cuDoubleComplex*)Q, nt,
+                      (const cuDoubleComplex*)x, ld, &zero, (cuDoubleComplex*)W, np);
+    } else {
+      const cuComplex one = make_cuComplex(1, 0), zero = make_cuComplex(0, 0);
+      r = cublasCgemm(h, CUBLAS_OP_C, CUBLAS_OP_N, np, nb, nt, &one, (const cuComplex*)Q, nt, (const cuComplex*)x, ld,
+                      &zero, (cuComplex*)W, np);
+    } }
+    if (r != CUBLAS_STATUS_SUCCESS) { set_error("projector GEMM (Q^H psi) failed"); return PW_ECUDA; }
+    { Launch L_(c, st, KK_MISC);
+    k_scale_rows_c<T><<<(unsigned)(((long)np * nb + 255) / 256), 256, 0, st>>>(W, reinterpret_cast<const T*>(c->qdk.p),
+                                                                                np, nb); }
+    { Launch L_(c, st, KK_LIBGEMM);
+    if constexpr (std::is_same<T, double>::value) {
+      const cuDoubleComplex one = make_cuDoubleComplex(1, 0);
+      r = cublasZgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, nt, nb, np, &one, (const cuDoubleComplex*)Q, nt,
+                      (const cuDoubleComplex*)W, np, &one, (cuDoubleComplex*)y, ldo);
+    } else {
+      const cuComplex one = make_cuComplex(1, 0);
+      r = cublasCgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, nt, nb, np, &one, (const cuComplex*)Q, nt, (const cuComplex*)W, np,
+                      &one, (cuComplex*)y, ldo);
+    } }
+    if (r != CUBLAS_STATUS_SUCCESS) { set_error("projector GEMM (Q W) failed"); return PW_ECUDA; }
+    PWB_CUDA(cudaGetLastError());
+    return PW_OK;
+  }
+
+  // complex coarse projectors at Bloch vector k: q_l = T(conj(e^{i k.d}) beta_l),
+  // one projector per complex field, into Qout (complex, leading dimension ntot)
+  static int build_q_k(pw_ctx* c, const int* d_idx, const double* d_beta, const double* d_disp, const long* d_pio,
+                       const long* d_pbo, const int* d_pnp, int nproj, const double kv[3], V* Qout, cudaStream_t st) {
+    int rc = set_attrs();
+    if (rc) return rc;
+    static bool attr = false;
+    if (!attr) {
+      PWB_CUDA(cudaFuncSetAttribute(k_cxy_inv<T, N0, N1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_cxy()));
+      attr = true;
+    }
+    const int cap = c->pair_cap;                 // complex fields per pass
+    const long nf = c->ntotf;
+    DevBuf fields;
+    if ((rc = fields.alloc((size_t)2 * cap * nf * sizeof(T)))) return rc;
+    V* AD = reinterpret_cast<V*>(c->s_ad.p);
+    V* BC = reinterpret_cast<V*>(c->s_bc.p);
+    const T inv_nf = (T)(1.0 / (double)c->ntotf);
+    for (int l0 = 0; l0 < nproj; l0 += cap) {
+      const int nl = std::min(cap, nproj - l0);
+      PWB_CUDA(cudaMemsetAsync(fields.p, 0, (size_t)2 * nl * nf * sizeof(T), st));
+      k_scatter_beta_k<T><<<dim3(64, nl), 256, 0, st>>>(reinterpret_cast<T*>(fields.p), nf, d_idx, d_beta, d_disp, d_pio,
+                                                         d_pbo, d_pnp, l0, nproj, kv[0], kv[1], kv[2]);
+      k_floc<T, NF0, NF1, 1><<<dim3(NF2, nl), FLOC_THREADS, sm_floc(), st>>>(
+          BC, nullptr, reinterpret_cast<const T*>(fields.p), nf, inv_nf, tw(c, 3), tw(c, 4));
+      k_zfold<T, N2, NF2, TXF><<<dim3(N1, (N0 + TXF - 1) / TXF, nl), PENCIL_THREADS, sm_zfold(), st>>>(
+          BC, nullptr, AD, N0, N1, tw(c, 2), tw(c, 5), 0, (T)0, 1);
+      k_cxy_inv<T, N0, N1, true><<<dim3(N2, nl), PLANE_THREADS, sm_cxy(), st>>>(
+          AD, reinterpret_cast<T*>(Qout), (int)c->ntot, 0, l0, 0, tw(c, 0), tw(c, 1));
+      PWB_CUDA(cudaGetLastError());
+    }
+    PWB_CUDA(cudaStreamSynchronize(st));
+    return PW_OK;
+  }
+
   // Build q_l = T(beta_l) for all projectors with the fine->coarse half of
   // the pipeline, two projectors per complex field.
   static int build_q(pw_ctx* c, const int* d_idx, const double* d_beta, const long* d_pio, const long* d_pbo,
@@ -1300,6 +1465,21 @@ static int ace_thunk(pw_ctx* c, const void* psi, int ld, int nb, void* out, int 
   return Plan<T, N0, N1, N2>::dense_apply(c, ds, (const T*)psi, ld, (T*)out, ldo, nb, st);
 }
 
+using HpsiKFn = int (*)(pw_ctx*, const void*, int, void*, int, int, int, int, cudaStream_t);
+template <typename T, int N0, int N1, int N2>
+static int hpsik_thunk(pw_ctx* c, const void* psi, int ld, void* out, int ldo, int band0, int nb, int acc,
+                       cudaStream_t st) {
+  using V = VT<T>;
+  return Plan<T, N0, N1, N2>::hpsi_batch_k(c, (const V*)psi, ld, (V*)out, ldo, band0, nb, acc, st);
+}
+using BuildQKFn = int (*)(pw_ctx*, const int*, const double*, const double*, const long*, const long*, const int*, int,
+                          const double*, void*, cudaStream_t);
+template <typename T, int N0, int N1, int N2>
+static int buildqk_thunk(pw_ctx* c, const int* a, const double* b, const double* d, const long* e, const long* f,
+                         const int* g, int n, const double* kv, void* out, cudaStream_t st) {
+  return Plan<T, N0, N1, N2>::build_q_k(c, a, b, d, e, f, g, n, kv, (VT<T>*)out, st);
+}
+
 struct GridEntry {
   int n0, n1, n2;
   HpsiFn hpsi[2];
@@ -1310,6 +1490,8 @@ struct GridEntry {
   TeterScratchFn teter_scratch[2];
   ExxFn exx[2];
   ExxFn ace[2];
+  HpsiKFn hpsik[2];
+  BuildQKFn bqk[2];
 };
 
 #define PWB_GRID(a, b, c)                                                                          \
@@ -1320,7 +1502,9 @@ struct GridEntry {
    {dens_thunk<double, a, b, c>, dens_thunk<float, a, b, c>},                                      \
    {teter_scratch_thunk<double, a, b, c>, teter_scratch_thunk<float, a, b, c>},                    \
    {exx_thunk<double, a, b, c>, exx_thunk<float, a, b, c>},                                        \
-   {ace_thunk<double, a, b, c>, ace_thunk<float, a, b, c>}},
+   {ace_thunk<double, a, b, c>, ace_thunk<float, a, b, c>},                                        \
+   {hpsik_thunk<double, a, b, c>, hpsik_thunk<float, a, b, c>},                                    \
+   {buildqk_thunk<double, a, b, c>, buildqk_thunk<float, a, b, c>}},
 
 static const GridEntry kGrids[] = {
 #include "grids.inc"
@@ -1363,6 +1547,19 @@ int run_exx(pw_ctx* c, const void* psi, int ld, int nb, void* out, int ldo, int 
   const GridEntry* g = find_grid(c->n);
   if (!g) { set_error("grid not built into this library"); return PW_EUNSUPPORTED; }
   return g->exx[c->prec == PW_F32 ? 1 : 0](c, psi, ld, nb, out, ldo, acc, st);
+}
+
+int run_hpsi_k(pw_ctx* c, const void* psi, int ld, void* out, int ldo, int band0, int nb, int acc, cudaStream_t st) {
+  const GridEntry* g = find_grid(c->n);
+  if (!g) { set_error("grid not built into this library"); return PW_EUNSUPPORTED; }
+  return g->hpsik[c->prec == PW_F32 ? 1 : 0](c, psi, ld, out, ldo, band0, nb, acc, st);
+}
+
+int run_build_q_k(pw_ctx* c, const int* d_idx, const double* d_beta, const double* d_disp, const long* d_pio,
+                  const long* d_pbo, const int* d_pnp, int nproj, const double* kv, void* out, cudaStream_t st) {
+  const GridEntry* g = find_grid(c->n);
+  if (!g) { set_error("grid not built into this library"); return PW_EUNSUPPORTED; }
+  return g->bqk[c->prec == PW_F32 ? 1 : 0](c, d_idx, d_beta, d_disp, d_pio, d_pbo, d_pnp, nproj, kv, out, st);
 }
 
 int run_ace(pw_ctx* c, const void* psi, int ld, int nb, void* out, int ldo, cudaStream_t st) {

@@ -1,0 +1,122 @@
+// k-point (complex band) Hamiltonian: KohnSham::MultSpinor for complex
+// wavefunctions, Spinor::AddMultSpinorFine complex version
+// (src/SCF/spinor_complex.cpp:292-542, real-space branch).  The tables follow
+// KohnSham::CalculateEkin, complex version (src/SCF/hamiltonian_complex.cpp:
+// 234-277: ekin = 1/2 |k+G|^2, Teter of |k+G|^2 on the full coarse grid) and
+// the projector Bloch phase e^{i k.(r - R_a)} of PeriodTable::CalculateNonlocalPP
+// (src/SCF/periodtable.cpp:1104-1121).
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "common.hpp"
+
+namespace pwb {
+
+int run_hpsi_k(pw_ctx* c, const void* psi, int ld, void* out, int ldo, int band0, int nb, int acc, cudaStream_t st);
+int run_build_q_k(pw_ctx* c, const int* d_idx, const double* d_beta, const double* d_disp, const long* d_pio,
+                  const long* d_pbo, const int* d_pnp, int nproj, const double* kv, void* out, cudaStream_t st);
+int ensure_scratch(pw_ctx* c, int npair);
+int upload_real(pw_ctx* c, DevBuf& dst, const double* src, size_t n);
+
+template <typename X> static int upload(DevBuf& b, const std::vector<X>& h) {
+  int rc = b.alloc(std::max<size_t>(h.size(), 1) * sizeof(X));
+  if (rc) return rc;
+  if (!h.empty()) PWB_CUDA(cudaMemcpy(b.p, h.data(), h.size() * sizeof(X), cudaMemcpyHostToDevice));
+  return PW_OK;
+}
+
+}  // namespace pwb
+
+using namespace pwb;
+
+extern "C" {
+
+int pw_set_kpoint(pw_ctx* ctx, const double k[3]) {
+  PWB_CHECK(ctx && k, PW_EINVAL, "null argument");
+  PWB_CUDA(cudaSetDevice(ctx->device));
+  const int n0 = ctx->n[0], n1 = ctx->n[1], n2 = ctx->n[2];
+  const long nt = ctx->ntot;
+  std::vector<double> ek(nt), te(nt);
+  for (int z = 0; z < n2; ++z)
+    for (int y = 0; y < n1; ++y)
+      for (int x = 0; x < n0; ++x) {
+        const double m0 = x <= n0 / 2 ? x : x - n0, m1 = y <= n1 / 2 ? y : y - n1, m2 = z <= n2 / 2 ? z : z - n2;
+        const double g0 = k[0] + 2 * M_PI / ctx->L[0] * m0, g1 = k[1] + 2 * M_PI / ctx->L[1] * m1,
+                     g2 = k[2] + 2 * M_PI / ctx->L[2] * m2;
+        const long i = x + (long)n0 * (y + (long)n1 * z);
+        ek[i] = 0.5 * (g0 * g0 + g1 * g1 + g2 * g2);
+        const double a = 2.0 * ek[i];
+        const double b = 27.0 + a * (18.0 + a * (12.0 + a * 8.0));
+        te[i] = b / (b + 16.0 * a * a * a * a);
+      }
+  int rc;
+  if ((rc = upload_real(ctx, ctx->ekin_k, ek.data(), nt)) || (rc = upload_real(ctx, ctx->teter_k, te.data(), nt)))
+    return rc;
+  const int np = (int)ctx->h_pnp.size();
+  ctx->qk.release();
+  if (np > 0) {
+    size_t tot = 0;
+    for (const auto& a : ctx->h_nl) tot += a.val.size();
+    PWB_CHECK(tot == (size_t)np && !ctx->h_nl.empty(), PW_ENOTREADY,
+              "k-point projectors need the sets of pw_set_atoms (grid-point displacements)");
+    std::vector<double> disp;
+    disp.reserve(3 * ctx->h_nl_idx.size());
+    for (const auto& a : ctx->h_nl) disp.insert(disp.end(), a.disp.begin(), a.disp.end());
+    PWB_CHECK(disp.size() == 3 * ctx->h_nl_idx.size(), PW_EINVAL, "projector sets changed since pw_set_atoms");
+    DevBuf d_idx, d_beta, d_disp, d_pio, d_pbo, d_pnp;
+    if ((rc = upload(d_idx, ctx->h_nl_idx)) || (rc = upload(d_beta, ctx->h_nl_beta)) || (rc = upload(d_disp, disp)) ||
+        (rc = upload(d_pio, ctx->h_pio)) || (rc = upload(d_pbo, ctx->h_pbo)) || (rc = upload(d_pnp, ctx->h_pnp)))
+      return rc;
+    if ((rc = ctx->qk.alloc((size_t)np * nt * 2 * ctx->esz))) return rc;
+    if ((rc = ensure_scratch(ctx, std::max(ctx->pair_cap, 1)))) return rc;
+    if ((rc = run_build_q_k(ctx, (const int*)d_idx.p, (const double*)d_beta.p, (const double*)d_disp.p,
+                            (const long*)d_pio.p, (const long*)d_pbo.p, (const int*)d_pnp.p, np, k, ctx->qk.p,
+                            nullptr)))
+      return rc;
+    std::vector<double> qd(np);
+    for (int l = 0; l < np; ++l) qd[l] = ctx->h_pgamma[l] * ctx->vol / (double)nt;
+    if ((rc = upload_real(ctx, ctx->qdk, qd.data(), np))) return rc;
+    ctx->launches += 5 * ((np + std::max(ctx->pair_cap, 1) - 1) / std::max(ctx->pair_cap, 1));
+  }
+  PWB_CUDA(cudaDeviceSynchronize());
+  for (int d = 0; d < 3; ++d) ctx->kvec[d] = k[d];
+  ctx->have_k = true;
+  return PW_OK;
+}
+
+int pw_hpsi_k(pw_ctx* ctx, const void* psi, int ld, void* hpsi, int ldh, int nband, int accumulate, void* stream) {
+  PWB_CHECK(ctx && (nband == 0 || (psi && hpsi)), PW_EINVAL, "null argument");
+  PWB_CHECK(nband >= 0 && ld >= ctx->ntot && ldh >= ctx->ntot, PW_EINVAL, "Domain size does not match.");
+  PWB_CHECK(ctx->have_vtot, PW_ENOTREADY, "local potential not set (pw_set_vtot)");
+  PWB_CHECK(ctx->have_k, PW_ENOTREADY, "Bloch vector not set (pw_set_kpoint)");
+  PWB_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t st = (cudaStream_t)stream;
+  const int cap = std::max(ctx->pair_cap, 1);
+  for (int b0 = 0; b0 < nband; b0 += cap) {
+    const int nb = std::min(cap, nband - b0);
+    int rc = run_hpsi_k(ctx, psi, ld, hpsi, ldh, b0, nb, accumulate, st);
+    if (rc) return rc;
+  }
+  return PW_OK;
+}
+
+int pw_get_kpoint_tables(const pw_ctx* ctx, double* ekin_host, double* teter_host) {
+  PWB_CHECK(ctx && ctx->have_k, PW_ENOTREADY, "Bloch vector not set (pw_set_kpoint)");
+  const long nt = ctx->ntot;
+  for (int which = 0; which < 2; ++which) {
+    double* dst = which == 0 ? ekin_host : teter_host;
+    if (!dst) continue;
+    const pwb::DevBuf& b = which == 0 ? ctx->ekin_k : ctx->teter_k;
+    if (ctx->prec == PW_F64) {
+      PWB_CUDA(cudaMemcpy(dst, b.p, nt * 8, cudaMemcpyDeviceToHost));
+    } else {
+      std::vector<float> h(nt);
+      PWB_CUDA(cudaMemcpy(h.data(), b.p, nt * 4, cudaMemcpyDeviceToHost));
+      for (long i = 0; i < nt; ++i) dst[i] = h[i];
+    }
+  }
+  return PW_OK;
+}
+
+}  // extern "C"

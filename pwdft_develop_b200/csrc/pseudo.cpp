@@ -257,6 +257,7 @@ static inline double cround(double x) { return x >= 0 ? std::floor(x + 0.5) : -s
 
 int nonlocal_pp(const Species& sp, const double pos[3], const double L[3], const int nG[3], AtomNL& out) {
   out.idx.clear();
+  out.disp.clear();
   out.val.clear();
   out.wgt.clear();
   const double R = sp.wavcut;
@@ -284,6 +285,9 @@ int nonlocal_pp(const Species& sp, const double pos[3], const double L[3], const
         const double dist = std::sqrt(gx * gx + gy * gy + gz * gz);
         if (dist < R) {
           out.idx.push_back(ii + jj * nG[0] + kk * nG[0] * nG[1]);
+          out.disp.push_back(gx);
+          out.disp.push_back(gy);
+          out.disp.push_back(gz);
           rad.push_back(dist);
           xx.push_back(gx);
           yy.push_back(gy);

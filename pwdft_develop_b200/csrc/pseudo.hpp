@@ -32,6 +32,7 @@ const Species* species(int znuc);
 struct AtomNL {
   int npts = 0;
   std::vector<int> idx;
+  std::vector<double> disp;   // 3 per point: Cartesian grid point - atom (unwrapped), for the Bloch phase
   std::vector<std::vector<double>> val;
   std::vector<double> wgt;
 };

@@ -271,3 +271,46 @@ def test_exx_operator_symmetric_and_ace_exact_on_span():
     assert np.linalg.eigvalsh(-0.5 * (M + M.T)).min() > 0      # V_x negative definite on span
     xi = exx.ace_build(dm, psi, phi, k, 0.25, occ)
     assert np.abs(exx.ace_apply(xi, psi) - Vx).max() <= 1e-11 * np.abs(Vx).max()
+
+
+def test_kpoint_hamiltonian_hermitian():
+    """H(k) of the complex restatement is Hermitian (<x, H y> = <H x, y>) and its
+    kinetic / Teter tables are positive."""
+    from oracle import kpoints
+    L, z, pos = pw.make_crystal("Si", (1, 1, 1), 10.26, 0.02, 5)
+    T, _ = pw.build_tables(L, z, pos, (8, 8, 8), (16, 16, 16), seed_v=2)
+    k = np.array([0.11, -0.05, 0.23])
+    x = kpoints.random_complex_psi(T.dm.ntot, 3, 1)
+    y = kpoints.random_complex_psi(T.dm.ntot, 3, 2)
+    hx = kpoints.mult_spinor_k(T, k, x)
+    hy = kpoints.mult_spinor_k(T, k, y)
+    lhs = np.conj(x) @ hy.T
+    rhs = np.conj(hx) @ y.T
+    assert np.abs(lhs - rhs).max() <= 1e-12 * np.abs(lhs).max()
+    ek, te = kpoints.ekin_teter_k(T.dm, k)
+    assert ek.min() > 0 and np.all((te > 0) & (te <= 1))
+
+
+def test_kpoint_gamma_matches_real_hamiltonian_without_nyquist():
+    """At k = 0, on real bands with no Nyquist content (where the R2C and the
+    complex placements agree), the complex H equals the Gamma-point real H."""
+    from oracle import kpoints
+    L, z, pos = pw.make_crystal("Si", (1, 1, 1), 10.26, 0.02, 5)
+    T, _ = pw.build_tables(L, z, pos, (8, 8, 8), (16, 16, 16), seed_v=2)
+    dm = T.dm
+    psi = pw.random_orthonormal_psi(dm.ntot, 3, 4)
+    X = np.fft.fftn(psi.reshape(3, 8, 8, 8), axes=(1, 2, 3))
+    X[:, 4, :, :] = 0
+    X[:, :, 4, :] = 0
+    X[:, :, :, 4] = 0
+    psi = np.fft.ifftn(X, axes=(1, 2, 3)).real.reshape(3, -1)
+    hr = pw.mult_spinor(T, psi)
+    hc = kpoints.mult_spinor_k(T, np.zeros(3), psi.astype(complex))
+    # outputs agree away from the Nyquist components, which the two paths treat differently
+    Fr = np.fft.fftn(hr.reshape(3, 8, 8, 8), axes=(1, 2, 3))
+    Fc = np.fft.fftn(hc.reshape(3, 8, 8, 8), axes=(1, 2, 3))
+    for F in (Fr, Fc):
+        F[:, 4, :, :] = 0
+        F[:, :, 4, :] = 0
+        F[:, :, :, 4] = 0
+    assert np.abs(Fr - Fc).max() <= 1e-10 * np.abs(Fr).max()
