@@ -261,6 +261,13 @@ PW_API int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, dou
 PW_API int pw_set_kpoint(pw_ctx* ctx, const double k[3]);
 PW_API int pw_hpsi_k(pw_ctx* ctx, const void* psi, int ld, void* hpsi, int ldh, int nband, int accumulate,
                      void* stream);
+/* A batch of nk Bloch vectors (kpts: host, nk x 3) kept resident (tables and
+ * projectors per k); pw_hpsi_kbatch applies H(k_i) to nband complex bands of
+ * every k-point in one pass: psi / hpsi hold nk * nband columns, k-point
+ * major (column i * nband + b is band b of k-point i). */
+PW_API int pw_set_kpoints(pw_ctx* ctx, int nk, const double* kpts);
+PW_API int pw_hpsi_kbatch(pw_ctx* ctx, const void* psi, int ld, void* hpsi, int ldh, int nband, int accumulate,
+                          void* stream);
 /* The kinetic and Teter tables of the current k on the full coarse grid (host,
  * N_coarse doubles each; either may be NULL). */
 PW_API int pw_get_kpoint_tables(const pw_ctx* ctx, double* ekin_host, double* teter_host);

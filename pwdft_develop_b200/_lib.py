@@ -97,6 +97,8 @@ SIGNATURES: dict[str, tuple] = {
     "pw_set_kpoint": (_i, [_vp, _dp]),
     "pw_hpsi_k": (_i, [_vp, _vp, _i, _vp, _i, _i, _i, _vp]),
     "pw_get_kpoint_tables": (_i, [_vp, _dp, _dp]),
+    "pw_set_kpoints": (_i, [_vp, _i, _dp]),
+    "pw_hpsi_kbatch": (_i, [_vp, _vp, _i, _vp, _i, _i, _i, _vp]),
     "pw_exx_get": (_i, [_vp, _dp, _dp]),
     "pw_exx_set_phi": (_i, [_vp, _vp, _i, _i, _dp]),
     "pw_exx_set_mode": (_i, [_vp, _i]),

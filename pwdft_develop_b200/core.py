@@ -451,6 +451,26 @@ def _ctx_kpoint_tables(self):
     return ek, te
 
 
+def _ctx_set_kpoints(self, kpts):
+    """A resident batch of Bloch vectors (nk x 3, Cartesian 1/bohr) for hpsi_kbatch."""
+    kk = np.ascontiguousarray(kpts, np.float64).reshape(-1, 3)
+    check(lib.pw_set_kpoints(self._h, kk.shape[0], kk.ctypes.data_as(_lib._dp)))
+    self._nkb = kk.shape[0]
+
+
+def _ctx_hpsi_kbatch(self, psi, out=None, accumulate: bool = False, stream=None):
+    """H(k_i) psi_i for psi of shape (nk, nband, N_coarse) complex on the device."""
+    import torch
+    if out is None:
+        out = torch.zeros_like(psi)
+    nb = psi.shape[1]
+    check(lib.pw_hpsi_kbatch(self._h, _ptr(psi), self.ntot, _ptr(out), self.ntot, nb, int(accumulate),
+                             _stream(stream)))
+    return out
+
+
+Context.set_kpoints = _ctx_set_kpoints
+Context.hpsi_kbatch = _ctx_hpsi_kbatch
 Context.set_kpoint = _ctx_set_kpoint
 Context.hpsi_k = _ctx_hpsi_k
 Context.kpoint_tables = _ctx_kpoint_tables

@@ -127,6 +127,9 @@ struct pw_ctx {
   pwb::DevBuf ekin_k, teter_k;      // T [ntot]  1/2 |k+G|^2 and Teter on the full coarse spectrum
   pwb::DevBuf qk;                   // complex T [nproj][ntot]  projectors with the Bloch phase
   pwb::DevBuf qdk;                  // T [nproj]  gamma_l * vol / ntot
+  int nkb = 0;                      // k-point batch (pw_set_kpoints)
+  std::vector<double> kb_k;         // nkb x 3
+  pwb::DevBuf ekin_kb, qkb;         // T [nkb][ntot], complex T [nkb][nproj][ntot]
   // hybrid exchange (AddMultSpinorEXX / CalculateVexxACE)
   int exx_mode = 0;                 // PW_EXX_OFF / PW_EXX_FULL / PW_EXX_ACE
   double exx_frac = 0.0, exx_mu = 0.0, exx_div = 0.0;

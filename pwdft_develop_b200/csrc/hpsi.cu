@@ -158,7 +158,7 @@ template <typename T, int NZ, int NZF, int TX>
 __global__ void __launch_bounds__(PENCIL_THREADS, sizeof(T) == 4 ? 4 : 1)
 k_zpad(const VT<T>* __restrict__ A, VT<T>* __restrict__ K, VT<T>* __restrict__ B,
        const T* __restrict__ ekin, int n0, int n1, T inv_nc,
-       const VT<T>* twz_g, const VT<T>* twzf_g, int cplx = 0) {
+       const VT<T>* twz_g, const VT<T>* twzf_g, int cplx = 0, int kf0 = 0, int fpk = 1 << 30, long kstride = 0) {
   using V = VT<T>;
   constexpr int PI = TX + 1;
   constexpr int PO = 2 * TX + 1;
@@ -192,7 +192,8 @@ k_zpad(const VT<T>* __restrict__ A, VT<T>* __restrict__ K, VT<T>* __restrict__ B
   smem_fft_cb<NZ, -1, PI, 1>(in, tw, twz);
   __syncthreads();
   V* Kp = K ? K + (long)p * NZ * nplane + (long)ky * n0 + kx0 : nullptr;
-  const T* ek = ekin + (long)ky * n0 + kx0;
+  // k-point batches: field kf0 + p belongs to k-point (kf0 + p) / fpk
+  const T* ek = ekin + (long)((kf0 + p) / fpk) * kstride + (long)ky * n0 + kx0;
   const bool splitrow = m.nyy;
   for (int i = threadIdx.x; i < NZ * TX; i += blockDim.x) {
     const int kz = i / TX, c = i - kz * TX;
@@ -1237,7 +1238,7 @@ struct Plan {
   // version, src/SCF/spinor_complex.cpp:292-542): one band per complex field,
   // idxFineGrid placement, kinetic 1/2 |k+G|^2, projectors with the Bloch phase
   static int hpsi_batch_k(pw_ctx* c, const V* psi, int ld, V* out, int ldo, int band0, int nb, int accumulate,
-                          cudaStream_t st) {
+                          cudaStream_t st, int fpk = 1 << 30, const T* ekin_all = nullptr, const V* qk_all = nullptr) {
     int rc = set_attrs();
     if (rc) return rc;
     static bool attr = false;
@@ -1257,7 +1258,8 @@ struct Plan {
     k_cxy_fwd<T, N0, N1, true><<<dim3(N2, nb), PLANE_THREADS, sm_cxy(), st>>>(pr, ld, 0, band0, AD, tw(c, 0), tw(c, 1)); }
     { Launch L_(c, st, KK_ZPAD);
     k_zpad<T, N2, NF2, TX><<<dim3(N1, ntx, nb), PENCIL_THREADS, sm_zpad(), st>>>(
-        AD, K, BC, reinterpret_cast<const T*>(c->ekin_k.p), N0, N1, inv_nc, tw(c, 2), tw(c, 5), 1); }
+        AD, K, BC, ekin_all ? ekin_all : reinterpret_cast<const T*>(c->ekin_k.p), N0, N1, inv_nc, tw(c, 2), tw(c, 5),
+        1, band0, fpk, ekin_all ? c->ntot : 0); }
     { Launch L_(c, st, KK_FPLANE_APPLY);
     k_floc<T, NF0, NF1, 0><<<dim3(NF2, nb), FLOC_THREADS, sm_floc(), st>>>(
         BC, reinterpret_cast<const T*>(c->vtot.p), nullptr, 0, inv_nf, tw(c, 3), tw(c, 4)); }
@@ -1268,16 +1270,26 @@ struct Plan {
     k_cxy_inv<T, N0, N1, true><<<dim3(N2, nb), PLANE_THREADS, sm_cxy(), st>>>(AD, reinterpret_cast<T*>(out), ldo, 0,
                                                                               band0, accumulate, tw(c, 0), tw(c, 1)); }
     PWB_CUDA(cudaGetLastError());
-    if (c->nproj == 0 || !c->qk.p) return PW_OK;
-    // V_nl psi = Q diag(d) Q^H psi with the complex coarse projector matrix Q of this k
+    if (c->nproj == 0 || !(qk_all ? qk_all : c->qk.p)) return PW_OK;
+    // V_nl psi = Q diag(d) Q^H psi with the complex coarse projector matrix Q of
+    // each k-point, one GEMM pair per k segment of the batch
+    for (int f = band0; f < band0 + nb;) {
+      const int kk = f / fpk;
+      const int f1 = (int)std::min<long>(band0 + nb, (long)(kk + 1) * fpk);
+      const V* Qk = qk_all ? qk_all + (long)kk * c->nproj * c->ntot : reinterpret_cast<const V*>(c->qk.p);
+      if ((rc = nl_k(c, Qk, psi + (long)f * ld, ld, out + (long)f * ldo, ldo, f1 - f, st))) return rc;
+      f = f1;
+    }
+    return PW_OK;
+  }
+
+  static int nl_k(pw_ctx* c, const V* Q, const V* x, int ld, V* y, int ldo, int nb, cudaStream_t st) {
+    int rc;
     cublasHandle_t h = (cublasHandle_t)c->blas;
     if (cublasSetStream(h, st) != CUBLAS_STATUS_SUCCESS) { set_error("cublasSetStream failed"); return PW_ECUDA; }
     const int np = c->nproj, nt = (int)c->ntot;
     if ((rc = c->s_wq.alloc((size_t)np * nb * sizeof(V)))) return rc;
     V* W = reinterpret_cast<V*>(c->s_wq.p);
-    const V* Q = reinterpret_cast<const V*>(c->qk.p);
-    const V* x = psi + (long)band0 * ld;
-    V* y = out + (long)band0 * ldo;
     cublasStatus_t r;
     { Launch L_(c, st, KK_LIBGEMM);
     if constexpr (std::is_same<T, double>::value) {
@@ -1472,6 +1484,15 @@ static int hpsik_thunk(pw_ctx* c, const void* psi, int ld, void* out, int ldo, i
   using V = VT<T>;
   return Plan<T, N0, N1, N2>::hpsi_batch_k(c, (const V*)psi, ld, (V*)out, ldo, band0, nb, acc, st);
 }
+using HpsiKBFn = int (*)(pw_ctx*, const void*, int, void*, int, int, int, int, cudaStream_t, int, const void*,
+                         const void*);
+template <typename T, int N0, int N1, int N2>
+static int hpsikb_thunk(pw_ctx* c, const void* psi, int ld, void* out, int ldo, int band0, int nb, int acc,
+                        cudaStream_t st, int fpk, const void* ekin_all, const void* qk_all) {
+  using V = VT<T>;
+  return Plan<T, N0, N1, N2>::hpsi_batch_k(c, (const V*)psi, ld, (V*)out, ldo, band0, nb, acc, st, fpk,
+                                           (const T*)ekin_all, (const V*)qk_all);
+}
 using BuildQKFn = int (*)(pw_ctx*, const int*, const double*, const double*, const long*, const long*, const int*, int,
                           const double*, void*, cudaStream_t);
 template <typename T, int N0, int N1, int N2>
@@ -1492,6 +1513,7 @@ struct GridEntry {
   ExxFn ace[2];
   HpsiKFn hpsik[2];
   BuildQKFn bqk[2];
+  HpsiKBFn hpsikb[2];
 };
 
 #define PWB_GRID(a, b, c)                                                                          \
@@ -1504,7 +1526,8 @@ struct GridEntry {
    {exx_thunk<double, a, b, c>, exx_thunk<float, a, b, c>},                                        \
    {ace_thunk<double, a, b, c>, ace_thunk<float, a, b, c>},                                        \
    {hpsik_thunk<double, a, b, c>, hpsik_thunk<float, a, b, c>},                                    \
-   {buildqk_thunk<double, a, b, c>, buildqk_thunk<float, a, b, c>}},
+   {buildqk_thunk<double, a, b, c>, buildqk_thunk<float, a, b, c>},                                \
+   {hpsikb_thunk<double, a, b, c>, hpsikb_thunk<float, a, b, c>}},
 
 static const GridEntry kGrids[] = {
 #include "grids.inc"
@@ -1553,6 +1576,13 @@ int run_hpsi_k(pw_ctx* c, const void* psi, int ld, void* out, int ldo, int band0
   const GridEntry* g = find_grid(c->n);
   if (!g) { set_error("grid not built into this library"); return PW_EUNSUPPORTED; }
   return g->hpsik[c->prec == PW_F32 ? 1 : 0](c, psi, ld, out, ldo, band0, nb, acc, st);
+}
+
+int run_hpsi_kbatch(pw_ctx* c, const void* psi, int ld, void* out, int ldo, int f0, int nf, int acc, cudaStream_t st,
+                    int fpk, const void* ekin_all, const void* qk_all) {
+  const GridEntry* g = find_grid(c->n);
+  if (!g) { set_error("grid not built into this library"); return PW_EUNSUPPORTED; }
+  return g->hpsikb[c->prec == PW_F32 ? 1 : 0](c, psi, ld, out, ldo, f0, nf, acc, st, fpk, ekin_all, qk_all);
 }
 
 int run_build_q_k(pw_ctx* c, const int* d_idx, const double* d_beta, const double* d_disp, const long* d_pio,

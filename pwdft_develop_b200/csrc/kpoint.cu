@@ -14,6 +14,8 @@
 namespace pwb {
 
 int run_hpsi_k(pw_ctx* c, const void* psi, int ld, void* out, int ldo, int band0, int nb, int acc, cudaStream_t st);
+int run_hpsi_kbatch(pw_ctx* c, const void* psi, int ld, void* out, int ldo, int f0, int nf, int acc, cudaStream_t st,
+                    int fpk, const void* ekin_all, const void* qk_all);
 int run_build_q_k(pw_ctx* c, const int* d_idx, const double* d_beta, const double* d_disp, const long* d_pio,
                   const long* d_pbo, const int* d_pnp, int nproj, const double* kv, void* out, cudaStream_t st);
 int ensure_scratch(pw_ctx* c, int npair);
@@ -96,6 +98,45 @@ int pw_hpsi_k(pw_ctx* ctx, const void* psi, int ld, void* hpsi, int ldh, int nba
   for (int b0 = 0; b0 < nband; b0 += cap) {
     const int nb = std::min(cap, nband - b0);
     int rc = run_hpsi_k(ctx, psi, ld, hpsi, ldh, b0, nb, accumulate, st);
+    if (rc) return rc;
+  }
+  return PW_OK;
+}
+
+int pw_set_kpoints(pw_ctx* ctx, int nk, const double* kpts) {
+  PWB_CHECK(ctx && nk > 0 && kpts, PW_EINVAL, "bad arguments");
+  PWB_CUDA(cudaSetDevice(ctx->device));
+  const long nt = ctx->ntot;
+  const size_t esz = ctx->esz;
+  const int np = (int)ctx->h_pnp.size();
+  int rc;
+  if ((rc = ctx->ekin_kb.alloc((size_t)nk * nt * esz))) return rc;
+  if (np > 0 && (rc = ctx->qkb.alloc((size_t)nk * np * nt * 2 * esz))) return rc;
+  for (int k = 0; k < nk; ++k) {
+    if ((rc = pw_set_kpoint(ctx, kpts + 3 * k))) return rc;
+    PWB_CUDA(cudaMemcpy((char*)ctx->ekin_kb.p + (size_t)k * nt * esz, ctx->ekin_k.p, nt * esz, cudaMemcpyDeviceToDevice));
+    if (np > 0)
+      PWB_CUDA(cudaMemcpy((char*)ctx->qkb.p + (size_t)k * np * nt * 2 * esz, ctx->qk.p, (size_t)np * nt * 2 * esz,
+                          cudaMemcpyDeviceToDevice));
+  }
+  ctx->kb_k.assign(kpts, kpts + 3 * nk);
+  ctx->nkb = nk;
+  return PW_OK;
+}
+
+int pw_hpsi_kbatch(pw_ctx* ctx, const void* psi, int ld, void* hpsi, int ldh, int nband, int accumulate, void* stream) {
+  PWB_CHECK(ctx && (nband == 0 || (psi && hpsi)), PW_EINVAL, "null argument");
+  PWB_CHECK(nband >= 0 && ld >= ctx->ntot && ldh >= ctx->ntot, PW_EINVAL, "Domain size does not match.");
+  PWB_CHECK(ctx->have_vtot, PW_ENOTREADY, "local potential not set (pw_set_vtot)");
+  PWB_CHECK(ctx->nkb > 0, PW_ENOTREADY, "k-point batch not set (pw_set_kpoints)");
+  PWB_CUDA(cudaSetDevice(ctx->device));
+  cudaStream_t st = (cudaStream_t)stream;
+  const int cap = std::max(ctx->pair_cap, 1);
+  const int nf = ctx->nkb * nband;
+  for (int f0 = 0; f0 < nf; f0 += cap) {
+    const int n = std::min(cap, nf - f0);
+    int rc = run_hpsi_kbatch(ctx, psi, ld, hpsi, ldh, f0, n, accumulate, st, nband, ctx->ekin_kb.p,
+                             ctx->nproj > 0 ? ctx->qkb.p : nullptr);
     if (rc) return rc;
   }
   return PW_OK;

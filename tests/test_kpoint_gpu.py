@@ -56,3 +56,21 @@ def test_hpsi_k_batches_and_accumulate():
     X = torch.tensor(psi, device="cuda")
     out = c.hpsi_k(X, out=torch.ones_like(X), accumulate=True).cpu().numpy()
     assert np.abs(out - 1.0 - ref).max() <= 1e-12 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("prec,tol", [("f64", 1e-12), ("f32", 1e-5)])
+def test_hpsi_kbatch_matches_per_k_oracle(prec, tol):
+    """A 2x2x2 Monkhorst-Pack batch in one pass, batches straddling k-points."""
+    import torch
+    L, z, pos, nc, nf, T, psi = _setup(nb=6)
+    b = 2 * np.pi / 10.26
+    kpts = np.array([[i, j, l] for i in (0.25, -0.25) for j in (0.25, -0.25) for l in (0.25, -0.25)]) * b
+    allpsi = np.stack([kpoints.random_complex_psi(T.dm.ntot, 6, 30 + i) for i in range(len(kpts))])
+    c = _ctx(L, z, pos, nc, nf, T, prec)
+    c.set_band_batch(10)                          # 5 complex bands per internal batch: straddles k boundaries
+    c.set_kpoints(kpts)
+    cdt = torch.complex128 if prec == "f64" else torch.complex64
+    out = c.hpsi_kbatch(torch.tensor(allpsi, dtype=cdt, device="cuda")).cpu().numpy().astype(np.complex128)
+    for i, k in enumerate(kpts):
+        ref = kpoints.mult_spinor_k(T, k, allpsi[i])
+        assert np.abs(out[i] - ref).max() <= tol * np.abs(ref).max(), i
