@@ -227,6 +227,7 @@ typedef struct pw_scf_params {
   unsigned long long seed;  /* random start */
   int ppcg_sbsize;          /* PPCG_sbSize (PW_SOLVER_PPCG), 1..8 */
   int davidson_maxdim;      /* subspace size in blocks (PW_SOLVER_DAVIDSON), >= 2 */
+  int graphs;               /* 1: replay the Chebyshev filter from a captured CUDA graph */
 } pw_scf_params;
 
 typedef struct pw_scf_result {
@@ -249,6 +250,17 @@ PW_API int pw_ctx_build_twin(pw_ctx* ctx);
  * energies of scf.cpp:1834-2140, all on the device.  eig_out: host, nocc+nextra
  * doubles; rho_out: host, N_fine doubles (either may be NULL). */
 PW_API int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* eig_out, double* rho_out);
+
+/* CUDA graph of one pw_hpsi call (same pointers, band count and accumulate
+ * flag on every replay; the inputs' contents may change between replays).
+ * The capture runs one ordinary call first (outside the graph).  Replays
+ * issue every kernel and library GEMM of the sweep with one launch. */
+typedef struct pw_graph pw_graph;
+PW_API int pw_graph_capture_hpsi(pw_ctx* ctx, const void* psi, int ld, void* hpsi, int ldh, int nband,
+                                 int accumulate, pw_graph** graph);
+PW_API int pw_graph_launch(pw_graph* graph, void* stream);
+PW_API int pw_graph_nodes(const pw_graph* graph, long* nodes);
+PW_API int pw_graph_destroy(pw_graph* graph);
 
 /* k-point mode (complex bands).  pw_set_kpoint builds, for the Bloch vector
  * k (Cartesian, bohr^-1), the kinetic 1/2 |k+G|^2 and Teter tables

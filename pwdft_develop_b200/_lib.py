@@ -44,7 +44,8 @@ class ScfParams(C.Structure):
                 ("mix_dim", C.c_int), ("mixed", C.c_int), ("verbose", C.c_int),
                 ("ecut", C.c_double), ("temperature", C.c_double), ("eig_tol", C.c_double),
                 ("mix_step", C.c_double), ("tol_efree", C.c_double), ("refine_threshold", C.c_double),
-                ("seed", C.c_ulonglong), ("ppcg_sbsize", C.c_int), ("davidson_maxdim", C.c_int)]
+                ("seed", C.c_ulonglong), ("ppcg_sbsize", C.c_int), ("davidson_maxdim", C.c_int),
+                ("graphs", C.c_int)]
 
 
 class ScfResult(C.Structure):
@@ -95,6 +96,10 @@ SIGNATURES: dict[str, tuple] = {
     "pw_scf_state": (_i, [_vp, _ip, _dp, _vp, _i, _vp]),
     "pw_exx_setup": (_i, [_vp, _d, _d, _i, _d]),
     "pw_set_kpoint": (_i, [_vp, _dp]),
+    "pw_graph_capture_hpsi": (_i, [_vp, _vp, _i, _vp, _i, _i, _i, C.POINTER(_vp)]),
+    "pw_graph_launch": (_i, [_vp, _vp]),
+    "pw_graph_nodes": (_i, [_vp, C.POINTER(_l)]),
+    "pw_graph_destroy": (_i, [_vp]),
     "pw_hpsi_k": (_i, [_vp, _vp, _i, _vp, _i, _i, _i, _vp]),
     "pw_get_kpoint_tables": (_i, [_vp, _dp, _dp]),
     "pw_set_kpoints": (_i, [_vp, _i, _dp]),

@@ -283,11 +283,12 @@ def _ctx_scf(self, nocc: int, nextra: int, ecut: float, solver: str = "chebfsi",
              temperature: float = 300.0, cheby_degree: int = 10, cheby_first_cycles: int = 5,
              eig_max_iter: int = 3, eig_tol: float = 1e-10, max_iter: int = 100, mix_dim: int = 8,
              mix_step: float = 0.7, tol_efree: float = 1e-6, refine_threshold: float = 1e-4, seed: int = 1,
-             verbose: bool = False, ppcg_sbsize: int = 1, davidson_maxdim: int = 2):
+             verbose: bool = False, ppcg_sbsize: int = 1, davidson_maxdim: int = 2, graphs: bool = False):
     """SCF::Iterate on the device (FP64 context; mixed=True runs the eigensolver in
     an FP32 twin and refines in FP64).  Returns (result dict, eigenvalues, rho)."""
     p = _lib.ScfParams(nocc=nocc, nextra=nextra,
                        solver=_SOLVERS[solver], ppcg_sbsize=ppcg_sbsize, davidson_maxdim=davidson_maxdim,
+                       graphs=int(graphs),
                        cheby_degree=cheby_degree, cheby_first_cycles=cheby_first_cycles, eig_max_iter=eig_max_iter,
                        max_iter=max_iter, mix_dim=mix_dim, mixed=int(mixed), verbose=int(verbose), ecut=ecut,
                        temperature=temperature, eig_tol=eig_tol, mix_step=mix_step, tol_efree=tol_efree,
@@ -469,6 +470,40 @@ def _ctx_hpsi_kbatch(self, psi, out=None, accumulate: bool = False, stream=None)
     return out
 
 
+class HpsiGraph:
+    """A captured pw_hpsi call: replay() applies H to the same buffers again."""
+
+    def __init__(self, ctx, psi, out, accumulate: bool = False):
+        self._ctx = ctx
+        self._keep = (psi, out)
+        h = C.c_void_p()
+        check(lib.pw_graph_capture_hpsi(ctx._h, _ptr(psi), ctx.ntot, _ptr(out), ctx.ntot, psi.shape[0],
+                                        int(accumulate), C.byref(h)))
+        self._g = h
+
+    @property
+    def nodes(self) -> int:
+        n = C.c_long(0)
+        check(lib.pw_graph_nodes(self._g, C.byref(n)))
+        return n.value
+
+    def replay(self, stream=None):
+        check(lib.pw_graph_launch(self._g, _stream(stream)))
+
+    def close(self):
+        if getattr(self, "_g", None):
+            lib.pw_graph_destroy(self._g)
+            self._g = None
+
+    def __del__(self):
+        self.close()
+
+
+def _ctx_capture_hpsi(self, psi, out, accumulate: bool = False) -> HpsiGraph:
+    return HpsiGraph(self, psi, out, accumulate)
+
+
+Context.capture_hpsi = _ctx_capture_hpsi
 Context.set_kpoints = _ctx_set_kpoints
 Context.hpsi_kbatch = _ctx_hpsi_kbatch
 Context.set_kpoint = _ctx_set_kpoint

@@ -182,6 +182,34 @@ __global__ void k_bdiag_rotate(int n, int width, int sb, const T* __restrict__ X
   }
 }
 
+// Chebyshev recurrence steps with device-resident coefficients (so that a
+// captured filter graph replays with new interval bounds):
+// Y = c[0] HY + c[1] X;  Z = c[0] HY + c[1] Y + c[2] X
+template <typename T>
+__global__ void k_cheb_lin(int n, const double* __restrict__ c, const T* __restrict__ HY, const T* __restrict__ Y,
+                           const T* __restrict__ X, T* __restrict__ Z, long ld, int three) {
+  const int j = blockIdx.y;
+  const double c0 = c[0], c1 = c[1], c2 = three ? c[2] : 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const long o = (long)j * ld + i;
+    double v = c0 * (double)HY[o] + c1 * (double)Y[o];
+    if (three) v += c2 * (double)X[o];
+    Z[o] = (T)v;
+  }
+}
+
+template <typename T>
+int cheb_lin(int n, int nb, const double* coef_dev, const T* HY, const T* Y, const T* X, T* Z, long ld,
+             cudaStream_t st) {
+  k_cheb_lin<T><<<grid2(n, nb), 256, 0, st>>>(n, coef_dev, HY, Y, X, Z, ld, X ? 1 : 0);
+  PWB_CUDA(cudaGetLastError());
+  return PW_OK;
+}
+template int cheb_lin<float>(int, int, const double*, const float*, const float*, const float*, float*, long,
+                             cudaStream_t);
+template int cheb_lin<double>(int, int, const double*, const double*, const double*, const double*, double*, long,
+                              cudaStream_t);
+
 template <typename T>
 int bdiag_dots(int n, int width, int sb, const T* U, const T* V, long ld, DevBuf& part, double* out_host,
                cudaStream_t st) {

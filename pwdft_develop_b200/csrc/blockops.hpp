@@ -23,6 +23,11 @@ int copy_f2d(long n, const float* x, double* y, cudaStream_t st);
 int copy_d2f_2d(int n, int nb, const double* x, long ldx, float* y, long ldy, cudaStream_t st);
 int copy_f2d_2d(int n, int nb, const float* x, long ldx, double* y, long ldy, cudaStream_t st);
 
+// Z = c[0] HY + c[1] Y (+ c[2] X when X is given); c device-resident (3 doubles)
+template <typename T>
+int cheb_lin(int n, int nb, const double* coef_dev, const T* HY, const T* Y, const T* X, T* Z, long ld,
+             cudaStream_t st);
+
 // Diagonal sb x sb blocks of U^T V (width columns, grid length n) for the PPCG
 // sub-block sweep: out_host[k * sb * sb + i + j * sb], k < ceil(width / sb),
 // FP64, summed over grid-point splits in a fixed order.  sb in 1..8.

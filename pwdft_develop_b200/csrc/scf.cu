@@ -166,6 +166,19 @@ struct Solver {
   DevBuf G1, G2, wbuf;                     // dense FP64 work (3nb x 3nb)
   std::vector<double> eig, res;
   void* ptr(DevBuf& b, long col = 0) { return (char*)b.p + (size_t)col * nt * esz; }
+  // Chebyshev filter replayed from a CUDA graph (coefficients in fcoef)
+  bool use_graph = false;
+  cudaStream_t st = nullptr;
+  cudaGraph_t fgraph = nullptr;
+  cudaGraphExec_t fexec = nullptr;
+  int f_nb = 0, f_m = 0, f_calls = 0;
+  void* f_res = nullptr;
+  DevBuf fcoef;
+  ~Solver() {
+    if (fexec) cudaGraphExecDestroy(fexec);
+    if (fgraph) cudaGraphDestroy(fgraph);
+    if (st) cudaStreamDestroy(st);
+  }
 };
 
 // eigensolver sub-phase timers (H*psi, Gram, dense FP64, rotations), seconds
@@ -267,39 +280,6 @@ static int rayleigh_ritz(Solver& s, Dense& d, void* Y, void* HY, void* X, void* 
 
 // Chebyshev filter of degree m on [a, b] scaled at a0 (Zhou et al. 2006,
 // Algorithm 3.2): on exit Y = p_m(H) X.  X is overwritten.
-static int cheby_filter(Solver& s, int nb, int m, double a, double b, double a0, void* X, void* Y, void* Z, void* HY,
-                        void** result) {
-  const double e = (b - a) / 2.0, cc = (b + a) / 2.0;
-  double sigma = e / (a0 - cc);
-  const double sigma1 = sigma, gamma = 2.0 / sigma1;
-  int rc;
-  if ((rc = hpsi(s.c, X, HY, nb, nullptr))) return rc;
-  // Y = (HX - c X) sigma1 / e
-  PWB_CUDA(cudaMemcpy(Y, HY, (size_t)nb * s.nt * s.esz, cudaMemcpyDeviceToDevice));
-  if ((rc = v_axpby(s, nb, -cc * sigma1 / e, X, sigma1 / e, Y))) return rc;
-  void* xp = X;
-  void* yp = Y;
-  void* zp = Z;
-  for (int i = 2; i <= m; ++i) {
-    const double sigma2 = 1.0 / (gamma - sigma);
-    if ((rc = hpsi(s.c, yp, HY, nb, nullptr))) return rc;
-    // Z = (2 sigma2 / e)(HY - c Y) - sigma sigma2 X
-    if (s.c->prec == PW_F64)
-      rc = axpbypcz<double>((int)s.nt, nb, 2 * sigma2 / e, (const double*)HY, -2 * sigma2 * cc / e, (const double*)yp,
-                            -sigma * sigma2, (const double*)xp, (double*)zp, s.nt, nullptr);
-    else
-      rc = axpbypcz<float>((int)s.nt, nb, 2 * sigma2 / e, (const float*)HY, -2 * sigma2 * cc / e, (const float*)yp,
-                           -sigma * sigma2, (const float*)xp, (float*)zp, s.nt, nullptr);
-    if (rc) return rc;
-    void* t = xp;
-    xp = yp;
-    yp = zp;
-    zp = t;
-    sigma = sigma2;
-  }
-  *result = yp;
-  return PW_OK;
-}
 
 // k-step Lanczos on a random vector: upper bound of the spectrum
 static int lanczos_upper(Solver& s, int k, double* upper, double* lower) {
@@ -386,10 +366,100 @@ static int lanczos_upper(Solver& s, int k, double* upper, double* lower) {
 }
 
 // one ChebFSI step on the block X (orthonormal on entry and exit); eigenvalues in s.eig
+// The same filter with device-resident coefficients on stream st (capturable):
+// coef[0..1] for the first step, coef[3 (i - 1) ..] for step i
+static int cheby_filter_dev(Solver& s, int nb, int m, const double* coef, void* X, void* Y, void* Z, void* HY,
+                            void** result, cudaStream_t st) {
+  int rc;
+  const bool f64 = s.c->prec == PW_F64;
+  auto lin = [&](const double* c, void* hy, void* y, void* x, void* z) {
+    return f64 ? cheb_lin<double>((int)s.nt, nb, c, (const double*)hy, (const double*)y, (const double*)x, (double*)z,
+                                  s.nt, st)
+               : cheb_lin<float>((int)s.nt, nb, c, (const float*)hy, (const float*)y, (const float*)x, (float*)z,
+                                 s.nt, st);
+  };
+  if ((rc = pw_hpsi(s.c, X, (int)s.nt, HY, (int)s.nt, nb, 0, st))) return rc;
+  if ((rc = lin(coef, HY, X, nullptr, Y))) return rc;
+  void* xp = X;
+  void* yp = Y;
+  void* zp = Z;
+  for (int i = 2; i <= m; ++i) {
+    if ((rc = pw_hpsi(s.c, yp, (int)s.nt, HY, (int)s.nt, nb, 0, st))) return rc;
+    if ((rc = lin(coef + 3 * (i - 1), HY, yp, xp, zp))) return rc;
+    void* t = xp;
+    xp = yp;
+    yp = zp;
+    zp = t;
+  }
+  *result = yp;
+  return PW_OK;
+}
+
+// Chebyshev filter (Zhou-Saad recurrence on [a, b], scaled by the lower bound
+// a0).  With s.use_graph the first call runs directly (allocations, library
+// handles), the second captures a CUDA graph, later calls only upload the new
+// coefficients and replay it; without it every call launches directly.  Both
+// run the same kernels in the same order.
+static int cheby_filter_run(Solver& s, int nb, int m, double a, double b, double a0, void** result) {
+  int rc;
+  if (!s.st) PWB_CUDA(cudaStreamCreateWithFlags(&s.st, cudaStreamNonBlocking));
+  {
+    // order after the work already queued on the default stream (X, bounds)
+    cudaEvent_t ev;
+    PWB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    PWB_CUDA(cudaEventRecord(ev, 0));
+    PWB_CUDA(cudaStreamWaitEvent(s.st, ev, 0));
+    cudaEventDestroy(ev);
+  }
+  const double e = (b - a) / 2.0, cc = (b + a) / 2.0;
+  double sigma = e / (a0 - cc);
+  const double sigma1 = sigma, gamma = 2.0 / sigma1;
+  std::vector<double> coef(3 * std::max(m, 1), 0.0);
+  coef[0] = sigma1 / e;
+  coef[1] = -cc * sigma1 / e;
+  for (int i = 2; i <= m; ++i) {
+    const double sigma2 = 1.0 / (gamma - sigma);
+    coef[3 * (i - 1) + 0] = 2 * sigma2 / e;
+    coef[3 * (i - 1) + 1] = -2 * sigma2 * cc / e;
+    coef[3 * (i - 1) + 2] = -sigma * sigma2;
+    sigma = sigma2;
+  }
+  if ((rc = s.fcoef.alloc(coef.size() * 8))) return rc;
+  PWB_CUDA(cudaMemcpyAsync(s.fcoef.p, coef.data(), coef.size() * 8, cudaMemcpyHostToDevice, s.st));
+  const double* cd = (const double*)s.fcoef.p;
+  if (s.fexec && (s.f_nb != nb || s.f_m != m)) {
+    cudaGraphExecDestroy(s.fexec);
+    cudaGraphDestroy(s.fgraph);
+    s.fexec = nullptr;
+    s.fgraph = nullptr;
+    s.f_calls = 0;
+  }
+  if (!s.use_graph || (!s.fexec && s.f_calls == 0)) {
+    rc = cheby_filter_dev(s, nb, m, cd, s.X.p, s.Y.p, s.Z.p, s.HY.p, result, s.st);
+    s.f_calls = 1;
+    s.f_nb = nb;
+    s.f_m = m;
+  } else {
+    if (!s.fexec) {
+      PWB_CUDA(cudaStreamSynchronize(s.st));
+      PWB_CUDA(cudaStreamBeginCapture(s.st, cudaStreamCaptureModeThreadLocal));
+      rc = cheby_filter_dev(s, nb, m, cd, s.X.p, s.Y.p, s.Z.p, s.HY.p, &s.f_res, s.st);
+      cudaError_t e1 = cudaStreamEndCapture(s.st, &s.fgraph);
+      if (rc) return rc;
+      PWB_CUDA(e1);
+      PWB_CUDA(cudaGraphInstantiate(&s.fexec, s.fgraph, 0));
+    }
+    PWB_CUDA(cudaGraphLaunch(s.fexec, s.st));
+    *result = s.f_res;
+  }
+  PWB_CUDA(cudaStreamSynchronize(s.st));
+  return rc;
+}
+
 static int chebfsi_step(Solver& s, Dense& d, int nb, int degree, double a, double b, double a0) {
   int rc;
   void* res = nullptr;
-  if ((rc = cheby_filter(s, nb, degree, a, b, a0, s.X.p, s.Y.p, s.Z.p, s.HY.p, &res))) return rc;
+  if ((rc = cheby_filter_run(s, nb, degree, a, b, a0, &res))) return rc;
   // res is one of X, Y, Z; orthonormalise it, then Rayleigh-Ritz into X / HX
   void* tmp = (res == s.Z.p) ? s.Y.p : s.Z.p;
   if ((rc = cholqr(s, d, res, nb, tmp))) return rc;
@@ -1137,7 +1207,14 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
   Dense dn;
   if ((rc = dn.init((cublasHandle_t)ctx->blas))) return rc;
   Solver sv;
+  sv.use_graph = p->graphs != 0 && !prof;   // the sub-phase timers synchronise, which a capture forbids
   auto bind = [&](pw_ctx* c) -> int {
+    // a captured filter refers to the previous context's buffers
+    if (sv.fexec) cudaGraphExecDestroy(sv.fexec);
+    if (sv.fgraph) cudaGraphDestroy(sv.fgraph);
+    sv.fexec = nullptr;
+    sv.fgraph = nullptr;
+    sv.f_calls = 0;
     sv.c = c;
     sv.nt = nt;
     sv.esz = c->esz;
