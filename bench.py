@@ -205,13 +205,13 @@ def scf_bench(device: int, max_iter: int = 60):
         # untimed warm-up (solver handles, first-use buffers), 2 SCF iterations
         c.scf(nocc=128, nextra=32, ecut=20.0, solver="chebfsi", mixed=(mode == "mixed"), cheby_degree=10,
               cheby_first_cycles=1, tol_efree=1e-6, refine_threshold=1e9 if mode == "mixed" else 1e-5, max_iter=2,
-              seed=SEED)
+              seed=SEED, graphs=True)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         res, eig, _ = c.scf(nocc=128, nextra=32, ecut=20.0, solver="chebfsi", mixed=(mode == "mixed"),
                             cheby_degree=10, cheby_first_cycles=5, tol_efree=1e-6, refine_threshold=1e-5,
-                            max_iter=max_iter, seed=SEED)
+                            max_iter=max_iter, seed=SEED, graphs=True)
         e1.record()
         torch.cuda.synchronize()
         out[mode] = dict(seconds=e0.elapsed_time(e1) / 1e3, iterations=res["iterations"],
@@ -227,8 +227,100 @@ def scf_bench(device: int, max_iter: int = 60):
         c.close()
     out["speedup_mixed_vs_f64"] = out["f64"]["seconds"] / out["mixed"]["seconds"]
     out["efree_agreement_per_atom"] = abs(out["f64"]["efree"] - out["mixed"]["efree"]) / 64
-    out["workload"] = "Si64, ChebFSI degree 10 (5 cycles in the first SCF step), Anderson(8, 0.7), 300 K, tol 1e-6 Ha/atom"
+    out["workload"] = ("Si64, ChebFSI degree 10 (5 cycles in the first SCF step), Anderson(8, 0.7), 300 K, "
+                       "tol 1e-6 Ha/atom, Chebyshev filter replayed from a CUDA graph")
     return out
+
+
+def exx_bench(device: int, reps: int = 3):
+    """Hybrid exchange on Si64 (48^3 coarse grid, 160 bands, 128 occupied;
+    PBE0 mixing 0.25, Coulomb kernel with the divergence correction): time of
+    V_x psi over all (band, occupied orbital) pairs in FP32 and FP64, the ACE
+    build, and the FP32 exchange energy against the FP64 one (per atom)."""
+    import torch
+    from pwdft_develop_b200 import Context
+    L, z, pos = si64_atoms()
+    nb, nocc = 160, 128
+    g = torch.Generator(device="cuda").manual_seed(SEED + 7)
+    X64 = torch.randn((nb, NC[0] * NC[1] * NC[2]), dtype=torch.float64, device="cuda", generator=g)
+    R = torch.linalg.cholesky(X64 @ X64.T).T
+    X64 = torch.linalg.solve_triangular(R, X64, upper=True, left=True).contiguous()
+    occ = np.zeros(nb)
+    occ[:nocc] = 1.0
+    out = {"workload": "Si64 48^3, 160 bands x 128 occupied orbitals, PBE0 fraction 0.25, divergence type 1",
+           "pairs": nb * nocc}
+    energies = {}
+    for prec in ("f32", "f64"):
+        c = Context(L, NC, NF, precision=prec, device=device)
+        c.set_atoms(z, pos)
+        c.exx_setup(0.25, 0.0, 1, 20.0)
+        X = X64.to(c.torch_dtype).contiguous()
+        c.exx_set_phi(X, occ)
+        Y = torch.empty_like(X)
+        c.exx_apply(X, out=Y)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            c.exx_apply(X, out=Y)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        s = 4 if prec == "f32" else 8
+        ntot = NC[0] * NC[1] * NC[2]
+        hc = (NC[0] // 2 + 1) * NC[1] * NC[2]
+        pair_bytes = 4 * s * ntot + 8 * s * hc
+        peak, peak_kind = load_peaks()
+        d = {"vx_psi_ms": ms, "pairs_per_s": nb * nocc / (ms / 1e3),
+             "model_bytes_per_pair": pair_bytes,
+             "model_frac_of_hbm": nb * nocc * pair_bytes / (ms / 1e3) / 1e9 / peak, "peak_source": peak_kind}
+        energies[prec] = c.exx_energy(X, occ)
+        e0.record()
+        c.ace_build(X)
+        e1.record()
+        torch.cuda.synchronize()
+        d["ace_build_ms"] = e0.elapsed_time(e1)
+        d["exchange_energy"] = energies[prec]
+        out[prec] = d
+        c.close()
+    out["exchange_energy_error_per_atom_f32"] = abs(energies["f32"] - energies["f64"]) / 64
+    return out
+
+
+def kpoint_bench(device: int, reps: int = 5):
+    """Si8 complex bands on a 4x4x4 Monkhorst-Pack k-mesh (64 k-points, 24
+    bands each, 24^3 / 48^3 grids, Ecut 10 Ha) in one batched H(k) psi pass, FP32."""
+    import torch
+    from pwdft_develop_b200 import Context
+    rng = np.random.Generator(np.random.Philox(SEED + 3))
+    base = np.array([[0, 0, 0], [0, .5, .5], [.5, 0, .5], [.5, .5, 0],
+                     [.25, .25, .25], [.25, .75, .75], [.75, .25, .75], [.75, .75, .25]])
+    pos = base * A_CELL + rng.uniform(-0.02, 0.02, size=(8, 3))
+    L, z = np.array([A_CELL] * 3), 14
+    nc, nf, nb = (24, 24, 24), (48, 48, 48), 24
+    b = 2 * np.pi / A_CELL
+    mp = [(2 * i - 3) / 8.0 for i in range(4)]
+    kpts = np.array([[x, y, w] for x in mp for y in mp for w in mp]) * b
+    c = Context(L, nc, nf, precision="f32", device=device)
+    c.set_atoms([z] * len(pos), pos)
+    c.set_vtot(synthetic_vtot(c.ntotFine))
+    c.set_band_batch(2 * 256)
+    c.set_kpoints(kpts)
+    g = torch.Generator(device="cuda").manual_seed(SEED + 9)
+    X = torch.randn((len(kpts), nb, c.ntot), dtype=torch.complex64, device="cuda", generator=g)
+    Y = torch.empty_like(X)
+    c.hpsi_kbatch(X, out=Y)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        c.hpsi_kbatch(X, out=Y)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    c.close()
+    return {"workload": "Si8 4x4x4 MP (64 k), 24 complex bands per k, 24^3/48^3, FP32",
+            "ms_per_pass": ms, "k_bands_per_s": len(kpts) * nb / (ms / 1e3)}
 
 
 def run_reference(args):
@@ -398,6 +490,10 @@ def run_ours(args):
         }
         if args.scf and world == 1:
             line["scf"] = scf_bench(local)
+        if args.exx and world == 1:
+            line["exx"] = exx_bench(local)
+        if args.kpoints and world == 1:
+            line["kpoints"] = kpoint_bench(local)
         if args.cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(args.cpu_bands)
         print(json.dumps(line), flush=True)
@@ -416,6 +512,8 @@ def main():
     ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-scf", dest="scf", action="store_false", help="skip the SCF time-to-solution leg")
+    ap.add_argument("--no-exx", dest="exx", action="store_false", help="skip the hybrid-exchange leg")
+    ap.add_argument("--no-kpoints", dest="kpoints", action="store_false", help="skip the k-point batch leg")
     ap.add_argument("--cpu-bands", type=int, default=64)
     ap.add_argument("--bands", type=int, default=NBAND, help="band block size (profiling runs use a small block)")
     args = ap.parse_args()
