@@ -190,7 +190,9 @@ def scf_bench(device: int, max_iter: int = 60):
     """SCF time to |E_free - E_Harris| / N_atom < 1e-6 Ha/atom on Si64 with
     ChebFSI (degree 10): plain FP64 against the mixed form (FP32 H*psi and
     Chebyshev filter, split-BF16 tensor-core Gram products, FP64 Cholesky /
-    Rayleigh-Ritz / mixing, FP64 refinement in the last iterations).  Each run
+    Rayleigh-Ritz / mixing, FP64 refinement once |E_free - E_Harris| / N_atom
+    falls below 3e-6, i.e. within a factor 3 of the tolerance: the FP32 fixed
+    point itself is biased by ~2e-6 Ha/atom).  Each run
     is bracketed by CUDA events on the device."""
     import torch
     from pwdft_develop_b200 import Context
@@ -210,7 +212,7 @@ def scf_bench(device: int, max_iter: int = 60):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         res, eig, _ = c.scf(nocc=128, nextra=32, ecut=20.0, solver="chebfsi", mixed=(mode == "mixed"),
-                            cheby_degree=10, cheby_first_cycles=5, tol_efree=1e-6, refine_threshold=1e-5,
+                            cheby_degree=10, cheby_first_cycles=5, tol_efree=1e-6, refine_threshold=3e-6,
                             max_iter=max_iter, seed=SEED, graphs=True)
         e1.record()
         torch.cuda.synchronize()
@@ -220,7 +222,7 @@ def scf_bench(device: int, max_iter: int = 60):
                          lumo=float(eig[128]))
         if os.environ.get("PWB_SCF_PHASES"):
             res2, _, _ = c.scf(nocc=128, nextra=32, ecut=20.0, solver="chebfsi", mixed=(mode == "mixed"),
-                               cheby_degree=10, cheby_first_cycles=5, tol_efree=1e-6, refine_threshold=1e-5,
+                               cheby_degree=10, cheby_first_cycles=5, tol_efree=1e-6, refine_threshold=3e-6,
                                max_iter=max_iter, seed=SEED, verbose=2)
             out[mode]["phase_s"] = res2["phase_s"]
             out[mode]["sub_s"] = res2["sub_s"]

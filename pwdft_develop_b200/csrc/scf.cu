@@ -1241,6 +1241,8 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
   const double tbeta = 315774.67 / p->temperature;
   double b_up = 0, lmin = 0;
   bool have_bounds = false, refined = !p->mixed;
+  double best_dif = 1e300;
+  int stall = 0;
   std::vector<double> occ, eig;
   double ef = 0, etot = 0, efree = 0, eharris = 0, ehart = 0;
   int it = 0;
@@ -1338,8 +1340,20 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
               sv.c->prec == PW_F32 ? "f32" : "f64", etot, efree, eharris, dif);
     PWB_CUDA(cudaMemcpy(rho, ro, nf * 8, cudaMemcpyDeviceToDevice));
     if (refined && dif < p->tol_efree) { conv = true; break; }
-    // switch the eigensolver to FP64 for the final iterations (iterative refinement)
-    if (!refined && dif < p->refine_threshold) {
+    // switch the eigensolver to FP64 for the final iterations (iterative
+    // refinement): below the threshold, or when the FP32 iteration has
+    // stagnated (no 10% gain on its best |E_free - E_Harris| for 4 steps)
+    // within a factor 100 of it -- the FP32 fixed point is biased at the
+    // 1e-6 Ha/atom level and cannot reach the tolerance by itself
+    if (!refined) {
+      if (dif < 0.9 * best_dif) {
+        best_dif = dif;
+        stall = 0;
+      } else {
+        ++stall;
+      }
+    }
+    if (!refined && (dif < p->refine_threshold || (stall >= 4 && dif < 100.0 * p->refine_threshold))) {
       PhaseTimer pt_(prof, &tph[5]);
       DevBuf x32;
       if ((rc = x32.alloc((size_t)nb * nt * 4))) return rc;
