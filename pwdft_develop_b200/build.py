@@ -9,6 +9,7 @@ from __future__ import annotations
 
 import concurrent.futures as cf
 import os
+import re
 import shutil
 import subprocess
 import sys
@@ -38,6 +39,16 @@ def _headers_mtime() -> float:
     return max((h.stat().st_mtime for h in hs), default=0.0)
 
 
+def grids() -> list[tuple[int, int, int]]:
+    """The coarse grids listed in csrc/grids.inc (PWB_GRID(n0, n1, n2) lines)."""
+    out = []
+    for line in (CSRC / "grids.inc").read_text().splitlines():
+        m = re.match(r"\s*PWB_GRID\((\d+),\s*(\d+),\s*(\d+)\)", line)
+        if m:
+            out.append(tuple(int(x) for x in m.groups()))
+    return out
+
+
 def _compile(src: Path, obj: Path, extra: list[str]) -> tuple[Path, str]:
     cmd = [nvcc()] + ARCH + NVCC_FLAGS + extra + ["-c", str(src), "-o", str(obj)]
     r = subprocess.run(cmd, capture_output=True, text=True)
@@ -49,7 +60,8 @@ def _compile(src: Path, obj: Path, extra: list[str]) -> tuple[Path, str]:
 def build(verbose: bool = False, jobs: int | None = None, extra: list[str] | None = None) -> Path:
     BUILD.mkdir(parents=True, exist_ok=True)
     extra = list(extra or [])
-    srcs = sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cpp"))
+    inst = CSRC / "grid_instance.cu"
+    srcs = [s for s in sorted(CSRC.glob("*.cu")) if s != inst] + sorted(CSRC.glob("*.cpp"))
     hmt = _headers_mtime()
     todo = []
     objs = []
@@ -57,11 +69,17 @@ def build(verbose: bool = False, jobs: int | None = None, extra: list[str] | Non
         o = BUILD / (s.name + ".o")
         objs.append(o)
         if not o.exists() or o.stat().st_mtime < max(s.stat().st_mtime, hmt):
-            todo.append((s, o))
+            todo.append((s, o, extra))
+    # one object per grid of grids.inc (parallel compilation of the templates)
+    for g in grids():
+        o = BUILD / f"grid_{g[0]}_{g[1]}_{g[2]}.o"
+        objs.append(o)
+        if not o.exists() or o.stat().st_mtime < max(inst.stat().st_mtime, hmt):
+            todo.append((inst, o, extra + [f"-DPWB_N0={g[0]}", f"-DPWB_N1={g[1]}", f"-DPWB_N2={g[2]}"]))
     jobs = jobs or min(len(todo) or 1, os.cpu_count() or 4)
     if todo:
         with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
-            futs = [ex.submit(_compile, s, o, extra) for s, o in todo]
+            futs = [ex.submit(_compile, s, o, e) for s, o, e in todo]
             for f in cf.as_completed(futs):
                 o, log = f.result()
                 if verbose:

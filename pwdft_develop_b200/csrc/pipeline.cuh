@@ -1,0 +1,1508 @@
+#pragma once
+// Band-pair H*psi pipeline on sm_100a (kernels and the per-grid Plan;
+// included by grid_instance.cu, one translation unit per grid).
+//
+// Two real bands a, b of the Gamma-point wavefunction are packed into one
+// complex field Z = psi_a + i psi_b.  The reference's real-to-complex path
+// (Spinor::AddMultSpinorFineR2C, src/SCF/spinor.cpp:377-525) is a real-linear
+// map, so running its complex-linear extension on Z gives H psi_a + i H psi_b.
+// The coarse->fine spectrum placement of IP_c2f / IP_f2c
+// (src/utility.cpp:3150-3275: a coefficient whose index is Nyquist in the set
+// S of axes goes, halved, to the all-plus and the all-minus fine positions)
+// is separable once every Nyquist coefficient is given a "+" and a "-" slot;
+// the z-pencil kernels do that unfolding so the fine-plane kernels only see
+// plain zero padding.
+//
+// Kernels (one launch each per band batch, all pairs in the grid):
+//   k_cxy_fwd    coarse plane: FFT x, FFT y                     psi -> A
+//   k_zpad       coarse z FFT, kinetic, unfold + pad, fine z IFFT  A -> K, B
+//   k_fplane<G>  fine plane: IFFT y, IFFT x, projector partial dots  B -> Wp
+//   k_nl_reduce  sum partial dots, scale by gamma*vol/N_fine     Wp -> W
+//   k_fplane<A>  fine plane: IFFT y, IFFT x, *V + projector scatter,
+//                FFT x, FFT y, truncate                           B -> C (in place)
+//   k_zfold      fine z FFT, fold (IP_f2c rule) + kinetic, coarse z IFFT  C,K -> D
+//   k_cxy_inv    coarse plane: IFFT y, IFFT x, (accumulate) into hpsi   D -> hpsi
+#include <cublas_v2.h>
+
+#include <mutex>
+#include <string>
+
+#include "common.hpp"
+#include "fft.cuh"
+#include "gemm.hpp"
+#include "grid_registry.hpp"
+
+namespace pwb {
+
+// kx columns per z-pencil CTA: 24 for FP32 grids divisible by 24 (two
+// balanced tiles at n0 = 48), otherwise 16
+template <typename T, int N0> struct PencilTile {
+  static constexpr int v = (sizeof(T) == 4 && N0 % 24 == 0) ? 24 : 16;
+};
+constexpr int PLANE_THREADS = 256;
+constexpr int PENCIL_THREADS = 256;
+
+template <typename T> using VT = typename C2<T>::t;
+
+__device__ __forceinline__ int sgn_idx(int k, int n) { return k <= n / 2 ? k : k - n; }
+// slot s in [0, n]: s < n is the FFT index (Nyquist = "+" slot), s == n is the "-" Nyquist slot
+__device__ __forceinline__ int slot_fine(int s, int n, int nf) {
+  int m = (s < n) ? sgn_idx(s, n) : -(n / 2);
+  return (m + nf) % nf;
+}
+
+template <typename V>
+__device__ __forceinline__ void load_tw(V* dst, const V* src, int n) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+}
+
+// ---------------------------------------------------------------------------
+// coarse plane forward: psi (two real bands) -> A[pair][z][ky][kx]
+// ---------------------------------------------------------------------------
+template <typename T, int N0, int N1, bool CPLX = false>
+__global__ void __launch_bounds__(PLANE_THREADS)
+k_cxy_fwd(const T* __restrict__ psi, int ld, int nband, int band0, VT<T>* __restrict__ A,
+          const VT<T>* twx_g, const VT<T>* twy_g) {
+  using V = VT<T>;
+  constexpr int P0 = N0 + 1;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  V* pl = reinterpret_cast<V*>(smraw);
+  V* twx = pl + N1 * P0;
+  V* twy = twx + N0;
+  load_tw(twx, twx_g, N0);
+  load_tw(twy, twy_g, N1);
+  const int z = blockIdx.x, p = blockIdx.y;
+  const long ntot_plane = (long)N0 * N1;
+  if (CPLX) {
+    // one complex band per field (ld in complex elements)
+    const V* pc = reinterpret_cast<const V*>(psi) + (long)(band0 + p) * ld + z * ntot_plane;
+    for (int i = threadIdx.x; i < N0 * N1; i += blockDim.x) {
+      const int y = i / N0, x = i - y * N0;
+      pl[y * P0 + x] = pc[i];
+    }
+  } else {
+    const int ba = band0 + 2 * p, bb = ba + 1;
+    const T* pa = psi + (long)ba * ld + z * ntot_plane;
+    const T* pb = (bb < nband) ? psi + (long)bb * ld + z * ntot_plane : nullptr;
+    for (int i = threadIdx.x; i < N0 * N1; i += blockDim.x) {
+      const int y = i / N0, x = i - y * N0;
+      pl[y * P0 + x] = mkc<V>(pa[i], pb ? pb[i] : (T)0);
+    }
+  }
+  __syncthreads();
+  smem_fft_cb<N0, -1, 1, P0>(pl, N1, twx);
+  __syncthreads();
+  smem_fft_cb<N1, -1, P0, 1>(pl, N0, twy);
+  __syncthreads();
+  const int N2 = gridDim.x;
+  V* Ap = A + ((long)p * N2 + z) * ntot_plane;
+  for (int i = threadIdx.x; i < N0 * N1; i += blockDim.x) {
+    const int y = i / N0, x = i - y * N0;
+    Ap[i] = pl[y * P0 + x];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// column bookkeeping shared by k_zpad and k_zfold.
+// Tile: fixed ky, kx in [kx0, kx0+TX).  Output/input columns:
+//   ky not Nyquist: col i <-> (ky, kx0+i); if kx0+i == n0/2 its "-" partner is col TX
+//   ky Nyquist:     col i <-> (ky+, kx0+i (+ slot)); col TX+i <-> (ky-, kx0+i or n0 if kx Nyquist)
+// ---------------------------------------------------------------------------
+struct ColMap {
+  int ncols;
+  bool nyy;
+  int nyx_i;  // tile-local index of the kx Nyquist column, -1 if none
+};
+template <int TX> __device__ __forceinline__ ColMap colmap(int ky, int kx0, int tw, int n0, int n1) {
+  ColMap m;
+  m.nyy = (ky == n1 / 2);
+  m.nyx_i = (n0 / 2 >= kx0 && n0 / 2 < kx0 + tw) ? (n0 / 2 - kx0) : -1;
+  m.ncols = m.nyy ? 2 * TX : (m.nyx_i >= 0 ? TX + 1 : TX);
+  return m;
+}
+// slot coordinates of column c
+template <int TX>
+__device__ __forceinline__ void col_slot(const ColMap& m, int c, int ky, int kx0, int n0, int n1,
+                                         int& ky_s, int& kx_s) {
+  if (m.nyy) {
+    if (c < TX) { ky_s = ky; kx_s = kx0 + c; }
+    else { ky_s = n1; kx_s = (kx0 + c - TX == n0 / 2) ? n0 : kx0 + c - TX; }
+  } else {
+    if (c < TX) { ky_s = ky; kx_s = kx0 + c; }
+    else { ky_s = ky; kx_s = n0; }
+  }
+}
+
+// The tile's used columns in compact order: j < tw -> column j, then the
+// Nyquist partners (column TX for a kx Nyquist, TX + j' for a ky Nyquist row).
+__device__ __forceinline__ int ncompact(const ColMap& m, int tw) {
+  return tw + (m.nyy ? tw : (m.nyx_i >= 0 ? 1 : 0));
+}
+template <int TX> __device__ __forceinline__ int compact_col(int j, int tw) { return j < tw ? j : TX + (j - tw); }
+
+// for (i = threadIdx.x; i < rows * n; i += blockDim.x) f(i / n, i % n) without
+// a division per step
+template <typename F> __device__ __forceinline__ void for_rows_cols(int rows, int n, F&& f) {
+  const int step = blockDim.x;
+  const int q = step / n, r = step - q * n;
+  int a = threadIdx.x / n, b = threadIdx.x - a * n;
+  while (a < rows) {
+    f(a, b);
+    a += q;
+    b += r;
+    if (b >= n) { b -= n; ++a; }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// z pencils: coarse FFT z, kinetic, Nyquist unfold, fine pad, fine IFFT z
+// ---------------------------------------------------------------------------
+template <typename T, int NZ, int NZF, int TX>
+__global__ void __launch_bounds__(PENCIL_THREADS, sizeof(T) == 4 ? 4 : 1)
+k_zpad(const VT<T>* __restrict__ A, VT<T>* __restrict__ K, VT<T>* __restrict__ B,
+       const T* __restrict__ ekin, int n0, int n1, T inv_nc,
+       const VT<T>* twz_g, const VT<T>* twzf_g, int cplx = 0, int kf0 = 0, int fpk = 1 << 30, long kstride = 0) {
+  using V = VT<T>;
+  constexpr int PI = TX + 1;
+  constexpr int PO = 2 * TX + 1;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  V* in = reinterpret_cast<V*>(smraw);     // [NZ][PI]
+  V* out = in + NZ * PI;                   // [NZF][PO]
+  V* twz = out + NZF * PO;
+  V* twzf = twz + NZ;
+  __shared__ int colofs[2 * TX];           // slot offset of output column c in a fine plane, -1 if unused
+  load_tw(twz, twz_g, NZ);
+  load_tw(twzf, twzf_g, NZF);
+  const int ky = blockIdx.x, kx0 = blockIdx.y * TX, p = blockIdx.z;
+  const int tw = min(TX, n0 - kx0);
+  const long nplane = (long)n0 * n1;
+  const int nsx = n0 + 1, nsy = n1 + 1;
+  const V* Ap = A + (long)p * NZ * nplane + (long)ky * n0 + kx0;
+  for (int i = threadIdx.x; i < NZ * TX; i += blockDim.x) {
+    const int z = i / TX, c = i - z * TX;
+    in[z * PI + c] = (c < tw) ? Ap[z * nplane + c] : mkc<V>(0, 0);
+  }
+  const ColMap m = colmap<TX>(ky, kx0, tw, n0, n1);
+  if (threadIdx.x < 2 * TX) {
+    const int c = threadIdx.x;
+    const bool valid = c < m.ncols && !(c < TX && c >= tw) && !(m.nyy && c >= TX && c - TX >= tw);
+    int ky_s = 0, kx_s = 0;
+    col_slot<TX>(m, c, ky, kx0, n0, n1, ky_s, kx_s);
+    colofs[c] = valid ? ky_s * nsx + kx_s : -1;
+  }
+  for (int i = threadIdx.x; i < NZF * PO; i += blockDim.x) out[i] = mkc<V>(0, 0);
+  __syncthreads();
+  smem_fft_cb<NZ, -1, PI, 1>(in, tw, twz);
+  __syncthreads();
+  V* Kp = K ? K + (long)p * NZ * nplane + (long)ky * n0 + kx0 : nullptr;
+  // k-point batches: field kf0 + p belongs to k-point (kf0 + p) / fpk
+  const T* ek = ekin + (long)((kf0 + p) / fpk) * kstride + (long)ky * n0 + kx0;
+  const bool splitrow = m.nyy;
+  for (int i = threadIdx.x; i < NZ * TX; i += blockDim.x) {
+    const int kz = i / TX, c = i - kz * TX;
+    if (c >= tw) continue;
+    const long g = kz * nplane + c;
+    const V v = cscale(in[kz * PI + c], inv_nc);
+    if (Kp) Kp[g] = cscale(v, ek[g]);
+    const bool nyz = (kz == NZ / 2);
+    const int fz = kz <= NZ / 2 ? kz : kz + (NZF - NZ);
+    const bool split = splitrow || (c == m.nyx_i);
+    if (cplx) {
+      // complex bands (idxFineGrid, fourier.cpp:291-311): a coarse Nyquist
+      // coefficient goes to the "+" fine position only; "-" slots stay zero
+      out[fz * PO + c] = v;
+    } else if (!split) {
+      if (nyz) {
+        out[(NZ / 2) * PO + c] = cscale(v, (T)0.5);
+        out[(NZF - NZ / 2) * PO + c] = cscale(v, (T)0.5);
+      } else {
+        out[fz * PO + c] = v;
+      }
+    } else {
+      const int cp = c, cm = splitrow ? TX + c : TX;
+      const V h = cscale(v, (T)0.5);
+      if (nyz) {
+        out[(NZ / 2) * PO + cp] = h;
+        out[(NZF - NZ / 2) * PO + cm] = h;
+      } else {
+        out[fz * PO + cp] = h;
+        out[fz * PO + cm] = h;
+      }
+    }
+  }
+  __syncthreads();
+  smem_fft_cb<NZF, +1, PO, 1>(out, m.ncols, twzf);
+  __syncthreads();
+  V* Bp = B + (long)p * NZF * nsy * nsx;
+  const long fplane = (long)nsy * nsx;
+  for_rows_cols(NZF, ncompact(m, tw), [&](int zf, int j) {
+    const int c = compact_col<TX>(j, tw);
+    Bp[zf * fplane + colofs[c]] = out[zf * PO + c];
+  });
+  // the two Nyquist corner slots that no coarse coefficient reaches
+  if (m.nyy && m.nyx_i >= 0) {
+    for (int zf = threadIdx.x; zf < NZF; zf += blockDim.x) {
+      Bp[((long)zf * nsy + n1 / 2) * nsx + n0] = mkc<V>(0, 0);
+      Bp[((long)zf * nsy + n1) * nsx + n0 / 2] = mkc<V>(0, 0);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// fine plane kernel (gather or apply mode)
+// ---------------------------------------------------------------------------
+struct NLArgs {
+  const int* ent_xy;
+  const void* ent_beta;
+  const int* tile_slot;
+  const int* slot_atom;
+  const int* slot_ent;
+  int nent, npmax, nchunk, cr;
+  bool present;
+};
+
+template <typename T, int NXF, int NYF, bool APPLY>
+__global__ void __launch_bounds__(PLANE_THREADS)
+k_fplane(VT<T>* __restrict__ BC, const T* __restrict__ vtot, NLArgs nl, VT<T>* __restrict__ Wp,
+         const VT<T>* __restrict__ W, int natom, int nslot, T inv_nf,
+         const VT<T>* twx_g, const VT<T>* twy_g) {
+  using V = VT<T>;
+  constexpr int n0 = NXF / 2, n1 = NYF / 2;
+  constexpr int nsx = n0 + 1, nsy = n1 + 1;
+  constexpr int PS = nsx;          // odd pitch
+  constexpr int PR = NXF + 1;      // odd pitch
+  const int CR = nl.cr;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  V* S = reinterpret_cast<V*>(smraw);     // [NYF][PS]
+  V* R = S + NYF * PS;                     // [CR][PR]
+  V* twx = R + CR * PR;
+  V* twy = twx + NXF;
+  load_tw(twx, twx_g, NXF);
+  load_tw(twy, twy_g, NYF);
+  const int zf = blockIdx.x, p = blockIdx.y;
+  const int NZF = gridDim.x;
+  V* Bp = BC + ((long)p * NZF + zf) * nsy * nsx;
+  for (int i = threadIdx.x; i < NYF * PS; i += blockDim.x) S[i] = mkc<V>(0, 0);
+  __syncthreads();
+  for (int i = threadIdx.x; i < nsy * nsx; i += blockDim.x) {
+    const int ys = i / nsx, xs = i - ys * nsx;
+    S[slot_fine(ys, n1, NYF) * PS + xs] = Bp[i];
+  }
+  __syncthreads();
+  smem_fft<NYF, +1>(S, nsx, PS, 1, twy);
+  __syncthreads();
+  const T* beta = reinterpret_cast<const T*>(nl.ent_beta);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int c = 0; c < nl.nchunk; ++c) {
+    const int y0 = c * CR;
+    for (int i = threadIdx.x; i < CR * PR; i += blockDim.x) R[i] = mkc<V>(0, 0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < CR * nsx; i += blockDim.x) {
+      const int yl = i / nsx, xs = i - yl * nsx;
+      R[yl * PR + slot_fine(xs, n0, NXF)] = S[(y0 + yl) * PS + xs];
+    }
+    __syncthreads();
+    smem_fft<NXF, +1>(R, CR, 1, PR, twx);
+    __syncthreads();
+    const int tile = zf * nl.nchunk + c;
+    if (!APPLY) {
+      if (nl.present) {
+        const int s0 = nl.tile_slot[tile], s1 = nl.tile_slot[tile + 1];
+        for (int s = s0 + warp; s < s1; s += nw) {
+          V acc[8];
+#pragma unroll
+          for (int q = 0; q < 8; ++q) acc[q] = mkc<V>(0, 0);
+          const int e0 = nl.slot_ent[s], e1 = nl.slot_ent[s + 1];
+          for (int e = e0 + lane; e < e1; e += 32) {
+            const int xy = nl.ent_xy[e];
+            const int yl = xy / NXF - y0, x = xy - (xy / NXF) * NXF;
+            const V v = R[yl * PR + x];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+              if (q < nl.npmax) {
+                const T b = beta[(long)q * nl.nent + e];
+                acc[q].x += b * v.x;
+                acc[q].y += b * v.y;
+              }
+            }
+          }
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            if (q < nl.npmax) {
+              T ax = acc[q].x, ay = acc[q].y;
+#pragma unroll
+              for (int o = 16; o > 0; o >>= 1) {
+                ax += __shfl_xor_sync(0xffffffffu, ax, o);
+                ay += __shfl_xor_sync(0xffffffffu, ay, o);
+              }
+              if (lane == 0) Wp[((long)p * nslot + s) * nl.npmax + q] = mkc<V>(ax, ay);
+            }
+          }
+        }
+      }
+      __syncthreads();
+    } else {
+      const T* vp = vtot + ((long)zf * NYF + y0) * NXF;
+      for (int i = threadIdx.x; i < CR * NXF; i += blockDim.x) {
+        const int yl = i / NXF, x = i - yl * NXF;
+        R[yl * PR + x] = cscale(R[yl * PR + x], vp[i]);
+      }
+      __syncthreads();
+      if (nl.present) {
+        const int s0 = nl.tile_slot[tile], s1 = nl.tile_slot[tile + 1];
+        for (int s = s0 + warp; s < s1; s += nw) {
+          const int a = nl.slot_atom[s];
+          V w[8];
+#pragma unroll
+          for (int q = 0; q < 8; ++q)
+            w[q] = (q < nl.npmax) ? W[((long)p * natom + a) * nl.npmax + q] : mkc<V>(0, 0);
+          const int e0 = nl.slot_ent[s], e1 = nl.slot_ent[s + 1];
+          for (int e = e0 + lane; e < e1; e += 32) {
+            const int xy = nl.ent_xy[e];
+            const int yl = xy / NXF - y0, x = xy - (xy / NXF) * NXF;
+            T ax = 0, ay = 0;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+              if (q < nl.npmax) {
+                const T b = beta[(long)q * nl.nent + e];
+                ax += b * w[q].x;
+                ay += b * w[q].y;
+              }
+            }
+            atomicAdd(&R[yl * PR + x].x, ax);
+            atomicAdd(&R[yl * PR + x].y, ay);
+          }
+        }
+      }
+      __syncthreads();
+      smem_fft<NXF, -1>(R, CR, 1, PR, twx);
+      __syncthreads();
+      for (int i = threadIdx.x; i < CR * nsx; i += blockDim.x) {
+        const int yl = i / nsx, xs = i - yl * nsx;
+        S[(y0 + yl) * PS + xs] = R[yl * PR + slot_fine(xs, n0, NXF)];
+      }
+      __syncthreads();
+    }
+  }
+  if (APPLY) {
+    smem_fft<NYF, -1>(S, nsx, PS, 1, twy);
+    __syncthreads();
+    for (int i = threadIdx.x; i < nsy * nsx; i += blockDim.x) {
+      const int ys = i / nsx, xs = i - ys * nsx;
+      Bp[i] = cscale(S[slot_fine(ys, n1, NYF) * PS + xs], inv_nf);
+    }
+  }
+}
+
+
+// ---------------------------------------------------------------------------
+// exact exchange pair fields (AddMultSpinorEXX, src/SCF/spinor.cpp:682-781).
+// Field f = (band k0 + f / njp, orbital pair jp = f % njp): the plane of
+// psi_k (phi_ja + i phi_jb), ja = j0 + 2 jp, jb = ja + 1 (zero past nphi),
+// forward 2-D FFT in shared memory, stored like k_cxy_fwd's output.
+// ---------------------------------------------------------------------------
+template <typename T, int N0, int N1>
+__global__ void __launch_bounds__(PLANE_THREADS)
+k_exx_fwd(const T* __restrict__ psi, int ld, int k0, const T* __restrict__ phi, int ldp, int j0, int nphi, int njp,
+          VT<T>* __restrict__ A, const VT<T>* twx_g, const VT<T>* twy_g) {
+  using V = VT<T>;
+  constexpr int P0 = N0 + 1;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  V* pl = reinterpret_cast<V*>(smraw);
+  V* twx = pl + N1 * P0;
+  V* twy = twx + N0;
+  load_tw(twx, twx_g, N0);
+  load_tw(twy, twy_g, N1);
+  const int z = blockIdx.x, f = blockIdx.y;
+  const int kk = f / njp, jp = f - kk * njp;
+  const long ntot_plane = (long)N0 * N1;
+  const int ja = j0 + 2 * jp, jb = ja + 1;
+  const T* pk = psi + (long)(k0 + kk) * ld + z * ntot_plane;
+  const T* pa = phi + (long)ja * ldp + z * ntot_plane;
+  const T* pb = (jb < nphi) ? phi + (long)jb * ldp + z * ntot_plane : nullptr;
+  for (int i = threadIdx.x; i < N0 * N1; i += blockDim.x) {
+    const int y = i / N0, x = i - y * N0;
+    const T v = pk[i];
+    pl[y * P0 + x] = mkc<V>(v * pa[i], pb ? v * pb[i] : (T)0);
+  }
+  __syncthreads();
+  smem_fft_cb<N0, -1, 1, P0>(pl, N1, twx);
+  __syncthreads();
+  smem_fft_cb<N1, -1, P0, 1>(pl, N0, twy);
+  __syncthreads();
+  const int N2 = gridDim.x;
+  V* Ap = A + ((long)f * N2 + z) * ntot_plane;
+  for (int i = threadIdx.x; i < N0 * N1; i += blockDim.x) {
+    const int y = i / N0, x = i - y * N0;
+    Ap[i] = pl[y * P0 + x];
+  }
+}
+
+// inverse 2-D FFT of the njp fields of band k0 + blockIdx.y on plane z and
+// out_k (+)= sum_jp w_ja phi_ja Re + w_jb phi_jb Im, accumulated in shared memory
+template <typename T, int N0, int N1>
+__global__ void __launch_bounds__(PLANE_THREADS)
+k_exx_inv(const VT<T>* __restrict__ A, int njp, const T* __restrict__ phi, int ldp, int j0, int nphi,
+          const T* __restrict__ wj, T* __restrict__ out, int ldo, int k0, int accumulate, const VT<T>* twx_g,
+          const VT<T>* twy_g) {
+  using V = VT<T>;
+  constexpr int P0 = N0 + 1;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  V* pl = reinterpret_cast<V*>(smraw);
+  V* twx = pl + N1 * P0;
+  V* twy = twx + N0;
+  T* acc = reinterpret_cast<T*>(twy + N1);
+  load_tw(twx, twx_g, N0);
+  load_tw(twy, twy_g, N1);
+  const int z = blockIdx.x, kk = blockIdx.y;
+  const int N2 = gridDim.x;
+  const long ntot_plane = (long)N0 * N1;
+  for (int i = threadIdx.x; i < N0 * N1; i += blockDim.x) acc[i] = (T)0;
+  for (int jp = 0; jp < njp; ++jp) {
+    const V* Dp = A + ((long)(kk * njp + jp) * N2 + z) * ntot_plane;
+    __syncthreads();
+    for (int i = threadIdx.x; i < N0 * N1; i += blockDim.x) {
+      const int y = i / N0, x = i - y * N0;
+      pl[y * P0 + x] = Dp[i];
+    }
+    __syncthreads();
+    smem_fft_cb<N1, +1, P0, 1>(pl, N0, twy);
+    __syncthreads();
+    smem_fft_cb<N0, +1, 1, P0>(pl, N1, twx);
+    __syncthreads();
+    const int ja = j0 + 2 * jp, jb = ja + 1;
+    const T wa = wj[ja], wb = (jb < nphi) ? wj[jb] : (T)0;
+    const T* pa = phi + (long)ja * ldp + z * ntot_plane;
+    const T* pb = (jb < nphi) ? phi + (long)jb * ldp + z * ntot_plane : pa;
+    for (int i = threadIdx.x; i < N0 * N1; i += blockDim.x) {
+      const int y = i / N0, x = i - y * N0;
+      const V v = pl[y * P0 + x];
+      acc[i] += wa * pa[i] * v.x + wb * pb[i] * v.y;
+    }
+  }
+  __syncthreads();
+  T* o = out + (long)(k0 + kk) * ldo + z * ntot_plane;
+  for (int i = threadIdx.x; i < N0 * N1; i += blockDim.x) o[i] = accumulate ? o[i] + acc[i] : acc[i];
+}
+
+// ---------------------------------------------------------------------------
+// fine plane, local potential only (the projectors are applied on the coarse
+// grid as dense GEMMs): IFFT y on the slot columns, then per warp a group of
+// rows: IFFT x, * V_loc, FFT x, truncate; FFT y; truncate.  MODE 1 starts
+// from two real fine-grid fields instead (used to build the coarse projector
+// matrix) and skips the inverse transforms and the potential.
+// ---------------------------------------------------------------------------
+constexpr int FLOC_THREADS = 256;
+
+template <typename T, int NXF, int NYF, int MODE>
+__global__ void __launch_bounds__(FLOC_THREADS, sizeof(T) == 4 ? 3 : 1)
+k_floc(VT<T>* __restrict__ BC, const T* __restrict__ vtot, const T* __restrict__ fin, long fin_pair_stride,
+       T inv_nf, const VT<T>* twx_g, const VT<T>* twy_g, int deriv = 0, T gfac = 0) {
+  using V = VT<T>;
+  constexpr int n0 = NXF / 2, n1 = NYF / 2;
+  constexpr int nsx = n0 + 1, nsy = n1 + 1;
+  constexpr int PS = nsx;
+  constexpr int PR = NXF + 1;
+  constexpr int F = FftGroup<NXF>::f;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  V* S = reinterpret_cast<V*>(smraw);          // [NYF][PS]
+  V* twx = S + NYF * PS;
+  V* twy = twx + NXF;
+  V* Rall = twy + NYF;                          // [nwarps][F][PR]
+  load_tw(twx, twx_g, NXF);
+  load_tw(twy, twy_g, NYF);
+  const int zf = blockIdx.x, p = blockIdx.y;
+  const int NZF = gridDim.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  V* Rw = Rall + warp * F * PR;
+  V* Bp = BC + ((long)p * NZF + zf) * nsy * nsx;
+  if (MODE == 0) {
+    for (int i = threadIdx.x; i < NYF * PS; i += blockDim.x) S[i] = mkc<V>(0, 0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < nsy * nsx; i += blockDim.x) {
+      const int ys = i / nsx, xs = i - ys * nsx;
+      S[slot_fine(ys, n1, NYF) * PS + xs] = Bp[i];
+    }
+    __syncthreads();
+    smem_fft_cb<NYF, +1, PS, 1>(S, nsx, twy);
+  }
+  __syncthreads();
+  for (int r0 = warp * F; r0 < NYF; r0 += nw * F) {
+    const int nr = min(F, NYF - r0);
+    if (MODE == 0) {
+      for (int i = lane; i < F * PR; i += 32) Rw[i] = mkc<V>(0, 0);
+      __syncwarp();
+      for (int i = lane; i < nr * nsx; i += 32) {
+        const int f = i / nsx, xs = i - f * nsx;
+        Rw[f * PR + slot_fine(xs, n0, NXF)] = S[(r0 + f) * PS + xs];
+      }
+      __syncwarp();
+      smem_fft_c<NXF, +1, 1, PR>(Rw, nr, twx, 0, 1);
+      const T* vp = vtot + ((long)zf * NYF + r0) * NXF;
+      for (int i = lane; i < nr * NXF; i += 32) {
+        const int f = i / NXF, x = i - f * NXF;
+        Rw[f * PR + x] = cscale(Rw[f * PR + x], vp[i]);
+      }
+    } else {
+      const T* fa = fin + (long)(2 * p) * fin_pair_stride + ((long)zf * NYF + r0) * NXF;
+      const T* fb = fin + (long)(2 * p + 1) * fin_pair_stride + ((long)zf * NYF + r0) * NXF;
+      for (int i = lane; i < nr * NXF; i += 32) {
+        const int f = i / NXF, x = i - f * NXF;
+        Rw[f * PR + x] = mkc<V>(fa[i], fb[i]);
+      }
+    }
+    __syncwarp();
+    smem_fft_c<NXF, -1, 1, PR>(Rw, nr, twx, 0, 1);
+    if (MODE == 1 && deriv == 1) {
+      // spectral d/dx: multiply by i G_x of the fine frequency
+      for (int i = lane; i < nr * NXF; i += 32) {
+        const int f = i / NXF, x = i - f * NXF;
+        const T g = gfac * (T)sgn_idx(x, NXF);
+        const V v = Rw[f * PR + x];
+        Rw[f * PR + x] = mkc<V>(-g * v.y, g * v.x);
+      }
+      __syncwarp();
+    }
+    for (int i = lane; i < nr * nsx; i += 32) {
+      const int f = i / nsx, xs = i - f * nsx;
+      S[(r0 + f) * PS + xs] = Rw[f * PR + slot_fine(xs, n0, NXF)];
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+  smem_fft_cb<NYF, -1, PS, 1>(S, nsx, twy);
+  __syncthreads();
+  if (MODE == 1 && deriv == 2) {
+    for (int i = threadIdx.x; i < NYF * nsx; i += blockDim.x) {
+      const int y = i / nsx, xs = i - y * nsx;
+      const T g = gfac * (T)sgn_idx(y, NYF);
+      const V v = S[y * PS + xs];
+      S[y * PS + xs] = mkc<V>(-g * v.y, g * v.x);
+    }
+    __syncthreads();
+  }
+  for (int i = threadIdx.x; i < nsy * nsx; i += blockDim.x) {
+    const int ys = i / nsx, xs = i - ys * nsx;
+    Bp[i] = cscale(S[slot_fine(ys, n1, NYF) * PS + xs], inv_nf);
+  }
+}
+
+
+// ---------------------------------------------------------------------------
+// density: rho(r) += w_a |Re psi_f|^2 + w_b |Im psi_f|^2 over the pairs of a
+// chunk (CalculateDensity, src/SCF/hamiltonian.cpp:2511-2547).  One CTA owns
+// one fine plane for `ppc` pairs and keeps its partial sums in registers.
+// ---------------------------------------------------------------------------
+template <typename T, int NXF, int NYF>
+__global__ void __launch_bounds__(FLOC_THREADS)
+k_fdens(const VT<T>* __restrict__ BC, int npair, int ppc, const double* __restrict__ w, double* __restrict__ rho,
+        const VT<T>* twx_g, const VT<T>* twy_g) {
+  using V = VT<T>;
+  constexpr int n0 = NXF / 2, n1 = NYF / 2;
+  constexpr int nsx = n0 + 1, nsy = n1 + 1;
+  constexpr int PS = nsx;
+  constexpr int PR = NXF + 1;
+  constexpr int F = FftGroup<NXF>::f;
+  constexpr int NW = FLOC_THREADS / 32;
+  constexpr int RG = (NYF + NW * F - 1) / (NW * F);
+  constexpr int EPL = (F * NXF + 31) / 32;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  V* S = reinterpret_cast<V*>(smraw);
+  V* twx = S + NYF * PS;
+  V* twy = twx + NXF;
+  V* Rall = twy + NYF;
+  load_tw(twx, twx_g, NXF);
+  load_tw(twy, twy_g, NYF);
+  const int zf = blockIdx.x;
+  const int NZF = gridDim.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  V* Rw = Rall + warp * F * PR;
+  double acc[RG][EPL];
+#pragma unroll
+  for (int a = 0; a < RG; ++a)
+#pragma unroll
+    for (int k = 0; k < EPL; ++k) acc[a][k] = 0.0;
+  const int p0 = blockIdx.y * ppc, p1 = min(npair, p0 + ppc);
+  for (int p = p0; p < p1; ++p) {
+    const V* Bp = BC + ((long)p * NZF + zf) * nsy * nsx;
+    const double wa = w[2 * p], wb = w[2 * p + 1];
+    __syncthreads();
+    for (int i = threadIdx.x; i < NYF * PS; i += blockDim.x) S[i] = mkc<V>(0, 0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < nsy * nsx; i += blockDim.x) {
+      const int ys = i / nsx, xs = i - ys * nsx;
+      S[slot_fine(ys, n1, NYF) * PS + xs] = Bp[i];
+    }
+    __syncthreads();
+    smem_fft_cb<NYF, +1, PS, 1>(S, nsx, twy);
+    __syncthreads();
+#pragma unroll
+    for (int rg = 0; rg < RG; ++rg) {
+      const int r0 = (warp + rg * NW) * F;
+      if (r0 < NYF) {
+        const int nr = min(F, NYF - r0);
+        for (int i = lane; i < F * PR; i += 32) Rw[i] = mkc<V>(0, 0);
+        __syncwarp();
+        for (int i = lane; i < nr * nsx; i += 32) {
+          const int f = i / nsx, xs = i - f * nsx;
+          Rw[f * PR + slot_fine(xs, n0, NXF)] = S[(r0 + f) * PS + xs];
+        }
+        __syncwarp();
+        smem_fft_c<NXF, +1, 1, PR>(Rw, nr, twx, 0, 1);
+#pragma unroll
+        for (int k = 0; k < EPL; ++k) {
+          const int i = lane + 32 * k;
+          if (i < nr * NXF) {
+            const int f = i / NXF, x = i - f * NXF;
+            const V v = Rw[f * PR + x];
+            acc[rg][k] += wa * (double)v.x * (double)v.x + wb * (double)v.y * (double)v.y;
+          }
+        }
+        __syncwarp();
+      }
+    }
+  }
+#pragma unroll
+  for (int rg = 0; rg < RG; ++rg) {
+    const int r0 = (warp + rg * NW) * F;
+    if (r0 < NYF) {
+      const int nr = min(F, NYF - r0);
+#pragma unroll
+      for (int k = 0; k < EPL; ++k) {
+        const int i = lane + 32 * k;
+        if (i < nr * NXF) atomicAdd(&rho[((long)zf * NYF + r0) * NXF + i], acc[rg][k]);
+      }
+    }
+  }
+}
+
+// projector fields: field[l][idx] = beta for the projectors of one batch
+template <typename T>
+__global__ void k_scatter_beta(T* __restrict__ fields, long nf, const int* __restrict__ idx,
+                               const double* __restrict__ beta, const long* __restrict__ pidx_off,
+                               const long* __restrict__ pbeta_off, const int* __restrict__ pnpts, int l0, int nl) {
+  const int l = blockIdx.y;
+  if (l0 + l >= nl) return;
+  const long io = pidx_off[l0 + l], bo = pbeta_off[l0 + l];
+  const int np = pnpts[l0 + l];
+  T* f = fields + (long)l * nf;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np; i += gridDim.x * blockDim.x) f[idx[io + i]] = (T)beta[bo + i];
+}
+
+// complex projector field conj(e^{i k.d}) beta for projector l0 + l into the
+// real / imaginary field pair (2l, 2l + 1); d = grid point - atom (Cartesian)
+template <typename T>
+__global__ void k_scatter_beta_k(T* __restrict__ fields, long nf, const int* __restrict__ idx,
+                                 const double* __restrict__ beta, const double* __restrict__ disp,
+                                 const long* __restrict__ pidx_off, const long* __restrict__ pbeta_off,
+                                 const int* __restrict__ pnpts, int l0, int nl, double kx, double ky, double kz) {
+  const int l = blockIdx.y;
+  if (l0 + l >= nl) return;
+  const long io = pidx_off[l0 + l], bo = pbeta_off[l0 + l];
+  const int np = pnpts[l0 + l];
+  T* fr = fields + (long)(2 * l) * nf;
+  T* fi = fr + nf;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < np; i += gridDim.x * blockDim.x) {
+    const double* d = disp + 3 * (io + i);
+    double sn, cs;
+    sincos(kx * d[0] + ky * d[1] + kz * d[2], &sn, &cs);
+    const double b = beta[bo + i];
+    fr[idx[io + i]] = (T)(b * cs);
+    fi[idx[io + i]] = (T)(-b * sn);
+  }
+}
+
+// complex W[l][b] *= d[l] (d real)
+template <typename T>
+__global__ void k_scale_rows_c(VT<T>* __restrict__ W, const T* __restrict__ d, int nproj, int nb) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i < (long)nproj * nb) W[i] = cscale(W[i], d[i % nproj]);
+}
+
+// W[l][b] *= d[l]  (W column-major nproj x nb)
+template <typename T>
+__global__ void k_scale_rows(T* __restrict__ W, const T* __restrict__ d, int nproj, int nb) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i < (long)nproj * nb) W[i] *= d[i % nproj];
+}
+
+// W[p][a][q] = wgt[a][q] * sum over the atom's slots of Wp[p][slot][q]
+template <typename T>
+__global__ void k_nl_reduce(const VT<T>* __restrict__ Wp, VT<T>* __restrict__ W, const int* atom_slot,
+                            const int* atom_slot_list, const T* wgt, int natom, int nslot, int npmax) {
+  using V = VT<T>;
+  const int p = blockIdx.y;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= natom * npmax) return;
+  const int a = i / npmax, q = i - a * npmax;
+  T sx = 0, sy = 0;
+  for (int j = atom_slot[a]; j < atom_slot[a + 1]; ++j) {
+    const V v = Wp[((long)p * nslot + atom_slot_list[j]) * npmax + q];
+    sx += v.x;
+    sy += v.y;
+  }
+  const T g = wgt[i];
+  W[(long)p * natom * npmax + i] = mkc<V>(sx * g, sy * g);
+}
+
+// ---------------------------------------------------------------------------
+// z pencils: fine FFT z, fold to coarse (IP_f2c), add kinetic, coarse IFFT z
+// ---------------------------------------------------------------------------
+template <typename T, int NZ, int NZF, int TX>
+__global__ void __launch_bounds__(PENCIL_THREADS, sizeof(T) == 4 ? 4 : 1)
+k_zfold(const VT<T>* __restrict__ C, const VT<T>* __restrict__ K, VT<T>* __restrict__ D, int n0, int n1,
+        const VT<T>* twz_g, const VT<T>* twzf_g, int deriv = 0, T gfac = 0, int cplx = 0) {
+  using V = VT<T>;
+  constexpr int PI = 2 * TX + 1;
+  constexpr int PA = TX + 1;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  V* in = reinterpret_cast<V*>(smraw);    // [NZF][PI]
+  V* acc = in + NZF * PI;                 // [NZ][PA]
+  V* twz = acc + NZ * PA;
+  V* twzf = twz + NZ;
+  __shared__ int colofs[2 * TX];          // slot offset of input column c in a fine plane, -1 if unused
+  load_tw(twz, twz_g, NZ);
+  load_tw(twzf, twzf_g, NZF);
+  const int ky = blockIdx.x, kx0 = blockIdx.y * TX, p = blockIdx.z;
+  const int tw = min(TX, n0 - kx0);
+  const ColMap m = colmap<TX>(ky, kx0, tw, n0, n1);
+  const int nsx = n0 + 1, nsy = n1 + 1;
+  if (threadIdx.x < 2 * TX) {
+    const int c = threadIdx.x;
+    const bool valid = c < m.ncols && !(c < TX && c >= tw) && !(m.nyy && c >= TX && c - TX >= tw);
+    int ky_s = 0, kx_s = 0;
+    col_slot<TX>(m, c, ky, kx0, n0, n1, ky_s, kx_s);
+    colofs[c] = valid ? ky_s * nsx + kx_s : -1;
+  }
+  __syncthreads();
+  const V* Cp = C + (long)p * NZF * nsy * nsx;
+  const long fplane = (long)nsy * nsx;
+  // columns the FFT reads but no slot feeds (c < ncols, not in the compact list)
+  if (tw < TX) {
+    for (int i = threadIdx.x; i < NZF * 2 * TX; i += blockDim.x) {
+      const int zf = i / (2 * TX), c = i - zf * (2 * TX);
+      if (c < m.ncols && colofs[c] < 0) in[zf * PI + c] = mkc<V>(0, 0);
+    }
+  }
+  for_rows_cols(NZF, ncompact(m, tw), [&](int zf, int j) {
+    const int c = compact_col<TX>(j, tw);
+    in[zf * PI + c] = Cp[zf * fplane + colofs[c]];
+  });
+  __syncthreads();
+  smem_fft_cb<NZF, -1, PI, 1>(in, m.ncols, twzf);
+  __syncthreads();
+  if (deriv == 3) {
+    // spectral d/dz before the fold: multiply by i G_z of the fine frequency
+    for (int i = threadIdx.x; i < NZF * 2 * TX; i += blockDim.x) {
+      const int zf = i / (2 * TX), c = i - zf * (2 * TX);
+      if (c >= m.ncols) continue;
+      const T g = gfac * (T)sgn_idx(zf, NZF);
+      const V v = in[zf * PI + c];
+      in[zf * PI + c] = mkc<V>(-g * v.y, g * v.x);
+    }
+    __syncthreads();
+  }
+  const long nplane = (long)n0 * n1;
+  const V* Kp = K ? K + (long)p * NZ * nplane + (long)ky * n0 + kx0 : nullptr;
+  const bool splitrow = m.nyy;
+  for (int i = threadIdx.x; i < NZ * TX; i += blockDim.x) {
+    const int kz = i / TX, c = i - kz * TX;
+    if (c >= tw) { acc[kz * PA + c] = mkc<V>(0, 0); continue; }
+    V v = Kp ? Kp[kz * nplane + c] : mkc<V>(0, 0);
+    const bool nyz = (kz == NZ / 2);
+    const int fz = kz <= NZ / 2 ? kz : kz + (NZF - NZ);
+    const bool split = splitrow || (c == m.nyx_i);
+    if (cplx) {
+      // complex bands: the "+" fine position only (idxFineGrid pick)
+      v = cadd(v, in[fz * PI + c]);
+    } else if (!split) {
+      if (nyz) v = cadd(v, cscale(cadd(in[(NZ / 2) * PI + c], in[(NZF - NZ / 2) * PI + c]), (T)0.5));
+      else v = cadd(v, in[fz * PI + c]);
+    } else {
+      const int cp = c, cm = splitrow ? TX + c : TX;
+      if (nyz) v = cadd(v, cscale(cadd(in[(NZ / 2) * PI + cp], in[(NZF - NZ / 2) * PI + cm]), (T)0.5));
+      else v = cadd(v, cscale(cadd(in[fz * PI + cp], in[fz * PI + cm]), (T)0.5));
+    }
+    acc[kz * PA + c] = v;
+  }
+  __syncthreads();
+  smem_fft_cb<NZ, +1, PA, 1>(acc, tw, twz);
+  __syncthreads();
+  V* Dp = D + (long)p * NZ * nplane + (long)ky * n0 + kx0;
+  for (int i = threadIdx.x; i < NZ * TX; i += blockDim.x) {
+    const int z = i / TX, c = i - z * TX;
+    if (c < tw) Dp[z * nplane + c] = acc[z * PA + c];
+  }
+}
+
+// z pencils for the Teter preconditioner: FFT z, * teter / N_c, IFFT z
+template <typename T, int NZ, int TX>
+__global__ void __launch_bounds__(PENCIL_THREADS, sizeof(T) == 4 ? 4 : 1)
+k_zteter(VT<T>* __restrict__ A, const T* __restrict__ teter, int n0, int n1, T inv_nc, const VT<T>* twz_g) {
+  using V = VT<T>;
+  constexpr int PI = TX + 1;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  V* in = reinterpret_cast<V*>(smraw);
+  V* twz = in + NZ * PI;
+  load_tw(twz, twz_g, NZ);
+  const int ky = blockIdx.x, kx0 = blockIdx.y * TX, p = blockIdx.z;
+  const int tw = min(TX, n0 - kx0);
+  const long nplane = (long)n0 * n1;
+  V* Ap = A + (long)p * NZ * nplane;
+  for (int i = threadIdx.x; i < NZ * TX; i += blockDim.x) {
+    const int z = i / TX, c = i - z * TX;
+    in[z * PI + c] = (c < tw) ? Ap[z * nplane + (long)ky * n0 + kx0 + c] : mkc<V>(0, 0);
+  }
+  __syncthreads();
+  smem_fft_cb<NZ, -1, PI, 1>(in, tw, twz);
+  __syncthreads();
+  for (int i = threadIdx.x; i < NZ * TX; i += blockDim.x) {
+    const int kz = i / TX, c = i - kz * TX;
+    if (c < tw) in[kz * PI + c] = cscale(in[kz * PI + c], teter[kz * nplane + (long)ky * n0 + kx0 + c] * inv_nc);
+  }
+  __syncthreads();
+  smem_fft_cb<NZ, +1, PI, 1>(in, tw, twz);
+  __syncthreads();
+  for (int i = threadIdx.x; i < NZ * TX; i += blockDim.x) {
+    const int z = i / TX, c = i - z * TX;
+    if (c < tw) Ap[z * nplane + (long)ky * n0 + kx0 + c] = in[z * PI + c];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// coarse plane inverse: D -> hpsi (two real bands)
+// ---------------------------------------------------------------------------
+template <typename T, int N0, int N1, bool CPLX = false>
+__global__ void __launch_bounds__(PLANE_THREADS)
+k_cxy_inv(const VT<T>* __restrict__ D, T* __restrict__ out, int ldo, int nband, int band0, int accumulate,
+          const VT<T>* twx_g, const VT<T>* twy_g) {
+  using V = VT<T>;
+  constexpr int P0 = N0 + 1;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  V* pl = reinterpret_cast<V*>(smraw);
+  V* twx = pl + N1 * P0;
+  V* twy = twx + N0;
+  load_tw(twx, twx_g, N0);
+  load_tw(twy, twy_g, N1);
+  const int z = blockIdx.x, p = blockIdx.y;
+  const int N2 = gridDim.x;
+  const long ntot_plane = (long)N0 * N1;
+  const V* Dp = D + ((long)p * N2 + z) * ntot_plane;
+  for (int i = threadIdx.x; i < N0 * N1; i += blockDim.x) {
+    const int y = i / N0, x = i - y * N0;
+    pl[y * P0 + x] = Dp[i];
+  }
+  __syncthreads();
+  smem_fft_cb<N1, +1, P0, 1>(pl, N0, twy);
+  __syncthreads();
+  smem_fft_cb<N0, +1, 1, P0>(pl, N1, twx);
+  __syncthreads();
+  if (CPLX) {
+    V* oc = reinterpret_cast<V*>(out) + (long)(band0 + p) * ldo + z * ntot_plane;
+    for (int i = threadIdx.x; i < N0 * N1; i += blockDim.x) {
+      const int y = i / N0, x = i - y * N0;
+      const V v = pl[y * P0 + x];
+      oc[i] = accumulate ? cadd(oc[i], v) : v;
+    }
+    return;
+  }
+  const int ba = band0 + 2 * p, bb = ba + 1;
+  T* oa = out + (long)ba * ldo + z * ntot_plane;
+  T* ob = (bb < nband) ? out + (long)bb * ldo + z * ntot_plane : nullptr;
+  for (int i = threadIdx.x; i < N0 * N1; i += blockDim.x) {
+    const int y = i / N0, x = i - y * N0;
+    const V v = pl[y * P0 + x];
+    if (accumulate) {
+      oa[i] += v.x;
+      if (ob) ob[i] += v.y;
+    } else {
+      oa[i] = v.x;
+      if (ob) ob[i] = v.y;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host-side launch plan for one (precision, grid) instantiation
+// ---------------------------------------------------------------------------
+// Records a launch; when profiling is on, brackets it with events on the stream.
+struct Launch {
+  pw_ctx* c;
+  cudaStream_t st;
+  int kind;
+  cudaEvent_t a = nullptr, b = nullptr;
+  static cudaEvent_t take(pw_ctx* c) {
+    if (!c->ev_pool.empty()) {
+      cudaEvent_t e = c->ev_pool.back();
+      c->ev_pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+  }
+  Launch(pw_ctx* c_, cudaStream_t st_, int kind_) : c(c_), st(st_), kind(kind_) {
+    if (kind == KK_LIBGEMM) c->lib_launches++; else c->launches++;
+    if (c->prof_on) {
+      a = take(c);
+      b = take(c);
+      cudaEventRecord(a, st);
+    }
+  }
+  ~Launch() {
+    if (a) {
+      cudaEventRecord(b, st);
+      c->prof.push_back({kind, a, b});
+    }
+  }
+};
+
+template <typename T> static int fplane_cr(int NXF, int NYF) {
+  // rows per chunk so that S + R (+ twiddles) fit in ~200 KB of shared memory
+  const size_t vs = sizeof(T) * 2;
+  const size_t S = (size_t)NYF * (NXF / 2 + 1) * vs;
+  const size_t budget = 200 * 1024;
+  int best = 1;
+  for (int cr = 1; cr <= NYF; ++cr) {
+    if (NYF % cr) continue;
+    if (S + (size_t)cr * (NXF + 1) * vs + (NXF + NYF) * vs <= budget) best = cr;
+  }
+  return best;
+}
+
+template <typename T, int N0, int N1, int N2>
+struct Plan {
+  static constexpr int TX = PencilTile<T, N0>::v;
+  static constexpr int TXF = TX;   // z-fold tile width
+  using V = VT<T>;
+  static constexpr int NF0 = 2 * N0, NF1 = 2 * N1, NF2 = 2 * N2;
+
+  static int chunk_rows() { return fplane_cr<T>(NF0, NF1); }
+
+  static size_t sm_cxy() { return sizeof(V) * (N1 * (N0 + 1) + N0 + N1); }
+  static size_t sm_zpad() { return sizeof(V) * (N2 * (TX + 1) + NF2 * (2 * TX + 1) + N2 + NF2); }
+  static size_t sm_zfold() { return sizeof(V) * (NF2 * (2 * TXF + 1) + N2 * (TXF + 1) + N2 + NF2); }
+  static size_t sm_zteter() { return sizeof(V) * (N2 * (TX + 1) + N2); }
+  static size_t sm_exx_inv() { return sm_cxy() + sizeof(T) * N0 * N1; }
+  static size_t sm_floc() {
+    return sizeof(V) * ((size_t)NF1 * (N0 + 1) + NF0 + NF1 + (size_t)(FLOC_THREADS / 32) * FftGroup<NF0>::f * (NF0 + 1));
+  }
+  static size_t sm_fplane(int cr) {
+    return sizeof(V) * ((size_t)NF1 * (N0 + 1) + (size_t)cr * (NF0 + 1) + NF0 + NF1);
+  }
+
+  static int set_attrs() {
+    static bool done = false;
+    if (done) return PW_OK;
+    const int cr = chunk_rows();
+    PWB_CUDA(cudaFuncSetAttribute(k_fplane<T, NF0, NF1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_fplane(cr)));
+    PWB_CUDA(cudaFuncSetAttribute(k_fplane<T, NF0, NF1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_fplane(cr)));
+    PWB_CUDA(cudaFuncSetAttribute(k_zpad<T, N2, NF2, TX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_zpad()));
+    PWB_CUDA(cudaFuncSetAttribute(k_zfold<T, N2, NF2, TXF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_zfold()));
+    PWB_CUDA(cudaFuncSetAttribute(k_cxy_fwd<T, N0, N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_cxy()));
+    PWB_CUDA(cudaFuncSetAttribute(k_cxy_inv<T, N0, N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_cxy()));
+    PWB_CUDA(cudaFuncSetAttribute(k_zteter<T, N2, TX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_zteter()));
+    PWB_CUDA(cudaFuncSetAttribute(k_floc<T, NF0, NF1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_floc()));
+    PWB_CUDA(cudaFuncSetAttribute(k_floc<T, NF0, NF1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_floc()));
+    done = true;
+    return PW_OK;
+  }
+
+  static const V* tw(pw_ctx* c, int i) { return reinterpret_cast<const V*>(c->tw[i].p); }
+
+  // one batch of npair band pairs starting at band0
+  static int hpsi_batch(pw_ctx* c, const T* psi, int ld, T* out, int ldo, int nband, int band0, int npair,
+                        int accumulate, cudaStream_t st) {
+    int rc = set_attrs();
+    if (rc) return rc;
+    V* AD = reinterpret_cast<V*>(c->s_ad.p);
+    V* K = reinterpret_cast<V*>(c->s_k.p);
+    V* BC = reinterpret_cast<V*>(c->s_bc.p);
+    V* Wp = reinterpret_cast<V*>(c->s_wp.p);
+    V* W = reinterpret_cast<V*>(c->s_w.p);
+    const T inv_nc = (T)(1.0 / (double)c->ntot);
+    const T inv_nf = (T)(1.0 / (double)c->ntotf);
+    const int ntx = (N0 + TX - 1) / TX;
+    { Launch L_(c, st, KK_CXY_FWD);
+    k_cxy_fwd<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(psi, ld, nband, band0, AD, tw(c, 0), tw(c, 1)); }
+    { Launch L_(c, st, KK_ZPAD);
+    k_zpad<T, N2, NF2, TX><<<dim3(N1, ntx, npair), PENCIL_THREADS, sm_zpad(), st>>>(
+        AD, K, BC, reinterpret_cast<const T*>(c->ekin.p), N0, N1, inv_nc, tw(c, 2), tw(c, 5)); }
+    if (c->nl_mode == PW_NL_DENSE) {
+      { Launch L_(c, st, KK_FPLANE_APPLY);
+      k_floc<T, NF0, NF1, 0><<<dim3(NF2, npair), FLOC_THREADS, sm_floc(), st>>>(
+          BC, reinterpret_cast<const T*>(c->vtot.p), nullptr, 0, inv_nf, tw(c, 3), tw(c, 4)); }
+      { Launch L_(c, st, KK_ZFOLD);
+      k_zfold<T, N2, NF2, TXF><<<dim3(N1, (N0 + TXF - 1) / TXF, npair), PENCIL_THREADS, sm_zfold(), st>>>(BC, K, AD, N0, N1, tw(c, 2), tw(c, 5)); }
+      { Launch L_(c, st, KK_CXY_INV);
+      k_cxy_inv<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(AD, out, ldo, nband, band0, accumulate, tw(c, 0), tw(c, 1)); }
+      PWB_CUDA(cudaGetLastError());
+      const int nb = std::min(2 * npair, nband - band0);
+      if (c->have_nl && c->nproj > 0 && nb > 0)
+        if ((rc = dense_apply(c, nl_set(c), psi + (long)band0 * ld, ld, out + (long)band0 * ldo, ldo, nb, st)))
+          return rc;
+      return exchange_batch(c, psi, ld, out, ldo, nband, band0, npair, st);
+    }
+    NLArgs nl{};
+    const int cr = chunk_rows();
+    nl.cr = cr;
+    nl.nchunk = NF1 / cr;
+    nl.present = c->have_nl && c->nl.nent > 0;
+    int natom = 0, nslot = 0;
+    if (nl.present) {
+      nl.ent_xy = reinterpret_cast<const int*>(c->nl.ent_xy.p);
+      nl.ent_beta = c->nl.ent_beta.p;
+      nl.tile_slot = reinterpret_cast<const int*>(c->nl.tile_slot.p);
+      nl.slot_atom = reinterpret_cast<const int*>(c->nl.slot_atom.p);
+      nl.slot_ent = reinterpret_cast<const int*>(c->nl.slot_ent.p);
+      nl.nent = c->nl.nent;
+      nl.npmax = c->nl.npmax;
+      natom = c->nl.natom;
+      nslot = c->nl.nslot;
+      if (c->nl.cr != cr) { set_error("projector tables built for another chunk size"); return PW_EINVAL; }
+      { Launch L_(c, st, KK_FPLANE_GATHER);
+    k_fplane<T, NF0, NF1, false><<<dim3(NF2, npair), PLANE_THREADS, sm_fplane(cr), st>>>(
+          BC, reinterpret_cast<const T*>(c->vtot.p), nl, Wp, W, natom, nslot, inv_nf, tw(c, 3), tw(c, 4)); }
+      const int nthr = 128;
+      { Launch L_(c, st, KK_NL_REDUCE);
+    k_nl_reduce<T><<<dim3((natom * nl.npmax + nthr - 1) / nthr, npair), nthr, 0, st>>>(
+          Wp, W, reinterpret_cast<const int*>(c->nl.atom_slot.p), reinterpret_cast<const int*>(c->nl.atom_slot_list.p),
+          reinterpret_cast<const T*>(c->nl.wgt.p), natom, nslot, nl.npmax); }
+    }
+    { Launch L_(c, st, KK_FPLANE_APPLY);
+    k_fplane<T, NF0, NF1, true><<<dim3(NF2, npair), PLANE_THREADS, sm_fplane(cr), st>>>(
+        BC, reinterpret_cast<const T*>(c->vtot.p), nl, Wp, W, natom, nslot, inv_nf, tw(c, 3), tw(c, 4)); }
+    { Launch L_(c, st, KK_ZFOLD);
+    k_zfold<T, N2, NF2, TXF><<<dim3(N1, (N0 + TXF - 1) / TXF, npair), PENCIL_THREADS, sm_zfold(), st>>>(BC, K, AD, N0, N1, tw(c, 2), tw(c, 5)); }
+    { Launch L_(c, st, KK_CXY_INV);
+    k_cxy_inv<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(AD, out, ldo, nband, band0, accumulate, tw(c, 0), tw(c, 1)); }
+    PWB_CUDA(cudaGetLastError());
+    return exchange_batch(c, psi, ld, out, ldo, nband, band0, npair, st);
+  }
+
+  // exact exchange of the batch's bands: the ACE operator (two GEMMs) or the
+  // full pair-FFT exchange, depending on the context's hybrid mode
+  static int exchange_batch(pw_ctx* c, const T* psi, int ld, T* out, int ldo, int nband, int band0, int npair,
+                            cudaStream_t st) {
+    const int nb = std::min(2 * npair, nband - band0);
+    if (nb <= 0 || c->exx_mode == PW_EXX_OFF) return PW_OK;
+    if (c->exx_mode == PW_EXX_ACE) {
+      if (c->ace_n == 0) return PW_OK;
+      DenseSet ds{c->ace_xi.p, c->ace_qd.p, c->ace_bf.p, c->ace_t_bf.p, c->ace_n, c->ace_npad};
+      return dense_apply(c, ds, psi + (long)band0 * ld, ld, out + (long)band0 * ldo, ldo, nb, st);
+    }
+    return exx_apply(c, psi + (long)band0 * ld, ld, nb, out + (long)band0 * ldo, ldo, 1, st);
+  }
+
+  static DenseSet nl_set(pw_ctx* c) { return DenseSet{c->q.p, c->qd.p, c->q_bf.p, c->qt_bf.p, c->nproj, c->nproj_pad}; }
+
+  // out (+)= V_x psi, AddMultSpinorEXX (src/SCF/spinor.cpp:682-781): for every
+  // band k and exchange orbital j, out_k -= alpha f_j phi_j (1/N_c) IFFT(v FFT(psi_k phi_j)).
+  // Two orbitals share one complex field (v is real and even, so the real and
+  // imaginary parts stay separate); batches of (band, orbital pair) fields.
+  static int exx_apply(pw_ctx* c, const T* psi, int ld, int nb, T* out, int ldo, int accumulate, cudaStream_t st) {
+    int rc = set_attrs();
+    if (rc) return rc;
+    static bool attr = false;
+    if (!attr) {
+      PWB_CUDA(cudaFuncSetAttribute(k_exx_fwd<T, N0, N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_cxy()));
+      PWB_CUDA(cudaFuncSetAttribute(k_exx_inv<T, N0, N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_exx_inv()));
+      attr = true;
+    }
+    const int nphi = c->exx_nphi;
+    if (nphi == 0 || nb == 0) {
+      if (!accumulate && nb > 0)
+        PWB_CUDA(cudaMemset2DAsync(out, (size_t)ldo * sizeof(T), 0, (size_t)c->ntot * sizeof(T), nb, st));
+      return PW_OK;
+    }
+    const long nt = c->ntot;
+    const int njp = (nphi + 1) / 2;
+    const long cap = std::max<long>(1, (long)(c->exx_scratch_bytes / ((size_t)nt * sizeof(V))));
+    const int jc = (int)std::min<long>(njp, std::max<long>(1, cap / nb));
+    const int kc = (int)std::max<long>(1, std::min<long>(nb, cap / jc));
+    if ((rc = c->s_exx.alloc((size_t)kc * jc * nt * sizeof(V)))) return rc;
+    V* A = reinterpret_cast<V*>(c->s_exx.p);
+    const T* phi = reinterpret_cast<const T*>(c->exx_phi.p);
+    const T* wj = reinterpret_cast<const T*>(c->exx_w.p);
+    const T* kern = reinterpret_cast<const T*>(c->exx_kern.p);
+    const T inv_nc = (T)(1.0 / (double)nt);
+    const int ntx = (N0 + TX - 1) / TX;
+    for (int k0 = 0; k0 < nb; k0 += kc) {
+      const int nk = std::min(kc, nb - k0);
+      for (int jp0 = 0; jp0 < njp; jp0 += jc) {
+        const int nj = std::min(jc, njp - jp0);
+        { Launch L_(c, st, KK_EXX);
+        k_exx_fwd<T, N0, N1><<<dim3(N2, nk * nj), PLANE_THREADS, sm_cxy(), st>>>(
+            psi, ld, k0, phi, (int)nt, 2 * jp0, nphi, nj, A, tw(c, 0), tw(c, 1)); }
+        { Launch L_(c, st, KK_EXX);
+        k_zteter<T, N2, TX><<<dim3(N1, ntx, nk * nj), PENCIL_THREADS, sm_zteter(), st>>>(A, kern, N0, N1, inv_nc, tw(c, 2)); }
+        { Launch L_(c, st, KK_EXX);
+        k_exx_inv<T, N0, N1><<<dim3(N2, nk), PLANE_THREADS, sm_exx_inv(), st>>>(
+            A, nj, phi, (int)nt, 2 * jp0, nphi, wj, out, ldo, k0, (accumulate || jp0 > 0) ? 1 : 0, tw(c, 0),
+            tw(c, 1)); }
+        PWB_CUDA(cudaGetLastError());
+      }
+    }
+    return PW_OK;
+  }
+
+  // H psi += Q diag(qd) Q^T psi  for nb bands (column-major, ld); Q is the
+  // coarse projector matrix or the ACE vectors (qd = -1)
+  static int dense_apply(pw_ctx* c, const DenseSet& ds, const T* psi, int ld, T* out, int ldo, int nb,
+                         cudaStream_t st) {
+    if constexpr (std::is_same<T, float>::value) {
+      if (c->gemm_mode == 0) return dense_apply_tc(c, ds, psi, ld, out, ldo, nb, st);
+    }
+    cublasHandle_t h = (cublasHandle_t)c->blas;
+    if (cublasSetStream(h, st) != CUBLAS_STATUS_SUCCESS) { set_error("cublasSetStream failed"); return PW_ECUDA; }
+    const int np = ds.np, nt = (int)c->ntot;
+    int rc;
+    if ((rc = c->s_wq.alloc((size_t)np * nb * sizeof(T)))) return rc;
+    T* W = reinterpret_cast<T*>(c->s_wq.p);
+    const T* Q = reinterpret_cast<const T*>(ds.q);
+    const T one = 1, zero = 0;
+    cublasStatus_t r;
+    { Launch L_(c, st, KK_LIBGEMM);
+    if constexpr (std::is_same<T, double>::value)
+      r = cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, np, nb, nt, &one, Q, nt, psi, ld, &zero, W, np);
+    else
+      r = cublasSgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, np, nb, nt, &one, Q, nt, psi, ld, &zero, W, np); }
+    if (r != CUBLAS_STATUS_SUCCESS) { set_error("projector GEMM (Q^T psi) failed"); return PW_ECUDA; }
+    { Launch L_(c, st, KK_MISC);
+    k_scale_rows<T><<<(unsigned)(((long)np * nb + 255) / 256), 256, 0, st>>>(W, reinterpret_cast<const T*>(ds.qd), np, nb); }
+    { Launch L_(c, st, KK_LIBGEMM);
+    if constexpr (std::is_same<T, double>::value)
+      r = cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, nt, nb, np, &one, Q, nt, W, np, &one, out, ldo);
+    else
+      r = cublasSgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, nt, nb, np, &one, Q, nt, W, np, &one, out, ldo); }
+    if (r != CUBLAS_STATUS_SUCCESS) { set_error("projector GEMM (Q W) failed"); return PW_ECUDA; }
+    PWB_CUDA(cudaGetLastError());
+    return PW_OK;
+  }
+
+  // rho += sum over the batch's bands of w_b |psi_b,fine|^2 (unnormalised)
+  static int density_batch(pw_ctx* c, const T* psi, int ld, int nband, int band0, int npair, const double* w,
+                           double* rho, cudaStream_t st) {
+    int rc = set_attrs();
+    if (rc) return rc;
+    static bool attr = false;
+    if (!attr) {
+      PWB_CUDA(cudaFuncSetAttribute(k_fdens<T, NF0, NF1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_floc()));
+      attr = true;
+    }
+    V* AD = reinterpret_cast<V*>(c->s_ad.p);
+    V* BC = reinterpret_cast<V*>(c->s_bc.p);
+    const T inv_nc = (T)(1.0 / (double)c->ntot);
+    const int ntx = (N0 + TX - 1) / TX;
+    { Launch L_(c, st, KK_DENSITY);
+    k_cxy_fwd<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(psi, ld, nband, band0, AD, tw(c, 0), tw(c, 1)); }
+    { Launch L_(c, st, KK_DENSITY);
+    k_zpad<T, N2, NF2, TX><<<dim3(N1, ntx, npair), PENCIL_THREADS, sm_zpad(), st>>>(
+        AD, nullptr, BC, reinterpret_cast<const T*>(c->ekin.p), N0, N1, inv_nc, tw(c, 2), tw(c, 5)); }
+    const int ppc = std::max(1, std::min(8, npair));
+    { Launch L_(c, st, KK_DENSITY);
+    k_fdens<T, NF0, NF1><<<dim3(NF2, (npair + ppc - 1) / ppc), FLOC_THREADS, sm_floc(), st>>>(
+        BC, npair, ppc, w + 2 * (band0 / 2), rho, tw(c, 3), tw(c, 4)); }
+    PWB_CUDA(cudaGetLastError());
+    return PW_OK;
+  }
+
+  // FP32 context: split-BF16 tcgen05 GEMMs
+  static int dense_apply_tc(pw_ctx* c, const DenseSet& ds, const float* psi, int ld, float* out, int ldo, int nb,
+                            cudaStream_t st) {
+    const int np = ds.np, nt = (int)c->ntot, npp = ds.npp;
+    int rc;
+    if ((rc = c->s_psi_bf.alloc((size_t)2 * nb * nt * 2))) return rc;
+    if ((rc = c->s_w_bf.alloc((size_t)2 * nb * npp * 2))) return rc;
+    char* pb = (char*)c->s_psi_bf.p;
+    char* wb = (char*)c->s_w_bf.p;
+    { Launch L_(c, st, KK_MISC);
+    if ((rc = split_bf16(psi, ld, nt, nb, pb, pb + (size_t)nb * nt * 2, nt, 1.0f, st))) return rc; }
+    // W^T[b][l] = d_l * sum_g Q[l][g] psi[b][g]   (split-K, deterministic reduce)
+    SplitOperand A{ds.q_bf, (const char*)ds.q_bf + (size_t)np * nt * 2, np, nt};
+    SplitOperand B{pb, pb + (size_t)nb * nt * 2, nb, nt};
+    ReduceOut ro;
+    ro.transpose = 1;
+    ro.row_scale = reinterpret_cast<const float*>(ds.qd);
+    ro.bf_hi = wb;
+    ro.bf_lo = wb + (size_t)nb * npp * 2;
+    ro.ldb = npp;
+    { Launch L_(c, st, KK_GRAM);
+    if ((rc = gemm_tn_reduce(A, B, nt, c->gemm_terms, c->s_ws, ro, st))) return rc; }
+    // out[b][g] += sum_l QT[g][l] W^T[b][l]  (tile rows = grid points: coalesced stores)
+    SplitOperand W{wb, wb + (size_t)nb * npp * 2, nb, npp};
+    SplitOperand QT{ds.qt_bf, (const char*)ds.qt_bf + (size_t)nt * npp * 2, nt, npp};
+    { Launch L_(c, st, KK_GRAM);
+    if ((rc = gemm_tn_store(QT, W, np, c->gemm_terms, out, ldo, 1, st, 1))) return rc; }
+    return PW_OK;
+  }
+
+  // complex bands at Bloch vector k (Spinor::AddMultSpinorFine, complex
+  // version, src/SCF/spinor_complex.cpp:292-542): one band per complex field,
+  // idxFineGrid placement, kinetic 1/2 |k+G|^2, projectors with the Bloch phase
+  static int hpsi_batch_k(pw_ctx* c, const V* psi, int ld, V* out, int ldo, int band0, int nb, int accumulate,
+                          cudaStream_t st, int fpk = 1 << 30, const T* ekin_all = nullptr, const V* qk_all = nullptr) {
+    int rc = set_attrs();
+    if (rc) return rc;
+    static bool attr = false;
+    if (!attr) {
+      PWB_CUDA(cudaFuncSetAttribute(k_cxy_fwd<T, N0, N1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_cxy()));
+      PWB_CUDA(cudaFuncSetAttribute(k_cxy_inv<T, N0, N1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_cxy()));
+      attr = true;
+    }
+    V* AD = reinterpret_cast<V*>(c->s_ad.p);
+    V* K = reinterpret_cast<V*>(c->s_k.p);
+    V* BC = reinterpret_cast<V*>(c->s_bc.p);
+    const T inv_nc = (T)(1.0 / (double)c->ntot);
+    const T inv_nf = (T)(1.0 / (double)c->ntotf);
+    const int ntx = (N0 + TX - 1) / TX;
+    const T* pr = reinterpret_cast<const T*>(psi);
+    { Launch L_(c, st, KK_CXY_FWD);
+    k_cxy_fwd<T, N0, N1, true><<<dim3(N2, nb), PLANE_THREADS, sm_cxy(), st>>>(pr, ld, 0, band0, AD, tw(c, 0), tw(c, 1)); }
+    { Launch L_(c, st, KK_ZPAD);
+    k_zpad<T, N2, NF2, TX><<<dim3(N1, ntx, nb), PENCIL_THREADS, sm_zpad(), st>>>(
+        AD, K, BC, ekin_all ? ekin_all : reinterpret_cast<const T*>(c->ekin_k.p), N0, N1, inv_nc, tw(c, 2), tw(c, 5),
+        1, band0, fpk, ekin_all ? c->ntot : 0); }
+    { Launch L_(c, st, KK_FPLANE_APPLY);
+    k_floc<T, NF0, NF1, 0><<<dim3(NF2, nb), FLOC_THREADS, sm_floc(), st>>>(
+        BC, reinterpret_cast<const T*>(c->vtot.p), nullptr, 0, inv_nf, tw(c, 3), tw(c, 4)); }
+    { Launch L_(c, st, KK_ZFOLD);
+    k_zfold<T, N2, NF2, TXF><<<dim3(N1, (N0 + TXF - 1) / TXF, nb), PENCIL_THREADS, sm_zfold(), st>>>(
+        BC, K, AD, N0, N1, tw(c, 2), tw(c, 5), 0, (T)0, 1); }
+    { Launch L_(c, st, KK_CXY_INV);
+    k_cxy_inv<T, N0, N1, true><<<dim3(N2, nb), PLANE_THREADS, sm_cxy(), st>>>(AD, reinterpret_cast<T*>(out), ldo, 0,
+                                                                              band0, accumulate, tw(c, 0), tw(c, 1)); }
+    PWB_CUDA(cudaGetLastError());
+    if (c->nproj == 0 || !(qk_all ? qk_all : c->qk.p)) return PW_OK;
+    // V_nl psi = Q diag(d) Q^H psi with the complex coarse projector matrix Q of
+    // each k-point, one GEMM pair per k segment of the batch
+    for (int f = band0; f < band0 + nb;) {
+      const int kk = f / fpk;
+      const int f1 = (int)std::min<long>(band0 + nb, (long)(kk + 1) * fpk);
+      const V* Qk = qk_all ? qk_all + (long)kk * c->nproj * c->ntot : reinterpret_cast<const V*>(c->qk.p);
+      if ((rc = nl_k(c, Qk, psi + (long)f * ld, ld, out + (long)f * ldo, ldo, f1 - f, st))) return rc;
+      f = f1;
+    }
+    return PW_OK;
+  }
+
+  static int nl_k(pw_ctx* c, const V* Q, const V* x, int ld, V* y, int ldo, int nb, cudaStream_t st) {
+    int rc;
+    cublasHandle_t h = (cublasHandle_t)c->blas;
+    if (cublasSetStream(h, st) != CUBLAS_STATUS_SUCCESS) { set_error("cublasSetStream failed"); return PW_ECUDA; }
+    const int np = c->nproj, nt = (int)c->ntot;
+    if ((rc = c->s_wq.alloc((size_t)np * nb * sizeof(V)))) return rc;
+    V* W = reinterpret_cast<V*>(c->s_wq.p);
+    cublasStatus_t r;
+    { Launch L_(c, st, KK_LIBGEMM);
+    if constexpr (std::is_same<T, double>::value) {
+      const cuDoubleComplex one = make_cuDoubleComplex(1, 0), zero = make_cuDoubleComplex(0, 0);
+      r = cublasZgemm(h, CUBLAS_OP_C, CUBLAS_OP_N, np, nb, nt, &one, (const cuDoubleComplex*)Q, nt,
+                      (const cuDoubleComplex*)x, ld, &zero, (cuDoubleComplex*)W, np);
+    } else {
+      const cuComplex one = make_cuComplex(1, 0), zero = make_cuComplex(0, 0);
+      r = cublasCgemm(h, CUBLAS_OP_C, CUBLAS_OP_N, np, nb, nt, &one, (const cuComplex*)Q, nt, (const cuComplex*)x, ld,
+                      &zero, (cuComplex*)W, np);
+    } }
+    if (r != CUBLAS_STATUS_SUCCESS) { set_error("projector GEMM (Q^H psi) failed"); return PW_ECUDA; }
+    { Launch L_(c, st, KK_MISC);
+    k_scale_rows_c<T><<<(unsigned)(((long)np * nb + 255) / 256), 256, 0, st>>>(W, reinterpret_cast<const T*>(c->qdk.p),
+                                                                                np, nb); }
+    { Launch L_(c, st, KK_LIBGEMM);
+    if constexpr (std::is_same<T, double>::value) {
+      const cuDoubleComplex one = make_cuDoubleComplex(1, 0);
+      r = cublasZgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, nt, nb, np, &one, (const cuDoubleComplex*)Q, nt,
+                      (const cuDoubleComplex*)W, np, &one, (cuDoubleComplex*)y, ldo);
+    } else {
+      const cuComplex one = make_cuComplex(1, 0);
+      r = cublasCgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, nt, nb, np, &one, (const cuComplex*)Q, nt, (const cuComplex*)W, np,
+                      &one, (cuComplex*)y, ldo);
+    } }
+    if (r != CUBLAS_STATUS_SUCCESS) { set_error("projector GEMM (Q W) failed"); return PW_ECUDA; }
+    PWB_CUDA(cudaGetLastError());
+    return PW_OK;
+  }
+
+  // complex coarse projectors at Bloch vector k: q_l = T(conj(e^{i k.d}) beta_l),
+  // one projector per complex field, into Qout (complex, leading dimension ntot)
+  static int build_q_k(pw_ctx* c, const int* d_idx, const double* d_beta, const double* d_disp, const long* d_pio,
+                       const long* d_pbo, const int* d_pnp, int nproj, const double kv[3], V* Qout, cudaStream_t st) {
+    int rc = set_attrs();
+    if (rc) return rc;
+    static bool attr = false;
+    if (!attr) {
+      PWB_CUDA(cudaFuncSetAttribute(k_cxy_inv<T, N0, N1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_cxy()));
+      attr = true;
+    }
+    const int cap = c->pair_cap;                 // complex fields per pass
+    const long nf = c->ntotf;
+    DevBuf fields;
+    if ((rc = fields.alloc((size_t)2 * cap * nf * sizeof(T)))) return rc;
+    V* AD = reinterpret_cast<V*>(c->s_ad.p);
+    V* BC = reinterpret_cast<V*>(c->s_bc.p);
+    const T inv_nf = (T)(1.0 / (double)c->ntotf);
+    for (int l0 = 0; l0 < nproj; l0 += cap) {
+      const int nl = std::min(cap, nproj - l0);
+      PWB_CUDA(cudaMemsetAsync(fields.p, 0, (size_t)2 * nl * nf * sizeof(T), st));
+      k_scatter_beta_k<T><<<dim3(64, nl), 256, 0, st>>>(reinterpret_cast<T*>(fields.p), nf, d_idx, d_beta, d_disp, d_pio,
+                                                         d_pbo, d_pnp, l0, nproj, kv[0], kv[1], kv[2]);
+      k_floc<T, NF0, NF1, 1><<<dim3(NF2, nl), FLOC_THREADS, sm_floc(), st>>>(
+          BC, nullptr, reinterpret_cast<const T*>(fields.p), nf, inv_nf, tw(c, 3), tw(c, 4));
+      k_zfold<T, N2, NF2, TXF><<<dim3(N1, (N0 + TXF - 1) / TXF, nl), PENCIL_THREADS, sm_zfold(), st>>>(
+          BC, nullptr, AD, N0, N1, tw(c, 2), tw(c, 5), 0, (T)0, 1);
+      k_cxy_inv<T, N0, N1, true><<<dim3(N2, nl), PLANE_THREADS, sm_cxy(), st>>>(
+          AD, reinterpret_cast<T*>(Qout), (int)c->ntot, 0, l0, 0, tw(c, 0), tw(c, 1));
+      PWB_CUDA(cudaGetLastError());
+    }
+    PWB_CUDA(cudaStreamSynchronize(st));
+    return PW_OK;
+  }
+
+  // Build q_l = T(beta_l) for all projectors with the fine->coarse half of
+  // the pipeline, two projectors per complex field.
+  static int build_q(pw_ctx* c, const int* d_idx, const double* d_beta, const long* d_pio, const long* d_pbo,
+                     const int* d_pnp, int nproj, cudaStream_t st, int deriv = 0, T* Qout = nullptr) {
+    int rc = set_attrs();
+    if (rc) return rc;
+    const int cap = c->pair_cap;                 // pairs per pass
+    const long nf = c->ntotf;
+    DevBuf fields;
+    if ((rc = fields.alloc((size_t)2 * cap * nf * sizeof(T)))) return rc;
+    V* AD = reinterpret_cast<V*>(c->s_ad.p);
+    V* BC = reinterpret_cast<V*>(c->s_bc.p);
+    T* Q = Qout ? Qout : reinterpret_cast<T*>(c->q.p);
+    const T inv_nf = (T)(1.0 / (double)c->ntotf);
+    const int ntx = (N0 + TX - 1) / TX;
+    const T gx = (T)(2 * M_PI / c->L[0]), gy = (T)(2 * M_PI / c->L[1]), gz = (T)(2 * M_PI / c->L[2]);
+    for (int l0 = 0; l0 < nproj; l0 += 2 * cap) {
+      const int nl = std::min(2 * cap, nproj - l0);
+      const int npair = (nl + 1) / 2;
+      PWB_CUDA(cudaMemsetAsync(fields.p, 0, (size_t)2 * npair * nf * sizeof(T), st));
+      k_scatter_beta<T><<<dim3(64, nl), 256, 0, st>>>(reinterpret_cast<T*>(fields.p), nf, d_idx, d_beta, d_pio, d_pbo, d_pnp, l0, nproj);
+      k_floc<T, NF0, NF1, 1><<<dim3(NF2, npair), FLOC_THREADS, sm_floc(), st>>>(
+          BC, nullptr, reinterpret_cast<const T*>(fields.p), nf, inv_nf, tw(c, 3), tw(c, 4), deriv,
+          deriv == 1 ? gx : gy);
+      k_zfold<T, N2, NF2, TXF><<<dim3(N1, (N0 + TXF - 1) / TXF, npair), PENCIL_THREADS, sm_zfold(), st>>>(BC, nullptr, AD, N0, N1, tw(c, 2),
+                                                                                     tw(c, 5), deriv, gz);
+      k_cxy_inv<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(AD, Q, (int)c->ntot, nproj, l0, 0, tw(c, 0), tw(c, 1));
+      PWB_CUDA(cudaGetLastError());
+    }
+    PWB_CUDA(cudaStreamSynchronize(st));
+    return PW_OK;
+  }
+
+  static int teter_batch(pw_ctx* c, const T* r, int ld, T* out, int ldo, int nband, int band0, int npair,
+                         int accumulate, cudaStream_t st) {
+    int rc = set_attrs();
+    if (rc) return rc;
+    V* AD = reinterpret_cast<V*>(c->s_ad.p);
+    const T inv_nc = (T)(1.0 / (double)c->ntot);
+    const int ntx = (N0 + TX - 1) / TX;
+    { Launch L_(c, st, KK_CXY_FWD);
+    k_cxy_fwd<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(r, ld, nband, band0, AD, tw(c, 0), tw(c, 1)); }
+    { Launch L_(c, st, KK_ZTETER);
+    k_zteter<T, N2, TX><<<dim3(N1, ntx, npair), PENCIL_THREADS, sm_zteter(), st>>>(
+        AD, reinterpret_cast<const T*>(c->teter.p), N0, N1, inv_nc, tw(c, 2)); }
+    { Launch L_(c, st, KK_CXY_INV);
+    k_cxy_inv<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(AD, out, ldo, nband, band0, accumulate, tw(c, 0), tw(c, 1)); }
+    PWB_CUDA(cudaGetLastError());
+    return PW_OK;
+  }
+
+  // Teter preconditioner with caller-provided device scratch (npair complex
+  // coarse fields); launches kernels only, allocates nothing.
+  static int teter_batch_scratch(pw_ctx* c, const T* r, int ld, T* out, int ldo, int nband, int band0, int npair,
+                                 int accumulate, cudaStream_t st, void* scratch) {
+    int rc = set_attrs();
+    if (rc) return rc;
+    V* AD = reinterpret_cast<V*>(scratch);
+    const T inv_nc = (T)(1.0 / (double)c->ntot);
+    const int ntx = (N0 + TX - 1) / TX;
+    c->launches += 3;
+    k_cxy_fwd<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(r, ld, nband, band0, AD, tw(c, 0), tw(c, 1));
+    k_zteter<T, N2, TX><<<dim3(N1, ntx, npair), PENCIL_THREADS, sm_zteter(), st>>>(
+        AD, reinterpret_cast<const T*>(c->teter.p), N0, N1, inv_nc, tw(c, 2));
+    k_cxy_inv<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(AD, out, ldo, nband, band0, accumulate,
+                                                                            tw(c, 0), tw(c, 1));
+    PWB_CUDA(cudaGetLastError());
+    return PW_OK;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// dispatch over the instantiated grids
+// ---------------------------------------------------------------------------
+
+template <typename T, int N0, int N1, int N2>
+static int hpsi_thunk(pw_ctx* c, const void* psi, int ld, void* out, int ldo, int nband, int band0, int npair,
+                      int acc, cudaStream_t st) {
+  return Plan<T, N0, N1, N2>::hpsi_batch(c, (const T*)psi, ld, (T*)out, ldo, nband, band0, npair, acc, st);
+}
+template <typename T, int N0, int N1, int N2>
+static int teter_thunk(pw_ctx* c, const void* psi, int ld, void* out, int ldo, int nband, int band0, int npair,
+                       int acc, cudaStream_t st) {
+  return Plan<T, N0, N1, N2>::teter_batch(c, (const T*)psi, ld, (T*)out, ldo, nband, band0, npair, acc, st);
+}
+template <typename T, int N0, int N1, int N2> static int cr_thunk() { return Plan<T, N0, N1, N2>::chunk_rows(); }
+template <typename T, int N0, int N1, int N2>
+static int teter_scratch_thunk(pw_ctx* c, const void* r, int ld, void* out, int ldo, int nband, int band0, int npair,
+                               int acc, cudaStream_t st, void* scratch) {
+  return Plan<T, N0, N1, N2>::teter_batch_scratch(c, (const T*)r, ld, (T*)out, ldo, nband, band0, npair, acc, st,
+                                                  scratch);
+}
+template <typename T, int N0, int N1, int N2>
+static int dens_thunk(pw_ctx* c, const void* psi, int ld, int nband, int band0, int npair, const double* w, double* rho,
+                      cudaStream_t st) {
+  return Plan<T, N0, N1, N2>::density_batch(c, (const T*)psi, ld, nband, band0, npair, w, rho, st);
+}
+template <typename T, int N0, int N1, int N2>
+static int buildq_thunk(pw_ctx* c, const int* a, const double* b, const long* d, const long* e, const int* f, int n,
+                        cudaStream_t st, int deriv, void* out) {
+  return Plan<T, N0, N1, N2>::build_q(c, a, b, d, e, f, n, st, deriv, (T*)out);
+}
+
+template <typename T, int N0, int N1, int N2>
+static int exx_thunk(pw_ctx* c, const void* psi, int ld, int nb, void* out, int ldo, int acc, cudaStream_t st) {
+  return Plan<T, N0, N1, N2>::exx_apply(c, (const T*)psi, ld, nb, (T*)out, ldo, acc, st);
+}
+
+template <typename T, int N0, int N1, int N2>
+static int ace_thunk(pw_ctx* c, const void* psi, int ld, int nb, void* out, int ldo, int acc, cudaStream_t st) {
+  (void)acc;
+  DenseSet ds{c->ace_xi.p, c->ace_qd.p, c->ace_bf.p, c->ace_t_bf.p, c->ace_n, c->ace_npad};
+  return Plan<T, N0, N1, N2>::dense_apply(c, ds, (const T*)psi, ld, (T*)out, ldo, nb, st);
+}
+
+template <typename T, int N0, int N1, int N2>
+static int hpsik_thunk(pw_ctx* c, const void* psi, int ld, void* out, int ldo, int band0, int nb, int acc,
+                       cudaStream_t st) {
+  using V = VT<T>;
+  return Plan<T, N0, N1, N2>::hpsi_batch_k(c, (const V*)psi, ld, (V*)out, ldo, band0, nb, acc, st);
+}
+template <typename T, int N0, int N1, int N2>
+static int hpsikb_thunk(pw_ctx* c, const void* psi, int ld, void* out, int ldo, int band0, int nb, int acc,
+                        cudaStream_t st, int fpk, const void* ekin_all, const void* qk_all) {
+  using V = VT<T>;
+  return Plan<T, N0, N1, N2>::hpsi_batch_k(c, (const V*)psi, ld, (V*)out, ldo, band0, nb, acc, st, fpk,
+                                           (const T*)ekin_all, (const V*)qk_all);
+}
+template <typename T, int N0, int N1, int N2>
+static int buildqk_thunk(pw_ctx* c, const int* a, const double* b, const double* d, const long* e, const long* f,
+                         const int* g, int n, const double* kv, void* out, cudaStream_t st) {
+  return Plan<T, N0, N1, N2>::build_q_k(c, a, b, d, e, f, g, n, kv, (VT<T>*)out, st);
+}
+
+#define PWB_GRID_ENTRY(a, b, c)                                                                          \
+  {a, b, c, {hpsi_thunk<double, a, b, c>, hpsi_thunk<float, a, b, c>},                             \
+   {teter_thunk<double, a, b, c>, teter_thunk<float, a, b, c>},                                    \
+   {cr_thunk<double, a, b, c>, cr_thunk<float, a, b, c>},                                          \
+   {buildq_thunk<double, a, b, c>, buildq_thunk<float, a, b, c>},                                  \
+   {dens_thunk<double, a, b, c>, dens_thunk<float, a, b, c>},                                      \
+   {teter_scratch_thunk<double, a, b, c>, teter_scratch_thunk<float, a, b, c>},                    \
+   {exx_thunk<double, a, b, c>, exx_thunk<float, a, b, c>},                                        \
+   {ace_thunk<double, a, b, c>, ace_thunk<float, a, b, c>},                                        \
+   {hpsik_thunk<double, a, b, c>, hpsik_thunk<float, a, b, c>},                                    \
+   {buildqk_thunk<double, a, b, c>, buildqk_thunk<float, a, b, c>},                                \
+   {hpsikb_thunk<double, a, b, c>, hpsikb_thunk<float, a, b, c>}}
+
+}  // namespace pwb
