@@ -289,6 +289,53 @@ def exx_bench(device: int, reps: int = 3):
     return out
 
 
+def cells_bench(device: int, reps: int = 5):
+    """48 independent uneven cells (Si8/16/64, Al4/32, Ecut 8-20 Ha, grids
+    20^3-48^3, 12-160 bands) applied sequentially, on forked streams, and as
+    one captured CUDA graph; FP32, synthetic V_loc and bands."""
+    import torch
+    from pwdft_develop_b200 import CellBatch, Context
+    from pwdft_develop_b200.cells import uneven_cells
+    cells = uneven_cells(48)
+    rng = np.random.Generator(np.random.Philox(SEED + 11))
+    ctxs, psis, outs = [], [], []
+    for cell in cells:
+        c = Context(cell["length"], cell["numGrid"], cell["numGridFine"], precision="f32", device=device)
+        c.set_atoms([cell["znuc"]] * len(cell["positions"]), cell["positions"])
+        c.set_vtot(rng.uniform(-1.0, 0.5, c.ntotFine))
+        c.set_band_batch(cell["nband"])
+        x = torch.tensor(rng.standard_normal((cell["nband"], c.ntot)) / np.sqrt(c.ntot), dtype=torch.float32,
+                         device="cuda")
+        ctxs.append(c)
+        psis.append(x)
+        outs.append(torch.empty_like(x))
+    nbands = sum(c["nband"] for c in cells)
+    b = CellBatch(ctxs, psis, outs)
+    g = b.capture()
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    t_seq = timed(lambda: [c.hpsi(x, out=o) for c, x, o in zip(ctxs, psis, outs)])
+    t_bat = timed(b.hpsi)
+    t_gr = timed(g.replay)
+    nodes = g.nodes
+    g.close()
+    for c in ctxs:
+        c.close()
+    return {"workload": "48 seeded cells (Si8/16/64, Al4/32, Ecut 8-20 Ha, 20^3-48^3 grids), FP32",
+            "bands": nbands, "sequential_ms": t_seq, "streams_ms": t_bat, "graph_ms": t_gr, "graph_nodes": nodes,
+            "graph_bands_per_s": nbands / (t_gr / 1e3), "sequential_bands_per_s": nbands / (t_seq / 1e3)}
+
+
 def kpoint_bench(device: int, reps: int = 5):
     """Si8 complex bands on a 4x4x4 Monkhorst-Pack k-mesh (64 k-points, 24
     bands each, 24^3 / 48^3 grids, Ecut 10 Ha) in one batched H(k) psi pass, FP32."""
@@ -496,6 +543,8 @@ def run_ours(args):
             line["exx"] = exx_bench(local)
         if args.kpoints and world == 1:
             line["kpoints"] = kpoint_bench(local)
+        if args.cells and world == 1:
+            line["cells"] = cells_bench(local)
         if args.cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(args.cpu_bands)
         print(json.dumps(line), flush=True)
@@ -516,6 +565,7 @@ def main():
     ap.add_argument("--no-scf", dest="scf", action="store_false", help="skip the SCF time-to-solution leg")
     ap.add_argument("--no-exx", dest="exx", action="store_false", help="skip the hybrid-exchange leg")
     ap.add_argument("--no-kpoints", dest="kpoints", action="store_false", help="skip the k-point batch leg")
+    ap.add_argument("--no-cells", dest="cells", action="store_false", help="skip the uneven-cell batch leg")
     ap.add_argument("--cpu-bands", type=int, default=64)
     ap.add_argument("--bands", type=int, default=NBAND, help="band block size (profiling runs use a small block)")
     args = ap.parse_args()

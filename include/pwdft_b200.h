@@ -259,6 +259,15 @@ typedef struct pw_graph pw_graph;
 PW_API int pw_graph_capture_hpsi(pw_ctx* ctx, const void* psi, int ld, void* hpsi, int ldh, int nband,
                                  int accumulate, pw_graph** graph);
 PW_API int pw_graph_launch(pw_graph* graph, void* stream);
+/* H*psi for ncell independent contexts at once (cells of uneven grids, band
+ * counts and precisions on one device): cell c applies ctxs[c] to nband[c]
+ * bands psi[c] -> out[c] (overwrite), each cell's sweep on its own stream
+ * forked from `stream` and joined back into it.  pw_graph_capture_batch
+ * captures the whole batch as one CUDA graph (one launch per replay). */
+PW_API int pw_hpsi_batch(int ncell, pw_ctx* const* ctxs, const void* const* psi, const int* ld, void* const* out,
+                         const int* ldo, const int* nband, void* stream);
+PW_API int pw_graph_capture_batch(int ncell, pw_ctx* const* ctxs, const void* const* psi, const int* ld,
+                                  void* const* out, const int* ldo, const int* nband, pw_graph** graph);
 PW_API int pw_graph_nodes(const pw_graph* graph, long* nodes);
 PW_API int pw_graph_destroy(pw_graph* graph);
 

@@ -7,4 +7,4 @@ C++ host code behind the C ABI in ``include/pwdft_b200.h``); this package is
 a thin Python host mirror used by tests and benchmarks.
 """
 from ._lib import PwError, lib  # noqa: F401  (fails loudly if the library is missing)
-from .core import Context  # noqa: F401
+from .core import CellBatch, Context, HpsiGraph  # noqa: F401

@@ -98,6 +98,9 @@ SIGNATURES: dict[str, tuple] = {
     "pw_set_kpoint": (_i, [_vp, _dp]),
     "pw_graph_capture_hpsi": (_i, [_vp, _vp, _i, _vp, _i, _i, _i, C.POINTER(_vp)]),
     "pw_graph_launch": (_i, [_vp, _vp]),
+    "pw_hpsi_batch": (_i, [_i, C.POINTER(_vp), C.POINTER(_vp), _ip, C.POINTER(_vp), _ip, _ip, _vp]),
+    "pw_graph_capture_batch": (_i, [_i, C.POINTER(_vp), C.POINTER(_vp), _ip, C.POINTER(_vp), _ip, _ip,
+                                    C.POINTER(_vp)]),
     "pw_graph_nodes": (_i, [_vp, C.POINTER(_l)]),
     "pw_graph_destroy": (_i, [_vp]),
     "pw_hpsi_k": (_i, [_vp, _vp, _i, _vp, _i, _i, _i, _vp]),

@@ -499,6 +499,33 @@ class HpsiGraph:
         self.close()
 
 
+class CellBatch:
+    """Independent contexts applied together: hpsi() runs every cell's H*psi
+    on forked streams (pw_hpsi_batch); capture() records the whole batch as
+    one CUDA graph and returns an object whose replay() launches it."""
+
+    def __init__(self, ctxs, psis, outs):
+        n = len(ctxs)
+        self._keep = (list(ctxs), list(psis), list(outs))
+        self._n = n
+        self._c = (C.c_void_p * n)(*[c._h for c in ctxs])
+        self._p = (C.c_void_p * n)(*[p.data_ptr() for p in psis])
+        self._o = (C.c_void_p * n)(*[o.data_ptr() for o in outs])
+        self._ld = (C.c_int * n)(*[c.ntot for c in ctxs])
+        self._nb = (C.c_int * n)(*[p.shape[0] for p in psis])
+
+    def hpsi(self, stream=None):
+        check(lib.pw_hpsi_batch(self._n, self._c, self._p, self._ld, self._o, self._ld, self._nb, _stream(stream)))
+
+    def capture(self):
+        h = C.c_void_p()
+        check(lib.pw_graph_capture_batch(self._n, self._c, self._p, self._ld, self._o, self._ld, self._nb,
+                                         C.byref(h)))
+        g = HpsiGraph.__new__(HpsiGraph)
+        g._ctx, g._keep, g._g = None, self._keep, h
+        return g
+
+
 def _ctx_capture_hpsi(self, psi, out, accumulate: bool = False) -> HpsiGraph:
     return HpsiGraph(self, psi, out, accumulate)
 
