@@ -420,6 +420,7 @@ def run_ours(args):
     ctx.set_vtot(synthetic_vtot(ctx.ntotFine))
     ctx.set_atoms(z, pos)
     ctx.set_band_batch(NBAND)
+    tune = ctx.autotune(NBAND)          # set-up (untimed): band batch and projector GEMM tiles
     dt_t = ctx.torch_dtype
     g = torch.Generator(device="cuda").manual_seed(SEED + rank)
     X = torch.randn((NBAND, ctx.ntot), dtype=torch.float64, device="cuda", generator=g)
@@ -481,7 +482,7 @@ def run_ours(args):
     npts_total = sum(len(hgh_atom_projectors(L, NF, 14, p)[0]) for p in pos)
     # tile slots ~ atoms x fine planes they touch (exact count from the library is not exported)
     nslot_est = int(natom * (2 * 3.5 / (2 * A_CELL) * NF[2] + 1))
-    alg = algorithmic_bytes(dom_kind, NBAND // 2, s, npts_total, 5, nslot_est, natom)
+    alg = algorithmic_bytes(dom_kind, tune["band_batch"] // 2, s, npts_total, 5, nslot_est, natom)
     achieved = alg / (kern[dom_name]["avg_us"] * 1e-6) / 1e9
     peak, peak_kind = load_peaks()
     traffic = None
@@ -523,7 +524,8 @@ def run_ours(args):
             "scaling": "weak", "vs_baseline": None, "dtype": prec, "data": "synthetic",
             "config": {"workload": WORKLOAD, "grid": list(NC), "fine_grid": list(NF), "bands": NBAND,
                        "nonlocal": "dense coarse-grid projector matrix (GEMM)",
-                       "band_batch": NBAND, "l2": "flushed between steps (256 MB device write)",
+                       "band_batch": tune["band_batch"], "gemm_tiles": [tune["gemm_bn"], tune["gemm_bn_store"]],
+                       "l2": "flushed between steps (256 MB device write)",
                        "parallelism": f"band blocks, {world} replica(s)"},
             "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,

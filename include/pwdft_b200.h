@@ -251,6 +251,23 @@ PW_API int pw_ctx_build_twin(pw_ctx* ctx);
  * doubles; rho_out: host, N_fine doubles (either may be NULL). */
 PW_API int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* eig_out, double* rho_out);
 
+/* Autotuner (no reference counterpart): times pw_hpsi on an internal block
+ * of nband bands for candidate band-batch widths and, for FP32 contexts with
+ * dense projectors, the tile widths of the two projector GEMMs; applies the
+ * fastest setting to the context and caches it for later contexts of the
+ * same grid, precision, band count and projector count (then cached = 1 and
+ * no timing runs).  The local potential must be set. */
+typedef struct pw_tune_result {
+  int band_batch;           /* bands per internal batch chosen */
+  int gemm_bn;              /* Q^T psi GEMM tile width (0: heuristic) */
+  int gemm_bn_store;        /* Q W GEMM tile width (0: heuristic) */
+  int tried;                /* configurations timed */
+  int cached;               /* 1: taken from the cache */
+  double ms_default;        /* sweep time with the defaults */
+  double ms_best;           /* sweep time with the chosen setting */
+} pw_tune_result;
+PW_API int pw_autotune(pw_ctx* ctx, int nband, pw_tune_result* result);
+
 /* CUDA graph of one pw_hpsi call (same pointers, band count and accumulate
  * flag on every replay; the inputs' contents may change between replays).
  * The capture runs one ordinary call first (outside the graph).  Replays

@@ -56,6 +56,11 @@ class ScfResult(C.Structure):
                 ("sub_s", C.c_double * 4)]
 
 
+class TuneResult(C.Structure):
+    _fields_ = [("band_batch", C.c_int), ("gemm_bn", C.c_int), ("gemm_bn_store", C.c_int), ("tried", C.c_int),
+                ("cached", C.c_int), ("ms_default", C.c_double), ("ms_best", C.c_double)]
+
+
 # name -> (restype, argtypes); every name here is declared in include/pwdft_b200.h
 SIGNATURES: dict[str, tuple] = {
     "pw_last_error": (C.c_char_p, []),
@@ -98,6 +103,7 @@ SIGNATURES: dict[str, tuple] = {
     "pw_set_kpoint": (_i, [_vp, _dp]),
     "pw_graph_capture_hpsi": (_i, [_vp, _vp, _i, _vp, _i, _i, _i, C.POINTER(_vp)]),
     "pw_graph_launch": (_i, [_vp, _vp]),
+    "pw_autotune": (_i, [_vp, _i, C.POINTER(TuneResult)]),
     "pw_hpsi_batch": (_i, [_i, C.POINTER(_vp), C.POINTER(_vp), _ip, C.POINTER(_vp), _ip, _ip, _vp]),
     "pw_graph_capture_batch": (_i, [_i, C.POINTER(_vp), C.POINTER(_vp), _ip, C.POINTER(_vp), _ip, _ip,
                                     C.POINTER(_vp)]),

@@ -530,6 +530,14 @@ def _ctx_capture_hpsi(self, psi, out, accumulate: bool = False) -> HpsiGraph:
     return HpsiGraph(self, psi, out, accumulate)
 
 
+def _ctx_autotune(self, nband: int) -> dict:
+    """pw_autotune: pick band-batch width and projector GEMM tiles by timing."""
+    r = _lib.TuneResult()
+    check(lib.pw_autotune(self._h, int(nband), C.byref(r)))
+    return {k: getattr(r, k) for k, _ in r._fields_}
+
+
+Context.autotune = _ctx_autotune
 Context.capture_hpsi = _ctx_capture_hpsi
 Context.set_kpoints = _ctx_set_kpoints
 Context.hpsi_kbatch = _ctx_hpsi_kbatch

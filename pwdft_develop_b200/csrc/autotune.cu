@@ -1,0 +1,149 @@
+// Autotuner for the H*psi sweep: times pw_hpsi on a scratch block for
+// candidate band-batch widths and, for FP32 contexts with projectors, the
+// tile widths of the two projector GEMMs (coordinate descent), keeps the
+// fastest setting in the context and caches it per (grid, precision, bands,
+// projectors) for later contexts of the same shape.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <map>
+#include <mutex>
+#include <tuple>
+#include <vector>
+
+#include "common.hpp"
+
+namespace pwb {
+
+template <typename T>
+__global__ void k_fill_hash(T* x, long n, unsigned seed, double scale) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    unsigned h = (unsigned)i * 2654435761u ^ seed;
+    h ^= h >> 16;
+    h *= 2246822519u;
+    h ^= h >> 13;
+    x[i] = (T)(scale * ((double)(h & 0xffffff) / 8388608.0 - 1.0));
+  }
+}
+
+using TuneKey = std::tuple<int, int, int, int, int, int>;
+struct TuneVal {
+  int band_batch, bn, bn_store;
+};
+static std::mutex g_tune_mu;
+static std::map<TuneKey, TuneVal>& tune_cache() {
+  static std::map<TuneKey, TuneVal> m;
+  return m;
+}
+
+}  // namespace pwb
+
+using namespace pwb;
+
+extern "C" {
+
+int pw_autotune(pw_ctx* ctx, int nband, pw_tune_result* res) {
+  PWB_CHECK(ctx && nband > 0, PW_EINVAL, "bad arguments");
+  PWB_CHECK(ctx->have_vtot, PW_ENOTREADY, "local potential not set (pw_set_vtot)");
+  PWB_CHECK(!ctx->prof_on, PW_EINVAL, "per-kernel profiling is on (pw_profile)");
+  PWB_CUDA(cudaSetDevice(ctx->device));
+  const long nt = ctx->ntot;
+  const TuneKey key{ctx->n[0], ctx->n[1], ctx->n[2], ctx->prec, nband, ctx->nproj};
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = tune_cache().find(key);
+    if (it != tune_cache().end()) {
+      int rc = pw_set_band_batch(ctx, it->second.band_batch);
+      if (rc) return rc;
+      ctx->gemm_bn = it->second.bn;
+      ctx->gemm_bn_store = it->second.bn_store;
+      if (res) {
+        *res = pw_tune_result{};
+        res->band_batch = it->second.band_batch;
+        res->gemm_bn = it->second.bn;
+        res->gemm_bn_store = it->second.bn_store;
+        res->cached = 1;
+      }
+      return PW_OK;
+    }
+  }
+  DevBuf X, Y;
+  int rc;
+  if ((rc = X.alloc((size_t)nband * nt * ctx->esz)) || (rc = Y.alloc((size_t)nband * nt * ctx->esz))) return rc;
+  const double sc = 1.0 / std::sqrt((double)nt);
+  if (ctx->prec == PW_F64) k_fill_hash<double><<<1024, 256>>>((double*)X.p, (long)nband * nt, 12345u, sc);
+  else k_fill_hash<float><<<1024, 256>>>((float*)X.p, (long)nband * nt, 12345u, sc);
+  PWB_CUDA(cudaGetLastError());
+  cudaEvent_t e0, e1;
+  PWB_CUDA(cudaEventCreate(&e0));
+  PWB_CUDA(cudaEventCreate(&e1));
+  int tried = 0;
+  auto run = [&](int bb, int bn, int bns, double* ms) -> int {
+    int q = pw_set_band_batch(ctx, bb);
+    if (q) return q;
+    ctx->gemm_bn = bn;
+    ctx->gemm_bn_store = bns;
+    if ((q = pw_hpsi(ctx, X.p, (int)nt, Y.p, (int)nt, nband, 0, nullptr))) return q;   // warm-up
+    double best = 1e30;
+    for (int r = 0; r < 3; ++r) {
+      PWB_CUDA(cudaEventRecord(e0));
+      if ((q = pw_hpsi(ctx, X.p, (int)nt, Y.p, (int)nt, nband, 0, nullptr))) return q;
+      PWB_CUDA(cudaEventRecord(e1));
+      PWB_CUDA(cudaEventSynchronize(e1));
+      float t = 0;
+      PWB_CUDA(cudaEventElapsedTime(&t, e0, e1));
+      best = std::min(best, (double)t);
+    }
+    ++tried;
+    *ms = best;
+    return PW_OK;
+  };
+  double t_def = 0;
+  if ((rc = run(nband, 0, 0, &t_def))) return rc;
+  int best_bb = nband, best_bn = 0, best_bns = 0;
+  double best = t_def;
+  std::vector<int> bbs;
+  for (int c : {nband / 2, 256, 128, 96, 64, 32}) {
+    const int e = std::max(2, c + (c & 1));
+    if (e < nband && std::find(bbs.begin(), bbs.end(), e) == bbs.end()) bbs.push_back(e);
+  }
+  for (int bb : bbs) {
+    double t;
+    if ((rc = run(bb, 0, 0, &t))) return rc;
+    if (t < best) { best = t; best_bb = bb; }
+  }
+  if (ctx->prec == PW_F32 && ctx->have_nl && ctx->nl_mode == PW_NL_DENSE && ctx->gemm_mode == 0) {
+    for (int bn : {64, 96, 128, 160, 256}) {
+      double t;
+      if ((rc = run(best_bb, bn, 0, &t))) return rc;
+      if (t < best) { best = t; best_bn = bn; }
+    }
+    for (int bns : {64, 128, 160, 256}) {
+      double t;
+      if ((rc = run(best_bb, best_bn, bns, &t))) return rc;
+      if (t < best) { best = t; best_bns = bns; }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if ((rc = pw_set_band_batch(ctx, best_bb))) return rc;
+  ctx->gemm_bn = best_bn;
+  ctx->gemm_bn_store = best_bns;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    tune_cache()[key] = TuneVal{best_bb, best_bn, best_bns};
+  }
+  if (res) {
+    *res = pw_tune_result{};
+    res->band_batch = best_bb;
+    res->gemm_bn = best_bn;
+    res->gemm_bn_store = best_bns;
+    res->ms_default = t_def;
+    res->ms_best = best;
+    res->tried = tried;
+    res->cached = 0;
+  }
+  return PW_OK;
+}
+
+}  // extern "C"

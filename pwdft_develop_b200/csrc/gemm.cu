@@ -542,10 +542,10 @@ int split_bf16_t(const float* x, long ld_in, int ncol, int nrow, void* hi, void*
 }
 
 int gemm_tn_reduce(const SplitOperand& A, const SplitOperand& B, int K, int nterms, DevBuf& ws,
-                   const ReduceOut& out, cudaStream_t st) {
+                   const ReduceOut& out, cudaStream_t st, int bn) {
   const int M = A.rows, N = B.rows;
   if (M == 0 || N == 0) return PW_OK;
-  const int BN = pick_bn(N);
+  const int BN = bn > 0 ? bn : pick_bn(N);
   const int tiles = ((M + GM - 1) / GM) * ((N + BN - 1) / BN);
   // enough CTAs to fill the GPU twice over, each with >= 4 K-blocks
   int nsplit = std::max(1, (2 * num_sms() + tiles - 1) / tiles);
@@ -568,10 +568,10 @@ int gemm_tn_reduce(const SplitOperand& A, const SplitOperand& B, int K, int nter
 }
 
 int gemm_tn_store(const SplitOperand& A, const SplitOperand& B, int K, int nterms, float* C, long ldc, int accumulate,
-                  cudaStream_t st, int transposed) {
+                  cudaStream_t st, int transposed, int bn) {
   const int M = A.rows, N = B.rows;
   if (M == 0 || N == 0) return PW_OK;
-  const int BN = N >= 256 ? 256 : pick_bn(N);
+  const int BN = bn > 0 ? bn : (N >= 256 ? 256 : pick_bn(N));
   GemmArgs g{};
   g.M = M; g.N = N; g.K = K; g.kchunk = ((K + GK - 1) / GK) * GK; g.nterms = nterms; g.epi = transposed ? 2 : 1;
   g.C = C; g.ldc = ldc; g.accumulate = accumulate;

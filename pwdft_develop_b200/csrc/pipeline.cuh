@@ -1228,12 +1228,12 @@ struct Plan {
     ro.bf_lo = wb + (size_t)nb * npp * 2;
     ro.ldb = npp;
     { Launch L_(c, st, KK_GRAM);
-    if ((rc = gemm_tn_reduce(A, B, nt, c->gemm_terms, c->s_ws, ro, st))) return rc; }
+    if ((rc = gemm_tn_reduce(A, B, nt, c->gemm_terms, c->s_ws, ro, st, c->gemm_bn))) return rc; }
     // out[b][g] += sum_l QT[g][l] W^T[b][l]  (tile rows = grid points: coalesced stores)
     SplitOperand W{wb, wb + (size_t)nb * npp * 2, nb, npp};
     SplitOperand QT{ds.qt_bf, (const char*)ds.qt_bf + (size_t)nt * npp * 2, nt, npp};
     { Launch L_(c, st, KK_GRAM);
-    if ((rc = gemm_tn_store(QT, W, np, c->gemm_terms, out, ldo, 1, st, 1))) return rc; }
+    if ((rc = gemm_tn_store(QT, W, np, c->gemm_terms, out, ldo, 1, st, 1, c->gemm_bn_store))) return rc; }
     return PW_OK;
   }
 
