@@ -128,6 +128,8 @@ PW_API int pw_hgh_species(int znuc, double* zion, double* eself, double* rcut_no
  * (src/SCF/hamiltonian.cpp:327-918).  Calls pw_set_nonlocal internally. */
 PW_API int pw_set_atoms(pw_ctx* ctx, int natom, const int* znuc, const double* pos);
 /* Pseudocharge rho_ps on the fine grid (host, N_fine doubles). */
+/* Number of atoms set by pw_set_atoms. */
+PW_API int pw_ctx_natom(const pw_ctx* ctx, int* natom);
 PW_API int pw_get_pseudocharge(const pw_ctx* ctx, double* rho_fine_host);
 /* One atom's projector set: npts, nproj, idx[npts], val4[nproj][npts][4]
  * (VAL, DX, DY, DZ), wgt[nproj].  Output pointers may be NULL. */

@@ -89,6 +89,7 @@ SIGNATURES: dict[str, tuple] = {
     "pw_hgh_species": (_i, [_i, _dp, _dp, _dp, _dp, _ip]),
     "pw_set_atoms": (_i, [_vp, _i, _ip, _dp]),
     "pw_get_pseudocharge": (_i, [_vp, _dp]),
+    "pw_ctx_natom": (_i, [_vp, _ip]),
     "pw_get_atom_projectors": (_i, [_vp, _i, _ip, _ip, _ip, _dp, _dp]),
     "pw_stats": (_i, [_vp, C.POINTER(_l), C.POINTER(_l)]),
     "pw_hgh_atom_projectors": (_i, [_dp, _ip, _i, _dp, _ip, _ip, _ip, _dp, _dp]),

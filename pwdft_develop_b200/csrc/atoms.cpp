@@ -68,6 +68,12 @@ int pw_set_atoms(pw_ctx* ctx, int natom, const int* znuc, const double* pos) {
   return PW_OK;
 }
 
+int pw_ctx_natom(const pw_ctx* ctx, int* natom) {
+  PWB_CHECK(ctx && natom, PW_EINVAL, "null argument");
+  *natom = (int)ctx->atom_z.size();
+  return PW_OK;
+}
+
 int pw_get_pseudocharge(const pw_ctx* ctx, double* rho_fine_host) {
   PWB_CHECK(ctx && rho_fine_host, PW_EINVAL, "null argument");
   PWB_CHECK(ctx->h_rhops.size() == (size_t)ctx->ntotf, PW_ENOTREADY, "atoms not set (pw_set_atoms)");
