@@ -589,6 +589,203 @@ k_floc(VT<T>* __restrict__ BC, const T* __restrict__ vtot, const T* __restrict__
 
 
 // ---------------------------------------------------------------------------
+// fine plane, local potential only, fused form (the hot apply of H*psi).
+// Same result as k_floc MODE 0 with fewer shared-memory passes:
+//  * the y inverse transform reads the slot rows of B straight from global
+//    memory (non-slot rows are zero), no zero fill or scatter;
+//  * per row the x inverse transform reads the slot columns of S, its second
+//    pass multiplies by V and runs the first stage of the forward transform
+//    in the same registers (the k1 + N1 k2 distribution of the inverse's output
+//    is the stride the forward's decimation needs), and the forward's second
+//    stage writes only the slot columns back;
+//  * the y forward transform's second pass writes the slot rows of C
+//    directly (x 1/N_fine).
+// ---------------------------------------------------------------------------
+// fine index e of a length-N axis -> slot (coarse size n = N/2), -1 if none;
+// slot n is the "-" Nyquist partner at fine index N - n/2
+template <int N> __device__ __forceinline__ int fine_slot(int e) {
+  constexpr int n = N / 2, h = n / 2;
+  return e <= h ? e : (e > N - h ? e - N + n : (e == N - h ? n : -1));
+}
+
+template <typename T, int NXF, int NYF>
+__global__ void __launch_bounds__(FLOC_THREADS, sizeof(T) == 4 ? 3 : 1)
+k_floc2(VT<T>* __restrict__ BC, const T* __restrict__ vtot, T inv_nf, const VT<T>* twx_g, const VT<T>* twy_g) {
+  using V = VT<T>;
+  constexpr int n0 = NXF / 2;
+  constexpr int nsx = n0 + 1, nsy = NYF / 2 + 1;
+  constexpr int PS = nsx;
+  constexpr int PR = NXF + 1;
+  constexpr int NX1 = Split<NXF>::n1, NX2 = NXF / NX1, FX = 32 / NX1;
+  constexpr int NY1 = Split<NYF>::n1, NY2 = NYF / NY1, FY = 32 / NY1;
+  constexpr int RX = (FX * NX2 + 31) / 32, RY = (FY * NY2 + 31) / 32;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  V* S = reinterpret_cast<V*>(smraw);          // [NYF][PS]
+  V* twx = S + NYF * PS;
+  V* twy = twx + NXF;
+  V* Rall = twy + NYF;                          // [nwarps][FX][PR]
+  load_tw(twx, twx_g, NXF);
+  load_tw(twy, twy_g, NYF);
+  const int zf = blockIdx.x, p = blockIdx.y;
+  const int NZF = gridDim.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  V* Bp = BC + ((long)p * NZF + zf) * nsy * nsx;
+  __syncthreads();
+
+  // A: inverse y transform of the nsx slot columns
+  for (int g = warp * FY; g < nsx; g += nw * FY) {
+#pragma unroll
+    for (int r = 0; r < RY; ++r) {
+      const int it = lane + 32 * r;
+      const int f = it / NY2, j2 = it - f * NY2;
+      const int c = g + f;
+      if (it < FY * NY2 && c < nsx) {
+        V t[NY1];
+#pragma unroll
+        for (int j1 = 0; j1 < NY1; ++j1) {
+          const int s = fine_slot<NYF>(NY2 * j1 + j2);
+          t[j1] = s >= 0 ? Bp[s * nsx + c] : mkc<V>(0, 0);
+        }
+        DFT<NY1, +1, V>::run(t);
+#pragma unroll
+        for (int k1 = 1; k1 < NY1; ++k1) {
+          V w = twy[j2 * k1];
+          w.y = -w.y;
+          t[k1] = cmul(t[k1], w);
+        }
+#pragma unroll
+        for (int k1 = 0; k1 < NY1; ++k1) S[(NY2 * k1 + j2) * PS + c] = t[k1];
+      }
+    }
+    __syncwarp();
+    {
+      const int f = lane / NY1, k1 = lane - f * NY1;
+      const int c = g + f;
+      const bool act = lane < FY * NY1 && c < nsx;
+      V u[NY2];
+      if (act) {
+#pragma unroll
+        for (int j2 = 0; j2 < NY2; ++j2) u[j2] = S[(NY2 * k1 + j2) * PS + c];
+        DFT<NY2, +1, V>::run(u);
+      }
+      __syncwarp();
+      if (act) {
+#pragma unroll
+        for (int k2 = 0; k2 < NY2; ++k2) S[(k1 + NY1 * k2) * PS + c] = u[k2];
+      }
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+
+  // B: rows (x): inverse, x V, forward, keep the slot columns
+  V* Rw = Rall + warp * FX * PR;
+  for (int r0 = warp * FX; r0 < NYF; r0 += nw * FX) {
+    const int nr = min(FX, NYF - r0);
+#pragma unroll
+    for (int r = 0; r < RX; ++r) {
+      const int it = lane + 32 * r;
+      const int f = it / NX2, j2 = it - f * NX2;
+      if (it < FX * NX2 && f < nr) {
+        V t[NX1];
+        const V* srow = S + (r0 + f) * PS;
+#pragma unroll
+        for (int j1 = 0; j1 < NX1; ++j1) {
+          const int s = fine_slot<NXF>(NX2 * j1 + j2);
+          t[j1] = s >= 0 ? srow[s] : mkc<V>(0, 0);
+        }
+        DFT<NX1, +1, V>::run(t);
+#pragma unroll
+        for (int k1 = 1; k1 < NX1; ++k1) {
+          V w = twx[j2 * k1];
+          w.y = -w.y;
+          t[k1] = cmul(t[k1], w);
+        }
+#pragma unroll
+        for (int k1 = 0; k1 < NX1; ++k1) Rw[f * PR + NX2 * k1 + j2] = t[k1];
+      }
+    }
+    __syncwarp();
+    {
+      const int f = lane / NX1, k1 = lane - f * NX1;
+      const bool act = lane < FX * NX1 && f < nr;
+      if (act) {
+        V u[NX2];
+        V* rr = Rw + f * PR + NX2 * k1;
+#pragma unroll
+        for (int j2 = 0; j2 < NX2; ++j2) u[j2] = rr[j2];
+        DFT<NX2, +1, V>::run(u);                    // u[k2] = x[k1 + NX1 k2]
+        const T* vrow = vtot + ((long)zf * NYF + r0 + f) * NXF + k1;
+#pragma unroll
+        for (int k2 = 0; k2 < NX2; ++k2) u[k2] = cscale(u[k2], vrow[NX1 * k2]);
+        DFT<NX2, -1, V>::run(u);                    // forward, first stage over k2
+#pragma unroll
+        for (int m2 = 1; m2 < NX2; ++m2) u[m2] = cmul(u[m2], twx[k1 * m2]);
+#pragma unroll
+        for (int m2 = 0; m2 < NX2; ++m2) rr[m2] = u[m2];
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < RX; ++r) {
+      const int it = lane + 32 * r;
+      const int f = it / NX2, m2 = it - f * NX2;
+      if (it < FX * NX2 && f < nr) {
+        V t[NX1];
+#pragma unroll
+        for (int k1 = 0; k1 < NX1; ++k1) t[k1] = Rw[f * PR + NX2 * k1 + m2];
+        DFT<NX1, -1, V>::run(t);                    // forward, second stage over k1
+        V* srow = S + (r0 + f) * PS;
+#pragma unroll
+        for (int m1 = 0; m1 < NX1; ++m1) {
+          const int s = fine_slot<NXF>(m2 + NX2 * m1);
+          if (s >= 0) srow[s] = t[m1];
+        }
+      }
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+
+  // C: forward y transform of the slot columns, slot rows straight to C
+  for (int g = warp * FY; g < nsx; g += nw * FY) {
+#pragma unroll
+    for (int r = 0; r < RY; ++r) {
+      const int it = lane + 32 * r;
+      const int f = it / NY2, j2 = it - f * NY2;
+      const int c = g + f;
+      if (it < FY * NY2 && c < nsx) {
+        V t[NY1];
+#pragma unroll
+        for (int j1 = 0; j1 < NY1; ++j1) t[j1] = S[(NY2 * j1 + j2) * PS + c];
+        DFT<NY1, -1, V>::run(t);
+#pragma unroll
+        for (int k1 = 1; k1 < NY1; ++k1) t[k1] = cmul(t[k1], twy[j2 * k1]);
+#pragma unroll
+        for (int k1 = 0; k1 < NY1; ++k1) S[(NY2 * k1 + j2) * PS + c] = t[k1];
+      }
+    }
+    __syncwarp();
+    {
+      const int f = lane / NY1, k1 = lane - f * NY1;
+      const int c = g + f;
+      if (lane < FY * NY1 && c < nsx) {
+        V u[NY2];
+#pragma unroll
+        for (int j2 = 0; j2 < NY2; ++j2) u[j2] = S[(NY2 * k1 + j2) * PS + c];
+        DFT<NY2, -1, V>::run(u);
+#pragma unroll
+        for (int k2 = 0; k2 < NY2; ++k2) {
+          const int s = fine_slot<NYF>(k1 + NY1 * k2);
+          if (s >= 0) Bp[s * nsx + c] = cscale(u[k2], inv_nf);
+        }
+      }
+    }
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
 // density: rho(r) += w_a |Re psi_f|^2 + w_b |Im psi_f|^2 over the pairs of a
 // chunk (CalculateDensity, src/SCF/hamiltonian.cpp:2511-2547).  One CTA owns
 // one fine plane for `ppc` pairs and keeps its partial sums in registers.
@@ -1003,6 +1200,7 @@ struct Plan {
     PWB_CUDA(cudaFuncSetAttribute(k_cxy_inv<T, N0, N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_cxy()));
     PWB_CUDA(cudaFuncSetAttribute(k_zteter<T, N2, TX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_zteter()));
     PWB_CUDA(cudaFuncSetAttribute(k_floc<T, NF0, NF1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_floc()));
+    PWB_CUDA(cudaFuncSetAttribute(k_floc2<T, NF0, NF1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_floc()));
     PWB_CUDA(cudaFuncSetAttribute(k_floc<T, NF0, NF1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_floc()));
     done = true;
     return PW_OK;
@@ -1030,8 +1228,8 @@ struct Plan {
         AD, K, BC, reinterpret_cast<const T*>(c->ekin.p), N0, N1, inv_nc, tw(c, 2), tw(c, 5)); }
     if (c->nl_mode == PW_NL_DENSE) {
       { Launch L_(c, st, KK_FPLANE_APPLY);
-      k_floc<T, NF0, NF1, 0><<<dim3(NF2, npair), FLOC_THREADS, sm_floc(), st>>>(
-          BC, reinterpret_cast<const T*>(c->vtot.p), nullptr, 0, inv_nf, tw(c, 3), tw(c, 4)); }
+      k_floc2<T, NF0, NF1><<<dim3(NF2, npair), FLOC_THREADS, sm_floc(), st>>>(
+          BC, reinterpret_cast<const T*>(c->vtot.p), inv_nf, tw(c, 3), tw(c, 4)); }
       { Launch L_(c, st, KK_ZFOLD);
       k_zfold<T, N2, NF2, TXF><<<dim3(N1, (N0 + TXF - 1) / TXF, npair), PENCIL_THREADS, sm_zfold(), st>>>(BC, K, AD, N0, N1, tw(c, 2), tw(c, 5)); }
       { Launch L_(c, st, KK_CXY_INV);
@@ -1264,8 +1462,8 @@ struct Plan {
         AD, K, BC, ekin_all ? ekin_all : reinterpret_cast<const T*>(c->ekin_k.p), N0, N1, inv_nc, tw(c, 2), tw(c, 5),
         1, band0, fpk, ekin_all ? c->ntot : 0); }
     { Launch L_(c, st, KK_FPLANE_APPLY);
-    k_floc<T, NF0, NF1, 0><<<dim3(NF2, nb), FLOC_THREADS, sm_floc(), st>>>(
-        BC, reinterpret_cast<const T*>(c->vtot.p), nullptr, 0, inv_nf, tw(c, 3), tw(c, 4)); }
+    k_floc2<T, NF0, NF1><<<dim3(NF2, nb), FLOC_THREADS, sm_floc(), st>>>(
+        BC, reinterpret_cast<const T*>(c->vtot.p), inv_nf, tw(c, 3), tw(c, 4)); }
     { Launch L_(c, st, KK_ZFOLD);
     k_zfold<T, N2, NF2, TXF><<<dim3(N1, (N0 + TXF - 1) / TXF, nb), PENCIL_THREADS, sm_zfold(), st>>>(
         BC, K, AD, N0, N1, tw(c, 2), tw(c, 5), 0, (T)0, 1); }
