@@ -56,6 +56,19 @@ __device__ __forceinline__ void load_tw(V* dst, const V* src, int n) {
   for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
 }
 
+// global -> shared copies that do not hold a register (cp.async): a thread
+// can issue all of its loads before waiting once
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+template <typename E> __device__ __forceinline__ void cp_async(E* dst, const E* src) {
+  static_assert(sizeof(E) == 4 || sizeof(E) == 8 || sizeof(E) == 16, "cp.async element size");
+  if constexpr (sizeof(E) == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(smem_addr(dst)), "l"(src), "n"((int)sizeof(E))
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // ---------------------------------------------------------------------------
 // coarse plane forward: psi (two real bands) -> A[pair][z][ky][kx]
 // ---------------------------------------------------------------------------
@@ -78,7 +91,7 @@ k_cxy_fwd(const T* __restrict__ psi, int ld, int nband, int band0, VT<T>* __rest
     const V* pc = reinterpret_cast<const V*>(psi) + (long)(band0 + p) * ld + z * ntot_plane;
     for (int i = threadIdx.x; i < N0 * N1; i += blockDim.x) {
       const int y = i / N0, x = i - y * N0;
-      pl[y * P0 + x] = pc[i];
+      cp_async(&pl[y * P0 + x], &pc[i]);
     }
   } else {
     const int ba = band0 + 2 * p, bb = ba + 1;
@@ -86,9 +99,13 @@ k_cxy_fwd(const T* __restrict__ psi, int ld, int nband, int band0, VT<T>* __rest
     const T* pb = (bb < nband) ? psi + (long)bb * ld + z * ntot_plane : nullptr;
     for (int i = threadIdx.x; i < N0 * N1; i += blockDim.x) {
       const int y = i / N0, x = i - y * N0;
-      pl[y * P0 + x] = mkc<V>(pa[i], pb ? pb[i] : (T)0);
+      T* d = reinterpret_cast<T*>(&pl[y * P0 + x]);
+      cp_async(d, &pa[i]);
+      if (pb) cp_async(d + 1, &pb[i]);
+      else d[1] = (T)0;
     }
   }
+  cp_async_wait_all();
   __syncthreads();
   smem_fft_cb<N0, -1, 1, P0>(pl, N1, twx);
   __syncthreads();
@@ -180,7 +197,8 @@ k_zpad(const VT<T>* __restrict__ A, VT<T>* __restrict__ K, VT<T>* __restrict__ B
   const V* Ap = A + (long)p * NZ * nplane + (long)ky * n0 + kx0;
   for (int i = threadIdx.x; i < NZ * TX; i += blockDim.x) {
     const int z = i / TX, c = i - z * TX;
-    in[z * PI + c] = (c < tw) ? Ap[z * nplane + c] : mkc<V>(0, 0);
+    if (c < tw) cp_async(&in[z * PI + c], &Ap[z * nplane + c]);
+    else in[z * PI + c] = mkc<V>(0, 0);
   }
   const ColMap m = colmap<TX>(ky, kx0, tw, n0, n1);
   if (threadIdx.x < 2 * TX) {
@@ -191,6 +209,7 @@ k_zpad(const VT<T>* __restrict__ A, VT<T>* __restrict__ K, VT<T>* __restrict__ B
     colofs[c] = valid ? ky_s * nsx + kx_s : -1;
   }
   for (int i = threadIdx.x; i < NZF * PO; i += blockDim.x) out[i] = mkc<V>(0, 0);
+  cp_async_wait_all();
   __syncthreads();
   smem_fft_cb<NZ, -1, PI, 1>(in, tw, twz);
   __syncthreads();
@@ -983,8 +1002,18 @@ k_zfold(const VT<T>* __restrict__ C, const VT<T>* __restrict__ K, VT<T>* __restr
   }
   for_rows_cols(NZF, ncompact(m, tw), [&](int zf, int j) {
     const int c = compact_col<TX>(j, tw);
-    in[zf * PI + c] = Cp[zf * fplane + colofs[c]];
+    cp_async(&in[zf * PI + c], &Cp[zf * fplane + colofs[c]]);
   });
+  // the kinetic term of this tile, needed after the fine transform
+  const long nplane = (long)n0 * n1;
+  const V* Kp = K ? K + (long)p * NZ * nplane + (long)ky * n0 + kx0 : nullptr;
+  V* ks = acc;   // staged in the accumulator array itself
+  for (int i = threadIdx.x; i < NZ * TX; i += blockDim.x) {
+    const int kz = i / TX, c = i - kz * TX;
+    if (Kp && c < tw) cp_async(&ks[kz * PA + c], &Kp[kz * nplane + c]);
+    else ks[kz * PA + c] = mkc<V>(0, 0);
+  }
+  cp_async_wait_all();
   __syncthreads();
   smem_fft_cb<NZF, -1, PI, 1>(in, m.ncols, twzf);
   __syncthreads();
@@ -999,13 +1028,11 @@ k_zfold(const VT<T>* __restrict__ C, const VT<T>* __restrict__ K, VT<T>* __restr
     }
     __syncthreads();
   }
-  const long nplane = (long)n0 * n1;
-  const V* Kp = K ? K + (long)p * NZ * nplane + (long)ky * n0 + kx0 : nullptr;
   const bool splitrow = m.nyy;
   for (int i = threadIdx.x; i < NZ * TX; i += blockDim.x) {
     const int kz = i / TX, c = i - kz * TX;
     if (c >= tw) { acc[kz * PA + c] = mkc<V>(0, 0); continue; }
-    V v = Kp ? Kp[kz * nplane + c] : mkc<V>(0, 0);
+    V v = acc[kz * PA + c];   // staged kinetic term
     const bool nyz = (kz == NZ / 2);
     const int fz = kz <= NZ / 2 ? kz : kz + (NZF - NZ);
     const bool split = splitrow || (c == m.nyx_i);
@@ -1087,8 +1114,9 @@ k_cxy_inv(const VT<T>* __restrict__ D, T* __restrict__ out, int ldo, int nband, 
   const V* Dp = D + ((long)p * N2 + z) * ntot_plane;
   for (int i = threadIdx.x; i < N0 * N1; i += blockDim.x) {
     const int y = i / N0, x = i - y * N0;
-    pl[y * P0 + x] = Dp[i];
+    cp_async(&pl[y * P0 + x], &Dp[i]);
   }
+  cp_async_wait_all();
   __syncthreads();
   smem_fft_cb<N1, +1, P0, 1>(pl, N0, twy);
   __syncthreads();
