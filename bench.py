@@ -336,6 +336,57 @@ def cells_bench(device: int, reps: int = 5):
             "graph_bands_per_s": nbands / (t_gr / 1e3), "sequential_bands_per_s": nbands / (t_seq / 1e3)}
 
 
+def gram_bench(device: int, reps: int = 10):
+    """Eigensolver Gram blocks X^T Y on the Si64 grid (K = 110,592) in FP32
+    contexts: split-BF16 tcgen05 GEMM (3 products, FP32 accumulation, split-K
+    with an FP64 reduction), for the ChebFSI / Cholesky-QR width (160) and the
+    LOBPCG [X W P] width (480).  Reports the whole pw_gram call (operand
+    split + GEMM + reduction) and the tensor-core kernel alone."""
+    import torch
+    from pwdft_develop_b200 import Context
+    from pwdft_develop_b200.core import KERNEL_KINDS
+    L, z, pos = si64_atoms()
+    c = Context(L, NC, NF, precision="f32", device=device)
+    K = c.ntot
+    peaks = {}
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        peaks = json.loads(p.read_text())
+    tpeak = float(peaks.get("bf16_tflops", 1590.0))
+    out = {"K": K, "tensor_peak_tflops": tpeak,
+           "peak_source": "measured" if "bf16_tflops" in peaks else "fallback"}
+    g = torch.Generator(device="cuda").manual_seed(SEED + 21)
+    gkind = [k for k, v in KERNEL_KINDS.items() if v == "gram"][0]
+    for n in (160, 480):
+        X = torch.randn((n, K), dtype=torch.float32, device="cuda", generator=g)
+        c.gram(X)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            c.gram(X)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        c.profile(True)
+        for _ in range(reps):
+            c.gram(X)
+        torch.cuda.synchronize()
+        kms, kn = c.profile_read(gkind)
+        c.profile(False)
+        useful = 2.0 * K * n * n
+        kern_ms = kms / kn if kn else None                  # tensor-core GEMM + split-K reduction
+        out[f"n{n}"] = {"call_ms": ms, "useful_tflops": useful / (ms / 1e3) / 1e12,
+                        "tensor_tflops_3products": 3 * useful / (ms / 1e3) / 1e12,
+                        "tensor_frac": 3 * useful / (ms / 1e3) / 1e12 / tpeak,
+                        "gemm_and_reduce_ms": kern_ms,
+                        "gemm_tensor_frac": (3 * useful / (kern_ms / 1e3) / 1e12 / tpeak) if kern_ms else None,
+                        "operand_bytes": 2 * n * K * 4,
+                        "hbm_frac_of_operand_reads": 2 * n * K * 4 / (ms / 1e3) / 1e9 / load_peaks()[0]}
+    c.close()
+    return out
+
+
 def kpoint_bench(device: int, reps: int = 5):
     """Si8 complex bands on a 4x4x4 Monkhorst-Pack k-mesh (64 k-points, 24
     bands each, 24^3 / 48^3 grids, Ecut 10 Ha) in one batched H(k) psi pass, FP32."""
@@ -547,6 +598,8 @@ def run_ours(args):
             line["kpoints"] = kpoint_bench(local)
         if args.cells and world == 1:
             line["cells"] = cells_bench(local)
+        if args.grams and world == 1:
+            line["gram"] = gram_bench(local)
         if args.cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(args.cpu_bands)
         print(json.dumps(line), flush=True)
@@ -568,6 +621,7 @@ def main():
     ap.add_argument("--no-exx", dest="exx", action="store_false", help="skip the hybrid-exchange leg")
     ap.add_argument("--no-kpoints", dest="kpoints", action="store_false", help="skip the k-point batch leg")
     ap.add_argument("--no-cells", dest="cells", action="store_false", help="skip the uneven-cell batch leg")
+    ap.add_argument("--no-grams", dest="grams", action="store_false", help="skip the eigensolver Gram leg")
     ap.add_argument("--cpu-bands", type=int, default=64)
     ap.add_argument("--bands", type=int, default=NBAND, help="band block size (profiling runs use a small block)")
     args = ap.parse_args()

@@ -163,3 +163,40 @@ struct pw_ctx {
   pwb::DevBuf s_ad, s_k, s_bc, s_wp, s_w;
   pwb::DevBuf s_host_in, s_host_out;   // device staging for the host-pointer entry points
 };
+
+namespace pwb {
+
+// One kernel (or library GEMM) launch: counted for pw_stats and, with
+// pw_profile on, bracketed by CUDA events on its stream.
+struct Launch {
+  pw_ctx* c;
+  cudaStream_t st;
+  int kind;
+  cudaEvent_t a = nullptr, b = nullptr;
+  static cudaEvent_t take(pw_ctx* c) {
+    if (!c->ev_pool.empty()) {
+      cudaEvent_t e = c->ev_pool.back();
+      c->ev_pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+  }
+  Launch(pw_ctx* c_, cudaStream_t st_, int kind_) : c(c_), st(st_), kind(kind_) {
+    if (kind == KK_LIBGEMM) c->lib_launches++; else c->launches++;
+    if (c->prof_on) {
+      a = take(c);
+      b = take(c);
+      cudaEventRecord(a, st);
+    }
+  }
+  ~Launch() {
+    if (a) {
+      cudaEventRecord(b, st);
+      c->prof.push_back({kind, a, b});
+    }
+  }
+};
+
+}  // namespace pwb

@@ -36,10 +36,12 @@ int gram(pw_ctx* c, const void* X, int ldx, int nx, const void* Y, int ldy, int 
   if ((rc = c->s_gx_bf.alloc(2 * bx)) || (!same && (rc = c->s_gy_bf.alloc(2 * by)))) return rc;
   char* xb = (char*)c->s_gx_bf.p;
   char* yb = same ? xb : (char*)c->s_gy_bf.p;
-  c->launches++;
-  if ((rc = split_bf16((const float*)X, ldx, nt, nx, xb, xb + bx, nt, 1.0f, st))) return rc;
+  {
+    Launch L_(c, st, KK_MISC);
+    if ((rc = split_bf16((const float*)X, ldx, nt, nx, xb, xb + bx, nt, 1.0f, st))) return rc;
+  }
   if (!same) {
-    c->launches++;
+    Launch L_(c, st, KK_MISC);
     if ((rc = split_bf16((const float*)Y, ldy, nt, ny, yb, yb + by, nt, 1.0f, st))) return rc;
   }
   SplitOperand A{xb, xb + bx, nx, nt};
@@ -49,7 +51,8 @@ int gram(pw_ctx* c, const void* X, int ldx, int nx, const void* Y, int ldy, int 
   ro.ldo = ldg;
   ro.f64 = 1;
   ro.transpose = 1;    // G[j*ldg + i] = sum_g X[i][g] Y[j][g]
-  c->launches += 2;
+  c->launches += 1;   // the reduction kernel; the GEMM is counted by L_
+  Launch L_(c, st, KK_GRAM);
   return gemm_tn_reduce(A, B, nt, c->gemm_terms, c->s_ws, ro, st);
 }
 

@@ -1151,36 +1151,6 @@ k_cxy_inv(const VT<T>* __restrict__ D, T* __restrict__ out, int ldo, int nband, 
 // host-side launch plan for one (precision, grid) instantiation
 // ---------------------------------------------------------------------------
 // Records a launch; when profiling is on, brackets it with events on the stream.
-struct Launch {
-  pw_ctx* c;
-  cudaStream_t st;
-  int kind;
-  cudaEvent_t a = nullptr, b = nullptr;
-  static cudaEvent_t take(pw_ctx* c) {
-    if (!c->ev_pool.empty()) {
-      cudaEvent_t e = c->ev_pool.back();
-      c->ev_pool.pop_back();
-      return e;
-    }
-    cudaEvent_t e;
-    cudaEventCreate(&e);
-    return e;
-  }
-  Launch(pw_ctx* c_, cudaStream_t st_, int kind_) : c(c_), st(st_), kind(kind_) {
-    if (kind == KK_LIBGEMM) c->lib_launches++; else c->launches++;
-    if (c->prof_on) {
-      a = take(c);
-      b = take(c);
-      cudaEventRecord(a, st);
-    }
-  }
-  ~Launch() {
-    if (a) {
-      cudaEventRecord(b, st);
-      c->prof.push_back({kind, a, b});
-    }
-  }
-};
 
 template <typename T> static int fplane_cr(int NXF, int NYF) {
   // rows per chunk so that S + R (+ twiddles) fit in ~200 KB of shared memory
