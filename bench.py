@@ -58,6 +58,23 @@ def synthetic_vtot(n):
     return rng.uniform(-1.0, 0.5, size=n)
 
 
+def load_traffic(prec: str, kind: str, npair: int):
+    """DRAM bytes per launch of one kernel kind from the committed ncu summary
+    (profiles/hpsi_si64_<prec>_dram_traffic.md, captured at 80 pairs per
+    launch), scaled to npair pairs; None when no summary exists."""
+    f = ROOT / "profiles" / f"hpsi_si64_{prec}_dram_traffic.md"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        cells = [c.strip() for c in line.strip().strip("|").split("|")]
+        if len(cells) == 6 and cells[0] == kind:
+            try:
+                return float(cells[4]) * 1e6 * npair / 80.0
+            except ValueError:
+                return None
+    return None
+
+
 def load_peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -471,7 +488,10 @@ def run_ours(args):
     ctx.set_vtot(synthetic_vtot(ctx.ntotFine))
     ctx.set_atoms(z, pos)
     ctx.set_band_batch(NBAND)
-    tune = ctx.autotune(NBAND)          # set-up (untimed): band batch and projector GEMM tiles
+    if args.autotune:
+        tune = ctx.autotune(NBAND)      # set-up (untimed): band batch and projector GEMM tiles
+    else:
+        tune = {"band_batch": NBAND, "gemm_bn": 0, "gemm_bn_store": 0}
     dt_t = ctx.torch_dtype
     g = torch.Generator(device="cuda").manual_seed(SEED + rank)
     X = torch.randn((NBAND, ctx.ntot), dtype=torch.float64, device="cuda", generator=g)
@@ -536,10 +556,7 @@ def run_ours(args):
     alg = algorithmic_bytes(dom_kind, tune["band_batch"] // 2, s, npts_total, 5, nslot_est, natom)
     achieved = alg / (kern[dom_name]["avg_us"] * 1e-6) / 1e9
     peak, peak_kind = load_peaks()
-    traffic = None
-    tf = ROOT / "profiles" / f"traffic_{prec}.json"
-    if tf.exists():
-        traffic = json.loads(tf.read_text()).get(dom_name)
+    traffic = load_traffic(prec, dom_name, tune["band_batch"] // 2)
     model = hpsi_model_bytes_per_band(s, NBAND, 5 * natom, natom, npts_total)
 
     # end to end through the host C-ABI entry (pinned host buffers)
@@ -622,6 +639,8 @@ def main():
     ap.add_argument("--no-kpoints", dest="kpoints", action="store_false", help="skip the k-point batch leg")
     ap.add_argument("--no-cells", dest="cells", action="store_false", help="skip the uneven-cell batch leg")
     ap.add_argument("--no-grams", dest="grams", action="store_false", help="skip the eigensolver Gram leg")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="default band batch and GEMM tiles (profiling runs: no tuning launches in the list)")
     ap.add_argument("--cpu-bands", type=int, default=64)
     ap.add_argument("--bands", type=int, default=NBAND, help="band block size (profiling runs use a small block)")
     args = ap.parse_args()
