@@ -409,6 +409,45 @@ PW_API int pw_teter_precond_noalloc(pw_ctx* ctx, const void* r, int ld, void* w,
  * Default 64. Scratch grows to hold ceil(nband_batch/2) band pairs. */
 PW_API int pw_set_band_batch(pw_ctx* ctx, int nband_batch);
 
+/* ---- Sphere-cut (G-space) mode, the reference's Use_Real_Space: 0 ----
+ * A band is its Fourier coefficients on the half sphere 1/2 |G|^2 < ecut, in
+ * the order of Fourier::idxCoarseCut (ascending R2C index, G_x >= 0 with the
+ * G_x = 0 half plane G_y > 0 or G_y = 0, G_z >= 0; src/SCF/fourier.cpp:542-640),
+ * complex, with the sqrt(2) convention of Spinor::wavefunG_ (c_0 = psi(0),
+ * c_s = sqrt(2) psi(G_s); src/SCF/spinor.cpp:568-590).  The entry points take
+ * a band as 2 ns reals (re, im interleaved, `ld` even, in reals), so
+ * pw_hpsi / pw_teter_precond / pw_eigsolve / pw_gram / pw_density / pw_scf_run
+ * run unchanged on a G-space context; their inner product is the reference's
+ * Re(X^H Y) Gram (src/MathLibs/blas.cpp:997-1029).  Im c_0 must be zero.
+ * pw_hpsi adds the nonlocal term of EigenSolver::NonlocalMultX
+ * (src/EigenSolver/eigensolver.cpp:471-515) to the local + kinetic part of
+ * Spinor::AddMultSpinorFineR2C's complex overload (spinor.cpp:528-680), the
+ * sum LOBPCGSolveReal forms (src/EigenSolver/lobpcg.cpp:201-211).
+ *
+ * pw_ctx_create_gspace replaces Fourier::Initialize with spherecut = true
+ * (fourier.cpp:542-640) and KohnSham::CalculateEkin's sphere branch
+ * (hamiltonian.cpp:2630-2667).  numGrid is the G-space grid N (the density
+ * grid: Density_Grid_Factor 1, src/esdf.cpp:2786-2856); N/2 must be a coarse
+ * grid built into the library and the sphere must satisfy |m_d| <= N_d / 4.
+ * After it, pw_ctx_sizes reports ntot = 2 ns and ntotFine = N.  Exact
+ * exchange, k-points and forces are not built for G-space contexts
+ * (PW_EUNSUPPORTED). */
+PW_API int pw_ctx_create_gspace(const double length[3], const int numGrid[3], double ecut, int precision, int device,
+                                pw_ctx** out);
+/* Sphere tables of a G-space context (host arrays, any may be NULL):
+ * ns, idxCoarseCut (ns), signed Miller indices (3 ns), ekin and Teter (ns). */
+PW_API int pw_gs_sphere(const pw_ctx* ctx, int* ns, int* idx_r2c, int* miller, double* ekin, double* teter);
+/* Nonlocal projectors of EigenSolver::NonlocalMultX (KohnSham::vnlc_,
+ * src/SCF/hamiltonian.cpp:700-797): vnlc (host, column-major ns x nproj
+ * complex as interleaved doubles, sqrt(2) convention) and weights wgt (nproj).
+ * pw_hpsi then adds vnlc (wgt o Re(vnlc^H c)).  pw_set_atoms on a G-space
+ * context builds them from the library's HGH tables
+ * (PeriodTable::CalculateNonlocalPP, Fourier space, src/SCF/periodtable.cpp:1599-1849). */
+PW_API int pw_gs_set_projectors(pw_ctx* ctx, int nproj, const double* vnlc, const double* wgt);
+/* The projector matrix a G-space context holds (host, as pw_gs_set_projectors
+ * takes it); nproj may be queried with vnlc = wgt = NULL. */
+PW_API int pw_gs_get_projectors(const pw_ctx* ctx, int* nproj, double* vnlc, double* wgt);
+
 #ifdef __cplusplus
 }
 #endif

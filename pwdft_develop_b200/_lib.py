@@ -25,7 +25,7 @@ class PwError(RuntimeError):
 
 def _load() -> C.CDLL:
     if not LIB_PATH.exists():
-        raise ImportError(f"{LIB_PATH} is missing: run pwdft_develop_b200.build.build() (nvcc, sm_100a)")
+        raise ImportError(f"{LIB_PATH} is missing: run __graft_entry__.build() or python pwdft_develop_b200/build.py (nvcc, sm_100a)")
     return C.CDLL(str(LIB_PATH))
 
 
@@ -123,6 +123,10 @@ SIGNATURES: dict[str, tuple] = {
     "pw_ace_apply": (_i, [_vp, _vp, _i, _vp, _i, _i, _vp]),
     "pw_exx_energy": (_i, [_vp, _vp, _i, _i, _dp, _i, _i, _dp]),
     "pw_band_energy_backward": (_i, [_vp, _vp, _i, _i, _dp, _vp, _dp]),
+    "pw_ctx_create_gspace": (_i, [_dp, _ip, C.c_double, _i, _i, C.POINTER(_vp)]),
+    "pw_gs_sphere": (_i, [_vp, _ip, _ip, _ip, _dp, _dp]),
+    "pw_gs_set_projectors": (_i, [_vp, _i, _dp, _dp]),
+    "pw_gs_get_projectors": (_i, [_vp, _ip, _dp, _dp]),
 }
 
 for _name, (_res, _args) in SIGNATURES.items():

@@ -48,6 +48,80 @@ class Context:
         self.numGridFine = tuple(int(x) for x in numGridFine)
         self.length = tuple(float(x) for x in length)
 
+    @classmethod
+    def gspace(cls, length, numGrid, ecut: float, precision: str = "f64", device: int = 0) -> "Context":
+        """Sphere-cut (G-space) context, the reference's ``Use_Real_Space: 0``
+        mode (Fourier::Initialize with spherecut, src/SCF/fourier.cpp:542-640).
+        ``numGrid`` is the G-space (= density) grid.  Bands are the half-sphere
+        coefficients in idxCoarseCut order with the sqrt(2) convention, passed
+        as real tensors of 2 ns numbers (see ``to_real`` / ``to_complex``)."""
+        self = cls.__new__(cls)
+        self.precision = precision
+        prec = PW_F64 if precision == "f64" else PW_F32
+        L = (C.c_double * 3)(*[float(x) for x in length])
+        n = (C.c_int * 3)(*[int(x) for x in numGrid])
+        h = C.c_void_p()
+        check(lib.pw_ctx_create_gspace(L, n, float(ecut), prec, device, C.byref(h)))
+        self._h = h
+        nt, ntf = C.c_long(), C.c_long()
+        check(lib.pw_ctx_sizes(h, C.byref(nt), C.byref(ntf)))
+        self.ntot, self.ntotFine = nt.value, ntf.value
+        self.numGrid = tuple(int(x) // 2 for x in numGrid)
+        self.numGridFine = tuple(int(x) for x in numGrid)
+        self.length = tuple(float(x) for x in length)
+        self.ecut = float(ecut)
+        self.ns = self.ntot // 2
+        return self
+
+    def gs_sphere(self):
+        """(idxCoarseCut, Miller indices (ns, 3), ekin, teter) of a G-space context."""
+        ns = C.c_int()
+        check(lib.pw_gs_sphere(self._h, C.byref(ns), None, None, None, None))
+        n = ns.value
+        idx = np.zeros(n, np.int32)
+        mil = np.zeros((n, 3), np.int32)
+        ek = np.zeros(n)
+        te = np.zeros(n)
+        check(lib.pw_gs_sphere(self._h, C.byref(ns), idx.ctypes.data_as(_lib._ip), mil.ctypes.data_as(_lib._ip),
+                               ek.ctypes.data_as(_lib._dp), te.ctypes.data_as(_lib._dp)))
+        return idx, mil, ek, te
+
+    def gs_set_projectors(self, vnlc: np.ndarray, wgt: np.ndarray):
+        """vnlc (ns, nproj) complex, wgt (nproj): EigenSolver::NonlocalMultX's table."""
+        v = np.asarray(vnlc, np.complex128)
+        flat = np.ascontiguousarray(v.T).view(np.float64).ravel()     # column l: 2 ns interleaved doubles
+        w = np.ascontiguousarray(wgt, np.float64)
+        check(lib.pw_gs_set_projectors(self._h, v.shape[1], flat.ctypes.data_as(_lib._dp), w.ctypes.data_as(_lib._dp)))
+
+    def gs_get_projectors(self):
+        npj = C.c_int()
+        check(lib.pw_gs_get_projectors(self._h, C.byref(npj), None, None))
+        n = npj.value
+        flat = np.zeros(n * self.ntot)
+        w = np.zeros(n)
+        if n:
+            check(lib.pw_gs_get_projectors(self._h, C.byref(npj), flat.ctypes.data_as(_lib._dp),
+                                           w.ctypes.data_as(_lib._dp)))
+        return flat.view(np.complex128).reshape(n, -1).T, w
+
+    @staticmethod
+    def to_real(c):
+        """(nb, ns) complex -> (nb, 2 ns) real view (numpy or torch)."""
+        if hasattr(c, "is_cuda"):
+            import torch
+            return torch.view_as_real(c.contiguous()).reshape(c.shape[0], -1)
+        return np.ascontiguousarray(c).view(np.float64 if c.dtype == np.complex128 else np.float32).reshape(
+            c.shape[0], -1)
+
+    @staticmethod
+    def to_complex(x):
+        """(nb, 2 ns) real -> (nb, ns) complex view (numpy or torch)."""
+        if hasattr(x, "is_cuda"):
+            import torch
+            return torch.view_as_complex(x.contiguous().reshape(x.shape[0], -1, 2))
+        return np.ascontiguousarray(x).view(np.complex128 if x.dtype == np.float64 else np.complex64).reshape(
+            x.shape[0], -1)
+
     @property
     def handle(self):
         return self._h

@@ -7,6 +7,10 @@
 
 #include "common.hpp"
 
+namespace pwb {
+int gs_set_atoms(pw_ctx* c);
+}
+
 using namespace pwb;
 
 extern "C" {
@@ -34,7 +38,7 @@ int pw_set_atoms(pw_ctx* ctx, int natom, const int* znuc, const double* pos) {
   for (int a = 0; a < natom; ++a) {
     const Species* sp = species(znuc[a]);
     PWB_CHECK(sp, PW_EUNSUPPORTED, "HGH table only built for Si (14) and Al (13)");
-    int rc = nonlocal_pp(*sp, pos + 3 * a, ctx->L, ctx->nf, nl[a]);
+    int rc = ctx->gs ? PW_OK : nonlocal_pp(*sp, pos + 3 * a, ctx->L, ctx->nf, nl[a]);
     if (rc) return rc;
     AtomRho rho;
     rc = pseudo_charge(*sp, pos + 3 * a, ctx->L, ctx->nf, rho);
@@ -45,6 +49,20 @@ int pw_set_atoms(pw_ctx* ctx, int natom, const int* znuc, const double* pos) {
       ps_val.push_back(rho.val[4 * i]);
     }
     ps_off.push_back((long)ps_idx.size());
+  }
+  if (ctx->gs) {
+    // sphere-cut context: Fourier-space projectors (PeriodTable::CalculateNonlocalPP,
+    // src/SCF/periodtable.cpp:1599-1849) instead of the real-space sets
+    ctx->atom_z.assign(znuc, znuc + natom);
+    ctx->atom_pos.assign(pos, pos + 3 * natom);
+    int rc = gs_set_atoms(ctx);
+    if (rc) return rc;
+    ctx->h_nl.clear();
+    ctx->h_rhops = std::move(rhops);
+    ctx->h_ps_off = std::move(ps_off);
+    ctx->h_ps_idx = std::move(ps_idx);
+    ctx->h_ps_val = std::move(ps_val);
+    return PW_OK;
   }
   std::vector<int> npts(natom), nproj(natom), idx;
   std::vector<double> beta, wgt;

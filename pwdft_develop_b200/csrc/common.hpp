@@ -131,6 +131,16 @@ struct pw_ctx {
   int nkb = 0;                      // k-point batch (pw_set_kpoints)
   std::vector<double> kb_k;         // nkb x 3
   pwb::DevBuf ekin_kb, qkb;         // T [nkb][ntot], complex T [nkb][nproj][ntot]
+  // sphere-cut (G-space) mode (Use_Real_Space 0): a band is its half-sphere
+  // Fourier coefficients, complex, handled as a real vector of 2 ns numbers
+  // (ntot = 2 ns); n = N/2 is the slot box and nf = N the G-space grid
+  bool gs = false;
+  double gs_ecut = 0.0;
+  int gs_ns = 0;
+  pwb::DevBuf gs_map;               // int [n1+1][n2+1][n0+1] slot -> sphere point map
+  pwb::DevBuf gs_ekin, gs_teter;    // T [ns]
+  std::vector<int> h_gs_idx;        // idxCoarseCut: flat R2C index of each sphere point
+  std::vector<int> h_gs_m;          // 3 signed Miller indices per sphere point
   // hybrid exchange (AddMultSpinorEXX / CalculateVexxACE)
   int exx_mode = 0;                 // PW_EXX_OFF / PW_EXX_FULL / PW_EXX_ACE
   double exx_frac = 0.0, exx_mu = 0.0, exx_div = 0.0;

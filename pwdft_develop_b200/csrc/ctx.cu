@@ -60,7 +60,7 @@ int upload_real(pw_ctx* c, DevBuf& dst, const double* src, size_t n) {
   return PW_OK;
 }
 
-static int upload_twiddles(pw_ctx* c, int slot, int n) {
+int upload_twiddles(pw_ctx* c, int slot, int n) {
   std::vector<double> t(2 * n);
   for (int m = 0; m < n; ++m) {
     // exact values at the quarter points, cos/sin of 2*pi*m/n elsewhere
@@ -73,6 +73,30 @@ static int upload_twiddles(pw_ctx* c, int slot, int n) {
     t[2 * m + 1] = -sn;
   }
   return upload_real(c, c->tw[slot], t.data(), 2 * (size_t)n);
+}
+
+// After ctx->q (T [nproj][ntot]) is filled: the split-BF16 copies of Q and Q^T
+// that the FP32 tensor-core projector GEMMs read
+int install_dense_q(pw_ctx* ctx, int nproj) {
+  int rc;
+  if (ctx->prec == PW_F32) {
+    const int npp = (nproj + 7) / 8 * 8;
+    ctx->nproj_pad = npp;
+    const size_t nt = ctx->ntot;
+    const size_t ntp = (nt + 7) / 8 * 8;   // bf16 row stride of Q (16-byte TMA rows)
+    if ((rc = ctx->q_bf.alloc((size_t)2 * nproj * ntp * 2)) || (rc = ctx->qt_bf.alloc((size_t)2 * nt * npp * 2)))
+      return rc;
+    PWB_CUDA(cudaMemset(ctx->qt_bf.p, 0, (size_t)2 * nt * npp * 2));
+    char* qb = (char*)ctx->q_bf.p;
+    char* qtb = (char*)ctx->qt_bf.p;
+    if ((rc = split_bf16((const float*)ctx->q.p, nt, (int)nt, nproj, qb, qb + (size_t)nproj * ntp * 2, ntp, 1.0f,
+                         nullptr)))
+      return rc;
+    if ((rc = split_bf16_t((const float*)ctx->q.p, nt, (int)nt, nproj, qtb, qtb + nt * npp * 2, npp, nullptr)))
+      return rc;
+    PWB_CUDA(cudaDeviceSynchronize());
+  }
+  return PW_OK;
 }
 
 int ensure_scratch(pw_ctx* c, int npair) {
@@ -250,6 +274,7 @@ int pw_set_band_batch(pw_ctx* ctx, int nband_batch) {
 int pw_set_nonlocal(pw_ctx* ctx, int natom, const int* atom_npts, const int* atom_nproj, const int* idx,
                     const double* beta, const double* weight) {
   PWB_CHECK(ctx && natom >= 0, PW_EINVAL, "bad arguments");
+  PWB_CHECK(!ctx->gs, PW_EUNSUPPORTED, "real-space projector sets do not apply to a G-space context (pw_gs_set_projectors)");
   PWB_CUDA(cudaSetDevice(ctx->device));
   NonlocalDev& nl = ctx->nl;
   const int NXF = ctx->nf[0], NYF = ctx->nf[1], NZF = ctx->nf[2];
@@ -330,22 +355,7 @@ int pw_set_nonlocal(pw_ctx* ctx, int natom, const int* atom_npts, const int* ato
       rc = run_build_q(ctx, (const int*)d_idx.p, (const double*)d_beta.p, (const long*)d_pio.p,
                        (const long*)d_pbo.p, (const int*)d_pnp.p, nproj, nullptr);
       if (rc) return rc;
-      if (ctx->prec == PW_F32) {
-        const int npp = (nproj + 7) / 8 * 8;
-        ctx->nproj_pad = npp;
-        const size_t nt = ctx->ntot;
-        if ((rc = ctx->q_bf.alloc((size_t)2 * nproj * nt * 2)) || (rc = ctx->qt_bf.alloc((size_t)2 * nt * npp * 2)))
-          return rc;
-        PWB_CUDA(cudaMemset(ctx->qt_bf.p, 0, (size_t)2 * nt * npp * 2));
-        char* qb = (char*)ctx->q_bf.p;
-        char* qtb = (char*)ctx->qt_bf.p;
-        if ((rc = split_bf16((const float*)ctx->q.p, nt, (int)nt, nproj, qb, qb + (size_t)nproj * nt * 2, nt, 1.0f,
-                             nullptr)))
-          return rc;
-        if ((rc = split_bf16_t((const float*)ctx->q.p, nt, (int)nt, nproj, qtb, qtb + nt * npp * 2, npp, nullptr)))
-          return rc;
-        PWB_CUDA(cudaDeviceSynchronize());
-      }
+      if ((rc = install_dense_q(ctx, nproj))) return rc;
     }
     nl.natom = natom;
     nl.npmax = npmax;
@@ -445,6 +455,10 @@ int pw_hpsi(pw_ctx* ctx, const void* psi, int ld, void* hpsi, int ldh, int nband
   PWB_CHECK(ctx && (nband == 0 || (psi && hpsi)), PW_EINVAL, "null argument");
   PWB_CHECK(nband >= 0 && ld >= ctx->ntot && ldh >= ctx->ntot, PW_EINVAL, "Domain size does not match.");
   PWB_CHECK(ctx->have_vtot, PW_ENOTREADY, "local potential not set (pw_set_vtot)");
+  PWB_CHECK(!ctx->gs || nband == 0 ||
+                (ld % 2 == 0 && ldh % 2 == 0 && (uintptr_t)psi % (2 * ctx->esz) == 0 &&
+                 (uintptr_t)hpsi % (2 * ctx->esz) == 0),
+            PW_EINVAL, "G-space bands are complex: even leading dimensions and complex-aligned pointers");
   PWB_CUDA(cudaSetDevice(ctx->device));
   cudaStream_t st = (cudaStream_t)stream;
   const int cap = ctx->pair_cap;

@@ -68,6 +68,7 @@ extern "C" {
 
 int pw_exx_setup(pw_ctx* ctx, double exx_fraction, double screen_mu, int divergence_type, double ecut_wavefunction) {
   PWB_CHECK(ctx, PW_EINVAL, "null context");
+  PWB_CHECK(!ctx->gs, PW_EUNSUPPORTED, "exact exchange is built for real-space contexts only");
   PWB_CHECK(divergence_type == 0 || divergence_type == 1, PW_EUNSUPPORTED,
             "EXX divergence types 0 and 1 are built (EXX_Divergence_Type)");
   PWB_CHECK(screen_mu >= 0.0 && ecut_wavefunction > 0.0, PW_EINVAL, "bad exchange parameters");

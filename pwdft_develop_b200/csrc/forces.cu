@@ -278,6 +278,7 @@ extern "C" {
 int pw_forces(pw_ctx* ctx, const double* rho_dev, const void* psi_dev, int ldpsi, int nband, const double* occ,
               int num_spin, double* force, double* force_local, double* force_nonlocal) {
   PWB_CHECK(ctx && force, PW_EINVAL, "null argument");
+  PWB_CHECK(!ctx->gs, PW_EUNSUPPORTED, "forces are built for real-space contexts only");
   PWB_CHECK(ctx->prec == PW_F64, PW_EINVAL, "forces take an FP64 context");
   PWB_CHECK(!ctx->atom_z.empty() && ctx->h_ps_off.size() == ctx->atom_z.size() + 1, PW_ENOTREADY,
             "atoms not set (pw_set_atoms)");
@@ -307,6 +308,7 @@ int pw_forces(pw_ctx* ctx, const double* rho_dev, const void* psi_dev, int ldpsi
 
 int pw_band_energy(pw_ctx* ctx, const void* psi, int ld, int nband, const double* w, double* e) {
   PWB_CHECK(ctx && e && (nband == 0 || (psi && w)), PW_EINVAL, "null argument");
+  PWB_CHECK(!ctx->gs, PW_EUNSUPPORTED, "the band-energy adjoint is built for real-space contexts only");
   PWB_CHECK(nband >= 0 && ld >= ctx->ntot, PW_EINVAL, "Domain size does not match.");
   PWB_CUDA(cudaSetDevice(ctx->device));
   *e = 0.0;
@@ -333,6 +335,7 @@ int pw_band_energy(pw_ctx* ctx, const void* psi, int ld, int nband, const double
 int pw_band_energy_backward(pw_ctx* ctx, const void* psi, int ld, int nband, const double* w, double* dE_dV_dev,
                             double* dE_dR) {
   PWB_CHECK(ctx && (nband == 0 || (psi && w)), PW_EINVAL, "null argument");
+  PWB_CHECK(!ctx->gs, PW_EUNSUPPORTED, "the band-energy adjoint is built for real-space contexts only");
   PWB_CHECK(nband >= 0 && ld >= ctx->ntot, PW_EINVAL, "Domain size does not match.");
   PWB_CHECK(!dE_dR || ctx->prec == PW_F64, PW_EINVAL, "d/dR takes an FP64 context");
   PWB_CHECK(!dE_dR || !ctx->atom_z.empty(), PW_ENOTREADY, "atoms not set (pw_set_atoms)");
@@ -388,6 +391,7 @@ int pw_scf_state(const pw_ctx* ctx, int* nband, double* occ, double* psi_dev, in
 
 int pw_scf_forces(pw_ctx* ctx, double* force, double* force_local, double* force_nonlocal) {
   PWB_CHECK(ctx, PW_EINVAL, "null context");
+  PWB_CHECK(!ctx->gs, PW_EUNSUPPORTED, "forces are built for real-space contexts only");
   PWB_CHECK(ctx->scf_nband > 0, PW_ENOTREADY, "no FP64 SCF state (run pw_scf_run to the FP64 stage first)");
   return pw_forces(ctx, (const double*)ctx->scf_rho.p, ctx->scf_psi.p, (int)ctx->ntot, ctx->scf_nband,
                    ctx->scf_occ.data(), 2, force, force_local, force_nonlocal);

@@ -35,6 +35,8 @@ struct GridEntry {
   HpsiKFn hpsik[2];
   BuildQKFn bqk[2];
   HpsiKBFn hpsikb[2];
+  HpsiFn hpsigs[2];     // sphere-cut (G-space) contexts whose G-space grid is twice this grid
+  DensFn densgs[2];
 };
 
 void register_grid(const GridEntry& e);

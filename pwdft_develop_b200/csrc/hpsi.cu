@@ -31,10 +31,21 @@ int grid_chunk_rows(const int n[3], int prec) {
   return g ? g->cr[prec == PW_F32 ? 1 : 0]() : -1;
 }
 
+int gs_teter(pw_ctx* c, const void* r, int ld, void* out, int ldo, int nband, int band0, int npair, int acc,
+             cudaStream_t st);
+
+// entry points of the real-space (dual-grid) path that have no sphere-cut form here
+static bool gs_refuse(const pw_ctx* c, const char* what) {
+  if (!c->gs) return false;
+  set_error(std::string(what) + " is not available on a G-space (sphere-cut) context");
+  return true;
+}
+
 int run_hpsi(pw_ctx* c, const void* psi, int ld, void* out, int ldo, int nband, int band0, int npair, int acc,
              cudaStream_t st) {
   const GridEntry* g = find_grid(c->n);
   if (!g) { set_error("grid not built into this library"); return PW_EUNSUPPORTED; }
+  if (c->gs) return g->hpsigs[c->prec == PW_F32 ? 1 : 0](c, psi, ld, out, ldo, nband, band0, npair, acc, st);
   return g->hpsi[c->prec == PW_F32 ? 1 : 0](c, psi, ld, out, ldo, nband, band0, npair, acc, st);
 }
 
@@ -42,6 +53,7 @@ int run_build_q(pw_ctx* c, const int* d_idx, const double* d_beta, const long* d
                 const int* d_pnp, int nproj, cudaStream_t st, int deriv, void* out) {
   const GridEntry* g = find_grid(c->n);
   if (!g) { set_error("grid not built into this library"); return PW_EUNSUPPORTED; }
+  if (gs_refuse(c, "the real-space projector build")) return PW_EUNSUPPORTED;
   return g->bq[c->prec == PW_F32 ? 1 : 0](c, d_idx, d_beta, d_pio, d_pbo, d_pnp, nproj, st, deriv, out);
 }
 
@@ -49,18 +61,21 @@ int run_density(pw_ctx* c, const void* psi, int ld, int nband, int band0, int np
                 cudaStream_t st) {
   const GridEntry* g = find_grid(c->n);
   if (!g) { set_error("grid not built into this library"); return PW_EUNSUPPORTED; }
+  if (c->gs) return g->densgs[c->prec == PW_F32 ? 1 : 0](c, psi, ld, nband, band0, npair, w, rho, st);
   return g->dens[c->prec == PW_F32 ? 1 : 0](c, psi, ld, nband, band0, npair, w, rho, st);
 }
 
 int run_exx(pw_ctx* c, const void* psi, int ld, int nb, void* out, int ldo, int acc, cudaStream_t st) {
   const GridEntry* g = find_grid(c->n);
   if (!g) { set_error("grid not built into this library"); return PW_EUNSUPPORTED; }
+  if (gs_refuse(c, "exact exchange")) return PW_EUNSUPPORTED;
   return g->exx[c->prec == PW_F32 ? 1 : 0](c, psi, ld, nb, out, ldo, acc, st);
 }
 
 int run_hpsi_k(pw_ctx* c, const void* psi, int ld, void* out, int ldo, int band0, int nb, int acc, cudaStream_t st) {
   const GridEntry* g = find_grid(c->n);
   if (!g) { set_error("grid not built into this library"); return PW_EUNSUPPORTED; }
+  if (gs_refuse(c, "the k-point H*psi")) return PW_EUNSUPPORTED;
   return g->hpsik[c->prec == PW_F32 ? 1 : 0](c, psi, ld, out, ldo, band0, nb, acc, st);
 }
 
@@ -68,6 +83,7 @@ int run_hpsi_kbatch(pw_ctx* c, const void* psi, int ld, void* out, int ldo, int 
                     int fpk, const void* ekin_all, const void* qk_all) {
   const GridEntry* g = find_grid(c->n);
   if (!g) { set_error("grid not built into this library"); return PW_EUNSUPPORTED; }
+  if (gs_refuse(c, "the k-point batch")) return PW_EUNSUPPORTED;
   return g->hpsikb[c->prec == PW_F32 ? 1 : 0](c, psi, ld, out, ldo, f0, nf, acc, st, fpk, ekin_all, qk_all);
 }
 
@@ -75,12 +91,14 @@ int run_build_q_k(pw_ctx* c, const int* d_idx, const double* d_beta, const doubl
                   const long* d_pbo, const int* d_pnp, int nproj, const double* kv, void* out, cudaStream_t st) {
   const GridEntry* g = find_grid(c->n);
   if (!g) { set_error("grid not built into this library"); return PW_EUNSUPPORTED; }
+  if (gs_refuse(c, "the k-point projector build")) return PW_EUNSUPPORTED;
   return g->bqk[c->prec == PW_F32 ? 1 : 0](c, d_idx, d_beta, d_disp, d_pio, d_pbo, d_pnp, nproj, kv, out, st);
 }
 
 int run_ace(pw_ctx* c, const void* psi, int ld, int nb, void* out, int ldo, cudaStream_t st) {
   const GridEntry* g = find_grid(c->n);
   if (!g) { set_error("grid not built into this library"); return PW_EUNSUPPORTED; }
+  if (gs_refuse(c, "ACE")) return PW_EUNSUPPORTED;
   return g->ace[c->prec == PW_F32 ? 1 : 0](c, psi, ld, nb, out, ldo, 1, st);
 }
 
@@ -88,6 +106,7 @@ int run_teter(pw_ctx* c, const void* r, int ld, void* out, int ldo, int nband, i
               cudaStream_t st) {
   const GridEntry* g = find_grid(c->n);
   if (!g) { set_error("grid not built into this library"); return PW_EUNSUPPORTED; }
+  if (c->gs) return gs_teter(c, r, ld, out, ldo, nband, band0, npair, acc, st);
   return g->teter[c->prec == PW_F32 ? 1 : 0](c, r, ld, out, ldo, nband, band0, npair, acc, st);
 }
 
@@ -144,6 +163,8 @@ extern "C" int pw_teter_precond_noalloc(pw_ctx* ctx, const void* r, int ld, void
   }
   const GridEntry* g = find_grid(ctx->n);
   PWB_CHECK(g, PW_EUNSUPPORTED, "grid not built into this library");
+  // sphere-cut contexts: the preconditioner is a diagonal product that needs no scratch
+  if (ctx->gs) return gs_teter(ctx, r, ld, w, ldw, nband, 0, (nband + 1) / 2, accumulate, (cudaStream_t)stream);
   const int max_pairs = (int)(PWB_NOALLOC_SCRATCH_BYTES / pair_bytes);
   cudaStream_t st = (cudaStream_t)stream;
   for (int b0 = 0; b0 < nband; b0 += 2 * max_pairs) {

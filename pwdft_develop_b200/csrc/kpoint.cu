@@ -36,6 +36,7 @@ extern "C" {
 
 int pw_set_kpoint(pw_ctx* ctx, const double k[3]) {
   PWB_CHECK(ctx && k, PW_EINVAL, "null argument");
+  PWB_CHECK(!ctx->gs, PW_EUNSUPPORTED, "k-points are built for real-space contexts only");
   PWB_CUDA(cudaSetDevice(ctx->device));
   const int n0 = ctx->n[0], n1 = ctx->n[1], n2 = ctx->n[2];
   const long nt = ctx->ntot;
@@ -105,6 +106,7 @@ int pw_hpsi_k(pw_ctx* ctx, const void* psi, int ld, void* hpsi, int ldh, int nba
 
 int pw_set_kpoints(pw_ctx* ctx, int nk, const double* kpts) {
   PWB_CHECK(ctx && nk > 0 && kpts, PW_EINVAL, "bad arguments");
+  PWB_CHECK(!ctx->gs, PW_EUNSUPPORTED, "k-points are built for real-space contexts only");
   PWB_CUDA(cudaSetDevice(ctx->device));
   const long nt = ctx->ntot;
   const size_t esz = ctx->esz;

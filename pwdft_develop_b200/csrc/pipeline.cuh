@@ -1094,6 +1094,132 @@ k_zteter(VT<T>* __restrict__ A, const T* __restrict__ teter, int n0, int n1, T i
 }
 
 // ---------------------------------------------------------------------------
+// Sphere-cut (G-space) mode, Spinor::AddMultSpinorFineR2C complex overload
+// (src/SCF/spinor.cpp:528-680).  A band is its coefficients c_s on the half
+// sphere 1/2|G|^2 < Ecut in the reference's order (idxCoarseCut,
+// src/SCF/fourier.cpp:542-640), complex, sqrt(2) convention (c_0 at G = 0,
+// sqrt(2) psi(G) elsewhere).  The G-space grid N is the fine grid of the
+// slot box n = N/2, so the sphere (|m_d| <= n_d/2) sits in the same
+// [pair][z][ky slot][kx slot] layout the fine-plane kernel works on.  The
+// pair field is Z(G) = psi_a(G) + i psi_b(G) over the whole sphere, the
+// stored half giving Z(G) = a' + i b' and the mirrored half
+// Z(-G) = conj(a') + i conj(b') (a' = c_a / sqrt(2), c_0 real).
+//
+// map: int [nsy][nsz][nsx] over slots: 0 empty, s+1 stored point s,
+// -(s+1) the mirror -G of stored point s.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int slot_to_fine(int s, int n, int nf) {
+  return s <= n / 2 ? s : (s < n ? nf - n + s : nf - n / 2);
+}
+__device__ __forceinline__ int mirror_slot(int s, int n) {
+  return s == 0 ? 0 : (s == n / 2 ? n : (s == n ? n / 2 : n - s));
+}
+
+// sphere scatter + inverse z transform of one slot row (all kx slots) of a pair
+template <typename T, int N0, int N1, int NZF>
+__global__ void __launch_bounds__(PENCIL_THREADS)
+k_gs_zinv(const T* __restrict__ psi, int ld, int nband, int band0, const int* __restrict__ map,
+          VT<T>* __restrict__ B, const VT<T>* twzf_g) {
+  using V = VT<T>;
+  constexpr int nsx = N0 + 1, nsy = N1 + 1, n2 = NZF / 2, nsz = n2 + 1;
+  constexpr int PI = nsx;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  V* in = reinterpret_cast<V*>(smraw);   // [NZF][PI]
+  V* twz = in + NZF * PI;
+  load_tw(twz, twzf_g, NZF);
+  const int ky = blockIdx.x, p = blockIdx.y;
+  const int ba = band0 + 2 * p, bb = ba + 1;
+  const bool hb = bb < nband;
+  const V* pa = reinterpret_cast<const V*>(psi + (long)ba * ld);
+  const V* pb = reinterpret_cast<const V*>(psi + (long)(hb ? bb : ba) * ld);
+  for (int i = threadIdx.x; i < NZF * PI; i += blockDim.x) in[i] = mkc<V>(0, 0);
+  __syncthreads();
+  const int* mrow = map + (long)ky * nsz * nsx;
+  const T r2 = (T)0.70710678118654752440;
+  for (int i = threadIdx.x; i < nsz * nsx; i += blockDim.x) {
+    const int sz = i / nsx, kx = i - sz * nsx;
+    const int m = mrow[i];
+    if (m == 0) continue;
+    const int s = (m > 0 ? m : -m) - 1;
+    V a = pa[s];
+    V b = hb ? pb[s] : mkc<V>(0, 0);
+    T f = r2;
+    if (s == 0) { a.y = 0; b.y = 0; f = 1; }
+    V z;
+    if (m > 0) z = mkc<V>(f * (a.x - b.y), f * (a.y + b.x));
+    else z = mkc<V>(f * (a.x + b.y), f * (b.x - a.y));
+    in[slot_to_fine(sz, n2, NZF) * PI + kx] = z;
+  }
+  __syncthreads();
+  smem_fft_cb<NZF, +1, PI, 1>(in, nsx, twz);
+  __syncthreads();
+  V* Bp = B + (long)p * NZF * nsy * nsx + (long)ky * nsx;
+  for_rows_cols(NZF, nsx, [&](int z, int kx) { Bp[(long)z * nsy * nsx + kx] = in[z * PI + kx]; });
+}
+
+// forward z transform of a slot row and its mirror row, pair unpack at the
+// stored sphere points, sqrt(2) and the kinetic term ekin_s c_s:
+// out_s (+)= ekin_s c_s + f_s (Vpsi)(G_s),  f_0 = 1, f_s = sqrt(2)
+template <typename T, int N0, int N1, int NZF>
+__global__ void __launch_bounds__(PENCIL_THREADS)
+k_gs_zfwd(const VT<T>* __restrict__ B, const T* __restrict__ psi, int ld, T* __restrict__ out, int ldo, int nband,
+          int band0, int accumulate, const int* __restrict__ map, const T* __restrict__ ekin, const VT<T>* twzf_g) {
+  using V = VT<T>;
+  constexpr int nsx = N0 + 1, nsy = N1 + 1, n2 = NZF / 2, nsz = n2 + 1;
+  constexpr int PI = 2 * nsx + 1;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  V* in = reinterpret_cast<V*>(smraw);   // [NZF][PI]: row r in columns [0, nsx), its mirror in [nsx, 2 nsx)
+  V* twz = in + NZF * PI;
+  load_tw(twz, twzf_g, NZF);
+  const int r = blockIdx.x, p = blockIdx.y;
+  const int rm = mirror_slot(r, N1);
+  const int nrow = (rm == r) ? 1 : 2;
+  const V* Bp = B + (long)p * NZF * nsy * nsx;
+  for_rows_cols(NZF, nrow * nsx, [&](int z, int j) {
+    const int row = j < nsx ? r : rm, kx = j < nsx ? j : j - nsx;
+    cp_async(&in[z * PI + j], &Bp[((long)z * nsy + row) * nsx + kx]);
+  });
+  cp_async_wait_all();
+  __syncthreads();
+  smem_fft_cb<NZF, -1, PI, 1>(in, nrow * nsx, twz);
+  __syncthreads();
+  const int ba = band0 + 2 * p, bb = ba + 1;
+  const bool hb = bb < nband;
+  const V* pa = reinterpret_cast<const V*>(psi + (long)ba * ld);
+  const V* pb = reinterpret_cast<const V*>(psi + (long)(hb ? bb : ba) * ld);
+  V* oa = reinterpret_cast<V*>(out + (long)ba * ldo);
+  V* ob = reinterpret_cast<V*>(out + (long)(hb ? bb : ba) * ldo);
+  const T sq2 = (T)1.41421356237309504880;
+  for (int i = threadIdx.x; i < nrow * nsz * nsx; i += blockDim.x) {
+    const int h = i / (nsz * nsx), rest = i - h * (nsz * nsx);
+    const int sz = rest / nsx, kx = rest - sz * nsx;
+    const int row = h ? rm : r;
+    const int m = map[((long)row * nsz + sz) * nsx + kx];
+    if (m <= 0) continue;
+    const int s = m - 1;
+    const int fz = slot_to_fine(sz, n2, NZF);
+    const int fzm = fz == 0 ? 0 : NZF - fz;
+    // the mirror point -G sits in the other row of the block (the same one for r == rm)
+    const int colm = (nrow == 2 && !h ? nsx : 0) + mirror_slot(kx, N0);
+    const V y = in[fz * PI + h * nsx + kx];
+    const V ym = in[fzm * PI + colm];
+    const T f = s == 0 ? (T)1 : sq2;
+    const T hf = (T)0.5 * f;
+    const T ek = ekin[s];
+    const V ca = pa[s];
+    V va = mkc<V>(hf * (y.x + ym.x) + ek * ca.x, hf * (y.y - ym.y) + ek * ca.y);
+    if (accumulate) va = cadd(va, oa[s]);
+    oa[s] = va;
+    if (hb) {
+      const V cb = pb[s];
+      V vb = mkc<V>(hf * (y.y + ym.y) + ek * cb.x, hf * (ym.x - y.x) + ek * cb.y);
+      if (accumulate) vb = cadd(vb, ob[s]);
+      ob[s] = vb;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // coarse plane inverse: D -> hpsi (two real bands)
 // ---------------------------------------------------------------------------
 template <typename T, int N0, int N1, bool CPLX = false>
@@ -1407,16 +1533,19 @@ struct Plan {
   static int dense_apply_tc(pw_ctx* c, const DenseSet& ds, const float* psi, int ld, float* out, int ldo, int nb,
                             cudaStream_t st) {
     const int np = ds.np, nt = (int)c->ntot, npp = ds.npp;
+    // bf16 row stride: a multiple of 8 elements (16-byte TMA rows); the tensor
+    // maps cover K = nt, so the pad is never read
+    const long ntp = (nt + 7) / 8 * 8;
     int rc;
-    if ((rc = c->s_psi_bf.alloc((size_t)2 * nb * nt * 2))) return rc;
+    if ((rc = c->s_psi_bf.alloc((size_t)2 * nb * ntp * 2))) return rc;
     if ((rc = c->s_w_bf.alloc((size_t)2 * nb * npp * 2))) return rc;
     char* pb = (char*)c->s_psi_bf.p;
     char* wb = (char*)c->s_w_bf.p;
     { Launch L_(c, st, KK_MISC);
-    if ((rc = split_bf16(psi, ld, nt, nb, pb, pb + (size_t)nb * nt * 2, nt, 1.0f, st))) return rc; }
+    if ((rc = split_bf16(psi, ld, nt, nb, pb, pb + (size_t)nb * ntp * 2, ntp, 1.0f, st))) return rc; }
     // W^T[b][l] = d_l * sum_g Q[l][g] psi[b][g]   (split-K, deterministic reduce)
-    SplitOperand A{ds.q_bf, (const char*)ds.q_bf + (size_t)np * nt * 2, np, nt};
-    SplitOperand B{pb, pb + (size_t)nb * nt * 2, nb, nt};
+    SplitOperand A{ds.q_bf, (const char*)ds.q_bf + (size_t)np * ntp * 2, np, ntp};
+    SplitOperand B{pb, pb + (size_t)nb * ntp * 2, nb, ntp};
     ReduceOut ro;
     ro.transpose = 1;
     ro.row_scale = reinterpret_cast<const float*>(ds.qd);
@@ -1568,7 +1697,6 @@ struct Plan {
     V* BC = reinterpret_cast<V*>(c->s_bc.p);
     T* Q = Qout ? Qout : reinterpret_cast<T*>(c->q.p);
     const T inv_nf = (T)(1.0 / (double)c->ntotf);
-    const int ntx = (N0 + TX - 1) / TX;
     const T gx = (T)(2 * M_PI / c->L[0]), gy = (T)(2 * M_PI / c->L[1]), gz = (T)(2 * M_PI / c->L[2]);
     for (int l0 = 0; l0 < nproj; l0 += 2 * cap) {
       const int nl = std::min(2 * cap, nproj - l0);
@@ -1623,7 +1751,70 @@ struct Plan {
     PWB_CUDA(cudaGetLastError());
     return PW_OK;
   }
+  // ---- sphere-cut (G-space) contexts: the G-space grid is (NF0, NF1, NF2) ----
+  static size_t sm_gs_zinv() { return sizeof(V) * ((size_t)NF2 * (N0 + 1) + NF2); }
+  static size_t sm_gs_zfwd() { return sizeof(V) * ((size_t)NF2 * (2 * (N0 + 1) + 1) + NF2); }
+  static int set_attrs_gs() {
+    static bool done = false;
+    if (done) return PW_OK;
+    int rc = set_attrs();
+    if (rc) return rc;
+    PWB_CUDA(cudaFuncSetAttribute(k_gs_zinv<T, N0, N1, NF2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)sm_gs_zinv()));
+    PWB_CUDA(cudaFuncSetAttribute(k_gs_zfwd<T, N0, N1, NF2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)sm_gs_zfwd()));
+    PWB_CUDA(cudaFuncSetAttribute(k_fdens<T, NF0, NF1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_floc()));
+    done = true;
+    return PW_OK;
+  }
+
+  // H c for one batch of npair band pairs of sphere coefficients (real view:
+  // 2 ns reals per band): local + kinetic through the slot layout, then the
+  // nonlocal V (wgt o Re(V^H c)) (EigenSolver::NonlocalMultX,
+  // src/EigenSolver/eigensolver.cpp:471-515) as the dense projector GEMMs on
+  // the real view
+  static int hpsi_gs_batch(pw_ctx* c, const T* psi, int ld, T* out, int ldo, int nband, int band0, int npair,
+                           int accumulate, cudaStream_t st) {
+    int rc = set_attrs_gs();
+    if (rc) return rc;
+    V* BC = reinterpret_cast<V*>(c->s_bc.p);
+    const int* map = reinterpret_cast<const int*>(c->gs_map.p);
+    const T inv_n = (T)(1.0 / (double)c->ntotf);
+    { Launch L_(c, st, KK_ZPAD);
+    k_gs_zinv<T, N0, N1, NF2><<<dim3(N1 + 1, npair), PENCIL_THREADS, sm_gs_zinv(), st>>>(
+        psi, ld, nband, band0, map, BC, tw(c, 5)); }
+    { Launch L_(c, st, KK_FPLANE_APPLY);
+    k_floc2<T, NF0, NF1><<<dim3(NF2, npair), FLOC_THREADS, sm_floc(), st>>>(
+        BC, reinterpret_cast<const T*>(c->vtot.p), inv_n, tw(c, 3), tw(c, 4)); }
+    { Launch L_(c, st, KK_ZFOLD);
+    k_gs_zfwd<T, N0, N1, NF2><<<dim3(N1 / 2 + 1, npair), PENCIL_THREADS, sm_gs_zfwd(), st>>>(
+        BC, psi, ld, out, ldo, nband, band0, accumulate, map, reinterpret_cast<const T*>(c->gs_ekin.p), tw(c, 5)); }
+    PWB_CUDA(cudaGetLastError());
+    const int nb = std::min(2 * npair, nband - band0);
+    if (c->have_nl && c->nproj > 0 && nb > 0)
+      return dense_apply(c, nl_set(c), psi + (long)band0 * ld, ld, out + (long)band0 * ldo, ldo, nb, st);
+    return PW_OK;
+  }
+
+  // rho += sum of w_b |psi_b(r)|^2 from sphere coefficients (CalculateDensity
+  // sphere branch, src/SCF/hamiltonian.cpp:2508-2547, unnormalised)
+  static int density_gs_batch(pw_ctx* c, const T* psi, int ld, int nband, int band0, int npair, const double* w,
+                              double* rho, cudaStream_t st) {
+    int rc = set_attrs_gs();
+    if (rc) return rc;
+    V* BC = reinterpret_cast<V*>(c->s_bc.p);
+    { Launch L_(c, st, KK_DENSITY);
+    k_gs_zinv<T, N0, N1, NF2><<<dim3(N1 + 1, npair), PENCIL_THREADS, sm_gs_zinv(), st>>>(
+        psi, ld, nband, band0, reinterpret_cast<const int*>(c->gs_map.p), BC, tw(c, 5)); }
+    const int ppc = std::max(1, std::min(8, npair));
+    { Launch L_(c, st, KK_DENSITY);
+    k_fdens<T, NF0, NF1><<<dim3(NF2, (npair + ppc - 1) / ppc), FLOC_THREADS, sm_floc(), st>>>(
+        BC, npair, ppc, w + 2 * (band0 / 2), rho, tw(c, 3), tw(c, 4)); }
+    PWB_CUDA(cudaGetLastError());
+    return PW_OK;
+  }
 };
+
 
 // ---------------------------------------------------------------------------
 // dispatch over the instantiated grids
@@ -1683,6 +1874,16 @@ static int hpsikb_thunk(pw_ctx* c, const void* psi, int ld, void* out, int ldo, 
                                            (const T*)ekin_all, (const V*)qk_all);
 }
 template <typename T, int N0, int N1, int N2>
+static int hpsigs_thunk(pw_ctx* c, const void* psi, int ld, void* out, int ldo, int nband, int band0, int npair,
+                        int acc, cudaStream_t st) {
+  return Plan<T, N0, N1, N2>::hpsi_gs_batch(c, (const T*)psi, ld, (T*)out, ldo, nband, band0, npair, acc, st);
+}
+template <typename T, int N0, int N1, int N2>
+static int densgs_thunk(pw_ctx* c, const void* psi, int ld, int nband, int band0, int npair, const double* w,
+                        double* rho, cudaStream_t st) {
+  return Plan<T, N0, N1, N2>::density_gs_batch(c, (const T*)psi, ld, nband, band0, npair, w, rho, st);
+}
+template <typename T, int N0, int N1, int N2>
 static int buildqk_thunk(pw_ctx* c, const int* a, const double* b, const double* d, const long* e, const long* f,
                          const int* g, int n, const double* kv, void* out, cudaStream_t st) {
   return Plan<T, N0, N1, N2>::build_q_k(c, a, b, d, e, f, g, n, kv, (VT<T>*)out, st);
@@ -1699,6 +1900,8 @@ static int buildqk_thunk(pw_ctx* c, const int* a, const double* b, const double*
    {ace_thunk<double, a, b, c>, ace_thunk<float, a, b, c>},                                        \
    {hpsik_thunk<double, a, b, c>, hpsik_thunk<float, a, b, c>},                                    \
    {buildqk_thunk<double, a, b, c>, buildqk_thunk<float, a, b, c>},                                \
-   {hpsikb_thunk<double, a, b, c>, hpsikb_thunk<float, a, b, c>}}
+   {hpsikb_thunk<double, a, b, c>, hpsikb_thunk<float, a, b, c>},                                  \
+   {hpsigs_thunk<double, a, b, c>, hpsigs_thunk<float, a, b, c>},                                  \
+   {densgs_thunk<double, a, b, c>, densgs_thunk<float, a, b, c>}}
 
 }  // namespace pwb

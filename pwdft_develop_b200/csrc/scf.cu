@@ -291,6 +291,11 @@ static int lanczos_upper(Solver& s, int k, double* upper, double* lower) {
   std::vector<double> hv(s.nt);
   double nrm = 0;
   for (auto& x : hv) { x = nd(gen); nrm += x * x; }
+  if (s.c->gs) {
+    // sphere-cut bands: Im c_0 is not a degree of freedom (H maps it to zero)
+    nrm -= hv[1] * hv[1];
+    hv[1] = 0;
+  }
   nrm = std::sqrt(nrm);
   for (auto& x : hv) x /= nrm;
   if (s.c->prec == PW_F64) PWB_CUDA(cudaMemcpy(v.p, hv.data(), s.nt * 8, cudaMemcpyHostToDevice));
@@ -1232,6 +1237,8 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
     if (cur->prec == PW_F64) k_gaussian<double><<<nblk(ntot_b / 4 + 1), 256>>>(ntot_b, p->seed, (double*)sv.X.p);
     else k_gaussian<float><<<nblk(ntot_b / 4 + 1), 256>>>(ntot_b, p->seed, (float*)sv.X.p);
     PWB_CUDA(cudaGetLastError());
+    if (cur->gs)   // sphere-cut bands: Im c_0 = 0
+      PWB_CUDA(cudaMemset2D((char*)sv.X.p + cur->esz, nt * cur->esz, 0, cur->esz, nb));
     if ((rc = cholqr(sv, dn, sv.X.p, nb, sv.Y.p))) return rc;
   }
   if (prof) {
@@ -1507,7 +1514,8 @@ int pw_ctx_build_twin(pw_ctx* ctx) {
   PWB_CHECK(!ctx->atom_z.empty(), PW_ENOTREADY, "atoms not set (pw_set_atoms)");
   if (ctx->twin) return PW_OK;
   pw_ctx* c32 = nullptr;
-  int rc = pw_ctx_create(ctx->L, ctx->n, ctx->nf, PW_F32, ctx->device, &c32);
+  int rc = ctx->gs ? pw_ctx_create_gspace(ctx->L, ctx->nf, ctx->gs_ecut, PW_F32, ctx->device, &c32)
+                   : pw_ctx_create(ctx->L, ctx->n, ctx->nf, PW_F32, ctx->device, &c32);
   if (rc) return rc;
   if ((rc = pw_set_band_batch(c32, std::max(2, 2 * ctx->pair_cap))) ||
       (rc = pw_set_atoms(c32, (int)ctx->atom_z.size(), ctx->atom_z.data(), ctx->atom_pos.data()))) {
@@ -1552,6 +1560,8 @@ int pw_eigsolve(pw_ctx* ctx, int solver, void* X, int nb, int maxit, double tol,
   for (DevBuf* b : {&sv.X, &sv.HX, &sv.Y, &sv.HY, &sv.Z})
     if ((rc = alloc_block(sv, *b, nb))) return rc;
   PWB_CUDA(cudaMemcpy(sv.X.p, X, (size_t)nb * sv.nt * sv.esz, cudaMemcpyDeviceToDevice));
+  if (ctx->gs)   // sphere-cut bands: Im c_0 is not a degree of freedom
+    PWB_CUDA(cudaMemset2D((char*)sv.X.p + ctx->esz, sv.nt * ctx->esz, 0, ctx->esz, nb));
   int it = 0;
   if (solver == PW_SOLVER_LOBPCG) {
     rc = lobpcg(sv, dn, nb, maxit, tol, true, &it);
@@ -1592,6 +1602,9 @@ int pw_eigsolve(pw_ctx* ctx, int solver, void* X, int nb, int maxit, double tol,
 int pw_density(pw_ctx* ctx, const void* psi, int ld, int nband, const double* occ_host, int nocc_total,
                double* rho_dev) {
   PWB_CHECK(ctx && psi && occ_host && rho_dev && nband > 0, PW_EINVAL, "bad arguments");
+  PWB_CHECK(ld >= ctx->ntot, PW_EINVAL, "Domain size does not match.");
+  PWB_CHECK(!ctx->gs || (ld % 2 == 0 && (uintptr_t)psi % (2 * ctx->esz) == 0), PW_EINVAL,
+            "G-space bands are complex: even leading dimension and complex-aligned pointer");
   PWB_CUDA(cudaSetDevice(ctx->device));
   DevBuf wv;
   int rc = wv.alloc((nband + 2) * 8);
