@@ -440,6 +440,67 @@ def kpoint_bench(device: int, reps: int = 5):
             "ms_per_pass": ms, "k_bands_per_s": len(kpts) * nb / (ms / 1e3)}
 
 
+def gspace_bench(device: int, reps: int = 10):
+    """Sphere-cut (G-space) H*psi on the Si64 cell: 96^3 G-space grid, Ecut
+    25 Ha, 160 bands of half-sphere coefficients, Fourier-space HGH
+    projectors; device-timed per sweep with the L2 flushed in between.  Byte
+    model per band pair: the slot field (N x (n+1)^2 complex) is written by
+    the scatter, read and written by the fine-plane kernel and read by the
+    gather (4 passes), and the two bands are read once and written once
+    (2 x 2 x 2 ns s)."""
+    import torch
+    from pwdft_develop_b200 import Context
+    from pwdft_develop_b200.core import KERNEL_KINDS
+    L, z, pos = si64_atoms()
+    N, ecut = (96, 96, 96), 25.0
+    peak = load_peaks()[0]
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    out = {"workload": "Si64 sphere-cut: 96^3 G-space grid, Ecut 25 Ha, 160 bands, Fourier-space HGH projectors "
+                       "(Use_Real_Space 0)"}
+    for prec in ("f32", "f64"):
+        c = Context.gspace(L, N, ecut, precision=prec, device=device)
+        c.set_atoms(z, pos)
+        c.set_vtot(synthetic_vtot(c.ntotFine))
+        c.set_band_batch(NBAND)
+        g = torch.Generator(device="cuda").manual_seed(SEED + 11)
+        X = torch.randn((NBAND, c.ntot), dtype=c.torch_dtype, device="cuda", generator=g)
+        X[:, 1] = 0                                    # Im c_0
+        Y = torch.empty_like(X)
+        for _ in range(3):
+            c.hpsi(X, out=Y)
+        torch.cuda.synchronize()
+        c.profile(True)
+        ms = 0.0
+        for _ in range(reps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            c.hpsi(X, out=Y)
+            e1.record()
+            torch.cuda.synchronize()
+            ms += e0.elapsed_time(e1)
+        ms /= reps
+        kern = {}
+        rename = {"z_pad": "sphere_scatter_z_inverse", "z_fold": "z_forward_sphere_gather",
+                  "gram": "projector_gemm", "other": "bf16_split"}
+        for kind, name in KERNEL_KINDS.items():
+            t, n = c.profile_read(kind)
+            if n:
+                kern[rename.get(name, name)] = {"launches": n, "avg_us": t / n * 1e3}
+        c.profile(False)
+        s = 4 if prec == "f32" else 8
+        ns = c.ns
+        field = N[2] * (N[1] // 2 + 1) * (N[0] // 2 + 1) * 2 * s
+        pair_bytes = 4 * field + 2 * (2 * 2 * ns * s)
+        bands_per_s = NBAND / (ms / 1e3)
+        out[prec] = {"ns": ns, "ms_per_sweep": ms, "bands_per_s": bands_per_s,
+                     "model_bytes_per_band": pair_bytes / 2,
+                     "model_frac_of_hbm": pair_bytes / 2 * bands_per_s / (peak * 1e9), "kernels": kern}
+        c.close()
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -613,6 +674,8 @@ def run_ours(args):
             line["exx"] = exx_bench(local)
         if args.kpoints and world == 1:
             line["kpoints"] = kpoint_bench(local)
+        if args.gspace and world == 1:
+            line["gspace"] = gspace_bench(local)
         if args.cells and world == 1:
             line["cells"] = cells_bench(local)
         if args.grams and world == 1:
@@ -637,6 +700,7 @@ def main():
     ap.add_argument("--no-scf", dest="scf", action="store_false", help="skip the SCF time-to-solution leg")
     ap.add_argument("--no-exx", dest="exx", action="store_false", help="skip the hybrid-exchange leg")
     ap.add_argument("--no-kpoints", dest="kpoints", action="store_false", help="skip the k-point batch leg")
+    ap.add_argument("--no-gspace", dest="gspace", action="store_false", help="skip the sphere-cut (G-space) leg")
     ap.add_argument("--no-cells", dest="cells", action="store_false", help="skip the uneven-cell batch leg")
     ap.add_argument("--no-grams", dest="grams", action="store_false", help="skip the eigensolver Gram leg")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
