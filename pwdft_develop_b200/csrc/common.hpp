@@ -137,7 +137,8 @@ struct pw_ctx {
   bool gs = false;
   double gs_ecut = 0.0;
   int gs_ns = 0;
-  pwb::DevBuf gs_map;               // int [n1+1][n2+1][n0+1] slot -> sphere point map
+  pwb::DevBuf gs_rows_inv, gs_ent_inv;   // scatter lists: int [n1+2] row offsets, int2 entries
+  pwb::DevBuf gs_rows_fwd, gs_ent_fwd;   // gather lists: int [n1/2+2] block offsets, int2 entries
   pwb::DevBuf gs_ekin, gs_teter;    // T [ns]
   std::vector<int> h_gs_idx;        // idxCoarseCut: flat R2C index of each sphere point
   std::vector<int> h_gs_m;          // 3 signed Miller indices per sphere point

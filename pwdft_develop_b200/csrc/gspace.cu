@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <utility>
 #include <cmath>
 #include <string>
 #include <vector>
@@ -30,8 +31,11 @@ int install_dense_q(pw_ctx* ctx, int nproj);
 
 namespace {
 
-// slot of a signed frequency f in [-n/2, n/2]
+// slot of a signed frequency f in [-n/2, n/2]; the fine (G-space grid)
+// index of a slot; the slot of the opposite frequency
 inline int slot_of(int f, int n) { return f >= 0 ? f : (f == -n / 2 ? n : n + f); }
+inline int slot_to_fine(int s, int n, int nf) { return s <= n / 2 ? s : (s < n ? nf - n + s : nf - n / 2); }
+inline int mirror_slot(int s, int n) { return s == 0 ? 0 : (s == n / 2 ? n : (s == n ? n / 2 : n - s)); }
 inline int kgrid(int i, int n) { return i <= n / 2 ? i : i - n; }
 
 template <typename T>
@@ -276,29 +280,67 @@ int pw_ctx_create_gspace(const double length[3], const int numGrid[3], double ec
     const double b = 27.0 + a * (18.0 + a * (12.0 + a * 8.0));
     te[s] = b / (b + 16.0 * std::pow(a, 4.0));
   }
-  // slot map [ky][kz][kx]: s + 1 at G_s, -(s + 1) at -G_s
+  // Entry lists of the scatter kernel (one block per slot row, all points
+  // G_s and -G_s of the row) and of the gather kernel (one block per slot
+  // row r <= n1/2 and its mirror row, the stored points G_s), in the shared
+  // memory layouts of k_gs_zinv ([N_z][n0+1]) and k_gs_zfwd ([N_z][2(n0+1)+1])
   const int nsx = box[0] + 1, nsy = box[1] + 1, nsz = box[2] + 1;
-  std::vector<int> map((size_t)nsx * nsy * nsz, 0);
+  const int pi1 = nsx, pi2 = 2 * nsx + 1, nblk = box[1] / 2 + 1;
+  std::vector<char> used((size_t)nsx * nsy * nsz, 0);
+  std::vector<std::vector<int>> inv_rows(nsy), fwd_rows(nblk);
   for (int s = 0; s < ns; ++s) {
     const int* m = &c->h_gs_m[3 * s];
     for (int sg = 1; sg >= -1; sg -= 2) {
       if (s == 0 && sg < 0) break;
       const int sx = slot_of(sg * m[0], box[0]), sy = slot_of(sg * m[1], box[1]), sz = slot_of(sg * m[2], box[2]);
-      int& e = map[((size_t)sy * nsz + sz) * nsx + sx];
-      if (e != 0) { delete c; set_error("sphere slot map collision"); return PW_EINVAL; }
-      e = sg * (s + 1);
+      char& u = used[((size_t)sy * nsz + sz) * nsx + sx];
+      if (u) { delete c; set_error("sphere slot collision"); return PW_EINVAL; }
+      u = 1;
+      const int fz = slot_to_fine(sz, box[2], n2);
+      inv_rows[sy].insert(inv_rows[sy].end(), {sg * (s + 1), fz * pi1 + sx});
+      if (sg < 0) continue;
+      const int h = sy <= box[1] / 2 ? 0 : 1;
+      const int r = h ? mirror_slot(sy, box[1]) : sy;
+      const int nrow = mirror_slot(r, box[1]) == r ? 1 : 2;
+      const int fzm = fz == 0 ? 0 : n2 - fz;
+      const int off = fz * pi2 + h * nsx + sx;
+      const int offm = fzm * pi2 + (nrow == 2 && h == 0 ? nsx : 0) + mirror_slot(sx, box[0]);
+      fwd_rows[r].insert(fwd_rows[r].end(), {s, off | (offm << 16)});
     }
   }
+  PWB_CHECK((long)n2 * pi2 < 65536, PW_EUNSUPPORTED, "G-space grid too large for the gather offsets");
+  // entries of a block in shared-memory offset order: a warp's stores (scatter)
+  // and loads (gather) then walk along kx, where consecutive sphere indices sit
+  auto flatten = [](const std::vector<std::vector<int>>& rows, std::vector<int>& ptr, std::vector<int>& ent) {
+    ptr.assign(1, 0);
+    for (const auto& r : rows) {
+      std::vector<std::pair<int, int>> e(r.size() / 2);
+      for (size_t i = 0; i < e.size(); ++i) e[i] = {r[2 * i], r[2 * i + 1]};
+      std::stable_sort(e.begin(), e.end(), [](const std::pair<int, int>& a, const std::pair<int, int>& b) {
+        return (a.second & 0xffff) < (b.second & 0xffff);
+      });
+      for (const auto& x : e) ent.insert(ent.end(), {x.first, x.second});
+      ptr.push_back((int)(ent.size() / 2));
+    }
+  };
+  std::vector<int> iptr, ient, fptr, fent;
+  flatten(inv_rows, iptr, ient);
+  flatten(fwd_rows, fptr, fent);
+  auto up = [](DevBuf& b, const std::vector<int>& v) -> int {
+    int r = b.alloc(std::max<size_t>(v.size(), 2) * 4);
+    if (r) return r;
+    if (cudaMemcpy(b.p, v.data(), v.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
+      set_error("cudaMemcpy of the sphere lists failed");
+      return PW_ECUDA;
+    }
+    return PW_OK;
+  };
   int rc;
   if ((rc = upload_real(c, c->gs_ekin, ek.data(), ns)) || (rc = upload_real(c, c->gs_teter, te.data(), ns)) ||
-      (rc = c->gs_map.alloc(map.size() * 4))) {
+      (rc = up(c->gs_rows_inv, iptr)) || (rc = up(c->gs_ent_inv, ient)) || (rc = up(c->gs_rows_fwd, fptr)) ||
+      (rc = up(c->gs_ent_fwd, fent))) {
     delete c;
     return rc;
-  }
-  if (cudaMemcpy(c->gs_map.p, map.data(), map.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
-    delete c;
-    set_error("cudaMemcpy of the sphere map failed");
-    return PW_ECUDA;
   }
   const int lens[6] = {box[0], box[1], box[2], n0, n1, n2};
   for (int s = 0; s < 6; ++s)

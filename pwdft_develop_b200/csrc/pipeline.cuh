@@ -1105,23 +1105,23 @@ k_zteter(VT<T>* __restrict__ A, const T* __restrict__ teter, int n0, int n1, T i
 // stored half giving Z(G) = a' + i b' and the mirrored half
 // Z(-G) = conj(a') + i conj(b') (a' = c_a / sqrt(2), c_0 real).
 //
-// map: int [nsy][nsz][nsx] over slots: 0 empty, s+1 stored point s,
-// -(s+1) the mirror -G of stored point s.
+// Per-row entry lists (built with the context, CSR by block):
+//   scatter list, one block per slot row ky: {s+1 at G_s or -(s+1) at -G_s,
+//     shared-memory offset fine_z * (n0+1) + kx_slot}
+//   gather list, one block per slot row r <= n1/2 and its mirror row: {s,
+//     offset of G_s | offset of -G_s << 16} in the block's two-row layout
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ int slot_to_fine(int s, int n, int nf) {
-  return s <= n / 2 ? s : (s < n ? nf - n + s : nf - n / 2);
-}
 __device__ __forceinline__ int mirror_slot(int s, int n) {
   return s == 0 ? 0 : (s == n / 2 ? n : (s == n ? n / 2 : n - s));
 }
 
 // sphere scatter + inverse z transform of one slot row (all kx slots) of a pair
 template <typename T, int N0, int N1, int NZF>
-__global__ void __launch_bounds__(PENCIL_THREADS)
-k_gs_zinv(const T* __restrict__ psi, int ld, int nband, int band0, const int* __restrict__ map,
-          VT<T>* __restrict__ B, const VT<T>* twzf_g) {
+__global__ void __launch_bounds__(PENCIL_THREADS, sizeof(T) == 4 ? 4 : 2)
+k_gs_zinv(const T* __restrict__ psi, int ld, int nband, int band0, const int* __restrict__ rows,
+          const int2* __restrict__ ent, VT<T>* __restrict__ B, const VT<T>* twzf_g) {
   using V = VT<T>;
-  constexpr int nsx = N0 + 1, nsy = N1 + 1, n2 = NZF / 2, nsz = n2 + 1;
+  constexpr int nsx = N0 + 1, nsy = N1 + 1;
   constexpr int PI = nsx;
   extern __shared__ __align__(16) unsigned char smraw[];
   V* in = reinterpret_cast<V*>(smraw);   // [NZF][PI]
@@ -1134,12 +1134,11 @@ k_gs_zinv(const T* __restrict__ psi, int ld, int nband, int band0, const int* __
   const V* pb = reinterpret_cast<const V*>(psi + (long)(hb ? bb : ba) * ld);
   for (int i = threadIdx.x; i < NZF * PI; i += blockDim.x) in[i] = mkc<V>(0, 0);
   __syncthreads();
-  const int* mrow = map + (long)ky * nsz * nsx;
   const T r2 = (T)0.70710678118654752440;
-  for (int i = threadIdx.x; i < nsz * nsx; i += blockDim.x) {
-    const int sz = i / nsx, kx = i - sz * nsx;
-    const int m = mrow[i];
-    if (m == 0) continue;
+  const int e1 = rows[ky + 1];
+  for (int e = rows[ky] + threadIdx.x; e < e1; e += blockDim.x) {
+    const int2 en = ent[e];
+    const int m = en.x;
     const int s = (m > 0 ? m : -m) - 1;
     V a = pa[s];
     V b = hb ? pb[s] : mkc<V>(0, 0);
@@ -1148,7 +1147,7 @@ k_gs_zinv(const T* __restrict__ psi, int ld, int nband, int band0, const int* __
     V z;
     if (m > 0) z = mkc<V>(f * (a.x - b.y), f * (a.y + b.x));
     else z = mkc<V>(f * (a.x + b.y), f * (b.x - a.y));
-    in[slot_to_fine(sz, n2, NZF) * PI + kx] = z;
+    in[en.y] = z;
   }
   __syncthreads();
   smem_fft_cb<NZF, +1, PI, 1>(in, nsx, twz);
@@ -1163,9 +1162,10 @@ k_gs_zinv(const T* __restrict__ psi, int ld, int nband, int band0, const int* __
 template <typename T, int N0, int N1, int NZF>
 __global__ void __launch_bounds__(PENCIL_THREADS)
 k_gs_zfwd(const VT<T>* __restrict__ B, const T* __restrict__ psi, int ld, T* __restrict__ out, int ldo, int nband,
-          int band0, int accumulate, const int* __restrict__ map, const T* __restrict__ ekin, const VT<T>* twzf_g) {
+          int band0, int accumulate, const int* __restrict__ rows, const int2* __restrict__ ent,
+          const T* __restrict__ ekin, const VT<T>* twzf_g) {
   using V = VT<T>;
-  constexpr int nsx = N0 + 1, nsy = N1 + 1, n2 = NZF / 2, nsz = n2 + 1;
+  constexpr int nsx = N0 + 1, nsy = N1 + 1;
   constexpr int PI = 2 * nsx + 1;
   extern __shared__ __align__(16) unsigned char smraw[];
   V* in = reinterpret_cast<V*>(smraw);   // [NZF][PI]: row r in columns [0, nsx), its mirror in [nsx, 2 nsx)
@@ -1190,19 +1190,13 @@ k_gs_zfwd(const VT<T>* __restrict__ B, const T* __restrict__ psi, int ld, T* __r
   V* oa = reinterpret_cast<V*>(out + (long)ba * ldo);
   V* ob = reinterpret_cast<V*>(out + (long)(hb ? bb : ba) * ldo);
   const T sq2 = (T)1.41421356237309504880;
-  for (int i = threadIdx.x; i < nrow * nsz * nsx; i += blockDim.x) {
-    const int h = i / (nsz * nsx), rest = i - h * (nsz * nsx);
-    const int sz = rest / nsx, kx = rest - sz * nsx;
-    const int row = h ? rm : r;
-    const int m = map[((long)row * nsz + sz) * nsx + kx];
-    if (m <= 0) continue;
-    const int s = m - 1;
-    const int fz = slot_to_fine(sz, n2, NZF);
-    const int fzm = fz == 0 ? 0 : NZF - fz;
-    // the mirror point -G sits in the other row of the block (the same one for r == rm)
-    const int colm = (nrow == 2 && !h ? nsx : 0) + mirror_slot(kx, N0);
-    const V y = in[fz * PI + h * nsx + kx];
-    const V ym = in[fzm * PI + colm];
+  const int e1 = rows[r + 1];
+  for (int e = rows[r] + threadIdx.x; e < e1; e += blockDim.x) {
+    const int2 en = ent[e];
+    const int s = en.x;
+    // G_s and its mirror -G_s (in the other row of the block, or the same row for r == rm)
+    const V y = in[en.y & 0xffff];
+    const V ym = in[(unsigned)en.y >> 16];
     const T f = s == 0 ? (T)1 : sq2;
     const T hf = (T)0.5 * f;
     const T ek = ekin[s];
@@ -1778,17 +1772,19 @@ struct Plan {
     int rc = set_attrs_gs();
     if (rc) return rc;
     V* BC = reinterpret_cast<V*>(c->s_bc.p);
-    const int* map = reinterpret_cast<const int*>(c->gs_map.p);
+    const int* rows_i = reinterpret_cast<const int*>(c->gs_rows_inv.p);
+    const int2* ent_i = reinterpret_cast<const int2*>(c->gs_ent_inv.p);
     const T inv_n = (T)(1.0 / (double)c->ntotf);
     { Launch L_(c, st, KK_ZPAD);
     k_gs_zinv<T, N0, N1, NF2><<<dim3(N1 + 1, npair), PENCIL_THREADS, sm_gs_zinv(), st>>>(
-        psi, ld, nband, band0, map, BC, tw(c, 5)); }
+        psi, ld, nband, band0, rows_i, ent_i, BC, tw(c, 5)); }
     { Launch L_(c, st, KK_FPLANE_APPLY);
     k_floc2<T, NF0, NF1><<<dim3(NF2, npair), FLOC_THREADS, sm_floc(), st>>>(
         BC, reinterpret_cast<const T*>(c->vtot.p), inv_n, tw(c, 3), tw(c, 4)); }
     { Launch L_(c, st, KK_ZFOLD);
     k_gs_zfwd<T, N0, N1, NF2><<<dim3(N1 / 2 + 1, npair), PENCIL_THREADS, sm_gs_zfwd(), st>>>(
-        BC, psi, ld, out, ldo, nband, band0, accumulate, map, reinterpret_cast<const T*>(c->gs_ekin.p), tw(c, 5)); }
+        BC, psi, ld, out, ldo, nband, band0, accumulate, reinterpret_cast<const int*>(c->gs_rows_fwd.p),
+        reinterpret_cast<const int2*>(c->gs_ent_fwd.p), reinterpret_cast<const T*>(c->gs_ekin.p), tw(c, 5)); }
     PWB_CUDA(cudaGetLastError());
     const int nb = std::min(2 * npair, nband - band0);
     if (c->have_nl && c->nproj > 0 && nb > 0)
@@ -1805,7 +1801,8 @@ struct Plan {
     V* BC = reinterpret_cast<V*>(c->s_bc.p);
     { Launch L_(c, st, KK_DENSITY);
     k_gs_zinv<T, N0, N1, NF2><<<dim3(N1 + 1, npair), PENCIL_THREADS, sm_gs_zinv(), st>>>(
-        psi, ld, nband, band0, reinterpret_cast<const int*>(c->gs_map.p), BC, tw(c, 5)); }
+        psi, ld, nband, band0, reinterpret_cast<const int*>(c->gs_rows_inv.p),
+        reinterpret_cast<const int2*>(c->gs_ent_inv.p), BC, tw(c, 5)); }
     const int ppc = std::max(1, std::min(8, npair));
     { Launch L_(c, st, KK_DENSITY);
     k_fdens<T, NF0, NF1><<<dim3(NF2, (npair + ppc - 1) / ppc), FLOC_THREADS, sm_floc(), st>>>(
