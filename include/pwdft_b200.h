@@ -208,6 +208,16 @@ PW_API int pw_hartree(pw_ctx* ctx, const double* drho_dev, double ecut, double* 
  * grid (device), points with rho < 1e-10 zeroed -- KohnSham::CalculateXC
  * (src/SCF/hamiltonian.cpp:1278-1308). */
 PW_API int pw_xc_teter93(pw_ctx* ctx, const double* rho_dev, double* eps_dev, double* vxc_dev);
+/* PBE exchange-correlation on the fine grid (device, N_fine doubles each): the
+ * Use_Libxc 0 branch of KohnSham::CalculateXC (src/SCF/hamiltonian.cpp:
+ * 1381-1419, 1560-1612, 1680-1760; Slater + PW92 + PBE gradient corrections of
+ * src/utility.cpp:3913-4244) with the spectral gradient of
+ * KohnSham::CalculateGradDensity (hamiltonian.cpp:1153-1239; components with
+ * gkk = 0 or gkk > 4 ecut dropped).  eps: energy per particle (E_xc = sum eps
+ * rho vol / N_fine); vxc = d e/d rho - div(2 d e/d|grad rho|^2 grad rho).
+ * Cubic cells and fine grids only. */
+PW_API int pw_xc_pbe(pw_ctx* ctx, const double* rho_dev, double ecut, double* eps_dev, double* vxc_dev);
+enum { PW_XC_TETER93 = 0, PW_XC_PBE = 1 };
 
 typedef struct pw_scf_params {
   int nocc;                 /* occupied states (numOccupiedState) */
@@ -230,6 +240,7 @@ typedef struct pw_scf_params {
   int ppcg_sbsize;          /* PPCG_sbSize (PW_SOLVER_PPCG), 1..8 */
   int davidson_maxdim;      /* subspace size in blocks (PW_SOLVER_DAVIDSON), >= 2 */
   int graphs;               /* 1: replay the Chebyshev filter from a captured CUDA graph */
+  int xc;                   /* PW_XC_TETER93 (LDA, default) or PW_XC_PBE (XC_Type XC_GGA_XC_PBE, Use_Libxc 0) */
 } pw_scf_params;
 
 typedef struct pw_scf_result {

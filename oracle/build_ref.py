@@ -4,8 +4,10 @@ Test infrastructure.  The reference's full build needs MPI, FFTW, MKL,
 libxc and yaml-cpp, which are absent, so it cannot be built.  Four of its
 functions are self-contained and are compiled here directly from the
 reference source tree (never copied into this repository): ``spline`` and
-``seval`` (src/utility.cpp:54-225) and ``IP_c2f`` / ``IP_f2c``
-(src/utility.cpp:3148-3275).  The recipe extracts each function body from
+``seval`` (src/utility.cpp:54-225), ``IP_c2f`` / ``IP_f2c``
+(src/utility.cpp:3148-3275) and the internal PBE pieces ``VExchange_sla``,
+``VCorrelation_pw``, ``VGCExchange_pbx``, ``VGCCorrelation_pbc``
+(src/utility.cpp:3913-4244, the ``Use_Libxc: 0`` path of KohnSham::CalculateXC).  The recipe extracts each function body from
 ``<reference>/src/utility.cpp`` by brace matching into ``oracle/_ref/`` (git
 ignored), prepends the two typedefs it needs, adds extern "C" wrappers and
 builds a shared object with g++.  Tests use it to pin the NumPy restatement.
@@ -23,12 +25,17 @@ LIB = OUT / "libpwref.so"
 DEFAULT_REF = Path(os.environ.get("PWDFT_REFERENCE", "/root/reference"))
 
 FUNCS = [("void spline(", "spline"), ("void seval(", "seval"),
-         ("void IP_c2f(", "IP_c2f"), ("void IP_f2c(", "IP_f2c")]
+         ("void IP_c2f(", "IP_c2f"), ("void IP_f2c(", "IP_f2c"),
+         ("void VExchange_sla(", "VExchange_sla"), ("void VCorrelation_pw(", "VCorrelation_pw"),
+         ("void VGCExchange_pbx(", "VGCExchange_pbx"), ("void VGCCorrelation_pbc(", "VGCCorrelation_pbc")]
 
 PRELUDE = """// generated: functions compiled from the reference source tree
+#include <cmath>
 #include <complex>
 #include <stdexcept>
 typedef std::complex<double> Complex;
+typedef double Real;
+static const double PI = 3.141592653589793;
 static void ErrorHandling(const char* m) { throw std::runtime_error(m); }
 namespace pwref {
 """
@@ -45,6 +52,13 @@ void ref_ip_c2f(int* Nc, int* Nf, double* tilde, double* tildef) {
 }
 void ref_ip_f2c(int* Nc, int* Nf, double* tilde, double* tildef) {
   pwref::IP_f2c(Nc, Nf, reinterpret_cast<Complex*>(tilde), reinterpret_cast<Complex*>(tildef));
+}
+// out: ux vx (Slater, at rs) uc vc (PW92, at rs) ugcx v1gcx v2gcx ugcc v1gcc v2gcc (PBE, at rho, grho2)
+void ref_pbe_parts(double rs, double rho, double grho2, double* out) {
+  pwref::VExchange_sla(rs, out[0], out[1]);
+  pwref::VCorrelation_pw(rs, out[2], out[3]);
+  pwref::VGCExchange_pbx(rho, grho2, out[4], out[5], out[6]);
+  pwref::VGCCorrelation_pbc(rho, grho2, out[7], out[8], out[9]);
 }
 }
 """

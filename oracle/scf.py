@@ -6,6 +6,12 @@ Test infrastructure (see ``oracle/__init__.py``).  Follows:
   * KohnSham::CalculateXC         src/SCF/hamiltonian.cpp:1242-1308 (LDA Teter93; the
     reference calls libxc XC_LDA_XC_TETER93, restated here from Goedecker, Teter,
     Hutter, PRB 54, 1703 (1996); parity at the libxc boundary is unpinned)
+  * KohnSham::CalculateGradDensity src/SCF/hamiltonian.cpp:1153-1239 and the PBE
+    branch of CalculateXC without libxc (Use_Libxc 0), hamiltonian.cpp:1381-1419,
+    1560-1612, 1680-1760: Slater + PW92 LDA, PBE gradient corrections
+    (VExchange_sla, VCorrelation_pw, VGCExchange_pbx, VGCCorrelation_pbc,
+    src/utility.cpp:3913-4244; pinned by tests/golden/ref_xc_pbe.npz from those
+    functions), V_xc = v1 - div(v2 grad rho) with spectral derivatives
   * KohnSham::CalculateVtot       src/SCF/hamiltonian.cpp:2029-2069 (Use_VLocal 0)
   * SCF::CalculateOccupationRate  src/SCF/scf.cpp:1748-1830, wgauss/getEntropy
     src/utility.cpp:4404-4444
@@ -53,6 +59,129 @@ def xc_teter93(rho: np.ndarray):
     eps = np.where(bad, 0.0, eps)
     v = np.where(bad, 0.0, v)
     return eps, v
+
+
+# ---------------------------------------------------------------------------
+# PBE (unpolarised), Perdew-Burke-Ernzerhof PRL 77, 3865 (1996) with the
+# Perdew-Wang 1992 LDA correlation, in the constants of the reference's
+# internal functions (src/utility.cpp:3913-4244)
+# ---------------------------------------------------------------------------
+_SLATER = -0.458165293283143               # -(3/4pi) (9pi/4)^(1/3)
+_PW92 = (0.031091, 0.21370, 7.5957, 3.5876, 1.6382, 0.49294)     # A, alpha1, beta1..beta4
+_KAPPA, _MU = 0.804, 0.2195149727645171
+_GAMMA, _BETA = 0.03109069086965, 0.06672455060314922
+_C2 = 3.093667726280136                    # (3 pi^2)^(1/3)
+_PI34, _XKF, _XKS = 0.6203504908994, 1.919158292677513, 1.128379167095513
+
+
+def slater(rs):
+    """(eps_x, v_x) of the uniform gas at rs (VExchange_sla)."""
+    ux = _SLATER / rs
+    return ux, 4.0 / 3.0 * ux
+
+
+def pw92(rs):
+    """(eps_c, v_c = eps_c - rs/3 d eps_c/d rs) (VCorrelation_pw)."""
+    a, a1, b1, b2, b3, b4 = _PW92
+    q = np.sqrt(rs)
+    om = 2 * a * (b1 * q + b2 * rs + b3 * rs * q + b4 * rs * rs)
+    rdom = 2 * a * (0.5 * b1 * q + b2 * rs + 1.5 * b3 * rs * q + 2 * b4 * rs * rs)   # rs d om / d rs
+    lg = np.log(1 + 1 / om)
+    ec = -2 * a * (1 + a1 * rs) * lg
+    vc = -2 * a * (1 + 2.0 / 3.0 * a1 * rs) * lg - 2.0 / 3.0 * a * (1 + a1 * rs) * rdom / (om * (om + 1))
+    return ec, vc
+
+
+def pbe_x(rho, sigma):
+    """Gradient part of PBE exchange: (e per particle, d(rho e)/d rho, 2 d(rho e)/d sigma)
+    with F_x - 1 = kappa - kappa / (1 + mu s^2 / kappa), s = |grad rho| / (2 k_F rho)
+    (VGCExchange_pbx)."""
+    g = np.sqrt(sigma)
+    kf = _C2 * np.power(rho, 1.0 / 3.0)
+    dsg = 0.5 / kf
+    sr = g * dsg / rho
+    den = 1 + sr * sr * _MU / _KAPPA
+    fx = _KAPPA - _KAPPA / den
+    exu = -0.75 / math.pi * kf
+    dfx = 2 * _MU * sr / (den * den)
+    e = exu * fx
+    return e, e + exu / 3 * fx - exu * dfx * (4.0 / 3.0) * sr, exu * dfx * dsg / g
+
+
+def pbe_c(rho, sigma):
+    """Gradient part of PBE correlation H(t, A) (VGCCorrelation_pbc):
+    (H, d(rho H)/d rho, 2 d(rho H)/d sigma)."""
+    rs = _PI34 / np.power(rho, 1.0 / 3.0)
+    ec, vc = pw92(rs)
+    ks = _XKS * np.sqrt(_XKF / rs)
+    t2 = sigma / (2 * ks * rho) ** 2
+    ex = np.exp(-ec / _GAMMA)
+    A = _BETA / _GAMMA * (1.0 / (ex - 1.0))
+    y = A * t2
+    d = 1 + y + y * y
+    xy = (1 + y) / d
+    qy = y * y * (2 + y) / (d * d)
+    s1 = 1 + _BETA / _GAMMA * t2 * xy
+    H = _GAMMA * np.log(s1)
+    # rho dH/drho: t^2 ~ rho^(-7/3) and A through eps_c (rho d eps_c / d rho = v_c - eps_c)
+    rdh = _BETA * t2 / s1 * (-7.0 / 3.0 * xy - qy * (A * ex * (vc - ec) / _BETA - 7.0 / 3.0))
+    return H, H + rdh, _BETA / (2 * ks * ks * rho) * (xy - qy) / s1
+
+
+def xc_pbe_point(rho, sigma):
+    """Per point (hamiltonian.cpp:1581-1612): LDA part where |rho| > 1e-10,
+    gradient part where |rho| > 1e-6 and sigma > 1e-10.  Returns (eps per
+    particle, v1 = d e/d rho, v2 = 2 d e/d sigma) with e = rho eps."""
+    rho = np.asarray(rho, np.float64)
+    sigma = np.asarray(sigma, np.float64)
+    ar = np.abs(rho)
+    eps = np.zeros_like(rho)
+    v1 = np.zeros_like(rho)
+    v2 = np.zeros_like(rho)
+    m = ar > 1e-10
+    if m.any():
+        rs = np.power(3.0 / 4.0 / math.pi / ar[m], 1.0 / 3.0)
+        ux, vx = slater(rs)
+        uc, vc = pw92(rs)
+        eps[m] += ux + uc
+        v1[m] += vx + vc
+    g = (ar > 1e-6) & (sigma > 1e-10)
+    if g.any():
+        ex, v1x, v2x = pbe_x(ar[g], sigma[g])
+        ec, v1c, v2c = pbe_c(ar[g], sigma[g])
+        eps[g] += ex + ec
+        v1[g] += v1x + v1c
+        v2[g] += v2x + v2c
+    return eps, v1, v2
+
+
+def _spectral_ik(dm: pw.Domain, ecut: float):
+    """i G_d on the fine grid, zero where gkk = 0 or gkk > 4 Ecut (ikFine with the
+    cut of hamiltonian.cpp:1196-1201)."""
+    g = pw.gvec_full(dm, fine=True)
+    gkk = 0.5 * np.sum(g * g, axis=-1)
+    keep = ~((gkk == 0) | (gkk > 4.0 * ecut))
+    return [1j * g[..., d] * keep for d in range(3)]
+
+
+def grad_density(dm: pw.Domain, rho: np.ndarray, ecut: float):
+    """CalculateGradDensity: d_d rho = Re IFFT(i G_d FFT(rho)) with the cut."""
+    N0, N1, N2 = dm.numGridFine
+    X = np.fft.fftn(rho.reshape(N2, N1, N0))
+    return np.stack([np.fft.ifftn(X * ik).real.reshape(-1) for ik in _spectral_ik(dm, ecut)])
+
+
+def xc_pbe(dm: pw.Domain, rho: np.ndarray, ecut: float):
+    """(eps per particle, V_xc) of PBE: V_xc = v1 - sum_d d_d(v2 d_d rho), the
+    divergence spectral with the same cut (hamiltonian.cpp:1750-1775)."""
+    N0, N1, N2 = dm.numGridFine
+    gr = grad_density(dm, rho, ecut)
+    sigma = np.sum(gr * gr, axis=0)
+    eps, v1, v2 = xc_pbe_point(rho, sigma)
+    div = np.zeros((N2, N1, N0), complex)
+    for d, ik in enumerate(_spectral_ik(dm, ecut)):
+        div += np.fft.fftn((v2 * gr[d]).reshape(N2, N1, N0)) * ik
+    return eps, v1 - np.fft.ifftn(div).real.reshape(-1)
 
 
 def density(T: pw.HamTables, psi: np.ndarray, occ: np.ndarray, nocc: int, numSpin: int = 2, chunk: int = 16):
@@ -168,7 +297,7 @@ def _eigsh(T: pw.HamTables, nband: int, v0=None, tol=1e-11):
 
 def scf(L, znuc, pos, numGrid, numGridFine, nocc: int, nextra: int, ecut: float,
         temperature: float = 300.0, tol_efree: float = 1e-7, max_iter: int = 60, mix_dim: int = 8,
-        mix_step: float = 0.7, eig_tol: float = 1e-11, verbose: bool = False) -> SCFResult:
+        mix_step: float = 0.7, eig_tol: float = 1e-11, verbose: bool = False, xc: str = "teter93") -> SCFResult:
     """Restated SCF::Iterate with potential Anderson mixing; converges when
     |E_free - E_Harris| / N_atom < tol_efree (the reference's efreeDifPerAtom,
     scf.cpp:467)."""
@@ -191,7 +320,8 @@ def scf(L, znuc, pos, numGrid, numGridFine, nocc: int, nextra: int, ecut: float,
     # initial density from the pseudocharge (scf.cpp:232-255)
     rho = np.where(rho_ps > 1e-6, rho_ps, 1e-6)
     rho *= rho_ps.sum() / rho.sum()
-    eps, vxc = xc_teter93(rho)
+    xcf = xc_teter93 if xc == "teter93" else (lambda r: xc_pbe(dm, r, ecut))
+    eps, vxc = xcf(rho)
     exc = float(np.sum(eps * rho) * w)
     vh = hartree(dm, rho, rho_ps, ecut, gkk)
     vtot = vh + vxc
@@ -213,7 +343,7 @@ def scf(L, znuc, pos, numGrid, numGridFine, nocc: int, nextra: int, ecut: float,
         efree_h = ekin_b + ecor_h + float(np.sum(2 * entropy(eig, ef, tbeta)))
         # new density and potentials
         rho_out = density(T, psi, occ, nocc)
-        eps, vxc = xc_teter93(rho_out)
+        eps, vxc = xcf(rho_out)
         exc = float(np.sum(eps * rho_out) * w)
         vh = hartree(dm, rho_out, rho_ps, ecut, gkk)
         vtot_new = vh + vxc

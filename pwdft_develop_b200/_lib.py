@@ -36,6 +36,7 @@ _ip, _dp = C.POINTER(C.c_int), C.POINTER(C.c_double)
 
 PW_EXX_OFF, PW_EXX_FULL, PW_EXX_ACE = 0, 1, 2
 PW_SOLVER_LOBPCG, PW_SOLVER_CHEBFSI, PW_SOLVER_PPCG, PW_SOLVER_DAVIDSON = 0, 1, 2, 3
+PW_XC_TETER93, PW_XC_PBE = 0, 1
 
 
 class ScfParams(C.Structure):
@@ -45,7 +46,7 @@ class ScfParams(C.Structure):
                 ("ecut", C.c_double), ("temperature", C.c_double), ("eig_tol", C.c_double),
                 ("mix_step", C.c_double), ("tol_efree", C.c_double), ("refine_threshold", C.c_double),
                 ("seed", C.c_ulonglong), ("ppcg_sbsize", C.c_int), ("davidson_maxdim", C.c_int),
-                ("graphs", C.c_int)]
+                ("graphs", C.c_int), ("xc", C.c_int)]
 
 
 class ScfResult(C.Structure):
@@ -83,6 +84,7 @@ SIGNATURES: dict[str, tuple] = {
     "pw_ctx_build_twin": (_i, [_vp]),
     "pw_hartree": (_i, [_vp, _vp, _d, _vp]),
     "pw_xc_teter93": (_i, [_vp, _vp, _vp, _vp]),
+    "pw_xc_pbe": (_i, [_vp, _vp, C.c_double, _vp, _vp]),
     "pw_eigsolve": (_i, [_vp, _i, _vp, _i, _i, _d, _i, _dp, _dp, _ip]),
     "pw_density": (_i, [_vp, _vp, _i, _i, _dp, _i, _vp]),
     "pw_scf_run": (_i, [_vp, C.POINTER(ScfParams), C.POINTER(ScfResult), _dp, _dp]),

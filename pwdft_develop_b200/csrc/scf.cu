@@ -122,6 +122,160 @@ __global__ void k_init_rho(long n, const double* __restrict__ rps, double* __res
 
 static inline int nblk(long n) { return (int)std::min<long>((n + 255) / 256, 148L * 8); }
 
+// ---------------------------------------------------------------------------
+// PBE (unpolarised): the Use_Libxc 0 branch of KohnSham::CalculateXC
+// (src/SCF/hamiltonian.cpp:1381-1419, 1560-1612, 1680-1760) with the
+// gradient of KohnSham::CalculateGradDensity (hamiltonian.cpp:1153-1239).
+// Point functions: Slater exchange, Perdew-Wang 1992 correlation and the PBE
+// gradient corrections (Perdew, Burke, Ernzerhof, PRL 77, 3865 (1996)) in the
+// constants of the reference's VExchange_sla / VCorrelation_pw /
+// VGCExchange_pbx / VGCCorrelation_pbc (src/utility.cpp:3913-4244).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void pw92_point(double rs, double& ec, double& vc) {
+  const double a = 0.031091, a1 = 0.21370, b1 = 7.5957, b2 = 3.5876, b3 = 1.6382, b4 = 0.49294;
+  const double q = sqrt(rs);
+  const double om = 2.0 * a * (b1 * q + b2 * rs + b3 * rs * q + b4 * rs * rs);
+  const double rdom = 2.0 * a * (0.5 * b1 * q + b2 * rs + 1.5 * b3 * rs * q + 2.0 * b4 * rs * rs);   // rs d om/d rs
+  const double lg = log(1.0 + 1.0 / om);
+  ec = -2.0 * a * (1.0 + a1 * rs) * lg;
+  vc = -2.0 * a * (1.0 + 2.0 / 3.0 * a1 * rs) * lg - 2.0 / 3.0 * a * (1.0 + a1 * rs) * rdom / (om * (om + 1.0));
+}
+
+// eps (per particle), v1 = d(rho eps)/d rho, v2 = 2 d(rho eps)/d sigma at one point
+__device__ __forceinline__ void pbe_point(double rho, double sigma, double& eps, double& v1, double& v2) {
+  const double third = 1.0 / 3.0;
+  const double ar = fabs(rho);
+  eps = 0.0;
+  v1 = 0.0;
+  v2 = 0.0;
+  if (ar > 1e-10) {
+    const double rs = pow(3.0 / 4.0 / M_PI / ar, third);
+    const double ux = -0.458165293283143 / rs;   // Slater, -(3/4pi)(9pi/4)^(1/3) / rs
+    double uc, vc;
+    pw92_point(rs, uc, vc);
+    eps = ux + uc;
+    v1 = 4.0 / 3.0 * ux + vc;
+  }
+  if (ar > 1e-6 && sigma > 1e-10) {
+    // exchange: F_x - 1 = kappa - kappa / (1 + mu s^2 / kappa), s = |grad rho| / (2 k_F rho)
+    const double kappa = 0.804, mu = 0.2195149727645171;
+    const double g = sqrt(sigma);
+    const double kf = 3.093667726280136 * pow(ar, third);
+    const double dsg = 0.5 / kf;
+    const double s = g * dsg / ar;
+    const double den = 1.0 + s * s * mu / kappa;
+    const double fx = kappa - kappa / den;
+    const double exu = -0.75 / M_PI * kf;
+    const double dfx = 2.0 * mu * s / (den * den);
+    const double ex = exu * fx;
+    // correlation: H = gamma ln(1 + beta/gamma t^2 (1 + A t^2) / (1 + A t^2 + A^2 t^4))
+    const double gam = 0.03109069086965, bet = 0.06672455060314922;
+    const double rs = 0.6203504908994 / pow(ar, third);
+    double ec0, vc0;
+    pw92_point(rs, ec0, vc0);
+    const double ks = 1.128379167095513 * sqrt(1.919158292677513 / rs);
+    const double t2 = sigma / ((2.0 * ks * ar) * (2.0 * ks * ar));
+    const double ee = exp(-ec0 / gam);
+    const double A = bet / gam * (1.0 / (ee - 1.0));
+    const double y = A * t2;
+    const double d = 1.0 + y + y * y;
+    const double xy = (1.0 + y) / d;
+    const double qy = y * y * (2.0 + y) / (d * d);
+    const double s1 = 1.0 + bet / gam * t2 * xy;
+    const double H = gam * log(s1);
+    const double rdh = bet * t2 / s1 * (-7.0 / 3.0 * xy - qy * (A * ee * (vc0 - ec0) / bet - 7.0 / 3.0));
+    eps += ex + H;
+    v1 += ex + exu / 3.0 * fx - exu * dfx * (4.0 / 3.0) * s + H + rdh;
+    v2 = exu * dfx * dsg / g + bet / (2.0 * ks * ks * ar) * (xy - qy) / s1;
+  }
+}
+
+// gradient components g0..g2 in, h_d = v2 g_d out (in place); eps, v1 out
+__global__ void k_pbe(long n, const double* __restrict__ rho, double* __restrict__ g0, double* __restrict__ g1,
+                      double* __restrict__ g2, double* __restrict__ eps, double* __restrict__ v1) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const double a = g0[i], b = g1[i], c = g2[i];
+    double e, u, w;
+    pbe_point(rho[i], a * a + b * b + c * c, e, u, w);
+    eps[i] = e;
+    v1[i] = u;
+    g0[i] = w * a;
+    g1[i] = w * b;
+    g2[i] = w * c;
+  }
+}
+
+// dst (+)= src * i G_d / N, zero where gkk = 0 or gkk > 4 Ecut (ikFine and the
+// cut of hamiltonian.cpp:1196-1201); full cubic fine spectrum, x fastest
+__global__ void k_spec_deriv(int N, double g, double gmax2, int d, const double2* __restrict__ src,
+                             double2* __restrict__ dst, int accumulate) {
+  const long n = (long)N * N * N;
+  const double inv = 1.0 / (double)n;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const int x = (int)(i % N), y = (int)((i / N) % N), z = (int)(i / ((long)N * N));
+    const double mx = x <= N / 2 ? x : x - N, my = y <= N / 2 ? y : y - N, mz = z <= N / 2 ? z : z - N;
+    const double gx = g * mx, gy = g * my, gz = g * mz;
+    const double gkk = (gx * gx + gy * gy + gz * gz) / 2;
+    const double gd = d == 0 ? gx : (d == 1 ? gy : gz);
+    const double k = (gkk == 0.0 || gkk > gmax2) ? 0.0 : gd * inv;
+    const double2 v = src[i];
+    const double2 r = make_double2(-k * v.y, k * v.x);
+    if (accumulate) dst[i] = make_double2(dst[i].x + r.x, dst[i].y + r.y);
+    else dst[i] = r;
+  }
+}
+
+// unnormalised forward 3-D FFT of a real field, and inverse to a real field
+template <int N> static void fft3_fwd_real(double2* w, const double* rin, const double2* tw, cudaStream_t st) {
+  const int nrowtiles = (N * N + AX_TILE - 1) / AX_TILE, nxt = (N + AX_TILE - 1) / AX_TILE;
+  k_fft_axis<N, -1, 0, 1><<<nrowtiles, AX_THREADS, 0, st>>>(w, N, N, N, rin, nullptr, nullptr, nullptr, 1.0, tw);
+  k_fft_axis<N, -1, 1, 0><<<dim3(nxt, N), AX_THREADS, 0, st>>>(w, N, N, N, nullptr, nullptr, nullptr, nullptr, 1.0, tw);
+  k_fft_axis<N, -1, 2, 0><<<dim3(nxt, N), AX_THREADS, 0, st>>>(w, N, N, N, nullptr, nullptr, nullptr, nullptr, 1.0, tw);
+}
+template <int N> static void fft3_inv_real(double2* w, double* rout, const double2* tw, cudaStream_t st) {
+  const int nrowtiles = (N * N + AX_TILE - 1) / AX_TILE, nxt = (N + AX_TILE - 1) / AX_TILE;
+  k_fft_axis<N, +1, 2, 0><<<dim3(nxt, N), AX_THREADS, 0, st>>>(w, N, N, N, nullptr, nullptr, nullptr, nullptr, 1.0, tw);
+  k_fft_axis<N, +1, 1, 0><<<dim3(nxt, N), AX_THREADS, 0, st>>>(w, N, N, N, nullptr, nullptr, nullptr, nullptr, 1.0, tw);
+  k_fft_axis<N, +1, 0, 3><<<nrowtiles, AX_THREADS, 0, st>>>(w, N, N, N, nullptr, nullptr, nullptr, rout, 1.0, tw);
+}
+
+// eps (per particle) and V_xc = v1 - sum_d d_d(v2 d_d rho) of PBE on the
+// cubic fine grid; scratch: two complex and three real fine fields
+template <int N>
+static int pbe_n(pw_ctx* c, const double* rho, double ecut, double* eps, double* vxc, double2* S, double2* T,
+                 double* g, const double2* tw, cudaStream_t st) {
+  const long n = (long)N * N * N;
+  const double gs = 2 * M_PI / c->L[0];
+  fft3_fwd_real<N>(S, rho, tw, st);
+  for (int d = 0; d < 3; ++d) {
+    k_spec_deriv<<<nblk(n), 256, 0, st>>>(N, gs, 4.0 * ecut, d, S, T, 0);
+    fft3_inv_real<N>(T, g + d * n, tw, st);
+  }
+  k_pbe<<<nblk(n), 256, 0, st>>>(n, rho, g, g + n, g + 2 * n, eps, vxc);
+  for (int d = 0; d < 3; ++d) {
+    fft3_fwd_real<N>(S, g + d * n, tw, st);
+    k_spec_deriv<<<nblk(n), 256, 0, st>>>(N, gs, 4.0 * ecut, d, S, T, d > 0);
+  }
+  fft3_inv_real<N>(T, g, tw, st);
+  k_lincomb<<<nblk(n), 256, 0, st>>>(n, 1.0, vxc, -1.0, g, vxc);
+  PWB_CUDA(cudaGetLastError());
+  return PW_OK;
+}
+
+static int xc_pbe(pw_ctx* c, const double* rho, double ecut, double* eps, double* vxc, double2* S, double2* T,
+                  double* g, const double2* tw, cudaStream_t st) {
+  PWB_CHECK(c->nf[0] == c->nf[1] && c->nf[1] == c->nf[2] && c->L[0] == c->L[1] && c->L[1] == c->L[2],
+            PW_EUNSUPPORTED, "PBE gradients need a cubic cell and fine grid");
+  switch (c->nf[0]) {
+    case 24: return pbe_n<24>(c, rho, ecut, eps, vxc, S, T, g, tw, st);
+    case 32: return pbe_n<32>(c, rho, ecut, eps, vxc, S, T, g, tw, st);
+    case 48: return pbe_n<48>(c, rho, ecut, eps, vxc, S, T, g, tw, st);
+    case 96: return pbe_n<96>(c, rho, ecut, eps, vxc, S, T, g, tw, st);
+    case 144: return pbe_n<144>(c, rho, ecut, eps, vxc, S, T, g, tw, st);
+    default: set_error("SCF fine grid size not built"); return PW_EUNSUPPORTED;
+  }
+}
+
 // Philox4x32-10 counter-based generator (Salmon, Moraes, Dror, Shaw, SC'11)
 // and Box-Muller: out[i] ~ N(0,1) for the key `seed`, counter = i / 4.
 __device__ __forceinline__ void philox4x32(uint32_t c[4], uint32_t k0, uint32_t k1) {
@@ -1049,6 +1203,7 @@ struct ScfState {
   pw_ctx* c64 = nullptr;
   pw_ctx* c32 = nullptr;
   DevBuf rho, rho_out, rps, vtot, vtot_new, vxc, eps, vh, kern, work, tw, dots, wocc;
+  DevBuf work2, grad;              // PBE: second complex field, three real gradient fields
   DevBuf dvh, dfh, dif_v, dif_f;   // Anderson history [mixdim][nf] and differences
   int nhist = 0, hpos = 0;
 };
@@ -1195,9 +1350,18 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
     if ((rc = dots(S, nf, {{rho, nullptr}, {rps, nullptr}}, sums))) return rc;
     k_lincomb<<<nblk(nf), 256>>>(nf, sums[1] / sums[0], rho, 0.0, nullptr, rho);
   }
+  const bool pbe = p->xc == PW_XC_PBE;
+  PWB_CHECK(p->xc == PW_XC_TETER93 || pbe, PW_EINVAL, "unknown exchange-correlation functional");
+  if (pbe && ((rc = S.work2.alloc(nf * 16)) || (rc = S.grad.alloc(3 * nf * 8)))) return rc;
   auto potentials = [&](const double* rh, double* exc_out) -> int {
-    k_xc_teter93<<<nblk(nf), 256>>>(nf, rh, (double*)S.eps.p, (double*)S.vxc.p);
-    int q = hartree(ctx, (double2*)S.work.p, rh, rps, (const double*)S.kern.p, (double*)S.vh.p, (const double2*)S.tw.p,
+    int q = PW_OK;
+    if (pbe)
+      q = xc_pbe(ctx, rh, p->ecut, (double*)S.eps.p, (double*)S.vxc.p, (double2*)S.work.p, (double2*)S.work2.p,
+                 (double*)S.grad.p, (const double2*)S.tw.p, nullptr);
+    else
+      k_xc_teter93<<<nblk(nf), 256>>>(nf, rh, (double*)S.eps.p, (double*)S.vxc.p);
+    if (q) return q;
+    q = hartree(ctx, (double2*)S.work.p, rh, rps, (const double*)S.kern.p, (double*)S.vh.p, (const double2*)S.tw.p,
                     nullptr);
     if (q) return q;
     double e;
@@ -1496,6 +1660,28 @@ int pw_hartree(pw_ctx* ctx, const double* drho_dev, double ecut, double* vh_dev)
   PWB_CUDA(cudaMemcpy(tw.p, t.data(), N0 * 16, cudaMemcpyHostToDevice));
   rc = hartree(ctx, (double2*)work.p, drho_dev, nullptr, (const double*)kern.p, vh_dev, (const double2*)tw.p, nullptr);
   if (rc) return rc;
+  PWB_CUDA(cudaDeviceSynchronize());
+  return PW_OK;
+}
+
+int pw_xc_pbe(pw_ctx* ctx, const double* rho_dev, double ecut, double* eps_dev, double* vxc_dev) {
+  PWB_CHECK(ctx && rho_dev && eps_dev && vxc_dev && ecut > 0, PW_EINVAL, "bad arguments");
+  PWB_CUDA(cudaSetDevice(ctx->device));
+  const long nf = ctx->ntotf;
+  const int N = ctx->nf[0];
+  DevBuf a, b, g, tw;
+  int rc;
+  if ((rc = a.alloc(nf * 16)) || (rc = b.alloc(nf * 16)) || (rc = g.alloc(3 * nf * 8)) || (rc = tw.alloc(N * 16)))
+    return rc;
+  std::vector<double> t(2 * N);
+  for (int m = 0; m < N; ++m) {
+    t[2 * m] = std::cos(2 * M_PI * m / N);
+    t[2 * m + 1] = -std::sin(2 * M_PI * m / N);
+  }
+  PWB_CUDA(cudaMemcpy(tw.p, t.data(), N * 16, cudaMemcpyHostToDevice));
+  if ((rc = xc_pbe(ctx, rho_dev, ecut, eps_dev, vxc_dev, (double2*)a.p, (double2*)b.p, (double*)g.p,
+                   (const double2*)tw.p, nullptr)))
+    return rc;
   PWB_CUDA(cudaDeviceSynchronize());
   return PW_OK;
 }

@@ -1,9 +1,12 @@
 """Regenerate the golden fixtures in this folder from reference functions.
 
 The vectors come from the reference's own ``IP_c2f``, ``IP_f2c``, ``spline``
-and ``seval`` (src/utility.cpp), compiled from the reference source tree by
-``oracle/build_ref.py``.  Inputs are seeded.  Run from the repository root:
-``python tests/golden/make_golden.py``.
+and ``seval`` (src/utility.cpp) -> ``ref_utility.npz``, and its internal PBE
+pieces ``VExchange_sla``, ``VCorrelation_pw``, ``VGCExchange_pbx``,
+``VGCCorrelation_pbc`` (src/utility.cpp:3913-4244) -> ``ref_xc_pbe.npz``, all
+compiled from the reference source tree by ``oracle/build_ref.py``.  Inputs
+are seeded.  Run from the repository root:
+``python tests/golden/make_golden.py [utility|pbe]`` (both by default).
 """
 import ctypes as C
 import sys
@@ -16,6 +19,7 @@ sys.path.insert(0, str(ROOT))
 from oracle import build_ref  # noqa: E402
 
 OUT = Path(__file__).resolve().parent / "ref_utility.npz"
+OUT_PBE = Path(__file__).resolve().parent / "ref_xc_pbe.npz"
 
 
 def main():
@@ -56,5 +60,29 @@ def main():
     print(OUT, OUT.stat().st_size)
 
 
+def pbe():
+    """(rs, rho, grho2) samples over densities 1e-6..10 and reduced gradients
+    s = |grad rho| / (2 k_F rho) in 0..6, and the ten outputs of the four
+    reference functions per sample."""
+    lib = C.CDLL(str(build_ref.build()))
+    dp = C.POINTER(C.c_double)
+    rng = np.random.Generator(np.random.Philox(20261203 + 77))
+    n = 400
+    rho = 10.0 ** rng.uniform(-6, 1, n)
+    s = np.concatenate([rng.uniform(0, 6, n - 20), np.zeros(10), rng.uniform(0, 1e-3, 10)])
+    kf = (3 * np.pi ** 2 * rho) ** (1 / 3)
+    grho2 = (s * 2 * kf * rho) ** 2 + 1e-9
+    rs = (3 / (4 * np.pi * rho)) ** (1 / 3)
+    out = np.zeros((n, 10))
+    for i in range(n):
+        lib.ref_pbe_parts(C.c_double(rs[i]), C.c_double(rho[i]), C.c_double(grho2[i]), out[i].ctypes.data_as(dp))
+    np.savez_compressed(OUT_PBE, rs=rs, rho=rho, grho2=grho2, out=out)
+    print(OUT_PBE, OUT_PBE.stat().st_size)
+
+
 if __name__ == "__main__":
-    main()
+    which = sys.argv[1] if len(sys.argv) > 1 else "all"
+    if which in ("all", "utility"):
+        main()
+    if which in ("all", "pbe"):
+        pbe()

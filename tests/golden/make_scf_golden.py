@@ -4,8 +4,9 @@ Si8 diamond (a = 10.26 bohr, seeded +-0.02 bohr displacements, seed
 20261203 + 1), HGH LDA, 16 occupied + 8 extra bands, 300 K, Anderson mixing
 (dim 8, step 0.7), converged to |E_free - E_Harris| / N_atom < 1e-9.
 Cases: 16^3 / 32^3 grids with Ecut 5 Ha, and the 24^3 / 48^3 grids with
-Ecut 10 Ha.  Run from the repository root:
-``python tests/golden/make_scf_golden.py [small|full]``.
+Ecut 10 Ha (LDA Teter93); ``pbe``: the small case with PBE (the reference's
+internal PBE path).  Run from the repository root:
+``python tests/golden/make_scf_golden.py [small|full|pbe]``.
 """
 import json
 import sys
@@ -18,15 +19,16 @@ ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT))
 from oracle import pw, scf  # noqa: E402
 
-CASES = {"small": ((16, 16, 16), (32, 32, 32), 5.0), "full": ((24, 24, 24), (48, 48, 48), 10.0)}
+CASES = {"small": ((16, 16, 16), (32, 32, 32), 5.0, "teter93"), "full": ((24, 24, 24), (48, 48, 48), 10.0, "teter93"),
+         "pbe": ((16, 16, 16), (32, 32, 32), 5.0, "pbe")}
 
 
 def main(which):
     L, z, pos = pw.make_crystal("Si", (1, 1, 1), 10.26, 0.02, 20261203 + 1)
-    nc, nf, ecut = CASES[which]
+    nc, nf, ecut, xc = CASES[which]
     t0 = time.time()
-    r = scf.scf(L, z, pos, nc, nf, nocc=16, nextra=8, ecut=ecut, tol_efree=1e-9, verbose=True)
-    out = dict(case=which, numGrid=nc, numGridFine=nf, ecut=ecut, nocc=16, nextra=8, temperature=300.0,
+    r = scf.scf(L, z, pos, nc, nf, nocc=16, nextra=8, ecut=ecut, tol_efree=1e-9, verbose=True, xc=xc)
+    out = dict(case=which, numGrid=nc, numGridFine=nf, ecut=ecut, xc=xc, nocc=16, nextra=8, temperature=300.0,
                length=list(map(float, L)), positions=pos.tolist(), znuc=int(z),
                etot=r.etot, efree=r.efree, eharris=r.eharris, exc=r.exc, ehart=r.ehart, eself=r.eself,
                eig=r.eig.tolist(), occ=r.occ.tolist(), iterations=r.iterations, seconds=time.time() - t0)
