@@ -241,7 +241,11 @@ typedef struct pw_scf_params {
   int davidson_maxdim;      /* subspace size in blocks (PW_SOLVER_DAVIDSON), >= 2 */
   int graphs;               /* 1: replay the Chebyshev filter from a captured CUDA graph */
   int xc;                   /* PW_XC_TETER93 (LDA, default) or PW_XC_PBE (XC_Type XC_GGA_XC_PBE, Use_Libxc 0) */
+  int mix_type;             /* PW_MIX_ANDERSON (default) or PW_MIX_BROYDEN (Mixing_Type, potential mixing) */
+  double tol_rho;           /* > 0: converged when the density change's scfNorm (SCF::CalculateError) < tol_rho
+                               instead of the E_free - E_Harris test */
 } pw_scf_params;
+enum { PW_MIX_ANDERSON = 0, PW_MIX_BROYDEN = 1 };
 
 typedef struct pw_scf_result {
   double etot, efree, eharris, exc, ehart, eself, fermi, time_s;
@@ -249,6 +253,7 @@ typedef struct pw_scf_result {
   long hpsi_bands;          /* single-band H*psi applications performed */
   double phase_s[6];        /* verbose >= 2: eigensolver, density, potentials, set-up, mixing, refine switch (s) */
   double sub_s[4];          /* verbose >= 2, inside the eigensolver: H*psi, Gram, dense FP64, rotations (s) */
+  double scf_norm;          /* last SCF::CalculateError of the output-density change (scf.cpp:2368-2396) */
 } pw_scf_result;
 
 /* Build (once) the FP32 twin of an FP64 context with the same cell, grids and

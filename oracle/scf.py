@@ -17,6 +17,7 @@ Test infrastructure (see ``oracle/__init__.py``).  Follows:
     src/utility.cpp:4404-4444
   * SCF::CalculateEnergy / CalculateHarrisEnergy  src/SCF/scf.cpp:1834-2140
   * SCF::andersonMix              src/SCF/scf.cpp:2299-2365
+  * SCF::BroydenMix / RhoDdot      src/SCF/scf.cpp:2144-2296 (potential mixing)
   * SCF::Iterate / InnerSolve     src/SCF/scf.cpp:372-591, 1261-1589
   * initial density from the pseudocharge  src/SCF/scf.cpp:232-255
 The eigensolver is ARPACK (scipy eigsh) on the FP64 operator: the converged SCF
@@ -297,7 +298,8 @@ def _eigsh(T: pw.HamTables, nband: int, v0=None, tol=1e-11):
 
 def scf(L, znuc, pos, numGrid, numGridFine, nocc: int, nextra: int, ecut: float,
         temperature: float = 300.0, tol_efree: float = 1e-7, max_iter: int = 60, mix_dim: int = 8,
-        mix_step: float = 0.7, eig_tol: float = 1e-11, verbose: bool = False, xc: str = "teter93") -> SCFResult:
+        mix_step: float = 0.7, eig_tol: float = 1e-11, verbose: bool = False, xc: str = "teter93",
+        mix: str = "anderson", tol_rho: float | None = None) -> SCFResult:
     """Restated SCF::Iterate with potential Anderson mixing; converges when
     |E_free - E_Harris| / N_atom < tol_efree (the reference's efreeDifPerAtom,
     scf.cpp:467)."""
@@ -327,6 +329,7 @@ def scf(L, znuc, pos, numGrid, numGridFine, nocc: int, nextra: int, ecut: float,
     vtot = vh + vxc
     T = pw.HamTables(dm, ekin, teter, vtot, pseudo)
     dv_hist, df_hist = [], []
+    bst = BroydenState(mix_dim)
     psi = None
     hist = []
     res = None
@@ -354,16 +357,21 @@ def scf(L, znuc, pos, numGrid, numGridFine, nocc: int, nextra: int, ecut: float,
         etot = ekin_b + ecor
         efree = etot + float(np.sum(2 * entropy(eig, ef, tbeta)))
         dif = abs(efree - efree_h) / natom
-        hist.append(dict(iter=it, etot=etot, efree=efree, eharris=efree_h, dif=dif))
+        snorm = scf_norm(dm, rho_out - rho, ecut)
+        hist.append(dict(iter=it, etot=etot, efree=efree, eharris=efree_h, dif=dif, scf_norm=snorm))
         if verbose:
-            print(f"iter {it:3d} Etot {etot:.10f} Efree {efree:.10f} Eharris {efree_h:.10f} dif {dif:.3e}")
+            print(f"iter {it:3d} Etot {etot:.10f} Efree {efree:.10f} Eharris {efree_h:.10f} dif {dif:.3e} "
+                  f"scfnorm {snorm:.3e}")
         res = SCFResult(eig=eig, occ=occ, etot=etot, efree=efree, eharris=efree_h, exc=exc, ehart=ehart,
                         eself=eself, history=hist, rho=rho_out, vtot=vtot, psi=psi, iterations=it)
         rho = rho_out
-        if dif < tol_efree:
+        if (tol_rho is None and dif < tol_efree) or (tol_rho is not None and snorm < tol_rho):
             break
         # Anderson mixing of the potential (scf.cpp:2299-2365)
-        vtot = anderson(it, mix_step, mix_dim, vtot, vtot_new, dv_hist, df_hist)
+        if mix == "broyden":
+            vtot = broyden(dm, it, mix_step, vtot, vtot_new, bst, ecut)
+        else:
+            vtot = anderson(it, mix_step, mix_dim, vtot, vtot_new, dv_hist, df_hist)
     return res
 
 
@@ -386,3 +394,66 @@ def anderson(it, step, mix_dim, vin, vout, dv_hist, df_hist):
         dv_hist.pop(0)
         df_hist.pop(0)
     return xbar + step * fbar
+
+
+class BroydenState:
+    """History of SCF::BroydenMix: df, dv (mix_dim slots) and the previous
+    (residual, input) pair (the reference's GdfMat_, GdvMat_, GcdfMat_)."""
+
+    def __init__(self, mix_dim: int):
+        self.mix_dim = mix_dim
+        self.df = [None] * mix_dim
+        self.dv = [None] * mix_dim
+        self.cdf = None
+
+
+def broyden(dm: pw.Domain, it: int, step: float, vin: np.ndarray, vout: np.ndarray, st: BroydenState,
+            ecut: float):
+    """SCF::BroydenMix (src/SCF/scf.cpp:2144-2261) for the potential: Fourier
+    components inside the density sphere 1/2|G|^2 < 4 Ecut (idxFineCutDensity),
+    inner product RhoDdot = pi vol sum Re(conj(a) b) / gkk over gkk != 0
+    (scf.cpp:2263-2296), the mixed potential back from those components only."""
+    N0, N1, N2 = dm.numGridFine
+    gkk = gkk_fine(dm).reshape(-1)
+    sph = gkk < 4.0 * ecut
+    wgt = np.where(sph & (gkk != 0), math.pi * dm.vol / np.where(gkk != 0, gkk, 1.0), 0.0)
+    fwd = lambda v: (np.fft.fftn(v.reshape(N2, N1, N0)) * (dm.vol / dm.ntotFine)).reshape(-1)[sph]
+
+    def ddot(a, b):
+        return float(np.sum(wgt[sph] * np.real(np.conj(a) * b)))
+
+    gold = fwd(vin)
+    gnew = fwd(vout) - gold
+    m = st.mix_dim
+    used = min(it - 1, m)
+    ipos = it - 1 - ((it - 2) // m) * m
+    if it > 1:
+        st.df[ipos - 1] = st.cdf[0] - gnew
+        st.dv[ipos - 1] = st.cdf[1] - gold
+    st.cdf = (gnew.copy(), gold.copy())
+    if used > 0:
+        beta = np.empty((used, used))
+        for i in range(used):
+            for j in range(i, used):
+                beta[i, j] = beta[j, i] = ddot(st.df[j], st.df[i])
+        beta = np.linalg.inv(beta)
+        work = np.array([ddot(st.df[i], gnew) for i in range(used)])
+        for i in range(used):
+            g0 = float(beta[:, i] @ work)
+            gold = gold - g0 * st.dv[i]
+            gnew = gnew - g0 * st.df[i]
+    gmix = gold + step * gnew
+    full = np.zeros(dm.ntotFine, complex)
+    full[sph] = gmix
+    return (np.fft.ifftn(full.reshape(N2, N1, N0)) * (dm.ntotFine / dm.vol)).real.reshape(-1)
+
+
+def scf_norm(dm: pw.Domain, drho: np.ndarray, ecut: float) -> float:
+    """SCF::CalculateError (src/SCF/scf.cpp:2368-2396): RhoDdot of the change of
+    the output density, pi vol sum_{G != 0, 1/2|G|^2 < 4 Ecut} |drho(G)|^2 / gkk
+    with drho(G) the forward transform (x vol/N) divided by vol."""
+    N0, N1, N2 = dm.numGridFine
+    gkk = gkk_fine(dm).reshape(-1)
+    X = np.fft.fftn(drho.reshape(N2, N1, N0)).reshape(-1) / dm.ntotFine
+    m = (gkk < 4.0 * ecut) & (gkk != 0)
+    return float(math.pi * dm.vol * np.sum(np.abs(X[m]) ** 2 / gkk[m]))

@@ -232,11 +232,56 @@ template <int N> static void fft3_fwd_real(double2* w, const double* rin, const 
   k_fft_axis<N, -1, 1, 0><<<dim3(nxt, N), AX_THREADS, 0, st>>>(w, N, N, N, nullptr, nullptr, nullptr, nullptr, 1.0, tw);
   k_fft_axis<N, -1, 2, 0><<<dim3(nxt, N), AX_THREADS, 0, st>>>(w, N, N, N, nullptr, nullptr, nullptr, nullptr, 1.0, tw);
 }
-template <int N> static void fft3_inv_real(double2* w, double* rout, const double2* tw, cudaStream_t st) {
+template <int N>
+static void fft3_inv_real(double2* w, double* rout, const double2* tw, cudaStream_t st, double scale = 1.0) {
   const int nrowtiles = (N * N + AX_TILE - 1) / AX_TILE, nxt = (N + AX_TILE - 1) / AX_TILE;
   k_fft_axis<N, +1, 2, 0><<<dim3(nxt, N), AX_THREADS, 0, st>>>(w, N, N, N, nullptr, nullptr, nullptr, nullptr, 1.0, tw);
   k_fft_axis<N, +1, 1, 0><<<dim3(nxt, N), AX_THREADS, 0, st>>>(w, N, N, N, nullptr, nullptr, nullptr, nullptr, 1.0, tw);
-  k_fft_axis<N, +1, 0, 3><<<nrowtiles, AX_THREADS, 0, st>>>(w, N, N, N, nullptr, nullptr, nullptr, rout, 1.0, tw);
+  k_fft_axis<N, +1, 0, 3><<<nrowtiles, AX_THREADS, 0, st>>>(w, N, N, N, nullptr, nullptr, nullptr, rout, scale, tw);
+}
+
+// unnormalised 3-D FFT of a real cubic fine-grid field (forward) or to one (inverse, times scale)
+static int fft3_real(int N, bool inverse, double2* w, const double* rin, double* rout, double scale,
+                     const double2* tw, cudaStream_t st) {
+  switch (N) {
+#define PWB_FFT3(n)                                       \
+    case n:                                               \
+      if (inverse) fft3_inv_real<n>(w, rout, tw, st, scale); \
+      else fft3_fwd_real<n>(w, rin, tw, st);              \
+      break;
+    PWB_FFT3(24) PWB_FFT3(32) PWB_FFT3(48) PWB_FFT3(96) PWB_FFT3(144)
+#undef PWB_FFT3
+    default: set_error("SCF fine grid size not built"); return PW_EUNSUPPORTED;
+  }
+  PWB_CUDA(cudaGetLastError());
+  return PW_OK;
+}
+
+// sum_i w_i Re(conj(a_i) b_i) (RhoDdot with the weights pi vol / gkk)
+__global__ void k_wdot(long n, const double* __restrict__ w, const double2* __restrict__ a,
+                       const double2* __restrict__ b, double* out) {
+  double s = 0.0;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    s += w[i] * (a[i].x * b[i].x + a[i].y * b[i].y);
+  __shared__ double red[32];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double v = (threadIdx.x < (blockDim.x >> 5)) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (threadIdx.x == 0) atomicAdd(out, v);
+  }
+}
+// z = a x + b y (complex arrays, real coefficients; y may be null); optional mask
+__global__ void k_clin(long n, double a, const double2* __restrict__ x, double b, const double2* __restrict__ y,
+                       const double* __restrict__ mask, double2* __restrict__ z) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    double2 v = make_double2(a * x[i].x, a * x[i].y);
+    if (y) { v.x += b * y[i].x; v.y += b * y[i].y; }
+    if (mask) { v.x *= mask[i]; v.y *= mask[i]; }
+    z[i] = v;
+  }
 }
 
 // eps (per particle) and V_xc = v1 - sum_d d_d(v2 d_d rho) of PBE on the
@@ -1204,6 +1249,9 @@ struct ScfState {
   pw_ctx* c32 = nullptr;
   DevBuf rho, rho_out, rps, vtot, vtot_new, vxc, eps, vh, kern, work, tw, dots, wocc;
   DevBuf work2, grad;              // PBE: second complex field, three real gradient fields
+  // density-sphere weights pi vol / gkk (G != 0, gkk < 4 Ecut) and mask (RhoDdot,
+  // CalculateError, BroydenMix); density change; Broyden spectra and history
+  DevBuf bw, bmask, dr, bA, bB, bdf, bdv, bcdf, bdots;
   DevBuf dvh, dfh, dif_v, dif_f;   // Anderson history [mixdim][nf] and differences
   int nhist = 0, hpos = 0;
 };
@@ -1326,6 +1374,23 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
               (gkk <= 1e-16 || gkk > 4.0 * p->ecut) ? 0.0 : 2.0 * M_PI / gkk / (double)nf;
         }
     PWB_CUDA(cudaMemcpy(S.kern.p, k.data(), nf * 8, cudaMemcpyHostToDevice));
+    // density-sphere weights and mask (idxFineCutDensity, RhoDdot: scf.cpp:2263-2296)
+    std::vector<double> bw(nf), bm(nf);
+    for (int z = 0; z < N2; ++z)
+      for (int y = 0; y < N1; ++y)
+        for (int x = 0; x < N0; ++x) {
+          const double m0 = x <= N0 / 2 ? x : x - N0, m1 = y <= N1 / 2 ? y : y - N1, m2 = z <= N2 / 2 ? z : z - N2;
+          const double g0 = 2 * M_PI / ctx->L[0] * m0, g1 = 2 * M_PI / ctx->L[1] * m1, g2 = 2 * M_PI / ctx->L[2] * m2;
+          const double gkk = (g0 * g0 + g1 * g1 + g2 * g2) / 2;
+          const size_t i = x + (size_t)N0 * (y + (size_t)N1 * z);
+          bm[i] = gkk < 4.0 * p->ecut ? 1.0 : 0.0;
+          bw[i] = (gkk != 0.0 && gkk < 4.0 * p->ecut) ? M_PI * ctx->vol / gkk : 0.0;
+        }
+    if ((rc = S.bw.alloc(nf * 8)) || (rc = S.bmask.alloc(nf * 8)) || (rc = S.dr.alloc(nf * 8)) ||
+        (rc = S.bdots.alloc((size_t)(std::max(1, p->mix_dim) + 1) * (std::max(1, p->mix_dim) + 1) * 8)))
+      return rc;
+    PWB_CUDA(cudaMemcpy(S.bw.p, bw.data(), nf * 8, cudaMemcpyHostToDevice));
+    PWB_CUDA(cudaMemcpy(S.bmask.p, bm.data(), nf * 8, cudaMemcpyHostToDevice));
     std::vector<double> t(2 * N0);
     for (int m = 0; m < N0; ++m) {
       t[2 * m] = std::cos(2 * M_PI * m / N0);
@@ -1350,6 +1415,14 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
     if ((rc = dots(S, nf, {{rho, nullptr}, {rps, nullptr}}, sums))) return rc;
     k_lincomb<<<nblk(nf), 256>>>(nf, sums[1] / sums[0], rho, 0.0, nullptr, rho);
   }
+  const bool broyden = p->mix_type == PW_MIX_BROYDEN;
+  PWB_CHECK(p->mix_type == PW_MIX_ANDERSON || broyden, PW_EINVAL, "unknown mixing scheme");
+  PWB_CHECK(!broyden || (ctx->nf[0] == ctx->nf[1] && ctx->nf[1] == ctx->nf[2]), PW_EUNSUPPORTED,
+            "Broyden mixing needs a cubic fine grid");
+  if (broyden && ((rc = S.bA.alloc(nf * 16)) || (rc = S.bB.alloc(nf * 16)) ||
+                  (rc = S.bdf.alloc((size_t)mixdim * nf * 16)) || (rc = S.bdv.alloc((size_t)mixdim * nf * 16)) ||
+                  (rc = S.bcdf.alloc((size_t)2 * nf * 16))))
+    return rc;
   const bool pbe = p->xc == PW_XC_PBE;
   PWB_CHECK(p->xc == PW_XC_TETER93 || pbe, PW_EINVAL, "unknown exchange-correlation functional");
   if (pbe && ((rc = S.work2.alloc(nf * 16)) || (rc = S.grad.alloc(3 * nf * 8)))) return rc;
@@ -1506,11 +1579,26 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
     etot = ekin + (-ed[0] * w) + exc + ehart - eself;
     efree = etot + ent;
     const double dif = std::fabs(efree - eharris) / natom;
+    // SCF::CalculateError of the change of the output density (scf.cpp:1492-1496, 2368-2396)
+    double snorm = 0.0;
+    {
+      double* drv = (double*)S.dr.p;
+      k_lincomb<<<nblk(nf), 256>>>(nf, 1.0, ro, -1.0, rho, drv);
+      if ((rc = fft3_real(ctx->nf[0], false, (double2*)S.work.p, drv, nullptr, 1.0, (const double2*)S.tw.p,
+                          nullptr)))
+        return rc;
+      PWB_CUDA(cudaMemset(S.bdots.p, 0, 8));
+      k_wdot<<<nblk(nf), 256>>>(nf, (const double*)S.bw.p, (const double2*)S.work.p, (const double2*)S.work.p,
+                                (double*)S.bdots.p);
+      PWB_CUDA(cudaMemcpy(&snorm, S.bdots.p, 8, cudaMemcpyDeviceToHost));
+      snorm /= (double)nf * (double)nf;
+      r->scf_norm = snorm;
+    }
     if (p->verbose)
-      fprintf(stderr, "SCF %3d %s Etot %.10f Efree %.10f Eharris %.10f dif %.3e\n", it,
-              sv.c->prec == PW_F32 ? "f32" : "f64", etot, efree, eharris, dif);
+      fprintf(stderr, "SCF %3d %s Etot %.10f Efree %.10f Eharris %.10f dif %.3e scfnorm %.3e\n", it,
+              sv.c->prec == PW_F32 ? "f32" : "f64", etot, efree, eharris, dif, snorm);
     PWB_CUDA(cudaMemcpy(rho, ro, nf * 8, cudaMemcpyDeviceToDevice));
-    if (refined && dif < p->tol_efree) { conv = true; break; }
+    if (refined && (p->tol_rho > 0 ? snorm < p->tol_rho : dif < p->tol_efree)) { conv = true; break; }
     // switch the eigensolver to FP64 for the final iterations (iterative
     // refinement): below the threshold, or when the FP32 iteration has
     // stagnated (no 10% gain on its best |E_free - E_Harris| for 4 steps)
@@ -1537,6 +1625,82 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
       refined = true;
       r->refine_iter = it;
     }
+    if (broyden) {
+      // Broyden mixing of the potential (SCF::BroydenMix, scf.cpp:2144-2261):
+      // density-sphere Fourier components, RhoDdot inner products
+      PhaseTimer pt_(prof, &tph[4]);
+      const int N = ctx->nf[0];
+      const double2* tw = (const double2*)S.tw.p;
+      const double* mask = (const double*)S.bmask.p;
+      const double* bwp = (const double*)S.bw.p;
+      double* vin = (double*)S.vtot.p;
+      double2* A = (double2*)S.bA.p;    // GvOld
+      double2* B = (double2*)S.bB.p;    // GvNew (the residual)
+      double2* df = (double2*)S.bdf.p;
+      double2* dv = (double2*)S.bdv.p;
+      double2* cdf0 = (double2*)S.bcdf.p;
+      double2* cdf1 = cdf0 + nf;
+      const double sc = ctx->vol / (double)nf;
+      if ((rc = fft3_real(N, false, A, vin, nullptr, 1.0, tw, nullptr))) return rc;
+      k_clin<<<nblk(nf), 256>>>(nf, sc, A, 0.0, nullptr, mask, A);
+      if ((rc = fft3_real(N, false, B, (const double*)S.vtot_new.p, nullptr, 1.0, tw, nullptr))) return rc;
+      k_clin<<<nblk(nf), 256>>>(nf, sc, B, -1.0, A, mask, B);
+      const int used = std::min(it - 1, mixdim);
+      const int ipos = it - 1 - ((it - 2) / mixdim) * mixdim;
+      if (it > 1) {
+        k_clin<<<nblk(nf), 256>>>(nf, 1.0, cdf0, -1.0, B, nullptr, df + (size_t)(ipos - 1) * nf);
+        k_clin<<<nblk(nf), 256>>>(nf, 1.0, cdf1, -1.0, A, nullptr, dv + (size_t)(ipos - 1) * nf);
+      }
+      PWB_CUDA(cudaMemcpy(cdf0, B, nf * 16, cudaMemcpyDeviceToDevice));
+      PWB_CUDA(cudaMemcpy(cdf1, A, nf * 16, cudaMemcpyDeviceToDevice));
+      if (used > 0) {
+        // beta_ij = RhoDdot(df_j, df_i) and work_i = RhoDdot(df_i, GvNew): one batch of reductions
+        double* dd = (double*)S.bdots.p;
+        const size_t ndd = (size_t)used * used + used;
+        PWB_CUDA(cudaMemset(dd, 0, ndd * 8));
+        for (int i = 0; i < used; ++i)
+          for (int j = i; j < used; ++j)
+            k_wdot<<<nblk(nf), 256>>>(nf, bwp, df + (size_t)j * nf, df + (size_t)i * nf, dd + i * used + j);
+        for (int i = 0; i < used; ++i)
+          k_wdot<<<nblk(nf), 256>>>(nf, bwp, df + (size_t)i * nf, B, dd + used * used + i);
+        std::vector<double> hd(ndd);
+        PWB_CUDA(cudaMemcpy(hd.data(), dd, ndd * 8, cudaMemcpyDeviceToHost));
+        // inverse of the symmetric (possibly indefinite) beta matrix (the
+        // reference's sytrf / sytri): Gauss-Jordan with partial pivoting
+        const int u = used;
+        std::vector<double> a((size_t)u * 2 * u, 0.0);
+        for (int i = 0; i < u; ++i) {
+          for (int j = 0; j < u; ++j) a[(size_t)i * 2 * u + j] = hd[std::min(i, j) * u + std::max(i, j)];
+          a[(size_t)i * 2 * u + u + i] = 1.0;
+        }
+        for (int c0 = 0; c0 < u; ++c0) {
+          int piv = c0;
+          for (int i = c0 + 1; i < u; ++i)
+            if (std::fabs(a[(size_t)i * 2 * u + c0]) > std::fabs(a[(size_t)piv * 2 * u + c0])) piv = i;
+          PWB_CHECK(a[(size_t)piv * 2 * u + c0] != 0.0, PW_ENUMERIC, "Broyden beta matrix is singular");
+          if (piv != c0)
+            for (int j = 0; j < 2 * u; ++j) std::swap(a[(size_t)piv * 2 * u + j], a[(size_t)c0 * 2 * u + j]);
+          const double d = a[(size_t)c0 * 2 * u + c0];
+          for (int j = 0; j < 2 * u; ++j) a[(size_t)c0 * 2 * u + j] /= d;
+          for (int i = 0; i < u; ++i) {
+            if (i == c0) continue;
+            const double f = a[(size_t)i * 2 * u + c0];
+            if (f != 0.0)
+              for (int j = 0; j < 2 * u; ++j) a[(size_t)i * 2 * u + j] -= f * a[(size_t)c0 * 2 * u + j];
+          }
+        }
+        for (int i = 0; i < u; ++i) {
+          double g0 = 0.0;
+          for (int j = 0; j < u; ++j) g0 += a[(size_t)j * 2 * u + u + i] * hd[(size_t)u * u + j];
+          k_clin<<<nblk(nf), 256>>>(nf, 1.0, A, -g0, dv + (size_t)i * nf, nullptr, A);
+          k_clin<<<nblk(nf), 256>>>(nf, 1.0, B, -g0, df + (size_t)i * nf, nullptr, B);
+        }
+      }
+      k_clin<<<nblk(nf), 256>>>(nf, 1.0, A, p->mix_step, B, nullptr, A);
+      // back to real space from the sphere components (backward x 1/vol)
+      if ((rc = fft3_real(N, true, A, nullptr, vin, 1.0 / ctx->vol, tw, nullptr))) return rc;
+      PWB_CUDA(cudaGetLastError());
+    } else
     // Anderson mixing of the potential (scf.cpp:2299-2365)
     {
       PhaseTimer pt_(prof, &tph[4]);
