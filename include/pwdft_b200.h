@@ -425,6 +425,33 @@ PW_API int pw_teter_precond_noalloc(pw_ctx* ctx, const void* r, int ld, void* w,
  * Default 64. Scratch grows to hold ceil(nband_batch/2) band pairs. */
 PW_API int pw_set_band_batch(pw_ctx* ctx, int nband_batch);
 
+/* ---- Restart files in the reference's binary layout ----
+ * serialize() layout (include/utility.hpp:1183-1278): a vector is an int32
+ * length then that many doubles; a matrix two int32 sizes then the
+ * column-major doubles; a 3-tensor three int32 sizes then the doubles; native
+ * byte order.  All buffers are host memory.
+ *   DEN  (scf.cpp:1070-1088, read at :164-178): the fine-grid fractional
+ *        positions i/N_d for d = x, y, z (UniformMeshFine, utility.cpp:405-420),
+ *        then the density (N_fine).  pw_read_density checks the grid sizes.
+ *   POT  (scf.cpp:1091-1108): the same grid vectors, then Vtot as N_fine x 1.
+ *   WFN_<rank> (scf.cpp:1110-1145 via SeparateWrite "name_<rank>", read at
+ *        :296-330): the bands as an ntot x 1 x nband tensor, then the
+ *        occupations (nband).  Real-space contexts.  pw_read_wfn with
+ *        psi = NULL returns the band count in *nband.
+ *   EIG  (scf.cpp:1247-1253): the eigenvalues as one vector.
+ * pw_scf_set_initial hands the next pw_scf_run a starting density (N_fine,
+ * used as given, as isRestartDensity does) and/or starting bands (nband must
+ * equal nocc + nextra of that run); either may be NULL.  Consumed by that run. */
+PW_API int pw_write_density(const pw_ctx* ctx, const char* path, const double* rho_fine);
+PW_API int pw_read_density(const pw_ctx* ctx, const char* path, double* rho_fine);
+PW_API int pw_write_potential(const pw_ctx* ctx, const char* path, const double* vtot_fine);
+PW_API int pw_write_wfn(const pw_ctx* ctx, const char* path, const double* psi, int ld, int nband, const double* occ);
+PW_API int pw_read_wfn(const pw_ctx* ctx, const char* path, double* psi, int ld, int nband_max, int* nband,
+                       double* occ);
+PW_API int pw_write_eig(const char* path, int n, const double* eig);
+PW_API int pw_read_eig(const char* path, int nmax, int* n, double* eig);
+PW_API int pw_scf_set_initial(pw_ctx* ctx, const double* rho_fine, const double* psi, int ld, int nband);
+
 /* ---- Sphere-cut (G-space) mode, the reference's Use_Real_Space: 0 ----
  * A band is its Fourier coefficients on the half sphere 1/2 |G|^2 < ecut, in
  * the order of Fourier::idxCoarseCut (ascending R2C index, G_x >= 0 with the

@@ -126,6 +126,14 @@ SIGNATURES: dict[str, tuple] = {
     "pw_ace_apply": (_i, [_vp, _vp, _i, _vp, _i, _i, _vp]),
     "pw_exx_energy": (_i, [_vp, _vp, _i, _i, _dp, _i, _i, _dp]),
     "pw_band_energy_backward": (_i, [_vp, _vp, _i, _i, _dp, _vp, _dp]),
+    "pw_write_density": (_i, [_vp, C.c_char_p, _dp]),
+    "pw_read_density": (_i, [_vp, C.c_char_p, _dp]),
+    "pw_write_potential": (_i, [_vp, C.c_char_p, _dp]),
+    "pw_write_wfn": (_i, [_vp, C.c_char_p, _dp, _i, _i, _dp]),
+    "pw_read_wfn": (_i, [_vp, C.c_char_p, _dp, _i, _i, _ip, _dp]),
+    "pw_write_eig": (_i, [C.c_char_p, _i, _dp]),
+    "pw_read_eig": (_i, [C.c_char_p, _i, _ip, _dp]),
+    "pw_scf_set_initial": (_i, [_vp, _dp, _dp, _i, _i]),
     "pw_ctx_create_gspace": (_i, [_dp, _ip, C.c_double, _i, _i, C.POINTER(_vp)]),
     "pw_gs_sphere": (_i, [_vp, _ip, _ip, _ip, _dp, _dp]),
     "pw_gs_set_projectors": (_i, [_vp, _i, _dp, _dp]),

@@ -653,3 +653,72 @@ Context.eigsolve = _ctx_eigsolve
 Context.density = _ctx_density
 Context.scf = _ctx_scf
 Context.build_twin = _ctx_build_twin
+
+
+# ---------------------------------------------------------------------------
+# restart files (DEN, POT, WFN_<rank>, EIG) in the reference's binary layout
+# ---------------------------------------------------------------------------
+def _ctx_write_density(self, path, rho):
+    r = np.ascontiguousarray(rho, np.float64).ravel()
+    assert r.size == self.ntotFine
+    check(lib.pw_write_density(self._h, str(path).encode(), r.ctypes.data_as(_lib._dp)))
+
+
+def _ctx_read_density(self, path) -> np.ndarray:
+    out = np.zeros(self.ntotFine)
+    check(lib.pw_read_density(self._h, str(path).encode(), out.ctypes.data_as(_lib._dp)))
+    return out
+
+
+def _ctx_write_potential(self, path, vtot):
+    v = np.ascontiguousarray(vtot, np.float64).ravel()
+    assert v.size == self.ntotFine
+    check(lib.pw_write_potential(self._h, str(path).encode(), v.ctypes.data_as(_lib._dp)))
+
+
+def _ctx_write_wfn(self, path, psi, occ):
+    """psi: (nband, ntot) host array (each row one band), occ: (nband,)."""
+    x = np.ascontiguousarray(psi, np.float64)
+    o = np.ascontiguousarray(occ, np.float64)
+    check(lib.pw_write_wfn(self._h, str(path).encode(), x.ctypes.data_as(_lib._dp), self.ntot, x.shape[0],
+                           o.ctypes.data_as(_lib._dp)))
+
+
+def _ctx_read_wfn(self, path):
+    nb = C.c_int(0)
+    check(lib.pw_read_wfn(self._h, str(path).encode(), None, self.ntot, 0, C.byref(nb), None))
+    x = np.zeros((nb.value, self.ntot))
+    o = np.zeros(nb.value)
+    check(lib.pw_read_wfn(self._h, str(path).encode(), x.ctypes.data_as(_lib._dp), self.ntot, nb.value,
+                          C.byref(nb), o.ctypes.data_as(_lib._dp)))
+    return x, o
+
+
+def write_eig(path, eig):
+    e = np.ascontiguousarray(eig, np.float64)
+    check(lib.pw_write_eig(str(path).encode(), e.size, e.ctypes.data_as(_lib._dp)))
+
+
+def read_eig(path) -> np.ndarray:
+    n = C.c_int(0)
+    check(lib.pw_read_eig(str(path).encode(), 0, C.byref(n), None))
+    e = np.zeros(n.value)
+    check(lib.pw_read_eig(str(path).encode(), n.value, C.byref(n), e.ctypes.data_as(_lib._dp)))
+    return e
+
+
+def _ctx_scf_set_initial(self, rho=None, psi=None):
+    """Starting density (N_fine) and/or bands (nband, ntot) for the next scf()."""
+    r = None if rho is None else np.ascontiguousarray(rho, np.float64).ravel()
+    x = None if psi is None else np.ascontiguousarray(psi, np.float64)
+    check(lib.pw_scf_set_initial(self._h, None if r is None else r.ctypes.data_as(_lib._dp),
+                                 None if x is None else x.ctypes.data_as(_lib._dp), self.ntot,
+                                 0 if x is None else x.shape[0]))
+
+
+Context.write_density = _ctx_write_density
+Context.read_density = _ctx_read_density
+Context.write_potential = _ctx_write_potential
+Context.write_wfn = _ctx_write_wfn
+Context.read_wfn = _ctx_read_wfn
+Context.scf_set_initial = _ctx_scf_set_initial

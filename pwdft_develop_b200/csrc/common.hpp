@@ -154,6 +154,9 @@ struct pw_ctx {
   size_t exx_scratch_bytes = (size_t)1 << 30;
   pwb::DevBuf ace_xi, ace_qd, ace_bf, ace_t_bf;   // ACE vectors xi (T [nace][ntot]) and -1 weights
   int ace_n = 0, ace_npad = 0;
+  // initial guess for the next pw_scf_run (pw_scf_set_initial, e.g. from restart files)
+  std::vector<double> init_rho, init_psi;
+  int init_nband = 0;
   // converged SCF state kept for pw_scf_forces: FP64 bands, occupations, density
   pwb::DevBuf scf_psi, scf_rho;
   std::vector<double> scf_occ;

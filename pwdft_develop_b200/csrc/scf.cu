@@ -1409,8 +1409,11 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
   // initial density from the pseudocharge (scf.cpp:232-255)
   double* rho = (double*)S.rho.p;
   double* rps = (double*)S.rps.p;
-  k_init_rho<<<nblk(nf), 256>>>(nf, rps, rho);
-  {
+  if (!ctx->init_rho.empty()) {
+    // restart density (isRestartDensity, scf.cpp:164-178), used as given
+    PWB_CUDA(cudaMemcpy(rho, ctx->init_rho.data(), nf * 8, cudaMemcpyHostToDevice));
+  } else {
+    k_init_rho<<<nblk(nf), 256>>>(nf, rps, rho);
     double sums[2];
     if ((rc = dots(S, nf, {{rho, nullptr}, {rps, nullptr}}, sums))) return rc;
     k_lincomb<<<nblk(nf), 256>>>(nf, sums[1] / sums[0], rho, 0.0, nullptr, rho);
@@ -1469,10 +1472,24 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
   pw_ctx* cur = p->mixed ? S.c32 : ctx;
   if ((rc = bind(cur))) return rc;
   {
-    // random start, Gaussian (seeded Philox on the device), orthonormalised by Cholesky-QR
+    // random start, Gaussian (seeded Philox on the device), orthonormalised by
+    // Cholesky-QR; or the bands of pw_scf_set_initial (isRestartWfn, scf.cpp:296-330)
     const long ntot_b = (long)nb * nt;
-    if (cur->prec == PW_F64) k_gaussian<double><<<nblk(ntot_b / 4 + 1), 256>>>(ntot_b, p->seed, (double*)sv.X.p);
-    else k_gaussian<float><<<nblk(ntot_b / 4 + 1), 256>>>(ntot_b, p->seed, (float*)sv.X.p);
+    if (ctx->init_nband == nb && (long)ctx->init_psi.size() == ntot_b) {
+      if (cur->prec == PW_F64) {
+        PWB_CUDA(cudaMemcpy(sv.X.p, ctx->init_psi.data(), ntot_b * 8, cudaMemcpyHostToDevice));
+      } else {
+        std::vector<float> f(ctx->init_psi.begin(), ctx->init_psi.end());
+        PWB_CUDA(cudaMemcpy(sv.X.p, f.data(), ntot_b * 4, cudaMemcpyHostToDevice));
+      }
+    } else {
+      PWB_CHECK(ctx->init_nband == 0, PW_EINVAL, "initial bands: count does not match nocc + nextra");
+      if (cur->prec == PW_F64) k_gaussian<double><<<nblk(ntot_b / 4 + 1), 256>>>(ntot_b, p->seed, (double*)sv.X.p);
+      else k_gaussian<float><<<nblk(ntot_b / 4 + 1), 256>>>(ntot_b, p->seed, (float*)sv.X.p);
+    }
+    ctx->init_rho.clear();
+    ctx->init_psi.clear();
+    ctx->init_nband = 0;
     PWB_CUDA(cudaGetLastError());
     if (cur->gs)   // sphere-cut bands: Im c_0 = 0
       PWB_CUDA(cudaMemset2D((char*)sv.X.p + cur->esz, nt * cur->esz, 0, cur->esz, nb));
