@@ -627,20 +627,43 @@ template <int N> __device__ __forceinline__ int fine_slot(int e) {
   return e <= h ? e : (e > N - h ? e - N + n : (e == N - h ? n : -1));
 }
 
+// Shared-memory layout of k_floc2: S tile (slot columns of the fine plane)
+// with row y at y PS + SKS (y / NY2), per-warp row buffers with element e of
+// row f at f PR + e + SKR (e / NX2), and whether the first pass of the column
+// and row transforms puts the transform index on the fastest lanes.  The
+// FP32 96 x 96 plane uses the layout with the fewest shared-memory
+// wavefronts found by a search over pitches, skews and lane maps with a
+// bank model of its 8-byte accesses (31 % fewer than plain padded rows);
+// other planes keep plain padded rows.
+template <typename T, int NXF, int NYF> struct FlocLayout {
+  static constexpr int PS = NXF / 2 + 1, SKS = 0;
+  static constexpr int PR = NXF + 1, SKR = 0;
+  static constexpr bool FAST_F = false;
+  template <int NY2> static constexpr int s_size() { return NYF * PS + SKS * (NYF / NY2); }
+};
+template <> struct FlocLayout<float, 96, 96> {
+  static constexpr int PS = 60, SKS = 2;
+  static constexpr int PR = 108, SKR = 1;
+  static constexpr bool FAST_F = true;
+  template <int NY2> static constexpr int s_size() { return 96 * PS + SKS * (96 / NY2); }
+};
+
 template <typename T, int NXF, int NYF>
 __global__ void __launch_bounds__(FLOC_THREADS, sizeof(T) == 4 ? 3 : 1)
 k_floc2(VT<T>* __restrict__ BC, const T* __restrict__ vtot, T inv_nf, const VT<T>* twx_g, const VT<T>* twy_g) {
   using V = VT<T>;
   constexpr int n0 = NXF / 2;
   constexpr int nsx = n0 + 1, nsy = NYF / 2 + 1;
-  constexpr int PS = nsx;
-  constexpr int PR = NXF + 1;
+  using LY = FlocLayout<T, NXF, NYF>;
+  constexpr int PS = LY::PS, SKS = LY::SKS, PR = LY::PR, SKR = LY::SKR;
+  constexpr bool FF = LY::FAST_F;
   constexpr int NX1 = Split<NXF>::n1, NX2 = NXF / NX1, FX = 32 / NX1;
   constexpr int NY1 = Split<NYF>::n1, NY2 = NYF / NY1, FY = 32 / NY1;
   constexpr int RX = (FX * NX2 + 31) / 32, RY = (FY * NY2 + 31) / 32;
+  static_assert(PS >= nsx && PR >= NXF + SKR * (NX1 - 1), "k_floc2 layout rows overlap");
   extern __shared__ __align__(16) unsigned char smraw[];
-  V* S = reinterpret_cast<V*>(smraw);          // [NYF][PS]
-  V* twx = S + NYF * PS;
+  V* S = reinterpret_cast<V*>(smraw);          // row y at y PS + SKS (y / NY2)
+  V* twx = S + LY::template s_size<NY2>();
   V* twy = twx + NXF;
   V* Rall = twy + NYF;                          // [nwarps][FX][PR]
   load_tw(twx, twx_g, NXF);
@@ -656,7 +679,7 @@ k_floc2(VT<T>* __restrict__ BC, const T* __restrict__ vtot, T inv_nf, const VT<T
 #pragma unroll
     for (int r = 0; r < RY; ++r) {
       const int it = lane + 32 * r;
-      const int f = it / NY2, j2 = it - f * NY2;
+      const int f = FF ? it % FY : it / NY2, j2 = FF ? it / FY : it - f * NY2;
       const int c = g + f;
       if (it < FY * NY2 && c < nsx) {
         V t[NY1];
@@ -673,7 +696,7 @@ k_floc2(VT<T>* __restrict__ BC, const T* __restrict__ vtot, T inv_nf, const VT<T
           t[k1] = cmul(t[k1], w);
         }
 #pragma unroll
-        for (int k1 = 0; k1 < NY1; ++k1) S[(NY2 * k1 + j2) * PS + c] = t[k1];
+        for (int k1 = 0; k1 < NY1; ++k1) S[(NY2 * k1 + j2) * PS + SKS * k1 + c] = t[k1];
       }
     }
     __syncwarp();
@@ -684,13 +707,16 @@ k_floc2(VT<T>* __restrict__ BC, const T* __restrict__ vtot, T inv_nf, const VT<T
       V u[NY2];
       if (act) {
 #pragma unroll
-        for (int j2 = 0; j2 < NY2; ++j2) u[j2] = S[(NY2 * k1 + j2) * PS + c];
+        for (int j2 = 0; j2 < NY2; ++j2) u[j2] = S[(NY2 * k1 + j2) * PS + SKS * k1 + c];
         DFT<NY2, +1, V>::run(u);
       }
       __syncwarp();
       if (act) {
 #pragma unroll
-        for (int k2 = 0; k2 < NY2; ++k2) S[(k1 + NY1 * k2) * PS + c] = u[k2];
+        for (int k2 = 0; k2 < NY2; ++k2) {
+          const int y = k1 + NY1 * k2;
+          S[y * PS + SKS * (y / NY2) + c] = u[k2];
+        }
       }
     }
     __syncwarp();
@@ -704,10 +730,10 @@ k_floc2(VT<T>* __restrict__ BC, const T* __restrict__ vtot, T inv_nf, const VT<T
 #pragma unroll
     for (int r = 0; r < RX; ++r) {
       const int it = lane + 32 * r;
-      const int f = it / NX2, j2 = it - f * NX2;
+      const int f = FF ? it % FX : it / NX2, j2 = FF ? it / FX : it - f * NX2;
       if (it < FX * NX2 && f < nr) {
         V t[NX1];
-        const V* srow = S + (r0 + f) * PS;
+        const V* srow = S + (r0 + f) * PS + SKS * ((r0 + f) / NY2);
 #pragma unroll
         for (int j1 = 0; j1 < NX1; ++j1) {
           const int s = fine_slot<NXF>(NX2 * j1 + j2);
@@ -721,7 +747,7 @@ k_floc2(VT<T>* __restrict__ BC, const T* __restrict__ vtot, T inv_nf, const VT<T
           t[k1] = cmul(t[k1], w);
         }
 #pragma unroll
-        for (int k1 = 0; k1 < NX1; ++k1) Rw[f * PR + NX2 * k1 + j2] = t[k1];
+        for (int k1 = 0; k1 < NX1; ++k1) Rw[f * PR + (NX2 + SKR) * k1 + j2] = t[k1];
       }
     }
     __syncwarp();
@@ -730,7 +756,7 @@ k_floc2(VT<T>* __restrict__ BC, const T* __restrict__ vtot, T inv_nf, const VT<T
       const bool act = lane < FX * NX1 && f < nr;
       if (act) {
         V u[NX2];
-        V* rr = Rw + f * PR + NX2 * k1;
+        V* rr = Rw + f * PR + (NX2 + SKR) * k1;
 #pragma unroll
         for (int j2 = 0; j2 < NX2; ++j2) u[j2] = rr[j2];
         DFT<NX2, +1, V>::run(u);                    // u[k2] = x[k1 + NX1 k2]
@@ -748,13 +774,13 @@ k_floc2(VT<T>* __restrict__ BC, const T* __restrict__ vtot, T inv_nf, const VT<T
 #pragma unroll
     for (int r = 0; r < RX; ++r) {
       const int it = lane + 32 * r;
-      const int f = it / NX2, m2 = it - f * NX2;
+      const int f = FF ? it % FX : it / NX2, m2 = FF ? it / FX : it - f * NX2;
       if (it < FX * NX2 && f < nr) {
         V t[NX1];
 #pragma unroll
-        for (int k1 = 0; k1 < NX1; ++k1) t[k1] = Rw[f * PR + NX2 * k1 + m2];
+        for (int k1 = 0; k1 < NX1; ++k1) t[k1] = Rw[f * PR + (NX2 + SKR) * k1 + m2];
         DFT<NX1, -1, V>::run(t);                    // forward, second stage over k1
-        V* srow = S + (r0 + f) * PS;
+        V* srow = S + (r0 + f) * PS + SKS * ((r0 + f) / NY2);
 #pragma unroll
         for (int m1 = 0; m1 < NX1; ++m1) {
           const int s = fine_slot<NXF>(m2 + NX2 * m1);
@@ -771,17 +797,17 @@ k_floc2(VT<T>* __restrict__ BC, const T* __restrict__ vtot, T inv_nf, const VT<T
 #pragma unroll
     for (int r = 0; r < RY; ++r) {
       const int it = lane + 32 * r;
-      const int f = it / NY2, j2 = it - f * NY2;
+      const int f = FF ? it % FY : it / NY2, j2 = FF ? it / FY : it - f * NY2;
       const int c = g + f;
       if (it < FY * NY2 && c < nsx) {
         V t[NY1];
 #pragma unroll
-        for (int j1 = 0; j1 < NY1; ++j1) t[j1] = S[(NY2 * j1 + j2) * PS + c];
+        for (int j1 = 0; j1 < NY1; ++j1) t[j1] = S[(NY2 * j1 + j2) * PS + SKS * j1 + c];
         DFT<NY1, -1, V>::run(t);
 #pragma unroll
         for (int k1 = 1; k1 < NY1; ++k1) t[k1] = cmul(t[k1], twy[j2 * k1]);
 #pragma unroll
-        for (int k1 = 0; k1 < NY1; ++k1) S[(NY2 * k1 + j2) * PS + c] = t[k1];
+        for (int k1 = 0; k1 < NY1; ++k1) S[(NY2 * k1 + j2) * PS + SKS * k1 + c] = t[k1];
       }
     }
     __syncwarp();
@@ -791,7 +817,7 @@ k_floc2(VT<T>* __restrict__ BC, const T* __restrict__ vtot, T inv_nf, const VT<T
       if (lane < FY * NY1 && c < nsx) {
         V u[NY2];
 #pragma unroll
-        for (int j2 = 0; j2 < NY2; ++j2) u[j2] = S[(NY2 * k1 + j2) * PS + c];
+        for (int j2 = 0; j2 < NY2; ++j2) u[j2] = S[(NY2 * k1 + j2) * PS + SKS * k1 + c];
         DFT<NY2, -1, V>::run(u);
 #pragma unroll
         for (int k2 = 0; k2 < NY2; ++k2) {
@@ -1302,6 +1328,11 @@ struct Plan {
   static size_t sm_floc() {
     return sizeof(V) * ((size_t)NF1 * (N0 + 1) + NF0 + NF1 + (size_t)(FLOC_THREADS / 32) * FftGroup<NF0>::f * (NF0 + 1));
   }
+  static size_t sm_floc2() {
+    using LY = FlocLayout<T, NF0, NF1>;
+    return sizeof(V) * ((size_t)LY::template s_size<NF1 / Split<NF1>::n1>() + NF0 + NF1 +
+                        (size_t)(FLOC_THREADS / 32) * FftGroup<NF0>::f * LY::PR);
+  }
   static size_t sm_fplane(int cr) {
     return sizeof(V) * ((size_t)NF1 * (N0 + 1) + (size_t)cr * (NF0 + 1) + NF0 + NF1);
   }
@@ -1318,7 +1349,7 @@ struct Plan {
     PWB_CUDA(cudaFuncSetAttribute(k_cxy_inv<T, N0, N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_cxy()));
     PWB_CUDA(cudaFuncSetAttribute(k_zteter<T, N2, TX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_zteter()));
     PWB_CUDA(cudaFuncSetAttribute(k_floc<T, NF0, NF1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_floc()));
-    PWB_CUDA(cudaFuncSetAttribute(k_floc2<T, NF0, NF1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_floc()));
+    PWB_CUDA(cudaFuncSetAttribute(k_floc2<T, NF0, NF1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_floc2()));
     PWB_CUDA(cudaFuncSetAttribute(k_floc<T, NF0, NF1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_floc()));
     done = true;
     return PW_OK;
@@ -1346,7 +1377,7 @@ struct Plan {
         AD, K, BC, reinterpret_cast<const T*>(c->ekin.p), N0, N1, inv_nc, tw(c, 2), tw(c, 5)); }
     if (c->nl_mode == PW_NL_DENSE) {
       { Launch L_(c, st, KK_FPLANE_APPLY);
-      k_floc2<T, NF0, NF1><<<dim3(NF2, npair), FLOC_THREADS, sm_floc(), st>>>(
+      k_floc2<T, NF0, NF1><<<dim3(NF2, npair), FLOC_THREADS, sm_floc2(), st>>>(
           BC, reinterpret_cast<const T*>(c->vtot.p), inv_nf, tw(c, 3), tw(c, 4)); }
       { Launch L_(c, st, KK_ZFOLD);
       k_zfold<T, N2, NF2, TXF><<<dim3(N1, (N0 + TXF - 1) / TXF, npair), PENCIL_THREADS, sm_zfold(), st>>>(BC, K, AD, N0, N1, tw(c, 2), tw(c, 5)); }
@@ -1583,7 +1614,7 @@ struct Plan {
         AD, K, BC, ekin_all ? ekin_all : reinterpret_cast<const T*>(c->ekin_k.p), N0, N1, inv_nc, tw(c, 2), tw(c, 5),
         1, band0, fpk, ekin_all ? c->ntot : 0); }
     { Launch L_(c, st, KK_FPLANE_APPLY);
-    k_floc2<T, NF0, NF1><<<dim3(NF2, nb), FLOC_THREADS, sm_floc(), st>>>(
+    k_floc2<T, NF0, NF1><<<dim3(NF2, nb), FLOC_THREADS, sm_floc2(), st>>>(
         BC, reinterpret_cast<const T*>(c->vtot.p), inv_nf, tw(c, 3), tw(c, 4)); }
     { Launch L_(c, st, KK_ZFOLD);
     k_zfold<T, N2, NF2, TXF><<<dim3(N1, (N0 + TXF - 1) / TXF, nb), PENCIL_THREADS, sm_zfold(), st>>>(
@@ -1779,7 +1810,7 @@ struct Plan {
     k_gs_zinv<T, N0, N1, NF2><<<dim3(N1 + 1, npair), PENCIL_THREADS, sm_gs_zinv(), st>>>(
         psi, ld, nband, band0, rows_i, ent_i, BC, tw(c, 5)); }
     { Launch L_(c, st, KK_FPLANE_APPLY);
-    k_floc2<T, NF0, NF1><<<dim3(NF2, npair), FLOC_THREADS, sm_floc(), st>>>(
+    k_floc2<T, NF0, NF1><<<dim3(NF2, npair), FLOC_THREADS, sm_floc2(), st>>>(
         BC, reinterpret_cast<const T*>(c->vtot.p), inv_n, tw(c, 3), tw(c, 4)); }
     { Launch L_(c, st, KK_ZFOLD);
     k_gs_zfwd<T, N0, N1, NF2><<<dim3(N1 / 2 + 1, npair), PENCIL_THREADS, sm_gs_zfwd(), st>>>(
