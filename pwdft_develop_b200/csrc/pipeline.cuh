@@ -630,23 +630,30 @@ template <int N> __device__ __forceinline__ int fine_slot(int e) {
 // Shared-memory layout of k_floc2: S tile (slot columns of the fine plane)
 // with row y at y PS + SKS (y / NY2), per-warp row buffers with element e of
 // row f at f PR + e + SKR (e / NX2), and whether the first pass of the column
-// and row transforms puts the transform index on the fastest lanes.  The
-// FP32 96 x 96 plane uses the layout with the fewest shared-memory
-// wavefronts found by a search over pitches, skews and lane maps with a
-// bank model of its 8-byte accesses (31 % fewer than plain padded rows);
-// other planes keep plain padded rows.
+// (FA) and row (FB) transforms puts the transform index on the fastest lanes.
+// The specialised planes use the layout with the fewest shared-memory
+// wavefronts found by a search over pitches, skews and lane maps with a bank
+// model of their 8- / 16-byte accesses (twiddle loads included; 96: 31 % /
+// 20 % fewer than plain padded rows for FP32 / FP64, 48: 19 % / 15 %, 144:
+// 9 % / 19 %); other planes keep plain padded rows.
 template <typename T, int NXF, int NYF> struct FlocLayout {
-  static constexpr int PS = NXF / 2 + 1, SKS = 0;
-  static constexpr int PR = NXF + 1, SKR = 0;
-  static constexpr bool FAST_F = false;
-  template <int NY2> static constexpr int s_size() { return NYF * PS + SKS * (NYF / NY2); }
+  static constexpr int PS = NXF / 2 + 1, SKS = 0, PR = NXF + 1, SKR = 0;
+  static constexpr bool FA = false, FB = false;
 };
-template <> struct FlocLayout<float, 96, 96> {
-  static constexpr int PS = 60, SKS = 2;
-  static constexpr int PR = 108, SKR = 1;
-  static constexpr bool FAST_F = true;
-  template <int NY2> static constexpr int s_size() { return 96 * PS + SKS * (96 / NY2); }
-};
+#define PWB_FLOC_LAYOUT(T_, N_, PS_, SKS_, PR_, SKR_, FA_, FB_)               \
+  template <> struct FlocLayout<T_, N_, N_> {                                 \
+    static constexpr int PS = PS_, SKS = SKS_, PR = PR_, SKR = SKR_;          \
+    static constexpr bool FA = FA_, FB = FB_;                                 \
+  };
+PWB_FLOC_LAYOUT(float, 96, 60, 2, 108, 1, true, true)
+PWB_FLOC_LAYOUT(double, 96, 52, 1, 106, 1, true, true)
+PWB_FLOC_LAYOUT(float, 48, 37, 3, 54, 1, true, true)
+PWB_FLOC_LAYOUT(double, 48, 29, 3, 54, 1, true, false)
+PWB_FLOC_LAYOUT(float, 144, 73, 1, 156, 1, false, false)
+PWB_FLOC_LAYOUT(double, 144, 74, 1, 156, 1, false, false)
+#undef PWB_FLOC_LAYOUT
+// elements of the S tile of k_floc2 for a plane of NYF rows split NY2 per skew step
+template <typename LY, int NYF, int NY2> constexpr int floc_s_size() { return NYF * LY::PS + LY::SKS * (NYF / NY2); }
 
 template <typename T, int NXF, int NYF>
 __global__ void __launch_bounds__(FLOC_THREADS, sizeof(T) == 4 ? 3 : 1)
@@ -656,14 +663,14 @@ k_floc2(VT<T>* __restrict__ BC, const T* __restrict__ vtot, T inv_nf, const VT<T
   constexpr int nsx = n0 + 1, nsy = NYF / 2 + 1;
   using LY = FlocLayout<T, NXF, NYF>;
   constexpr int PS = LY::PS, SKS = LY::SKS, PR = LY::PR, SKR = LY::SKR;
-  constexpr bool FF = LY::FAST_F;
+  constexpr bool FA = LY::FA, FB = LY::FB;
   constexpr int NX1 = Split<NXF>::n1, NX2 = NXF / NX1, FX = 32 / NX1;
   constexpr int NY1 = Split<NYF>::n1, NY2 = NYF / NY1, FY = 32 / NY1;
   constexpr int RX = (FX * NX2 + 31) / 32, RY = (FY * NY2 + 31) / 32;
   static_assert(PS >= nsx && PR >= NXF + SKR * (NX1 - 1), "k_floc2 layout rows overlap");
   extern __shared__ __align__(16) unsigned char smraw[];
   V* S = reinterpret_cast<V*>(smraw);          // row y at y PS + SKS (y / NY2)
-  V* twx = S + LY::template s_size<NY2>();
+  V* twx = S + floc_s_size<LY, NYF, NY2>();
   V* twy = twx + NXF;
   V* Rall = twy + NYF;                          // [nwarps][FX][PR]
   load_tw(twx, twx_g, NXF);
@@ -679,7 +686,7 @@ k_floc2(VT<T>* __restrict__ BC, const T* __restrict__ vtot, T inv_nf, const VT<T
 #pragma unroll
     for (int r = 0; r < RY; ++r) {
       const int it = lane + 32 * r;
-      const int f = FF ? it % FY : it / NY2, j2 = FF ? it / FY : it - f * NY2;
+      const int f = FA ? it % FY : it / NY2, j2 = FA ? it / FY : it - f * NY2;
       const int c = g + f;
       if (it < FY * NY2 && c < nsx) {
         V t[NY1];
@@ -730,7 +737,7 @@ k_floc2(VT<T>* __restrict__ BC, const T* __restrict__ vtot, T inv_nf, const VT<T
 #pragma unroll
     for (int r = 0; r < RX; ++r) {
       const int it = lane + 32 * r;
-      const int f = FF ? it % FX : it / NX2, j2 = FF ? it / FX : it - f * NX2;
+      const int f = FB ? it % FX : it / NX2, j2 = FB ? it / FX : it - f * NX2;
       if (it < FX * NX2 && f < nr) {
         V t[NX1];
         const V* srow = S + (r0 + f) * PS + SKS * ((r0 + f) / NY2);
@@ -774,7 +781,7 @@ k_floc2(VT<T>* __restrict__ BC, const T* __restrict__ vtot, T inv_nf, const VT<T
 #pragma unroll
     for (int r = 0; r < RX; ++r) {
       const int it = lane + 32 * r;
-      const int f = FF ? it % FX : it / NX2, m2 = FF ? it / FX : it - f * NX2;
+      const int f = FB ? it % FX : it / NX2, m2 = FB ? it / FX : it - f * NX2;
       if (it < FX * NX2 && f < nr) {
         V t[NX1];
 #pragma unroll
@@ -797,7 +804,7 @@ k_floc2(VT<T>* __restrict__ BC, const T* __restrict__ vtot, T inv_nf, const VT<T
 #pragma unroll
     for (int r = 0; r < RY; ++r) {
       const int it = lane + 32 * r;
-      const int f = FF ? it % FY : it / NY2, j2 = FF ? it / FY : it - f * NY2;
+      const int f = FA ? it % FY : it / NY2, j2 = FA ? it / FY : it - f * NY2;
       const int c = g + f;
       if (it < FY * NY2 && c < nsx) {
         V t[NY1];
@@ -1330,7 +1337,7 @@ struct Plan {
   }
   static size_t sm_floc2() {
     using LY = FlocLayout<T, NF0, NF1>;
-    return sizeof(V) * ((size_t)LY::template s_size<NF1 / Split<NF1>::n1>() + NF0 + NF1 +
+    return sizeof(V) * ((size_t)floc_s_size<LY, NF1, NF1 / Split<NF1>::n1>() + NF0 + NF1 +
                         (size_t)(FLOC_THREADS / 32) * FftGroup<NF0>::f * LY::PR);
   }
   static size_t sm_fplane(int cr) {
