@@ -175,7 +175,7 @@ template <typename F> __device__ __forceinline__ void for_rows_cols(int rows, in
 // z pencils: coarse FFT z, kinetic, Nyquist unfold, fine pad, fine IFFT z
 // ---------------------------------------------------------------------------
 template <typename T, int NZ, int NZF, int TX>
-__global__ void __launch_bounds__(PENCIL_THREADS, sizeof(T) == 4 ? 4 : 1)
+__global__ void __launch_bounds__(PENCIL_THREADS, sizeof(T) == 4 ? 4 : 2)
 k_zpad(const VT<T>* __restrict__ A, VT<T>* __restrict__ K, VT<T>* __restrict__ B,
        const T* __restrict__ ekin, int n0, int n1, T inv_nc,
        const VT<T>* twz_g, const VT<T>* twzf_g, int cplx = 0, int kf0 = 0, int fpk = 1 << 30, long kstride = 0) {
@@ -998,7 +998,7 @@ __global__ void k_nl_reduce(const VT<T>* __restrict__ Wp, VT<T>* __restrict__ W,
 // z pencils: fine FFT z, fold to coarse (IP_f2c), add kinetic, coarse IFFT z
 // ---------------------------------------------------------------------------
 template <typename T, int NZ, int NZF, int TX>
-__global__ void __launch_bounds__(PENCIL_THREADS, sizeof(T) == 4 ? 4 : 1)
+__global__ void __launch_bounds__(PENCIL_THREADS, sizeof(T) == 4 ? 4 : 2)
 k_zfold(const VT<T>* __restrict__ C, const VT<T>* __restrict__ K, VT<T>* __restrict__ D, int n0, int n1,
         const VT<T>* twz_g, const VT<T>* twzf_g, int deriv = 0, T gfac = 0, int cplx = 0) {
   using V = VT<T>;
