@@ -221,19 +221,26 @@ def scf_bench(device: int, max_iter: int = 60):
         c.set_band_batch(NBAND)
         if mode == "mixed":
             c.build_twin()          # set-up, like set_atoms: FP32 tables and projector matrix
-        # untimed warm-up (solver handles, first-use buffers), 2 SCF iterations
-        c.scf(nocc=128, nextra=32, ecut=20.0, solver="chebfsi", mixed=(mode == "mixed"), cheby_degree=10,
-              cheby_first_cycles=1, tol_efree=1e-6, refine_threshold=1e9 if mode == "mixed" else 1e-5, max_iter=2,
-              seed=SEED, graphs=True)
+        # untimed warm-up on the timed path (solver handles, first-use buffers and
+        # kernel modules of both eigensolver precisions): 3 SCF iterations, then
+        # one iteration forced to the FP64 refinement
+        kw = dict(nocc=128, nextra=32, ecut=20.0, solver="chebfsi", mixed=(mode == "mixed"), cheby_degree=10,
+                  seed=SEED, graphs=True)
+        c.scf(cheby_first_cycles=5, tol_efree=1e-6, refine_threshold=3e-6, max_iter=3, **kw)
+        c.scf(cheby_first_cycles=1, tol_efree=1e-6, refine_threshold=1e9, max_iter=1, **kw)
         torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        res, eig, _ = c.scf(nocc=128, nextra=32, ecut=20.0, solver="chebfsi", mixed=(mode == "mixed"),
-                            cheby_degree=10, cheby_first_cycles=5, tol_efree=1e-6, refine_threshold=3e-6,
-                            max_iter=max_iter, seed=SEED, graphs=True)
-        e1.record()
-        torch.cuda.synchronize()
-        out[mode] = dict(seconds=e0.elapsed_time(e1) / 1e3, iterations=res["iterations"],
+        # two timed runs (the SCF makes many small host round trips per iteration,
+        # so a busy shared host shows up as run-to-run spread); the faster is reported
+        samples = []
+        for _ in range(2):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            res, eig, _ = c.scf(cheby_first_cycles=5, tol_efree=1e-6, refine_threshold=3e-6, max_iter=max_iter,
+                                **kw)
+            e1.record()
+            torch.cuda.synchronize()
+            samples.append(e0.elapsed_time(e1) / 1e3)
+        out[mode] = dict(seconds=min(samples), samples_s=samples, iterations=res["iterations"],
                          converged=bool(res["converged"]), efree=res["efree"], etot=res["etot"],
                          refine_iter=res["refine_iter"], hpsi_bands=res["hpsi_bands"], homo=float(eig[127]),
                          lumo=float(eig[128]))
@@ -247,7 +254,7 @@ def scf_bench(device: int, max_iter: int = 60):
     out["speedup_mixed_vs_f64"] = out["f64"]["seconds"] / out["mixed"]["seconds"]
     out["efree_agreement_per_atom"] = abs(out["f64"]["efree"] - out["mixed"]["efree"]) / 64
     out["workload"] = ("Si64, ChebFSI degree 10 (5 cycles in the first SCF step), Anderson(8, 0.7), 300 K, "
-                       "tol 1e-6 Ha/atom, Chebyshev filter replayed from a CUDA graph")
+                       "tol 1e-6 Ha/atom, Chebyshev filter replayed from a CUDA graph; faster of two timed runs")
     return out
 
 
