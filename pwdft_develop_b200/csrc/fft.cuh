@@ -228,8 +228,10 @@ __device__ __forceinline__ void smem_fft(V* base, int count, int es, int bs, con
 }
 
 // Same transform with compile-time element stride ES and batch stride BS:
-// addresses fold to 32-bit immediates.
-template <int N, int DIR, int ES, int BS, typename V>
+// addresses fold to 32-bit immediates.  FB puts the transform index on the
+// fastest lanes of the first pass (lane -> (f = it % F, j2 = it / F)), which
+// spreads a warp's accesses over more banks when BS is small against ES.
+template <int N, int DIR, int ES, int BS, bool FB = false, typename V>
 __device__ __forceinline__ void smem_fft_c(V* base, int count, const V* tw, int warp, int nw) {
   constexpr int N1 = Split<N>::n1;
   constexpr int N2 = N / N1;
@@ -241,7 +243,7 @@ __device__ __forceinline__ void smem_fft_c(V* base, int count, const V* tw, int 
 #pragma unroll
     for (int r = 0; r < R1; ++r) {
       const int it = lane + 32 * r;
-      const int f = it / N2, j2 = it - f * N2;
+      const int f = FB ? it % F : it / N2, j2 = FB ? it / F : it - f * N2;
       const int b = g + f;
       if (it < F * N2 && b < count) {
         V* p = base + b * BS + j2 * ES;
@@ -277,9 +279,9 @@ __device__ __forceinline__ void smem_fft_c(V* base, int count, const V* tw, int 
   }
 }
 
-template <int N, int DIR, int ES, int BS, typename V>
+template <int N, int DIR, int ES, int BS, bool FB = false, typename V>
 __device__ __forceinline__ void smem_fft_cb(V* base, int count, const V* tw) {
-  smem_fft_c<N, DIR, ES, BS>(base, count, tw, (int)(threadIdx.x >> 5), (int)(blockDim.x >> 5));
+  smem_fft_c<N, DIR, ES, BS, FB>(base, count, tw, (int)(threadIdx.x >> 5), (int)(blockDim.x >> 5));
 }
 
 // Number of transforms one warp processes together for length N.

@@ -44,6 +44,33 @@ constexpr int PENCIL_THREADS = 256;
 
 template <typename T> using VT = typename C2<T>::t;
 
+// Shared-memory layout of the coarse plane kernels (k_cxy_*, k_exx_*): row y
+// at y P0, FR / FC the first-pass lane maps (smem_fft_c's FB) of the x (row)
+// and y (column) transforms.  The specialised planes use the pitch and maps
+// with the fewest shared-memory wavefronts in a bank model of their 8- /
+// 16-byte accesses (twiddle loads included): 48 x 48 27 % (FP32) / 6 % (FP64)
+// fewer than P0 = 49 (measured FP32: forward 69 -> 63 us, inverse 54 -> 50 us
+// on the 160-band Si64 batch), 24 x 24 17 % / 20 %, 72 x 72 23 % / 4 %.  The
+// same search on the z pencils found 12-15 % fewer wavefronts in the
+// transforms but slower kernels (the copy phases lose more), so they keep
+// rows padded by one.
+template <typename T, int N0, int N1> struct PlaneLayout {
+  static constexpr int P0 = N0 + 1;
+  static constexpr bool FR = false, FC = false;
+};
+#define PWB_PLANE_LAYOUT(T_, N_, P0_, FR_, FC_) \
+  template <> struct PlaneLayout<T_, N_, N_> {  \
+    static constexpr int P0 = P0_;              \
+    static constexpr bool FR = FR_, FC = FC_;   \
+  };
+PWB_PLANE_LAYOUT(float, 24, 28, true, true)
+PWB_PLANE_LAYOUT(double, 24, 25, true, true)
+PWB_PLANE_LAYOUT(float, 48, 53, false, true)
+PWB_PLANE_LAYOUT(double, 48, 53, true, true)
+PWB_PLANE_LAYOUT(float, 72, 76, true, true)
+PWB_PLANE_LAYOUT(double, 72, 73, true, true)
+#undef PWB_PLANE_LAYOUT
+
 __device__ __forceinline__ int sgn_idx(int k, int n) { return k <= n / 2 ? k : k - n; }
 // slot s in [0, n]: s < n is the FFT index (Nyquist = "+" slot), s == n is the "-" Nyquist slot
 __device__ __forceinline__ int slot_fine(int s, int n, int nf) {
@@ -77,7 +104,8 @@ __global__ void __launch_bounds__(PLANE_THREADS)
 k_cxy_fwd(const T* __restrict__ psi, int ld, int nband, int band0, VT<T>* __restrict__ A,
           const VT<T>* twx_g, const VT<T>* twy_g) {
   using V = VT<T>;
-  constexpr int P0 = N0 + 1;
+  using PL = PlaneLayout<T, N0, N1>;
+  constexpr int P0 = PL::P0;
   extern __shared__ __align__(16) unsigned char smraw[];
   V* pl = reinterpret_cast<V*>(smraw);
   V* twx = pl + N1 * P0;
@@ -107,9 +135,9 @@ k_cxy_fwd(const T* __restrict__ psi, int ld, int nband, int band0, VT<T>* __rest
   }
   cp_async_wait_all();
   __syncthreads();
-  smem_fft_cb<N0, -1, 1, P0>(pl, N1, twx);
+  smem_fft_cb<N0, -1, 1, P0, PL::FR>(pl, N1, twx);
   __syncthreads();
-  smem_fft_cb<N1, -1, P0, 1>(pl, N0, twy);
+  smem_fft_cb<N1, -1, P0, 1, PL::FC>(pl, N0, twy);
   __syncthreads();
   const int N2 = gridDim.x;
   V* Ap = A + ((long)p * N2 + z) * ntot_plane;
@@ -425,7 +453,8 @@ __global__ void __launch_bounds__(PLANE_THREADS)
 k_exx_fwd(const T* __restrict__ psi, int ld, int k0, const T* __restrict__ phi, int ldp, int j0, int nphi, int njp,
           VT<T>* __restrict__ A, const VT<T>* twx_g, const VT<T>* twy_g) {
   using V = VT<T>;
-  constexpr int P0 = N0 + 1;
+  using PL = PlaneLayout<T, N0, N1>;
+  constexpr int P0 = PL::P0;
   extern __shared__ __align__(16) unsigned char smraw[];
   V* pl = reinterpret_cast<V*>(smraw);
   V* twx = pl + N1 * P0;
@@ -445,9 +474,9 @@ k_exx_fwd(const T* __restrict__ psi, int ld, int k0, const T* __restrict__ phi, 
     pl[y * P0 + x] = mkc<V>(v * pa[i], pb ? v * pb[i] : (T)0);
   }
   __syncthreads();
-  smem_fft_cb<N0, -1, 1, P0>(pl, N1, twx);
+  smem_fft_cb<N0, -1, 1, P0, PL::FR>(pl, N1, twx);
   __syncthreads();
-  smem_fft_cb<N1, -1, P0, 1>(pl, N0, twy);
+  smem_fft_cb<N1, -1, P0, 1, PL::FC>(pl, N0, twy);
   __syncthreads();
   const int N2 = gridDim.x;
   V* Ap = A + ((long)f * N2 + z) * ntot_plane;
@@ -465,7 +494,8 @@ k_exx_inv(const VT<T>* __restrict__ A, int njp, const T* __restrict__ phi, int l
           const T* __restrict__ wj, T* __restrict__ out, int ldo, int k0, int accumulate, const VT<T>* twx_g,
           const VT<T>* twy_g) {
   using V = VT<T>;
-  constexpr int P0 = N0 + 1;
+  using PL = PlaneLayout<T, N0, N1>;
+  constexpr int P0 = PL::P0;
   extern __shared__ __align__(16) unsigned char smraw[];
   V* pl = reinterpret_cast<V*>(smraw);
   V* twx = pl + N1 * P0;
@@ -485,9 +515,9 @@ k_exx_inv(const VT<T>* __restrict__ A, int njp, const T* __restrict__ phi, int l
       pl[y * P0 + x] = Dp[i];
     }
     __syncthreads();
-    smem_fft_cb<N1, +1, P0, 1>(pl, N0, twy);
+    smem_fft_cb<N1, +1, P0, 1, PL::FC>(pl, N0, twy);
     __syncthreads();
-    smem_fft_cb<N0, +1, 1, P0>(pl, N1, twx);
+    smem_fft_cb<N0, +1, 1, P0, PL::FR>(pl, N1, twx);
     __syncthreads();
     const int ja = j0 + 2 * jp, jb = ja + 1;
     const T wa = wj[ja], wb = (jb < nphi) ? wj[jb] : (T)0;
@@ -1144,6 +1174,14 @@ k_zteter(VT<T>* __restrict__ A, const T* __restrict__ teter, int n0, int n1, T i
 //   gather list, one block per slot row r <= n1/2 and its mirror row: {s,
 //     offset of G_s | offset of -G_s << 16} in the block's two-row layout
 // ---------------------------------------------------------------------------
+// First-pass lane maps of the scatter (FI) and gather (FF) z transforms at the
+// fixed pitches n0+1 and 2(n0+1)+1 the entry lists are built for; on the 96
+// grid the transform-fastest map saves 7 % / 13 % (FP64) and 4 % (FP32
+// gather) of the shared-memory wavefronts in the bank model.
+template <typename T, int NZF> struct GsLanes { static constexpr bool FI = false, FF = false; };
+template <> struct GsLanes<float, 96> { static constexpr bool FI = false, FF = true; };
+template <> struct GsLanes<double, 96> { static constexpr bool FI = true, FF = true; };
+
 __device__ __forceinline__ int mirror_slot(int s, int n) {
   return s == 0 ? 0 : (s == n / 2 ? n : (s == n ? n / 2 : n - s));
 }
@@ -1183,7 +1221,7 @@ k_gs_zinv(const T* __restrict__ psi, int ld, int nband, int band0, const int* __
     in[en.y] = z;
   }
   __syncthreads();
-  smem_fft_cb<NZF, +1, PI, 1>(in, nsx, twz);
+  smem_fft_cb<NZF, +1, PI, 1, GsLanes<T, NZF>::FI>(in, nsx, twz);
   __syncthreads();
   V* Bp = B + (long)p * NZF * nsy * nsx + (long)ky * nsx;
   for_rows_cols(NZF, nsx, [&](int z, int kx) { Bp[(long)z * nsy * nsx + kx] = in[z * PI + kx]; });
@@ -1214,7 +1252,7 @@ k_gs_zfwd(const VT<T>* __restrict__ B, const T* __restrict__ psi, int ld, T* __r
   });
   cp_async_wait_all();
   __syncthreads();
-  smem_fft_cb<NZF, -1, PI, 1>(in, nrow * nsx, twz);
+  smem_fft_cb<NZF, -1, PI, 1, GsLanes<T, NZF>::FF>(in, nrow * nsx, twz);
   __syncthreads();
   const int ba = band0 + 2 * p, bb = ba + 1;
   const bool hb = bb < nband;
@@ -1254,7 +1292,8 @@ __global__ void __launch_bounds__(PLANE_THREADS)
 k_cxy_inv(const VT<T>* __restrict__ D, T* __restrict__ out, int ldo, int nband, int band0, int accumulate,
           const VT<T>* twx_g, const VT<T>* twy_g) {
   using V = VT<T>;
-  constexpr int P0 = N0 + 1;
+  using PL = PlaneLayout<T, N0, N1>;
+  constexpr int P0 = PL::P0;
   extern __shared__ __align__(16) unsigned char smraw[];
   V* pl = reinterpret_cast<V*>(smraw);
   V* twx = pl + N1 * P0;
@@ -1271,9 +1310,9 @@ k_cxy_inv(const VT<T>* __restrict__ D, T* __restrict__ out, int ldo, int nband, 
   }
   cp_async_wait_all();
   __syncthreads();
-  smem_fft_cb<N1, +1, P0, 1>(pl, N0, twy);
+  smem_fft_cb<N1, +1, P0, 1, PL::FC>(pl, N0, twy);
   __syncthreads();
-  smem_fft_cb<N0, +1, 1, P0>(pl, N1, twx);
+  smem_fft_cb<N0, +1, 1, P0, PL::FR>(pl, N1, twx);
   __syncthreads();
   if (CPLX) {
     V* oc = reinterpret_cast<V*>(out) + (long)(band0 + p) * ldo + z * ntot_plane;
@@ -1327,7 +1366,7 @@ struct Plan {
 
   static int chunk_rows() { return fplane_cr<T>(NF0, NF1); }
 
-  static size_t sm_cxy() { return sizeof(V) * (N1 * (N0 + 1) + N0 + N1); }
+  static size_t sm_cxy() { return sizeof(V) * (N1 * PlaneLayout<T, N0, N1>::P0 + N0 + N1); }
   static size_t sm_zpad() { return sizeof(V) * (N2 * (TX + 1) + NF2 * (2 * TX + 1) + N2 + NF2); }
   static size_t sm_zfold() { return sizeof(V) * (NF2 * (2 * TXF + 1) + N2 * (TXF + 1) + N2 + NF2); }
   static size_t sm_zteter() { return sizeof(V) * (N2 * (TX + 1) + N2); }
