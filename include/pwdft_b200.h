@@ -217,6 +217,14 @@ PW_API int pw_xc_teter93(pw_ctx* ctx, const double* rho_dev, double* eps_dev, do
  * rho vol / N_fine); vxc = d e/d rho - div(2 d e/d|grad rho|^2 grad rho).
  * Cubic cells and fine grids only. */
 PW_API int pw_xc_pbe(pw_ctx* ctx, const double* rho_dev, double ecut, double* eps_dev, double* vxc_dev);
+/* Semilocal part of HSE06 on the fine grid (same arguments and layout as
+ * pw_xc_pbe): PBE minus 0.25 times the erfc-screened (omega = 0.106) PBE
+ * exchange where |rho| > 1e-6 and |grad rho|^2 > 1e-10 -- the
+ * XC_HYB_GGA_XC_HSE06 branch of KohnSham::CalculateXC (src/SCF/
+ * hamiltonian.cpp:1563, 1614-1627) with pbexsr / wpbe_analy_erfc_approx_grad
+ * (src/utility.cpp:3340-3846).  The exact-exchange part of the hybrid is
+ * pw_exx_setup(ctx, 0.25, 0.106, ...) and the pw_exx_* calls. */
+PW_API int pw_xc_hse06(pw_ctx* ctx, const double* rho_dev, double ecut, double* eps_dev, double* vxc_dev);
 enum { PW_XC_TETER93 = 0, PW_XC_PBE = 1 };
 
 typedef struct pw_scf_params {

@@ -7,9 +7,13 @@ reference source tree (never copied into this repository): ``spline`` and
 ``seval`` (src/utility.cpp:54-225), ``IP_c2f`` / ``IP_f2c``
 (src/utility.cpp:3148-3275) and the internal PBE pieces ``VExchange_sla``,
 ``VCorrelation_pw``, ``VGCExchange_pbx``, ``VGCCorrelation_pbc``
-(src/utility.cpp:3913-4244, the ``Use_Libxc: 0`` path of KohnSham::CalculateXC).  The recipe extracts each function body from
+(src/utility.cpp:3913-4244, the ``Use_Libxc: 0`` path of KohnSham::CalculateXC)
+and the HSE06 short-range PBE exchange ``pbexsr`` with
+``wpbe_analy_erfc_approx_grad`` and ``EXPINT`` (src/utility.cpp:3340-3911).  The recipe extracts each function body from
 ``<reference>/src/utility.cpp`` by brace matching into ``oracle/_ref/`` (git
-ignored), prepends the two typedefs it needs, adds extern "C" wrappers and
+ignored), prepends the headers and typedefs it needs (``<stdlib.h>`` first, as
+include/utility.hpp:49 has it: it puts the floating-point ``abs`` overloads
+that ``EXPINT`` relies on into the global namespace), adds extern "C" wrappers and
 builds a shared object with g++.  Tests use it to pin the NumPy restatement.
 """
 from __future__ import annotations
@@ -27,17 +31,23 @@ DEFAULT_REF = Path(os.environ.get("PWDFT_REFERENCE", "/root/reference"))
 FUNCS = [("void spline(", "spline"), ("void seval(", "seval"),
          ("void IP_c2f(", "IP_c2f"), ("void IP_f2c(", "IP_f2c"),
          ("void VExchange_sla(", "VExchange_sla"), ("void VCorrelation_pw(", "VCorrelation_pw"),
-         ("void VGCExchange_pbx(", "VGCExchange_pbx"), ("void VGCCorrelation_pbc(", "VGCCorrelation_pbc")]
+         ("void VGCExchange_pbx(", "VGCExchange_pbx"), ("void VGCCorrelation_pbc(", "VGCCorrelation_pbc"),
+         ("void pbexsr(", "pbexsr"), ("void wpbe_analy_erfc_approx_grad(", "wpbe_analy_erfc_approx_grad"),
+         ("Real EXPINT(", "EXPINT")]
 
 PRELUDE = """// generated: functions compiled from the reference source tree
+#include <stdlib.h>
 #include <cmath>
 #include <complex>
 #include <stdexcept>
 typedef std::complex<double> Complex;
 typedef double Real;
+typedef int Int;
 static const double PI = 3.141592653589793;
 static void ErrorHandling(const char* m) { throw std::runtime_error(m); }
 namespace pwref {
+void wpbe_analy_erfc_approx_grad(Real rho, Real s, Real omega, Real& Fx_wpbe, Real& d1rfx, Real& d1sfx);
+Real EXPINT(Int n, Real x);
 """
 
 WRAPPERS = """
@@ -60,6 +70,15 @@ void ref_pbe_parts(double rs, double rho, double grho2, double* out) {
   pwref::VGCExchange_pbx(rho, grho2, out[4], out[5], out[6]);
   pwref::VGCCorrelation_pbc(rho, grho2, out[7], out[8], out[9]);
 }
+// out: sx v1x v2x of the short-range PBE exchange at (rho, grho2, omega)
+void ref_pbexsr(double rho, double grho2, double omega, double* out) {
+  pwref::pbexsr(rho, grho2, omega, out[0], out[1], out[2]);
+}
+// out: F_x d1rfx d1sfx of the screened enhancement factor at (rho, s, omega)
+void ref_wpbe(double rho, double s, double omega, double* out) {
+  pwref::wpbe_analy_erfc_approx_grad(rho, s, omega, out[0], out[1], out[2]);
+}
+double ref_expint(int n, double x) { return pwref::EXPINT(n, x); }
 }
 """
 

@@ -172,13 +172,15 @@ def grad_density(dm: pw.Domain, rho: np.ndarray, ecut: float):
     return np.stack([np.fft.ifftn(X * ik).real.reshape(-1) for ik in _spectral_ik(dm, ecut)])
 
 
-def xc_pbe(dm: pw.Domain, rho: np.ndarray, ecut: float):
+def xc_pbe(dm: pw.Domain, rho: np.ndarray, ecut: float, point=None):
     """(eps per particle, V_xc) of PBE: V_xc = v1 - sum_d d_d(v2 d_d rho), the
-    divergence spectral with the same cut (hamiltonian.cpp:1750-1775)."""
+    divergence spectral with the same cut (hamiltonian.cpp:1750-1775).
+    ``point`` replaces the point functional (default xc_pbe_point; the
+    semilocal HSE06 passes oracle.hse.hse06_point)."""
     N0, N1, N2 = dm.numGridFine
     gr = grad_density(dm, rho, ecut)
     sigma = np.sum(gr * gr, axis=0)
-    eps, v1, v2 = xc_pbe_point(rho, sigma)
+    eps, v1, v2 = (point or xc_pbe_point)(rho, sigma)
     div = np.zeros((N2, N1, N0), complex)
     for d, ik in enumerate(_spectral_ik(dm, ecut)):
         div += np.fft.fftn((v2 * gr[d]).reshape(N2, N1, N0)) * ik

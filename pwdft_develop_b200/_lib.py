@@ -86,6 +86,7 @@ SIGNATURES: dict[str, tuple] = {
     "pw_hartree": (_i, [_vp, _vp, _d, _vp]),
     "pw_xc_teter93": (_i, [_vp, _vp, _vp, _vp]),
     "pw_xc_pbe": (_i, [_vp, _vp, C.c_double, _vp, _vp]),
+    "pw_xc_hse06": (_i, [_vp, _vp, C.c_double, _vp, _vp]),
     "pw_eigsolve": (_i, [_vp, _i, _vp, _i, _i, _d, _i, _dp, _dp, _ip]),
     "pw_density": (_i, [_vp, _vp, _i, _i, _dp, _i, _vp]),
     "pw_scf_run": (_i, [_vp, C.POINTER(ScfParams), C.POINTER(ScfResult), _dp, _dp]),

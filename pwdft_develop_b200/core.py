@@ -392,6 +392,19 @@ def _ctx_xc_pbe(self, rho, ecut: float):
 Context.xc_pbe = _ctx_xc_pbe
 
 
+def _ctx_xc_hse06(self, rho, ecut: float):
+    """Semilocal HSE06 (eps per particle, V_xc) of a fine-grid density: PBE minus
+    0.25 times the omega = 0.106 short-range PBE exchange (float64 device tensors)."""
+    import torch
+    eps = torch.empty_like(rho)
+    vxc = torch.empty_like(rho)
+    check(lib.pw_xc_hse06(self._h, _ptr(rho), float(ecut), _ptr(eps), _ptr(vxc)))
+    return eps, vxc
+
+
+Context.xc_hse06 = _ctx_xc_hse06
+
+
 def _ctx_build_twin(self):
     check(lib.pw_ctx_build_twin(self._h))
 

@@ -27,6 +27,7 @@
 #include "fft.cuh"
 #include "fft3d.cuh"
 #include "gemm.hpp"
+#include "wpbe.cuh"
 
 namespace pwb {
 
@@ -190,13 +191,26 @@ __device__ __forceinline__ void pbe_point(double rho, double sigma, double& eps,
   }
 }
 
-// gradient components g0..g2 in, h_d = v2 g_d out (in place); eps, v1 out
+// gradient components g0..g2 in, h_d = v2 g_d out (in place); eps, v1 out.
+// hse_frac > 0: semilocal HSE06, minus hse_frac times the short-range PBE
+// exchange of screening omega where |rho| > 1e-6 and sigma > 1e-10
+// (hamiltonian.cpp:1614-1627; |rho| is passed where the reference passes rho,
+// which differs only for rho < -1e-6, where its cube root is not a number)
 __global__ void k_pbe(long n, const double* __restrict__ rho, double* __restrict__ g0, double* __restrict__ g1,
-                      double* __restrict__ g2, double* __restrict__ eps, double* __restrict__ v1) {
+                      double* __restrict__ g2, double* __restrict__ eps, double* __restrict__ v1, double hse_frac,
+                      double omega) {
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
     const double a = g0[i], b = g1[i], c = g2[i];
+    const double r = rho[i], sigma = a * a + b * b + c * c;
     double e, u, w;
-    pbe_point(rho[i], a * a + b * b + c * c, e, u, w);
+    pbe_point(r, sigma, e, u, w);
+    if (hse_frac != 0.0 && fabs(r) > 1e-6 && sigma > 1e-10) {
+      double sx, v1x, v2x;
+      wpbe::pbexsr(fabs(r), sigma, omega, sx, v1x, v2x);
+      e -= hse_frac * sx / r;
+      u -= hse_frac * v1x;
+      w -= hse_frac * v2x;
+    }
     eps[i] = e;
     v1[i] = u;
     g0[i] = w * a;
@@ -288,7 +302,7 @@ __global__ void k_clin(long n, double a, const double2* __restrict__ x, double b
 // cubic fine grid; scratch: two complex and three real fine fields
 template <int N>
 static int pbe_n(pw_ctx* c, const double* rho, double ecut, double* eps, double* vxc, double2* S, double2* T,
-                 double* g, const double2* tw, cudaStream_t st) {
+                 double* g, const double2* tw, cudaStream_t st, double hse_frac) {
   const long n = (long)N * N * N;
   const double gs = 2 * M_PI / c->L[0];
   fft3_fwd_real<N>(S, rho, tw, st);
@@ -296,7 +310,7 @@ static int pbe_n(pw_ctx* c, const double* rho, double ecut, double* eps, double*
     k_spec_deriv<<<nblk(n), 256, 0, st>>>(N, gs, 4.0 * ecut, d, S, T, 0);
     fft3_inv_real<N>(T, g + d * n, tw, st);
   }
-  k_pbe<<<nblk(n), 256, 0, st>>>(n, rho, g, g + n, g + 2 * n, eps, vxc);
+  k_pbe<<<nblk(n), 256, 0, st>>>(n, rho, g, g + n, g + 2 * n, eps, vxc, hse_frac, 0.106);
   for (int d = 0; d < 3; ++d) {
     fft3_fwd_real<N>(S, g + d * n, tw, st);
     k_spec_deriv<<<nblk(n), 256, 0, st>>>(N, gs, 4.0 * ecut, d, S, T, d > 0);
@@ -308,15 +322,15 @@ static int pbe_n(pw_ctx* c, const double* rho, double ecut, double* eps, double*
 }
 
 static int xc_pbe(pw_ctx* c, const double* rho, double ecut, double* eps, double* vxc, double2* S, double2* T,
-                  double* g, const double2* tw, cudaStream_t st) {
+                  double* g, const double2* tw, cudaStream_t st, double hse_frac = 0.0) {
   PWB_CHECK(c->nf[0] == c->nf[1] && c->nf[1] == c->nf[2] && c->L[0] == c->L[1] && c->L[1] == c->L[2],
             PW_EUNSUPPORTED, "PBE gradients need a cubic cell and fine grid");
   switch (c->nf[0]) {
-    case 24: return pbe_n<24>(c, rho, ecut, eps, vxc, S, T, g, tw, st);
-    case 32: return pbe_n<32>(c, rho, ecut, eps, vxc, S, T, g, tw, st);
-    case 48: return pbe_n<48>(c, rho, ecut, eps, vxc, S, T, g, tw, st);
-    case 96: return pbe_n<96>(c, rho, ecut, eps, vxc, S, T, g, tw, st);
-    case 144: return pbe_n<144>(c, rho, ecut, eps, vxc, S, T, g, tw, st);
+    case 24: return pbe_n<24>(c, rho, ecut, eps, vxc, S, T, g, tw, st, hse_frac);
+    case 32: return pbe_n<32>(c, rho, ecut, eps, vxc, S, T, g, tw, st, hse_frac);
+    case 48: return pbe_n<48>(c, rho, ecut, eps, vxc, S, T, g, tw, st, hse_frac);
+    case 96: return pbe_n<96>(c, rho, ecut, eps, vxc, S, T, g, tw, st, hse_frac);
+    case 144: return pbe_n<144>(c, rho, ecut, eps, vxc, S, T, g, tw, st, hse_frac);
     default: set_error("SCF fine grid size not built"); return PW_EUNSUPPORTED;
   }
 }
@@ -1845,7 +1859,8 @@ int pw_hartree(pw_ctx* ctx, const double* drho_dev, double ecut, double* vh_dev)
   return PW_OK;
 }
 
-int pw_xc_pbe(pw_ctx* ctx, const double* rho_dev, double ecut, double* eps_dev, double* vxc_dev) {
+static int xc_gga_entry(pw_ctx* ctx, const double* rho_dev, double ecut, double* eps_dev, double* vxc_dev,
+                        double hse_frac) {
   PWB_CHECK(ctx && rho_dev && eps_dev && vxc_dev && ecut > 0, PW_EINVAL, "bad arguments");
   PWB_CUDA(cudaSetDevice(ctx->device));
   const long nf = ctx->ntotf;
@@ -1861,10 +1876,18 @@ int pw_xc_pbe(pw_ctx* ctx, const double* rho_dev, double ecut, double* eps_dev, 
   }
   PWB_CUDA(cudaMemcpy(tw.p, t.data(), N * 16, cudaMemcpyHostToDevice));
   if ((rc = xc_pbe(ctx, rho_dev, ecut, eps_dev, vxc_dev, (double2*)a.p, (double2*)b.p, (double*)g.p,
-                   (const double2*)tw.p, nullptr)))
+                   (const double2*)tw.p, nullptr, hse_frac)))
     return rc;
   PWB_CUDA(cudaDeviceSynchronize());
   return PW_OK;
+}
+
+int pw_xc_pbe(pw_ctx* ctx, const double* rho_dev, double ecut, double* eps_dev, double* vxc_dev) {
+  return xc_gga_entry(ctx, rho_dev, ecut, eps_dev, vxc_dev, 0.0);
+}
+
+int pw_xc_hse06(pw_ctx* ctx, const double* rho_dev, double ecut, double* eps_dev, double* vxc_dev) {
+  return xc_gga_entry(ctx, rho_dev, ecut, eps_dev, vxc_dev, 0.25);
 }
 
 int pw_xc_teter93(pw_ctx* ctx, const double* rho_dev, double* eps_dev, double* vxc_dev) {

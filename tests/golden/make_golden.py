@@ -3,10 +3,12 @@
 The vectors come from the reference's own ``IP_c2f``, ``IP_f2c``, ``spline``
 and ``seval`` (src/utility.cpp) -> ``ref_utility.npz``, and its internal PBE
 pieces ``VExchange_sla``, ``VCorrelation_pw``, ``VGCExchange_pbx``,
-``VGCCorrelation_pbc`` (src/utility.cpp:3913-4244) -> ``ref_xc_pbe.npz``, all
-compiled from the reference source tree by ``oracle/build_ref.py``.  Inputs
-are seeded.  Run from the repository root:
-``python tests/golden/make_golden.py [utility|pbe]`` (both by default).
+``VGCCorrelation_pbc`` (src/utility.cpp:3913-4244) -> ``ref_xc_pbe.npz``, and
+the HSE06 short-range exchange ``pbexsr`` / ``wpbe_analy_erfc_approx_grad``
+(src/utility.cpp:3340-3846) -> ``ref_xc_hse.npz``, all compiled from the
+reference source tree by ``oracle/build_ref.py``.  Inputs are seeded.  Run
+from the repository root:
+``python tests/golden/make_golden.py [utility|pbe|hse]`` (all by default).
 """
 import ctypes as C
 import sys
@@ -20,6 +22,7 @@ from oracle import build_ref  # noqa: E402
 
 OUT = Path(__file__).resolve().parent / "ref_utility.npz"
 OUT_PBE = Path(__file__).resolve().parent / "ref_xc_pbe.npz"
+OUT_HSE = Path(__file__).resolve().parent / "ref_xc_hse.npz"
 
 
 def main():
@@ -80,9 +83,33 @@ def pbe():
     print(OUT_PBE, OUT_PBE.stat().st_size)
 
 
+def hse():
+    """pbexsr at (rho, grho2) samples over densities 1e-6..10 and reduced
+    gradients s in 0..10 (s > 8.3 exercises the clamp, s < 0.08 the series
+    branch of the normalisation), omega = 0.106: (sx, v1x, v2x); and the
+    screened enhancement factor at (rho, s): (F_x, d1rfx, d1sfx)."""
+    lib = C.CDLL(str(build_ref.build()))
+    dp = C.POINTER(C.c_double)
+    rng = np.random.Generator(np.random.Philox(20261203 + 78))
+    n = 400
+    rho = 10.0 ** rng.uniform(-5.9, 1, n)
+    s = np.concatenate([rng.uniform(0, 10, n - 40), rng.uniform(0, 0.08, 20), rng.uniform(8.2, 9, 20)])
+    kf = (3 * np.pi ** 2 * rho) ** (1 / 3)
+    grho2 = (s * 2 * kf * rho) ** 2 + 1e-9
+    out = np.zeros((n, 3))
+    fx = np.zeros((n, 3))
+    for i in range(n):
+        lib.ref_pbexsr(C.c_double(rho[i]), C.c_double(grho2[i]), C.c_double(0.106), out[i].ctypes.data_as(dp))
+        lib.ref_wpbe(C.c_double(rho[i]), C.c_double(min(s[i], 8.5)), C.c_double(0.106), fx[i].ctypes.data_as(dp))
+    np.savez_compressed(OUT_HSE, rho=rho, grho2=grho2, out=out, s=np.minimum(s, 8.5), fx=fx)
+    print(OUT_HSE, OUT_HSE.stat().st_size)
+
+
 if __name__ == "__main__":
     which = sys.argv[1] if len(sys.argv) > 1 else "all"
     if which in ("all", "utility"):
         main()
     if which in ("all", "pbe"):
         pbe()
+    if which in ("all", "hse"):
+        hse()
