@@ -225,7 +225,7 @@ PW_API int pw_xc_pbe(pw_ctx* ctx, const double* rho_dev, double ecut, double* ep
  * (src/utility.cpp:3340-3846).  The exact-exchange part of the hybrid is
  * pw_exx_setup(ctx, 0.25, 0.106, ...) and the pw_exx_* calls. */
 PW_API int pw_xc_hse06(pw_ctx* ctx, const double* rho_dev, double ecut, double* eps_dev, double* vxc_dev);
-enum { PW_XC_TETER93 = 0, PW_XC_PBE = 1 };
+enum { PW_XC_TETER93 = 0, PW_XC_PBE = 1, PW_XC_HSE06 = 2 };
 
 typedef struct pw_scf_params {
   int nocc;                 /* occupied states (numOccupiedState) */
@@ -248,10 +248,13 @@ typedef struct pw_scf_params {
   int ppcg_sbsize;          /* PPCG_sbSize (PW_SOLVER_PPCG), 1..8 */
   int davidson_maxdim;      /* subspace size in blocks (PW_SOLVER_DAVIDSON), >= 2 */
   int graphs;               /* 1: replay the Chebyshev filter from a captured CUDA graph */
-  int xc;                   /* PW_XC_TETER93 (LDA, default) or PW_XC_PBE (XC_Type XC_GGA_XC_PBE, Use_Libxc 0) */
+  int xc;                   /* PW_XC_TETER93 (LDA, default), PW_XC_PBE (XC_Type XC_GGA_XC_PBE, Use_Libxc 0) or
+                               PW_XC_HSE06 (XC_HYB_GGA_XC_HSE06: PBE SCF, then nested phi iterations with ACE) */
   int mix_type;             /* PW_MIX_ANDERSON (default) or PW_MIX_BROYDEN (Mixing_Type, potential mixing) */
   double tol_rho;           /* > 0: converged when the density change's scfNorm (SCF::CalculateError) < tol_rho
                                instead of the E_free - E_Harris test */
+  int phi_max_iter;         /* PW_XC_HSE06: outer phi (ACE) iterations, Hybrid_Phi_MaxIter (0: 10) */
+  double phi_tol;           /* PW_XC_HSE06: converged when dExx = 4 |fock1 - (fock0 + fock2) / 2| < phi_tol */
 } pw_scf_params;
 enum { PW_MIX_ANDERSON = 0, PW_MIX_BROYDEN = 1 };
 
@@ -262,6 +265,9 @@ typedef struct pw_scf_result {
   double phase_s[6];        /* verbose >= 2: eigensolver, density, potentials, set-up, mixing, refine switch (s) */
   double sub_s[4];          /* verbose >= 2, inside the eigensolver: H*psi, Gram, dense FP64, rotations (s) */
   double scf_norm;          /* last SCF::CalculateError of the output-density change (scf.cpp:2368-2396) */
+  double efock;             /* PW_XC_HSE06: exchange energy of the last ACE (Efock, included in etot / efree) */
+  double dexx;              /* PW_XC_HSE06: last dExx */
+  int phi_iterations;       /* PW_XC_HSE06: outer phi iterations run */
 } pw_scf_result;
 
 /* Build (once) the FP32 twin of an FP64 context with the same cell, grids and
@@ -274,7 +280,16 @@ PW_API int pw_ctx_build_twin(pw_ctx* ctx);
  * (src/SCF/scf.cpp:372-591, 1261-1589, 2299-2365), density, Hartree and LDA
  * Teter93 XC (src/SCF/hamiltonian.cpp:1242-1308, 1990-2069, 2455-2627) and the
  * energies of scf.cpp:1834-2140, all on the device.  eig_out: host, nocc+nextra
- * doubles; rho_out: host, N_fine doubles (either may be NULL). */
+ * doubles; rho_out: host, N_fine doubles (either may be NULL).
+ * xc = PW_XC_HSE06 runs the reference's nested hybrid scheme (scf.cpp:409-
+ * 623, 628-925): a PBE SCF, then the semilocal HSE06 potential and phi
+ * iterations -- phi <- psi, ACE from the bands (exchange kernel of
+ * pw_exx_setup(ctx, 0.25, 0.106, 1, ecut)), an inner SCF with the ACE term in
+ * H, Fock energies fock1 (old ACE) / fock2 (new ACE), E += fock2 - 2 fock1,
+ * until dExx < phi_tol.  Inner SCF loops restart the mixing history; with
+ * tol_rho > 0 their criterion is the scfNorm of the potential change, as the
+ * reference's nested loop has it.  The hybrid phase runs in FP64 (a mixed run
+ * switches before it); the context keeps the ACE operator afterwards. */
 PW_API int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* eig_out, double* rho_out);
 
 /* Autotuner (no reference counterpart): times pw_hpsi on an internal block

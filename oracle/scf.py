@@ -19,6 +19,9 @@ Test infrastructure (see ``oracle/__init__.py``).  Follows:
   * SCF::andersonMix              src/SCF/scf.cpp:2299-2365
   * SCF::BroydenMix / RhoDdot      src/SCF/scf.cpp:2144-2296 (potential mixing)
   * SCF::Iterate / InnerSolve     src/SCF/scf.cpp:372-591, 1261-1589
+  * the nested hybrid scheme of SCF::Iterate (scf.cpp:409-425, 628-925): PBE SCF,
+    then the semilocal HSE06 (oracle/hse.py) with phi iterations over an ACE
+    operator (oracle/exx.py), Fock energies and dExx
   * initial density from the pseudocharge  src/SCF/scf.cpp:232-255
 The eigensolver is ARPACK (scipy eigsh) on the FP64 operator: the converged SCF
 fixed point does not depend on the eigensolver.
@@ -278,19 +281,27 @@ class SCFResult:
     vtot: np.ndarray = None
     psi: np.ndarray = None
     iterations: int = 0
+    efock: float = 0.0
+    dexx: float = 0.0
+    phi_iterations: int = 0
 
 
-def _eigsh(T: pw.HamTables, nband: int, v0=None, tol=1e-11):
+def _eigsh(T: pw.HamTables, nband: int, v0=None, tol=1e-11, xi=None):
+    """Lowest eigenpairs of H (plus the ACE term -xi^T xi when xi is given)."""
     from scipy.sparse.linalg import LinearOperator, eigsh
     n = T.dm.ntot
 
+    def hx(rows):
+        out = pw.mult_spinor(T, np.ascontiguousarray(rows))
+        if xi is not None:
+            out = out - (rows @ xi.T) @ xi
+        return out
+
     def mv(x):
-        x = np.asarray(x).reshape(-1, n) if x.ndim > 1 else x.reshape(1, n)
-        return pw.mult_spinor(T, np.ascontiguousarray(x.reshape(-1, n))).reshape(x.shape).T.squeeze() \
-            if False else pw.mult_spinor(T, x.reshape(1, n)).reshape(-1)
+        return hx(np.asarray(x).reshape(1, n)).reshape(-1)
 
     def mm(X):
-        return pw.mult_spinor(T, np.ascontiguousarray(X.T)).T
+        return hx(X.T).T
 
     A = LinearOperator((n, n), matvec=mv, matmat=mm, dtype=np.float64)
     w, V = eigsh(A, k=nband, which="SA", tol=tol, v0=v0, ncv=min(n, max(2 * nband + 1, nband + 32)))
@@ -301,10 +312,13 @@ def _eigsh(T: pw.HamTables, nband: int, v0=None, tol=1e-11):
 def scf(L, znuc, pos, numGrid, numGridFine, nocc: int, nextra: int, ecut: float,
         temperature: float = 300.0, tol_efree: float = 1e-7, max_iter: int = 60, mix_dim: int = 8,
         mix_step: float = 0.7, eig_tol: float = 1e-11, verbose: bool = False, xc: str = "teter93",
-        mix: str = "anderson", tol_rho: float | None = None) -> SCFResult:
+        mix: str = "anderson", tol_rho: float | None = None, phi_max_iter: int = 10,
+        phi_tol: float = 1e-6) -> SCFResult:
     """Restated SCF::Iterate with potential Anderson mixing; converges when
     |E_free - E_Harris| / N_atom < tol_efree (the reference's efreeDifPerAtom,
-    scf.cpp:467)."""
+    scf.cpp:467).  xc = "hse06": the nested hybrid scheme (PBE SCF, then phi
+    iterations with ACE until dExx < phi_tol; inner loops restart the mixing
+    history and, with tol_rho, test the scfNorm of the potential change)."""
     L = np.asarray(L, dtype=np.float64)
     zs = np.broadcast_to(np.asarray(znuc), (len(pos),))
     dm = pw.Domain(tuple(L), tuple(numGrid), tuple(numGridFine))
@@ -324,21 +338,32 @@ def scf(L, znuc, pos, numGrid, numGridFine, nocc: int, nextra: int, ecut: float,
     # initial density from the pseudocharge (scf.cpp:232-255)
     rho = np.where(rho_ps > 1e-6, rho_ps, 1e-6)
     rho *= rho_ps.sum() / rho.sum()
+    hybrid = xc == "hse06"
     xcf = xc_teter93 if xc == "teter93" else (lambda r: xc_pbe(dm, r, ecut))
     eps, vxc = xcf(rho)
     exc = float(np.sum(eps * rho) * w)
     vh = hartree(dm, rho, rho_ps, ecut, gkk)
     vtot = vh + vxc
     T = pw.HamTables(dm, ekin, teter, vtot, pseudo)
-    dv_hist, df_hist = [], []
-    bst = BroydenState(mix_dim)
     psi = None
     hist = []
     res = None
-    for it in range(1, max_iter + 1):
+    xi = None
+    inner = False
+
+    def loop():
+        nonlocal vtot, rho, exc, vxc, vh, psi, res
+        dv_hist, df_hist = [], []
+        bst = BroydenState(mix_dim)
+        for it in range(1, max_iter + 1):
+            if step(it, dv_hist, df_hist, bst):
+                return
+
+    def step(it, dv_hist, df_hist, bst):
+        nonlocal vtot, rho, exc, vxc, vh, psi, res
         T.vtot = vtot
         v0 = psi[0] if psi is not None else None
-        eig, psi = _eigsh(T, nband, v0=v0, tol=eig_tol)
+        eig, psi = _eigsh(T, nband, v0=v0, tol=eig_tol, xi=xi)
         occ, ef = occupations(eig, nocc, tbeta)
         # Harris energy with the input density / potentials (scf.cpp:1987-2140)
         ekin_b = float(np.sum(2 * eig * occ))
@@ -359,21 +384,65 @@ def scf(L, znuc, pos, numGrid, numGridFine, nocc: int, nextra: int, ecut: float,
         etot = ekin_b + ecor
         efree = etot + float(np.sum(2 * entropy(eig, ef, tbeta)))
         dif = abs(efree - efree_h) / natom
-        snorm = scf_norm(dm, rho_out - rho, ecut)
+        snorm = scf_norm(dm, (vtot_new - vtot) if inner else (rho_out - rho), ecut)
         hist.append(dict(iter=it, etot=etot, efree=efree, eharris=efree_h, dif=dif, scf_norm=snorm))
         if verbose:
             print(f"iter {it:3d} Etot {etot:.10f} Efree {efree:.10f} Eharris {efree_h:.10f} dif {dif:.3e} "
                   f"scfnorm {snorm:.3e}")
         res = SCFResult(eig=eig, occ=occ, etot=etot, efree=efree, eharris=efree_h, exc=exc, ehart=ehart,
-                        eself=eself, history=hist, rho=rho_out, vtot=vtot, psi=psi, iterations=it)
+                        eself=eself, history=hist, rho=rho_out, vtot=vtot, psi=psi, iterations=len(hist))
         rho = rho_out
         if (tol_rho is None and dif < tol_efree) or (tol_rho is not None and snorm < tol_rho):
-            break
+            return True
         # Anderson mixing of the potential (scf.cpp:2299-2365)
         if mix == "broyden":
             vtot = broyden(dm, it, mix_step, vtot, vtot_new, bst, ecut)
         else:
             vtot = anderson(it, mix_step, mix_dim, vtot, vtot_new, dv_hist, df_hist)
+        return False
+
+    loop()
+    if not hybrid:
+        return res
+    # hybrid part (scf.cpp:628-925): semilocal HSE06 from the last density,
+    # phi <- psi, ACE, Fock energies
+    from . import exx as _exx
+    from . import hse as _hse
+    xcf = lambda r: _hse.xc_hse06(dm, r, ecut)  # noqa: E731
+    eps, vxc = xcf(rho)
+    exc = float(np.sum(eps * rho) * w)
+    vh = hartree(dm, rho, rho_ps, ecut, gkk)
+    vtot = vh + vxc
+    kern = _exx.exx_kernel_r2c(dm, ecut, mu=_hse.OMEGA_HSE06, div_type=1)[0]
+
+    def fock(p_, o_, xi_):
+        return _exx.exx_energy(-(p_ @ xi_.T) @ xi_, p_, o_, numSpin=2)
+
+    def ace(p_, o_):
+        return _exx.ace_build(dm, p_, _exx.set_phi(dm, p_), kern, _hse.FRAC_HSE06, o_)
+
+    xi = ace(psi, res.occ)
+    fock0 = fock(psi, res.occ, xi)
+    inner = True
+    conv = False
+    efock = dexx = 0.0
+    for phi_it in range(1, phi_max_iter + 1):
+        loop()
+        fock1 = fock(psi, res.occ, xi)
+        xi = ace(psi, res.occ)
+        fock2 = fock(psi, res.occ, xi)
+        dexx = 4.0 * abs(fock1 - 0.5 * (fock0 + fock2))
+        fock0 = fock2
+        efock = fock2
+        res.etot = res.etot - 2.0 * fock1 + efock
+        res.efree = res.efree - 2.0 * fock1 + efock
+        if verbose:
+            print(f"phi {phi_it} Efock {efock:.10f} Etot {res.etot:.10f} dExx {dexx:.3e}")
+        if dexx < phi_tol:
+            conv = True
+            break
+    res.efock, res.dexx, res.phi_iterations = efock, dexx, phi_it
+    res.converged = conv
     return res
 
 

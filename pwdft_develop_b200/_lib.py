@@ -36,7 +36,7 @@ _ip, _dp = C.POINTER(C.c_int), C.POINTER(C.c_double)
 
 PW_EXX_OFF, PW_EXX_FULL, PW_EXX_ACE = 0, 1, 2
 PW_SOLVER_LOBPCG, PW_SOLVER_CHEBFSI, PW_SOLVER_PPCG, PW_SOLVER_DAVIDSON = 0, 1, 2, 3
-PW_XC_TETER93, PW_XC_PBE = 0, 1
+PW_XC_TETER93, PW_XC_PBE, PW_XC_HSE06 = 0, 1, 2
 PW_MIX_ANDERSON, PW_MIX_BROYDEN = 0, 1
 
 
@@ -47,7 +47,8 @@ class ScfParams(C.Structure):
                 ("ecut", C.c_double), ("temperature", C.c_double), ("eig_tol", C.c_double),
                 ("mix_step", C.c_double), ("tol_efree", C.c_double), ("refine_threshold", C.c_double),
                 ("seed", C.c_ulonglong), ("ppcg_sbsize", C.c_int), ("davidson_maxdim", C.c_int),
-                ("graphs", C.c_int), ("xc", C.c_int), ("mix_type", C.c_int), ("tol_rho", C.c_double)]
+                ("graphs", C.c_int), ("xc", C.c_int), ("mix_type", C.c_int), ("tol_rho", C.c_double),
+                ("phi_max_iter", C.c_int), ("phi_tol", C.c_double)]
 
 
 class ScfResult(C.Structure):
@@ -55,7 +56,8 @@ class ScfResult(C.Structure):
                 ("ehart", C.c_double), ("eself", C.c_double), ("fermi", C.c_double), ("time_s", C.c_double),
                 ("iterations", C.c_int), ("converged", C.c_int), ("refine_iter", C.c_int),
                 ("hpsi_bands", C.c_long), ("phase_s", C.c_double * 6),
-                ("sub_s", C.c_double * 4), ("scf_norm", C.c_double)]
+                ("sub_s", C.c_double * 4), ("scf_norm", C.c_double), ("efock", C.c_double), ("dexx", C.c_double),
+                ("phi_iterations", C.c_int)]
 
 
 class TuneResult(C.Structure):

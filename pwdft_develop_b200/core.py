@@ -358,14 +358,19 @@ def _ctx_scf(self, nocc: int, nextra: int, ecut: float, solver: str = "chebfsi",
              eig_max_iter: int = 3, eig_tol: float = 1e-10, max_iter: int = 100, mix_dim: int = 8,
              mix_step: float = 0.7, tol_efree: float = 1e-6, refine_threshold: float = 1e-4, seed: int = 1,
              verbose: bool = False, ppcg_sbsize: int = 1, davidson_maxdim: int = 2, graphs: bool = False,
-             xc: str = "teter93", mix: str = "anderson", tol_rho: float = 0.0):
+             xc: str = "teter93", mix: str = "anderson", tol_rho: float = 0.0, phi_max_iter: int = 10,
+             phi_tol: float = 1e-6):
     """SCF::Iterate on the device (FP64 context; mixed=True runs the eigensolver in
-    an FP32 twin and refines in FP64).  Returns (result dict, eigenvalues, rho)."""
+    an FP32 twin and refines in FP64).  xc: "teter93", "pbe" or "hse06" (nested
+    hybrid scheme with ACE).  Returns (result dict, eigenvalues, rho)."""
+    xcs = {"teter93": _lib.PW_XC_TETER93, "pbe": _lib.PW_XC_PBE, "hse06": _lib.PW_XC_HSE06}
+    if xc not in xcs:
+        raise ValueError(f"unknown exchange-correlation functional {xc!r}")
     p = _lib.ScfParams(nocc=nocc, nextra=nextra,
                        solver=_SOLVERS[solver], ppcg_sbsize=ppcg_sbsize, davidson_maxdim=davidson_maxdim,
-                       graphs=int(graphs), xc=_lib.PW_XC_PBE if xc == "pbe" else _lib.PW_XC_TETER93,
+                       graphs=int(graphs), xc=xcs[xc],
                        mix_type=_lib.PW_MIX_BROYDEN if mix == "broyden" else _lib.PW_MIX_ANDERSON,
-                       tol_rho=float(tol_rho),
+                       tol_rho=float(tol_rho), phi_max_iter=int(phi_max_iter), phi_tol=float(phi_tol),
                        cheby_degree=cheby_degree, cheby_first_cycles=cheby_first_cycles, eig_max_iter=eig_max_iter,
                        max_iter=max_iter, mix_dim=mix_dim, mixed=int(mixed), verbose=int(verbose), ecut=ecut,
                        temperature=temperature, eig_tol=eig_tol, mix_step=mix_step, tol_efree=tol_efree,

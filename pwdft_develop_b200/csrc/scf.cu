@@ -1440,14 +1440,21 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
                   (rc = S.bdf.alloc((size_t)mixdim * nf * 16)) || (rc = S.bdv.alloc((size_t)mixdim * nf * 16)) ||
                   (rc = S.bcdf.alloc((size_t)2 * nf * 16))))
     return rc;
-  const bool pbe = p->xc == PW_XC_PBE;
+  // HSE06: the reference's nested hybrid scheme runs a PBE SCF first
+  // (Setup_XC("XC_GGA_XC_PBE"), scf.cpp:409-425) and switches to the
+  // semilocal HSE06 for the phi iterations (scf.cpp:628-640)
+  const bool hse = p->xc == PW_XC_HSE06;
+  const bool pbe = p->xc == PW_XC_PBE || hse;
   PWB_CHECK(p->xc == PW_XC_TETER93 || pbe, PW_EINVAL, "unknown exchange-correlation functional");
+  PWB_CHECK(!hse || !ctx->gs, PW_EUNSUPPORTED, "the hybrid SCF is built for real-space contexts");
   if (pbe && ((rc = S.work2.alloc(nf * 16)) || (rc = S.grad.alloc(3 * nf * 8)))) return rc;
+  if (hse) ctx->exx_mode = PW_EXX_OFF;
+  double hse_frac = 0.0;
   auto potentials = [&](const double* rh, double* exc_out) -> int {
     int q = PW_OK;
     if (pbe)
       q = xc_pbe(ctx, rh, p->ecut, (double*)S.eps.p, (double*)S.vxc.p, (double2*)S.work.p, (double2*)S.work2.p,
-                 (double*)S.grad.p, (const double2*)S.tw.p, nullptr);
+                 (double*)S.grad.p, (const double2*)S.tw.p, nullptr, hse_frac);
     else
       k_xc_teter93<<<nblk(nf), 256>>>(nf, rh, (double*)S.eps.p, (double*)S.vxc.p);
     if (q) return q;
@@ -1520,10 +1527,34 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
   int stall = 0;
   std::vector<double> occ, eig;
   double ef = 0, etot = 0, efree = 0, eharris = 0, ehart = 0;
-  int it = 0;
+  int it = 0, total_it = 0;
   bool conv = false;
   r->hpsi_bands = 0;
+  // switch the eigensolver from the FP32 twin to FP64 (iterative refinement)
+  auto refine_now = [&]() -> int {
+    PhaseTimer pt_(prof, &tph[5]);
+    DevBuf x32;
+    int q;
+    if ((q = x32.alloc((size_t)nb * nt * 4))) return q;
+    PWB_CUDA(cudaMemcpy(x32.p, sv.X.p, (size_t)nb * nt * 4, cudaMemcpyDeviceToDevice));
+    std::vector<double> keep_eig = sv.eig;
+    if ((q = bind(ctx))) return q;
+    if ((q = copy_f2d_2d((int)nt, nb, (const float*)x32.p, nt, (double*)sv.X.p, nt, nullptr))) return q;
+    if ((q = cholqr(sv, dn, sv.X.p, nb, sv.Y.p))) return q;
+    sv.eig = keep_eig;
+    refined = true;
+    r->refine_iter = total_it;
+    return PW_OK;
+  };
+  bool hybrid_phase = false;   // inner loop of a phi iteration
+  // one SCF loop (SCF::Iterate's iteration, scf.cpp:430-620); the mixing
+  // history restarts with it, as the reference's loop index does
+  auto scf_loop = [&]() -> int {
+  conv = false;
+  S.nhist = 0;
+  S.hpos = 0;
   for (it = 1; it <= p->max_iter; ++it) {
+    ++total_it;
     if ((rc = set_vtot_dev(sv.c, (const double*)S.vtot.p))) return rc;
     {
     PhaseTimer pt_(prof, &tph[0]);
@@ -1610,11 +1641,16 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
     etot = ekin + (-ed[0] * w) + exc + ehart - eself;
     efree = etot + ent;
     const double dif = std::fabs(efree - eharris) / natom;
-    // SCF::CalculateError of the change of the output density (scf.cpp:1492-1496, 2368-2396)
+    // SCF::CalculateError of the change of the output density (scf.cpp:1492-1496,
+    // 2368-2396); of the potential change vtotNew - vtot in the phi
+    // iterations' inner loop (scf.cpp:728-739)
     double snorm = 0.0;
     {
       double* drv = (double*)S.dr.p;
-      k_lincomb<<<nblk(nf), 256>>>(nf, 1.0, ro, -1.0, rho, drv);
+      if (hybrid_phase)
+        k_lincomb<<<nblk(nf), 256>>>(nf, 1.0, (const double*)S.vtot_new.p, -1.0, (const double*)S.vtot.p, drv);
+      else
+        k_lincomb<<<nblk(nf), 256>>>(nf, 1.0, ro, -1.0, rho, drv);
       if ((rc = fft3_real(ctx->nf[0], false, (double2*)S.work.p, drv, nullptr, 1.0, (const double2*)S.tw.p,
                           nullptr)))
         return rc;
@@ -1644,17 +1680,7 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
       }
     }
     if (!refined && (dif < p->refine_threshold || (stall >= 4 && dif < 100.0 * p->refine_threshold))) {
-      PhaseTimer pt_(prof, &tph[5]);
-      DevBuf x32;
-      if ((rc = x32.alloc((size_t)nb * nt * 4))) return rc;
-      PWB_CUDA(cudaMemcpy(x32.p, sv.X.p, (size_t)nb * nt * 4, cudaMemcpyDeviceToDevice));
-      std::vector<double> keep_eig = sv.eig;
-      if ((rc = bind(ctx))) return rc;
-      if ((rc = copy_f2d_2d((int)nt, nb, (const float*)x32.p, nt, (double*)sv.X.p, nt, nullptr))) return rc;
-      if ((rc = cholqr(sv, dn, sv.X.p, nb, sv.Y.p))) return rc;
-      sv.eig = keep_eig;
-      refined = true;
-      r->refine_iter = it;
+      if ((rc = refine_now())) return rc;
     }
     if (broyden) {
       // Broyden mixing of the potential (SCF::BroydenMix, scf.cpp:2144-2261):
@@ -1799,6 +1825,58 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
       PWB_CUDA(cudaGetLastError());
     }
   }
+  return PW_OK;
+  };
+  if ((rc = scf_loop())) return rc;
+  double efock = 0.0, dexx = 0.0;
+  int phi_it = 0;
+  if (hse) {
+    // SCF::Iterate hybrid part, "nested" mixing (scf.cpp:628-925)
+    if (!refined && (rc = refine_now())) return rc;
+    // the graph-captured filter holds H*psi without the exchange term
+    if (sv.fexec) cudaGraphExecDestroy(sv.fexec);
+    if (sv.fgraph) cudaGraphDestroy(sv.fgraph);
+    sv.fexec = nullptr;
+    sv.fgraph = nullptr;
+    sv.use_graph = false;
+    hse_frac = 0.25;
+    if ((rc = potentials(rho, &exc))) return rc;
+    k_lincomb<<<nblk(nf), 256>>>(nf, 1.0, (double*)S.vh.p, 1.0, (double*)S.vxc.p, (double*)S.vtot.p);
+    if ((rc = pw_exx_setup(ctx, 0.25, 0.106, 1, p->ecut))) return rc;
+    // phi <- psi, ACE (SetPhiEXX + CalculateVexxACE) and the Fock energy with it
+    auto update_ace = [&]() -> int {
+      int q;
+      if ((q = pw_exx_set_phi(ctx, sv.X.p, (int)nt, nb, occ.data()))) return q;
+      return pw_ace_build(ctx, sv.X.p, (int)nt, nb);
+    };
+    auto fock = [&](double* e) -> int { return pw_exx_energy(ctx, sv.X.p, (int)nt, nb, occ.data(), 2, 1, e); };
+    double fock0 = 0.0, fock1 = 0.0, fock2 = 0.0;
+    if ((rc = update_ace()) || (rc = fock(&fock0))) return rc;
+    hybrid_phase = true;
+    const int phimax = p->phi_max_iter > 0 ? p->phi_max_iter : 10;
+    bool phi_conv = false;
+    for (phi_it = 1; phi_it <= phimax; ++phi_it) {
+      if ((rc = scf_loop())) return rc;
+      if ((rc = fock(&fock1)) || (rc = update_ace()) || (rc = fock(&fock2))) return rc;
+      dexx = 4.0 * std::fabs(fock1 - 0.5 * (fock0 + fock2));
+      fock0 = fock2;
+      efock = fock2;
+      etot = etot - 2.0 * fock1 + efock;
+      efree = efree - 2.0 * fock1 + efock;
+      if (p->verbose)
+        fprintf(stderr, "phi %3d inner %3d Efock %.10f Etot %.10f Efree %.10f dExx %.3e\n", phi_it, it, efock, etot,
+                efree, dexx);
+      if (dexx < p->phi_tol) {
+        phi_conv = true;
+        break;
+      }
+    }
+    phi_it = std::min(phi_it, phimax);
+    conv = phi_conv;
+  }
+  r->efock = efock;
+  r->dexx = dexx;
+  r->phi_iterations = phi_it;
   PWB_CUDA(cudaDeviceSynchronize());
   const auto t_end = std::chrono::steady_clock::now();
   r->etot = etot;
@@ -1808,7 +1886,7 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
   r->ehart = ehart;
   r->eself = eself;
   r->fermi = ef;
-  r->iterations = std::min(it, p->max_iter);
+  r->iterations = total_it;
   r->converged = conv ? 1 : 0;
   r->time_s = std::chrono::duration<double>(t_end - t_start).count();
   for (int i = 0; i < 6; ++i) r->phase_s[i] = tph[i];

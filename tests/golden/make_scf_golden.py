@@ -5,9 +5,10 @@ Si8 diamond (a = 10.26 bohr, seeded +-0.02 bohr displacements, seed
 (dim 8, step 0.7), converged to |E_free - E_Harris| / N_atom < 1e-9.
 Cases: 16^3 / 32^3 grids with Ecut 5 Ha, and the 24^3 / 48^3 grids with
 Ecut 10 Ha (LDA Teter93); ``pbe``: the small case with PBE (the reference's
-internal PBE path); ``broyden``: the small case with Broyden potential mixing.
-Run from the repository root:
-``python tests/golden/make_scf_golden.py [small|full|pbe|broyden]``.
+internal PBE path); ``broyden``: the small case with Broyden potential mixing;
+``hse06``: the small case with the nested HSE06 hybrid scheme (PBE SCF, then
+phi iterations with ACE until dExx < 1e-8).  Run from the repository root:
+``python tests/golden/make_scf_golden.py [small|full|pbe|broyden|hse06]``.
 """
 import json
 import sys
@@ -21,7 +22,8 @@ sys.path.insert(0, str(ROOT))
 from oracle import pw, scf  # noqa: E402
 
 CASES = {"small": ((16, 16, 16), (32, 32, 32), 5.0, "teter93"), "full": ((24, 24, 24), (48, 48, 48), 10.0, "teter93"),
-         "pbe": ((16, 16, 16), (32, 32, 32), 5.0, "pbe"), "broyden": ((16, 16, 16), (32, 32, 32), 5.0, "teter93")}
+         "pbe": ((16, 16, 16), (32, 32, 32), 5.0, "pbe"), "broyden": ((16, 16, 16), (32, 32, 32), 5.0, "teter93"),
+         "hse06": ((16, 16, 16), (32, 32, 32), 5.0, "hse06")}
 
 
 def main(which):
@@ -33,13 +35,16 @@ def main(which):
     # |E_free - E_Harris| has a floor; it converges on the density change (scfNorm)
     tol_rho = 1e-13 if mix == "broyden" else None
     r = scf.scf(L, z, pos, nc, nf, nocc=16, nextra=8, ecut=ecut, tol_efree=1e-9, verbose=True, xc=xc, mix=mix,
-                max_iter=80, tol_rho=tol_rho)
+                max_iter=80, tol_rho=tol_rho, phi_max_iter=20, phi_tol=1e-8)
     out = dict(case=which, numGrid=nc, numGridFine=nf, ecut=ecut, xc=xc, mix=mix, nocc=16, nextra=8,
                temperature=300.0,
                length=list(map(float, L)), positions=pos.tolist(), znuc=int(z),
                tol_rho=tol_rho, scf_norm=r.history[-1]["scf_norm"],
                etot=r.etot, efree=r.efree, eharris=r.eharris, exc=r.exc, ehart=r.ehart, eself=r.eself,
                eig=r.eig.tolist(), occ=r.occ.tolist(), iterations=r.iterations, seconds=time.time() - t0)
+    if xc == "hse06":
+        out.update(efock=r.efock, dexx=r.dexx, phi_iterations=r.phi_iterations, phi_tol=1e-8,
+                   converged=bool(r.converged))
     path = Path(__file__).resolve().parent / f"si8_scf_{which}.json"
     path.write_text(json.dumps(out, indent=1))
     print(path, r.efree, r.iterations)

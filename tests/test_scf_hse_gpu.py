@@ -1,0 +1,33 @@
+"""Hybrid (HSE06) SCF on the device against the FP64 oracle's nested hybrid
+run (tests/golden/si8_scf_hse06.json, oracle/scf.py with oracle/hse.py and
+oracle/exx.py): PBE SCF, semilocal HSE06, phi iterations with the ACE
+operator until dExx < phi_tol.  Tolerances: E_free and the Fock energy
+1e-6 Ha/atom, eigenvalues 1e-6 Ha (the SCF tolerance of the other SCF
+parity tests); the device's dExx below its own phi_tol."""
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+GOLD = Path(__file__).resolve().parent / "golden"
+
+
+@pytest.mark.parametrize("solver,mixed", [("chebfsi", False), ("lobpcg", True)])
+def test_scf_hse06_matches_oracle(solver, mixed):
+    from pwdft_develop_b200 import Context
+    g = json.loads((GOLD / "si8_scf_hse06.json").read_text())
+    L = np.array(g["length"])
+    pos = np.array(g["positions"])
+    c = Context(L, tuple(g["numGrid"]), tuple(g["numGridFine"]))
+    c.set_atoms([g["znuc"]] * len(pos), pos)
+    res, eig, rho = c.scf(nocc=16, nextra=8, ecut=g["ecut"], solver=solver, mixed=mixed, tol_efree=1e-9,
+                          eig_max_iter=4, eig_tol=1e-10, max_iter=80, xc="hse06", phi_max_iter=20, phi_tol=1e-8)
+    assert res["converged"] == 1, res
+    assert res["dexx"] < 1e-8 and res["phi_iterations"] >= 1
+    nat = len(pos)
+    assert abs(res["efree"] - g["efree"]) / nat < 1e-6, (res["efree"], g["efree"])
+    assert abs(res["efock"] - g["efock"]) / nat < 1e-6, (res["efock"], g["efock"])
+    assert np.abs(eig[:16] - np.array(g["eig"][:16])).max() < 1e-6
+    assert abs(rho.sum() * np.prod(L) / rho.size - 32.0) < 1e-8

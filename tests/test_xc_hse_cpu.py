@@ -130,3 +130,21 @@ def test_potential_is_the_functional_derivative():
     fd = (exc(rho + h * dlt) - exc(rho - h * dlt)) / (2 * h)
     an = float(np.sum(v * dlt) * w)
     assert abs(fd - an) <= 1e-6 * abs(an), (fd, an)
+
+
+def test_ace_reproduces_the_screened_exchange_on_its_bands():
+    """The hybrid loop's Fock energies use the ACE operator: built from psi,
+    -xi xi^T equals V_x on span(psi), so the ACE Fock energy of those bands is
+    the full-operator one (HSE06 kernel, mu = 0.106) to 1e-12."""
+    from oracle import exx
+    L, z, pos = pw.make_crystal("Si", (1, 1, 1), 10.26, 0.02, 20261203 + 1)
+    dm = pw.Domain(tuple(L), (12, 12, 12), (24, 24, 24))
+    psi = pw.random_orthonormal_psi(dm.ntot, 10, 3)
+    occ = np.linspace(1.0, 0.0, 10)
+    kern = exx.exx_kernel_r2c(dm, 5.0, mu=hse.OMEGA_HSE06, div_type=1)[0]
+    phi = exx.set_phi(dm, psi)
+    vx = exx.add_mult_spinor_exx(dm, psi, phi, kern, hse.FRAC_HSE06, occ)
+    xi = exx.ace_build(dm, psi, phi, kern, hse.FRAC_HSE06, occ)
+    e_full = exx.exx_energy(vx, psi, occ)
+    e_ace = exx.exx_energy(-(psi @ xi.T) @ xi, psi, occ)
+    assert e_full < 0 and abs(e_ace - e_full) <= 1e-12 * abs(e_full)
