@@ -52,3 +52,179 @@ def gram_row_partitioned(X_rows, Y_rows):
     bands): local product then a sum over ranks."""
     G = X_rows.transpose(0, 1) @ Y_rows
     return allreduce_sum_(G)
+
+
+# ---------------------------------------------------------------------------
+# Distributed eigensolver blocks.  Bands are sharded (band_range) for H*psi,
+# which needs no exchange; the subspace steps need sums over the grid, so the
+# block is transposed to grid rows (all bands of this rank's rows) with one
+# all-to-all, reduced with an all-reduce of the n x n FP64 Gram, and
+# transposed back -- the reference's AlltoallForward / AlltoallBackward
+# (src/utility.cpp:1159-1197) around the local GEMM and MPI_Allreduce of
+# EigenSolver (src/EigenSolver/lobpcg.cpp:683-687, eigensolver.cpp:301-384).
+# With one rank (no process group) every collective is the identity.
+# ---------------------------------------------------------------------------
+
+def _world():
+    import torch.distributed as dist
+    if dist.is_available() and dist.is_initialized():
+        return dist.get_world_size(), dist.get_rank()
+    return 1, 0
+
+
+def band_to_rows(Xb, nband: int):
+    """(this rank's bands x all grid points) -> (all bands x this rank's grid rows)."""
+    import torch
+    import torch.distributed as dist
+    world, rank = _world()
+    if world == 1:
+        return Xb
+    ntot = Xb.shape[1]
+    bands = [band_range(nband, world, r) for r in range(world)]
+    rows = [grid_range(ntot, world, r) for r in range(world)]
+    assert Xb.shape[0] == bands[rank][1]
+    send = torch.cat([Xb[:, s:s + n].reshape(-1) for s, n in rows])
+    nr = rows[rank][1]
+    recv = torch.empty(nband * nr, dtype=Xb.dtype, device=Xb.device)
+    dist.all_to_all_single(recv, send, output_split_sizes=[b[1] * nr for b in bands],
+                           input_split_sizes=[Xb.shape[0] * n for _, n in rows])
+    return recv.view(nband, nr)
+
+
+def rows_to_band(Xr, ntot: int):
+    """Inverse of band_to_rows: (all bands x this rank's rows) -> (this rank's bands x all points)."""
+    import torch
+    import torch.distributed as dist
+    world, rank = _world()
+    if world == 1:
+        return Xr
+    nband = Xr.shape[0]
+    bands = [band_range(nband, world, r) for r in range(world)]
+    rows = [grid_range(ntot, world, r) for r in range(world)]
+    nr = rows[rank][1]
+    assert Xr.shape[1] == nr
+    send = torch.cat([Xr[s:s + n].reshape(-1) for s, n in bands])
+    nbm = bands[rank][1]
+    recv = torch.empty(nbm * ntot, dtype=Xr.dtype, device=Xr.device)
+    dist.all_to_all_single(recv, send, output_split_sizes=[nbm * n for _, n in rows],
+                           input_split_sizes=[n * nr for _, n in bands])
+    parts, off = [], 0
+    for _, n in rows:
+        parts.append(recv[off:off + nbm * n].view(nbm, n))
+        off += nbm * n
+    return torch.cat(parts, 1)
+
+
+def _bcast_(t):
+    import torch.distributed as dist
+    if _world()[0] > 1:
+        dist.broadcast(t, 0)
+    return t
+
+
+def cholqr_rows(Xr):
+    """Cholesky-QR of a row-partitioned block (EigenSolver::Orthogonalize,
+    src/EigenSolver/eigensolver.cpp:301-384): S = sum_ranks Xr Xr^T, S = U^T U,
+    X <- X U^-1 (rows: Xr <- U^-T Xr)."""
+    import torch
+    S = allreduce_sum_(Xr @ Xr.transpose(0, 1))
+    U = _bcast_(torch.linalg.cholesky(0.5 * (S + S.transpose(0, 1)), upper=True))
+    return torch.linalg.solve_triangular(U.transpose(0, 1), Xr, upper=False)
+
+
+def rayleigh_ritz_rows(Xr, HXr):
+    """Rayleigh-Ritz on row-partitioned X and HX: A = sum_ranks Xr HXr^T,
+    A = C diag(l) C^T (solved on rank 0 and broadcast, as the reference's
+    rank-0 Syevd), X <- X C, HX <- HX C.  Returns (l, Xr, HXr)."""
+    import torch
+    A = allreduce_sum_(Xr @ HXr.transpose(0, 1))
+    lam, C = torch.linalg.eigh(0.5 * (A + A.transpose(0, 1)))
+    lam, C = _bcast_(lam.contiguous()), _bcast_(C.contiguous())
+    Ct = C.transpose(0, 1)
+    return lam, Ct @ Xr, Ct @ HXr
+
+
+def chebyshev_filter(apply_h, X, degree: int, a: float, b: float, a0: float):
+    """Scaled Chebyshev filter p_m(H) X damping [a, b] (Zhou, Saad, Tiago,
+    Chelikowsky, J. Comput. Phys. 219, 172 (2006)); X: this rank's bands."""
+    e = (b - a) / 2.0
+    c = (b + a) / 2.0
+    sigma = e / (a0 - c)
+    sigma1 = sigma
+    gamma = 2.0 / sigma1
+    Y = (apply_h(X) - c * X) * (sigma1 / e)
+    for _ in range(2, degree + 1):
+        sigma2 = 1.0 / (gamma - sigma)
+        Z = (apply_h(Y) - c * Y) * (2.0 * sigma2 / e) - (sigma * sigma2) * X
+        X, Y = Y, Z
+        sigma = sigma2
+    return Y
+
+
+def lanczos_upper_bound(apply_h, x0, steps: int = 16) -> float:
+    """Upper bound of the spectrum from a k-step Lanczos run on one vector
+    (rank 0's first band; the bound is broadcast): largest Ritz value plus
+    the last off-diagonal magnitude."""
+    import torch
+    world, rank = _world()
+    out = torch.zeros(1, dtype=torch.float64, device=x0.device)
+    if rank == 0:
+        v = x0[:1] / torch.linalg.norm(x0[:1])
+        vprev = torch.zeros_like(v)
+        al, be = [], [0.0]
+        for k in range(steps):
+            w = apply_h(v)
+            a_ = float((w * v).sum())
+            w = w - a_ * v - be[-1] * vprev
+            b_ = float(torch.linalg.norm(w))
+            al.append(a_)
+            be.append(b_)
+            if b_ == 0.0:
+                break
+            vprev, v = v, w / b_
+        n = len(al)
+        T = torch.zeros(n, n, dtype=torch.float64)
+        for i in range(n):
+            T[i, i] = al[i]
+            if i + 1 < n:
+                T[i, i + 1] = T[i + 1, i] = be[i + 1]
+        out[0] = float(torch.linalg.eigvalsh(T)[-1]) + abs(be[-1])
+    return float(_bcast_(out)[0])
+
+
+def chebfsi_dist(apply_h, Xb, nband: int, degree: int = 10, max_iter: int = 100, tol: float = 1e-9,
+                 nconv: int | None = None):
+    """Distributed ChebFSI: Chebyshev-filtered subspace iteration over band
+    shards (filter and H*psi local to each rank; Cholesky-QR and Rayleigh-Ritz
+    on grid rows after an all-to-all transpose).  Xb: this rank's bands
+    (band_range(nband, world, rank)) x all grid points, FP64; apply_h maps a
+    block of this rank's bands to H times it (pw_hpsi on the rank's GPU).
+    Returns (eigenvalues, Xb, iterations, max residual) with residuals
+    ||H x - l x|| / max(1, |l|) of the lowest nconv (default all) pairs,
+    gathered over ranks."""
+    import torch
+    world, rank = _world()
+    ntot = Xb.shape[1]
+    b_up = lanczos_upper_bound(apply_h, Xb)
+    s, n = band_range(nband, world, rank)
+    # first pass: orthonormalise and Rayleigh-Ritz the start block
+    Xr = cholqr_rows(band_to_rows(Xb, nband))
+    Xb = rows_to_band(Xr, ntot)
+    lam, Xr, HXr = rayleigh_ritz_rows(Xr, band_to_rows(apply_h(Xb), nband))
+    Xb = rows_to_band(Xr, ntot)
+    res_max = float("inf")
+    it = 0
+    for it in range(1, max_iter + 1):
+        Y = chebyshev_filter(apply_h, Xb, degree, float(lam[-1]), b_up, float(lam[0]))
+        Yr = cholqr_rows(band_to_rows(Y, nband))
+        Yb = rows_to_band(Yr, ntot)
+        lam, Xr, HXr = rayleigh_ritz_rows(Yr, band_to_rows(apply_h(Yb), nband))
+        Xb = rows_to_band(Xr, ntot)
+        HXb = rows_to_band(HXr, ntot)
+        loc = torch.linalg.norm(HXb - lam[s:s + n, None] * Xb, dim=1) / torch.clamp(lam[s:s + n].abs(), min=1.0)
+        res = torch.zeros(nband, dtype=torch.float64, device=Xb.device)
+        res[s:s + n] = loc
+        res_max = float(allreduce_sum_(res)[:nconv or nband].max())
+        if res_max < tol:
+            break
+    return lam, Xb, it, res_max

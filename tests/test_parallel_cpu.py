@@ -66,3 +66,64 @@ def test_gloo_two_ranks_gram_and_max():
         assert p.exitcode == 0
     assert np.abs(G - ref).max() <= 1e-12 * np.abs(ref).max()
     assert t == 2.0
+
+
+def _eig_worker(rank, world, port, q):
+    import torch
+    import torch.distributed as dist
+    from oracle import pw
+    from pwdft_develop_b200.parallel import band_range, band_to_rows, chebfsi_dist, rows_to_band
+    if world > 1:
+        os.environ["MASTER_ADDR"] = "127.0.0.1"
+        os.environ["MASTER_PORT"] = str(port)
+        dist.init_process_group("gloo", rank=rank, world_size=world)
+    T, _ = pw.build_tables(*_si8(), (12, 12, 12), (24, 24, 24), seed_v=4)
+    nband = 20
+    X0 = torch.tensor(pw.random_orthonormal_psi(T.dm.ntot, nband, 7))
+    s, n = band_range(nband, world, rank)
+    # the transposes are inverse to each other and lay out all bands of a row block
+    Xr = band_to_rows(X0[s:s + n].clone(), nband)
+    assert torch.equal(rows_to_band(Xr, T.dm.ntot), X0[s:s + n])
+
+    def apply_h(X):
+        return torch.from_numpy(pw.mult_spinor(T, X.numpy()))
+
+    lam, Xb, it, res = chebfsi_dist(apply_h, X0[s:s + n].clone(), nband, degree=10, max_iter=200, tol=1e-9,
+                                    nconv=14)
+    if rank == 0:
+        q.put((lam.numpy(), it, res))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def _si8():
+    from oracle import pw
+    L, z, pos = pw.make_crystal("Si", (1, 1, 1), 10.26, 0.02, 20261203 + 1)
+    return L, z, pos
+
+
+def test_distributed_chebfsi_two_ranks_matches_one_rank_and_arpack():
+    """ChebFSI over two gloo ranks (band shards, all-to-all transposes,
+    all-reduced Gram and Rayleigh-Ritz) reaches the same lowest eigenvalues as
+    one rank and as ARPACK on the oracle operator (1e-9 Ha)."""
+    import torch.multiprocessing as mp
+    from oracle import pw, scf
+    ctx = mp.get_context("spawn")
+    out = {}
+    for world in (1, 2):
+        q = ctx.Queue()
+        port = _free_port()
+        procs = [ctx.Process(target=_eig_worker, args=(r, world, port, q)) for r in range(world)]
+        for p in procs:
+            p.start()
+        out[world] = q.get(timeout=600)
+        for p in procs:
+            p.join(timeout=120)
+            assert p.exitcode == 0
+    T, _ = pw.build_tables(*_si8(), (12, 12, 12), (24, 24, 24), seed_v=4)
+    ref, _ = scf._eigsh(T, 20, tol=1e-12)
+    for world in (1, 2):
+        lam, it, res = out[world]
+        assert res < 1e-9, (world, it, res)
+        assert np.abs(lam[:14] - ref[:14]).max() < 1e-9, (world, lam[:14] - ref[:14])
