@@ -104,9 +104,13 @@ PW_API int pw_hpsi(pw_ctx* ctx, const void* psi, int ld, void* hpsi, int ldh, in
             int accumulate, void* stream);
 
 /* Same as pw_hpsi with host buffers: copies psi in and hpsi out around the
- * device computation (the path a host-side reference caller binds). */
+ * device computation (the path a host-side reference caller binds).  With
+ * page-locked host buffers the bands move in chunks whose copies in and out
+ * overlap the H*psi of the neighbouring chunks; returns when hpsi is written. */
 PW_API int pw_hpsi_host(pw_ctx* ctx, const void* psi, int ld, void* hpsi, int ldh, int nband,
                  int accumulate);
+/* Bands per pw_hpsi_host chunk (rounded up to even; 0: the default 32). */
+PW_API int pw_set_host_chunk(pw_ctx* ctx, int nband);
 
 /* Teter preconditioner: w (+)= C2R(teter * R2C(r)).  Replaces
  * Spinor::AddTeterPrecond(Fourier*, DblNumVec& teter, NumTns<Real>& a3)

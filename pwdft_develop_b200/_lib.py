@@ -76,6 +76,7 @@ SIGNATURES: dict[str, tuple] = {
     "pw_set_nonlocal": (_i, [_vp, _i, _ip, _ip, _ip, _dp, _dp]),
     "pw_hpsi": (_i, [_vp, _vp, _i, _vp, _i, _i, _i, _vp]),
     "pw_hpsi_host": (_i, [_vp, _vp, _i, _vp, _i, _i, _i]),
+    "pw_set_host_chunk": (_i, [_vp, C.c_int]),
     "pw_teter_precond": (_i, [_vp, _vp, _i, _vp, _i, _i, _i, _vp]),
     "pw_teter_precond_noalloc": (_i, [_vp, _vp, _i, _vp, _i, _i, _i, _vp]),
     "pw_set_band_batch": (_i, [_vp, _i]),

@@ -176,6 +176,8 @@ struct pw_ctx {
   int pair_cap = 0;
   pwb::DevBuf s_ad, s_k, s_bc, s_wp, s_w;
   pwb::DevBuf s_host_in, s_host_out;   // device staging for the host-pointer entry points
+  cudaStream_t io_st[3] = {nullptr, nullptr, nullptr};   // host->device, compute, device->host (pw_hpsi_host)
+  int host_chunk = 32;                                    // bands per pw_hpsi_host chunk
 };
 
 namespace pwb {

@@ -194,6 +194,8 @@ int pw_ctx_destroy(pw_ctx* ctx) {
   for (auto& r : ctx->prof) { cudaEventDestroy(r.a); cudaEventDestroy(r.b); }
   for (auto e : ctx->ev_pool) cudaEventDestroy(e);
   if (ctx->blas) cublasDestroy((cublasHandle_t)ctx->blas);
+  for (cudaStream_t st : ctx->io_st)
+    if (st) cudaStreamDestroy(st);
   if (ctx->twin) pw_ctx_destroy(ctx->twin);
   delete ctx;
   return PW_OK;
@@ -485,23 +487,112 @@ int pw_teter_precond(pw_ctx* ctx, const void* r, int ld, void* w, int ldw, int n
   return PW_OK;
 }
 
+int pw_set_host_chunk(pw_ctx* ctx, int nband) {
+  PWB_CHECK(ctx && nband >= 0, PW_EINVAL, "bad arguments");
+  ctx->host_chunk = nband == 0 ? 32 : std::max(2, nband + (nband & 1));
+  return PW_OK;
+}
+
+static bool host_pinned(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+// Host-buffer H*psi.  With page-locked host buffers the bands move in chunks:
+// every chunk's host->device copy is queued on one stream, its H*psi on a
+// second (after that copy) and its device->host copy on a third (after that
+// H*psi), so the link carries chunk i+1 in and chunk i-1 out while chunk i
+// computes (chunk: pw_set_host_chunk, 32 bands by default; the first and the
+// last chunk are half as long, to shorten the fill and drain).  Pageable
+// buffers, and blocks of at most 1.5 chunks, take one synchronous copy each way.
 int pw_hpsi_host(pw_ctx* ctx, const void* psi, int ld, void* hpsi, int ldh, int nband, int accumulate) {
   PWB_CHECK(ctx && (nband == 0 || (psi && hpsi)), PW_EINVAL, "null argument");
   if (nband == 0) return PW_OK;
   PWB_CHECK(nband >= 0 && ld >= ctx->ntot && ldh >= ctx->ntot, PW_EINVAL, "Domain size does not match.");
   PWB_CUDA(cudaSetDevice(ctx->device));
-  const size_t bytes = (size_t)ctx->ntot * nband * ctx->esz;
+  const size_t esz = ctx->esz, row = (size_t)ctx->ntot * esz;
+  const size_t bytes = row * nband;
   int rc;
   if ((rc = ctx->s_host_in.alloc(bytes)) || (rc = ctx->s_host_out.alloc(bytes))) return rc;
-  PWB_CUDA(cudaMemcpy2D(ctx->s_host_in.p, ctx->ntot * ctx->esz, psi, (size_t)ld * ctx->esz, ctx->ntot * ctx->esz,
-                        nband, cudaMemcpyHostToDevice));
-  if (accumulate)
-    PWB_CUDA(cudaMemcpy2D(ctx->s_host_out.p, ctx->ntot * ctx->esz, hpsi, (size_t)ldh * ctx->esz,
-                          ctx->ntot * ctx->esz, nband, cudaMemcpyHostToDevice));
-  rc = pw_hpsi(ctx, ctx->s_host_in.p, (int)ctx->ntot, ctx->s_host_out.p, (int)ctx->ntot, nband, accumulate, nullptr);
+  char* din = (char*)ctx->s_host_in.p;
+  char* dout = (char*)ctx->s_host_out.p;
+  const int chunk = ctx->host_chunk;
+  if (nband <= chunk + chunk / 2 || !host_pinned(psi) || !host_pinned(hpsi)) {
+    PWB_CUDA(cudaMemcpy2D(din, row, psi, (size_t)ld * esz, row, nband, cudaMemcpyHostToDevice));
+    if (accumulate)
+      PWB_CUDA(cudaMemcpy2D(dout, row, hpsi, (size_t)ldh * esz, row, nband, cudaMemcpyHostToDevice));
+    rc = pw_hpsi(ctx, din, (int)ctx->ntot, dout, (int)ctx->ntot, nband, accumulate, nullptr);
+    if (rc) return rc;
+    PWB_CUDA(cudaMemcpy2D(hpsi, (size_t)ldh * esz, dout, row, row, nband, cudaMemcpyDeviceToHost));
+    return PW_OK;
+  }
+  for (cudaStream_t& st : ctx->io_st)
+    if (!st) PWB_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  cudaStream_t sh = ctx->io_st[0], sc = ctx->io_st[1], sd = ctx->io_st[2];
+  // chunk sizes: half a chunk first and last (the pipeline's fill and drain)
+  std::vector<int> start;
+  {
+    const int h = std::max(2, (chunk / 2) & ~1);
+    int b = 0;
+    start.push_back(0);
+    b += h;
+    while (nband - b > chunk + h) {
+      start.push_back(b);
+      b += chunk;
+    }
+    const int r = nband - b;   // at most chunk + h: one chunk, or an even one and a short last one
+    start.push_back(b);
+    if (r > chunk && ((r - h) & ~1) > 0) start.push_back(b + ((r - h) & ~1));
+    start.push_back(nband);
+  }
+  const int nch = (int)start.size() - 1;
+  std::vector<cudaEvent_t> ev((size_t)2 * nch + 1, nullptr);
+  for (auto& e : ev) PWB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  auto done = [&]() {
+    for (auto e : ev)
+      if (e) cudaEventDestroy(e);
+  };
+  // after the work already queued on the legacy default stream
+  cudaEvent_t e0 = ev[2 * nch];
+  cudaEventRecord(e0, 0);
+  cudaStreamWaitEvent(sh, e0, 0);
+  cudaStreamWaitEvent(sc, e0, 0);
+  cudaStreamWaitEvent(sd, e0, 0);
+  for (int i = 0; i < nch; ++i) {
+    const int b0 = start[i], nb = start[i + 1] - b0;
+    const char* hin = (const char*)psi + (size_t)b0 * ld * esz;
+    cudaError_t e1 = cudaMemcpy2DAsync(din + b0 * row, row, hin, (size_t)ld * esz, row, nb, cudaMemcpyHostToDevice, sh);
+    if (e1 == cudaSuccess && accumulate)
+      e1 = cudaMemcpy2DAsync(dout + b0 * row, row, (const char*)hpsi + (size_t)b0 * ldh * esz, (size_t)ldh * esz,
+                             row, nb, cudaMemcpyHostToDevice, sh);
+    if (e1 == cudaSuccess) e1 = cudaEventRecord(ev[2 * i], sh);
+    if (e1 != cudaSuccess) {
+      cudaStreamSynchronize(sh);
+      done();
+      PWB_CUDA(e1);
+    }
+  }
+  for (int i = 0; i < nch && rc == PW_OK; ++i) {
+    const int b0 = start[i], nb = start[i + 1] - b0;
+    cudaStreamWaitEvent(sc, ev[2 * i], 0);
+    rc = pw_hpsi(ctx, din + b0 * row, (int)ctx->ntot, dout + b0 * row, (int)ctx->ntot, nb, accumulate, sc);
+    if (rc) break;
+    cudaEventRecord(ev[2 * i + 1], sc);
+    cudaStreamWaitEvent(sd, ev[2 * i + 1], 0);
+    cudaMemcpy2DAsync((char*)hpsi + (size_t)b0 * ldh * esz, (size_t)ldh * esz, dout + b0 * row, row, row, nb,
+                      cudaMemcpyDeviceToHost, sd);
+  }
+  const cudaError_t s1 = cudaStreamSynchronize(sh), s2 = cudaStreamSynchronize(sc), s3 = cudaStreamSynchronize(sd);
+  done();
   if (rc) return rc;
-  PWB_CUDA(cudaMemcpy2D(hpsi, (size_t)ldh * ctx->esz, ctx->s_host_out.p, ctx->ntot * ctx->esz, ctx->ntot * ctx->esz,
-                        nband, cudaMemcpyDeviceToHost));
+  PWB_CUDA(s1);
+  PWB_CUDA(s2);
+  PWB_CUDA(s3);
+  PWB_CUDA(cudaGetLastError());
   return PW_OK;
 }
 

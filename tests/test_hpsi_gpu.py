@@ -118,6 +118,33 @@ def test_hpsi_host_entry_matches_device(si8):
     assert _rel(host, dev) <= 1e-14
 
 
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_hpsi_host_pinned_chunks_match_device(si8, prec):
+    """Page-locked host buffers take the chunked path (copies in and out on
+    their own streams around each chunk's H*psi): 101 bands (chunks of 32 and a
+    ragged, odd last one), leading dimension > ntot, overwrite and accumulate
+    agree with the device entry to rounding; padding columns stay untouched."""
+    import ctypes as C
+    import torch
+    from pwdft_develop_b200._lib import check, lib
+    T = si8
+    nb, nt = 101, T.dm.ntot
+    ld = nt + 8
+    c = make_ctx(T, prec)
+    dt = torch.float64 if prec == "f64" else torch.float32
+    X = torch.tensor(pw.random_orthonormal_psi(nt, nb, 33), dtype=dt)
+    dev = c.hpsi(X.cuda()).cpu()
+    Xh = torch.zeros((nb, ld), dtype=dt).pin_memory()
+    Xh[:, :nt] = X
+    for acc in (0, 1):
+        Yh = torch.full((nb, ld), 1.0, dtype=dt).pin_memory()
+        check(lib.pw_hpsi_host(c.handle, C.c_void_p(Xh.data_ptr()), ld, C.c_void_p(Yh.data_ptr()), ld, nb, acc))
+        got = Yh[:, :nt] - (1.0 if acc else 0.0)
+        tol = 1e-14 if prec == "f64" else 1e-6
+        assert float((got - dev).abs().max() / dev.abs().max()) <= tol
+        assert bool((Yh[:, nt:] == 1.0).all())
+
+
 def test_hpsi_local_only_and_no_projectors(si8):
     import torch
     from pwdft_develop_b200 import Context
