@@ -229,10 +229,10 @@ def scf_bench(device: int, max_iter: int = 60):
         c.scf(cheby_first_cycles=5, tol_efree=1e-6, refine_threshold=3e-6, max_iter=3, **kw)
         c.scf(cheby_first_cycles=1, tol_efree=1e-6, refine_threshold=1e9, max_iter=1, **kw)
         torch.cuda.synchronize()
-        # two timed runs (the SCF makes many small host round trips per iteration,
-        # so a busy shared host shows up as run-to-run spread); the faster is reported
+        # three timed runs (the SCF makes many small host round trips per iteration,
+        # so a busy shared host shows up as run-to-run spread); the fastest is reported
         samples = []
-        for _ in range(2):
+        for _ in range(3):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
             res, eig, _ = c.scf(cheby_first_cycles=5, tol_efree=1e-6, refine_threshold=3e-6, max_iter=max_iter,
@@ -254,7 +254,7 @@ def scf_bench(device: int, max_iter: int = 60):
     out["speedup_mixed_vs_f64"] = out["f64"]["seconds"] / out["mixed"]["seconds"]
     out["efree_agreement_per_atom"] = abs(out["f64"]["efree"] - out["mixed"]["efree"]) / 64
     out["workload"] = ("Si64, ChebFSI degree 10 (5 cycles in the first SCF step), Anderson(8, 0.7), 300 K, "
-                       "tol 1e-6 Ha/atom, Chebyshev filter replayed from a CUDA graph; faster of two timed runs")
+                       "tol 1e-6 Ha/atom, Chebyshev filter replayed from a CUDA graph; fastest of three timed runs")
     return out
 
 
