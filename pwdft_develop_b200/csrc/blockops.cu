@@ -358,6 +358,33 @@ __global__ void k_sym_upper(int n, double* A, int lda) {
   const int j = blockIdx.x;
   for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) A[(long)j * lda + i] = A[(long)i * lda + j];
 }
+// column j of an n x n column-major block: strict lower part zero (mode 0), or
+// the identity (mode 1)
+__global__ void k_tri_fill(int n, double* A, int lda, int mode) {
+  const int j = blockIdx.x;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    if (mode == 1) A[(long)j * lda + i] = (i == j) ? 1.0 : 0.0;
+    else if (i > j) A[(long)j * lda + i] = 0.0;
+  }
+}
+int dense_sym_upper(int n, double* A, int lda, cudaStream_t st) {
+  if (n <= 0) return PW_OK;
+  k_sym_upper<<<n, 128, 0, st>>>(n, A, lda);
+  PWB_CUDA(cudaGetLastError());
+  return PW_OK;
+}
+int dense_zero_lower(int n, double* A, int lda, cudaStream_t st) {
+  if (n <= 0) return PW_OK;
+  k_tri_fill<<<n, 128, 0, st>>>(n, A, lda, 0);
+  PWB_CUDA(cudaGetLastError());
+  return PW_OK;
+}
+int dense_identity(int n, double* A, int lda, cudaStream_t st) {
+  if (n <= 0) return PW_OK;
+  k_tri_fill<<<n, 128, 0, st>>>(n, A, lda, 1);
+  PWB_CUDA(cudaGetLastError());
+  return PW_OK;
+}
 // A(i,j) *= s[i] * s[j]  (s device)
 __global__ void k_scale_sym(int n, double* A, int lda, const double* s, int both) {
   const int j = blockIdx.x;

@@ -63,6 +63,12 @@ struct Dense {
   int potrf_upper(int n, double* A, int lda, cudaStream_t st);
 };
 
+// n x n column-major blocks on the device, queued on st: lower part from the
+// upper triangle, strict lower part zeroed, identity
+int dense_sym_upper(int n, double* A, int lda, cudaStream_t st);
+int dense_zero_lower(int n, double* A, int lda, cudaStream_t st);
+int dense_identity(int n, double* A, int lda, cudaStream_t st);
+
 // Symmetric generalized eigenproblem of EigenSolver::SolveGenEig (serial path,
 // src/EigenSolver/eigensolver.cpp:224-297): symmetrise from the upper triangle,
 // eig(B), keep sigma/sigma_max > 1e-8, eig of the reduced A, C = U sigma^-1/2 Z.

@@ -445,17 +445,11 @@ static int cholqr(Solver& s, Dense& d, void* X, int nb, void* tmp) {
   // Uinv = U^{-1} (upper): solve U * Uinv = I
   if ((rc = s.G2.alloc((size_t)nb * nb * 8))) return rc;
   double* Ui = (double*)s.G2.p;
-  std::vector<double> I((size_t)nb * nb, 0.0);
-  for (int i = 0; i < nb; ++i) I[(size_t)i * nb + i] = 1.0;
-  PWB_CUDA(cudaMemcpy(Ui, I.data(), (size_t)nb * nb * 8, cudaMemcpyHostToDevice));
+  if ((rc = dense_identity(nb, Ui, nb, st))) return rc;
   const double one = 1.0;
   cublasSetStream(d.blas, st);
   // zero the strict lower part of G first (potrf leaves it untouched)
-  std::vector<double> hg((size_t)nb * nb);
-  PWB_CUDA(cudaMemcpy(hg.data(), G, hg.size() * 8, cudaMemcpyDeviceToHost));
-  for (int j = 0; j < nb; ++j)
-    for (int i = j + 1; i < nb; ++i) hg[(size_t)j * nb + i] = 0.0;
-  PWB_CUDA(cudaMemcpy(G, hg.data(), hg.size() * 8, cudaMemcpyHostToDevice));
+  if ((rc = dense_zero_lower(nb, G, nb, st))) return rc;
   if (cublasDtrsm(d.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, nb, nb, &one, G,
                   nb, Ui, nb) != CUBLAS_STATUS_SUCCESS) {
     set_error("trsm failed");
@@ -475,11 +469,7 @@ static int rayleigh_ritz(Solver& s, Dense& d, void* Y, void* HY, void* X, void* 
   double* A = (double*)s.G1.p;
   { SubTimer t_(1); if ((rc = gram(s.c, Y, (int)s.nt, nb, HY, (int)s.nt, nb, A, nb, nullptr))) return rc; }
   // symmetrise from the upper triangle
-  std::vector<double> ha((size_t)nb * nb);
-  PWB_CUDA(cudaMemcpy(ha.data(), A, ha.size() * 8, cudaMemcpyDeviceToHost));
-  for (int j = 0; j < nb; ++j)
-    for (int i = j + 1; i < nb; ++i) ha[(size_t)j * nb + i] = ha[(size_t)i * nb + j];
-  PWB_CUDA(cudaMemcpy(A, ha.data(), ha.size() * 8, cudaMemcpyHostToDevice));
+  if ((rc = dense_sym_upper(nb, A, nb, nullptr))) return rc;
   double* w = (double*)s.wbuf.p;
   { SubTimer t_(2); if ((rc = d.syevd(nb, A, nb, w, nullptr))) return rc; }
   s.eig.resize(nb);
@@ -959,15 +949,9 @@ static int cholqr_pair(Solver& s, Dense& d, void* X, void* AX, int nb, void* tmp
   double* G = (double*)s.G1.p;
   if ((rc = gram(s.c, X, (int)s.nt, nb, X, (int)s.nt, nb, G, nb, st))) return rc;
   if ((rc = d.potrf_upper(nb, G, nb, st))) return rc;
-  std::vector<double> hg((size_t)nb * nb);
-  PWB_CUDA(cudaMemcpy(hg.data(), G, hg.size() * 8, cudaMemcpyDeviceToHost));
-  for (int j = 0; j < nb; ++j)
-    for (int i = j + 1; i < nb; ++i) hg[(size_t)j * nb + i] = 0.0;
-  PWB_CUDA(cudaMemcpy(G, hg.data(), hg.size() * 8, cudaMemcpyHostToDevice));
+  if ((rc = dense_zero_lower(nb, G, nb, st))) return rc;
   double* Ui = (double*)s.G2.p;
-  std::vector<double> I((size_t)nb * nb, 0.0);
-  for (int i = 0; i < nb; ++i) I[(size_t)i * nb + i] = 1.0;
-  PWB_CUDA(cudaMemcpy(Ui, I.data(), I.size() * 8, cudaMemcpyHostToDevice));
+  if ((rc = dense_identity(nb, Ui, nb, st))) return rc;
   const double one = 1.0;
   cublasSetStream(d.blas, st);
   if (cublasDtrsm(d.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, nb, nb, &one, G,
@@ -1461,6 +1445,7 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
     q = hartree(ctx, (double2*)S.work.p, rh, rps, (const double*)S.kern.p, (double*)S.vh.p, (const double2*)S.tw.p,
                     nullptr);
     if (q) return q;
+    if (!exc_out) return PW_OK;   // the caller reduces eps rho with its own sums
     double e;
     if ((q = dots(S, nf, {{(const double*)S.eps.p, rh}}, &e))) return q;
     *exc_out = e * w;
@@ -1604,43 +1589,33 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
       ekin += 2.0 * eig[i] * occ[i];
       ent += 2.0 * fd_entropy(eig[i], ef, tbeta);
     }
-    // Harris energy with the input density (scf.cpp:2025-2060)
-    double hd[3];
-    if ((rc = dots(S, nf, {{(const double*)S.vh.p, rho}, {(const double*)S.vh.p, rps}, {(const double*)S.vxc.p, rho}}, hd)))
-      return rc;
-    const double ehart_h = 0.5 * (hd[0] + hd[1]) * w, evxc = hd[2] * w;
-    eharris = ekin + (exc - evxc) - ehart_h - eself + ent;
-    // new density
+    // new density, and with its norm (one reduction) the Harris energy of the
+    // input density and potentials (scf.cpp:2025-2060)
+    double* ro = (double*)S.rho_out.p;
     {
       PhaseTimer pt_(prof, &tph[1]);
       std::vector<double> wv(nb + 2, 0.0);
       for (int i = 0; i < nb; ++i) wv[i] = 2.0 * occ[i];
       PWB_CUDA(cudaMemcpy(S.wocc.p, wv.data(), wv.size() * 8, cudaMemcpyHostToDevice));
-      double* ro = (double*)S.rho_out.p;
       PWB_CUDA(cudaMemset(ro, 0, nf * 8));
       const int cap = sv.c->pair_cap;
       for (int b0 = 0; b0 < nb; b0 += 2 * cap) {
         const int npair = std::min(cap, (nb - b0 + 1) / 2);
         if ((rc = run_density(sv.c, sv.X.p, (int)nt, nb, b0, npair, (const double*)S.wocc.p, ro, nullptr))) return rc;
       }
-      double tot;
-      if ((rc = dots(S, nf, {{ro, nullptr}}, &tot))) return rc;
-      k_lincomb<<<nblk(nf), 256>>>(nf, (2.0 * p->nocc * (double)nf) / (ctx->vol * tot), ro, 0.0, nullptr, ro);
+      double hd[4];
+      if ((rc = dots(S, nf, {{(const double*)S.vh.p, rho}, {(const double*)S.vh.p, rps},
+                             {(const double*)S.vxc.p, rho}, {ro, nullptr}}, hd)))
+        return rc;
+      const double ehart_h = 0.5 * (hd[0] + hd[1]) * w, evxc = hd[2] * w;
+      eharris = ekin + (exc - evxc) - ehart_h - eself + ent;
+      k_lincomb<<<nblk(nf), 256>>>(nf, (2.0 * p->nocc * (double)nf) / (ctx->vol * hd[3]), ro, 0.0, nullptr, ro);
     }
-    double* ro = (double*)S.rho_out.p;
     {
       PhaseTimer pt_(prof, &tph[2]);
-      if ((rc = potentials(ro, &exc))) return rc;
+      if ((rc = potentials(ro, nullptr))) return rc;
     }
     k_lincomb<<<nblk(nf), 256>>>(nf, 1.0, (double*)S.vh.p, 1.0, (double*)S.vxc.p, (double*)S.vtot_new.p);
-    double ed[2];
-    if ((rc = dots(S, nf, {{(const double*)S.vtot.p, ro}, {(const double*)S.vh.p, ro}}, ed))) return rc;
-    double ehps;
-    if ((rc = dots(S, nf, {{(const double*)S.vh.p, rps}}, &ehps))) return rc;
-    ehart = 0.5 * (ed[1] - ehps) * w;
-    etot = ekin + (-ed[0] * w) + exc + ehart - eself;
-    efree = etot + ent;
-    const double dif = std::fabs(efree - eharris) / natom;
     // SCF::CalculateError of the change of the output density (scf.cpp:1492-1496,
     // 2368-2396); of the potential change vtotNew - vtot in the phi
     // iterations' inner loop (scf.cpp:728-739)
@@ -1657,10 +1632,20 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
       PWB_CUDA(cudaMemset(S.bdots.p, 0, 8));
       k_wdot<<<nblk(nf), 256>>>(nf, (const double*)S.bw.p, (const double2*)S.work.p, (const double2*)S.work.p,
                                 (double*)S.bdots.p);
-      PWB_CUDA(cudaMemcpy(&snorm, S.bdots.p, 8, cudaMemcpyDeviceToHost));
-      snorm /= (double)nf * (double)nf;
-      r->scf_norm = snorm;
     }
+    // KS energy terms (scf.cpp:1834-1984) in one reduction; it also waits for the scfNorm sum
+    double ed[4];
+    if ((rc = dots(S, nf, {{(const double*)S.eps.p, ro}, {(const double*)S.vtot.p, ro}, {(const double*)S.vh.p, ro},
+                           {(const double*)S.vh.p, rps}}, ed)))
+      return rc;
+    exc = ed[0] * w;
+    ehart = 0.5 * (ed[2] - ed[3]) * w;
+    etot = ekin + (-ed[1] * w) + exc + ehart - eself;
+    efree = etot + ent;
+    const double dif = std::fabs(efree - eharris) / natom;
+    PWB_CUDA(cudaMemcpy(&snorm, S.bdots.p, 8, cudaMemcpyDeviceToHost));
+    snorm /= (double)nf * (double)nf;
+    r->scf_norm = snorm;
     if (p->verbose)
       fprintf(stderr, "SCF %3d %s Etot %.10f Efree %.10f Eharris %.10f dif %.3e scfnorm %.3e\n", it,
               sv.c->prec == PW_F32 ? "f32" : "f64", etot, efree, eharris, dif, snorm);
