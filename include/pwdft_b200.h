@@ -355,7 +355,10 @@ PW_API int pw_hpsi_kbatch(pw_ctx* ctx, const void* psi, int ld, void* hpsi, int 
  * N_coarse doubles each; either may be NULL). */
 PW_API int pw_get_kpoint_tables(const pw_ctx* ctx, double* ekin_host, double* teter_host);
 
-/* Hybrid exact exchange (Gamma point, real bands).  Modes of the exchange
+/* Hybrid exact exchange (Gamma point, real bands; sphere-cut FP64 contexts:
+ * the complex overload of Spinor::AddMultSpinorEXX, src/SCF/spinor.cpp:
+ * 783-945, with pair products on the full G-space grid, the kernel on the
+ * Fock set 1/2 |G|^2 < 4 Ecut and phi = sqrt(1 / (vol N)) c).  Modes of the exchange
  * term inside pw_hpsi: off, the full pair-FFT operator
  * (Spinor::AddMultSpinorEXX, src/SCF/spinor.cpp:682-781) or the ACE operator
  * (KohnSham::MultSpinor, src/SCF/hamiltonian.cpp:3135-3218). */
@@ -369,7 +372,8 @@ enum { PW_EXX_OFF = 0, PW_EXX_FULL = 1, PW_EXX_ACE = 2 };
 PW_API int pw_exx_setup(pw_ctx* ctx, double exx_fraction, double screen_mu, int divergence_type,
                         double ecut_wavefunction);
 /* exxDiv and the kernel on the full coarse spectrum (host, N_coarse doubles;
- * either pointer may be NULL). */
+ * sphere-cut contexts: the full G-space grid, N_fine doubles; either pointer
+ * may be NULL). */
 PW_API int pw_exx_get(const pw_ctx* ctx, double* exx_div, double* kern_host);
 /* Exchange orbitals phi = sqrt(N_c / vol) psi with their occupation rates
  * (KohnSham::SetPhiEXX, hamiltonian.cpp:3554-3641).  psi: device, context
@@ -500,8 +504,8 @@ PW_API int pw_scf_set_initial(pw_ctx* ctx, const double* rho_fine, const double*
  * grid: Density_Grid_Factor 1, src/esdf.cpp:2786-2856); N/2 must be a coarse
  * grid built into the library and the sphere must satisfy |m_d| <= N_d / 4.
  * After it, pw_ctx_sizes reports ntot = 2 ns and ntotFine = N.  Exact
- * exchange, k-points and forces are not built for G-space contexts
- * (PW_EUNSUPPORTED). */
+ * exchange (pw_exx_*, pw_ace_*) is built for FP64 G-space contexts; k-points
+ * and forces are not built for them (PW_EUNSUPPORTED). */
 PW_API int pw_ctx_create_gspace(const double length[3], const int numGrid[3], double ecut, int precision, int device,
                                 pw_ctx** out);
 /* Sphere tables of a G-space context (host arrays, any may be NULL):

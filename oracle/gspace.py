@@ -330,3 +330,78 @@ def real_view(c: np.ndarray) -> np.ndarray:
 
 def complex_view(x: np.ndarray) -> np.ndarray:
     return np.ascontiguousarray(x).view(np.complex128).reshape(x.shape[0], -1)
+
+
+def _full_g2(sp: Sphere) -> np.ndarray:
+    """|G|^2 on the full N^3 grid, (N2, N1, N0) x fastest."""
+    n0, n1, n2 = sp.N
+    m0 = np.fft.fftfreq(n0, 1.0 / n0)
+    m1 = np.fft.fftfreq(n1, 1.0 / n1)
+    m2 = np.fft.fftfreq(n2, 1.0 / n2)
+    L = np.asarray(sp.L, float)
+    g0 = 2 * np.pi / L[0] * m0
+    g1 = 2 * np.pi / L[1] * m1
+    g2 = 2 * np.pi / L[2] * m2
+    return g2[:, None, None] ** 2 + g1[None, :, None] ** 2 + g0[None, None, :] ** 2
+
+
+def exx_kernel(sp: Sphere, ecut: float, mu: float = 0.0, div_type: int = 1):
+    """(exxgkkR2C on the R2C half grid, zero outside the Fock set, exxDiv) of
+    KohnSham::InitializeEXX with a sphere cut (src/SCF/hamiltonian.cpp:
+    3454-3551): exxDiv sums over eps < |G|^2 < 4 Ecut of the full grid, the
+    kernel lives on the R2C points with 1/2 |G|^2 < 4 Ecut (Fock set,
+    src/SCF/fourier.cpp:642-666)."""
+    eps = 1e-8
+    alpha = 10.0 / (ecut * 2.0)
+    q = _full_g2(sp).reshape(-1)
+    div = 0.0
+    if div_type == 1:
+        sel = (q > eps) & (q < ecut * 4.0)
+        if mu > 0.0:
+            div = float(np.sum(np.exp(-alpha * q[sel]) / q[sel] * (1.0 - np.exp(-q[sel] / (4 * mu * mu)))))
+            div += 1.0 / (4 * mu * mu)
+        else:
+            div = float(np.sum(np.exp(-alpha * q[sel]) / q[sel])) - alpha
+        div *= 4.0 * np.pi
+        aa = 1.0 / math.sqrt(alpha * np.pi)
+        if mu > 0.0:
+            aa -= 1.0 / math.sqrt(np.pi * (alpha + 1.0 / (4 * mu * mu)))
+        div -= sp.vol * aa
+    n0, n1, n2 = sp.N
+    qh = _full_g2(sp)[:, :, : n0 // 2 + 1]
+    k = np.zeros_like(qh)
+    fock = 0.5 * qh < 4.0 * ecut
+    big = fock & (qh > eps)
+    if mu > 0.0:
+        k[big] = 4 * np.pi / qh[big] * (1.0 - np.exp(-qh[big] / (4 * mu * mu)))
+    else:
+        k[big] = 4 * np.pi / qh[big]
+    zero = fock & (qh <= eps)
+    k[zero] = -div + (np.pi / (mu * mu) if mu > 0.0 else 0.0)
+    return k, div
+
+
+def set_phi(sp: Sphere, c: np.ndarray) -> np.ndarray:
+    """phi = sqrt(1 / (vol N)) c (SetPhiEXX sphere-cut branch, hamiltonian.cpp:3568-3580)."""
+    return c * math.sqrt(1.0 / (sp.vol * sp.ntot))
+
+
+def add_mult_spinor_exx(sp: Sphere, c: np.ndarray, phi: np.ndarray, kern: np.ndarray, frac: float,
+                        occ: np.ndarray) -> np.ndarray:
+    """V_x c of Spinor::AddMultSpinorEXX, complex overload
+    (src/SCF/spinor.cpp:783-945): psi(r), phi(r) by the unnormalised C2R of
+    their sphere coefficients, pair products transformed with the reference's
+    forward (x vol/N) and backward (x 1/vol) conventions around the kernel,
+    times -alpha f_j phi_j, unnormalised R2C and sqrt(2) on G != 0."""
+    n0, n1, n2 = sp.N
+    shp = (n2, n1, n0)
+    pr = c2r_unnormalised(sp, to_r2c(sp, c))
+    fr = c2r_unnormalised(sp, to_r2c(sp, phi))
+    acc = np.zeros_like(pr)
+    for j in range(fr.shape[0]):
+        prod = (pr * fr[j][None, :]).reshape((-1,) + shp)
+        X = np.fft.rfftn(prod, axes=(1, 2, 3)) * (sp.vol / sp.ntot) * kern[None]
+        v = np.fft.irfftn(X, s=shp, axes=(1, 2, 3)) * sp.ntot / sp.vol
+        acc += -frac * occ[j] * v.reshape(pr.shape) * fr[j][None, :]
+    Y = np.fft.rfftn(acc.reshape((-1,) + shp), axes=(1, 2, 3))
+    return from_r2c(sp, Y)

@@ -490,11 +490,14 @@ def _ctx_exx_setup(self, fraction: float = 0.25, screen_mu: float = 0.0, diverge
 
 
 def _ctx_exx_kernel(self):
-    """(exxDiv, kernel on the full coarse spectrum as an (n2, n1, n0) array)."""
+    """(exxDiv, kernel on the full coarse spectrum as an (n2, n1, n0) array;
+    G-space contexts: on the full G-space grid, zero outside the Fock set)."""
     d = C.c_double(0.0)
-    k = np.zeros(self.ntot)
+    gs = getattr(self, "ns", None) is not None
+    grid = self.numGridFine if gs else self.numGrid
+    k = np.zeros(int(np.prod(grid)))
     check(lib.pw_exx_get(self._h, C.byref(d), k.ctypes.data_as(_lib._dp)))
-    return d.value, k.reshape(self.numGrid[2], self.numGrid[1], self.numGrid[0])
+    return d.value, k.reshape(grid[2], grid[1], grid[0])
 
 
 def _ctx_exx_set_phi(self, psi, occ):

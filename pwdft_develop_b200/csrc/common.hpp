@@ -176,6 +176,7 @@ struct pw_ctx {
   int pair_cap = 0;
   pwb::DevBuf s_ad, s_k, s_bc, s_wp, s_w;
   pwb::DevBuf s_host_in, s_host_out;   // device staging for the host-pointer entry points
+  pwb::DevBuf gs_full_idx, gs_exx_tw;   // G-space exchange: full-grid index of G_s and -G_s, N-point twiddles
   cudaStream_t io_st[3] = {nullptr, nullptr, nullptr};   // host->device, compute, device->host (pw_hpsi_host)
   int host_chunk = 32;                                    // bands per pw_hpsi_host chunk
 };
@@ -214,5 +215,9 @@ struct Launch {
     }
   }
 };
+
+// exact exchange of sphere-cut (G-space) FP64 contexts (gs_exx.cu)
+int gs_exx_setup(pw_ctx* c, double frac, double mu, int divergence_type, double ecut);
+int gs_exx_apply(pw_ctx* c, const void* psi, int ld, int nb, void* out, int ldo, int accumulate, cudaStream_t st);
 
 }  // namespace pwb

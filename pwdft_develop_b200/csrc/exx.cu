@@ -68,11 +68,20 @@ extern "C" {
 
 int pw_exx_setup(pw_ctx* ctx, double exx_fraction, double screen_mu, int divergence_type, double ecut_wavefunction) {
   PWB_CHECK(ctx, PW_EINVAL, "null context");
-  PWB_CHECK(!ctx->gs, PW_EUNSUPPORTED, "exact exchange is built for real-space contexts only");
   PWB_CHECK(divergence_type == 0 || divergence_type == 1, PW_EUNSUPPORTED,
             "EXX divergence types 0 and 1 are built (EXX_Divergence_Type)");
   PWB_CHECK(screen_mu >= 0.0 && ecut_wavefunction > 0.0, PW_EINVAL, "bad exchange parameters");
   PWB_CUDA(cudaSetDevice(ctx->device));
+  if (ctx->gs) {
+    int rc = gs_exx_setup(ctx, exx_fraction, screen_mu, divergence_type, ecut_wavefunction);
+    if (rc) return rc;
+    if (ctx->exx_nphi > 0 && !ctx->exx_occ.empty()) {
+      std::vector<double> w(ctx->exx_nphi);
+      for (int j = 0; j < ctx->exx_nphi; ++j) w[j] = -exx_fraction * ctx->exx_occ[j];
+      if ((rc = upload_real(ctx, ctx->exx_w, w.data(), w.size()))) return rc;
+    }
+    return PW_OK;
+  }
   const int n0 = ctx->n[0], n1 = ctx->n[1], n2 = ctx->n[2];
   const long nt = ctx->ntot;
   const double eps_div = 1e-8;
@@ -132,7 +141,7 @@ int pw_exx_get(const pw_ctx* ctx, double* exx_div, double* kern_host) {
   if (rc) return rc;
   if (exx_div) *exx_div = ctx->exx_div;
   if (kern_host) {
-    const long nt = ctx->ntot;
+    const long nt = ctx->gs ? ctx->ntotf : ctx->ntot;   // G-space: the full N^3 grid
     if (ctx->prec == PW_F64) {
       PWB_CUDA(cudaMemcpy(kern_host, ctx->exx_kern.p, nt * 8, cudaMemcpyDeviceToHost));
     } else {
@@ -154,7 +163,9 @@ int pw_exx_set_phi(pw_ctx* ctx, const void* psi, int ld, int nphi, const double*
   ctx->exx_occ.assign(occ, occ + nphi);
   if (nphi == 0) return PW_OK;
   if ((rc = ctx->exx_phi.alloc((size_t)nphi * nt * ctx->esz))) return rc;
-  const double fac = std::sqrt((double)nt / ctx->vol);
+  // SetPhiEXX (hamiltonian.cpp:3568-3580, 3598-3612): sqrt(N_c / vol) for
+  // real-space bands, sqrt(1 / (vol N)) for sphere coefficients
+  const double fac = ctx->gs ? std::sqrt(1.0 / (ctx->vol * (double)ctx->ntotf)) : std::sqrt((double)nt / ctx->vol);
   const int nblk = (int)std::min<long>(4096, ((long)nphi * nt + 255) / 256);
   if (ctx->prec == PW_F64)
     k_exx_scale_copy<double><<<nblk, 256>>>(nt, (const double*)psi, ld, nphi, fac, (double*)ctx->exx_phi.p);

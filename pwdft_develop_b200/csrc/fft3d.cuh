@@ -10,7 +10,10 @@ constexpr int AX_TILE = 16;
 constexpr int AX_THREADS = 256;
 
 // axis 0 (x, contiguous): CTA = 16 consecutive rows; axis 1 (y): CTA = (z, x tile);
-// axis 2 (z): CTA = (y, x tile).  MODE 0: plain, 1: real input (load re(x) -
+// axis 2 (z): CTA = (y, x tile, field blockIdx.z).  A batch of F fields stored
+// back to back runs as one launch: nz * F planes for axes 0 and 1 (nz = N * F
+// for axis 0, gridDim.y = nz * F for axis 1), gridDim.z = F for axis 2, whose
+// multiplier kern (MODE 2 / 4) is the same nx * ny * nz array for every field.  MODE 0: plain, 1: real input (load re(x) -
 // y_sub), 2: multiply by kern after the forward transform and inverse in place,
 // 3: store the real part scaled into out, 4: as 2 with the multiplier i * kern
 // (a spectral derivative).
@@ -48,9 +51,10 @@ k_fft_axis(double2* __restrict__ data, int nx, int ny, int nz, const double* __r
     cnt = min(AX_TILE, nx - x0);
     if (AXIS == 1) { base = (long)blockIdx.y * nx * ny + x0; estride = nx; }
     else { base = (long)blockIdx.y * nx + x0; estride = (long)nx * ny; }
+    const long fofs = AXIS == 2 ? (long)blockIdx.z * nx * ny * nz : 0;
     for (int i = threadIdx.x; i < N * AX_TILE; i += blockDim.x) {
       const int e = i / AX_TILE, c = i - e * AX_TILE;
-      buf[e * P + c] = (c < cnt) ? data[base + e * estride + c] : make_double2(0, 0);
+      buf[e * P + c] = (c < cnt) ? data[fofs + base + e * estride + c] : make_double2(0, 0);
     }
   }
   __syncthreads();
@@ -79,9 +83,10 @@ k_fft_axis(double2* __restrict__ data, int nx, int ny, int nz, const double* __r
       }
     }
   } else {
+    const long fofs = AXIS == 2 ? (long)blockIdx.z * nx * ny * nz : 0;
     for (int i = threadIdx.x; i < N * AX_TILE; i += blockDim.x) {
       const int e = i / AX_TILE, c = i - e * AX_TILE;
-      if (c < cnt) data[base + e * estride + c] = buf[e * P + c];
+      if (c < cnt) data[fofs + base + e * estride + c] = buf[e * P + c];
     }
   }
 }

@@ -68,7 +68,7 @@ int run_density(pw_ctx* c, const void* psi, int ld, int nband, int band0, int np
 int run_exx(pw_ctx* c, const void* psi, int ld, int nb, void* out, int ldo, int acc, cudaStream_t st) {
   const GridEntry* g = find_grid(c->n);
   if (!g) { set_error("grid not built into this library"); return PW_EUNSUPPORTED; }
-  if (gs_refuse(c, "exact exchange")) return PW_EUNSUPPORTED;
+  if (c->gs) return gs_exx_apply(c, psi, ld, nb, out, ldo, acc, st);
   return g->exx[c->prec == PW_F32 ? 1 : 0](c, psi, ld, nb, out, ldo, acc, st);
 }
 
@@ -98,7 +98,6 @@ int run_build_q_k(pw_ctx* c, const int* d_idx, const double* d_beta, const doubl
 int run_ace(pw_ctx* c, const void* psi, int ld, int nb, void* out, int ldo, cudaStream_t st) {
   const GridEntry* g = find_grid(c->n);
   if (!g) { set_error("grid not built into this library"); return PW_EUNSUPPORTED; }
-  if (gs_refuse(c, "ACE")) return PW_EUNSUPPORTED;
   return g->ace[c->prec == PW_F32 ? 1 : 0](c, psi, ld, nb, out, ldo, 1, st);
 }
 

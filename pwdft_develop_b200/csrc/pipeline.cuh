@@ -1484,6 +1484,7 @@ struct Plan {
       DenseSet ds{c->ace_xi.p, c->ace_qd.p, c->ace_bf.p, c->ace_t_bf.p, c->ace_n, c->ace_npad};
       return dense_apply(c, ds, psi + (long)band0 * ld, ld, out + (long)band0 * ldo, ldo, nb, st);
     }
+    if (c->gs) return gs_exx_apply(c, psi + (long)band0 * ld, ld, nb, out + (long)band0 * ldo, ldo, 1, st);
     return exx_apply(c, psi + (long)band0 * ld, ld, nb, out + (long)band0 * ldo, ldo, 1, st);
   }
 
@@ -1864,9 +1865,10 @@ struct Plan {
         reinterpret_cast<const int2*>(c->gs_ent_fwd.p), reinterpret_cast<const T*>(c->gs_ekin.p), tw(c, 5)); }
     PWB_CUDA(cudaGetLastError());
     const int nb = std::min(2 * npair, nband - band0);
-    if (c->have_nl && c->nproj > 0 && nb > 0)
-      return dense_apply(c, nl_set(c), psi + (long)band0 * ld, ld, out + (long)band0 * ldo, ldo, nb, st);
-    return PW_OK;
+    if (c->have_nl && c->nproj > 0 && nb > 0 &&
+        (rc = dense_apply(c, nl_set(c), psi + (long)band0 * ld, ld, out + (long)band0 * ldo, ldo, nb, st)))
+      return rc;
+    return exchange_batch(c, psi, ld, out, ldo, nband, band0, npair, st);
   }
 
   // rho += sum of w_b |psi_b(r)|^2 from sphere coefficients (CalculateDensity

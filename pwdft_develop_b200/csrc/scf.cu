@@ -1430,7 +1430,6 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
   const bool hse = p->xc == PW_XC_HSE06;
   const bool pbe = p->xc == PW_XC_PBE || hse;
   PWB_CHECK(p->xc == PW_XC_TETER93 || pbe, PW_EINVAL, "unknown exchange-correlation functional");
-  PWB_CHECK(!hse || !ctx->gs, PW_EUNSUPPORTED, "the hybrid SCF is built for real-space contexts");
   if (pbe && ((rc = S.work2.alloc(nf * 16)) || (rc = S.grad.alloc(3 * nf * 8)))) return rc;
   if (hse) ctx->exx_mode = PW_EXX_OFF;
   double hse_frac = 0.0;

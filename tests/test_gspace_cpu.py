@@ -137,3 +137,44 @@ def test_gspace_and_real_space_eigenvalues_agree():
     Hr = np.concatenate([pw.mult_spinor(T, I[i:i + 512]) for i in range(0, nc, 512)])
     er = np.linalg.eigvalsh(0.5 * (Hr + Hr.T))[:12]
     assert np.abs(eg - er).max() <= 3e-3, np.abs(eg - er).max()
+
+
+def test_gspace_exchange_matches_the_real_space_exchange():
+    """Without the divergence correction the sphere-cut kernel (Fock set
+    1/2|G|^2 < 4 Ecut) and the real-space kernel agree on every pair product of
+    sphere functions (their spectra lie inside the Fock set), so the G-space
+    V_x c equals the real-space V_x of the same functions on the same grid
+    (oracle/exx.py, pinned against direct convolution) to 1e-13."""
+    from oracle import exx
+    L, z, pos, sp = _si8((24, 24, 24), 6.0)
+    c = gs.random_orthonormal_c(sp, 6, 3)
+    occ = np.linspace(1.0, 0.2, 6)
+    dm = pw.Domain(tuple(L), sp.N, sp.N)
+    psi_rs = gs.c2r_unnormalised(sp, gs.to_r2c(sp, c)) / math.sqrt(sp.ntot)
+    for mu in (0.0, 0.106):
+        k, _ = gs.exx_kernel(sp, 6.0, mu=mu, div_type=0)
+        vg = gs.add_mult_spinor_exx(sp, c, gs.set_phi(sp, c), k, 0.25, occ)
+        kr, _ = exx.exx_kernel_r2c(dm, 6.0, mu=mu, div_type=0)
+        vr = exx.add_mult_spinor_exx(dm, psi_rs, exx.set_phi(dm, psi_rs), kr, 0.25, occ)
+        ref = gs.from_r2c(sp, np.fft.rfftn(vr.reshape((-1,) + sp.N[::-1]), axes=(1, 2, 3))) / math.sqrt(sp.ntot)
+        assert np.abs(vg - ref).max() <= 1e-13 * np.abs(vg).max()
+
+
+def test_gspace_exchange_symmetric_negative_and_ace_exact():
+    """Divergence type 1 (auxiliary function over eps < |G|^2 < 4 Ecut): the
+    Gram Re(c^H V_x c) is symmetric and negative definite, Im (V_x c)_0 = 0,
+    and the ACE operator built from the bands reproduces V_x on their span."""
+    L, z, pos, sp = _si8((24, 24, 24), 6.0)
+    c = gs.random_orthonormal_c(sp, 8, 5)
+    occ = np.linspace(1.0, 0.1, 8)
+    k, div = gs.exx_kernel(sp, 6.0, mu=0.106, div_type=1)
+    assert div > 0
+    v = gs.add_mult_spinor_exx(sp, c, gs.set_phi(sp, c), k, 0.25, occ)
+    assert np.abs(v[:, 0].imag).max() == 0.0
+    A = np.real(c.conj() @ v.T)
+    assert np.abs(A - A.T).max() <= 1e-13 * np.abs(A).max()
+    assert np.linalg.eigvalsh(0.5 * (A + A.T)).max() < 0
+    W, X = gs.real_view(v), gs.real_view(c)
+    M = -(X @ W.T)
+    xi = np.linalg.solve(np.linalg.cholesky(0.5 * (M + M.T)), W)
+    assert np.abs(-(X @ xi.T) @ xi - W).max() <= 1e-12 * np.abs(W).max()
