@@ -179,6 +179,8 @@ struct pw_ctx {
   pwb::DevBuf gs_full_idx, gs_exx_tw;   // G-space exchange: full-grid index of G_s and -G_s, N-point twiddles
   cudaStream_t io_st[3] = {nullptr, nullptr, nullptr};   // host->device, compute, device->host (pw_hpsi_host)
   int host_chunk = 32;                                    // bands per pw_hpsi_host chunk
+  void* scf_cache = nullptr;                              // pw_scf_run workspace kept between runs
+  void (*scf_cache_free)(void*) = nullptr;
 };
 
 namespace pwb {

@@ -196,6 +196,7 @@ int pw_ctx_destroy(pw_ctx* ctx) {
   if (ctx->blas) cublasDestroy((cublasHandle_t)ctx->blas);
   for (cudaStream_t st : ctx->io_st)
     if (st) cudaStreamDestroy(st);
+  if (ctx->scf_cache_free) ctx->scf_cache_free(ctx->scf_cache);
   if (ctx->twin) pw_ctx_destroy(ctx->twin);
   delete ctx;
   return PW_OK;

@@ -1254,6 +1254,24 @@ struct ScfState {
   int nhist = 0, hpos = 0;
 };
 
+// pw_scf_run's device workspace, eigensolver blocks, dense-solver handle and
+// the grid tables of the last cut-off, kept in the context between runs (the
+// buffers are reused when large enough; the tables depend on the cell, the
+// fine grid and Ecut only)
+struct ScfCache {
+  ScfState S;
+  Solver sv;
+  Dense dn;
+  double ecut = -1.0;   // cut-off of the tables in S (Hartree kernel, density-sphere weights)
+  ~ScfCache() { dn.release(); }
+};
+void* scf_cache_new() { return new ScfCache(); }
+void scf_cache_free(void* p) { delete static_cast<ScfCache*>(p); }
+ScfState& cache_state(ScfCache& c) { return c.S; }
+Solver& cache_solver(ScfCache& c) { return c.sv; }
+Dense& cache_dense(ScfCache& c) { return c.dn; }
+double& cache_ecut(ScfCache& c) { return c.ecut; }
+
 struct PhaseTimer {
   bool on;
   std::chrono::steady_clock::time_point t0;
@@ -1332,8 +1350,16 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
   PWB_CHECK(p->solver >= PW_SOLVER_LOBPCG && p->solver <= PW_SOLVER_DAVIDSON, PW_EINVAL, "unknown eigensolver");
   PWB_CUDA(cudaSetDevice(ctx->device));
   const auto t_start = std::chrono::steady_clock::now();
-  ScfState S;
+  if (!ctx->scf_cache) {
+    ctx->scf_cache = scf_cache_new();
+    ctx->scf_cache_free = scf_cache_free;
+  }
+  ScfCache& cache = *(ScfCache*)ctx->scf_cache;
+  ScfState& S = cache_state(cache);
   S.c64 = ctx;
+  S.c32 = nullptr;
+  S.nhist = 0;
+  S.hpos = 0;
   const long nf = ctx->ntotf, nt = ctx->ntot;
   const int nb = p->nocc + p->nextra;
   const int natom = (int)ctx->atom_z.size();
@@ -1358,7 +1384,7 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
       (rc = S.dif_v.alloc((size_t)mixdim * nf * 8)) || (rc = S.dif_f.alloc((size_t)mixdim * nf * 8)))
     return rc;
   PWB_CUDA(cudaMemcpy(S.rps.p, ctx->h_rhops.data(), nf * 8, cudaMemcpyHostToDevice));
-  {
+  if (cache_ecut(cache) != p->ecut || !S.kern.p || !S.bw.p) {
     // Hartree kernel 2 pi / gkk / N on the fine grid (fourier.cpp:323-344 gkkFine)
     std::vector<double> k(nf);
     const int N0 = ctx->nf[0], N1 = ctx->nf[1], N2 = ctx->nf[2];
@@ -1396,6 +1422,10 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
     }
     if ((rc = S.tw.alloc(N0 * 16))) return rc;
     PWB_CUDA(cudaMemcpy(S.tw.p, t.data(), N0 * 16, cudaMemcpyHostToDevice));
+    cache_ecut(cache) = p->ecut;
+  } else if ((rc = S.dr.alloc(nf * 8)) ||
+             (rc = S.bdots.alloc((size_t)(std::max(1, p->mix_dim) + 1) * (std::max(1, p->mix_dim) + 1) * 8))) {
+    return rc;
   }
   const double w = ctx->vol / (double)nf;
   double eself = 0;
@@ -1454,9 +1484,11 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
   if ((rc = potentials(rho, &exc))) return rc;
   k_lincomb<<<nblk(nf), 256>>>(nf, 1.0, (double*)S.vh.p, 1.0, (double*)S.vxc.p, (double*)S.vtot.p);
   // eigensolver state: start in the FP32 twin when mixed
-  Dense dn;
+  Dense& dn = cache_dense(cache);
   if ((rc = dn.init((cublasHandle_t)ctx->blas))) return rc;
-  Solver sv;
+  Solver& sv = cache_solver(cache);
+  sv.eig.clear();
+  sv.res.clear();
   sv.use_graph = p->graphs != 0 && !prof;   // the sub-phase timers synchronise, which a capture forbids
   auto bind = [&](pw_ctx* c) -> int {
     // a captured filter refers to the previous context's buffers
@@ -1887,7 +1919,6 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
     ctx->scf_occ = occ;
     ctx->scf_nband = nb;
   }
-  dn.release();
   return PW_OK;
 }
 
