@@ -504,6 +504,24 @@ def gspace_bench(device: int, reps: int = 10):
         out[prec] = {"ns": ns, "ms_per_sweep": ms, "bands_per_s": bands_per_s,
                      "model_bytes_per_band": pair_bytes / 2,
                      "model_frac_of_hbm": pair_bytes / 2 * bands_per_s / (peak * 1e9), "kernels": kern}
+        if prec == "f64":
+            # sphere-cut exact exchange (HSE06 kernel): 32 bands x 128 occupied
+            # orbitals, pair products on the full 96^3 grid (FP64 axis FFTs)
+            nk, nphi = 32, 128
+            c.exx_setup(0.25, 0.106, 1, ecut)
+            c.exx_set_phi(X[:nphi].contiguous(), np.ones(nphi))
+            Xk = X[:nk].contiguous()
+            V = c.exx_apply(Xk)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            c.exx_apply(Xk, out=V)
+            e1.record()
+            torch.cuda.synchronize()
+            xms = e0.elapsed_time(e1)
+            out["exx_f64"] = {"workload": "sphere-cut V_x psi, 32 bands x 128 orbitals (64 pair fields per band), "
+                                          "96^3 grid, HSE06 kernel (mu 0.106)",
+                              "ms": xms, "pairs_per_s": nk * nphi / (xms / 1e3)}
         c.close()
     return out
 
