@@ -177,6 +177,8 @@ struct pw_ctx {
   pwb::DevBuf s_ad, s_k, s_bc, s_wp, s_w;
   pwb::DevBuf s_host_in, s_host_out;   // device staging for the host-pointer entry points
   pwb::DevBuf gs_full_idx, gs_exx_tw;   // G-space exchange: full-grid index of G_s and -G_s, N-point twiddles
+  pwb::DevBuf gsx_psir, gsx_phir, gsx_acc, gsx_fields;   // G-space exchange workspace (real fields, pair fields)
+  bool gsx_phi_ready = false;            // gsx_phir holds phi(r) of the current exchange orbitals
   cudaStream_t io_st[3] = {nullptr, nullptr, nullptr};   // host->device, compute, device->host (pw_hpsi_host)
   int host_chunk = 32;                                    // bands per pw_hpsi_host chunk
   void* scf_cache = nullptr;                              // pw_scf_run workspace kept between runs

@@ -160,6 +160,7 @@ int pw_exx_set_phi(pw_ctx* ctx, const void* psi, int ld, int nphi, const double*
   const long nt = ctx->ntot;
   int rc;
   ctx->exx_nphi = 0;
+  ctx->gsx_phi_ready = false;
   ctx->exx_occ.assign(occ, occ + nphi);
   if (nphi == 0) return PW_OK;
   if ((rc = ctx->exx_phi.alloc((size_t)nphi * nt * ctx->esz))) return rc;

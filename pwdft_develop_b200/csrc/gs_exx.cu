@@ -272,16 +272,22 @@ int gs_exx_apply(pw_ctx* c, const void* psi_v, int ld, int nb, void* out_v, int 
   const long fcap = std::min<long>(fmax, std::max<long>(njp, (long)(c->exx_scratch_bytes / (size_t)(n3 * 16))));
   const int kb = (int)std::max<long>(1, std::min<long>(nb, fcap / njp));
   const int pcap = (int)std::max<long>(1, std::min<long>((std::max(nb, nphi) + 1) / 2, fcap));
-  DevBuf psir, phir, acc, F;
+  // workspace kept in the context (reused while large enough); phi(r) is
+  // transformed once per pw_exx_set_phi
+  DevBuf &psir = c->gsx_psir, &phir = c->gsx_phir, &acc = c->gsx_acc, &F = c->gsx_fields;
   int rc;
-  if ((rc = psir.alloc((size_t)nb * n3 * 8)) || (rc = phir.alloc((size_t)nphi * n3 * 8)) ||
-      (rc = acc.alloc((size_t)nb * n3 * 8)) ||
+  const size_t phib = (size_t)nphi * n3 * 8;
+  if (phir.bytes < phib) c->gsx_phi_ready = false;
+  if ((rc = psir.alloc((size_t)nb * n3 * 8)) || (rc = phir.alloc(phib)) || (rc = acc.alloc((size_t)nb * n3 * 8)) ||
       (rc = F.alloc((size_t)std::max<long>((long)kb * njp, pcap) * n3 * 16)))
     return rc;
   double2* Z = (double2*)F.p;
-  if ((rc = gs_to_real(c, (const double*)c->exx_phi.p, (int)c->ntot, nphi, 1.0, (double*)phir.p, Z, pcap, st)) ||
-      (rc = gs_to_real(c, psi, ld, nb, 1.0, (double*)psir.p, Z, pcap, st)))
-    return rc;
+  if (!c->gsx_phi_ready) {
+    if ((rc = gs_to_real(c, (const double*)c->exx_phi.p, (int)c->ntot, nphi, 1.0, (double*)phir.p, Z, pcap, st)))
+      return rc;
+    c->gsx_phi_ready = true;
+  }
+  if ((rc = gs_to_real(c, psi, ld, nb, 1.0, (double*)psir.p, Z, pcap, st))) return rc;
   PWB_CUDA(cudaMemsetAsync(acc.p, 0, (size_t)nb * n3 * 8, st));
   for (int k0 = 0; k0 < nb; k0 += kb) {
     const int kn = std::min(kb, nb - k0);
@@ -302,8 +308,6 @@ int gs_exx_apply(pw_ctx* c, const void* psi_v, int ld, int nb, void* out_v, int 
     c->launches += 5;
   }
   PWB_CUDA(cudaGetLastError());
-  // the scratch buffers are released on return: finish their work first
-  PWB_CUDA(cudaStreamSynchronize(st));
   return PW_OK;
 }
 
