@@ -293,7 +293,9 @@ PW_API int pw_ctx_build_twin(pw_ctx* ctx);
  * until dExx < phi_tol.  Inner SCF loops restart the mixing history; with
  * tol_rho > 0 their criterion is the scfNorm of the potential change, as the
  * reference's nested loop has it.  The hybrid phase runs in FP64 (a mixed run
- * switches before it); the context keeps the ACE operator afterwards. */
+ * switches before it); the context keeps the ACE operator afterwards.  Other
+ * functionals run without an exchange term whatever pw_exx_set_mode chose
+ * (the mode is restored on return). */
 PW_API int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* eig_out, double* rho_out);
 
 /* Autotuner (no reference counterpart): times pw_hpsi on an internal block

@@ -1461,7 +1461,14 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
   const bool pbe = p->xc == PW_XC_PBE || hse;
   PWB_CHECK(p->xc == PW_XC_TETER93 || pbe, PW_EINVAL, "unknown exchange-correlation functional");
   if (pbe && ((rc = S.work2.alloc(nf * 16)) || (rc = S.grad.alloc(3 * nf * 8)))) return rc;
-  if (hse) ctx->exx_mode = PW_EXX_OFF;
+  // H*psi of a non-hybrid SCF carries no exchange term, whatever mode the
+  // context was left in (restored on return); the hybrid SCF starts without it
+  struct ExxModeGuard {
+    pw_ctx* c;
+    int mode;
+    ~ExxModeGuard() { c->exx_mode = mode; }
+  } exx_guard{ctx, ctx->exx_mode};
+  ctx->exx_mode = PW_EXX_OFF;
   double hse_frac = 0.0;
   auto potentials = [&](const double* rh, double* exc_out) -> int {
     int q = PW_OK;
@@ -1889,6 +1896,7 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
     }
     phi_it = std::min(phi_it, phimax);
     conv = phi_conv;
+    exx_guard.mode = ctx->exx_mode;   // the context keeps the final ACE operator
   }
   r->efock = efock;
   r->dexx = dexx;

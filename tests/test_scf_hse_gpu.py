@@ -31,3 +31,23 @@ def test_scf_hse06_matches_oracle(solver, mixed):
     assert abs(res["efock"] - g["efock"]) / nat < 1e-6, (res["efock"], g["efock"])
     assert np.abs(eig[:16] - np.array(g["eig"][:16])).max() < 1e-6
     assert abs(rho.sum() * np.prod(L) / rho.size - 32.0) < 1e-8
+
+
+def test_pbe_scf_after_hybrid_has_no_exchange_term():
+    """The context keeps the ACE operator after the hybrid SCF; a later PBE SCF
+    on it runs without the exchange term and lands on the oracle's PBE SCF
+    (tests/golden/si8_scf_pbe.json) to 1e-6 Ha/atom."""
+    from pwdft_develop_b200 import Context
+    g = json.loads((GOLD / "si8_scf_pbe.json").read_text())
+    L = np.array(g["length"])
+    pos = np.array(g["positions"])
+    c = Context(L, tuple(g["numGrid"]), tuple(g["numGridFine"]))
+    c.set_atoms([g["znuc"]] * len(pos), pos)
+    kw = dict(nocc=16, nextra=8, ecut=g["ecut"], solver="chebfsi", tol_efree=1e-8, eig_max_iter=4, eig_tol=1e-10,
+              max_iter=80)
+    res_h, _, _ = c.scf(xc="hse06", phi_max_iter=3, phi_tol=1e-6, **kw)
+    assert res_h["phi_iterations"] >= 1
+    res, eig, _ = c.scf(xc="pbe", **kw)
+    assert res["converged"] == 1
+    assert abs(res["efree"] - g["efree"]) / len(pos) < 1e-6, (res["efree"], g["efree"])
+    assert np.abs(eig[:16] - np.array(g["eig"][:16])).max() < 1e-6
