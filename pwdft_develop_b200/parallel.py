@@ -228,3 +228,31 @@ def chebfsi_dist(apply_h, Xb, nband: int, degree: int = 10, max_iter: int = 100,
         if res_max < tol:
             break
     return lam, Xb, it, res_max
+
+
+def gather_bands(Xb, nband: int):
+    """All bands on every rank from the band shards (band_range order):
+    (nband x ntot).  The exact-exchange orbitals are needed whole by every
+    rank; the reference passes them round the ranks with MPI_Bcast
+    (src/SCF/spinor.cpp:722-776), here one all-gather."""
+    import torch
+    import torch.distributed as dist
+    world, rank = _world()
+    if world == 1:
+        return Xb
+    ntot = Xb.shape[1]
+    bands = [band_range(nband, world, r) for r in range(world)]
+    nmax = max(n for _, n in bands)
+    buf = torch.zeros((nmax, ntot), dtype=Xb.dtype, device=Xb.device)
+    buf[:Xb.shape[0]] = Xb
+    parts = [torch.empty_like(buf) for _ in range(world)]
+    dist.all_gather(parts, buf)
+    return torch.cat([parts[r][:n] for r, (_, n) in enumerate(bands)], 0)
+
+
+def exx_apply_dist(set_phi, apply_exx, Xb, occ, nband: int):
+    """V_x of this rank's bands with the exchange orbitals of all ranks:
+    set_phi(all bands, occ) then apply_exx(this rank's bands) -- on a GPU,
+    Context.exx_set_phi and Context.exx_apply."""
+    set_phi(gather_bands(Xb, nband), occ)
+    return apply_exx(Xb)

@@ -127,3 +127,54 @@ def test_distributed_chebfsi_two_ranks_matches_one_rank_and_arpack():
         lam, it, res = out[world]
         assert res < 1e-9, (world, it, res)
         assert np.abs(lam[:14] - ref[:14]).max() < 1e-9, (world, lam[:14] - ref[:14])
+
+
+def _exx_worker(rank, world, port, q):
+    import torch
+    import torch.distributed as dist
+    from oracle import exx, pw
+    from pwdft_develop_b200.parallel import band_range, exx_apply_dist
+    if world > 1:
+        os.environ["MASTER_ADDR"] = "127.0.0.1"
+        os.environ["MASTER_PORT"] = str(port)
+        dist.init_process_group("gloo", rank=rank, world_size=world)
+    T, _ = pw.build_tables(*_si8(), (12, 12, 12), (24, 24, 24), seed_v=4)
+    nband = 9
+    X = pw.random_orthonormal_psi(T.dm.ntot, nband, 13)
+    occ = np.linspace(1.0, 0.2, nband)
+    kern, _ = exx.exx_kernel_r2c(T.dm, 5.0, mu=0.106)
+    s, n = band_range(nband, world, rank)
+    state = {}
+
+    def set_phi(phi, o):
+        state["phi"] = exx.set_phi(T.dm, phi.numpy())
+        state["occ"] = o
+
+    def apply_exx(Xb):
+        return torch.from_numpy(exx.add_mult_spinor_exx(T.dm, Xb.numpy(), state["phi"], kern, 0.25, state["occ"]))
+
+    out = exx_apply_dist(set_phi, apply_exx, torch.tensor(X[s:s + n]), occ, nband)
+    q.put((rank, s, out.numpy()))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def test_distributed_exchange_two_ranks_matches_one_rank():
+    """V_x on band shards with the exchange orbitals all-gathered (two gloo
+    ranks, uneven shards 5 + 4) equals the one-rank V_x bit for bit."""
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    res = {}
+    for world in (1, 2):
+        q = ctx.Queue()
+        port = _free_port()
+        procs = [ctx.Process(target=_exx_worker, args=(r, world, port, q)) for r in range(world)]
+        for p in procs:
+            p.start()
+        parts = sorted(q.get(timeout=300) for _ in range(world))
+        for p in procs:
+            p.join(timeout=120)
+            assert p.exitcode == 0
+        res[world] = np.concatenate([o for _, _, o in parts], 0)
+    assert np.array_equal(res[1], res[2])
