@@ -235,3 +235,25 @@ def test_scf_gspace_hse06():
     h = out["hse06"]
     assert h["efock"] < 0 and h["dexx"] < 1e-8 and h["phi_iterations"] >= 1
     assert h["efree"] < out["pbe"]["efree"]
+
+
+def test_scf_gspace_broyden_and_pbe():
+    """Broyden mixing and PBE on a sphere-cut context: Broyden (converged on
+    the density change) reaches the Anderson fixed point (E_free 1e-6
+    Ha/atom), and the PBE SCF lands within the discretisation difference
+    (5 mHa/atom) of the dual-grid PBE SCF of the same cell."""
+    from pwdft_develop_b200 import Context
+    L, z, pos = pw.make_crystal("Si", (1, 1, 1), 10.26, 0.02, 20261203 + 1)
+    nat = len(pos)
+    kw = dict(nocc=16, nextra=8, ecut=10.0, solver="chebfsi", eig_max_iter=4, eig_tol=1e-10, max_iter=80)
+    cx = _ctx(L, (32, 32, 32), 10.0, z=z, pos=pos)
+    ra, _, _ = cx.scf(tol_efree=1e-8, **kw)
+    rb, _, _ = cx.scf(mix="broyden", tol_rho=1e-13, tol_efree=1e-8, **kw)
+    assert ra["converged"] == 1 and rb["converged"] == 1
+    assert abs(ra["efree"] - rb["efree"]) / nat < 1e-6, (ra["efree"], rb["efree"])
+    rp, _, _ = cx.scf(xc="pbe", tol_efree=1e-8, **kw)
+    rs = Context(L, (16, 16, 16), (32, 32, 32))
+    rs.set_atoms([z] * nat, pos)
+    rr, _, _ = rs.scf(xc="pbe", tol_efree=1e-8, **kw)
+    assert rp["converged"] == 1 and rr["converged"] == 1
+    assert abs(rp["efree"] - rr["efree"]) / nat < 5e-3, (rp["efree"], rr["efree"])
