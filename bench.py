@@ -10,7 +10,10 @@ H*psi inside the timed region).  Under torchrun each rank runs its own
 the JSON line with the max-over-ranks time.
 
 --impl reference times the reference algorithm's CPU form (the FP64 NumPy
-restatement in oracle/, one band per worker process over all host cores).
+restatement in oracle/): one worker process per host core, tables built once
+per process, each step a bounded sample of single-band H*psi applications.
+The end of the JSON line carries a `summary` of the headline figures (FP32
+and FP64 sweeps, e2e, SCF mixed vs FP64, Gram tensor fraction, CPU baselines).
 """
 from __future__ import annotations
 
@@ -51,6 +54,18 @@ def si64_atoms():
                     pos.append((np.array([cx, cy, cz]) + f) * A_CELL)
     pos = np.array(pos) + rng.uniform(-0.02, 0.02, size=(64, 3))
     return np.array([2 * A_CELL] * 3), np.full(64, 14, np.int32), pos
+
+
+EXX_GOLDEN = ROOT / "tests" / "golden" / "si64_exx_energy.json"
+
+
+def seeded_orthonormal_bands(ntot: int, nb: int, seed: int) -> np.ndarray:
+    """nb Gaussian bands (Philox stream `seed`, drawn as an ntot x nb matrix)
+    orthonormalised by Cholesky-QR, returned as rows (nb, ntot)."""
+    rng = np.random.Generator(np.random.Philox(seed))
+    X = rng.standard_normal((ntot, nb))
+    U = np.linalg.cholesky(X.T @ X).T
+    return np.ascontiguousarray(np.linalg.solve(U.T, X.T))
 
 
 def synthetic_vtot(n):
@@ -172,35 +187,98 @@ class Clocks:
                 "samples": len(sm)}
 
 
-def oracle_sample_worker(args):
-    """One H*psi band through the FP64 NumPy restatement (CPU baseline)."""
-    os.environ["OMP_NUM_THREADS"] = "1"
-    band = args
+_W = {}
+
+
+_THREAD_VARS = ("OMP_NUM_THREADS", "OPENBLAS_NUM_THREADS", "MKL_NUM_THREADS")
+
+
+def _oracle_worker_init(backend: str = "numpy", workers: int = 1):
+    """Pool initializer: one thread per process, the Si64 tables built once
+    per worker (set-up, outside every timed region)."""
+    try:
+        from threadpoolctl import threadpool_limits
+        threadpool_limits(1)
+    except ImportError:
+        pass
     from oracle import pw
+    pw.set_fft_backend(backend, workers)
     L, z, pos = si64_atoms()
-    T, _ = pw.build_tables(L, 14, pos, NC, NF, vtot=synthetic_vtot(int(np.prod(NF))))
-    rng = np.random.Generator(np.random.Philox(SEED + 7 + band))
-    psi = rng.standard_normal((1, T.dm.ntot))
+    _W["T"], _ = pw.build_tables(L, 14, pos, NC, NF, vtot=synthetic_vtot(int(np.prod(NF))))
+
+
+def _oracle_worker_hpsi(job):
+    """`nb` single-band H*psi applications (FP64 NumPy restatement of the
+    reference path) on seeded bands; returns the time spent in mult_spinor."""
+    from oracle import pw
+    seed, nb = job
+    T = _W["T"]
+    rng = np.random.Generator(np.random.Philox(SEED + 7 + seed))
+    psi = rng.standard_normal((nb, T.dm.ntot))
     t0 = time.perf_counter()
-    pw.mult_spinor(T, psi)
+    for b in range(nb):
+        pw.mult_spinor(T, psi[b:b + 1])
     return time.perf_counter() - t0
 
 
-def cpu_baseline(bands: int = 4):
-    """Serial oracle on a bounded sample: `bands` single-band H*psi calls."""
+def _oracle_pool(ncores: int):
+    """`ncores` spawned worker processes, each limited to one BLAS / OpenMP
+    thread (the variables are set before the children import NumPy)."""
+    import multiprocessing as mp
+    saved = {k: os.environ.get(k) for k in _THREAD_VARS}
+    for k in _THREAD_VARS:
+        os.environ[k] = "1"
+    try:
+        return mp.get_context("spawn").Pool(ncores, initializer=_oracle_worker_init)
+    finally:
+        for k, v in saved.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+
+
+def _pool_sweep(pool, ncores: int, bands_per_core: int, seed0: int):
+    """One sample: every worker applies H to `bands_per_core` bands; wall time
+    of the whole sample (all workers busy at once) and the summed compute time."""
+    t0 = time.perf_counter()
+    ts = pool.map(_oracle_worker_hpsi, [(seed0 + i, bands_per_core) for i in range(ncores)], chunksize=1)
+    return time.perf_counter() - t0, sum(ts)
+
+
+def cpu_baseline(bands_per_core: int = 4):
+    """The FP64 NumPy restatement on all host cores (one process per core, one
+    band per call, tables built once per process), plus the same bands with
+    scipy.fft on `nproc` threads in one process (batched transforms, the
+    projector sums in NumPy)."""
+    ncores = os.cpu_count() or 1
+    with _oracle_pool(ncores) as pool:
+        _pool_sweep(pool, ncores, 1, 10_000)               # warm: imports, FFT plans
+        wall, busy = _pool_sweep(pool, ncores, bands_per_core, 0)
+    nb = ncores * bands_per_core
+    out = {"value": nb / wall, "unit": "bands/s", "cores": ncores, "kind": "port",
+           "sample": f"{nb} single-band H*psi applications of the Si64 workload through the FP64 NumPy restatement "
+                     f"of the reference path (oracle/pw.py), {ncores} processes x {bands_per_core} bands, tables "
+                     f"built once per process, {wall:.1f} s wall ({busy / nb * 1e3:.0f} ms per band per core)"}
+    # scipy.fft with nproc worker threads on a block of bands in one process
     from oracle import pw
     L, z, pos = si64_atoms()
     T, _ = pw.build_tables(L, 14, pos, NC, NF, vtot=synthetic_vtot(int(np.prod(NF))))
-    rng = np.random.Generator(np.random.Philox(SEED + 7))
-    psi = rng.standard_normal((bands, T.dm.ntot))
-    pw.mult_spinor(T, psi[:1])      # warm
-    t0 = time.perf_counter()
-    for b in range(bands):
-        pw.mult_spinor(T, psi[b:b + 1])
-    dt = time.perf_counter() - t0
-    return {"value": bands / dt, "unit": "bands/s", "cores": 1, "kind": "port",
-            "sample": f"{bands} single-band H*psi applications of the Si64 workload through the FP64 NumPy "
-                      f"restatement (oracle/pw.py), one thread, {dt:.1f} s"}
+    pw.set_fft_backend("scipy", ncores)
+    try:
+        rng = np.random.Generator(np.random.Philox(SEED + 7))
+        psi = rng.standard_normal((nb, T.dm.ntot))
+        pw.mult_spinor(T, psi[:2])
+        t0 = time.perf_counter()
+        for b0 in range(0, nb, 16):
+            pw.mult_spinor(T, psi[b0:b0 + 16])
+        dt = time.perf_counter() - t0
+    finally:
+        pw.set_fft_backend("numpy", 1)
+    out["scipy_fft"] = {"value": nb / dt, "unit": "bands/s", "threads": ncores,
+                        "sample": f"{nb} bands in blocks of 16 through the same restatement with scipy.fft "
+                                  f"(workers={ncores}), {dt:.1f} s"}
+    return out
 
 
 def scf_bench(device: int, max_iter: int = 60):
@@ -297,10 +375,9 @@ def exx_bench(device: int, reps: int = 3):
     from pwdft_develop_b200 import Context
     L, z, pos = si64_atoms()
     nb, nocc = 160, 128
-    g = torch.Generator(device="cuda").manual_seed(SEED + 7)
-    X64 = torch.randn((nb, NC[0] * NC[1] * NC[2]), dtype=torch.float64, device="cuda", generator=g)
-    R = torch.linalg.cholesky(X64 @ X64.T).T
-    X64 = torch.linalg.solve_triangular(R, X64, upper=True, left=True).contiguous()
+    gold = json.loads(EXX_GOLDEN.read_text()) if EXX_GOLDEN.exists() else None
+    X64 = torch.tensor(seeded_orthonormal_bands(NC[0] * NC[1] * NC[2], nb, gold["psi_seed"] if gold else SEED + 7),
+                       device="cuda")
     occ = np.zeros(nb)
     occ[:nocc] = 1.0
     out = {"workload": "Si64 48^3, 160 bands x 128 occupied orbitals, PBE0 fraction 0.25, divergence type 1",
@@ -340,6 +417,11 @@ def exx_bench(device: int, reps: int = 3):
         out[prec] = d
         c.close()
     out["exchange_energy_error_per_atom_f32"] = abs(energies["f32"] - energies["f64"]) / 64
+    if gold is not None:
+        # against the FP64 oracle's energy of the same bands (committed fixture)
+        out["oracle_exchange_energy"] = gold["exchange_energy"]
+        out["exchange_energy_error_per_atom_vs_oracle"] = {
+            p: abs(energies[p] - gold["exchange_energy"]) / gold["natom"] for p in ("f32", "f64")}
     return out
 
 
@@ -556,28 +638,116 @@ def gspace_bench(device: int, reps: int = 10):
     return out
 
 
+def f64_sweep_bench(device: int, steps: int, warmup: int):
+    """The same Si64 sweep in FP64 (the reference path's precision):
+    device-timed per 160-band sweep with the L2 flushed in between, and the
+    dominant kernel's achieved bandwidth on its algorithmic bytes."""
+    import torch
+    from pwdft_develop_b200 import Context
+    from pwdft_develop_b200.core import KERNEL_KINDS
+    L, z, pos = si64_atoms()
+    c = Context(L, NC, NF, precision="f64", device=device)
+    c.set_vtot(synthetic_vtot(c.ntotFine))
+    c.set_atoms(z, pos)
+    c.set_band_batch(NBAND)
+    g = torch.Generator(device="cuda").manual_seed(SEED)
+    X = torch.randn((NBAND, c.ntot), dtype=torch.float64, device="cuda", generator=g) / math.sqrt(c.ntot)
+    Y = torch.empty_like(X)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    for _ in range(warmup):
+        c.hpsi(X, out=Y)
+    torch.cuda.synchronize()
+    ms = 0.0
+    for _ in range(steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        c.hpsi(X, out=Y)
+        e1.record()
+        torch.cuda.synchronize()
+        ms += e0.elapsed_time(e1)
+    ms /= steps
+    c.profile(True)
+    for _ in range(steps):
+        flush.zero_()
+        c.hpsi(X, out=Y)
+    torch.cuda.synchronize()
+    kern = {}
+    for k in range(12):
+        t, n = c.profile_read(k)
+        if n:
+            kern[KERNEL_KINDS[k]] = {"launches": n, "avg_us": t / n * 1e3, "total_ms": t}
+    c.profile(False)
+    c.close()
+    dom = max((k for k in kern if k != "library_gemm"), key=lambda k: kern[k]["total_ms"])
+    kind = [k for k, v in KERNEL_KINDS.items() if v == dom][0]
+    alg = algorithmic_bytes(kind, NBAND // 2, 8, 0, 5, 0, len(pos))
+    peak, peak_kind = load_peaks()
+    ach = alg / (kern[dom]["avg_us"] * 1e-6) / 1e9
+    return {"value": NBAND / (ms / 1e3), "unit": "bands/s", "ms_per_sweep": ms, "dtype": "f64",
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
+                         "frac": ach / peak, "peak_source": peak_kind, "algorithmic_bytes_per_launch": alg,
+                         "avg_launch_us": kern[dom]["avg_us"]},
+            "kernels": kern}
+
+
+def summary(line: dict) -> dict:
+    """The headline figures of the line, gathered at its end."""
+    out = {"hpsi_f32_bands_per_s": line.get("value"), "e2e_bands_per_s": line.get("e2e", {}).get("value"),
+           "roofline_frac": line.get("roofline", {}).get("frac"),
+           "hpsi_model_frac": line.get("hpsi_model", {}).get("frac")}
+    if "f64_sweep" in line:
+        out["hpsi_f64_bands_per_s"] = line["f64_sweep"]["value"]
+        out["f64_roofline_frac"] = line["f64_sweep"]["roofline"]["frac"]
+    if "scf" in line:
+        sc = line["scf"]
+        out["scf_f64_s"] = sc["f64"]["seconds"]
+        out["scf_mixed_s"] = sc["mixed"]["seconds"]
+        out["scf_speedup_mixed_vs_f64"] = sc["speedup_mixed_vs_f64"]
+        out["scf_efree_agreement_per_atom"] = sc["efree_agreement_per_atom"]
+    if "exx" in line and "exchange_energy_error_per_atom_vs_oracle" in line["exx"]:
+        out["exx_energy_error_per_atom_vs_oracle"] = line["exx"]["exchange_energy_error_per_atom_vs_oracle"]
+    if "gram" in line:
+        out["gram_n480_tensor_frac"] = line["gram"]["n480"]["tensor_frac"]
+        out["gram_n160_tensor_frac"] = line["gram"]["n160"]["tensor_frac"]
+    if "cpu_baseline" in line:
+        cb = line["cpu_baseline"]
+        out["cpu_baseline_bands_per_s"] = cb["value"]
+        out["cpu_baseline_cores"] = cb["cores"]
+        if "scipy_fft" in cb:
+            out["cpu_scipy_fft_bands_per_s"] = cb["scipy_fft"]["value"]
+    return out
+
+
 def run_reference(args):
+    """The reference path's CPU form on the host cores: each step is a bounded
+    sample of the Si64 sweep -- every core applies H to `--ref-bands-per-core`
+    bands through the FP64 NumPy restatement (tables built once per process,
+    outside the timed steps)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    import multiprocessing as mp
     ncores = os.cpu_count() or 1
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(ncores) as pool:
+    bpc = args.ref_bands_per_core
+    with _oracle_pool(ncores) as pool:
         for w in range(args.warmup):
-            pool.map(oracle_sample_worker, list(range(ncores)))
-        t0 = time.perf_counter()
+            _pool_sweep(pool, ncores, 1, 100_000 + w * ncores)
+        wall = busy = 0.0
         for s in range(args.steps):
-            pool.map(oracle_sample_worker, [s * ncores + i for i in range(ncores)])
-        dt = time.perf_counter() - t0
-    v = args.steps * ncores / dt
+            dw, db = _pool_sweep(pool, ncores, bpc, s * ncores)
+            wall += dw
+            busy += db
+    nb = args.steps * ncores * bpc
+    v = nb / wall
     line = {"impl": "reference", "metric": "H*psi bands/s", "value": v, "unit": "bands/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": wall / args.steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": {"workload": WORKLOAD, "sample_bands_per_step": ncores},
+            "data": "synthetic", "config": {"workload": WORKLOAD, "sample_bands_per_step": ncores * bpc},
             "cpu_baseline": {"value": v, "unit": "bands/s", "cores": ncores, "kind": "port",
-                             "sample": f"each step: {ncores} single-band H*psi (one per process) through the FP64 "
-                                       f"NumPy restatement of the reference path (oracle/pw.py)"},
+                             "sample": f"each step: {ncores} processes x {bpc} single-band H*psi through the FP64 "
+                                       f"NumPy restatement of the reference path (oracle/pw.py), tables built "
+                                       f"once per process; {busy / nb * 1e3:.0f} ms per band per core"},
             "e2e": {"value": v, "unit": "bands/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -713,6 +883,9 @@ def run_ours(args):
                        "parallelism": f"band blocks, {world} replica(s)"},
             "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
+                         "traffic_source": (f"profiles/hpsi_si64_{prec}_dram_traffic.md (ncu dram__bytes of a "
+                                            f"separate capture, scaled to this batch; not measured in this run)"
+                                            if traffic is not None else None),
                          "algorithmic_bytes_per_launch": alg, "avg_launch_us": kern[dom_name]["avg_us"]},
             "hpsi_model": {"bytes_per_band": model, "achieved_GBs": model * value / world / 1e9,
                            "frac": model * value / world / 1e9 / peak},
@@ -723,6 +896,8 @@ def run_ours(args):
                     "h2d_bytes_per_step": bytes_io, "d2h_bytes_per_step": bytes_io},
             "clocks": ck,
         }
+        if prec == "f32" and args.f64_sweep and world == 1:
+            line["f64_sweep"] = f64_sweep_bench(local, args.steps, args.warmup)
         if args.scf and world == 1:
             line["scf"] = scf_bench(local)
         if args.exx and world == 1:
@@ -738,6 +913,7 @@ def run_ours(args):
             line["gram"] = gram_bench(local)
         if args.cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(args.cpu_bands)
+        line["summary"] = summary(line)     # last key: the headline figures in one place
         print(json.dumps(line), flush=True)
     ctx.close()
     if world > 1:
@@ -753,6 +929,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="f32", choices=["f32", "f64"])
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--no-f64-sweep", dest="f64_sweep", action="store_false", help="skip the FP64 sweep leg")
     ap.add_argument("--no-scf", dest="scf", action="store_false", help="skip the SCF time-to-solution leg")
     ap.add_argument("--no-exx", dest="exx", action="store_false", help="skip the hybrid-exchange leg")
     ap.add_argument("--no-kpoints", dest="kpoints", action="store_false", help="skip the k-point batch leg")
@@ -761,7 +938,8 @@ def main():
     ap.add_argument("--no-grams", dest="grams", action="store_false", help="skip the eigensolver Gram leg")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="default band batch and GEMM tiles (profiling runs: no tuning launches in the list)")
-    ap.add_argument("--cpu-bands", type=int, default=64)
+    ap.add_argument("--cpu-bands", type=int, default=4, help="CPU baseline: bands per host core")
+    ap.add_argument("--ref-bands-per-core", type=int, default=4, help="reference arm: bands per core per step")
     ap.add_argument("--bands", type=int, default=NBAND, help="band block size (profiling runs use a small block)")
     args = ap.parse_args()
     if args.impl == "reference":

@@ -447,10 +447,12 @@ PW_API int pw_scf_forces(pw_ctx* ctx, double* force, double* force_local, double
  * 16 MiB (ntot * 2 * sizeof(real) bytes) is rejected with PW_EINVAL; larger
  * band counts run in batches that fit.  The first call on a device looks up
  * the array's device address: make that first call before any stream
- * capture.  All calls share the array (each call writes every element it
- * reads, so nothing needs clearing between calls); calls that overlap on the
- * GPU -- concurrent streams, devices sharing the process' array on the same
- * device -- race on it and must be serialised by the caller. */
+ * capture.  The address is kept for the life of the process, so calls after a
+ * cudaDeviceReset of that device are not supported.  All calls share the array
+ * (each call writes every element it reads, so nothing needs clearing between
+ * calls); calls that overlap on the same GPU (several streams, or several
+ * contexts on one device) race on the array and must be serialised by the
+ * caller. */
 PW_API int pw_teter_precond_noalloc(pw_ctx* ctx, const void* r, int ld, void* w, int ldw, int nband, int accumulate,
                                     void* stream);
 

@@ -97,17 +97,43 @@ def ekin_teter(dm: Domain):
 # ---------------------------------------------------------------------------
 # FFTWExecute normalisations (src/SCF/fourier.cpp:695-764)
 # ---------------------------------------------------------------------------
+_FFT = {"backend": "numpy", "workers": 1}
+
+
+def set_fft_backend(backend: str = "numpy", workers: int = 1):
+    """FFT engine of r2c / c2r: "numpy" (pocketfft, one thread) or "scipy"
+    (scipy.fft's pocketfft with `workers` threads over the batch and axes).
+    Both compute the same transforms; the choice only changes the CPU time."""
+    if backend not in ("numpy", "scipy"):
+        raise ValueError(backend)
+    _FFT["backend"], _FFT["workers"] = backend, int(workers)
+
+
+def _rfftn(x):
+    if _FFT["backend"] == "scipy":
+        import scipy.fft as sf
+        return sf.rfftn(x, axes=(-3, -2, -1), workers=_FFT["workers"])
+    return np.fft.rfftn(x, axes=(-3, -2, -1))
+
+
+def _irfftn(X, s):
+    if _FFT["backend"] == "scipy":
+        import scipy.fft as sf
+        return sf.irfftn(X, s=s, axes=(-3, -2, -1), workers=_FFT["workers"])
+    return np.fft.irfftn(X, s=s, axes=(-3, -2, -1))
+
+
 def r2c(x, dm: Domain, fine: bool = False):
     """forward R2C with factor vol/N; x has shape (..., n2, n1, n0)."""
     N = dm.ntotFine if fine else dm.ntot
-    return np.fft.rfftn(x, axes=(-3, -2, -1)) * (dm.vol / N)
+    return _rfftn(x) * (dm.vol / N)
 
 
 def c2r(X, dm: Domain, fine: bool = False):
     """backward C2R (unnormalised FFTW) with factor 1/vol."""
     n = dm.numGridFine if fine else dm.numGrid
     N = n[0] * n[1] * n[2]
-    return np.fft.irfftn(X, s=(n[2], n[1], n[0]), axes=(-3, -2, -1)) * (N / dm.vol)
+    return _irfftn(X, (n[2], n[1], n[0])) * (N / dm.vol)
 
 
 # ---------------------------------------------------------------------------
@@ -403,10 +429,18 @@ def add_mult_spinor_fine_r2c(T: HamTables, psi: np.ndarray, a3: np.ndarray | Non
     upd = psiF * T.vtot[None, :]                                   # :449-456
     fac = dm.vol / dm.ntotFine
     for atom_pp in T.pseudo:                                       # :459-482
+        idx = atom_pp[0].idx
+        # one index set per atom: gather once; a set without repeated points
+        # takes a plain indexed add (the same single addition per point)
+        uniq = len(np.unique(idx)) == len(idx)
+        sub = psiF[:, idx]
         for pp in atom_pp:
-            w = psiF[:, pp.idx] @ pp.val[:, 0]
+            w = sub @ pp.val[:, 0]
             w = w * fac * pp.wgt
-            np.add.at(upd, (slice(None), pp.idx), w[:, None] * pp.val[None, :, 0])
+            if uniq and pp.idx is idx:
+                upd[:, idx] += w[:, None] * pp.val[None, :, 0]
+            else:
+                np.add.at(upd, (slice(None), pp.idx), w[:, None] * pp.val[None, :, 0])
     Xc = Xc * T.ekin[None]                                         # :485-488
     Yf = r2c(upd.reshape(nb, N2, N1, N0), dm, fine=True)           # :493-498
     Xc = Xc.reshape(nb, -1) + T.ip.f2c(Yf.reshape(nb, -1))         # :501-506
@@ -430,10 +464,30 @@ def add_teter_precond(T: HamTables, r: np.ndarray, a3: np.ndarray | None = None)
     return a3
 
 
-def mult_spinor(T: HamTables, psi: np.ndarray):
+def wfn_ecut_filter(T: HamTables, psi: np.ndarray, ecut: float):
+    """The wavefunction cut-off filter of ``KohnSham::MultSpinor``
+    (src/SCF/hamiltonian.cpp:3090-3116 on psi, :3240-3265 on a3): forward R2C,
+    coefficients with gkkR2C = |G|^2/2 > ecut set to zero, backward C2R (the
+    two normalisations cancel).  Switched on for CheFSI with
+    wfn_cutoff_ = Ecut_Wavefunction (hamiltonian.cpp:316-321)."""
+    dm = T.dm
+    n0, n1, n2 = dm.numGrid
+    nb = psi.shape[0]
+    X = r2c(psi.reshape(nb, n2, n1, n0), dm)
+    X[:, T.ekin > ecut] = 0.0
+    return c2r(X, dm).reshape(nb, -1)
+
+
+def mult_spinor(T: HamTables, psi: np.ndarray, wfn_ecut: float | None = None):
     """``KohnSham::MultSpinor`` (src/SCF/hamiltonian.cpp:3059-3268) without
-    hybrid exchange and without the wavefunction filter: a3 = 0, then a2."""
-    return add_mult_spinor_fine_r2c(T, psi, np.zeros_like(psi))
+    hybrid exchange: a3 = 0, then a2.  With ``wfn_ecut`` the exit filter is
+    applied to a3 (:3240-3265), i.e. a3 = P H psi; the reference's first call
+    also replaces psi by P psi in place (:3090-3116), which a caller does with
+    ``wfn_ecut_filter`` before the first application."""
+    out = add_mult_spinor_fine_r2c(T, psi, np.zeros_like(psi))
+    if wfn_ecut is not None:
+        out = wfn_ecut_filter(T, out, wfn_ecut)
+    return out
 
 
 # ---------------------------------------------------------------------------

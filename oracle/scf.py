@@ -23,8 +23,13 @@ Test infrastructure (see ``oracle/__init__.py``).  Follows:
     then the semilocal HSE06 (oracle/hse.py) with phi iterations over an ACE
     operator (oracle/exx.py), Fock energies and dExx
   * initial density from the pseudocharge  src/SCF/scf.cpp:232-255
-The eigensolver is ARPACK (scipy eigsh) on the FP64 operator: the converged SCF
-fixed point does not depend on the eigensolver.
+The eigensolver is ARPACK (scipy eigsh) on the FP64 operator, or, for large
+cells, scipy's block LOBPCG over a caller-supplied block H*psi
+(``set_block_hx``, e.g. a process pool): the converged SCF fixed point does not
+depend on the eigensolver.  With ``wfn_ecut`` the SCF runs on the filtered
+operator of the reference's CheFSI path (KohnSham::MultSpinor's wavefunction
+cut-off filter, hamiltonian.cpp:316-321, 3090-3116, 3240-3265): P H P on the
+span of P, the complement shifted out of the wanted spectrum.
 """
 from __future__ import annotations
 
@@ -286,16 +291,49 @@ class SCFResult:
     phi_iterations: int = 0
 
 
-def _eigsh(T: pw.HamTables, nband: int, v0=None, tol=1e-11, xi=None):
-    """Lowest eigenpairs of H (plus the ACE term -xi^T xi when xi is given)."""
+_BLOCK = {"hx": None, "tol": 1e-8, "maxiter": 400}
+NULL_SHIFT = 100.0      # Ha: where the filtered operator puts the span of I - P
+
+
+def set_block_hx(hx_block=None, tol: float = 1e-8, maxiter: int = 400):
+    """Use block LOBPCG (scipy) with ``hx_block(T, rows) -> H rows`` (rows:
+    nb x ntot) instead of ARPACK; None restores ARPACK.  ``tol`` is the
+    residual tolerance of the last SCF steps (earlier steps use a looser one)."""
+    _BLOCK["hx"], _BLOCK["tol"], _BLOCK["maxiter"] = hx_block, tol, maxiter
+
+
+def _operator(T: pw.HamTables, xi=None, wfn_ecut=None, hx_block=None):
+    """rows -> rows of H (+ ACE), or of P H P + NULL_SHIFT (I - P) with the filter."""
+    def hx(rows):
+        rows = np.ascontiguousarray(rows)
+        f = pw.wfn_ecut_filter(T, rows, wfn_ecut) if wfn_ecut is not None else rows
+        out = hx_block(T, f) if hx_block is not None else pw.mult_spinor(T, f)
+        if xi is not None:
+            out = out - (f @ xi.T) @ xi
+        if wfn_ecut is not None:
+            out = pw.wfn_ecut_filter(T, out, wfn_ecut) + NULL_SHIFT * (rows - f)
+        return out
+    return hx
+
+
+def _lobpcg(T: pw.HamTables, nband: int, X0: np.ndarray, tol: float, xi=None, wfn_ecut=None):
+    """Lowest eigenpairs by scipy's block LOBPCG (Teter preconditioner, the
+    block H*psi of set_block_hx), started from X0 (nband x ntot)."""
+    from scipy.sparse.linalg import lobpcg
+    hx = _operator(T, xi, wfn_ecut, _BLOCK["hx"])
+    A = lambda X: hx(np.asarray(X).T).T                         # noqa: E731
+    M = lambda R: pw.add_teter_precond(T, np.ascontiguousarray(np.asarray(R).T)).T   # noqa: E731
+    w, V = lobpcg(A, np.ascontiguousarray(X0.T), M=M, tol=tol, maxiter=_BLOCK["maxiter"], largest=False)
+    o = np.argsort(w)
+    return w[o], np.ascontiguousarray(V[:, o].T)
+
+
+def _eigsh(T: pw.HamTables, nband: int, v0=None, tol=1e-11, xi=None, wfn_ecut=None):
+    """Lowest eigenpairs of H (plus the ACE term -xi^T xi when xi is given;
+    the filtered operator with wfn_ecut)."""
     from scipy.sparse.linalg import LinearOperator, eigsh
     n = T.dm.ntot
-
-    def hx(rows):
-        out = pw.mult_spinor(T, np.ascontiguousarray(rows))
-        if xi is not None:
-            out = out - (rows @ xi.T) @ xi
-        return out
+    hx = _operator(T, xi, wfn_ecut)
 
     def mv(x):
         return hx(np.asarray(x).reshape(1, n)).reshape(-1)
@@ -313,7 +351,7 @@ def scf(L, znuc, pos, numGrid, numGridFine, nocc: int, nextra: int, ecut: float,
         temperature: float = 300.0, tol_efree: float = 1e-7, max_iter: int = 60, mix_dim: int = 8,
         mix_step: float = 0.7, eig_tol: float = 1e-11, verbose: bool = False, xc: str = "teter93",
         mix: str = "anderson", tol_rho: float | None = None, phi_max_iter: int = 10,
-        phi_tol: float = 1e-6) -> SCFResult:
+        phi_tol: float = 1e-6, wfn_ecut: float | None = None, seed: int = 20261203) -> SCFResult:
     """Restated SCF::Iterate with potential Anderson mixing; converges when
     |E_free - E_Harris| / N_atom < tol_efree (the reference's efreeDifPerAtom,
     scf.cpp:467).  xc = "hse06": the nested hybrid scheme (PBE SCF, then phi
@@ -362,8 +400,17 @@ def scf(L, znuc, pos, numGrid, numGridFine, nocc: int, nextra: int, ecut: float,
     def step(it, dv_hist, df_hist, bst):
         nonlocal vtot, rho, exc, vxc, vh, psi, res
         T.vtot = vtot
-        v0 = psi[0] if psi is not None else None
-        eig, psi = _eigsh(T, nband, v0=v0, tol=eig_tol, xi=xi)
+        if _BLOCK["hx"] is not None:
+            X0 = psi if psi is not None else pw.random_orthonormal_psi(dm.ntot, nband, seed)
+            if wfn_ecut is not None:
+                X0 = pw.wfn_ecut_filter(T, X0, wfn_ecut)
+            # loose residual tolerance while the potential still moves
+            prev = hist[-1]["dif"] if hist else 1.0
+            tol = float(np.clip(1e-4 * math.sqrt(prev), _BLOCK["tol"], 1e-5))
+            eig, psi = _lobpcg(T, nband, X0, tol, xi=xi, wfn_ecut=wfn_ecut)
+        else:
+            v0 = psi[0] if psi is not None else None
+            eig, psi = _eigsh(T, nband, v0=v0, tol=eig_tol, xi=xi, wfn_ecut=wfn_ecut)
         occ, ef = occupations(eig, nocc, tbeta)
         # Harris energy with the input density / potentials (scf.cpp:1987-2140)
         ekin_b = float(np.sum(2 * eig * occ))

@@ -1,7 +1,9 @@
 """Seeded batches of independent, uneven cells (Si diamond 8/16/64 atoms, fcc
 Al 4/32 atoms) for the batched H*psi path: geometry, cut-off, grid and band
 count per cell.  The grid of a cell is the smallest coarse grid built into the
-library that resolves sqrt(2 Ecut) L / pi points per direction (at least 20)."""
+library that resolves sqrt(2 Ecut) L / pi points per direction (at least 20);
+one cell in four (seeded) is forced to a larger built grid, up to 60^3, so the
+batch spans the 20^3 - 60^3 range."""
 from __future__ import annotations
 
 import math
@@ -21,7 +23,7 @@ KINDS = {
     "Al4": (13, 3, A_AL, _AL_BASE, (1, 1, 1)),
     "Al32": (13, 3, A_AL, _AL_BASE, (2, 2, 2)),
 }
-CUBIC = (20, 24, 30, 32, 36, 40, 48)
+CUBIC = (20, 24, 30, 32, 36, 40, 48, 60)
 ELONGATED = ((40, 20, 20), (48, 24, 24))
 
 
@@ -57,6 +59,14 @@ def uneven_cells(n: int = 48, seed: int = 20261203 + 3):
         pos = np.array(pos) + rng.uniform(-0.02, 0.02, size=(len(pos), 3))
         L = (a * reps[0], a * reps[1], a * reps[2])
         nc = _grid(L, ecut)
+        if rng.random() < 0.25:
+            # forced to a larger grid than the cut-off needs
+            if nc in ELONGATED:
+                nc = ELONGATED[-1]
+            else:
+                bigger = [g for g in CUBIC if g >= nc[0]]
+                g = bigger[int(rng.integers(len(bigger)))]
+                nc = (g, g, g)
         nocc = zval * len(pos) // 2
         nband = nocc + max(6, nocc // 4)
         nband += nband % 2

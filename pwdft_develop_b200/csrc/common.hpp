@@ -1,6 +1,7 @@
 // Shared declarations for the pwdft_b200 native library.
 #pragma once
 #include <cuda_runtime.h>
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <string>
@@ -30,6 +31,20 @@ void set_error(const std::string& msg);
       return (code);                                                                \
     }                                                                               \
   } while (0)
+
+// A one-time set-up step (kernel attributes) tracked per device: cudaFuncSetAttribute
+// applies to the current device only, so a process that drives several GPUs
+// repeats the step once on each of them.
+struct PerDeviceOnce {
+  std::atomic<unsigned long long> bits{0};
+  static int dev() {
+    int d = 0;
+    cudaGetDevice(&d);
+    return d & 63;
+  }
+  bool done() const { return (bits.load(std::memory_order_acquire) >> dev()) & 1ull; }
+  void mark() { bits.fetch_or(1ull << dev(), std::memory_order_release); }
+};
 
 // Device buffer owned by a context.
 struct DevBuf {

@@ -466,10 +466,10 @@ static int num_sms() {
 template <int BN> static int launch_bn(const SplitOperand& A, const SplitOperand& B, const GemmArgs& g, int nsplit,
                                        cudaStream_t st) {
   using SM = GemmSmem<BN>;
-  static bool attr = false;
-  if (!attr) {
+  static PerDeviceOnce attr;
+  if (!attr.done()) {
     PWB_CUDA(cudaFuncSetAttribute(k_gemm_tn<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, SM::BYTES));
-    attr = true;
+    attr.mark();
   }
   CUtensorMap ah, al, bh, bl;
   int rc;

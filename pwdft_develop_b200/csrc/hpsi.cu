@@ -128,7 +128,11 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[PWB_NOALLOC_SCR
 
 namespace {
 std::mutex g_noalloc_mu;
-void* g_noalloc_addr[64] = {nullptr};   // device address of g_noalloc_scratch, per device ordinal
+// Device address of g_noalloc_scratch per device ordinal, taken once and kept
+// for the life of the process.  A cudaDeviceReset (or anything else that
+// replaces the device's primary context) invalidates it: calls after such a
+// reset are not supported.
+void* g_noalloc_addr[64] = {nullptr};
 }  // namespace
 
 extern "C" int pw_teter_precond_noalloc(pw_ctx* ctx, const void* r, int ld, void* w, int ldw, int nband,
@@ -153,6 +157,7 @@ extern "C" int pw_teter_precond_noalloc(pw_ctx* ctx, const void* r, int ld, void
       void* ptr = nullptr;
       cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
       if (e != cudaSuccess || !ptr) {
+        cudaGetLastError();     // clear it: a later, unrelated check must not report this failure as its own
         set_error(std::string("cudaGetSymbolAddress(g_noalloc_scratch) failed: ") + cudaGetErrorString(e));
         return PW_ECUDA;
       }

@@ -1384,8 +1384,8 @@ struct Plan {
   }
 
   static int set_attrs() {
-    static bool done = false;
-    if (done) return PW_OK;
+    static PerDeviceOnce once;
+    if (once.done()) return PW_OK;
     const int cr = chunk_rows();
     PWB_CUDA(cudaFuncSetAttribute(k_fplane<T, NF0, NF1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_fplane(cr)));
     PWB_CUDA(cudaFuncSetAttribute(k_fplane<T, NF0, NF1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_fplane(cr)));
@@ -1397,7 +1397,7 @@ struct Plan {
     PWB_CUDA(cudaFuncSetAttribute(k_floc<T, NF0, NF1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_floc()));
     PWB_CUDA(cudaFuncSetAttribute(k_floc2<T, NF0, NF1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_floc2()));
     PWB_CUDA(cudaFuncSetAttribute(k_floc<T, NF0, NF1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_floc()));
-    done = true;
+    once.mark();
     return PW_OK;
   }
 
@@ -1497,11 +1497,11 @@ struct Plan {
   static int exx_apply(pw_ctx* c, const T* psi, int ld, int nb, T* out, int ldo, int accumulate, cudaStream_t st) {
     int rc = set_attrs();
     if (rc) return rc;
-    static bool attr = false;
-    if (!attr) {
+    static PerDeviceOnce attr;
+    if (!attr.done()) {
       PWB_CUDA(cudaFuncSetAttribute(k_exx_fwd<T, N0, N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_cxy()));
       PWB_CUDA(cudaFuncSetAttribute(k_exx_inv<T, N0, N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_exx_inv()));
-      attr = true;
+      attr.mark();
     }
     const int nphi = c->exx_nphi;
     if (nphi == 0 || nb == 0) {
@@ -1579,10 +1579,10 @@ struct Plan {
                            double* rho, cudaStream_t st) {
     int rc = set_attrs();
     if (rc) return rc;
-    static bool attr = false;
-    if (!attr) {
+    static PerDeviceOnce attr;
+    if (!attr.done()) {
       PWB_CUDA(cudaFuncSetAttribute(k_fdens<T, NF0, NF1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_floc()));
-      attr = true;
+      attr.mark();
     }
     V* AD = reinterpret_cast<V*>(c->s_ad.p);
     V* BC = reinterpret_cast<V*>(c->s_bc.p);
@@ -1641,11 +1641,11 @@ struct Plan {
                           cudaStream_t st, int fpk = 1 << 30, const T* ekin_all = nullptr, const V* qk_all = nullptr) {
     int rc = set_attrs();
     if (rc) return rc;
-    static bool attr = false;
-    if (!attr) {
+    static PerDeviceOnce attr;
+    if (!attr.done()) {
       PWB_CUDA(cudaFuncSetAttribute(k_cxy_fwd<T, N0, N1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_cxy()));
       PWB_CUDA(cudaFuncSetAttribute(k_cxy_inv<T, N0, N1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_cxy()));
-      attr = true;
+      attr.mark();
     }
     V* AD = reinterpret_cast<V*>(c->s_ad.p);
     V* K = reinterpret_cast<V*>(c->s_k.p);
@@ -1726,10 +1726,10 @@ struct Plan {
                        const long* d_pbo, const int* d_pnp, int nproj, const double kv[3], V* Qout, cudaStream_t st) {
     int rc = set_attrs();
     if (rc) return rc;
-    static bool attr = false;
-    if (!attr) {
+    static PerDeviceOnce attr;
+    if (!attr.done()) {
       PWB_CUDA(cudaFuncSetAttribute(k_cxy_inv<T, N0, N1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_cxy()));
-      attr = true;
+      attr.mark();
     }
     const int cap = c->pair_cap;                 // complex fields per pass
     const long nf = c->ntotf;
@@ -1827,8 +1827,8 @@ struct Plan {
   static size_t sm_gs_zinv() { return sizeof(V) * ((size_t)NF2 * (N0 + 1) + NF2); }
   static size_t sm_gs_zfwd() { return sizeof(V) * ((size_t)NF2 * (2 * (N0 + 1) + 1) + NF2); }
   static int set_attrs_gs() {
-    static bool done = false;
-    if (done) return PW_OK;
+    static PerDeviceOnce once;
+    if (once.done()) return PW_OK;
     int rc = set_attrs();
     if (rc) return rc;
     PWB_CUDA(cudaFuncSetAttribute(k_gs_zinv<T, N0, N1, NF2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1836,7 +1836,7 @@ struct Plan {
     PWB_CUDA(cudaFuncSetAttribute(k_gs_zfwd<T, N0, N1, NF2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)sm_gs_zfwd()));
     PWB_CUDA(cudaFuncSetAttribute(k_fdens<T, NF0, NF1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_floc()));
-    done = true;
+    once.mark();
     return PW_OK;
   }
 

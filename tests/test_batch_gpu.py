@@ -55,3 +55,42 @@ def test_batch_and_graph_match_individual_calls():
     for o, r in zip(outs, refs):
         assert torch.equal(o, r)
     g.close()
+
+
+def test_batch_cells_match_oracle():
+    """Cells of the uneven batch, applied together, against the FP64 oracle
+    (same cell, grid, potential and bands): FP64 1e-12, FP32 1e-5 relative."""
+    import torch
+    from pwdft_develop_b200 import CellBatch
+    from pwdft_develop_b200.cells import uneven_cells
+
+    from oracle import pw
+    cells = uneven_cells(48)
+    seen, pick = set(), []
+    for c in cells:     # one cell of each kind, the smaller grids (oracle cost)
+        if c["kind"] not in seen and c["numGrid"][0] <= 40:
+            seen.add(c["kind"])
+            pick.append(c)
+    precs = ["f64" if i % 2 else "f32" for i in range(len(pick))]
+    ctxs, psis, outs, refs = [], [], [], []
+    from pwdft_develop_b200 import Context
+    for i, (cell, prec) in enumerate(zip(pick, precs)):
+        T, _ = pw.build_tables(cell["length"], cell["znuc"], cell["positions"], cell["numGrid"],
+                               cell["numGridFine"], seed_v=31 + i)
+        nb = min(cell["nband"], 10)
+        psi = pw.random_orthonormal_psi(T.dm.ntot, nb, 41 + i)
+        refs.append(pw.mult_spinor(T, psi))
+        c = Context(cell["length"], cell["numGrid"], cell["numGridFine"], precision=prec)
+        c.set_atoms([cell["znuc"]] * len(cell["positions"]), cell["positions"])
+        c.set_vtot(T.vtot)
+        x = torch.tensor(psi, dtype=c.torch_dtype, device="cuda")
+        ctxs.append(c)
+        psis.append(x)
+        outs.append(torch.empty_like(x))
+    CellBatch(ctxs, psis, outs).hpsi()
+    torch.cuda.synchronize()
+    for o, r, prec, cell in zip(outs, refs, precs, pick):
+        err = np.abs(o.double().cpu().numpy() - r).max() / np.abs(r).max()
+        assert err <= (1e-12 if prec == "f64" else 1e-5), (cell["kind"], cell["numGrid"], prec, err)
+    for c in ctxs:
+        c.close()

@@ -119,3 +119,33 @@ def test_exx_energy(prec):
     else:
         assert abs(e_full - e_ref) / nat <= 1e-6, (e_full - e_ref) / nat
         assert abs(e_ace - e_ref) / nat <= 1e-6, (e_ace - e_ref) / nat
+
+
+@pytest.mark.parametrize("prec,tol", [("f64", 1e-10), ("f32", 1e-6)])
+def test_exx_energy_si64_matches_oracle(prec, tol):
+    """The hybrid-exchange configuration at size: Si64 (48^3), 160 bands of
+    which 128 occupied, PBE0 kernel; the exchange energy against the FP64
+    oracle's (tests/golden/si64_exx_energy.json, make_si64_exx_golden.py),
+    per atom: 1e-10 Ha in FP64, 1e-6 Ha in FP32 (the energy parity bar)."""
+    import json
+    from pathlib import Path
+
+    import torch
+    from pwdft_develop_b200 import Context
+    p = Path(__file__).resolve().parent / "golden" / "si64_exx_energy.json"
+    if not p.exists():
+        pytest.skip("si64_exx_energy.json missing")
+    g = json.loads(p.read_text())
+    L, z, pos = pw.make_crystal("Si", (2, 2, 2), 10.26, 0.02, 20261203 + 2)
+    nc = tuple(g["numGrid"])
+    psi = pw.random_orthonormal_psi(int(np.prod(nc)), g["nband"], g["psi_seed"])
+    occ = np.zeros(g["nband"])
+    occ[: g["nocc"]] = 1.0
+    c = Context(L, nc, tuple(2 * n for n in nc), precision=prec)
+    c.set_atoms([z] * len(pos), pos)
+    c.exx_setup(g["exx_fraction"], g["screen_mu"], g["divergence_type"], g["ecut"])
+    X = torch.tensor(psi, dtype=c.torch_dtype, device="cuda")
+    c.exx_set_phi(X, occ)
+    e = c.exx_energy(X, occ)
+    assert abs(e - g["exchange_energy"]) / g["natom"] <= tol, (e, g["exchange_energy"])
+    c.close()

@@ -118,3 +118,21 @@ def test_scf_si8_small_matches_oracle(solver, mixed):
     nat = len(pos)
     assert abs(res["efree"] - g["efree"]) / nat < 1e-6
     assert np.abs(eig[:16] - np.array(g["eig"][:16])).max() < 1e-6
+
+
+@pytest.mark.parametrize("solver,mixed", [("lobpcg", False), ("chebfsi", False), ("chebfsi", True)])
+def test_scf_si8_full_matches_oracle(solver, mixed):
+    """The Si8 configuration at its stated size: 24^3 / 48^3 grids, Ecut 10 Ha,
+    16 occupied + 8 extra bands, Anderson mixing, against the oracle's
+    converged SCF: E_free within 1e-6 Ha/atom, occupied eigenvalues 1e-6 Ha."""
+    g = _gold("full")
+    L = np.array(g["length"])
+    pos = np.array(g["positions"])
+    c = _ctx(L, g["znuc"], pos, tuple(g["numGrid"]), tuple(g["numGridFine"]))
+    res, eig, rho = c.scf(nocc=16, nextra=8, ecut=g["ecut"], solver=solver, mixed=mixed, tol_efree=1e-8,
+                          eig_max_iter=4, eig_tol=1e-10, max_iter=80, cheby_degree=12, refine_threshold=1e-6)
+    assert res["converged"] == 1
+    nat = len(pos)
+    assert abs(res["efree"] - g["efree"]) / nat < 1e-6, (res["efree"], g["efree"])
+    assert np.abs(eig[:16] - np.array(g["eig"][:16])).max() < 1e-6
+    c.close()

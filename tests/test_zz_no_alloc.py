@@ -45,6 +45,15 @@ def test_noalloc_matches_allocating_entry(prec, nc, nb):
         torch.cuda.synchronize()
         err = float((w_new.double() - w_ref.double()).abs().max() / w_ref.double().abs().max())
         assert err <= TOL[prec], (call, err)
+    # after the calls above have loaded every kernel, a further call leaves the
+    # device's free memory unchanged: it allocates nothing
+    from pwdft_develop_b200._lib import check, lib
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    check(lib.pw_teter_precond_noalloc(c.handle, C.c_void_p(r.data_ptr()), c.ntot, C.c_void_p(w_new.data_ptr()),
+                                       c.ntot, nb, 0, C.c_void_p(0)))
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
     # accumulate semantics: w += T r
     r = torch.randn((nb, c.ntot), dtype=dt, device="cuda", generator=g)
     base = torch.randn_like(r)
