@@ -93,6 +93,18 @@ PW_API int pw_set_gemm_mode(pw_ctx* ctx, int mode, int terms);
 /* When enabled, every H*psi call synchronises and returns PW_ETIMEOUT if a
  * bounded device-side pipeline wait gave up (default off). */
 PW_API int pw_set_check_errors(pw_ctx* ctx, int enable);
+/* Limit of every bounded wait inside the tensor-core GEMM pipeline on the
+ * context's device (all contexts of that device; default 2 s).  On timeout a
+ * kernel records an error code, waits (at least 2 s) for the copies and MMAs it
+ * issued itself, frees its tensor memory and returns; the next checked call
+ * reports PW_ETIMEOUT.  No reference counterpart (the reference has no device
+ * waits). */
+PW_API int pw_set_wait_limit(pw_ctx* ctx, double seconds);
+/* Exercises that failure path without a fault: one thread waits, with the
+ * given limit (at most 10 s), on a barrier that nothing releases, records the
+ * timeout and returns; the call returns PW_ETIMEOUT and clears the record, and
+ * the context stays usable.  No reference counterpart. */
+PW_API int pw_wait_probe(pw_ctx* ctx, double seconds);
 
 /* H*psi for nband bands: hpsi (+)= (-1/2 Laplacian + V_loc + V_nl) psi.
  * Replaces Spinor::AddMultSpinorFineR2C(fft, ekin, vtot, pseudo, a3)
@@ -111,6 +123,25 @@ PW_API int pw_hpsi_host(pw_ctx* ctx, const void* psi, int ld, void* hpsi, int ld
                  int accumulate);
 /* Bands per pw_hpsi_host chunk (rounded up to even; 0: the default 32). */
 PW_API int pw_set_host_chunk(pw_ctx* ctx, int nband);
+
+/* Wavefunction cut-off filter of KohnSham::MultSpinor, which the reference
+ * switches on for PW_Solver CheFSI with the cut-off Ecut_Wavefunction
+ * (set_wfn_filter(PWDFT_Cheby_apply_wfn_ecut_filt, 1, ecutWavefunction),
+ * src/SCF/hamiltonian.cpp:316-321; PWDFT_Cheby_apply_wfn_ecut_filt defaults to
+ * 1, src/esdf.cpp:2719).  P = C2R o (zero every coefficient with
+ * gkkR2C = |G|^2/2 > ecut) o R2C.  While enabled, an overwriting pw_hpsi
+ * (accumulate = 0, MultSpinor) returns P H psi -- the exit filter of
+ * hamiltonian.cpp:3240-3265, fused into the z-fold kernel and into the
+ * store-side projector / ACE matrices (P Q, P xi, built once per geometry); an
+ * accumulating call (AddMultSpinorFineR2C) is not filtered, as in the
+ * reference.  The reference's first MultSpinor call also replaces psi by
+ * P psi in place (hamiltonian.cpp:3090-3116): pw_wfn_filter does that step
+ * (pw_eigsolve and pw_scf_run do it on their start blocks; the C++ mirror's
+ * Hamiltonian::MultSpinor does it on its first call).  Real-space contexts;
+ * enable = 0 switches the filter off. */
+PW_API int pw_set_wfn_filter(pw_ctx* ctx, int enable, double ecut);
+/* X <- P X in place for nband device columns (needs pw_set_wfn_filter). */
+PW_API int pw_wfn_filter(pw_ctx* ctx, void* X, int ld, int nband, void* stream);
 
 /* Teter preconditioner: w (+)= C2R(teter * R2C(r)).  Replaces
  * Spinor::AddTeterPrecond(Fourier*, DblNumVec& teter, NumTns<Real>& a3)
@@ -259,6 +290,9 @@ typedef struct pw_scf_params {
                                instead of the E_free - E_Harris test */
   int phi_max_iter;         /* PW_XC_HSE06: outer phi (ACE) iterations, Hybrid_Phi_MaxIter (0: 10) */
   double phi_tol;           /* PW_XC_HSE06: converged when dExx = 4 |fock1 - (fock0 + fock2) / 2| < phi_tol */
+  int no_wfn_filter;        /* PW_SOLVER_CHEBFSI: 0 (default) runs H*psi with the wavefunction cut-off filter at
+                               ecut, as the reference's CheFSI does (PWDFT_Cheby_apply_wfn_ecut_filt 1); 1 runs
+                               the unfiltered operator (PWDFT_Cheby_apply_wfn_ecut_filt 0).  Other solvers: no filter */
 } pw_scf_params;
 enum { PW_MIX_ANDERSON = 0, PW_MIX_BROYDEN = 1 };
 

@@ -8,7 +8,9 @@
 //   * NumTns<Real>(ntot, ncom = 1, nband) column-major wavefunction blocks
 //     (include/spinor.hpp:80): `BandBlock` is a non-owning view of the same layout.
 //   * Hamiltonian::MultSpinor(Spinor&, NumTns<Real>& a3, Fourier&)
-//     (include/hamiltonian.hpp:261): `Hamiltonian::MultSpinor` (a3 overwritten).
+//     (include/hamiltonian.hpp:261): `Hamiltonian::MultSpinor` (a3 overwritten),
+//     with the wavefunction filter state of KohnSham::set_wfn_filter
+//     (include/hamiltonian.hpp:347-356).
 //   * Spinor::AddTeterPrecond(Fourier*, teter, a3) (include/spinor.hpp:327):
 //     `Hamiltonian::AddTeterPrecond` (a3 accumulated).
 //   * EigenSolver::{LOBPCGSolveReal, PPCGSolveReal, DavidsonSolveReal} and
@@ -89,9 +91,30 @@ class Hamiltonian {
   // KohnSham::vtot_ (fine grid, host)
   void SetVtot(const double* vtot_fine) { check(pw_set_vtot(ctx_, vtot_fine)); }
 
-  // a3 := H psi (host blocks; FP64 contexts)
+  // KohnSham::set_wfn_filter(apply_filter, apply_first, wfn_cutoff)
+  // (include/hamiltonian.hpp:347-352): with apply_filter the next MultSpinor
+  // call with apply_first set replaces psi by P psi in place, and every
+  // MultSpinor call returns a3 = P H psi (hamiltonian.cpp:3090-3116, 3240-3265).
+  void set_wfn_filter(int apply_filter, int apply_first, double wfn_cutoff) {
+    check(pw_set_wfn_filter(ctx_, apply_filter, wfn_cutoff));
+    apply_filter_ = apply_filter != 0;
+    apply_first_ = apply_first != 0;
+  }
+  // KohnSham::set_wfn_filter(apply_first) (include/hamiltonian.hpp:353-356)
+  void set_wfn_filter(int apply_first) { apply_first_ = apply_first != 0; }
+
+  // a3 := H psi (host blocks; FP64 contexts).  The view's bands are modified
+  // only by the first call of a filtered Hamiltonian (psi <- P psi).
   void MultSpinor(const BandBlock& psi, BandBlock& a3) {
     require_f64();
+    if (apply_filter_ && apply_first_) {
+      apply_first_ = false;
+      const size_t bytes = (size_t)psi.nband * psi.ntot * sizeof(double);
+      DeviceBlock dx(bytes);
+      cu(cudaMemcpy(dx.get(), psi.data, bytes, cudaMemcpyHostToDevice));
+      check(pw_wfn_filter(ctx_, dx.get(), psi.ntot, psi.nband, nullptr));
+      cu(cudaMemcpy(psi.data, dx.get(), bytes, cudaMemcpyDeviceToHost));
+    }
     check(pw_hpsi_host(ctx_, psi.data, psi.ntot, a3.data, a3.ntot, psi.nband, 0));
   }
   // a3 += T r (host blocks; FP64 contexts)
@@ -130,6 +153,7 @@ class Hamiltonian {
   Domain dm_;
   int prec_;
   pw_ctx* ctx_ = nullptr;
+  bool apply_filter_ = false, apply_first_ = false;
 };
 
 // EigenSolver over a Hamiltonian: the lowest nband eigenpairs from the host

@@ -48,7 +48,7 @@ class ScfParams(C.Structure):
                 ("mix_step", C.c_double), ("tol_efree", C.c_double), ("refine_threshold", C.c_double),
                 ("seed", C.c_ulonglong), ("ppcg_sbsize", C.c_int), ("davidson_maxdim", C.c_int),
                 ("graphs", C.c_int), ("xc", C.c_int), ("mix_type", C.c_int), ("tol_rho", C.c_double),
-                ("phi_max_iter", C.c_int), ("phi_tol", C.c_double)]
+                ("phi_max_iter", C.c_int), ("phi_tol", C.c_double), ("no_wfn_filter", C.c_int)]
 
 
 class ScfResult(C.Structure):
@@ -79,6 +79,10 @@ SIGNATURES: dict[str, tuple] = {
     "pw_set_host_chunk": (_i, [_vp, C.c_int]),
     "pw_teter_precond": (_i, [_vp, _vp, _i, _vp, _i, _i, _i, _vp]),
     "pw_teter_precond_noalloc": (_i, [_vp, _vp, _i, _vp, _i, _i, _i, _vp]),
+    "pw_set_wfn_filter": (_i, [_vp, _i, C.c_double]),
+    "pw_set_wait_limit": (_i, [_vp, C.c_double]),
+    "pw_wait_probe": (_i, [_vp, C.c_double]),
+    "pw_wfn_filter": (_i, [_vp, _vp, _i, _i, _vp]),
     "pw_set_band_batch": (_i, [_vp, _i]),
     "pw_set_nonlocal_mode": (_i, [_vp, _i]),
     "pw_set_gemm_mode": (_i, [_vp, _i, _i]),

@@ -359,10 +359,12 @@ def _ctx_scf(self, nocc: int, nextra: int, ecut: float, solver: str = "chebfsi",
              mix_step: float = 0.7, tol_efree: float = 1e-6, refine_threshold: float = 1e-4, seed: int = 1,
              verbose: bool = False, ppcg_sbsize: int = 1, davidson_maxdim: int = 2, graphs: bool = False,
              xc: str = "teter93", mix: str = "anderson", tol_rho: float = 0.0, phi_max_iter: int = 10,
-             phi_tol: float = 1e-6):
+             phi_tol: float = 1e-6, wfn_filter: bool | None = None):
     """SCF::Iterate on the device (FP64 context; mixed=True runs the eigensolver in
     an FP32 twin and refines in FP64).  xc: "teter93", "pbe" or "hse06" (nested
-    hybrid scheme with ACE).  Returns (result dict, eigenvalues, rho)."""
+    hybrid scheme with ACE).  wfn_filter: ChebFSI's wavefunction cut-off filter
+    at ecut (None or True: on, the reference's CheFSI default; False: off).
+    Returns (result dict, eigenvalues, rho)."""
     xcs = {"teter93": _lib.PW_XC_TETER93, "pbe": _lib.PW_XC_PBE, "hse06": _lib.PW_XC_HSE06}
     if xc not in xcs:
         raise ValueError(f"unknown exchange-correlation functional {xc!r}")
@@ -374,7 +376,7 @@ def _ctx_scf(self, nocc: int, nextra: int, ecut: float, solver: str = "chebfsi",
                        cheby_degree=cheby_degree, cheby_first_cycles=cheby_first_cycles, eig_max_iter=eig_max_iter,
                        max_iter=max_iter, mix_dim=mix_dim, mixed=int(mixed), verbose=int(verbose), ecut=ecut,
                        temperature=temperature, eig_tol=eig_tol, mix_step=mix_step, tol_efree=tol_efree,
-                       refine_threshold=refine_threshold, seed=seed)
+                       refine_threshold=refine_threshold, seed=seed, no_wfn_filter=int(wfn_filter is False))
     r = _lib.ScfResult()
     eig = np.zeros(nocc + nextra)
     rho = np.zeros(self.ntotFine)
@@ -383,6 +385,23 @@ def _ctx_scf(self, nocc: int, nextra: int, ecut: float, solver: str = "chebfsi",
     res["phase_s"] = list(r.phase_s)
     res["sub_s"] = list(r.sub_s)
     return res, eig, rho
+
+
+def _ctx_set_wfn_filter(self, ecut: float | None):
+    """KohnSham::MultSpinor's wavefunction cut-off filter: an overwriting hpsi
+    returns P H psi (P zeroes the coefficients with |G|^2/2 > ecut); None
+    switches it off."""
+    check(lib.pw_set_wfn_filter(self._h, 0 if ecut is None else 1, 0.0 if ecut is None else float(ecut)))
+
+
+def _ctx_wfn_filter(self, X, stream=None):
+    """X <- P X in place (the filter's first-call step on psi)."""
+    check(lib.pw_wfn_filter(self._h, _ptr(X), self.ntot, X.shape[0], _stream(stream)))
+    return X
+
+
+Context.set_wfn_filter = _ctx_set_wfn_filter
+Context.wfn_filter = _ctx_wfn_filter
 
 
 def _ctx_xc_pbe(self, rho, ecut: float):

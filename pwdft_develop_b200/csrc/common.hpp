@@ -82,12 +82,15 @@ enum KernelKind {
 // A dense coarse-grid operator Q diag(qd) Q^T: the projector matrix, or the
 // ACE vectors with qd = -1.  q: T [np][ntot]; q_bf / qt_bf: split-BF16 copies
 // (FP32 contexts) of Q (np x ntot) and Q^T (ntot x npp, npp = np padded to 8).
+// q_st is the matrix the accumulating (store) product reads -- Q itself, or
+// P Q while the wavefunction cut-off filter is on (qt_bf then holds P Q too).
 struct DenseSet {
   const void* q;
   const void* qd;
   const void* q_bf;
   const void* qt_bf;
   int np, npp;
+  const void* q_st;
 };
 
 }  // namespace pwb
@@ -146,6 +149,13 @@ struct pw_ctx {
   int nkb = 0;                      // k-point batch (pw_set_kpoints)
   std::vector<double> kb_k;         // nkb x 3
   pwb::DevBuf ekin_kb, qkb;         // T [nkb][ntot], complex T [nkb][nproj][ntot]
+  // FP32 contexts: the complex projector products as real split-BF16 GEMMs.  Per
+  // k-point: A1 = [Q; Q'] as real rows (2 nproj x 2 ntot, Q' = i Q, so that
+  // A1 psi = [Re; Im] of Q^H psi) and A2 = its store-side partner (2 ntot x
+  // nkp2 rows: (Re, Im) of Q W from [Re W; Im W]), each as bf16 hi / lo
+  pwb::DevBuf qk_bf, qkb_bf;        // single k (pw_set_kpoint) / batch (pw_set_kpoints)
+  pwb::DevBuf qdk2;                 // float [2 nproj]  the weights twice (rows of A1)
+  int nkp2 = 0;                     // 2 nproj rounded up to 8
   // sphere-cut (G-space) mode (Use_Real_Space 0): a band is its half-sphere
   // Fourier coefficients, complex, handled as a real vector of 2 ns numbers
   // (ntot = 2 ns); n = N/2 is the slot box and nf = N the G-space grid
@@ -169,6 +179,17 @@ struct pw_ctx {
   size_t exx_scratch_bytes = (size_t)1 << 30;
   pwb::DevBuf ace_xi, ace_qd, ace_bf, ace_t_bf;   // ACE vectors xi (T [nace][ntot]) and -1 weights
   int ace_n = 0, ace_npad = 0;
+  // wavefunction cut-off filter of KohnSham::MultSpinor (the CheFSI path): while
+  // on, an overwriting H*psi returns P H psi, P = C2R o (zero |G|^2/2 > wfn_ecut) o R2C
+  bool wfn_filter = false;
+  double wfn_ecut = 0.0;
+  pwb::DevBuf wmask;                // T [ntot]  1 where |G|^2/2 <= wfn_ecut on the full coarse spectrum, else 0
+  long q_version = 0, ace_version = 0;           // bumped when Q / the ACE vectors are rebuilt
+  long qf_version = -1, acef_version = -1;       // versions the filtered copies below were made from
+  double qf_ecut = -1.0, acef_ecut = -1.0;
+  pwb::DevBuf qf, qtf_bf;           // P Q and its split-BF16 transpose (store side of the projector GEMMs)
+  pwb::DevBuf acef_xi, acef_t_bf;   // P xi and its split-BF16 transpose (store side of the ACE GEMMs)
+  const void* teter_tab = nullptr;  // table of the next Teter-pipeline pass (nullptr: the Teter table)
   // initial guess for the next pw_scf_run (pw_scf_set_initial, e.g. from restart files)
   std::vector<double> init_rho, init_psi;
   int init_nband = 0;

@@ -79,6 +79,7 @@ int upload_twiddles(pw_ctx* c, int slot, int n) {
 // that the FP32 tensor-core projector GEMMs read
 int install_dense_q(pw_ctx* ctx, int nproj) {
   int rc;
+  ++ctx->q_version;
   if (ctx->prec == PW_F32) {
     const int npp = (nproj + 7) / 8 * 8;
     ctx->nproj_pad = npp;
@@ -95,6 +96,57 @@ int install_dense_q(pw_ctx* ctx, int nproj) {
     if ((rc = split_bf16_t((const float*)ctx->q.p, nt, (int)nt, nproj, qtb, qtb + nt * npp * 2, npp, nullptr)))
       return rc;
     PWB_CUDA(cudaDeviceSynchronize());
+  }
+  return PW_OK;
+}
+
+// In-place P X for nb columns: the Teter pipeline with the 0/1 filter mask as
+// its table (forward transform, mask, inverse transform; the normalisations of
+// the pair pipeline cancel like FFTWExecute's vol/N and 1/vol).
+int wfn_filter_pass(pw_ctx* c, void* X, int ld, int nb, cudaStream_t st) {
+  const void* saved = c->teter_tab;
+  c->teter_tab = c->wmask.p;
+  int rc = PW_OK;
+  const int cap = c->pair_cap;
+  for (int b0 = 0; b0 < nb && !rc; b0 += 2 * cap) {
+    const int npair = std::min(cap, (nb - b0 + 1) / 2);
+    rc = run_teter(c, X, ld, X, ld, nb, b0, npair, 0, st);
+  }
+  c->teter_tab = saved;
+  return rc;
+}
+
+// rows (T [n][ntot]) -> P rows, and for FP32 contexts the split-BF16 transpose
+// the accumulating projector GEMM reads (npad padded columns)
+static int filtered_copy(pw_ctx* c, const DevBuf& src, int n, int npad, DevBuf& dst, DevBuf& dst_t_bf) {
+  const size_t nt = c->ntot;
+  int rc;
+  if ((rc = dst.alloc((size_t)n * nt * c->esz))) return rc;
+  PWB_CUDA(cudaMemcpy(dst.p, src.p, (size_t)n * nt * c->esz, cudaMemcpyDeviceToDevice));
+  if ((rc = wfn_filter_pass(c, dst.p, (int)nt, n, nullptr))) return rc;
+  if (c->prec == PW_F32) {
+    if ((rc = dst_t_bf.alloc((size_t)2 * nt * npad * 2))) return rc;
+    PWB_CUDA(cudaMemset(dst_t_bf.p, 0, (size_t)2 * nt * npad * 2));
+    char* bt = (char*)dst_t_bf.p;
+    if ((rc = split_bf16_t((const float*)dst.p, nt, (int)nt, n, bt, bt + nt * npad * 2, npad, nullptr))) return rc;
+  }
+  PWB_CUDA(cudaDeviceSynchronize());
+  return PW_OK;
+}
+
+// The filtered store-side copies P Q and P xi, made again whenever the
+// projectors, the ACE vectors or the cut-off changed since the last copy.
+int prepare_wfn_filter(pw_ctx* c) {
+  int rc;
+  if (c->nproj > 0 && c->nl_mode == PW_NL_DENSE && (c->qf_version != c->q_version || c->qf_ecut != c->wfn_ecut)) {
+    if ((rc = filtered_copy(c, c->q, c->nproj, c->nproj_pad, c->qf, c->qtf_bf))) return rc;
+    c->qf_version = c->q_version;
+    c->qf_ecut = c->wfn_ecut;
+  }
+  if (c->ace_n > 0 && (c->acef_version != c->ace_version || c->acef_ecut != c->wfn_ecut)) {
+    if ((rc = filtered_copy(c, c->ace_xi, c->ace_n, c->ace_npad, c->acef_xi, c->acef_t_bf))) return rc;
+    c->acef_version = c->ace_version;
+    c->acef_ecut = c->wfn_ecut;
   }
   return PW_OK;
 }
@@ -464,6 +516,10 @@ int pw_hpsi(pw_ctx* ctx, const void* psi, int ld, void* hpsi, int ldh, int nband
             PW_EINVAL, "G-space bands are complex: even leading dimensions and complex-aligned pointers");
   PWB_CUDA(cudaSetDevice(ctx->device));
   cudaStream_t st = (cudaStream_t)stream;
+  if (ctx->wfn_filter && !accumulate) {
+    int rc = prepare_wfn_filter(ctx);
+    if (rc) return rc;
+  }
   const int cap = ctx->pair_cap;
   for (int b0 = 0; b0 < nband; b0 += 2 * cap) {
     const int npair = std::min(cap, (nband - b0 + 1) / 2);
@@ -472,6 +528,58 @@ int pw_hpsi(pw_ctx* ctx, const void* psi, int ld, void* hpsi, int ldh, int nband
   }
   if (ctx->check_errors) return gemm_error_check();
   return PW_OK;
+}
+
+int pw_set_wait_limit(pw_ctx* ctx, double seconds) {
+  PWB_CHECK(ctx && seconds > 0 && seconds < 3600, PW_EINVAL, "wait limit must be in (0, 3600) s");
+  PWB_CUDA(cudaSetDevice(ctx->device));
+  return set_wait_limit_ns((unsigned long long)(seconds * 1e9));
+}
+
+int pw_wait_probe(pw_ctx* ctx, double seconds) {
+  PWB_CHECK(ctx && seconds > 0 && seconds <= 10, PW_EINVAL, "probe limit must be in (0, 10] s");
+  PWB_CUDA(cudaSetDevice(ctx->device));
+  return wait_probe((unsigned long long)(seconds * 1e9), nullptr);
+}
+
+int pw_set_wfn_filter(pw_ctx* ctx, int enable, double ecut) {
+  PWB_CHECK(ctx, PW_EINVAL, "null argument");
+  if (!enable) {
+    ctx->wfn_filter = false;
+    return PW_OK;
+  }
+  PWB_CHECK(ecut > 0, PW_EINVAL, "the wavefunction filter needs a positive cut-off");
+  PWB_CHECK(!ctx->gs, PW_EUNSUPPORTED,
+            "sphere-cut contexts hold only the coefficients inside their Ecut sphere; the wavefunction filter "
+            "belongs to real-space contexts");
+  PWB_CUDA(cudaSetDevice(ctx->device));
+  if (!ctx->wmask.p || ctx->wfn_ecut != ecut) {
+    // the mask on the full coarse spectrum from the same |G|^2/2 as the kinetic
+    // table, in double: zero where gkk > ecut (hamiltonian.cpp:3107-3111)
+    std::vector<double> m(ctx->ntot);
+    const int n0 = ctx->n[0], n1 = ctx->n[1], n2 = ctx->n[2];
+    for (int k = 0; k < n2; ++k)
+      for (int j = 0; j < n1; ++j)
+        for (int i = 0; i < n0; ++i) {
+          const double m0 = i <= n0 / 2 ? i : i - n0, m1 = j <= n1 / 2 ? j : j - n1, m2 = k <= n2 / 2 ? k : k - n2;
+          const double g0 = 2 * M_PI / ctx->L[0] * m0, g1 = 2 * M_PI / ctx->L[1] * m1,
+                       g2 = 2 * M_PI / ctx->L[2] * m2;
+          m[i + (long)n0 * (j + (long)n1 * k)] = (g0 * g0 + g1 * g1 + g2 * g2) / 2 > ecut ? 0.0 : 1.0;
+        }
+    int rc = upload_real(ctx, ctx->wmask, m.data(), m.size());
+    if (rc) return rc;
+  }
+  ctx->wfn_ecut = ecut;
+  ctx->wfn_filter = true;
+  return prepare_wfn_filter(ctx);
+}
+
+int pw_wfn_filter(pw_ctx* ctx, void* X, int ld, int nband, void* stream) {
+  PWB_CHECK(ctx && (nband == 0 || X), PW_EINVAL, "null argument");
+  PWB_CHECK(nband >= 0 && ld >= ctx->ntot, PW_EINVAL, "Domain size does not match.");
+  PWB_CHECK(ctx->wfn_filter, PW_ENOTREADY, "wavefunction filter not set (pw_set_wfn_filter)");
+  PWB_CUDA(cudaSetDevice(ctx->device));
+  return wfn_filter_pass(ctx, X, ld, nband, (cudaStream_t)stream);
 }
 
 int pw_teter_precond(pw_ctx* ctx, const void* r, int ld, void* w, int ldw, int nband, int accumulate, void* stream) {

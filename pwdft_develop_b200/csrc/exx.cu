@@ -282,6 +282,7 @@ int pw_ace_build(pw_ctx* ctx, const void* psi, int ld, int nband) {
   PWB_CUDA(cudaDeviceSynchronize());
   ctx->ace_n = nband;
   ctx->ace_npad = npad;
+  ++ctx->ace_version;
   ctx->exx_mode = PW_EXX_ACE;
   return PW_OK;
 }

@@ -33,9 +33,12 @@ namespace pwb {
 constexpr int GM = 128;             // tile rows (UMMA M)
 constexpr int GK = 64;              // K per stage (one 128-byte swizzle row of bf16)
 constexpr int GEMM_THREADS = 192;   // 6 warps
-constexpr unsigned long long WAIT_NS = 2000000000ull;   // 2 s per wait
+constexpr unsigned long long WAIT_NS = 2000000000ull;   // 2 s per wait (default, and the floor of drain waits)
 
 __device__ int g_gemm_error = 0;
+// limit of the pipeline waits on this device (pw_set_wait_limit); the drain
+// waits at the end of a CTA keep at least WAIT_NS so issued copies always land
+__device__ unsigned long long g_wait_ns = WAIT_NS;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -63,16 +66,34 @@ __device__ __forceinline__ unsigned long long gtimer() {
   asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
   return t;
 }
-// bounded wait; returns false (and records code) on timeout
-__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, int code) {
+// bounded wait; returns false (and records code) on timeout.  drain: a wait
+// for copies or MMAs this CTA issued itself, which must finish before exit
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, uint32_t parity, int code, bool drain = false) {
   if (mbar_try(b, parity)) return true;
+  const unsigned long long lim = drain ? max(g_wait_ns, WAIT_NS) : g_wait_ns;
   const unsigned long long t0 = gtimer();
   for (unsigned it = 1;; ++it) {
     if (mbar_try(b, parity)) return true;
-    if ((it & 255) == 0 && gtimer() - t0 > WAIT_NS) break;
+    if ((it & 255) == 0 && gtimer() - t0 > lim) break;
   }
   atomicCAS(&g_gemm_error, 0, code);
   return false;
+}
+
+// The failure path of the bounded waits, exercised without a fault: one
+// thread waits on an mbarrier that nothing arrives on, with the given limit,
+// records code 7 when it gives up and returns.
+__global__ void k_wait_probe(unsigned long long limit_ns) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x != 0) return;
+  mbar_init(&bar, 1);
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  const unsigned long long t0 = gtimer();
+  for (unsigned it = 1;; ++it) {
+    if (mbar_try(&bar, 0)) return;
+    if ((it & 255) == 0 && gtimer() - t0 > limit_ns) break;
+  }
+  atomicCAS(&g_gemm_error, 0, 7);
 }
 
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
@@ -222,7 +243,7 @@ k_gemm_tn(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant__ CU
       }
       // drain: every issued stage must have landed before the CTA exits
       for (long k = (it > SM::NSTAGE ? it - SM::NSTAGE : 0); k < it; ++k)
-        mbar_wait(&full[k % SM::NSTAGE], (uint32_t)((k / SM::NSTAGE) & 1), 2);
+        mbar_wait(&full[k % SM::NSTAGE], (uint32_t)((k / SM::NSTAGE) & 1), 2, true);
     }
   } else if (warp == 1) {
     if (lane == 0) {
@@ -264,7 +285,7 @@ k_gemm_tn(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant__ CU
       // every issued MMA must have completed before the tensor memory is freed
       if (any) {
         umma_commit(final_bar);
-        mbar_wait(final_bar, 0, 6);
+        mbar_wait(final_bar, 0, 6, true);
       }
     }
   } else {
@@ -511,6 +532,18 @@ static int pick_bn(int N) {
   return best;
 }
 
+int set_wait_limit_ns(unsigned long long ns) {
+  PWB_CUDA(cudaMemcpyToSymbol(g_wait_ns, &ns, sizeof(ns)));
+  return PW_OK;
+}
+
+int wait_probe(unsigned long long limit_ns, cudaStream_t st) {
+  k_wait_probe<<<1, 32, 0, st>>>(limit_ns);
+  PWB_CUDA(cudaGetLastError());
+  PWB_CUDA(cudaStreamSynchronize(st));
+  return gemm_error_check();
+}
+
 int gemm_error_check() {
   int h = 0;
   PWB_CUDA(cudaMemcpyFromSymbol(&h, g_gemm_error, sizeof(int)));
@@ -551,6 +584,12 @@ int gemm_tn_reduce(const SplitOperand& A, const SplitOperand& B, int K, int nter
   int nsplit = std::max(1, (2 * num_sms() + tiles - 1) / tiles);
   const int maxsplit = std::max(1, (K + 4 * GK - 1) / (4 * GK));
   nsplit = std::min(nsplit, maxsplit);
+  // at most KCHUNK_MAX per tensor-memory accumulator: the accumulation of the
+  // UMMA partial sums loses low-order bits, so its error grows with the number
+  // of k-steps summed in one accumulator (measured: a 124k-long chunk at
+  // K = 373,248 was off by 8e-4 relative, 64-block chunks stay below 3e-5)
+  constexpr int KCHUNK_MAX = 64 * GK;
+  nsplit = std::max(nsplit, (K + KCHUNK_MAX - 1) / KCHUNK_MAX);
   int kchunk = ((K + nsplit - 1) / nsplit + GK - 1) / GK * GK;
   nsplit = (K + kchunk - 1) / kchunk;
   int rc = ws.alloc((size_t)nsplit * M * N * sizeof(float));

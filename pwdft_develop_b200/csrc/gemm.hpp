@@ -41,5 +41,9 @@ int gemm_tn_store(const SplitOperand& A, const SplitOperand& B, int K, int nterm
                   cudaStream_t st, int transposed = 0, int bn = 0);
 // PW_ETIMEOUT (and clears the flag) if a GEMM pipeline wait gave up
 int gemm_error_check();
+// limit of the GEMM pipeline waits on the current device (drain waits keep >= 2 s)
+int set_wait_limit_ns(unsigned long long ns);
+// a bounded wait that nothing releases: PW_ETIMEOUT after limit_ns, the context stays usable
+int wait_probe(unsigned long long limit_ns, cudaStream_t st);
 
 }  // namespace pwb

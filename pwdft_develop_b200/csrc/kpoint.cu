@@ -5,6 +5,8 @@
 // 234-277: ekin = 1/2 |k+G|^2, Teter of |k+G|^2 on the full coarse grid) and
 // the projector Bloch phase e^{i k.(r - R_a)} of PeriodTable::CalculateNonlocalPP
 // (src/SCF/periodtable.cpp:1104-1121).
+#include <cuda_bf16.h>
+
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -12,6 +14,60 @@
 #include "common.hpp"
 
 namespace pwb {
+
+// bytes of one k-point's split-BF16 projector operands (A1 and A2, hi and lo)
+size_t kq_bf_bytes(const pw_ctx* c) {
+  const size_t np = c->nproj, nt = c->ntot;
+  return 2 * (2 * np * 2 * nt + 2 * nt * (size_t)c->nkp2) * sizeof(__nv_bfloat16);
+}
+
+static __device__ __forceinline__ void split2(float v, __nv_bfloat16* h, __nv_bfloat16* l) {
+  const __nv_bfloat16 a = __float2bfloat16_rn(v);
+  *h = a;
+  *l = __float2bfloat16_rn(v - __bfloat162float(a));
+}
+
+// Q (complex, [np][nt]) -> the real GEMM operands of V_nl = Q diag(d) Q^H:
+//   A1[l][2g], A1[l][2g+1]           = Re q, Im q       (row l:      Re(Q^H psi)_l)
+//   A1[np+l][2g], A1[np+l][2g+1]     = -Im q, Re q      (row np + l: Im(Q^H psi)_l)
+//   A2[2g][l] = Re q, A2[2g][np+l] = -Im q, A2[2g+1][l] = Im q, A2[2g+1][np+l] = Re q
+// so that [Re; Im] of Q W = A2 [Re W; Im W] on interleaved (re, im) rows.
+__global__ void k_kq_split(const float2* __restrict__ Q, int np, long nt, int nkp2, __nv_bfloat16* a1h,
+                           __nv_bfloat16* a1l, __nv_bfloat16* a2h, __nv_bfloat16* a2l) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= (long)np * nt) return;
+  const int l = (int)(i / nt);
+  const long g = i - (long)l * nt;
+  const float2 q = Q[i];
+  const long r0 = (long)l * 2 * nt + 2 * g, r1 = (long)(np + l) * 2 * nt + 2 * g;
+  split2(q.x, a1h + r0, a1l + r0);
+  split2(q.y, a1h + r0 + 1, a1l + r0 + 1);
+  split2(-q.y, a1h + r1, a1l + r1);
+  split2(q.x, a1h + r1 + 1, a1l + r1 + 1);
+  const long s0 = 2 * g * (long)nkp2, s1 = s0 + nkp2;
+  split2(q.x, a2h + s0 + l, a2l + s0 + l);
+  split2(-q.y, a2h + s0 + np + l, a2l + s0 + np + l);
+  split2(q.y, a2h + s1 + l, a2l + s1 + l);
+  split2(q.x, a2h + s1 + np + l, a2l + s1 + np + l);
+}
+
+// the split operands of one k-point's projectors (FP32 contexts) at dst
+int build_kq_bf(pw_ctx* c, const void* Qk, void* dst) {
+  const long nt = c->ntot;
+  const int np = c->nproj;
+  __nv_bfloat16* a1h = (__nv_bfloat16*)dst;
+  __nv_bfloat16* a1l = a1h + (size_t)2 * np * 2 * nt;
+  __nv_bfloat16* a2h = a1l + (size_t)2 * np * 2 * nt;
+  __nv_bfloat16* a2l = a2h + (size_t)2 * nt * c->nkp2;
+  PWB_CUDA(cudaMemset(a2h, 0, (size_t)2 * (2 * nt * c->nkp2) * sizeof(__nv_bfloat16)));
+  const long n = (long)np * nt;
+  k_kq_split<<<(unsigned)((n + 255) / 256), 256>>>((const float2*)Qk, np, nt, c->nkp2, a1h, a1l, a2h, a2l);
+  PWB_CUDA(cudaGetLastError());
+  c->launches += 1;
+  return PW_OK;
+}
+
+static bool kq_tensor_cores(const pw_ctx* c) { return c->prec == PW_F32 && c->gemm_mode == 0 && c->nproj > 0; }
 
 int run_hpsi_k(pw_ctx* c, const void* psi, int ld, void* out, int ldo, int band0, int nb, int acc, cudaStream_t st);
 int run_hpsi_kbatch(pw_ctx* c, const void* psi, int ld, void* out, int ldo, int f0, int nf, int acc, cudaStream_t st,
@@ -81,6 +137,15 @@ int pw_set_kpoint(pw_ctx* ctx, const double k[3]) {
     for (int l = 0; l < np; ++l) qd[l] = ctx->h_pgamma[l] * ctx->vol / (double)nt;
     if ((rc = upload_real(ctx, ctx->qdk, qd.data(), np))) return rc;
     ctx->launches += 5 * ((np + std::max(ctx->pair_cap, 1) - 1) / std::max(ctx->pair_cap, 1));
+    if (kq_tensor_cores(ctx)) {
+      ctx->nkp2 = (2 * np + 7) / 8 * 8;
+      std::vector<float> d2(2 * np);
+      for (int l = 0; l < np; ++l) d2[l] = d2[np + l] = (float)qd[l];
+      if ((rc = ctx->qdk2.alloc(d2.size() * 4))) return rc;
+      PWB_CUDA(cudaMemcpy(ctx->qdk2.p, d2.data(), d2.size() * 4, cudaMemcpyHostToDevice));
+      if ((rc = ctx->qk_bf.alloc(kq_bf_bytes(ctx)))) return rc;
+      if ((rc = build_kq_bf(ctx, ctx->qk.p, ctx->qk_bf.p))) return rc;
+    }
   }
   PWB_CUDA(cudaDeviceSynchronize());
   for (int d = 0; d < 3; ++d) ctx->kvec[d] = k[d];
@@ -114,12 +179,18 @@ int pw_set_kpoints(pw_ctx* ctx, int nk, const double* kpts) {
   int rc;
   if ((rc = ctx->ekin_kb.alloc((size_t)nk * nt * esz))) return rc;
   if (np > 0 && (rc = ctx->qkb.alloc((size_t)nk * np * nt * 2 * esz))) return rc;
+  const bool tc = kq_tensor_cores(ctx) && np > 0;
   for (int k = 0; k < nk; ++k) {
     if ((rc = pw_set_kpoint(ctx, kpts + 3 * k))) return rc;
     PWB_CUDA(cudaMemcpy((char*)ctx->ekin_kb.p + (size_t)k * nt * esz, ctx->ekin_k.p, nt * esz, cudaMemcpyDeviceToDevice));
     if (np > 0)
       PWB_CUDA(cudaMemcpy((char*)ctx->qkb.p + (size_t)k * np * nt * 2 * esz, ctx->qk.p, (size_t)np * nt * 2 * esz,
                           cudaMemcpyDeviceToDevice));
+    if (tc) {
+      const size_t per = kq_bf_bytes(ctx);
+      if (k == 0 && (rc = ctx->qkb_bf.alloc((size_t)nk * per))) return rc;
+      PWB_CUDA(cudaMemcpy((char*)ctx->qkb_bf.p + (size_t)k * per, ctx->qk_bf.p, per, cudaMemcpyDeviceToDevice));
+    }
   }
   ctx->kb_k.assign(kpts, kpts + 3 * nk);
   ctx->nkb = nk;

@@ -34,6 +34,9 @@
 
 namespace pwb {
 
+// bytes of one k-point's split-BF16 projector operands (kpoint.cu)
+size_t kq_bf_bytes(const pw_ctx* c);
+
 // kx columns per z-pencil CTA: 24 for FP32 grids divisible by 24 (two
 // balanced tiles at n0 = 48), otherwise 16
 template <typename T, int N0> struct PencilTile {
@@ -1030,7 +1033,8 @@ __global__ void k_nl_reduce(const VT<T>* __restrict__ Wp, VT<T>* __restrict__ W,
 template <typename T, int NZ, int NZF, int TX>
 __global__ void __launch_bounds__(PENCIL_THREADS, sizeof(T) == 4 ? 4 : 2)
 k_zfold(const VT<T>* __restrict__ C, const VT<T>* __restrict__ K, VT<T>* __restrict__ D, int n0, int n1,
-        const VT<T>* twz_g, const VT<T>* twzf_g, int deriv = 0, T gfac = 0, int cplx = 0) {
+        const VT<T>* twz_g, const VT<T>* twzf_g, int deriv = 0, T gfac = 0, int cplx = 0,
+        const T* __restrict__ fmask = nullptr) {
   using V = VT<T>;
   constexpr int PI = 2 * TX + 1;
   constexpr int PA = TX + 1;
@@ -1110,6 +1114,9 @@ k_zfold(const VT<T>* __restrict__ C, const VT<T>* __restrict__ K, VT<T>* __restr
       if (nyz) v = cadd(v, cscale(cadd(in[(NZ / 2) * PI + cp], in[(NZF - NZ / 2) * PI + cm]), (T)0.5));
       else v = cadd(v, cscale(cadd(in[fz * PI + cp], in[fz * PI + cm]), (T)0.5));
     }
+    // wavefunction cut-off filter (MultSpinor's exit filter): coefficients with
+    // |G|^2/2 above the cut-off are zero in the output spectrum
+    if (fmask && fmask[(long)kz * nplane + (long)ky * n0 + kx0 + c] == (T)0) v = mkc<V>(0, 0);
     acc[kz * PA + c] = v;
   }
   __syncthreads();
@@ -1408,6 +1415,8 @@ struct Plan {
                         int accumulate, cudaStream_t st) {
     int rc = set_attrs();
     if (rc) return rc;
+    // MultSpinor's exit filter applies to an overwriting call (a3 = P H psi)
+    const bool filt = c->wfn_filter && !accumulate;
     V* AD = reinterpret_cast<V*>(c->s_ad.p);
     V* K = reinterpret_cast<V*>(c->s_k.p);
     V* BC = reinterpret_cast<V*>(c->s_bc.p);
@@ -1426,15 +1435,16 @@ struct Plan {
       k_floc2<T, NF0, NF1><<<dim3(NF2, npair), FLOC_THREADS, sm_floc2(), st>>>(
           BC, reinterpret_cast<const T*>(c->vtot.p), inv_nf, tw(c, 3), tw(c, 4)); }
       { Launch L_(c, st, KK_ZFOLD);
-      k_zfold<T, N2, NF2, TXF><<<dim3(N1, (N0 + TXF - 1) / TXF, npair), PENCIL_THREADS, sm_zfold(), st>>>(BC, K, AD, N0, N1, tw(c, 2), tw(c, 5)); }
+      k_zfold<T, N2, NF2, TXF><<<dim3(N1, (N0 + TXF - 1) / TXF, npair), PENCIL_THREADS, sm_zfold(), st>>>(
+          BC, K, AD, N0, N1, tw(c, 2), tw(c, 5), 0, (T)0, 0, filt ? reinterpret_cast<const T*>(c->wmask.p) : nullptr); }
       { Launch L_(c, st, KK_CXY_INV);
       k_cxy_inv<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(AD, out, ldo, nband, band0, accumulate, tw(c, 0), tw(c, 1)); }
       PWB_CUDA(cudaGetLastError());
       const int nb = std::min(2 * npair, nband - band0);
       if (c->have_nl && c->nproj > 0 && nb > 0)
-        if ((rc = dense_apply(c, nl_set(c), psi + (long)band0 * ld, ld, out + (long)band0 * ldo, ldo, nb, st)))
+        if ((rc = dense_apply(c, nl_set(c, filt), psi + (long)band0 * ld, ld, out + (long)band0 * ldo, ldo, nb, st)))
           return rc;
-      return exchange_batch(c, psi, ld, out, ldo, nband, band0, npair, st);
+      return exchange_batch(c, psi, ld, out, ldo, nband, band0, npair, st, filt);
     }
     NLArgs nl{};
     const int cr = chunk_rows();
@@ -1466,29 +1476,46 @@ struct Plan {
     k_fplane<T, NF0, NF1, true><<<dim3(NF2, npair), PLANE_THREADS, sm_fplane(cr), st>>>(
         BC, reinterpret_cast<const T*>(c->vtot.p), nl, Wp, W, natom, nslot, inv_nf, tw(c, 3), tw(c, 4)); }
     { Launch L_(c, st, KK_ZFOLD);
-    k_zfold<T, N2, NF2, TXF><<<dim3(N1, (N0 + TXF - 1) / TXF, npair), PENCIL_THREADS, sm_zfold(), st>>>(BC, K, AD, N0, N1, tw(c, 2), tw(c, 5)); }
+    k_zfold<T, N2, NF2, TXF><<<dim3(N1, (N0 + TXF - 1) / TXF, npair), PENCIL_THREADS, sm_zfold(), st>>>(
+        BC, K, AD, N0, N1, tw(c, 2), tw(c, 5), 0, (T)0, 0, filt ? reinterpret_cast<const T*>(c->wmask.p) : nullptr); }
     { Launch L_(c, st, KK_CXY_INV);
     k_cxy_inv<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(AD, out, ldo, nband, band0, accumulate, tw(c, 0), tw(c, 1)); }
     PWB_CUDA(cudaGetLastError());
-    return exchange_batch(c, psi, ld, out, ldo, nband, band0, npair, st);
+    return exchange_batch(c, psi, ld, out, ldo, nband, band0, npair, st, filt);
   }
 
   // exact exchange of the batch's bands: the ACE operator (two GEMMs) or the
   // full pair-FFT exchange, depending on the context's hybrid mode
   static int exchange_batch(pw_ctx* c, const T* psi, int ld, T* out, int ldo, int nband, int band0, int npair,
-                            cudaStream_t st) {
+                            cudaStream_t st, bool filt = false) {
     const int nb = std::min(2 * npair, nband - band0);
     if (nb <= 0 || c->exx_mode == PW_EXX_OFF) return PW_OK;
     if (c->exx_mode == PW_EXX_ACE) {
       if (c->ace_n == 0) return PW_OK;
-      DenseSet ds{c->ace_xi.p, c->ace_qd.p, c->ace_bf.p, c->ace_t_bf.p, c->ace_n, c->ace_npad};
-      return dense_apply(c, ds, psi + (long)band0 * ld, ld, out + (long)band0 * ldo, ldo, nb, st);
+      return dense_apply(c, ace_set(c, filt), psi + (long)band0 * ld, ld, out + (long)band0 * ldo, ldo, nb, st);
     }
     if (c->gs) return gs_exx_apply(c, psi + (long)band0 * ld, ld, nb, out + (long)band0 * ldo, ldo, 1, st);
-    return exx_apply(c, psi + (long)band0 * ld, ld, nb, out + (long)band0 * ldo, ldo, 1, st);
+    int rc = exx_apply(c, psi + (long)band0 * ld, ld, nb, out + (long)band0 * ldo, ldo, 1, st);
+    if (rc || !filt) return rc;
+    // the pair-FFT exchange has no fused filter: one explicit P pass over the
+    // batch's output bands (the local, kinetic and projector parts are already
+    // in the filtered space, and P is idempotent)
+    const void* saved = c->teter_tab;
+    c->teter_tab = c->wmask.p;
+    rc = teter_batch(c, out, ldo, out, ldo, nband, band0, npair, 0, st);
+    c->teter_tab = saved;
+    return rc;
   }
 
-  static DenseSet nl_set(pw_ctx* c) { return DenseSet{c->q.p, c->qd.p, c->q_bf.p, c->qt_bf.p, c->nproj, c->nproj_pad}; }
+  // the projector matrix; with the filter the accumulating product reads P Q
+  static DenseSet nl_set(pw_ctx* c, bool filt = false) {
+    return DenseSet{c->q.p, c->qd.p, c->q_bf.p, filt ? c->qtf_bf.p : c->qt_bf.p, c->nproj, c->nproj_pad,
+                    filt ? c->qf.p : c->q.p};
+  }
+  static DenseSet ace_set(pw_ctx* c, bool filt = false) {
+    return DenseSet{c->ace_xi.p, c->ace_qd.p, c->ace_bf.p, filt ? c->acef_t_bf.p : c->ace_t_bf.p, c->ace_n,
+                    c->ace_npad, filt ? c->acef_xi.p : c->ace_xi.p};
+  }
 
   // out (+)= V_x psi, AddMultSpinorEXX (src/SCF/spinor.cpp:682-781): for every
   // band k and exchange orbital j, out_k -= alpha f_j phi_j (1/N_c) IFFT(v FFT(psi_k phi_j)).
@@ -1564,11 +1591,12 @@ struct Plan {
     if (r != CUBLAS_STATUS_SUCCESS) { set_error("projector GEMM (Q^T psi) failed"); return PW_ECUDA; }
     { Launch L_(c, st, KK_MISC);
     k_scale_rows<T><<<(unsigned)(((long)np * nb + 255) / 256), 256, 0, st>>>(W, reinterpret_cast<const T*>(ds.qd), np, nb); }
+    const T* Qs = reinterpret_cast<const T*>(ds.q_st ? ds.q_st : ds.q);
     { Launch L_(c, st, KK_LIBGEMM);
     if constexpr (std::is_same<T, double>::value)
-      r = cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, nt, nb, np, &one, Q, nt, W, np, &one, out, ldo);
+      r = cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, nt, nb, np, &one, Qs, nt, W, np, &one, out, ldo);
     else
-      r = cublasSgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, nt, nb, np, &one, Q, nt, W, np, &one, out, ldo); }
+      r = cublasSgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, nt, nb, np, &one, Qs, nt, W, np, &one, out, ldo); }
     if (r != CUBLAS_STATUS_SUCCESS) { set_error("projector GEMM (Q W) failed"); return PW_ECUDA; }
     PWB_CUDA(cudaGetLastError());
     return PW_OK;
@@ -1673,18 +1701,62 @@ struct Plan {
     if (c->nproj == 0 || !(qk_all ? qk_all : c->qk.p)) return PW_OK;
     // V_nl psi = Q diag(d) Q^H psi with the complex coarse projector matrix Q of
     // each k-point, one GEMM pair per k segment of the batch
+    const size_t kq_per = kq_bf_bytes(c);
     for (int f = band0; f < band0 + nb;) {
       const int kk = f / fpk;
       const int f1 = (int)std::min<long>(band0 + nb, (long)(kk + 1) * fpk);
       const V* Qk = qk_all ? qk_all + (long)kk * c->nproj * c->ntot : reinterpret_cast<const V*>(c->qk.p);
-      if ((rc = nl_k(c, Qk, psi + (long)f * ld, ld, out + (long)f * ldo, ldo, f1 - f, st))) return rc;
+      const void* qbf = qk_all ? (c->qkb_bf.p ? (const char*)c->qkb_bf.p + (size_t)kk * kq_per : nullptr)
+                               : c->qk_bf.p;
+      if ((rc = nl_k(c, Qk, qbf, psi + (long)f * ld, ld, out + (long)f * ldo, ldo, f1 - f, st))) return rc;
       f = f1;
     }
     return PW_OK;
   }
 
-  static int nl_k(pw_ctx* c, const V* Q, const V* x, int ld, V* y, int ldo, int nb, cudaStream_t st) {
+  // FP32, tensor cores: V_nl psi as two real split-BF16 GEMMs over the
+  // interleaved (re, im) view.  [Re W; Im W] = d o (A1 psi) (K = 2 ntot, split-K
+  // reduced, written as the bf16 operand of the next product), then
+  // psi_out += A2 [Re W; Im W] (K = 2 nproj) on the grid-major rows.
+  static int nl_k_tc(pw_ctx* c, const void* qbf, const float* x, int ld, float* y, int ldo, int nb, cudaStream_t st) {
+    const int np = c->nproj, np2 = c->nkp2;
+    const long nt = c->ntot, nt2 = 2 * nt;
+    const char* a1h = (const char*)qbf;
+    const char* a1l = a1h + (size_t)2 * np * nt2 * 2;
+    const char* a2h = a1l + (size_t)2 * np * nt2 * 2;
+    const char* a2l = a2h + (size_t)nt2 * np2 * 2;
     int rc;
+    if ((rc = c->s_psi_bf.alloc((size_t)2 * nb * nt2 * 2))) return rc;
+    if ((rc = c->s_w_bf.alloc((size_t)2 * nb * np2 * 2))) return rc;
+    char* pb = (char*)c->s_psi_bf.p;
+    char* wb = (char*)c->s_w_bf.p;
+    PWB_CUDA(cudaMemsetAsync(wb, 0, (size_t)2 * nb * np2 * 2, st));
+    { Launch L_(c, st, KK_MISC);
+    if ((rc = split_bf16(x, 2L * ld, (int)nt2, nb, pb, pb + (size_t)nb * nt2 * 2, nt2, 1.0f, st))) return rc; }
+    SplitOperand A{a1h, a1l, 2 * np, nt2};
+    SplitOperand B{pb, pb + (size_t)nb * nt2 * 2, nb, nt2};
+    ReduceOut ro;
+    ro.transpose = 1;
+    ro.row_scale = reinterpret_cast<const float*>(c->qdk2.p);
+    ro.bf_hi = wb;
+    ro.bf_lo = wb + (size_t)nb * np2 * 2;
+    ro.ldb = np2;
+    { Launch L_(c, st, KK_GRAM);
+    if ((rc = gemm_tn_reduce(A, B, (int)nt2, c->gemm_terms, c->s_ws, ro, st, c->gemm_bn))) return rc; }
+    SplitOperand W{wb, wb + (size_t)nb * np2 * 2, nb, np2};
+    SplitOperand QT{a2h, a2l, (int)nt2, np2};
+    { Launch L_(c, st, KK_GRAM);
+    if ((rc = gemm_tn_store(QT, W, 2 * np, c->gemm_terms, y, 2L * ldo, 1, st, 1, c->gemm_bn_store))) return rc; }
+    return PW_OK;
+  }
+
+  static int nl_k(pw_ctx* c, const V* Q, const void* qbf, const V* x, int ld, V* y, int ldo, int nb,
+                  cudaStream_t st) {
+    int rc;
+    if constexpr (std::is_same<T, float>::value) {
+      if (qbf && c->gemm_mode == 0)
+        return nl_k_tc(c, qbf, reinterpret_cast<const float*>(x), ld, reinterpret_cast<float*>(y), ldo, nb, st);
+    }
     cublasHandle_t h = (cublasHandle_t)c->blas;
     if (cublasSetStream(h, st) != CUBLAS_STATUS_SUCCESS) { set_error("cublasSetStream failed"); return PW_ECUDA; }
     const int np = c->nproj, nt = (int)c->ntot;
@@ -1798,7 +1870,7 @@ struct Plan {
     k_cxy_fwd<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(r, ld, nband, band0, AD, tw(c, 0), tw(c, 1)); }
     { Launch L_(c, st, KK_ZTETER);
     k_zteter<T, N2, TX><<<dim3(N1, ntx, npair), PENCIL_THREADS, sm_zteter(), st>>>(
-        AD, reinterpret_cast<const T*>(c->teter.p), N0, N1, inv_nc, tw(c, 2)); }
+        AD, reinterpret_cast<const T*>(c->teter_tab ? c->teter_tab : c->teter.p), N0, N1, inv_nc, tw(c, 2)); }
     { Launch L_(c, st, KK_CXY_INV);
     k_cxy_inv<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(AD, out, ldo, nband, band0, accumulate, tw(c, 0), tw(c, 1)); }
     PWB_CUDA(cudaGetLastError());
@@ -1932,8 +2004,8 @@ static int exx_thunk(pw_ctx* c, const void* psi, int ld, int nb, void* out, int 
 template <typename T, int N0, int N1, int N2>
 static int ace_thunk(pw_ctx* c, const void* psi, int ld, int nb, void* out, int ldo, int acc, cudaStream_t st) {
   (void)acc;
-  DenseSet ds{c->ace_xi.p, c->ace_qd.p, c->ace_bf.p, c->ace_t_bf.p, c->ace_n, c->ace_npad};
-  return Plan<T, N0, N1, N2>::dense_apply(c, ds, (const T*)psi, ld, (T*)out, ldo, nb, st);
+  return Plan<T, N0, N1, N2>::dense_apply(c, Plan<T, N0, N1, N2>::ace_set(c), (const T*)psi, ld, (T*)out, ldo, nb,
+                                          st);
 }
 
 template <typename T, int N0, int N1, int N2>

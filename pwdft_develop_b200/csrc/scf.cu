@@ -36,6 +36,7 @@ int run_density(pw_ctx* c, const void* psi, int ld, int nband, int band0, int np
 int gram(pw_ctx* c, const void* X, int ldx, int nx, const void* Y, int ldy, int ny, double* G, int ldg,
          cudaStream_t st);
 int upload_real(pw_ctx* c, DevBuf& dst, const double* src, size_t n);
+int wfn_filter_pass(pw_ctx* c, void* X, int ld, int nb, cudaStream_t st);
 
 // Hartree on the fine grid: vh = (1/N) IFFT( kern * FFT(rho - rho_ps) ),
 // kern = 2 pi / gkk (0 for gkk <= 1e-16 or gkk > 4 Ecut).  Cubic grids only.
@@ -510,6 +511,15 @@ static int lanczos_upper(Solver& s, int k, double* upper, double* lower) {
   std::vector<double> al, be;
   DevBuf dot;
   if ((rc = dot.alloc(16))) return rc;
+  if (s.c->wfn_filter) {
+    // with the cut-off filter the Krylov space must start inside the span of P
+    // (where P H is the symmetric P H P): filter and renormalise the start vector
+    if ((rc = wfn_filter_pass(s.c, v.p, (int)s.nt, 1, nullptr))) return rc;
+    if ((rc = v_colnorm2(s, 1, v.p, (double*)dot.p))) return rc;
+    double n2;
+    PWB_CUDA(cudaMemcpy(&n2, dot.p, 8, cudaMemcpyDeviceToHost));
+    if ((rc = v_axpby(s, 1, 0.0, v.p, 1.0 / std::sqrt(n2), v.p))) return rc;
+  }
   double beta = 0;
   for (int j = 0; j < k; ++j) {
     if ((rc = hpsi(s.c, v.p, w.p, 1, nullptr))) return rc;
@@ -1369,6 +1379,31 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
     S.c32 = ctx->twin;
     if ((rc = pw_set_band_batch(S.c32, nb))) return rc;
   }
+  // CheFSI runs H*psi with the wavefunction cut-off filter at Ecut unless the
+  // caller turns it off (KohnSham::Setup, hamiltonian.cpp:316-321); the
+  // contexts' own filter settings are restored on return
+  struct FilterGuard {
+    pw_ctx* c[2];
+    bool on[2];
+    double ecut[2];
+    ~FilterGuard() {
+      for (int i = 0; i < 2; ++i) {
+        if (!c[i]) continue;
+        if (on[i]) pw_set_wfn_filter(c[i], 1, ecut[i]);
+        else c[i]->wfn_filter = false;
+      }
+    }
+  } fguard{{ctx, S.c32}, {ctx->wfn_filter, S.c32 ? S.c32->wfn_filter : false},
+           {ctx->wfn_ecut, S.c32 ? S.c32->wfn_ecut : 0.0}};
+  const bool use_filter = p->solver == PW_SOLVER_CHEBFSI && !p->no_wfn_filter && !ctx->gs;
+  for (pw_ctx* c : {ctx, S.c32}) {
+    if (!c) continue;
+    if (use_filter) {
+      if ((rc = pw_set_wfn_filter(c, 1, p->ecut))) return rc;
+    } else {
+      c->wfn_filter = false;
+    }
+  }
   const bool prof = p->verbose >= 2;
   g_sub_on = prof;
   for (double& x : g_sub) x = 0;
@@ -1537,6 +1572,9 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
     PWB_CUDA(cudaGetLastError());
     if (cur->gs)   // sphere-cut bands: Im c_0 = 0
       PWB_CUDA(cudaMemset2D((char*)sv.X.p + cur->esz, nt * cur->esz, 0, cur->esz, nb));
+    // filtered CheFSI: the start block lies in the span of P (the first
+    // MultSpinor call filters psi in place, hamiltonian.cpp:3090-3116)
+    if (use_filter && (rc = wfn_filter_pass(cur, sv.X.p, (int)nt, nb, nullptr))) return rc;
     if ((rc = cholqr(sv, dn, sv.X.p, nb, sv.Y.p))) return rc;
   }
   if (prof) {
@@ -1563,6 +1601,8 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
     std::vector<double> keep_eig = sv.eig;
     if ((q = bind(ctx))) return q;
     if ((q = copy_f2d_2d((int)nt, nb, (const float*)x32.p, nt, (double*)sv.X.p, nt, nullptr))) return q;
+    // the FP32 bands carry rounding outside the span of P: filter them again in FP64
+    if (use_filter && (q = wfn_filter_pass(ctx, sv.X.p, (int)nt, nb, nullptr))) return q;
     if ((q = cholqr(sv, dn, sv.X.p, nb, sv.Y.p))) return q;
     sv.eig = keep_eig;
     refined = true;
@@ -2053,6 +2093,9 @@ int pw_eigsolve(pw_ctx* ctx, int solver, void* X, int nb, int maxit, double tol,
   PWB_CUDA(cudaMemcpy(sv.X.p, X, (size_t)nb * sv.nt * sv.esz, cudaMemcpyDeviceToDevice));
   if (ctx->gs)   // sphere-cut bands: Im c_0 is not a degree of freedom
     PWB_CUDA(cudaMemset2D((char*)sv.X.p + ctx->esz, sv.nt * ctx->esz, 0, ctx->esz, nb));
+  // the first MultSpinor call of a filtered Hamiltonian replaces psi by P psi
+  // (hamiltonian.cpp:3090-3116)
+  if (ctx->wfn_filter && (rc = wfn_filter_pass(ctx, sv.X.p, (int)sv.nt, nb, nullptr))) return rc;
   int it = 0;
   if (solver == PW_SOLVER_LOBPCG) {
     rc = lobpcg(sv, dn, nb, maxit, tol, true, &it);

@@ -93,7 +93,8 @@ def test_backward_matches_hellmann_feynman_nonlocal_force():
     c = Context(L, nc, nf, precision="f64")
     c.set_atoms([z] * len(pos), pos)
     res, _, _ = c.scf(nocc=16, nextra=8, ecut=10.0, solver="chebfsi", tol_efree=1e-9, eig_max_iter=4,
-                      eig_tol=1e-11, max_iter=120, cheby_degree=12)
+                      eig_tol=1e-11, max_iter=120, cheby_degree=12,
+                      wfn_filter=False)
     assert res["converged"] == 1
     F, Floc, Fnl = c.scf_forces()
     del F, Floc

@@ -21,7 +21,8 @@ def test_scf_broyden_matches_oracle(solver, mixed):
     c = Context(L, tuple(g["numGrid"]), tuple(g["numGridFine"]))
     c.set_atoms([g["znuc"]] * len(pos), pos)
     res, eig, rho = c.scf(nocc=16, nextra=8, ecut=g["ecut"], solver=solver, mixed=mixed, eig_max_iter=4,
-                          eig_tol=1e-10, max_iter=80, mix="broyden", tol_rho=1e-12)
+                          eig_tol=1e-10, max_iter=80, mix="broyden", tol_rho=1e-12,
+                          wfn_filter=False)
     assert res["converged"] == 1
     assert res["scf_norm"] < 1e-12
     nat = len(pos)
@@ -38,6 +39,6 @@ def test_anderson_with_the_density_criterion():
     c = Context(L, tuple(g["numGrid"]), tuple(g["numGridFine"]))
     c.set_atoms([g["znuc"]] * len(pos), pos)
     res, eig, rho = c.scf(nocc=16, nextra=8, ecut=g["ecut"], solver="chebfsi", eig_max_iter=4, eig_tol=1e-10,
-                          max_iter=80, tol_rho=1e-12)
+                          max_iter=80, tol_rho=1e-12, wfn_filter=False)
     assert res["converged"] == 1 and res["scf_norm"] < 1e-12
     assert abs(res["efree"] - g["efree"]) / len(pos) < 1e-6

@@ -71,7 +71,7 @@ def test_scf_forces_finite_difference():
     leave ~4e-5 Ha/bohr (measured on a B200) against forces of ~1e-2 Ha/bohr;
     the bar is 2e-4 Ha/bohr."""
     L, z, pos, nc, nf = _setup()
-    kw = dict(nocc=16, nextra=8, ecut=10.0, solver="chebfsi", tol_efree=1e-10, eig_max_iter=4, eig_tol=1e-11,
+    kw = dict(nocc=16, nextra=8, ecut=10.0, solver="chebfsi", wfn_filter=False, tol_efree=1e-10, eig_max_iter=4, eig_tol=1e-11,
               max_iter=120, cheby_degree=12)
     c = _ctx(L, z, pos, nc, nf)
     res, _, _ = c.scf(**kw)

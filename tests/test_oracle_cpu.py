@@ -314,3 +314,22 @@ def test_kpoint_gamma_matches_real_hamiltonian_without_nyquist():
         F[:, :, 4, :] = 0
         F[:, :, :, 4] = 0
     assert np.abs(Fr - Fc).max() <= 1e-10 * np.abs(Fr).max()
+
+
+def test_wfn_ecut_filter_is_an_orthogonal_projector():
+    """MultSpinor's wavefunction filter (hamiltonian.cpp:3090-3116): P is
+    idempotent and symmetric, keeps exactly the coefficients with
+    |G|^2/2 <= Ecut, and the filtered MultSpinor is P applied to H psi."""
+    L, z, pos = pw.make_crystal("Si", (1, 1, 1), 10.26, 0.02, 20261203 + 1)
+    T, _ = pw.build_tables(L, z, pos, (16, 16, 16), (32, 32, 32), seed_v=4)
+    rng = np.random.default_rng(2)
+    x, y = rng.standard_normal((2, 3, T.dm.ntot))
+    ecut = 5.0
+    px = pw.wfn_ecut_filter(T, x, ecut)
+    assert np.abs(pw.wfn_ecut_filter(T, px, ecut) - px).max() < 1e-13
+    assert abs(np.sum(px * y) - np.sum(x * pw.wfn_ecut_filter(T, y, ecut))) < 1e-10
+    X = pw.r2c(px.reshape(3, 16, 16, 16), T.dm)
+    assert np.abs(X[:, T.ekin > ecut]).max() < 1e-12
+    assert np.abs(X[:, T.ekin <= ecut] - pw.r2c(x.reshape(3, 16, 16, 16), T.dm)[:, T.ekin <= ecut]).max() < 1e-12
+    h = pw.mult_spinor(T, x, wfn_ecut=ecut)
+    assert np.abs(h - pw.wfn_ecut_filter(T, pw.mult_spinor(T, x), ecut)).max() < 1e-12

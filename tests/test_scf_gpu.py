@@ -113,7 +113,7 @@ def test_scf_si8_small_matches_oracle(solver, mixed):
     nc = tuple(g["numGrid"])
     c = _ctx(L, g["znuc"], pos, nc, tuple(g["numGridFine"]))
     res, eig, rho = c.scf(nocc=16, nextra=8, ecut=g["ecut"], solver=solver, mixed=mixed, tol_efree=1e-8,
-                          eig_max_iter=4, eig_tol=1e-10, max_iter=80)
+                          eig_max_iter=4, eig_tol=1e-10, max_iter=80, wfn_filter=False)
     assert res["converged"] == 1
     nat = len(pos)
     assert abs(res["efree"] - g["efree"]) / nat < 1e-6
@@ -130,7 +130,8 @@ def test_scf_si8_full_matches_oracle(solver, mixed):
     pos = np.array(g["positions"])
     c = _ctx(L, g["znuc"], pos, tuple(g["numGrid"]), tuple(g["numGridFine"]))
     res, eig, rho = c.scf(nocc=16, nextra=8, ecut=g["ecut"], solver=solver, mixed=mixed, tol_efree=1e-8,
-                          eig_max_iter=4, eig_tol=1e-10, max_iter=80, cheby_degree=12, refine_threshold=1e-6)
+                          eig_max_iter=4, eig_tol=1e-10, max_iter=80, cheby_degree=12, refine_threshold=1e-6,
+                          wfn_filter=False)
     assert res["converged"] == 1
     nat = len(pos)
     assert abs(res["efree"] - g["efree"]) / nat < 1e-6, (res["efree"], g["efree"])

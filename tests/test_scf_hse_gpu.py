@@ -23,7 +23,8 @@ def test_scf_hse06_matches_oracle(solver, mixed):
     c = Context(L, tuple(g["numGrid"]), tuple(g["numGridFine"]))
     c.set_atoms([g["znuc"]] * len(pos), pos)
     res, eig, rho = c.scf(nocc=16, nextra=8, ecut=g["ecut"], solver=solver, mixed=mixed, tol_efree=1e-9,
-                          eig_max_iter=4, eig_tol=1e-10, max_iter=80, xc="hse06", phi_max_iter=20, phi_tol=1e-8)
+                          eig_max_iter=4, eig_tol=1e-10, max_iter=80, xc="hse06", phi_max_iter=20, phi_tol=1e-8,
+                          wfn_filter=False)
     assert res["converged"] == 1, res
     assert res["dexx"] < 1e-8 and res["phi_iterations"] >= 1
     nat = len(pos)
@@ -43,7 +44,7 @@ def test_pbe_scf_after_hybrid_has_no_exchange_term():
     pos = np.array(g["positions"])
     c = Context(L, tuple(g["numGrid"]), tuple(g["numGridFine"]))
     c.set_atoms([g["znuc"]] * len(pos), pos)
-    kw = dict(nocc=16, nextra=8, ecut=g["ecut"], solver="chebfsi", tol_efree=1e-8, eig_max_iter=4, eig_tol=1e-10,
+    kw = dict(nocc=16, nextra=8, ecut=g["ecut"], solver="chebfsi", wfn_filter=False, tol_efree=1e-8, eig_max_iter=4, eig_tol=1e-10,
               max_iter=80)
     res_h, _, _ = c.scf(xc="hse06", phi_max_iter=3, phi_tol=1e-6, **kw)
     assert res_h["phi_iterations"] >= 1

@@ -46,7 +46,7 @@ def test_scf_pbe_matches_oracle(solver, mixed):
     c = Context(L, tuple(g["numGrid"]), tuple(g["numGridFine"]))
     c.set_atoms([g["znuc"]] * len(pos), pos)
     res, eig, rho = c.scf(nocc=16, nextra=8, ecut=g["ecut"], solver=solver, mixed=mixed, tol_efree=1e-8,
-                          eig_max_iter=4, eig_tol=1e-10, max_iter=80, xc="pbe")
+                          eig_max_iter=4, eig_tol=1e-10, max_iter=80, xc="pbe", wfn_filter=False)
     assert res["converged"] == 1
     nat = len(pos)
     assert abs(res["efree"] - g["efree"]) / nat < 1e-6, (res["efree"], g["efree"])
