@@ -187,7 +187,8 @@ PW_API int pw_stats(const pw_ctx* ctx, long* kernel_launches, long* library_call
  * launches of one kernel kind: 0 coarse-plane FFT, 1 z-pad, 2 fine-plane
  * projector gather, 3 projector reduce, 4 fine-plane apply, 5 z-fold,
  * 6 coarse-plane inverse, 7 Teter z-pencil, 8 Gram, 9 density, 10 other,
- * 11 vendor-library GEMM, 12 exact-exchange pair FFTs. */
+ * 11 vendor-library GEMM, 12 exact-exchange pair FFTs, 13 subspace rotation
+ * (X C of the eigensolvers). */
 PW_API int pw_profile(pw_ctx* ctx, int enable);
 PW_API int pw_profile_read(pw_ctx* ctx, int kind, double* total_ms, long* count);
 
@@ -200,6 +201,41 @@ PW_API int pw_profile_read(pw_ctx* ctx, int kind, double* total_ms, long* count)
  * split-BF16 tensor-core GEMMs with FP32 accumulation. */
 PW_API int pw_gram(pw_ctx* ctx, const void* X, int ldx, int nx, const void* Y, int ldy, int ny, double* G, int ldg,
                    void* stream);
+
+/* ---------------------------------------------------------------------------
+ * Small dense FP64 algebra of the eigensolvers (device pointers, column-major;
+ * this library's kernels, where the reference calls LAPACK on rank 0)
+ * ------------------------------------------------------------------------- */
+/* Upper Cholesky A = U^T U in place (lapack::Potrf('U') of
+ * EigenSolver::Orthogonalize, src/EigenSolver/eigensolver.cpp:301-384); the
+ * strict lower part is left as it was; PW_ENUMERIC if A is not positive definite. */
+PW_API int pw_dense_potrf(pw_ctx* ctx, int n, double* A, int lda);
+/* Ui = U^{-1} for an upper-triangular U (the Trsm of Orthogonalize applied to
+ * the identity); the strict lower part of Ui is zeroed. */
+PW_API int pw_dense_trtri(pw_ctx* ctx, int n, const double* U, int ldu, double* Ui, int ldi);
+/* Symmetric eigen-decomposition (lapack::Syevd('V', 'U'), the Rayleigh-Ritz
+ * solves of src/EigenSolver/lobpcg.cpp and eigensolver.cpp:133-299): the upper
+ * triangle of A is read, A's columns receive the eigenvectors, w (device) the
+ * eigenvalues ascending.  Cyclic Jacobi; sweeps (host, may be NULL) reports
+ * the sweeps it took. */
+PW_API int pw_dense_syev(pw_ctx* ctx, int n, double* A, int lda, double* w, int* sweeps);
+/* EigenSolver::SolveGenEig (src/EigenSolver/eigensolver.cpp:133-299, serial
+ * path): symmetrise A and B from their upper triangles, eig(B) = U sigma U^T,
+ * keep the directions with sigma / sigma_max > 1e-8 (numKeep, at least width),
+ * A~ = sigma^-1/2 U^T A U sigma^-1/2, eig(A~), C = U sigma^-1/2 Z.  On exit A
+ * holds C (numCol x numKeep), eig (host) the lowest `width` values. */
+PW_API int pw_solve_gen_eig(pw_ctx* ctx, int lda, int numCol, int width, double* A, double* B, double* eig,
+                            int* numKeep);
+
+/* Subspace rotation Out (+)= X C over the coarse grid: X (ntot x k, ldx) and
+ * Out (ntot x m, ldo) in the context's precision, C (k x m, ldc) FP64 on the
+ * device; the X <- X C updates of Orthogonalize and LOBPCGSolveReal
+ * (blas::Gemm('N', 'N'), src/EigenSolver/eigensolver.cpp:301-384,
+ * lobpcg.cpp:869-1000).  FP32 contexts: split-BF16 tensor-core GEMM (C rounded
+ * to FP32, then split); FP64 contexts: this library's FP64 kernel.  Out must
+ * not overlap X. */
+PW_API int pw_rotate(pw_ctx* ctx, const void* X, int ldx, int k, const double* C, int ldc, int m, void* Out, int ldo,
+                     int accumulate, void* stream);
 
 /* ---------------------------------------------------------------------------
  * Block eigensolvers and SCF

@@ -81,6 +81,11 @@ SIGNATURES: dict[str, tuple] = {
     "pw_teter_precond_noalloc": (_i, [_vp, _vp, _i, _vp, _i, _i, _i, _vp]),
     "pw_set_wfn_filter": (_i, [_vp, _i, C.c_double]),
     "pw_set_wait_limit": (_i, [_vp, C.c_double]),
+    "pw_dense_potrf": (_i, [_vp, _i, _vp, _i]),
+    "pw_rotate": (_i, [_vp, _vp, _i, _i, _vp, _i, _i, _vp, _i, _i, _vp]),
+    "pw_dense_trtri": (_i, [_vp, _i, _vp, _i, _vp, _i]),
+    "pw_dense_syev": (_i, [_vp, _i, _vp, _i, _vp, _ip]),
+    "pw_solve_gen_eig": (_i, [_vp, _i, _i, _i, _vp, _vp, _dp, _ip]),
     "pw_wait_probe": (_i, [_vp, C.c_double]),
     "pw_wfn_filter": (_i, [_vp, _vp, _i, _i, _vp]),
     "pw_set_band_batch": (_i, [_vp, _i]),

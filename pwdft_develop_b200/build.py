@@ -88,7 +88,7 @@ def build(verbose: bool = False, jobs: int | None = None, extra: list[str] | Non
                         print(log, file=sys.stderr)
     if todo or not LIB.exists():
         cmd = [nvcc()] + ARCH + ["-shared", "-o", str(LIB)] + [str(o) for o in objs] + \
-            ["-lcublas", "-lcusolver", "-lcudart"]
+            ["-lcublas", "-lcudart"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{' '.join(cmd)}\n{r.stdout}\n{r.stderr}")

@@ -314,7 +314,7 @@ Context.profile_read = _ctx_profile_read
 
 KERNEL_KINDS = {0: "coarse_xy_fwd", 1: "z_pad", 2: "fine_plane_gather", 3: "nl_reduce", 4: "fine_plane_apply",
                 5: "z_fold", 6: "coarse_xy_inv", 7: "z_teter", 8: "gram", 9: "density", 10: "other",
-                11: "library_gemm", 12: "exchange"}
+                11: "library_gemm", 12: "exchange", 13: "rotation"}
 
 
 # ---------------------------------------------------------------------------

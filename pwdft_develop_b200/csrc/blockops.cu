@@ -1,4 +1,6 @@
 // Device block operations for the eigensolvers and the SCF driver.
+#include <cuda_bf16.h>
+
 #include <algorithm>
 #include <vector>
 
@@ -266,28 +268,123 @@ template int bdiag_rotate<float>(int, int, int, const float*, long, const double
 template int bdiag_rotate<double>(int, int, int, const double*, long, const double*, double*, long, double,
                                   cudaStream_t);
 
+// C (k x m, FP64 column-major) -> C^T as bf16 hi / lo rows (m rows of k, row stride ldo)
+__global__ void k_split_c_t(const double* __restrict__ C, int ldc, int k, int m, __nv_bfloat16* __restrict__ hi,
+                            __nv_bfloat16* __restrict__ lo, long ldo) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= (long)k * m) return;
+  const int b = (int)(i % k), j = (int)(i / k);
+  const float v = (float)C[(long)j * ldc + b];
+  const __nv_bfloat16 h = __float2bfloat16_rn(v);
+  hi[(long)j * ldo + b] = h;
+  lo[(long)j * ldo + b] = __float2bfloat16_rn(v - __bfloat162float(h));
+}
+
+// FP64 tall-skinny rotation Out (n x m) (+)= X (n x k) C (k x m), column-major
+// (X and Out grid-fastest): a CTA owns 128 grid rows x 64 columns, C and X
+// staged through shared memory in k-chunks of 16, 8 x 4 outputs per thread
+constexpr int RT_M = 128, RT_N = 64, RT_K = 16;
+__global__ void __launch_bounds__(256) k_rot_f64(int n, int m, int k, const double* __restrict__ X, long ldx,
+                                                 const double* __restrict__ C, int ldc, double* __restrict__ Out,
+                                                 long ldo, int accumulate) {
+  __shared__ double Xs[RT_K][RT_M + 1];
+  __shared__ double Cs[RT_K][RT_N + 1];
+  const int g0 = blockIdx.x * RT_M, j0 = blockIdx.y * RT_N;
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;    // 16 x 16 threads
+  double acc[8][4];
+#pragma unroll
+  for (int a = 0; a < 8; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+  for (int b0 = 0; b0 < k; b0 += RT_K) {
+    for (int e = threadIdx.x; e < RT_K * RT_M; e += 256) {
+      const int bb = e / RT_M, gg = e % RT_M;
+      const int b = b0 + bb, g = g0 + gg;
+      Xs[bb][gg] = (b < k && g < n) ? X[(long)b * ldx + g] : 0.0;
+    }
+    for (int e = threadIdx.x; e < RT_K * RT_N; e += 256) {
+      const int bb = e % RT_K, jj = e / RT_K;
+      const int b = b0 + bb, j = j0 + jj;
+      Cs[bb][jj] = (b < k && j < m) ? C[(long)j * ldc + b] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int bb = 0; bb < RT_K; ++bb) {
+      double xv[8], cv[4];
+#pragma unroll
+      for (int a = 0; a < 8; ++a) xv[a] = Xs[bb][tx + 16 * a];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) cv[b] = Cs[bb][ty + 16 * b];
+#pragma unroll
+      for (int a = 0; a < 8; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = fma(xv[a], cv[b], acc[a][b]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int b = 0; b < 4; ++b) {
+    const int j = j0 + ty + 16 * b;
+    if (j >= m) continue;
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+      const int g = g0 + tx + 16 * a;
+      if (g < n) {
+        double* o = Out + (long)j * ldo + g;
+        *o = accumulate ? *o + acc[a][b] : acc[a][b];
+      }
+    }
+  }
+}
+
+// FP32 rotation on the split-BF16 tensor-core GEMM: X^T split into bf16 hi / lo
+// rows (grid-major, K = k bands), C^T likewise, Out^T written grid-fastest
+static int rotate_tc(pw_ctx* c, int n, int m, const RotBlock& B, float* out, long ldo, int accumulate,
+                     cudaStream_t st) {
+  const int k = B.k;
+  const long kp = (k + 7) / 8 * 8;
+  int rc;
+  if ((rc = c->s_rot_x.alloc((size_t)2 * n * kp * 2)) || (rc = c->s_rot.alloc((size_t)2 * m * kp * 2))) return rc;
+  char* xh = (char*)c->s_rot_x.p;
+  char* xl = xh + (size_t)n * kp * 2;
+  char* ch = (char*)c->s_rot.p;
+  char* cl = ch + (size_t)m * kp * 2;
+  { Launch L_(c, st, KK_MISC);
+  if ((rc = split_bf16_t((const float*)B.X, B.ldx, n, k, xh, xl, kp, st))) return rc; }
+  { Launch L_(c, st, KK_MISC);
+  const long tot = (long)k * m;
+  k_split_c_t<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(B.C, B.ldc, k, m, (__nv_bfloat16*)ch,
+                                                             (__nv_bfloat16*)cl, kp);
+  PWB_CUDA(cudaGetLastError()); }
+  SplitOperand A{xh, xl, n, kp};
+  SplitOperand Bo{ch, cl, m, kp};
+  Launch L_(c, st, KK_ROT);
+  return gemm_tn_store(A, Bo, k, c->gemm_terms, out, ldo, accumulate, st, 1, 0);
+}
+
 int rotate(pw_ctx* c, int n, int m, const RotBlock* blocks, int nblk, void* out, long ldo, double beta, cudaStream_t st) {
-  cublasHandle_t h = (cublasHandle_t)c->blas;
-  cublasSetStream(h, st);
+  PWB_CHECK(beta == 0.0 || beta == 1.0, PW_EINVAL, "rotation: beta must be 0 or 1");
   for (int b = 0; b < nblk; ++b) {
     const RotBlock& B = blocks[b];
     if (B.k == 0) continue;
-    const double be = (b == 0) ? beta : 1.0;
-    c->lib_launches++;
+    const int acc = (b == 0) ? (beta != 0.0) : 1;
+    int rc;
     if (c->prec == PW_F64) {
-      const double one = 1.0;
-      if (cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, m, B.k, &one, (const double*)B.X, (int)B.ldx, B.C, B.ldc, &be,
-                      (double*)out, (int)ldo) != CUBLAS_STATUS_SUCCESS) {
-        set_error("rotation GEMM failed");
-        return PW_ECUDA;
-      }
+      dim3 grid((n + RT_M - 1) / RT_M, (m + RT_N - 1) / RT_N);
+      Launch L_(c, st, KK_ROT);
+      k_rot_f64<<<grid, 256, 0, st>>>(n, m, B.k, (const double*)B.X, B.ldx, B.C, B.ldc, (double*)out, ldo, acc);
+      PWB_CUDA(cudaGetLastError());
+    } else if (c->gemm_mode == 0) {
+      if ((rc = rotate_tc(c, n, m, B, (float*)out, ldo, acc, st))) return rc;
     } else {
-      // FP32 storage: the small FP64 coefficient block is rounded to FP32
-      int rc = c->s_rot.alloc((size_t)B.k * m * 4);
-      if (rc) return rc;
+      // vendor SGEMM comparator mode (pw_set_gemm_mode 1): the FP64 block rounded to FP32
+      cublasHandle_t h = (cublasHandle_t)c->blas;
+      cublasSetStream(h, st);
+      c->lib_launches++;
+      if ((rc = c->s_rot.alloc((size_t)B.k * m * 4))) return rc;
       float* Cf = (float*)c->s_rot.p;
       if ((rc = copy_d2f_2d(B.k, m, B.C, B.ldc, Cf, B.k, st))) return rc;
-      const float one = 1.0f, bf = (float)be;
+      const float one = 1.0f, bf = (float)acc;
       if (cublasSgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, m, B.k, &one, (const float*)B.X, (int)B.ldx, Cf, B.k, &bf,
                       (float*)out, (int)ldo) != CUBLAS_STATUS_SUCCESS) {
         set_error("rotation GEMM failed");
@@ -300,53 +397,19 @@ int rotate(pw_ctx* c, int n, int m, const RotBlock* blocks, int nblk, void* out,
 
 int Dense::init(cublasHandle_t b) {
   blas = b;
-  if (!sol && cusolverDnCreate(&sol) != CUSOLVER_STATUS_SUCCESS) {
-    set_error("cusolverDnCreate failed");
-    return PW_ECUDA;
-  }
   return info.alloc(64);
 }
-void Dense::release() {
-  if (sol) cusolverDnDestroy(sol);
-  sol = nullptr;
-}
+void Dense::release() {}
 
+// eigenvectors (in A) and ascending eigenvalues by the library's Jacobi
+// kernel (smalldense.cu)
 int Dense::syevd(int n, double* A, int lda, double* w, cudaStream_t st) {
-  cusolverDnSetStream(sol, st);
-  int lw = 0;
-  if (cusolverDnDsyevd_bufferSize(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, n, A, lda, w, &lw) !=
-      CUSOLVER_STATUS_SUCCESS) {
-    set_error("syevd buffer query failed");
-    return PW_ECUDA;
-  }
-  int rc = work.alloc((size_t)std::max(lw, 1) * 8);
-  if (rc) return rc;
-  if (cusolverDnDsyevd(sol, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, n, A, lda, w, (double*)work.p, lw,
-                       (int*)info.p) != CUSOLVER_STATUS_SUCCESS) {
-    set_error("syevd failed");
-    return PW_ECUDA;
-  }
-  int hinfo = 0;
-  PWB_CUDA(cudaMemcpyAsync(&hinfo, info.p, sizeof(int), cudaMemcpyDeviceToHost, st));
-  PWB_CUDA(cudaStreamSynchronize(st));
-  PWB_CHECK(hinfo == 0, PW_ENUMERIC, "syevd did not converge");
-  return PW_OK;
+  return dense_syevj(n, A, lda, w, work, nullptr, st);
 }
 
 int Dense::potrf_upper(int n, double* A, int lda, cudaStream_t st) {
-  cusolverDnSetStream(sol, st);
-  int lw = 0;
-  if (cusolverDnDpotrf_bufferSize(sol, CUBLAS_FILL_MODE_UPPER, n, A, lda, &lw) != CUSOLVER_STATUS_SUCCESS) {
-    set_error("potrf buffer query failed");
-    return PW_ECUDA;
-  }
-  int rc = work.alloc((size_t)std::max(lw, 1) * 8);
+  int rc = dense_potrf_upper(n, A, lda, (int*)info.p, st);
   if (rc) return rc;
-  if (cusolverDnDpotrf(sol, CUBLAS_FILL_MODE_UPPER, n, A, lda, (double*)work.p, lw, (int*)info.p) !=
-      CUSOLVER_STATUS_SUCCESS) {
-    set_error("potrf failed");
-    return PW_ECUDA;
-  }
   int hinfo = 0;
   PWB_CUDA(cudaMemcpyAsync(&hinfo, info.p, sizeof(int), cudaMemcpyDeviceToHost, st));
   PWB_CUDA(cudaStreamSynchronize(st));
@@ -417,26 +480,16 @@ int solve_gen_eig(Dense& d, int lda, int numCol, int width, double* A, double* B
   // Atilde = U_k^T A U_k
   if ((rc = d.tmp1.alloc((size_t)lda * lda * 8))) return rc;
   double* T1 = (double*)d.tmp1.p;
-  const double one = 1.0, zero = 0.0;
-  cublasSetStream(d.blas, st);
   const double* Uk = B + (long)(numCol - numKeep) * lda;
-  if (cublasDgemm(d.blas, CUBLAS_OP_N, CUBLAS_OP_N, numCol, numKeep, numCol, &one, A, lda, Uk, lda, &zero, T1, lda) !=
-          CUBLAS_STATUS_SUCCESS ||
-      cublasDgemm(d.blas, CUBLAS_OP_T, CUBLAS_OP_N, numKeep, numKeep, numCol, &one, Uk, lda, T1, lda, &zero, A, lda) !=
-          CUBLAS_STATUS_SUCCESS) {
-    set_error("SolveGenEig GEMM failed");
-    return PW_ECUDA;
-  }
+  if ((rc = dense_gemm(0, 0, numCol, numKeep, numCol, A, lda, Uk, lda, T1, lda, st)) ||
+      (rc = dense_gemm(1, 0, numKeep, numKeep, numCol, Uk, lda, T1, lda, A, lda, st)))
+    return rc;
   k_scale_sym<<<numKeep, 128, 0, st>>>(numKeep, A, lda, inv, 1);
   if ((rc = d.syevd(numKeep, A, lda, eigs, st))) return rc;
   PWB_CUDA(cudaMemcpyAsync(eig_host, eigs, width * 8, cudaMemcpyDeviceToHost, st));
   k_scale_sym<<<numKeep, 128, 0, st>>>(numKeep, A, lda, inv, 0);
   // C = U_k * Z'
-  if (cublasDgemm(d.blas, CUBLAS_OP_N, CUBLAS_OP_N, numCol, numKeep, numKeep, &one, Uk, lda, A, lda, &zero, T1, lda) !=
-      CUBLAS_STATUS_SUCCESS) {
-    set_error("SolveGenEig GEMM failed");
-    return PW_ECUDA;
-  }
+  if ((rc = dense_gemm(0, 0, numCol, numKeep, numKeep, Uk, lda, A, lda, T1, lda, st))) return rc;
   PWB_CUDA(cudaMemcpy2DAsync(A, (size_t)lda * 8, T1, (size_t)lda * 8, (size_t)numCol * 8, numKeep,
                              cudaMemcpyDeviceToDevice, st));
   PWB_CUDA(cudaStreamSynchronize(st));

@@ -1,7 +1,6 @@
 // Device block operations used by the eigensolvers and the SCF driver.
 #pragma once
 #include <cublas_v2.h>
-#include <cusolverDn.h>
 
 #include "common.hpp"
 
@@ -50,18 +49,28 @@ struct RotBlock {
 };
 int rotate(pw_ctx* c, int n, int m, const RotBlock* blocks, int nblk, void* out, long ldo, double beta, cudaStream_t st);
 
-// Small dense FP64 algebra on the device (cuSOLVER / cuBLAS), n <= a few thousand.
+// Small dense FP64 algebra on the device with this library's kernels
+// (smalldense.cu), n up to a few thousand.
 struct Dense {
-  cusolverDnHandle_t sol = nullptr;
   cublasHandle_t blas = nullptr;
   DevBuf work, info, tmp1, tmp2, tmp3, wvec;
   int init(cublasHandle_t b);
   void release();
-  // eigen-decomposition in place: A (n x n, lda) -> eigenvectors, w (device) ascending
+  // eigen-decomposition in place: A (n x n, lda; upper triangle read) -> eigenvectors, w (device) ascending
   int syevd(int n, double* A, int lda, double* w, cudaStream_t st);
   // upper Cholesky A = U^T U in place; returns PW_ENUMERIC if not positive definite
   int potrf_upper(int n, double* A, int lda, cudaStream_t st);
 };
+
+// smalldense.cu: blocked upper Cholesky (info_dev: 0, or the failing column + 1),
+// inverse of an upper-triangular matrix (strict lower part of Ui zeroed),
+// C = op(A) op(B) (ta / tb: 1 = transposed), Jacobi eigen-decomposition (ws:
+// workspace, sweeps_dev may be NULL)
+int dense_potrf_upper(int n, double* A, int lda, int* info_dev, cudaStream_t st);
+int dense_trtri_upper(int n, const double* U, int ldu, double* Ui, int ldi, cudaStream_t st);
+int dense_gemm(int ta, int tb, int m, int n, int k, const double* A, int lda, const double* B, int ldb, double* C,
+               int ldc, cudaStream_t st);
+int dense_syevj(int n, double* A, int lda, double* w, DevBuf& ws, int* sweeps_dev, cudaStream_t st);
 
 // n x n column-major blocks on the device, queued on st: lower part from the
 // upper triangle, strict lower part zeroed, identity

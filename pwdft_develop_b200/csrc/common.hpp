@@ -76,7 +76,7 @@ struct NonlocalDev {
 // Kernel kinds for pw_profile_read.
 enum KernelKind {
   KK_CXY_FWD = 0, KK_ZPAD, KK_FPLANE_GATHER, KK_NL_REDUCE, KK_FPLANE_APPLY, KK_ZFOLD, KK_CXY_INV, KK_ZTETER,
-  KK_GRAM, KK_DENSITY, KK_MISC, KK_LIBGEMM, KK_EXX, KK_COUNT
+  KK_GRAM, KK_DENSITY, KK_MISC, KK_LIBGEMM, KK_EXX, KK_ROT, KK_COUNT
 };
 
 // A dense coarse-grid operator Q diag(qd) Q^T: the projector matrix, or the
@@ -129,7 +129,7 @@ struct pw_ctx {
   bool check_errors = false;     // read the device error flag after each call (synchronises)
   pw_ctx* twin = nullptr;        // FP32 twin of an FP64 context (mixed-precision SCF), owned
   int nproj_pad = 0;
-  pwb::DevBuf q_bf, qt_bf, s_psi_bf, s_w_bf, s_ws, s_gx_bf, s_gy_bf, s_rot;
+  pwb::DevBuf q_bf, qt_bf, s_psi_bf, s_w_bf, s_ws, s_gx_bf, s_gy_bf, s_rot, s_rot_x;
   // host copies kept for setup-time work
   std::vector<double> h_vtot;
   // atoms set through pw_set_atoms (HGH species built in this library)

@@ -7,6 +7,7 @@
 #include <algorithm>
 
 #include "common.hpp"
+#include "blockops.hpp"
 #include "gemm.hpp"
 
 using namespace pwb;
@@ -66,6 +67,25 @@ int pw_gram(pw_ctx* ctx, const void* X, int ldx, int nx, const void* Y, int ldy,
   PWB_CHECK(ldx >= ctx->ntot && ldy >= ctx->ntot && ldg >= nx, PW_EINVAL, "bad leading dimension");
   PWB_CUDA(cudaSetDevice(ctx->device));
   int rc = gram(ctx, X, ldx, nx, Y, ldy, ny, G, ldg, (cudaStream_t)stream);
+  if (rc) return rc;
+  if (ctx->check_errors) return gemm_error_check();
+  return PW_OK;
+}
+
+int pw_rotate(pw_ctx* ctx, const void* X, int ldx, int k, const double* C, int ldc, int m, void* Out, int ldo,
+              int accumulate, void* stream) {
+  PWB_CHECK(ctx && k >= 0 && m >= 0 && (k * m == 0 || (X && C && Out)), PW_EINVAL, "null argument");
+  PWB_CHECK(ldx >= ctx->ntot && ldo >= ctx->ntot && ldc >= k, PW_EINVAL, "bad leading dimension");
+  PWB_CUDA(cudaSetDevice(ctx->device));
+  if (m == 0) return PW_OK;
+  if (k == 0) {
+    if (!accumulate)
+      PWB_CUDA(cudaMemset2DAsync(Out, (size_t)ldo * ctx->esz, 0, (size_t)ctx->ntot * ctx->esz, m,
+                                 (cudaStream_t)stream));
+    return PW_OK;
+  }
+  RotBlock rb{X, ldx, k, C, ldc};
+  int rc = rotate(ctx, (int)ctx->ntot, m, &rb, 1, Out, ldo, accumulate ? 1.0 : 0.0, (cudaStream_t)stream);
   if (rc) return rc;
   if (ctx->check_errors) return gemm_error_check();
   return PW_OK;

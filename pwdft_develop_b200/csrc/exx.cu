@@ -243,23 +243,8 @@ int pw_ace_build(pw_ctx* ctx, const void* psi, int ld, int nband) {
     dn.release();
     return PW_ENUMERIC;
   }
-  PWB_CUDA(cudaMemcpy(h.data(), M.p, h.size() * 8, cudaMemcpyDeviceToHost));
-  for (int j = 0; j < nband; ++j)
-    for (int i = j + 1; i < nband; ++i) h[(size_t)j * nband + i] = 0.0;
-  PWB_CUDA(cudaMemcpy(M.p, h.data(), h.size() * 8, cudaMemcpyHostToDevice));
-  std::vector<double> I((size_t)nband * nband, 0.0);
-  for (int i = 0; i < nband; ++i) I[(size_t)i * nband + i] = 1.0;
-  PWB_CUDA(cudaMemcpy(Ui.p, I.data(), I.size() * 8, cudaMemcpyHostToDevice));
-  const double one = 1.0;
-  cublasSetStream(dn.blas, nullptr);
-  if (cublasDtrsm(dn.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, nband, nband,
-                  &one, (const double*)M.p, nband, (double*)Ui.p, nband) != CUBLAS_STATUS_SUCCESS) {
-    dn.release();
-    set_error("ACE: trsm failed");
-    return PW_ECUDA;
-  }
+  if ((rc = dense_trtri_upper(nband, (const double*)M.p, nband, (double*)Ui.p, nband, nullptr))) return rc;
   dn.release();
-  ctx->lib_launches += 2;
   if ((rc = ctx->ace_xi.alloc((size_t)nband * nt * esz))) return rc;
   RotBlock rb{W.p, nt, nband, (const double*)Ui.p, nband};
   if ((rc = rotate(ctx, (int)nt, nband, &rb, 1, ctx->ace_xi.p, nt, 0.0, nullptr))) return rc;

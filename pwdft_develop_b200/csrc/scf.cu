@@ -443,19 +443,10 @@ static int cholqr(Solver& s, Dense& d, void* X, int nb, void* tmp) {
   { SubTimer t_(1); if ((rc = gram(s.c, X, (int)s.nt, nb, X, (int)s.nt, nb, G, nb, st))) return rc; }
   SubTimer td_(2);
   if ((rc = d.potrf_upper(nb, G, nb, st))) return rc;
-  // Uinv = U^{-1} (upper): solve U * Uinv = I
+  // Uinv = U^{-1} (upper): U * Uinv = I
   if ((rc = s.G2.alloc((size_t)nb * nb * 8))) return rc;
   double* Ui = (double*)s.G2.p;
-  if ((rc = dense_identity(nb, Ui, nb, st))) return rc;
-  const double one = 1.0;
-  cublasSetStream(d.blas, st);
-  // zero the strict lower part of G first (potrf leaves it untouched)
-  if ((rc = dense_zero_lower(nb, G, nb, st))) return rc;
-  if (cublasDtrsm(d.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, nb, nb, &one, G,
-                  nb, Ui, nb) != CUBLAS_STATUS_SUCCESS) {
-    set_error("trsm failed");
-    return PW_ECUDA;
-  }
+  if ((rc = dense_trtri_upper(nb, G, nb, Ui, nb, st))) return rc;
   RotBlock rb{X, s.nt, nb, Ui, nb};
   { SubTimer t_(3); if ((rc = rotate(s.c, (int)s.nt, nb, &rb, 1, tmp, s.nt, 0.0, st))) return rc; }
   PWB_CUDA(cudaMemcpy(X, tmp, (size_t)nb * s.nt * s.esz, cudaMemcpyDeviceToDevice));
@@ -678,6 +669,12 @@ static int chebfsi_step(Solver& s, Dense& d, int nb, int degree, double a, doubl
   int rc;
   void* res = nullptr;
   if ((rc = cheby_filter_run(s, nb, degree, a, b, a0, &res))) return rc;
+  // With the wavefunction cut-off filter, P H is P H P on the span of P and
+  // zero on its complement; the shifted recurrence amplifies whatever part of
+  // the block lies in the complement (rounding of the transforms) at the
+  // eigenvalue 0, which sits inside the wanted part of the spectrum.  One P
+  // pass over the filtered block keeps the iteration in the span of P.
+  if (s.c->wfn_filter && (rc = wfn_filter_pass(s.c, res, (int)s.nt, nb, nullptr))) return rc;
   // res is one of X, Y, Z; orthonormalise it, then Rayleigh-Ritz into X / HX
   void* tmp = (res == s.Z.p) ? s.Y.p : s.Z.p;
   if ((rc = cholqr(s, d, res, nb, tmp))) return rc;
@@ -959,16 +956,8 @@ static int cholqr_pair(Solver& s, Dense& d, void* X, void* AX, int nb, void* tmp
   double* G = (double*)s.G1.p;
   if ((rc = gram(s.c, X, (int)s.nt, nb, X, (int)s.nt, nb, G, nb, st))) return rc;
   if ((rc = d.potrf_upper(nb, G, nb, st))) return rc;
-  if ((rc = dense_zero_lower(nb, G, nb, st))) return rc;
   double* Ui = (double*)s.G2.p;
-  if ((rc = dense_identity(nb, Ui, nb, st))) return rc;
-  const double one = 1.0;
-  cublasSetStream(d.blas, st);
-  if (cublasDtrsm(d.blas, CUBLAS_SIDE_LEFT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N, CUBLAS_DIAG_NON_UNIT, nb, nb, &one, G,
-                  nb, Ui, nb) != CUBLAS_STATUS_SUCCESS) {
-    set_error("trsm failed");
-    return PW_ECUDA;
-  }
+  if ((rc = dense_trtri_upper(nb, G, nb, Ui, nb, st))) return rc;
   RotBlock rb{X, s.nt, nb, Ui, nb};
   if ((rc = rotate(s.c, (int)s.nt, nb, &rb, 1, tmp, s.nt, 0.0, st))) return rc;
   PWB_CUDA(cudaMemcpy(X, tmp, (size_t)nb * s.nt * s.esz, cudaMemcpyDeviceToDevice));
