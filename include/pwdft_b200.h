@@ -236,6 +236,15 @@ PW_API int pw_solve_gen_eig(pw_ctx* ctx, int lda, int numCol, int width, double*
  * not overlap X. */
 PW_API int pw_rotate(pw_ctx* ctx, const void* X, int ldx, int k, const double* C, int ldc, int m, void* Out, int ldo,
                      int accumulate, void* stream);
+/* The Gram block and the rotation over the first nrow rows only: a row block
+ * of the grid, the local product of the reference's band <-> grid-row
+ * transposed eigensolver steps (AlltoallForward, local Gemm, MPI_Allreduce;
+ * src/utility.cpp:1159-1197, src/EigenSolver/lobpcg.cpp:683-687).  FP32
+ * contexts need nrow and the leading dimensions to be multiples of 8. */
+PW_API int pw_gram_rows(pw_ctx* ctx, int nrow, const void* X, int ldx, int nx, const void* Y, int ldy, int ny,
+                        double* G, int ldg, void* stream);
+PW_API int pw_rotate_rows(pw_ctx* ctx, int nrow, const void* X, int ldx, int k, const double* C, int ldc, int m,
+                          void* Out, int ldo, int accumulate, void* stream);
 
 /* ---------------------------------------------------------------------------
  * Block eigensolvers and SCF

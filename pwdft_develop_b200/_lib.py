@@ -83,6 +83,8 @@ SIGNATURES: dict[str, tuple] = {
     "pw_set_wait_limit": (_i, [_vp, C.c_double]),
     "pw_dense_potrf": (_i, [_vp, _i, _vp, _i]),
     "pw_rotate": (_i, [_vp, _vp, _i, _i, _vp, _i, _i, _vp, _i, _i, _vp]),
+    "pw_gram_rows": (_i, [_vp, _i, _vp, _i, _i, _vp, _i, _i, _vp, _i, _vp]),
+    "pw_rotate_rows": (_i, [_vp, _i, _vp, _i, _i, _vp, _i, _i, _vp, _i, _i, _vp]),
     "pw_dense_trtri": (_i, [_vp, _i, _vp, _i, _vp, _i]),
     "pw_dense_syev": (_i, [_vp, _i, _vp, _i, _vp, _ip]),
     "pw_solve_gen_eig": (_i, [_vp, _i, _i, _i, _vp, _vp, _dp, _ip]),

@@ -114,6 +114,60 @@ template int axpbypcz<double>(int, int, double, const double*, double, const dou
                               long, cudaStream_t);
 template int colnorm2<float>(int, int, const float*, long, double*, cudaStream_t);
 template int colnorm2<double>(int, int, const double*, long, double*, cudaStream_t);
+// B = alpha A for an m x n column-major block
+__global__ void k_dense_scale(int m, int n, double alpha, const double* __restrict__ A, int lda, double* __restrict__ B,
+                              int ldb) {
+  const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (i >= (long)m * n) return;
+  const int r = (int)(i % m), c = (int)(i / m);
+  B[(long)c * ldb + r] = alpha * A[(long)c * lda + r];
+}
+int dense_scale(int m, int n, double alpha, const double* A, int lda, double* B, int ldb, cudaStream_t st) {
+  if ((long)m * n == 0) return PW_OK;
+  k_dense_scale<<<(unsigned)(((long)m * n + 255) / 256), 256, 0, st>>>(m, n, alpha, A, lda, B, ldb);
+  PWB_CUDA(cudaGetLastError());
+  return PW_OK;
+}
+
+// v[i] <- 1 / sqrt(v[i])
+__global__ void k_rsqrt(int n, double* v) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) v[i] = v[i] > 1e-300 ? 1.0 / sqrt(v[i]) : 0.0;
+}
+int vec_rsqrt(int n, double* v, cudaStream_t st) {
+  if (n <= 0) return PW_OK;
+  k_rsqrt<<<(n + 255) / 256, 256, 0, st>>>(n, v);
+  PWB_CUDA(cudaGetLastError());
+  return PW_OK;
+}
+
+// residual norms of the eigensolvers, ||r_k|| / max(1, |lambda_k|) with
+// lambda_k = G(k, k) (lobpcg.cpp:705-709), and their maximum in out[n]; one CTA
+__global__ void k_resnorm(int n, const double* __restrict__ nrm2, const double* __restrict__ G, int ldg,
+                          double* __restrict__ out) {
+  __shared__ double red[32];
+  double mx = 0.0;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    const double r = sqrt(nrm2[k]) / fmax(1.0, fabs(G[(long)k * ldg + k]));
+    out[k] = r;
+    mx = fmax(mx, r);
+  }
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, red[w]);
+    out[n] = m;
+  }
+}
+int resnorms(int n, const double* nrm2, const double* G, int ldg, double* out, cudaStream_t st) {
+  if (n <= 0) return PW_OK;
+  k_resnorm<<<1, 256, 0, st>>>(n, nrm2, G, ldg, out);
+  PWB_CUDA(cudaGetLastError());
+  return PW_OK;
+}
+
 template int colscale<float>(int, int, float*, long, const double*, cudaStream_t);
 template int colscale<double>(int, int, double*, long, const double*, cudaStream_t);
 
@@ -245,6 +299,215 @@ int bdiag_dots(int n, int width, int sb, const T* U, const T* V, long ld, DevBuf
   return PW_OK;
 }
 
+// out[k * sb * sb + i + j * sb] = sum over the grid splits (fixed order)
+__global__ void k_bdiag_sum(const double* __restrict__ part, int nsplit, int nsb, int SBp, int sb,
+                            double* __restrict__ out) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= nsb * sb * sb) return;
+  const int k = idx / (sb * sb), r = idx % (sb * sb), i = r % sb, j = r / sb;
+  double x = 0;
+  for (int sp = 0; sp < nsplit; ++sp) x += part[((long)sp * nsb + k) * SBp * SBp + i + j * SBp];
+  out[idx] = x;
+}
+
+template <typename T>
+int bdiag_dots_dev(int n, int width, int sb, const T* U, const T* V, long ld, DevBuf& part, double* out_dev,
+                   cudaStream_t st) {
+  PWB_CHECK(sb >= 1 && sb <= 8, PW_EUNSUPPORTED, "sub-block size 1..8");
+  const int nsb = (width + sb - 1) / sb;
+  const int nsplit = std::max(1, std::min(64, (n + 4095) / 4096));
+  const int chunk = (n + nsplit - 1) / nsplit;
+  const int SBp = sb == 1 ? 1 : sb == 2 ? 2 : sb <= 4 ? 4 : 8;
+  int rc = part.alloc((size_t)nsplit * nsb * SBp * SBp * 8);
+  if (rc) return rc;
+  double* pp = (double*)part.p;
+  dim3 grid(nsb, nsplit);
+  switch (SBp) {
+    case 1: k_bdiag_dots<T, 1><<<grid, 256, 0, st>>>(n, width, sb, U, V, ld, chunk, pp); break;
+    case 2: k_bdiag_dots<T, 2><<<grid, 256, 0, st>>>(n, width, sb, U, V, ld, chunk, pp); break;
+    case 4: k_bdiag_dots<T, 4><<<grid, 256, 0, st>>>(n, width, sb, U, V, ld, chunk, pp); break;
+    default: k_bdiag_dots<T, 8><<<grid, 256, 0, st>>>(n, width, sb, U, V, ld, chunk, pp); break;
+  }
+  const int tot = nsb * sb * sb;
+  k_bdiag_sum<<<(tot + 255) / 256, 256, 0, st>>>(pp, nsplit, nsb, SBp, sb, out_dev);
+  PWB_CUDA(cudaGetLastError());
+  return PW_OK;
+}
+template int bdiag_dots_dev<float>(int, int, int, const float*, const float*, long, DevBuf&, double*, cudaStream_t);
+template int bdiag_dots_dev<double>(int, int, int, const double*, const double*, long, DevBuf&, double*,
+                                    cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// PPCG sub-block generalized eigenproblems on the device: one warp per
+// sub-block k solves A z = lambda B z (dim = numSet * m <= 24) with the cut of
+// SolveGenEig: cyclic Jacobi of B, directions with sigma / sigma_max > 1e-8
+// kept, Q = U_k sigma_k^-1/2, Jacobi of Q^T A Q, ascending order, Z = Q V; the
+// coefficient blocks cx, cw, cp of x <- x cx + w cw + p cp (ppcg.cpp:
+// 1001-1090).  Fewer kept directions than columns: x is kept (cx = I).
+// ---------------------------------------------------------------------------
+constexpr int SYGV_MAX = 24;
+
+__device__ void warp_jacobi(int n, double* M, double* V) {
+  const int lane = threadIdx.x & 31;
+  for (int e = lane; e < n * n; e += 32) V[e] = (e % n == e / n) ? 1.0 : 0.0;
+  __syncwarp();
+  for (int sweep = 0; sweep < 100; ++sweep) {
+    double off = 0.0, tot = 0.0;
+    for (int e = lane; e < n * n; e += 32) {
+      const double x = M[e];
+      tot += x * x;
+      if (e % n != e / n) off += x * x;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      off += __shfl_xor_sync(0xffffffffu, off, o);
+      tot += __shfl_xor_sync(0xffffffffu, tot, o);
+    }
+    if (off == 0.0 || off <= 1e-30 * tot) break;
+    for (int p = 0; p < n - 1; ++p)
+      for (int q = p + 1; q < n; ++q) {
+        const double apq = M[p + q * n];
+        if (apq == 0.0) continue;
+        const double app = M[p + p * n], aqq = M[q + q * n];
+        const double theta = (aqq - app) / (2.0 * apq);
+        const double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+        const double c = 1.0 / sqrt(t * t + 1.0), sn = t * c;
+        __syncwarp();
+        for (int k = lane; k < n; k += 32) {
+          const double mkp = M[k + p * n], mkq = M[k + q * n];
+          M[k + p * n] = c * mkp - sn * mkq;
+          M[k + q * n] = sn * mkp + c * mkq;
+        }
+        __syncwarp();
+        for (int k = lane; k < n; k += 32) {
+          const double mpk = M[p + k * n], mqk = M[q + k * n];
+          M[p + k * n] = c * mpk - sn * mqk;
+          M[q + k * n] = sn * mpk + c * mqk;
+        }
+        for (int k = lane; k < n; k += 32) {
+          const double vkp = V[k + p * n], vkq = V[k + q * n];
+          V[k + p * n] = c * vkp - sn * vkq;
+          V[k + q * n] = sn * vkp + c * vkq;
+        }
+        __syncwarp();
+      }
+  }
+}
+
+struct SubGrams {
+  const double *xax, *waw, *xaw, *xx, *ww, *xw, *pap, *xap, *wap, *pp, *xp, *wp;
+};
+
+__global__ void __launch_bounds__(32) k_ppcg_sygv(int width, int sb, int numSet, SubGrams g, double* Cx, double* Cw,
+                                                  double* Cp) {
+  __shared__ double a[SYGV_MAX * SYGV_MAX], b[SYGV_MAX * SYGV_MAX], U[SYGV_MAX * SYGV_MAX], Q[SYGV_MAX * SYGV_MAX],
+      AQ[SYGV_MAX * SYGV_MAX], V[SYGV_MAX * SYGV_MAX];
+  __shared__ int kept[SYGV_MAX], ord[SYGV_MAX];
+  __shared__ int nkept;
+  const int lane = threadIdx.x;
+  const int k = blockIdx.x;
+  const int m = min(sb, width - k * sb), n = numSet * m;
+  const long o = (long)k * sb * sb;
+  // A and B from the upper blocks (symmetric fill)
+  for (int e = lane; e < n * n; e += 32) {
+    const int i = e % n, j = e / n;
+    const int ii = min(i, j), jj = max(i, j);
+    const int bi = ii / m, bj = jj / m, ri = ii % m, rj = jj % m;
+    const double *sa, *sbm;
+    if (bi == 0 && bj == 0) { sa = g.xax; sbm = g.xx; }
+    else if (bi == 1 && bj == 1) { sa = g.waw; sbm = g.ww; }
+    else if (bi == 0 && bj == 1) { sa = g.xaw; sbm = g.xw; }
+    else if (bi == 2 && bj == 2) { sa = g.pap; sbm = g.pp; }
+    else if (bi == 0 && bj == 2) { sa = g.xap; sbm = g.xp; }
+    else { sa = g.wap; sbm = g.wp; }
+    a[e] = sa[o + ri + rj * sb];
+    b[e] = sbm[o + ri + rj * sb];
+  }
+  __syncwarp();
+  warp_jacobi(n, b, U);
+  if (lane == 0) {
+    double smax = 0.0;
+    for (int i = 0; i < n; ++i) smax = fmax(smax, b[i + i * n]);
+    int r = 0;
+    for (int i = 0; i < n; ++i)
+      if (smax > 0.0 && b[i + i * n] / smax > 1e-8) kept[r++] = i;
+    nkept = r;
+  }
+  __syncwarp();
+  const int r = nkept;
+  double* cx = Cx + o;
+  double* cw = Cw + o;
+  double* cp = Cp + o;
+  for (int e = lane; e < sb * sb; e += 32) {
+    cx[e] = 0.0;
+    cw[e] = 0.0;
+    cp[e] = 0.0;
+  }
+  __syncwarp();
+  if (r < m) {
+    // fewer independent directions than columns: keep x
+    for (int i = lane; i < m; i += 32) cx[i + i * sb] = 1.0;
+    return;
+  }
+  for (int e = lane; e < n * r; e += 32) {
+    const int i = e % n, j = e / n, c = kept[j];
+    Q[i + j * n] = U[i + c * n] * (1.0 / sqrt(b[c + c * n]));
+  }
+  __syncwarp();
+  for (int e = lane; e < n * r; e += 32) {
+    const int i = e % n, j = e / n;
+    double t = 0.0;
+    for (int kk = 0; kk < n; ++kk) t += a[i + kk * n] * Q[kk + j * n];
+    AQ[i + j * n] = t;
+  }
+  __syncwarp();
+  double* M = b;   // B is no longer needed
+  for (int e = lane; e < r * r; e += 32) {
+    const int i = e % r, j = e / r;
+    double t = 0.0;
+    for (int kk = 0; kk < n; ++kk) t += Q[kk + i * n] * AQ[kk + j * n];
+    U[i + j * r] = t;
+  }
+  __syncwarp();
+  for (int e = lane; e < r * r; e += 32) {
+    const int i = e % r, j = e / r;
+    M[i + j * r] = (i == j) ? U[e] : 0.5 * (U[i + j * r] + U[j + i * r]);
+  }
+  __syncwarp();
+  warp_jacobi(r, M, V);
+  if (lane == 0) {
+    for (int i = 0; i < r; ++i) ord[i] = i;
+    for (int i = 1; i < r; ++i) {       // stable insertion sort by eigenvalue
+      const int x = ord[i];
+      int j = i - 1;
+      while (j >= 0 && M[ord[j] + ord[j] * r] > M[x + x * r]) {
+        ord[j + 1] = ord[j];
+        --j;
+      }
+      ord[j + 1] = x;
+    }
+  }
+  __syncwarp();
+  for (int e = lane; e < n * m; e += 32) {
+    const int i = e % n, jj = e / n, j = ord[jj];
+    double t = 0.0;
+    for (int kk = 0; kk < r; ++kk) t += Q[i + kk * n] * V[kk + j * r];
+    const int blk = i / m, ri = i % m;
+    double* dst = blk == 0 ? cx : blk == 1 ? cw : cp;
+    dst[ri + jj * sb] = t;
+  }
+}
+
+int ppcg_subblock_solve(int width, int sb, int numSet, const double* const* grams, double* Cx, double* Cw, double* Cp,
+                        cudaStream_t st) {
+  PWB_CHECK(sb >= 1 && sb <= 8 && numSet >= 2 && numSet <= 3, PW_EUNSUPPORTED, "PPCG sub-block 1..8");
+  const int nsb = (width + sb - 1) / sb;
+  SubGrams g{grams[0], grams[1], grams[2], grams[3], grams[4], grams[5],
+             grams[6], grams[7], grams[8], grams[9], grams[10], grams[11]};
+  k_ppcg_sygv<<<nsb, 32, 0, st>>>(width, sb, numSet, g, Cx, Cw, Cp);
+  PWB_CUDA(cudaGetLastError());
+  return PW_OK;
+}
+
 template <typename T>
 int bdiag_rotate(int n, int width, int sb, const T* X, long ldx, const double* C_dev, T* Y, long ldy, double beta,
                  cudaStream_t st) {
@@ -284,8 +547,9 @@ __global__ void k_split_c_t(const double* __restrict__ C, int ldc, int k, int m,
 // (X and Out grid-fastest): a CTA owns 128 grid rows x 64 columns, C and X
 // staged through shared memory in k-chunks of 16, 8 x 4 outputs per thread
 constexpr int RT_M = 128, RT_N = 64, RT_K = 16;
-__global__ void __launch_bounds__(256) k_rot_f64(int n, int m, int k, const double* __restrict__ X, long ldx,
-                                                 const double* __restrict__ C, int ldc, double* __restrict__ Out,
+template <typename T>
+__global__ void __launch_bounds__(256) k_rot_f64(int n, int m, int k, const T* __restrict__ X, long ldx,
+                                                 const double* __restrict__ C, int ldc, T* __restrict__ Out,
                                                  long ldo, int accumulate) {
   __shared__ double Xs[RT_K][RT_M + 1];
   __shared__ double Cs[RT_K][RT_N + 1];
@@ -300,7 +564,7 @@ __global__ void __launch_bounds__(256) k_rot_f64(int n, int m, int k, const doub
     for (int e = threadIdx.x; e < RT_K * RT_M; e += 256) {
       const int bb = e / RT_M, gg = e % RT_M;
       const int b = b0 + bb, g = g0 + gg;
-      Xs[bb][gg] = (b < k && g < n) ? X[(long)b * ldx + g] : 0.0;
+      Xs[bb][gg] = (b < k && g < n) ? (double)X[(long)b * ldx + g] : 0.0;
     }
     for (int e = threadIdx.x; e < RT_K * RT_N; e += 256) {
       const int bb = e % RT_K, jj = e / RT_K;
@@ -330,8 +594,8 @@ __global__ void __launch_bounds__(256) k_rot_f64(int n, int m, int k, const doub
     for (int a = 0; a < 8; ++a) {
       const int g = g0 + tx + 16 * a;
       if (g < n) {
-        double* o = Out + (long)j * ldo + g;
-        *o = accumulate ? *o + acc[a][b] : acc[a][b];
+        T* o = Out + (long)j * ldo + g;
+        *o = (T)(accumulate ? (double)*o + acc[a][b] : acc[a][b]);
       }
     }
   }
@@ -362,17 +626,25 @@ static int rotate_tc(pw_ctx* c, int n, int m, const RotBlock& B, float* out, lon
   return gemm_tn_store(A, Bo, k, c->gemm_terms, out, ldo, accumulate, st, 1, 0);
 }
 
-int rotate(pw_ctx* c, int n, int m, const RotBlock* blocks, int nblk, void* out, long ldo, double beta, cudaStream_t st) {
+int rotate(pw_ctx* c, int n, int m, const RotBlock* blocks, int nblk, void* out, long ldo, double beta, cudaStream_t st,
+           bool exact) {
   PWB_CHECK(beta == 0.0 || beta == 1.0, PW_EINVAL, "rotation: beta must be 0 or 1");
   for (int b = 0; b < nblk; ++b) {
     const RotBlock& B = blocks[b];
     if (B.k == 0) continue;
     const int acc = (b == 0) ? (beta != 0.0) : 1;
     int rc;
-    if (c->prec == PW_F64) {
+    if (c->prec == PW_F64 || exact) {
+      // FP64 accumulation (FP32 contexts: FP32 storage, the one-off products
+      // that need more than the split-BF16 accuracy, e.g. the ACE vectors)
       dim3 grid((n + RT_M - 1) / RT_M, (m + RT_N - 1) / RT_N);
       Launch L_(c, st, KK_ROT);
-      k_rot_f64<<<grid, 256, 0, st>>>(n, m, B.k, (const double*)B.X, B.ldx, B.C, B.ldc, (double*)out, ldo, acc);
+      if (c->prec == PW_F64)
+        k_rot_f64<double><<<grid, 256, 0, st>>>(n, m, B.k, (const double*)B.X, B.ldx, B.C, B.ldc, (double*)out, ldo,
+                                                acc);
+      else
+        k_rot_f64<float><<<grid, 256, 0, st>>>(n, m, B.k, (const float*)B.X, B.ldx, B.C, B.ldc, (float*)out, ldo,
+                                               acc);
       PWB_CUDA(cudaGetLastError());
     } else if (c->gemm_mode == 0) {
       if ((rc = rotate_tc(c, n, m, B, (float*)out, ldo, acc, st))) return rc;

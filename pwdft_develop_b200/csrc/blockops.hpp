@@ -16,6 +16,11 @@ int axpbypcz(int n, int nb, double a, const T* X, double b, const T* Y, double c
 template <typename T> int colnorm2(int n, int nb, const T* X, long ld, double* out, cudaStream_t st);
 // X[:, j] *= s[j]
 template <typename T> int colscale(int n, int nb, T* X, long ld, const double* s, cudaStream_t st);
+// B = alpha A (m x n column-major FP64, B may be A); v <- 1 / sqrt(v) (0 where v <= 1e-300); residual norms
+// out[k] = sqrt(nrm2[k]) / max(1, |G(k, k)|) with their maximum in out[n]
+int dense_scale(int m, int n, double alpha, const double* A, int lda, double* B, int ldb, cudaStream_t st);
+int vec_rsqrt(int n, double* v, cudaStream_t st);
+int resnorms(int n, const double* nrm2, const double* G, int ldg, double* out, cudaStream_t st);
 // copy with precision change
 int copy_d2f(long n, const double* x, float* y, cudaStream_t st);
 int copy_f2d(long n, const float* x, double* y, cudaStream_t st);
@@ -33,6 +38,15 @@ int cheb_lin(int n, int nb, const double* coef_dev, const T* HY, const T* Y, con
 template <typename T>
 int bdiag_dots(int n, int width, int sb, const T* U, const T* V, long ld, DevBuf& part, double* out_host,
                cudaStream_t st);
+// The same sums into a device array out_dev[k * sb * sb + i + j * sb]
+template <typename T>
+int bdiag_dots_dev(int n, int width, int sb, const T* U, const T* V, long ld, DevBuf& part, double* out_dev,
+                   cudaStream_t st);
+// PPCG sub-block eigenproblems on the device from the twelve sub-block Gram
+// arrays (xax, waw, xaw, xx, ww, xw, pap, xap, wap, pp, xp, wp; the last six
+// unused when numSet = 2) into the coefficient blocks Cx, Cw, Cp
+int ppcg_subblock_solve(int width, int sb, int numSet, const double* const* grams, double* Cx, double* Cw, double* Cp,
+                        cudaStream_t st);
 // Y (+)= X * blockdiag(C_k): Y[:, k*sb + j] = beta Y + sum_i X[:, k*sb + i] C[k*sb*sb + i + j*sb]
 template <typename T>
 int bdiag_rotate(int n, int width, int sb, const T* X, long ldx, const double* C_dev, T* Y, long ldy, double beta,
@@ -47,7 +61,10 @@ struct RotBlock {
   const double* C;   // device, FP64
   int ldc;
 };
-int rotate(pw_ctx* c, int n, int m, const RotBlock* blocks, int nblk, void* out, long ldo, double beta, cudaStream_t st);
+// exact: FP64 accumulation also in FP32 contexts (otherwise FP32 contexts use
+// the split-BF16 tensor-core GEMM)
+int rotate(pw_ctx* c, int n, int m, const RotBlock* blocks, int nblk, void* out, long ldo, double beta, cudaStream_t st,
+           bool exact = false);
 
 // Small dense FP64 algebra on the device with this library's kernels
 // (smalldense.cu), n up to a few thousand.

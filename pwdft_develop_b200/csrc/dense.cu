@@ -14,10 +14,11 @@ using namespace pwb;
 
 namespace pwb {
 
-// G (nx x ny, column-major, ldg, double, device) = alpha * X^T Y over the grid
+// G (nx x ny, column-major, ldg, double, device) = X^T Y over the first nrow
+// grid rows (nrow < 0: the whole coarse grid)
 int gram(pw_ctx* c, const void* X, int ldx, int nx, const void* Y, int ldy, int ny, double* G, int ldg,
-         cudaStream_t st) {
-  const int nt = (int)c->ntot;
+         cudaStream_t st, int nrow = -1) {
+  const int nt = nrow >= 0 ? nrow : (int)c->ntot;
   if (nx == 0 || ny == 0) return PW_OK;
   if (c->prec == PW_F64) {
     cublasHandle_t h = (cublasHandle_t)c->blas;
@@ -72,23 +73,46 @@ int pw_gram(pw_ctx* ctx, const void* X, int ldx, int nx, const void* Y, int ldy,
   return PW_OK;
 }
 
-int pw_rotate(pw_ctx* ctx, const void* X, int ldx, int k, const double* C, int ldc, int m, void* Out, int ldo,
-              int accumulate, void* stream) {
-  PWB_CHECK(ctx && k >= 0 && m >= 0 && (k * m == 0 || (X && C && Out)), PW_EINVAL, "null argument");
-  PWB_CHECK(ldx >= ctx->ntot && ldo >= ctx->ntot && ldc >= k, PW_EINVAL, "bad leading dimension");
+int pw_gram_rows(pw_ctx* ctx, int nrow, const void* X, int ldx, int nx, const void* Y, int ldy, int ny, double* G,
+                 int ldg, void* stream) {
+  PWB_CHECK(ctx && nrow >= 0 && (nx == 0 || X) && (ny == 0 || Y) && (nx * ny == 0 || G), PW_EINVAL, "null argument");
+  PWB_CHECK(ldx >= nrow && ldy >= nrow && ldg >= nx, PW_EINVAL, "bad leading dimension");
+  PWB_CHECK(ctx->prec == PW_F64 || (nrow % 8 == 0 && ldx % 8 == 0 && ldy % 8 == 0), PW_EINVAL,
+            "FP32 row blocks: row count and leading dimensions must be multiples of 8 (16-byte tensor rows)");
   PWB_CUDA(cudaSetDevice(ctx->device));
-  if (m == 0) return PW_OK;
-  if (k == 0) {
-    if (!accumulate)
-      PWB_CUDA(cudaMemset2DAsync(Out, (size_t)ldo * ctx->esz, 0, (size_t)ctx->ntot * ctx->esz, m,
-                                 (cudaStream_t)stream));
+  if (nrow == 0) {
+    for (int j = 0; j < ny; ++j) PWB_CUDA(cudaMemsetAsync(G + (size_t)j * ldg, 0, (size_t)nx * 8, (cudaStream_t)stream));
     return PW_OK;
   }
-  RotBlock rb{X, ldx, k, C, ldc};
-  int rc = rotate(ctx, (int)ctx->ntot, m, &rb, 1, Out, ldo, accumulate ? 1.0 : 0.0, (cudaStream_t)stream);
+  int rc = gram(ctx, X, ldx, nx, Y, ldy, ny, G, ldg, (cudaStream_t)stream, nrow);
   if (rc) return rc;
   if (ctx->check_errors) return gemm_error_check();
   return PW_OK;
+}
+
+int pw_rotate_rows(pw_ctx* ctx, int nrow, const void* X, int ldx, int k, const double* C, int ldc, int m, void* Out,
+                   int ldo, int accumulate, void* stream) {
+  PWB_CHECK(ctx && nrow >= 0 && k >= 0 && m >= 0 && (k * m == 0 || (X && C && Out)), PW_EINVAL, "null argument");
+  PWB_CHECK(ldx >= nrow && ldo >= nrow && ldc >= k, PW_EINVAL, "bad leading dimension");
+  PWB_CUDA(cudaSetDevice(ctx->device));
+  if (m == 0 || nrow == 0) return PW_OK;
+  if (k == 0) {
+    if (!accumulate)
+      PWB_CUDA(cudaMemset2DAsync(Out, (size_t)ldo * ctx->esz, 0, (size_t)nrow * ctx->esz, m, (cudaStream_t)stream));
+    return PW_OK;
+  }
+  RotBlock rb{X, ldx, k, C, ldc};
+  int rc = rotate(ctx, nrow, m, &rb, 1, Out, ldo, accumulate ? 1.0 : 0.0, (cudaStream_t)stream);
+  if (rc) return rc;
+  if (ctx->check_errors) return gemm_error_check();
+  return PW_OK;
+}
+
+int pw_rotate(pw_ctx* ctx, const void* X, int ldx, int k, const double* C, int ldc, int m, void* Out, int ldo,
+              int accumulate, void* stream) {
+  PWB_CHECK(ctx, PW_EINVAL, "null argument");
+  PWB_CHECK(ldx >= ctx->ntot && ldo >= ctx->ntot, PW_EINVAL, "bad leading dimension");
+  return pw_rotate_rows(ctx, (int)ctx->ntot, X, ldx, k, C, ldc, m, Out, ldo, accumulate, stream);
 }
 
 }  // extern "C"

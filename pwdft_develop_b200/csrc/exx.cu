@@ -26,7 +26,7 @@ namespace pwb {
 int run_exx(pw_ctx* c, const void* psi, int ld, int nb, void* out, int ldo, int acc, cudaStream_t st);
 int run_ace(pw_ctx* c, const void* psi, int ld, int nb, void* out, int ldo, cudaStream_t st);
 int gram(pw_ctx* c, const void* X, int ldx, int nx, const void* Y, int ldy, int ny, double* G, int ldg,
-         cudaStream_t st);
+         cudaStream_t st, int nrow = -1);
 int upload_real(pw_ctx* c, DevBuf& dst, const double* src, size_t n);
 
 template <typename T>
@@ -247,7 +247,7 @@ int pw_ace_build(pw_ctx* ctx, const void* psi, int ld, int nband) {
   dn.release();
   if ((rc = ctx->ace_xi.alloc((size_t)nband * nt * esz))) return rc;
   RotBlock rb{W.p, nt, nband, (const double*)Ui.p, nband};
-  if ((rc = rotate(ctx, (int)nt, nband, &rb, 1, ctx->ace_xi.p, nt, 0.0, nullptr))) return rc;
+  if ((rc = rotate(ctx, (int)nt, nband, &rb, 1, ctx->ace_xi.p, nt, 0.0, nullptr, true))) return rc;
   std::vector<double> m1(nband, -1.0);
   if ((rc = upload_real(ctx, ctx->ace_qd, m1.data(), nband))) return rc;
   const int npad = (nband + 7) / 8 * 8;

@@ -34,7 +34,7 @@ namespace pwb {
 int run_density(pw_ctx* c, const void* psi, int ld, int nband, int band0, int npair, const double* w, double* rho,
                 cudaStream_t st);
 int gram(pw_ctx* c, const void* X, int ldx, int nx, const void* Y, int ldy, int ny, double* G, int ldg,
-         cudaStream_t st);
+         cudaStream_t st, int nrow = -1);
 int upload_real(pw_ctx* c, DevBuf& dst, const double* src, size_t n);
 int wfn_filter_pass(pw_ctx* c, void* X, int ld, int nb, cudaStream_t st);
 
@@ -727,45 +727,39 @@ static int lobpcg(Solver& s, Dense& d, int width, int maxit, double tol, bool fi
   if (first_scf && (rc = cholqr(s, d, X, width, s.Y.p))) return rc;
   if ((rc = hpsi(s.c, X, AX, width, nullptr))) return rc;
   if ((rc = s.G1.alloc((size_t)lda * lda * 8)) || (rc = s.G2.alloc((size_t)lda * lda * 8))) return rc;
-  DevBuf xtx, dvec;
-  if ((rc = xtx.alloc((size_t)width * width * 8)) || (rc = dvec.alloc((size_t)3 * width * 8))) return rc;
-  std::vector<double> eigS(lda), hXTX((size_t)width * width);
+  DevBuf xtx, dvec, rvec;
+  if ((rc = xtx.alloc((size_t)width * width * 8)) || (rc = dvec.alloc((size_t)3 * width * 8)) ||
+      (rc = rvec.alloc((size_t)(width + 1) * 8)))
+    return rc;
+  std::vector<double> eigS(lda);
   double resMax = 0;
   int iter = 0;
   std::vector<double> resNorm(width);
   do {
     ++iter;
     const int numSet = (iter == 1) ? 2 : 3;
-    // XTX = X^T AX;  R = AX - X XTX
+    // XTX = X^T AX;  R = AX - X XTX  (all on the device; only the largest
+    // residual norm, the convergence test, comes back to the host)
     double* XTX = (double*)xtx.p;
     if ((rc = gram(s.c, X, (int)nt, width, AX, (int)nt, width, XTX, width, nullptr))) return rc;
-    PWB_CUDA(cudaMemcpy(hXTX.data(), XTX, hXTX.size() * 8, cudaMemcpyDeviceToHost));
-    PWB_CUDA(cudaMemcpy(s.Y.p, AX, (size_t)width * nt * esz, cudaMemcpyDeviceToDevice));
-    std::vector<double> mX((size_t)width * width);
-    for (size_t i = 0; i < mX.size(); ++i) mX[i] = -hXTX[i];
-    PWB_CUDA(cudaMemcpy(s.G2.p, mX.data(), mX.size() * 8, cudaMemcpyHostToDevice));
+    PWB_CUDA(cudaMemcpyAsync(s.Y.p, AX, (size_t)width * nt * esz, cudaMemcpyDeviceToDevice, nullptr));
+    if ((rc = dense_scale(width, width, -1.0, XTX, width, (double*)s.G2.p, width, nullptr))) return rc;
     RotBlock rb{X, nt, width, (double*)s.G2.p, width};
-    if ((rc = rotate(s.c, (int)nt, width, &rb, 1, s.Y.p, nt, 1.0, nullptr))) return rc;
+    if ((rc = rotate(s.c, (int)nt, width, &rb, 1, s.Y.p, nt, 1.0, nullptr, true))) return rc;
     double* nrm = (double*)dvec.p;
+    double* rn = (double*)rvec.p;
     if ((rc = v_colnorm2(s, width, s.Y.p, nrm))) return rc;
-    std::vector<double> hn(width);
-    PWB_CUDA(cudaMemcpy(hn.data(), nrm, width * 8, cudaMemcpyDeviceToHost));
-    for (int k = 0; k < width; ++k)
-      resNorm[k] = std::sqrt(hn[k]) / std::max(1.0, std::fabs(hXTX[(size_t)k * width + k]));
-    resMax = *std::max_element(resNorm.begin(), resNorm.end());
+    if ((rc = resnorms(width, nrm, XTX, width, rn, nullptr))) return rc;
+    PWB_CUDA(cudaMemcpy(&resMax, rn + width, 8, cudaMemcpyDeviceToHost));
     // W = Teter * R, normalised
     if ((rc = pw_teter_precond(s.c, s.Y.p, (int)nt, W, (int)nt, width, 0, nullptr))) return rc;
-    if ((rc = v_colnorm2(s, width, W, nrm))) return rc;
-    PWB_CUDA(cudaMemcpy(hn.data(), nrm, width * 8, cudaMemcpyDeviceToHost));
-    for (int k = 0; k < width; ++k) hn[k] = 1.0 / std::sqrt(hn[k]);
-    PWB_CUDA(cudaMemcpy(nrm, hn.data(), width * 8, cudaMemcpyHostToDevice));
-    if ((rc = v_colscale(s, width, W, nrm))) return rc;
+    if ((rc = v_colnorm2(s, width, W, nrm)) || (rc = vec_rsqrt(width, nrm, nullptr)) ||
+        (rc = v_colscale(s, width, W, nrm)))
+      return rc;
     if (numSet == 3) {
-      if ((rc = v_colnorm2(s, width, P, nrm))) return rc;
-      PWB_CUDA(cudaMemcpy(hn.data(), nrm, width * 8, cudaMemcpyDeviceToHost));
-      for (int k = 0; k < width; ++k) hn[k] = 1.0 / std::sqrt(hn[k]);
-      PWB_CUDA(cudaMemcpy(nrm, hn.data(), width * 8, cudaMemcpyHostToDevice));
-      if ((rc = v_colscale(s, width, P, nrm)) || (rc = v_colscale(s, width, AP, nrm))) return rc;
+      if ((rc = v_colnorm2(s, width, P, nrm)) || (rc = vec_rsqrt(width, nrm, nullptr)) ||
+          (rc = v_colscale(s, width, P, nrm)) || (rc = v_colscale(s, width, AP, nrm)))
+        return rc;
     }
     if ((rc = hpsi(s.c, W, AW, width, nullptr))) return rc;
     // AMat = S^T AS, BMat = S^T S over the active sets (upper blocks used)
@@ -796,6 +790,7 @@ static int lobpcg(Solver& s, Dense& d, int width, int maxit, double tol, bool fi
     if ((rc = v_axpby(s, width, 1.0, s.Y.p, 1.0, AX))) return rc;
     PWB_CUDA(cudaMemcpy(AP, s.Y.p, (size_t)width * nt * esz, cudaMemcpyDeviceToDevice));
   } while (iter < maxit && resMax > tol);
+  PWB_CUDA(cudaMemcpy(resNorm.data(), rvec.p, width * 8, cudaMemcpyDeviceToHost));
   // final Rayleigh-Ritz with X^T AX (lobpcg.cpp:991-1003)
   if ((rc = rayleigh_ritz(s, d, X, AX, s.X.p, s.HX.p, width))) return rc;
   s.res = resNorm;
@@ -803,113 +798,10 @@ static int lobpcg(Solver& s, Dense& d, int width, int maxit, double tol, bool fi
   return PW_OK;
 }
 
-// ---------------------------------------------------------------------------
-// small dense generalized symmetric eigenproblem on the host (PPCG sub-blocks)
-// ---------------------------------------------------------------------------
-// cyclic Jacobi: M (n x n, column major, symmetric) -> V diag(M) V^T, in place
-static void jacobi_eig(int n, std::vector<double>& M, std::vector<double>& V) {
-  V.assign((size_t)n * n, 0.0);
-  for (int i = 0; i < n; ++i) V[i + (size_t)i * n] = 1.0;
-  for (int sweep = 0; sweep < 100; ++sweep) {
-    double off = 0.0, tot = 0.0;
-    for (int j = 0; j < n; ++j)
-      for (int i = 0; i < n; ++i) {
-        const double x = M[i + (size_t)j * n];
-        tot += x * x;
-        if (i != j) off += x * x;
-      }
-    if (off == 0.0 || off <= 1e-30 * tot) break;
-    for (int p = 0; p < n - 1; ++p)
-      for (int q = p + 1; q < n; ++q) {
-        const double apq = M[p + (size_t)q * n];
-        if (apq == 0.0) continue;
-        const double app = M[p + (size_t)p * n], aqq = M[q + (size_t)q * n];
-        const double theta = (aqq - app) / (2.0 * apq);
-        const double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
-        const double c = 1.0 / std::sqrt(t * t + 1.0), sn = t * c;
-        for (int k = 0; k < n; ++k) {
-          const double mkp = M[k + (size_t)p * n], mkq = M[k + (size_t)q * n];
-          M[k + (size_t)p * n] = c * mkp - sn * mkq;
-          M[k + (size_t)q * n] = sn * mkp + c * mkq;
-        }
-        for (int k = 0; k < n; ++k) {
-          const double mpk = M[p + (size_t)k * n], mqk = M[q + (size_t)k * n];
-          M[p + (size_t)k * n] = c * mpk - sn * mqk;
-          M[q + (size_t)k * n] = sn * mpk + c * mqk;
-        }
-        for (int k = 0; k < n; ++k) {
-          const double vkp = V[k + (size_t)p * n], vkq = V[k + (size_t)q * n];
-          V[k + (size_t)p * n] = c * vkp - sn * vkq;
-          V[k + (size_t)q * n] = sn * vkp + c * vkq;
-        }
-      }
-  }
-}
-
-// A z = lambda B z for n <= 24 from the upper triangles of A and B (column
-// major, leading dimension ld).  The reference calls LAPACK dsygvd here; to
-// stay defined when the sub-block's search directions become numerically
-// dependent (a converged column's residual), B is diagonalised first and only
-// directions with sigma / sigma_max > 1e-8 are kept -- the SolveGenEig
-// treatment (eigensolver.cpp:224-297) -- which equals dsygvd for a
-// well-conditioned B.  Returns the number r of kept directions; Z (n x r) holds
-// B-orthonormal eigenvectors for the r ascending eigenvalues w.
-static int small_sygv(int n, const double* A, const double* B, int ld, double* w, double* Z) {
-  std::vector<double> a((size_t)n * n), b((size_t)n * n), U;
-  for (int j = 0; j < n; ++j)
-    for (int i = 0; i <= j; ++i) {
-      a[i + (size_t)j * n] = a[j + (size_t)i * n] = A[i + (size_t)j * ld];
-      b[i + (size_t)j * n] = b[j + (size_t)i * n] = B[i + (size_t)j * ld];
-    }
-  jacobi_eig(n, b, U);
-  double smax = 0.0;
-  for (int i = 0; i < n; ++i) smax = std::max(smax, b[i + (size_t)i * n]);
-  std::vector<int> kept;
-  for (int i = 0; i < n; ++i)
-    if (smax > 0.0 && b[i + (size_t)i * n] / smax > 1e-8) kept.push_back(i);
-  const int r = (int)kept.size();
-  if (r == 0) return 0;
-  // Q = U_k sigma_k^-1/2 (n x r); M = Q^T A Q
-  std::vector<double> Q((size_t)n * r), AQ((size_t)n * r), M((size_t)r * r), V;
-  for (int j = 0; j < r; ++j) {
-    const int c = kept[j];
-    const double f = 1.0 / std::sqrt(b[c + (size_t)c * n]);
-    for (int i = 0; i < n; ++i) Q[i + (size_t)j * n] = U[i + (size_t)c * n] * f;
-  }
-  for (int j = 0; j < r; ++j)
-    for (int i = 0; i < n; ++i) {
-      double t = 0.0;
-      for (int k = 0; k < n; ++k) t += a[i + (size_t)k * n] * Q[k + (size_t)j * n];
-      AQ[i + (size_t)j * n] = t;
-    }
-  for (int j = 0; j < r; ++j)
-    for (int i = 0; i < r; ++i) {
-      double t = 0.0;
-      for (int k = 0; k < n; ++k) t += Q[k + (size_t)i * n] * AQ[k + (size_t)j * n];
-      M[i + (size_t)j * r] = t;
-    }
-  for (int j = 0; j < r; ++j)
-    for (int i = 0; i < j; ++i) M[i + (size_t)j * r] = M[j + (size_t)i * r] = 0.5 * (M[i + (size_t)j * r] + M[j + (size_t)i * r]);
-  jacobi_eig(r, M, V);
-  std::vector<int> ord(r);
-  for (int i = 0; i < r; ++i) ord[i] = i;
-  std::sort(ord.begin(), ord.end(), [&](int x, int y) { return M[x + (size_t)x * r] < M[y + (size_t)y * r]; });
-  for (int jj = 0; jj < r; ++jj) {
-    const int j = ord[jj];
-    w[jj] = M[j + (size_t)j * r];
-    for (int i = 0; i < n; ++i) {
-      double t = 0.0;
-      for (int k = 0; k < r; ++k) t += Q[i + (size_t)k * n] * V[k + (size_t)j * r];
-      Z[i + (size_t)jj * n] = t;
-    }
-  }
-  return r;
-}
-
-static int v_bdiag_dots(Solver& s, int width, int sb, const void* U, const void* V, DevBuf& part, double* out) {
+static int v_bdiag_dots_dev(Solver& s, int width, int sb, const void* U, const void* V, DevBuf& part, double* out) {
   return s.c->prec == PW_F64
-             ? bdiag_dots<double>((int)s.nt, width, sb, (const double*)U, (const double*)V, s.nt, part, out, nullptr)
-             : bdiag_dots<float>((int)s.nt, width, sb, (const float*)U, (const float*)V, s.nt, part, out, nullptr);
+             ? bdiag_dots_dev<double>((int)s.nt, width, sb, (const double*)U, (const double*)V, s.nt, part, out, nullptr)
+             : bdiag_dots_dev<float>((int)s.nt, width, sb, (const float*)U, (const float*)V, s.nt, part, out, nullptr);
 }
 static int v_bdiag_rotate(Solver& s, int width, int sb, const void* X, const double* C, void* Y, double beta) {
   return s.c->prec == PW_F64
@@ -923,14 +815,11 @@ static int project_out(Solver& s, int width, void* X, void* AX, void* V, void* A
   if ((rc = G.alloc((size_t)width * width * 8))) return rc;
   double* g = (double*)G.p;
   if ((rc = gram(s.c, X, (int)s.nt, width, V, (int)s.nt, width, g, width, nullptr))) return rc;
-  std::vector<double> h((size_t)width * width);
-  PWB_CUDA(cudaMemcpy(h.data(), g, h.size() * 8, cudaMemcpyDeviceToHost));
-  for (double& x : h) x = -x;
-  PWB_CUDA(cudaMemcpy(g, h.data(), h.size() * 8, cudaMemcpyHostToDevice));
+  if ((rc = dense_scale(width, width, -1.0, g, width, g, width, nullptr))) return rc;
   RotBlock rb{X, s.nt, width, g, width};
-  if ((rc = rotate(s.c, (int)s.nt, width, &rb, 1, V, s.nt, 1.0, nullptr))) return rc;
+  if ((rc = rotate(s.c, (int)s.nt, width, &rb, 1, V, s.nt, 1.0, nullptr, true))) return rc;
   RotBlock ra{AX, s.nt, width, g, width};
-  return rotate(s.c, (int)s.nt, width, &ra, 1, AV, s.nt, 1.0, nullptr);
+  return rotate(s.c, (int)s.nt, width, &ra, 1, AV, s.nt, 1.0, nullptr, true);
 }
 
 // V, AV /= ||V|| column-wise
@@ -938,12 +827,9 @@ static int normalize_pair(Solver& s, int width, void* V, void* AV, DevBuf& tmp) 
   int rc;
   if ((rc = tmp.alloc((size_t)width * 8))) return rc;
   double* d = (double*)tmp.p;
-  if ((rc = v_colnorm2(s, width, V, d))) return rc;
-  std::vector<double> h(width);
-  PWB_CUDA(cudaMemcpy(h.data(), d, width * 8, cudaMemcpyDeviceToHost));
-  // a vanishing direction (exactly converged column) stays zero instead of 0/0
-  for (double& x : h) x = x > 1e-300 ? 1.0 / std::sqrt(x) : 0.0;
-  PWB_CUDA(cudaMemcpy(d, h.data(), width * 8, cudaMemcpyHostToDevice));
+  // 1 / ||v|| on the device; a vanishing direction (an exactly converged
+  // column) stays zero instead of 0/0
+  if ((rc = v_colnorm2(s, width, V, d)) || (rc = vec_rsqrt(width, d, nullptr))) return rc;
   if ((rc = v_colscale(s, width, V, d))) return rc;
   return AV ? v_colscale(s, width, AV, d) : PW_OK;
 }
@@ -989,39 +875,37 @@ static int ppcg(Solver& s, Dense& d, int width, int sb, int maxit, double tol, b
   PWB_CUDA(cudaMemcpy(X, s.X.p, (size_t)width * nt * esz, cudaMemcpyDeviceToDevice));
   if (first_scf && (rc = cholqr(s, d, X, width, s.Y.p))) return rc;
   if ((rc = hpsi(s.c, X, AX, width, nullptr))) return rc;
-  DevBuf G, tmpv, part, Cd;
+  DevBuf G, G2, tmpv, part, Cd, Gs, rvec;
   if ((rc = Cd.alloc((size_t)3 * nsb * sb * sb * 8))) return rc;
   double* Cx = (double*)Cd.p;
   double* Cw = Cx + (size_t)nsb * sb * sb;
   double* Cp = Cw + (size_t)nsb * sb * sb;
   const size_t bs = (size_t)nsb * sb * sb;
-  std::vector<double> xax(bs), waw(bs), xaw(bs), xx(bs), ww(bs), xw(bs), pap(bs), xap(bs), wap(bs), pp(bs), xp(bs),
-      wp(bs), hc(3 * bs);
+  // the twelve sub-block Gram arrays, device-resident
+  if ((rc = Gs.alloc(12 * bs * 8)) || (rc = rvec.alloc((size_t)(width + 1) * 8))) return rc;
+  double* gp[12];
+  for (int i = 0; i < 12; ++i) gp[i] = (double*)Gs.p + i * bs;
+  double *xax = gp[0], *waw = gp[1], *xaw = gp[2], *xx = gp[3], *ww = gp[4], *xw = gp[5], *pap = gp[6],
+         *xap = gp[7], *wap = gp[8], *pp = gp[9], *xp = gp[10], *wp = gp[11];
   std::vector<double> resNorm(width);
   double resMax = 0;
   int iter = 0;
   do {
     ++iter;
     const int numSet = (iter == 1) ? 2 : 3;
-    // R = AX - X (X^T AX) into Y
-    if ((rc = G.alloc((size_t)width * width * 8))) return rc;
+    // R = AX - X (X^T AX) into Y, on the device; only the largest residual
+    // norm (the convergence test) comes back to the host
+    if ((rc = G.alloc((size_t)width * width * 8)) || (rc = G2.alloc((size_t)width * width * 8))) return rc;
     double* g = (double*)G.p;
     if ((rc = gram(s.c, X, (int)nt, width, AX, (int)nt, width, g, width, nullptr))) return rc;
-    std::vector<double> hg((size_t)width * width);
-    PWB_CUDA(cudaMemcpy(hg.data(), g, hg.size() * 8, cudaMemcpyDeviceToHost));
-    std::vector<double> mg(hg.size());
-    for (size_t i = 0; i < hg.size(); ++i) mg[i] = -hg[i];
-    PWB_CUDA(cudaMemcpy(g, mg.data(), mg.size() * 8, cudaMemcpyHostToDevice));
-    PWB_CUDA(cudaMemcpy(s.Y.p, AX, (size_t)width * nt * esz, cudaMemcpyDeviceToDevice));
-    RotBlock rb{X, nt, width, g, width};
-    if ((rc = rotate(s.c, (int)nt, width, &rb, 1, s.Y.p, nt, 1.0, nullptr))) return rc;
+    if ((rc = dense_scale(width, width, -1.0, g, width, (double*)G2.p, width, nullptr))) return rc;
+    PWB_CUDA(cudaMemcpyAsync(s.Y.p, AX, (size_t)width * nt * esz, cudaMemcpyDeviceToDevice, nullptr));
+    RotBlock rb{X, nt, width, (double*)G2.p, width};
+    if ((rc = rotate(s.c, (int)nt, width, &rb, 1, s.Y.p, nt, 1.0, nullptr, true))) return rc;
     if ((rc = tmpv.alloc((size_t)width * 8))) return rc;
     if ((rc = v_colnorm2(s, width, s.Y.p, (double*)tmpv.p))) return rc;
-    std::vector<double> hn(width);
-    PWB_CUDA(cudaMemcpy(hn.data(), tmpv.p, width * 8, cudaMemcpyDeviceToHost));
-    for (int k = 0; k < width; ++k)
-      resNorm[k] = std::sqrt(hn[k]) / std::max(1.0, std::fabs(hg[(size_t)k * width + k]));
-    resMax = *std::max_element(resNorm.begin(), resNorm.end());
+    if ((rc = resnorms(width, (const double*)tmpv.p, g, width, (double*)rvec.p, nullptr))) return rc;
+    PWB_CUDA(cudaMemcpy(&resMax, (double*)rvec.p + width, 8, cudaMemcpyDeviceToHost));
     // W = T R, AW = H W, orthogonal to X, normalised
     if ((rc = pw_teter_precond(s.c, s.Y.p, (int)nt, W, (int)nt, width, 0, nullptr))) return rc;
     if ((rc = hpsi(s.c, W, AW, width, nullptr))) return rc;
@@ -1031,57 +915,30 @@ static int ppcg(Solver& s, Dense& d, int width, int sb, int maxit, double tol, b
       if ((rc = project_out(s, width, X, AX, P, AP, G))) return rc;
       if ((rc = normalize_pair(s, width, P, AP, tmpv))) return rc;
     }
-    // sub-block Gram blocks
+    // sub-block Gram blocks (device)
     {
       SubTimer t_(1);
-      if ((rc = v_bdiag_dots(s, width, sb, X, AX, part, xax.data())) ||
-          (rc = v_bdiag_dots(s, width, sb, W, AW, part, waw.data())) ||
-          (rc = v_bdiag_dots(s, width, sb, X, AW, part, xaw.data())) ||
-          (rc = v_bdiag_dots(s, width, sb, X, X, part, xx.data())) ||
-          (rc = v_bdiag_dots(s, width, sb, W, W, part, ww.data())) ||
-          (rc = v_bdiag_dots(s, width, sb, X, W, part, xw.data())))
+      if ((rc = v_bdiag_dots_dev(s, width, sb, X, AX, part, xax)) ||
+          (rc = v_bdiag_dots_dev(s, width, sb, W, AW, part, waw)) ||
+          (rc = v_bdiag_dots_dev(s, width, sb, X, AW, part, xaw)) ||
+          (rc = v_bdiag_dots_dev(s, width, sb, X, X, part, xx)) ||
+          (rc = v_bdiag_dots_dev(s, width, sb, W, W, part, ww)) ||
+          (rc = v_bdiag_dots_dev(s, width, sb, X, W, part, xw)))
         return rc;
       if (numSet == 3 &&
-          ((rc = v_bdiag_dots(s, width, sb, P, AP, part, pap.data())) ||
-           (rc = v_bdiag_dots(s, width, sb, X, AP, part, xap.data())) ||
-           (rc = v_bdiag_dots(s, width, sb, W, AP, part, wap.data())) ||
-           (rc = v_bdiag_dots(s, width, sb, P, P, part, pp.data())) ||
-           (rc = v_bdiag_dots(s, width, sb, X, P, part, xp.data())) ||
-           (rc = v_bdiag_dots(s, width, sb, W, P, part, wp.data()))))
+          ((rc = v_bdiag_dots_dev(s, width, sb, P, AP, part, pap)) ||
+           (rc = v_bdiag_dots_dev(s, width, sb, X, AP, part, xap)) ||
+           (rc = v_bdiag_dots_dev(s, width, sb, W, AP, part, wap)) ||
+           (rc = v_bdiag_dots_dev(s, width, sb, P, P, part, pp)) ||
+           (rc = v_bdiag_dots_dev(s, width, sb, X, P, part, xp)) ||
+           (rc = v_bdiag_dots_dev(s, width, sb, W, P, part, wp))))
         return rc;
     }
-    // nsb small generalized eigenproblems (Sygvd)
-    std::fill(hc.begin(), hc.end(), 0.0);
-    for (int k = 0; k < nsb; ++k) {
-      const int m = std::min(sb, width - k * sb);
-      const int dim = numSet * m, ld = 3 * sb;
-      std::vector<double> A((size_t)ld * ld, 0.0), B((size_t)ld * ld, 0.0), Z((size_t)dim * dim), ev(dim);
-      auto put = [&](std::vector<double>& M, int r0, int c0, const std::vector<double>& src) {
-        for (int j = 0; j < m; ++j)
-          for (int i = 0; i < m; ++i) M[(r0 + i) + (size_t)(c0 + j) * ld] = src[(size_t)k * sb * sb + i + j * sb];
-      };
-      put(A, 0, 0, xax); put(A, m, m, waw); put(A, 0, m, xaw);
-      put(B, 0, 0, xx); put(B, m, m, ww); put(B, 0, m, xw);
-      if (numSet == 3) {
-        put(A, 2 * m, 2 * m, pap); put(A, 0, 2 * m, xap); put(A, m, 2 * m, wap);
-        put(B, 2 * m, 2 * m, pp); put(B, 0, 2 * m, xp); put(B, m, 2 * m, wp);
-      }
-      double* cx = &hc[(size_t)k * sb * sb];
-      double* cw = cx + bs;
-      double* cp = cw + bs;
-      if (small_sygv(dim, A.data(), B.data(), ld, ev.data(), Z.data()) >= m) {
-        for (int j = 0; j < m; ++j)
-          for (int i = 0; i < m; ++i) {
-            cx[i + j * sb] = Z[i + (size_t)j * dim];
-            cw[i + j * sb] = Z[(m + i) + (size_t)j * dim];
-            if (numSet == 3) cp[i + j * sb] = Z[(2 * m + i) + (size_t)j * dim];
-          }
-      } else {
-        // fewer independent directions than columns: keep x
-        for (int i = 0; i < m; ++i) cx[i + i * sb] = 1.0;
-      }
+    // nsb small generalized eigenproblems (Sygvd), one warp each on the device
+    {
+      const double* grams[12] = {xax, waw, xaw, xx, ww, xw, pap, xap, wap, pp, xp, wp};
+      if ((rc = ppcg_subblock_solve(width, sb, numSet, grams, Cx, Cw, Cp, nullptr))) return rc;
     }
-    PWB_CUDA(cudaMemcpy(Cx, hc.data(), hc.size() * 8, cudaMemcpyHostToDevice));
     {
       SubTimer t_(3);
       // p = w cw (+ p cp); ap = aw cw (+ ap cp)
@@ -1109,6 +966,7 @@ static int ppcg(Solver& s, Dense& d, int width, int sb, int maxit, double tol, b
     // Cholesky-QR of X, AX transformed alongside
     if ((rc = cholqr_pair(s, d, X, AX, width, s.Y.p))) return rc;
   } while (iter < maxit && resMax > tol);
+  PWB_CUDA(cudaMemcpy(resNorm.data(), rvec.p, width * 8, cudaMemcpyDeviceToHost));
   // final Rayleigh-Ritz (ppcg.cpp:1112-1166)
   if ((rc = rayleigh_ritz(s, d, X, AX, s.X.p, s.HX.p, width))) return rc;
   if (iters) *iters = iter;

@@ -214,10 +214,12 @@ int dense_gemm(int ta, int tb, int m, int n, int k, const double* A, int lda, co
 __device__ __forceinline__ int rr_index(int pos, int r, int m) { return pos == 0 ? 0 : ((pos - 1 + r) % (m - 1)) + 1; }
 
 // One CTA brings the m x m working matrix W (ldw = m; for odd n the last row
-// and column are a zero dummy that never rotates) to diagonal form and
-// accumulates the rotations into V (m x m, starts as the identity).  A pair
-// (p, q) rotates when |W_pq| > tol * scale.  Returns the sweeps run.
-__device__ int jacobi_cta(int m, double* W, double* V, int* sp, int* sq, double* sc, double* ss, int max_sweeps,
+// and column are a zero dummy that never rotates) to diagonal form.  A pair
+// (p, q) rotates when |W_pq| > tol * scale.  The rotations are not applied to
+// the eigenvector matrix here: each round's (c, s) pairs go to `log`
+// (round-major, np per round), and k_jacobi_vectors replays them on the rows
+// of V afterwards, all rows in parallel.  Returns the sweeps run.
+__device__ int jacobi_cta(int m, double* W, double2* log, int* sp, int* sq, double* sc, double* ss, int max_sweeps,
                           double tol, double scale) {
   const int np = m / 2;
   __shared__ int rotated;
@@ -243,64 +245,52 @@ __device__ int jacobi_cta(int m, double* W, double* V, int* sp, int* sq, double*
         sq[k] = b;
         sc[k] = c;
         ss[k] = s;
+        log[((long)sweep * (m - 1) + r) * np + k] = make_double2(c, s);
       }
       __syncthreads();
-      // 2 x 2 blocks (bi <= bj) of W' = J^T W J, then the column pairs of V' = V J
-      const long nblk = (long)np * np, nvr = (long)m * np;
-      for (long e = threadIdx.x; e < nblk + nvr; e += blockDim.x) {
-        if (e < nblk) {
-          const int bi = (int)(e % np), bj = (int)(e / np);
-          if (bj < bi) continue;
-          const int p = sp[bi], q = sq[bi], r2 = sp[bj], s2 = sq[bj];
-          const double ci = sc[bi], si = ss[bi], cj = sc[bj], sj = ss[bj];
-          if (bi == bj) {
-            if (si != 0.0) {
-              const double apq = W[(long)q * m + p];
-              const double t = si / ci;
-              W[(long)p * m + p] -= t * apq;
-              W[(long)q * m + q] += t * apq;
-              W[(long)q * m + p] = 0.0;
-              W[(long)p * m + q] = 0.0;
-            }
-            continue;
-          }
-          if (si == 0.0 && sj == 0.0) continue;
-          const double apr = W[(long)r2 * m + p], aps = W[(long)s2 * m + p];
-          const double aqr = W[(long)r2 * m + q], aqs = W[(long)s2 * m + q];
-          // (M J_j), then J_i^T (M J_j); J = [[c, s], [-s, c]] on (p, q)
-          const double t1 = cj * apr - sj * aps, t2 = sj * apr + cj * aps;
-          const double t3 = cj * aqr - sj * aqs, t4 = sj * aqr + cj * aqs;
-          const double npr = ci * t1 - si * t3, nps = ci * t2 - si * t4;
-          const double nqr = si * t1 + ci * t3, nqs = si * t2 + ci * t4;
-          W[(long)r2 * m + p] = npr;
-          W[(long)s2 * m + p] = nps;
-          W[(long)r2 * m + q] = nqr;
-          W[(long)s2 * m + q] = nqs;
-          W[(long)p * m + r2] = npr;
-          W[(long)p * m + s2] = nps;
-          W[(long)q * m + r2] = nqr;
-          W[(long)q * m + s2] = nqs;
-        } else {
-          const long f = e - nblk;
-          const int row = (int)(f % m), k = (int)(f / m);
-          const double s = ss[k];
-          if (s == 0.0) continue;
-          const int p = sp[k], q = sq[k];
-          const double c = sc[k];
-          const double vp = V[(long)p * m + row], vq = V[(long)q * m + row];
-          V[(long)p * m + row] = c * vp - s * vq;
-          V[(long)q * m + row] = s * vp + c * vq;
+      // 2 x 2 blocks (bi <= bj) of W' = J^T W J
+      for (int e = threadIdx.x; e < np * np; e += blockDim.x) {
+        const int bi = e % np, bj = e / np;
+        if (bj < bi) continue;
+        const double si = ss[bi], sj = ss[bj];
+        if (si == 0.0 && sj == 0.0) continue;
+        const int p = sp[bi], q = sq[bi], r2 = sp[bj], s2 = sq[bj];
+        const double ci = sc[bi], cj = sc[bj];
+        if (bi == bj) {
+          const double apq = W[(long)q * m + p];
+          const double t = si / ci;
+          W[(long)p * m + p] -= t * apq;
+          W[(long)q * m + q] += t * apq;
+          W[(long)q * m + p] = 0.0;
+          W[(long)p * m + q] = 0.0;
+          continue;
         }
+        const double apr = W[(long)r2 * m + p], aps = W[(long)s2 * m + p];
+        const double aqr = W[(long)r2 * m + q], aqs = W[(long)s2 * m + q];
+        // (M J_j), then J_i^T (M J_j); J = [[c, s], [-s, c]] on (p, q)
+        const double t1 = cj * apr - sj * aps, t2 = sj * apr + cj * aps;
+        const double t3 = cj * aqr - sj * aqs, t4 = sj * aqr + cj * aqs;
+        const double npr = ci * t1 - si * t3, nps = ci * t2 - si * t4;
+        const double nqr = si * t1 + ci * t3, nqs = si * t2 + ci * t4;
+        W[(long)r2 * m + p] = npr;
+        W[(long)s2 * m + p] = nps;
+        W[(long)r2 * m + q] = nqr;
+        W[(long)s2 * m + q] = nqs;
+        W[(long)p * m + r2] = npr;
+        W[(long)p * m + s2] = nps;
+        W[(long)q * m + r2] = nqr;
+        W[(long)q * m + s2] = nqs;
       }
       __syncthreads();
     }
     if (!rotated) break;
   }
-  return sweep + 1;
+  return min(sweep + 1, max_sweeps);
 }
 
 constexpr int JAC_THREADS = 1024;
 constexpr int JAC_SMEM_MAX = 160;   // working matrix in shared memory up to m = 160 (FP64)
+constexpr int JAC_MAX_SWEEPS = 40;
 
 size_t syevj_smem(int n) {
   const int m = n + (n & 1), np = m / 2;
@@ -309,11 +299,16 @@ size_t syevj_smem(int n) {
   if (m <= JAC_SMEM_MAX) b += (size_t)m * m * sizeof(double);
   return b;
 }
+// doubles of global workspace: the working matrix when it does not fit shared
+// memory, the rotation log, the ranks
+size_t syevj_ws(int n) {
+  const int m = n + (n & 1), np = m / 2;
+  return (size_t)m * m + (size_t)2 * JAC_MAX_SWEEPS * (m - 1) * np + (size_t)m;
+}
 
-// A (n x n, lda; the upper triangle is read, as syevd's UPLO = U) ->
-// eigenvectors in A's first n columns, w ascending.  ws: 2 m^2 doubles
-// (V, and the working matrix when it does not fit shared memory).
-__global__ void __launch_bounds__(JAC_THREADS) k_syevj(int n, double* A, int lda, double* w, double* ws,
+// A (n x n, lda; the upper triangle is read, as syevd's UPLO = U): the
+// eigenvalues ascending into w, their ranks and the rotation log into ws
+__global__ void __launch_bounds__(JAC_THREADS) k_syevj(int n, const double* A, int lda, double* w, double* ws,
                                                        int* sweeps_out, double tol) {
   extern __shared__ __align__(16) unsigned char jsm_raw[];
   const int m = n + (n & 1), np = m / 2;
@@ -322,8 +317,9 @@ __global__ void __launch_bounds__(JAC_THREADS) k_syevj(int n, double* A, int lda
   int* sp = reinterpret_cast<int*>(ss + np);
   int* sq = sp + np;
   double* wsm = reinterpret_cast<double*>(jsm_raw + (((size_t)2 * np * 8 + (size_t)2 * np * 4 + 16 + 15) / 16 * 16));
-  double* W = (m <= JAC_SMEM_MAX) ? wsm : ws + (size_t)m * m;
-  double* V = ws;
+  double* W = (m <= JAC_SMEM_MAX) ? wsm : ws;
+  double2* log = reinterpret_cast<double2*>(ws + (size_t)m * m);
+  int* rank = reinterpret_cast<int*>(ws + (size_t)m * m + (size_t)2 * JAC_MAX_SWEEPS * (m - 1) * np);
   __shared__ double red[JAC_THREADS / 32];
   double f2 = 0;
   for (long e = threadIdx.x; e < (long)m * m; e += blockDim.x) {
@@ -331,7 +327,6 @@ __global__ void __launch_bounds__(JAC_THREADS) k_syevj(int n, double* A, int lda
     double v = 0.0;
     if (r < n && c < n) v = r <= c ? A[(long)c * lda + r] : A[(long)r * lda + c];
     W[e] = v;
-    V[e] = (r == c) ? 1.0 : 0.0;
     f2 += v * v;
   }
   for (int o = 16; o > 0; o >>= 1) f2 += __shfl_xor_sync(0xffffffffu, f2, o);
@@ -344,33 +339,68 @@ __global__ void __launch_bounds__(JAC_THREADS) k_syevj(int n, double* A, int lda
     scale = sqrt(t);
   }
   __syncthreads();
-  const int sw = jacobi_cta(m, W, V, sp, sq, sc, ss, 40, tol, scale);
-  // ascending order: w[rank_i] = W_ii, A[:, rank_i] = V[:, i] (first n rows)
+  const int sw = jacobi_cta(m, W, log, sp, sq, sc, ss, JAC_MAX_SWEEPS, tol, scale);
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     const double di = W[(long)i * m + i];
-    int rank = 0;
+    int rk = 0;
     for (int j = 0; j < n; ++j) {
       const double dj = W[(long)j * m + j];
-      rank += (dj < di) || (dj == di && j < i);
+      rk += (dj < di) || (dj == di && j < i);
     }
-    w[rank] = di;
-    for (int r = 0; r < n; ++r) A[(long)rank * lda + r] = V[(long)i * m + r];
+    w[rk] = di;
+    rank[i] = rk;
   }
-  if (threadIdx.x == 0 && sweeps_out) *sweeps_out = sw;
+  if (threadIdx.x == 0) *sweeps_out = sw;
+}
+
+// V = J_1 J_2 ... from the rotation log, one warp per row of V (a row starts
+// as e_row); columns written to A in ascending eigenvalue order
+__global__ void __launch_bounds__(256) k_jacobi_vectors(int n, double* A, int lda, const double* ws,
+                                                        const int* sweeps_in) {
+  extern __shared__ double rows[];
+  const int m = n + (n & 1), np = m / 2;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int row = blockIdx.x * (blockDim.x >> 5) + wid;
+  double* v = rows + (size_t)wid * m;
+  const double2* log = reinterpret_cast<const double2*>(ws + (size_t)m * m);
+  const int* rank = reinterpret_cast<const int*>(ws + (size_t)m * m + (size_t)2 * JAC_MAX_SWEEPS * (m - 1) * np);
+  if (row >= n) return;
+  for (int i = lane; i < m; i += 32) v[i] = (i == row) ? 1.0 : 0.0;
+  __syncwarp();
+  const int nsteps = *sweeps_in * (m - 1);
+  for (int st = 0; st < nsteps; ++st) {
+    const int r = st % (m - 1);
+    const double2* lg = log + (long)st * np;
+    for (int k = lane; k < np; k += 32) {
+      const double2 cs = lg[k];
+      if (cs.y == 0.0) continue;
+      int a = rr_index(k, r, m), b = rr_index(m - 1 - k, r, m);
+      if (a > b) { const int t = a; a = b; b = t; }
+      const double vp = v[a], vq = v[b];
+      v[a] = cs.x * vp - cs.y * vq;
+      v[b] = cs.y * vp + cs.x * vq;
+    }
+    __syncwarp();
+  }
+  for (int i = lane; i < n; i += 32) A[(long)rank[i] * lda + row] = v[i];
 }
 
 int dense_syevj(int n, double* A, int lda, double* w, DevBuf& ws, int* sweeps_dev, cudaStream_t st) {
   if (n <= 0) return PW_OK;
   const int m = n + (n & 1);
   int rc;
-  if ((rc = ws.alloc((size_t)2 * m * m * sizeof(double)))) return rc;
+  if ((rc = ws.alloc((syevj_ws(n) + 2) * sizeof(double)))) return rc;
+  int* sw = sweeps_dev ? sweeps_dev : reinterpret_cast<int*>((double*)ws.p + syevj_ws(n));
   static PerDeviceOnce attr;
   if (!attr.done()) {
     PWB_CUDA(cudaFuncSetAttribute(k_syevj, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)syevj_smem(JAC_SMEM_MAX)));
     attr.mark();
   }
-  k_syevj<<<1, JAC_THREADS, syevj_smem(n), st>>>(n, A, lda, w, (double*)ws.p, sweeps_dev, 1e-15);
+  k_syevj<<<1, JAC_THREADS, syevj_smem(n), st>>>(n, A, lda, w, (double*)ws.p, sw, 1e-15);
+  const int rows_per_cta = 8;
+  k_jacobi_vectors<<<(n + rows_per_cta - 1) / rows_per_cta, 32 * rows_per_cta, (size_t)rows_per_cta * m * 8, st>>>(
+      n, A, lda, (const double*)ws.p, sw);
   PWB_CUDA(cudaGetLastError());
   return PW_OK;
 }

@@ -24,8 +24,13 @@ def band_range(nband: int, world: int, rank: int) -> tuple[int, int]:
 
 
 def grid_range(ntot: int, world: int, rank: int) -> tuple[int, int]:
-    """(first grid point, number of points) of the row partition used for Gram blocks."""
-    return band_range(ntot, world, rank)
+    """(first grid point, number of points) of the row partition used for Gram
+    blocks: the band_range split in units of 8 points (16-byte rows of the FP32
+    tensor-core operands); the last rank takes any remainder."""
+    if ntot % 8:
+        return band_range(ntot, world, rank)
+    s, n = band_range(ntot // 8, world, rank)
+    return 8 * s, 8 * n
 
 
 def allreduce_sum_(t):
@@ -47,11 +52,117 @@ def max_over_ranks(value: float, device=None) -> float:
     return float(t.item())
 
 
-def gram_row_partitioned(X_rows, Y_rows):
+class DeviceOps:
+    """The local steps of the distributed eigensolver on this rank's GPU, all
+    through the library: Gram blocks and rotations over a row block of the
+    grid (pw_gram_rows / pw_rotate_rows: split-BF16 tensor cores in FP32
+    contexts), the upper Cholesky factor, the triangular inverse and the
+    symmetric eigen-decomposition (pw_dense_potrf / _trtri / _syev).  Blocks
+    are (bands, rows) tensors, i.e. column-major rows x bands matrices."""
+
+    def __init__(self, ctx):
+        self.ctx = ctx
+
+    @staticmethod
+    def _p(t):
+        import ctypes as C
+        return C.c_void_p(t.data_ptr())
+
+    def gram(self, Xr, Yr):
+        """Xr Yr^T (nx x ny, FP64) over this rank's rows."""
+        import torch
+        from ._lib import check, lib
+        nx, nr = Xr.shape
+        ny = Yr.shape[0]
+        G = torch.empty((ny, nx), dtype=torch.float64, device=Xr.device)     # column-major nx x ny
+        check(lib.pw_gram_rows(self.ctx.handle, nr, self._p(Xr), nr, nx, self._p(Yr), nr, ny, self._p(G), nx, None))
+        return G.transpose(0, 1)
+
+    def rotate(self, C, Xr):
+        """C^T Xr: rows of X C for the column-major C (k x m, FP64)."""
+        import torch
+        from ._lib import check, lib
+        k, nr = Xr.shape
+        m = C.shape[1]
+        Cc = C.transpose(0, 1).contiguous()            # column-major k x m
+        out = torch.empty((m, nr), dtype=Xr.dtype, device=Xr.device)
+        check(lib.pw_rotate_rows(self.ctx.handle, nr, self._p(Xr), nr, k, self._p(Cc), k, m, self._p(out), nr, 0,
+                                 None))
+        return out
+
+    def cholesky_upper(self, S):
+        """U with S = U^T U."""
+        import torch
+        from ._lib import check, lib
+        n = S.shape[0]
+        buf = S.contiguous().clone()                   # symmetric: the same in either layout
+        check(lib.pw_dense_potrf(self.ctx.handle, n, self._p(buf), n))
+        return torch.triu(buf.transpose(0, 1))
+
+    def solve_upper_t(self, U, Xr):
+        """U^-T Xr (rows of X U^-1)."""
+        import torch
+        from ._lib import check, lib
+        n = U.shape[0]
+        ub = U.transpose(0, 1).contiguous()            # column-major U
+        ui = torch.empty_like(ub)
+        check(lib.pw_dense_trtri(self.ctx.handle, n, self._p(ub), n, self._p(ui), n))
+        return self.rotate(ui.transpose(0, 1), Xr)
+
+    def eigh(self, A):
+        """(ascending eigenvalues, column eigenvectors) of a symmetric A."""
+        import ctypes as C
+
+        import torch
+        from ._lib import check, lib
+        n = A.shape[0]
+        buf = (0.5 * (A + A.transpose(0, 1))).contiguous()
+        w = torch.empty(n, dtype=torch.float64, device=A.device)
+        sw = C.c_int(0)
+        check(lib.pw_dense_syev(self.ctx.handle, n, self._p(buf), n, self._p(w), C.byref(sw)))
+        return w, buf.transpose(0, 1)
+
+
+class HostOps:
+    """The same local steps with torch on the CPU: the form the multi-process
+    tests on CPU ranks (gloo) use to check the transposes and reductions."""
+
+    def gram(self, Xr, Yr):
+        return Xr @ Yr.transpose(0, 1)
+
+    def rotate(self, C, Xr):
+        return C.transpose(0, 1) @ Xr
+
+    def cholesky_upper(self, S):
+        import torch
+        return torch.linalg.cholesky(0.5 * (S + S.transpose(0, 1)), upper=True)
+
+    def solve_upper_t(self, U, Xr):
+        import torch
+        return torch.linalg.solve_triangular(U.transpose(0, 1), Xr, upper=False)
+
+    def eigh(self, A):
+        import torch
+        return torch.linalg.eigh(0.5 * (A + A.transpose(0, 1)))
+
+
+def local_ops(t, ctx=None):
+    """DeviceOps for CUDA tensors (a library context is required: the product
+    path has no fallback), HostOps for CPU tensors."""
+    if t.is_cuda:
+        if ctx is None:
+            raise ValueError("device blocks need the rank's library context (ctx) for the local steps")
+        return DeviceOps(ctx)
+    return HostOps()
+
+
+def gram_row_partitioned(X_rows, Y_rows, ctx=None):
     """X^T Y for blocks partitioned by grid rows (each rank holds rows of all
-    bands): local product then a sum over ranks."""
-    G = X_rows.transpose(0, 1) @ Y_rows
-    return allreduce_sum_(G)
+    bands; tensors (rows, bands)): local product then a sum over ranks."""
+    Xb = X_rows.transpose(0, 1).contiguous()
+    Yb = Y_rows.transpose(0, 1).contiguous()
+    G = local_ops(Xb, ctx).gram(Xb, Yb)
+    return allreduce_sum_(G.contiguous())
 
 
 # ---------------------------------------------------------------------------
@@ -122,26 +233,25 @@ def _bcast_(t):
     return t
 
 
-def cholqr_rows(Xr):
+def cholqr_rows(Xr, ctx=None):
     """Cholesky-QR of a row-partitioned block (EigenSolver::Orthogonalize,
-    src/EigenSolver/eigensolver.cpp:301-384): S = sum_ranks Xr Xr^T, S = U^T U,
-    X <- X U^-1 (rows: Xr <- U^-T Xr)."""
-    import torch
-    S = allreduce_sum_(Xr @ Xr.transpose(0, 1))
-    U = _bcast_(torch.linalg.cholesky(0.5 * (S + S.transpose(0, 1)), upper=True))
-    return torch.linalg.solve_triangular(U.transpose(0, 1), Xr, upper=False)
+    src/EigenSolver/eigensolver.cpp:301-384): S = sum_ranks Xr Xr^T, S = U^T U
+    (rank 0, broadcast), X <- X U^-1 (rows: Xr <- U^-T Xr)."""
+    ops = local_ops(Xr, ctx)
+    S = allreduce_sum_(ops.gram(Xr, Xr).contiguous())
+    U = _bcast_(ops.cholesky_upper(S).contiguous())
+    return ops.solve_upper_t(U, Xr)
 
 
-def rayleigh_ritz_rows(Xr, HXr):
+def rayleigh_ritz_rows(Xr, HXr, ctx=None):
     """Rayleigh-Ritz on row-partitioned X and HX: A = sum_ranks Xr HXr^T,
     A = C diag(l) C^T (solved on rank 0 and broadcast, as the reference's
     rank-0 Syevd), X <- X C, HX <- HX C.  Returns (l, Xr, HXr)."""
-    import torch
-    A = allreduce_sum_(Xr @ HXr.transpose(0, 1))
-    lam, C = torch.linalg.eigh(0.5 * (A + A.transpose(0, 1)))
+    ops = local_ops(Xr, ctx)
+    A = allreduce_sum_(ops.gram(Xr, HXr).contiguous())
+    lam, C = ops.eigh(A)
     lam, C = _bcast_(lam.contiguous()), _bcast_(C.contiguous())
-    Ct = C.transpose(0, 1)
-    return lam, Ct @ Xr, Ct @ HXr
+    return lam, ops.rotate(C, Xr), ops.rotate(C, HXr)
 
 
 def chebyshev_filter(apply_h, X, degree: int, a: float, b: float, a0: float):
@@ -193,7 +303,7 @@ def lanczos_upper_bound(apply_h, x0, steps: int = 16) -> float:
 
 
 def chebfsi_dist(apply_h, Xb, nband: int, degree: int = 10, max_iter: int = 100, tol: float = 1e-9,
-                 nconv: int | None = None):
+                 nconv: int | None = None, ctx=None):
     """Distributed ChebFSI: Chebyshev-filtered subspace iteration over band
     shards (filter and H*psi local to each rank; Cholesky-QR and Rayleigh-Ritz
     on grid rows after an all-to-all transpose).  Xb: this rank's bands
@@ -201,24 +311,25 @@ def chebfsi_dist(apply_h, Xb, nband: int, degree: int = 10, max_iter: int = 100,
     block of this rank's bands to H times it (pw_hpsi on the rank's GPU).
     Returns (eigenvalues, Xb, iterations, max residual) with residuals
     ||H x - l x|| / max(1, |l|) of the lowest nconv (default all) pairs,
-    gathered over ranks."""
+    gathered over ranks.  ctx: the rank's library context, required for
+    device blocks (the local Gram, rotation and dense steps run through it)."""
     import torch
     world, rank = _world()
     ntot = Xb.shape[1]
     b_up = lanczos_upper_bound(apply_h, Xb)
     s, n = band_range(nband, world, rank)
     # first pass: orthonormalise and Rayleigh-Ritz the start block
-    Xr = cholqr_rows(band_to_rows(Xb, nband))
+    Xr = cholqr_rows(band_to_rows(Xb, nband), ctx)
     Xb = rows_to_band(Xr, ntot)
-    lam, Xr, HXr = rayleigh_ritz_rows(Xr, band_to_rows(apply_h(Xb), nband))
+    lam, Xr, HXr = rayleigh_ritz_rows(Xr, band_to_rows(apply_h(Xb), nband), ctx)
     Xb = rows_to_band(Xr, ntot)
     res_max = float("inf")
     it = 0
     for it in range(1, max_iter + 1):
         Y = chebyshev_filter(apply_h, Xb, degree, float(lam[-1]), b_up, float(lam[0]))
-        Yr = cholqr_rows(band_to_rows(Y, nband))
+        Yr = cholqr_rows(band_to_rows(Y, nband), ctx)
         Yb = rows_to_band(Yr, ntot)
-        lam, Xr, HXr = rayleigh_ritz_rows(Yr, band_to_rows(apply_h(Yb), nband))
+        lam, Xr, HXr = rayleigh_ritz_rows(Yr, band_to_rows(apply_h(Yb), nband), ctx)
         Xb = rows_to_band(Xr, ntot)
         HXb = rows_to_band(HXr, ntot)
         loc = torch.linalg.norm(HXb - lam[s:s + n, None] * Xb, dim=1) / torch.clamp(lam[s:s + n].abs(), min=1.0)
