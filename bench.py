@@ -777,7 +777,7 @@ def run_ours(args):
     if args.autotune:
         tune = ctx.autotune(NBAND)      # set-up (untimed): band batch and projector GEMM tiles
     else:
-        tune = {"band_batch": NBAND, "gemm_bn": 0, "gemm_bn_store": 0}
+        tune = {"band_batch": NBAND, "gemm_bn": 0, "gemm_bn_store": 0, "fft_variant": 0}
     dt_t = ctx.torch_dtype
     g = torch.Generator(device="cuda").manual_seed(SEED + rank)
     X = torch.randn((NBAND, ctx.ntot), dtype=torch.float64, device="cuda", generator=g)
@@ -879,6 +879,7 @@ def run_ours(args):
             "config": {"workload": WORKLOAD, "grid": list(NC), "fine_grid": list(NF), "bands": NBAND,
                        "nonlocal": "dense coarse-grid projector matrix (GEMM)",
                        "band_batch": tune["band_batch"], "gemm_tiles": [tune["gemm_bn"], tune["gemm_bn_store"]],
+                       "fft_variant": tune.get("fft_variant", 0),
                        "l2": "flushed between steps (256 MB device write)",
                        "parallelism": f"band blocks, {world} replica(s)"},
             "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -378,8 +378,9 @@ PW_API int pw_ctx_build_twin(pw_ctx* ctx);
 PW_API int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* eig_out, double* rho_out);
 
 /* Autotuner (no reference counterpart): times pw_hpsi on an internal block
- * of nband bands for candidate band-batch widths and, for FP32 contexts with
- * dense projectors, the tile widths of the two projector GEMMs; applies the
+ * of nband bands for candidate band-batch widths, the two radix decompositions
+ * of the fused fine-plane transforms and, for FP32 contexts with dense
+ * projectors, the tile widths of the two projector GEMMs; applies the
  * fastest setting to the context and caches it for later contexts of the
  * same grid, precision, band count and projector count (then cached = 1 and
  * no timing runs).  The local potential must be set. */
@@ -391,7 +392,12 @@ typedef struct pw_tune_result {
   int cached;               /* 1: taken from the cache */
   double ms_default;        /* sweep time with the defaults */
   double ms_best;           /* sweep time with the chosen setting */
+  int fft_variant;          /* radix decomposition of the fused fine-plane transforms (0: default, 1: second) */
 } pw_tune_result;
+/* Select the radix decomposition of the fused fine-plane transforms directly
+ * (0: the default N = n1 x n2 of each length, 1: the second one, e.g. 96 =
+ * 12 x 8 instead of 8 x 12); pw_autotune times both.  No reference counterpart. */
+PW_API int pw_set_fft_variant(pw_ctx* ctx, int variant);
 PW_API int pw_autotune(pw_ctx* ctx, int nband, pw_tune_result* result);
 
 /* CUDA graph of one pw_hpsi call (same pointers, band count and accumulate

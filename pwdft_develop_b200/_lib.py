@@ -62,7 +62,7 @@ class ScfResult(C.Structure):
 
 class TuneResult(C.Structure):
     _fields_ = [("band_batch", C.c_int), ("gemm_bn", C.c_int), ("gemm_bn_store", C.c_int), ("tried", C.c_int),
-                ("cached", C.c_int), ("ms_default", C.c_double), ("ms_best", C.c_double)]
+                ("cached", C.c_int), ("ms_default", C.c_double), ("ms_best", C.c_double), ("fft_variant", C.c_int)]
 
 
 # name -> (restype, argtypes); every name here is declared in include/pwdft_b200.h
@@ -81,6 +81,7 @@ SIGNATURES: dict[str, tuple] = {
     "pw_teter_precond_noalloc": (_i, [_vp, _vp, _i, _vp, _i, _i, _i, _vp]),
     "pw_set_wfn_filter": (_i, [_vp, _i, C.c_double]),
     "pw_set_wait_limit": (_i, [_vp, C.c_double]),
+    "pw_set_fft_variant": (_i, [_vp, _i]),
     "pw_dense_potrf": (_i, [_vp, _i, _vp, _i]),
     "pw_rotate": (_i, [_vp, _vp, _i, _i, _vp, _i, _i, _vp, _i, _i, _vp]),
     "pw_gram_rows": (_i, [_vp, _i, _vp, _i, _i, _vp, _i, _i, _vp, _i, _vp]),

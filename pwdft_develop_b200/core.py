@@ -660,10 +660,19 @@ def _ctx_capture_hpsi(self, psi, out, accumulate: bool = False) -> HpsiGraph:
 
 
 def _ctx_autotune(self, nband: int) -> dict:
-    """pw_autotune: pick band-batch width and projector GEMM tiles by timing."""
+    """pw_autotune: pick band-batch width, fine-plane FFT radix decomposition
+    and projector GEMM tiles by timing."""
     r = _lib.TuneResult()
     check(lib.pw_autotune(self._h, int(nband), C.byref(r)))
     return {k: getattr(r, k) for k, _ in r._fields_}
+
+
+def _ctx_set_fft_variant(self, variant: int):
+    """Radix decomposition of the fused fine-plane transforms (0 default, 1 second)."""
+    check(lib.pw_set_fft_variant(self._h, int(variant)))
+
+
+Context.set_fft_variant = _ctx_set_fft_variant
 
 
 Context.autotune = _ctx_autotune

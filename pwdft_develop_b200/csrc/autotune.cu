@@ -1,6 +1,7 @@
 // Autotuner for the H*psi sweep: times pw_hpsi on a scratch block (L2
-// flushed before each timed sweep) for candidate band-batch widths and, for
-// FP32 contexts with projectors, the tile widths of the two projector GEMMs
+// flushed before each timed sweep) for candidate band-batch widths, the two
+// radix decompositions of the fused fine-plane transforms and, for FP32
+// contexts with projectors, the tile widths of the two projector GEMMs
 // (coordinate descent; a candidate must beat the current best by 3%), keeps
 // the fastest setting in the context and caches it per (grid, precision,
 // bands, projectors) for later contexts of the same shape.
@@ -29,7 +30,7 @@ __global__ void k_fill_hash(T* x, long n, unsigned seed, double scale) {
 
 using TuneKey = std::tuple<int, int, int, int, int, int>;
 struct TuneVal {
-  int band_batch, bn, bn_store;
+  int band_batch, bn, bn_store, fft_variant;
 };
 static std::mutex g_tune_mu;
 static std::map<TuneKey, TuneVal>& tune_cache() {
@@ -58,11 +59,13 @@ int pw_autotune(pw_ctx* ctx, int nband, pw_tune_result* res) {
       if (rc) return rc;
       ctx->gemm_bn = it->second.bn;
       ctx->gemm_bn_store = it->second.bn_store;
+      ctx->fft_variant = it->second.fft_variant;
       if (res) {
         *res = pw_tune_result{};
         res->band_batch = it->second.band_batch;
         res->gemm_bn = it->second.bn;
         res->gemm_bn_store = it->second.bn_store;
+        res->fft_variant = it->second.fft_variant;
         res->cached = 1;
       }
       return PW_OK;
@@ -105,6 +108,7 @@ int pw_autotune(pw_ctx* ctx, int nband, pw_tune_result* res) {
     *ms = best;
     return PW_OK;
   };
+  ctx->fft_variant = 0;
   double t_def = 0;
   if ((rc = run(nband, 0, 0, &t_def))) return rc;
   int best_bb = nband, best_bn = 0, best_bns = 0;
@@ -118,6 +122,16 @@ int pw_autotune(pw_ctx* ctx, int nband, pw_tune_result* res) {
     double t;
     if ((rc = run(bb, 0, 0, &t))) return rc;
     if (t < 0.97 * best) { best = t; best_bb = bb; }
+  }
+  // the second radix decomposition of the fine-plane transforms (dense
+  // projector mode: the fused fine-plane kernel)
+  int best_var = 0;
+  if (ctx->nl_mode == PW_NL_DENSE && !ctx->gs) {
+    ctx->fft_variant = 1;
+    double t;
+    if ((rc = run(best_bb, 0, 0, &t))) return rc;
+    if (t < 0.97 * best) { best = t; best_var = 1; }
+    ctx->fft_variant = best_var;
   }
   if (ctx->prec == PW_F32 && ctx->have_nl && ctx->nl_mode == PW_NL_DENSE && ctx->gemm_mode == 0) {
     for (int bn : {64, 96, 128, 160, 256}) {
@@ -136,15 +150,17 @@ int pw_autotune(pw_ctx* ctx, int nband, pw_tune_result* res) {
   if ((rc = pw_set_band_batch(ctx, best_bb))) return rc;
   ctx->gemm_bn = best_bn;
   ctx->gemm_bn_store = best_bns;
+  ctx->fft_variant = best_var;
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    tune_cache()[key] = TuneVal{best_bb, best_bn, best_bns};
+    tune_cache()[key] = TuneVal{best_bb, best_bn, best_bns, best_var};
   }
   if (res) {
     *res = pw_tune_result{};
     res->band_batch = best_bb;
     res->gemm_bn = best_bn;
     res->gemm_bn_store = best_bns;
+    res->fft_variant = best_var;
     res->ms_default = t_def;
     res->ms_best = best;
     res->tried = tried;

@@ -126,6 +126,7 @@ struct pw_ctx {
   int gemm_mode = 0;             // 0 tensor-core split-BF16, 1 vendor SGEMM
   int gemm_terms = 3;            // split products per k-step (3 or 4)
   int gemm_bn = 0, gemm_bn_store = 0;   // projector GEMM tile widths (0: heuristic; set by pw_autotune)
+  int fft_variant = 0;           // radix decomposition of the fine-plane transforms (0 / 1; set by pw_autotune)
   bool check_errors = false;     // read the device error flag after each call (synchronises)
   pw_ctx* twin = nullptr;        // FP32 twin of an FP64 context (mixed-precision SCF), owned
   int nproj_pad = 0;

@@ -530,6 +530,12 @@ int pw_hpsi(pw_ctx* ctx, const void* psi, int ld, void* hpsi, int ldh, int nband
   return PW_OK;
 }
 
+int pw_set_fft_variant(pw_ctx* ctx, int variant) {
+  PWB_CHECK(ctx && (variant == 0 || variant == 1), PW_EINVAL, "FFT variant must be 0 or 1");
+  ctx->fft_variant = variant;
+  return PW_OK;
+}
+
 int pw_set_wait_limit(pw_ctx* ctx, double seconds) {
   PWB_CHECK(ctx && seconds > 0 && seconds < 3600, PW_EINVAL, "wait limit must be in (0, 3600) s");
   PWB_CUDA(cudaSetDevice(ctx->device));

@@ -284,6 +284,16 @@ __device__ __forceinline__ void smem_fft_cb(V* base, int count, const V* tw) {
   smem_fft_c<N, DIR, ES, BS, FB>(base, count, tw, (int)(threadIdx.x >> 5), (int)(blockDim.x >> 5));
 }
 
+// Second radix decomposition N = n1 x (N / n1) of the longer lengths, the
+// alternative the autotuner times against Split (the fine-plane kernel takes
+// either; the other lengths have one).
+template <int N> struct SplitAlt { static constexpr int n1 = Split<N>::n1; };
+#define PWB_SPLIT_ALT(N_, N1_) template <> struct SplitAlt<N_> { static constexpr int n1 = N1_; };
+PWB_SPLIT_ALT(48, 8) PWB_SPLIT_ALT(60, 10) PWB_SPLIT_ALT(64, 16) PWB_SPLIT_ALT(72, 12) PWB_SPLIT_ALT(80, 10)
+PWB_SPLIT_ALT(96, 12) PWB_SPLIT_ALT(120, 12) PWB_SPLIT_ALT(128, 16) PWB_SPLIT_ALT(144, 16)
+#undef PWB_SPLIT_ALT
+template <int N, int VAR> struct SplitVar { static constexpr int n1 = VAR ? SplitAlt<N>::n1 : Split<N>::n1; };
+
 // Number of transforms one warp processes together for length N.
 template <int N> struct FftGroup {
   static constexpr int f = 32 / Split<N>::n1;

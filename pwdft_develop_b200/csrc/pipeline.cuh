@@ -26,6 +26,7 @@
 
 #include <mutex>
 #include <string>
+#include <type_traits>
 
 #include "common.hpp"
 #include "fft.cuh"
@@ -687,18 +688,27 @@ PWB_FLOC_LAYOUT(double, 144, 74, 1, 156, 1, false, false)
 #undef PWB_FLOC_LAYOUT
 // elements of the S tile of k_floc2 for a plane of NYF rows split NY2 per skew step
 template <typename LY, int NYF, int NY2> constexpr int floc_s_size() { return NYF * LY::PS + LY::SKS * (NYF / NY2); }
+// the plain padded layout (the alternative radix decomposition uses it)
+template <int NXF> struct FlocLayoutPlain {
+  static constexpr int PS = NXF / 2 + 1, SKS = 0, PR = NXF + 1, SKR = 0;
+  static constexpr bool FA = false, FB = false;
+};
+template <typename T, int NXF, int NYF, int VAR>
+using FlocLayoutVar = typename std::conditional<VAR == 0, FlocLayout<T, NXF, NYF>, FlocLayoutPlain<NXF>>::type;
 
-template <typename T, int NXF, int NYF>
+// VAR selects the radix decomposition of the x and y transforms (0: Split,
+// 1: SplitAlt), the autotuner's FFT candidate
+template <typename T, int NXF, int NYF, int VAR = 0>
 __global__ void __launch_bounds__(FLOC_THREADS, sizeof(T) == 4 ? 3 : 1)
 k_floc2(VT<T>* __restrict__ BC, const T* __restrict__ vtot, T inv_nf, const VT<T>* twx_g, const VT<T>* twy_g) {
   using V = VT<T>;
   constexpr int n0 = NXF / 2;
   constexpr int nsx = n0 + 1, nsy = NYF / 2 + 1;
-  using LY = FlocLayout<T, NXF, NYF>;
+  using LY = FlocLayoutVar<T, NXF, NYF, VAR>;
   constexpr int PS = LY::PS, SKS = LY::SKS, PR = LY::PR, SKR = LY::SKR;
   constexpr bool FA = LY::FA, FB = LY::FB;
-  constexpr int NX1 = Split<NXF>::n1, NX2 = NXF / NX1, FX = 32 / NX1;
-  constexpr int NY1 = Split<NYF>::n1, NY2 = NYF / NY1, FY = 32 / NY1;
+  constexpr int NX1 = SplitVar<NXF, VAR>::n1, NX2 = NXF / NX1, FX = 32 / NX1;
+  constexpr int NY1 = SplitVar<NYF, VAR>::n1, NY2 = NYF / NY1, FY = 32 / NY1;
   constexpr int RX = (FX * NX2 + 31) / 32, RY = (FY * NY2 + 31) / 32;
   static_assert(PS >= nsx && PR >= NXF + SKR * (NX1 - 1), "k_floc2 layout rows overlap");
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -1381,10 +1391,17 @@ struct Plan {
   static size_t sm_floc() {
     return sizeof(V) * ((size_t)NF1 * (N0 + 1) + NF0 + NF1 + (size_t)(FLOC_THREADS / 32) * FftGroup<NF0>::f * (NF0 + 1));
   }
-  static size_t sm_floc2() {
-    using LY = FlocLayout<T, NF0, NF1>;
-    return sizeof(V) * ((size_t)floc_s_size<LY, NF1, NF1 / Split<NF1>::n1>() + NF0 + NF1 +
-                        (size_t)(FLOC_THREADS / 32) * FftGroup<NF0>::f * LY::PR);
+  template <int VAR = 0> static size_t sm_floc2() {
+    using LY = FlocLayoutVar<T, NF0, NF1, VAR>;
+    return sizeof(V) * ((size_t)floc_s_size<LY, NF1, NF1 / SplitVar<NF1, VAR>::n1>() + NF0 + NF1 +
+                        (size_t)(FLOC_THREADS / 32) * (32 / SplitVar<NF0, VAR>::n1) * LY::PR);
+  }
+  // the fused fine-plane kernel in the context's radix decomposition
+  static void launch_floc2(pw_ctx* c, V* BC, const T* vt, T inv_nf, int nblk, cudaStream_t st) {
+    if (c->fft_variant == 1)
+      k_floc2<T, NF0, NF1, 1><<<dim3(NF2, nblk), FLOC_THREADS, sm_floc2<1>(), st>>>(BC, vt, inv_nf, tw(c, 3), tw(c, 4));
+    else
+      k_floc2<T, NF0, NF1, 0><<<dim3(NF2, nblk), FLOC_THREADS, sm_floc2<0>(), st>>>(BC, vt, inv_nf, tw(c, 3), tw(c, 4));
   }
   static size_t sm_fplane(int cr) {
     return sizeof(V) * ((size_t)NF1 * (N0 + 1) + (size_t)cr * (NF0 + 1) + NF0 + NF1);
@@ -1402,7 +1419,8 @@ struct Plan {
     PWB_CUDA(cudaFuncSetAttribute(k_cxy_inv<T, N0, N1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_cxy()));
     PWB_CUDA(cudaFuncSetAttribute(k_zteter<T, N2, TX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_zteter()));
     PWB_CUDA(cudaFuncSetAttribute(k_floc<T, NF0, NF1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_floc()));
-    PWB_CUDA(cudaFuncSetAttribute(k_floc2<T, NF0, NF1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_floc2()));
+    PWB_CUDA(cudaFuncSetAttribute(k_floc2<T, NF0, NF1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_floc2<0>()));
+    PWB_CUDA(cudaFuncSetAttribute(k_floc2<T, NF0, NF1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_floc2<1>()));
     PWB_CUDA(cudaFuncSetAttribute(k_floc<T, NF0, NF1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_floc()));
     once.mark();
     return PW_OK;
@@ -1432,8 +1450,7 @@ struct Plan {
         AD, K, BC, reinterpret_cast<const T*>(c->ekin.p), N0, N1, inv_nc, tw(c, 2), tw(c, 5)); }
     if (c->nl_mode == PW_NL_DENSE) {
       { Launch L_(c, st, KK_FPLANE_APPLY);
-      k_floc2<T, NF0, NF1><<<dim3(NF2, npair), FLOC_THREADS, sm_floc2(), st>>>(
-          BC, reinterpret_cast<const T*>(c->vtot.p), inv_nf, tw(c, 3), tw(c, 4)); }
+      launch_floc2(c, BC, reinterpret_cast<const T*>(c->vtot.p), inv_nf, npair, st); }
       { Launch L_(c, st, KK_ZFOLD);
       k_zfold<T, N2, NF2, TXF><<<dim3(N1, (N0 + TXF - 1) / TXF, npair), PENCIL_THREADS, sm_zfold(), st>>>(
           BC, K, AD, N0, N1, tw(c, 2), tw(c, 5), 0, (T)0, 0, filt ? reinterpret_cast<const T*>(c->wmask.p) : nullptr); }
@@ -1689,8 +1706,7 @@ struct Plan {
         AD, K, BC, ekin_all ? ekin_all : reinterpret_cast<const T*>(c->ekin_k.p), N0, N1, inv_nc, tw(c, 2), tw(c, 5),
         1, band0, fpk, ekin_all ? c->ntot : 0); }
     { Launch L_(c, st, KK_FPLANE_APPLY);
-    k_floc2<T, NF0, NF1><<<dim3(NF2, nb), FLOC_THREADS, sm_floc2(), st>>>(
-        BC, reinterpret_cast<const T*>(c->vtot.p), inv_nf, tw(c, 3), tw(c, 4)); }
+    launch_floc2(c, BC, reinterpret_cast<const T*>(c->vtot.p), inv_nf, nb, st); }
     { Launch L_(c, st, KK_ZFOLD);
     k_zfold<T, N2, NF2, TXF><<<dim3(N1, (N0 + TXF - 1) / TXF, nb), PENCIL_THREADS, sm_zfold(), st>>>(
         BC, K, AD, N0, N1, tw(c, 2), tw(c, 5), 0, (T)0, 1); }
@@ -1929,8 +1945,7 @@ struct Plan {
     k_gs_zinv<T, N0, N1, NF2><<<dim3(N1 + 1, npair), PENCIL_THREADS, sm_gs_zinv(), st>>>(
         psi, ld, nband, band0, rows_i, ent_i, BC, tw(c, 5)); }
     { Launch L_(c, st, KK_FPLANE_APPLY);
-    k_floc2<T, NF0, NF1><<<dim3(NF2, npair), FLOC_THREADS, sm_floc2(), st>>>(
-        BC, reinterpret_cast<const T*>(c->vtot.p), inv_n, tw(c, 3), tw(c, 4)); }
+    launch_floc2(c, BC, reinterpret_cast<const T*>(c->vtot.p), inv_n, npair, st); }
     { Launch L_(c, st, KK_ZFOLD);
     k_gs_zfwd<T, N0, N1, NF2><<<dim3(N1 / 2 + 1, npair), PENCIL_THREADS, sm_gs_zfwd(), st>>>(
         BC, psi, ld, out, ldo, nband, band0, accumulate, reinterpret_cast<const int*>(c->gs_rows_fwd.p),

@@ -8,7 +8,15 @@ the HSE06 short-range exchange ``pbexsr`` / ``wpbe_analy_erfc_approx_grad``
 (src/utility.cpp:3340-3846) -> ``ref_xc_hse.npz``, all compiled from the
 reference source tree by ``oracle/build_ref.py``.  Inputs are seeded.  Run
 from the repository root:
-``python tests/golden/make_golden.py [utility|pbe|hse]`` (all by default).
+``python tests/golden/make_golden.py [utility|pbe|hse|hpsi]`` (all by default).
+
+``hpsi`` -> ``ref_hpsi.npz``: the reference's own H*psi composition,
+Spinor::AddMultSpinorFineR2C and Spinor::AddTeterPrecond (src/SCF/spinor.cpp:
+310-346, 377-525) with FFTWExecute (src/SCF/fourier.cpp:695-764) and
+IP_c2f / IP_f2c, compiled by ``oracle/build_ref.py`` (``libpwref_hpsi.so``), on
+seeded Si8 cells: the projector sets, kinetic and Teter tables come from the
+oracle's restatement of PeriodTable::CalculateNonlocalPP / CalculateEkin
+(oracle/pw.py), the potential and the bands from the seeds stored with them.
 """
 import ctypes as C
 import sys
@@ -105,6 +113,45 @@ def hse():
     print(OUT_HSE, OUT_HSE.stat().st_size)
 
 
+OUT_HPSI = Path(__file__).resolve().parent / "ref_hpsi.npz"
+HPSI_CASES = {"c12": ((12, 12, 12), 3), "c16": ((16, 16, 16), 2)}
+
+
+def hpsi():
+    from oracle import pw
+    lib = C.CDLL(str(build_ref.build_hpsi()))
+    dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+    ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+    lib.ref_add_mult_spinor.argtypes = [ip, ip, dp, dp, dp, C.c_int, ip, ip, ip, dp, dp, C.c_int, dp, dp]
+    lib.ref_add_teter.argtypes = [ip, ip, dp, dp, C.c_int, dp, dp]
+    data = {}
+    for tag, (nc, nb) in HPSI_CASES.items():
+        seed_cell, seed_v, seed_psi = 20261203 + 1, 31, 32
+        L, z, pos = pw.make_crystal("Si", (1, 1, 1), 10.26, 0.02, seed_cell)
+        nf = tuple(2 * n for n in nc)
+        T, _ = pw.build_tables(L, z, pos, nc, nf, seed_v=seed_v)
+        psi = pw.random_orthonormal_psi(T.dm.ntot, nb, seed_psi)
+        npts = np.array([len(a[0].idx) for a in T.pseudo], np.int32)
+        nproj = np.array([len(a) for a in T.pseudo], np.int32)
+        idx = np.concatenate([a[0].idx for a in T.pseudo]).astype(np.int32)
+        beta = np.concatenate([pp.val[:, 0] for a in T.pseudo for pp in a]).astype(np.float64)
+        wgt = np.array([pp.wgt for a in T.pseudo for pp in a], np.float64)
+        h = np.zeros_like(psi)
+        w = np.zeros_like(psi)
+        ncv, nfv, Lv = np.array(nc, np.int32), np.array(nf, np.int32), np.array(L, np.float64)
+        assert lib.ref_add_mult_spinor(ncv, nfv, Lv, np.ascontiguousarray(T.ekin.ravel()), T.vtot, len(T.pseudo),
+                                       npts, nproj, idx, beta, wgt, nb, np.ascontiguousarray(psi), h) == 0
+        assert lib.ref_add_teter(ncv, nfv, Lv, np.ascontiguousarray(T.teter.ravel()), nb, np.ascontiguousarray(psi),
+                                 w) == 0
+        data[f"{tag}_grid"] = np.array(nc)
+        data[f"{tag}_seeds"] = np.array([seed_cell, seed_v, seed_psi])
+        data[f"{tag}_nband"] = np.array(nb)
+        data[f"{tag}_hpsi"] = h
+        data[f"{tag}_teter"] = w
+    np.savez_compressed(OUT_HPSI, **data)
+    print(OUT_HPSI, OUT_HPSI.stat().st_size)
+
+
 if __name__ == "__main__":
     which = sys.argv[1] if len(sys.argv) > 1 else "all"
     if which in ("all", "utility"):
@@ -113,3 +160,5 @@ if __name__ == "__main__":
         pbe()
     if which in ("all", "hse"):
         hse()
+    if which in ("all", "hpsi"):
+        hpsi()

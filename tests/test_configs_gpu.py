@@ -89,3 +89,27 @@ def test_gram_at_lobpcg_widths(n, K):
     G = c.gram(X, Y)
     assert bool(((G - ref[:, : n // 3]).abs() <= bound[:, : n // 3]).all())
     c.close()
+
+
+@pytest.mark.parametrize("kind,reps,a,nc", [("Si", (1, 1, 1), 10.26, (24, 24, 24)), ("Si", (2, 2, 2), 10.26, (48, 48, 48)),
+                                            ("Al", (2, 2, 2), 7.65, (60, 60, 60)), ("Si", (2, 1, 1), 10.26, (48, 24, 24)),
+                                            ("Si", (3, 3, 3), 10.26, (72, 72, 72))])
+def test_hpsi_second_fft_decomposition_matches_oracle(kind, reps, a, nc):
+    """The fused fine-plane kernel in its second radix decomposition (the
+    autotuner's FFT candidate: 48 = 8 x 6, 96 = 12 x 8, 120 = 12 x 10,
+    144 = 16 x 9) against the oracle: FP64 1e-12, FP32 1e-5."""
+    import torch
+    from pwdft_develop_b200 import Context
+    L, z, pos = pw.make_crystal(kind, reps, a, 0.02, 77)
+    nf = tuple(2 * n for n in nc)
+    T, _ = pw.build_tables(L, z, pos, nc, nf, seed_v=78)
+    psi = pw.random_orthonormal_psi(T.dm.ntot, 3, 79)
+    ref = pw.mult_spinor(T, psi)
+    for prec in ("f64", "f32"):
+        c = Context(L, nc, nf, precision=prec)
+        c.set_vtot(T.vtot)
+        c.set_atoms([z] * len(pos), pos)
+        c.set_fft_variant(1)
+        got = c.hpsi(torch.tensor(psi, dtype=c.torch_dtype, device="cuda")).double().cpu().numpy()
+        assert np.abs(got - ref).max() / np.abs(ref).max() <= TOL[prec], (nc, prec)
+        c.close()

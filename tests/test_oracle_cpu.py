@@ -333,3 +333,59 @@ def test_wfn_ecut_filter_is_an_orthogonal_projector():
     assert np.abs(X[:, T.ekin <= ecut] - pw.r2c(x.reshape(3, 16, 16, 16), T.dm)[:, T.ekin <= ecut]).max() < 1e-12
     h = pw.mult_spinor(T, x, wfn_ecut=ecut)
     assert np.abs(h - pw.wfn_ecut_filter(T, pw.mult_spinor(T, x), ecut)).max() < 1e-12
+
+
+def _ref_hpsi_case(tag):
+    g = np.load(GOLD.parent / "ref_hpsi.npz")
+    nc = tuple(int(x) for x in g[f"{tag}_grid"])
+    seed_cell, seed_v, seed_psi = (int(x) for x in g[f"{tag}_seeds"])
+    L, z, pos = pw.make_crystal("Si", (1, 1, 1), 10.26, 0.02, seed_cell)
+    T, _ = pw.build_tables(L, z, pos, nc, tuple(2 * n for n in nc), seed_v=seed_v)
+    psi = pw.random_orthonormal_psi(T.dm.ntot, int(g[f"{tag}_nband"]), seed_psi)
+    return g, T, psi
+
+
+@pytest.mark.parametrize("tag", ["c12", "c16"])
+def test_oracle_hpsi_matches_reference_composition(tag):
+    """The restated H*psi and Teter (oracle/pw.py) against the outputs of the
+    reference's own Spinor::AddMultSpinorFineR2C / AddTeterPrecond compiled
+    from its source (tests/golden/ref_hpsi.npz, make_golden.py hpsi): 1e-13."""
+    g, T, psi = _ref_hpsi_case(tag)
+    h = pw.mult_spinor(T, psi)
+    ref = g[f"{tag}_hpsi"]
+    assert np.abs(h - ref).max() / np.abs(ref).max() < 1e-13
+    w = pw.add_teter_precond(T, psi)
+    wr = g[f"{tag}_teter"]
+    assert np.abs(w - wr).max() / np.abs(wr).max() < 1e-13
+
+
+def test_oracle_hpsi_against_compiled_reference_other_grids():
+    """Where the reference tree is present (the build container), the compiled
+    composition on a non-cubic grid with uneven dimensions (24 x 16 x 20) and
+    an fcc Al cell, against the restatement: 1e-13."""
+    import ctypes as C
+
+    from oracle import build_ref
+    lib_path = build_ref.LIB_HPSI
+    if not lib_path.exists():
+        pytest.skip("reference composition not built here (oracle/_ref)")
+    lib = C.CDLL(str(lib_path))
+    dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+    ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+    lib.ref_add_mult_spinor.argtypes = [ip, ip, dp, dp, dp, C.c_int, ip, ip, ip, dp, dp, C.c_int, dp, dp]
+    for kind, a, nc in (("Si", 10.26, (24, 16, 20)), ("Al", 7.65, (12, 12, 12))):
+        L, z, pos = pw.make_crystal(kind, (1, 1, 1), a, 0.02, 9)
+        nf = tuple(2 * n for n in nc)
+        T, _ = pw.build_tables(L, z, pos, nc, nf, seed_v=4)
+        psi = pw.random_orthonormal_psi(T.dm.ntot, 2, 5)
+        npts = np.array([len(at[0].idx) for at in T.pseudo], np.int32)
+        nproj = np.array([len(at) for at in T.pseudo], np.int32)
+        idx = np.concatenate([at[0].idx for at in T.pseudo]).astype(np.int32)
+        beta = np.concatenate([pp.val[:, 0] for at in T.pseudo for pp in at]).astype(np.float64)
+        wgt = np.array([pp.wgt for at in T.pseudo for pp in at], np.float64)
+        h = np.zeros_like(psi)
+        assert lib.ref_add_mult_spinor(np.array(nc, np.int32), np.array(nf, np.int32), np.array(L, np.float64),
+                                       np.ascontiguousarray(T.ekin.ravel()), T.vtot, len(T.pseudo), npts, nproj, idx,
+                                       beta, wgt, 2, np.ascontiguousarray(psi), h) == 0
+        ref = pw.mult_spinor(T, psi)
+        assert np.abs(h - ref).max() / np.abs(ref).max() < 1e-13, (kind, nc)
