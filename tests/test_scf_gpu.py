@@ -137,3 +137,32 @@ def test_scf_si8_full_matches_oracle(solver, mixed):
     assert abs(res["efree"] - g["efree"]) / nat < 1e-6, (res["efree"], g["efree"])
     assert np.abs(eig[:16] - np.array(g["eig"][:16])).max() < 1e-6
     c.close()
+
+
+def _si64_gold(which):
+    p = GOLD / f"si64_scf_{which}.json"
+    if not p.exists():
+        pytest.skip(f"{p.name} missing")
+    return json.loads(p.read_text())
+
+
+@pytest.mark.parametrize("which,mixed", [("plain", False), ("plain", True), ("filter", False), ("filter", True)])
+def test_scf_si64_matches_oracle(which, mixed):
+    """The Si64 configuration (48^3 / 96^3, Ecut 20 Ha, 128 + 32 bands, ChebFSI
+    degree 10) against the oracle's converged FP64 SCF of the same operator:
+    unfiltered (si64_scf_plain.json) and with CheFSI's wavefunction cut-off
+    filter (si64_scf_filter.json); FP64 and mixed precision.  Bars:
+    |E_free - E_oracle| / N_atom < 1e-6 Ha, occupied eigenvalues 1e-6 Ha."""
+    g = _si64_gold(which)
+    L = np.array(g["length"])
+    pos = np.array(g["positions"])
+    c = _ctx(L, g["znuc"], pos, tuple(g["numGrid"]), tuple(g["numGridFine"]))
+    res, eig, rho = c.scf(nocc=g["nocc"], nextra=g["nextra"], ecut=g["ecut"], solver="chebfsi", mixed=mixed,
+                          cheby_degree=10, cheby_first_cycles=5, tol_efree=1e-8, refine_threshold=3e-6,
+                          max_iter=80, graphs=True, wfn_filter=bool(g["wfn_filter"]))
+    assert res["converged"] == 1
+    nat = len(pos)
+    assert abs(res["efree"] - g["efree"]) / nat < 1e-6, (res["efree"], g["efree"])
+    nocc = g["nocc"]
+    assert np.abs(eig[:nocc] - np.array(g["eig"][:nocc])).max() < 1e-6
+    c.close()
