@@ -519,6 +519,24 @@ def gram_bench(device: int, reps: int = 10):
                         "gemm_tensor_frac": (3 * useful / (kern_ms / 1e3) / 1e12 / tpeak) if kern_ms else None,
                         "operand_bytes": 2 * n * K * 4,
                         "hbm_frac_of_operand_reads": 2 * n * K * 4 / (ms / 1e3) / 1e9 / load_peaks()[0]}
+        # the subspace rotation X C (n x n coefficients) on the same tensor cores
+        import ctypes as C
+        from pwdft_develop_b200._lib import check, lib
+        Cm = torch.randn((n, n), dtype=torch.float64, device="cuda", generator=g)
+        Out = torch.empty_like(X)
+        rot = lambda: check(lib.pw_rotate(c.handle, C.c_void_p(X.data_ptr()), K, n, C.c_void_p(Cm.data_ptr()), n,  # noqa
+                                          n, C.c_void_p(Out.data_ptr()), K, 0, None))
+        rot()
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(reps):
+            rot()
+        e1.record()
+        torch.cuda.synchronize()
+        rms = e0.elapsed_time(e1) / reps
+        out[f"n{n}"]["rotation"] = {"call_ms": rms, "useful_tflops": useful / (rms / 1e3) / 1e12,
+                                    "tensor_frac": 3 * useful / (rms / 1e3) / 1e12 / tpeak,
+                                    "hbm_frac_of_in_out": 2 * n * K * 4 / (rms / 1e3) / 1e9 / load_peaks()[0]}
     c.close()
     return out
 
@@ -711,6 +729,9 @@ def summary(line: dict) -> dict:
     if "gram" in line:
         out["gram_n480_tensor_frac"] = line["gram"]["n480"]["tensor_frac"]
         out["gram_n160_tensor_frac"] = line["gram"]["n160"]["tensor_frac"]
+        if "rotation" in line["gram"]["n160"]:
+            out["rotation_n160_ms"] = line["gram"]["n160"]["rotation"]["call_ms"]
+            out["rotation_n480_tensor_frac"] = line["gram"]["n480"]["rotation"]["tensor_frac"]
     if "cpu_baseline" in line:
         cb = line["cpu_baseline"]
         out["cpu_baseline_bands_per_s"] = cb["value"]

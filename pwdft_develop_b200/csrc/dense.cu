@@ -55,7 +55,7 @@ int gram(pw_ctx* c, const void* X, int ldx, int nx, const void* Y, int ldy, int 
   ro.transpose = 1;    // G[j*ldg + i] = sum_g X[i][g] Y[j][g]
   c->launches += 1;   // the reduction kernel; the GEMM is counted by L_
   Launch L_(c, st, KK_GRAM);
-  return gemm_tn_reduce(A, B, nt, c->gemm_terms, c->s_ws, ro, st);
+  return gemm_tn_reduce(A, B, nt, c->gemm_terms, c->s_ws, ro, st, 0, same ? 1 : 0);
 }
 
 }  // namespace pwb

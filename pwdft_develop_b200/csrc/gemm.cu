@@ -152,7 +152,15 @@ struct GemmArgs {
   float* C;              // epi 1: C[m*ldc + n], epi 2: C[n*ldc + m]
   long ldc;
   int accumulate;        // epi 1 / 2: C += tile
+  int sym;               // symmetric product (A = B): only tiles not strictly below the diagonal
+  int ntiles;            // sym: number of those tiles
 };
+
+// tiles of column block nt that are not strictly below the diagonal of a
+// symmetric product (row tile m0 < n0 + BN)
+__host__ __device__ __forceinline__ int sym_tiles_in_col(int nt, int bn, int tilesM) {
+  return min(tilesM, ((nt + 1) * bn + GM - 1) / GM);
+}
 
 __device__ __forceinline__ void mbar_arrive(uint64_t* b) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
@@ -179,7 +187,7 @@ k_gemm_tn(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant__ CU
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int tilesM = (g.M + GM - 1) / GM, tilesN = (g.N + BN - 1) / BN;
-  const int total = tilesM * tilesN * g.nsplit;
+  const int total = (g.sym ? g.ntiles : tilesM * tilesN) * g.nsplit;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < SM::NSTAGE; ++s) {
@@ -205,10 +213,23 @@ k_gemm_tn(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant__ CU
   const uint32_t tmem = *tmem_slot;
 
   auto coords = [&](int t, int& m0, int& n0, int& split, int& kbeg, int& nkb) {
-    const int mt = t % tilesM;
-    const int r = t / tilesM;
-    const int ntl = r % tilesN;
-    split = r / tilesN;
+    int mt, ntl;
+    if (g.sym) {
+      // the upper tiles, column block by column block
+      int idx = t % g.ntiles;
+      split = t / g.ntiles;
+      ntl = 0;
+      for (int c = sym_tiles_in_col(0, BN, tilesM); idx >= c; c = sym_tiles_in_col(ntl, BN, tilesM)) {
+        idx -= c;
+        ++ntl;
+      }
+      mt = idx;
+    } else {
+      mt = t % tilesM;
+      const int r = t / tilesM;
+      ntl = r % tilesN;
+      split = r / tilesN;
+    }
     m0 = mt * GM;
     n0 = ntl * BN;
     kbeg = split * g.kchunk;
@@ -421,12 +442,16 @@ __global__ void k_split_bf16_t(const float* __restrict__ x, long ld_in, int ncol
 // scale, written as double or float, directly or transposed.
 __global__ void k_splitk_reduce(const float* __restrict__ ws, int nsplit, int M, int N, const float* __restrict__ rs,
                                 const float* __restrict__ cs, int transpose, int out_f64, void* out, long ldo,
-                                __nv_bfloat16* bhi, __nv_bfloat16* blo, long ldb) {
+                                __nv_bfloat16* bhi, __nv_bfloat16* blo, long ldb, int sym_bn) {
   const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (i >= (long)M * N) return;
   const int n = (int)(i / M), m = (int)(i - (long)n * M);
+  // symmetric product: an entry of a tile strictly below the diagonal was not
+  // computed; its mirror (n, m) was
+  const bool mirror = sym_bn > 0 && (n / sym_bn) * sym_bn + sym_bn <= (m / GM) * GM;
+  const long src = mirror ? (long)m * M + n : (long)n * M + m;
   double s = 0;
-  for (int k = 0; k < nsplit; ++k) s += (double)ws[((long)k * N + n) * M + m];
+  for (int k = 0; k < nsplit; ++k) s += (double)ws[(long)k * N * M + src];
   if (rs) s *= rs[m];
   if (cs) s *= cs[n];
   const long o = transpose ? (long)n * ldo + m : (long)m * ldo + n;
@@ -499,7 +524,12 @@ template <int BN> static int launch_bn(const SplitOperand& A, const SplitOperand
     return rc;
   GemmArgs ga = g;
   ga.nsplit = nsplit;
-  const long total = (long)((g.M + GM - 1) / GM) * ((g.N + BN - 1) / BN) * nsplit;
+  const int tilesM = (g.M + GM - 1) / GM, tilesN = (g.N + BN - 1) / BN;
+  if (ga.sym) {
+    ga.ntiles = 0;
+    for (int nt = 0; nt < tilesN; ++nt) ga.ntiles += sym_tiles_in_col(nt, BN, tilesM);
+  }
+  const long total = (long)(ga.sym ? ga.ntiles : tilesM * tilesN) * nsplit;
   const int grid = (int)std::min<long>(total, num_sms());
   k_gemm_tn<BN><<<grid, GEMM_THREADS, SM::BYTES, st>>>(ah, al, bh, bl, ga);
   PWB_CUDA(cudaGetLastError());
@@ -575,11 +605,16 @@ int split_bf16_t(const float* x, long ld_in, int ncol, int nrow, void* hi, void*
 }
 
 int gemm_tn_reduce(const SplitOperand& A, const SplitOperand& B, int K, int nterms, DevBuf& ws,
-                   const ReduceOut& out, cudaStream_t st, int bn) {
+                   const ReduceOut& out, cudaStream_t st, int bn, int sym) {
   const int M = A.rows, N = B.rows;
   if (M == 0 || N == 0) return PW_OK;
   const int BN = bn > 0 ? bn : pick_bn(N);
-  const int tiles = ((M + GM - 1) / GM) * ((N + BN - 1) / BN);
+  sym = sym && M == N;
+  int tiles = ((M + GM - 1) / GM) * ((N + BN - 1) / BN);
+  if (sym) {
+    tiles = 0;
+    for (int nt = 0; nt < (N + BN - 1) / BN; ++nt) tiles += sym_tiles_in_col(nt, BN, (M + GM - 1) / GM);
+  }
   // enough CTAs to fill the GPU twice over, each with >= 4 K-blocks
   int nsplit = std::max(1, (2 * num_sms() + tiles - 1) / tiles);
   const int maxsplit = std::max(1, (K + 4 * GK - 1) / (4 * GK));
@@ -597,11 +632,12 @@ int gemm_tn_reduce(const SplitOperand& A, const SplitOperand& B, int K, int nter
   GemmArgs g{};
   g.M = M; g.N = N; g.K = K; g.kchunk = kchunk; g.nterms = nterms; g.epi = 0;
   g.ws = reinterpret_cast<float*>(ws.p);
+  g.sym = sym;
   if ((rc = launch(A, B, g, BN, nsplit, st))) return rc;
   const long tot = (long)M * N;
   k_splitk_reduce<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(
       g.ws, nsplit, M, N, out.row_scale, out.col_scale, out.transpose, out.f64, out.out, out.ldo,
-      (__nv_bfloat16*)out.bf_hi, (__nv_bfloat16*)out.bf_lo, out.ldb);
+      (__nv_bfloat16*)out.bf_hi, (__nv_bfloat16*)out.bf_lo, out.ldb, sym ? BN : 0);
   PWB_CUDA(cudaGetLastError());
   return PW_OK;
 }

@@ -33,8 +33,10 @@ int split_bf16(const float* x, long ld_in, int ncol, int nrow, void* hi, void* l
 int split_bf16_t(const float* x, long ld_in, int ncol, int nrow, void* hi, void* lo, long ld_out, cudaStream_t st);
 // C[m][n] = sum_k A[m][k] B[n][k] with split-K and a deterministic reduction
 // bn: tile width override (0 = heuristic; otherwise one of 32, 64, 96, 128, 160, 192, 256)
+// sym: A and B are the same operand (a symmetric product): only the tiles not
+// strictly below the diagonal are computed, the reduction mirrors the rest
 int gemm_tn_reduce(const SplitOperand& A, const SplitOperand& B, int K, int nterms, DevBuf& ws, const ReduceOut& out,
-                   cudaStream_t st, int bn = 0);
+                   cudaStream_t st, int bn = 0, int sym = 0);
 // C[m*ldc + n] (+)= sum_k A[m][k] B[n][k]  (K small); with transposed = 1
 // the tile is written as C[n*ldc + m] (coalesced when M is the long dimension)
 int gemm_tn_store(const SplitOperand& A, const SplitOperand& B, int K, int nterms, float* C, long ldc, int accumulate,
