@@ -257,69 +257,177 @@ struct FFTPlanRec {
   Complex* cdata;
 };
 typedef FFTPlanRec* fftw_plan;
-static void fft1(Complex* a, int n, int sign) {
-  if (n <= 1) return;
-  int p = 2;
-  while (n % p) ++p;
-  if (p == n) {
-    std::vector<Complex> out(n);
-    for (int k = 0; k < n; ++k) {
-      Complex s(0, 0);
-      for (int j = 0; j < n; ++j) s += a[j] * std::polar(1.0, sign * 2.0 * M_PI * (double)((long)j * k % n) / n);
-      out[k] = s;
+// One length: the radices (4, 2, 3, 5, then any prime) and, per stage, the
+// twiddles w^(j k) of a Stockham autosort pass.
+struct FFTLen {
+  int n = 0;
+  std::vector<int> radix;
+  std::vector<std::vector<Complex>> tw[2];   // [sign > 0][stage][j * r + k]
+  std::vector<std::vector<Complex>> root[2]; // [sign > 0][stage][s * r + k] = exp(sign 2 pi i k s / r)
+  explicit FFTLen(int n_) : n(n_) {
+    int m = n;
+    for (int r : {4, 2, 3, 5})
+      while (m % r == 0) { radix.push_back(r); m /= r; }
+    for (int r = 7; m > 1; r += 2)
+      while (m % r == 0) { radix.push_back(r); m /= r; }
+    for (int sg = 0; sg < 2; ++sg) {
+      const double sign = sg ? 1.0 : -1.0;
+      int l = 1;
+      for (int r : radix) {
+        std::vector<Complex> t((size_t)l * r);
+        for (int j = 0; j < l; ++j)
+          for (int k = 0; k < r; ++k) t[(size_t)j * r + k] = std::polar(1.0, sign * 2.0 * M_PI * j * k / (double)(l * r));
+        tw[sg].push_back(t);
+        std::vector<Complex> rt((size_t)r * r);
+        for (int s2 = 0; s2 < r; ++s2)
+          for (int k = 0; k < r; ++k) rt[(size_t)s2 * r + k] = std::polar(1.0, sign * 2.0 * M_PI * ((k * s2) % r) / (double)r);
+        root[sg].push_back(rt);
+        l *= r;
+      }
     }
-    for (int k = 0; k < n; ++k) a[k] = out[k];
+  }
+};
+// in place, unnormalised, sign -1 forward / +1 backward; work: n scratch values
+static void fft1(const FFTLen& L, Complex* a, Complex* work, int sign) {
+  const int n = L.n;
+  if (n <= 1) return;
+  const int sg = sign > 0 ? 1 : 0;
+  Complex* x = a;
+  Complex* y = work;
+  int l = 1;   // size of the transforms already done
+  for (size_t st = 0; st < L.radix.size(); ++st) {
+    const int r = L.radix[st];
+    const int m = n / (l * r);   // number of interleaved sub-problems left
+    const Complex* w = L.tw[sg][st].data();
+    const Complex* rt = L.root[sg][st].data();
+    if (r == 2) {
+      for (int q = 0; q < m; ++q)
+        for (int j = 0; j < l; ++j) {
+          const Complex v0 = x[(size_t)q * l + j], v1 = x[(size_t)(m + q) * l + j] * w[2 * j + 1];
+          y[(size_t)(2 * q) * l + j] = v0 + v1;
+          y[(size_t)(2 * q + 1) * l + j] = v0 - v1;
+        }
+    } else if (r == 4) {
+      // exp(sign i pi / 2) = sign i
+      const double si = sign > 0 ? 1.0 : -1.0;
+      for (int q = 0; q < m; ++q)
+        for (int j = 0; j < l; ++j) {
+          const Complex v0 = x[(size_t)q * l + j];
+          const Complex v1 = x[(size_t)(m + q) * l + j] * w[4 * j + 1];
+          const Complex v2 = x[(size_t)(2 * m + q) * l + j] * w[4 * j + 2];
+          const Complex v3 = x[(size_t)(3 * m + q) * l + j] * w[4 * j + 3];
+          const Complex s02 = v0 + v2, d02 = v0 - v2, s13 = v1 + v3, d13 = v1 - v3;
+          const Complex id13(-si * d13.imag(), si * d13.real());
+          y[(size_t)(4 * q) * l + j] = s02 + s13;
+          y[(size_t)(4 * q + 1) * l + j] = d02 + id13;
+          y[(size_t)(4 * q + 2) * l + j] = s02 - s13;
+          y[(size_t)(4 * q + 3) * l + j] = d02 - id13;
+        }
+    } else {
+      Complex v[64];
+      for (int q = 0; q < m; ++q)
+        for (int j = 0; j < l; ++j) {
+          v[0] = x[(size_t)q * l + j];
+          for (int k = 1; k < r; ++k) v[k] = x[(size_t)(k * m + q) * l + j] * w[(size_t)j * r + k];
+          for (int s2 = 0; s2 < r; ++s2) {
+            Complex acc = v[0];
+            for (int k = 1; k < r; ++k) acc += v[k] * rt[s2 * r + k];
+            y[(size_t)(q * r + s2) * l + j] = acc;
+          }
+        }
+    }
+    std::swap(x, y);
+    l *= r;
+  }
+  if (x != a)
+    for (int i = 0; i < n; ++i) a[i] = x[i];
+}
+static const FFTLen& fft_len(int n) {
+  static std::vector<FFTLen*> cache;
+  for (FFTLen* f : cache)
+    if (f->n == n) return *f;
+  cache.push_back(new FFTLen(n));
+  return *cache.back();
+}
+// complex 3-D transform of an x-fastest (nx, ny, nz) array along one axis;
+// along y and z, blocks of up to 8 neighbouring x columns are gathered together
+static void fft_axis(Complex* a, int nx, int ny, int nz, int axis, int sign, int xlen) {
+  const int n = axis == 0 ? nx : axis == 1 ? ny : nz;
+  const FFTLen& L = fft_len(n);
+  constexpr int B = 8;
+  std::vector<Complex> lines((size_t)B * n), work(n);
+  const long sy = xlen, sz = (long)xlen * ny;
+  if (axis == 0) {
+    for (int k = 0; k < nz; ++k)
+      for (int j = 0; j < ny; ++j) fft1(L, a + j * sy + k * sz, work.data(), sign);
     return;
   }
-  const int m = n / p;
-  std::vector<std::vector<Complex>> sub(p, std::vector<Complex>(m));
-  for (int r = 0; r < p; ++r)
-    for (int j = 0; j < m; ++j) sub[r][j] = a[j * p + r];
-  for (int r = 0; r < p; ++r) fft1(sub[r].data(), m, sign);
-  for (int k = 0; k < n; ++k) {
-    Complex s(0, 0);
-    for (int r = 0; r < p; ++r) s += sub[r][k % m] * std::polar(1.0, sign * 2.0 * M_PI * (double)((long)r * k % n) / n);
-    a[k] = s;
-  }
+  const long stride = axis == 1 ? sy : sz;
+  const int c1 = axis == 1 ? 1 : ny;
+  const int c2 = axis == 2 ? 1 : nz;
+  for (int k = 0; k < c2; ++k)
+    for (int j = 0; j < c1; ++j)
+      for (int i0 = 0; i0 < nx; i0 += B) {
+        const int nb = std::min(B, nx - i0);
+        Complex* base = a + i0 + j * sy + k * sz;
+        for (int t = 0; t < n; ++t)
+          for (int b = 0; b < nb; ++b) lines[(size_t)b * n + t] = base[t * stride + b];
+        for (int b = 0; b < nb; ++b) fft1(L, lines.data() + (size_t)b * n, work.data(), sign);
+        for (int t = 0; t < n; ++t)
+          for (int b = 0; b < nb; ++b) base[t * stride + b] = lines[(size_t)b * n + t];
+      }
 }
-static void fft3(std::vector<Complex>& a, const int* n, int sign) {
-  std::vector<Complex> line;
-  for (int ax = 0; ax < 3; ++ax) {
-    const long stride = ax == 0 ? 1 : ax == 1 ? n[0] : (long)n[0] * n[1];
-    const int len = n[ax];
-    line.resize(len);
-    const long total = (long)n[0] * n[1] * n[2];
-    for (long base = 0; base < total; ++base) {
-      // base enumerates the lines: skip points that are not the start of a line
-      const long pos = (base / stride) % len;
-      if (pos != 0) continue;
-      for (int t = 0; t < len; ++t) line[t] = a[base + t * stride];
-      fft1(line.data(), len, sign);
-      for (int t = 0; t < len; ++t) a[base + t * stride] = line[t];
-    }
-  }
-}
+// FFTW's r2c / c2r (unnormalised, exp(-i ...) forward), x fastest: x by pairs
+// of real lines packed into one complex line, then y and z on the half spectrum
 static void fftw_execute(fftw_plan p) {
   const int n0 = p->n[0], n1 = p->n[1], n2 = p->n[2], h0 = n0 / 2 + 1;
-  const long N = (long)n0 * n1 * n2;
-  std::vector<Complex> a(N);
+  const FFTLen& Lx = fft_len(n0);
+  std::vector<Complex> line(n0), work(n0);
+  const long nlines = (long)n1 * n2;
+  Complex* H = p->cdata;                           // half spectrum, rows of h0
   if (p->real_to_complex) {
-    for (long i = 0; i < N; ++i) a[i] = Complex(p->rdata[i], 0.0);
-    fft3(a, p->n, -1);
-    for (int k = 0; k < n2; ++k)
-      for (int j = 0; j < n1; ++j)
-        for (int i = 0; i < h0; ++i) p->cdata[(k * (long)n1 + j) * h0 + i] = a[(k * (long)n1 + j) * n0 + i];
+    for (long r = 0; r < nlines; r += 2) {
+      const Real* x0 = p->rdata + r * n0;
+      const Real* x1 = (r + 1 < nlines) ? x0 + n0 : nullptr;
+      for (int t = 0; t < n0; ++t) line[t] = Complex(x0[t], x1 ? x1[t] : 0.0);
+      fft1(Lx, line.data(), work.data(), -1);
+      for (int k = 0; k < h0; ++k) {
+        const Complex a = line[k], b = std::conj(line[(n0 - k) % n0]);
+        H[r * h0 + k] = 0.5 * (a + b);
+        if (x1) H[(r + 1) * h0 + k] = Complex(0.0, -0.5) * (a - b);
+      }
+    }
+    fft_axis(H, h0, n1, n2, 1, -1, h0);
+    fft_axis(H, h0, n1, n2, 2, -1, h0);
   } else {
-    for (int k = 0; k < n2; ++k)
-      for (int j = 0; j < n1; ++j)
-        for (int i = 0; i < n0; ++i) {
-          Complex v;
-          if (i < h0) v = p->cdata[(k * (long)n1 + j) * h0 + i];
-          else v = std::conj(p->cdata[(((n2 - k) % n2) * (long)n1 + (n1 - j) % n1) * h0 + (n0 - i)]);
-          a[(k * (long)n1 + j) * n0 + i] = v;
+    std::vector<Complex> G(H, H + (size_t)h0 * nlines);
+    fft_axis(G.data(), h0, n1, n2, 2, +1, h0);
+    fft_axis(G.data(), h0, n1, n2, 1, +1, h0);
+    for (long r = 0; r < nlines; r += 2) {
+      const bool two = r + 1 < nlines;
+      // a Hermitian-extended line x0 + i x1 from the two half rows
+      for (int k = 0; k < n0; ++k) {
+        Complex a, b;
+        if (k < h0) {
+          a = G[r * h0 + k];
+          b = two ? G[(r + 1) * h0 + k] : Complex(0, 0);
+        } else {
+          a = std::conj(G[r * h0 + (n0 - k)]);
+          b = two ? std::conj(G[(r + 1) * h0 + (n0 - k)]) : Complex(0, 0);
         }
-    fft3(a, p->n, +1);
-    for (long i = 0; i < N; ++i) p->rdata[i] = a[i].real();
+        // c2r reads only the real part of the DC and Nyquist entries
+        if (k == 0 || 2 * k == n0) {
+          a = Complex(a.real(), 0.0);
+          b = Complex(b.real(), 0.0);
+        }
+        line[k] = a + Complex(0.0, 1.0) * b;
+      }
+      fft1(Lx, line.data(), work.data(), +1);
+      for (int t = 0; t < n0; ++t) {
+        p->rdata[r * n0 + t] = line[t].real();
+        if (two) p->rdata[(r + 1) * n0 + t] = line[t].imag();
+      }
+    }
   }
 }
 struct Fourier {
@@ -409,6 +517,62 @@ int ref_add_mult_spinor(const int* n, const int* nf, const double* L, const doub
   }
   return 0;
 }
+// ref_add_mult_spinor with the bands split over nthreads OpenMP threads, one
+// Fourier per thread (the reference's MPI ranks each hold their own)
+int ref_add_mult_spinor_omp(const int* n, const int* nf, const double* L, const double* ekin_r2c, const double* vtot,
+                            int natom, const int* atom_npts, const int* atom_nproj, const int* idx, const double* beta,
+                            const double* wgt, int nb, double* psi, double* a3, int nthreads) {
+  using namespace pwref;
+  int bad = 0;
+  try {
+    Fourier f0;
+    f0.setup(n, nf, L);
+    for (int d = 0; d < 3; ++d) {   // the length tables are built before the threads start
+      fft_len(n[d]);
+      fft_len(nf[d]);
+    }
+    DblNumVec ekin(f0.numGridTotalR2C), vt(f0.domain.NumGridTotalFine());
+    for (Int i = 0; i < f0.numGridTotalR2C; ++i) ekin[i] = ekin_r2c[i];
+    for (Int i = 0; i < f0.domain.NumGridTotalFine(); ++i) vt[i] = vtot[i];
+    std::vector<PseudoPot> pseudo(natom);
+    long io = 0, bo = 0, wo = 0;
+    for (int a = 0; a < natom; ++a) {
+      for (int l = 0; l < atom_nproj[a]; ++l) {
+        SparseVec sv;
+        sv.first = IntNumVec(atom_npts[a]);
+        sv.second = DblNumMat(atom_npts[a], 4);
+        for (int i = 0; i < atom_npts[a]; ++i) {
+          sv.first[i] = idx[io + i];
+          sv.second.VecData(VAL)[i] = beta[bo + (long)l * atom_npts[a] + i];
+        }
+        pseudo[a].vnlList.push_back(std::make_pair(sv, wgt[wo + l]));
+      }
+      io += atom_npts[a];
+      bo += (long)atom_nproj[a] * atom_npts[a];
+      wo += atom_nproj[a];
+    }
+    const long ntot = f0.domain.NumGridTotal();
+#pragma omp parallel num_threads(nthreads)
+    {
+      Fourier fft;   // per thread, reused over its bands
+      fft.setup(n, nf, L);
+#pragma omp for schedule(dynamic, 1)
+      for (int b = 0; b < nb; ++b) {
+        try {
+          Spinor sp(fft.domain, psi + b * ntot, 1);
+          NumTns<Real> out(ntot, 1, 1, a3 + b * ntot);
+          sp.AddMultSpinorFineR2C(fft, ekin, vt, pseudo, out);
+        } catch (...) {
+#pragma omp atomic write
+          bad = 1;
+        }
+      }
+    }
+  } catch (...) {
+    return -1;
+  }
+  return bad ? -1 : 0;
+}
 // a3 += C2R(teter * R2C(r)) for nb bands
 int ref_add_teter(const int* n, const int* nf, const double* L, const double* teter_r2c, int nb, double* r,
                   double* a3) {
@@ -446,8 +610,8 @@ def build_hpsi(ref_root: Path = DEFAULT_REF) -> Path | None:
     OUT.mkdir(exist_ok=True)
     cpp = OUT / "ref_hpsi.cpp"
     cpp.write_text(HPSI_HARNESS + "\n\n".join(parts) + HPSI_WRAPPERS)
-    r = subprocess.run(["g++", "-O2", "-fPIC", "-shared", "-o", str(LIB_HPSI), str(cpp)], capture_output=True,
-                       text=True)
+    r = subprocess.run(["g++", "-O3", "-march=x86-64-v2", "-fcx-limited-range", "-fopenmp", "-fPIC", "-shared", "-o", str(LIB_HPSI), str(cpp)],
+                       capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(r.stderr)
     return LIB_HPSI

@@ -389,3 +389,36 @@ def test_oracle_hpsi_against_compiled_reference_other_grids():
                                        beta, wgt, 2, np.ascontiguousarray(psi), h) == 0
         ref = pw.mult_spinor(T, psi)
         assert np.abs(h - ref).max() / np.abs(ref).max() < 1e-13, (kind, nc)
+
+
+def test_compiled_reference_threaded_sweep_matches_restatement():
+    """The multi-threaded form of the compiled composition (bands spread over
+    OpenMP threads, one Fourier per thread) that the CPU baseline times: every
+    band against the restatement, 1e-13."""
+    import ctypes as C
+
+    from oracle import build_ref
+    lib_path = build_ref.LIB_HPSI
+    if not lib_path.exists():
+        pytest.skip("reference composition not built here (oracle/_ref)")
+    lib = C.CDLL(str(lib_path))
+    dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+    ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+    lib.ref_add_mult_spinor_omp.argtypes = [ip, ip, dp, dp, dp, C.c_int, ip, ip, ip, dp, dp, C.c_int, dp, dp,
+                                            C.c_int]
+    nc = (16, 16, 16)
+    nf = (32, 32, 32)
+    L, z, pos = pw.make_crystal("Si", (1, 1, 1), 10.26, 0.02, 21)
+    T, _ = pw.build_tables(L, z, pos, nc, nf, seed_v=22)
+    psi = pw.random_orthonormal_psi(T.dm.ntot, 7, 23)
+    npts = np.array([len(at[0].idx) for at in T.pseudo], np.int32)
+    nproj = np.array([len(at) for at in T.pseudo], np.int32)
+    idx = np.concatenate([at[0].idx for at in T.pseudo]).astype(np.int32)
+    beta = np.concatenate([pp.val[:, 0] for at in T.pseudo for pp in at]).astype(np.float64)
+    wgt = np.array([pp.wgt for at in T.pseudo for pp in at], np.float64)
+    h = np.zeros_like(psi)
+    assert lib.ref_add_mult_spinor_omp(np.array(nc, np.int32), np.array(nf, np.int32), np.array(L, np.float64),
+                                       np.ascontiguousarray(T.ekin.ravel()), T.vtot, len(T.pseudo), npts, nproj, idx,
+                                       beta, wgt, 7, np.ascontiguousarray(psi), h, 3) == 0
+    ref = pw.mult_spinor(T, psi)
+    assert np.abs(h - ref).max() / np.abs(ref).max() < 1e-13
