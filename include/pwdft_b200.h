@@ -86,9 +86,9 @@ PW_API int pw_set_nonlocal(pw_ctx* ctx, int natom, const int* atom_npts, const i
 /* Select the nonlocal apply mode (call before pw_set_nonlocal / pw_set_atoms). */
 PW_API int pw_set_nonlocal_mode(pw_ctx* ctx, int mode);
 
-/* GEMM engine for FP32 contexts: mode 0 = split-BF16 tcgen05 kernels with
- * `terms` products per k-step (3: hi*hi + hi*lo + lo*hi, 4: + lo*lo),
- * mode 1 = vendor SGEMM.  FP64 contexts always use FP64 GEMMs. */
+/* GEMM settings for FP32 contexts: mode must be 0 (the split-BF16 tcgen05
+ * kernels), with `terms` products per k-step (3: hi*hi + hi*lo + lo*hi,
+ * 4: + lo*lo); any other mode is PW_EINVAL.  FP64 contexts use FP64 GEMMs. */
 PW_API int pw_set_gemm_mode(pw_ctx* ctx, int mode, int terms);
 /* When enabled, every H*psi call synchronises and returns PW_ETIMEOUT if a
  * bounded device-side pipeline wait gave up (default off). */

@@ -294,7 +294,11 @@ def _ctx_gram(self, X, Y=None, stream=None):
 
 
 def _ctx_set_gemm_mode(self, mode: str = "tc", terms: int = 3):
-    check(lib.pw_set_gemm_mode(self._h, 0 if mode == "tc" else 1, int(terms)))
+    """Split-BF16 tensor-core GEMMs with 3 or 4 products per k-step ("tc" is
+    the only engine)."""
+    if mode != "tc":
+        raise ValueError("the split-BF16 tensor-core GEMM is the only engine")
+    check(lib.pw_set_gemm_mode(self._h, 0, int(terms)))
 
 
 def _ctx_set_check_errors(self, on: bool = True):

@@ -133,7 +133,7 @@ int pw_autotune(pw_ctx* ctx, int nband, pw_tune_result* res) {
     if (t < 0.97 * best) { best = t; best_var = 1; }
     ctx->fft_variant = best_var;
   }
-  if (ctx->prec == PW_F32 && ctx->have_nl && ctx->nl_mode == PW_NL_DENSE && ctx->gemm_mode == 0) {
+  if (ctx->prec == PW_F32 && ctx->have_nl && ctx->nl_mode == PW_NL_DENSE) {
     for (int bn : {64, 96, 128, 160, 256}) {
       double t;
       if ((rc = run(best_bb, bn, 0, &t))) return rc;

@@ -646,22 +646,8 @@ int rotate(pw_ctx* c, int n, int m, const RotBlock* blocks, int nblk, void* out,
         k_rot_f64<float><<<grid, 256, 0, st>>>(n, m, B.k, (const float*)B.X, B.ldx, B.C, B.ldc, (float*)out, ldo,
                                                acc);
       PWB_CUDA(cudaGetLastError());
-    } else if (c->gemm_mode == 0) {
-      if ((rc = rotate_tc(c, n, m, B, (float*)out, ldo, acc, st))) return rc;
     } else {
-      // vendor SGEMM comparator mode (pw_set_gemm_mode 1): the FP64 block rounded to FP32
-      cublasHandle_t h = (cublasHandle_t)c->blas;
-      cublasSetStream(h, st);
-      c->lib_launches++;
-      if ((rc = c->s_rot.alloc((size_t)B.k * m * 4))) return rc;
-      float* Cf = (float*)c->s_rot.p;
-      if ((rc = copy_d2f_2d(B.k, m, B.C, B.ldc, Cf, B.k, st))) return rc;
-      const float one = 1.0f, bf = (float)acc;
-      if (cublasSgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, m, B.k, &one, (const float*)B.X, (int)B.ldx, Cf, B.k, &bf,
-                      (float*)out, (int)ldo) != CUBLAS_STATUS_SUCCESS) {
-        set_error("rotation GEMM failed");
-        return PW_ECUDA;
-      }
+      if ((rc = rotate_tc(c, n, m, B, (float*)out, ldo, acc, st))) return rc;
     }
   }
   return PW_OK;

@@ -123,7 +123,6 @@ struct pw_ctx {
   void* blas = nullptr;          // cublasHandle_t
   // FP32 contexts: bf16 hi/lo copies of Q ([l][g]) and Q^T ([g][l], rows padded
   // to nproj_pad) for the split-BF16 tensor-core GEMMs
-  int gemm_mode = 0;             // 0 tensor-core split-BF16, 1 vendor SGEMM
   int gemm_terms = 3;            // split products per k-step (3 or 4)
   int gemm_bn = 0, gemm_bn_store = 0;   // projector GEMM tile widths (0: heuristic; set by pw_autotune)
   int fft_variant = 0;           // radix decomposition of the fine-plane transforms (0 / 1; set by pw_autotune)

@@ -307,8 +307,7 @@ int pw_set_nonlocal_mode(pw_ctx* ctx, int mode) {
 }
 
 int pw_set_gemm_mode(pw_ctx* ctx, int mode, int terms) {
-  PWB_CHECK(ctx && (mode == 0 || mode == 1) && (terms == 3 || terms == 4), PW_EINVAL, "bad GEMM mode");
-  ctx->gemm_mode = mode;
+  PWB_CHECK(ctx && mode == 0 && (terms == 3 || terms == 4), PW_EINVAL, "bad GEMM mode");
   ctx->gemm_terms = terms;
   return PW_OK;
 }

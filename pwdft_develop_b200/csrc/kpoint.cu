@@ -67,7 +67,7 @@ int build_kq_bf(pw_ctx* c, const void* Qk, void* dst) {
   return PW_OK;
 }
 
-static bool kq_tensor_cores(const pw_ctx* c) { return c->prec == PW_F32 && c->gemm_mode == 0 && c->nproj > 0; }
+static bool kq_tensor_cores(const pw_ctx* c) { return c->prec == PW_F32 && c->nproj > 0; }
 
 int run_hpsi_k(pw_ctx* c, const void* psi, int ld, void* out, int ldo, int band0, int nb, int acc, cudaStream_t st);
 int run_hpsi_kbatch(pw_ctx* c, const void* psi, int ld, void* out, int ldo, int f0, int nf, int acc, cudaStream_t st,

@@ -1589,8 +1589,8 @@ struct Plan {
   static int dense_apply(pw_ctx* c, const DenseSet& ds, const T* psi, int ld, T* out, int ldo, int nb,
                          cudaStream_t st) {
     if constexpr (std::is_same<T, float>::value) {
-      if (c->gemm_mode == 0) return dense_apply_tc(c, ds, psi, ld, out, ldo, nb, st);
-    }
+      return dense_apply_tc(c, ds, psi, ld, out, ldo, nb, st);
+    } else {
     cublasHandle_t h = (cublasHandle_t)c->blas;
     if (cublasSetStream(h, st) != CUBLAS_STATUS_SUCCESS) { set_error("cublasSetStream failed"); return PW_ECUDA; }
     const int np = ds.np, nt = (int)c->ntot;
@@ -1601,22 +1601,17 @@ struct Plan {
     const T one = 1, zero = 0;
     cublasStatus_t r;
     { Launch L_(c, st, KK_LIBGEMM);
-    if constexpr (std::is_same<T, double>::value)
-      r = cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, np, nb, nt, &one, Q, nt, psi, ld, &zero, W, np);
-    else
-      r = cublasSgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, np, nb, nt, &one, Q, nt, psi, ld, &zero, W, np); }
+      r = cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, np, nb, nt, &one, Q, nt, psi, ld, &zero, W, np); }
     if (r != CUBLAS_STATUS_SUCCESS) { set_error("projector GEMM (Q^T psi) failed"); return PW_ECUDA; }
     { Launch L_(c, st, KK_MISC);
     k_scale_rows<T><<<(unsigned)(((long)np * nb + 255) / 256), 256, 0, st>>>(W, reinterpret_cast<const T*>(ds.qd), np, nb); }
     const T* Qs = reinterpret_cast<const T*>(ds.q_st ? ds.q_st : ds.q);
     { Launch L_(c, st, KK_LIBGEMM);
-    if constexpr (std::is_same<T, double>::value)
-      r = cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, nt, nb, np, &one, Qs, nt, W, np, &one, out, ldo);
-    else
-      r = cublasSgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, nt, nb, np, &one, Qs, nt, W, np, &one, out, ldo); }
+      r = cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, nt, nb, np, &one, Qs, nt, W, np, &one, out, ldo); }
     if (r != CUBLAS_STATUS_SUCCESS) { set_error("projector GEMM (Q W) failed"); return PW_ECUDA; }
     PWB_CUDA(cudaGetLastError());
     return PW_OK;
+    }
   }
 
   // rho += sum over the batch's bands of w_b |psi_b,fine|^2 (unnormalised)
@@ -1770,9 +1765,9 @@ struct Plan {
                   cudaStream_t st) {
     int rc;
     if constexpr (std::is_same<T, float>::value) {
-      if (qbf && c->gemm_mode == 0)
-        return nl_k_tc(c, qbf, reinterpret_cast<const float*>(x), ld, reinterpret_cast<float*>(y), ldo, nb, st);
-    }
+      if (!qbf) { set_error("k-point projector bf16 copies missing"); return PW_ENOTREADY; }
+      return nl_k_tc(c, qbf, reinterpret_cast<const float*>(x), ld, reinterpret_cast<float*>(y), ldo, nb, st);
+    } else {
     cublasHandle_t h = (cublasHandle_t)c->blas;
     if (cublasSetStream(h, st) != CUBLAS_STATUS_SUCCESS) { set_error("cublasSetStream failed"); return PW_ECUDA; }
     const int np = c->nproj, nt = (int)c->ntot;
@@ -1780,32 +1775,21 @@ struct Plan {
     V* W = reinterpret_cast<V*>(c->s_wq.p);
     cublasStatus_t r;
     { Launch L_(c, st, KK_LIBGEMM);
-    if constexpr (std::is_same<T, double>::value) {
       const cuDoubleComplex one = make_cuDoubleComplex(1, 0), zero = make_cuDoubleComplex(0, 0);
       r = cublasZgemm(h, CUBLAS_OP_C, CUBLAS_OP_N, np, nb, nt, &one, (const cuDoubleComplex*)Q, nt,
-                      (const cuDoubleComplex*)x, ld, &zero, (cuDoubleComplex*)W, np);
-    } else {
-      const cuComplex one = make_cuComplex(1, 0), zero = make_cuComplex(0, 0);
-      r = cublasCgemm(h, CUBLAS_OP_C, CUBLAS_OP_N, np, nb, nt, &one, (const cuComplex*)Q, nt, (const cuComplex*)x, ld,
-                      &zero, (cuComplex*)W, np);
-    } }
+                      (const cuDoubleComplex*)x, ld, &zero, (cuDoubleComplex*)W, np); }
     if (r != CUBLAS_STATUS_SUCCESS) { set_error("projector GEMM (Q^H psi) failed"); return PW_ECUDA; }
     { Launch L_(c, st, KK_MISC);
     k_scale_rows_c<T><<<(unsigned)(((long)np * nb + 255) / 256), 256, 0, st>>>(W, reinterpret_cast<const T*>(c->qdk.p),
                                                                                 np, nb); }
     { Launch L_(c, st, KK_LIBGEMM);
-    if constexpr (std::is_same<T, double>::value) {
       const cuDoubleComplex one = make_cuDoubleComplex(1, 0);
       r = cublasZgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, nt, nb, np, &one, (const cuDoubleComplex*)Q, nt,
-                      (const cuDoubleComplex*)W, np, &one, (cuDoubleComplex*)y, ldo);
-    } else {
-      const cuComplex one = make_cuComplex(1, 0);
-      r = cublasCgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, nt, nb, np, &one, (const cuComplex*)Q, nt, (const cuComplex*)W, np,
-                      &one, (cuComplex*)y, ldo);
-    } }
+                      (const cuDoubleComplex*)W, np, &one, (cuDoubleComplex*)y, ldo); }
     if (r != CUBLAS_STATUS_SUCCESS) { set_error("projector GEMM (Q W) failed"); return PW_ECUDA; }
     PWB_CUDA(cudaGetLastError());
     return PW_OK;
+    }
   }
 
   // complex coarse projectors at Bloch vector k: q_l = T(conj(e^{i k.d}) beta_l),
