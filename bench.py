@@ -870,7 +870,8 @@ def run_ours(args):
     if args.autotune:
         tune = ctx.autotune(NBAND)      # set-up (untimed): band batch and projector GEMM tiles
     else:
-        tune = {"band_batch": NBAND, "gemm_bn": 0, "gemm_bn_store": 0, "fft_variant": 0}
+        tune = {"band_batch": NBAND, "gemm_bn": 0, "gemm_bn_store": 0, "fft_variant": args.fft_variant}
+        ctx.set_fft_variant(args.fft_variant)
     dt_t = ctx.torch_dtype
     g = torch.Generator(device="cuda").manual_seed(SEED + rank)
     X = torch.randn((NBAND, ctx.ntot), dtype=torch.float64, device="cuda", generator=g)
@@ -1035,6 +1036,8 @@ def main():
     ap.add_argument("--cpu-bands", type=int, default=4, help="CPU baseline: bands per host core")
     ap.add_argument("--ref-bands-per-core", type=int, default=4, help="reference arm: bands per core per step")
     ap.add_argument("--bands", type=int, default=NBAND, help="band block size (profiling runs use a small block)")
+    ap.add_argument("--fft-variant", type=int, default=2, choices=[0, 1, 2],
+                    help="fine-plane transform form when the autotuner is off (pw_set_fft_variant)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

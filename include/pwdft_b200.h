@@ -216,8 +216,9 @@ PW_API int pw_dense_trtri(pw_ctx* ctx, int n, const double* U, int ldu, double* 
 /* Symmetric eigen-decomposition (lapack::Syevd('V', 'U'), the Rayleigh-Ritz
  * solves of src/EigenSolver/lobpcg.cpp and eigensolver.cpp:133-299): the upper
  * triangle of A is read, A's columns receive the eigenvectors, w (device) the
- * eigenvalues ascending.  Cyclic Jacobi; sweeps (host, may be NULL) reports
- * the sweeps it took. */
+ * eigenvalues ascending.  Up to n = 160: Householder tridiagonalisation,
+ * multisection on Sturm counts and inverse iteration (sweeps = 0); beyond:
+ * cyclic Jacobi, and sweeps (host, may be NULL) reports the sweeps it took. */
 PW_API int pw_dense_syev(pw_ctx* ctx, int n, double* A, int lda, double* w, int* sweeps);
 /* EigenSolver::SolveGenEig (src/EigenSolver/eigensolver.cpp:133-299, serial
  * path): symmetrise A and B from their upper triangles, eig(B) = U sigma U^T,
@@ -392,11 +393,15 @@ typedef struct pw_tune_result {
   int cached;               /* 1: taken from the cache */
   double ms_default;        /* sweep time with the defaults */
   double ms_best;           /* sweep time with the chosen setting */
-  int fft_variant;          /* radix decomposition of the fused fine-plane transforms (0: default, 1: second) */
+  int fft_variant;          /* fused fine-plane transforms: 0 table twiddles, 1 second radix split, 2 (default) register twiddles */
 } pw_tune_result;
-/* Select the radix decomposition of the fused fine-plane transforms directly
- * (0: the default N = n1 x n2 of each length, 1: the second one, e.g. 96 =
- * 12 x 8 instead of 8 x 12); pw_autotune times both.  No reference counterpart. */
+/* Select the form of the fused fine-plane transforms directly (0: the first
+ * radix decomposition N = n1 x n2 of each length with the inter-stage
+ * twiddles read from shared-memory tables, 1: the second decomposition, e.g.
+ * 96 = 12 x 8 instead of 8 x 12, 2 (the default): the first decomposition
+ * with the twiddles of a transform formed in registers from one table entry
+ * and the local potential read in the row pass's lane order); pw_autotune
+ * times all three.  No reference counterpart. */
 PW_API int pw_set_fft_variant(pw_ctx* ctx, int variant);
 PW_API int pw_autotune(pw_ctx* ctx, int nband, pw_tune_result* result);
 

@@ -1,6 +1,7 @@
 // Autotuner for the H*psi sweep: times pw_hpsi on a scratch block (L2
-// flushed before each timed sweep) for candidate band-batch widths, the two
-// radix decompositions of the fused fine-plane transforms and, for FP32
+// flushed before each timed sweep) for candidate band-batch widths, the three
+// forms of the fused fine-plane transforms (two radix decompositions, and
+// register-formed twiddles) and, for FP32
 // contexts with projectors, the tile widths of the two projector GEMMs
 // (coordinate descent; a candidate must beat the current best by 3%), keeps
 // the fastest setting in the context and caches it per (grid, precision,
@@ -108,7 +109,7 @@ int pw_autotune(pw_ctx* ctx, int nband, pw_tune_result* res) {
     *ms = best;
     return PW_OK;
   };
-  ctx->fft_variant = 0;
+  ctx->fft_variant = 2;
   double t_def = 0;
   if ((rc = run(nband, 0, 0, &t_def))) return rc;
   int best_bb = nband, best_bn = 0, best_bns = 0;
@@ -123,14 +124,16 @@ int pw_autotune(pw_ctx* ctx, int nband, pw_tune_result* res) {
     if ((rc = run(bb, 0, 0, &t))) return rc;
     if (t < 0.97 * best) { best = t; best_bb = bb; }
   }
-  // the second radix decomposition of the fine-plane transforms (dense
-  // projector mode: the fused fine-plane kernel)
-  int best_var = 0;
+  // the other forms of the fine-plane transforms (dense projector mode: the
+  // fused fine-plane kernel)
+  int best_var = 2;
   if (ctx->nl_mode == PW_NL_DENSE && !ctx->gs) {
-    ctx->fft_variant = 1;
-    double t;
-    if ((rc = run(best_bb, 0, 0, &t))) return rc;
-    if (t < 0.97 * best) { best = t; best_var = 1; }
+    for (int var : {0, 1}) {
+      ctx->fft_variant = var;
+      double t;
+      if ((rc = run(best_bb, 0, 0, &t))) return rc;
+      if (t < 0.97 * best) { best = t; best_var = var; }
+    }
     ctx->fft_variant = best_var;
   }
   if (ctx->prec == PW_F32 && ctx->have_nl && ctx->nl_mode == PW_NL_DENSE) {

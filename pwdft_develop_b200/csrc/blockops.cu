@@ -659,10 +659,11 @@ int Dense::init(cublasHandle_t b) {
 }
 void Dense::release() {}
 
-// eigenvectors (in A) and ascending eigenvalues by the library's Jacobi
-// kernel (smalldense.cu)
+// eigenvectors (in A) and ascending eigenvalues by the library's kernels
+// (smalldense.cu): tridiagonal reduction, multisection and inverse iteration
+// up to n = 160, cyclic Jacobi beyond
 int Dense::syevd(int n, double* A, int lda, double* w, cudaStream_t st) {
-  return dense_syevj(n, A, lda, w, work, nullptr, st);
+  return dense_syevh(n, A, lda, w, work, st);
 }
 
 int Dense::potrf_upper(int n, double* A, int lda, cudaStream_t st) {

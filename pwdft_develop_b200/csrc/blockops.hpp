@@ -88,6 +88,10 @@ int dense_trtri_upper(int n, const double* U, int ldu, double* Ui, int ldi, cuda
 int dense_gemm(int ta, int tb, int m, int n, int k, const double* A, int lda, const double* B, int ldb, double* C,
                int ldc, cudaStream_t st);
 int dense_syevj(int n, double* A, int lda, double* w, DevBuf& ws, int* sweeps_dev, cudaStream_t st);
+// the same result through the tridiagonal form (Householder reduction,
+// multisection on Sturm counts, inverse iteration) for n <= 160; larger n
+// fall back to dense_syevj
+int dense_syevh(int n, double* A, int lda, double* w, DevBuf& ws, cudaStream_t st);
 
 // n x n column-major blocks on the device, queued on st: lower part from the
 // upper triangle, strict lower part zeroed, identity

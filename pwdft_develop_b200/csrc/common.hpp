@@ -109,6 +109,8 @@ struct pw_ctx {
   pwb::DevBuf ekin;             // T [n2][n1][n0]  |G|^2/2 on the full coarse spectrum
   pwb::DevBuf teter;            // T [n2][n1][n0]
   pwb::DevBuf vtot;             // T [N_fine]
+  pwb::DevBuf vperm;            // T: vtot in the lane order of the fused fine-plane kernel's
+                                //    row pass (fft_variant 2), rebuilt whenever vtot is written
   pwb::DevBuf tw[6];            // complex T twiddles for n0,n1,n2,nf0,nf1,nf2
   bool have_vtot = false;
   bool have_nl = false;
@@ -125,7 +127,7 @@ struct pw_ctx {
   // to nproj_pad) for the split-BF16 tensor-core GEMMs
   int gemm_terms = 3;            // split products per k-step (3 or 4)
   int gemm_bn = 0, gemm_bn_store = 0;   // projector GEMM tile widths (0: heuristic; set by pw_autotune)
-  int fft_variant = 0;           // radix decomposition of the fine-plane transforms (0 / 1; set by pw_autotune)
+  int fft_variant = 2;           // form of the fused fine-plane transforms (0 / 1 / 2; set by pw_autotune)
   bool check_errors = false;     // read the device error flag after each call (synchronises)
   pw_ctx* twin = nullptr;        // FP32 twin of an FP64 context (mixed-precision SCF), owned
   int nproj_pad = 0;

@@ -10,6 +10,7 @@
 #include "common.hpp"
 #include "fft.cuh"
 #include "gemm.hpp"
+#include "grid_registry.hpp"
 
 namespace pwb {
 
@@ -36,8 +37,6 @@ void DevBuf::release() {
 }
 
 // defined in hpsi.cu
-struct GridEntry;
-const GridEntry* find_grid(const int n[3]);
 int grid_chunk_rows(const int n[3], int prec);
 int run_hpsi(pw_ctx* c, const void* psi, int ld, void* out, int ldo, int nband, int band0, int npair, int acc,
              cudaStream_t st);
@@ -57,6 +56,18 @@ int upload_real(pw_ctx* c, DevBuf& dst, const double* src, size_t n) {
     for (size_t i = 0; i < n; ++i) tmp[i] = (float)src[i];
     PWB_CUDA(cudaMemcpy(dst.p, tmp.data(), n * 4, cudaMemcpyHostToDevice));
   }
+  return PW_OK;
+}
+
+// the fine-plane kernel's permuted copy of vtot, rebuilt after every write of
+// vtot (on the legacy stream, finished before returning, so that streams and
+// graph replays that read it afterwards see the new potential)
+int refresh_vperm(pw_ctx* c) {
+  const GridEntry* g = find_grid(c->n);
+  if (!g || !c->vtot.p) return PW_OK;
+  int rc = g->vperm[c->prec == PW_F32 ? 1 : 0](c, nullptr);
+  if (rc) return rc;
+  PWB_CUDA(cudaStreamSynchronize(nullptr));
   return PW_OK;
 }
 
@@ -293,7 +304,7 @@ int pw_set_vtot(pw_ctx* ctx, const double* vtot) {
   PWB_CHECK(ctx && vtot, PW_EINVAL, "null argument");
   PWB_CUDA(cudaSetDevice(ctx->device));
   int rc = upload_real(ctx, ctx->vtot, vtot, ctx->ntotf);
-  if (rc) return rc;
+  if (rc || (rc = refresh_vperm(ctx))) return rc;
   ctx->h_vtot.assign(vtot, vtot + ctx->ntotf);
   ctx->have_vtot = true;
   return PW_OK;
@@ -530,7 +541,7 @@ int pw_hpsi(pw_ctx* ctx, const void* psi, int ld, void* hpsi, int ldh, int nband
 }
 
 int pw_set_fft_variant(pw_ctx* ctx, int variant) {
-  PWB_CHECK(ctx && (variant == 0 || variant == 1), PW_EINVAL, "FFT variant must be 0 or 1");
+  PWB_CHECK(ctx && variant >= 0 && variant <= 2, PW_EINVAL, "FFT variant must be 0, 1 or 2");
   ctx->fft_variant = variant;
   return PW_OK;
 }

@@ -62,6 +62,21 @@ template <int R, int M, int DIR, typename V> __device__ __forceinline__ V twmul(
   }
 }
 
+// p[k] = w^k for k = 1 .. R-1 (even k: the square of w^{k/2}, odd k: w^{k-1} w),
+// each power at most about 2 log2(R) rounded products from w
+template <int R, typename V> __device__ __forceinline__ void twiddle_powers(V w, V* p) {
+  p[1] = w;
+  sfor<2, R>([&](auto kI) {
+    constexpr int k = decltype(kI)::value;
+    if constexpr (k % 2 == 0) {
+      const V h = p[k / 2];
+      p[k] = mkc<V>(h.x * h.x - h.y * h.y, (h.x + h.x) * h.y);
+    } else {
+      p[k] = cmul(p[k - 1], w);
+    }
+  });
+}
+
 template <int R> struct FirstFactor {
   static constexpr int v = (R % 4 == 0 && R != 4) ? 4
                          : (R % 2 == 0 && R != 2) ? 2
@@ -292,7 +307,7 @@ template <int N> struct SplitAlt { static constexpr int n1 = Split<N>::n1; };
 PWB_SPLIT_ALT(48, 8) PWB_SPLIT_ALT(60, 10) PWB_SPLIT_ALT(64, 16) PWB_SPLIT_ALT(72, 12) PWB_SPLIT_ALT(80, 10)
 PWB_SPLIT_ALT(96, 12) PWB_SPLIT_ALT(120, 12) PWB_SPLIT_ALT(128, 16) PWB_SPLIT_ALT(144, 16)
 #undef PWB_SPLIT_ALT
-template <int N, int VAR> struct SplitVar { static constexpr int n1 = VAR ? SplitAlt<N>::n1 : Split<N>::n1; };
+template <int N, int VAR> struct SplitVar { static constexpr int n1 = VAR == 1 ? SplitAlt<N>::n1 : Split<N>::n1; };
 
 // Number of transforms one warp processes together for length N.
 template <int N> struct FftGroup {

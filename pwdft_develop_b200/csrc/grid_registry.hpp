@@ -19,6 +19,7 @@ using ExxFn = int (*)(pw_ctx*, const void*, int, int, void*, int, int, cudaStrea
 using HpsiKFn = int (*)(pw_ctx*, const void*, int, void*, int, int, int, int, cudaStream_t);
 using HpsiKBFn = int (*)(pw_ctx*, const void*, int, void*, int, int, int, int, cudaStream_t, int, const void*,
                          const void*);
+using VpermFn = int (*)(pw_ctx*, cudaStream_t);
 using BuildQKFn = int (*)(pw_ctx*, const int*, const double*, const double*, const long*, const long*, const int*, int,
                           const double*, void*, cudaStream_t);
 
@@ -37,6 +38,7 @@ struct GridEntry {
   HpsiKBFn hpsikb[2];
   HpsiFn hpsigs[2];     // sphere-cut (G-space) contexts whose G-space grid is twice this grid
   DensFn densgs[2];
+  VpermFn vperm[2];     // rebuild pw_ctx::vperm from pw_ctx::vtot
 };
 
 void register_grid(const GridEntry& e);

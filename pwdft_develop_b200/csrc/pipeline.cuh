@@ -694,19 +694,55 @@ template <int NXF> struct FlocLayoutPlain {
   static constexpr bool FA = false, FB = false;
 };
 template <typename T, int NXF, int NYF, int VAR>
-using FlocLayoutVar = typename std::conditional<VAR == 0, FlocLayout<T, NXF, NYF>, FlocLayoutPlain<NXF>>::type;
+using FlocLayoutVar = typename std::conditional<VAR == 1, FlocLayoutPlain<NXF>, FlocLayout<T, NXF, NYF>>::type;
+
+// Lane order of the local potential for the row pass of k_floc2 (fft_variant
+// 2): lane f NX1 + k1 of a warp holds row r0 + f (rows in groups of FX) and
+// needs V(x = k1 + NX1 k2) for k2 = 0 .. NX2-1.  The permuted copy stores, per
+// fine plane and row group, NQ blocks of 32 lanes x VW consecutive k2 values,
+// so each vector load of a warp reads 32 VW contiguous reals.  Unused lanes
+// (rows past the plane, lanes past FX NX1) hold zeros.
+template <typename T, int NXF, int NYF> struct VpermLayout {
+  static constexpr int NX1 = Split<NXF>::n1, NX2 = NXF / NX1, FX = 32 / NX1;
+  static constexpr int VW = 16 / (int)sizeof(T);                // reals per 16-byte load
+  static constexpr bool OK = NX2 % VW == 0;
+  static constexpr int NQ = NX2 / VW, NG = (NYF + FX - 1) / FX;
+  static constexpr long PLANE = (long)NG * NQ * 32 * VW;        // reals per fine plane
+};
+template <typename T, int NXF, int NYF>
+__global__ void k_vperm(const T* __restrict__ v, T* __restrict__ vp, int nzf) {
+  using LY = VpermLayout<T, NXF, NYF>;
+  const long total = LY::PLANE * nzf;
+  for (long o = blockIdx.x * (long)blockDim.x + threadIdx.x; o < total; o += (long)gridDim.x * blockDim.x) {
+    const long zf = o / LY::PLANE;
+    long r = o - zf * LY::PLANE;
+    const int i = (int)(r % LY::VW);
+    r /= LY::VW;
+    const int lane = (int)(r % 32);
+    r /= 32;
+    const int q = (int)(r % LY::NQ);
+    const int g = (int)(r / LY::NQ);
+    const int f = lane / LY::NX1, k1 = lane - f * LY::NX1;
+    const int y = g * LY::FX + f, x = k1 + LY::NX1 * (q * LY::VW + i);
+    vp[o] = (f < LY::FX && y < NYF) ? v[(zf * NYF + y) * NXF + x] : (T)0;
+  }
+}
 
 // VAR selects the radix decomposition of the x and y transforms (0: Split,
-// 1: SplitAlt), the autotuner's FFT candidate
+// 1: SplitAlt) and where the inter-stage twiddles come from (0, 1: the shared
+// tables; 2: Split with W^{j k} formed in registers from one table entry per
+// transform), the autotuner's FFT candidates
 template <typename T, int NXF, int NYF, int VAR = 0>
 __global__ void __launch_bounds__(FLOC_THREADS, sizeof(T) == 4 ? 3 : 1)
-k_floc2(VT<T>* __restrict__ BC, const T* __restrict__ vtot, T inv_nf, const VT<T>* twx_g, const VT<T>* twy_g) {
+k_floc2(VT<T>* __restrict__ BC, const T* __restrict__ vtot, T inv_nf, const VT<T>* twx_g, const VT<T>* twy_g,
+        const T* __restrict__ vperm) {
   using V = VT<T>;
   constexpr int n0 = NXF / 2;
   constexpr int nsx = n0 + 1, nsy = NYF / 2 + 1;
   using LY = FlocLayoutVar<T, NXF, NYF, VAR>;
   constexpr int PS = LY::PS, SKS = LY::SKS, PR = LY::PR, SKR = LY::SKR;
   constexpr bool FA = LY::FA, FB = LY::FB;
+  constexpr bool RTW = VAR == 2;
   constexpr int NX1 = SplitVar<NXF, VAR>::n1, NX2 = NXF / NX1, FX = 32 / NX1;
   constexpr int NY1 = SplitVar<NYF, VAR>::n1, NY2 = NYF / NY1, FY = 32 / NY1;
   constexpr int RX = (FX * NX2 + 31) / 32, RY = (FY * NY2 + 31) / 32;
@@ -739,11 +775,20 @@ k_floc2(VT<T>* __restrict__ BC, const T* __restrict__ vtot, T inv_nf, const VT<T
           t[j1] = s >= 0 ? Bp[s * nsx + c] : mkc<V>(0, 0);
         }
         DFT<NY1, +1, V>::run(t);
-#pragma unroll
-        for (int k1 = 1; k1 < NY1; ++k1) {
-          V w = twy[j2 * k1];
+        if constexpr (RTW) {
+          V p_[NY1];
+          V w = twy[j2];
           w.y = -w.y;
-          t[k1] = cmul(t[k1], w);
+          twiddle_powers<NY1>(w, p_);
+#pragma unroll
+          for (int k1 = 1; k1 < NY1; ++k1) t[k1] = cmul(t[k1], p_[k1]);
+        } else {
+#pragma unroll
+          for (int k1 = 1; k1 < NY1; ++k1) {
+            V w = twy[j2 * k1];
+            w.y = -w.y;
+            t[k1] = cmul(t[k1], w);
+          }
         }
 #pragma unroll
         for (int k1 = 0; k1 < NY1; ++k1) S[(NY2 * k1 + j2) * PS + SKS * k1 + c] = t[k1];
@@ -790,11 +835,20 @@ k_floc2(VT<T>* __restrict__ BC, const T* __restrict__ vtot, T inv_nf, const VT<T
           t[j1] = s >= 0 ? srow[s] : mkc<V>(0, 0);
         }
         DFT<NX1, +1, V>::run(t);
-#pragma unroll
-        for (int k1 = 1; k1 < NX1; ++k1) {
-          V w = twx[j2 * k1];
+        if constexpr (RTW) {
+          V p_[NX1];
+          V w = twx[j2];
           w.y = -w.y;
-          t[k1] = cmul(t[k1], w);
+          twiddle_powers<NX1>(w, p_);
+#pragma unroll
+          for (int k1 = 1; k1 < NX1; ++k1) t[k1] = cmul(t[k1], p_[k1]);
+        } else {
+#pragma unroll
+          for (int k1 = 1; k1 < NX1; ++k1) {
+            V w = twx[j2 * k1];
+            w.y = -w.y;
+            t[k1] = cmul(t[k1], w);
+          }
         }
 #pragma unroll
         for (int k1 = 0; k1 < NX1; ++k1) Rw[f * PR + (NX2 + SKR) * k1 + j2] = t[k1];
@@ -810,12 +864,38 @@ k_floc2(VT<T>* __restrict__ BC, const T* __restrict__ vtot, T inv_nf, const VT<T
 #pragma unroll
         for (int j2 = 0; j2 < NX2; ++j2) u[j2] = rr[j2];
         DFT<NX2, +1, V>::run(u);                    // u[k2] = x[k1 + NX1 k2]
-        const T* vrow = vtot + ((long)zf * NYF + r0 + f) * NXF + k1;
+        if constexpr (RTW && VpermLayout<T, NXF, NYF>::OK) {
+          using PL = VpermLayout<T, NXF, NYF>;
+          using VV = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+          const VV* vq = reinterpret_cast<const VV*>(vperm + ((long)zf * PL::NG + r0 / FX) * PL::NQ * 32 * PL::VW) + lane;
 #pragma unroll
-        for (int k2 = 0; k2 < NX2; ++k2) u[k2] = cscale(u[k2], vrow[NX1 * k2]);
+          for (int q = 0; q < PL::NQ; ++q) {
+            const VV vv = vq[32 * q];
+            if constexpr (sizeof(T) == 4) {
+              u[4 * q + 0] = cscale(u[4 * q + 0], (T)vv.x);
+              u[4 * q + 1] = cscale(u[4 * q + 1], (T)vv.y);
+              u[4 * q + 2] = cscale(u[4 * q + 2], (T)vv.z);
+              u[4 * q + 3] = cscale(u[4 * q + 3], (T)vv.w);
+            } else {
+              u[2 * q + 0] = cscale(u[2 * q + 0], (T)vv.x);
+              u[2 * q + 1] = cscale(u[2 * q + 1], (T)vv.y);
+            }
+          }
+        } else {
+          const T* vrow = vtot + ((long)zf * NYF + r0 + f) * NXF + k1;
+#pragma unroll
+          for (int k2 = 0; k2 < NX2; ++k2) u[k2] = cscale(u[k2], vrow[NX1 * k2]);
+        }
         DFT<NX2, -1, V>::run(u);                    // forward, first stage over k2
+        if constexpr (RTW) {
+          V p_[NX2];
+          twiddle_powers<NX2>(twx[k1], p_);
 #pragma unroll
-        for (int m2 = 1; m2 < NX2; ++m2) u[m2] = cmul(u[m2], twx[k1 * m2]);
+          for (int m2 = 1; m2 < NX2; ++m2) u[m2] = cmul(u[m2], p_[m2]);
+        } else {
+#pragma unroll
+          for (int m2 = 1; m2 < NX2; ++m2) u[m2] = cmul(u[m2], twx[k1 * m2]);
+        }
 #pragma unroll
         for (int m2 = 0; m2 < NX2; ++m2) rr[m2] = u[m2];
       }
@@ -854,8 +934,15 @@ k_floc2(VT<T>* __restrict__ BC, const T* __restrict__ vtot, T inv_nf, const VT<T
 #pragma unroll
         for (int j1 = 0; j1 < NY1; ++j1) t[j1] = S[(NY2 * j1 + j2) * PS + SKS * j1 + c];
         DFT<NY1, -1, V>::run(t);
+        if constexpr (RTW) {
+          V p_[NY1];
+          twiddle_powers<NY1>(twy[j2], p_);
 #pragma unroll
-        for (int k1 = 1; k1 < NY1; ++k1) t[k1] = cmul(t[k1], twy[j2 * k1]);
+          for (int k1 = 1; k1 < NY1; ++k1) t[k1] = cmul(t[k1], p_[k1]);
+        } else {
+#pragma unroll
+          for (int k1 = 1; k1 < NY1; ++k1) t[k1] = cmul(t[k1], twy[j2 * k1]);
+        }
 #pragma unroll
         for (int k1 = 0; k1 < NY1; ++k1) S[(NY2 * k1 + j2) * PS + SKS * k1 + c] = t[k1];
       }
@@ -1398,10 +1485,27 @@ struct Plan {
   }
   // the fused fine-plane kernel in the context's radix decomposition
   static void launch_floc2(pw_ctx* c, V* BC, const T* vt, T inv_nf, int nblk, cudaStream_t st) {
-    if (c->fft_variant == 1)
-      k_floc2<T, NF0, NF1, 1><<<dim3(NF2, nblk), FLOC_THREADS, sm_floc2<1>(), st>>>(BC, vt, inv_nf, tw(c, 3), tw(c, 4));
+    const T* vp = reinterpret_cast<const T*>(c->vperm.p);
+    if (c->fft_variant == 2 && (vp || !VpermLayout<T, NF0, NF1>::OK))
+      k_floc2<T, NF0, NF1, 2><<<dim3(NF2, nblk), FLOC_THREADS, sm_floc2<2>(), st>>>(BC, vt, inv_nf, tw(c, 3), tw(c, 4),
+                                                                                   vp);
+    else if (c->fft_variant == 1)
+      k_floc2<T, NF0, NF1, 1><<<dim3(NF2, nblk), FLOC_THREADS, sm_floc2<1>(), st>>>(BC, vt, inv_nf, tw(c, 3), tw(c, 4),
+                                                                                   nullptr);
     else
-      k_floc2<T, NF0, NF1, 0><<<dim3(NF2, nblk), FLOC_THREADS, sm_floc2<0>(), st>>>(BC, vt, inv_nf, tw(c, 3), tw(c, 4));
+      k_floc2<T, NF0, NF1, 0><<<dim3(NF2, nblk), FLOC_THREADS, sm_floc2<0>(), st>>>(BC, vt, inv_nf, tw(c, 3), tw(c, 4),
+                                                                                   nullptr);
+  }
+  // pw_ctx::vperm from pw_ctx::vtot (the lane order of VpermLayout)
+  static int vperm_build(pw_ctx* c, cudaStream_t st) {
+    using PL = VpermLayout<T, NF0, NF1>;
+    if (!PL::OK || !c->vtot.p) return PW_OK;
+    int rc = c->vperm.alloc((size_t)PL::PLANE * NF2 * sizeof(T));
+    if (rc) return rc;
+    k_vperm<T, NF0, NF1><<<148 * 4, 256, 0, st>>>(reinterpret_cast<const T*>(c->vtot.p),
+                                                   reinterpret_cast<T*>(c->vperm.p), NF2);
+    PWB_CUDA(cudaGetLastError());
+    return PW_OK;
   }
   static size_t sm_fplane(int cr) {
     return sizeof(V) * ((size_t)NF1 * (N0 + 1) + (size_t)cr * (NF0 + 1) + NF0 + NF1);
@@ -1421,6 +1525,7 @@ struct Plan {
     PWB_CUDA(cudaFuncSetAttribute(k_floc<T, NF0, NF1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_floc()));
     PWB_CUDA(cudaFuncSetAttribute(k_floc2<T, NF0, NF1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_floc2<0>()));
     PWB_CUDA(cudaFuncSetAttribute(k_floc2<T, NF0, NF1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_floc2<1>()));
+    PWB_CUDA(cudaFuncSetAttribute(k_floc2<T, NF0, NF1, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_floc2<2>()));
     PWB_CUDA(cudaFuncSetAttribute(k_floc<T, NF0, NF1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_floc()));
     once.mark();
     return PW_OK;
@@ -2030,6 +2135,9 @@ static int densgs_thunk(pw_ctx* c, const void* psi, int ld, int nband, int band0
                         double* rho, cudaStream_t st) {
   return Plan<T, N0, N1, N2>::density_gs_batch(c, (const T*)psi, ld, nband, band0, npair, w, rho, st);
 }
+template <typename T, int N0, int N1, int N2> static int vperm_thunk(pw_ctx* c, cudaStream_t st) {
+  return Plan<T, N0, N1, N2>::vperm_build(c, st);
+}
 template <typename T, int N0, int N1, int N2>
 static int buildqk_thunk(pw_ctx* c, const int* a, const double* b, const double* d, const long* e, const long* f,
                          const int* g, int n, const double* kv, void* out, cudaStream_t st) {
@@ -2049,6 +2157,7 @@ static int buildqk_thunk(pw_ctx* c, const int* a, const double* b, const double*
    {buildqk_thunk<double, a, b, c>, buildqk_thunk<float, a, b, c>},                                \
    {hpsikb_thunk<double, a, b, c>, hpsikb_thunk<float, a, b, c>},                                  \
    {hpsigs_thunk<double, a, b, c>, hpsigs_thunk<float, a, b, c>},                                  \
-   {densgs_thunk<double, a, b, c>, densgs_thunk<float, a, b, c>}}
+   {densgs_thunk<double, a, b, c>, densgs_thunk<float, a, b, c>},                                  \
+   {vperm_thunk<double, a, b, c>, vperm_thunk<float, a, b, c>}}
 
 }  // namespace pwb

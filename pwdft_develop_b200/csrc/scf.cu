@@ -37,6 +37,7 @@ int gram(pw_ctx* c, const void* X, int ldx, int nx, const void* Y, int ldy, int 
          cudaStream_t st, int nrow = -1);
 int upload_real(pw_ctx* c, DevBuf& dst, const double* src, size_t n);
 int wfn_filter_pass(pw_ctx* c, void* X, int ld, int nb, cudaStream_t st);
+int refresh_vperm(pw_ctx* c);
 
 // Hartree on the fine grid: vh = (1/N) IFFT( kern * FFT(rho - rho_ps) ),
 // kern = 2 pi / gkk (0 for gkk <= 1e-16 or gkk > 4 Ecut).  Cubic grids only.
@@ -1163,6 +1164,7 @@ int set_vtot_dev(pw_ctx* c, const double* vtot_dev) {
   if (rc) return rc;
   if (c->prec == PW_F64) PWB_CUDA(cudaMemcpy(c->vtot.p, vtot_dev, c->ntotf * 8, cudaMemcpyDeviceToDevice));
   else if ((rc = copy_d2f(c->ntotf, vtot_dev, (float*)c->vtot.p, nullptr))) return rc;
+  if ((rc = refresh_vperm(c))) return rc;
   c->have_vtot = true;
   return PW_OK;
 }

@@ -7,7 +7,8 @@
 //   * the inverse of an upper-triangular U (the Trsm of Orthogonalize applied
 //     to the identity), one CTA per column, column-oriented back substitution;
 //   * the symmetric eigen-decomposition (Syevd of SolveGenEig and of the final
-//     Rayleigh-Ritz, eigensolver.cpp:133-299, lobpcg.cpp) by cyclic two-sided
+//     Rayleigh-Ritz, eigensolver.cpp:133-299, lobpcg.cpp): up to n = 160
+//     through the tridiagonal form (below), beyond that by cyclic two-sided
 //     Jacobi in one CTA: round-robin pairings, all n/2 rotations of a round at
 //     once (2 x 2 block updates J_i^T A_ij J_j), the working matrix in shared
 //     memory when it fits, eigenvectors accumulated in global memory, then a
@@ -41,25 +42,28 @@ __global__ void __launch_bounds__(256) k_chol_panel(int n, double* A, int lda, i
   }
   __syncthreads();
   __shared__ int bad;
-  if (threadIdx.x == 0) bad = 0;
-  __syncthreads();
-  for (int j = 0; j < b; ++j) {
-    if (threadIdx.x == 0) {
-      const double d = D[j][j];
-      if (!(d > 0.0)) bad = k0 + j + 1;
-      else D[j][j] = sqrt(d);
+  // the diagonal block by warp 0 alone (lane c owns column c): no block-wide
+  // barrier inside the factorisation
+  if (threadIdx.x < 32) {
+    const int c = threadIdx.x;
+    int fail = 0;
+    for (int j = 0; j < b; ++j) {
+      const double djj = D[j][j];
+      if (!(djj > 0.0)) { fail = k0 + j + 1; break; }
+      const double ujj = sqrt(djj);
+      __syncwarp();
+      if (c == j) D[j][j] = ujj;
+      if (c > j && c < b) D[j][c] /= ujj;
+      __syncwarp();
+      if (c > j && c < b) {
+        const double ujc = D[j][c];
+        for (int i = j + 1; i <= c; ++i) D[i][c] -= D[j][i] * ujc;
+      }
+      __syncwarp();
     }
-    __syncthreads();
-    if (bad) break;
-    const double ujj = D[j][j];
-    for (int c = j + 1 + threadIdx.x; c < b; c += blockDim.x) D[j][c] /= ujj;
-    __syncthreads();
-    for (int t = threadIdx.x; t < b * b; t += blockDim.x) {
-      const int i = t % b, c = t / b;
-      if (i > j && i <= c) D[i][c] -= D[j][i] * D[j][c];
-    }
-    __syncthreads();
+    if (c == 0) bad = fail;
   }
+  __syncthreads();
   if (bad) {
     if (threadIdx.x == 0) *info = bad;
     return;
@@ -133,24 +137,59 @@ int dense_potrf_upper(int n, double* A, int lda, int* info_dev, cudaStream_t st)
 // ---------------------------------------------------------------------------
 // Ui = U^{-1} for an upper-triangular U: column j solves U x = e_j
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_trtri_upper(int n, const double* U, int ldu, double* Ui, int ldi) {
-  extern __shared__ double x[];
-  const int j = blockIdx.x;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) x[i] = (i == j) ? 1.0 : 0.0;
-  __syncthreads();
-  for (int l = j; l >= 0; --l) {
-    const double xl = x[l] / U[(long)l * ldu + l];
-    __syncthreads();
-    if (threadIdx.x == 0) x[l] = xl;
-    for (int i = threadIdx.x; i < l; i += blockDim.x) x[i] -= U[(long)l * ldu + i] * xl;
+// one warp per column (8 columns per CTA), x in the warp's shared row; only
+// warp-level synchronisation.  STAGE: U (n <= TRTRI_NSTAGE) is first copied
+// into shared memory with its diagonal inverted, so the steps read no global
+// memory and divide nowhere
+constexpr int TRTRI_WARPS = 8;
+constexpr int TRTRI_NSTAGE = 160;
+template <bool STAGE>
+__global__ void __launch_bounds__(32 * TRTRI_WARPS) k_trtri_upper(int n, const double* U, int ldu, double* Ui, int ldi) {
+  extern __shared__ double xs[];
+  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+  const int j = blockIdx.x * TRTRI_WARPS + wl;
+  double* x = xs + (size_t)wl * n;
+  double* us = xs + (size_t)TRTRI_WARPS * n;     // STAGE: U column-major, ld n, 1/U(l,l) on the diagonal
+  if constexpr (STAGE) {
+    const int jmax = min(n - 1, (int)(blockIdx.x * TRTRI_WARPS + TRTRI_WARPS - 1));
+    for (int idx = threadIdx.x; idx < (jmax + 1) * n; idx += blockDim.x) {
+      const int l = idx / n, i = idx - l * n;
+      const double u = i <= l ? U[(long)l * ldu + i] : 0.0;
+      us[idx] = (i == l) ? 1.0 / u : u;
+    }
     __syncthreads();
   }
-  for (int i = threadIdx.x; i < n; i += blockDim.x) Ui[(long)j * ldi + i] = (i <= j) ? x[i] : 0.0;
+  if (j >= n) return;
+  for (int i = lane; i < n; i += 32) x[i] = (i == j) ? 1.0 : 0.0;
+  __syncwarp();
+  for (int l = j; l >= 0; --l) {
+    const double* ul = STAGE ? us + (size_t)l * n : U + (long)l * ldu;
+    const double xl = STAGE ? x[l] * ul[l] : x[l] / ul[l];
+    __syncwarp();
+    if (lane == 0) x[l] = xl;
+    for (int i = lane; i < l; i += 32) x[i] -= ul[i] * xl;
+    __syncwarp();
+  }
+  for (int i = lane; i < n; i += 32) Ui[(long)j * ldi + i] = (i <= j) ? x[i] : 0.0;
 }
 
 int dense_trtri_upper(int n, const double* U, int ldu, double* Ui, int ldi, cudaStream_t st) {
   if (n <= 0) return PW_OK;
-  k_trtri_upper<<<n, 256, (size_t)n * 8, st>>>(n, U, ldu, Ui, ldi);
+  static PerDeviceOnce attr;
+  if (!attr.done()) {
+    PWB_CUDA(cudaFuncSetAttribute(k_trtri_upper<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+    PWB_CUDA(cudaFuncSetAttribute(k_trtri_upper<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+    attr.mark();
+  }
+  const int nblk = (n + TRTRI_WARPS - 1) / TRTRI_WARPS;
+  if (n <= TRTRI_NSTAGE) {
+    const size_t sm = ((size_t)TRTRI_WARPS * n + (size_t)n * n) * 8;
+    k_trtri_upper<true><<<nblk, 32 * TRTRI_WARPS, sm, st>>>(n, U, ldu, Ui, ldi);
+  } else {
+    const size_t sm = (size_t)TRTRI_WARPS * n * 8;
+    PWB_CHECK(sm <= 227 * 1024, PW_EUNSUPPORTED, "triangular inverse: n too large");
+    k_trtri_upper<false><<<nblk, 32 * TRTRI_WARPS, sm, st>>>(n, U, ldu, Ui, ldi);
+  }
   PWB_CUDA(cudaGetLastError());
   return PW_OK;
 }
@@ -385,6 +424,420 @@ __global__ void __launch_bounds__(256) k_jacobi_vectors(int n, double* A, int ld
   for (int i = lane; i < n; i += 32) A[(long)rank[i] * lda + row] = v[i];
 }
 
+// ---------------------------------------------------------------------------
+// Symmetric eigen-decomposition through the tridiagonal form (n <= TRD_NMAX):
+//   1. Householder reduction A = Q T Q^T in one CTA, the matrix in shared
+//      memory (lower form: reflector k zeroes column k below the subdiagonal,
+//      H_k = I - tau_k v_k v_k^T with v_k(k+1) = 1);
+//   2. all eigenvalues of T by multisection on Sturm counts: one warp per
+//      eigenvalue counts at 32 points of its bracket per step (a step shrinks
+//      the bracket 33-fold; 11 steps reach the rounding level);
+//   3. eigenvectors of T by inverse iteration with each computed eigenvalue
+//      as the shift (LU of T - lambda I with partial pivoting), three solves
+//      per vector, each followed by Gram-Schmidt against the earlier vectors
+//      of its cluster (neighbours closer than 1e-3 ||T||), one warp per
+//      cluster;
+//   4. X = Q Z: the reflectors applied to the columns of Z, 16 threads per
+//      column, no block-wide synchronisation.
+// About 8/3 n^3 flops against ~60 n^3 for ten Jacobi sweeps, and the
+// sequential parts (a reflector step, a tridiagonal solve) cost O(n) each.
+// ---------------------------------------------------------------------------
+constexpr int TRD_THREADS = 1024;   // 32 warps: the reduction's row map assumes it
+constexpr int TRD_NMAX = 160;
+constexpr int TRD_RPW = (TRD_NMAX + 31) / 32;   // rows of a step per warp
+constexpr int TRD_WARPS_STEIN = 4;
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+// sum over the block, returned to every thread (two barriers; red holds 32)
+__device__ double block_sum_d(double v, double* red) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  v = warp_sum_d(v);
+  __syncthreads();
+  if (lane == 0) red[wid] = v;
+  __syncthreads();
+  double t = 0;
+  for (int i = 0; i < nw; ++i) t += red[i];
+  return t;
+}
+
+// workspace (doubles): V [n n] reflectors (column k), Z [n n] eigenvectors of
+// T, d [n], e [n], tau [n]
+size_t trd_ws(int n) { return (size_t)2 * n * n + 3 * (size_t)n; }
+
+__global__ void __launch_bounds__(TRD_THREADS) k_trd_reduce(int n, const double* A, int lda, double* ws) {
+  extern __shared__ __align__(16) double trd_sm[];
+  const int P = n | 1;
+  double* W = trd_sm;                  // W[i P + j] = A(i, j), full symmetric
+  double* v = W + (size_t)n * P;       // reflector (rows k+1 .. n-1)
+  double* p = v + n;                   // tau A v, then w
+  __shared__ double s_tk;
+  double* V = ws;
+  double* d = ws + 2 * (size_t)n * n;
+  double* e = d + n;
+  double* tau = e + n;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  for (int idx = tid; idx < n * n; idx += blockDim.x) {
+    const int i = idx / n, j = idx - i * n;
+    W[i * P + j] = i <= j ? A[(long)j * lda + i] : A[(long)i * lda + j];
+    V[idx] = 0.0;
+  }
+  __syncthreads();
+  for (int k = 0; k + 2 < n; ++k) {
+    // warp 0: the reflector of column k (the other warps wait at the barrier)
+    if (wid == 0) {
+      double s = 0;
+      for (int i = k + 2 + lane; i < n; i += 32) {
+        const double x = W[i * P + k];
+        s += x * x;
+      }
+      s = warp_sum_d(s);
+      const double alpha = W[(k + 1) * P + k];
+      double tk = 0.0, beta = alpha, scal = 0.0;
+      if (s != 0.0) {
+        const double mu = sqrt(alpha * alpha + s);
+        beta = alpha <= 0.0 ? mu : -mu;
+        tk = (beta - alpha) / beta;
+        scal = 1.0 / (alpha - beta);
+      }
+      for (int i = k + 1 + lane; i < n; i += 32) {
+        const double vi = (i == k + 1) ? 1.0 : W[i * P + k] * scal;
+        v[i] = vi;
+        V[(long)k * n + i] = vi;
+      }
+      if (lane == 0) {
+        d[k] = W[k * P + k];
+        e[k] = beta;
+        tau[k] = tk;
+        s_tk = tk;
+      }
+    }
+    __syncthreads();
+    const double tk = s_tk;
+    if (tk == 0.0) continue;
+    // p = tau A22 v: warp wid owns rows k+1+wid+32m, their sums interleaved
+    {
+      double acc[TRD_RPW];
+#pragma unroll
+      for (int m = 0; m < TRD_RPW; ++m) acc[m] = 0.0;
+      for (int j = k + 1 + lane; j < n; j += 32) {
+        const double vj = v[j];
+#pragma unroll
+        for (int m = 0; m < TRD_RPW; ++m) {
+          const int i = k + 1 + wid + 32 * m;
+          if (i < n) acc[m] += W[i * P + j] * vj;
+        }
+      }
+#pragma unroll
+      for (int m = 0; m < TRD_RPW; ++m) acc[m] = warp_sum_d(acc[m]);
+      if (lane == 0) {
+#pragma unroll
+        for (int m = 0; m < TRD_RPW; ++m) {
+          const int i = k + 1 + wid + 32 * m;
+          if (i < n) p[i] = tk * acc[m];
+        }
+      }
+    }
+    __syncthreads();
+    // warp 0: w = p - (tau/2) (p.v) v
+    if (wid == 0) {
+      double t = 0;
+      for (int i = k + 1 + lane; i < n; i += 32) t += p[i] * v[i];
+      t = warp_sum_d(t);
+      const double kc = 0.5 * tk * t;
+      for (int i = k + 1 + lane; i < n; i += 32) p[i] -= kc * v[i];
+    }
+    __syncthreads();
+    // A22 -= v w^T + w v^T on the same rows
+    {
+      double vi[TRD_RPW], pi[TRD_RPW];
+#pragma unroll
+      for (int m = 0; m < TRD_RPW; ++m) {
+        const int i = k + 1 + wid + 32 * m;
+        vi[m] = i < n ? v[i] : 0.0;
+        pi[m] = i < n ? p[i] : 0.0;
+      }
+      for (int j = k + 1 + lane; j < n; j += 32) {
+        const double vj = v[j], pj = p[j];
+#pragma unroll
+        for (int m = 0; m < TRD_RPW; ++m) {
+          const int i = k + 1 + wid + 32 * m;
+          if (i < n) W[i * P + j] -= vi[m] * pj + pi[m] * vj;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    if (n >= 2) {
+      d[n - 2] = W[(n - 2) * P + n - 2];
+      e[n - 2] = W[(n - 1) * P + n - 2];
+      tau[n - 2] = 0.0;
+    }
+    d[n - 1] = W[(n - 1) * P + n - 1];
+    tau[n - 1] = 0.0;
+  }
+}
+
+// number of eigenvalues of T below x: negative pivots of the LDL^T
+// factorisation of T - x I (Sturm sequence in ratio form), pivots kept off
+// zero by pivmin
+__device__ __forceinline__ int trd_sturm(int n, const double* d, const double* e2, double x, double pivmin) {
+  double q = d[0] - x;
+  if (fabs(q) < pivmin) q = -pivmin;
+  int c = q <= 0.0;
+  for (int j = 1; j < n; ++j) {
+    q = d[j] - e2[j - 1] / q - x;
+    if (fabs(q) < pivmin) q = -pivmin;
+    c += q <= 0.0;
+  }
+  return c;
+}
+
+// eigenvalues ascending into w: one warp per eigenvalue, its 32 lanes count
+// at 32 interior points of the bracket per step (33-fold shrink: 11 steps
+// reach the rounding level); T's diagonal and squared off-diagonal in shared
+// memory, the Gershgorin interval recomputed by every CTA
+constexpr int TRD_BIS_WARPS = 4;
+constexpr int TRD_BIS_STEPS = 11;
+__global__ void __launch_bounds__(32 * TRD_BIS_WARPS) k_trd_bisect(int n, const double* ws, double* w) {
+  __shared__ double sd[TRD_NMAX], se2[TRD_NMAX];
+  __shared__ double s_gl, s_gu, s_pivmin;
+  const double* d = ws + 2 * (size_t)n * n;
+  const double* e = d + n;
+  const int tid = threadIdx.x, lane = tid & 31;
+  for (int i = tid; i < n; i += blockDim.x) {
+    sd[i] = d[i];
+    se2[i] = i + 1 < n ? e[i] * e[i] : 0.0;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    double gl = 1e300, gu = -1e300, emax = 0.0;
+    for (int i = 0; i < n; ++i) {
+      const double r = (i > 0 ? fabs(e[i - 1]) : 0.0) + (i + 1 < n ? fabs(e[i]) : 0.0);
+      gl = fmin(gl, sd[i] - r);
+      gu = fmax(gu, sd[i] + r);
+      emax = fmax(emax, se2[i]);
+    }
+    const double tn = fmax(fabs(gl), fabs(gu));
+    s_gl = gl - 2.3e-16 * tn * n - 1e-300;
+    s_gu = gu + 2.3e-16 * tn * n + 1e-300;
+    s_pivmin = 2.3e-308 * fmax(1.0, emax);
+  }
+  __syncthreads();
+  const int i = blockIdx.x * TRD_BIS_WARPS + (tid >> 5);
+  if (i >= n) return;
+  double lo = s_gl, hi = s_gu;
+  for (int step = 0; step < TRD_BIS_STEPS; ++step) {
+    const double x = lo + (hi - lo) * (double)(lane + 1) / 33.0;
+    const int c = trd_sturm(n, sd, se2, x, s_pivmin);
+    // eigenvalue i lies where the count passes i: count(lo) <= i < count(hi)
+    double nl = c <= i ? x : lo, nh = c > i ? x : hi;
+    for (int o = 16; o > 0; o >>= 1) {
+      nl = fmax(nl, __shfl_xor_sync(0xffffffffu, nl, o));
+      nh = fmin(nh, __shfl_xor_sync(0xffffffffu, nh, o));
+    }
+    lo = nl;
+    hi = nh;
+  }
+  if (lane == 0) w[i] = 0.5 * (lo + hi);
+}
+
+__device__ __forceinline__ double trd_rand(int i, int r) {
+  unsigned long long x = ((unsigned long long)(i + 1) << 32) ^ (unsigned long long)(r * 2654435761u + 12345u);
+  x ^= x >> 33;
+  x *= 0xff51afd7ed558ccdULL;
+  x ^= x >> 33;
+  x *= 0xc4ceb9fe1a85ec53ULL;
+  x ^= x >> 33;
+  return (double)(x >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+}
+
+// eigenvectors of T: one warp per cluster; lane 0 factors T - lambda I with
+// partial pivoting and runs the solves, the warp orthogonalises and normalises
+__global__ void __launch_bounds__(32 * TRD_WARPS_STEIN) k_trd_stein(int n, double* ws, const double* w) {
+  extern __shared__ __align__(16) double st_sm[];
+  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+  const int g = blockIdx.x * TRD_WARPS_STEIN + wl;
+  double* Z = ws + (size_t)n * n;
+  const double* d = ws + 2 * (size_t)n * n;
+  const double* e = d + n;
+  // clusters: neighbours closer than 1e-3 ||T|| (every CTA scans w itself)
+  __shared__ int clus[TRD_NMAX + 2];
+  if (threadIdx.x == 0) {
+    double tn0 = 0.0;
+    for (int i = 0; i < n; ++i) tn0 = fmax(tn0, fabs(d[i]) + (i + 1 < n ? 2.0 * fabs(e[i]) : 0.0));
+    const double ortol = 1e-3 * tn0;
+    int nc = 0;
+    for (int i = 0; i < n; ++i)
+      if (i == 0 || w[i] - w[i - 1] > ortol) clus[1 + nc++] = i;
+    clus[1 + nc] = n;
+    clus[0] = nc;
+  }
+  __syncthreads();
+  if (g >= clus[0]) return;
+  double* u = st_sm + (size_t)wl * 6 * n;
+  double* s1 = u + n;
+  double* s2 = s1 + n;
+  double* l = s2 + n;
+  double* y = l + n;
+  double* sw = y + n;          // row interchange at step k (1) or not (0)
+  double tn = 0.0;
+  for (int i = lane; i < n; i += 32) tn = fmax(tn, fabs(d[i]) + (i + 1 < n ? 2.0 * fabs(e[i]) : 0.0));
+  for (int o = 16; o > 0; o >>= 1) tn = fmax(tn, __shfl_xor_sync(0xffffffffu, tn, o));
+  const double eps = 2.3e-16 * fmax(tn, 1e-300);
+  const int c0 = clus[1 + g], c1 = clus[2 + g];
+  for (int i = c0; i < c1; ++i) {
+    const double lam = w[i];
+    if (lane == 0) {
+      // LU of T - lam I with row interchanges (U: pivot u, superdiagonals s1,
+      // s2; u then holds the pivots' reciprocals)
+      double ak = d[0] - lam, bk = n > 1 ? e[0] : 0.0;
+      for (int k = 0; k + 1 < n; ++k) {
+        const double ck = e[k];
+        double an = d[k + 1] - lam;
+        const double bn = k + 2 < n ? e[k + 1] : 0.0;
+        if (fabs(ak) >= fabs(ck)) {
+          if (ak == 0.0) ak = eps;
+          const double m = ck / ak;
+          u[k] = ak; s1[k] = bk; s2[k] = 0.0; l[k] = m; sw[k] = 0.0;
+          an -= m * bk;
+          ak = an;
+          bk = bn;
+        } else {
+          const double m = ak / ck;
+          u[k] = ck; s1[k] = an; s2[k] = bn; l[k] = m; sw[k] = 1.0;
+          ak = bk - m * an;
+          bk = -m * bn;
+        }
+      }
+      u[n - 1] = fabs(ak) < eps ? (ak < 0.0 ? -eps : eps) : ak;
+      // the solves multiply by the pivots' reciprocals (tiny pivots raised to eps)
+      for (int k = 0; k < n; ++k) {
+        const double uk = u[k];
+        u[k] = 1.0 / (fabs(uk) < eps ? (uk < 0.0 ? -eps : eps) : uk);
+      }
+    }
+    for (int r = lane; r < n; r += 32) y[r] = trd_rand(i, r);
+    __syncwarp();
+    for (int it = 0; it < 3; ++it) {
+      if (lane == 0) {
+        for (int k = 0; k + 1 < n; ++k) {
+          if (sw[k] != 0.0) {
+            const double t = y[k];
+            y[k] = y[k + 1];
+            y[k + 1] = t;
+          }
+          y[k + 1] -= l[k] * y[k];
+        }
+        for (int k = n - 1; k >= 0; --k) {
+          double t = y[k];
+          if (k + 1 < n) t -= s1[k] * y[k + 1];
+          if (k + 2 < n) t -= s2[k] * y[k + 2];
+          y[k] = t * u[k];
+        }
+      }
+      __syncwarp();
+      // Gram-Schmidt against the cluster's earlier vectors, then normalise
+      for (int j = c0; j < i; ++j) {
+        const double* zj = Z + (size_t)j * n;
+        double dt = 0;
+        for (int r = lane; r < n; r += 32) dt += zj[r] * y[r];
+        dt = warp_sum_d(dt);
+        for (int r = lane; r < n; r += 32) y[r] -= dt * zj[r];
+        __syncwarp();
+      }
+      double nr = 0;
+      for (int r = lane; r < n; r += 32) nr += y[r] * y[r];
+      nr = warp_sum_d(nr);
+      const double inv = nr > 0.0 ? 1.0 / sqrt(nr) : 0.0;
+      for (int r = lane; r < n; r += 32) y[r] *= inv;
+      __syncwarp();
+    }
+    for (int r = lane; r < n; r += 32) Z[(size_t)i * n + r] = y[r];
+    __syncwarp();
+  }
+}
+
+// X = H_0 H_1 ... H_{n-3} Z into A's columns; 16 threads per column, the
+// reflectors staged through shared memory TRD_KC at a time
+constexpr int TRD_QMAX = (TRD_NMAX + 15) / 16;
+constexpr int TRD_KC = 16;
+__global__ void __launch_bounds__(256) k_trd_back(int n, double* A, int lda, const double* ws) {
+  __shared__ double vs[TRD_KC][TRD_NMAX];
+  __shared__ double ts[TRD_KC];
+  const double* V = ws;
+  const double* Z = ws + (size_t)n * n;
+  const double* tau = ws + 2 * (size_t)n * n + 2 * (size_t)n;
+  const int c = blockIdx.x * 16 + (threadIdx.x >> 4), t = threadIdx.x & 15;
+  const bool act = c < n;
+  double z[TRD_QMAX];
+#pragma unroll
+  for (int q = 0; q < TRD_QMAX; ++q) {
+    const int r = t + 16 * q;
+    z[q] = (act && r < n) ? Z[(size_t)c * n + r] : 0.0;
+  }
+  for (int kt = n - 3; kt >= 0; kt -= TRD_KC) {
+    const int kb = max(0, kt - TRD_KC + 1), nk = kt - kb + 1;   // reflectors kb .. kt
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < nk * n; idx += blockDim.x) {
+      const int kk = idx / n, r = idx - kk * n;
+      vs[kk][r] = V[(size_t)(kb + kk) * n + r];
+    }
+    if (threadIdx.x < nk) ts[threadIdx.x] = tau[kb + threadIdx.x];
+    __syncthreads();
+    for (int kk = nk - 1; kk >= 0; --kk) {
+      const double tk = ts[kk];
+      if (tk == 0.0) continue;
+      const double* vk = vs[kk];
+      double s = 0.0;
+#pragma unroll
+      for (int q = 0; q < TRD_QMAX; ++q) {
+        const int r = t + 16 * q;
+        if (r < n) s += vk[r] * z[q];
+      }
+      for (int o = 8; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      s *= tk;
+#pragma unroll
+      for (int q = 0; q < TRD_QMAX; ++q) {
+        const int r = t + 16 * q;
+        if (r < n) z[q] -= vk[r] * s;
+      }
+    }
+  }
+  if (!act) return;
+#pragma unroll
+  for (int q = 0; q < TRD_QMAX; ++q) {
+    const int r = t + 16 * q;
+    if (r < n) A[(long)c * lda + r] = z[q];
+  }
+}
+
+int dense_syevh(int n, double* A, int lda, double* w, DevBuf& ws, cudaStream_t st) {
+  if (n <= 0) return PW_OK;
+  if (n > TRD_NMAX) return dense_syevj(n, A, lda, w, ws, nullptr, st);
+  int rc;
+  if ((rc = ws.alloc(trd_ws(n) * sizeof(double)))) return rc;
+  static PerDeviceOnce attr;
+  const size_t sm_red = ((size_t)TRD_NMAX * (TRD_NMAX | 1) + 2 * TRD_NMAX) * sizeof(double);
+  const size_t sm_st = (size_t)TRD_WARPS_STEIN * 6 * TRD_NMAX * sizeof(double);
+  if (!attr.done()) {
+    PWB_CUDA(cudaFuncSetAttribute(k_trd_reduce, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_red));
+    PWB_CUDA(cudaFuncSetAttribute(k_trd_stein, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_st));
+    attr.mark();
+  }
+  double* wsp = (double*)ws.p;
+  k_trd_reduce<<<1, TRD_THREADS, ((size_t)n * (n | 1) + 2 * (size_t)n) * sizeof(double), st>>>(n, A, lda, wsp);
+  k_trd_bisect<<<(n + TRD_BIS_WARPS - 1) / TRD_BIS_WARPS, 32 * TRD_BIS_WARPS, 0, st>>>(n, wsp, w);
+  k_trd_stein<<<(n + TRD_WARPS_STEIN - 1) / TRD_WARPS_STEIN, 32 * TRD_WARPS_STEIN,
+                (size_t)TRD_WARPS_STEIN * 6 * n * sizeof(double), st>>>(n, wsp, w);
+  k_trd_back<<<(n + 15) / 16, 256, 0, st>>>(n, A, lda, wsp);
+  PWB_CUDA(cudaGetLastError());
+  return PW_OK;
+}
+
 int dense_syevj(int n, double* A, int lda, double* w, DevBuf& ws, int* sweeps_dev, cudaStream_t st) {
   if (n <= 0) return PW_OK;
   const int m = n + (n & 1);
@@ -434,6 +887,12 @@ int pw_dense_syev(pw_ctx* ctx, int n, double* A, int lda, double* w, int* sweeps
   PWB_CUDA(cudaSetDevice(ctx->device));
   DevBuf ws, sw;
   int rc;
+  if (n <= TRD_NMAX) {
+    if ((rc = dense_syevh(n, A, lda, w, ws, nullptr))) return rc;
+    PWB_CUDA(cudaDeviceSynchronize());
+    if (sweeps) *sweeps = 0;
+    return PW_OK;
+  }
   if ((rc = sw.alloc(16))) return rc;
   if ((rc = dense_syevj(n, A, lda, w, ws, (int*)sw.p, nullptr))) return rc;
   PWB_CUDA(cudaDeviceSynchronize());

@@ -91,13 +91,16 @@ def test_gram_at_lobpcg_widths(n, K):
     c.close()
 
 
+@pytest.mark.parametrize("variant", [0, 1])
 @pytest.mark.parametrize("kind,reps,a,nc", [("Si", (1, 1, 1), 10.26, (24, 24, 24)), ("Si", (2, 2, 2), 10.26, (48, 48, 48)),
                                             ("Al", (2, 2, 2), 7.65, (60, 60, 60)), ("Si", (2, 1, 1), 10.26, (48, 24, 24)),
                                             ("Si", (3, 3, 3), 10.26, (72, 72, 72))])
-def test_hpsi_second_fft_decomposition_matches_oracle(kind, reps, a, nc):
-    """The fused fine-plane kernel in its second radix decomposition (the
-    autotuner's FFT candidate: 48 = 8 x 6, 96 = 12 x 8, 120 = 12 x 10,
-    144 = 16 x 9) against the oracle: FP64 1e-12, FP32 1e-5."""
+def test_hpsi_second_fft_decomposition_matches_oracle(kind, reps, a, nc, variant):
+    """The fused fine-plane kernel in the autotuner's non-default forms (the
+    default, variant 2, runs in every other test) against the oracle: the
+    inter-stage twiddles read from shared-memory tables (variant 0) and the
+    second radix decomposition (variant 1: 48 = 8 x 6, 96 = 12 x 8,
+    120 = 12 x 10, 144 = 16 x 9); FP64 1e-12, FP32 1e-5."""
     import torch
     from pwdft_develop_b200 import Context
     L, z, pos = pw.make_crystal(kind, reps, a, 0.02, 77)
@@ -109,7 +112,7 @@ def test_hpsi_second_fft_decomposition_matches_oracle(kind, reps, a, nc):
         c = Context(L, nc, nf, precision=prec)
         c.set_vtot(T.vtot)
         c.set_atoms([z] * len(pos), pos)
-        c.set_fft_variant(1)
+        c.set_fft_variant(variant)
         got = c.hpsi(torch.tensor(psi, dtype=c.torch_dtype, device="cuda")).double().cpu().numpy()
         assert np.abs(got - ref).max() / np.abs(ref).max() <= TOL[prec], (nc, prec)
         c.close()

@@ -1,10 +1,11 @@
 """The library's small dense FP64 kernels (Cholesky, triangular inverse,
-Jacobi eigen-decomposition, SolveGenEig) through the C ABI, against torch.linalg
+symmetric eigen-decomposition: tridiagonal form up to n = 160, Jacobi beyond;
+SolveGenEig) through the C ABI, against torch.linalg
 (cuSOLVER, used here only as the comparator) and against their defining
 identities: U^T U = A, U Ui = I, A V = V diag(w) with V^T V = I, ascending
 w, and the SolveGenEig result C^T B C = I, C^T A C = diag(eig).  Sizes cover
-one block, block edges (31, 32, 33), the shared-memory limit of the Jacobi
-kernel (160, 161), odd sizes, the LOBPCG Gram width 480, and clustered
+one block, block edges (31, 32, 33), the switch between the tridiagonal and
+the Jacobi eigensolvers (160, 161), odd sizes, the LOBPCG Gram width 480, and clustered
 (degenerate) spectra.  Tolerances: 1e-12 relative for factorisations and
 eigenvalues, 1e-10 for eigenvector residuals."""
 import ctypes as C
@@ -70,7 +71,7 @@ def test_potrf_reports_indefinite():
 
 @pytest.mark.parametrize("n", SIZES)
 @pytest.mark.parametrize("kind", ["random", "clustered"])
-def test_syev_jacobi(n, kind):
+def test_syev(n, kind):
     import torch
     from pwdft_develop_b200._lib import check, lib
     c = _ctx()
@@ -98,7 +99,8 @@ def test_syev_jacobi(n, kind):
     assert float((E @ E.T - torch.eye(n, dtype=torch.float64, device="cuda")).abs().max()) < 1e-10
     R = E @ A - w[:, None] * E
     assert float(R.abs().max()) < 1e-10 * max(scale, 1.0)
-    assert 1 <= sw.value <= 40
+    # up to n = 160 the tridiagonal path runs (no sweeps), beyond it Jacobi
+    assert sw.value == 0 if n <= 160 else 1 <= sw.value <= 40
     c.close()
 
 

@@ -152,14 +152,18 @@ def test_scf_si64_matches_oracle(which, mixed):
     degree 10) against the oracle's converged FP64 SCF of the same operator:
     unfiltered (si64_scf_plain.json) and with CheFSI's wavefunction cut-off
     filter (si64_scf_filter.json); FP64 and mixed precision.  Bars:
-    |E_free - E_oracle| / N_atom < 1e-6 Ha, occupied eigenvalues 1e-6 Ha."""
+    |E_free - E_oracle| / N_atom < 1e-6 Ha, occupied eigenvalues 1e-6 Ha.
+    The device SCF stops at |E_free - E_Harris| / N_atom < 1e-10: the energy
+    criterion is second order in the density error and the eigenvalues first
+    order, and at 1e-8 a mixed run could stop where E_Harris crosses E_free
+    with occupied eigenvalues still ~1e-5 Ha from the fixed point."""
     g = _si64_gold(which)
     L = np.array(g["length"])
     pos = np.array(g["positions"])
     c = _ctx(L, g["znuc"], pos, tuple(g["numGrid"]), tuple(g["numGridFine"]))
     res, eig, rho = c.scf(nocc=g["nocc"], nextra=g["nextra"], ecut=g["ecut"], solver="chebfsi", mixed=mixed,
-                          cheby_degree=10, cheby_first_cycles=5, tol_efree=1e-8, refine_threshold=3e-6,
-                          max_iter=80, graphs=True, wfn_filter=bool(g["wfn_filter"]))
+                          cheby_degree=10, cheby_first_cycles=5, tol_efree=1e-10, refine_threshold=3e-6,
+                          max_iter=100, graphs=True, wfn_filter=bool(g["wfn_filter"]))
     assert res["converged"] == 1
     nat = len(pos)
     assert abs(res["efree"] - g["efree"]) / nat < 1e-6, (res["efree"], g["efree"])
