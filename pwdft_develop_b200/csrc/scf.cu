@@ -389,9 +389,28 @@ struct Solver {
   int f_nb = 0, f_m = 0, f_calls = 0;
   void* f_res = nullptr;
   DevBuf fcoef;
-  ~Solver() {
+  // the whole ChebFSI step (coefficients from the device Ritz values, filter,
+  // cut-off filter pass, Cholesky-QR, H*psi, Rayleigh-Ritz) as one graph
+  cudaGraph_t sgraph = nullptr;
+  cudaGraphExec_t sexec = nullptr;
+  int s_nb = 0, s_m = 0, s_calls = 0;
+  bool s_off = false;       // capture failed once: the step runs directly
+  DevBuf bup;               // upper bound of the spectrum (device scalar)
+  double bup_host = 0.0;
+  void drop_graphs() {
     if (fexec) cudaGraphExecDestroy(fexec);
     if (fgraph) cudaGraphDestroy(fgraph);
+    if (sexec) cudaGraphExecDestroy(sexec);
+    if (sgraph) cudaGraphDestroy(sgraph);
+    fexec = nullptr;
+    fgraph = nullptr;
+    sexec = nullptr;
+    sgraph = nullptr;
+    f_calls = 0;
+    s_calls = 0;
+  }
+  ~Solver() {
+    drop_graphs();
     if (st) cudaStreamDestroy(st);
   }
 };
@@ -435,43 +454,51 @@ static int v_colscale(Solver& s, int nb, void* X, const double* sc) {
 
 static int alloc_block(Solver& s, DevBuf& b, int ncol) { return b.alloc((size_t)ncol * s.nt * s.esz); }
 
-// Cholesky-QR: X <- X U^{-1}, S = X^T X = U^T U (Orthogonalize, eigensolver.cpp:301-384)
-static int cholqr(Solver& s, Dense& d, void* X, int nb, void* tmp) {
-  const cudaStream_t st = nullptr;
+// Cholesky-QR: X <- X U^{-1}, S = X^T X = U^T U (Orthogonalize, eigensolver.cpp:301-384).
+// On stream st; defer_check: the factorisation's status stays in d.info (no
+// host round trip, for a captured step) instead of being checked here
+static int cholqr(Solver& s, Dense& d, void* X, int nb, void* tmp, cudaStream_t st = nullptr,
+                  bool defer_check = false) {
   int rc;
   if ((rc = s.G1.alloc((size_t)nb * nb * 8))) return rc;
   double* G = (double*)s.G1.p;
   { SubTimer t_(1); if ((rc = gram(s.c, X, (int)s.nt, nb, X, (int)s.nt, nb, G, nb, st))) return rc; }
   SubTimer td_(2);
-  if ((rc = d.potrf_upper(nb, G, nb, st))) return rc;
+  if (defer_check) rc = dense_potrf_upper(nb, G, nb, (int*)d.info.p, st);
+  else rc = d.potrf_upper(nb, G, nb, st);
+  if (rc) return rc;
   // Uinv = U^{-1} (upper): U * Uinv = I
   if ((rc = s.G2.alloc((size_t)nb * nb * 8))) return rc;
   double* Ui = (double*)s.G2.p;
   if ((rc = dense_trtri_upper(nb, G, nb, Ui, nb, st))) return rc;
   RotBlock rb{X, s.nt, nb, Ui, nb};
   { SubTimer t_(3); if ((rc = rotate(s.c, (int)s.nt, nb, &rb, 1, tmp, s.nt, 0.0, st))) return rc; }
-  PWB_CUDA(cudaMemcpy(X, tmp, (size_t)nb * s.nt * s.esz, cudaMemcpyDeviceToDevice));
+  PWB_CUDA(cudaMemcpyAsync(X, tmp, (size_t)nb * s.nt * s.esz, cudaMemcpyDeviceToDevice, st));
   return PW_OK;
 }
 
 // Rayleigh-Ritz on an orthonormal block Y with HY: eig(Y^T HY) = V diag(l),
-// X = Y V, HX = HY V
-static int rayleigh_ritz(Solver& s, Dense& d, void* Y, void* HY, void* X, void* HX, int nb) {
+// X = Y V, HX = HY V; the eigenvalues in s.wbuf and, unless deferred, s.eig
+static int rayleigh_ritz(Solver& s, Dense& d, void* Y, void* HY, void* X, void* HX, int nb, cudaStream_t st = nullptr,
+                         bool defer_eig = false) {
   int rc;
   if ((rc = s.G1.alloc((size_t)nb * nb * 8)) || (rc = s.wbuf.alloc((size_t)nb * 8 * 2))) return rc;
   double* A = (double*)s.G1.p;
-  { SubTimer t_(1); if ((rc = gram(s.c, Y, (int)s.nt, nb, HY, (int)s.nt, nb, A, nb, nullptr))) return rc; }
+  { SubTimer t_(1); if ((rc = gram(s.c, Y, (int)s.nt, nb, HY, (int)s.nt, nb, A, nb, st))) return rc; }
   // symmetrise from the upper triangle
-  if ((rc = dense_sym_upper(nb, A, nb, nullptr))) return rc;
+  if ((rc = dense_sym_upper(nb, A, nb, st))) return rc;
   double* w = (double*)s.wbuf.p;
-  { SubTimer t_(2); if ((rc = d.syevd(nb, A, nb, w, nullptr))) return rc; }
-  s.eig.resize(nb);
-  PWB_CUDA(cudaMemcpy(s.eig.data(), w, nb * 8, cudaMemcpyDeviceToHost));
+  { SubTimer t_(2); if ((rc = d.syevd(nb, A, nb, w, st))) return rc; }
+  if (!defer_eig) {
+    s.eig.resize(nb);
+    PWB_CUDA(cudaMemcpyAsync(s.eig.data(), w, nb * 8, cudaMemcpyDeviceToHost, st));
+    PWB_CUDA(cudaStreamSynchronize(st));
+  }
   SubTimer t_(3);
   RotBlock r1{Y, s.nt, nb, A, nb};
-  if ((rc = rotate(s.c, (int)s.nt, nb, &r1, 1, X, s.nt, 0.0, nullptr))) return rc;
+  if ((rc = rotate(s.c, (int)s.nt, nb, &r1, 1, X, s.nt, 0.0, st))) return rc;
   RotBlock r2{HY, s.nt, nb, A, nb};
-  return rotate(s.c, (int)s.nt, nb, &r2, 1, HX, s.nt, 0.0, nullptr);
+  return rotate(s.c, (int)s.nt, nb, &r2, 1, HX, s.nt, 0.0, st);
 }
 
 // Chebyshev filter of degree m on [a, b] scaled at a0 (Zhou et al. 2006,
@@ -683,6 +710,103 @@ static int chebfsi_step(Solver& s, Dense& d, int nb, int degree, double a, doubl
   void* outX = (res == s.X.p) ? tmp : s.X.p;
   if ((rc = rayleigh_ritz(s, d, res, s.HY.p, outX, s.HX.p, nb))) return rc;
   if (outX != s.X.p) PWB_CUDA(cudaMemcpy(s.X.p, outX, (size_t)nb * s.nt * s.esz, cudaMemcpyDeviceToDevice));
+  return PW_OK;
+}
+
+// Chebyshev coefficients of cheby_filter_run's recurrence from the previous
+// step's Ritz values on the device: a = w[nb-1], a0 = w[0], b = *bup
+__global__ void k_cheb_coef(const double* w, int nb, const double* bup, int m, double* coef) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const double a = w[nb - 1], a0 = w[0], b = *bup;
+  const double e = (b - a) / 2.0, cc = (b + a) / 2.0;
+  double sigma = e / (a0 - cc);
+  const double sigma1 = sigma, gamma = 2.0 / sigma1;
+  coef[0] = sigma1 / e;
+  coef[1] = -cc * sigma1 / e;
+  coef[2] = 0.0;
+  for (int i = 2; i <= m; ++i) {
+    const double sigma2 = 1.0 / (gamma - sigma);
+    coef[3 * (i - 1) + 0] = 2 * sigma2 / e;
+    coef[3 * (i - 1) + 1] = -2 * sigma2 * cc / e;
+    coef[3 * (i - 1) + 2] = -sigma * sigma2;
+    sigma = sigma2;
+  }
+}
+
+// the ChebFSI step with the bounds of the previous Rayleigh-Ritz (a =
+// eig[nb-1], a0 = eig[0]) and the Lanczos upper bound b_up, all on s.st with
+// no host round trip inside: with s.use_graph the first call runs directly,
+// the second captures it as one CUDA graph, later calls replay it; the host
+// then reads the Cholesky status and the new Ritz values once
+static int chebfsi_step_dev(Solver& s, Dense& d, int nb, int m, cudaStream_t st) {
+  int rc;
+  k_cheb_coef<<<1, 32, 0, st>>>((const double*)s.wbuf.p, nb, (const double*)s.bup.p, m, (double*)s.fcoef.p);
+  PWB_CUDA(cudaGetLastError());
+  void* res = nullptr;
+  if ((rc = cheby_filter_dev(s, nb, m, (const double*)s.fcoef.p, s.X.p, s.Y.p, s.Z.p, s.HY.p, &res, st))) return rc;
+  if (s.c->wfn_filter && (rc = wfn_filter_pass(s.c, res, (int)s.nt, nb, st))) return rc;
+  void* tmp = (res == s.Z.p) ? s.Y.p : s.Z.p;
+  if ((rc = cholqr(s, d, res, nb, tmp, st, true))) return rc;
+  if ((rc = pw_hpsi(s.c, res, (int)s.nt, s.HY.p, (int)s.nt, nb, 0, st))) return rc;
+  void* outX = (res == s.X.p) ? tmp : s.X.p;
+  if ((rc = rayleigh_ritz(s, d, res, s.HY.p, outX, s.HX.p, nb, st, true))) return rc;
+  if (outX != s.X.p) PWB_CUDA(cudaMemcpyAsync(s.X.p, outX, (size_t)nb * s.nt * s.esz, cudaMemcpyDeviceToDevice, st));
+  return PW_OK;
+}
+
+static int chebfsi_step_graph(Solver& s, Dense& d, int nb, int m, double b_up) {
+  if (!s.use_graph || s.s_off || s.eig.size() < (size_t)nb || !s.wbuf.p)
+    return chebfsi_step(s, d, nb, m, s.eig[nb - 1], b_up, s.eig[0]);
+  int rc;
+  if (!s.st) PWB_CUDA(cudaStreamCreateWithFlags(&s.st, cudaStreamNonBlocking));
+  {
+    cudaEvent_t ev;
+    PWB_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    PWB_CUDA(cudaEventRecord(ev, 0));
+    PWB_CUDA(cudaStreamWaitEvent(s.st, ev, 0));
+    cudaEventDestroy(ev);
+  }
+  if ((rc = s.fcoef.alloc((size_t)3 * std::max(m, 1) * 8)) || (rc = s.bup.alloc(8))) return rc;
+  s.bup_host = b_up;
+  PWB_CUDA(cudaMemcpyAsync(s.bup.p, &s.bup_host, 8, cudaMemcpyHostToDevice, s.st));
+  if (s.sexec && (s.s_nb != nb || s.s_m != m)) {
+    cudaGraphExecDestroy(s.sexec);
+    cudaGraphDestroy(s.sgraph);
+    s.sexec = nullptr;
+    s.sgraph = nullptr;
+    s.s_calls = 0;
+  }
+  if (!s.sexec && s.s_calls == 0) {
+    if ((rc = chebfsi_step_dev(s, d, nb, m, s.st))) return rc;
+    s.s_calls = 1;
+    s.s_nb = nb;
+    s.s_m = m;
+  } else {
+    if (!s.sexec) {
+      PWB_CUDA(cudaStreamSynchronize(s.st));
+      PWB_CUDA(cudaStreamBeginCapture(s.st, cudaStreamCaptureModeThreadLocal));
+      rc = chebfsi_step_dev(s, d, nb, m, s.st);
+      cudaError_t e1 = cudaStreamEndCapture(s.st, &s.sgraph);
+      cudaError_t e2 = (rc == PW_OK && e1 == cudaSuccess) ? cudaGraphInstantiate(&s.sexec, s.sgraph, 0) : e1;
+      if (rc != PW_OK || e2 != cudaSuccess) {
+        // a step that cannot be captured runs directly from now on
+        cudaGetLastError();
+        if (s.sgraph) cudaGraphDestroy(s.sgraph);
+        s.sgraph = nullptr;
+        s.sexec = nullptr;
+        s.s_off = true;
+        PWB_CUDA(cudaStreamSynchronize(s.st));
+        return chebfsi_step(s, d, nb, m, s.eig[nb - 1], b_up, s.eig[0]);
+      }
+    }
+    PWB_CUDA(cudaGraphLaunch(s.sexec, s.st));
+  }
+  int info = 0;
+  s.eig.resize(nb);
+  PWB_CUDA(cudaMemcpyAsync(&info, d.info.p, sizeof(int), cudaMemcpyDeviceToHost, s.st));
+  PWB_CUDA(cudaMemcpyAsync(s.eig.data(), s.wbuf.p, (size_t)nb * 8, cudaMemcpyDeviceToHost, s.st));
+  PWB_CUDA(cudaStreamSynchronize(s.st));
+  PWB_CHECK(info == 0, PW_ENUMERIC, "Cholesky factorisation of the Gram matrix failed");
   return PW_OK;
 }
 
@@ -1382,12 +1506,8 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
   sv.res.clear();
   sv.use_graph = p->graphs != 0 && !prof;   // the sub-phase timers synchronise, which a capture forbids
   auto bind = [&](pw_ctx* c) -> int {
-    // a captured filter refers to the previous context's buffers
-    if (sv.fexec) cudaGraphExecDestroy(sv.fexec);
-    if (sv.fgraph) cudaGraphDestroy(sv.fgraph);
-    sv.fexec = nullptr;
-    sv.fgraph = nullptr;
-    sv.f_calls = 0;
+    // captured graphs refer to the previous context's buffers
+    sv.drop_graphs();
     sv.c = c;
     sv.nt = nt;
     sv.esz = c->esz;
@@ -1488,7 +1608,7 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
           lmin = sv.eig[0];
         }
       } else {
-        if ((rc = chebfsi_step(sv, dn, nb, p->cheby_degree, sv.eig[nb - 1], b_up, sv.eig[0]))) return rc;
+        if ((rc = chebfsi_step_graph(sv, dn, nb, p->cheby_degree, b_up))) return rc;
         r->hpsi_bands += (long)nb * (p->cheby_degree + 1);
       }
     } else if (p->solver == PW_SOLVER_PPCG) {
@@ -1745,11 +1865,8 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
   if (hse) {
     // SCF::Iterate hybrid part, "nested" mixing (scf.cpp:628-925)
     if (!refined && (rc = refine_now())) return rc;
-    // the graph-captured filter holds H*psi without the exchange term
-    if (sv.fexec) cudaGraphExecDestroy(sv.fexec);
-    if (sv.fgraph) cudaGraphDestroy(sv.fgraph);
-    sv.fexec = nullptr;
-    sv.fgraph = nullptr;
+    // the graph-captured filter and step hold H*psi without the exchange term
+    sv.drop_graphs();
     sv.use_graph = false;
     hse_frac = 0.25;
     if ((rc = potentials(rho, &exc))) return rc;

@@ -473,6 +473,7 @@ __global__ void __launch_bounds__(TRD_THREADS) k_trd_reduce(int n, const double*
   double* W = trd_sm;                  // W[i P + j] = A(i, j), full symmetric
   double* v = W + (size_t)n * P;       // reflector (rows k+1 .. n-1)
   double* p = v + n;                   // tau A v, then w
+  double* zrow = p + n;                // a row of zeros: the rows of a warp past n point here
   __shared__ double s_tk;
   double* V = ws;
   double* d = ws + 2 * (size_t)n * n;
@@ -484,6 +485,7 @@ __global__ void __launch_bounds__(TRD_THREADS) k_trd_reduce(int n, const double*
     W[i * P + j] = i <= j ? A[(long)j * lda + i] : A[(long)i * lda + j];
     V[idx] = 0.0;
   }
+  for (int j = tid; j < n; j += blockDim.x) zrow[j] = 0.0;
   __syncthreads();
   for (int k = 0; k + 2 < n; ++k) {
     // warp 0: the reflector of column k (the other warps wait at the barrier)
@@ -517,7 +519,14 @@ __global__ void __launch_bounds__(TRD_THREADS) k_trd_reduce(int n, const double*
     __syncthreads();
     const double tk = s_tk;
     if (tk == 0.0) continue;
-    // p = tau A22 v: warp wid owns rows k+1+wid+32m, their sums interleaved
+    // p = tau A22 v: warp wid owns rows k+1+wid+32m (rows past n read the
+    // zero row), their sums interleaved
+    double* wr[TRD_RPW];
+#pragma unroll
+    for (int m = 0; m < TRD_RPW; ++m) {
+      const int i = k + 1 + wid + 32 * m;
+      wr[m] = i < n ? W + i * P : zrow;
+    }
     {
       double acc[TRD_RPW];
 #pragma unroll
@@ -525,10 +534,7 @@ __global__ void __launch_bounds__(TRD_THREADS) k_trd_reduce(int n, const double*
       for (int j = k + 1 + lane; j < n; j += 32) {
         const double vj = v[j];
 #pragma unroll
-        for (int m = 0; m < TRD_RPW; ++m) {
-          const int i = k + 1 + wid + 32 * m;
-          if (i < n) acc[m] += W[i * P + j] * vj;
-        }
+        for (int m = 0; m < TRD_RPW; ++m) acc[m] += wr[m][j] * vj;
       }
 #pragma unroll
       for (int m = 0; m < TRD_RPW; ++m) acc[m] = warp_sum_d(acc[m]);
@@ -550,7 +556,7 @@ __global__ void __launch_bounds__(TRD_THREADS) k_trd_reduce(int n, const double*
       for (int i = k + 1 + lane; i < n; i += 32) p[i] -= kc * v[i];
     }
     __syncthreads();
-    // A22 -= v w^T + w v^T on the same rows
+    // A22 -= v w^T + w v^T on the same rows (the zero row gets 0 v + 0 w)
     {
       double vi[TRD_RPW], pi[TRD_RPW];
 #pragma unroll
@@ -562,10 +568,7 @@ __global__ void __launch_bounds__(TRD_THREADS) k_trd_reduce(int n, const double*
       for (int j = k + 1 + lane; j < n; j += 32) {
         const double vj = v[j], pj = p[j];
 #pragma unroll
-        for (int m = 0; m < TRD_RPW; ++m) {
-          const int i = k + 1 + wid + 32 * m;
-          if (i < n) W[i * P + j] -= vi[m] * pj + pi[m] * vj;
-        }
+        for (int m = 0; m < TRD_RPW; ++m) wr[m][j] -= vi[m] * pj + pi[m] * vj;
       }
     }
     __syncthreads();
@@ -821,7 +824,7 @@ int dense_syevh(int n, double* A, int lda, double* w, DevBuf& ws, cudaStream_t s
   int rc;
   if ((rc = ws.alloc(trd_ws(n) * sizeof(double)))) return rc;
   static PerDeviceOnce attr;
-  const size_t sm_red = ((size_t)TRD_NMAX * (TRD_NMAX | 1) + 2 * TRD_NMAX) * sizeof(double);
+  const size_t sm_red = ((size_t)TRD_NMAX * (TRD_NMAX | 1) + 3 * TRD_NMAX) * sizeof(double);
   const size_t sm_st = (size_t)TRD_WARPS_STEIN * 6 * TRD_NMAX * sizeof(double);
   if (!attr.done()) {
     PWB_CUDA(cudaFuncSetAttribute(k_trd_reduce, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_red));
@@ -829,7 +832,7 @@ int dense_syevh(int n, double* A, int lda, double* w, DevBuf& ws, cudaStream_t s
     attr.mark();
   }
   double* wsp = (double*)ws.p;
-  k_trd_reduce<<<1, TRD_THREADS, ((size_t)n * (n | 1) + 2 * (size_t)n) * sizeof(double), st>>>(n, A, lda, wsp);
+  k_trd_reduce<<<1, TRD_THREADS, ((size_t)n * (n | 1) + 3 * (size_t)n) * sizeof(double), st>>>(n, A, lda, wsp);
   k_trd_bisect<<<(n + TRD_BIS_WARPS - 1) / TRD_BIS_WARPS, 32 * TRD_BIS_WARPS, 0, st>>>(n, wsp, w);
   k_trd_stein<<<(n + TRD_WARPS_STEIN - 1) / TRD_WARPS_STEIN, 32 * TRD_WARPS_STEIN,
                 (size_t)TRD_WARPS_STEIN * 6 * n * sizeof(double), st>>>(n, wsp, w);
