@@ -368,16 +368,22 @@ def scf_bench(device: int, max_iter: int = 60):
         torch.cuda.synchronize()
         # three timed runs (the SCF makes many small host round trips per iteration,
         # so a busy shared host shows up as run-to-run spread); the fastest is reported
-        samples = []
+        samples, sample_it = [], []
+        best = None
         for _ in range(3):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
-            res, eig, _ = c.scf(cheby_first_cycles=5, tol_efree=1e-6, refine_threshold=3e-6, max_iter=max_iter,
-                                **kw)
+            r_, eig_, _ = c.scf(cheby_first_cycles=5, tol_efree=1e-6, refine_threshold=3e-6, max_iter=max_iter,
+                                verbose=1 if os.environ.get("PWB_SCF_VERBOSE") else 0, **kw)
             e1.record()
             torch.cuda.synchronize()
             samples.append(e0.elapsed_time(e1) / 1e3)
-        out[mode] = dict(seconds=min(samples), samples_s=samples, iterations=res["iterations"],
+            sample_it.append([r_["iterations"], r_["refine_iter"]])
+            if best is None or samples[-1] <= min(samples):
+                best = (r_, eig_)
+        res, eig = best
+        out[mode] = dict(seconds=min(samples), samples_s=samples, samples_iterations_refine=sample_it,
+                         iterations=res["iterations"],
                          converged=bool(res["converged"]), efree=res["efree"], etot=res["etot"],
                          refine_iter=res["refine_iter"], hpsi_bands=res["hpsi_bands"], homo=float(eig[127]),
                          lumo=float(eig[128]))
@@ -693,22 +699,22 @@ def gspace_bench(device: int, reps: int = 10):
         out[prec] = {"ns": ns, "ms_per_sweep": ms, "bands_per_s": bands_per_s,
                      "model_bytes_per_band": pair_bytes / 2,
                      "model_frac_of_hbm": pair_bytes / 2 * bands_per_s / (peak * 1e9), "kernels": kern}
-        if prec == "f64":
-            # sphere-cut exact exchange (HSE06 kernel): 32 bands x 128 occupied
-            # orbitals, pair products on the full 96^3 grid (FP64 axis FFTs)
-            nk, nphi = 32, 128
-            c.exx_setup(0.25, 0.106, 1, ecut)
-            c.exx_set_phi(X[:nphi].contiguous(), np.ones(nphi))
-            Xk = X[:nk].contiguous()
-            V = c.exx_apply(Xk)
-            torch.cuda.synchronize()
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record()
-            c.exx_apply(Xk, out=V)
-            e1.record()
-            torch.cuda.synchronize()
-            xms = e0.elapsed_time(e1)
-            out["exx_f64"] = {"workload": "sphere-cut V_x psi, 32 bands x 128 orbitals (64 pair fields per band), "
+        # sphere-cut exact exchange (HSE06 kernel): 32 bands x 128 occupied
+        # orbitals, pair products on the full 96^3 grid (axis FFTs in the
+        # context's precision)
+        nk, nphi = 32, 128
+        c.exx_setup(0.25, 0.106, 1, ecut)
+        c.exx_set_phi(X[:nphi].contiguous(), np.ones(nphi))
+        Xk = X[:nk].contiguous()
+        V = c.exx_apply(Xk)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        c.exx_apply(Xk, out=V)
+        e1.record()
+        torch.cuda.synchronize()
+        xms = e0.elapsed_time(e1)
+        out["exx_" + prec] = {"workload": "sphere-cut V_x psi, 32 bands x 128 orbitals (64 pair fields per band), "
                                           "96^3 grid, HSE06 kernel (mu 0.106)",
                               "ms": xms, "pairs_per_s": nk * nphi / (xms / 1e3)}
         c.close()

@@ -598,8 +598,9 @@ PW_API int pw_scf_set_initial(pw_ctx* ctx, const double* rho_fine, const double*
  * grid: Density_Grid_Factor 1, src/esdf.cpp:2786-2856); N/2 must be a coarse
  * grid built into the library and the sphere must satisfy |m_d| <= N_d / 4.
  * After it, pw_ctx_sizes reports ntot = 2 ns and ntotFine = N.  Exact
- * exchange (pw_exx_*, pw_ace_*) is built for FP64 G-space contexts; k-points
- * and forces are not built for them (PW_EUNSUPPORTED). */
+ * exchange (pw_exx_*, pw_ace_*) runs on G-space contexts of either precision
+ * (FP32: FP32 pair fields and transforms); k-points and forces are not built
+ * for them (PW_EUNSUPPORTED). */
 PW_API int pw_ctx_create_gspace(const double length[3], const int numGrid[3], double ecut, int precision, int device,
                                 pw_ctx** out);
 /* Sphere tables of a G-space context (host arrays, any may be NULL):

@@ -34,20 +34,23 @@ int gram(pw_ctx* c, const void* X, int ldx, int nx, const void* Y, int ldy, int 
   }
   int rc;
   const bool same = (X == Y && ldx == ldy && nx == ny);
-  const size_t bx = (size_t)nx * nt * 2, by = (size_t)ny * nt * 2;
+  // split rows padded to a multiple of 8 elements (16-byte TMA strides; the
+  // tensor maps cover K = nt, so the pad is never read)
+  const long ntp = (nt + 7) / 8 * 8;
+  const size_t bx = (size_t)nx * ntp * 2, by = (size_t)ny * ntp * 2;
   if ((rc = c->s_gx_bf.alloc(2 * bx)) || (!same && (rc = c->s_gy_bf.alloc(2 * by)))) return rc;
   char* xb = (char*)c->s_gx_bf.p;
   char* yb = same ? xb : (char*)c->s_gy_bf.p;
   {
     Launch L_(c, st, KK_MISC);
-    if ((rc = split_bf16((const float*)X, ldx, nt, nx, xb, xb + bx, nt, 1.0f, st))) return rc;
+    if ((rc = split_bf16((const float*)X, ldx, nt, nx, xb, xb + bx, ntp, 1.0f, st))) return rc;
   }
   if (!same) {
     Launch L_(c, st, KK_MISC);
-    if ((rc = split_bf16((const float*)Y, ldy, nt, ny, yb, yb + by, nt, 1.0f, st))) return rc;
+    if ((rc = split_bf16((const float*)Y, ldy, nt, ny, yb, yb + by, ntp, 1.0f, st))) return rc;
   }
-  SplitOperand A{xb, xb + bx, nx, nt};
-  SplitOperand B{yb, yb + (same ? bx : by), ny, nt};
+  SplitOperand A{xb, xb + bx, nx, ntp};
+  SplitOperand B{yb, yb + (same ? bx : by), ny, ntp};
   ReduceOut ro;
   ro.out = G;
   ro.ldo = ldg;

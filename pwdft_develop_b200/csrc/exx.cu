@@ -252,12 +252,15 @@ int pw_ace_build(pw_ctx* ctx, const void* psi, int ld, int nband) {
   if ((rc = upload_real(ctx, ctx->ace_qd, m1.data(), nband))) return rc;
   const int npad = (nband + 7) / 8 * 8;
   if (ctx->prec == PW_F32) {
-    if ((rc = ctx->ace_bf.alloc((size_t)2 * nband * nt * 2)) || (rc = ctx->ace_t_bf.alloc((size_t)2 * nt * npad * 2)))
+    // rows of xi padded to a multiple of 8 (16-byte TMA strides; the tensor
+    // maps cover K = nt, so the pad is never read), as the projector matrix
+    const long ntp = (nt + 7) / 8 * 8;
+    if ((rc = ctx->ace_bf.alloc((size_t)2 * nband * ntp * 2)) || (rc = ctx->ace_t_bf.alloc((size_t)2 * nt * npad * 2)))
       return rc;
     PWB_CUDA(cudaMemset(ctx->ace_t_bf.p, 0, (size_t)2 * nt * npad * 2));
     char* b = (char*)ctx->ace_bf.p;
     char* bt = (char*)ctx->ace_t_bf.p;
-    if ((rc = split_bf16((const float*)ctx->ace_xi.p, nt, (int)nt, nband, b, b + (size_t)nband * nt * 2, nt, 1.0f,
+    if ((rc = split_bf16((const float*)ctx->ace_xi.p, nt, (int)nt, nband, b, b + (size_t)nband * ntp * 2, ntp, 1.0f,
                          nullptr)))
       return rc;
     if ((rc = split_bf16_t((const float*)ctx->ace_xi.p, nt, (int)nt, nband, bt, bt + (size_t)nt * npad * 2, npad,

@@ -1,5 +1,5 @@
-// FP64 3-D FFT of the fine grid, one axis per launch (used for the Hartree
-// potential and its gradient).
+// 3-D FFT of the fine grid, one axis per launch (FP64 for the Hartree
+// potential and its gradient; FP64 or FP32 for the sphere-cut exchange).
 #pragma once
 #include "fft.cuh"
 
@@ -17,14 +17,18 @@ constexpr int AX_THREADS = 256;
 // y_sub), 2: multiply by kern after the forward transform and inverse in place,
 // 3: store the real part scaled into out, 4: as 2 with the multiplier i * kern
 // (a spectral derivative).
-template <int N, int DIR, int AXIS, int MODE>
+// T (the real type) is never deduced from the arguments: FP64 unless given
+template <typename T> struct AxNoDeduce { using t = T; };
+template <int N, int DIR, int AXIS, int MODE, typename T = double>
 __global__ void __launch_bounds__(AX_THREADS)
-k_fft_axis(double2* __restrict__ data, int nx, int ny, int nz, const double* __restrict__ rin,
-           const double* __restrict__ rsub, const double* __restrict__ kern, double* __restrict__ rout, double scale,
-           const double2* tw_g) {
+k_fft_axis(typename C2<T>::t* __restrict__ data, int nx, int ny, int nz,
+           const typename AxNoDeduce<T>::t* __restrict__ rin, const typename AxNoDeduce<T>::t* __restrict__ rsub,
+           const typename AxNoDeduce<T>::t* __restrict__ kern, typename AxNoDeduce<T>::t* __restrict__ rout,
+           typename AxNoDeduce<T>::t scale, const typename C2<T>::t* tw_g) {
+  using V = typename C2<T>::t;
   constexpr int P = AX_TILE + 1;
-  __shared__ double2 buf[N * P];
-  __shared__ double2 tw[N];
+  __shared__ V buf[N * P];
+  __shared__ V tw[N];
   for (int i = threadIdx.x; i < N; i += blockDim.x) tw[i] = tw_g[i];
   long base;
   long estride;
@@ -38,10 +42,10 @@ k_fft_axis(double2* __restrict__ data, int nx, int ny, int nz, const double* __r
     // rows: element e of row r at base + r*nx + e -> buf[e*P + r]
     for (int i = threadIdx.x; i < N * AX_TILE; i += blockDim.x) {
       const int r = i / N, e = i - r * N;
-      double2 v = make_double2(0, 0);
+      V v = mkc<V>(0, 0);
       if (r < cnt) {
         const long g = base + (long)r * nx + e;
-        if (MODE == 1) v = make_double2(rin[g] - (rsub ? rsub[g] : 0.0), 0.0);
+        if (MODE == 1) v = mkc<V>(rin[g] - (rsub ? rsub[g] : (T)0), (T)0);
         else v = data[g];
       }
       buf[e * P + r] = v;
@@ -54,7 +58,7 @@ k_fft_axis(double2* __restrict__ data, int nx, int ny, int nz, const double* __r
     const long fofs = AXIS == 2 ? (long)blockIdx.z * nx * ny * nz : 0;
     for (int i = threadIdx.x; i < N * AX_TILE; i += blockDim.x) {
       const int e = i / AX_TILE, c = i - e * AX_TILE;
-      buf[e * P + c] = (c < cnt) ? data[fofs + base + e * estride + c] : make_double2(0, 0);
+      buf[e * P + c] = (c < cnt) ? data[fofs + base + e * estride + c] : mkc<V>(0, 0);
     }
   }
   __syncthreads();
@@ -64,9 +68,9 @@ k_fft_axis(double2* __restrict__ data, int nx, int ny, int nz, const double* __r
     for (int i = threadIdx.x; i < N * AX_TILE; i += blockDim.x) {
       const int e = i / AX_TILE, c = i - e * AX_TILE;
       if (c < cnt) {
-        const double k = kern[base + e * estride + c];
-        const double2 v = buf[e * P + c];
-        buf[e * P + c] = MODE == 2 ? cscale(v, k) : make_double2(-k * v.y, k * v.x);
+        const T k = kern[base + e * estride + c];
+        const V v = buf[e * P + c];
+        buf[e * P + c] = MODE == 2 ? cscale(v, k) : mkc<V>(-k * v.y, k * v.x);
       }
     }
     __syncthreads();

@@ -1,4 +1,4 @@
-// Exact exchange in the sphere-cut (G-space) mode, FP64: the complex
+// Exact exchange in the sphere-cut (G-space) mode, FP64 or FP32: the complex
 // overload of Spinor::AddMultSpinorEXX (src/SCF/spinor.cpp:783-945) with the
 // kernel of KohnSham::InitializeEXX for a sphere cut (src/SCF/hamiltonian.cpp:
 // 3454-3551) on the Fock set of Fourier::InitializeSphere
@@ -27,35 +27,40 @@ namespace pwb {
 
 int upload_real(pw_ctx* c, DevBuf& dst, const double* src, size_t n);   // ctx.cu
 
+template <typename T> using VT = typename C2<T>::t;
+
 namespace {
 
 // sphere -> full spectrum of band pairs: Z(G_s) = a + i b, Z(-G_s) = conj(a) + i conj(b)
-__global__ void k_gsx_scatter(const double* __restrict__ psi, int ld, int nb, int b0, int npair,
-                              const int2* __restrict__ gidx, int ns, double scale, long n3, double2* __restrict__ Z) {
+template <typename T>
+__global__ void k_gsx_scatter(const T* __restrict__ psi, int ld, int nb, int b0, int npair,
+                              const int2* __restrict__ gidx, int ns, T scale, long n3, VT<T>* __restrict__ Z) {
+  using V = VT<T>;
   const long tot = (long)npair * ns;
-  const double r2 = 0.70710678118654752440;
+  const T r2 = (T)0.70710678118654752440;
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot; t += (long)gridDim.x * blockDim.x) {
     const int p = (int)(t / ns), s = (int)(t - (long)p * ns);
     const int ba = b0 + 2 * p, bb = ba + 1;
-    const double f = scale * (s == 0 ? 1.0 : r2);
-    double2 a = make_double2(f * psi[(long)ba * ld + 2 * s], f * psi[(long)ba * ld + 2 * s + 1]);
-    double2 b = make_double2(0.0, 0.0);
-    if (bb < nb) b = make_double2(f * psi[(long)bb * ld + 2 * s], f * psi[(long)bb * ld + 2 * s + 1]);
-    if (s == 0) { a.y = 0.0; b.y = 0.0; }
-    double2* zp = Z + (long)p * n3;
+    const T f = scale * (s == 0 ? (T)1 : r2);
+    V a = mkc<V>(f * psi[(long)ba * ld + 2 * s], f * psi[(long)ba * ld + 2 * s + 1]);
+    V b = mkc<V>(0, 0);
+    if (bb < nb) b = mkc<V>(f * psi[(long)bb * ld + 2 * s], f * psi[(long)bb * ld + 2 * s + 1]);
+    if (s == 0) { a.y = 0; b.y = 0; }
+    V* zp = Z + (long)p * n3;
     const int2 g = gidx[s];
-    zp[g.x] = make_double2(a.x - b.y, a.y + b.x);
-    zp[g.y] = make_double2(a.x + b.y, b.x - a.y);
+    zp[g.x] = mkc<V>(a.x - b.y, a.y + b.x);
+    zp[g.y] = mkc<V>(a.x + b.y, b.x - a.y);
   }
 }
 
 // real and imaginary parts of pair fields -> bands b0 + 2p, b0 + 2p + 1
-__global__ void k_gsx_unpack(const double2* __restrict__ Z, int npair, long n3, int b0, int nb, double* __restrict__ R) {
+template <typename T>
+__global__ void k_gsx_unpack(const VT<T>* __restrict__ Z, int npair, long n3, int b0, int nb, T* __restrict__ R) {
   const long tot = (long)npair * n3;
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot; t += (long)gridDim.x * blockDim.x) {
     const int p = (int)(t / n3);
     const long r = t - (long)p * n3;
-    const double2 v = Z[t];
+    const VT<T> v = Z[t];
     const int ba = b0 + 2 * p;
     R[(long)ba * n3 + r] = v.x;
     if (ba + 1 < nb) R[(long)(ba + 1) * n3 + r] = v.y;
@@ -63,29 +68,31 @@ __global__ void k_gsx_unpack(const double2* __restrict__ Z, int npair, long n3, 
 }
 
 // pair fields of bands k0 .. k0 + kb - 1: F[kk * njp + jp] = psi_k (phi_2jp + i phi_2jp+1) / N
-__global__ void k_gsx_product(const double* __restrict__ psi_r, const double* __restrict__ phi_r, int k0, int kb,
-                              int njp, int nphi, long n3, double inv_n, double2* __restrict__ F) {
+template <typename T>
+__global__ void k_gsx_product(const T* __restrict__ psi_r, const T* __restrict__ phi_r, int k0, int kb,
+                              int njp, int nphi, long n3, T inv_n, VT<T>* __restrict__ F) {
   const long tot = (long)kb * njp * n3;
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot; t += (long)gridDim.x * blockDim.x) {
     const long f = t / n3, r = t - f * n3;
     const int kk = (int)(f / njp), jp = (int)(f - (long)kk * njp);
     const int ja = 2 * jp, jb = ja + 1;
-    const double p = psi_r[(long)(k0 + kk) * n3 + r] * inv_n;
-    F[t] = make_double2(p * phi_r[(long)ja * n3 + r], jb < nphi ? p * phi_r[(long)jb * n3 + r] : 0.0);
+    const T p = psi_r[(long)(k0 + kk) * n3 + r] * inv_n;
+    F[t] = mkc<VT<T>>(p * phi_r[(long)ja * n3 + r], jb < nphi ? p * phi_r[(long)jb * n3 + r] : (T)0);
   }
 }
 
 // acc_k(r) += sum_jp w_ja phi_ja(r) Re F + w_jb phi_jb(r) Im F
-__global__ void k_gsx_accumulate(const double2* __restrict__ F, const double* __restrict__ phi_r,
-                                 const double* __restrict__ w, int k0, int kb, int njp, int nphi, long n3,
-                                 double* __restrict__ acc) {
+template <typename T>
+__global__ void k_gsx_accumulate(const VT<T>* __restrict__ F, const T* __restrict__ phi_r,
+                                 const T* __restrict__ w, int k0, int kb, int njp, int nphi, long n3,
+                                 T* __restrict__ acc) {
   const long tot = (long)kb * n3;
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot; t += (long)gridDim.x * blockDim.x) {
     const int kk = (int)(t / n3);
     const long r = t - (long)kk * n3;
-    double s = 0.0;
+    T s = 0;
     for (int jp = 0; jp < njp; ++jp) {
-      const double2 v = F[((long)kk * njp + jp) * n3 + r];
+      const VT<T> v = F[((long)kk * njp + jp) * n3 + r];
       const int ja = 2 * jp, jb = ja + 1;
       s += w[ja] * phi_r[(long)ja * n3 + r] * v.x;
       if (jb < nphi) s += w[jb] * phi_r[(long)jb * n3 + r] * v.y;
@@ -95,35 +102,38 @@ __global__ void k_gsx_accumulate(const double2* __restrict__ F, const double* __
 }
 
 // bands b0 + 2p, b0 + 2p + 1 of acc -> complex pair fields
-__global__ void k_gsx_pack(const double* __restrict__ acc, int b0, int nb, int npair, long n3, double2* __restrict__ Z) {
+template <typename T>
+__global__ void k_gsx_pack(const T* __restrict__ acc, int b0, int nb, int npair, long n3, VT<T>* __restrict__ Z) {
   const long tot = (long)npair * n3;
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot; t += (long)gridDim.x * blockDim.x) {
     const int p = (int)(t / n3);
     const long r = t - (long)p * n3;
     const int ba = b0 + 2 * p;
-    Z[t] = make_double2(acc[(long)ba * n3 + r], ba + 1 < nb ? acc[(long)(ba + 1) * n3 + r] : 0.0);
+    Z[t] = mkc<VT<T>>(acc[(long)ba * n3 + r], ba + 1 < nb ? acc[(long)(ba + 1) * n3 + r] : (T)0);
   }
 }
 
 // spectrum of a band pair -> sphere: a = (Y(G) + conj Y(-G)) / 2, b = (Y(G) - conj Y(-G)) / 2i
-__global__ void k_gsx_gather(const double2* __restrict__ Z, int npair, long n3, const int2* __restrict__ gidx, int ns,
-                             int b0, int nb, double* __restrict__ out, int ldo, int accumulate) {
+template <typename T>
+__global__ void k_gsx_gather(const VT<T>* __restrict__ Z, int npair, long n3, const int2* __restrict__ gidx, int ns,
+                             int b0, int nb, T* __restrict__ out, int ldo, int accumulate) {
+  using V = VT<T>;
   const long tot = (long)npair * ns;
-  const double sq2 = 1.41421356237309504880;
+  const T sq2 = (T)1.41421356237309504880;
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < tot; t += (long)gridDim.x * blockDim.x) {
     const int p = (int)(t / ns), s = (int)(t - (long)p * ns);
-    const double2* zp = Z + (long)p * n3;
+    const V* zp = Z + (long)p * n3;
     const int2 g = gidx[s];
-    const double2 y = zp[g.x], ym = zp[g.y];
-    const double f = s == 0 ? 1.0 : sq2;
-    double2 a = make_double2(0.5 * f * (y.x + ym.x), 0.5 * f * (y.y - ym.y));
-    double2 b = make_double2(0.5 * f * (y.y + ym.y), 0.5 * f * (ym.x - y.x));
-    if (s == 0) { a.y = 0.0; b.y = 0.0; }
+    const V y = zp[g.x], ym = zp[g.y];
+    const T f = s == 0 ? (T)1 : sq2;
+    V a = mkc<V>((T)0.5 * f * (y.x + ym.x), (T)0.5 * f * (y.y - ym.y));
+    V b = mkc<V>((T)0.5 * f * (y.y + ym.y), (T)0.5 * f * (ym.x - y.x));
+    if (s == 0) { a.y = 0; b.y = 0; }
     const int ba = b0 + 2 * p, bb = ba + 1;
-    double* oa = out + (long)ba * ldo + 2 * s;
+    T* oa = out + (long)ba * ldo + 2 * s;
     if (accumulate) { oa[0] += a.x; oa[1] += a.y; } else { oa[0] = a.x; oa[1] = a.y; }
     if (bb < nb) {
-      double* ob = out + (long)bb * ldo + 2 * s;
+      T* ob = out + (long)bb * ldo + 2 * s;
       if (accumulate) { ob[0] += b.x; ob[1] += b.y; } else { ob[0] = b.x; ob[1] = b.y; }
     }
   }
@@ -132,52 +142,115 @@ __global__ void k_gsx_gather(const double2* __restrict__ Z, int npair, long n3, 
 inline int gs_blocks(long n) { return (int)std::min<long>((n + 255) / 256, 148L * 16); }
 
 // F complex N^3 fields back to back: mode 0 forward, 1 inverse, 2 convolution with kern
-template <int N> int fft3_fields(double2* d, int F, int mode, const double* kern, const double2* tw, cudaStream_t st) {
+template <typename T, int N>
+int fft3_fields(VT<T>* d, int F, int mode, const T* kern, const VT<T>* tw, cudaStream_t st) {
   const int nxt = (N + AX_TILE - 1) / AX_TILE;
   const int rows = (int)(((long)N * N * F + AX_TILE - 1) / AX_TILE);
+  const T one = 1;
   if (mode == 1) {
-    k_fft_axis<N, +1, 2, 0><<<dim3(nxt, N, F), AX_THREADS, 0, st>>>(d, N, N, N, nullptr, nullptr, nullptr, nullptr, 1.0, tw);
-    k_fft_axis<N, +1, 1, 0><<<dim3(nxt, N * F), AX_THREADS, 0, st>>>(d, N, N, N * F, nullptr, nullptr, nullptr, nullptr, 1.0, tw);
-    k_fft_axis<N, +1, 0, 0><<<rows, AX_THREADS, 0, st>>>(d, N, N, N * F, nullptr, nullptr, nullptr, nullptr, 1.0, tw);
+    k_fft_axis<N, +1, 2, 0, T><<<dim3(nxt, N, F), AX_THREADS, 0, st>>>(d, N, N, N, nullptr, nullptr, nullptr, nullptr, one, tw);
+    k_fft_axis<N, +1, 1, 0, T><<<dim3(nxt, N * F), AX_THREADS, 0, st>>>(d, N, N, N * F, nullptr, nullptr, nullptr, nullptr, one, tw);
+    k_fft_axis<N, +1, 0, 0, T><<<rows, AX_THREADS, 0, st>>>(d, N, N, N * F, nullptr, nullptr, nullptr, nullptr, one, tw);
   } else {
-    k_fft_axis<N, -1, 0, 0><<<rows, AX_THREADS, 0, st>>>(d, N, N, N * F, nullptr, nullptr, nullptr, nullptr, 1.0, tw);
-    k_fft_axis<N, -1, 1, 0><<<dim3(nxt, N * F), AX_THREADS, 0, st>>>(d, N, N, N * F, nullptr, nullptr, nullptr, nullptr, 1.0, tw);
+    k_fft_axis<N, -1, 0, 0, T><<<rows, AX_THREADS, 0, st>>>(d, N, N, N * F, nullptr, nullptr, nullptr, nullptr, one, tw);
+    k_fft_axis<N, -1, 1, 0, T><<<dim3(nxt, N * F), AX_THREADS, 0, st>>>(d, N, N, N * F, nullptr, nullptr, nullptr, nullptr, one, tw);
     if (mode == 0) {
-      k_fft_axis<N, -1, 2, 0><<<dim3(nxt, N, F), AX_THREADS, 0, st>>>(d, N, N, N, nullptr, nullptr, nullptr, nullptr, 1.0, tw);
+      k_fft_axis<N, -1, 2, 0, T><<<dim3(nxt, N, F), AX_THREADS, 0, st>>>(d, N, N, N, nullptr, nullptr, nullptr, nullptr, one, tw);
     } else {
-      k_fft_axis<N, -1, 2, 2><<<dim3(nxt, N, F), AX_THREADS, 0, st>>>(d, N, N, N, nullptr, nullptr, kern, nullptr, 1.0, tw);
-      k_fft_axis<N, +1, 1, 0><<<dim3(nxt, N * F), AX_THREADS, 0, st>>>(d, N, N, N * F, nullptr, nullptr, nullptr, nullptr, 1.0, tw);
-      k_fft_axis<N, +1, 0, 0><<<rows, AX_THREADS, 0, st>>>(d, N, N, N * F, nullptr, nullptr, nullptr, nullptr, 1.0, tw);
+      k_fft_axis<N, -1, 2, 2, T><<<dim3(nxt, N, F), AX_THREADS, 0, st>>>(d, N, N, N, nullptr, nullptr, kern, nullptr, one, tw);
+      k_fft_axis<N, +1, 1, 0, T><<<dim3(nxt, N * F), AX_THREADS, 0, st>>>(d, N, N, N * F, nullptr, nullptr, nullptr, nullptr, one, tw);
+      k_fft_axis<N, +1, 0, 0, T><<<rows, AX_THREADS, 0, st>>>(d, N, N, N * F, nullptr, nullptr, nullptr, nullptr, one, tw);
     }
   }
   PWB_CUDA(cudaGetLastError());
   return PW_OK;
 }
 
-int fft3_fields_n(int N, double2* d, int F, int mode, const double* kern, const double2* tw, cudaStream_t st) {
+template <typename T>
+int fft3_fields_n(int N, VT<T>* d, int F, int mode, const T* kern, const VT<T>* tw, cudaStream_t st) {
   switch (N) {
-    case 24: return fft3_fields<24>(d, F, mode, kern, tw, st);
-    case 32: return fft3_fields<32>(d, F, mode, kern, tw, st);
-    case 48: return fft3_fields<48>(d, F, mode, kern, tw, st);
-    case 96: return fft3_fields<96>(d, F, mode, kern, tw, st);
-    case 144: return fft3_fields<144>(d, F, mode, kern, tw, st);
+    case 24: return fft3_fields<T, 24>(d, F, mode, kern, tw, st);
+    case 32: return fft3_fields<T, 32>(d, F, mode, kern, tw, st);
+    case 48: return fft3_fields<T, 48>(d, F, mode, kern, tw, st);
+    case 96: return fft3_fields<T, 96>(d, F, mode, kern, tw, st);
+    case 144: return fft3_fields<T, 144>(d, F, mode, kern, tw, st);
     default: set_error("G-space exact exchange: grid size not built (24, 32, 48, 96, 144)"); return PW_EUNSUPPORTED;
   }
 }
 
 // sphere bands (real view, ld) -> real fields [nb][N^3] through pair fields of at most cap pairs
-int gs_to_real(pw_ctx* c, const double* psi, int ld, int nb, double scale, double* R, double2* Z, int cap,
-               cudaStream_t st) {
+template <typename T>
+int gs_to_real(pw_ctx* c, const T* psi, int ld, int nb, T scale, T* R, VT<T>* Z, int cap, cudaStream_t st) {
   const int N = c->nf[0];
   const long n3 = (long)N * N * N;
   for (int b0 = 0; b0 < nb; b0 += 2 * cap) {
     const int np = std::min(cap, (nb - b0 + 1) / 2);
-    PWB_CUDA(cudaMemsetAsync(Z, 0, (size_t)np * n3 * 16, st));
-    k_gsx_scatter<<<gs_blocks((long)np * c->gs_ns), 256, 0, st>>>(psi, ld, nb, b0, np, (const int2*)c->gs_full_idx.p,
-                                                                  (int)c->gs_ns, scale, n3, Z);
-    int rc = fft3_fields_n(N, Z, np, 1, nullptr, (const double2*)c->gs_exx_tw.p, st);
+    PWB_CUDA(cudaMemsetAsync(Z, 0, (size_t)np * n3 * sizeof(VT<T>), st));
+    k_gsx_scatter<T><<<gs_blocks((long)np * c->gs_ns), 256, 0, st>>>(psi, ld, nb, b0, np,
+                                                                     (const int2*)c->gs_full_idx.p, (int)c->gs_ns,
+                                                                     scale, n3, Z);
+    int rc = fft3_fields_n<T>(N, Z, np, 1, nullptr, (const VT<T>*)c->gs_exx_tw.p, st);
     if (rc) return rc;
-    k_gsx_unpack<<<gs_blocks((long)np * n3), 256, 0, st>>>(Z, np, n3, b0, nb, R);
+    k_gsx_unpack<T><<<gs_blocks((long)np * n3), 256, 0, st>>>(Z, np, n3, b0, nb, R);
+    c->launches += 5;
+  }
+  PWB_CUDA(cudaGetLastError());
+  return PW_OK;
+}
+
+// out (+)= V_x psi for nb sphere bands
+template <typename T>
+int gs_exx_apply_t(pw_ctx* c, const T* psi, int ld, int nb, T* out, int ldo, int accumulate, cudaStream_t st) {
+  using V = VT<T>;
+  const int N = c->nf[0];
+  const long n3 = (long)N * N * N;
+  const int nphi = c->exx_nphi;
+  if (nphi == 0) {
+    if (!accumulate) PWB_CUDA(cudaMemset2DAsync(out, (size_t)ldo * sizeof(T), 0, (size_t)c->ntot * sizeof(T), nb, st));
+    return PW_OK;
+  }
+  const int njp = (nphi + 1) / 2;
+  // fields per batch from the scratch budget (at least one band's pair fields)
+  // (gridDim.y of the axis-1 pass is N * fields: at most 65535)
+  const long fmax = 65535 / N;
+  PWB_CHECK(njp <= fmax, PW_EUNSUPPORTED, "G-space exact exchange: too many exchange orbitals for one band batch");
+  const long fcap = std::min<long>(fmax, std::max<long>(njp, (long)(c->exx_scratch_bytes / (size_t)(n3 * sizeof(V)))));
+  const int kb = (int)std::max<long>(1, std::min<long>(nb, fcap / njp));
+  const int pcap = (int)std::max<long>(1, std::min<long>((std::max(nb, nphi) + 1) / 2, fcap));
+  // workspace kept in the context (reused while large enough); phi(r) is
+  // transformed once per pw_exx_set_phi
+  DevBuf &psir = c->gsx_psir, &phir = c->gsx_phir, &acc = c->gsx_acc, &F = c->gsx_fields;
+  int rc;
+  const size_t phib = (size_t)nphi * n3 * sizeof(T);
+  if (phir.bytes < phib) c->gsx_phi_ready = false;
+  if ((rc = psir.alloc((size_t)nb * n3 * sizeof(T))) || (rc = phir.alloc(phib)) ||
+      (rc = acc.alloc((size_t)nb * n3 * sizeof(T))) ||
+      (rc = F.alloc((size_t)std::max<long>((long)kb * njp, pcap) * n3 * sizeof(V))))
+    return rc;
+  V* Z = (V*)F.p;
+  const V* tw = (const V*)c->gs_exx_tw.p;
+  if (!c->gsx_phi_ready) {
+    if ((rc = gs_to_real<T>(c, (const T*)c->exx_phi.p, (int)c->ntot, nphi, (T)1, (T*)phir.p, Z, pcap, st))) return rc;
+    c->gsx_phi_ready = true;
+  }
+  if ((rc = gs_to_real<T>(c, psi, ld, nb, (T)1, (T*)psir.p, Z, pcap, st))) return rc;
+  PWB_CUDA(cudaMemsetAsync(acc.p, 0, (size_t)nb * n3 * sizeof(T), st));
+  for (int k0 = 0; k0 < nb; k0 += kb) {
+    const int kn = std::min(kb, nb - k0);
+    const int nf = kn * njp;
+    k_gsx_product<T><<<gs_blocks((long)nf * n3), 256, 0, st>>>((const T*)psir.p, (const T*)phir.p, k0, kn, njp, nphi,
+                                                               n3, (T)(1.0 / (double)n3), Z);
+    if ((rc = fft3_fields_n<T>(N, Z, nf, 2, (const T*)c->exx_kern.p, tw, st))) return rc;
+    k_gsx_accumulate<T><<<gs_blocks((long)kn * n3), 256, 0, st>>>(Z, (const T*)phir.p, (const T*)c->exx_w.p, k0, kn,
+                                                                  njp, nphi, n3, (T*)acc.p);
+    c->launches += 7;
+  }
+  for (int b0 = 0; b0 < nb; b0 += 2 * pcap) {
+    const int np = std::min(pcap, (nb - b0 + 1) / 2);
+    k_gsx_pack<T><<<gs_blocks((long)np * n3), 256, 0, st>>>((const T*)acc.p, b0, nb, np, n3, Z);
+    if ((rc = fft3_fields_n<T>(N, Z, np, 0, nullptr, tw, st))) return rc;
+    k_gsx_gather<T><<<gs_blocks((long)np * c->gs_ns), 256, 0, st>>>(Z, np, n3, (const int2*)c->gs_full_idx.p,
+                                                                    (int)c->gs_ns, b0, nb, out, ldo, accumulate);
     c->launches += 5;
   }
   PWB_CUDA(cudaGetLastError());
@@ -188,7 +261,6 @@ int gs_to_real(pw_ctx* c, const double* psi, int ld, int nb, double scale, doubl
 
 // exchange kernel and its auxiliary (Fock set, full-grid sphere indices, twiddles) of a G-space context
 int gs_exx_setup(pw_ctx* c, double frac, double mu, int divergence_type, double ecut) {
-  PWB_CHECK(c->prec == PW_F64, PW_EUNSUPPORTED, "G-space exact exchange is built for FP64 contexts");
   const int N = c->nf[0];
   PWB_CHECK(c->nf[1] == N && c->nf[2] == N, PW_EUNSUPPORTED, "G-space exact exchange needs a cubic grid");
   const long n3 = (long)N * N * N;
@@ -242,73 +314,20 @@ int gs_exx_setup(pw_ctx* c, double frac, double mu, int divergence_type, double 
     tw[2 * m] = std::cos(2 * M_PI * m / N);
     tw[2 * m + 1] = -std::sin(2 * M_PI * m / N);
   }
-  if ((rc = c->gs_exx_tw.alloc(N * 16))) return rc;
-  PWB_CUDA(cudaMemcpy(c->gs_exx_tw.p, tw.data(), N * 16, cudaMemcpyHostToDevice));
+  if ((rc = upload_real(c, c->gs_exx_tw, tw.data(), 2 * (size_t)N))) return rc;   // complex, context precision
   c->exx_frac = frac;
   c->exx_mu = mu;
   c->exx_div = div;
   return PW_OK;
 }
 
-// out (+)= V_x psi for nb sphere bands
-int gs_exx_apply(pw_ctx* c, const void* psi_v, int ld, int nb, void* out_v, int ldo, int accumulate, cudaStream_t st) {
-  PWB_CHECK(c->prec == PW_F64, PW_EUNSUPPORTED, "G-space exact exchange is built for FP64 contexts");
+// out (+)= V_x psi for nb sphere bands, in the context's precision
+int gs_exx_apply(pw_ctx* c, const void* psi, int ld, int nb, void* out, int ldo, int accumulate, cudaStream_t st) {
   PWB_CHECK(c->gs_full_idx.p && c->exx_kern.p, PW_ENOTREADY, "exchange kernel not set (pw_exx_setup)");
-  const double* psi = (const double*)psi_v;
-  double* out = (double*)out_v;
-  const int N = c->nf[0];
-  const long n3 = (long)N * N * N;
-  const int nphi = c->exx_nphi;
   if (nb <= 0) return PW_OK;
-  if (nphi == 0) {
-    if (!accumulate) PWB_CUDA(cudaMemset2DAsync(out, (size_t)ldo * 8, 0, (size_t)c->ntot * 8, nb, st));
-    return PW_OK;
-  }
-  const int njp = (nphi + 1) / 2;
-  // fields per batch from the scratch budget (at least one band's pair fields)
-  // (gridDim.y of the axis-1 pass is N * fields: at most 65535)
-  const long fmax = 65535 / N;
-  PWB_CHECK(njp <= fmax, PW_EUNSUPPORTED, "G-space exact exchange: too many exchange orbitals for one band batch");
-  const long fcap = std::min<long>(fmax, std::max<long>(njp, (long)(c->exx_scratch_bytes / (size_t)(n3 * 16))));
-  const int kb = (int)std::max<long>(1, std::min<long>(nb, fcap / njp));
-  const int pcap = (int)std::max<long>(1, std::min<long>((std::max(nb, nphi) + 1) / 2, fcap));
-  // workspace kept in the context (reused while large enough); phi(r) is
-  // transformed once per pw_exx_set_phi
-  DevBuf &psir = c->gsx_psir, &phir = c->gsx_phir, &acc = c->gsx_acc, &F = c->gsx_fields;
-  int rc;
-  const size_t phib = (size_t)nphi * n3 * 8;
-  if (phir.bytes < phib) c->gsx_phi_ready = false;
-  if ((rc = psir.alloc((size_t)nb * n3 * 8)) || (rc = phir.alloc(phib)) || (rc = acc.alloc((size_t)nb * n3 * 8)) ||
-      (rc = F.alloc((size_t)std::max<long>((long)kb * njp, pcap) * n3 * 16)))
-    return rc;
-  double2* Z = (double2*)F.p;
-  if (!c->gsx_phi_ready) {
-    if ((rc = gs_to_real(c, (const double*)c->exx_phi.p, (int)c->ntot, nphi, 1.0, (double*)phir.p, Z, pcap, st)))
-      return rc;
-    c->gsx_phi_ready = true;
-  }
-  if ((rc = gs_to_real(c, psi, ld, nb, 1.0, (double*)psir.p, Z, pcap, st))) return rc;
-  PWB_CUDA(cudaMemsetAsync(acc.p, 0, (size_t)nb * n3 * 8, st));
-  for (int k0 = 0; k0 < nb; k0 += kb) {
-    const int kn = std::min(kb, nb - k0);
-    const int nf = kn * njp;
-    k_gsx_product<<<gs_blocks((long)nf * n3), 256, 0, st>>>((const double*)psir.p, (const double*)phir.p, k0, kn, njp,
-                                                            nphi, n3, 1.0 / (double)n3, Z);
-    if ((rc = fft3_fields_n(N, Z, nf, 2, (const double*)c->exx_kern.p, (const double2*)c->gs_exx_tw.p, st))) return rc;
-    k_gsx_accumulate<<<gs_blocks((long)kn * n3), 256, 0, st>>>(Z, (const double*)phir.p, (const double*)c->exx_w.p,
-                                                               k0, kn, njp, nphi, n3, (double*)acc.p);
-    c->launches += 7;
-  }
-  for (int b0 = 0; b0 < nb; b0 += 2 * pcap) {
-    const int np = std::min(pcap, (nb - b0 + 1) / 2);
-    k_gsx_pack<<<gs_blocks((long)np * n3), 256, 0, st>>>((const double*)acc.p, b0, nb, np, n3, Z);
-    if ((rc = fft3_fields_n(N, Z, np, 0, nullptr, (const double2*)c->gs_exx_tw.p, st))) return rc;
-    k_gsx_gather<<<gs_blocks((long)np * c->gs_ns), 256, 0, st>>>(Z, np, n3, (const int2*)c->gs_full_idx.p,
-                                                                 (int)c->gs_ns, b0, nb, out, ldo, accumulate);
-    c->launches += 5;
-  }
-  PWB_CUDA(cudaGetLastError());
-  return PW_OK;
+  if (c->prec == PW_F64)
+    return gs_exx_apply_t<double>(c, (const double*)psi, ld, nb, (double*)out, ldo, accumulate, st);
+  return gs_exx_apply_t<float>(c, (const float*)psi, ld, nb, (float*)out, ldo, accumulate, st);
 }
 
 }  // namespace pwb

@@ -1694,8 +1694,9 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
     snorm /= (double)nf * (double)nf;
     r->scf_norm = snorm;
     if (p->verbose)
-      fprintf(stderr, "SCF %3d %s Etot %.10f Efree %.10f Eharris %.10f dif %.3e scfnorm %.3e\n", it,
-              sv.c->prec == PW_F32 ? "f32" : "f64", etot, efree, eharris, dif, snorm);
+      fprintf(stderr, "SCF %3d %s Etot %.10f Efree %.10f Eharris %.10f dif %.3e scfnorm %.3e t %.4f s\n", it,
+              sv.c->prec == PW_F32 ? "f32" : "f64", etot, efree, eharris, dif, snorm,
+              std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count());
     PWB_CUDA(cudaMemcpy(rho, ro, nf * 8, cudaMemcpyDeviceToDevice));
     if (refined && (p->tol_rho > 0 ? snorm < p->tol_rho : dif < p->tol_efree)) { conv = true; break; }
     // switch the eigensolver to FP64 for the final iterations (iterative

@@ -1,9 +1,10 @@
 // Small dense FP64 algebra of the block eigensolvers on the device, written
 // for this library (the reference calls LAPACK on its rank 0):
 //   * upper Cholesky A = U^T U (EigenSolver::Orthogonalize's Potrf,
-//     src/EigenSolver/eigensolver.cpp:301-384), blocked right-looking:
-//     one CTA factors the diagonal block and solves its panel row, a grid of
-//     CTAs applies the rank-32 update to the trailing upper triangle;
+//     src/EigenSolver/eigensolver.cpp:301-384): in one CTA with the matrix in
+//     shared memory up to n = 160; beyond, blocked right-looking: one CTA
+//     factors the diagonal block and solves its panel row, a grid of CTAs
+//     applies the rank-32 update to the trailing upper triangle;
 //   * the inverse of an upper-triangular U (the Trsm of Orthogonalize applied
 //     to the identity), one CTA per column, column-oriented back substitution;
 //   * the symmetric eigen-decomposition (Syevd of SolveGenEig and of the final
@@ -120,8 +121,61 @@ __global__ void __launch_bounds__(256) k_chol_update(int n, double* A, int lda, 
   }
 }
 
+// the whole factorisation in one CTA for n <= CHOL1_NMAX, the upper triangle
+// in shared memory: per column one barrier after the scaled row is formed and
+// one after the trailing update (warp per row, upper part only)
+constexpr int CHOL1_NMAX = 160;
+__global__ void __launch_bounds__(1024) k_chol_small(int n, double* A, int lda, int* info) {
+  extern __shared__ __align__(16) double cs[];
+  const int P = n | 1;
+  double* W = cs;                  // W[i P + j] = A(i, j), i <= j
+  double* r = W + (size_t)n * P;   // row k of U
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+  for (int idx = tid; idx < n * n; idx += blockDim.x) {
+    const int i = idx % n, j = idx / n;
+    if (i <= j) W[i * P + j] = A[(long)j * lda + i];
+  }
+  __syncthreads();
+  for (int k = 0; k < n; ++k) {
+    const double dkk = W[k * P + k];
+    if (!(dkk > 0.0)) {
+      if (tid == 0) *info = k + 1;
+      return;
+    }
+    const double ukk = sqrt(dkk), inv = 1.0 / ukk;
+    for (int j = k + tid; j < n; j += blockDim.x) {
+      const double x = (j == k) ? ukk : W[k * P + j] * inv;
+      r[j] = x;
+      W[k * P + j] = x;
+    }
+    __syncthreads();
+    for (int i = k + 1 + wid; i < n; i += nw) {
+      const double ri = r[i];
+      double* wr = W + i * P;
+      for (int j = i + lane; j < n; j += 32) wr[j] -= ri * r[j];
+    }
+    __syncthreads();
+  }
+  for (int idx = tid; idx < n * n; idx += blockDim.x) {
+    const int i = idx % n, j = idx / n;
+    if (i <= j) A[(long)j * lda + i] = W[i * P + j];
+  }
+}
+
 int dense_potrf_upper(int n, double* A, int lda, int* info_dev, cudaStream_t st) {
   PWB_CUDA(cudaMemsetAsync(info_dev, 0, sizeof(int), st));
+  if (n <= CHOL1_NMAX) {
+    static PerDeviceOnce attr;
+    const size_t smax = ((size_t)CHOL1_NMAX * (CHOL1_NMAX | 1) + CHOL1_NMAX) * sizeof(double);
+    if (!attr.done()) {
+      PWB_CUDA(cudaFuncSetAttribute(k_chol_small, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax));
+      attr.mark();
+    }
+    if (n > 0)
+      k_chol_small<<<1, 1024, ((size_t)n * (n | 1) + n) * sizeof(double), st>>>(n, A, lda, info_dev);
+    PWB_CUDA(cudaGetLastError());
+    return PW_OK;
+  }
   for (int k0 = 0; k0 < n; k0 += CHOL_NB) {
     k_chol_panel<<<1, 256, 0, st>>>(n, A, lda, k0, info_dev);
     const int k1 = std::min(n, k0 + CHOL_NB);
@@ -428,7 +482,7 @@ __global__ void __launch_bounds__(256) k_jacobi_vectors(int n, double* A, int ld
 // Symmetric eigen-decomposition through the tridiagonal form (n <= TRD_NMAX):
 //   1. Householder reduction A = Q T Q^T in one CTA, the matrix in shared
 //      memory (lower form: reflector k zeroes column k below the subdiagonal,
-//      H_k = I - tau_k v_k v_k^T with v_k(k+1) = 1);
+//      H_k = I - tau_k v_k v_k^T with v_k(k+1) = 1), two barriers per column;
 //   2. all eigenvalues of T by multisection on Sturm counts: one warp per
 //      eigenvalue counts at 32 points of its bracket per step (a step shrinks
 //      the bracket 33-fold; 11 steps reach the rounding level);
@@ -471,10 +525,8 @@ __global__ void __launch_bounds__(TRD_THREADS) k_trd_reduce(int n, const double*
   extern __shared__ __align__(16) double trd_sm[];
   const int P = n | 1;
   double* W = trd_sm;                  // W[i P + j] = A(i, j), full symmetric
-  double* v = W + (size_t)n * P;       // reflector (rows k+1 .. n-1)
-  double* p = v + n;                   // tau A v, then w
+  double* p = W + (size_t)n * P;       // tau A v of the current step
   double* zrow = p + n;                // a row of zeros: the rows of a warp past n point here
-  __shared__ double s_tk;
   double* V = ws;
   double* d = ws + 2 * (size_t)n * n;
   double* e = d + n;
@@ -487,54 +539,70 @@ __global__ void __launch_bounds__(TRD_THREADS) k_trd_reduce(int n, const double*
   }
   for (int j = tid; j < n; j += blockDim.x) zrow[j] = 0.0;
   __syncthreads();
+  // Step k, two barriers.  Every warp forms the reflector of row k (= column
+  // k, the matrix stays symmetric) itself: its lanes hold v at the columns
+  // j_t = k+1+lane+32t, and v at its own rows i_m = k+1+wid+32m.  The warps
+  // then form p = tau A22 v on their rows (barrier), and each warp the update
+  // A22 -= v w^T + w v^T on its rows with w = p - (tau/2)(p.v) v formed from p
+  // in registers (barrier).
   for (int k = 0; k + 2 < n; ++k) {
-    // warp 0: the reflector of column k (the other warps wait at the barrier)
+    const double* rk = W + k * P;
+    double vj[TRD_RPW];
+    double s = 0.0;
+#pragma unroll
+    for (int t = 0; t < TRD_RPW; ++t) {
+      const int j = k + 1 + lane + 32 * t;
+      const double x = j < n ? rk[j] : 0.0;
+      vj[t] = x;
+      if (j >= k + 2) s += x * x;
+    }
+    s = warp_sum_d(s);
+    const double alpha = rk[k + 1];
+    double tk = 0.0, beta = alpha, scal = 0.0;
+    if (s != 0.0) {
+      const double mu = sqrt(alpha * alpha + s);
+      beta = alpha <= 0.0 ? mu : -mu;
+      tk = (beta - alpha) / beta;
+      scal = 1.0 / (alpha - beta);
+    }
+#pragma unroll
+    for (int t = 0; t < TRD_RPW; ++t) {
+      const int j = k + 1 + lane + 32 * t;
+      vj[t] = j == k + 1 ? 1.0 : vj[t] * scal;
+    }
     if (wid == 0) {
-      double s = 0;
-      for (int i = k + 2 + lane; i < n; i += 32) {
-        const double x = W[i * P + k];
-        s += x * x;
-      }
-      s = warp_sum_d(s);
-      const double alpha = W[(k + 1) * P + k];
-      double tk = 0.0, beta = alpha, scal = 0.0;
-      if (s != 0.0) {
-        const double mu = sqrt(alpha * alpha + s);
-        beta = alpha <= 0.0 ? mu : -mu;
-        tk = (beta - alpha) / beta;
-        scal = 1.0 / (alpha - beta);
-      }
-      for (int i = k + 1 + lane; i < n; i += 32) {
-        const double vi = (i == k + 1) ? 1.0 : W[i * P + k] * scal;
-        v[i] = vi;
-        V[(long)k * n + i] = vi;
+#pragma unroll
+      for (int t = 0; t < TRD_RPW; ++t) {
+        const int j = k + 1 + lane + 32 * t;
+        if (j < n) V[(long)k * n + j] = vj[t];
       }
       if (lane == 0) {
-        d[k] = W[k * P + k];
+        d[k] = rk[k];
         e[k] = beta;
         tau[k] = tk;
-        s_tk = tk;
       }
     }
-    __syncthreads();
-    const double tk = s_tk;
-    if (tk == 0.0) continue;
-    // p = tau A22 v: warp wid owns rows k+1+wid+32m (rows past n read the
-    // zero row), their sums interleaved
+    if (tk == 0.0) continue;          // nothing to update; W is unchanged (every warp agrees)
     double* wr[TRD_RPW];
+    double vi[TRD_RPW];
 #pragma unroll
     for (int m = 0; m < TRD_RPW; ++m) {
       const int i = k + 1 + wid + 32 * m;
       wr[m] = i < n ? W + i * P : zrow;
+      vi[m] = i < n ? (i == k + 1 ? 1.0 : rk[i] * scal) : 0.0;
     }
+    // p = tau A22 v on the warp's rows, the row sums interleaved
     {
       double acc[TRD_RPW];
 #pragma unroll
       for (int m = 0; m < TRD_RPW; ++m) acc[m] = 0.0;
-      for (int j = k + 1 + lane; j < n; j += 32) {
-        const double vj = v[j];
 #pragma unroll
-        for (int m = 0; m < TRD_RPW; ++m) acc[m] += wr[m][j] * vj;
+      for (int t = 0; t < TRD_RPW; ++t) {
+        const int j = k + 1 + lane + 32 * t;
+        if (j < n) {
+#pragma unroll
+          for (int m = 0; m < TRD_RPW; ++m) acc[m] += wr[m][j] * vj[t];
+        }
       }
 #pragma unroll
       for (int m = 0; m < TRD_RPW; ++m) acc[m] = warp_sum_d(acc[m]);
@@ -547,28 +615,31 @@ __global__ void __launch_bounds__(TRD_THREADS) k_trd_reduce(int n, const double*
       }
     }
     __syncthreads();
-    // warp 0: w = p - (tau/2) (p.v) v
-    if (wid == 0) {
-      double t = 0;
-      for (int i = k + 1 + lane; i < n; i += 32) t += p[i] * v[i];
-      t = warp_sum_d(t);
-      const double kc = 0.5 * tk * t;
-      for (int i = k + 1 + lane; i < n; i += 32) p[i] -= kc * v[i];
-    }
-    __syncthreads();
-    // A22 -= v w^T + w v^T on the same rows (the zero row gets 0 v + 0 w)
+    // w = p - (tau/2)(p.v) v, then A22 -= v w^T + w v^T on the warp's rows
     {
-      double vi[TRD_RPW], pi[TRD_RPW];
+      double pj[TRD_RPW];
+      double t2 = 0.0;
+#pragma unroll
+      for (int t = 0; t < TRD_RPW; ++t) {
+        const int j = k + 1 + lane + 32 * t;
+        pj[t] = j < n ? p[j] : 0.0;
+        t2 += pj[t] * vj[t];
+      }
+      const double kc = 0.5 * tk * warp_sum_d(t2);
+      double wi[TRD_RPW];
 #pragma unroll
       for (int m = 0; m < TRD_RPW; ++m) {
         const int i = k + 1 + wid + 32 * m;
-        vi[m] = i < n ? v[i] : 0.0;
-        pi[m] = i < n ? p[i] : 0.0;
+        wi[m] = i < n ? p[i] - kc * vi[m] : 0.0;
       }
-      for (int j = k + 1 + lane; j < n; j += 32) {
-        const double vj = v[j], pj = p[j];
 #pragma unroll
-        for (int m = 0; m < TRD_RPW; ++m) wr[m][j] -= vi[m] * pj + pi[m] * vj;
+      for (int t = 0; t < TRD_RPW; ++t) {
+        const int j = k + 1 + lane + 32 * t;
+        if (j < n) {
+          const double wj = pj[t] - kc * vj[t];
+#pragma unroll
+          for (int m = 0; m < TRD_RPW; ++m) wr[m][j] -= vi[m] * wj + wi[m] * vj[t];
+        }
       }
     }
     __syncthreads();
@@ -717,6 +788,8 @@ __global__ void __launch_bounds__(32 * TRD_WARPS_STEIN) k_trd_stein(int n, doubl
         }
       }
       u[n - 1] = fabs(ak) < eps ? (ak < 0.0 ? -eps : eps) : ak;
+      s1[n - 1] = 0.0;       // read (times zero) by the register-carried back substitution
+      s2[n - 1] = 0.0;
       // the solves multiply by the pivots' reciprocals (tiny pivots raised to eps)
       for (int k = 0; k < n; ++k) {
         const double uk = u[k];
@@ -727,19 +800,29 @@ __global__ void __launch_bounds__(32 * TRD_WARPS_STEIN) k_trd_stein(int n, doubl
     __syncwarp();
     for (int it = 0; it < 3; ++it) {
       if (lane == 0) {
+        // the running values stay in registers: one FMA (forward) or two
+        // FMAs and a product (backward) per step on the dependency chain
+        double yk = y[0];
+#pragma unroll 4
         for (int k = 0; k + 1 < n; ++k) {
+          double yn = y[k + 1];
           if (sw[k] != 0.0) {
-            const double t = y[k];
-            y[k] = y[k + 1];
-            y[k + 1] = t;
+            const double t = yk;
+            yk = yn;
+            yn = t;
           }
-          y[k + 1] -= l[k] * y[k];
+          yn -= l[k] * yk;
+          y[k] = yk;
+          yk = yn;
         }
+        y[n - 1] = yk;
+        double y1 = 0.0, y2 = 0.0;   // y[k+1], y[k+2] (zero past the end)
+#pragma unroll 4
         for (int k = n - 1; k >= 0; --k) {
-          double t = y[k];
-          if (k + 1 < n) t -= s1[k] * y[k + 1];
-          if (k + 2 < n) t -= s2[k] * y[k + 2];
-          y[k] = t * u[k];
+          const double t = (y[k] - s1[k] * y1 - s2[k] * y2) * u[k];
+          y[k] = t;
+          y2 = y1;
+          y1 = t;
         }
       }
       __syncwarp();
@@ -824,7 +907,7 @@ int dense_syevh(int n, double* A, int lda, double* w, DevBuf& ws, cudaStream_t s
   int rc;
   if ((rc = ws.alloc(trd_ws(n) * sizeof(double)))) return rc;
   static PerDeviceOnce attr;
-  const size_t sm_red = ((size_t)TRD_NMAX * (TRD_NMAX | 1) + 3 * TRD_NMAX) * sizeof(double);
+  const size_t sm_red = ((size_t)TRD_NMAX * (TRD_NMAX | 1) + 2 * TRD_NMAX) * sizeof(double);
   const size_t sm_st = (size_t)TRD_WARPS_STEIN * 6 * TRD_NMAX * sizeof(double);
   if (!attr.done()) {
     PWB_CUDA(cudaFuncSetAttribute(k_trd_reduce, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_red));
@@ -832,7 +915,7 @@ int dense_syevh(int n, double* A, int lda, double* w, DevBuf& ws, cudaStream_t s
     attr.mark();
   }
   double* wsp = (double*)ws.p;
-  k_trd_reduce<<<1, TRD_THREADS, ((size_t)n * (n | 1) + 3 * (size_t)n) * sizeof(double), st>>>(n, A, lda, wsp);
+  k_trd_reduce<<<1, TRD_THREADS, ((size_t)n * (n | 1) + 2 * (size_t)n) * sizeof(double), st>>>(n, A, lda, wsp);
   k_trd_bisect<<<(n + TRD_BIS_WARPS - 1) / TRD_BIS_WARPS, 32 * TRD_BIS_WARPS, 0, st>>>(n, wsp, w);
   k_trd_stein<<<(n + TRD_WARPS_STEIN - 1) / TRD_WARPS_STEIN, 32 * TRD_WARPS_STEIN,
                 (size_t)TRD_WARPS_STEIN * 6 * n * sizeof(double), st>>>(n, wsp, w);
