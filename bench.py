@@ -374,7 +374,7 @@ def scf_bench(device: int, max_iter: int = 60):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
             r_, eig_, _ = c.scf(cheby_first_cycles=5, tol_efree=1e-6, refine_threshold=3e-6, max_iter=max_iter,
-                                verbose=1 if os.environ.get("PWB_SCF_VERBOSE") else 0, **kw)
+                                verbose=int(os.environ.get("PWB_SCF_VERBOSE", "0")), **kw)
             e1.record()
             torch.cuda.synchronize()
             samples.append(e0.elapsed_time(e1) / 1e3)

@@ -318,7 +318,8 @@ typedef struct pw_scf_params {
   int max_iter;             /* SCF_Outer_MaxIter */
   int mix_dim;              /* Mixing_MaxDim */
   int mixed;                /* 1: FP32 H*psi / split-BF16 Gram eigensolver, FP64 refinement */
-  int verbose;
+  int verbose;              /* 1: a line per SCF iteration (stderr); 2: phase timers (graphs off);
+                               3: as 1 plus the synchronised wall time of each step */
   double ecut;              /* Ecut_Wavefunction (Hartree cut-off 4*Ecut) */
   double temperature;       /* Kelvin, Fermi-Dirac */
   double eig_tol;           /* Eig_Tolerance */
@@ -346,8 +347,8 @@ typedef struct pw_scf_result {
   double etot, efree, eharris, exc, ehart, eself, fermi, time_s;
   int iterations, converged, refine_iter;
   long hpsi_bands;          /* single-band H*psi applications performed */
-  double phase_s[6];        /* verbose >= 2: eigensolver, density, potentials, set-up, mixing, refine switch (s) */
-  double sub_s[4];          /* verbose >= 2, inside the eigensolver: H*psi, Gram, dense FP64, rotations (s) */
+  double phase_s[6];        /* verbose == 2: eigensolver, density, potentials, set-up, mixing, refine switch (s) */
+  double sub_s[4];          /* verbose == 2, inside the eigensolver: H*psi, Gram, dense FP64, rotations (s) */
   double scf_norm;          /* last SCF::CalculateError of the output-density change (scf.cpp:2368-2396) */
   double efock;             /* PW_XC_HSE06: exchange energy of the last ACE (Efock, included in etot / efree) */
   double dexx;              /* PW_XC_HSE06: last dExx */

@@ -176,6 +176,86 @@ template <int DIR, typename V> struct DFT<5, DIR, V> {
   }
 };
 
+// DFT of R elements in registers whose inputs in the bit mask ZM are known,
+// at compile time, to be zero (the padded slots of a coarse spectrum): the
+// butterflies that would add a known zero are not emitted.  Same result as
+// DFT<R, DIR, V> up to the sign of zero results.
+template <int R, int DIR, typename V, unsigned ZM> struct DFTZ {
+  static constexpr unsigned ALL = (1u << R) - 1u;
+  static constexpr unsigned Z = ZM & ALL;
+  static __device__ __forceinline__ void run(V* v) {
+    if constexpr (Z == 0) {
+      DFT<R, DIR, V>::run(v);
+    } else if constexpr (Z == ALL) {
+      sfor<0, R>([&](auto kI) { v[decltype(kI)::value] = mkc<V>(0, 0); });
+    } else if constexpr (R == 2) {
+      // one of the two inputs is zero
+      if constexpr (Z & 1u) {
+        const V b = v[1];
+        v[0] = b;
+        v[1] = mkc<V>(-b.x, -b.y);
+      } else {
+        v[1] = v[0];
+      }
+    } else if constexpr (FirstFactor<R>::v == R) {
+      // prime length: direct sum over the inputs that can be nonzero
+      V out[R];
+      sfor<0, R>([&](auto kI) {
+        constexpr int k = decltype(kI)::value;
+        V acc = mkc<V>(0, 0);
+        bool first = true;
+        sfor<0, R>([&](auto nI) {
+          constexpr int n = decltype(nI)::value;
+          if constexpr (!((Z >> n) & 1u)) {
+            const V term = twmul<R, n * k, DIR>(v[n]);
+            acc = first ? term : cadd(acc, term);
+            first = false;
+          }
+        });
+        out[k] = acc;
+      });
+      sfor<0, R>([&](auto kI) { v[decltype(kI)::value] = out[decltype(kI)::value]; });
+    } else {
+      constexpr int A = FirstFactor<R>::v;
+      constexpr int B = R / A;
+      V t[R];
+      sfor<0, B>([&](auto bI) {
+        constexpr int b = decltype(bI)::value;
+        constexpr unsigned sub = [] {
+          unsigned m = 0;
+          for (int a = 0; a < A; ++a)
+            if ((Z >> (B * a + b)) & 1u) m |= 1u << a;
+          return m;
+        }();
+        V a_[A];
+        sfor<0, A>([&](auto aI) { a_[decltype(aI)::value] = v[B * decltype(aI)::value + b]; });
+        DFTZ<A, DIR, V, sub>::run(a_);
+        sfor<0, A>([&](auto kaI) {
+          constexpr int ka = decltype(kaI)::value;
+          t[ka * B + b] = twmul<R, b * ka, DIR>(a_[ka]);
+        });
+      });
+      // a first-stage transform whose inputs were all zero gives zeros
+      constexpr unsigned zb = [] {
+        unsigned m = 0;
+        for (int b = 0; b < B; ++b) {
+          bool all = true;
+          for (int a = 0; a < A; ++a) all = all && ((Z >> (B * a + b)) & 1u);
+          if (all) m |= 1u << b;
+        }
+        return m;
+      }();
+      sfor<0, A>([&](auto kaI) {
+        constexpr int ka = decltype(kaI)::value;
+        V c_[B];
+        sfor<0, B>([&](auto bI) { c_[decltype(bI)::value] = t[ka * B + decltype(bI)::value]; });
+        DFTZ<B, DIR, V, zb>::run(c_);
+        sfor<0, B>([&](auto kbI) { v[ka + A * decltype(kbI)::value] = c_[decltype(kbI)::value]; });
+      });
+    }
+  }
+};
+
 // Length split used for each supported 1D size (N1 <= 16, N2 <= 16).
 template <int N> struct Split;
 #define PWB_SPLIT(N_, N1_) template <> struct Split<N_> { static constexpr int n1 = N1_; };
@@ -246,7 +326,11 @@ __device__ __forceinline__ void smem_fft(V* base, int count, int es, int bs, con
 // addresses fold to 32-bit immediates.  FB puts the transform index on the
 // fastest lanes of the first pass (lane -> (f = it % F, j2 = it / F)), which
 // spreads a warp's accesses over more banks when BS is small against ES.
-template <int N, int DIR, int ES, int BS, bool FB = false, typename V>
+// ZIN: first-pass inputs j1 (elements N2 j1 + j2) known to be zero for every
+// j2, not read and pruned from the register transforms; DOUT: second-pass
+// outputs k2 (elements k1 + N1 k2) never read afterwards, not written (and so
+// not computed).  Both 0: the plain transform.
+template <int N, int DIR, int ES, int BS, bool FB = false, unsigned ZIN = 0u, unsigned DOUT = 0u, typename V>
 __device__ __forceinline__ void smem_fft_c(V* base, int count, const V* tw, int warp, int nw) {
   constexpr int N1 = Split<N>::n1;
   constexpr int N2 = N / N1;
@@ -263,9 +347,12 @@ __device__ __forceinline__ void smem_fft_c(V* base, int count, const V* tw, int 
       if (it < F * N2 && b < count) {
         V* p = base + b * BS + j2 * ES;
         V t[N1];
-#pragma unroll
-        for (int j1 = 0; j1 < N1; ++j1) t[j1] = p[N2 * j1 * ES];
-        DFT<N1, DIR, V>::run(t);
+        sfor<0, N1>([&](auto jI) {
+          constexpr int j1 = decltype(jI)::value;
+          if constexpr ((ZIN >> j1) & 1u) t[j1] = mkc<V>(0, 0);
+          else t[j1] = p[N2 * j1 * ES];
+        });
+        DFTZ<N1, DIR, V, ZIN>::run(t);
 #pragma unroll
         for (int k1 = 1; k1 < N1; ++k1) {
           V w = tw[j2 * k1];
@@ -287,16 +374,18 @@ __device__ __forceinline__ void smem_fft_c(V* base, int count, const V* tw, int 
     }
     __syncwarp();
     if (act) {
-#pragma unroll
-      for (int k2 = 0; k2 < N2; ++k2) p[(k1_2 + N1 * k2) * ES] = u[k2];
+      sfor<0, N2>([&](auto kI) {
+        constexpr int k2 = decltype(kI)::value;
+        if constexpr (!((DOUT >> k2) & 1u)) p[(k1_2 + N1 * k2) * ES] = u[k2];
+      });
     }
     __syncwarp();
   }
 }
 
-template <int N, int DIR, int ES, int BS, bool FB = false, typename V>
+template <int N, int DIR, int ES, int BS, bool FB = false, unsigned ZIN = 0u, unsigned DOUT = 0u, typename V>
 __device__ __forceinline__ void smem_fft_cb(V* base, int count, const V* tw) {
-  smem_fft_c<N, DIR, ES, BS, FB>(base, count, tw, (int)(threadIdx.x >> 5), (int)(blockDim.x >> 5));
+  smem_fft_c<N, DIR, ES, BS, FB, ZIN, DOUT>(base, count, tw, (int)(threadIdx.x >> 5), (int)(blockDim.x >> 5));
 }
 
 // Second radix decomposition N = n1 x (N / n1) of the longer lengths, the

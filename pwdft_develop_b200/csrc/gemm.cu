@@ -450,8 +450,17 @@ __global__ void k_splitk_reduce(const float* __restrict__ ws, int nsplit, int M,
   // computed; its mirror (n, m) was
   const bool mirror = sym_bn > 0 && (n / sym_bn) * sym_bn + sym_bn <= (m / GM) * GM;
   const long src = mirror ? (long)m * M + n : (long)n * M + m;
-  double s = 0;
-  for (int k = 0; k < nsplit; ++k) s += (double)ws[(long)k * N * M + src];
+  // four interleaved partial sums (a fixed order: deterministic), eight loads in flight
+  const long stride = (long)N * M;
+  double s4[4] = {0, 0, 0, 0};
+  int k = 0;
+#pragma unroll 2
+  for (; k + 4 <= nsplit; k += 4) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) s4[q] += (double)ws[(long)(k + q) * stride + src];
+  }
+  for (; k < nsplit; ++k) s4[0] += (double)ws[(long)k * stride + src];
+  double s = (s4[0] + s4[1]) + (s4[2] + s4[3]);
   if (rs) s *= rs[m];
   if (cs) s *= cs[n];
   const long o = transpose ? (long)n * ldo + m : (long)m * ldo + n;

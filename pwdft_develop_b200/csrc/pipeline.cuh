@@ -82,6 +82,37 @@ __device__ __forceinline__ int slot_fine(int s, int n, int nf) {
   return (m + nf) % nf;
 }
 
+// fine index e of a length-N axis -> slot (coarse size n = N/2), -1 if none;
+// slot n is the "-" Nyquist partner at fine index N - n/2
+template <int N> __host__ __device__ constexpr int fine_slot(int e) {
+  constexpr int n = N / 2, h = n / 2;
+  return e <= h ? e : (e > N - h ? e - N + n : (e == N - h ? n : -1));
+}
+// whether any fine index in [lo, lo + cnt) of a length-N axis has a slot: the
+// transform stages of k_floc2 skip, at compile time, inputs known to be zero
+// and outputs known to be discarded
+template <int N> constexpr bool any_slot(int lo, int cnt) {
+  for (int e = lo; e < lo + cnt; ++e)
+    if (fine_slot<N>(e) >= 0) return true;
+  return false;
+}
+// inputs j1 of the first stage (fine index N2 j1 + j2, j2 < N2) that are
+// zero for every j2, as a bit mask
+template <int N, int N1, int N2> constexpr unsigned zero_inputs() {
+  unsigned m = 0;
+  for (int j1 = 0; j1 < N1; ++j1)
+    if (!any_slot<N>(N2 * j1, N2)) m |= 1u << j1;
+  return m;
+}
+// outputs k2 of the second stage (fine index k1 + N1 k2, k1 < N1) that are no
+// slot for any k1, as a bit mask
+template <int N, int N1, int N2> constexpr unsigned dead_outputs() {
+  unsigned m = 0;
+  for (int k2 = 0; k2 < N2; ++k2)
+    if (!any_slot<N>(N1 * k2, N1)) m |= 1u << k2;
+  return m;
+}
+
 template <typename V>
 __device__ __forceinline__ void load_tw(V* dst, const V* src, int n) {
   for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
@@ -282,7 +313,9 @@ k_zpad(const VT<T>* __restrict__ A, VT<T>* __restrict__ K, VT<T>* __restrict__ B
     }
   }
   __syncthreads();
-  smem_fft_cb<NZF, +1, PO, 1>(out, m.ncols, twzf);
+  // the padded rows between the coarse halves are zero: the first pass of the
+  // fine transform skips them
+  smem_fft_cb<NZF, +1, PO, 1, false, zero_inputs<NZF, Split<NZF>::n1, NZF / Split<NZF>::n1>()>(out, m.ncols, twzf);
   __syncthreads();
   V* Bp = B + (long)p * NZF * nsy * nsx;
   const long fplane = (long)nsy * nsx;
@@ -654,13 +687,6 @@ k_floc(VT<T>* __restrict__ BC, const T* __restrict__ vtot, const T* __restrict__
 //  * the y forward transform's second pass writes the slot rows of C
 //    directly (x 1/N_fine).
 // ---------------------------------------------------------------------------
-// fine index e of a length-N axis -> slot (coarse size n = N/2), -1 if none;
-// slot n is the "-" Nyquist partner at fine index N - n/2
-template <int N> __device__ __forceinline__ int fine_slot(int e) {
-  constexpr int n = N / 2, h = n / 2;
-  return e <= h ? e : (e > N - h ? e - N + n : (e == N - h ? n : -1));
-}
-
 // Shared-memory layout of k_floc2: S tile (slot columns of the fine plane)
 // with row y at y PS + SKS (y / NY2), per-warp row buffers with element e of
 // row f at f PR + e + SKR (e / NX2), and whether the first pass of the column
@@ -745,7 +771,7 @@ k_floc2(VT<T>* __restrict__ BC, const T* __restrict__ vtot, T inv_nf, const VT<T
   constexpr bool RTW = VAR == 2;
   constexpr int NX1 = SplitVar<NXF, VAR>::n1, NX2 = NXF / NX1, FX = 32 / NX1;
   constexpr int NY1 = SplitVar<NYF, VAR>::n1, NY2 = NYF / NY1, FY = 32 / NY1;
-  constexpr int RX = (FX * NX2 + 31) / 32, RY = (FY * NY2 + 31) / 32;
+  constexpr int RX = (FX * NX2 + 31) / 32;
   static_assert(PS >= nsx && PR >= NXF + SKR * (NX1 - 1), "k_floc2 layout rows overlap");
   extern __shared__ __align__(16) unsigned char smraw[];
   V* S = reinterpret_cast<V*>(smraw);          // row y at y PS + SKS (y / NY2)
@@ -761,20 +787,27 @@ k_floc2(VT<T>* __restrict__ BC, const T* __restrict__ vtot, T inv_nf, const VT<T
   __syncthreads();
 
   // A: inverse y transform of the nsx slot columns
-  for (int g = warp * FY; g < nsx; g += nw * FY) {
+  constexpr int GA = FY;
+  constexpr int RA = (GA * NY2 + 31) / 32;
+  for (int g = warp * GA; g < nsx; g += nw * GA) {
 #pragma unroll
-    for (int r = 0; r < RY; ++r) {
+    for (int r = 0; r < RA; ++r) {
       const int it = lane + 32 * r;
-      const int f = FA ? it % FY : it / NY2, j2 = FA ? it / FY : it - f * NY2;
+      const int f = FA ? it % GA : it / NY2, j2 = FA ? it / GA : it - f * NY2;
       const int c = g + f;
-      if (it < FY * NY2 && c < nsx) {
+      if (it < GA * NY2 && c < nsx) {
         V t[NY1];
-#pragma unroll
-        for (int j1 = 0; j1 < NY1; ++j1) {
-          const int s = fine_slot<NYF>(NY2 * j1 + j2);
-          t[j1] = s >= 0 ? Bp[s * nsx + c] : mkc<V>(0, 0);
-        }
-        DFT<NY1, +1, V>::run(t);
+        sfor<0, NY1>([&](auto jI) {
+          constexpr int j1 = decltype(jI)::value;
+          if constexpr (!RTW || any_slot<NYF>(NY2 * j1, NY2)) {
+            const int s = fine_slot<NYF>(NY2 * j1 + j2);
+            t[j1] = s >= 0 ? Bp[s * nsx + c] : mkc<V>(0, 0);
+          } else {
+            t[j1] = mkc<V>(0, 0);
+          }
+        });
+        if constexpr (RTW) DFTZ<NY1, +1, V, zero_inputs<NYF, NY1, NY2>()>::run(t);
+        else DFT<NY1, +1, V>::run(t);
         if constexpr (RTW) {
           V p_[NY1];
           V w = twy[j2];
@@ -795,9 +828,10 @@ k_floc2(VT<T>* __restrict__ BC, const T* __restrict__ vtot, T inv_nf, const VT<T
       }
     }
     __syncwarp();
-    {
+#pragma unroll
+    for (int h = 0; h < GA / FY; ++h) {
       const int f = lane / NY1, k1 = lane - f * NY1;
-      const int c = g + f;
+      const int c = g + h * FY + f;
       const bool act = lane < FY * NY1 && c < nsx;
       V u[NY2];
       if (act) {
@@ -829,12 +863,17 @@ k_floc2(VT<T>* __restrict__ BC, const T* __restrict__ vtot, T inv_nf, const VT<T
       if (it < FX * NX2 && f < nr) {
         V t[NX1];
         const V* srow = S + (r0 + f) * PS + SKS * ((r0 + f) / NY2);
-#pragma unroll
-        for (int j1 = 0; j1 < NX1; ++j1) {
-          const int s = fine_slot<NXF>(NX2 * j1 + j2);
-          t[j1] = s >= 0 ? srow[s] : mkc<V>(0, 0);
-        }
-        DFT<NX1, +1, V>::run(t);
+        sfor<0, NX1>([&](auto jI) {
+          constexpr int j1 = decltype(jI)::value;
+          if constexpr (!RTW || any_slot<NXF>(NX2 * j1, NX2)) {
+            const int s = fine_slot<NXF>(NX2 * j1 + j2);
+            t[j1] = s >= 0 ? srow[s] : mkc<V>(0, 0);
+          } else {
+            t[j1] = mkc<V>(0, 0);
+          }
+        });
+        if constexpr (RTW) DFTZ<NX1, +1, V, zero_inputs<NXF, NX1, NX2>()>::run(t);
+        else DFT<NX1, +1, V>::run(t);
         if constexpr (RTW) {
           V p_[NX1];
           V w = twx[j2];
@@ -911,11 +950,13 @@ k_floc2(VT<T>* __restrict__ BC, const T* __restrict__ vtot, T inv_nf, const VT<T
         for (int k1 = 0; k1 < NX1; ++k1) t[k1] = Rw[f * PR + (NX2 + SKR) * k1 + m2];
         DFT<NX1, -1, V>::run(t);                    // forward, second stage over k1
         V* srow = S + (r0 + f) * PS + SKS * ((r0 + f) / NY2);
-#pragma unroll
-        for (int m1 = 0; m1 < NX1; ++m1) {
-          const int s = fine_slot<NXF>(m2 + NX2 * m1);
-          if (s >= 0) srow[s] = t[m1];
-        }
+        sfor<0, NX1>([&](auto mI) {
+          constexpr int m1 = decltype(mI)::value;
+          if constexpr (!RTW || any_slot<NXF>(NX2 * m1, NX2)) {
+            const int s = fine_slot<NXF>(m2 + NX2 * m1);
+            if (s >= 0) srow[s] = t[m1];
+          }
+        });
       }
     }
     __syncwarp();
@@ -923,13 +964,13 @@ k_floc2(VT<T>* __restrict__ BC, const T* __restrict__ vtot, T inv_nf, const VT<T
   __syncthreads();
 
   // C: forward y transform of the slot columns, slot rows straight to C
-  for (int g = warp * FY; g < nsx; g += nw * FY) {
+  for (int g = warp * GA; g < nsx; g += nw * GA) {
 #pragma unroll
-    for (int r = 0; r < RY; ++r) {
+    for (int r = 0; r < RA; ++r) {
       const int it = lane + 32 * r;
-      const int f = FA ? it % FY : it / NY2, j2 = FA ? it / FY : it - f * NY2;
+      const int f = FA ? it % GA : it / NY2, j2 = FA ? it / GA : it - f * NY2;
       const int c = g + f;
-      if (it < FY * NY2 && c < nsx) {
+      if (it < GA * NY2 && c < nsx) {
         V t[NY1];
 #pragma unroll
         for (int j1 = 0; j1 < NY1; ++j1) t[j1] = S[(NY2 * j1 + j2) * PS + SKS * j1 + c];
@@ -948,19 +989,22 @@ k_floc2(VT<T>* __restrict__ BC, const T* __restrict__ vtot, T inv_nf, const VT<T
       }
     }
     __syncwarp();
-    {
+#pragma unroll
+    for (int h = 0; h < GA / FY; ++h) {
       const int f = lane / NY1, k1 = lane - f * NY1;
-      const int c = g + f;
+      const int c = g + h * FY + f;
       if (lane < FY * NY1 && c < nsx) {
         V u[NY2];
 #pragma unroll
         for (int j2 = 0; j2 < NY2; ++j2) u[j2] = S[(NY2 * k1 + j2) * PS + SKS * k1 + c];
         DFT<NY2, -1, V>::run(u);
-#pragma unroll
-        for (int k2 = 0; k2 < NY2; ++k2) {
-          const int s = fine_slot<NYF>(k1 + NY1 * k2);
-          if (s >= 0) Bp[s * nsx + c] = cscale(u[k2], inv_nf);
-        }
+        sfor<0, NY2>([&](auto kI) {
+          constexpr int k2 = decltype(kI)::value;
+          if constexpr (!RTW || any_slot<NYF>(NY1 * k2, NY1)) {
+            const int s = fine_slot<NYF>(k1 + NY1 * k2);
+            if (s >= 0) Bp[s * nsx + c] = cscale(u[k2], inv_nf);
+          }
+        });
       }
     }
     __syncwarp();
@@ -1179,7 +1223,9 @@ k_zfold(const VT<T>* __restrict__ C, const VT<T>* __restrict__ K, VT<T>* __restr
   }
   cp_async_wait_all();
   __syncthreads();
-  smem_fft_cb<NZF, -1, PI, 1>(in, m.ncols, twzf);
+  // only the fine rows that fold onto the coarse spectrum are read afterwards
+  smem_fft_cb<NZF, -1, PI, 1, false, 0u, dead_outputs<NZF, Split<NZF>::n1, NZF / Split<NZF>::n1>()>(in, m.ncols,
+                                                                                                 twzf);
   __syncthreads();
   if (deriv == 3) {
     // spectral d/dz before the fold: multiply by i G_z of the fine frequency

@@ -396,6 +396,7 @@ struct Solver {
   int s_nb = 0, s_m = 0, s_calls = 0;
   bool s_off = false;       // capture failed once: the step runs directly
   DevBuf bup;               // upper bound of the spectrum (device scalar)
+  DevBuf x32;               // the FP32 block at the switch to FP64 (mixed precision)
   double bup_host = 0.0;
   void drop_graphs() {
     if (fexec) cudaGraphExecDestroy(fexec);
@@ -1377,7 +1378,7 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
       c->wfn_filter = false;
     }
   }
-  const bool prof = p->verbose >= 2;
+  const bool prof = p->verbose == 2;
   g_sub_on = prof;
   for (double& x : g_sub) x = 0;
   double tph[6] = {0, 0, 0, 0, 0, 0};   // eigensolver, density, potentials, set-up, mixing, refine switch
@@ -1561,18 +1562,30 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
   bool conv = false;
   r->hpsi_bands = 0;
   // switch the eigensolver from the FP32 twin to FP64 (iterative refinement)
+  // verbose == 3: the wall time of the steps of an iteration (synchronising;
+  // graphs stay on)
+  auto mark = [&](const char* what) {
+    if (p->verbose != 3) return;
+    cudaDeviceSynchronize();
+    fprintf(stderr, "  %-10s t %.4f s\n", what,
+            std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count());
+  };
   auto refine_now = [&]() -> int {
     PhaseTimer pt_(prof, &tph[5]);
-    DevBuf x32;
+    DevBuf& x32 = sv.x32;      // kept in the solver: no allocation per run
     int q;
+    mark("refine");
     if ((q = x32.alloc((size_t)nb * nt * 4))) return q;
     PWB_CUDA(cudaMemcpy(x32.p, sv.X.p, (size_t)nb * nt * 4, cudaMemcpyDeviceToDevice));
     std::vector<double> keep_eig = sv.eig;
     if ((q = bind(ctx))) return q;
+    mark("bind");
     if ((q = copy_f2d_2d((int)nt, nb, (const float*)x32.p, nt, (double*)sv.X.p, nt, nullptr))) return q;
     // the FP32 bands carry rounding outside the span of P: filter them again in FP64
     if (use_filter && (q = wfn_filter_pass(ctx, sv.X.p, (int)nt, nb, nullptr))) return q;
+    mark("filter");
     if ((q = cholqr(sv, dn, sv.X.p, nb, sv.Y.p))) return q;
+    mark("cholqr");
     sv.eig = keep_eig;
     refined = true;
     r->refine_iter = total_it;
@@ -1587,7 +1600,9 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
   S.hpos = 0;
   for (it = 1; it <= p->max_iter; ++it) {
     ++total_it;
+    mark("iteration");
     if ((rc = set_vtot_dev(sv.c, (const double*)S.vtot.p))) return rc;
+    mark("vtot");
     {
     PhaseTimer pt_(prof, &tph[0]);
     if (p->solver == PW_SOLVER_CHEBFSI) {
@@ -1639,6 +1654,7 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
     // new density, and with its norm (one reduction) the Harris energy of the
     // input density and potentials (scf.cpp:2025-2060)
     double* ro = (double*)S.rho_out.p;
+    mark("eigensolve");
     {
       PhaseTimer pt_(prof, &tph[1]);
       std::vector<double> wv(nb + 2, 0.0);
@@ -1658,6 +1674,7 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
       eharris = ekin + (exc - evxc) - ehart_h - eself + ent;
       k_lincomb<<<nblk(nf), 256>>>(nf, (2.0 * p->nocc * (double)nf) / (ctx->vol * hd[3]), ro, 0.0, nullptr, ro);
     }
+    mark("density");
     {
       PhaseTimer pt_(prof, &tph[2]);
       if ((rc = potentials(ro, nullptr))) return rc;

@@ -655,6 +655,18 @@ __global__ void __launch_bounds__(TRD_THREADS) k_trd_reduce(int n, const double*
   }
 }
 
+// 1/q by two Newton-Raphson steps, r <- r (2 - q r) (quadratic convergence),
+// from the hardware's approximate reciprocal (q stays a finite normal number:
+// the Sturm pivots are kept between pivmin >= the smallest normal double and
+// 1e300 in magnitude)
+__device__ __forceinline__ double recip_nr(double q) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(q));
+  r = r * fma(-q, r, 2.0);
+  r = r * fma(-q, r, 2.0);
+  return r;
+}
+
 // number of eigenvalues of T below x: negative pivots of the LDL^T
 // factorisation of T - x I (Sturm sequence in ratio form), pivots kept off
 // zero by pivmin
@@ -663,9 +675,10 @@ __device__ __forceinline__ int trd_sturm(int n, const double* d, const double* e
   if (fabs(q) < pivmin) q = -pivmin;
   int c = q <= 0.0;
   for (int j = 1; j < n; ++j) {
-    q = d[j] - e2[j - 1] / q - x;
+    q = (d[j] - x) - e2[j - 1] * recip_nr(q);
     if (fabs(q) < pivmin) q = -pivmin;
     c += q <= 0.0;
+    q = fmin(fmax(q, -1e300), 1e300);   // keep q finite for the reciprocal (an overflow counts by its sign)
   }
   return c;
 }
