@@ -786,8 +786,11 @@ k_floc2(VT<T>* __restrict__ BC, const T* __restrict__ vtot, T inv_nf, const VT<T
   V* Bp = BC + ((long)p * NZF + zf) * nsy * nsx;
   __syncthreads();
 
-  // A: inverse y transform of the nsx slot columns
-  constexpr int GA = FY;
+  // A: inverse y transform of the nsx slot columns, GA columns per warp step
+  // (variant 2: twice the FY of the second pass when that fills whole warp
+  // rounds in the first pass, 96: 8 columns x 12 = 3 rounds instead of 4 x 12
+  // in two half-empty rounds)
+  constexpr int GA = (RTW && (2 * FY * NY2) % 32 == 0) ? 2 * FY : FY;
   constexpr int RA = (GA * NY2 + 31) / 32;
   for (int g = warp * GA; g < nsx; g += nw * GA) {
 #pragma unroll
