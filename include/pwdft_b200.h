@@ -275,7 +275,9 @@ PW_API int pw_eigsolve(pw_ctx* ctx, int solver, void* X, int nb, int maxit, doub
 /* Electron density on the fine grid from nband device wavefunctions and host
  * occupation rates (numSpin = 2), renormalised to 2*nocc_total electrons:
  * KohnSham::CalculateDensity (src/SCF/hamiltonian.cpp:2455-2627).  rho_dev:
- * device, N_fine doubles. */
+ * device, N_fine doubles.  nocc_total <= 0: no renormalisation (the raw
+ * sum 2 f_k |psi_k|^2 of these bands, a rank's part of a band-distributed
+ * density, normalised once after the reduction as the reference does). */
 PW_API int pw_density(pw_ctx* ctx, const void* psi, int ld, int nband, const double* occ_host, int nocc_total,
                       double* rho_dev);
 

@@ -47,6 +47,7 @@ class Context:
         self.numGrid = tuple(int(x) for x in numGrid)
         self.numGridFine = tuple(int(x) for x in numGridFine)
         self.length = tuple(float(x) for x in length)
+        self.device = int(device)
 
     @classmethod
     def gspace(cls, length, numGrid, ecut: float, precision: str = "f64", device: int = 0) -> "Context":
@@ -69,6 +70,7 @@ class Context:
         self.numGrid = tuple(int(x) // 2 for x in numGrid)
         self.numGridFine = tuple(int(x) for x in numGrid)
         self.length = tuple(float(x) for x in length)
+        self.device = int(device)
         self.ecut = float(ecut)
         self.ns = self.ntot // 2
         return self

@@ -2136,7 +2136,12 @@ int pw_density(pw_ctx* ctx, const void* psi, int ld, int nband, const double* oc
     const int npair = std::min(cap, (nband - b0 + 1) / 2);
     if ((rc = run_density(ctx, psi, ld, nband, b0, npair, (const double*)wv.p, rho_dev, nullptr))) return rc;
   }
-  // renormalise to 2 * nocc electrons (hamiltonian.cpp:2596-2600)
+  // renormalise to 2 * nocc electrons (hamiltonian.cpp:2596-2600); nocc_total
+  // <= 0: the raw sum (a rank's part of a band-distributed density)
+  if (nocc_total <= 0) {
+    PWB_CUDA(cudaDeviceSynchronize());
+    return PW_OK;
+  }
   DevBuf d;
   if ((rc = d.alloc(64))) return rc;
   PWB_CUDA(cudaMemset(d.p, 0, 64));

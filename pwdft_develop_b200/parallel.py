@@ -367,3 +367,200 @@ def exx_apply_dist(set_phi, apply_exx, Xb, occ, nband: int):
     Context.exx_set_phi and Context.exx_apply."""
     set_phi(gather_bands(Xb, nband), occ)
     return apply_exx(Xb)
+
+
+# ---------------------------------------------------------------------------
+# Distributed SCF (SCF::Iterate over band shards)
+# ---------------------------------------------------------------------------
+AU2K = 315774.67
+
+
+def fermi_occupations(eig, nocc: int, tbeta: float):
+    """Fermi-Dirac occupation rates and Fermi level by bisection on the
+    electron count (SCF::CalculateOccupationRate, src/SCF/scf.cpp:1780-1822);
+    eig: all bands, ascending.  numpy arrays."""
+    import numpy as np
+    ev = np.asarray(eig, dtype=np.float64)
+    if ev.size == nocc:
+        return np.ones(ev.size), float(ev[-1])
+
+    def wg(ef):
+        return 1.0 / (1.0 + np.exp(np.clip(-tbeta * (ef - ev), -700.0, 700.0)))
+    lb, ub = float(ev.min()), float(ev.max())
+    ef = 0.5 * (lb + ub)
+    for _ in range(200):
+        s = wg(ef).sum()
+        if abs(s - nocc) <= 1e-16:
+            break
+        if s < nocc:
+            lb = ef
+        else:
+            ub = ef
+        ef = 0.5 * (lb + ub)
+    return wg(ef), ef
+
+
+def fermi_entropy(eig, ef: float, tbeta: float):
+    """Per-band -T S term of the free energy (scf.cpp:1960-1984), numpy."""
+    import numpy as np
+    x = tbeta * (ef - np.asarray(eig, dtype=np.float64))
+    out = np.zeros_like(x)
+    m = np.abs(x) <= 36.0
+    f = 1.0 / (1.0 + np.exp(-x[m]))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        out[m] = np.nan_to_num((f * np.log(f) + (1.0 - f) * np.log(1.0 - f)) / tbeta)
+    return out
+
+
+class AndersonMixer:
+    """Anderson mixing of the potential (SCF::AndersonMix, src/SCF/scf.cpp:
+    2299-2365): history of inputs and residuals, least-squares coefficients,
+    the mixed input plus step times the mixed residual.  Every rank runs it on
+    the same data (the potential is replicated), as the reference does."""
+
+    def __init__(self, mix_dim: int = 8, step: float = 0.7):
+        self.dim, self.step = mix_dim, step
+        self.dv, self.df = [], []
+
+    def __call__(self, vin, vout):
+        import torch
+        F = vout - vin
+        if self.dv:
+            difv = torch.stack([h - vin for h in self.dv], 1)
+            diff = torch.stack([h - F for h in self.df], 1)
+            theta = torch.linalg.solve(diff.T @ diff, diff.T @ F)
+            xbar, fbar = vin - difv @ theta, F - diff @ theta
+        else:
+            xbar, fbar = vin, F
+        self.dv.append(vin.clone())
+        self.df.append(F.clone())
+        if len(self.dv) > self.dim:
+            self.dv.pop(0)
+            self.df.pop(0)
+        return xbar + self.step * fbar
+
+
+def scf_dist(ops, Xb, nband: int, nocc: int, tol_efree: float = 1e-6, max_iter: int = 60, degree: int = 10,
+             first_cycles: int = 5, mix_dim: int = 8, mix_step: float = 0.7, temperature: float = 300.0,
+             ctx=None, verbose: bool = False):
+    """SCF::Iterate (src/SCF/scf.cpp:372-591) over band shards: each rank
+    filters and holds its bands (band_range), the subspace steps run on grid
+    rows (chebfsi_dist's Cholesky-QR and Rayleigh-Ritz), the density is the
+    all-reduced sum of the ranks' partial densities, normalised once to
+    2 nocc electrons (hamiltonian.cpp:2455-2600 with the reference's
+    MPI_Allreduce), and the potentials, energies and Anderson mixing run on
+    every rank on the same replicated data.  Converges when
+    |E_free - E_Harris| / N_atom < tol_efree (efreeDifPerAtom, scf.cpp:464-471).
+
+    ops: the rank's operators --
+      set_vtot(vtot)          the local potential (fine grid, FP64 tensor)
+      apply_h(Xb)             H times a block of this rank's bands
+      density_raw(Xb, w)      sum_k w_k |psi_k,fine|^2 over this rank's bands
+      potentials(rho)         (vh, vxc, eps): Hartree of rho - rho_ps and XC
+      rho_ps, vol, natom, eself
+    Xb: this rank's start bands (band_range(nband, world, rank) x all grid
+    points).  Returns a dict (efree, etot, eharris, eig, occ, iterations,
+    converged, rho, vtot) and the final bands of this rank."""
+    import numpy as np
+    import torch
+    world, rank = _world()
+    s, n = band_range(nband, world, rank)
+    ntot = Xb.shape[1]
+    rho_ps = ops.rho_ps
+    nf = rho_ps.numel()
+    w = ops.vol / nf
+    tbeta = AU2K / temperature
+    # initial density from the pseudocharge (scf.cpp:232-255)
+    rho = torch.where(rho_ps > 1e-6, rho_ps, torch.full_like(rho_ps, 1e-6))
+    rho = rho * (rho_ps.sum() / rho.sum())
+    vh, vxc, eps = ops.potentials(rho)
+    exc = float((eps * rho).sum()) * w
+    vtot = vh + vxc
+    mixer = AndersonMixer(mix_dim, mix_step)
+    b_up = None
+    lam = None
+    out = dict(converged=False)
+    for it in range(1, max_iter + 1):
+        ops.set_vtot(vtot)
+        if b_up is None:
+            b_up = lanczos_upper_bound(ops.apply_h, Xb)
+            Xr = cholqr_rows(band_to_rows(Xb, nband), ctx)
+            Xb = rows_to_band(Xr, ntot)
+            lam, Xr, _ = rayleigh_ritz_rows(Xr, band_to_rows(ops.apply_h(Xb), nband), ctx)
+            Xb = rows_to_band(Xr, ntot)
+            cycles = max(1, first_cycles)
+        else:
+            cycles = 1
+        for _ in range(cycles):
+            Y = chebyshev_filter(ops.apply_h, Xb, degree, float(lam[-1]), b_up, float(lam[0]))
+            Yr = cholqr_rows(band_to_rows(Y, nband), ctx)
+            Yb = rows_to_band(Yr, ntot)
+            lam, Xr, _ = rayleigh_ritz_rows(Yr, band_to_rows(ops.apply_h(Yb), nband), ctx)
+            Xb = rows_to_band(Xr, ntot)
+        eig = lam.double().cpu().numpy()
+        occ, ef = fermi_occupations(eig, nocc, tbeta)
+        ent = float(np.sum(2.0 * fermi_entropy(eig, ef, tbeta)))
+        ekin = float(np.sum(2.0 * eig * occ))
+        # Harris energy with the input density and potentials (scf.cpp:1987-2140)
+        ehart_h = float((0.5 * vh * (rho + rho_ps)).sum()) * w
+        evxc = float((vxc * rho).sum()) * w
+        eharris = ekin + (exc - evxc) - ehart_h - ops.eself + ent
+        # new density: partial sums over the ranks' bands, then one normalisation
+        part = ops.density_raw(Xb, torch.as_tensor(2.0 * occ[s:s + n], dtype=torch.float64))
+        rho_out = allreduce_sum_(part.double().contiguous())
+        rho_out = rho_out * (2.0 * nocc * nf / (ops.vol * float(rho_out.sum())))
+        vh, vxc, eps = ops.potentials(rho_out)
+        exc = float((eps * rho_out).sum()) * w
+        vtot_new = vh + vxc
+        # Kohn-Sham energy with the input potential (scf.cpp:1834-1984)
+        ecor = -float((vtot * rho_out).sum()) * w + exc + float((0.5 * vh * (rho_out - rho_ps)).sum()) * w \
+            - ops.eself
+        etot = ekin + ecor
+        efree = etot + ent
+        dif = abs(efree - eharris) / ops.natom
+        if verbose and rank == 0:
+            print(f"scf_dist {it:3d} Efree {efree:.10f} Eharris {eharris:.10f} dif {dif:.3e}")
+        out = dict(efree=efree, etot=etot, eharris=eharris, eig=eig, occ=occ, iterations=it, converged=False,
+                   rho=rho_out, vtot=vtot)
+        rho = rho_out
+        if dif < tol_efree:
+            out["converged"] = True
+            break
+        vtot = mixer(vtot, vtot_new)
+    return out, Xb
+
+
+class DeviceScfOps:
+    """scf_dist's operators on this rank's GPU through the library: an FP64
+    context with its atoms set (pw_set_atoms); H*psi pw_hpsi, the partial
+    density pw_density without renormalisation, pw_hartree and pw_xc_teter93
+    (LDA) on the fine grid."""
+
+    def __init__(self, ctx, ecut: float, znuc, natom: int):
+        import numpy as np
+        import torch
+        from .core import hgh_species
+        self.ctx, self.ecut = ctx, float(ecut)
+        dev = torch.device("cuda", ctx.device)
+        self.rho_ps = torch.as_tensor(ctx.pseudocharge(), dtype=torch.float64, device=dev)
+        L = np.asarray(ctx.length, dtype=np.float64)
+        self.vol = float(L.prod())
+        zs = np.broadcast_to(np.asarray(znuc), (natom,))
+        self.natom = natom
+        self.eself = float(sum(hgh_species(int(z))["eself"] for z in zs))
+
+    def set_vtot(self, vtot):
+        self.ctx.set_vtot(vtot.double().cpu().numpy())
+
+    def apply_h(self, Xb):
+        return self.ctx.hpsi(Xb)
+
+    def density_raw(self, Xb, w):
+        import numpy as np
+        # pw_density takes occupation rates (it doubles them); nocc_total 0: no renormalisation
+        return self.ctx.density(Xb, np.asarray(w.cpu().numpy()) / 2.0, 0)
+
+    def potentials(self, rho):
+        vh = self.ctx.hartree((rho - self.rho_ps).contiguous(), self.ecut)
+        eps, vxc = self.ctx.xc(rho.contiguous())
+        return vh, vxc, eps
