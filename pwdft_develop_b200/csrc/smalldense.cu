@@ -690,7 +690,9 @@ __device__ __forceinline__ int trd_sturm(int n, const double* d, const double* e
 constexpr int TRD_BIS_WARPS = 4;
 constexpr int TRD_BIS_STEPS = 11;
 __global__ void __launch_bounds__(32 * TRD_BIS_WARPS) k_trd_bisect(int n, const double* ws, double* w) {
-  __shared__ double sd[TRD_NMAX], se2[TRD_NMAX];
+  extern __shared__ __align__(16) double bis_sm[];   // 2 n doubles
+  double* sd = bis_sm;
+  double* se2 = bis_sm + n;
   __shared__ double s_gl, s_gu, s_pivmin;
   const double* d = ws + 2 * (size_t)n * n;
   const double* e = d + n;
@@ -743,20 +745,23 @@ __device__ __forceinline__ double trd_rand(int i, int r) {
 }
 
 // eigenvectors of T: one warp per cluster; lane 0 factors T - lambda I with
-// partial pivoting and runs the solves, the warp orthogonalises and normalises
-__global__ void __launch_bounds__(32 * TRD_WARPS_STEIN) k_trd_stein(int n, double* ws, const double* w) {
+// partial pivoting and runs the solves, the warp orthogonalises and normalises.
+// Shared memory: 6 n doubles per warp, then the cluster table (n + 2 ints).
+// Clusters: neighbours closer than ortol_rel ||T||.
+__global__ void __launch_bounds__(32 * TRD_WARPS_STEIN) k_trd_stein(int n, double* ws, const double* w,
+                                                                    double ortol_rel) {
   extern __shared__ __align__(16) double st_sm[];
-  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
-  const int g = blockIdx.x * TRD_WARPS_STEIN + wl;
+  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5, wpc = blockDim.x >> 5;
+  const int g = blockIdx.x * wpc + wl;
   double* Z = ws + (size_t)n * n;
   const double* d = ws + 2 * (size_t)n * n;
   const double* e = d + n;
-  // clusters: neighbours closer than 1e-3 ||T|| (every CTA scans w itself)
-  __shared__ int clus[TRD_NMAX + 2];
+  // every CTA scans w itself
+  int* clus = reinterpret_cast<int*>(st_sm + (size_t)wpc * 6 * n);
   if (threadIdx.x == 0) {
     double tn0 = 0.0;
     for (int i = 0; i < n; ++i) tn0 = fmax(tn0, fabs(d[i]) + (i + 1 < n ? 2.0 * fabs(e[i]) : 0.0));
-    const double ortol = 1e-3 * tn0;
+    const double ortol = ortol_rel * tn0;
     int nc = 0;
     for (int i = 0; i < n; ++i)
       if (i == 0 || w[i] - w[i - 1] > ortol) clus[1 + nc++] = i;
@@ -914,25 +919,353 @@ __global__ void __launch_bounds__(256) k_trd_back(int n, double* A, int lda, con
   }
 }
 
+// ---------------------------------------------------------------------------
+// The same method for n > TRD_NMAX (LOBPCG's 3n subspace, Rayleigh-Ritz of
+// several hundred bands):
+//   1. the reduction runs on G co-resident CTAs (a cooperative launch), the
+//      matrix held in their shared memory by rows (row i on CTA i mod G).
+//      Step k: the owner of row k forms the reflector and publishes it
+//      (column k of V, a release flag); every CTA forms p = tau A22 v on its
+//      rows and publishes them (a counting barrier over the G CTAs, p double
+//      buffered by the barrier's parity); every CTA then forms w = p - (tau/2)(p.v) v and updates its
+//      rows.  One flag wait and one barrier per column, both bounded by
+//      %globaltimer (TRD_WAIT_NS; on timeout the CTA records code 1 in the
+//      sync record and returns).
+//   2./3. multisection and inverse iteration as above (the cluster tolerance
+//      scaled by 160 / n, so the expected cluster sizes stay those of n = 160);
+//   4. X = Q Z with one warp per column of Z, the column in registers, the
+//      reflectors staged through shared memory TRDB_KC at a time.
+// ---------------------------------------------------------------------------
+constexpr int TRDL_THREADS = 512;
+constexpr int TRD_NMAX_L = 2048;
+constexpr unsigned long long TRD_WAIT_NS = 2000000000ull;
+constexpr int TRDB_KC = 8;
+
+struct TrdSync {
+  unsigned int count;   // barrier arrivals
+  unsigned int vflag;   // reflectors published (k + 1 after step k)
+  int err;              // 1: a wait ran out
+  int pad;
+};
+// workspace of the large form: trd_ws(n) doubles, then p (2 n), then the sync record
+size_t trd_ws_large(int n) { return trd_ws(n) + 2 * (size_t)n + 2; }
+
+__device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* p) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_u32(unsigned int* p, unsigned int v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long trd_gtimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+// wait until *p >= target; false after TRD_WAIT_NS
+__device__ bool trd_wait_geq(const unsigned int* p, unsigned int target) {
+  if (ld_acquire_u32(p) >= target) return true;
+  const unsigned long long t0 = trd_gtimer();
+  for (;;) {
+    __nanosleep(64);
+    if (ld_acquire_u32(p) >= target) return true;
+    if (trd_gtimer() - t0 > TRD_WAIT_NS) return false;
+  }
+}
+
+__global__ void __launch_bounds__(TRDL_THREADS) k_trd_reduce_mc(int n, const double* A, int lda, double* ws) {
+  extern __shared__ __align__(16) double rm_sm[];
+  const int G = gridDim.x, c = blockIdx.x;
+  const int nr = (n - c + G - 1) / G;      // rows c, c + G, c + 2G, ...
+  double* R = rm_sm;                       // R[li n + j] = A(c + li G, j)
+  double* vs = R + (size_t)nr * n;         // v of the step (entries past k)
+  double* wsm = vs + n;                    // p, then w
+  __shared__ double red[32];
+  __shared__ int abort_s;
+  double* V = ws;
+  double* d = ws + 2 * (size_t)n * n;
+  double* e = d + n;
+  double* tau = e + n;
+  double* pg = tau + n;                    // 2 n: p, double buffered
+  TrdSync* sy = reinterpret_cast<TrdSync*>(pg + 2 * (size_t)n);
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+  for (int idx = tid; idx < nr * n; idx += blockDim.x) {
+    const int li = idx / n, j = idx - li * n;
+    const int i = c + li * G;
+    R[idx] = i <= j ? A[(long)j * lda + i] : A[(long)i * lda + j];
+  }
+  if (tid == 0) abort_s = 0;
+  __syncthreads();
+  unsigned int nbar = 0;
+  for (int k = 0; k + 2 < n; ++k) {
+    if (k % G == c && wid == 0) {
+      // the owner forms the reflector of row k (= column k) and publishes it
+      const double* rk = R + (size_t)(k / G) * n;
+      double s = 0.0;
+      for (int j = k + 2 + lane; j < n; j += 32) s += rk[j] * rk[j];
+      s = warp_sum_d(s);
+      const double alpha = rk[k + 1];
+      double tk = 0.0, beta = alpha, scal = 0.0;
+      if (s != 0.0) {
+        const double mu = sqrt(alpha * alpha + s);
+        beta = alpha <= 0.0 ? mu : -mu;
+        tk = (beta - alpha) / beta;
+        scal = 1.0 / (alpha - beta);
+      }
+      for (int j = lane; j < n; j += 32) V[(size_t)k * n + j] = j <= k ? 0.0 : (j == k + 1 ? 1.0 : rk[j] * scal);
+      if (lane == 0) {
+        d[k] = rk[k];
+        e[k] = beta;
+        tau[k] = tk;
+      }
+      __syncwarp();
+      if (lane == 0) {
+        __threadfence();
+        st_release_u32(&sy->vflag, (unsigned int)(k + 1));
+      }
+    }
+    if (tid == 0 && !trd_wait_geq(&sy->vflag, (unsigned int)(k + 1))) {
+      abort_s = 1;
+      atomicExch(&sy->err, 1);
+    }
+    __syncthreads();
+    if (abort_s) return;
+    const double tk = __ldcg(&tau[k]);
+    if (tk == 0.0) continue;          // the same on every CTA: nothing to update
+    for (int j = k + 1 + tid; j < n; j += blockDim.x) vs[j] = __ldcg(&V[(size_t)k * n + j]);
+    __syncthreads();
+    // first local row past k
+    const int li0 = k + 1 <= c ? 0 : (k + 1 - c + G - 1) / G;
+    // p in half nbar & 1 (barriers completed so far): the last data in that half
+    // belonged to barrier nbar - 2, read by every CTA before it arrived at nbar - 1
+    double* ph = pg + (size_t)(nbar & 1) * n;
+    for (int li = li0 + wid; li < nr; li += nw) {
+      const double* r = R + (size_t)li * n;
+      double acc = 0.0;
+      for (int j = k + 1 + lane; j < n; j += 32) acc += r[j] * vs[j];
+      acc = warp_sum_d(acc);
+      if (lane == 0) ph[c + li * G] = tk * acc;
+    }
+    __syncthreads();
+    ++nbar;
+    if (tid == 0) {
+      __threadfence();
+      atomicAdd(&sy->count, 1u);
+      if (!trd_wait_geq(&sy->count, nbar * (unsigned int)G)) {
+        abort_s = 1;
+        atomicExch(&sy->err, 1);
+      }
+    }
+    __syncthreads();
+    if (abort_s) return;
+    double part = 0.0;
+    for (int j = k + 1 + tid; j < n; j += blockDim.x) {
+      const double pj = __ldcg(&ph[j]);
+      wsm[j] = pj;
+      part += pj * vs[j];
+    }
+    const double kc = 0.5 * tk * block_sum_d(part, red);
+    for (int j = k + 1 + tid; j < n; j += blockDim.x) wsm[j] -= kc * vs[j];
+    __syncthreads();
+    for (int li = li0 + wid; li < nr; li += nw) {
+      const int i = c + li * G;
+      const double vi = vs[i], wi = wsm[i];
+      double* r = R + (size_t)li * n;
+      for (int j = k + 1 + lane; j < n; j += 32) r[j] -= vi * wsm[j] + wi * vs[j];
+    }
+    __syncthreads();
+  }
+  // the trailing 2 x 2 block (e from row n - 1, as in the one-CTA form)
+  if (tid == 0) {
+    if ((n - 2) % G == c) {
+      d[n - 2] = R[(size_t)((n - 2) / G) * n + n - 2];
+      tau[n - 2] = 0.0;
+    }
+    if ((n - 1) % G == c) {
+      const double* r = R + (size_t)((n - 1) / G) * n;
+      e[n - 2] = r[n - 2];
+      d[n - 1] = r[n - 1];
+      tau[n - 1] = 0.0;
+    }
+  }
+}
+
+// X = H_0 H_1 ... H_{n-3} Z into A's columns: one warp per column, rows
+// lane + 32 q of the column in registers (QM >= n / 32)
+template <int QM>
+__global__ void __launch_bounds__(256) k_trd_back_w(int n, double* A, int lda, const double* ws) {
+  extern __shared__ __align__(16) double bw_sm[];   // TRDB_KC x n reflectors, then TRDB_KC taus
+  double* ts = bw_sm + (size_t)TRDB_KC * n;
+  const double* V = ws;
+  const double* Z = ws + (size_t)n * n;
+  const double* tau = ws + 2 * (size_t)n * n + 2 * (size_t)n;
+  const int lane = threadIdx.x & 31;
+  const int col = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const bool act = col < n;
+  double z[QM];
+#pragma unroll
+  for (int q = 0; q < QM; ++q) {
+    const int r = lane + 32 * q;
+    z[q] = (act && r < n) ? Z[(size_t)col * n + r] : 0.0;
+  }
+  for (int kt = n - 3; kt >= 0; kt -= TRDB_KC) {
+    const int kb = max(0, kt - TRDB_KC + 1), nk = kt - kb + 1;   // reflectors kb .. kt
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < nk * n; idx += blockDim.x) bw_sm[idx] = V[(size_t)kb * n + idx];
+    if (threadIdx.x < nk) ts[threadIdx.x] = tau[kb + threadIdx.x];
+    __syncthreads();
+    for (int kk = nk - 1; kk >= 0; --kk) {
+      const double tk = ts[kk];
+      if (tk == 0.0) continue;
+      const int k = kb + kk;
+      const double* vk = bw_sm + (size_t)kk * n;
+      double sacc = 0.0;
+#pragma unroll
+      for (int q = 0; q < QM; ++q) {
+        const int r = lane + 32 * q;
+        if (r > k && r < n) sacc += vk[r] * z[q];
+      }
+      sacc = warp_sum_d(sacc) * tk;
+#pragma unroll
+      for (int q = 0; q < QM; ++q) {
+        const int r = lane + 32 * q;
+        if (r > k && r < n) z[q] -= vk[r] * sacc;
+      }
+    }
+  }
+  if (!act) return;
+#pragma unroll
+  for (int q = 0; q < QM; ++q) {
+    const int r = lane + 32 * q;
+    if (r < n) A[(long)col * lda + r] = z[q];
+  }
+}
+
+// CTAs of the cooperative reduction for this n on this device (0: the rows do
+// not fit in shared memory), and its dynamic shared memory
+struct TrdLargePlan {
+  int G = 0;
+  size_t smem = 0;
+};
+static TrdLargePlan trd_large_plan(int n) {
+  TrdLargePlan pl;
+  if (n <= TRD_NMAX || n > TRD_NMAX_L) return pl;
+  int dev = 0, nsm = 0, optin = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+    return pl;
+  // one CTA per SM at most; about 16 rows per CTA where the SMs allow
+  int G = std::min(nsm, std::max(1, (n + 15) / 16));
+  for (;; ++G) {
+    if (G > nsm) return pl;
+    const int nr = (n + G - 1) / G;
+    const size_t sm = ((size_t)nr * n + 2 * (size_t)n) * sizeof(double) + 1024;
+    if (sm <= (size_t)optin) {
+      pl.G = G;
+      pl.smem = sm - 1024;
+      return pl;
+    }
+  }
+}
+
+bool trd_supported(int n) { return n <= TRD_NMAX || trd_large_plan(n).G > 0; }
+
+static int trd_reduce_large(int n, const double* A, int lda, double* wsp, cudaStream_t st) {
+  const TrdLargePlan pl = trd_large_plan(n);
+  PWB_CHECK(pl.G > 0, PW_EUNSUPPORTED, "tridiagonal reduction: n too large for shared memory");
+  int optin = 0, dev = 0;
+  PWB_CUDA(cudaGetDevice(&dev));
+  PWB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  static PerDeviceOnce attr;
+  if (!attr.done()) {
+    PWB_CUDA(cudaFuncSetAttribute(k_trd_reduce_mc, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - 1024));
+    attr.mark();
+  }
+  int per_sm = 0;
+  PWB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trd_reduce_mc, TRDL_THREADS, pl.smem));
+  PWB_CHECK(per_sm >= 1, PW_EUNSUPPORTED, "tridiagonal reduction: no resident CTA");
+  TrdSync* sy = reinterpret_cast<TrdSync*>(wsp + trd_ws(n) + 2 * (size_t)n);
+  PWB_CUDA(cudaMemsetAsync(sy, 0, sizeof(TrdSync), st));
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(pl.G);
+  cfg.blockDim = dim3(TRDL_THREADS);
+  cfg.dynamicSmemBytes = pl.smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  PWB_CUDA(cudaLaunchKernelEx(&cfg, k_trd_reduce_mc, n, A, lda, wsp));
+  return PW_OK;
+}
+
+static int trd_back_large(int n, double* A, int lda, const double* wsp, cudaStream_t st) {
+  const int wpc = n <= 512 ? 4 : 8;
+  const size_t sm = ((size_t)TRDB_KC * n + TRDB_KC) * sizeof(double);
+  const dim3 grid((n + wpc - 1) / wpc), block(32 * wpc);
+  static PerDeviceOnce attr;
+  if (!attr.done()) {
+    const int mx = (int)(((size_t)TRDB_KC * TRD_NMAX_L + TRDB_KC) * sizeof(double));
+    PWB_CUDA(cudaFuncSetAttribute(k_trd_back_w<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    PWB_CUDA(cudaFuncSetAttribute(k_trd_back_w<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    PWB_CUDA(cudaFuncSetAttribute(k_trd_back_w<48>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    PWB_CUDA(cudaFuncSetAttribute(k_trd_back_w<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    attr.mark();
+  }
+  if (n <= 512) k_trd_back_w<16><<<grid, block, sm, st>>>(n, A, lda, wsp);
+  else if (n <= 1024) k_trd_back_w<32><<<grid, block, sm, st>>>(n, A, lda, wsp);
+  else if (n <= 1536) k_trd_back_w<48><<<grid, block, sm, st>>>(n, A, lda, wsp);
+  else k_trd_back_w<64><<<grid, block, sm, st>>>(n, A, lda, wsp);
+  return PW_OK;
+}
+
+// code recorded by the large reduction's waits (0: none); synchronous
+int trd_error(int n, const DevBuf& ws) {
+  if (n <= TRD_NMAX || !ws.p) return 0;
+  TrdSync h{};
+  if (cudaMemcpy(&h, (const double*)ws.p + trd_ws(n) + 2 * (size_t)n, sizeof(h), cudaMemcpyDeviceToHost) !=
+      cudaSuccess)
+    return -1;
+  return h.err;
+}
+
 int dense_syevh(int n, double* A, int lda, double* w, DevBuf& ws, cudaStream_t st) {
   if (n <= 0) return PW_OK;
-  if (n > TRD_NMAX) return dense_syevj(n, A, lda, w, ws, nullptr, st);
+  if (!trd_supported(n)) return dense_syevj(n, A, lda, w, ws, nullptr, st);
+  const bool large = n > TRD_NMAX;
   int rc;
-  if ((rc = ws.alloc(trd_ws(n) * sizeof(double)))) return rc;
+  if ((rc = ws.alloc((large ? trd_ws_large(n) : trd_ws(n)) * sizeof(double)))) return rc;
   static PerDeviceOnce attr;
   const size_t sm_red = ((size_t)TRD_NMAX * (TRD_NMAX | 1) + 2 * TRD_NMAX) * sizeof(double);
-  const size_t sm_st = (size_t)TRD_WARPS_STEIN * 6 * TRD_NMAX * sizeof(double);
+  int optin = 0, dev = 0;
+  PWB_CUDA(cudaGetDevice(&dev));
+  PWB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
   if (!attr.done()) {
     PWB_CUDA(cudaFuncSetAttribute(k_trd_reduce, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_red));
-    PWB_CUDA(cudaFuncSetAttribute(k_trd_stein, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_st));
+    PWB_CUDA(cudaFuncSetAttribute(k_trd_stein, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     attr.mark();
   }
   double* wsp = (double*)ws.p;
-  k_trd_reduce<<<1, TRD_THREADS, ((size_t)n * (n | 1) + 2 * (size_t)n) * sizeof(double), st>>>(n, A, lda, wsp);
-  k_trd_bisect<<<(n + TRD_BIS_WARPS - 1) / TRD_BIS_WARPS, 32 * TRD_BIS_WARPS, 0, st>>>(n, wsp, w);
-  k_trd_stein<<<(n + TRD_WARPS_STEIN - 1) / TRD_WARPS_STEIN, 32 * TRD_WARPS_STEIN,
-                (size_t)TRD_WARPS_STEIN * 6 * n * sizeof(double), st>>>(n, wsp, w);
-  k_trd_back<<<(n + 15) / 16, 256, 0, st>>>(n, A, lda, wsp);
+  if (large) {
+    if ((rc = trd_reduce_large(n, A, lda, wsp, st))) return rc;
+  } else {
+    k_trd_reduce<<<1, TRD_THREADS, ((size_t)n * (n | 1) + 2 * (size_t)n) * sizeof(double), st>>>(n, A, lda, wsp);
+  }
+  k_trd_bisect<<<(n + TRD_BIS_WARPS - 1) / TRD_BIS_WARPS, 32 * TRD_BIS_WARPS, 2 * (size_t)n * sizeof(double), st>>>(
+      n, wsp, w);
+  // warps per CTA of the inverse iteration: 6 n doubles each, plus the cluster table
+  const size_t per_warp = 6 * (size_t)n * sizeof(double), tab = ((size_t)n + 2) * sizeof(int);
+  const int wpc = (int)std::max<size_t>(1, std::min<size_t>(TRD_WARPS_STEIN, ((size_t)optin - tab) / per_warp));
+  const double ortol = large ? 1e-3 * (double)TRD_NMAX / n : 1e-3;
+  k_trd_stein<<<(n + wpc - 1) / wpc, 32 * wpc, wpc * per_warp + tab, st>>>(n, wsp, w, ortol);
+  if (large) {
+    if ((rc = trd_back_large(n, A, lda, wsp, st))) return rc;
+  } else {
+    k_trd_back<<<(n + 15) / 16, 256, 0, st>>>(n, A, lda, wsp);
+  }
   PWB_CUDA(cudaGetLastError());
   return PW_OK;
 }
@@ -986,9 +1319,10 @@ int pw_dense_syev(pw_ctx* ctx, int n, double* A, int lda, double* w, int* sweeps
   PWB_CUDA(cudaSetDevice(ctx->device));
   DevBuf ws, sw;
   int rc;
-  if (n <= TRD_NMAX) {
+  if (trd_supported(n)) {
     if ((rc = dense_syevh(n, A, lda, w, ws, nullptr))) return rc;
     PWB_CUDA(cudaDeviceSynchronize());
+    PWB_CHECK(trd_error(n, ws) == 0, PW_ETIMEOUT, "tridiagonal reduction: a wait ran out");
     if (sweeps) *sweeps = 0;
     return PW_OK;
   }

@@ -99,8 +99,50 @@ def test_syev(n, kind):
     assert float((E @ E.T - torch.eye(n, dtype=torch.float64, device="cuda")).abs().max()) < 1e-10
     R = E @ A - w[:, None] * E
     assert float(R.abs().max()) < 1e-10 * max(scale, 1.0)
-    # up to n = 160 the tridiagonal path runs (no sweeps), beyond it Jacobi
-    assert sw.value == 0 if n <= 160 else 1 <= sw.value <= 40
+    # the tridiagonal path runs (no Jacobi sweeps): one CTA up to n = 160,
+    # the cooperative reduction beyond
+    assert sw.value == 0
+    c.close()
+
+
+@pytest.mark.parametrize("n", [161, 480, 1440])
+@pytest.mark.parametrize("kind", ["overlap", "ritz"])
+def test_syev_large_subspace(n, kind):
+    """The cooperative tridiagonal path on the matrices of LOBPCG's 3n
+    subspace: an overlap matrix S^T S of normalised, partly dependent columns
+    (eigenvalues from ~1e-9 to ~3, dense near 1) and a Ritz matrix with
+    threefold-degenerate levels spread like a band structure."""
+    import torch
+    from pwdft_develop_b200._lib import check, lib
+    c = _ctx()
+    g = torch.Generator().manual_seed(7 * n)
+    if kind == "overlap":
+        X = torch.linalg.qr(torch.randn(4 * n, n // 3, generator=g, dtype=torch.float64))[0].T
+        W = X[torch.randint(0, n // 3, (n // 3,), generator=g)] + (0.3 / (4 * n) ** 0.5) * torch.randn(
+            n // 3, 4 * n, generator=g, dtype=torch.float64)
+        P = torch.randn(n - 2 * (n // 3), 4 * n, generator=g, dtype=torch.float64)
+        P[0] = X[0] + 1e-5 * P[0]
+        S = torch.cat([X, W, P], 0)
+        S = S / S.norm(dim=1, keepdim=True)
+        A = (S @ S.T).cuda()
+    else:
+        Q, _ = torch.linalg.qr(torch.randn(n, n, generator=g, dtype=torch.float64))
+        d = torch.sort(torch.rand((n + 2) // 3, generator=g, dtype=torch.float64) * 1.8 - 0.3).values
+        d = torch.repeat_interleave(d, 3)[:n] + 1e-13 * torch.randn(n, generator=g, dtype=torch.float64)
+        A = ((Q * d) @ Q.T).cuda()
+        A = 0.5 * (A + A.T)
+    V = A.clone()
+    w = torch.empty(n, dtype=torch.float64, device="cuda")
+    sw = C.c_int(-1)
+    check(lib.pw_dense_syev(c.handle, n, _ptr(V), n, _ptr(w), C.byref(sw)))
+    assert sw.value == 0
+    ref = torch.linalg.eigvalsh(A)
+    scale = float(A.abs().max())
+    assert float((w - ref).abs().max()) < 1e-12 * max(scale, 1.0) * n ** 0.5
+    E = V
+    assert float((E @ E.T - torch.eye(n, dtype=torch.float64, device="cuda")).abs().max()) < 1e-10
+    R = E @ A - w[:, None] * E
+    assert float(R.abs().max()) < 1e-10 * max(scale, 1.0)
     c.close()
 
 
