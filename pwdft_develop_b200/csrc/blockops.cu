@@ -661,7 +661,7 @@ void Dense::release() {}
 
 // eigenvectors (in A) and ascending eigenvalues by the library's kernels
 // (smalldense.cu): tridiagonal reduction, multisection and inverse iteration
-// up to n = 160, cyclic Jacobi beyond
+// up to n = 2048 where the rows fit in shared memory, cyclic Jacobi beyond
 int Dense::syevd(int n, double* A, int lda, double* w, cudaStream_t st) {
   return dense_syevh(n, A, lda, w, work, st);
 }

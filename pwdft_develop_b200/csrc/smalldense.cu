@@ -931,15 +931,22 @@ __global__ void __launch_bounds__(256) k_trd_back(int n, double* A, int lda, con
 //      rows.  One flag wait and one barrier per column, both bounded by
 //      %globaltimer (TRD_WAIT_NS; on timeout the CTA records code 1 in the
 //      sync record and returns).
-//   2./3. multisection and inverse iteration as above (the cluster tolerance
-//      scaled by 160 / n, so the expected cluster sizes stay those of n = 160);
+//   2./3. multisection and inverse iteration as above, but Gram-Schmidt only
+//      within clusters closer than 1e-8 ||T|| (the near-degenerate sets, where
+//      independent solves may give nearly parallel vectors); every other pair
+//      of computed vectors overlaps by at most ~ r / gap <= ~1e-6 (r ~ n eps
+//      ||T|| the residual of a solve), and two symmetric (Loewdin) steps
+//      Z <- Z (3 I - Z^T Z) / 2 make Z orthonormal to rounding.  Mixing two
+//      vectors with coefficient ~ r / gap moves each residual by ~ r, so the
+//      eigenpairs keep their accuracy; the 1e-3 ||T|| clusters of the
+//      one-CTA form chain into sets of hundreds of vectors at these sizes
+//      (LOBPCG's overlap matrices), each solved one after another;
 //   4. X = Q Z with one warp per column of Z, the column in registers, the
-//      reflectors staged through shared memory TRDB_KC at a time.
+//      reflectors applied eight at a time in compact WY form.
 // ---------------------------------------------------------------------------
 constexpr int TRDL_THREADS = 512;
 constexpr int TRD_NMAX_L = 2048;
 constexpr unsigned long long TRD_WAIT_NS = 2000000000ull;
-constexpr int TRDB_KC = 8;
 
 struct TrdSync {
   unsigned int count;   // barrier arrivals
@@ -947,8 +954,18 @@ struct TrdSync {
   int err;              // 1: a wait ran out
   int pad;
 };
-// workspace of the large form: trd_ws(n) doubles, then p (2 n), then the sync record
-size_t trd_ws_large(int n) { return trd_ws(n) + 2 * (size_t)n + 2; }
+// workspace of the large form: trd_ws(n) doubles, then p (2 n), the sync
+// record (2), and two n x n blocks for the orthonormalisation of Z
+size_t trd_ws_large(int n) { return trd_ws(n) + 2 * (size_t)n + 2 + 2 * (size_t)n * n; }
+
+// M = (3 I - G) / 2 in place: one first-order step towards (Z^T Z)^{-1/2}
+__global__ void k_lowdin_step(int n, double* G) {
+  const int j = blockIdx.x;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const double g = G[(size_t)j * n + i];
+    G[(size_t)j * n + i] = (i == j ? 1.5 : 0.0) - 0.5 * g;
+  }
+}
 
 __device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* p) {
   unsigned int v;
@@ -1031,10 +1048,11 @@ __global__ void __launch_bounds__(TRDL_THREADS) k_trd_reduce_mc(int n, const dou
     }
     __syncthreads();
     if (abort_s) return;
-    const double tk = __ldcg(&tau[k]);
-    if (tk == 0.0) continue;          // the same on every CTA: nothing to update
+    // v and tau in the same round trip (v is staged even when tau is zero)
     for (int j = k + 1 + tid; j < n; j += blockDim.x) vs[j] = __ldcg(&V[(size_t)k * n + j]);
+    const double tk = __ldcg(&tau[k]);
     __syncthreads();
+    if (tk == 0.0) continue;          // the same on every CTA: nothing to update
     // first local row past k
     const int li0 = k + 1 <= c ? 0 : (k + 1 - c + G - 1) / G;
     // p in half nbar & 1 (barriers completed so far): the last data in that half
@@ -1091,48 +1109,295 @@ __global__ void __launch_bounds__(TRDL_THREADS) k_trd_reduce_mc(int n, const dou
   }
 }
 
+// The reduction on one thread-block cluster (n up to ~640): the CL CTAs hold
+// the rows in their shared memory (row i on CTA i mod CL) and exchange v and p
+// through distributed shared memory; per column two hardware cluster barriers
+// and no global round trip.  Step k: the owner of row k forms v in its own
+// buffer (and writes it to V); barrier; every CTA copies v from the owner,
+// forms p on its rows into its own buffer; barrier; every CTA gathers p from
+// the owners of its entries, forms w and updates its rows.  A CTA rewrites
+// its v / p buffers only after a later barrier that every reader of the old
+// contents has passed.
+__device__ __forceinline__ unsigned cluster_rank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+// load a double at the same shared-memory offset in CTA `rank` of the cluster
+__device__ __forceinline__ double ld_dsmem(const double* local, unsigned rank) {
+  unsigned a = (unsigned)__cvta_generic_to_shared(local), ra;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(ra) : "r"(a), "r"(rank));
+  double v;
+  asm volatile("ld.shared::cluster.f64 %0, [%1];" : "=d"(v) : "r"(ra) : "memory");
+  return v;
+}
+
+__global__ void __launch_bounds__(TRDL_THREADS) k_trd_reduce_cl(int n, const double* A, int lda, double* ws) {
+  extern __shared__ __align__(16) double rc_sm[];
+  const int CL = (int)gridDim.x, c = (int)cluster_rank();
+  const int nr = (n - c + CL - 1) / CL;
+  // the buffers read by other CTAs sit at the same offset in every CTA (the
+  // row counts differ by one between CTAs, so they come before the rows)
+  double* vown = rc_sm;                    // v formed here when this CTA owns row k; vown[n] = tau
+  double* vs = vown + n + 2;               // this CTA's copy of v
+  double* pl = vs + n;                     // p at this CTA's rows (by global row index)
+  double* wsm = pl + n;                    // p, then w, gathered
+  double* R = wsm + n;                     // R[li n + j] = A(c + li CL, j)
+  __shared__ double red[32];
+  double* V = ws;
+  double* d = ws + 2 * (size_t)n * n;
+  double* e = d + n;
+  double* tau = e + n;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+  for (int idx = tid; idx < nr * n; idx += blockDim.x) {
+    const int li = idx / n, j = idx - li * n;
+    const int i = c + li * CL;
+    R[idx] = i <= j ? A[(long)j * lda + i] : A[(long)i * lda + j];
+  }
+  __syncthreads();
+  for (int k = 0; k + 2 < n; ++k) {
+    const int own = k % CL;
+    if (own == c && wid == 0) {
+      const double* rk = R + (size_t)(k / CL) * n;
+      double sq = 0.0;
+      for (int j = k + 2 + lane; j < n; j += 32) sq += rk[j] * rk[j];
+      sq = warp_sum_d(sq);
+      const double alpha = rk[k + 1];
+      double tk = 0.0, beta = alpha, scal = 0.0;
+      if (sq != 0.0) {
+        const double mu = sqrt(alpha * alpha + sq);
+        beta = alpha <= 0.0 ? mu : -mu;
+        tk = (beta - alpha) / beta;
+        scal = 1.0 / (alpha - beta);
+      }
+      for (int j = lane; j < n; j += 32) vown[j] = j <= k ? 0.0 : (j == k + 1 ? 1.0 : rk[j] * scal);
+      __syncwarp();
+      if (lane == 0) {
+        vown[n] = tk;
+        vown[n + 1] = beta;
+        // row k past the diagonal is dead after its reflector: beta and tau go there
+        double* rw = R + (size_t)(k / CL) * n;
+        rw[k + 1] = beta;
+        rw[k + 2] = tk;
+      }
+    }
+    cluster_sync_all();
+    for (int j = k + 1 + tid; j < n; j += blockDim.x) vs[j] = ld_dsmem(vown + j, (unsigned)own);
+    const double tk = ld_dsmem(vown + n, (unsigned)own);
+    __syncthreads();
+    // v(i) of the CTA's rows i >= k + 2 into their dead slot k (column k of V,
+    // written out at the end: no global store inside the loop)
+    {
+      const int lk2 = k + 2 <= c ? 0 : (k + 2 - c + CL - 1) / CL;
+      for (int li = lk2 + tid; li < nr; li += blockDim.x) R[(size_t)li * n + k] = vs[c + li * CL];
+    }
+    if (tk == 0.0) continue;          // the same on every CTA: nothing to update
+    const int li0 = k + 1 <= c ? 0 : (k + 1 - c + CL - 1) / CL;
+    // two rows per warp at a time (independent accumulations), four columns per lane step
+    for (int li = li0 + 2 * wid; li < nr; li += 2 * nw) {
+      const bool two = li + 1 < nr;
+      const double* r0 = R + (size_t)li * n;
+      const double* r1 = two ? r0 + n : r0;
+      double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;
+      int j = k + 1 + lane;
+      for (; j + 32 < n; j += 64) {
+        const double v0 = vs[j], v1 = vs[j + 32];
+        a0 += r0[j] * v0;
+        b0 += r0[j + 32] * v1;
+        a1 += r1[j] * v0;
+        b1 += r1[j + 32] * v1;
+      }
+      if (j < n) {
+        a0 += r0[j] * vs[j];
+        a1 += r1[j] * vs[j];
+      }
+      a0 += b0;
+      a1 += b1;
+      for (int o = 16; o > 0; o >>= 1) {
+        a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+        a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+      }
+      if (lane == 0) {
+        pl[c + li * CL] = tk * a0;
+        if (two) pl[c + (li + 1) * CL] = tk * a1;
+      }
+    }
+    cluster_sync_all();
+    double part = 0.0;
+    for (int j = k + 1 + tid; j < n; j += blockDim.x) {
+      const double pj = ld_dsmem(pl + j, (unsigned)(j % CL));
+      wsm[j] = pj;
+      part += pj * vs[j];
+    }
+    const double kc = 0.5 * tk * block_sum_d(part, red);
+    for (int j = k + 1 + tid; j < n; j += blockDim.x) wsm[j] -= kc * vs[j];
+    __syncthreads();
+    // the rank-2 update, two rows per warp at a time
+    for (int li = li0 + 2 * wid; li < nr; li += 2 * nw) {
+      const bool two = li + 1 < nr;
+      const int i0 = c + li * CL, i1 = two ? i0 + CL : i0;
+      const double v0 = vs[i0], w0 = wsm[i0], v1 = vs[i1], w1 = wsm[i1];
+      double* r0 = R + (size_t)li * n;
+      double* r1 = two ? r0 + n : r0;
+      for (int j = k + 1 + lane; j < n; j += 32) {
+        const double vj = vs[j], wj = wsm[j];
+        r0[j] -= v0 * wj + w0 * vj;
+        if (two) r1[j] -= v1 * wj + w1 * vj;
+      }
+    }
+    __syncthreads();
+  }
+  // write out: d, e, tau of the CTA's rows and its entries of V (V(k, i) =
+  // v_k(i): 0 for i <= k, 1 for i = k + 1, the stored slot beyond; e(n-2)
+  // from row n - 1, as in the one-CTA form)
+  for (int li = tid; li < nr; li += blockDim.x) {
+    const int i = c + li * CL;
+    const double* r = R + (size_t)li * n;
+    d[i] = r[i];
+    if (i + 2 < n) {
+      e[i] = r[i + 1];
+      tau[i] = r[i + 2];
+    } else {
+      tau[i] = 0.0;
+      if (i == n - 1) e[n - 2] = r[n - 2];
+    }
+  }
+  for (int idx = tid; idx < nr * (n - 2); idx += blockDim.x) {
+    const int k = idx / nr, li = idx - k * nr;
+    const int i = c + li * CL;
+    V[(size_t)k * n + i] = i <= k ? 0.0 : (i == k + 1 ? 1.0 : R[(size_t)li * n + k]);
+  }
+  cluster_sync_all();     // no CTA leaves while another may still read its shared memory
+}
+
+// global -> shared copies that hold no register (cp.async, 8-byte elements)
+__device__ __forceinline__ void cpa8(double* dst, const double* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cpa_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+// The back-transformation in blocks of kc <= 8 reflectors (compact WY form):
+// H_kb H_kb+1 ... H_kt = I - V T V^T with T upper triangular, T_ii = tau_i,
+// T(0:i, i) = -tau_i T(0:i, 0:i) (V(:, 0:i)^T v_i).  Chunk c holds the
+// reflectors kb .. kt with kt = n - 3 - c kc; its T goes to Tg[64 c] (8 x 8,
+// T(j, i) at j * 8 + i), one CTA per chunk.
+__global__ void __launch_bounds__(256) k_trd_wy_t(int n, int kc, const double* ws, double* Tg) {
+  __shared__ double S[64], T[64];
+  const int c = blockIdx.x, lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int kt = n - 3 - c * kc, kb = max(0, kt - kc + 1), nk = kt - kb + 1;
+  const double* V = ws + (size_t)kb * n;
+  const double* tau = ws + 2 * (size_t)n * n + 2 * (size_t)n + kb;
+  for (int e = wid; e < nk * nk; e += nw) {
+    const int l = e / nk, i = e - l * nk;
+    if (l > i) continue;
+    double acc = 0.0;
+    for (int r = lane; r < n; r += 32) acc += V[(size_t)l * n + r] * V[(size_t)i * n + r];
+    acc = warp_sum_d(acc);
+    if (lane == 0) S[l * 8 + i] = acc;
+  }
+  if (threadIdx.x < 64) T[threadIdx.x] = 0.0;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < nk; ++i) {
+      const double ti = tau[i];
+      for (int j = 0; j < i; ++j) {
+        double acc = 0.0;
+        for (int l = j; l < i; ++l) acc += T[j * 8 + l] * S[l * 8 + i];
+        T[j * 8 + i] = -ti * acc;
+      }
+      T[i * 8 + i] = ti;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 64) Tg[(size_t)c * 64 + threadIdx.x] = T[threadIdx.x];
+}
+
 // X = H_0 H_1 ... H_{n-3} Z into A's columns: one warp per column, rows
-// lane + 32 q of the column in registers (QM >= n / 32)
+// lane + 32 q of the column in registers (QM >= n / 32).  Per chunk (from the
+// last): y = V^T z (kc independent dots), u = T y, z -= V u.  The chunks are
+// double-buffered in shared memory by cp.async (the next chunk's copies in
+// flight while this one is applied).
+// warps per CTA at most: one wave of CTAs over the SMs where the registers allow
+template <int QM> constexpr int trd_back_maxw() { return QM == 48 ? 10 : 8; }
 template <int QM>
-__global__ void __launch_bounds__(256) k_trd_back_w(int n, double* A, int lda, const double* ws) {
-  extern __shared__ __align__(16) double bw_sm[];   // TRDB_KC x n reflectors, then TRDB_KC taus
-  double* ts = bw_sm + (size_t)TRDB_KC * n;
+__global__ void __launch_bounds__(32 * trd_back_maxw<QM>()) k_trd_back_w(int n, int kc, double* A, int lda,
+                                                                         const double* ws, const double* Tg) {
+  extern __shared__ __align__(16) double bw_sm[];   // two stages of kc x n reflectors + 64 (T)
+  const size_t stage = (size_t)kc * n + 64;
   const double* V = ws;
   const double* Z = ws + (size_t)n * n;
-  const double* tau = ws + 2 * (size_t)n * n + 2 * (size_t)n;
   const int lane = threadIdx.x & 31;
   const int col = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const bool act = col < n;
+  const int nchunk = (n - 2 + kc - 1) / kc;    // reflectors 0 .. n - 3
   double z[QM];
 #pragma unroll
   for (int q = 0; q < QM; ++q) {
     const int r = lane + 32 * q;
     z[q] = (act && r < n) ? Z[(size_t)col * n + r] : 0.0;
   }
-  for (int kt = n - 3; kt >= 0; kt -= TRDB_KC) {
-    const int kb = max(0, kt - TRDB_KC + 1), nk = kt - kb + 1;   // reflectors kb .. kt
+  auto issue = [&](int c, int b) {
+    const int kt = n - 3 - c * kc, kb = max(0, kt - kc + 1), nk = kt - kb + 1;
+    double* dst = bw_sm + b * stage;
+    const double* src = V + (size_t)kb * n;
+    for (int idx = threadIdx.x; idx < nk * n; idx += blockDim.x) cpa8(dst + idx, src + idx);
+    if (threadIdx.x < 64) cpa8(dst + (size_t)kc * n + threadIdx.x, Tg + (size_t)c * 64 + threadIdx.x);
+  };
+  issue(0, 0);
+  cpa_commit();
+  for (int c = 0; c < nchunk; ++c) {
+    const int b = c & 1;
+    if (c + 1 < nchunk) issue(c + 1, b ^ 1);
+    cpa_commit();
+    cpa_wait1();
     __syncthreads();
-    for (int idx = threadIdx.x; idx < nk * n; idx += blockDim.x) bw_sm[idx] = V[(size_t)kb * n + idx];
-    if (threadIdx.x < nk) ts[threadIdx.x] = tau[kb + threadIdx.x];
-    __syncthreads();
-    for (int kk = nk - 1; kk >= 0; --kk) {
-      const double tk = ts[kk];
-      if (tk == 0.0) continue;
-      const int k = kb + kk;
-      const double* vk = bw_sm + (size_t)kk * n;
-      double sacc = 0.0;
+    const int kt = n - 3 - c * kc, kb = max(0, kt - kc + 1), nk = kt - kb + 1;
+    const double* Vb = bw_sm + b * stage;          // Vb[l n + r] = v_{kb + l}(r)
+    const double* Tb = Vb + (size_t)kc * n;
+    double y[8];
 #pragma unroll
-      for (int q = 0; q < QM; ++q) {
-        const int r = lane + 32 * q;
-        if (r > k && r < n) sacc += vk[r] * z[q];
-      }
-      sacc = warp_sum_d(sacc) * tk;
+    for (int l = 0; l < 8; ++l) y[l] = 0.0;
 #pragma unroll
-      for (int q = 0; q < QM; ++q) {
-        const int r = lane + 32 * q;
-        if (r > k && r < n) z[q] -= vk[r] * sacc;
+    for (int q = 0; q < QM; ++q) {
+      const int r = lane + 32 * q;
+      if (r < n) {
+        const double zq = z[q];
+#pragma unroll
+        for (int l = 0; l < 8; ++l)
+          if (l < nk) y[l] += Vb[(size_t)l * n + r] * zq;
       }
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+      for (int l = 0; l < 8; ++l) y[l] += __shfl_xor_sync(0xffffffffu, y[l], o);
+    }
+    double u[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      double acc = 0.0;
+#pragma unroll
+      for (int l = j; l < 8; ++l)
+        if (l < nk) acc += Tb[j * 8 + l] * y[l];
+      u[j] = acc;
+    }
+#pragma unroll
+    for (int q = 0; q < QM; ++q) {
+      const int r = lane + 32 * q;
+      if (r < n) {
+        double acc = z[q];
+#pragma unroll
+        for (int l = 0; l < 8; ++l)
+          if (l < nk) acc -= Vb[(size_t)l * n + r] * u[l];
+        z[q] = acc;
+      }
+    }
+    __syncthreads();    // the next issue refills this buffer
   }
   if (!act) return;
 #pragma unroll
@@ -1172,7 +1437,81 @@ static TrdLargePlan trd_large_plan(int n) {
 
 bool trd_supported(int n) { return n <= TRD_NMAX || trd_large_plan(n).G > 0; }
 
+// the cluster form: CTAs per cluster (0: not possible here) and shared memory
+struct TrdClusterPlan {
+  int CL = 0;
+  size_t smem = 0;
+};
+static TrdClusterPlan trd_cluster_plan(int n) {
+  TrdClusterPlan pl;
+  int dev = 0, optin = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+    return pl;
+  static PerDeviceOnce attr;
+  if (!attr.done()) {
+    if (cudaFuncSetAttribute(k_trd_reduce_cl, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - 1024) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(k_trd_reduce_cl, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+      cudaGetLastError();
+      return pl;
+    }
+    attr.mark();
+  }
+  for (int CL : {8, 16}) {
+    const int nr = (n + CL - 1) / CL;
+    const size_t sm = ((size_t)nr * n + 4 * (size_t)n + 2) * sizeof(double);
+    if (sm + 1024 > (size_t)optin) continue;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(CL);
+    cfg.blockDim = dim3(TRDL_THREADS);
+    cfg.dynamicSmemBytes = sm;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = CL;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int ncl = 0;
+    if (cudaOccupancyMaxActiveClusters(&ncl, k_trd_reduce_cl, &cfg) != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    if (ncl >= 1) {
+      pl.CL = CL;
+      pl.smem = sm;
+      return pl;
+    }
+  }
+  return pl;
+}
+
+static int trd_reduce_cluster(int n, const double* A, int lda, double* wsp, const TrdClusterPlan& pl,
+                              cudaStream_t st) {
+  // the sync record is unused here; cleared so that trd_error reads no stale code
+  PWB_CUDA(cudaMemsetAsync(wsp + trd_ws(n) + 2 * (size_t)n, 0, sizeof(TrdSync), st));
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(pl.CL);
+  cfg.blockDim = dim3(TRDL_THREADS);
+  cfg.dynamicSmemBytes = pl.smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = pl.CL;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  PWB_CUDA(cudaLaunchKernelEx(&cfg, k_trd_reduce_cl, n, A, lda, wsp));
+  return PW_OK;
+}
+
 static int trd_reduce_large(int n, const double* A, int lda, double* wsp, cudaStream_t st) {
+  {
+    const TrdClusterPlan cp = trd_cluster_plan(n);
+    if (cp.CL > 0) return trd_reduce_cluster(n, A, lda, wsp, cp, st);
+  }
   const TrdLargePlan pl = trd_large_plan(n);
   PWB_CHECK(pl.G > 0, PW_EUNSUPPORTED, "tridiagonal reduction: n too large for shared memory");
   int optin = 0, dev = 0;
@@ -1202,23 +1541,35 @@ static int trd_reduce_large(int n, const double* A, int lda, double* wsp, cudaSt
   return PW_OK;
 }
 
-static int trd_back_large(int n, double* A, int lda, const double* wsp, cudaStream_t st) {
-  const int wpc = n <= 512 ? 4 : 8;
-  const size_t sm = ((size_t)TRDB_KC * n + TRDB_KC) * sizeof(double);
+// Tg: at least 64 ceil((n - 2) / 8) doubles of scratch for the chunks' T
+static int trd_back_large(int n, double* A, int lda, const double* wsp, double* Tg, cudaStream_t st) {
+  int optin = 0, dev = 0;
+  PWB_CUDA(cudaGetDevice(&dev));
+  PWB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  // chunk size: two stages of kc x n reflectors (+ T) within shared memory
+  const int kc = std::max(1, std::min(8, (int)(((size_t)optin / 16 - 64) / (size_t)n)));
+  const int nchunk = (n - 2 + kc - 1) / kc;
+  k_trd_wy_t<<<nchunk, 256, 0, st>>>(n, kc, wsp, Tg);
+  // one warp per column, the columns spread over the SMs in one wave where the
+  // CTA size allows (1 CTA per SM: the shared stages and the registers)
+  int nsm = 148;
+  PWB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  const int maxw = n <= 1024 ? 8 : (n <= 1536 ? 10 : 8);
+  const int wpc = std::max(4, std::min(maxw, (n + nsm - 1) / nsm));
+  const size_t sm = 2 * ((size_t)kc * n + 64) * sizeof(double);
   const dim3 grid((n + wpc - 1) / wpc), block(32 * wpc);
   static PerDeviceOnce attr;
   if (!attr.done()) {
-    const int mx = (int)(((size_t)TRDB_KC * TRD_NMAX_L + TRDB_KC) * sizeof(double));
-    PWB_CUDA(cudaFuncSetAttribute(k_trd_back_w<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-    PWB_CUDA(cudaFuncSetAttribute(k_trd_back_w<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-    PWB_CUDA(cudaFuncSetAttribute(k_trd_back_w<48>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-    PWB_CUDA(cudaFuncSetAttribute(k_trd_back_w<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+    PWB_CUDA(cudaFuncSetAttribute(k_trd_back_w<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    PWB_CUDA(cudaFuncSetAttribute(k_trd_back_w<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    PWB_CUDA(cudaFuncSetAttribute(k_trd_back_w<48>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    PWB_CUDA(cudaFuncSetAttribute(k_trd_back_w<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
     attr.mark();
   }
-  if (n <= 512) k_trd_back_w<16><<<grid, block, sm, st>>>(n, A, lda, wsp);
-  else if (n <= 1024) k_trd_back_w<32><<<grid, block, sm, st>>>(n, A, lda, wsp);
-  else if (n <= 1536) k_trd_back_w<48><<<grid, block, sm, st>>>(n, A, lda, wsp);
-  else k_trd_back_w<64><<<grid, block, sm, st>>>(n, A, lda, wsp);
+  if (n <= 512) k_trd_back_w<16><<<grid, block, sm, st>>>(n, kc, A, lda, wsp, Tg);
+  else if (n <= 1024) k_trd_back_w<32><<<grid, block, sm, st>>>(n, kc, A, lda, wsp, Tg);
+  else if (n <= 1536) k_trd_back_w<48><<<grid, block, sm, st>>>(n, kc, A, lda, wsp, Tg);
+  else k_trd_back_w<64><<<grid, block, sm, st>>>(n, kc, A, lda, wsp, Tg);
   return PW_OK;
 }
 
@@ -1259,10 +1610,20 @@ int dense_syevh(int n, double* A, int lda, double* w, DevBuf& ws, cudaStream_t s
   // warps per CTA of the inverse iteration: 6 n doubles each, plus the cluster table
   const size_t per_warp = 6 * (size_t)n * sizeof(double), tab = ((size_t)n + 2) * sizeof(int);
   const int wpc = (int)std::max<size_t>(1, std::min<size_t>(TRD_WARPS_STEIN, ((size_t)optin - tab) / per_warp));
-  const double ortol = large ? 1e-3 * (double)TRD_NMAX / n : 1e-3;
+  const double ortol = large ? 1e-8 : 1e-3;
   k_trd_stein<<<(n + wpc - 1) / wpc, 32 * wpc, wpc * per_warp + tab, st>>>(n, wsp, w, ortol);
   if (large) {
-    if ((rc = trd_back_large(n, A, lda, wsp, st))) return rc;
+    double* Z = wsp + (size_t)n * n;
+    double* Gm = wsp + trd_ws(n) + 2 * (size_t)n + 2;
+    double* Z2 = Gm + (size_t)n * n;
+    for (int pass = 0; pass < 2; ++pass) {
+      double* zi = pass == 0 ? Z : Z2;
+      double* zo = pass == 0 ? Z2 : Z;
+      if ((rc = dense_gemm(1, 0, n, n, n, zi, n, zi, n, Gm, n, st))) return rc;
+      k_lowdin_step<<<n, 128, 0, st>>>(n, Gm);
+      if ((rc = dense_gemm(0, 0, n, n, n, zi, n, Gm, n, zo, n, st))) return rc;
+    }
+    if ((rc = trd_back_large(n, A, lda, wsp, Gm, st))) return rc;   // Gm is free again: the chunks' T
   } else {
     k_trd_back<<<(n + 15) / 16, 256, 0, st>>>(n, A, lda, wsp);
   }
