@@ -518,8 +518,21 @@ __device__ double block_sum_d(double v, double* red) {
 }
 
 // workspace (doubles): V [n n] reflectors (column k), Z [n n] eigenvectors of
-// T, d [n], e [n], tau [n]
-size_t trd_ws(int n) { return (size_t)2 * n * n + 3 * (size_t)n; }
+// T, d [n], e [n], tau [n], the eigenvalues in block order lam [n], then 3 n
+// ints (in 2 n doubles): the first row of each row's block, one past its last
+// row, and the ascending rank of each block-ordered eigenvalue
+__host__ __device__ inline size_t trd_ws(int n) { return (size_t)2 * n * n + 6 * (size_t)n; }
+struct TrdAux {
+  double* lam;
+  int* bs;
+  int* be;
+  int* rank;
+};
+__host__ __device__ inline TrdAux trd_aux(double* ws, int n) {
+  double* lam = ws + 2 * (size_t)n * n + 3 * (size_t)n;
+  int* ib = reinterpret_cast<int*>(lam + n);
+  return TrdAux{lam, ib, ib + n, ib + 2 * n};
+}
 
 __global__ void __launch_bounds__(TRD_THREADS) k_trd_reduce(int n, const double* A, int lda, double* ws) {
   extern __shared__ __align__(16) double trd_sm[];
@@ -683,19 +696,46 @@ __device__ __forceinline__ int trd_sturm(int n, const double* d, const double* e
   return c;
 }
 
-// eigenvalues ascending into w: one warp per eigenvalue, its 32 lanes count
-// at 32 interior points of the bracket per step (33-fold shrink: 11 steps
-// reach the rounding level); T's diagonal and squared off-diagonal in shared
-// memory, the Gershgorin interval recomputed by every CTA
+// T splits where an off-diagonal is negligible, |e_i| <= eps (|d_i| +
+// |d_i+1|) (set to zero; the eigenvalues move by at most eps ||T||): the
+// blocks' eigenvectors have disjoint supports, so degenerate eigenvalues of
+// different blocks (an identity-like overlap matrix splits into 1 x 1 blocks)
+// need no orthogonalisation against each other.  One thread; bs / be: the
+// block of each row.
+__global__ void k_trd_split(int n, double* ws) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double* d = ws + 2 * (size_t)n * n;
+  double* e = d + n;
+  const TrdAux ax = trd_aux(ws, n);
+  int s0 = 0;
+  for (int i = 0; i < n; ++i) {
+    const bool cut = i + 1 == n || fabs(e[i]) <= 2.3e-16 * (fabs(d[i]) + fabs(d[i + 1]));
+    if (i + 1 < n && cut) e[i] = 0.0;
+    if (cut) {
+      for (int r = s0; r <= i; ++r) {
+        ax.bs[r] = s0;
+        ax.be[r] = i + 1;
+      }
+      s0 = i + 1;
+    }
+  }
+}
+
+// eigenvalues by blocks: warp g finds eigenvalue g - bs[g] of the block of row
+// g (lam[g]; ascending within each block), its 32 lanes counting at 32
+// interior points of the bracket per step (33-fold shrink: 11 steps reach the
+// rounding level); T's diagonal and squared off-diagonal in shared memory,
+// the Gershgorin interval of the whole T recomputed by every CTA
 constexpr int TRD_BIS_WARPS = 4;
 constexpr int TRD_BIS_STEPS = 11;
-__global__ void __launch_bounds__(32 * TRD_BIS_WARPS) k_trd_bisect(int n, const double* ws, double* w) {
+__global__ void __launch_bounds__(32 * TRD_BIS_WARPS) k_trd_bisect(int n, double* ws) {
   extern __shared__ __align__(16) double bis_sm[];   // 2 n doubles
   double* sd = bis_sm;
   double* se2 = bis_sm + n;
   __shared__ double s_gl, s_gu, s_pivmin;
   const double* d = ws + 2 * (size_t)n * n;
   const double* e = d + n;
+  const TrdAux ax = trd_aux(ws, n);
   const int tid = threadIdx.x, lane = tid & 31;
   for (int i = tid; i < n; i += blockDim.x) {
     sd[i] = d[i];
@@ -716,13 +756,14 @@ __global__ void __launch_bounds__(32 * TRD_BIS_WARPS) k_trd_bisect(int n, const 
     s_pivmin = 2.3e-308 * fmax(1.0, emax);
   }
   __syncthreads();
-  const int i = blockIdx.x * TRD_BIS_WARPS + (tid >> 5);
-  if (i >= n) return;
+  const int g = blockIdx.x * TRD_BIS_WARPS + (tid >> 5);
+  if (g >= n) return;
+  const int b0 = ax.bs[g], m = ax.be[g] - b0, i = g - b0;
   double lo = s_gl, hi = s_gu;
   for (int step = 0; step < TRD_BIS_STEPS; ++step) {
     const double x = lo + (hi - lo) * (double)(lane + 1) / 33.0;
-    const int c = trd_sturm(n, sd, se2, x, s_pivmin);
-    // eigenvalue i lies where the count passes i: count(lo) <= i < count(hi)
+    const int c = trd_sturm(m, sd + b0, se2 + b0, x, s_pivmin);
+    // eigenvalue i of the block lies where its count passes i: count(lo) <= i < count(hi)
     double nl = c <= i ? x : lo, nh = c > i ? x : hi;
     for (int o = 16; o > 0; o >>= 1) {
       nl = fmax(nl, __shfl_xor_sync(0xffffffffu, nl, o));
@@ -731,7 +772,23 @@ __global__ void __launch_bounds__(32 * TRD_BIS_WARPS) k_trd_bisect(int n, const 
     lo = nl;
     hi = nh;
   }
-  if (lane == 0) w[i] = 0.5 * (lo + hi);
+  if (lane == 0) ax.lam[g] = 0.5 * (lo + hi);
+}
+
+// ascending rank of each block-ordered eigenvalue (ties by block order) and
+// the sorted eigenvalues into w
+__global__ void k_trd_rank(int n, double* ws, double* w) {
+  const TrdAux ax = trd_aux(ws, n);
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n) return;
+  const double x = ax.lam[g];
+  int r = 0;
+  for (int h = 0; h < n; ++h) {
+    const double y = ax.lam[h];
+    r += (y < x) || (y == x && h < g);
+  }
+  ax.rank[g] = r;
+  w[r] = x;
 }
 
 __device__ __forceinline__ double trd_rand(int i, int r) {
@@ -748,28 +805,34 @@ __device__ __forceinline__ double trd_rand(int i, int r) {
 // partial pivoting and runs the solves, the warp orthogonalises and normalises.
 // Shared memory: 6 n doubles per warp, then the cluster table (n + 2 ints).
 // Clusters: neighbours closer than ortol_rel ||T||.
-__global__ void __launch_bounds__(32 * TRD_WARPS_STEIN) k_trd_stein(int n, double* ws, const double* w,
-                                                                    double ortol_rel) {
+__global__ void __launch_bounds__(32 * TRD_WARPS_STEIN) k_trd_stein(int n, double* ws, double ortol_rel) {
   extern __shared__ __align__(16) double st_sm[];
   const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5, wpc = blockDim.x >> 5;
   const int g = blockIdx.x * wpc + wl;
   double* Z = ws + (size_t)n * n;
-  const double* d = ws + 2 * (size_t)n * n;
-  const double* e = d + n;
-  // every CTA scans w itself
+  const double* dT = ws + 2 * (size_t)n * n;
+  const double* eT = dT + n;
+  const TrdAux ax = trd_aux(ws, n);
+  const double* w = ax.lam;
+  // clusters of the block-ordered eigenvalues (every CTA scans them itself):
+  // a new cluster at each block start and wherever the gap exceeds ortol
   int* clus = reinterpret_cast<int*>(st_sm + (size_t)wpc * 6 * n);
   if (threadIdx.x == 0) {
     double tn0 = 0.0;
-    for (int i = 0; i < n; ++i) tn0 = fmax(tn0, fabs(d[i]) + (i + 1 < n ? 2.0 * fabs(e[i]) : 0.0));
+    for (int i = 0; i < n; ++i) tn0 = fmax(tn0, fabs(dT[i]) + (i + 1 < n ? 2.0 * fabs(eT[i]) : 0.0));
     const double ortol = ortol_rel * tn0;
     int nc = 0;
     for (int i = 0; i < n; ++i)
-      if (i == 0 || w[i] - w[i - 1] > ortol) clus[1 + nc++] = i;
+      if (i == 0 || ax.bs[i] == i || w[i] - w[i - 1] > ortol) clus[1 + nc++] = i;
     clus[1 + nc] = n;
     clus[0] = nc;
   }
   __syncthreads();
   if (g >= clus[0]) return;
+  // the cluster's block: rows [b0, b0 + nb) of T
+  const int b0 = ax.bs[clus[1 + g]], nb = ax.be[clus[1 + g]] - b0;
+  const double* d = dT + b0;
+  const double* e = eT + b0;
   double* u = st_sm + (size_t)wl * 6 * n;
   double* s1 = u + n;
   double* s2 = s1 + n;
@@ -777,20 +840,20 @@ __global__ void __launch_bounds__(32 * TRD_WARPS_STEIN) k_trd_stein(int n, doubl
   double* y = l + n;
   double* sw = y + n;          // row interchange at step k (1) or not (0)
   double tn = 0.0;
-  for (int i = lane; i < n; i += 32) tn = fmax(tn, fabs(d[i]) + (i + 1 < n ? 2.0 * fabs(e[i]) : 0.0));
+  for (int i = lane; i < n; i += 32) tn = fmax(tn, fabs(dT[i]) + (i + 1 < n ? 2.0 * fabs(eT[i]) : 0.0));
   for (int o = 16; o > 0; o >>= 1) tn = fmax(tn, __shfl_xor_sync(0xffffffffu, tn, o));
   const double eps = 2.3e-16 * fmax(tn, 1e-300);
   const int c0 = clus[1 + g], c1 = clus[2 + g];
   for (int i = c0; i < c1; ++i) {
     const double lam = w[i];
     if (lane == 0) {
-      // LU of T - lam I with row interchanges (U: pivot u, superdiagonals s1,
-      // s2; u then holds the pivots' reciprocals)
-      double ak = d[0] - lam, bk = n > 1 ? e[0] : 0.0;
-      for (int k = 0; k + 1 < n; ++k) {
+      // LU of the block's T - lam I with row interchanges (U: pivot u,
+      // superdiagonals s1, s2; u then holds the pivots' reciprocals)
+      double ak = d[0] - lam, bk = nb > 1 ? e[0] : 0.0;
+      for (int k = 0; k + 1 < nb; ++k) {
         const double ck = e[k];
         double an = d[k + 1] - lam;
-        const double bn = k + 2 < n ? e[k + 1] : 0.0;
+        const double bn = k + 2 < nb ? e[k + 1] : 0.0;
         if (fabs(ak) >= fabs(ck)) {
           if (ak == 0.0) ak = eps;
           const double m = ck / ak;
@@ -805,16 +868,16 @@ __global__ void __launch_bounds__(32 * TRD_WARPS_STEIN) k_trd_stein(int n, doubl
           bk = -m * bn;
         }
       }
-      u[n - 1] = fabs(ak) < eps ? (ak < 0.0 ? -eps : eps) : ak;
-      s1[n - 1] = 0.0;       // read (times zero) by the register-carried back substitution
-      s2[n - 1] = 0.0;
+      u[nb - 1] = fabs(ak) < eps ? (ak < 0.0 ? -eps : eps) : ak;
+      s1[nb - 1] = 0.0;       // read (times zero) by the register-carried back substitution
+      s2[nb - 1] = 0.0;
       // the solves multiply by the pivots' reciprocals (tiny pivots raised to eps)
-      for (int k = 0; k < n; ++k) {
+      for (int k = 0; k < nb; ++k) {
         const double uk = u[k];
         u[k] = 1.0 / (fabs(uk) < eps ? (uk < 0.0 ? -eps : eps) : uk);
       }
     }
-    for (int r = lane; r < n; r += 32) y[r] = trd_rand(i, r);
+    for (int r = lane; r < nb; r += 32) y[r] = trd_rand(i, b0 + r);
     __syncwarp();
     for (int it = 0; it < 3; ++it) {
       if (lane == 0) {
@@ -822,7 +885,7 @@ __global__ void __launch_bounds__(32 * TRD_WARPS_STEIN) k_trd_stein(int n, doubl
         // FMAs and a product (backward) per step on the dependency chain
         double yk = y[0];
 #pragma unroll 4
-        for (int k = 0; k + 1 < n; ++k) {
+        for (int k = 0; k + 1 < nb; ++k) {
           double yn = y[k + 1];
           if (sw[k] != 0.0) {
             const double t = yk;
@@ -833,10 +896,10 @@ __global__ void __launch_bounds__(32 * TRD_WARPS_STEIN) k_trd_stein(int n, doubl
           y[k] = yk;
           yk = yn;
         }
-        y[n - 1] = yk;
+        y[nb - 1] = yk;
         double y1 = 0.0, y2 = 0.0;   // y[k+1], y[k+2] (zero past the end)
 #pragma unroll 4
-        for (int k = n - 1; k >= 0; --k) {
+        for (int k = nb - 1; k >= 0; --k) {
           const double t = (y[k] - s1[k] * y1 - s2[k] * y2) * u[k];
           y[k] = t;
           y2 = y1;
@@ -844,23 +907,25 @@ __global__ void __launch_bounds__(32 * TRD_WARPS_STEIN) k_trd_stein(int n, doubl
         }
       }
       __syncwarp();
-      // Gram-Schmidt against the cluster's earlier vectors, then normalise
+      // Gram-Schmidt against the cluster's earlier vectors (same block), then normalise
       for (int j = c0; j < i; ++j) {
-        const double* zj = Z + (size_t)j * n;
+        const double* zj = Z + (size_t)ax.rank[j] * n + b0;
         double dt = 0;
-        for (int r = lane; r < n; r += 32) dt += zj[r] * y[r];
+        for (int r = lane; r < nb; r += 32) dt += zj[r] * y[r];
         dt = warp_sum_d(dt);
-        for (int r = lane; r < n; r += 32) y[r] -= dt * zj[r];
+        for (int r = lane; r < nb; r += 32) y[r] -= dt * zj[r];
         __syncwarp();
       }
       double nr = 0;
-      for (int r = lane; r < n; r += 32) nr += y[r] * y[r];
+      for (int r = lane; r < nb; r += 32) nr += y[r] * y[r];
       nr = warp_sum_d(nr);
       const double inv = nr > 0.0 ? 1.0 / sqrt(nr) : 0.0;
-      for (int r = lane; r < n; r += 32) y[r] *= inv;
+      for (int r = lane; r < nb; r += 32) y[r] *= inv;
       __syncwarp();
     }
-    for (int r = lane; r < n; r += 32) Z[(size_t)i * n + r] = y[r];
+    // column rank(i) of Z: the block's rows, zero elsewhere
+    double* zc = Z + (size_t)ax.rank[i] * n;
+    for (int r = lane; r < n; r += 32) zc[r] = (r >= b0 && r < b0 + nb) ? y[r - b0] : 0.0;
     __syncwarp();
   }
 }
@@ -1004,7 +1069,7 @@ __global__ void __launch_bounds__(TRDL_THREADS) k_trd_reduce_mc(int n, const dou
   double* d = ws + 2 * (size_t)n * n;
   double* e = d + n;
   double* tau = e + n;
-  double* pg = tau + n;                    // 2 n: p, double buffered
+  double* pg = ws + trd_ws(n);             // 2 n: p, double buffered
   TrdSync* sy = reinterpret_cast<TrdSync*>(pg + 2 * (size_t)n);
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
   for (int idx = tid; idx < nr * n; idx += blockDim.x) {
@@ -1605,13 +1670,15 @@ int dense_syevh(int n, double* A, int lda, double* w, DevBuf& ws, cudaStream_t s
   } else {
     k_trd_reduce<<<1, TRD_THREADS, ((size_t)n * (n | 1) + 2 * (size_t)n) * sizeof(double), st>>>(n, A, lda, wsp);
   }
+  k_trd_split<<<1, 32, 0, st>>>(n, wsp);
   k_trd_bisect<<<(n + TRD_BIS_WARPS - 1) / TRD_BIS_WARPS, 32 * TRD_BIS_WARPS, 2 * (size_t)n * sizeof(double), st>>>(
-      n, wsp, w);
+      n, wsp);
+  k_trd_rank<<<(n + 127) / 128, 128, 0, st>>>(n, wsp, w);
   // warps per CTA of the inverse iteration: 6 n doubles each, plus the cluster table
   const size_t per_warp = 6 * (size_t)n * sizeof(double), tab = ((size_t)n + 2) * sizeof(int);
   const int wpc = (int)std::max<size_t>(1, std::min<size_t>(TRD_WARPS_STEIN, ((size_t)optin - tab) / per_warp));
   const double ortol = large ? 1e-8 : 1e-3;
-  k_trd_stein<<<(n + wpc - 1) / wpc, 32 * wpc, wpc * per_warp + tab, st>>>(n, wsp, w, ortol);
+  k_trd_stein<<<(n + wpc - 1) / wpc, 32 * wpc, wpc * per_warp + tab, st>>>(n, wsp, ortol);
   if (large) {
     double* Z = wsp + (size_t)n * n;
     double* Gm = wsp + trd_ws(n) + 2 * (size_t)n + 2;
