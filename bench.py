@@ -401,6 +401,93 @@ def scf_bench(device: int, max_iter: int = 60):
     return out
 
 
+def solvers_bench(device: int, max_iter: int = 60):
+    """The block eigensolvers of the reference in the Si64 SCF (FP64, 128
+    occupied + 32 extra bands, tol 1e-6 Ha/atom, eig_max_iter 3): LOBPCG (the
+    reference's default PW_Solver, its [X W P] subspace of 3 x 160 = 480
+    through the library's generalized eigensolver twice per iteration), PPCG
+    (sub-block size 1) and Davidson (2 blocks).  One untimed 2-iteration
+    warm-up per solver, then one timed run bracketed by CUDA events."""
+    import torch
+    from pwdft_develop_b200 import Context
+    L, z, pos = si64_atoms()
+    out = {}
+    for solver in ("lobpcg", "ppcg", "davidson"):
+        c = Context(L, NC, NF, precision="f64", device=device)
+        c.set_atoms(z, pos)
+        c.set_band_batch(NBAND)
+        kw = dict(nocc=128, nextra=32, ecut=20.0, solver=solver, seed=SEED, tol_efree=1e-6)
+        c.scf(max_iter=2, **kw)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        r_, _, _ = c.scf(max_iter=max_iter, **kw)
+        e1.record()
+        torch.cuda.synchronize()
+        out[solver] = dict(seconds=e0.elapsed_time(e1) / 1e3, iterations=r_["iterations"],
+                           converged=bool(r_["converged"]), efree=r_["efree"], hpsi_bands=r_["hpsi_bands"])
+        c.close()
+    out["workload"] = ("Si64 FP64, 160 bands, Anderson(8, 0.7), 300 K, tol 1e-6 Ha/atom, 3 eigensolver "
+                       "iterations per SCF step")
+    return out
+
+
+def dense_bench(device: int):
+    """The library's FP64 dense kernels at the subspace sizes of the Si64
+    eigensolvers: the symmetric eigen-decomposition (pw_dense_syev) at
+    n = 160 (ChebFSI Rayleigh-Ritz), 480 (LOBPCG's 3n) and 1440 (LOBPCG at 480
+    bands), Cholesky and triangular inverse at n = 160.  Random symmetric
+    matrices (seeded); median of 5 calls after 2 untimed, each synchronous."""
+    import ctypes as C
+    import torch
+    from pwdft_develop_b200 import Context
+    from pwdft_develop_b200._lib import check, lib
+    c = Context((10.26,) * 3, (12, 12, 12), (24, 24, 24), precision="f64", device=device)
+
+    def P(t):
+        return C.c_void_p(t.data_ptr())
+    out = {}
+    dev = torch.device("cuda", device)
+    for n in (160, 480, 1440):
+        g = torch.Generator().manual_seed(n)
+        M = torch.randn(n, n, generator=g, dtype=torch.float64)
+        A = (M + M.T).to(dev)
+        w = torch.empty(n, dtype=torch.float64, device=dev)
+        sw = C.c_int(0)
+        ts = []
+        for r in range(7):
+            B = A.clone()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            check(lib.pw_dense_syev(c.handle, n, P(B), n, P(w), C.byref(sw)))
+            ts.append(time.perf_counter() - t0)
+        V = B.T
+        res = float((A @ V - V * w).abs().max() / A.abs().max())
+        orth = float((V.T @ V - torch.eye(n, dtype=torch.float64, device=dev)).abs().max())
+        out[f"syev_n{n}"] = dict(ms=float(np.median(ts[2:])) * 1e3, residual=res, orthogonality=orth,
+                                 jacobi_sweeps=sw.value)
+    n = 160
+    M = torch.randn(n, n, generator=torch.Generator().manual_seed(3), dtype=torch.float64)
+    S = (M @ M.T + n * torch.eye(n, dtype=torch.float64)).to(dev)
+    tp, tt = [], []
+    for r in range(7):
+        B = S.clone()
+        Ui = torch.empty_like(B)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        check(lib.pw_dense_potrf(c.handle, n, P(B), n))
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        check(lib.pw_dense_trtri(c.handle, n, P(B), n, P(Ui), n))
+        torch.cuda.synchronize()
+        tp.append(t1 - t0)
+        tt.append(time.perf_counter() - t1)
+    out["potrf_n160_ms"] = float(np.median(tp[2:])) * 1e3
+    out["trtri_n160_ms"] = float(np.median(tt[2:])) * 1e3
+    c.close()
+    return out
+
+
 def hybrid_bench(device: int):
     """HSE06 SCF time to solution on Si64 (48^3 / 96^3, 128 occupied + 32 extra
     bands, ChebFSI degree 10, mixed precision): the reference's nested scheme
@@ -789,6 +876,12 @@ def summary(line: dict) -> dict:
         out["scf_mixed_s"] = sc["mixed"]["seconds"]
         out["scf_speedup_mixed_vs_f64"] = sc["speedup_mixed_vs_f64"]
         out["scf_efree_agreement_per_atom"] = sc["efree_agreement_per_atom"]
+    if "solvers" in line:
+        for k in ("lobpcg", "ppcg", "davidson"):
+            out[f"scf_{k}_f64_s"] = line["solvers"][k]["seconds"]
+    if "dense" in line:
+        out["syev_n480_ms"] = line["dense"]["syev_n480"]["ms"]
+        out["syev_n1440_ms"] = line["dense"]["syev_n1440"]["ms"]
     if "exx" in line and "exchange_energy_error_per_atom_vs_oracle" in line["exx"]:
         out["exx_energy_error_per_atom_vs_oracle"] = line["exx"]["exchange_energy_error_per_atom_vs_oracle"]
     if "gram" in line:
@@ -1001,6 +1094,10 @@ def run_ours(args):
             line["f64_sweep"] = f64_sweep_bench(local, args.steps, args.warmup)
         if args.scf and world == 1:
             line["scf"] = scf_bench(local)
+        if args.solvers and world == 1:
+            line["solvers"] = solvers_bench(local)
+        if args.dense and world == 1:
+            line["dense"] = dense_bench(local)
         if args.exx and world == 1:
             line["exx"] = exx_bench(local)
             line["hybrid_scf"] = hybrid_bench(local)
@@ -1032,6 +1129,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-f64-sweep", dest="f64_sweep", action="store_false", help="skip the FP64 sweep leg")
     ap.add_argument("--no-scf", dest="scf", action="store_false", help="skip the SCF time-to-solution leg")
+    ap.add_argument("--no-solvers", dest="solvers", action="store_false",
+                    help="skip the LOBPCG / PPCG / Davidson SCF leg")
+    ap.add_argument("--no-dense", dest="dense", action="store_false", help="skip the dense FP64 kernel leg")
     ap.add_argument("--no-exx", dest="exx", action="store_false", help="skip the hybrid-exchange leg")
     ap.add_argument("--no-kpoints", dest="kpoints", action="store_false", help="skip the k-point batch leg")
     ap.add_argument("--no-gspace", dest="gspace", action="store_false", help="skip the sphere-cut (G-space) leg")
