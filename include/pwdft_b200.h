@@ -323,7 +323,7 @@ typedef struct pw_scf_params {
   int verbose;              /* 1: a line per SCF iteration (stderr); 2: phase timers (graphs off);
                                3: as 1 plus the synchronised wall time of each step */
   double ecut;              /* Ecut_Wavefunction (Hartree cut-off 4*Ecut) */
-  double temperature;       /* Kelvin, Fermi-Dirac */
+  double temperature;       /* Kelvin (the smearing width) */
   double eig_tol;           /* Eig_Tolerance */
   double mix_step;          /* Mixing_StepLength */
   double tol_efree;         /* converged when |E_free - E_Harris| / N_atom < tol_efree */
@@ -342,6 +342,8 @@ typedef struct pw_scf_params {
   int no_wfn_filter;        /* PW_SOLVER_CHEBFSI: 0 (default) runs H*psi with the wavefunction cut-off filter at
                                ecut, as the reference's CheFSI does (PWDFT_Cheby_apply_wfn_ecut_filt 1); 1 runs
                                the unfiltered operator (PWDFT_Cheby_apply_wfn_ecut_filt 0).  Other solvers: no filter */
+  int smearing;             /* Smearing_Scheme: 0 "FD" (Fermi-Dirac, default), 1 "GB" (Gaussian, occupation
+                               erfc(-x) / 2, -T S term -exp(-x^2) / (2 beta sqrt(pi)), x = beta (E_F - e)) */
 } pw_scf_params;
 enum { PW_MIX_ANDERSON = 0, PW_MIX_BROYDEN = 1 };
 

@@ -9,7 +9,8 @@ reference source tree (never copied into this repository): ``spline`` and
 ``VCorrelation_pw``, ``VGCExchange_pbx``, ``VGCCorrelation_pbc``
 (src/utility.cpp:3913-4244, the ``Use_Libxc: 0`` path of KohnSham::CalculateXC)
 and the HSE06 short-range PBE exchange ``pbexsr`` with
-``wpbe_analy_erfc_approx_grad`` and ``EXPINT`` (src/utility.cpp:3340-3911).  The recipe extracts each function body from
+``wpbe_analy_erfc_approx_grad`` and ``EXPINT`` (src/utility.cpp:3340-3911), and the smearing functions
+``wgauss`` and ``getEntropy`` (src/utility.cpp:4404-4444).  The recipe extracts each function body from
 ``<reference>/src/utility.cpp`` by brace matching into ``oracle/_ref/`` (git
 ignored), prepends the headers and typedefs it needs (``<stdlib.h>`` first, as
 include/utility.hpp:49 has it: it puts the floating-point ``abs`` overloads
@@ -33,13 +34,15 @@ FUNCS = [("void spline(", "spline"), ("void seval(", "seval"),
          ("void VExchange_sla(", "VExchange_sla"), ("void VCorrelation_pw(", "VCorrelation_pw"),
          ("void VGCExchange_pbx(", "VGCExchange_pbx"), ("void VGCCorrelation_pbc(", "VGCCorrelation_pbc"),
          ("void pbexsr(", "pbexsr"), ("void wpbe_analy_erfc_approx_grad(", "wpbe_analy_erfc_approx_grad"),
-         ("Real EXPINT(", "EXPINT")]
+         ("Real EXPINT(", "EXPINT"), ("Real wgauss(", "wgauss"), ("Real getEntropy(", "getEntropy")]
 
 PRELUDE = """// generated: functions compiled from the reference source tree
 #include <stdlib.h>
 #include <cmath>
 #include <complex>
 #include <stdexcept>
+#include <string>
+#include <algorithm>
 typedef std::complex<double> Complex;
 typedef double Real;
 typedef int Int;
@@ -79,6 +82,11 @@ void ref_wpbe(double rho, double s, double omega, double* out) {
   pwref::wpbe_analy_erfc_approx_grad(rho, s, omega, out[0], out[1], out[2]);
 }
 double ref_expint(int n, double x) { return pwref::EXPINT(n, x); }
+// smearing: 0 "FD", 1 "GB"
+double ref_wgauss(double ev, double ef, double tbeta, int gb) { return pwref::wgauss(ev, ef, tbeta, gb ? "GB" : "FD"); }
+double ref_entropy(double ev, double ef, double tbeta, int gb) {
+  return pwref::getEntropy(ev, ef, tbeta, gb ? "GB" : "FD");
+}
 }
 """
 

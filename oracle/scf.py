@@ -235,13 +235,26 @@ def hartree(dm: pw.Domain, rho: np.ndarray, rho_ps: np.ndarray, ecut: float, gkk
     return v.real.reshape(-1)
 
 
-def wgauss(ev, ef, tbeta):
-    return 1.0 / (1.0 + np.exp(-tbeta * (ef - ev)))
+def wgauss(ev, ef, tbeta, smearing: str = "FD"):
+    """Occupation rate of a state (wgauss, src/utility.cpp:4404-4420):
+    Fermi-Dirac 1 / (1 + exp(-x)) or Gaussian erfc(-x) / 2, x = beta (E_F - e)."""
+    x = tbeta * (ef - np.asarray(ev, dtype=np.float64))
+    if smearing == "GB":
+        return 0.5 * _erfc(-x)
+    return 1.0 / (1.0 + np.exp(-x))
 
 
-def entropy(ev, ef, tbeta):
-    x = tbeta * (ef - ev)
-    out = np.zeros_like(np.asarray(ev, dtype=np.float64))
+def _erfc(x):
+    from scipy.special import erfc
+    return erfc(x)
+
+
+def entropy(ev, ef, tbeta, smearing: str = "FD"):
+    """-T S term of a state (getEntropy, src/utility.cpp:4422-4444)."""
+    x = tbeta * (ef - np.asarray(ev, dtype=np.float64))
+    if smearing == "GB":
+        return -0.5 / tbeta * np.exp(-np.minimum(200.0, x * x)) / math.sqrt(math.pi)
+    out = np.zeros_like(x)
     m = np.abs(x) <= 36.0
     occ = 1.0 / (1.0 + np.exp(-x[m]))
     with np.errstate(divide="ignore", invalid="ignore"):
@@ -250,15 +263,15 @@ def entropy(ev, ef, tbeta):
     return out
 
 
-def occupations(eig: np.ndarray, nocc: int, tbeta: float):
-    """Fermi-Dirac bisection, scf.cpp:1780-1822."""
+def occupations(eig: np.ndarray, nocc: int, tbeta: float, smearing: str = "FD"):
+    """Bisection on the electron count, scf.cpp:1780-1822 (either smearing)."""
     ev = np.sort(eig)
     npsi = ev.size
     if npsi == nocc:
         return np.ones(npsi), ev[-1]
     lb, ub = ev[0], ev[-1]
     ef = 0.5 * (lb + ub)
-    occsum = wgauss(ev, ef, tbeta).sum()
+    occsum = wgauss(ev, ef, tbeta, smearing).sum()
     it = 1
     while abs(occsum - nocc) > 1e-16 and it < 200:
         if occsum < nocc:
@@ -266,9 +279,9 @@ def occupations(eig: np.ndarray, nocc: int, tbeta: float):
         else:
             ub = ef
         ef = 0.5 * (lb + ub)
-        occsum = wgauss(ev, ef, tbeta).sum()
+        occsum = wgauss(ev, ef, tbeta, smearing).sum()
         it += 1
-    return wgauss(eig, ef, tbeta), ef
+    return wgauss(eig, ef, tbeta, smearing), ef
 
 
 @dataclass
@@ -351,7 +364,8 @@ def scf(L, znuc, pos, numGrid, numGridFine, nocc: int, nextra: int, ecut: float,
         temperature: float = 300.0, tol_efree: float = 1e-7, max_iter: int = 60, mix_dim: int = 8,
         mix_step: float = 0.7, eig_tol: float = 1e-11, verbose: bool = False, xc: str = "teter93",
         mix: str = "anderson", tol_rho: float | None = None, phi_max_iter: int = 10,
-        phi_tol: float = 1e-6, wfn_ecut: float | None = None, seed: int = 20261203) -> SCFResult:
+        phi_tol: float = 1e-6, wfn_ecut: float | None = None, seed: int = 20261203,
+        smearing: str = "FD") -> SCFResult:
     """Restated SCF::Iterate with potential Anderson mixing; converges when
     |E_free - E_Harris| / N_atom < tol_efree (the reference's efreeDifPerAtom,
     scf.cpp:467).  xc = "hse06": the nested hybrid scheme (PBE SCF, then phi
@@ -411,13 +425,13 @@ def scf(L, znuc, pos, numGrid, numGridFine, nocc: int, nextra: int, ecut: float,
         else:
             v0 = psi[0] if psi is not None else None
             eig, psi = _eigsh(T, nband, v0=v0, tol=eig_tol, xi=xi, wfn_ecut=wfn_ecut)
-        occ, ef = occupations(eig, nocc, tbeta)
+        occ, ef = occupations(eig, nocc, tbeta, smearing)
         # Harris energy with the input density / potentials (scf.cpp:1987-2140)
         ekin_b = float(np.sum(2 * eig * occ))
         ehart_h = float(np.sum(0.5 * vh * (rho + rho_ps)) * w)
         evxc = float(np.sum(vxc * rho) * w)
         ecor_h = (exc - evxc) - ehart_h - eself
-        efree_h = ekin_b + ecor_h + float(np.sum(2 * entropy(eig, ef, tbeta)))
+        efree_h = ekin_b + ecor_h + float(np.sum(2 * entropy(eig, ef, tbeta, smearing)))
         # new density and potentials
         rho_out = density(T, psi, occ, nocc)
         eps, vxc = xcf(rho_out)
@@ -429,7 +443,7 @@ def scf(L, znuc, pos, numGrid, numGridFine, nocc: int, nextra: int, ecut: float,
         ehart = float(np.sum(0.5 * vh * (rho_out - rho_ps)) * w)
         ecor = ecor + exc + ehart - eself
         etot = ekin_b + ecor
-        efree = etot + float(np.sum(2 * entropy(eig, ef, tbeta)))
+        efree = etot + float(np.sum(2 * entropy(eig, ef, tbeta, smearing)))
         dif = abs(efree - efree_h) / natom
         snorm = scf_norm(dm, (vtot_new - vtot) if inner else (rho_out - rho), ecut)
         hist.append(dict(iter=it, etot=etot, efree=efree, eharris=efree_h, dif=dif, scf_norm=snorm))

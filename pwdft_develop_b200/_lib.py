@@ -48,7 +48,8 @@ class ScfParams(C.Structure):
                 ("mix_step", C.c_double), ("tol_efree", C.c_double), ("refine_threshold", C.c_double),
                 ("seed", C.c_ulonglong), ("ppcg_sbsize", C.c_int), ("davidson_maxdim", C.c_int),
                 ("graphs", C.c_int), ("xc", C.c_int), ("mix_type", C.c_int), ("tol_rho", C.c_double),
-                ("phi_max_iter", C.c_int), ("phi_tol", C.c_double), ("no_wfn_filter", C.c_int)]
+                ("phi_max_iter", C.c_int), ("phi_tol", C.c_double), ("no_wfn_filter", C.c_int),
+                ("smearing", C.c_int)]
 
 
 class ScfResult(C.Structure):

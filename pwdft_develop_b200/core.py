@@ -365,15 +365,18 @@ def _ctx_scf(self, nocc: int, nextra: int, ecut: float, solver: str = "chebfsi",
              mix_step: float = 0.7, tol_efree: float = 1e-6, refine_threshold: float = 1e-4, seed: int = 1,
              verbose: bool = False, ppcg_sbsize: int = 1, davidson_maxdim: int = 2, graphs: bool = False,
              xc: str = "teter93", mix: str = "anderson", tol_rho: float = 0.0, phi_max_iter: int = 10,
-             phi_tol: float = 1e-6, wfn_filter: bool | None = None):
+             phi_tol: float = 1e-6, wfn_filter: bool | None = None, smearing: str = "FD"):
     """SCF::Iterate on the device (FP64 context; mixed=True runs the eigensolver in
     an FP32 twin and refines in FP64).  xc: "teter93", "pbe" or "hse06" (nested
     hybrid scheme with ACE).  wfn_filter: ChebFSI's wavefunction cut-off filter
     at ecut (None or True: on, the reference's CheFSI default; False: off).
-    Returns (result dict, eigenvalues, rho)."""
+    smearing: the reference's Smearing_Scheme, "FD" (Fermi-Dirac) or "GB"
+    (Gaussian).  Returns (result dict, eigenvalues, rho)."""
     xcs = {"teter93": _lib.PW_XC_TETER93, "pbe": _lib.PW_XC_PBE, "hse06": _lib.PW_XC_HSE06}
     if xc not in xcs:
         raise ValueError(f"unknown exchange-correlation functional {xc!r}")
+    if smearing not in ("FD", "GB"):
+        raise ValueError(f"unknown smearing scheme {smearing!r}")
     p = _lib.ScfParams(nocc=nocc, nextra=nextra,
                        solver=_SOLVERS[solver], ppcg_sbsize=ppcg_sbsize, davidson_maxdim=davidson_maxdim,
                        graphs=int(graphs), xc=xcs[xc],
@@ -382,7 +385,8 @@ def _ctx_scf(self, nocc: int, nextra: int, ecut: float, solver: str = "chebfsi",
                        cheby_degree=cheby_degree, cheby_first_cycles=cheby_first_cycles, eig_max_iter=eig_max_iter,
                        max_iter=max_iter, mix_dim=mix_dim, mixed=int(mixed), verbose=int(verbose), ecut=ecut,
                        temperature=temperature, eig_tol=eig_tol, mix_step=mix_step, tol_efree=tol_efree,
-                       refine_threshold=refine_threshold, seed=seed, no_wfn_filter=int(wfn_filter is False))
+                       refine_threshold=refine_threshold, seed=seed, no_wfn_filter=int(wfn_filter is False),
+                       smearing=int(smearing == "GB"))
     r = _lib.ScfResult()
     eig = np.zeros(nocc + nextra)
     rho = np.zeros(self.ntotFine)

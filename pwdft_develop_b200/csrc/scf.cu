@@ -1294,15 +1294,22 @@ int set_vtot_dev(pw_ctx* c, const double* vtot_dev) {
   return PW_OK;
 }
 
-double wgauss(double ev, double ef, double tbeta) { return 1.0 / (1.0 + std::exp(-tbeta * (ef - ev))); }
-double fd_entropy(double ev, double ef, double tbeta) {
+// occupation rate and the -T S term of one state (wgauss / getEntropy,
+// src/utility.cpp:4404-4444): gb = 0 Fermi-Dirac ("FD"), 1 Gaussian ("GB")
+double wgauss(double ev, double ef, double tbeta, int gb) {
   const double x = tbeta * (ef - ev);
+  return gb ? 0.5 * std::erfc(-x) : 1.0 / (1.0 + std::exp(-x));
+}
+double smear_entropy(double ev, double ef, double tbeta, int gb) {
+  const double x = tbeta * (ef - ev);
+  if (gb) return -0.5 / tbeta * std::exp(-std::min(200.0, x * x)) / std::sqrt(M_PI);
   if (std::fabs(x) > 36.0) return 0.0;
   const double occ = 1.0 / (1.0 + std::exp(-x));
   return (occ * std::log(occ) + (1.0 - occ) * std::log(1.0 - occ)) / tbeta;
 }
 
-void occupations(const std::vector<double>& eig, int nocc, double tbeta, std::vector<double>& occ, double& ef) {
+void occupations(const std::vector<double>& eig, int nocc, double tbeta, int gb, std::vector<double>& occ,
+                 double& ef) {
   std::vector<double> ev(eig);
   std::sort(ev.begin(), ev.end());
   const int npsi = (int)ev.size();
@@ -1310,7 +1317,7 @@ void occupations(const std::vector<double>& eig, int nocc, double tbeta, std::ve
   if (npsi == nocc) { ef = ev[npsi - 1]; return; }
   double lb = ev[0], ub = ev[npsi - 1];
   ef = 0.5 * (lb + ub);
-  auto sum = [&](double f) { double s = 0; for (double e : ev) s += wgauss(e, f, tbeta); return s; };
+  auto sum = [&](double f) { double s = 0; for (double e : ev) s += wgauss(e, f, tbeta, gb); return s; };
   double os = sum(ef);
   int it = 1;
   while (std::fabs(os - nocc) > 1e-16 && it < 200) {
@@ -1319,7 +1326,7 @@ void occupations(const std::vector<double>& eig, int nocc, double tbeta, std::ve
     os = sum(ef);
     ++it;
   }
-  for (int j = 0; j < npsi; ++j) occ[j] = wgauss(eig[j], ef, tbeta);
+  for (int j = 0; j < npsi; ++j) occ[j] = wgauss(eig[j], ef, tbeta, gb);
 }
 
 }  // namespace
@@ -1332,6 +1339,7 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
   PWB_CHECK(!ctx->atom_z.empty(), PW_ENOTREADY, "atoms not set (pw_set_atoms)");
   PWB_CHECK(p->nocc > 0 && p->nextra >= 0 && p->ecut > 0, PW_EINVAL, "bad SCF parameters");
   PWB_CHECK(p->solver >= PW_SOLVER_LOBPCG && p->solver <= PW_SOLVER_DAVIDSON, PW_EINVAL, "unknown eigensolver");
+  PWB_CHECK(p->smearing == 0 || p->smearing == 1, PW_EINVAL, "unknown smearing scheme");
   PWB_CUDA(cudaSetDevice(ctx->device));
   const auto t_start = std::chrono::steady_clock::now();
   if (!ctx->scf_cache) {
@@ -1645,11 +1653,11 @@ int pw_scf_run(pw_ctx* ctx, const pw_scf_params* p, pw_scf_result* r, double* ei
     }
     }
     eig = sv.eig;
-    occupations(eig, p->nocc, tbeta, occ, ef);
+    occupations(eig, p->nocc, tbeta, p->smearing, occ, ef);
     double ekin = 0, ent = 0;
     for (int i = 0; i < nb; ++i) {
       ekin += 2.0 * eig[i] * occ[i];
-      ent += 2.0 * fd_entropy(eig[i], ef, tbeta);
+      ent += 2.0 * smear_entropy(eig[i], ef, tbeta, p->smearing);
     }
     // new density, and with its norm (one reduction) the Harris energy of the
     // input density and potentials (scf.cpp:2025-2060)

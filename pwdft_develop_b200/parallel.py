@@ -375,21 +375,28 @@ def exx_apply_dist(set_phi, apply_exx, Xb, occ, nband: int):
 AU2K = 315774.67
 
 
-def fermi_occupations(eig, nocc: int, tbeta: float):
-    """Fermi-Dirac occupation rates and Fermi level by bisection on the
-    electron count (SCF::CalculateOccupationRate, src/SCF/scf.cpp:1780-1822);
-    eig: all bands, ascending.  numpy arrays."""
+def _wgauss(ev, ef, tbeta, smearing):
+    import numpy as np
+    x = np.clip(tbeta * (ef - ev), -700.0, 700.0)
+    if smearing == "GB":
+        from scipy.special import erfc
+        return 0.5 * erfc(-x)
+    return 1.0 / (1.0 + np.exp(-x))
+
+
+def fermi_occupations(eig, nocc: int, tbeta: float, smearing: str = "FD"):
+    """Occupation rates and Fermi level by bisection on the electron count
+    (SCF::CalculateOccupationRate, src/SCF/scf.cpp:1780-1822) with wgauss
+    (src/utility.cpp:4404-4420): smearing "FD" (Fermi-Dirac) or "GB"
+    (Gaussian); eig: all bands, ascending.  numpy arrays."""
     import numpy as np
     ev = np.asarray(eig, dtype=np.float64)
     if ev.size == nocc:
         return np.ones(ev.size), float(ev[-1])
-
-    def wg(ef):
-        return 1.0 / (1.0 + np.exp(np.clip(-tbeta * (ef - ev), -700.0, 700.0)))
     lb, ub = float(ev.min()), float(ev.max())
     ef = 0.5 * (lb + ub)
     for _ in range(200):
-        s = wg(ef).sum()
+        s = _wgauss(ev, ef, tbeta, smearing).sum()
         if abs(s - nocc) <= 1e-16:
             break
         if s < nocc:
@@ -397,13 +404,16 @@ def fermi_occupations(eig, nocc: int, tbeta: float):
         else:
             ub = ef
         ef = 0.5 * (lb + ub)
-    return wg(ef), ef
+    return _wgauss(ev, ef, tbeta, smearing), ef
 
 
-def fermi_entropy(eig, ef: float, tbeta: float):
-    """Per-band -T S term of the free energy (scf.cpp:1960-1984), numpy."""
+def fermi_entropy(eig, ef: float, tbeta: float, smearing: str = "FD"):
+    """Per-band -T S term of the free energy (getEntropy, src/utility.cpp:
+    4422-4444; scf.cpp:1960-1984), numpy."""
     import numpy as np
     x = tbeta * (ef - np.asarray(eig, dtype=np.float64))
+    if smearing == "GB":
+        return -0.5 / tbeta * np.exp(-np.minimum(200.0, x * x)) / np.sqrt(np.pi)
     out = np.zeros_like(x)
     m = np.abs(x) <= 36.0
     f = 1.0 / (1.0 + np.exp(-x[m]))
@@ -442,7 +452,7 @@ class AndersonMixer:
 
 def scf_dist(ops, Xb, nband: int, nocc: int, tol_efree: float = 1e-6, max_iter: int = 60, degree: int = 10,
              first_cycles: int = 5, mix_dim: int = 8, mix_step: float = 0.7, temperature: float = 300.0,
-             ctx=None, verbose: bool = False):
+             ctx=None, verbose: bool = False, smearing: str = "FD"):
     """SCF::Iterate (src/SCF/scf.cpp:372-591) over band shards: each rank
     filters and holds its bands (band_range), the subspace steps run on grid
     rows (chebfsi_dist's Cholesky-QR and Rayleigh-Ritz), the density is the
@@ -498,8 +508,8 @@ def scf_dist(ops, Xb, nband: int, nocc: int, tol_efree: float = 1e-6, max_iter: 
             lam, Xr, _ = rayleigh_ritz_rows(Yr, band_to_rows(ops.apply_h(Yb), nband), ctx)
             Xb = rows_to_band(Xr, ntot)
         eig = lam.double().cpu().numpy()
-        occ, ef = fermi_occupations(eig, nocc, tbeta)
-        ent = float(np.sum(2.0 * fermi_entropy(eig, ef, tbeta)))
+        occ, ef = fermi_occupations(eig, nocc, tbeta, smearing)
+        ent = float(np.sum(2.0 * fermi_entropy(eig, ef, tbeta, smearing)))
         ekin = float(np.sum(2.0 * eig * occ))
         # Harris energy with the input density and potentials (scf.cpp:1987-2140)
         ehart_h = float((0.5 * vh * (rho + rho_ps)).sum()) * w

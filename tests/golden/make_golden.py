@@ -8,7 +8,11 @@ the HSE06 short-range exchange ``pbexsr`` / ``wpbe_analy_erfc_approx_grad``
 (src/utility.cpp:3340-3846) -> ``ref_xc_hse.npz``, all compiled from the
 reference source tree by ``oracle/build_ref.py``.  Inputs are seeded.  Run
 from the repository root:
-``python tests/golden/make_golden.py [utility|pbe|hse|hpsi]`` (all by default).
+``python tests/golden/make_golden.py [utility|pbe|hse|hpsi|smearing]`` (all by default).
+
+``smearing`` -> ``ref_smearing.npz``: the occupation and entropy functions
+``wgauss`` / ``getEntropy`` (src/utility.cpp:4404-4444) for the Fermi-Dirac
+and Gaussian schemes at seeded arguments.
 
 ``hpsi`` -> ``ref_hpsi.npz``: the reference's own H*psi composition,
 Spinor::AddMultSpinorFineR2C and Spinor::AddTeterPrecond (src/SCF/spinor.cpp:
@@ -152,6 +156,30 @@ def hpsi():
     print(OUT_HPSI, OUT_HPSI.stat().st_size)
 
 
+OUT_SMEAR = Path(__file__).resolve().parent / "ref_smearing.npz"
+
+
+def smearing():
+    """wgauss and getEntropy (src/utility.cpp:4404-4444) for both smearing
+    schemes ("FD", "GB") at seeded (e, E_F, beta) triples spanning the
+    |x| <= 36 cut of the Fermi-Dirac entropy and the 200 cap of the Gaussian
+    one -> ref_smearing.npz."""
+    lib = C.CDLL(str(build_ref.build()))
+    lib.ref_wgauss.restype = C.c_double
+    lib.ref_entropy.restype = C.c_double
+    rng = np.random.Generator(np.random.Philox(20261203 + 7))
+    n = 400
+    ev = rng.uniform(-0.5, 0.5, n)
+    ef = rng.uniform(-0.2, 0.2, n)
+    tbeta = 10.0 ** rng.uniform(1.0, 4.0, n)
+    out = np.zeros((n, 4))
+    for i in range(n):
+        a = (C.c_double(ev[i]), C.c_double(ef[i]), C.c_double(tbeta[i]))
+        out[i] = [lib.ref_wgauss(*a, 0), lib.ref_wgauss(*a, 1), lib.ref_entropy(*a, 0), lib.ref_entropy(*a, 1)]
+    np.savez_compressed(OUT_SMEAR, ev=ev, ef=ef, tbeta=tbeta, out=out)
+    print(OUT_SMEAR, OUT_SMEAR.stat().st_size)
+
+
 if __name__ == "__main__":
     which = sys.argv[1] if len(sys.argv) > 1 else "all"
     if which in ("all", "utility"):
@@ -162,3 +190,5 @@ if __name__ == "__main__":
         hse()
     if which in ("all", "hpsi"):
         hpsi()
+    if which in ("all", "smearing"):
+        smearing()

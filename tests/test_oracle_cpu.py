@@ -422,3 +422,26 @@ def test_compiled_reference_threaded_sweep_matches_restatement():
                                        beta, wgt, 7, np.ascontiguousarray(psi), h, 3) == 0
     ref = pw.mult_spinor(T, psi)
     assert np.abs(h - ref).max() / np.abs(ref).max() < 1e-13
+
+
+def test_smearing_matches_reference_functions():
+    """The occupation rate and -T S term of one state for both smearing schemes
+    (Fermi-Dirac "FD", Gaussian "GB") against the reference's wgauss /
+    getEntropy compiled from its source (ref_smearing.npz, 400 seeded points):
+    the oracle's restatement and the band-distributed SCF's host copy."""
+    from oracle import scf
+    from pwdft_develop_b200.parallel import fermi_entropy
+    g = np.load(Path(__file__).resolve().parent / "golden" / "ref_smearing.npz")
+    ev, ef, tb, out = g["ev"], g["ef"], g["tbeta"], g["out"]
+    for j, sm in enumerate(("FD", "GB")):
+        w = np.array([scf.wgauss(ev[i], ef[i], tb[i], sm) for i in range(len(ev))])
+        e = np.array([scf.entropy(np.array([ev[i]]), ef[i], tb[i], sm)[0] for i in range(len(ev))])
+        assert np.abs(w - out[:, j]).max() <= 1e-15
+        assert np.abs(e - out[:, 2 + j]).max() <= 1e-15 * max(1.0, np.abs(out[:, 2 + j]).max())
+    e = np.array([fermi_entropy(np.array([ev[i]]), ef[i], tb[i])[0] for i in range(len(ev))])
+    assert np.abs(e - out[:, 2]).max() <= 1e-15
+    # the electron count the bisection fixes, either scheme
+    eig = np.sort(np.random.default_rng(5).uniform(-0.3, 0.4, 24))
+    for sm in ("FD", "GB"):
+        occ, efermi = scf.occupations(eig, 16, 315774.67 / 3000.0, sm)
+        assert abs(occ.sum() - 16) < 1e-10
