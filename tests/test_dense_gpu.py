@@ -105,6 +105,50 @@ def test_syev(n, kind):
     c.close()
 
 
+@pytest.mark.parametrize("n", [40, 161, 480, 1440])
+@pytest.mark.parametrize("kind", ["identity", "blocks"])
+def test_syev_split_tridiagonal(n, kind):
+    """Matrices whose tridiagonal form splits into blocks at negligible
+    off-diagonals: the identity plus rounding-level noise (LOBPCG / Davidson
+    overlap matrices of orthonormal blocks: n 1 x 1 blocks, all eigenvalues
+    equal) and a block-diagonal matrix of three decoupled blocks sharing a
+    threefold eigenvalue (degenerate across blocks).  Eigenvalues ascending,
+    eigenvectors orthonormal and accurate."""
+    import torch
+    from pwdft_develop_b200._lib import check, lib
+    c = _ctx()
+    g = torch.Generator().manual_seed(11 * n)
+    if kind == "identity":
+        E = 1e-17 * torch.randn(n, n, generator=g, dtype=torch.float64)
+        A = torch.eye(n, dtype=torch.float64) + E + E.T
+    else:
+        A = torch.zeros(n, n, dtype=torch.float64)
+        sizes = [n // 3, n // 3, n - 2 * (n // 3)]
+        o = 0
+        for m in sizes:
+            Q, _ = torch.linalg.qr(torch.randn(m, m, generator=g, dtype=torch.float64))
+            d = torch.linspace(-1.0, 1.0, m, dtype=torch.float64)
+            d[m // 2] = 0.25       # the eigenvalue every block shares
+            A[o:o + m, o:o + m] = (Q * d) @ Q.T
+            o += m
+        A = 0.5 * (A + A.T)
+        P = torch.randperm(n, generator=g)
+        A = A[P][:, P]             # the blocks interleaved: the reduction has to find them
+    A = A.cuda()
+    V = A.clone()
+    w = torch.empty(n, dtype=torch.float64, device="cuda")
+    sw = C.c_int(-1)
+    check(lib.pw_dense_syev(c.handle, n, _ptr(V), n, _ptr(w), C.byref(sw)))
+    ref = torch.linalg.eigvalsh(A)
+    assert float((w - ref).abs().max()) < 1e-12 * n ** 0.5
+    assert bool((w[1:] >= w[:-1]).all())
+    E = V
+    assert float((E @ E.T - torch.eye(n, dtype=torch.float64, device="cuda")).abs().max()) < 1e-10
+    R = E @ A - w[:, None] * E
+    assert float(R.abs().max()) < 1e-10
+    c.close()
+
+
 @pytest.mark.parametrize("n", [161, 480, 1440])
 @pytest.mark.parametrize("kind", ["overlap", "ritz"])
 def test_syev_large_subspace(n, kind):
