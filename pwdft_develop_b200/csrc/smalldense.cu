@@ -20,6 +20,9 @@
 // until the caller reads them.
 #include <algorithm>
 #include <cmath>
+#include <map>
+#include <mutex>
+#include <utility>
 
 #include "blockops.hpp"
 #include "common.hpp"
@@ -700,24 +703,47 @@ __device__ __forceinline__ int trd_sturm(int n, const double* d, const double* e
 // |d_i+1|) (set to zero; the eigenvalues move by at most eps ||T||): the
 // blocks' eigenvectors have disjoint supports, so degenerate eigenvalues of
 // different blocks (an identity-like overlap matrix splits into 1 x 1 blocks)
-// need no orthogonalisation against each other.  One thread; bs / be: the
-// block of each row.
-__global__ void k_trd_split(int n, double* ws) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// need no orthogonalisation against each other.  One CTA of TRD_SPLIT_T
+// threads, n <= 2 TRD_SPLIT_T: bs[r] (the block's first row) is the running
+// maximum of the block starts up to r, be[r] (one past its last row) the
+// running minimum of the block ends from r on, both by scans in shared memory.
+constexpr int TRD_SPLIT_T = 1024;
+__global__ void __launch_bounds__(TRD_SPLIT_T) k_trd_split(int n, double* ws) {
+  __shared__ int st[2 * TRD_SPLIT_T], en[2 * TRD_SPLIT_T];
   double* d = ws + 2 * (size_t)n * n;
   double* e = d + n;
   const TrdAux ax = trd_aux(ws, n);
-  int s0 = 0;
-  for (int i = 0; i < n; ++i) {
-    const bool cut = i + 1 == n || fabs(e[i]) <= 2.3e-16 * (fabs(d[i]) + fabs(d[i + 1]));
-    if (i + 1 < n && cut) e[i] = 0.0;
-    if (cut) {
-      for (int r = s0; r <= i; ++r) {
-        ax.bs[r] = s0;
-        ax.be[r] = i + 1;
-      }
-      s0 = i + 1;
+  for (int r = threadIdx.x; r < n; r += blockDim.x) {
+    const bool cut = r + 1 == n || fabs(e[r]) <= 2.3e-16 * (fabs(d[r]) + fabs(d[r + 1]));
+    // row r + 1 starts a block when r ends one
+    en[r] = cut ? r + 1 : n;
+    if (r + 1 < n) st[r + 1] = cut ? r + 1 : 0;
+    if (r == 0) st[0] = 0;
+  }
+  __syncthreads();
+  for (int r = threadIdx.x; r + 1 < n; r += blockDim.x)
+    if (en[r] == r + 1) e[r] = 0.0;
+  // inclusive max-scan of st (forward) and min-scan of en (backward)
+  for (int off = 1; off < n; off <<= 1) {
+    int a[2], b[2];
+    for (int q = 0; q < 2; ++q) {
+      const int r = threadIdx.x + q * blockDim.x;
+      a[q] = (r < n && r >= off) ? max(st[r], st[r - off]) : (r < n ? st[r] : 0);
+      b[q] = (r < n && r + off < n) ? min(en[r], en[r + off]) : (r < n ? en[r] : n);
     }
+    __syncthreads();
+    for (int q = 0; q < 2; ++q) {
+      const int r = threadIdx.x + q * blockDim.x;
+      if (r < n) {
+        st[r] = a[q];
+        en[r] = b[q];
+      }
+    }
+    __syncthreads();
+  }
+  for (int r = threadIdx.x; r < n; r += blockDim.x) {
+    ax.bs[r] = st[r];
+    ax.be[r] = en[r];
   }
 }
 
@@ -1478,7 +1504,7 @@ struct TrdLargePlan {
   int G = 0;
   size_t smem = 0;
 };
-static TrdLargePlan trd_large_plan(int n) {
+static TrdLargePlan trd_large_plan_build(int n) {
   TrdLargePlan pl;
   if (n <= TRD_NMAX || n > TRD_NMAX_L) return pl;
   int dev = 0, nsm = 0, optin = 0;
@@ -1500,6 +1526,7 @@ static TrdLargePlan trd_large_plan(int n) {
   }
 }
 
+static TrdLargePlan trd_large_plan(int n);
 bool trd_supported(int n) { return n <= TRD_NMAX || trd_large_plan(n).G > 0; }
 
 // the cluster form: CTAs per cluster (0: not possible here) and shared memory
@@ -1507,7 +1534,7 @@ struct TrdClusterPlan {
   int CL = 0;
   size_t smem = 0;
 };
-static TrdClusterPlan trd_cluster_plan(int n) {
+static TrdClusterPlan trd_cluster_plan_build(int n) {
   TrdClusterPlan pl;
   int dev = 0, optin = 0;
   if (cudaGetDevice(&dev) != cudaSuccess ||
@@ -1550,6 +1577,31 @@ static TrdClusterPlan trd_cluster_plan(int n) {
     }
   }
   return pl;
+}
+
+// the plans per (device, n), built once (the occupancy queries cost host time)
+static std::mutex g_trd_mu;
+static TrdLargePlan trd_large_plan(int n) {
+  static std::map<std::pair<int, int>, TrdLargePlan> cache;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(g_trd_mu);
+  auto it = cache.find({dev, n});
+  if (it != cache.end()) return it->second;
+  return cache[{dev, n}] = trd_large_plan_build(n);
+}
+static TrdClusterPlan trd_cluster_plan(int n) {
+  static std::map<std::pair<int, int>, TrdClusterPlan> cache;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  {
+    std::lock_guard<std::mutex> lk(g_trd_mu);
+    auto it = cache.find({dev, n});
+    if (it != cache.end()) return it->second;
+  }
+  const TrdClusterPlan pl = trd_cluster_plan_build(n);
+  std::lock_guard<std::mutex> lk(g_trd_mu);
+  return cache[{dev, n}] = pl;
 }
 
 static int trd_reduce_cluster(int n, const double* A, int lda, double* wsp, const TrdClusterPlan& pl,
@@ -1670,7 +1722,7 @@ int dense_syevh(int n, double* A, int lda, double* w, DevBuf& ws, cudaStream_t s
   } else {
     k_trd_reduce<<<1, TRD_THREADS, ((size_t)n * (n | 1) + 2 * (size_t)n) * sizeof(double), st>>>(n, A, lda, wsp);
   }
-  k_trd_split<<<1, 32, 0, st>>>(n, wsp);
+  k_trd_split<<<1, TRD_SPLIT_T, 0, st>>>(n, wsp);
   k_trd_bisect<<<(n + TRD_BIS_WARPS - 1) / TRD_BIS_WARPS, 32 * TRD_BIS_WARPS, 2 * (size_t)n * sizeof(double), st>>>(
       n, wsp);
   k_trd_rank<<<(n + 127) / 128, 128, 0, st>>>(n, wsp, w);
