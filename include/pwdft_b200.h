@@ -93,6 +93,15 @@ PW_API int pw_set_gemm_mode(pw_ctx* ctx, int mode, int terms);
 /* When enabled, every H*psi call synchronises and returns PW_ETIMEOUT if a
  * bounded device-side pipeline wait gave up (default off). */
 PW_API int pw_set_check_errors(pw_ctx* ctx, int enable);
+/* Dense projector mode: run the projector GEMMs of an H*psi batch (Q D Q^T psi
+ * depends on psi only) on a second stream of the context while the FFT chain
+ * runs, joined before the last coarse transform, which then accumulates
+ * into the GEMMs' output (1; the default of FP32 contexts); 0 runs them
+ * after the FFT chain on the caller's stream (the default of FP64 contexts,
+ * whose FP64 GEMMs gain nothing from the overlap).  Overwriting calls give
+ * the same bits either way.  While pw_profile is on the GEMMs run after the
+ * FFT chain, so each kernel is timed alone.  No reference counterpart. */
+PW_API int pw_set_nl_overlap(pw_ctx* ctx, int on);
 /* Limit of every bounded wait inside the tensor-core GEMM pipeline on the
  * context's device (all contexts of that device; default 2 s).  On timeout a
  * kernel records an error code, waits (at least 2 s) for the copies and MMAs it

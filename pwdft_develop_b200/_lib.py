@@ -82,6 +82,7 @@ SIGNATURES: dict[str, tuple] = {
     "pw_teter_precond_noalloc": (_i, [_vp, _vp, _i, _vp, _i, _i, _i, _vp]),
     "pw_set_wfn_filter": (_i, [_vp, _i, C.c_double]),
     "pw_set_wait_limit": (_i, [_vp, C.c_double]),
+    "pw_set_nl_overlap": (_i, [_vp, _i]),
     "pw_set_fft_variant": (_i, [_vp, _i]),
     "pw_dense_potrf": (_i, [_vp, _i, _vp, _i]),
     "pw_rotate": (_i, [_vp, _vp, _i, _i, _vp, _i, _i, _vp, _i, _i, _vp]),

@@ -303,6 +303,12 @@ def _ctx_set_gemm_mode(self, mode: str = "tc", terms: int = 3):
     check(lib.pw_set_gemm_mode(self._h, 0, int(terms)))
 
 
+def _ctx_set_nl_overlap(self, on: bool = True):
+    """Dense projector mode: the projector GEMMs of an H*psi batch on a
+    second stream alongside the FFT chain (default on)."""
+    check(lib.pw_set_nl_overlap(self._h, int(bool(on))))
+
+
 def _ctx_set_check_errors(self, on: bool = True):
     check(lib.pw_set_check_errors(self._h, int(on)))
 
@@ -310,6 +316,7 @@ def _ctx_set_check_errors(self, on: bool = True):
 Context.gram = _ctx_gram
 Context.set_gemm_mode = _ctx_set_gemm_mode
 Context.set_check_errors = _ctx_set_check_errors
+Context.set_nl_overlap = _ctx_set_nl_overlap
 Context.set_atoms = _ctx_set_atoms
 Context.pseudocharge = _ctx_pseudocharge
 Context.launches = _ctx_launches

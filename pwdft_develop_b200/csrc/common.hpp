@@ -219,6 +219,11 @@ struct pw_ctx {
   bool gsx_phi_ready = false;            // gsx_phir holds phi(r) of the current exchange orbitals
   cudaStream_t io_st[3] = {nullptr, nullptr, nullptr};   // host->device, compute, device->host (pw_hpsi_host)
   int host_chunk = 32;                                    // bands per pw_hpsi_host chunk
+  // dense projector mode: the projector GEMMs of an H*psi batch on their own
+  // stream alongside the FFT chain (pw_set_nl_overlap; set per precision at creation)
+  int nl_overlap = 1;
+  cudaStream_t nl_st = nullptr;
+  cudaEvent_t nl_fork = nullptr, nl_join = nullptr;
   void* scf_cache = nullptr;                              // pw_scf_run workspace kept between runs
   void (*scf_cache_free)(void*) = nullptr;
 };

@@ -1597,6 +1597,27 @@ struct Plan {
     const T inv_nc = (T)(1.0 / (double)c->ntot);
     const T inv_nf = (T)(1.0 / (double)c->ntotf);
     const int ntx = (N0 + TX - 1) / TX;
+    // dense projector mode: Q D Q^T psi depends on psi only, so its GEMMs run
+    // on a second stream while the FFT chain runs (their first output goes to
+    // the rows of out, which k_cxy_inv then accumulates into after the join);
+    // with pw_profile on they run after it, so each kernel is timed alone
+    const int nbnl = std::min(2 * npair, nband - band0);
+    const bool dense_nl = c->nl_mode == PW_NL_DENSE && c->have_nl && c->nproj > 0 && nbnl > 0;
+    cudaStream_t sn = nullptr;
+    if (dense_nl && c->nl_overlap && !c->prof_on) {
+      if (!c->nl_st) PWB_CUDA(cudaStreamCreateWithFlags(&c->nl_st, cudaStreamNonBlocking));
+      if (!c->nl_fork) PWB_CUDA(cudaEventCreateWithFlags(&c->nl_fork, cudaEventDisableTiming));
+      if (!c->nl_join) PWB_CUDA(cudaEventCreateWithFlags(&c->nl_join, cudaEventDisableTiming));
+      sn = c->nl_st;
+      PWB_CUDA(cudaEventRecord(c->nl_fork, st));
+      PWB_CUDA(cudaStreamWaitEvent(sn, c->nl_fork, 0));
+      if ((rc = dense_apply(c, nl_set(c, filt), psi + (long)band0 * ld, ld, out + (long)band0 * ldo, ldo, nbnl, sn,
+                            accumulate))) {
+        cudaStreamWaitEvent(st, c->nl_fork, 0);
+        return rc;
+      }
+      PWB_CUDA(cudaEventRecord(c->nl_join, sn));
+    }
     { Launch L_(c, st, KK_CXY_FWD);
     k_cxy_fwd<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(psi, ld, nband, band0, AD, tw(c, 0), tw(c, 1)); }
     { Launch L_(c, st, KK_ZPAD);
@@ -1608,12 +1629,13 @@ struct Plan {
       { Launch L_(c, st, KK_ZFOLD);
       k_zfold<T, N2, NF2, TXF><<<dim3(N1, (N0 + TXF - 1) / TXF, npair), PENCIL_THREADS, sm_zfold(), st>>>(
           BC, K, AD, N0, N1, tw(c, 2), tw(c, 5), 0, (T)0, 0, filt ? reinterpret_cast<const T*>(c->wmask.p) : nullptr); }
+      if (sn) PWB_CUDA(cudaStreamWaitEvent(st, c->nl_join, 0));
       { Launch L_(c, st, KK_CXY_INV);
-      k_cxy_inv<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(AD, out, ldo, nband, band0, accumulate, tw(c, 0), tw(c, 1)); }
+      k_cxy_inv<T, N0, N1><<<dim3(N2, npair), PLANE_THREADS, sm_cxy(), st>>>(AD, out, ldo, nband, band0,
+                                                                          sn ? 1 : accumulate, tw(c, 0), tw(c, 1)); }
       PWB_CUDA(cudaGetLastError());
-      const int nb = std::min(2 * npair, nband - band0);
-      if (c->have_nl && c->nproj > 0 && nb > 0)
-        if ((rc = dense_apply(c, nl_set(c, filt), psi + (long)band0 * ld, ld, out + (long)band0 * ldo, ldo, nb, st)))
+      if (dense_nl && !sn)
+        if ((rc = dense_apply(c, nl_set(c, filt), psi + (long)band0 * ld, ld, out + (long)band0 * ldo, ldo, nbnl, st)))
           return rc;
       return exchange_batch(c, psi, ld, out, ldo, nband, band0, npair, st, filt);
     }
@@ -1740,10 +1762,11 @@ struct Plan {
 
   // H psi += Q diag(qd) Q^T psi  for nb bands (column-major, ld); Q is the
   // coarse projector matrix or the ACE vectors (qd = -1)
+  // out (+)= Q D Q^T psi: acc 1 accumulates into out, 0 overwrites it
   static int dense_apply(pw_ctx* c, const DenseSet& ds, const T* psi, int ld, T* out, int ldo, int nb,
-                         cudaStream_t st) {
+                         cudaStream_t st, int acc = 1) {
     if constexpr (std::is_same<T, float>::value) {
-      return dense_apply_tc(c, ds, psi, ld, out, ldo, nb, st);
+      return dense_apply_tc(c, ds, psi, ld, out, ldo, nb, st, acc);
     } else {
     cublasHandle_t h = (cublasHandle_t)c->blas;
     if (cublasSetStream(h, st) != CUBLAS_STATUS_SUCCESS) { set_error("cublasSetStream failed"); return PW_ECUDA; }
@@ -1761,7 +1784,7 @@ struct Plan {
     k_scale_rows<T><<<(unsigned)(((long)np * nb + 255) / 256), 256, 0, st>>>(W, reinterpret_cast<const T*>(ds.qd), np, nb); }
     const T* Qs = reinterpret_cast<const T*>(ds.q_st ? ds.q_st : ds.q);
     { Launch L_(c, st, KK_LIBGEMM);
-      r = cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, nt, nb, np, &one, Qs, nt, W, np, &one, out, ldo); }
+      r = cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, nt, nb, np, &one, Qs, nt, W, np, acc ? &one : &zero, out, ldo); }
     if (r != CUBLAS_STATUS_SUCCESS) { set_error("projector GEMM (Q W) failed"); return PW_ECUDA; }
     PWB_CUDA(cudaGetLastError());
     return PW_OK;
@@ -1797,7 +1820,7 @@ struct Plan {
 
   // FP32 context: split-BF16 tcgen05 GEMMs
   static int dense_apply_tc(pw_ctx* c, const DenseSet& ds, const float* psi, int ld, float* out, int ldo, int nb,
-                            cudaStream_t st) {
+                            cudaStream_t st, int acc = 1) {
     const int np = ds.np, nt = (int)c->ntot, npp = ds.npp;
     // bf16 row stride: a multiple of 8 elements (16-byte TMA rows); the tensor
     // maps cover K = nt, so the pad is never read
@@ -1824,7 +1847,7 @@ struct Plan {
     SplitOperand W{wb, wb + (size_t)nb * npp * 2, nb, npp};
     SplitOperand QT{ds.qt_bf, (const char*)ds.qt_bf + (size_t)nt * npp * 2, nt, npp};
     { Launch L_(c, st, KK_GRAM);
-    if ((rc = gemm_tn_store(QT, W, np, c->gemm_terms, out, ldo, 1, st, 1, c->gemm_bn_store))) return rc; }
+    if ((rc = gemm_tn_store(QT, W, np, c->gemm_terms, out, ldo, acc, st, 1, c->gemm_bn_store))) return rc; }
     return PW_OK;
   }
 

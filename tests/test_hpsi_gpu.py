@@ -231,3 +231,29 @@ def test_hpsi_matches_reference_compiled_composition(tag, prec, tol, mode):
     wr = g[f"{tag}_teter"]
     assert np.abs(w - wr).max() / np.abs(wr).max() <= tol
     c.close()
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_projector_overlap_same_result(prec):
+    """The dense projector GEMMs on a second stream beside the FFT chain
+    (pw_set_nl_overlap 1) give the same bits as after it for an overwriting
+    H*psi, and agree to rounding when accumulating; both against the oracle."""
+    import torch
+    T = make_system((16, 16, 16))
+    c = make_ctx(T, prec)
+    psi = pw.random_orthonormal_psi(T.dm.ntot, 7, 31)
+    X = torch.tensor(psi, dtype=c.torch_dtype, device="cuda")
+    out = {}
+    for ov in (0, 1):
+        c.set_nl_overlap(ov)
+        out[ov] = c.hpsi(X).clone()
+        Y = torch.ones_like(X)
+        c.hpsi(X, out=Y, accumulate=True)
+        out[(ov, "acc")] = Y
+    assert torch.equal(out[0], out[1])
+    tol = 1e-12 if prec == "f64" else 1e-6
+    assert float((out[(0, "acc")] - out[(1, "acc")]).abs().max()) <= tol * float(out[(0, "acc")].abs().max())
+    ref = pw.mult_spinor(T, psi)
+    got = out[1].double().cpu().numpy()
+    assert np.abs(got - ref).max() / np.abs(ref).max() <= (1e-12 if prec == "f64" else 1e-5)
+    c.close()
