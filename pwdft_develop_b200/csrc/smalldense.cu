@@ -294,11 +294,77 @@ __global__ void __launch_bounds__(256) k_dgemm_small(int ta, int tb, int m, int 
   }
 }
 
+// the same product for m, n >= 64: 64 x 64 tiles, 16-deep k steps, each
+// thread 4 x 4 outputs (rows ti + 16 a, columns tj + 16 b: the tile reads are
+// one 128-byte row of A and a broadcast of B per warp)
+__global__ void __launch_bounds__(256) k_dgemm_t64(int ta, int tb, int m, int n, int k, const double* A, int lda,
+                                                   const double* B, int ldb, double* C, int ldc) {
+  __shared__ double As[16][65], Bs[16][65];
+  const int i0 = blockIdx.x * 64, j0 = blockIdx.y * 64;
+  const int t = threadIdx.x, ti = t % 16, tj = t / 16;
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+  for (int l0 = 0; l0 < k; l0 += 16) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int idx = t + 256 * q;
+      {
+        // As[l][i] = op(A)(i0 + i, l0 + l), the contiguous index on the fastest threads
+        const int i = ta ? idx / 16 : idx % 64, l = ta ? idx % 16 : idx / 64;
+        const int gi = i0 + i, gl = l0 + l;
+        double v = 0.0;
+        if (gi < m && gl < k) v = ta ? A[(long)gi * lda + gl] : A[(long)gl * lda + gi];
+        As[l][i] = v;
+      }
+      {
+        // Bs[l][j] = op(B)(l0 + l, j0 + j)
+        const int j = tb ? idx % 64 : idx / 16, l = tb ? idx / 64 : idx % 16;
+        const int gl = l0 + l, gj = j0 + j;
+        double v = 0.0;
+        if (gl < k && gj < n) v = tb ? B[(long)gl * ldb + gj] : B[(long)gj * ldb + gl];
+        Bs[l][j] = v;
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int l = 0; l < 16; ++l) {
+      double av[4], bv[4];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) av[a] = As[l][ti + 16 * a];
+#pragma unroll
+      for (int b = 0; b < 4; ++b) bv[b] = Bs[l][tj + 16 * b];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] += av[a] * bv[b];
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int b = 0; b < 4; ++b) {
+    const int j = j0 + tj + 16 * b;
+    if (j >= n) continue;
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      const int i = i0 + ti + 16 * a;
+      if (i < m) C[(long)j * ldc + i] = acc[a][b];
+    }
+  }
+}
+
 int dense_gemm(int ta, int tb, int m, int n, int k, const double* A, int lda, const double* B, int ldb, double* C,
                int ldc, cudaStream_t st) {
   if (m <= 0 || n <= 0) return PW_OK;
-  dim3 grid((m + 31) / 32, (n + 31) / 32);
-  k_dgemm_small<<<grid, 256, 0, st>>>(ta, tb, m, n, k, A, lda, B, ldb, C, ldc);
+  if (m >= 64 && n >= 64) {
+    dim3 grid((m + 63) / 64, (n + 63) / 64);
+    k_dgemm_t64<<<grid, 256, 0, st>>>(ta, tb, m, n, k, A, lda, B, ldb, C, ldc);
+  } else {
+    dim3 grid((m + 31) / 32, (n + 31) / 32);
+    k_dgemm_small<<<grid, 256, 0, st>>>(ta, tb, m, n, k, A, lda, B, ldb, C, ldc);
+  }
   PWB_CUDA(cudaGetLastError());
   return PW_OK;
 }
