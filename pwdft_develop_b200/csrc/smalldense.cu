@@ -358,7 +358,9 @@ __global__ void __launch_bounds__(256) k_dgemm_t64(int ta, int tb, int m, int n,
 int dense_gemm(int ta, int tb, int m, int n, int k, const double* A, int lda, const double* B, int ldb, double* C,
                int ldc, cudaStream_t st) {
   if (m <= 0 || n <= 0) return PW_OK;
-  if (m >= 64 && n >= 64) {
+  // the 64-wide tiles where their grid still covers the SMs (n = 480: 64 CTAs
+  // of 64 x 64 leave most SMs idle and run no faster than 225 of 32 x 32)
+  if (m >= 64 && n >= 64 && (long)((m + 63) / 64) * ((n + 63) / 64) >= 128) {
     dim3 grid((m + 63) / 64, (n + 63) / 64);
     k_dgemm_t64<<<grid, 256, 0, st>>>(ta, tb, m, n, k, A, lda, B, ldb, C, ldc);
   } else {
