@@ -560,8 +560,9 @@ __global__ void __launch_bounds__(256) k_jacobi_vectors(int n, double* A, int ld
 //   3. eigenvectors of T by inverse iteration with each computed eigenvalue
 //      as the shift (LU of T - lambda I with partial pivoting), three solves
 //      per vector, each followed by Gram-Schmidt against the earlier vectors
-//      of its cluster (neighbours closer than 1e-3 ||T||), one warp per
-//      cluster;
+//      of its cluster (neighbours closer than 1e-8 ||T||), one warp per
+//      cluster, then two Loewdin steps on all vectors (described with the
+//      large form below);
 //   4. X = Q Z: the reflectors applied to the columns of Z, 16 threads per
 //      column, no block-wide synchronisation.
 // About 8/3 n^3 flops against ~60 n^3 for ten Jacobi sweeps, and the
@@ -1097,9 +1098,9 @@ __global__ void __launch_bounds__(256) k_trd_back(int n, double* A, int lda, con
 //      ||T|| the residual of a solve), and two symmetric (Loewdin) steps
 //      Z <- Z (3 I - Z^T Z) / 2 make Z orthonormal to rounding.  Mixing two
 //      vectors with coefficient ~ r / gap moves each residual by ~ r, so the
-//      eigenpairs keep their accuracy; the 1e-3 ||T|| clusters of the
-//      one-CTA form chain into sets of hundreds of vectors at these sizes
-//      (LOBPCG's overlap matrices), each solved one after another;
+//      eigenpairs keep their accuracy; the 1e-3 ||T|| clusters of LAPACK's
+//      inverse iteration chain into sets of hundreds of vectors at these
+//      sizes (LOBPCG's overlap matrices), each solved one after another;
 //   4. X = Q Z with one warp per column of Z, the column in registers, the
 //      reflectors applied eight at a time in compact WY form.
 // ---------------------------------------------------------------------------
@@ -1773,7 +1774,7 @@ int dense_syevh(int n, double* A, int lda, double* w, DevBuf& ws, cudaStream_t s
   if (!trd_supported(n)) return dense_syevj(n, A, lda, w, ws, nullptr, st);
   const bool large = n > TRD_NMAX;
   int rc;
-  if ((rc = ws.alloc((large ? trd_ws_large(n) : trd_ws(n)) * sizeof(double)))) return rc;
+  if ((rc = ws.alloc(trd_ws_large(n) * sizeof(double)))) return rc;
   static PerDeviceOnce attr;
   const size_t sm_red = ((size_t)TRD_NMAX * (TRD_NMAX | 1) + 2 * TRD_NMAX) * sizeof(double);
   int optin = 0, dev = 0;
@@ -1797,11 +1798,13 @@ int dense_syevh(int n, double* A, int lda, double* w, DevBuf& ws, cudaStream_t s
   // warps per CTA of the inverse iteration: 6 n doubles each, plus the cluster table
   const size_t per_warp = 6 * (size_t)n * sizeof(double), tab = ((size_t)n + 2) * sizeof(int);
   const int wpc = (int)std::max<size_t>(1, std::min<size_t>(TRD_WARPS_STEIN, ((size_t)optin - tab) / per_warp));
-  const double ortol = large ? 1e-8 : 1e-3;
-  k_trd_stein<<<(n + wpc - 1) / wpc, 32 * wpc, wpc * per_warp + tab, st>>>(n, wsp, ortol);
-  if (large) {
+  // Gram-Schmidt only inside near-degenerate sets, then two Loewdin steps (at
+  // every size: the Rayleigh-Ritz matrices of symmetric cells chain their
+  // 1e-3 ||T|| neighbours into long clusters even at n = 160)
+  k_trd_stein<<<(n + wpc - 1) / wpc, 32 * wpc, wpc * per_warp + tab, st>>>(n, wsp, 1e-8);
+  double* Gm = wsp + trd_ws(n) + 2 * (size_t)n + 2;
+  {
     double* Z = wsp + (size_t)n * n;
-    double* Gm = wsp + trd_ws(n) + 2 * (size_t)n + 2;
     double* Z2 = Gm + (size_t)n * n;
     for (int pass = 0; pass < 2; ++pass) {
       double* zi = pass == 0 ? Z : Z2;
@@ -1810,6 +1813,8 @@ int dense_syevh(int n, double* A, int lda, double* w, DevBuf& ws, cudaStream_t s
       k_lowdin_step<<<n, 128, 0, st>>>(n, Gm);
       if ((rc = dense_gemm(0, 0, n, n, n, zi, n, Gm, n, zo, n, st))) return rc;
     }
+  }
+  if (large) {
     if ((rc = trd_back_large(n, A, lda, wsp, Gm, st))) return rc;   // Gm is free again: the chunks' T
   } else {
     k_trd_back<<<(n + 15) / 16, 256, 0, st>>>(n, A, lda, wsp);
